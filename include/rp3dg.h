@@ -1,0 +1,204 @@
+/*
+ * rp3dg.h -- C ABI of the B200 collision-and-dynamics hot path.
+ *
+ * Everything here is plain C: pointers, sizes and POD structs, no C++ or torch
+ * types.  The library (reactphysics3d_b200/_lib/librp3dg.so) owns all device
+ * memory it allocates; callers own the buffers they pass in.
+ *
+ * Reference interfaces replaced (paths inside ReactPhysics3D v0.10.2):
+ *   - the narrow-phase data contract NarrowPhaseInput / NarrowPhaseInfoBatch
+ *       include/reactphysics3d/collision/narrowphase/NarrowPhaseInput.h:52-160
+ *       include/reactphysics3d/collision/narrowphase/NarrowPhaseInfoBatch.h:48-190
+ *     and the six algorithm entry points
+ *       bool XxxAlgorithm::testCollision(NarrowPhaseInfoBatch&, uint32 start,
+ *                                        uint32 n, [bool clipWithPrevAxis,]
+ *                                        MemoryAllocator&)
+ *       (SphereVsSphereAlgorithm.h:68, SphereVsCapsuleAlgorithm.h:68,
+ *        CapsuleVsCapsuleAlgorithm.h:68, SphereVsConvexPolyhedronAlgorithm.h:70,
+ *        CapsuleVsConvexPolyhedronAlgorithm.h:70,
+ *        ConvexPolyhedronVsConvexPolyhedronAlgorithm.h:68)
+ *   - the temporal-coherence cache LastFrameCollisionInfo
+ *       include/reactphysics3d/engine/OverlappingPairs.h:55-93
+ *   - the per-pair contact output ContactPointInfo
+ *       include/reactphysics3d/collision/ContactPointInfo.h:46-64
+ *
+ * Return convention: 0 on success, a negative RP3DG_E* code on failure;
+ * rp3dg_last_error() gives a message.  The reference reports errors by
+ * assert + log only, so every failure mode here is new and explicit.
+ */
+#ifndef RP3DG_H
+#define RP3DG_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* NB_MAX_CONTACT_POINTS_IN_NARROWPHASE_INFO, configuration.h:109 */
+#define RP3DG_MAX_CONTACTS_PER_PAIR 16
+
+/* error codes */
+#define RP3DG_OK 0
+#define RP3DG_EINVAL -1      /* bad argument (null pointer, unknown algorithm, bad shape) */
+#define RP3DG_ECUDA -2       /* a CUDA runtime call failed */
+#define RP3DG_ENOMEM -3      /* a device allocation failed */
+#define RP3DG_ECAPACITY -4   /* a fixed-capacity table is full */
+#define RP3DG_ENODEV -5      /* no CUDA device */
+
+/* Collision shape kinds.  The reference's CollisionShapeType has SPHERE,
+ * CAPSULE, CONVEX_POLYHEDRON, CONCAVE_SHAPE (CollisionShape.h:49); boxes and
+ * convex meshes are both CONVEX_POLYHEDRON there and are told apart by
+ * CollisionShapeName.  Here the concrete kind is stored directly. */
+enum rp3dg_shape_kind {
+    RP3DG_SHAPE_SPHERE = 0,
+    RP3DG_SHAPE_CAPSULE = 1,
+    RP3DG_SHAPE_BOX = 2,
+    RP3DG_SHAPE_CONVEX_MESH = 3
+};
+
+/* Narrow-phase algorithms, same numbering as the reference's
+ * NarrowPhaseAlgorithmType (CollisionDispatch.h:42-50). */
+enum rp3dg_algorithm {
+    RP3DG_ALGO_NONE = 0,
+    RP3DG_ALGO_SPHERE_VS_SPHERE = 1,
+    RP3DG_ALGO_SPHERE_VS_CAPSULE = 2,
+    RP3DG_ALGO_CAPSULE_VS_CAPSULE = 3,
+    RP3DG_ALGO_SPHERE_VS_CONVEX_POLYHEDRON = 4,
+    RP3DG_ALGO_CAPSULE_VS_CONVEX_POLYHEDRON = 5,
+    RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON = 6
+};
+
+typedef struct rp3dg_float4 { float x, y, z, w; } rp3dg_float4;
+
+/* One collision shape (32 bytes).
+ *   sphere:       params = (radius, 0, 0, 0)
+ *   capsule:      params = (radius, halfHeight, 0, 0)
+ *                 (the reference stores mHalfHeight = height * 0.5,
+ *                  CapsuleShape.cpp:41, and getHeight() = 2 * halfHeight)
+ *   box:          params = (halfExtent.x, .y, .z, 0)
+ *   convex mesh:  params unused; mesh = index returned by
+ *                 rp3dg_create_convex_mesh_shape (mesh + scale instance) */
+typedef struct rp3dg_shape {
+    float params[4];
+    int32_t kind;
+    int32_t mesh;
+    int32_t reserved[2];
+} rp3dg_shape;
+
+/* LastFrameCollisionInfo (OverlappingPairs.h:55-93) packed into 16 bytes. */
+#define RP3DG_LF_IS_VALID        0x01u
+#define RP3DG_LF_WAS_COLLIDING   0x02u
+#define RP3DG_LF_WAS_USING_GJK   0x04u
+#define RP3DG_LF_WAS_USING_SAT   0x08u
+#define RP3DG_LF_SAT_FACE_POLY1  0x10u
+#define RP3DG_LF_SAT_FACE_POLY2  0x20u
+#define RP3DG_LF_IS_OBSOLETE     0x40u
+typedef struct rp3dg_lastframe {
+    float gjk_axis[3];        /* gjkSeparatingAxis, initially (0,1,0) */
+    uint8_t flags;            /* RP3DG_LF_* bits */
+    uint8_t sat_face;         /* satMinAxisFaceIndex */
+    uint8_t sat_edge1;        /* satMinEdge1Index */
+    uint8_t sat_edge2;        /* satMinEdge2Index */
+} rp3dg_lastframe;
+
+/* A batch of pairs for one algorithm, struct-of-arrays.  All pointers are
+ * device pointers for rp3dg_narrowphase_device and host pointers for
+ * rp3dg_narrowphase_host.  pos*.w is ignored; rot* are unit quaternions
+ * stored (x, y, z, w) like the reference's Quaternion. */
+typedef struct rp3dg_pair_batch {
+    uint32_t n;
+    const int32_t* shape1;          /* index into the context's shape table */
+    const int32_t* shape2;
+    const rp3dg_float4* pos1;       /* shape1ToWorldTransform position */
+    const rp3dg_float4* rot1;       /* shape1ToWorldTransform orientation */
+    const rp3dg_float4* pos2;
+    const rp3dg_float4* rot2;
+    const uint8_t* report_contacts; /* NULL: every pair reports contacts */
+    rp3dg_lastframe* cache;         /* in/out; NULL: fresh (isValid=false), not written */
+} rp3dg_pair_batch;
+
+/* Per-pair results.  Contact slot k of pair i lives at index k * n + i
+ * (slot-major, so that consecutive pairs write consecutive addresses).
+ *   normal_depth = (world normal from shape 1 to shape 2, penetration depth)
+ *   local1       = (contact point in shape-1 local space, 0)
+ *   local2       = (contact point in shape-2 local space, 0)
+ * Slots >= nb_contacts[i] are left untouched.  max_contacts (1..16) bounds the
+ * slots the caller allocated; points beyond it are counted in nb_contacts
+ * only up to max_contacts, exactly like the reference's cap of 16. */
+typedef struct rp3dg_contact_batch {
+    uint8_t* is_colliding;
+    uint8_t* nb_contacts;
+    rp3dg_float4* normal_depth;
+    rp3dg_float4* local1;
+    rp3dg_float4* local2;
+    uint32_t max_contacts;
+} rp3dg_contact_batch;
+
+typedef struct rp3dg_ctx rp3dg_ctx;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Create a context on CUDA device `device` with its own stream.
+ * Replaces the PhysicsCommon + world memory managers (MemoryManager.h:72). */
+int rp3dg_create(int device, rp3dg_ctx** out);
+void rp3dg_destroy(rp3dg_ctx* ctx);
+const char* rp3dg_last_error(const rp3dg_ctx* ctx);
+/* cudaStream_t of the context, as void* (for callers that order work). */
+void* rp3dg_stream(rp3dg_ctx* ctx);
+int rp3dg_synchronize(rp3dg_ctx* ctx);
+
+/* ---- shapes (immutable after creation) -------------------------------- */
+
+/* Convex mesh from polygon faces: replaces
+ * PhysicsCommon::createConvexMesh(const PolygonVertexArray&, ...)
+ * (PhysicsCommon.h:214; ConvexMesh::init ConvexMesh.cpp:47-79).  Builds the
+ * half-edge structure (HalfEdgeStructure.cpp:34-127), Newell face normals
+ * (ConvexMesh.cpp:217-240) and the centroid (ConvexMesh.cpp:83-108) on the
+ * host.  vertices: nb_vertices * 3 floats; faces: face_sizes[f] indices each,
+ * concatenated in face_indices.  Returns the mesh id in *mesh_id. */
+int rp3dg_create_convex_mesh(rp3dg_ctx* ctx, const float* vertices, uint32_t nb_vertices,
+                             const uint32_t* face_indices, const uint32_t* face_sizes,
+                             uint32_t nb_faces, int32_t* mesh_id);
+
+/* Convex mesh shape = mesh + scale: replaces
+ * PhysicsCommon::createConvexMeshShape(ConvexMesh*, const Vector3& scaling)
+ * (PhysicsCommon.h:196; scaled normals ConvexMeshShape.cpp:50-70).
+ * Returns the instance id to store in rp3dg_shape.mesh. */
+int rp3dg_create_convex_mesh_shape(rp3dg_ctx* ctx, int32_t mesh_id, float sx, float sy, float sz,
+                                   int32_t* instance_id);
+
+/* Read back the tables built for a mesh instance (for parity checks):
+ * half-edges as 4 uint32 (vertexIndex, twinEdgeIndex, faceIndex,
+ * nextEdgeIndex), face normals (3 floats), face first edge, centroid. */
+int rp3dg_get_convex_mesh_tables(rp3dg_ctx* ctx, int32_t instance_id,
+                                 uint32_t* nb_vertices, uint32_t* nb_faces, uint32_t* nb_half_edges,
+                                 uint32_t* half_edges, float* face_normals, uint32_t* face_edge,
+                                 float* centroid, uint32_t capacity_half_edges, uint32_t capacity_faces);
+
+/* Replace the context's shape table (device copy of `shapes`). */
+int rp3dg_set_shapes(rp3dg_ctx* ctx, const rp3dg_shape* shapes, uint32_t nb_shapes);
+
+/* ---- narrow phase ----------------------------------------------------- */
+
+/* Run one algorithm over a batch whose arrays are already in device memory,
+ * asynchronously on the context stream.  clip_with_previous_axis mirrors the
+ * clipWithPreviousAxisIfStillColliding argument (true in
+ * CollisionDetectionSystem::computeNarrowPhase, false for world queries). */
+int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* pairs,
+                             const rp3dg_contact_batch* out, int clip_with_previous_axis);
+
+/* Same, with every array in host memory: uploads the batch, runs it, copies
+ * the results back and synchronizes.  This is the call a CPU-side engine
+ * would make in place of XxxAlgorithm::testCollision. */
+int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* pairs,
+                           const rp3dg_contact_batch* out, int clip_with_previous_axis);
+
+/* Number of kernels this context launched so far (instrumentation). */
+uint64_t rp3dg_kernel_launches(const rp3dg_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RP3DG_H */

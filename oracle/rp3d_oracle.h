@@ -1,0 +1,38 @@
+/* Test infrastructure, not product code.
+ *
+ * rp3d_oracle: a plain-C restatement of ReactPhysics3D v0.10.2's narrow-phase
+ * algorithms (single precision, one pair at a time, the reference's operation
+ * order) used as a CPU checker for the CUDA library.  It consumes and produces
+ * the struct-of-arrays batches of include/rp3dg.h.  It is pinned against the
+ * reference engine itself (oracle/_ref, built from the reference sources) by
+ * tests/test_oracle_vs_reference.py and against the committed golden fixtures.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
+ */
+#ifndef RP3D_ORACLE_H
+#define RP3D_ORACLE_H
+#include "../include/rp3dg.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Convex mesh from polygon faces (ConvexMesh::init, ConvexMesh.cpp:47-79). */
+int rp3do_create_convex_mesh(const float* vertices, uint32_t nb_vertices, const uint32_t* face_indices,
+                             const uint32_t* face_sizes, uint32_t nb_faces, int32_t* mesh_id);
+/* Mesh + scale (ConvexMeshShape, ConvexMeshShape.cpp:38-70). */
+int rp3do_create_convex_mesh_shape(int32_t mesh_id, float sx, float sy, float sz, int32_t* instance_id);
+int rp3do_get_convex_mesh_tables(int32_t instance_id, uint32_t* nb_vertices, uint32_t* nb_faces,
+                                 uint32_t* nb_half_edges, uint32_t* half_edges, float* face_normals,
+                                 uint32_t* face_edge, float* centroid, uint32_t cap_he, uint32_t cap_faces);
+/* Forget every mesh (tests call it between cases). */
+void rp3do_reset(void);
+
+/* One algorithm over a host batch; same semantics as rp3dg_narrowphase_host. */
+int rp3do_narrowphase(int algorithm, const rp3dg_shape* shapes, uint32_t nb_shapes, const rp3dg_pair_batch* pairs,
+                      const rp3dg_contact_batch* out, int clip_with_previous_axis);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

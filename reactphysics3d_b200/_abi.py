@@ -1,0 +1,109 @@
+"""ctypes mirror of the C ABI in include/rp3dg.h.
+
+The structs here are byte-for-byte the ones the CUDA library exports; the
+numpy helpers build struct-of-arrays pair batches and contact buffers and hand
+their data pointers to the library.  Both the library (`librp3dg.so`) and any
+other shared object exporting the same layout can be driven through them.
+"""
+import ctypes as C
+
+import numpy as np
+
+MAX_CONTACTS = 16  # NB_MAX_CONTACT_POINTS_IN_NARROWPHASE_INFO (configuration.h:109)
+
+SHAPE_SPHERE, SHAPE_CAPSULE, SHAPE_BOX, SHAPE_CONVEX_MESH = 0, 1, 2, 3
+
+ALGO_NONE = 0
+ALGO_SPHERE_VS_SPHERE = 1
+ALGO_SPHERE_VS_CAPSULE = 2
+ALGO_CAPSULE_VS_CAPSULE = 3
+ALGO_SPHERE_VS_CONVEX_POLYHEDRON = 4
+ALGO_CAPSULE_VS_CONVEX_POLYHEDRON = 5
+ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON = 6
+
+LF_IS_VALID = 0x01
+LF_WAS_COLLIDING = 0x02
+LF_WAS_USING_GJK = 0x04
+LF_WAS_USING_SAT = 0x08
+LF_SAT_FACE_POLY1 = 0x10
+LF_SAT_FACE_POLY2 = 0x20
+LF_IS_OBSOLETE = 0x40
+
+SHAPE_DTYPE = np.dtype([("params", "<f4", (4,)), ("kind", "<i4"), ("mesh", "<i4"), ("reserved", "<i4", (2,))])
+CACHE_DTYPE = np.dtype([("gjk_axis", "<f4", (3,)), ("flags", "u1"), ("sat_face", "u1"),
+                        ("sat_edge1", "u1"), ("sat_edge2", "u1")])
+assert SHAPE_DTYPE.itemsize == 32 and CACHE_DTYPE.itemsize == 16
+
+
+class PairBatch(C.Structure):
+    _fields_ = [("n", C.c_uint32),
+                ("shape1", C.c_void_p), ("shape2", C.c_void_p),
+                ("pos1", C.c_void_p), ("rot1", C.c_void_p),
+                ("pos2", C.c_void_p), ("rot2", C.c_void_p),
+                ("report_contacts", C.c_void_p), ("cache", C.c_void_p)]
+
+
+class ContactBatch(C.Structure):
+    _fields_ = [("is_colliding", C.c_void_p), ("nb_contacts", C.c_void_p),
+                ("normal_depth", C.c_void_p), ("local1", C.c_void_p), ("local2", C.c_void_p),
+                ("max_contacts", C.c_uint32)]
+
+
+def fresh_cache(n):
+    """LastFrameCollisionInfo() defaults (OverlappingPairs.h:86-91)."""
+    c = np.zeros(n, dtype=CACHE_DTYPE)
+    c["gjk_axis"][:, 1] = 1.0
+    return c
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+class HostPairs:
+    """A pair batch held in numpy arrays (host memory)."""
+
+    def __init__(self, shape1, shape2, pos1, rot1, pos2, rot2, report=None, cache=None):
+        self.shape1 = np.ascontiguousarray(shape1, dtype=np.int32)
+        self.shape2 = np.ascontiguousarray(shape2, dtype=np.int32)
+        self.pos1 = np.ascontiguousarray(pos1, dtype=np.float32).reshape(-1, 4)
+        self.rot1 = np.ascontiguousarray(rot1, dtype=np.float32).reshape(-1, 4)
+        self.pos2 = np.ascontiguousarray(pos2, dtype=np.float32).reshape(-1, 4)
+        self.rot2 = np.ascontiguousarray(rot2, dtype=np.float32).reshape(-1, 4)
+        self.report = None if report is None else np.ascontiguousarray(report, dtype=np.uint8)
+        self.cache = None if cache is None else np.ascontiguousarray(cache, dtype=CACHE_DTYPE)
+
+    @property
+    def n(self):
+        return int(self.shape1.shape[0])
+
+    def slice(self, begin, end):
+        return HostPairs(self.shape1[begin:end], self.shape2[begin:end], self.pos1[begin:end],
+                         self.rot1[begin:end], self.pos2[begin:end], self.rot2[begin:end],
+                         None if self.report is None else self.report[begin:end],
+                         None if self.cache is None else self.cache[begin:end].copy())
+
+    def struct(self):
+        return PairBatch(self.n, _ptr(self.shape1), _ptr(self.shape2), _ptr(self.pos1), _ptr(self.rot1),
+                         _ptr(self.pos2), _ptr(self.rot2), _ptr(self.report), _ptr(self.cache))
+
+
+class HostContacts:
+    """Per-pair narrow-phase results in host memory (slot-major contacts)."""
+
+    def __init__(self, n, max_contacts=MAX_CONTACTS):
+        self.n = n
+        self.max_contacts = max_contacts
+        self.is_colliding = np.zeros(n, dtype=np.uint8)
+        self.nb_contacts = np.zeros(n, dtype=np.uint8)
+        self.normal_depth = np.zeros((max_contacts, n, 4), dtype=np.float32)
+        self.local1 = np.zeros((max_contacts, n, 4), dtype=np.float32)
+        self.local2 = np.zeros((max_contacts, n, 4), dtype=np.float32)
+
+    def struct(self):
+        return ContactBatch(_ptr(self.is_colliding), _ptr(self.nb_contacts), _ptr(self.normal_depth),
+                            _ptr(self.local1), _ptr(self.local2), self.max_contacts)
+
+    def valid_mask(self):
+        """Boolean [max_contacts, n] mask of the slots that hold a contact."""
+        return np.arange(self.max_contacts)[:, None] < self.nb_contacts[None, :]

@@ -1,0 +1,181 @@
+"""Seeded synthetic workloads for the narrow-phase hot path.
+
+The narrow-phase microbenchmark draws 1,048,576 shape pairs split over seven
+algorithm batches (sphere-sphere, sphere-capsule, capsule-capsule, sphere-box,
+capsule-box, box-box, convex hull-box).  Sizes, value ranges and the pair
+placement rule are those of the reference workload description: relative
+orientation uniform, centre offset direction uniform on the sphere with
+length U[0.5, 1.5] x (sum of bounding radii), so about half the pairs touch.
+All values are drawn with numpy's PCG64 from a recorded seed and stored as
+float32, so every engine that consumes them sees identical bytes.
+"""
+import json
+import os
+
+import numpy as np
+
+from . import _abi as A
+
+BATCH_NAMES = ("sphere_sphere", "sphere_capsule", "capsule_capsule", "sphere_box",
+               "capsule_box", "box_box", "hull_box")
+BATCH_ALGO = {
+    "sphere_sphere": A.ALGO_SPHERE_VS_SPHERE,
+    "sphere_capsule": A.ALGO_SPHERE_VS_CAPSULE,
+    "capsule_capsule": A.ALGO_CAPSULE_VS_CAPSULE,
+    "sphere_box": A.ALGO_SPHERE_VS_CONVEX_POLYHEDRON,
+    "capsule_box": A.ALGO_CAPSULE_VS_CONVEX_POLYHEDRON,
+    "box_box": A.ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON,
+    "hull_box": A.ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON,
+}
+TOTAL_PAIRS = 1_048_576
+
+REPO_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+# Reference QuickHull output for icosphere42_points(); written by tests/golden/make_golden.py.
+HULL_FILE = os.path.join(REPO_ROOT, "tests", "golden", "hull42.json")
+
+
+def batch_sizes(total=TOTAL_PAIRS, nb=7):
+    """Even split with the remainder given to the first batches (149,796 each + 4 extra)."""
+    base, rem = divmod(total, nb)
+    return [base + (1 if i < rem else 0) for i in range(nb)]
+
+
+def random_quaternions(rng, n):
+    """Uniform unit quaternions (Shoemake), returned as float32 (x, y, z, w)."""
+    u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)
+    a, b = np.sqrt(1.0 - u1), np.sqrt(u1)
+    q = np.stack([a * np.sin(2 * np.pi * u2), a * np.cos(2 * np.pi * u2),
+                  b * np.sin(2 * np.pi * u3), b * np.cos(2 * np.pi * u3)], axis=1)
+    return q.astype(np.float32)
+
+
+def random_unit_vectors(rng, n):
+    v = rng.normal(size=(n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def icosphere42_points(seed=7, radius=0.8, noise=0.05):
+    """42-vertex once-subdivided icosahedron of the given radius, each vertex
+    pushed radially by U[-noise, noise] (relative)."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t),
+         (0, -1, -t), (0, 1, -t), (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4),
+         (11, 10, 2), (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8),
+         (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    pts = [np.array(p, dtype=np.float64) for p in v]
+    mid = {}
+    for a, b, c in f:
+        for i, j in ((a, b), (b, c), (c, a)):
+            key = (min(i, j), max(i, j))
+            if key not in mid:
+                mid[key] = len(pts)
+                pts.append((pts[i] + pts[j]) / 2.0)
+    p = np.array(pts)
+    p /= np.linalg.norm(p, axis=1, keepdims=True)
+    rng = np.random.default_rng(seed)
+    scale = radius * (1.0 + rng.uniform(-noise, noise, size=len(p)))
+    return (p * scale[:, None]).astype(np.float32)
+
+
+def load_hull():
+    """The hull used by the hull-box batch: vertices and polygon faces as
+    produced by the reference's QuickHull on icosphere42_points()."""
+    with open(HULL_FILE) as fh:
+        d = json.load(fh)
+    vertices = np.array(d["vertices"], dtype=np.float32).reshape(-1, 3)
+    faces = [list(map(int, f)) for f in d["faces"]]
+    return vertices, faces
+
+
+def _bounding_radius(kind, params, hull_radius):
+    if kind == A.SHAPE_SPHERE:
+        return params[:, 0]
+    if kind == A.SHAPE_CAPSULE:
+        return params[:, 0] + params[:, 1]
+    if kind == A.SHAPE_BOX:
+        return np.linalg.norm(params[:, :3], axis=1)
+    return np.full(params.shape[0], hull_radius, dtype=np.float64)
+
+
+def _draw_shapes(rng, kind, n):
+    p = np.zeros((n, 4), dtype=np.float32)
+    if kind == A.SHAPE_SPHERE:
+        p[:, 0] = rng.uniform(0.2, 1.0, n)
+    elif kind == A.SHAPE_CAPSULE:
+        p[:, 0] = rng.uniform(0.2, 0.5, n)
+        p[:, 1] = rng.uniform(0.3, 1.0, n)
+    elif kind == A.SHAPE_BOX:
+        p[:, :3] = rng.uniform(0.2, 1.0, (n, 3))
+    return p
+
+
+BATCH_KINDS = {
+    "sphere_sphere": (A.SHAPE_SPHERE, A.SHAPE_SPHERE),
+    "sphere_capsule": (A.SHAPE_SPHERE, A.SHAPE_CAPSULE),
+    "capsule_capsule": (A.SHAPE_CAPSULE, A.SHAPE_CAPSULE),
+    "sphere_box": (A.SHAPE_SPHERE, A.SHAPE_BOX),
+    "capsule_box": (A.SHAPE_CAPSULE, A.SHAPE_BOX),
+    "box_box": (A.SHAPE_BOX, A.SHAPE_BOX),
+    "hull_box": (A.SHAPE_CONVEX_MESH, A.SHAPE_BOX),
+}
+
+
+class NarrowphaseScene:
+    """Shapes + per-batch pair arrays for the narrow-phase microbenchmark.
+
+    shapes: structured array (rp3dg_shape) holding every shape of every batch.
+    batches: dict name -> (algorithm, HostPairs) in BATCH_NAMES order.
+    Hull shapes reference convex-mesh instance 0 (the caller registers the
+    hull returned by load_hull() once, scale (1,1,1))."""
+
+    def __init__(self, shapes, batches, hull_vertices, hull_faces, seed):
+        self.shapes = shapes
+        self.batches = batches
+        self.hull_vertices = hull_vertices
+        self.hull_faces = hull_faces
+        self.seed = seed
+
+    @property
+    def n_pairs(self):
+        return sum(p.n for _, p in self.batches.values())
+
+
+def narrowphase_scene(total_pairs=TOTAL_PAIRS, seed=1234, names=BATCH_NAMES, position_range=10.0,
+                      hull=None):
+    rng = np.random.default_rng(seed)
+    hull_vertices, hull_faces = hull if hull is not None else load_hull()
+    hull_radius = float(np.max(np.linalg.norm(hull_vertices.astype(np.float64), axis=1)))
+    sizes = batch_sizes(total_pairs, len(BATCH_NAMES))
+    all_shapes = []
+    batches = {}
+    base = 0
+    for name, n in zip(BATCH_NAMES, sizes):
+        if name not in names:
+            continue
+        k1, k2 = BATCH_KINDS[name]
+        p1, p2 = _draw_shapes(rng, k1, n), _draw_shapes(rng, k2, n)
+        sh = np.zeros(2 * n, dtype=A.SHAPE_DTYPE)
+        sh["params"][0::2] = p1
+        sh["params"][1::2] = p2
+        sh["kind"][0::2] = k1
+        sh["kind"][1::2] = k2
+        sh["mesh"] = -1
+        sh["mesh"][0::2] = 0 if k1 == A.SHAPE_CONVEX_MESH else -1
+        sh["mesh"][1::2] = 0 if k2 == A.SHAPE_CONVEX_MESH else -1
+        r = (_bounding_radius(k1, p1.astype(np.float64), hull_radius)
+             + _bounding_radius(k2, p2.astype(np.float64), hull_radius))
+        q1, q2 = random_quaternions(rng, n), random_quaternions(rng, n)
+        c1 = rng.uniform(-position_range, position_range, (n, 3))
+        d = random_unit_vectors(rng, n) * (rng.uniform(0.5, 1.5, n) * r)[:, None]
+        pos1 = np.zeros((n, 4), np.float32)
+        pos2 = np.zeros((n, 4), np.float32)
+        pos1[:, :3] = c1
+        pos2[:, :3] = c1 + d
+        idx = base + 2 * np.arange(n, dtype=np.int64)
+        pairs = A.HostPairs(idx, idx + 1, pos1, q1, pos2, q2)
+        batches[name] = (BATCH_ALGO[name], pairs)
+        all_shapes.append(sh)
+        base += 2 * n
+    shapes = np.concatenate(all_shapes) if all_shapes else np.zeros(0, A.SHAPE_DTYPE)
+    return NarrowphaseScene(shapes, batches, hull_vertices, hull_faces, seed)

@@ -1,0 +1,190 @@
+"""Loader for the oracles (test infrastructure).
+
+- oracle/_ref/librp3d_ref_{f32,f64}.so: the reference engine itself, built
+  from its sources by oracle/Makefile, driven through oracle/ref_harness.cpp.
+- oracle/librp3d_oracle.so: the C restatement (oracle/rp3d_oracle.c).
+Both take the rp3dg.h struct-of-arrays batches."""
+import ctypes as C
+import os
+
+import numpy as np
+
+from reactphysics3d_b200 import _abi as A
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+REF_LIB = {"f32": os.path.join(ORACLE_DIR, "_ref", "librp3d_ref_f32.so"),
+           "f64": os.path.join(ORACLE_DIR, "_ref", "librp3d_ref_f64.so")}
+PORT_LIB = os.path.join(ORACLE_DIR, "librp3d_oracle.so")
+
+
+def have_ref(prec="f32"):
+    return os.path.exists(REF_LIB[prec])
+
+
+class RefEngine:
+    """The reference's own narrow-phase algorithms (FP32 or FP64 build)."""
+
+    def __init__(self, prec="f32"):
+        self.lib = C.CDLL(REF_LIB[prec])
+        L = self.lib
+        L.ref_narrowphase.argtypes = [C.c_int, C.c_void_p, C.c_uint32, C.POINTER(A.PairBatch),
+                                      C.POINTER(A.ContactBatch), C.c_int, C.c_int, C.c_int,
+                                      C.POINTER(C.c_double)]
+        L.ref_create_convex_mesh.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32,
+                                             C.POINTER(C.c_int32)]
+        L.ref_create_convex_mesh_shape.argtypes = [C.c_int32, C.c_float, C.c_float, C.c_float,
+                                                   C.POINTER(C.c_int32)]
+        L.ref_get_convex_mesh_tables.argtypes = [C.c_int32] + [C.c_void_p] * 8 + [C.c_uint32, C.c_uint32]
+        L.ref_quickhull.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                    C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p]
+
+    def create_convex_mesh(self, vertices, faces):
+        v = np.ascontiguousarray(vertices, dtype=np.float32)
+        idx = np.ascontiguousarray(np.concatenate([np.asarray(f, np.uint32) for f in faces]), dtype=np.uint32)
+        sizes = np.array([len(f) for f in faces], dtype=np.uint32)
+        out = C.c_int32()
+        rc = self.lib.ref_create_convex_mesh(v.ctypes.data, len(v), idx.ctypes.data, sizes.ctypes.data,
+                                             len(faces), C.byref(out))
+        assert rc == 0, rc
+        return out.value
+
+    def create_convex_mesh_shape(self, mesh, scale=(1.0, 1.0, 1.0)):
+        out = C.c_int32()
+        rc = self.lib.ref_create_convex_mesh_shape(mesh, *map(float, scale), C.byref(out))
+        assert rc == 0, rc
+        return out.value
+
+    def mesh_tables(self, instance, cap=4096):
+        nv, nf, nh = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        he = np.zeros(4 * cap, np.uint32)
+        fn = np.zeros(3 * cap, np.float32)
+        fe = np.zeros(cap, np.uint32)
+        cen = np.zeros(3, np.float32)
+        verts = np.zeros(3 * cap, np.float32)
+        rc = self.lib.ref_get_convex_mesh_tables(instance, C.addressof(nv), C.addressof(nf), C.addressof(nh),
+                                                 he.ctypes.data, fn.ctypes.data, fe.ctypes.data,
+                                                 cen.ctypes.data, verts.ctypes.data, cap, cap)
+        assert rc == 0, rc
+        return dict(half_edges=he[:4 * nh.value].reshape(-1, 4), face_normals=fn[:3 * nf.value].reshape(-1, 3),
+                    face_edge=fe[:nf.value], centroid=cen, vertices=verts[:3 * nv.value].reshape(-1, 3))
+
+    def quickhull(self, points):
+        p = np.ascontiguousarray(points, dtype=np.float32)
+        cap = 4096
+        ov = np.zeros(3 * cap, np.float32)
+        oi = np.zeros(4 * cap, np.uint32)
+        osz = np.zeros(cap, np.uint32)
+        nv, nf = C.c_uint32(), C.c_uint32()
+        rc = self.lib.ref_quickhull(p.ctypes.data, len(p), ov.ctypes.data, cap, C.addressof(nv), oi.ctypes.data,
+                                    4 * cap, osz.ctypes.data, cap, C.addressof(nf))
+        assert rc == 0, rc
+        verts = ov[:3 * nv.value].reshape(-1, 3).copy()
+        faces, k = [], 0
+        for s in osz[:nf.value]:
+            faces.append([int(x) for x in oi[k:k + s]])
+            k += int(s)
+        return verts, faces
+
+    def narrowphase(self, algo, shapes, pairs, out=None, clip=True, nthreads=1, repeats=1):
+        """Run the reference algorithm; returns (HostContacts, seconds)."""
+        if out is None:
+            out = A.HostContacts(pairs.n)
+        sh = np.ascontiguousarray(shapes)
+        pb, cb = pairs.struct(), out.struct()
+        sec = C.c_double()
+        rc = self.lib.ref_narrowphase(algo, sh.ctypes.data, len(sh), C.byref(pb), C.byref(cb), int(clip),
+                                      nthreads, repeats, C.byref(sec))
+        assert rc == 0, rc
+        return out, sec.value
+
+
+class PortEngine:
+    """The C restatement (oracle/rp3d_oracle.c) with the RefEngine interface."""
+
+    def __init__(self):
+        self.lib = C.CDLL(PORT_LIB)
+        L = self.lib
+        L.rp3do_narrowphase.argtypes = [C.c_int, C.c_void_p, C.c_uint32, C.POINTER(A.PairBatch),
+                                        C.POINTER(A.ContactBatch), C.c_int]
+        L.rp3do_create_convex_mesh.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32,
+                                               C.POINTER(C.c_int32)]
+        L.rp3do_create_convex_mesh_shape.argtypes = [C.c_int32, C.c_float, C.c_float, C.c_float,
+                                                     C.POINTER(C.c_int32)]
+        L.rp3do_get_convex_mesh_tables.argtypes = [C.c_int32] + [C.c_void_p] * 7 + [C.c_uint32, C.c_uint32]
+        L.rp3do_reset()
+
+    def create_convex_mesh(self, vertices, faces):
+        v = np.ascontiguousarray(vertices, dtype=np.float32)
+        idx = np.ascontiguousarray(np.concatenate([np.asarray(f, np.uint32) for f in faces]), dtype=np.uint32)
+        sizes = np.array([len(f) for f in faces], dtype=np.uint32)
+        out = C.c_int32()
+        rc = self.lib.rp3do_create_convex_mesh(v.ctypes.data, len(v), idx.ctypes.data, sizes.ctypes.data,
+                                               len(faces), C.byref(out))
+        assert rc == 0, rc
+        return out.value
+
+    def create_convex_mesh_shape(self, mesh, scale=(1.0, 1.0, 1.0)):
+        out = C.c_int32()
+        rc = self.lib.rp3do_create_convex_mesh_shape(mesh, *map(float, scale), C.byref(out))
+        assert rc == 0, rc
+        return out.value
+
+    def mesh_tables(self, instance, cap=4096):
+        nv, nf, nh = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        he = np.zeros(4 * cap, np.uint32)
+        fn = np.zeros(3 * cap, np.float32)
+        fe = np.zeros(cap, np.uint32)
+        cen = np.zeros(3, np.float32)
+        rc = self.lib.rp3do_get_convex_mesh_tables(instance, C.addressof(nv), C.addressof(nf), C.addressof(nh),
+                                                   he.ctypes.data, fn.ctypes.data, fe.ctypes.data, cen.ctypes.data,
+                                                   cap, cap)
+        assert rc == 0, rc
+        return dict(half_edges=he[:4 * nh.value].reshape(-1, 4), face_normals=fn[:3 * nf.value].reshape(-1, 3),
+                    face_edge=fe[:nf.value], centroid=cen)
+
+    def narrowphase(self, algo, shapes, pairs, out=None, clip=True):
+        if out is None:
+            out = A.HostContacts(pairs.n)
+        sh = np.ascontiguousarray(shapes)
+        pb, cb = pairs.struct(), out.struct()
+        rc = self.lib.rp3do_narrowphase(algo, sh.ctypes.data, len(sh), C.byref(pb), C.byref(cb), int(clip))
+        assert rc == 0, rc
+        return out, 0.0
+
+
+def compare_contacts(a, b, pairs_n):
+    """Bit-level comparison of two HostContacts; returns a dict of mismatch counts."""
+    res = {"is_colliding": int(np.sum(a.is_colliding != b.is_colliding)),
+           "nb_contacts": int(np.sum(a.nb_contacts != b.nb_contacts))}
+    same_nb = a.nb_contacts == b.nb_contacts
+    mask = a.valid_mask() & same_nb[None, :]
+    for f in ("normal_depth", "local1", "local2"):
+        x = getattr(a, f).view(np.uint32)[mask]
+        y = getattr(b, f).view(np.uint32)[mask]
+        res[f] = int(np.sum(np.any(x != y, axis=-1)))
+    return res
+
+
+def perturb_pairs(pairs, rng, dpos=0.02, drot=0.02):
+    """Small pose changes between two passes (exercises the temporal-coherence
+    branches).  Quaternions are re-normalised in float64 then stored as float32."""
+    q = A.HostPairs(pairs.shape1, pairs.shape2, pairs.pos1.copy(), pairs.rot1.copy(), pairs.pos2.copy(),
+                    pairs.rot2.copy(), pairs.report, None if pairs.cache is None else pairs.cache.copy())
+    n = pairs.n
+    q.pos2[:, :3] += rng.uniform(-dpos, dpos, (n, 3)).astype(np.float32)
+    r = q.rot2.astype(np.float64) + rng.uniform(-drot, drot, (n, 4))
+    q.rot2[:] = (r / np.linalg.norm(r, axis=1, keepdims=True)).astype(np.float32)
+    return q
+
+
+def next_frame_cache(cache, out):
+    """What the reference's collision detection does to a pair's cache between
+    frames: the info becomes valid and remembers whether the pair collided
+    (CollisionDetectionSystem::processPotentialContacts and
+    OverlappingPairs::addLastFrameInfoIfNecessary)."""
+    c = cache.copy()
+    c["flags"] |= A.LF_IS_VALID
+    c["flags"] &= ~np.uint8(A.LF_WAS_COLLIDING)
+    c["flags"] |= np.where(out.is_colliding != 0, A.LF_WAS_COLLIDING, 0).astype(np.uint8)
+    return c
