@@ -1,0 +1,345 @@
+"""Narrow-phase microbenchmark: 1,048,576 shape pairs in seven algorithm
+batches (sphere-sphere, sphere-capsule, capsule-capsule, sphere-box,
+capsule-box, box-box, hull-box), FP32, seeded synthetic inputs.
+
+One step = one pass of the six ReactPhysics3D narrow-phase algorithms over
+the whole pair set (seven kernel launches, one per batch), inputs resident in
+device memory, L2 flushed between steps.  Each rank runs its own pair set
+(pairs are independent: weak scaling, no data-path collective).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `--impl reference` times the reference
+engine's own CPU algorithms (built from its sources into oracle/_ref) on the
+host cores over a bounded sample of the same workload.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from reactphysics3d_b200 import _abi as A  # noqa: E402
+from reactphysics3d_b200 import scenes  # noqa: E402
+
+METRIC = "narrowphase pairs/sec"
+UNIT = "pairs/s"
+WORKLOAD = "narrowphase microbenchmark: 1,048,576 pairs in 7 algorithm batches (FP32)"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def peaks():
+    try:
+        with open(PEAKS_FILE) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# Algorithmic bytes per pair (unit of the HBM roofline): inputs read
+# (shape indices 8 B + two shape records 64 B + four float4 transform rows
+# 64 B) + outputs written (flag + count 2 B + 48 B per reported contact).
+IN_BYTES_PER_PAIR = 8 + 64 + 64
+
+
+def run_ours(args):
+    import torch
+    from reactphysics3d_b200 import engine
+
+    rank, local_rank, world = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
+
+    sc = scenes.narrowphase_scene(total_pairs=args.pairs, seed=args.seed + rank)
+    ctx = engine.Context(local_rank)
+    mesh = ctx.create_convex_mesh(sc.hull_vertices, sc.hull_faces)
+    ctx.create_convex_mesh_shape(mesh)
+    ctx.set_shapes(sc.shapes)
+    names = list(sc.batches.keys())
+    dpairs = {nm: engine.DevicePairs(sc.batches[nm][1], device=dev) for nm in names}
+    douts = {nm: engine.DeviceContacts(sc.batches[nm][1].n, device=dev) for nm in names}
+    algos = {nm: sc.batches[nm][0] for nm in names}
+    stream = ctx.torch_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+
+    def one_step(evs=None):
+        for k, nm in enumerate(names):
+            if evs is not None:
+                evs[k][0].record(stream)
+            ctx.narrowphase_device(algos[nm], dpairs[nm], douts[nm])
+            if evs is not None:
+                evs[k][1].record(stream)
+
+    for _ in range(args.warmup):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        one_step()
+    ctx.synchronize()
+
+    sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local_rank)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    launches0 = ctx.kernel_launches()
+    step_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    batch_ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in names]
+                for _ in range(args.steps)]
+    for s in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        step_ev[s][0].record(stream)
+        one_step(batch_ev[s])
+        step_ev[s][1].record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    launches = ctx.kernel_launches() - launches0
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in step_ev]
+    batch_ms = {nm: [batch_ev[s][k][0].elapsed_time(batch_ev[s][k][1]) for s in range(args.steps)]
+                for k, nm in enumerate(names)}
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    pairs_total = sc.n_pairs * world
+    value = pairs_total / (ms_per_step / 1e3)
+
+    # ---- per-kernel roofline of the dominant kernel ----------------------
+    mean_batch = {nm: float(np.mean(v)) for nm, v in batch_ms.items()}
+    dom = max(mean_batch, key=mean_batch.get)
+    host_out = {nm: douts[nm].nb_contacts.cpu().numpy() for nm in names}
+    n_dom = sc.batches[dom][1].n
+    contacts_dom = int(host_out[dom].astype(np.int64).sum())
+    alg_bytes = n_dom * (IN_BYTES_PER_PAIR + 2) + contacts_dom * 48
+    hbm_peak, peak_src = peaks()
+    achieved = alg_bytes / (mean_batch[dom] / 1e3) / 1e9
+    share = {nm: round(mean_batch[nm] / sum(mean_batch.values()), 4) for nm in names}
+    roofline = {"bound": "hbm", "kernel": f"narrowphase_kernel<{algos[dom]}> ({dom})", "achieved": round(achieved, 2),
+                "peak": hbm_peak, "unit": "GB/s", "frac": round(achieved / hbm_peak, 5), "traffic": None,
+                "peak_source": peak_src, "kernel_ms": round(mean_batch[dom], 4), "share": share,
+                "note": "FP32 SAT/GJK kernels are issue/latency-bound; HBM fraction is reported because no "
+                        "FP32 CUDA-core peak is in MEASURED_PEAKS.json"}
+    if args.traffic_bytes:
+        roofline["traffic"] = args.traffic_bytes
+
+    # ---- end to end through the host-memory C-ABI call -------------------
+    e2e = None
+    if not args.no_e2e:
+        pinned = {}
+        for nm in names:
+            hp = sc.batches[nm][1]
+            pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+            pp = A.HostPairs(pin(hp.shape1), pin(hp.shape2), pin(hp.pos1), pin(hp.rot1), pin(hp.pos2), pin(hp.rot2))
+            ho = A.HostContacts(hp.n)
+            for f in ("is_colliding", "nb_contacts", "normal_depth", "local1", "local2"):
+                setattr(ho, f, torch.from_numpy(getattr(ho, f)).pin_memory().numpy())
+            pinned[nm] = (pp, ho)
+        for _ in range(max(1, args.warmup)):
+            for nm in names:
+                ctx.narrowphase_host(algos[nm], *pinned[nm])
+        h2d = sum(p.shape1.nbytes + p.shape2.nbytes + p.pos1.nbytes + p.rot1.nbytes + p.pos2.nbytes + p.rot2.nbytes
+                  for p, _ in pinned.values())
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            for nm in names:
+                ctx.narrowphase_host(algos[nm], *pinned[nm])
+        e2e_s = (time.perf_counter() - t0) / args.steps
+        d2h = 0
+        for nm in names:
+            _, ho = pinned[nm]
+            used = int(ho.nb_contacts.max())
+            d2h += 2 * ho.n + 3 * used * ho.n * 16
+        e2e_val = sc.n_pairs / e2e_s
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([e2e_s], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_val = pairs_total / float(t.item())
+        e2e = {"value": round(e2e_val, 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_s * 1e3, 4),
+               "api": "rp3dg_narrowphase_host (pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(sc, args)
+
+    line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "pairs_per_gpu": sc.n_pairs, "batches": names,
+                       "seed": args.seed, "l2": "flushed between steps (256 MB write)",
+                       "parallelism": f"independent pair sets per rank x{world}"},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": int(launches),
+            "clocks": clocks, "batch_ms": {k: round(v, 4) for k, v in mean_batch.items()}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _reference_engine():
+    """The reference's own algorithms (oracle/_ref, built from its sources);
+    the C restatement (oracle/librp3d_oracle.so) when the reference build is
+    absent.  Returns (engine, kind)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import reflib
+    if reflib.have_ref("f32"):
+        return reflib.RefEngine("f32"), "reference"
+    if not os.path.exists(reflib.PORT_LIB):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True, stdout=subprocess.DEVNULL)
+    return reflib.PortEngine(), "port"
+
+
+def _threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(sc, args, sample_frac=None, repeats=1):
+    """Time the reference engine's algorithms on the host cores over a bounded
+    sample (every batch cut to the same fraction) of the workload."""
+    eng, kind = _reference_engine()
+    m = eng.create_convex_mesh(sc.hull_vertices, sc.hull_faces)
+    eng.create_convex_mesh_shape(m)
+    threads = _threads() if kind == "reference" else 1
+    frac = sample_frac if sample_frac is not None else args.cpu_sample
+    total_pairs, total_s = 0, 0.0
+    for nm, (algo, pairs) in sc.batches.items():
+        k = max(threads, int(pairs.n * frac))
+        sub = pairs.slice(0, k)
+        if kind == "reference":
+            _, sec = eng.narrowphase(algo, sc.shapes, sub, nthreads=threads, repeats=repeats)
+        else:
+            t0 = time.perf_counter()
+            eng.narrowphase(algo, sc.shapes, sub)
+            sec = time.perf_counter() - t0
+        total_pairs += k
+        total_s += sec
+    return {"value": round(total_pairs / total_s, 1), "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"first {frac:.0%} of every batch ({total_pairs} pairs), testCollision on pre-filled "
+                      f"NarrowPhaseInfoBatch, one batch slice per thread",
+            "seconds": round(total_s, 3)}
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    sc = scenes.narrowphase_scene(total_pairs=args.pairs, seed=args.seed)
+    vals = []
+    base = None
+    for s in range(args.warmup + args.steps):
+        r = cpu_baseline(sc, args, repeats=1)
+        if s >= args.warmup:
+            vals.append(r["value"])
+            base = r
+    value = float(np.mean(vals))
+    base["value"] = round(value, 1)
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * args.pairs / value, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "pairs_per_gpu": args.pairs, "seed": args.seed,
+                       "sample": base["sample"]},
+            "cpu_baseline": base,
+            "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--pairs", type=int, default=scenes.TOTAL_PAIRS)
+    ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--cpu-sample", type=float, default=0.25)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--traffic-bytes", type=float, default=None)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -191,9 +191,18 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
 
 /* Same, with every array in host memory: uploads the batch, runs it, copies
  * the results back and synchronizes.  This is the call a CPU-side engine
- * would make in place of XxxAlgorithm::testCollision. */
+ * would make in place of XxxAlgorithm::testCollision.  Only the contact slots
+ * some pair of the batch uses are copied back; slot k >= nb_contacts[i] of
+ * pair i holds unspecified values afterwards.  Pinned host buffers make the
+ * copies asynchronous DMA transfers. */
 int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* pairs,
                            const rp3dg_contact_batch* out, int clip_with_previous_axis);
+
+/* Device-side error bits accumulated by the kernels since the last clear
+ * (bit 0: a pair named a shape outside the shape table; such pairs are
+ * reported as not colliding; bit 1: a GJK run hit the 1024-iteration safety
+ * bound).  Synchronizes the context stream. */
+int rp3dg_device_errors(rp3dg_ctx* ctx, uint32_t* flags, int clear);
 
 /* Number of kernels this context launched so far (instrumentation). */
 uint64_t rp3dg_kernel_launches(const rp3dg_ctx* ctx);

@@ -1,0 +1,189 @@
+// Narrow-phase kernels: one launch per algorithm batch, one pair per thread.
+// Pair inputs are struct-of-arrays (float4 transforms, int32 shape indices),
+// outputs are slot-major so consecutive pairs write consecutive addresses.
+// Convex-mesh tables (half-edges, faces, normals, vertices) are staged in
+// shared memory once per CTA; the box topology comes from constant memory.
+#include <cuda_runtime.h>
+
+#include "narrowphase.cuh"
+#include "np_launch.h"
+
+namespace rp3dg {
+
+__constant__ BoxTables c_box_tables;
+
+void upload_box_tables(const BoxTables& t, cudaStream_t s) {
+    cudaMemcpyToSymbolAsync(c_box_tables, &t, sizeof(BoxTables), 0, cudaMemcpyHostToDevice, s);
+}
+
+struct ShapeRec {
+    float4 params;
+    int kind, mesh;
+};
+
+RD ShapeRec load_shape(const rp3dg_shape* shapes, int32_t idx) {
+    const float4* p = reinterpret_cast<const float4*>(shapes + idx);
+    const int4* k = reinterpret_cast<const int4*>(shapes + idx) + 1;
+    ShapeRec s;
+    s.params = __ldg(p);
+    const int4 kk = __ldg(k);
+    s.kind = kk.x;
+    s.mesh = kk.y;
+    return s;
+}
+
+RD MeshPoly mesh_poly(const uint32_t* words, int32_t inst) {
+    MeshPoly m;
+    m.h = reinterpret_cast<const MeshHdr*>(words) + inst;
+    m.w = words;
+    return m;
+}
+
+RD BoxPoly box_poly(const ShapeRec& s, const BoxTables* t) {
+    BoxPoly b;
+    b.he = V(s.params.x, s.params.y, s.params.z);
+    b.t = t;
+    return b;
+}
+
+template <int ALGO>
+RD void process_pair(const NpArgs& a, uint32_t i, const BoxTables* box, const uint32_t* mesh_words) {
+    const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
+    if (uint32_t(i1) >= a.nb_shapes || uint32_t(i2) >= a.nb_shapes) {
+        // a pair naming a shape outside the table is reported as not colliding
+        a.is_colliding[i] = 0;
+        a.nb_contacts[i] = 0;
+        atomicOr(a.error, 1u);
+        return;
+    }
+    const ShapeRec s1 = load_shape(a.shapes, i1);
+    const ShapeRec s2 = load_shape(a.shapes, i2);
+    Item it;
+    {
+        const float4 p1 = a.pos1[i], q1 = a.rot1[i], p2 = a.pos2[i], q2 = a.rot2[i];
+        it.t1 = X(V(p1.x, p1.y, p1.z), Q(q1.x, q1.y, q1.z, q1.w));
+        it.t2 = X(V(p2.x, p2.y, p2.z), Q(q2.x, q2.y, q2.z, q2.w));
+    }
+    it.report = a.report ? a.report[i] != 0 : true;
+    it.colliding = false;
+    it.gjk_capped = false;
+    if (a.cache) {
+        const uint4 c = reinterpret_cast<const uint4*>(a.cache)[i];
+        it.lf.gjk_axis = V(__uint_as_float(c.x), __uint_as_float(c.y), __uint_as_float(c.z));
+        it.lf.flags = c.w & 0xffu;
+        it.lf.sat_face = (c.w >> 8) & 0xffu;
+        it.lf.sat_e1 = (c.w >> 16) & 0xffu;
+        it.lf.sat_e2 = (c.w >> 24) & 0xffu;
+    } else {
+        it.lf.gjk_axis = V(0.0f, 1.0f, 0.0f);
+        it.lf.flags = 0;
+        it.lf.sat_face = it.lf.sat_e1 = it.lf.sat_e2 = 0;
+    }
+    it.out.nd = a.normal_depth;
+    it.out.l1 = a.local1;
+    it.out.l2 = a.local2;
+    it.out.n = a.n;
+    it.out.i = i;
+    it.out.max = a.max_contacts;
+    it.out.count = 0;
+    it.out.first_normal = V(0.0f, 0.0f, 0.0f);
+    it.out.first_depth = 0.0f;
+
+    if (ALGO == RP3DG_ALGO_SPHERE_VS_SPHERE) {
+        sphere_sphere(it, s1.params.x, s2.params.x);
+    } else if (ALGO == RP3DG_ALGO_SPHERE_VS_CAPSULE) {
+        const bool sphere1 = s1.kind == RP3DG_SHAPE_SPHERE;
+        const ShapeRec& ss = sphere1 ? s1 : s2;
+        const ShapeRec& cs = sphere1 ? s2 : s1;
+        sphere_capsule(it, sphere1, SphereS{ss.params.x}, CapsuleS{cs.params.x, cs.params.y});
+    } else if (ALGO == RP3DG_ALGO_CAPSULE_VS_CAPSULE) {
+        capsule_capsule(it, CapsuleS{s1.params.x, s1.params.y}, CapsuleS{s2.params.x, s2.params.y});
+    } else if (ALGO == RP3DG_ALGO_SPHERE_VS_CONVEX_POLYHEDRON) {
+        const bool sphere1 = s1.kind == RP3DG_SHAPE_SPHERE;
+        const ShapeRec& ss = sphere1 ? s1 : s2;
+        const ShapeRec& ps = sphere1 ? s2 : s1;
+        if (ps.kind == RP3DG_SHAPE_BOX) sphere_poly(it, sphere1, SphereS{ss.params.x}, box_poly(ps, box));
+        else sphere_poly(it, sphere1, SphereS{ss.params.x}, mesh_poly(mesh_words, ps.mesh));
+    } else if (ALGO == RP3DG_ALGO_CAPSULE_VS_CONVEX_POLYHEDRON) {
+        const bool cap1 = s1.kind == RP3DG_SHAPE_CAPSULE;
+        const ShapeRec& cs = cap1 ? s1 : s2;
+        const ShapeRec& ps = cap1 ? s2 : s1;
+        const CapsuleS cap{cs.params.x, cs.params.y};
+        if (ps.kind == RP3DG_SHAPE_BOX) capsule_poly(it, cap1, cap, box_poly(ps, box));
+        else capsule_poly(it, cap1, cap, mesh_poly(mesh_words, ps.mesh));
+    } else {
+        const bool b1 = s1.kind == RP3DG_SHAPE_BOX, b2 = s2.kind == RP3DG_SHAPE_BOX;
+        if (b1 && b2) sat_poly_poly(it, box_poly(s1, box), box_poly(s2, box), a.clip);
+        else if (!b1 && b2) sat_poly_poly(it, mesh_poly(mesh_words, s1.mesh), box_poly(s2, box), a.clip);
+        else if (b1 && !b2) sat_poly_poly(it, box_poly(s1, box), mesh_poly(mesh_words, s2.mesh), a.clip);
+        else sat_poly_poly(it, mesh_poly(mesh_words, s1.mesh), mesh_poly(mesh_words, s2.mesh), a.clip);
+        // ConvexPolyhedronVsConvexPolyhedronAlgorithm.cpp:53-61
+        it.lf.set(RP3DG_LF_WAS_USING_SAT, true);
+        it.lf.set(RP3DG_LF_WAS_USING_GJK, false);
+    }
+
+    if (it.gjk_capped) atomicOr(a.error, 2u);
+    a.is_colliding[i] = it.colliding ? 1 : 0;
+    a.nb_contacts[i] = uint8_t(it.out.count < a.max_contacts ? it.out.count : a.max_contacts);
+    if (a.cache) {
+        uint4 c;
+        c.x = __float_as_uint(it.lf.gjk_axis.x);
+        c.y = __float_as_uint(it.lf.gjk_axis.y);
+        c.z = __float_as_uint(it.lf.gjk_axis.z);
+        c.w = (it.lf.flags & 0xffu) | ((it.lf.sat_face & 0xffu) << 8) | ((it.lf.sat_e1 & 0xffu) << 16) |
+              ((it.lf.sat_e2 & 0xffu) << 24);
+        reinterpret_cast<uint4*>(a.cache)[i] = c;
+    }
+}
+
+template <int ALGO>
+__global__ void __launch_bounds__(NP_BLOCK) narrowphase_kernel(const NpArgs a) {
+    extern __shared__ uint32_t s_mesh[];
+    __shared__ BoxTables s_box;
+    constexpr bool uses_poly = ALGO >= RP3DG_ALGO_SPHERE_VS_CONVEX_POLYHEDRON;
+    const uint32_t* mesh_words = a.mesh_words;
+    if (uses_poly) {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&c_box_tables);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&s_box);
+        for (uint32_t k = threadIdx.x; k < sizeof(BoxTables) / 4; k += blockDim.x) dst[k] = src[k];
+        if (a.stage_mesh) {
+            for (uint32_t k = threadIdx.x; k < a.mesh_nwords; k += blockDim.x) s_mesh[k] = __ldg(a.mesh_words + k);
+            mesh_words = s_mesh;
+        }
+        __syncthreads();
+    }
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride)
+        process_pair<ALGO>(a, i, &s_box, mesh_words);
+}
+
+static const void* kernel_ptr(int algo) {
+    switch (algo) {
+        case 1: return reinterpret_cast<const void*>(&narrowphase_kernel<1>);
+        case 2: return reinterpret_cast<const void*>(&narrowphase_kernel<2>);
+        case 3: return reinterpret_cast<const void*>(&narrowphase_kernel<3>);
+        case 4: return reinterpret_cast<const void*>(&narrowphase_kernel<4>);
+        case 5: return reinterpret_cast<const void*>(&narrowphase_kernel<5>);
+        case 6: return reinterpret_cast<const void*>(&narrowphase_kernel<6>);
+    }
+    return nullptr;
+}
+
+cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaStream_t stream) {
+    if (args.n == 0) return cudaSuccess;
+    const void* k = kernel_ptr(algo);
+    if (!k) return cudaErrorInvalidValue;
+    size_t smem = args.stage_mesh ? size_t(args.mesh_nwords) * 4 : 0;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+    }
+    const uint32_t blocks_needed = (args.n + NP_BLOCK - 1) / NP_BLOCK;
+    // Enough CTAs to fill every SM several times; the grid-stride loop covers the rest.
+    const uint32_t cap = uint32_t(num_sms) * 16u;
+    const uint32_t blocks = blocks_needed < cap ? blocks_needed : cap;
+    void* params[] = {const_cast<NpArgs*>(&args)};
+    return cudaLaunchKernel(k, dim3(blocks), dim3(NP_BLOCK), params, smem, stream);
+}
+
+}  // namespace rp3dg

@@ -1,0 +1,44 @@
+// Kernel-launch interface between the host runtime and the narrow-phase kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/rp3dg.h"
+#include "rp3dg_internal.h"
+
+namespace rp3dg {
+
+constexpr int NP_BLOCK = 128;
+// Mesh arenas up to this size are staged in shared memory by every CTA.
+constexpr uint32_t MESH_STAGE_MAX_BYTES = 96 * 1024;
+
+struct NpArgs {
+    uint32_t n;
+    uint32_t nb_shapes;
+    uint32_t* error;  // device word: bit 0 = a pair named a shape outside the table
+    uint32_t max_contacts;
+    int clip;
+    int stage_mesh;
+    uint32_t mesh_nwords;
+    const uint32_t* mesh_words;
+    const rp3dg_shape* shapes;
+    const int32_t* shape1;
+    const int32_t* shape2;
+    const float4* pos1;
+    const float4* rot1;
+    const float4* pos2;
+    const float4* rot2;
+    const uint8_t* report;
+    rp3dg_lastframe* cache;
+    uint8_t* is_colliding;
+    uint8_t* nb_contacts;
+    float4* normal_depth;
+    float4* local1;
+    float4* local2;
+};
+
+void upload_box_tables(const BoxTables& t, cudaStream_t s);
+cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaStream_t stream);
+
+}  // namespace rp3dg

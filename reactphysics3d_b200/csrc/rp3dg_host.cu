@@ -1,0 +1,532 @@
+// Host runtime behind the C ABI of include/rp3dg.h: context (device, stream),
+// immutable shape tables (box topology, convex-mesh arenas), the shape table,
+// and the narrow-phase entry points.  Convex-mesh set-up restates
+// ConvexMesh::init (reference src/collision/ConvexMesh.cpp:47-264) and
+// HalfEdgeStructure::computeHalfEdges (src/collision/HalfEdgeStructure.cpp:34-127)
+// in single precision with the reference's operation order, so the tables the
+// kernels read are bit-identical to the ones the reference builds.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/rp3dg.h"
+#include "np_launch.h"
+#include "rp3dg_internal.h"
+
+using rp3dg::BoxTables;
+using rp3dg::MeshHdr;
+
+namespace {
+
+struct HalfEdge { uint32_t vertex, twin, face, next; };
+
+struct MeshTopo {
+    std::vector<float> verts;  // nv*3
+    std::vector<uint32_t> face_start, face_count, face_verts, face_edge;
+    std::vector<HalfEdge> edges;
+    std::vector<float> normals;  // nf*3 (unit, unscaled mesh)
+    float centroid[3] = {0, 0, 0};
+    uint32_t nv = 0, nf = 0;
+};
+
+struct MeshInstance {
+    int32_t mesh;
+    float scale[3];
+    std::vector<float> sverts;   // vertex * scale
+    std::vector<float> snormals; // scaled unit normals
+    float scentroid[3];
+};
+
+// HalfEdgeStructure::computeHalfEdges: half-edges are appended in pairs when
+// the second face using an undirected edge is met (earlier face's half-edge
+// first); next pointers follow each face's winding; a face's edgeIndex is its
+// closing half-edge (last vertex -> first vertex).
+bool compute_half_edges(const std::vector<uint32_t>& face_start, const std::vector<uint32_t>& face_count,
+                        const std::vector<uint32_t>& face_verts, uint32_t nv, std::vector<HalfEdge>& out,
+                        std::vector<uint32_t>& face_edge) {
+    typedef std::pair<uint32_t, uint32_t> Key;
+    std::map<Key, HalfEdge> pending;      // the reference's 'edges' map
+    std::map<Key, Key> next_key;          // 'nextEdges'
+    std::map<Key, uint32_t> index_of;     // 'mapEdgeToIndex'
+    std::vector<Key> key_of;              // 'mapEdgeIndexToKey'
+    std::vector<Key> face_key(face_count.size());
+    out.clear();
+    for (uint32_t f = 0; f < face_count.size(); f++) {
+        const uint32_t n = face_count[f];
+        const uint32_t* fv = face_verts.data() + face_start[f];
+        Key first(0, 0), prev(0, 0);
+        for (uint32_t v = 0; v < n; v++) {
+            const uint32_t v1 = fv[v], v2 = fv[v == n - 1 ? 0 : v + 1];
+            if (v1 >= nv || v2 >= nv) return false;
+            const Key k12(v1, v2), k21(v2, v1);
+            HalfEdge e{v1, 0, f, 0};
+            if (v == 0) first = k12;
+            else next_key[prev] = k12;
+            if (v == n - 1) next_key[k12] = first;
+            pending.emplace(k12, e);
+            face_key[f] = k12;
+            auto it = pending.find(k21);
+            if (it != pending.end() && index_of.find(k21) == index_of.end()) {
+                const uint32_t idx = uint32_t(out.size());
+                it->second.twin = idx + 1;
+                e.twin = idx;
+                if (key_of.size() < idx + 2) key_of.resize(idx + 2);
+                key_of[idx] = k21;
+                key_of[idx + 1] = k12;
+                index_of[k12] = idx + 1;
+                index_of[k21] = idx;
+                out.push_back(it->second);
+                out.push_back(e);
+            }
+            prev = k12;
+        }
+    }
+    for (uint32_t i = 0; i < out.size(); i++) {
+        auto nk = next_key.find(key_of[i]);
+        if (nk == next_key.end()) return false;
+        auto ni = index_of.find(nk->second);
+        if (ni == index_of.end()) return false;
+        out[i].next = ni->second;
+    }
+    face_edge.resize(face_count.size());
+    for (uint32_t f = 0; f < face_count.size(); f++) {
+        auto fi = index_of.find(face_key[f]);
+        if (fi == index_of.end()) return false;
+        face_edge[f] = fi->second;
+    }
+    // A closed, consistently wound mesh: twins pair up, and walking `next`
+    // from each face's edge returns to it after exactly face_count steps.
+    // The kernels walk these cycles, so anything else is rejected here.
+    for (uint32_t i = 0; i < out.size(); i++) {
+        if (out[i].twin >= out.size() || out[out[i].twin].twin != i || out[i].next >= out.size()) return false;
+    }
+    if (out.size() != face_verts.size()) return false;
+    for (uint32_t f = 0; f < face_count.size(); f++) {
+        uint32_t e = face_edge[f], steps = 0;
+        do {
+            if (out[e].face != f) return false;
+            e = out[e].next;
+        } while (e != face_edge[f] && ++steps <= face_count[f]);
+        if (steps + 1 != face_count[f]) return false;
+    }
+    return true;
+}
+
+BoxTables make_box_tables() {
+    // PhysicsCommon::initBoxShapeHalfEdgeStructure (reference src/engine/PhysicsCommon.cpp:73-109)
+    static const uint32_t faces[24] = {0, 1, 2, 3, 1, 5, 6, 2, 4, 7, 6, 5, 4, 0, 3, 7, 4, 5, 1, 0, 2, 6, 7, 3};
+    std::vector<uint32_t> fs(6), fc(6, 4), fv(faces, faces + 24), fe;
+    for (int f = 0; f < 6; f++) fs[f] = 4 * f;
+    std::vector<HalfEdge> edges;
+    compute_half_edges(fs, fc, fv, 8, edges, fe);
+    BoxTables t;
+    std::memset(&t, 0, sizeof(t));
+    for (int e = 0; e < 24; e++) {
+        t.edges[e][0] = uint8_t(edges[e].vertex);
+        t.edges[e][1] = uint8_t(edges[e].twin);
+        t.edges[e][2] = uint8_t(edges[e].face);
+        t.edges[e][3] = uint8_t(edges[e].next);
+    }
+    for (int i = 0; i < 24; i++) t.face_verts[i] = uint8_t(faces[i]);
+    for (int f = 0; f < 6; f++) t.face_edge[f] = uint8_t(fe[f]);
+    return t;
+}
+
+}  // namespace
+
+struct rp3dg_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    uint64_t launches = 0;
+    // shapes
+    rp3dg_shape* d_shapes = nullptr;
+    uint32_t nb_shapes = 0, cap_shapes = 0;
+    // convex meshes
+    std::vector<MeshTopo> meshes;
+    std::vector<MeshInstance> instances;
+    std::vector<uint32_t> arena;  // host copy of the device mesh arena
+    uint32_t* d_arena = nullptr;
+    size_t cap_arena = 0;
+    // device error word written by the kernels (bit 0: a pair named a shape outside the table)
+    uint32_t* d_error = nullptr;
+    // staging buffers for rp3dg_narrowphase_host
+    void* d_stage = nullptr;
+    size_t cap_stage = 0;
+};
+
+namespace {
+
+int fail(rp3dg_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_fail(rp3dg_ctx* ctx, cudaError_t e, const char* what) {
+    return fail(ctx, RP3DG_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Lay out every instance: headers first, then per-instance tables.
+void rebuild_arena(rp3dg_ctx* ctx) {
+    std::vector<uint32_t>& w = ctx->arena;
+    const uint32_t nin = uint32_t(ctx->instances.size());
+    const uint32_t hdr_words = nin * (sizeof(MeshHdr) / 4);
+    w.assign(hdr_words, 0u);
+    auto push_f = [&](float x) { uint32_t u; std::memcpy(&u, &x, 4); w.push_back(u); };
+    for (uint32_t k = 0; k < nin; k++) {
+        const MeshInstance& in = ctx->instances[k];
+        const MeshTopo& m = ctx->meshes[in.mesh];
+        MeshHdr h;
+        std::memset(&h, 0, sizeof(h));
+        h.nv = m.nv; h.nf = m.nf; h.nhe = uint32_t(m.edges.size());
+        h.off_verts = uint32_t(w.size());
+        for (float x : m.verts) push_f(x);
+        h.off_sverts = uint32_t(w.size());
+        for (float x : in.sverts) push_f(x);
+        h.off_normals = uint32_t(w.size());
+        for (float x : in.snormals) push_f(x);
+        h.off_face_start = uint32_t(w.size());
+        for (uint32_t x : m.face_start) w.push_back(x);
+        h.off_face_count = uint32_t(w.size());
+        for (uint32_t x : m.face_count) w.push_back(x);
+        h.off_face_verts = uint32_t(w.size());
+        for (uint32_t x : m.face_verts) w.push_back(x);
+        h.off_face_edge = uint32_t(w.size());
+        for (uint32_t x : m.face_edge) w.push_back(x);
+        h.off_edges = uint32_t(w.size());
+        for (const HalfEdge& e : m.edges) { w.push_back(e.vertex); w.push_back(e.twin); w.push_back(e.face); w.push_back(e.next); }
+        h.centroid[0] = in.scentroid[0]; h.centroid[1] = in.scentroid[1]; h.centroid[2] = in.scentroid[2];
+        std::memcpy(w.data() + k * (sizeof(MeshHdr) / 4), &h, sizeof(h));
+    }
+}
+
+int upload_arena(rp3dg_ctx* ctx) {
+    const size_t bytes = ctx->arena.size() * 4;
+    if (bytes > ctx->cap_arena) {
+        if (ctx->d_arena) cudaFree(ctx->d_arena);
+        ctx->d_arena = nullptr;
+        cudaError_t e = cudaMalloc(&ctx->d_arena, bytes);
+        if (e != cudaSuccess) { ctx->cap_arena = 0; return cuda_fail(ctx, e, "cudaMalloc(mesh arena)"); }
+        ctx->cap_arena = bytes;
+    }
+    cudaError_t e = cudaMemcpyAsync(ctx->d_arena, ctx->arena.data(), bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "upload mesh arena");
+}
+
+}  // namespace
+
+extern "C" {
+
+int rp3dg_create(int device, rp3dg_ctx** out) {
+    if (!out) return RP3DG_EINVAL;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return RP3DG_ENODEV;
+    if (device < 0 || device >= count) return RP3DG_EINVAL;
+    rp3dg_ctx* ctx = new rp3dg_ctx();
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_error, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_error, 0, sizeof(uint32_t), ctx->stream);
+    if (e != cudaSuccess) { delete ctx; return RP3DG_ECUDA; }
+    const BoxTables t = make_box_tables();
+    rp3dg::upload_box_tables(t, ctx->stream);
+    e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) { cudaStreamDestroy(ctx->stream); delete ctx; return RP3DG_ECUDA; }
+    *out = ctx;
+    return 0;
+}
+
+void rp3dg_destroy(rp3dg_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->d_shapes);
+    cudaFree(ctx->d_arena);
+    cudaFree(ctx->d_stage);
+    cudaFree(ctx->d_error);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* rp3dg_last_error(const rp3dg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void* rp3dg_stream(rp3dg_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+int rp3dg_synchronize(rp3dg_ctx* ctx) {
+    if (!ctx) return RP3DG_EINVAL;
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "cudaStreamSynchronize");
+}
+
+uint64_t rp3dg_kernel_launches(const rp3dg_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int rp3dg_device_errors(rp3dg_ctx* ctx, uint32_t* flags, int clear) {
+    if (!ctx || !flags) return fail(ctx, RP3DG_EINVAL, "null argument");
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaMemcpyAsync(flags, ctx->d_error, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && clear) e = cudaMemsetAsync(ctx->d_error, 0, sizeof(uint32_t), ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "read device error word");
+}
+
+int rp3dg_create_convex_mesh(rp3dg_ctx* ctx, const float* vertices, uint32_t nv, const uint32_t* face_indices,
+                             const uint32_t* face_sizes, uint32_t nf, int32_t* mesh_id) {
+    if (!ctx || !vertices || !face_indices || !face_sizes || !mesh_id) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (nv == 0 || nf == 0) return fail(ctx, RP3DG_EINVAL, "empty mesh");
+    if (nv > rp3dg::MAX_MESH_VERTICES || nf > rp3dg::MAX_MESH_FACES)
+        return fail(ctx, RP3DG_ECAPACITY, "mesh exceeds 4096 vertices or 256 faces");
+    MeshTopo m;
+    m.nv = nv; m.nf = nf;
+    m.verts.assign(vertices, vertices + 3 * size_t(nv));
+    uint32_t total = 0;
+    for (uint32_t f = 0; f < nf; f++) {
+        if (face_sizes[f] < 3) return fail(ctx, RP3DG_EINVAL, "face with fewer than three vertices");
+        if (face_sizes[f] > rp3dg::MAX_FACE_VERTICES) return fail(ctx, RP3DG_ECAPACITY, "face with more than 16 vertices");
+        m.face_start.push_back(total);
+        m.face_count.push_back(face_sizes[f]);
+        total += face_sizes[f];
+    }
+    m.face_verts.assign(face_indices, face_indices + total);
+    if (!compute_half_edges(m.face_start, m.face_count, m.face_verts, nv, m.edges, m.face_edge))
+        return fail(ctx, RP3DG_EINVAL, "faces do not form a closed half-edge mesh");
+    if (m.edges.size() > rp3dg::MAX_MESH_HALF_EDGES) return fail(ctx, RP3DG_ECAPACITY, "mesh exceeds 256 half-edges");
+    // centroid: ConvexMesh::copyVertices (ConvexMesh.cpp:83-108), sequential sum then division
+    float c[3] = {0.0f, 0.0f, 0.0f};
+    for (uint32_t i = 0; i < nv; i++) { c[0] = c[0] + m.verts[3 * i]; c[1] = c[1] + m.verts[3 * i + 1]; c[2] = c[2] + m.verts[3 * i + 2]; }
+    const float fnv = float(nv);
+    m.centroid[0] = c[0] / fnv; m.centroid[1] = c[1] / fnv; m.centroid[2] = c[2] / fnv;
+    // Newell normals, normalised: ConvexMesh::computeFacesNormals / computeFaceNormal (ConvexMesh.cpp:185-240)
+    m.normals.resize(3 * size_t(nf));
+    for (uint32_t f = 0; f < nf; f++) {
+        float n[3] = {0.0f, 0.0f, 0.0f};
+        const uint32_t cnt = m.face_count[f];
+        for (uint32_t i = cnt - 1, j = 0; j < cnt; i = j, j++) {
+            const float* a = &m.verts[3 * m.face_verts[m.face_start[f] + i]];
+            const float* b = &m.verts[3 * m.face_verts[m.face_start[f] + j]];
+            const float x = (a[1] - b[1]) * (a[2] + b[2]);
+            const float y = (a[2] - b[2]) * (a[0] + b[0]);
+            const float z = (a[0] - b[0]) * (a[1] + b[1]);
+            n[0] = n[0] + x; n[1] = n[1] + y; n[2] = n[2] + z;
+        }
+        const float len = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        if (!(len > FLT_EPSILON)) return fail(ctx, RP3DG_EINVAL, "face with zero area");
+        m.normals[3 * f] = n[0] / len; m.normals[3 * f + 1] = n[1] / len; m.normals[3 * f + 2] = n[2] / len;
+    }
+    ctx->meshes.push_back(std::move(m));
+    *mesh_id = int32_t(ctx->meshes.size() - 1);
+    return 0;
+}
+
+int rp3dg_create_convex_mesh_shape(rp3dg_ctx* ctx, int32_t mesh_id, float sx, float sy, float sz,
+                                   int32_t* instance_id) {
+    if (!ctx || !instance_id) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (mesh_id < 0 || size_t(mesh_id) >= ctx->meshes.size()) return fail(ctx, RP3DG_EINVAL, "unknown mesh id");
+    if (!(sx > 0.0f && sy > 0.0f && sz > 0.0f)) return fail(ctx, RP3DG_EINVAL, "scale must be positive");
+    const MeshTopo& m = ctx->meshes[mesh_id];
+    MeshInstance in;
+    in.mesh = mesh_id;
+    in.scale[0] = sx; in.scale[1] = sy; in.scale[2] = sz;
+    in.sverts.resize(3 * size_t(m.nv));
+    for (uint32_t i = 0; i < m.nv; i++) {
+        in.sverts[3 * i] = m.verts[3 * i] * sx;
+        in.sverts[3 * i + 1] = m.verts[3 * i + 1] * sy;
+        in.sverts[3 * i + 2] = m.verts[3 * i + 2] * sz;
+    }
+    // ConvexMeshShape::computeScaledFacesNormals (ConvexMeshShape.cpp:50-70):
+    // the reciprocal scale is computed in double and stored as float
+    const float inv[3] = {float(1.0 / double(sx)), float(1.0 / double(sy)), float(1.0 / double(sz))};
+    in.snormals.resize(3 * size_t(m.nf));
+    for (uint32_t f = 0; f < m.nf; f++) {
+        const float x = inv[0] * m.normals[3 * f], y = inv[1] * m.normals[3 * f + 1], z = inv[2] * m.normals[3 * f + 2];
+        const float len = std::sqrt(x * x + y * y + z * z);
+        in.snormals[3 * f] = x / len; in.snormals[3 * f + 1] = y / len; in.snormals[3 * f + 2] = z / len;
+    }
+    in.scentroid[0] = m.centroid[0] * sx; in.scentroid[1] = m.centroid[1] * sy; in.scentroid[2] = m.centroid[2] * sz;
+    ctx->instances.push_back(std::move(in));
+    rebuild_arena(ctx);
+    cudaSetDevice(ctx->device);
+    const int rc = upload_arena(ctx);
+    if (rc) { ctx->instances.pop_back(); rebuild_arena(ctx); return rc; }
+    *instance_id = int32_t(ctx->instances.size() - 1);
+    return 0;
+}
+
+int rp3dg_get_convex_mesh_tables(rp3dg_ctx* ctx, int32_t instance_id, uint32_t* nb_vertices, uint32_t* nb_faces,
+                                 uint32_t* nb_half_edges, uint32_t* half_edges, float* face_normals,
+                                 uint32_t* face_edge, float* centroid, uint32_t cap_he, uint32_t cap_faces) {
+    if (!ctx) return RP3DG_EINVAL;
+    if (instance_id < 0 || size_t(instance_id) >= ctx->instances.size()) return fail(ctx, RP3DG_EINVAL, "unknown instance");
+    const MeshInstance& in = ctx->instances[instance_id];
+    const MeshTopo& m = ctx->meshes[in.mesh];
+    *nb_vertices = m.nv; *nb_faces = m.nf; *nb_half_edges = uint32_t(m.edges.size());
+    if (m.edges.size() > cap_he || m.nf > cap_faces) return fail(ctx, RP3DG_ECAPACITY, "output capacity too small");
+    for (size_t e = 0; e < m.edges.size(); e++) {
+        half_edges[4 * e] = m.edges[e].vertex; half_edges[4 * e + 1] = m.edges[e].twin;
+        half_edges[4 * e + 2] = m.edges[e].face; half_edges[4 * e + 3] = m.edges[e].next;
+    }
+    std::memcpy(face_normals, in.snormals.data(), in.snormals.size() * sizeof(float));
+    std::memcpy(face_edge, m.face_edge.data(), m.face_edge.size() * sizeof(uint32_t));
+    std::memcpy(centroid, in.scentroid, 3 * sizeof(float));
+    return 0;
+}
+
+int rp3dg_set_shapes(rp3dg_ctx* ctx, const rp3dg_shape* shapes, uint32_t nb) {
+    if (!ctx || (!shapes && nb)) return fail(ctx, RP3DG_EINVAL, "null argument");
+    for (uint32_t i = 0; i < nb; i++) {
+        const rp3dg_shape& s = shapes[i];
+        if (s.kind < RP3DG_SHAPE_SPHERE || s.kind > RP3DG_SHAPE_CONVEX_MESH) return fail(ctx, RP3DG_EINVAL, "unknown shape kind");
+        if (s.kind == RP3DG_SHAPE_CONVEX_MESH && (s.mesh < 0 || size_t(s.mesh) >= ctx->instances.size()))
+            return fail(ctx, RP3DG_EINVAL, "shape refers to an unknown convex mesh instance");
+    }
+    cudaSetDevice(ctx->device);
+    if (nb > ctx->cap_shapes) {
+        cudaFree(ctx->d_shapes);
+        ctx->d_shapes = nullptr;
+        cudaError_t e = cudaMalloc(&ctx->d_shapes, size_t(nb) * sizeof(rp3dg_shape));
+        if (e != cudaSuccess) { ctx->cap_shapes = 0; return cuda_fail(ctx, e, "cudaMalloc(shapes)"); }
+        ctx->cap_shapes = nb;
+    }
+    if (nb) {
+        cudaError_t e = cudaMemcpyAsync(ctx->d_shapes, shapes, size_t(nb) * sizeof(rp3dg_shape), cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "upload shapes");
+    }
+    ctx->nb_shapes = nb;
+    return 0;
+}
+
+int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3dg_contact_batch* out,
+                             int clip_with_previous_axis) {
+    if (!ctx || !p || !out) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (algorithm < RP3DG_ALGO_SPHERE_VS_SPHERE || algorithm > RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON)
+        return fail(ctx, RP3DG_EINVAL, "unknown algorithm");
+    if (p->n == 0) return 0;
+    if (!p->shape1 || !p->shape2 || !p->pos1 || !p->rot1 || !p->pos2 || !p->rot2)
+        return fail(ctx, RP3DG_EINVAL, "null pair array");
+    if (!out->is_colliding || !out->nb_contacts || !out->normal_depth || !out->local1 || !out->local2)
+        return fail(ctx, RP3DG_EINVAL, "null output array");
+    if (out->max_contacts < 1 || out->max_contacts > RP3DG_MAX_CONTACTS_PER_PAIR)
+        return fail(ctx, RP3DG_EINVAL, "max_contacts must be in 1..16");
+    if (!ctx->d_shapes) return fail(ctx, RP3DG_EINVAL, "no shape table (rp3dg_set_shapes)");
+    rp3dg::NpArgs a;
+    a.n = p->n;
+    a.nb_shapes = ctx->nb_shapes;
+    a.error = ctx->d_error;
+    a.max_contacts = out->max_contacts;
+    a.clip = clip_with_previous_axis ? 1 : 0;
+    a.mesh_nwords = uint32_t(ctx->arena.size());
+    a.mesh_words = ctx->d_arena;
+    a.stage_mesh = (algorithm >= RP3DG_ALGO_SPHERE_VS_CONVEX_POLYHEDRON && a.mesh_nwords > 0 &&
+                    size_t(a.mesh_nwords) * 4 <= rp3dg::MESH_STAGE_MAX_BYTES) ? 1 : 0;
+    a.shapes = ctx->d_shapes;
+    a.shape1 = p->shape1; a.shape2 = p->shape2;
+    a.pos1 = reinterpret_cast<const float4*>(p->pos1); a.rot1 = reinterpret_cast<const float4*>(p->rot1);
+    a.pos2 = reinterpret_cast<const float4*>(p->pos2); a.rot2 = reinterpret_cast<const float4*>(p->rot2);
+    a.report = p->report_contacts;
+    a.cache = p->cache;
+    a.is_colliding = out->is_colliding;
+    a.nb_contacts = out->nb_contacts;
+    a.normal_depth = reinterpret_cast<float4*>(out->normal_depth);
+    a.local1 = reinterpret_cast<float4*>(out->local1);
+    a.local2 = reinterpret_cast<float4*>(out->local2);
+    cudaSetDevice(ctx->device);
+    cudaError_t e = rp3dg::launch_narrowphase(algorithm, a, ctx->num_sms, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "narrowphase launch");
+    ctx->launches++;
+    return 0;
+}
+
+int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3dg_contact_batch* out,
+                           int clip_with_previous_axis) {
+    if (!ctx || !p || !out) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (p->n == 0) return 0;
+    if (out->max_contacts < 1 || out->max_contacts > RP3DG_MAX_CONTACTS_PER_PAIR)
+        return fail(ctx, RP3DG_EINVAL, "max_contacts must be in 1..16");
+    const size_t n = p->n, mc = out->max_contacts;
+    // staging layout: inputs then outputs, each array 256-byte aligned
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    size_t off = 0;
+    const size_t o_s1 = off; off += al(n * 4);
+    const size_t o_s2 = off; off += al(n * 4);
+    const size_t o_p1 = off; off += al(n * 16);
+    const size_t o_r1 = off; off += al(n * 16);
+    const size_t o_p2 = off; off += al(n * 16);
+    const size_t o_r2 = off; off += al(n * 16);
+    const size_t o_rep = off; off += p->report_contacts ? al(n) : 0;
+    const size_t o_cache = off; off += p->cache ? al(n * sizeof(rp3dg_lastframe)) : 0;
+    const size_t o_col = off; off += al(n);
+    const size_t o_nb = off; off += al(n);
+    const size_t o_nd = off; off += al(n * mc * 16);
+    const size_t o_l1 = off; off += al(n * mc * 16);
+    const size_t o_l2 = off; off += al(n * mc * 16);
+    cudaSetDevice(ctx->device);
+    if (off > ctx->cap_stage) {
+        cudaFree(ctx->d_stage);
+        ctx->d_stage = nullptr;
+        cudaError_t e = cudaMalloc(&ctx->d_stage, off);
+        if (e != cudaSuccess) { ctx->cap_stage = 0; return cuda_fail(ctx, e, "cudaMalloc(staging)"); }
+        ctx->cap_stage = off;
+    }
+    char* b = static_cast<char*>(ctx->d_stage);
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaSuccess;
+    auto up = [&](size_t o, const void* src, size_t bytes) {
+        if (e == cudaSuccess && src) e = cudaMemcpyAsync(b + o, src, bytes, cudaMemcpyHostToDevice, s);
+    };
+    up(o_s1, p->shape1, n * 4); up(o_s2, p->shape2, n * 4);
+    up(o_p1, p->pos1, n * 16); up(o_r1, p->rot1, n * 16);
+    up(o_p2, p->pos2, n * 16); up(o_r2, p->rot2, n * 16);
+    up(o_rep, p->report_contacts, n);
+    up(o_cache, p->cache, n * sizeof(rp3dg_lastframe));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "upload batch");
+    rp3dg_pair_batch dp;
+    dp.n = p->n;
+    dp.shape1 = reinterpret_cast<const int32_t*>(b + o_s1);
+    dp.shape2 = reinterpret_cast<const int32_t*>(b + o_s2);
+    dp.pos1 = reinterpret_cast<const rp3dg_float4*>(b + o_p1);
+    dp.rot1 = reinterpret_cast<const rp3dg_float4*>(b + o_r1);
+    dp.pos2 = reinterpret_cast<const rp3dg_float4*>(b + o_p2);
+    dp.rot2 = reinterpret_cast<const rp3dg_float4*>(b + o_r2);
+    dp.report_contacts = p->report_contacts ? reinterpret_cast<const uint8_t*>(b + o_rep) : nullptr;
+    dp.cache = p->cache ? reinterpret_cast<rp3dg_lastframe*>(b + o_cache) : nullptr;
+    rp3dg_contact_batch dout;
+    dout.is_colliding = reinterpret_cast<uint8_t*>(b + o_col);
+    dout.nb_contacts = reinterpret_cast<uint8_t*>(b + o_nb);
+    dout.normal_depth = reinterpret_cast<rp3dg_float4*>(b + o_nd);
+    dout.local1 = reinterpret_cast<rp3dg_float4*>(b + o_l1);
+    dout.local2 = reinterpret_cast<rp3dg_float4*>(b + o_l2);
+    dout.max_contacts = out->max_contacts;
+    int rc = rp3dg_narrowphase_device(ctx, algorithm, &dp, &dout, clip_with_previous_axis);
+    if (rc) return rc;
+    auto down = [&](void* dst, size_t o, size_t bytes) {
+        if (e == cudaSuccess && dst) e = cudaMemcpyAsync(dst, b + o, bytes, cudaMemcpyDeviceToHost, s);
+    };
+    down(out->is_colliding, o_col, n);
+    down(out->nb_contacts, o_nb, n);
+    down(p->cache, o_cache, p->cache ? n * sizeof(rp3dg_lastframe) : 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "narrowphase (host arrays)");
+    // copy back only the slots in use (slot-major: slot k of every pair is contiguous)
+    uint32_t used = 0;
+    for (size_t i = 0; i < n; i++) used = out->nb_contacts[i] > used ? out->nb_contacts[i] : used;
+    down(out->normal_depth, o_nd, n * used * 16);
+    down(out->local1, o_l1, n * used * 16);
+    down(out->local2, o_l2, n * used * 16);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "narrowphase (host arrays)");
+}
+
+}  // extern "C"

@@ -1,0 +1,209 @@
+"""Python binding of the C ABI (include/rp3dg.h) of librp3dg.so.
+
+`Context` owns one rp3dg_ctx (one CUDA device, one stream).  Batches can be
+given as numpy arrays in host memory (`narrowphase_host`, the call a CPU-side
+engine would make in place of XxxAlgorithm::testCollision) or as torch CUDA
+tensors already resident in device memory (`narrowphase_device`).
+
+There is no CPU fallback: if the library is missing or no GPU is present the
+calls raise.
+"""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+from . import _abi as A
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "librp3dg.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "rp3dg.h")
+
+RP3DG_OK, RP3DG_EINVAL, RP3DG_ECUDA, RP3DG_ENOMEM, RP3DG_ECAPACITY, RP3DG_ENODEV = 0, -1, -2, -3, -4, -5
+
+_lib = None
+
+
+class Rp3dgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"rp3dg error {code}: {msg}")
+        self.code = code
+
+
+def declared_symbols(header=HEADER):
+    """Function names declared in include/rp3dg.h."""
+    text = open(header).read()
+    return sorted(set(re.findall(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b(rp3dg_\w+)\s*\(", text, re.M)))
+
+
+def load_library(path=LIB_PATH):
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with `python -m reactphysics3d_b200.build` "
+                                "(there is no CPU fallback)")
+    L = C.CDLL(path)
+    P = C.c_void_p
+    L.rp3dg_create.argtypes = [C.c_int, C.POINTER(P)]
+    L.rp3dg_destroy.argtypes = [P]
+    L.rp3dg_destroy.restype = None
+    L.rp3dg_last_error.argtypes = [P]
+    L.rp3dg_last_error.restype = C.c_char_p
+    L.rp3dg_stream.argtypes = [P]
+    L.rp3dg_stream.restype = P
+    L.rp3dg_synchronize.argtypes = [P]
+    L.rp3dg_kernel_launches.argtypes = [P]
+    L.rp3dg_kernel_launches.restype = C.c_uint64
+    L.rp3dg_create_convex_mesh.argtypes = [P, P, C.c_uint32, P, P, C.c_uint32, C.POINTER(C.c_int32)]
+    L.rp3dg_create_convex_mesh_shape.argtypes = [P, C.c_int32, C.c_float, C.c_float, C.c_float,
+                                                 C.POINTER(C.c_int32)]
+    L.rp3dg_get_convex_mesh_tables.argtypes = [P, C.c_int32] + [P] * 7 + [C.c_uint32, C.c_uint32]
+    L.rp3dg_set_shapes.argtypes = [P, P, C.c_uint32]
+    L.rp3dg_device_errors.argtypes = [P, C.POINTER(C.c_uint32), C.c_int]
+    L.rp3dg_narrowphase_device.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_int]
+    L.rp3dg_narrowphase_host.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_int]
+    _lib = L
+    return L
+
+
+class DevicePairs:
+    """A pair batch resident in device memory (torch CUDA tensors)."""
+
+    def __init__(self, host_pairs, device="cuda"):
+        import torch
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)
+        h = host_pairs
+        self.n = h.n
+        self.shape1, self.shape2 = t(h.shape1), t(h.shape2)
+        self.pos1, self.rot1, self.pos2, self.rot2 = t(h.pos1), t(h.rot1), t(h.pos2), t(h.rot2)
+        self.report = None if h.report is None else t(h.report)
+        self.cache = None if h.cache is None else t(h.cache.view(np.uint8).reshape(-1, 16))
+
+    def struct(self):
+        p = lambda x: None if x is None else x.data_ptr()
+        return A.PairBatch(self.n, p(self.shape1), p(self.shape2), p(self.pos1), p(self.rot1), p(self.pos2),
+                           p(self.rot2), p(self.report), p(self.cache))
+
+    def host_cache(self):
+        return None if self.cache is None else self.cache.cpu().numpy().reshape(-1).view(A.CACHE_DTYPE)
+
+
+class DeviceContacts:
+    """Narrow-phase results in device memory (torch CUDA tensors)."""
+
+    def __init__(self, n, max_contacts=A.MAX_CONTACTS, device="cuda"):
+        import torch
+        self.n, self.max_contacts = n, max_contacts
+        self.is_colliding = torch.zeros(n, dtype=torch.uint8, device=device)
+        self.nb_contacts = torch.zeros(n, dtype=torch.uint8, device=device)
+        self.normal_depth = torch.zeros((max_contacts, n, 4), dtype=torch.float32, device=device)
+        self.local1 = torch.zeros((max_contacts, n, 4), dtype=torch.float32, device=device)
+        self.local2 = torch.zeros((max_contacts, n, 4), dtype=torch.float32, device=device)
+
+    def struct(self):
+        return A.ContactBatch(self.is_colliding.data_ptr(), self.nb_contacts.data_ptr(),
+                              self.normal_depth.data_ptr(), self.local1.data_ptr(), self.local2.data_ptr(),
+                              self.max_contacts)
+
+    def to_host(self):
+        h = A.HostContacts(self.n, self.max_contacts)
+        h.is_colliding[:] = self.is_colliding.cpu().numpy()
+        h.nb_contacts[:] = self.nb_contacts.cpu().numpy()
+        h.normal_depth[:] = self.normal_depth.cpu().numpy()
+        h.local1[:] = self.local1.cpu().numpy()
+        h.local2[:] = self.local2.cpu().numpy()
+        return h
+
+
+class Context:
+    """One rp3dg_ctx: device, stream, shape and mesh tables."""
+
+    def __init__(self, device=0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        rc = self.lib.rp3dg_create(int(device), C.byref(h))
+        if rc != 0:
+            raise Rp3dgError(rc, "rp3dg_create failed (no CUDA device?)")
+        self.h = h
+        self.device = device
+        self._shapes = None
+
+    def close(self):
+        if self.h:
+            self.lib.rp3dg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.h).decode())
+
+    @property
+    def stream_ptr(self):
+        return self.lib.rp3dg_stream(self.h)
+
+    def torch_stream(self):
+        import torch
+        return torch.cuda.ExternalStream(self.stream_ptr, device=f"cuda:{self.device}")
+
+    def synchronize(self):
+        self._check(self.lib.rp3dg_synchronize(self.h))
+
+    def device_errors(self, clear=True):
+        f = C.c_uint32()
+        self._check(self.lib.rp3dg_device_errors(self.h, C.byref(f), int(clear)))
+        return f.value
+
+    def kernel_launches(self):
+        return int(self.lib.rp3dg_kernel_launches(self.h))
+
+    def create_convex_mesh(self, vertices, faces):
+        v = np.ascontiguousarray(vertices, dtype=np.float32)
+        idx = np.ascontiguousarray(np.concatenate([np.asarray(f, np.uint32) for f in faces]), dtype=np.uint32)
+        sizes = np.array([len(f) for f in faces], dtype=np.uint32)
+        out = C.c_int32()
+        self._check(self.lib.rp3dg_create_convex_mesh(self.h, v.ctypes.data, len(v), idx.ctypes.data,
+                                                      sizes.ctypes.data, len(faces), C.byref(out)))
+        return out.value
+
+    def create_convex_mesh_shape(self, mesh, scale=(1.0, 1.0, 1.0)):
+        out = C.c_int32()
+        self._check(self.lib.rp3dg_create_convex_mesh_shape(self.h, mesh, *map(float, scale), C.byref(out)))
+        return out.value
+
+    def mesh_tables(self, instance, cap=4096):
+        nv, nf, nh = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        he = np.zeros(4 * cap, np.uint32)
+        fn = np.zeros(3 * cap, np.float32)
+        fe = np.zeros(cap, np.uint32)
+        cen = np.zeros(3, np.float32)
+        self._check(self.lib.rp3dg_get_convex_mesh_tables(self.h, instance, C.addressof(nv), C.addressof(nf),
+                                                          C.addressof(nh), he.ctypes.data, fn.ctypes.data,
+                                                          fe.ctypes.data, cen.ctypes.data, cap, cap))
+        return dict(half_edges=he[:4 * nh.value].reshape(-1, 4), face_normals=fn[:3 * nf.value].reshape(-1, 3),
+                    face_edge=fe[:nf.value], centroid=cen)
+
+    def set_shapes(self, shapes):
+        sh = np.ascontiguousarray(shapes, dtype=A.SHAPE_DTYPE)
+        self._check(self.lib.rp3dg_set_shapes(self.h, sh.ctypes.data, len(sh)))
+        self._shapes = sh
+
+    def narrowphase_host(self, algo, pairs, out=None, clip=True):
+        if out is None:
+            out = A.HostContacts(pairs.n)
+        pb, cb = pairs.struct(), out.struct()
+        self._check(self.lib.rp3dg_narrowphase_host(self.h, int(algo), C.byref(pb), C.byref(cb), int(clip)))
+        return out
+
+    def narrowphase_device(self, algo, pairs, out, clip=True):
+        """Asynchronous on the context stream; pairs/out are DevicePairs/DeviceContacts."""
+        pb, cb = pairs.struct(), out.struct()
+        self._check(self.lib.rp3dg_narrowphase_device(self.h, int(algo), C.byref(pb), C.byref(cb), int(clip)))
+        return out
