@@ -46,24 +46,12 @@ RD BoxPoly box_poly(const ShapeRec& s, const BoxTables* t) {
     return b;
 }
 
-template <int ALGO>
-RD void process_pair(const NpArgs& a, uint32_t i, const BoxTables* box, const uint32_t* mesh_words) {
-    const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
-    if (uint32_t(i1) >= a.nb_shapes || uint32_t(i2) >= a.nb_shapes) {
-        // a pair naming a shape outside the table is reported as not colliding
-        a.is_colliding[i] = 0;
-        a.nb_contacts[i] = 0;
-        atomicOr(a.error, 1u);
-        return;
-    }
-    const ShapeRec s1 = load_shape(a.shapes, i1);
-    const ShapeRec s2 = load_shape(a.shapes, i2);
-    Item it;
-    {
-        const float4 p1 = a.pos1[i], q1 = a.rot1[i], p2 = a.pos2[i], q2 = a.rot2[i];
-        it.t1 = X(V(p1.x, p1.y, p1.z), Q(q1.x, q1.y, q1.z, q1.w));
-        it.t2 = X(V(p2.x, p2.y, p2.z), Q(q2.x, q2.y, q2.z, q2.w));
-    }
+// Load one pair's inputs into an Item (every lane of a warp may call this for
+// the same pair: the loads are broadcasts).
+RD void load_item(const NpArgs& a, uint32_t i, Item& it) {
+    const float4 p1 = a.pos1[i], q1 = a.rot1[i], p2 = a.pos2[i], q2 = a.rot2[i];
+    it.t1 = X(V(p1.x, p1.y, p1.z), Q(q1.x, q1.y, q1.z, q1.w));
+    it.t2 = X(V(p2.x, p2.y, p2.z), Q(q2.x, q2.y, q2.z, q2.w));
     it.report = a.report ? a.report[i] != 0 : true;
     it.colliding = false;
     it.gjk_capped = false;
@@ -88,6 +76,37 @@ RD void process_pair(const NpArgs& a, uint32_t i, const BoxTables* box, const ui
     it.out.count = 0;
     it.out.first_normal = V(0.0f, 0.0f, 0.0f);
     it.out.first_depth = 0.0f;
+}
+
+RD void store_item(const NpArgs& a, uint32_t i, const Item& it) {
+    if (it.gjk_capped) atomicOr(a.error, 2u);
+    a.is_colliding[i] = it.colliding ? 1 : 0;
+    a.nb_contacts[i] = uint8_t(it.out.count < a.max_contacts ? it.out.count : a.max_contacts);
+    if (a.cache) {
+        uint4 c;
+        c.x = __float_as_uint(it.lf.gjk_axis.x);
+        c.y = __float_as_uint(it.lf.gjk_axis.y);
+        c.z = __float_as_uint(it.lf.gjk_axis.z);
+        c.w = (it.lf.flags & 0xffu) | ((it.lf.sat_face & 0xffu) << 8) | ((it.lf.sat_e1 & 0xffu) << 16) |
+              ((it.lf.sat_e2 & 0xffu) << 24);
+        reinterpret_cast<uint4*>(a.cache)[i] = c;
+    }
+}
+
+template <int ALGO>
+RD void process_pair(const NpArgs& a, uint32_t i, const BoxTables* box, const uint32_t* mesh_words) {
+    const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
+    if (uint32_t(i1) >= a.nb_shapes || uint32_t(i2) >= a.nb_shapes) {
+        // a pair naming a shape outside the table is reported as not colliding
+        a.is_colliding[i] = 0;
+        a.nb_contacts[i] = 0;
+        atomicOr(a.error, 1u);
+        return;
+    }
+    const ShapeRec s1 = load_shape(a.shapes, i1);
+    const ShapeRec s2 = load_shape(a.shapes, i2);
+    Item it;
+    load_item(a, i, it);
 
     if (ALGO == RP3DG_ALGO_SPHERE_VS_SPHERE) {
         sphere_sphere(it, s1.params.x, s2.params.x);
@@ -122,18 +141,34 @@ RD void process_pair(const NpArgs& a, uint32_t i, const BoxTables* box, const ui
         it.lf.set(RP3DG_LF_WAS_USING_GJK, false);
     }
 
-    if (it.gjk_capped) atomicOr(a.error, 2u);
-    a.is_colliding[i] = it.colliding ? 1 : 0;
-    a.nb_contacts[i] = uint8_t(it.out.count < a.max_contacts ? it.out.count : a.max_contacts);
-    if (a.cache) {
-        uint4 c;
-        c.x = __float_as_uint(it.lf.gjk_axis.x);
-        c.y = __float_as_uint(it.lf.gjk_axis.y);
-        c.z = __float_as_uint(it.lf.gjk_axis.z);
-        c.w = (it.lf.flags & 0xffu) | ((it.lf.sat_face & 0xffu) << 8) | ((it.lf.sat_e1 & 0xffu) << 16) |
-              ((it.lf.sat_e2 & 0xffu) << 24);
-        reinterpret_cast<uint4*>(a.cache)[i] = c;
+    store_item(a, i, it);
+}
+
+// Convex polyhedron vs convex polyhedron, one warp per pair.
+RD void process_pair_warp(const NpArgs& a, uint32_t i, int lane, const BoxTables* box, const uint32_t* mesh_words,
+                          Edge1Stage* stage) {
+    const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
+    if (uint32_t(i1) >= a.nb_shapes || uint32_t(i2) >= a.nb_shapes) {
+        if (lane == 0) {
+            a.is_colliding[i] = 0;
+            a.nb_contacts[i] = 0;
+            atomicOr(a.error, 1u);
+        }
+        return;
     }
+    const ShapeRec s1 = load_shape(a.shapes, i1);
+    const ShapeRec s2 = load_shape(a.shapes, i2);
+    Item it;
+    load_item(a, i, it);
+    const bool b1 = s1.kind == RP3DG_SHAPE_BOX, b2 = s2.kind == RP3DG_SHAPE_BOX;
+    if (b1 && b2) warp_sat_poly_poly(it, box_poly(s1, box), box_poly(s2, box), a.clip, lane, stage);
+    else if (!b1 && b2) warp_sat_poly_poly(it, mesh_poly(mesh_words, s1.mesh), box_poly(s2, box), a.clip, lane, stage);
+    else if (b1 && !b2) warp_sat_poly_poly(it, box_poly(s1, box), mesh_poly(mesh_words, s2.mesh), a.clip, lane, stage);
+    else warp_sat_poly_poly(it, mesh_poly(mesh_words, s1.mesh), mesh_poly(mesh_words, s2.mesh), a.clip, lane, stage);
+    // ConvexPolyhedronVsConvexPolyhedronAlgorithm.cpp:53-61
+    it.lf.set(RP3DG_LF_WAS_USING_SAT, true);
+    it.lf.set(RP3DG_LF_WAS_USING_GJK, false);
+    if (lane == 0) store_item(a, i, it);
 }
 
 template <int ALGO>
@@ -152,9 +187,17 @@ __global__ void __launch_bounds__(NP_BLOCK) narrowphase_kernel(const NpArgs a) {
         }
         __syncthreads();
     }
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride)
-        process_pair<ALGO>(a, i, &s_box, mesh_words);
+    if constexpr (ALGO == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON) {
+        __shared__ Edge1Stage s_stage[NP_BLOCK / 32][WARP_EDGE_CAP];
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const uint32_t nwarps = gridDim.x * (NP_BLOCK / 32);
+        for (uint32_t i = blockIdx.x * (NP_BLOCK / 32) + warp; i < a.n; i += nwarps)
+            process_pair_warp(a, i, lane, &s_box, mesh_words, s_stage[warp]);
+    } else {
+        const uint32_t stride = gridDim.x * blockDim.x;
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride)
+            process_pair<ALGO>(a, i, &s_box, mesh_words);
+    }
 }
 
 static const void* kernel_ptr(int algo) {
@@ -178,7 +221,8 @@ cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaSt
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
     }
-    const uint32_t blocks_needed = (args.n + NP_BLOCK - 1) / NP_BLOCK;
+    const uint32_t per_block = algo == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON ? NP_BLOCK / 32 : NP_BLOCK;
+    const uint32_t blocks_needed = (args.n + per_block - 1) / per_block;
     // Enough CTAs to fill every SM several times; the grid-stride loop covers the rest.
     const uint32_t cap = uint32_t(num_sms) * 16u;
     const uint32_t blocks = blocks_needed < cap ? blocks_needed : cap;

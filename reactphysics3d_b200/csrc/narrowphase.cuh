@@ -1062,4 +1062,231 @@ RD void capsule_poly(Item& it, bool cap1, CapsuleS cap, const P& poly) {
     }
 }
 
+
+// ===========================================================================
+// Warp-cooperative SAT for two convex polyhedra: one warp per pair.
+//
+// The reference visits faces and edge pairs one after another and keeps
+// (a) the first candidate axis (in visiting order) that separates the shapes
+// and (b) otherwise the minimum penetration depth, first occurrence on ties.
+// Here the 32 lanes evaluate 32 consecutive candidates at a time with the
+// reference's per-candidate arithmetic, then
+//   - a ballot over "separates" in visiting order finds the same first
+//     separating candidate (earlier groups had none), and
+//   - an (depth, index) arg-min with the smaller index winning ties gives
+//     the same minimum and the same index.
+// For the edge pairs the reference biases the comparison against the face
+// minimum: an edge pair k only takes over if fl(fl(d_k*1.002)+0.0005) <
+// faceMin, after which later pairs need only d < current minimum.  Because
+// rounding is monotonic, every pair before the first qualifying k has a
+// larger depth than d_k, so the final choice is the global first arg-min,
+// taken exactly when that minimum itself qualifies.  Results are therefore
+// bit-identical to the sequential loops.
+// ===========================================================================
+constexpr unsigned FULL_MASK = 0xffffffffu;
+constexpr uint32_t WARP_EDGE_CAP = 128;  // even half-edges of polyhedron 1 staged per warp
+
+// Per-edge data of polyhedron 1 in polyhedron-2 space, staged in shared memory.
+struct Edge1Stage {
+    float e1A[3], dir1[3], a[3], b[3], bxa[3];
+};
+
+RD void warp_argmin(float& d, uint32_t& idx) {
+    for (int o = 16; o; o >>= 1) {
+        const float od = __shfl_xor_sync(FULL_MASK, d, o);
+        const uint32_t oi = __shfl_xor_sync(FULL_MASK, idx, o);
+        if (od < d || (od == d && oi < idx)) { d = od; idx = oi; }
+    }
+}
+
+// testFacesDirectionPolyhedronVsPolyhedron (SATAlgorithm.cpp:1113-1142), faces spread over lanes
+template <class PA, class PB>
+RD float warp_sat_faces(const PA& pa, const PB& pb, const xform& a2b, uint32_t& minFace, int lane) {
+    const uint32_t nf = pa.nfaces();
+    float best = DECIMAL_LARGEST;
+    uint32_t bestF = 0xffffffffu;
+    for (uint32_t base = 0; base < nf; base += 32) {
+        const uint32_t f = base + lane;
+        const bool valid = f < nf;
+        const float d = valid ? sat_single_face(pa, pb, a2b, f) : DECIMAL_LARGEST;
+        const unsigned sep = __ballot_sync(FULL_MASK, valid && d <= 0.0f);
+        if (sep) {
+            const int l = __ffs(sep) - 1;
+            minFace = base + l;
+            return __shfl_sync(FULL_MASK, d, l);
+        }
+        if (valid && d < best) { best = d; bestF = f; }
+    }
+    warp_argmin(best, bestF);
+    minFace = bestF;
+    return best;
+}
+
+template <class P2>
+RD void edge2_data(const P2& p2, uint32_t j, hedge& e2, v3& e2A, v3& dir2) {
+    e2 = p2.edge(j);
+    e2A = p2.vertex(e2.vertex);
+    dir2 = vsub(p2.vertex(p2.edge(e2.next).vertex), e2A);
+}
+
+// testCollisionConvexPolyhedronVsConvexPolyhedron (SATAlgorithm.cpp:485-889), one warp per pair.
+// Every lane holds the same pair state; contacts and outputs are produced by lane 0.
+template <class P1, class P2>
+RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, int lane, Edge1Stage* stage) {
+    const xform p1to2 = xmul(xinv(it.t2), it.t1);
+    const xform p2to1 = xinv(p1to2);
+    LastFrame& lf = it.lf;
+
+    const bool cacheInRange = lf.has(RP3DG_LF_SAT_FACE_POLY1)   ? lf.sat_face < p1.nfaces()
+                              : lf.has(RP3DG_LF_SAT_FACE_POLY2) ? lf.sat_face < p2.nfaces()
+                                                                : (lf.sat_e1 < p1.nhe() && lf.sat_e2 < p2.nhe());
+    if (cacheInRange && lf.has(RP3DG_LF_IS_VALID) && lf.has(RP3DG_LF_WAS_USING_SAT)) {
+        const bool wasColliding = lf.has(RP3DG_LF_WAS_COLLIDING);
+        if (lf.has(RP3DG_LF_SAT_FACE_POLY1) || lf.has(RP3DG_LF_SAT_FACE_POLY2)) {
+            const bool face1 = lf.has(RP3DG_LF_SAT_FACE_POLY1);
+            const float d = face1 ? sat_single_face(p1, p2, p1to2, lf.sat_face) : sat_single_face(p2, p1, p2to1, lf.sat_face);
+            if (!wasColliding && d <= 0.0f) return;
+            if (wasColliding && clipPrev && d > 0.0f) {
+                bool found = false;
+                if (lane == 0) found = poly_face_contacts(face1, p1, p2, p1to2, p2to1, lf.sat_face, it);
+                found = __shfl_sync(FULL_MASK, found, 0);
+                if (found) {
+                    lf.set(RP3DG_LF_SAT_FACE_POLY1, face1);
+                    lf.set(RP3DG_LF_SAT_FACE_POLY2, !face1);
+                    it.colliding = true;
+                    return;
+                }
+            }
+        } else {
+            const hedge e1 = p1.edge(lf.sat_e1);
+            const hedge e2 = p2.edge(lf.sat_e2);
+            const v3 e1A = xapply(p1to2, p1.vertex(e1.vertex));
+            const v3 e1B = xapply(p1to2, p1.vertex(p1.edge(e1.next).vertex));
+            const v3 d1 = vsub(e1B, e1A);
+            const v3 e2A = p2.vertex(e2.vertex);
+            const v3 e2B = p2.vertex(p2.edge(e2.next).vertex);
+            const v3 d2 = vsub(e2B, e2A);
+            if (edges_minkowski(edge1_gauss(p1, e1, p1to2), p2, e2)) {
+                v3 axis;
+                const v3 c1 = xapply(p1to2, p1.centroid());
+                const float d = sat_edge_distance(e1A, e2A, c1, d1, d2, axis);
+                if (!wasColliding && d <= 0.0f) return;
+                if (wasColliding && clipPrev && d > 0.0f && d < DECIMAL_LARGEST) {
+                    v3 cp1, cp2;
+                    closest_points_segments(e1A, e1B, e2A, e2B, cp1, cp2);
+                    const float l1 = vlen2(d1), l2 = vlen2(d2);
+                    const float t1 = vdot(vsub(cp1, e2A), d2) / l2;
+                    const float t2 = vdot(vsub(cp2, e1A), d1) / l1;
+                    if (t1 >= 0.0f && t1 <= 1.0f && t2 >= 0.0f && t2 <= 1.0f) {
+                        if (it.report && lane == 0) it.out.add(qrot(it.t2.q, axis), d, xapply(p2to1, cp1), cp2);
+                        it.colliding = true;
+                        return;
+                    }
+                }
+            }
+        }
+    }
+
+    uint32_t f1 = 0, f2 = 0;
+    const float d1 = warp_sat_faces(p1, p2, p1to2, f1, lane);
+    if (d1 <= 0.0f) {
+        lf.set(RP3DG_LF_SAT_FACE_POLY1, true); lf.set(RP3DG_LF_SAT_FACE_POLY2, false); lf.sat_face = f1;
+        return;
+    }
+    const float d2 = warp_sat_faces(p2, p1, p2to1, f2, lane);
+    if (d2 <= 0.0f) {
+        lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, true); lf.sat_face = f2;
+        return;
+    }
+    const float faceMin = smin(d1, d2);
+    uint32_t minFace;
+    bool isFace1;
+    if (d1 < d2 * SAT_REL_TOL + SAT_ABS_TOL) { minFace = f1; isFace1 = true; }
+    else { minFace = f2; isFace1 = false; }
+
+    // stage the even half-edges of polyhedron 1 (in polyhedron-2 space)
+    const uint32_t n1h = (p1.nhe() + 1) / 2, n2h = (p2.nhe() + 1) / 2;
+    const v3 c1 = xapply(p1to2, p1.centroid());
+    for (uint32_t ih = lane; ih < n1h; ih += 32) {
+        const hedge e1 = p1.edge(2 * ih);
+        const v3 e1A = xapply(p1to2, p1.vertex(e1.vertex));
+        const v3 e1B = xapply(p1to2, p1.vertex(p1.edge(e1.next).vertex));
+        const v3 dir1 = vsub(e1B, e1A);
+        const Edge1Gauss g = edge1_gauss(p1, e1, p1to2);
+        Edge1Stage& s = stage[ih];
+        s.e1A[0] = e1A.x; s.e1A[1] = e1A.y; s.e1A[2] = e1A.z;
+        s.dir1[0] = dir1.x; s.dir1[1] = dir1.y; s.dir1[2] = dir1.z;
+        s.a[0] = g.a.x; s.a[1] = g.a.y; s.a[2] = g.a.z;
+        s.b[0] = g.b.x; s.b[1] = g.b.y; s.b[2] = g.b.z;
+        s.bxa[0] = g.bxa.x; s.bxa[1] = g.bxa.y; s.bxa[2] = g.bxa.z;
+    }
+    __syncwarp();
+    const uint32_t total = n1h * n2h;
+    float best = DECIMAL_LARGEST;
+    uint32_t bestIdx = 0xffffffffu;
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t idx = base + lane;
+        bool pass = false;
+        float d = DECIMAL_LARGEST;
+        if (idx < total) {
+            const uint32_t ih = idx / n2h, jh = idx - ih * n2h;
+            const Edge1Stage& s = stage[ih];
+            Edge1Gauss g;
+            g.a = V(s.a[0], s.a[1], s.a[2]);
+            g.b = V(s.b[0], s.b[1], s.b[2]);
+            g.bxa = V(s.bxa[0], s.bxa[1], s.bxa[2]);
+            hedge e2;
+            v3 e2A, dir2;
+            edge2_data(p2, 2 * jh, e2, e2A, dir2);
+            if (edges_minkowski(g, p2, e2)) {
+                pass = true;
+                v3 axis;
+                d = sat_edge_distance(V(s.e1A[0], s.e1A[1], s.e1A[2]), e2A, c1, V(s.dir1[0], s.dir1[1], s.dir1[2]),
+                                      dir2, axis);
+            }
+        }
+        const unsigned sep = __ballot_sync(FULL_MASK, pass && d <= 0.0f);
+        if (sep) {
+            const uint32_t first = base + uint32_t(__ffs(sep) - 1);
+            const uint32_t ih = first / n2h;
+            lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, false);
+            lf.sat_e1 = 2 * ih;
+            lf.sat_e2 = 2 * (first - ih * n2h);
+            __syncwarp();
+            return;
+        }
+        if (pass && d < best) { best = d; bestIdx = idx; }
+    }
+    warp_argmin(best, bestIdx);
+    __syncwarp();
+    const bool edgeWins = bestIdx != 0xffffffffu && best * SAT_REL_TOL + SAT_ABS_TOL < faceMin;
+
+    if (!edgeWins) {
+        bool found = false;
+        if (lane == 0) found = poly_face_contacts(isFace1, p1, p2, p1to2, p2to1, minFace, it);
+        found = __shfl_sync(FULL_MASK, found, 0);
+        lf.set(RP3DG_LF_SAT_FACE_POLY1, isFace1); lf.set(RP3DG_LF_SAT_FACE_POLY2, !isFace1); lf.sat_face = minFace;
+        if (!found) return;
+    } else {
+        const uint32_t ih = bestIdx / n2h, jh = bestIdx - ih * n2h;
+        if (it.report && lane == 0) {
+            const hedge e1 = p1.edge(2 * ih);
+            const v3 e1A = xapply(p1to2, p1.vertex(e1.vertex));
+            const v3 e1B = xapply(p1to2, p1.vertex(p1.edge(e1.next).vertex));
+            hedge e2;
+            v3 e2A, dir2;
+            edge2_data(p2, 2 * jh, e2, e2A, dir2);
+            const v3 e2B = p2.vertex(p2.edge(e2.next).vertex);
+            v3 axis;
+            sat_edge_distance(e1A, e2A, c1, vsub(e1B, e1A), dir2, axis);
+            v3 cp1, cp2;
+            closest_points_segments(e1A, e1B, e2A, e2B, cp1, cp2);
+            it.out.add(qrot(it.t2.q, axis), best, xapply(p2to1, cp1), cp2);
+        }
+        lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, false);
+        lf.sat_e1 = 2 * ih; lf.sat_e2 = 2 * jh;
+    }
+    it.colliding = true;
+}
+
 }  // namespace rp3dg
