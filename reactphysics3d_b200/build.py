@@ -21,17 +21,17 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std
          "-Xcompiler", "-fPIC,-ffp-contract=off", "--shared", "-Xptxas", "-v"] + FP_FLAGS
 
 
-def build(verbose=False):
-    os.makedirs(LIBDIR, exist_ok=True)
+def build(verbose=False, out=LIB, defines=()):
+    os.makedirs(os.path.dirname(out), exist_ok=True)
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    cmd = [NVCC] + FLAGS + srcs + ["-o", LIB, "-lcudart"]
+    cmd = [NVCC] + FLAGS + [f"-D{d}" for d in defines] + srcs + ["-o", out, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("nvcc failed building librp3dg.so")
     if verbose:
         sys.stdout.write(r.stderr)
-    return LIB
+    return out
 
 
 if __name__ == "__main__":

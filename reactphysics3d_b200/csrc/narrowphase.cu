@@ -8,7 +8,21 @@
 #include "narrowphase.cuh"
 #include "np_launch.h"
 
+// Kernel tuning knobs (compile time).  POLY_SCHEDULE: 0 = one thread per
+// polyhedron pair, 1 = box-box pairs per thread and mesh pairs per warp,
+// 2 = one warp per pair.  NP_MIN_BLOCKS: resident CTAs per SM requested from
+// the register allocator.
+#ifndef RP3DG_POLY_SCHEDULE
+#define RP3DG_POLY_SCHEDULE 1
+#endif
+#ifndef RP3DG_NP_MIN_BLOCKS
+#define RP3DG_NP_MIN_BLOCKS 3
+#endif
+
 namespace rp3dg {
+
+constexpr int POLY_SCHEDULE = RP3DG_POLY_SCHEDULE;
+constexpr int NP_MIN_BLOCKS = RP3DG_NP_MIN_BLOCKS;
 
 __constant__ BoxTables c_box_tables;
 
@@ -172,7 +186,7 @@ RD void process_pair_warp(const NpArgs& a, uint32_t i, int lane, const BoxTables
 }
 
 template <int ALGO>
-__global__ void __launch_bounds__(NP_BLOCK) narrowphase_kernel(const NpArgs a) {
+__global__ void __launch_bounds__(NP_BLOCK, NP_MIN_BLOCKS) narrowphase_kernel(const NpArgs a) {
     extern __shared__ uint32_t s_mesh[];
     __shared__ BoxTables s_box;
     constexpr bool uses_poly = ALGO >= RP3DG_ALGO_SPHERE_VS_CONVEX_POLYHEDRON;
@@ -188,11 +202,32 @@ __global__ void __launch_bounds__(NP_BLOCK) narrowphase_kernel(const NpArgs a) {
         __syncthreads();
     }
     if constexpr (ALGO == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON) {
+        // Hybrid schedule: each warp takes a tile of 32 pairs.  Box-box pairs
+        // (12x12 edge pairs) run one per thread; pairs with a convex mesh
+        // (up to 128 x 128 edge pairs) then run one at a time on the whole warp.
         __shared__ Edge1Stage s_stage[NP_BLOCK / 32][WARP_EDGE_CAP];
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const uint32_t nwarps = gridDim.x * (NP_BLOCK / 32);
-        for (uint32_t i = blockIdx.x * (NP_BLOCK / 32) + warp; i < a.n; i += nwarps)
-            process_pair_warp(a, i, lane, &s_box, mesh_words, s_stage[warp]);
+        for (uint32_t tile = blockIdx.x * (NP_BLOCK / 32) + warp; tile * 32u < a.n; tile += nwarps) {
+            const uint32_t i = tile * 32u + lane;
+            bool boxbox = false;
+            if (i < a.n) {
+                const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
+                if (uint32_t(i1) < a.nb_shapes && uint32_t(i2) < a.nb_shapes) {
+                    const ShapeRec r1 = load_shape(a.shapes, i1), r2 = load_shape(a.shapes, i2);
+                    boxbox = r1.kind == RP3DG_SHAPE_BOX && r2.kind == RP3DG_SHAPE_BOX;
+                }
+            }
+            if (POLY_SCHEDULE == 2) boxbox = false;      // every pair warp-cooperative
+            if (POLY_SCHEDULE == 0) boxbox = i < a.n;    // every pair on its own thread
+            if (boxbox) process_pair<ALGO>(a, i, &s_box, mesh_words);
+            unsigned coop = __ballot_sync(FULL_MASK, i < a.n && !boxbox);
+            while (coop) {
+                const int l = __ffs(coop) - 1;
+                coop &= coop - 1;
+                process_pair_warp(a, tile * 32u + uint32_t(l), lane, &s_box, mesh_words, s_stage[warp]);
+            }
+        }
     } else {
         const uint32_t stride = gridDim.x * blockDim.x;
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride)
@@ -221,8 +256,7 @@ cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaSt
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
     }
-    const uint32_t per_block = algo == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON ? NP_BLOCK / 32 : NP_BLOCK;
-    const uint32_t blocks_needed = (args.n + per_block - 1) / per_block;
+    const uint32_t blocks_needed = (args.n + NP_BLOCK - 1) / NP_BLOCK;
     // Enough CTAs to fill every SM several times; the grid-stride loop covers the rest.
     const uint32_t cap = uint32_t(num_sms) * 16u;
     const uint32_t blocks = blocks_needed < cap ? blocks_needed : cap;

@@ -794,6 +794,31 @@ RD bool edges_minkowski(const Edge1Gauss& g, const P2& p2, const hedge& e2) {
     const v3 dxc = vsub(p2.vertex(e2.vertex), p2.vertex(tw.vertex));
     return gauss_arcs(g.a, g.b, vneg(c), vneg(d), g.bxa, dxc);
 }
+// The same test when polyhedron 2 is a box.  The box's face normals and edge
+// vectors have one non-zero coordinate, so each of the four dot products of
+// testGaussMapArcsIntersect equals one product (the other terms are signed
+// zeros that cannot change a non-zero sum, and a zero result gives the same
+// comparison outcome whatever its sign).  c and d are the negated normals, so
+// c.bxa = -/+ bxa[m] exactly, and a.dxc = a[k] * D with D = +/-2h_k exactly.
+RD float axis_component(v3 v, uint32_t axis) { return axis == 0 ? v.x : (axis == 1 ? v.y : v.z); }
+RD bool edges_minkowski(const Edge1Gauss& g, const BoxPoly& p2, const hedge& e2, uint32_t j) {
+    const uint8_t* gi = p2.t->gauss[j];
+    const uint32_t k = gi[0] & 3u, m = gi[1] & 3u, n = gi[2] & 3u;
+    const float hk = axis_component(p2.he, k);
+    const float D = (gi[0] & 4u) ? -(hk + hk) : (hk + hk);
+    const float bm = axis_component(g.bxa, m), bn = axis_component(g.bxa, n);
+    const float cba = (gi[1] & 4u) ? -bm : bm;
+    const float dba = (gi[2] & 4u) ? -bn : bn;
+    const float adc = axis_component(g.a, k) * D;
+    const float bdc = axis_component(g.b, k) * D;
+    (void)e2;
+    return cba * dba < 0.0f && adc * bdc < 0.0f && cba * bdc > 0.0f;
+}
+template <class P2>
+RD bool edges_minkowski(const Edge1Gauss& g, const P2& p2, const hedge& e2, uint32_t) {
+    return edges_minkowski(g, p2, e2);
+}
+
 // computeDistanceBetweenEdges (SATAlgorithm.cpp:1040-1083); shape 1 is never a triangle here
 RD float sat_edge_distance(v3 e1A, v3 e2A, v3 c1, v3 d1, v3 d2, v3& outAxis) {
     if (are_parallel(d1, d2)) return DECIMAL_LARGEST;
@@ -920,7 +945,7 @@ RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
             const v3 e2A = p2.vertex(e2.vertex);
             const v3 e2B = p2.vertex(p2.edge(e2.next).vertex);
             const v3 d2 = vsub(e2B, e2A);
-            if (edges_minkowski(edge1_gauss(p1, e1, p1to2), p2, e2)) {
+            if (edges_minkowski(edge1_gauss(p1, e1, p1to2), p2, e2, lf.sat_e2)) {
                 v3 axis;
                 const v3 c1 = xapply(p1to2, p1.centroid());
                 const float d = sat_edge_distance(e1A, e2A, c1, d1, d2, axis);
@@ -972,7 +997,7 @@ RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
         const Edge1Gauss g = edge1_gauss(p1, e1, p1to2);
         for (uint32_t j = 0; j < nhe2; j += 2) {
             const hedge e2 = p2.edge(j);
-            if (edges_minkowski(g, p2, e2)) {
+            if (edges_minkowski(g, p2, e2, j)) {
                 const v3 e2A = p2.vertex(e2.vertex);
                 const v3 e2B = p2.vertex(p2.edge(e2.next).vertex);
                 v3 axis;
@@ -1166,7 +1191,7 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
             const v3 e2A = p2.vertex(e2.vertex);
             const v3 e2B = p2.vertex(p2.edge(e2.next).vertex);
             const v3 d2 = vsub(e2B, e2A);
-            if (edges_minkowski(edge1_gauss(p1, e1, p1to2), p2, e2)) {
+            if (edges_minkowski(edge1_gauss(p1, e1, p1to2), p2, e2, lf.sat_e2)) {
                 v3 axis;
                 const v3 c1 = xapply(p1to2, p1.centroid());
                 const float d = sat_edge_distance(e1A, e2A, c1, d1, d2, axis);
@@ -1238,7 +1263,7 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
             hedge e2;
             v3 e2A, dir2;
             edge2_data(p2, 2 * jh, e2, e2A, dir2);
-            if (edges_minkowski(g, p2, e2)) {
+            if (edges_minkowski(g, p2, e2, 2 * jh)) {
                 pass = true;
                 v3 axis;
                 d = sat_edge_distance(V(s.e1A[0], s.e1A[1], s.e1A[2]), e2A, c1, V(s.dir1[0], s.dir1[1], s.dir1[2]),

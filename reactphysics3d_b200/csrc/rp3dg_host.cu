@@ -136,6 +136,28 @@ BoxTables make_box_tables() {
     }
     for (int i = 0; i < 24; i++) t.face_verts[i] = uint8_t(faces[i]);
     for (int f = 0; f < 6; f++) t.face_edge[f] = uint8_t(fe[f]);
+    // Axis-aligned Gauss-map data (see BoxTables): vertex v has +x for
+    // v in {1,2,5,6}, +y for {2,3,6,7}, +z for {0,1,2,3}; face normals are
+    // 0:+z 1:+x 2:-z 3:-x 4:-y 5:+y.
+    auto pos = [](int v, int axis) {
+        const int masks[3] = {0x66, 0xCC, 0x0F};
+        return (masks[axis] >> v) & 1;
+    };
+    const int face_axis[6] = {2, 0, 2, 0, 1, 1};
+    const int face_neg[6] = {0, 0, 1, 1, 1, 0};
+    for (int e = 0; e < 24; e++) {
+        const int v1 = edges[e].vertex, v2 = edges[edges[e].twin].vertex;
+        int k = 0;
+        for (int ax = 0; ax < 3; ax++)
+            if (pos(v1, ax) != pos(v2, ax)) k = ax;
+        const int negD = pos(v1, k) ? 0 : 1;  // v1.k - v2.k = +2h when v1 is on the positive side
+        const int f1 = edges[e].face, f2 = edges[edges[e].twin].face;
+        // c = -normal: negative when the normal is positive
+        t.gauss[e][0] = uint8_t(k | (negD << 2));
+        t.gauss[e][1] = uint8_t(face_axis[f1] | ((face_neg[f1] ? 0 : 1) << 2));
+        t.gauss[e][2] = uint8_t(face_axis[f2] | ((face_neg[f2] ? 0 : 1) << 2));
+        t.gauss[e][3] = 0;
+    }
     return t;
 }
 

@@ -31,11 +31,17 @@ struct MeshHdr {
 static_assert(sizeof(MeshHdr) == 64, "MeshHdr layout");
 
 // Box topology (PhysicsCommon::initBoxShapeHalfEdgeStructure).
+// gauss[e] describes half-edge e for the Gauss-map test against a box:
+//   [0] = k | (negD << 2):  edge vector v(e.vertex) - v(twin.vertex) lies on
+//                           axis k, negative when negD is set
+//   [1] = m | (negC << 2):  c = -normal(e.face) lies on axis m
+//   [2] = n | (negD2 << 2): d = -normal(twin.face) lies on axis n
 struct BoxTables {
     uint8_t edges[24][4];  // vertex, twin, face, next
     uint8_t face_verts[24];
     uint8_t face_edge[6];
     uint8_t pad[2];
+    uint8_t gauss[24][4];
 };
 
 }  // namespace rp3dg
