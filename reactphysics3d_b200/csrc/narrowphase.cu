@@ -247,6 +247,23 @@ static const void* kernel_ptr(int algo) {
     return nullptr;
 }
 
+#ifdef RP3DG_PROFILE_PHASES
+// Profiling builds only: per-phase cycles (summed over warps) and counts of the
+// warp-cooperative SAT; phases 0 = setup + temporal coherence, 1 = faces of
+// polyhedron 1, 2 = faces of polyhedron 2, 3 = edge staging, 4 = edge pairs,
+// 5 = contact generation.  clear != 0 zeroes the counters after reading.
+extern "C" int rp3dg_profile_phases(unsigned long long* cycles, unsigned long long* counts, int clear) {
+    cudaMemcpyFromSymbol(cycles, g_phase_cycles, sizeof(unsigned long long) * 8);
+    cudaMemcpyFromSymbol(counts, g_phase_count, sizeof(unsigned long long) * 8);
+    if (clear) {
+        const unsigned long long z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        cudaMemcpyToSymbol(g_phase_cycles, z, sizeof(z));
+        cudaMemcpyToSymbol(g_phase_count, z, sizeof(z));
+    }
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -2;
+}
+#endif
+
 cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaStream_t stream) {
     if (args.n == 0) return cudaSuccess;
     const void* k = kernel_ptr(algo);

@@ -1111,6 +1111,34 @@ RD void capsule_poly(Item& it, bool cap1, CapsuleS cap, const P& poly) {
 constexpr unsigned FULL_MASK = 0xffffffffu;
 constexpr uint32_t WARP_EDGE_CAP = 128;  // even half-edges of polyhedron 1 staged per warp
 
+// Optional per-phase cycle counters (the device counterpart of the
+// reference's RP3D_PROFILE scopes), compiled in with -DRP3DG_PROFILE_PHASES.
+#ifdef RP3DG_PROFILE_PHASES
+__device__ unsigned long long g_phase_cycles[8];
+__device__ unsigned long long g_phase_count[8];
+struct PhaseTimer {
+    long long t;
+    int lane;
+    RD PhaseTimer(int l) : t(0), lane(l) {
+#ifdef __CUDA_ARCH__
+        t = clock64();
+#endif
+    }
+    RD void mark(int phase) {
+#ifdef __CUDA_ARCH__
+        const long long now = clock64();
+        if (lane == 0) { atomicAdd(&g_phase_cycles[phase], (unsigned long long)(now - t)); atomicAdd(&g_phase_count[phase], 1ull); }
+        t = now;
+#endif
+    }
+};
+#else
+struct PhaseTimer {
+    RD PhaseTimer(int) {}
+    RD void mark(int) {}
+};
+#endif
+
 // Per-edge data of polyhedron 1 in polyhedron-2 space, staged in shared memory.
 struct Edge1Stage {
     float e1A[3], dir1[3], a[3], b[3], bxa[3];
@@ -1158,6 +1186,7 @@ RD void edge2_data(const P2& p2, uint32_t j, hedge& e2, v3& e2A, v3& dir2) {
 // Every lane holds the same pair state; contacts and outputs are produced by lane 0.
 template <class P1, class P2>
 RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, int lane, Edge1Stage* stage) {
+    PhaseTimer timer(lane);
     const xform p1to2 = xmul(xinv(it.t2), it.t1);
     const xform p2to1 = xinv(p1to2);
     LastFrame& lf = it.lf;
@@ -1212,13 +1241,16 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
         }
     }
 
+    timer.mark(0);
     uint32_t f1 = 0, f2 = 0;
     const float d1 = warp_sat_faces(p1, p2, p1to2, f1, lane);
+    timer.mark(1);
     if (d1 <= 0.0f) {
         lf.set(RP3DG_LF_SAT_FACE_POLY1, true); lf.set(RP3DG_LF_SAT_FACE_POLY2, false); lf.sat_face = f1;
         return;
     }
     const float d2 = warp_sat_faces(p2, p1, p2to1, f2, lane);
+    timer.mark(2);
     if (d2 <= 0.0f) {
         lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, true); lf.sat_face = f2;
         return;
@@ -1246,6 +1278,7 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
         s.bxa[0] = g.bxa.x; s.bxa[1] = g.bxa.y; s.bxa[2] = g.bxa.z;
     }
     __syncwarp();
+    timer.mark(3);
     const uint32_t total = n1h * n2h;
     float best = DECIMAL_LARGEST;
     uint32_t bestIdx = 0xffffffffu;
@@ -1284,6 +1317,7 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
     }
     warp_argmin(best, bestIdx);
     __syncwarp();
+    timer.mark(4);
     const bool edgeWins = bestIdx != 0xffffffffu && best * SAT_REL_TOL + SAT_ABS_TOL < faceMin;
 
     if (!edgeWins) {
@@ -1311,6 +1345,7 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
         lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, false);
         lf.sat_e1 = 2 * ih; lf.sat_e2 = 2 * jh;
     }
+    timer.mark(5);
     it.colliding = true;
 }
 
