@@ -160,7 +160,7 @@ RD void process_pair(const NpArgs& a, uint32_t i, const BoxTables* box, const ui
 
 // Convex polyhedron vs convex polyhedron, one warp per pair.
 RD void process_pair_warp(const NpArgs& a, uint32_t i, int lane, const BoxTables* box, const uint32_t* mesh_words,
-                          Edge1Stage* stage) {
+                          WarpScratch& stage) {
     const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
     if (uint32_t(i1) >= a.nb_shapes || uint32_t(i2) >= a.nb_shapes) {
         if (lane == 0) {
@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(NP_BLOCK, NP_MIN_BLOCKS) narrowphase_kernel(co
         // Hybrid schedule: each warp takes a tile of 32 pairs.  Box-box pairs
         // (12x12 edge pairs) run one per thread; pairs with a convex mesh
         // (up to 128 x 128 edge pairs) then run one at a time on the whole warp.
-        __shared__ Edge1Stage s_stage[NP_BLOCK / 32][WARP_EDGE_CAP];
+        __shared__ WarpScratch s_stage[NP_BLOCK / 32];
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const uint32_t nwarps = gridDim.x * (NP_BLOCK / 32);
         for (uint32_t tile = blockIdx.x * (NP_BLOCK / 32) + warp; tile * 32u < a.n; tile += nwarps) {

@@ -157,10 +157,10 @@ struct ContactSink {
     v3 first_normal;
     float first_depth;
     // NarrowPhaseInfoBatch::addContactPoint (NarrowPhaseInfoBatch.h:170-185)
-    RD void add(v3 nrm, float depth, v3 p1, v3 p2) {
+    RD void add(v3 nrm, float depth, v3 p1, v3 p2, bool write = true) {
         if (count < MAX_CONTACTS) {
             if (count == 0) { first_normal = nrm; first_depth = depth; }
-            if (count < max) {
+            if (write && count < max) {
                 const size_t o = size_t(count) * n + i;
                 nd[o] = make_float4(nrm.x, nrm.y, nrm.z, depth);
                 l1[o] = make_float4(p1.x, p1.y, p1.z, 0.0f);
@@ -1143,6 +1143,14 @@ struct PhaseTimer {
 struct Edge1Stage {
     float e1A[3], dir1[3], a[3], b[3], bxa[3];
 };
+// Shared-memory scratch of one warp: staged edges, the list of edge pairs
+// that pass the Gauss-map test (in visiting order) and the clip polygon.
+constexpr uint32_t WARP_CAND_CAP = 512;
+struct WarpScratch {
+    Edge1Stage stage[WARP_EDGE_CAP];
+    uint16_t cand[WARP_CAND_CAP];
+    v3 poly[CLIP_MAX];
+};
 
 RD void warp_argmin(float& d, uint32_t& idx) {
     for (int o = 16; o; o >>= 1) {
@@ -1182,10 +1190,127 @@ RD void edge2_data(const P2& p2, uint32_t j, hedge& e2, v3& e2A, v3& dir2) {
     dir2 = vsub(p2.vertex(p2.edge(e2.next).vertex), e2A);
 }
 
+// findMostAntiParallelFace with the faces spread over lanes: minimum dot
+// product, first face on ties (the reference's strict '<' keeps the first).
+template <class P>
+RD uint32_t warp_most_antiparallel_face(const P& p, v3 dir, int lane) {
+    float best = DECIMAL_LARGEST;
+    uint32_t bestF = 0xffffffffu;
+    const uint32_t nf = p.nfaces();
+    for (uint32_t f = lane; f < nf; f += 32) {
+        const float d = vdot(p.normal(f), dir);
+        if (d < best) { best = d; bestF = f; }
+    }
+    warp_argmin(best, bestF);
+    return bestF == 0xffffffffu ? 0u : bestF;
+}
+
+RD uint32_t warp_exclusive_scan(uint32_t v, int lane, uint32_t& total) {
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL_MASK, x, o);
+        if (lane >= o) x += y;
+    }
+    total = __shfl_sync(FULL_MASK, x, 31);
+    return x - v;
+}
+
+// computePolyhedronVsPolyhedronFaceContactPoints (SATAlgorithm.cpp:893-1036)
+// on a whole warp.  Each Sutherland-Hodgman pass (clipPolygonWithPlane,
+// mathematics_functions.h:332-393) gives lane l the polygon edge that ends at
+// vertex l; its 0, 1 or 2 output points go to position (exclusive prefix sum
+// of the counts), which is exactly the sequential output order.  Vertex dot
+// products are the same expressions as in the sequential pass.  Contacts are
+// appended in clipped-vertex order.  All lanes return the same value.
+template <class PR, class PI>
+RD bool warp_face_contacts(bool ref1, const PR& refP, const PI& incP, const xform& r2i, const xform& i2r,
+                           uint32_t minFace, Item& it, int lane, v3* poly) {
+    const v3 axisR = refP.normal(minFace);
+    const v3 axisI = qrot(r2i.q, axisR);
+    const v3 nw = ref1 ? qrot(it.t1.q, axisR) : vneg(qrot(it.t2.q, axisR));
+    const uint32_t incFace = warp_most_antiparallel_face(incP, axisI, lane);
+    uint32_t n = incP.face_count(incFace);
+    if (n > CLIP_MAX) n = CLIP_MAX;
+    v3 P = V(0.0f, 0.0f, 0.0f);
+    if (uint32_t(lane) < n) P = xapply(i2r, incP.vertex(incP.face_vertex(incFace, lane)));
+    const uint32_t firstEdge = refP.face_edge(minFace);
+    hedge cur = refP.edge(firstEdge);
+    v3 ev1 = refP.vertex(cur.vertex);
+    uint32_t curIdx, guard = 0;
+    do {
+        const hedge nxt = refP.edge(cur.next);
+        const v3 ev2 = refP.vertex(nxt.vertex);
+        const v3 pn = vcross(axisR, vsub(ev2, ev1));
+        const float pnpp = vdot(pn, ev1);
+        const bool active = uint32_t(lane) < n;
+        const float ven = active ? vdot(vsub(P, ev1), pn) : 0.0f;
+        const int src = lane == 0 ? int(n) - 1 : lane - 1;
+        const v3 S = V(__shfl_sync(FULL_MASK, P.x, src), __shfl_sync(FULL_MASK, P.y, src), __shfl_sync(FULL_MASK, P.z, src));
+        const float vsn = __shfl_sync(FULL_MASK, ven, src);
+        v3 o0 = V(0.0f, 0.0f, 0.0f), o1 = V(0.0f, 0.0f, 0.0f);
+        uint32_t cnt = 0;
+        if (active) {
+            if (ven >= 0.0f) {
+                if (vsn < 0.0f) {
+                    const float t = plane_segment_intersection(S, P, pnpp, pn);
+                    o0 = (t >= 0.0f && t <= 1.0f) ? vadd(S, vmul(vsub(P, S), t)) : P;
+                    o1 = P;
+                    cnt = 2;
+                } else {
+                    o0 = P;
+                    cnt = 1;
+                }
+            } else if (vsn >= 0.0f) {
+                const float t = plane_segment_intersection(S, P, -pnpp, vneg(pn));
+                o0 = (t >= 0.0f && t <= 1.0f) ? vadd(S, vmul(vsub(P, S), t)) : S;
+                cnt = 1;
+            }
+        }
+        uint32_t total;
+        const uint32_t pos = warp_exclusive_scan(cnt, lane, total);
+        __syncwarp();
+        if (cnt >= 1 && pos < CLIP_MAX) poly[pos] = o0;
+        if (cnt == 2 && pos + 1 < CLIP_MAX) poly[pos + 1] = o1;
+        __syncwarp();
+        n = total < CLIP_MAX ? total : CLIP_MAX;
+        if (uint32_t(lane) < n) P = poly[lane];
+        __syncwarp();
+        curIdx = cur.next;
+        cur = nxt;
+        ev1 = ev2;
+    } while (curIdx != firstEdge && n > 0 && ++guard < MAX_FACE_VERTICES);
+    const v3 refV = refP.vertex(refP.edge(firstEdge).vertex);
+    const bool active = uint32_t(lane) < n;
+    const float depth = active ? vdot(vsub(refV, P), axisR) : 0.0f;
+    const bool hit = active && depth > 0.0f;
+    const unsigned mask = __ballot_sync(FULL_MASK, hit);
+    if (mask && it.report) {
+        const uint32_t slot = it.out.count + __popc(mask & ((1u << lane) - 1u));
+        if (hit && slot < MAX_CONTACTS) {
+            const v3 pInc = xapply(r2i, P);
+            const v3 pRef = project_onto_plane(P, axisR, refV);
+            ContactSink s = it.out;
+            s.count = slot;
+            s.add(nw, depth, ref1 ? pRef : pInc, ref1 ? pInc : pRef);
+        }
+        const uint32_t c = it.out.count + __popc(mask);
+        it.out.count = c < MAX_CONTACTS ? c : MAX_CONTACTS;
+    }
+    return mask != 0;
+}
+
+template <class P1, class P2>
+RD bool warp_poly_face_contacts(bool ref1, const P1& p1, const P2& p2, const xform& p1to2, const xform& p2to1,
+                                uint32_t minFace, Item& it, int lane, v3* poly) {
+    if (ref1) return warp_face_contacts(true, p1, p2, p1to2, p2to1, minFace, it, lane, poly);
+    return warp_face_contacts(false, p2, p1, p2to1, p1to2, minFace, it, lane, poly);
+}
+
 // testCollisionConvexPolyhedronVsConvexPolyhedron (SATAlgorithm.cpp:485-889), one warp per pair.
 // Every lane holds the same pair state; contacts and outputs are produced by lane 0.
 template <class P1, class P2>
-RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, int lane, Edge1Stage* stage) {
+RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, int lane, WarpScratch& ws) {
+    Edge1Stage* stage = ws.stage;
     PhaseTimer timer(lane);
     const xform p1to2 = xmul(xinv(it.t2), it.t1);
     const xform p2to1 = xinv(p1to2);
@@ -1201,9 +1326,7 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
             const float d = face1 ? sat_single_face(p1, p2, p1to2, lf.sat_face) : sat_single_face(p2, p1, p2to1, lf.sat_face);
             if (!wasColliding && d <= 0.0f) return;
             if (wasColliding && clipPrev && d > 0.0f) {
-                bool found = false;
-                if (lane == 0) found = poly_face_contacts(face1, p1, p2, p1to2, p2to1, lf.sat_face, it);
-                found = __shfl_sync(FULL_MASK, found, 0);
+                const bool found = warp_poly_face_contacts(face1, p1, p2, p1to2, p2to1, lf.sat_face, it, lane, ws.poly);
                 if (found) {
                     lf.set(RP3DG_LF_SAT_FACE_POLY1, face1);
                     lf.set(RP3DG_LF_SAT_FACE_POLY2, !face1);
@@ -1232,7 +1355,7 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
                     const float t1 = vdot(vsub(cp1, e2A), d2) / l2;
                     const float t2 = vdot(vsub(cp2, e1A), d1) / l1;
                     if (t1 >= 0.0f && t1 <= 1.0f && t2 >= 0.0f && t2 <= 1.0f) {
-                        if (it.report && lane == 0) it.out.add(qrot(it.t2.q, axis), d, xapply(p2to1, cp1), cp2);
+                        if (it.report) it.out.add(qrot(it.t2.q, axis), d, xapply(p2to1, cp1), cp2, lane == 0);
                         it.colliding = true;
                         return;
                     }
@@ -1282,38 +1405,65 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
     const uint32_t total = n1h * n2h;
     float best = DECIMAL_LARGEST;
     uint32_t bestIdx = 0xffffffffu;
-    for (uint32_t base = 0; base < total; base += 32) {
-        const uint32_t idx = base + lane;
-        bool pass = false;
-        float d = DECIMAL_LARGEST;
-        if (idx < total) {
-            const uint32_t ih = idx / n2h, jh = idx - ih * n2h;
-            const Edge1Stage& s = stage[ih];
-            Edge1Gauss g;
-            g.a = V(s.a[0], s.a[1], s.a[2]);
-            g.b = V(s.b[0], s.b[1], s.b[2]);
-            g.bxa = V(s.bxa[0], s.bxa[1], s.bxa[2]);
-            hedge e2;
-            v3 e2A, dir2;
-            edge2_data(p2, 2 * jh, e2, e2A, dir2);
-            if (edges_minkowski(g, p2, e2, 2 * jh)) {
-                pass = true;
-                v3 axis;
+    // Pass 1 walks the edge pairs in visiting order and appends the ones that
+    // pass the Gauss-map test to ws.cand; pass 2 (run whenever the list could
+    // overflow, and at the end) computes their distances 32 at a time.  The
+    // list keeps visiting order, so the first separating pair and the
+    // first arg-min are those of the sequential loop.
+    uint32_t ih = uint32_t(lane) / n2h, jh = uint32_t(lane) - (uint32_t(lane) / n2h) * n2h;
+    const uint32_t qstep = 32u / n2h, rstep = 32u - qstep * n2h;
+    uint32_t ncand = 0;
+    bool separated = false;
+    for (uint32_t base = 0; base < total || ncand > 0;) {
+        if (base < total && ncand + 32 <= WARP_CAND_CAP) {
+            const uint32_t idx = base + lane;
+            bool pass = false;
+            if (idx < total) {
+                const Edge1Stage& s = stage[ih];
+                Edge1Gauss g;
+                g.a = V(s.a[0], s.a[1], s.a[2]);
+                g.b = V(s.b[0], s.b[1], s.b[2]);
+                g.bxa = V(s.bxa[0], s.bxa[1], s.bxa[2]);
+                pass = edges_minkowski(g, p2, p2.edge(2 * jh), 2 * jh);
+            }
+            const unsigned m = __ballot_sync(FULL_MASK, pass);
+            if (pass) ws.cand[ncand + __popc(m & ((1u << lane) - 1u))] = uint16_t(idx);
+            ncand += __popc(m);
+            base += 32;
+            jh += rstep; ih += qstep;
+            if (jh >= n2h) { jh -= n2h; ih++; }
+            continue;
+        }
+        __syncwarp();
+        for (uint32_t c0 = 0; c0 < ncand && !separated; c0 += 32) {
+            const uint32_t c = c0 + lane;
+            float d = DECIMAL_LARGEST;
+            uint32_t idx = 0xffffffffu;
+            if (c < ncand) {
+                idx = ws.cand[c];
+                const uint32_t ci = idx / n2h, cj = idx - ci * n2h;
+                const Edge1Stage& s = stage[ci];
+                hedge e2;
+                v3 e2A, dir2, axis;
+                edge2_data(p2, 2 * cj, e2, e2A, dir2);
                 d = sat_edge_distance(V(s.e1A[0], s.e1A[1], s.e1A[2]), e2A, c1, V(s.dir1[0], s.dir1[1], s.dir1[2]),
                                       dir2, axis);
             }
+            const unsigned sep = __ballot_sync(FULL_MASK, c < ncand && d <= 0.0f);
+            if (sep) {
+                const uint32_t first = __shfl_sync(FULL_MASK, idx, __ffs(sep) - 1);
+                const uint32_t fi = first / n2h;
+                lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, false);
+                lf.sat_e1 = 2 * fi;
+                lf.sat_e2 = 2 * (first - fi * n2h);
+                separated = true;
+            } else if (c < ncand && d < best) {
+                best = d; bestIdx = idx;
+            }
         }
-        const unsigned sep = __ballot_sync(FULL_MASK, pass && d <= 0.0f);
-        if (sep) {
-            const uint32_t first = base + uint32_t(__ffs(sep) - 1);
-            const uint32_t ih = first / n2h;
-            lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, false);
-            lf.sat_e1 = 2 * ih;
-            lf.sat_e2 = 2 * (first - ih * n2h);
-            __syncwarp();
-            return;
-        }
-        if (pass && d < best) { best = d; bestIdx = idx; }
+        __syncwarp();
+        if (separated) return;
+        ncand = 0;
     }
     warp_argmin(best, bestIdx);
     __syncwarp();
@@ -1321,14 +1471,12 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
     const bool edgeWins = bestIdx != 0xffffffffu && best * SAT_REL_TOL + SAT_ABS_TOL < faceMin;
 
     if (!edgeWins) {
-        bool found = false;
-        if (lane == 0) found = poly_face_contacts(isFace1, p1, p2, p1to2, p2to1, minFace, it);
-        found = __shfl_sync(FULL_MASK, found, 0);
+        const bool found = warp_poly_face_contacts(isFace1, p1, p2, p1to2, p2to1, minFace, it, lane, ws.poly);
         lf.set(RP3DG_LF_SAT_FACE_POLY1, isFace1); lf.set(RP3DG_LF_SAT_FACE_POLY2, !isFace1); lf.sat_face = minFace;
         if (!found) return;
     } else {
         const uint32_t ih = bestIdx / n2h, jh = bestIdx - ih * n2h;
-        if (it.report && lane == 0) {
+        if (it.report) {
             const hedge e1 = p1.edge(2 * ih);
             const v3 e1A = xapply(p1to2, p1.vertex(e1.vertex));
             const v3 e1B = xapply(p1to2, p1.vertex(p1.edge(e1.next).vertex));
@@ -1340,7 +1488,7 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
             sat_edge_distance(e1A, e2A, c1, vsub(e1B, e1A), dir2, axis);
             v3 cp1, cp2;
             closest_points_segments(e1A, e1B, e2A, e2B, cp1, cp2);
-            it.out.add(qrot(it.t2.q, axis), best, xapply(p2to1, cp1), cp2);
+            it.out.add(qrot(it.t2.q, axis), best, xapply(p2to1, cp1), cp2, lane == 0);
         }
         lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, false);
         lf.sat_e1 = 2 * ih; lf.sat_e2 = 2 * jh;
