@@ -13,7 +13,7 @@
 // 2 = one warp per pair.  NP_MIN_BLOCKS: resident CTAs per SM requested from
 // the register allocator.
 #ifndef RP3DG_POLY_SCHEDULE
-#define RP3DG_POLY_SCHEDULE 1
+#define RP3DG_POLY_SCHEDULE 2
 #endif
 #ifndef RP3DG_NP_MIN_BLOCKS
 #define RP3DG_NP_MIN_BLOCKS 3
@@ -269,8 +269,12 @@ cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaSt
     const void* k = kernel_ptr(algo);
     if (!k) return cudaErrorInvalidValue;
     size_t smem = args.stage_mesh ? size_t(args.mesh_nwords) * 4 : 0;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, k);
+    if (e != cudaSuccess) return e;
+    // static + dynamic shared memory above 48 KB needs the opt-in attribute
+    if (smem > 0 && fa.sharedSizeBytes + smem > 48 * 1024) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
     }
     const uint32_t blocks_needed = (args.n + NP_BLOCK - 1) / NP_BLOCK;

@@ -1183,6 +1183,42 @@ RD float warp_sat_faces(const PA& pa, const PB& pb, const xform& a2b, uint32_t& 
     return best;
 }
 
+// Support point of a convex mesh with the vertices spread over lanes
+// (ConvexMeshShape::getLocalSupportPointWithoutMargin, ConvexMeshShape.cpp:80-102):
+// the first vertex with the largest dot product; a dot product only counts
+// when it beats DECIMAL_SMALLEST, exactly like the reference's running maximum.
+RD v3 warp_mesh_support(const MeshPoly& m, v3 d, int lane) {
+    float best = DECIMAL_SMALLEST;
+    uint32_t bi = 0xffffffffu;
+    const uint32_t nv = m.h->nv, o = m.h->off_verts;
+    for (uint32_t i = lane; i < nv; i += 32) {
+        const float dp = vdot(d, V(m.f(o + 3 * i), m.f(o + 3 * i + 1), m.f(o + 3 * i + 2)));
+        if (dp > best) { best = dp; bi = i; }
+    }
+    for (int s = 16; s; s >>= 1) {
+        const float ob = __shfl_xor_sync(FULL_MASK, best, s);
+        const uint32_t oi = __shfl_xor_sync(FULL_MASK, bi, s);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    return m.vertex(bi == 0xffffffffu ? 0u : bi);
+}
+
+// testFacesDirectionPolyhedronVsPolyhedron for the faces of a box against a
+// convex mesh: faces in order (first separating face, strict minimum), the
+// mesh support search spread over the lanes.
+RD float warp_sat_faces(const BoxPoly& pa, const MeshPoly& pb, const xform& a2b, uint32_t& minFace, int lane) {
+    float minDepth = DECIMAL_LARGEST;
+    for (uint32_t f = 0; f < 6; f++) {
+        const v3 fn2 = qrot(a2b.q, pa.normal(f));
+        const v3 sp = warp_mesh_support(pb, vneg(fn2), lane);
+        const v3 fv = xapply(a2b, pa.vertex(pa.face_vertex(f, 0)));
+        const float d = vdot(vsub(fv, sp), fn2);
+        if (d <= 0.0f) { minFace = f; return d; }
+        if (d < minDepth) { minDepth = d; minFace = f; }
+    }
+    return minDepth;
+}
+
 template <class P2>
 RD void edge2_data(const P2& p2, uint32_t j, hedge& e2, v3& e2A, v3& dir2) {
     e2 = p2.edge(j);
@@ -1306,6 +1342,71 @@ RD bool warp_poly_face_contacts(bool ref1, const P1& p1, const P2& p2, const xfo
     return warp_face_contacts(false, p2, p1, p2to1, p1to2, minFace, it, lane, poly);
 }
 
+// Walks the edge pairs (i, j) of the reference's double loop in visiting
+// order, a round at a time; lane `offset` of a round holds pair base + offset.
+// Generic polyhedron 2: 32 consecutive pairs per round.
+template <class P2>
+struct EdgePairWalker {
+    const P2& p2;
+    uint32_t n2h, ih, jh, qstep, rstep, offset, per_round;
+    bool active;
+    RD EdgePairWalker(const P2& p, uint32_t n2, int lane) : p2(p), n2h(n2) {
+        ih = uint32_t(lane) / n2h;
+        jh = uint32_t(lane) - ih * n2h;
+        qstep = 32u / n2h;
+        rstep = 32u - qstep * n2h;
+        offset = uint32_t(lane);
+        per_round = 32;
+        active = true;
+    }
+    RD bool test(const Edge1Stage* stage) const {
+        const Edge1Stage& s = stage[ih];
+        Edge1Gauss g;
+        g.a = V(s.a[0], s.a[1], s.a[2]);
+        g.b = V(s.b[0], s.b[1], s.b[2]);
+        g.bxa = V(s.bxa[0], s.bxa[1], s.bxa[2]);
+        return edges_minkowski(g, p2, p2.edge(2 * jh), 2 * jh);
+    }
+    RD void advance() {
+        jh += rstep; ih += qstep;
+        if (jh >= n2h) { jh -= n2h; ih++; }
+    }
+};
+// Box polyhedron 2: its 12 even half-edges are fixed per lane (lanes 0..23 =
+// two rows i of the loop), so each lane keeps its box edge's Gauss-map data in
+// registers and reads only the three components of the staged edge it needs.
+template <>
+struct EdgePairWalker<BoxPoly> {
+    uint32_t ih, offset, per_round;
+    bool active;
+    uint32_t k, m, n;
+    bool negC, negD2;
+    float D;
+    RD EdgePairWalker(const BoxPoly& p2, uint32_t, int lane) {
+        active = lane < 24;
+        const uint32_t jh = uint32_t(lane) % 12u, half = uint32_t(lane) / 12u;
+        ih = half;
+        offset = uint32_t(lane);
+        per_round = 24;
+        const uint8_t* gi = p2.t->gauss[2 * jh];
+        k = gi[0] & 3u; m = gi[1] & 3u; n = gi[2] & 3u;
+        negC = (gi[1] & 4u) != 0;
+        negD2 = (gi[2] & 4u) != 0;
+        const float hk = axis_component(p2.he, k);
+        D = (gi[0] & 4u) ? -(hk + hk) : (hk + hk);
+    }
+    RD bool test(const Edge1Stage* stage) const {
+        const Edge1Stage& s = stage[ih];
+        const float bm = s.bxa[m], bn = s.bxa[n];
+        const float cba = negC ? -bm : bm;
+        const float dba = negD2 ? -bn : bn;
+        const float adc = s.a[k] * D;
+        const float bdc = s.b[k] * D;
+        return cba * dba < 0.0f && adc * bdc < 0.0f && cba * bdc > 0.0f;
+    }
+    RD void advance() { ih += 2; }
+};
+
 // testCollisionConvexPolyhedronVsConvexPolyhedron (SATAlgorithm.cpp:485-889), one warp per pair.
 // Every lane holds the same pair state; contacts and outputs are produced by lane 0.
 template <class P1, class P2>
@@ -1410,28 +1511,18 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
     // overflow, and at the end) computes their distances 32 at a time.  The
     // list keeps visiting order, so the first separating pair and the
     // first arg-min are those of the sequential loop.
-    uint32_t ih = uint32_t(lane) / n2h, jh = uint32_t(lane) - (uint32_t(lane) / n2h) * n2h;
-    const uint32_t qstep = 32u / n2h, rstep = 32u - qstep * n2h;
     uint32_t ncand = 0;
     bool separated = false;
+    EdgePairWalker<P2> walk(p2, n2h, lane);
     for (uint32_t base = 0; base < total || ncand > 0;) {
         if (base < total && ncand + 32 <= WARP_CAND_CAP) {
-            const uint32_t idx = base + lane;
-            bool pass = false;
-            if (idx < total) {
-                const Edge1Stage& s = stage[ih];
-                Edge1Gauss g;
-                g.a = V(s.a[0], s.a[1], s.a[2]);
-                g.b = V(s.b[0], s.b[1], s.b[2]);
-                g.bxa = V(s.bxa[0], s.bxa[1], s.bxa[2]);
-                pass = edges_minkowski(g, p2, p2.edge(2 * jh), 2 * jh);
-            }
+            const uint32_t idx = base + walk.offset;
+            const bool pass = walk.active && idx < total && walk.test(stage);
             const unsigned m = __ballot_sync(FULL_MASK, pass);
             if (pass) ws.cand[ncand + __popc(m & ((1u << lane) - 1u))] = uint16_t(idx);
             ncand += __popc(m);
-            base += 32;
-            jh += rstep; ih += qstep;
-            if (jh >= n2h) { jh -= n2h; ih++; }
+            base += walk.per_round;
+            walk.advance();
             continue;
         }
         __syncwarp();
