@@ -16,7 +16,7 @@
 #define RP3DG_POLY_SCHEDULE 2
 #endif
 #ifndef RP3DG_NP_MIN_BLOCKS
-#define RP3DG_NP_MIN_BLOCKS 3
+#define RP3DG_NP_MIN_BLOCKS 4
 #endif
 
 namespace rp3dg {

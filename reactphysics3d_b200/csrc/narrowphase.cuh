@@ -1207,10 +1207,38 @@ RD v3 warp_mesh_support(const MeshPoly& m, v3 d, int lane) {
 // convex mesh: faces in order (first separating face, strict minimum), the
 // mesh support search spread over the lanes.
 RD float warp_sat_faces(const BoxPoly& pa, const MeshPoly& pb, const xform& a2b, uint32_t& minFace, int lane) {
+    // the six support searches run side by side (independent accumulators)
+    v3 dir[6];
+    float best[6];
+    uint32_t bi[6];
+#pragma unroll
+    for (uint32_t f = 0; f < 6; f++) {
+        dir[f] = vneg(qrot(a2b.q, pa.normal(f)));
+        best[f] = DECIMAL_SMALLEST;
+        bi[f] = 0xffffffffu;
+    }
+    const uint32_t nv = pb.h->nv, o = pb.h->off_verts;
+    for (uint32_t i = lane; i < nv; i += 32) {
+        const v3 v = V(pb.f(o + 3 * i), pb.f(o + 3 * i + 1), pb.f(o + 3 * i + 2));
+#pragma unroll
+        for (uint32_t f = 0; f < 6; f++) {
+            const float dp = vdot(dir[f], v);
+            if (dp > best[f]) { best[f] = dp; bi[f] = i; }
+        }
+    }
+#pragma unroll
+    for (int sft = 16; sft; sft >>= 1) {
+#pragma unroll
+        for (uint32_t f = 0; f < 6; f++) {
+            const float ob = __shfl_xor_sync(FULL_MASK, best[f], sft);
+            const uint32_t oi = __shfl_xor_sync(FULL_MASK, bi[f], sft);
+            if (ob > best[f] || (ob == best[f] && oi < bi[f])) { best[f] = ob; bi[f] = oi; }
+        }
+    }
     float minDepth = DECIMAL_LARGEST;
     for (uint32_t f = 0; f < 6; f++) {
         const v3 fn2 = qrot(a2b.q, pa.normal(f));
-        const v3 sp = warp_mesh_support(pb, vneg(fn2), lane);
+        const v3 sp = pb.vertex(bi[f] == 0xffffffffu ? 0u : bi[f]);
         const v3 fv = xapply(a2b, pa.vertex(pa.face_vertex(f, 0)));
         const float d = vdot(vsub(fv, sp), fn2);
         if (d <= 0.0f) { minFace = f; return d; }
@@ -1371,6 +1399,9 @@ struct EdgePairWalker {
         jh += rstep; ih += qstep;
         if (jh >= n2h) { jh -= n2h; ih++; }
     }
+    static constexpr int UNROLL = 1;
+    RD bool test_ahead(const Edge1Stage* stage, int) const { return test(stage); }
+    RD void advance_by(int u) { for (int k = 0; k < u; k++) advance(); }
 };
 // Box polyhedron 2: its 12 even half-edges are fixed per lane (lanes 0..23 =
 // two rows i of the loop), so each lane keeps its box edge's Gauss-map data in
@@ -1395,8 +1426,9 @@ struct EdgePairWalker<BoxPoly> {
         const float hk = axis_component(p2.he, k);
         D = (gi[0] & 4u) ? -(hk + hk) : (hk + hk);
     }
-    RD bool test(const Edge1Stage* stage) const {
-        const Edge1Stage& s = stage[ih];
+    RD bool test(const Edge1Stage* stage) const { return test_ahead(stage, 0); }
+    RD bool test_ahead(const Edge1Stage* stage, int u) const {
+        const Edge1Stage& s = stage[ih + 2 * u];
         const float bm = s.bxa[m], bn = s.bxa[n];
         const float cba = negC ? -bm : bm;
         const float dba = negD2 ? -bn : bn;
@@ -1405,6 +1437,8 @@ struct EdgePairWalker<BoxPoly> {
         return cba * dba < 0.0f && adc * bdc < 0.0f && cba * bdc > 0.0f;
     }
     RD void advance() { ih += 2; }
+    static constexpr int UNROLL = 4;
+    RD void advance_by(int u) { ih += 2 * u; }
 };
 
 // testCollisionConvexPolyhedronVsConvexPolyhedron (SATAlgorithm.cpp:485-889), one warp per pair.
@@ -1515,6 +1549,27 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
     bool separated = false;
     EdgePairWalker<P2> walk(p2, n2h, lane);
     for (uint32_t base = 0; base < total || ncand > 0;) {
+        if (EdgePairWalker<P2>::UNROLL > 1 && base < total && ncand + 32 * EdgePairWalker<P2>::UNROLL <= WARP_CAND_CAP) {
+            // several rounds at once: independent loads and tests, then the
+            // ballots in round order (keeps the visiting order)
+            constexpr int U = EdgePairWalker<P2>::UNROLL;
+            bool pass[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const uint32_t idx = base + u * walk.per_round + walk.offset;
+                pass[u] = walk.active && idx < total && walk.test_ahead(stage, u);
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const uint32_t idx = base + u * walk.per_round + walk.offset;
+                const unsigned m = __ballot_sync(FULL_MASK, pass[u]);
+                if (pass[u]) ws.cand[ncand + __popc(m & ((1u << lane) - 1u))] = uint16_t(idx);
+                ncand += __popc(m);
+            }
+            base += U * walk.per_round;
+            walk.advance_by(U);
+            continue;
+        }
         if (base < total && ncand + 32 <= WARP_CAND_CAP) {
             const uint32_t idx = base + walk.offset;
             const bool pass = walk.active && idx < total && walk.test(stage);
