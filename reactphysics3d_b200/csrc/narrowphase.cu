@@ -8,20 +8,16 @@
 #include "narrowphase.cuh"
 #include "np_launch.h"
 
-// Kernel tuning knobs (compile time).  POLY_SCHEDULE: 0 = one thread per
-// polyhedron pair, 1 = box-box pairs per thread and mesh pairs per warp,
-// 2 = one warp per pair.  NP_MIN_BLOCKS: resident CTAs per SM requested from
-// the register allocator.
-#ifndef RP3DG_POLY_SCHEDULE
-#define RP3DG_POLY_SCHEDULE 2
-#endif
+// Kernel tuning knob (compile time): resident CTAs per SM requested from the
+// register allocator.
 #ifndef RP3DG_NP_MIN_BLOCKS
 #define RP3DG_NP_MIN_BLOCKS 4
 #endif
 
 namespace rp3dg {
 
-constexpr int POLY_SCHEDULE = RP3DG_POLY_SCHEDULE;
+// Internal kernel id: the per-thread half of the polyhedron schedule.
+constexpr int ALGO_POLY_PER_THREAD = 7;
 constexpr int NP_MIN_BLOCKS = RP3DG_NP_MIN_BLOCKS;
 
 __constant__ BoxTables c_box_tables;
@@ -195,22 +191,25 @@ __global__ void __launch_bounds__(NP_BLOCK, NP_MIN_BLOCKS) narrowphase_kernel(co
         const uint32_t* src = reinterpret_cast<const uint32_t*>(&c_box_tables);
         uint32_t* dst = reinterpret_cast<uint32_t*>(&s_box);
         for (uint32_t k = threadIdx.x; k < sizeof(BoxTables) / 4; k += blockDim.x) dst[k] = src[k];
-        if (a.stage_mesh) {
+        if (a.stage_mesh && ALGO != ALGO_POLY_PER_THREAD) {
             for (uint32_t k = threadIdx.x; k < a.mesh_nwords; k += blockDim.x) s_mesh[k] = __ldg(a.mesh_words + k);
             mesh_words = s_mesh;
         }
         __syncthreads();
     }
-    if constexpr (ALGO == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON) {
-        // Hybrid schedule: each warp takes a tile of 32 pairs.  Box-box pairs
-        // (12x12 edge pairs) run one per thread; pairs with a convex mesh
-        // (up to 128 x 128 edge pairs) then run one at a time on the whole warp.
-        __shared__ WarpScratch s_stage[NP_BLOCK / 32];
+    if constexpr (ALGO == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON || ALGO == ALGO_POLY_PER_THREAD) {
+        // Polyhedron pairs are split by tiles of 32 consecutive pairs: a tile
+        // whose pairs are all box-box (12 x 12 edge pairs) is done one pair per
+        // thread by the ALGO_POLY_PER_THREAD launch; any other tile (it holds a
+        // convex mesh, up to 128 x 128 edge pairs) is done one pair at a time
+        // by a whole warp in the ALGO 6 launch.  Both launches read the same
+        // tiles, so every pair is processed exactly once.
+        __shared__ WarpScratch s_stage[ALGO == ALGO_POLY_PER_THREAD ? 1 : NP_BLOCK / 32];
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const uint32_t nwarps = gridDim.x * (NP_BLOCK / 32);
         for (uint32_t tile = blockIdx.x * (NP_BLOCK / 32) + warp; tile * 32u < a.n; tile += nwarps) {
             const uint32_t i = tile * 32u + lane;
-            bool boxbox = false;
+            bool boxbox = i >= a.n;  // lanes past the end do not force the warp path
             if (i < a.n) {
                 const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
                 if (uint32_t(i1) < a.nb_shapes && uint32_t(i2) < a.nb_shapes) {
@@ -218,14 +217,13 @@ __global__ void __launch_bounds__(NP_BLOCK, NP_MIN_BLOCKS) narrowphase_kernel(co
                     boxbox = r1.kind == RP3DG_SHAPE_BOX && r2.kind == RP3DG_SHAPE_BOX;
                 }
             }
-            if (POLY_SCHEDULE == 2) boxbox = false;      // every pair warp-cooperative
-            if (POLY_SCHEDULE == 0) boxbox = i < a.n;    // every pair on its own thread
-            if (boxbox) process_pair<ALGO>(a, i, &s_box, mesh_words);
-            unsigned coop = __ballot_sync(FULL_MASK, i < a.n && !boxbox);
-            while (coop) {
-                const int l = __ffs(coop) - 1;
-                coop &= coop - 1;
-                process_pair_warp(a, tile * 32u + uint32_t(l), lane, &s_box, mesh_words, s_stage[warp]);
+            const bool all_box = __all_sync(FULL_MASK, boxbox);
+            if (ALGO == ALGO_POLY_PER_THREAD) {
+                if (all_box && i < a.n) process_pair<RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON>(a, i, &s_box, mesh_words);
+            } else if (!all_box) {
+                const uint32_t cnt = a.n - tile * 32u < 32u ? a.n - tile * 32u : 32u;
+                for (uint32_t l = 0; l < cnt; l++)
+                    process_pair_warp(a, tile * 32u + l, lane, &s_box, mesh_words, s_stage[warp]);
             }
         }
     } else {
@@ -243,6 +241,7 @@ static const void* kernel_ptr(int algo) {
         case 4: return reinterpret_cast<const void*>(&narrowphase_kernel<4>);
         case 5: return reinterpret_cast<const void*>(&narrowphase_kernel<5>);
         case 6: return reinterpret_cast<const void*>(&narrowphase_kernel<6>);
+        case ALGO_POLY_PER_THREAD: return reinterpret_cast<const void*>(&narrowphase_kernel<ALGO_POLY_PER_THREAD>);
     }
     return nullptr;
 }
@@ -264,11 +263,21 @@ extern "C" int rp3dg_profile_phases(unsigned long long* cycles, unsigned long lo
 }
 #endif
 
+static cudaError_t launch_one(int algo, const NpArgs& args, int num_sms, cudaStream_t stream);
+
 cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaStream_t stream) {
     if (args.n == 0) return cudaSuccess;
+    if (algo == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON) {
+        cudaError_t e = launch_one(ALGO_POLY_PER_THREAD, args, num_sms, stream);
+        if (e != cudaSuccess) return e;
+    }
+    return launch_one(algo, args, num_sms, stream);
+}
+
+static cudaError_t launch_one(int algo, const NpArgs& args, int num_sms, cudaStream_t stream) {
     const void* k = kernel_ptr(algo);
     if (!k) return cudaErrorInvalidValue;
-    size_t smem = args.stage_mesh ? size_t(args.mesh_nwords) * 4 : 0;
+    size_t smem = (args.stage_mesh && algo != ALGO_POLY_PER_THREAD) ? size_t(args.mesh_nwords) * 4 : 0;
     cudaFuncAttributes fa;
     cudaError_t e = cudaFuncGetAttributes(&fa, k);
     if (e != cudaSuccess) return e;
