@@ -204,7 +204,8 @@ int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch
  * bound).  Synchronizes the context stream. */
 int rp3dg_device_errors(rp3dg_ctx* ctx, uint32_t* flags, int clear);
 
-/* Number of kernels this context launched so far (instrumentation). */
+/* Number of kernels this context launched so far (instrumentation; a
+ * convex-polyhedron batch takes two). */
 uint64_t rp3dg_kernel_launches(const rp3dg_ctx* ctx);
 
 #ifdef __cplusplus

@@ -265,13 +265,17 @@ extern "C" int rp3dg_profile_phases(unsigned long long* cycles, unsigned long lo
 
 static cudaError_t launch_one(int algo, const NpArgs& args, int num_sms, cudaStream_t stream);
 
-cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaStream_t stream) {
+cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaStream_t stream, int* launches) {
+    *launches = 0;
     if (args.n == 0) return cudaSuccess;
     if (algo == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON) {
         cudaError_t e = launch_one(ALGO_POLY_PER_THREAD, args, num_sms, stream);
         if (e != cudaSuccess) return e;
+        ++*launches;
     }
-    return launch_one(algo, args, num_sms, stream);
+    cudaError_t e = launch_one(algo, args, num_sms, stream);
+    if (e == cudaSuccess) ++*launches;
+    return e;
 }
 
 static cudaError_t launch_one(int algo, const NpArgs& args, int num_sms, cudaStream_t stream) {

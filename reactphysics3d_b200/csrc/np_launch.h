@@ -39,6 +39,7 @@ struct NpArgs {
 };
 
 void upload_box_tables(const BoxTables& t, cudaStream_t s);
-cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaStream_t stream);
+// Launches the kernels of one algorithm batch; *launches receives how many.
+cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaStream_t stream, int* launches);
 
 }  // namespace rp3dg

@@ -464,9 +464,10 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
     a.local1 = reinterpret_cast<float4*>(out->local1);
     a.local2 = reinterpret_cast<float4*>(out->local2);
     cudaSetDevice(ctx->device);
-    cudaError_t e = rp3dg::launch_narrowphase(algorithm, a, ctx->num_sms, ctx->stream);
+    int launched = 0;
+    cudaError_t e = rp3dg::launch_narrowphase(algorithm, a, ctx->num_sms, ctx->stream, &launched);
+    ctx->launches += uint64_t(launched);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "narrowphase launch");
-    ctx->launches++;
     return 0;
 }
 
