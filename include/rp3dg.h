@@ -204,6 +204,44 @@ int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch
  * bound).  Synchronizes the context stream. */
 int rp3dg_device_errors(rp3dg_ctx* ctx, uint32_t* flags, int clear);
 
+/* ---- learned separating-axis proposal ----------------------------------
+ * No counterpart in the reference engine.  A 24 -> 64 -> 64 -> 16 MLP (bf16
+ * weights, fp32 accumulation) proposes a separating feature for convex
+ * polyhedron pairs: 0..2 a face of polyhedron 1 along local x/y/z, 3..5 a face
+ * of polyhedron 2 along x/y/z, 6..14 an edge pair (axis of 1 * 3 + axis of
+ * 2, box-box only), 15 none.  When enabled, the convex-polyhedron narrow
+ * phase tests the proposal with the reference's exact SAT test before its
+ * full SAT and skips the full SAT when the proposal separates the shapes; the
+ * contacts are unchanged, the cached separating feature may differ.
+ * RP3DG_MLP_NPARAMS fp32 parameters: w1[24][64] b1[64] w2[64][64] b2[64]
+ * w3[64][16] b3[16]. */
+#define RP3DG_MLP_NPARAMS 6800
+#define RP3DG_MLP_FEATURES 24
+#define RP3DG_MLP_CLASSES 16
+
+/* He-uniform initialisation from a seed; clears the Adam state. */
+int rp3dg_axis_mlp_init(rp3dg_ctx* ctx, uint64_t seed);
+int rp3dg_axis_mlp_get_params(rp3dg_ctx* ctx, float* params);
+int rp3dg_axis_mlp_set_params(rp3dg_ctx* ctx, const float* params);
+/* Features (n x 24 floats, device) of a device pair batch of polyhedron pairs. */
+int rp3dg_axis_features(rp3dg_ctx* ctx, const rp3dg_pair_batch* pairs, float* features);
+/* Class labels (device) of a device pair batch from the outcome of a fresh
+ * full-SAT narrow phase (its is_colliding output and the cache it wrote). */
+int rp3dg_axis_labels(rp3dg_ctx* ctx, const rp3dg_pair_batch* pairs, const uint8_t* is_colliding, uint8_t* labels);
+/* Gradients (device, RP3DG_MLP_NPARAMS floats) of the mean softmax
+ * cross-entropy over n device samples; *loss (host, may be NULL) receives it. */
+int rp3dg_axis_mlp_grads(rp3dg_ctx* ctx, const float* features, const uint8_t* labels, uint32_t n, float* grads,
+                         float* loss);
+/* One Adam step (lr, betas 0.9/0.999, eps 1e-8) on n device samples. */
+int rp3dg_axis_mlp_train_step(rp3dg_ctx* ctx, const float* features, const uint8_t* labels, uint32_t n, float lr,
+                              float* loss);
+/* Tensor-core inference: classes (device) of n device feature rows. */
+int rp3dg_axis_mlp_predict(rp3dg_ctx* ctx, const float* features, uint32_t n, uint8_t* classes);
+/* Use the proposal in the convex-polyhedron narrow phase (0 = off, default). */
+int rp3dg_set_learned_axis(rp3dg_ctx* ctx, int enable);
+/* Proposals tested and confirmed since the last clear (synchronizes). */
+int rp3dg_learned_axis_stats(rp3dg_ctx* ctx, uint64_t* tested, uint64_t* confirmed, int clear);
+
 /* Number of kernels this context launched so far (instrumentation; a
  * convex-polyhedron batch takes two). */
 uint64_t rp3dg_kernel_launches(const rp3dg_ctx* ctx);

@@ -5,6 +5,7 @@
 // shared memory once per CTA; the box topology comes from constant memory.
 #include <cuda_runtime.h>
 
+#include "axis_mlp.cuh"
 #include "narrowphase.cuh"
 #include "np_launch.h"
 
@@ -65,6 +66,8 @@ RD void load_item(const NpArgs& a, uint32_t i, Item& it) {
     it.report = a.report ? a.report[i] != 0 : true;
     it.colliding = false;
     it.gjk_capped = false;
+    it.proposal = MLP_NO_PROPOSAL;
+    it.proposal_tested = it.proposal_confirmed = false;
     if (a.cache) {
         const uint4 c = reinterpret_cast<const uint4*>(a.cache)[i];
         it.lf.gjk_axis = V(__uint_as_float(c.x), __uint_as_float(c.y), __uint_as_float(c.z));
@@ -103,20 +106,23 @@ RD void store_item(const NpArgs& a, uint32_t i, const Item& it) {
     }
 }
 
+// Returns bit 0 = a learned proposal was tested, bit 1 = it was confirmed.
 template <int ALGO>
-RD void process_pair(const NpArgs& a, uint32_t i, const BoxTables* box, const uint32_t* mesh_words) {
+RD uint32_t process_pair(const NpArgs& a, uint32_t i, const BoxTables* box, const uint32_t* mesh_words,
+                         uint32_t proposal = MLP_NO_PROPOSAL) {
     const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
     if (uint32_t(i1) >= a.nb_shapes || uint32_t(i2) >= a.nb_shapes) {
         // a pair naming a shape outside the table is reported as not colliding
         a.is_colliding[i] = 0;
         a.nb_contacts[i] = 0;
         atomicOr(a.error, 1u);
-        return;
+        return 0;
     }
     const ShapeRec s1 = load_shape(a.shapes, i1);
     const ShapeRec s2 = load_shape(a.shapes, i2);
     Item it;
     load_item(a, i, it);
+    it.proposal = proposal;
 
     if (ALGO == RP3DG_ALGO_SPHERE_VS_SPHERE) {
         sphere_sphere(it, s1.params.x, s2.params.x);
@@ -152,11 +158,12 @@ RD void process_pair(const NpArgs& a, uint32_t i, const BoxTables* box, const ui
     }
 
     store_item(a, i, it);
+    return (it.proposal_tested ? 1u : 0u) | (it.proposal_confirmed ? 2u : 0u);
 }
 
 // Convex polyhedron vs convex polyhedron, one warp per pair.
-RD void process_pair_warp(const NpArgs& a, uint32_t i, int lane, const BoxTables* box, const uint32_t* mesh_words,
-                          WarpScratch& stage) {
+RD uint32_t process_pair_warp(const NpArgs& a, uint32_t i, int lane, const BoxTables* box, const uint32_t* mesh_words,
+                              WarpScratch& stage, uint32_t proposal) {
     const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
     if (uint32_t(i1) >= a.nb_shapes || uint32_t(i2) >= a.nb_shapes) {
         if (lane == 0) {
@@ -164,12 +171,13 @@ RD void process_pair_warp(const NpArgs& a, uint32_t i, int lane, const BoxTables
             a.nb_contacts[i] = 0;
             atomicOr(a.error, 1u);
         }
-        return;
+        return 0;
     }
     const ShapeRec s1 = load_shape(a.shapes, i1);
     const ShapeRec s2 = load_shape(a.shapes, i2);
     Item it;
     load_item(a, i, it);
+    it.proposal = proposal;
     const bool b1 = s1.kind == RP3DG_SHAPE_BOX, b2 = s2.kind == RP3DG_SHAPE_BOX;
     if (b1 && b2) warp_sat_poly_poly(it, box_poly(s1, box), box_poly(s2, box), a.clip, lane, stage);
     else if (!b1 && b2) warp_sat_poly_poly(it, mesh_poly(mesh_words, s1.mesh), box_poly(s2, box), a.clip, lane, stage);
@@ -179,6 +187,26 @@ RD void process_pair_warp(const NpArgs& a, uint32_t i, int lane, const BoxTables
     it.lf.set(RP3DG_LF_WAS_USING_SAT, true);
     it.lf.set(RP3DG_LF_WAS_USING_GJK, false);
     if (lane == 0) store_item(a, i, it);
+    return (it.proposal_tested ? 1u : 0u) | (it.proposal_confirmed ? 2u : 0u);
+}
+
+// MLP input features of a polyhedron pair (zero for a pair that is not one).
+RD void pair_features(const NpArgs& a, uint32_t i, const BoxTables* box, const uint32_t* mesh_words, float* f) {
+    for (int k = 0; k < 32; k++) f[k] = 0.0f;
+    if (i >= a.n) return;
+    const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
+    if (uint32_t(i1) >= a.nb_shapes || uint32_t(i2) >= a.nb_shapes) return;
+    const ShapeRec s1 = load_shape(a.shapes, i1), s2 = load_shape(a.shapes, i2);
+    const float4 p1 = a.pos1[i], q1 = a.rot1[i], p2 = a.pos2[i], q2 = a.rot2[i];
+    const xform t1 = X(V(p1.x, p1.y, p1.z), Q(q1.x, q1.y, q1.z, q1.w));
+    const xform t2 = X(V(p2.x, p2.y, p2.z), Q(q2.x, q2.y, q2.z, q2.w));
+    const bool b1 = s1.kind == RP3DG_SHAPE_BOX, b2 = s2.kind == RP3DG_SHAPE_BOX;
+    float g[MLP_IN];
+    if (b1 && b2) axis_features(t1, t2, box_poly(s1, box), box_poly(s2, box), false, g);
+    else if (!b1 && b2) axis_features(t1, t2, mesh_poly(mesh_words, s1.mesh), box_poly(s2, box), true, g);
+    else if (b1 && !b2) axis_features(t1, t2, box_poly(s1, box), mesh_poly(mesh_words, s2.mesh), false, g);
+    else axis_features(t1, t2, mesh_poly(mesh_words, s1.mesh), mesh_poly(mesh_words, s2.mesh), true, g);
+    for (int k = 0; k < MLP_IN; k++) f[k] = g[k];
 }
 
 template <int ALGO>
@@ -204,9 +232,10 @@ __global__ void __launch_bounds__(NP_BLOCK, NP_MIN_BLOCKS) narrowphase_kernel(co
         // convex mesh, up to 128 x 128 edge pairs) is done one pair at a time
         // by a whole warp in the ALGO 6 launch.  Both launches read the same
         // tiles, so every pair is processed exactly once.
-        __shared__ WarpScratch s_stage[ALGO == ALGO_POLY_PER_THREAD ? 1 : NP_BLOCK / 32];
+        __shared__ WarpScratch s_stage[NP_BLOCK / 32];
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const uint32_t nwarps = gridDim.x * (NP_BLOCK / 32);
+        uint32_t tested = 0, confirmed = 0;
         for (uint32_t tile = blockIdx.x * (NP_BLOCK / 32) + warp; tile * 32u < a.n; tile += nwarps) {
             const uint32_t i = tile * 32u + lane;
             bool boxbox = i >= a.n;  // lanes past the end do not force the warp path
@@ -218,13 +247,37 @@ __global__ void __launch_bounds__(NP_BLOCK, NP_MIN_BLOCKS) narrowphase_kernel(co
                 }
             }
             const bool all_box = __all_sync(FULL_MASK, boxbox);
-            if (ALGO == ALGO_POLY_PER_THREAD) {
-                if (all_box && i < a.n) process_pair<RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON>(a, i, &s_box, mesh_words);
-            } else if (!all_box) {
-                const uint32_t cnt = a.n - tile * 32u < 32u ? a.n - tile * 32u : 32u;
-                for (uint32_t l = 0; l < cnt; l++)
-                    process_pair_warp(a, tile * 32u + l, lane, &s_box, mesh_words, s_stage[warp]);
+            if ((ALGO == ALGO_POLY_PER_THREAD) != all_box) continue;  // the other launch takes this tile
+            WarpScratch& ws = s_stage[warp];
+            uint32_t proposal = MLP_NO_PROPOSAL;
+            if (a.mlp) {
+                // learned proposals of the tile's 32 pairs on the bf16 tensor cores
+                pair_features(a, i, &s_box, mesh_words, ws.feat[lane]);
+                __syncwarp();
+                proposal = mlp_infer_tile(ws.feat, *static_cast<const MlpPacked*>(a.mlp), lane, ws.cls);
+                if (proposal >= MLP_OUT) proposal = MLP_NO_PROPOSAL;
+                ws.cls[lane] = proposal;
+                __syncwarp();
             }
+            if (ALGO == ALGO_POLY_PER_THREAD) {
+                uint32_t r = 0;
+                if (i < a.n) r = process_pair<RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON>(a, i, &s_box, mesh_words, proposal);
+                tested += __popc(__ballot_sync(FULL_MASK, r & 1u));
+                confirmed += __popc(__ballot_sync(FULL_MASK, (r & 2u) != 0));
+            } else {
+                const uint32_t cnt = a.n - tile * 32u < 32u ? a.n - tile * 32u : 32u;
+                for (uint32_t l = 0; l < cnt; l++) {
+                    const uint32_t r = process_pair_warp(a, tile * 32u + l, lane, &s_box, mesh_words, ws,
+                                                         a.mlp ? ws.cls[l] : uint32_t(MLP_NO_PROPOSAL));
+                    tested += r & 1u;
+                    confirmed += (r >> 1) & 1u;
+                }
+            }
+            __syncwarp();
+        }
+        if (a.mlp_stats && lane == 0 && tested) {
+            atomicAdd(&a.mlp_stats[0], (unsigned long long)tested);
+            atomicAdd(&a.mlp_stats[1], (unsigned long long)confirmed);
         }
     } else {
         const uint32_t stride = gridDim.x * blockDim.x;

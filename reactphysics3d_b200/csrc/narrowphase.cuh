@@ -177,6 +177,8 @@ struct Item {
     bool report;
     bool colliding;
     bool gjk_capped;
+    uint32_t proposal;        // learned separating-feature class, 15 = none
+    bool proposal_tested, proposal_confirmed;
     LastFrame lf;
     ContactSink out;
 };
@@ -910,6 +912,76 @@ RD bool poly_face_contacts(bool ref1, const P1& p1, const P2& p2, const xform& p
     return face_contacts(false, p2, p1, p2to1, p1to2, minFace, it);
 }
 
+template <class P> struct IsBox { static constexpr bool value = false; };
+template <> struct IsBox<BoxPoly> { static constexpr bool value = true; };
+RD const BoxTables* box_tables_of(const BoxPoly& b, const BoxPoly&) { return b.t; }
+RD const BoxTables* box_tables_of(const BoxPoly& b, const MeshPoly&) { return b.t; }
+RD const BoxTables* box_tables_of(const MeshPoly&, const BoxPoly& b) { return b.t; }
+RD const BoxTables* box_tables_of(const MeshPoly&, const MeshPoly&) { return nullptr; }
+
+// ---------------------------------------------------------------------------
+// exact confirmation of a proposed feature
+// ---------------------------------------------------------------------------
+// Tests the proposed feature with the reference's own arithmetic; on a
+// separating axis fills the cache like the reference's full SAT would for
+// that feature and returns true.
+template <class P1, class P2>
+RD bool confirm_proposal(uint32_t cls, const P1& p1, const P2& p2, const xform& p1to2, const xform& p2to1,
+                         LastFrame& lf, bool box1, bool box2, const BoxTables* bt) {
+    if (cls < 3) {
+        if (!box1) return false;
+        const uint32_t fp = cls == 0 ? 1u : (cls == 1 ? 5u : 0u), fm = cls == 0 ? 3u : (cls == 1 ? 4u : 2u);
+        for (int s = 0; s < 2; s++) {
+            const uint32_t f = s == 0 ? fp : fm;
+            if (sat_single_face(p1, p2, p1to2, f) <= 0.0f) {
+                lf.set(RP3DG_LF_SAT_FACE_POLY1, true); lf.set(RP3DG_LF_SAT_FACE_POLY2, false); lf.sat_face = f;
+                return true;
+            }
+        }
+        return false;
+    }
+    if (cls < 6) {
+        if (!box2) return false;
+        const uint32_t c = cls - 3;
+        const uint32_t fp = c == 0 ? 1u : (c == 1 ? 5u : 0u), fm = c == 0 ? 3u : (c == 1 ? 4u : 2u);
+        for (int s = 0; s < 2; s++) {
+            const uint32_t f = s == 0 ? fp : fm;
+            if (sat_single_face(p2, p1, p2to1, f) <= 0.0f) {
+                lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, true); lf.sat_face = f;
+                return true;
+            }
+        }
+        return false;
+    }
+    if (cls < 15 && box1 && box2) {
+        const uint32_t a = (cls - 6) / 3, b = (cls - 6) % 3;
+        const v3 c1 = xapply(p1to2, p1.centroid());
+        for (int ii = 0; ii < 4; ii++) {
+            const uint32_t i = bt->axis_edges[a][ii];
+            const hedge e1 = p1.edge(i);
+            const v3 e1A = xapply(p1to2, p1.vertex(e1.vertex));
+            const v3 e1B = xapply(p1to2, p1.vertex(p1.edge(e1.next).vertex));
+            const Edge1Gauss g = edge1_gauss(p1, e1, p1to2);
+            for (int jj = 0; jj < 4; jj++) {
+                const uint32_t j = bt->axis_edges[b][jj];
+                const hedge e2 = p2.edge(j);
+                if (edges_minkowski(g, p2, e2, j)) {
+                    const v3 e2A = p2.vertex(e2.vertex);
+                    const v3 e2B = p2.vertex(p2.edge(e2.next).vertex);
+                    v3 axis;
+                    const float d = sat_edge_distance(e1A, e2A, c1, vsub(e1B, e1A), vsub(e2B, e2A), axis);
+                    if (d <= 0.0f) {
+                        lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, false);
+                        lf.sat_e1 = i; lf.sat_e2 = j;
+                        return true;
+                    }
+                }
+            }
+        }
+    }
+    return false;
+}
+
 // testCollisionConvexPolyhedronVsConvexPolyhedron (SATAlgorithm.cpp:485-889)
 template <class P1, class P2>
 RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
@@ -966,6 +1038,14 @@ RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
         }
     }
 
+    // learned proposal: tested where the reference starts its full SAT
+    if (it.proposal < 15) {
+        it.proposal_tested = true;
+        if (confirm_proposal(it.proposal, p1, p2, p1to2, p2to1, lf, IsBox<P1>::value, IsBox<P2>::value, box_tables_of(p1, p2))) {
+            it.proposal_confirmed = true;
+            return;
+        }
+    }
     float minDepth;
     uint32_t minFace;
     bool isFace1;
@@ -1147,9 +1227,13 @@ struct Edge1Stage {
 // that pass the Gauss-map test (in visiting order) and the clip polygon.
 constexpr uint32_t WARP_CAND_CAP = 512;
 struct WarpScratch {
-    Edge1Stage stage[WARP_EDGE_CAP];
+    union {
+        Edge1Stage stage[WARP_EDGE_CAP];
+        float feat[32][32];  // a tile's MLP input rows (consumed before the SAT starts)
+    };
     uint16_t cand[WARP_CAND_CAP];
     v3 poly[CLIP_MAX];
+    uint32_t cls[32];
 };
 
 RD void warp_argmin(float& d, uint32_t& idx) {
@@ -1499,6 +1583,13 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
         }
     }
 
+    if (it.proposal < 15) {
+        it.proposal_tested = true;
+        if (confirm_proposal(it.proposal, p1, p2, p1to2, p2to1, lf, IsBox<P1>::value, IsBox<P2>::value, box_tables_of(p1, p2))) {
+            it.proposal_confirmed = true;
+            return;
+        }
+    }
     timer.mark(0);
     uint32_t f1 = 0, f2 = 0;
     const float d1 = warp_sat_faces(p1, p2, p1to2, f1, lane);

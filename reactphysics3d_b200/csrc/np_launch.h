@@ -36,6 +36,8 @@ struct NpArgs {
     float4* normal_depth;
     float4* local1;
     float4* local2;
+    const void* mlp;                 // packed MLP weights (MlpPacked) or nullptr: no proposals
+    unsigned long long* mlp_stats;   // [0] proposals tested, [1] confirmed
 };
 
 void upload_box_tables(const BoxTables& t, cudaStream_t s);

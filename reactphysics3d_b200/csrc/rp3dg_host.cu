@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/rp3dg.h"
+#include "mlp_launch.h"
 #include "np_launch.h"
 #include "rp3dg_internal.h"
 
@@ -158,6 +159,11 @@ BoxTables make_box_tables() {
         t.gauss[e][2] = uint8_t(face_axis[f2] | ((face_neg[f2] ? 0 : 1) << 2));
         t.gauss[e][3] = 0;
     }
+    int fillc[3] = {0, 0, 0};
+    for (int e = 0; e < 24; e += 2) {
+        const int k = t.gauss[e][0] & 3;
+        if (fillc[k] < 4) t.axis_edges[k][fillc[k]++] = uint8_t(e);
+    }
     return t;
 }
 
@@ -183,7 +189,36 @@ struct rp3dg_ctx {
     // staging buffers for rp3dg_narrowphase_host
     void* d_stage = nullptr;
     size_t cap_stage = 0;
+    // learned separating-axis MLP: one device block holding the fp32
+    // parameters, Adam moments, gradients, packed bf16 fragments, loss word
+    // and proposal counters; training scratch grows with the batch
+    char* d_mlp = nullptr;
+    float* d_mlp_scratch = nullptr;
+    size_t cap_mlp_scratch = 0;
+    int mlp_step = 0;
+    bool mlp_ready = false;
+    bool learned_axis = false;
 };
+
+namespace {
+constexpr size_t MLP_PARAM_BYTES = size_t(RP3DG_MLP_NPARAMS) * 4;
+constexpr size_t MLP_OFF_PARAMS = 0;
+constexpr size_t MLP_OFF_M = MLP_OFF_PARAMS + MLP_PARAM_BYTES;
+constexpr size_t MLP_OFF_V = MLP_OFF_M + MLP_PARAM_BYTES;
+constexpr size_t MLP_OFF_G = MLP_OFF_V + MLP_PARAM_BYTES;
+constexpr size_t MLP_OFF_PACKED = (MLP_OFF_G + MLP_PARAM_BYTES + 255) & ~size_t(255);
+constexpr size_t MLP_PACKED_BYTES = 16384;  // >= sizeof(rp3dg::MlpPacked)
+constexpr size_t MLP_OFF_LOSS = MLP_OFF_PACKED + MLP_PACKED_BYTES;
+constexpr size_t MLP_OFF_STATS = MLP_OFF_LOSS + 256;
+constexpr size_t MLP_BLOCK_BYTES = MLP_OFF_STATS + 256;
+float* mlp_params(rp3dg_ctx* c) { return reinterpret_cast<float*>(c->d_mlp + MLP_OFF_PARAMS); }
+float* mlp_m(rp3dg_ctx* c) { return reinterpret_cast<float*>(c->d_mlp + MLP_OFF_M); }
+float* mlp_v(rp3dg_ctx* c) { return reinterpret_cast<float*>(c->d_mlp + MLP_OFF_V); }
+float* mlp_g(rp3dg_ctx* c) { return reinterpret_cast<float*>(c->d_mlp + MLP_OFF_G); }
+rp3dg::MlpPacked* mlp_packed(rp3dg_ctx* c) { return reinterpret_cast<rp3dg::MlpPacked*>(c->d_mlp + MLP_OFF_PACKED); }
+float* mlp_loss(rp3dg_ctx* c) { return reinterpret_cast<float*>(c->d_mlp + MLP_OFF_LOSS); }
+unsigned long long* mlp_stats(rp3dg_ctx* c) { return reinterpret_cast<unsigned long long*>(c->d_mlp + MLP_OFF_STATS); }
+}  // namespace
 
 namespace {
 
@@ -264,6 +299,7 @@ int rp3dg_create(int device, rp3dg_ctx** out) {
     if (e != cudaSuccess) { delete ctx; return RP3DG_ECUDA; }
     const BoxTables t = make_box_tables();
     rp3dg::upload_box_tables(t, ctx->stream);
+    rp3dg::upload_mlp_box_tables(t, ctx->stream);
     e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) { cudaStreamDestroy(ctx->stream); delete ctx; return RP3DG_ECUDA; }
     *out = ctx;
@@ -278,6 +314,8 @@ void rp3dg_destroy(rp3dg_ctx* ctx) {
     cudaFree(ctx->d_arena);
     cudaFree(ctx->d_stage);
     cudaFree(ctx->d_error);
+    cudaFree(ctx->d_mlp);
+    cudaFree(ctx->d_mlp_scratch);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -463,6 +501,9 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
     a.normal_depth = reinterpret_cast<float4*>(out->normal_depth);
     a.local1 = reinterpret_cast<float4*>(out->local1);
     a.local2 = reinterpret_cast<float4*>(out->local2);
+    const bool learned = ctx->learned_axis && ctx->mlp_ready && algorithm == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON;
+    a.mlp = learned ? static_cast<const void*>(mlp_packed(ctx)) : nullptr;
+    a.mlp_stats = learned ? mlp_stats(ctx) : nullptr;
     cudaSetDevice(ctx->device);
     int launched = 0;
     cudaError_t e = rp3dg::launch_narrowphase(algorithm, a, ctx->num_sms, ctx->stream, &launched);
@@ -550,6 +591,187 @@ int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e == cudaSuccess) e = cudaGetLastError();
     return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "narrowphase (host arrays)");
+}
+
+namespace {
+
+int ensure_mlp(rp3dg_ctx* ctx) {
+    if (ctx->d_mlp) return 0;
+    cudaError_t e = cudaMalloc(&ctx->d_mlp, MLP_BLOCK_BYTES);
+    if (e != cudaSuccess) { ctx->d_mlp = nullptr; return cuda_fail(ctx, e, "cudaMalloc(mlp)"); }
+    e = cudaMemsetAsync(ctx->d_mlp, 0, MLP_BLOCK_BYTES, ctx->stream);
+    return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "clear mlp state");
+}
+
+int mlp_repack(rp3dg_ctx* ctx) {
+    cudaError_t e = rp3dg::launch_mlp_pack(mlp_params(ctx), mlp_packed(ctx), ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "mlp pack");
+    ctx->launches++;
+    ctx->mlp_ready = true;
+    return 0;
+}
+
+int mlp_pair_args(rp3dg_ctx* ctx, const rp3dg_pair_batch* p, rp3dg::MlpPairArgs& a) {
+    if (!p->shape1 || !p->shape2 || !p->pos1 || !p->rot1 || !p->pos2 || !p->rot2) return fail(ctx, RP3DG_EINVAL, "null pair array");
+    if (!ctx->d_shapes) return fail(ctx, RP3DG_EINVAL, "no shape table (rp3dg_set_shapes)");
+    a.n = p->n;
+    a.nb_shapes = ctx->nb_shapes;
+    a.shapes = ctx->d_shapes;
+    a.shape1 = p->shape1; a.shape2 = p->shape2;
+    a.pos1 = reinterpret_cast<const float4*>(p->pos1); a.rot1 = reinterpret_cast<const float4*>(p->rot1);
+    a.pos2 = reinterpret_cast<const float4*>(p->pos2); a.rot2 = reinterpret_cast<const float4*>(p->rot2);
+    a.mesh_words = ctx->d_arena;
+    a.box = nullptr;
+    return 0;
+}
+
+int mlp_grads_into(rp3dg_ctx* ctx, const float* x, const uint8_t* y, uint32_t n, float* grads, float* loss) {
+    const size_t need = size_t(n) * rp3dg::MLP_SCRATCH_ROW * sizeof(float);
+    if (need > ctx->cap_mlp_scratch) {
+        cudaFree(ctx->d_mlp_scratch);
+        ctx->d_mlp_scratch = nullptr;
+        cudaError_t e = cudaMalloc(&ctx->d_mlp_scratch, need);
+        if (e != cudaSuccess) { ctx->cap_mlp_scratch = 0; return cuda_fail(ctx, e, "cudaMalloc(mlp scratch)"); }
+        ctx->cap_mlp_scratch = need;
+    }
+    cudaError_t e = cudaMemsetAsync(mlp_loss(ctx), 0, sizeof(float), ctx->stream);
+    if (e == cudaSuccess) e = rp3dg::launch_mlp_grads(mlp_params(ctx), x, y, n, ctx->d_mlp_scratch, grads, mlp_loss(ctx), ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "mlp gradients");
+    ctx->launches += 2;
+    if (loss) {
+        float sum = 0.0f;
+        e = cudaMemcpyAsync(&sum, mlp_loss(ctx), sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "read mlp loss");
+        *loss = sum / float(n);
+    }
+    return 0;
+}
+
+}  // namespace
+
+int rp3dg_axis_mlp_init(rp3dg_ctx* ctx, uint64_t seed) {
+    if (!ctx) return RP3DG_EINVAL;
+    cudaSetDevice(ctx->device);
+    int rc = ensure_mlp(ctx);
+    if (rc) return rc;
+    // He-uniform weights from a splitmix64 stream, zero biases
+    std::vector<float> p(RP3DG_MLP_NPARAMS, 0.0f);
+    uint64_t st = seed;
+    auto next = [&st]() {
+        uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return double((z ^ (z >> 31)) >> 11) * (1.0 / 9007199254740992.0);
+    };
+    auto fill = [&](int off, int fan_in, int count) {
+        const double lim = std::sqrt(6.0 / fan_in);
+        for (int k = 0; k < count; k++) p[off + k] = float((2.0 * next() - 1.0) * lim);
+    };
+    fill(rp3dg::MLP_OFF_W1, rp3dg::MLP_IN, rp3dg::MLP_IN * rp3dg::MLP_H);
+    fill(rp3dg::MLP_OFF_W2, rp3dg::MLP_H, rp3dg::MLP_H * rp3dg::MLP_H);
+    fill(rp3dg::MLP_OFF_W3, rp3dg::MLP_H, rp3dg::MLP_H * rp3dg::MLP_OUT);
+    cudaError_t e = cudaMemcpyAsync(mlp_params(ctx), p.data(), MLP_PARAM_BYTES, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(mlp_m(ctx), 0, 2 * MLP_PARAM_BYTES, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "mlp init");
+    ctx->mlp_step = 0;
+    return mlp_repack(ctx);
+}
+
+int rp3dg_axis_mlp_get_params(rp3dg_ctx* ctx, float* params) {
+    if (!ctx || !params) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (!ctx->d_mlp) return fail(ctx, RP3DG_EINVAL, "mlp not initialised");
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaMemcpyAsync(params, mlp_params(ctx), MLP_PARAM_BYTES, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "read mlp params");
+}
+
+int rp3dg_axis_mlp_set_params(rp3dg_ctx* ctx, const float* params) {
+    if (!ctx || !params) return fail(ctx, RP3DG_EINVAL, "null argument");
+    cudaSetDevice(ctx->device);
+    int rc = ensure_mlp(ctx);
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpyAsync(mlp_params(ctx), params, MLP_PARAM_BYTES, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "write mlp params");
+    return mlp_repack(ctx);
+}
+
+int rp3dg_axis_features(rp3dg_ctx* ctx, const rp3dg_pair_batch* p, float* features) {
+    if (!ctx || !p || !features) return fail(ctx, RP3DG_EINVAL, "null argument");
+    rp3dg::MlpPairArgs a;
+    int rc = mlp_pair_args(ctx, p, a);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = rp3dg::launch_axis_features(a, features, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "axis features");
+    ctx->launches += p->n ? 1 : 0;
+    return 0;
+}
+
+int rp3dg_axis_labels(rp3dg_ctx* ctx, const rp3dg_pair_batch* p, const uint8_t* is_colliding, uint8_t* labels) {
+    if (!ctx || !p || !is_colliding || !labels || !p->cache) return fail(ctx, RP3DG_EINVAL, "null argument (labels need the cache)");
+    rp3dg::MlpPairArgs a;
+    int rc = mlp_pair_args(ctx, p, a);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = rp3dg::launch_axis_labels(a, is_colliding, p->cache, labels, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "axis labels");
+    ctx->launches += p->n ? 1 : 0;
+    return 0;
+}
+
+int rp3dg_axis_mlp_grads(rp3dg_ctx* ctx, const float* x, const uint8_t* y, uint32_t n, float* grads, float* loss) {
+    if (!ctx || !x || !y || !grads || n == 0) return fail(ctx, RP3DG_EINVAL, "bad argument");
+    if (!ctx->d_mlp) return fail(ctx, RP3DG_EINVAL, "mlp not initialised");
+    cudaSetDevice(ctx->device);
+    return mlp_grads_into(ctx, x, y, n, grads, loss);
+}
+
+int rp3dg_axis_mlp_train_step(rp3dg_ctx* ctx, const float* x, const uint8_t* y, uint32_t n, float lr, float* loss) {
+    if (!ctx || !x || !y || n == 0) return fail(ctx, RP3DG_EINVAL, "bad argument");
+    if (!ctx->d_mlp) return fail(ctx, RP3DG_EINVAL, "mlp not initialised");
+    cudaSetDevice(ctx->device);
+    int rc = mlp_grads_into(ctx, x, y, n, mlp_g(ctx), loss);
+    if (rc) return rc;
+    ctx->mlp_step++;
+    cudaError_t e = rp3dg::launch_mlp_adam(mlp_params(ctx), mlp_g(ctx), mlp_m(ctx), mlp_v(ctx), lr, ctx->mlp_step, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "mlp adam");
+    ctx->launches++;
+    return mlp_repack(ctx);
+}
+
+int rp3dg_axis_mlp_predict(rp3dg_ctx* ctx, const float* x, uint32_t n, uint8_t* classes) {
+    if (!ctx || !x || !classes) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (!ctx->mlp_ready) return fail(ctx, RP3DG_EINVAL, "mlp not initialised");
+    cudaSetDevice(ctx->device);
+    cudaError_t e = rp3dg::launch_mlp_predict(mlp_packed(ctx), x, n, classes, ctx->num_sms, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "mlp predict");
+    ctx->launches += n ? 1 : 0;
+    return 0;
+}
+
+int rp3dg_set_learned_axis(rp3dg_ctx* ctx, int enable) {
+    if (!ctx) return RP3DG_EINVAL;
+    if (enable && !ctx->mlp_ready) return fail(ctx, RP3DG_EINVAL, "mlp not initialised");
+    ctx->learned_axis = enable != 0;
+    return 0;
+}
+
+int rp3dg_learned_axis_stats(rp3dg_ctx* ctx, uint64_t* tested, uint64_t* confirmed, int clear) {
+    if (!ctx || !tested || !confirmed) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (!ctx->d_mlp) { *tested = *confirmed = 0; return 0; }
+    cudaSetDevice(ctx->device);
+    unsigned long long h[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(h, mlp_stats(ctx), sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && clear) e = cudaMemsetAsync(mlp_stats(ctx), 0, sizeof(h), ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "read learned-axis stats");
+    *tested = h[0];
+    *confirmed = h[1];
+    return 0;
 }
 
 }  // extern "C"

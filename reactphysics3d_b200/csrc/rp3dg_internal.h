@@ -42,6 +42,7 @@ struct BoxTables {
     uint8_t face_edge[6];
     uint8_t pad[2];
     uint8_t gauss[24][4];
+    uint8_t axis_edges[3][4];  // even half-edges along x, y, z (increasing index)
 };
 
 }  // namespace rp3dg

@@ -64,6 +64,16 @@ def load_library(path=LIB_PATH):
     L.rp3dg_device_errors.argtypes = [P, C.POINTER(C.c_uint32), C.c_int]
     L.rp3dg_narrowphase_device.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_int]
     L.rp3dg_narrowphase_host.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_int]
+    L.rp3dg_axis_mlp_init.argtypes = [P, C.c_uint64]
+    L.rp3dg_axis_mlp_get_params.argtypes = [P, P]
+    L.rp3dg_axis_mlp_set_params.argtypes = [P, P]
+    L.rp3dg_axis_features.argtypes = [P, C.POINTER(A.PairBatch), P]
+    L.rp3dg_axis_labels.argtypes = [P, C.POINTER(A.PairBatch), P, P]
+    L.rp3dg_axis_mlp_grads.argtypes = [P, P, P, C.c_uint32, P, P]
+    L.rp3dg_axis_mlp_train_step.argtypes = [P, P, P, C.c_uint32, C.c_float, P]
+    L.rp3dg_axis_mlp_predict.argtypes = [P, P, C.c_uint32, P]
+    L.rp3dg_set_learned_axis.argtypes = [P, C.c_int]
+    L.rp3dg_learned_axis_stats.argtypes = [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_int]
     _lib = L
     return L
 
@@ -207,3 +217,93 @@ class Context:
         pb, cb = pairs.struct(), out.struct()
         self._check(self.lib.rp3dg_narrowphase_device(self.h, int(algo), C.byref(pb), C.byref(cb), int(clip)))
         return out
+
+
+MLP_NPARAMS = 6800
+MLP_FEATURES = 24
+MLP_CLASSES = 16
+
+
+class AxisMLP:
+    """The learned separating-axis proposal of a Context (device-side model)."""
+
+    def __init__(self, ctx, seed=0):
+        self.ctx = ctx
+        ctx._check(ctx.lib.rp3dg_axis_mlp_init(ctx.h, int(seed)))
+
+    def params(self):
+        p = np.zeros(MLP_NPARAMS, np.float32)
+        self.ctx._check(self.ctx.lib.rp3dg_axis_mlp_get_params(self.ctx.h, p.ctypes.data))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == MLP_NPARAMS
+        self.ctx._check(self.ctx.lib.rp3dg_axis_mlp_set_params(self.ctx.h, p.ctypes.data))
+
+    def features(self, dpairs):
+        import torch
+        f = torch.empty((dpairs.n, MLP_FEATURES), dtype=torch.float32, device=dpairs.shape1.device)
+        pb = dpairs.struct()
+        self.ctx._check(self.ctx.lib.rp3dg_axis_features(self.ctx.h, C.byref(pb), f.data_ptr()))
+        return f
+
+    def labels(self, dpairs, dcontacts):
+        """Classes from the outcome of a fresh full-SAT pass over dpairs (its cache and flags)."""
+        import torch
+        y = torch.empty(dpairs.n, dtype=torch.uint8, device=dpairs.shape1.device)
+        pb = dpairs.struct()
+        self.ctx._check(self.ctx.lib.rp3dg_axis_labels(self.ctx.h, C.byref(pb), dcontacts.is_colliding.data_ptr(),
+                                                       y.data_ptr()))
+        return y
+
+    def grads(self, x, y):
+        import torch
+        g = torch.empty(MLP_NPARAMS, dtype=torch.float32, device=x.device)
+        loss = C.c_float()
+        self.ctx._check(self.ctx.lib.rp3dg_axis_mlp_grads(self.ctx.h, x.data_ptr(), y.data_ptr(), int(x.shape[0]),
+                                                          g.data_ptr(), C.addressof(loss)))
+        return g, loss.value
+
+    def train_step(self, x, y, lr=1e-3, want_loss=False):
+        loss = C.c_float()
+        self.ctx._check(self.ctx.lib.rp3dg_axis_mlp_train_step(self.ctx.h, x.data_ptr(), y.data_ptr(), int(x.shape[0]),
+                                                               float(lr), C.addressof(loss) if want_loss else None))
+        return loss.value if want_loss else None
+
+    def predict(self, x):
+        import torch
+        c = torch.empty(x.shape[0], dtype=torch.uint8, device=x.device)
+        self.ctx._check(self.ctx.lib.rp3dg_axis_mlp_predict(self.ctx.h, x.data_ptr(), int(x.shape[0]), c.data_ptr()))
+        return c
+
+    def enable(self, on=True):
+        self.ctx._check(self.ctx.lib.rp3dg_set_learned_axis(self.ctx.h, int(on)))
+
+    def stats(self, clear=True):
+        t, c = C.c_uint64(), C.c_uint64()
+        self.ctx._check(self.ctx.lib.rp3dg_learned_axis_stats(self.ctx.h, C.byref(t), C.byref(c), int(clear)))
+        return t.value, c.value
+
+
+def train_axis_mlp(ctx, mlp, x, y, epochs=4, batch=8192, lr=2e-3, seed=0, log=None):
+    """Minibatch Adam over device tensors x (n x 24) and y (n); returns the
+    per-epoch mean losses.  Shuffling uses a seeded permutation."""
+    import torch
+    n = int(x.shape[0])
+    gen = torch.Generator(device="cpu").manual_seed(seed)
+    losses = []
+    for ep in range(epochs):
+        perm = torch.randperm(n, generator=gen).to(x.device)
+        xs, ys = x[perm].contiguous(), y[perm].contiguous()
+        tot, cnt = 0.0, 0
+        for b0 in range(0, n - batch + 1, batch):
+            want = (b0 // batch) % 16 == 0
+            l = mlp.train_step(xs[b0:b0 + batch], ys[b0:b0 + batch], lr=lr, want_loss=want)
+            if want:
+                tot += l
+                cnt += 1
+        losses.append(tot / max(cnt, 1))
+        if log:
+            log(f"epoch {ep}: loss {losses[-1]:.4f}")
+    return losses
