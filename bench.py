@@ -134,9 +134,12 @@ def run_ours(args):
             if evs is not None:
                 evs[k][1].record(stream)
 
+    # everything below is queued on the library's stream (torch made current
+    # on it), so the kernels need no cross-stream ordering
+    torch.cuda.synchronize()
+    torch.cuda.set_stream(stream)
     for _ in range(args.warmup):
-        with torch.cuda.stream(stream):
-            flush.zero_()
+        flush.zero_()
         one_step()
     ctx.synchronize()
 
@@ -150,13 +153,13 @@ def run_ours(args):
     batch_ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in names]
                 for _ in range(args.steps)]
     for s in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
+        flush.zero_()
         step_ev[s][0].record(stream)
         one_step(batch_ev[s])
         step_ev[s][1].record(stream)
     ctx.synchronize()
     torch.cuda.synchronize()
+    torch.cuda.set_stream(torch.cuda.default_stream())
     launches = ctx.kernel_launches() - launches0
     clocks = sampler.stop()
     step_ms = [a.elapsed_time(b) for a, b in step_ev]

@@ -161,7 +161,29 @@ class Context:
 
     def torch_stream(self):
         import torch
-        return torch.cuda.ExternalStream(self.stream_ptr, device=f"cuda:{self.device}")
+        if getattr(self, "_tstream", None) is None:
+            self._tstream = torch.cuda.ExternalStream(self.stream_ptr, device=f"cuda:{self.device}")
+        return self._tstream
+
+    def order_in(self):
+        """Make the context stream wait for work queued on torch's current
+        stream (tensors just created or filled there)."""
+        import torch
+        cur = torch.cuda.current_stream(self.device)
+        if cur.cuda_stream != self.stream_ptr:
+            ev = torch.cuda.Event()
+            ev.record(cur)
+            self.torch_stream().wait_event(ev)
+
+    def order_out(self):
+        """Make torch's current stream wait for the context stream (results
+        read or reused there)."""
+        import torch
+        cur = torch.cuda.current_stream(self.device)
+        if cur.cuda_stream != self.stream_ptr:
+            ev = torch.cuda.Event()
+            ev.record(self.torch_stream())
+            cur.wait_event(ev)
 
     def synchronize(self):
         self._check(self.lib.rp3dg_synchronize(self.h))
@@ -213,9 +235,12 @@ class Context:
         return out
 
     def narrowphase_device(self, algo, pairs, out, clip=True):
-        """Asynchronous on the context stream; pairs/out are DevicePairs/DeviceContacts."""
+        """Asynchronous on the context stream, ordered after torch's current
+        stream and before later work on it; pairs/out are DevicePairs/DeviceContacts."""
         pb, cb = pairs.struct(), out.struct()
+        self.order_in()
         self._check(self.lib.rp3dg_narrowphase_device(self.h, int(algo), C.byref(pb), C.byref(cb), int(clip)))
+        self.order_out()
         return out
 
 
@@ -245,7 +270,9 @@ class AxisMLP:
         import torch
         f = torch.empty((dpairs.n, MLP_FEATURES), dtype=torch.float32, device=dpairs.shape1.device)
         pb = dpairs.struct()
+        self.ctx.order_in()
         self.ctx._check(self.ctx.lib.rp3dg_axis_features(self.ctx.h, C.byref(pb), f.data_ptr()))
+        self.ctx.order_out()
         return f
 
     def labels(self, dpairs, dcontacts):
@@ -253,28 +280,36 @@ class AxisMLP:
         import torch
         y = torch.empty(dpairs.n, dtype=torch.uint8, device=dpairs.shape1.device)
         pb = dpairs.struct()
+        self.ctx.order_in()
         self.ctx._check(self.ctx.lib.rp3dg_axis_labels(self.ctx.h, C.byref(pb), dcontacts.is_colliding.data_ptr(),
                                                        y.data_ptr()))
+        self.ctx.order_out()
         return y
 
     def grads(self, x, y):
         import torch
         g = torch.empty(MLP_NPARAMS, dtype=torch.float32, device=x.device)
         loss = C.c_float()
+        self.ctx.order_in()
         self.ctx._check(self.ctx.lib.rp3dg_axis_mlp_grads(self.ctx.h, x.data_ptr(), y.data_ptr(), int(x.shape[0]),
                                                           g.data_ptr(), C.addressof(loss)))
+        self.ctx.order_out()
         return g, loss.value
 
     def train_step(self, x, y, lr=1e-3, want_loss=False):
         loss = C.c_float()
+        self.ctx.order_in()
         self.ctx._check(self.ctx.lib.rp3dg_axis_mlp_train_step(self.ctx.h, x.data_ptr(), y.data_ptr(), int(x.shape[0]),
                                                                float(lr), C.addressof(loss) if want_loss else None))
+        self.ctx.order_out()
         return loss.value if want_loss else None
 
     def predict(self, x):
         import torch
         c = torch.empty(x.shape[0], dtype=torch.uint8, device=x.device)
+        self.ctx.order_in()
         self.ctx._check(self.ctx.lib.rp3dg_axis_mlp_predict(self.ctx.h, x.data_ptr(), int(x.shape[0]), c.data_ptr()))
+        self.ctx.order_out()
         return c
 
     def enable(self, on=True):
