@@ -115,6 +115,8 @@ def trained(ctx):
     ctx.synchronize()
     x, y = torch.cat(xs), torch.cat(ys)
     n = x.shape[0]
+    perm = torch.randperm(n, generator=torch.Generator().manual_seed(1)).cuda()
+    x, y = x[perm].contiguous(), y[perm].contiguous()
     ntr = int(0.8 * n)
     losses = engine.train_axis_mlp(ctx, mlp, x[:ntr], y[:ntr], epochs=6, batch=4096, lr=3e-3)
     return dict(mlp=mlp, x_test=x[ntr:], y_test=y[ntr:], losses=losses, scene=sc)
@@ -127,6 +129,7 @@ def test_training_on_sat_labels(trained):
     y = trained["y_test"].cpu().numpy()
     acc = float(np.mean(pred == y))
     majority = float(np.max(np.bincount(y, minlength=16))) / len(y)
+    print(f"held-out accuracy {acc:.3f} (majority class {majority:.3f}), losses {losses}")
     assert acc > majority + 0.05, (acc, majority)
 
 
