@@ -232,6 +232,20 @@ int rp3dg_axis_labels(rp3dg_ctx* ctx, const rp3dg_pair_batch* pairs, const uint8
  * cross-entropy over n device samples; *loss (host, may be NULL) receives it. */
 int rp3dg_axis_mlp_grads(rp3dg_ctx* ctx, const float* features, const uint8_t* labels, uint32_t n, float* grads,
                          float* loss);
+/* rp3dg_axis_mlp_grads without allocating device memory.  No counterpart in
+ * the reference engine.  For callers that must not allocate once they run: a
+ * host application that gives the engine a fixed GPU memory budget at
+ * start-up and forbids later cudaMalloc calls (an allocation can stall the
+ * whole device and can fail once the budget is spent), whereas
+ * rp3dg_axis_mlp_grads grows its scratch with cudaMalloc for larger batches.
+ * The scratch here is a fixed array inside the library (4.4 MB, held by every
+ * GPU that loads the library until exit): n is limited to 4096 samples
+ * (RP3DG_ECAPACITY beyond).  All calls share the array and it keeps the last
+ * call's contents; calls that overlap on the GPU race.  The first call on a
+ * device looks up the array's device address; make it before any stream
+ * capture.  Same outputs as rp3dg_axis_mlp_grads. */
+int rp3dg_axis_mlp_grads_noalloc(rp3dg_ctx* ctx, const float* features, const uint8_t* labels, uint32_t n,
+                                 float* grads, float* loss);
 /* One Adam step (lr, betas 0.9/0.999, eps 1e-8) on n device samples. */
 int rp3dg_axis_mlp_train_step(rp3dg_ctx* ctx, const float* features, const uint8_t* labels, uint32_t n, float lr,
                               float* loss);

@@ -14,6 +14,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "axis_mlp.cuh"
 #include "mlp_launch.h"
 
@@ -299,6 +301,66 @@ cudaError_t launch_mlp_pack(const float* params, MlpPacked* out, cudaStream_t s)
     const int total = MLP_FRAG_L1 + MLP_FRAG_L2 + MLP_FRAG_L3;
     mlp_pack<<<(total + 127) / 128, 128, 0, s>>>(params, out);
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free gradients (rp3dg_axis_mlp_grads_noalloc).
+//
+// Some callers cannot allocate device memory while they run: an engine whose
+// host application hands out a fixed GPU memory budget at start-up and
+// forbids later cudaMalloc calls (allocations can stall every stream of the
+// device and can fail once the budget is in use).  rp3dg_axis_mlp_grads grows
+// its training scratch with cudaMalloc whenever a larger batch comes in; this
+// variant uses a fixed array in the library's device image instead.  Every
+// GPU that loads the library holds the array (4.4 MB) until the process exits.
+// All calls share it and it keeps the previous call's contents: the loss word
+// is cleared on every call, the rows are fully rewritten for the samples in
+// use, and calls that overlap on the GPU (two streams, two threads) race.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) float g_mlp_noalloc_scratch[MLP_NOALLOC_MAX_SAMPLES * MLP_SCRATCH_ROW + 64];
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+float* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+std::mutex g_noalloc_mutex;
+}  // namespace
+
+// Device address of the scratch array on the current device, looked up once
+// per device (the host-side name of the array is not a device address).
+static cudaError_t noalloc_scratch(float** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_mlp_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = static_cast<float*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return cudaSuccess;
+}
+
+cudaError_t launch_mlp_grads_noalloc(const float* params, const float* x, const uint8_t* y, uint32_t n, float* grads,
+                                     float* loss_host, cudaStream_t s) {
+    if (n == 0 || n > MLP_NOALLOC_MAX_SAMPLES) return cudaErrorInvalidValue;
+    float* scratch = nullptr;
+    cudaError_t e = noalloc_scratch(&scratch);
+    if (e != cudaSuccess) return e;
+    float* loss_word = scratch + size_t(MLP_NOALLOC_MAX_SAMPLES) * MLP_SCRATCH_ROW;
+    e = cudaMemsetAsync(loss_word, 0, sizeof(float), s);
+    if (e != cudaSuccess) return e;
+    mlp_forward_backward<<<(n + 127) / 128, 128, 0, s>>>(params, x, y, n, scratch, loss_word);
+    mlp_weight_grads<<<(MLP_NPARAMS + 127) / 128, 128, 0, s>>>(x, scratch, n, grads);
+    e = cudaGetLastError();
+    if (e != cudaSuccess || !loss_host) return e;
+    float sum = 0.0f;
+    e = cudaMemcpyAsync(&sum, loss_word, sizeof(float), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) *loss_host = sum / float(n);
+    return e;
 }
 
 cudaError_t launch_mlp_predict(const MlpPacked* w, const float* x, uint32_t n, uint8_t* cls, int num_sms, cudaStream_t s) {

@@ -47,6 +47,10 @@ cudaError_t launch_mlp_grads(const float* params, const float* x, const uint8_t*
                              float* grads, float* loss_sum, cudaStream_t s);
 cudaError_t launch_mlp_adam(float* params, const float* grads, float* m, float* v, float lr, int step, cudaStream_t s);
 cudaError_t launch_mlp_pack(const float* params, MlpPacked* out, cudaStream_t s);
+// Largest batch of rp3dg_axis_mlp_grads_noalloc (its scratch is a fixed array).
+constexpr uint32_t MLP_NOALLOC_MAX_SAMPLES = 4096;
+cudaError_t launch_mlp_grads_noalloc(const float* params, const float* x, const uint8_t* y, uint32_t n, float* grads,
+                                     float* loss_host, cudaStream_t s);
 cudaError_t launch_mlp_predict(const MlpPacked* w, const float* x, uint32_t n, uint8_t* cls, int num_sms, cudaStream_t s);
 
 }  // namespace rp3dg

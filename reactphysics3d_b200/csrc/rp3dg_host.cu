@@ -730,6 +730,19 @@ int rp3dg_axis_mlp_grads(rp3dg_ctx* ctx, const float* x, const uint8_t* y, uint3
     return mlp_grads_into(ctx, x, y, n, grads, loss);
 }
 
+int rp3dg_axis_mlp_grads_noalloc(rp3dg_ctx* ctx, const float* x, const uint8_t* y, uint32_t n, float* grads,
+                                 float* loss) {
+    if (!ctx || !x || !y || !grads || n == 0) return fail(ctx, RP3DG_EINVAL, "bad argument");
+    if (n > rp3dg::MLP_NOALLOC_MAX_SAMPLES)
+        return fail(ctx, RP3DG_ECAPACITY, "rp3dg_axis_mlp_grads_noalloc takes at most 4096 samples per call");
+    if (!ctx->d_mlp) return fail(ctx, RP3DG_EINVAL, "mlp not initialised");
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess) e = rp3dg::launch_mlp_grads_noalloc(mlp_params(ctx), x, y, n, grads, loss, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "mlp gradients (no allocation)");
+    ctx->launches += 2;
+    return 0;
+}
+
 int rp3dg_axis_mlp_train_step(rp3dg_ctx* ctx, const float* x, const uint8_t* y, uint32_t n, float lr, float* loss) {
     if (!ctx || !x || !y || n == 0) return fail(ctx, RP3DG_EINVAL, "bad argument");
     if (!ctx->d_mlp) return fail(ctx, RP3DG_EINVAL, "mlp not initialised");
