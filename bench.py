@@ -230,6 +230,10 @@ def run_ours(args):
                "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_s * 1e3, 4),
                "api": "rp3dg_narrowphase_host (pinned host buffers)"}
 
+    learned = None
+    if not args.no_learned:
+        learned = learned_axis_section(ctx, sc, args, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(sc, args)
@@ -240,7 +244,8 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "pairs_per_gpu": sc.n_pairs, "batches": names,
                        "seed": args.seed, "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"independent pair sets per rank x{world}"},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": int(launches),
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "learned_axis": learned,
+            "gpu_launches": int(launches),
             "clocks": clocks, "batch_ms": {k: round(v, 4) for k, v in mean_batch.items()}}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -249,6 +254,121 @@ def run_ours(args):
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+
+
+def learned_axis_section(ctx, sc, args, dev):
+    """Learned separating-axis proposal vs plain SAT on the box-box and
+    hull-box batches of the workload (the polyhedron pairs): train the MLP on
+    labels from a fresh full-SAT frame, then time both variants on that frame
+    (fresh caches) and on the next frame (moved poses, caches of the previous
+    frame: the temporal-coherence path), checking contacts are bit-identical."""
+    import torch
+    from reactphysics3d_b200 import engine
+    names = [nm for nm in ("box_box", "hull_box") if nm in sc.batches]
+    mlp = engine.AxisMLP(ctx, seed=args.seed)
+    stream = ctx.torch_stream()
+    frames = {}
+    xs, ys = [], []
+    rng = np.random.default_rng(args.seed + 7)
+    for nm in names:
+        algo, pairs = sc.batches[nm]
+        p1 = pairs.slice(0, pairs.n)
+        p1.cache = A.fresh_cache(p1.n)
+        dp = engine.DevicePairs(p1, device=dev)
+        out = engine.DeviceContacts(p1.n, device=dev)
+        ctx.narrowphase_device(algo, dp, out)
+        xs.append(mlp.features(dp))
+        ys.append(mlp.labels(dp, out))
+        ctx.synchronize()
+        c1 = dp.host_cache()
+        p2 = _moved(p1, rng)
+        p2.cache = _next_cache(c1, out.is_colliding.cpu().numpy())
+        frames[nm] = (algo, A.fresh_cache(p1.n), p1, p2)
+    x, y = torch.cat(xs), torch.cat(ys)
+    perm = torch.randperm(x.shape[0], generator=torch.Generator().manual_seed(args.seed)).to(dev)
+    x, y = x[perm].contiguous(), y[perm].contiguous()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    engine.train_axis_mlp(ctx, mlp, x, y, epochs=args.learned_epochs, batch=4096, lr=3e-3, seed=args.seed)
+    ctx.synchronize()
+    train_s = time.perf_counter() - t0
+    pred = mlp.predict(x).cpu().numpy()
+    acc = float(np.mean(pred == y.cpu().numpy()))
+
+    def timed(frame, learned_on, reps=5):
+        res = {}
+        for nm in names:
+            algo, fresh, p1, p2 = frames[nm]
+            src = p1 if frame == 1 else p2
+            dp = engine.DevicePairs(src, device=dev)
+            cache0 = dp.cache.clone()
+            out = engine.DeviceContacts(src.n, device=dev)
+            mlp.enable(learned_on)
+            ms = []
+            for r in range(reps + 1):
+                dp.cache.copy_(cache0)
+                torch.cuda.synchronize()
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ev0.record(stream)
+                ctx.narrowphase_device(algo, dp, out)
+                ev1.record(stream)
+                ctx.synchronize()
+                if r > 0:
+                    ms.append(ev0.elapsed_time(ev1))
+            mlp.enable(False)
+            res[nm] = (float(np.median(ms)), out.to_host())
+        return res
+
+    report = {"train_samples": int(x.shape[0]), "train_epochs": args.learned_epochs,
+              "train_seconds": round(train_s, 3), "train_accuracy": round(acc, 4)}
+    identical = True
+    for frame in (1, 2):
+        plain = timed(frame, False)
+        mlp.stats(clear=True)
+        learn = timed(frame, True)
+        tested, confirmed = mlp.stats(clear=True)
+        n = sum(frames[nm][2].n for nm in names)
+        for nm in names:
+            mism = _compare(plain[nm][1], learn[nm][1])
+            identical = identical and mism == 0
+        pl_ms = sum(plain[nm][0] for nm in names)
+        le_ms = sum(learn[nm][0] for nm in names)
+        report[f"frame{frame}"] = {
+            "cache": "fresh" if frame == 1 else "previous frame",
+            "plain_pairs_per_s": round(n / (pl_ms / 1e3), 1), "learned_pairs_per_s": round(n / (le_ms / 1e3), 1),
+            "plain_ms": {nm: round(plain[nm][0], 4) for nm in names},
+            "learned_ms": {nm: round(learn[nm][0], 4) for nm in names},
+            "speedup": round(pl_ms / le_ms, 3),
+            "proposals_tested": int(tested // 6), "proposals_confirmed": int(confirmed // 6),
+            "confirmed_rate": round(confirmed / max(1, 6 * n), 4)}
+    report["contacts_bit_identical"] = bool(identical)
+    return report
+
+
+def _moved(p, rng, dpos=0.02, drot=0.02):
+    q = A.HostPairs(p.shape1, p.shape2, p.pos1.copy(), p.rot1.copy(), p.pos2.copy(), p.rot2.copy())
+    q.pos2[:, :3] += rng.uniform(-dpos, dpos, (p.n, 3)).astype(np.float32)
+    r = q.rot2.astype(np.float64) + rng.uniform(-drot, drot, (p.n, 4))
+    q.rot2[:] = (r / np.linalg.norm(r, axis=1, keepdims=True)).astype(np.float32)
+    return q
+
+
+def _next_cache(cache, colliding):
+    c = cache.copy()
+    c["flags"] |= A.LF_IS_VALID
+    c["flags"] &= ~np.uint8(A.LF_WAS_COLLIDING)
+    c["flags"] |= np.where(colliding != 0, A.LF_WAS_COLLIDING, 0).astype(np.uint8)
+    return c
+
+
+def _compare(a, b):
+    if not (np.array_equal(a.is_colliding, b.is_colliding) and np.array_equal(a.nb_contacts, b.nb_contacts)):
+        return 1
+    m = a.valid_mask()
+    bad = 0
+    for f in ("normal_depth", "local1", "local2"):
+        bad += int(np.sum(getattr(a, f)[m].view(np.uint32) != getattr(b, f)[m].view(np.uint32)))
+    return bad
 
 
 def _reference_engine():
@@ -334,6 +454,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--traffic-bytes", type=float, default=None)
+    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--learned-epochs", type=int, default=4)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
