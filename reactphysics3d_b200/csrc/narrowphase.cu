@@ -9,10 +9,17 @@
 #include "narrowphase.cuh"
 #include "np_launch.h"
 
-// Kernel tuning knob (compile time): resident CTAs per SM requested from the
-// register allocator.
+// Kernel tuning knobs (compile time): resident CTAs per SM requested from the
+// register allocator, for the closed-form/GJK kernels, the warp-per-pair
+// polyhedron kernel and the thread-per-pair polyhedron kernel.
 #ifndef RP3DG_NP_MIN_BLOCKS
 #define RP3DG_NP_MIN_BLOCKS 4
+#endif
+#ifndef RP3DG_NP_MIN_BLOCKS_POLY_WARP
+#define RP3DG_NP_MIN_BLOCKS_POLY_WARP 4
+#endif
+#ifndef RP3DG_NP_MIN_BLOCKS_POLY_THREAD
+#define RP3DG_NP_MIN_BLOCKS_POLY_THREAD 4
 #endif
 
 namespace rp3dg {
@@ -20,6 +27,8 @@ namespace rp3dg {
 // Internal kernel id: the per-thread half of the polyhedron schedule.
 constexpr int ALGO_POLY_PER_THREAD = 7;
 constexpr int NP_MIN_BLOCKS = RP3DG_NP_MIN_BLOCKS;
+constexpr int NP_MIN_BLOCKS_POLY_WARP = RP3DG_NP_MIN_BLOCKS_POLY_WARP;
+constexpr int NP_MIN_BLOCKS_POLY_THREAD = RP3DG_NP_MIN_BLOCKS_POLY_THREAD;
 
 __constant__ BoxTables c_box_tables;
 
@@ -210,7 +219,14 @@ RD void pair_features(const NpArgs& a, uint32_t i, const BoxTables* box, const u
 }
 
 template <int ALGO>
-__global__ void __launch_bounds__(NP_BLOCK, NP_MIN_BLOCKS) narrowphase_kernel(const NpArgs a) {
+struct MinBlocks { static constexpr int value = NP_MIN_BLOCKS; };
+template <>
+struct MinBlocks<RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON> { static constexpr int value = NP_MIN_BLOCKS_POLY_WARP; };
+template <>
+struct MinBlocks<ALGO_POLY_PER_THREAD> { static constexpr int value = NP_MIN_BLOCKS_POLY_THREAD; };
+
+template <int ALGO>
+__global__ void __launch_bounds__(NP_BLOCK, MinBlocks<ALGO>::value) narrowphase_kernel(const NpArgs a) {
     extern __shared__ uint32_t s_mesh[];
     __shared__ BoxTables s_box;
     constexpr bool uses_poly = ALGO >= RP3DG_ALGO_SPHERE_VS_CONVEX_POLYHEDRON;
@@ -250,11 +266,9 @@ __global__ void __launch_bounds__(NP_BLOCK, NP_MIN_BLOCKS) narrowphase_kernel(co
             if ((ALGO == ALGO_POLY_PER_THREAD) != all_box) continue;  // the other launch takes this tile
             WarpScratch& ws = s_stage[warp];
             uint32_t proposal = MLP_NO_PROPOSAL;
-            if (a.mlp) {
-                // learned proposals of the tile's 32 pairs on the bf16 tensor cores
-                pair_features(a, i, &s_box, mesh_words, ws.feat[lane]);
-                __syncwarp();
-                proposal = mlp_infer_tile(ws.feat, *static_cast<const MlpPacked*>(a.mlp), lane, ws.cls);
+            if (a.proposals) {
+                // learned proposals written by narrowphase_propose for this batch
+                proposal = i < a.n ? a.proposals[i] : uint32_t(MLP_NO_PROPOSAL);
                 if (proposal >= MLP_OUT) proposal = MLP_NO_PROPOSAL;
                 ws.cls[lane] = proposal;
                 __syncwarp();
@@ -268,7 +282,7 @@ __global__ void __launch_bounds__(NP_BLOCK, NP_MIN_BLOCKS) narrowphase_kernel(co
                 const uint32_t cnt = a.n - tile * 32u < 32u ? a.n - tile * 32u : 32u;
                 for (uint32_t l = 0; l < cnt; l++) {
                     const uint32_t r = process_pair_warp(a, tile * 32u + l, lane, &s_box, mesh_words, ws,
-                                                         a.mlp ? ws.cls[l] : uint32_t(MLP_NO_PROPOSAL));
+                                                         a.proposals ? ws.cls[l] : uint32_t(MLP_NO_PROPOSAL));
                     tested += r & 1u;
                     confirmed += (r >> 1) & 1u;
                 }
@@ -284,6 +298,41 @@ __global__ void __launch_bounds__(NP_BLOCK, NP_MIN_BLOCKS) narrowphase_kernel(co
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride)
             process_pair<ALGO>(a, i, &s_box, mesh_words);
     }
+}
+
+// Learned proposals of a polyhedron batch: per tile of 32 pairs the warp
+// computes the features and runs the MLP on the bf16 tensor cores; one class
+// byte per pair (15 = none).
+__global__ void __launch_bounds__(NP_BLOCK) narrowphase_propose(const NpArgs a, uint8_t* __restrict__ proposals) {
+    __shared__ float s_feat[NP_BLOCK / 32][32][MLP_KPAD];
+    __shared__ uint32_t s_cls[NP_BLOCK / 32][32];
+    __shared__ BoxTables s_box;
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&c_box_tables);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&s_box);
+        for (uint32_t k = threadIdx.x; k < sizeof(BoxTables) / 4; k += blockDim.x) dst[k] = src[k];
+        __syncthreads();
+    }
+    const MlpPacked& w = *static_cast<const MlpPacked*>(a.mlp);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t nwarps = gridDim.x * (NP_BLOCK / 32);
+    for (uint32_t tile = blockIdx.x * (NP_BLOCK / 32) + warp; tile * 32u < a.n; tile += nwarps) {
+        const uint32_t i = tile * 32u + lane;
+        pair_features(a, i, &s_box, a.mesh_words, s_feat[warp][lane]);
+        __syncwarp();
+        uint32_t c = mlp_infer_tile(s_feat[warp], w, lane, s_cls[warp]);
+        if (c >= MLP_OUT) c = MLP_NO_PROPOSAL;
+        if (i < a.n) proposals[i] = uint8_t(c);
+        __syncwarp();
+    }
+}
+
+cudaError_t launch_narrowphase_propose(const NpArgs& args, uint8_t* proposals, int num_sms, cudaStream_t stream) {
+    if (args.n == 0) return cudaSuccess;
+    const uint32_t blocks_needed = (args.n + NP_BLOCK - 1) / NP_BLOCK;
+    const uint32_t cap = uint32_t(num_sms) * 16u;
+    narrowphase_propose<<<blocks_needed < cap ? blocks_needed : cap, NP_BLOCK, 0, stream>>>(args, proposals);
+    return cudaGetLastError();
 }
 
 static const void* kernel_ptr(int algo) {

@@ -36,12 +36,15 @@ struct NpArgs {
     float4* normal_depth;
     float4* local1;
     float4* local2;
-    const void* mlp;                 // packed MLP weights (MlpPacked) or nullptr: no proposals
+    const void* mlp;                 // packed MLP weights (MlpPacked), read by narrowphase_propose
+    const uint8_t* proposals;        // per-pair learned proposal (15 = none) or nullptr
     unsigned long long* mlp_stats;   // [0] proposals tested, [1] confirmed
 };
 
 void upload_box_tables(const BoxTables& t, cudaStream_t s);
 // Launches the kernels of one algorithm batch; *launches receives how many.
 cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaStream_t stream, int* launches);
+// Learned proposals of a polyhedron batch (args.mlp must be set).
+cudaError_t launch_narrowphase_propose(const NpArgs& args, uint8_t* proposals, int num_sms, cudaStream_t stream);
 
 }  // namespace rp3dg

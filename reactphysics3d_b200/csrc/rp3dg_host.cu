@@ -194,6 +194,8 @@ struct rp3dg_ctx {
     // and proposal counters; training scratch grows with the batch
     char* d_mlp = nullptr;
     float* d_mlp_scratch = nullptr;
+    uint8_t* d_proposals = nullptr;
+    uint32_t cap_proposals = 0;
     size_t cap_mlp_scratch = 0;
     int mlp_step = 0;
     bool mlp_ready = false;
@@ -316,6 +318,7 @@ void rp3dg_destroy(rp3dg_ctx* ctx) {
     cudaFree(ctx->d_error);
     cudaFree(ctx->d_mlp);
     cudaFree(ctx->d_mlp_scratch);
+    cudaFree(ctx->d_proposals);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -504,7 +507,22 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
     const bool learned = ctx->learned_axis && ctx->mlp_ready && algorithm == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON;
     a.mlp = learned ? static_cast<const void*>(mlp_packed(ctx)) : nullptr;
     a.mlp_stats = learned ? mlp_stats(ctx) : nullptr;
+    a.proposals = nullptr;
     cudaSetDevice(ctx->device);
+    if (learned) {
+        // one proposal byte per pair, in a buffer that grows with the batch
+        if (p->n > ctx->cap_proposals) {
+            cudaFree(ctx->d_proposals);
+            ctx->d_proposals = nullptr;
+            cudaError_t e = cudaMalloc(&ctx->d_proposals, p->n);
+            if (e != cudaSuccess) { ctx->cap_proposals = 0; return cuda_fail(ctx, e, "cudaMalloc(proposals)"); }
+            ctx->cap_proposals = p->n;
+        }
+        cudaError_t e = rp3dg::launch_narrowphase_propose(a, ctx->d_proposals, ctx->num_sms, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "learned proposals");
+        ctx->launches++;
+        a.proposals = ctx->d_proposals;
+    }
     int launched = 0;
     cudaError_t e = rp3dg::launch_narrowphase(algorithm, a, ctx->num_sms, ctx->stream, &launched);
     ctx->launches += uint64_t(launched);
@@ -629,6 +647,7 @@ int mlp_grads_into(rp3dg_ctx* ctx, const float* x, const uint8_t* y, uint32_t n,
     const size_t need = size_t(n) * rp3dg::MLP_SCRATCH_ROW * sizeof(float);
     if (need > ctx->cap_mlp_scratch) {
         cudaFree(ctx->d_mlp_scratch);
+    cudaFree(ctx->d_proposals);
         ctx->d_mlp_scratch = nullptr;
         cudaError_t e = cudaMalloc(&ctx->d_mlp_scratch, need);
         if (e != cudaSuccess) { ctx->cap_mlp_scratch = 0; return cuda_fail(ctx, e, "cudaMalloc(mlp scratch)"); }
