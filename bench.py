@@ -194,7 +194,7 @@ def run_ours(args):
         roofline["traffic"] = args.traffic_bytes
 
     # ---- end to end through the host-memory C-ABI call -------------------
-    e2e = None
+    e2e, pinned = None, None
     if not args.no_e2e:
         pinned = {}
         for nm in names:
@@ -230,6 +230,11 @@ def run_ours(args):
                "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_s * 1e3, 4),
                "api": "rp3dg_narrowphase_host (pinned host buffers)"}
 
+    manifolds = None
+    if not args.no_manifolds:
+        manifolds = manifold_section(ctx, sc, names, algos, dpairs, douts, args, dev,
+                                     pinned)
+
     learned = None
     if not args.no_learned:
         learned = learned_axis_section(ctx, sc, args, dev)
@@ -244,7 +249,7 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "pairs_per_gpu": sc.n_pairs, "batches": names,
                        "seed": args.seed, "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"independent pair sets per rank x{world}"},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "learned_axis": learned,
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "manifolds": manifolds, "learned_axis": learned,
             "gpu_launches": int(launches),
             "clocks": clocks, "batch_ms": {k: round(v, 4) for k, v in mean_batch.items()}}
     if rank == 0:
@@ -254,6 +259,67 @@ def run_ours(args):
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+
+
+def manifold_section(ctx, sc, names, algos, dpairs, douts, args, dev, pinned):
+    """The convex manifold step after the narrow phase (reduction to <= 4
+    points, de-duplication, last-frame update): device time of the reduction
+    kernel on each batch's narrow-phase output (restored before every
+    repetition, outside the timed events), its HBM roofline, and the host-array
+    call that runs narrow phase + reduction and copies back only kept slots."""
+    import torch
+    from reactphysics3d_b200 import engine
+    stream = ctx.torch_stream()
+    reps = max(3, min(args.steps, 20))
+    per = {}
+    tot_ms, tot_bytes = 0.0, 0
+    with torch.cuda.stream(stream):
+        for nm in names:
+            src = douts[nm]
+            n = src.n
+            work = engine.DeviceContacts(n, device=dev)
+            kept = torch.empty((n, 4), dtype=torch.uint8, device=dev)
+            nb = src.nb_contacts.to(torch.int64)
+            ms = []
+            for r in range(reps + 2):
+                for f in ("is_colliding", "nb_contacts", "normal_depth", "local1", "local2"):
+                    getattr(work, f).copy_(getattr(src, f))
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                ctx.reduce_contacts_device(dpairs[nm], work, kept)
+                b.record(stream)
+                if r >= 2:
+                    ms.append((a, b))
+            ctx.synchronize()
+            t = float(np.mean([x.elapsed_time(y) for x, y in ms]))
+            m = work.nb_contacts.to(torch.int64)
+            # per pair: flag, count, orientation, cache flag byte, kept row, count
+            # written; per raw point its local1 (16 B); per kept point 48 B read
+            # and 48 B written
+            alg = n * (1 + 1 + 16 + 1 + 4 + 1) + int(nb.sum()) * 16 + int(m.sum()) * 96
+            per[nm] = {"ms": round(t, 4), "pairs_with_more_than_4": int((nb > 4).sum()),
+                       "points_in": int(nb.sum()), "points_kept": int(m.sum()),
+                       "achieved_gbs": round(alg / (t / 1e3) / 1e9, 1)}
+            tot_ms += t
+            tot_bytes += alg
+    hbm_peak, _ = peaks()
+    out = {"kernel": "contacts_reduce_kernel", "batches": per, "ms_per_step": round(tot_ms, 4),
+           "pairs_per_s": round(sc.n_pairs / (tot_ms / 1e3), 1),
+           "roofline": {"bound": "hbm", "achieved": round(tot_bytes / (tot_ms / 1e3) / 1e9, 1), "peak": hbm_peak,
+                        "unit": "GB/s", "frac": round(tot_bytes / (tot_ms / 1e3) / 1e9 / hbm_peak, 4)}}
+    if pinned is not None:
+        for _ in range(2):
+            for nm in names:
+                ctx.narrowphase_manifolds_host(algos[nm], *pinned[nm], want_kept=False)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            for nm in names:
+                ctx.narrowphase_manifolds_host(algos[nm], *pinned[nm], want_kept=False)
+        dt = (time.perf_counter() - t0) / args.steps
+        out["e2e_narrowphase_plus_manifolds"] = {"value": round(sc.n_pairs / dt, 1), "unit": UNIT,
+                                                 "ms_per_step": round(dt * 1e3, 4),
+                                                 "api": "rp3dg_narrowphase_manifolds_host (pinned host buffers)"}
+    return out
 
 
 def learned_axis_section(ctx, sc, args, dev):
@@ -455,6 +521,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--traffic-bytes", type=float, default=None)
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-manifolds", action="store_true")
     ap.add_argument("--learned-epochs", type=int, default=4)
     args = ap.parse_args()
     if args.impl == "reference":

@@ -256,6 +256,32 @@ int rp3dg_set_learned_axis(rp3dg_ctx* ctx, int enable);
 /* Proposals tested and confirmed since the last clear (synchronizes). */
 int rp3dg_learned_axis_stats(rp3dg_ctx* ctx, uint64_t* tested, uint64_t* confirmed, int clear);
 
+/* ---- contact manifolds ------------------------------------------------ */
+
+/* Manifold of every colliding convex pair, as the reference builds it after
+ * the narrow phase: all points of the pair in one manifold
+ * (CollisionDetectionSystem::processPotentialContacts,
+ * CollisionDetectionSystem.cpp:1198-1391), reduced to at most 4 points when it
+ * has more (reduceContactPoints, :1483-1662, using the shape-1 orientation
+ * rot1 of the batch) and de-duplicated (points closer than 0.01,
+ * removeDuplicatedContactPointsInManifold, :1673-1705).  Device arrays, in
+ * place: the kept points move to slots 0..k-1 in manifold order and
+ * nb_contacts becomes k; kept (n x 4, may be NULL) receives the original slot
+ * of each kept point (255 = none).  When pairs->cache is not NULL the step
+ * also updates the temporal-coherence records as the reference does before
+ * the next frame (processPotentialContacts with updateLastFrameInfo,
+ * :1209-1217): IS_VALID set, WAS_COLLIDING = is_colliding.  Only rot1 and
+ * cache of the pair batch are read.  Asynchronous on the context stream. */
+int rp3dg_reduce_contacts_device(rp3dg_ctx* ctx, const rp3dg_pair_batch* pairs, const rp3dg_contact_batch* contacts,
+                                 uint8_t* kept);
+
+/* rp3dg_narrowphase_host followed on the device by rp3dg_reduce_contacts_device:
+ * the per-algorithm narrow phase and the convex manifold step of
+ * CollisionDetectionSystem (:1198-1458) in one call on host arrays; only the
+ * (at most 4) kept slots are copied back.  kept (host, n x 4) may be NULL. */
+int rp3dg_narrowphase_manifolds_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* pairs,
+                                     const rp3dg_contact_batch* out, int clip_with_previous_axis, uint8_t* kept);
+
 /* Number of kernels this context launched so far (instrumentation; a
  * convex-polyhedron batch takes two). */
 uint64_t rp3dg_kernel_launches(const rp3dg_ctx* ctx);

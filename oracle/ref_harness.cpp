@@ -9,6 +9,21 @@
 //
 // Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load
 // the resulting oracle/_ref/librp3d_ref_*.so.
+// The manifold-reduction entry below calls two private members of
+// CollisionDetectionSystem directly; access is widened for this translation
+// unit only (the reference objects themselves are compiled unchanged).
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <functional>
+#include <map>
+#include <mutex>
+#include <set>
+#include <sstream>
+#include <string>
+#include <unordered_map>
+#define private public
+#define protected public
 #include <reactphysics3d/reactphysics3d.h>
 #include <reactphysics3d/collision/narrowphase/NarrowPhaseInfoBatch.h>
 #include <reactphysics3d/collision/narrowphase/SphereVsSphereAlgorithm.h>
@@ -337,6 +352,63 @@ int ref_narrowphase(int algorithm, const rp3dg_shape* shapes, uint32_t nb_shapes
     for (auto& s : slices) worst = std::max(worst, s.seconds);
     if (seconds) *seconds = worst;
     destroy_shapes(shapes, shp);
+    return 0;
+}
+
+// Manifold of every colliding convex pair reduced by the reference's own
+// CollisionDetectionSystem::reduceContactPoints (when it has more than 4
+// points) and removeDuplicatedContactPointsInManifold, exactly as
+// reducePotentialContactManifolds applies them (CollisionDetectionSystem.cpp:
+// 1394-1458).  Same in/out convention as rp3do_reduce_contacts.
+int ref_reduce_contacts(const rp3dg_pair_batch* p, const rp3dg_contact_batch* c, uint8_t* kept) {
+    Harness& h = H();
+    static PhysicsWorld* world = nullptr;
+    if (!world) world = h.common.createPhysicsWorld();
+    const CollisionDetectionSystem& cds = world->mCollisionDetection;
+    DefaultAllocator alloc;
+    const uint32_t n = p->n;
+    for (uint32_t i = 0; i < n; i++) {
+        if (p->cache) {
+            // the two assignments of processPotentialContacts (:1209-1217) on the
+            // reference's own LastFrameCollisionInfo
+            LastFrameCollisionInfo l = unpack_cache(p->cache[i]);
+            l.wasColliding = c->is_colliding[i] != 0;
+            l.isValid = true;
+            pack_cache(l, p->cache[i]);
+        }
+        uint32_t nb = c->nb_contacts[i];
+        Array<ContactPointInfo> pts(alloc, 16);
+        for (uint32_t k = 0; k < nb; k++) {
+            const size_t o = size_t(k) * n + i;
+            ContactPointInfo cp;
+            cp.normal = Vector3(c->normal_depth[o].x, c->normal_depth[o].y, c->normal_depth[o].z);
+            cp.penetrationDepth = c->normal_depth[o].w;
+            cp.localPoint1 = Vector3(c->local1[o].x, c->local1[o].y, c->local1[o].z);
+            cp.localPoint2 = Vector3(c->local2[o].x, c->local2[o].y, c->local2[o].z);
+            pts.add(cp);
+        }
+        ContactManifoldInfo m(i);
+        for (uint32_t k = 0; k < nb; k++) m.potentialContactPointsIndices[k] = k;
+        m.nbPotentialContactPoints = uint8_t(nb);
+        if (nb > 0 && c->is_colliding[i]) {
+            const Transform t1(Vector3(p->pos1[i].x, p->pos1[i].y, p->pos1[i].z),
+                               Quaternion(p->rot1[i].x, p->rot1[i].y, p->rot1[i].z, p->rot1[i].w));
+            if (nb > 4) cds.reduceContactPoints(m, t1, pts);
+            cds.removeDuplicatedContactPointsInManifold(m, pts);
+        }
+        const uint32_t mm = std::min<uint32_t>(m.nbPotentialContactPoints, 4);
+        rp3dg_float4 nd[4], l1[4], l2[4];
+        for (uint32_t k = 0; k < mm; k++) {
+            const size_t o = size_t(m.potentialContactPointsIndices[k]) * n + i;
+            nd[k] = c->normal_depth[o]; l1[k] = c->local1[o]; l2[k] = c->local2[o];
+        }
+        for (uint32_t k = 0; k < mm; k++) {
+            const size_t o = size_t(k) * n + i;
+            c->normal_depth[o] = nd[k]; c->local1[o] = l1[k]; c->local2[o] = l2[k];
+        }
+        if (kept) for (uint32_t k = 0; k < 4; k++) kept[4 * size_t(i) + k] = uint8_t(k < mm ? m.potentialContactPointsIndices[k] : 255);
+        c->nb_contacts[i] = uint8_t(mm);
+    }
     return 0;
 }
 

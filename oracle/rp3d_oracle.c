@@ -1547,3 +1547,133 @@ int rp3do_narrowphase(int algorithm, const rp3dg_shape* shapes, uint32_t nb_shap
     }
     return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* contact manifold of a convex pair (CollisionDetectionSystem.cpp)    */
+/* ------------------------------------------------------------------ */
+#define MAX_POINTS_IN_MANIFOLD 4                      /* configuration.h:143 */
+static const float SAME_POINT_DIST = 0.01f;           /* configuration.h:146 */
+
+static void remove_at(uint32_t* a, uint32_t idx, uint32_t* size) { a[idx] = a[*size - 1]; (*size)--; }
+
+/* reduceContactPoints (CollisionDetectionSystem.cpp:1483-1662); idx[] holds
+ * the manifold's point indices (slots), nb > 4 on entry, 4 on exit */
+static void reduce_points(uint32_t* idx, uint32_t* nb, const v3* lp1, v3 normal0_world, quat q1) {
+    uint32_t cand[RP3DG_MAX_CONTACTS_PER_PAIR];
+    uint32_t ncand = *nb;
+    for (uint32_t i = 0; i < ncand; i++) cand[i] = idx[i];
+    uint32_t keep[4] = {0, 0, 0, 0};
+    const v3 nLocal = qrot(qinv(q1), normal0_world);
+    /* first point: max (1,1,1) . localPoint1 */
+    float maxDot = DECIMAL_SMALLEST;
+    uint32_t k = 0;
+    for (uint32_t i = 0; i < ncand; i++) {
+        const float d = vdot(V(1, 1, 1), lp1[cand[i]]);
+        if (d > maxDot) { maxDot = d; k = i; }
+    }
+    keep[0] = cand[k];
+    remove_at(cand, k, &ncand);
+    /* second: farthest from the first (>=) */
+    float maxDist = 0.0f;
+    k = 0;
+    for (uint32_t i = 0; i < ncand; i++) {
+        const float d = vlen2(vsub(lp1[keep[0]], lp1[cand[i]]));
+        if (d >= maxDist) { maxDist = d; k = i; }
+    }
+    keep[1] = cand[k];
+    remove_at(cand, k, &ncand);
+    /* third: largest positive or negative area */
+    uint32_t kmax = 0, kmin = 0;
+    float minArea = 0.0f, maxArea = 0.0f;
+    int prevPositive;
+    for (uint32_t i = 0; i < ncand; i++) {
+        const v3 a = vsub(lp1[keep[0]], lp1[cand[i]]);
+        const v3 b = vsub(lp1[keep[1]], lp1[cand[i]]);
+        const float area = vdot(vcross(a, b), nLocal);
+        if (area >= maxArea) { maxArea = area; kmax = i; }
+        if (area <= minArea) { minArea = area; kmin = i; }
+    }
+    if (maxArea > (-minArea)) { prevPositive = 1; keep[2] = cand[kmax]; remove_at(cand, kmax, &ncand); }
+    else { prevPositive = 0; keep[2] = cand[kmin]; remove_at(cand, kmin, &ncand); }
+    /* fourth: largest area of opposite winding over the triangle's edges */
+    float largest = 0.0f;
+    k = 0;
+    for (uint32_t i = 0; i < ncand; i++) {
+        for (uint32_t j = 0; j < 3; j++) {
+            const uint32_t e1 = j, e2 = j < 2 ? j + 1 : 0;
+            const v3 a = vsub(lp1[keep[e1]], lp1[cand[i]]);
+            const v3 b = vsub(lp1[keep[e2]], lp1[cand[i]]);
+            const float area = vdot(vcross(a, b), nLocal);
+            if (prevPositive && area <= largest) { largest = area; k = i; }
+            else if (!prevPositive && area >= largest) { largest = area; k = i; }
+        }
+    }
+    keep[3] = cand[k];
+    for (int i = 0; i < 4; i++) idx[i] = keep[i];
+    *nb = 4;
+}
+
+/* removeDuplicatedContactPointsInManifold (CollisionDetectionSystem.cpp:1673-1705) */
+static void remove_duplicates(uint32_t* idx, uint32_t* nb, const v3* lp1) {
+    const float thr = SAME_POINT_DIST * SAME_POINT_DIST;
+    for (uint32_t i = 0; i < *nb; i++) {
+        for (uint32_t j = i + 1; j < *nb; j++) {
+            const float d = vlen2(vsub(lp1[idx[j]], lp1[idx[i]]));
+            if (d < thr) {
+                idx[j] = idx[*nb - 1];
+                (*nb)--;
+                j--;
+            }
+        }
+    }
+}
+
+/* The manifold of each colliding convex pair (processPotentialContacts,
+ * CollisionDetectionSystem.cpp:1198-1391, convex branch: one manifold holding
+ * every point), reduced to at most 4 points and de-duplicated
+ * (reducePotentialContactManifolds, :1394-1458).  Rewrites the contact slots
+ * of every pair in place (kept points first, in manifold order) and
+ * nb_contacts; kept[4*i..] receives the original slot of each kept point. */
+int rp3do_reduce_contacts(const rp3dg_pair_batch* p, const rp3dg_contact_batch* c, uint8_t* kept) {
+    if (!p || !c) return RP3DG_EINVAL;
+    const uint32_t n = p->n;
+    for (uint32_t i = 0; i < n; i++) {
+        if (p->cache) {
+            /* processPotentialContacts, CollisionDetectionSystem.cpp:1209-1217 */
+            uint8_t f = p->cache[i].flags;
+            f = (uint8_t)((f | RP3DG_LF_IS_VALID) & ~RP3DG_LF_WAS_COLLIDING);
+            if (c->is_colliding[i]) f |= RP3DG_LF_WAS_COLLIDING;
+            p->cache[i].flags = f;
+        }
+        uint32_t nb = c->nb_contacts[i];
+        uint32_t idx[RP3DG_MAX_CONTACTS_PER_PAIR];
+        v3 lp1[RP3DG_MAX_CONTACTS_PER_PAIR];
+        for (uint32_t k = 0; k < nb; k++) {
+            idx[k] = k;
+            const rp3dg_float4 l = c->local1[(size_t)k * n + i];
+            lp1[k] = V(l.x, l.y, l.z);
+        }
+        if (nb > 0 && c->is_colliding[i]) {
+            if (nb > MAX_POINTS_IN_MANIFOLD) {
+                const rp3dg_float4 nd = c->normal_depth[i];
+                reduce_points(idx, &nb, lp1, V(nd.x, nd.y, nd.z), Q(p->rot1[i].x, p->rot1[i].y, p->rot1[i].z, p->rot1[i].w));
+            }
+            remove_duplicates(idx, &nb, lp1);
+        }
+        rp3dg_float4 nd[4], l1[4], l2[4];
+        const uint32_t m = nb < 4 ? nb : 4;
+        for (uint32_t k = 0; k < m; k++) {
+            nd[k] = c->normal_depth[(size_t)idx[k] * n + i];
+            l1[k] = c->local1[(size_t)idx[k] * n + i];
+            l2[k] = c->local2[(size_t)idx[k] * n + i];
+        }
+        for (uint32_t k = 0; k < m; k++) {
+            c->normal_depth[(size_t)k * n + i] = nd[k];
+            c->local1[(size_t)k * n + i] = l1[k];
+            c->local2[(size_t)k * n + i] = l2[k];
+        }
+        if (kept) for (uint32_t k = 0; k < 4; k++) kept[4 * (size_t)i + k] = (uint8_t)(k < m ? idx[k] : 255);
+        c->nb_contacts[i] = (uint8_t)m;
+    }
+    return 0;
+}

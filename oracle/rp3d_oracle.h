@@ -32,6 +32,9 @@ void rp3do_reset(void);
 int rp3do_narrowphase(int algorithm, const rp3dg_shape* shapes, uint32_t nb_shapes, const rp3dg_pair_batch* pairs,
                       const rp3dg_contact_batch* out, int clip_with_previous_axis);
 
+/* Convex-pair manifold reduction (<= 4 points, de-duplicated), in place. */
+int rp3do_reduce_contacts(const rp3dg_pair_batch* pairs, const rp3dg_contact_batch* contacts, uint8_t* kept);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/rp3dg.h"
+#include "contacts_launch.h"
 #include "mlp_launch.h"
 #include "np_launch.h"
 #include "rp3dg_internal.h"
@@ -228,6 +229,10 @@ int fail(rp3dg_ctx* ctx, int code, const std::string& msg) {
     if (ctx) ctx->err = msg;
     return code;
 }
+
+// Device arrays are read with vector loads: float4 arrays and the 16-byte
+// cache records need 16-byte alignment, int32 arrays 4-byte.
+bool aligned(const void* ptr, uintptr_t a) { return (reinterpret_cast<uintptr_t>(ptr) & (a - 1)) == 0; }
 
 int cuda_fail(rp3dg_ctx* ctx, cudaError_t e, const char* what) {
     return fail(ctx, RP3DG_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -483,6 +488,10 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
     if (out->max_contacts < 1 || out->max_contacts > RP3DG_MAX_CONTACTS_PER_PAIR)
         return fail(ctx, RP3DG_EINVAL, "max_contacts must be in 1..16");
     if (!ctx->d_shapes) return fail(ctx, RP3DG_EINVAL, "no shape table (rp3dg_set_shapes)");
+    if (!aligned(p->pos1, 16) || !aligned(p->rot1, 16) || !aligned(p->pos2, 16) || !aligned(p->rot2, 16) ||
+        !aligned(p->cache, 16) || !aligned(out->normal_depth, 16) || !aligned(out->local1, 16) ||
+        !aligned(out->local2, 16) || !aligned(p->shape1, 4) || !aligned(p->shape2, 4))
+        return fail(ctx, RP3DG_EINVAL, "misaligned device array (float4 and cache arrays need 16 bytes, shape ids 4)");
     rp3dg::NpArgs a;
     a.n = p->n;
     a.nb_shapes = ctx->nb_shapes;
@@ -530,8 +539,40 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
     return 0;
 }
 
-int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3dg_contact_batch* out,
-                           int clip_with_previous_axis) {
+int rp3dg_reduce_contacts_device(rp3dg_ctx* ctx, const rp3dg_pair_batch* p, const rp3dg_contact_batch* c, uint8_t* kept) {
+    if (!ctx || !p || !c) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (p->n == 0) return 0;
+    if (!p->rot1 || !c->is_colliding || !c->nb_contacts || !c->normal_depth || !c->local1 || !c->local2)
+        return fail(ctx, RP3DG_EINVAL, "null array");
+    if (c->max_contacts < 1 || c->max_contacts > RP3DG_MAX_CONTACTS_PER_PAIR)
+        return fail(ctx, RP3DG_EINVAL, "max_contacts must be in 1..16");
+    if (!aligned(p->rot1, 16) || !aligned(p->cache, 16) || !aligned(c->normal_depth, 16) || !aligned(c->local1, 16) ||
+        !aligned(c->local2, 16) || !aligned(kept, 4))
+        return fail(ctx, RP3DG_EINVAL, "misaligned device array (float4 arrays need 16 bytes, kept 4)");
+    rp3dg::ReduceArgs a;
+    a.n = p->n;
+    a.max_contacts = c->max_contacts;
+    a.rot1 = reinterpret_cast<const float4*>(p->rot1);
+    a.cache = p->cache;
+    a.is_colliding = c->is_colliding;
+    a.nb_contacts = c->nb_contacts;
+    a.normal_depth = reinterpret_cast<float4*>(c->normal_depth);
+    a.local1 = reinterpret_cast<float4*>(c->local1);
+    a.local2 = reinterpret_cast<float4*>(c->local2);
+    a.kept = kept;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = rp3dg::launch_contacts_reduce(a, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "contact reduction");
+    ctx->launches++;
+    return 0;
+}
+
+namespace {
+
+// Host-array narrow phase through the staging buffer; with reduce set, the
+// manifold reduction runs on the device before the copy back (kept: n x 4).
+int narrowphase_host_impl(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3dg_contact_batch* out,
+                          int clip_with_previous_axis, bool reduce, uint8_t* kept) {
     if (!ctx || !p || !out) return fail(ctx, RP3DG_EINVAL, "null argument");
     if (p->n == 0) return 0;
     if (out->max_contacts < 1 || out->max_contacts > RP3DG_MAX_CONTACTS_PER_PAIR)
@@ -553,6 +594,7 @@ int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch
     const size_t o_nd = off; off += al(n * mc * 16);
     const size_t o_l1 = off; off += al(n * mc * 16);
     const size_t o_l2 = off; off += al(n * mc * 16);
+    const size_t o_kept = off; off += (reduce && kept) ? al(n * 4) : 0;
     cudaSetDevice(ctx->device);
     if (off > ctx->cap_stage) {
         cudaFree(ctx->d_stage);
@@ -592,9 +634,14 @@ int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch
     dout.max_contacts = out->max_contacts;
     int rc = rp3dg_narrowphase_device(ctx, algorithm, &dp, &dout, clip_with_previous_axis);
     if (rc) return rc;
+    if (reduce) {
+        rc = rp3dg_reduce_contacts_device(ctx, &dp, &dout, kept ? reinterpret_cast<uint8_t*>(b + o_kept) : nullptr);
+        if (rc) return rc;
+    }
     auto down = [&](void* dst, size_t o, size_t bytes) {
         if (e == cudaSuccess && dst) e = cudaMemcpyAsync(dst, b + o, bytes, cudaMemcpyDeviceToHost, s);
     };
+    if (reduce) down(kept, o_kept, n * 4);
     down(out->is_colliding, o_col, n);
     down(out->nb_contacts, o_nb, n);
     down(p->cache, o_cache, p->cache ? n * sizeof(rp3dg_lastframe) : 0);
@@ -609,6 +656,18 @@ int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e == cudaSuccess) e = cudaGetLastError();
     return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "narrowphase (host arrays)");
+}
+
+}  // namespace
+
+int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3dg_contact_batch* out,
+                           int clip_with_previous_axis) {
+    return narrowphase_host_impl(ctx, algorithm, p, out, clip_with_previous_axis, false, nullptr);
+}
+
+int rp3dg_narrowphase_manifolds_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p,
+                                     const rp3dg_contact_batch* out, int clip_with_previous_axis, uint8_t* kept) {
+    return narrowphase_host_impl(ctx, algorithm, p, out, clip_with_previous_axis, true, kept);
 }
 
 namespace {

@@ -64,6 +64,9 @@ def load_library(path=LIB_PATH):
     L.rp3dg_device_errors.argtypes = [P, C.POINTER(C.c_uint32), C.c_int]
     L.rp3dg_narrowphase_device.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_int]
     L.rp3dg_narrowphase_host.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_int]
+    L.rp3dg_reduce_contacts_device.argtypes = [P, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), P]
+    L.rp3dg_narrowphase_manifolds_host.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch),
+                                                   C.c_int, P]
     L.rp3dg_axis_mlp_init.argtypes = [P, C.c_uint64]
     L.rp3dg_axis_mlp_get_params.argtypes = [P, P]
     L.rp3dg_axis_mlp_set_params.argtypes = [P, P]
@@ -233,6 +236,25 @@ class Context:
         pb, cb = pairs.struct(), out.struct()
         self._check(self.lib.rp3dg_narrowphase_host(self.h, int(algo), C.byref(pb), C.byref(cb), int(clip)))
         return out
+
+    def narrowphase_manifolds_host(self, algo, pairs, out=None, clip=True, want_kept=True):
+        """Narrow phase + manifold reduction on host arrays; returns (out, kept)."""
+        out = out if out is not None else A.HostContacts(pairs.n)
+        kept = np.zeros((pairs.n, 4), np.uint8) if want_kept else None
+        pb, cb = pairs.struct(), out.struct()
+        self._check(self.lib.rp3dg_narrowphase_manifolds_host(self.h, algo, C.byref(pb), C.byref(cb), int(clip),
+                                                              None if kept is None else kept.ctypes.data))
+        return out, kept
+
+    def reduce_contacts_device(self, pairs, contacts, kept=None):
+        """Convex-pair manifold reduction in place on DeviceContacts; kept is an
+        optional (n, 4) uint8 CUDA tensor receiving the kept slots."""
+        pb, cb = pairs.struct(), contacts.struct()
+        self.order_in()
+        self._check(self.lib.rp3dg_reduce_contacts_device(self.h, C.byref(pb), C.byref(cb),
+                                                          None if kept is None else kept.data_ptr()))
+        self.order_out()
+        return contacts
 
     def narrowphase_device(self, algo, pairs, out, clip=True):
         """Asynchronous on the context stream, ordered after torch's current

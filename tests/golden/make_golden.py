@@ -16,6 +16,15 @@ Writes:
                    capsules, resting and edge-crossing boxes, deep and
                    margin-only sphere/capsule vs box and hull, reversed shape
                    order, report_contacts off, a scaled hull, max_contacts 2)
+  np_manifold.npz  contact-manifold reduction: per batch of a seeded scene,
+                   the reference narrow phase's raw points of selected pairs
+                   (every pair with more than 4 points, up to 160, plus
+                   colliding pairs with 1-4 points and separated pairs), and
+                   the reference's reduceContactPoints +
+                   removeDuplicatedContactPointsInManifold result ("red_"
+                   arrays and the kept-slot table)
+
+`python tests/golden/make_golden.py manifold` rewrites np_manifold.npz only.
 """
 import json
 import os
@@ -35,9 +44,116 @@ import reflib  # noqa: E402
 import edgecases  # noqa: E402
 
 
-def main():
+MANIFOLD_FIELDS = ("is_colliding", "nb_contacts", "normal_depth", "local1", "local2")
+
+
+def pick(c, idx, max_contacts):
+    """The pairs idx of a HostContacts, keeping max_contacts slots."""
+    s = A.HostContacts(len(idx), max_contacts)
+    s.is_colliding[:] = c.is_colliding[idx]
+    s.nb_contacts[:] = c.nb_contacts[idx]
+    for f in ("normal_depth", "local1", "local2"):
+        getattr(s, f)[...] = getattr(c, f)[:max_contacts, idx]
+    return s
+
+
+def manifold_fixture(ref, verts, faces):
+    sc = scenes.narrowphase_scene(total_pairs=7 * 8192, seed=29, hull=(verts, faces))
+    d = {}
+    rng = np.random.default_rng(30)
+    for name, (algo, pairs) in sc.batches.items():
+        pairs.cache = A.fresh_cache(pairs.n)
+        out, _ = ref.narrowphase(algo, sc.shapes, pairs.slice(0, pairs.n))
+        col = out.is_colliding.astype(bool)
+        many = np.flatnonzero(col & (out.nb_contacts > 4))[:160]
+        few = np.flatnonzero(col & (out.nb_contacts > 0) & (out.nb_contacts <= 4))
+        sep = np.flatnonzero(~col)
+        few = rng.choice(few, size=min(48, len(few)), replace=False) if len(few) else few
+        sep = rng.choice(sep, size=min(8, len(sep)), replace=False) if len(sep) else sep
+        idx = np.sort(np.concatenate([many, few, sep]).astype(np.int64))
+        mc = max(4, int(out.nb_contacts[idx].max()) if len(idx) else 4)
+        raw = pick(out, idx, mc)
+        sub = A.HostPairs(pairs.shape1[idx], pairs.shape2[idx], pairs.pos1[idx], pairs.rot1[idx],
+                          pairs.pos2[idx], pairs.rot2[idx])
+        red = reflib.copy_contacts(raw)
+        kept = reflib.reduce_contacts(ref.lib, "ref_reduce_contacts", sub, red)
+        d[name + "_pos1"], d[name + "_rot1"] = sub.pos1, sub.rot1
+        for f in MANIFOLD_FIELDS:
+            d[name + "_" + f] = getattr(raw, f)
+            d[name + "_red_" + f] = getattr(red, f)
+        d[name + "_kept"] = kept
+        print(name, "pairs", len(idx), ">4:", len(many), "max points", mc,
+              "de-duplicated:", int(np.sum(np.minimum(raw.nb_contacts, 4) != red.nb_contacts)))
+    pairs, raw = synthetic_manifolds(np.random.default_rng(31))
+    red = reflib.copy_contacts(raw)
+    kept = reflib.reduce_contacts(ref.lib, "ref_reduce_contacts", pairs, red)
+    d["synthetic_pos1"], d["synthetic_rot1"] = pairs.pos1, pairs.rot1
+    for f in MANIFOLD_FIELDS:
+        d["synthetic_" + f] = getattr(raw, f)
+        d["synthetic_red_" + f] = getattr(red, f)
+    d["synthetic_kept"] = kept
+    print("synthetic pairs", pairs.n, "de-duplicated:",
+          int(np.sum(np.minimum(raw.nb_contacts, 4) != red.nb_contacts)))
+    np.savez_compressed(os.path.join(HERE, "np_manifold.npz"), **d)
+
+
+def synthetic_manifolds(rng, n=512):
+    """Raw manifolds the reduction must handle beyond what a narrow phase
+    emits often: 1-16 points, exact and near (< 0.01) duplicates, collinear
+    and coincident sets, points on a grid (equal dot products and areas), a
+    separated pair that still holds points."""
+    mc = A.MAX_CONTACTS
+    c = A.HostContacts(n, mc)
+    q = rng.normal(size=(n, 4)).astype(np.float32)
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    nrm = rng.normal(size=(n, 3)).astype(np.float32)
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    for i in range(n):
+        kind = i % 8
+        nb = int(rng.integers(1, mc + 1)) if kind != 7 else int(rng.integers(5, mc + 1))
+        if kind == 0:
+            p = rng.uniform(-1, 1, size=(nb, 3))
+        elif kind == 1:       # exact duplicates
+            base = rng.uniform(-1, 1, size=(max(1, nb // 2), 3))
+            p = base[rng.integers(0, len(base), size=nb)]
+        elif kind == 2:       # near duplicates, within and just outside 0.01
+            base = rng.uniform(-1, 1, size=(max(1, nb // 3), 3))
+            p = base[rng.integers(0, len(base), size=nb)] + rng.normal(scale=0.006, size=(nb, 3))
+        elif kind == 3:       # collinear
+            t = rng.uniform(-1, 1, size=(nb, 1))
+            p = rng.uniform(-1, 1, size=(1, 3)) + t * rng.normal(size=(1, 3))
+        elif kind == 4:       # all the same point
+            p = np.repeat(rng.uniform(-1, 1, size=(1, 3)), nb, axis=0)
+        elif kind == 5:       # a grid in a plane: ties in every comparison
+            g = np.array([(x, y, 0.0) for x in range(4) for y in range(4)], np.float64) * 0.25
+            p = g[rng.permutation(16)[:nb]]
+        elif kind == 6:       # a box-face octagon with the normal along z
+            a = np.arange(nb) * (2 * np.pi / nb)
+            p = np.stack([np.cos(a), np.sin(a), np.zeros(nb)], 1)
+            nrm[i] = (0.0, 0.0, 1.0)
+            q[i] = (0.0, 0.0, 0.0, 1.0)
+        else:
+            p = rng.uniform(-1, 1, size=(nb, 3)) * np.array([1.0, 1.0, 1e-3])
+        c.nb_contacts[i] = nb
+        c.is_colliding[i] = 0 if i % 61 == 60 else 1
+        c.normal_depth[:nb, i, :3] = nrm[i]
+        c.normal_depth[:nb, i, 3] = rng.uniform(0.001, 0.2, size=nb)
+        c.local1[:nb, i, :3] = p
+        c.local2[:nb, i, :3] = p + rng.normal(scale=0.01, size=(nb, 3))
+    z = np.zeros(n, np.int32)
+    pairs = A.HostPairs(z, z, np.zeros((n, 4)), q, np.zeros((n, 4)), np.tile([0, 0, 0, 1.0], (n, 1)))
+    return pairs, c
+
+
+def main(parts=("scene", "manifold")):
     ref = reflib.RefEngine("f32")
     verts, faces = ref.quickhull(scenes.icosphere42_points())
+    if "scene" not in parts:
+        mesh = ref.create_convex_mesh(verts, faces)
+        ref.create_convex_mesh_shape(mesh)
+        ref.create_convex_mesh_shape(mesh, edgecases.HULL_SCALE)
+        manifold_fixture(ref, verts, faces)
+        return
     with open(os.path.join(HERE, "hull42.json"), "w") as fh:
         json.dump({"source": "reference QuickHull of scenes.icosphere42_points(seed=7, radius=0.8, noise=0.05)",
                    "vertices": [[float(x) for x in v] for v in verts], "faces": faces}, fh)
@@ -71,7 +187,9 @@ def main():
         goldenio.pack_case(e, f"{cname}_", algo, pin, out, pairs.cache)
         print(cname, "colliding:", out.is_colliding.tolist(), "contacts:", out.nb_contacts.tolist())
     np.savez_compressed(os.path.join(HERE, "np_edge.npz"), **e)
+    if "manifold" in parts:
+        manifold_fixture(ref, verts, faces)
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]) or ("scene", "manifold"))

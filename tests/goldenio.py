@@ -37,3 +37,25 @@ def unpack_case(z, prefix):
 
 def case_prefixes(z):
     return sorted({k[: k.index("algo")] for k in z.files if k.endswith("algo")})
+
+
+MANIFOLD_FIELDS = ("is_colliding", "nb_contacts", "normal_depth", "local1", "local2")
+
+
+def manifold_groups(z):
+    return sorted({k[: -len("_kept")] for k in z.files if k.endswith("_kept")})
+
+
+def unpack_manifold(z, name):
+    """(pairs, raw contacts, reduced contacts, kept table) of one group of
+    np_manifold.npz; the pairs carry only the shape-1 poses."""
+    rot1 = z[name + "_rot1"]
+    n = len(rot1)
+    zi = np.zeros(n, np.int32)
+    pairs = A.HostPairs(zi, zi, z[name + "_pos1"], rot1, np.zeros((n, 4)), np.tile([0, 0, 0, 1.0], (n, 1)))
+    mc = z[name + "_normal_depth"].shape[0]
+    raw, red = A.HostContacts(n, mc), A.HostContacts(n, mc)
+    for f in MANIFOLD_FIELDS:
+        getattr(raw, f)[...] = z[name + "_" + f]
+        getattr(red, f)[...] = z[name + "_red_" + f]
+    return pairs, raw, red, z[name + "_kept"]

@@ -188,3 +188,21 @@ def next_frame_cache(cache, out):
     c["flags"] &= ~np.uint8(A.LF_WAS_COLLIDING)
     c["flags"] |= np.where(out.is_colliding != 0, A.LF_WAS_COLLIDING, 0).astype(np.uint8)
     return c
+
+
+def reduce_contacts(lib, fn, pairs, contacts):
+    """Run a manifold-reduction entry point (ref_reduce_contacts or
+    rp3do_reduce_contacts) in place; returns the kept-slot table (n x 4)."""
+    getattr(lib, fn).argtypes = [C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_void_p]
+    kept = np.zeros((pairs.n, 4), np.uint8)
+    pb, cb = pairs.struct(), contacts.struct()
+    rc = getattr(lib, fn)(C.byref(pb), C.byref(cb), kept.ctypes.data)
+    assert rc == 0, rc
+    return kept
+
+
+def copy_contacts(c):
+    d = A.HostContacts(c.n, c.max_contacts)
+    for f in ("is_colliding", "nb_contacts", "normal_depth", "local1", "local2"):
+        getattr(d, f)[...] = getattr(c, f)
+    return d
