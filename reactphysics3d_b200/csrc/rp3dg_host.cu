@@ -706,7 +706,6 @@ int mlp_grads_into(rp3dg_ctx* ctx, const float* x, const uint8_t* y, uint32_t n,
     const size_t need = size_t(n) * rp3dg::MLP_SCRATCH_ROW * sizeof(float);
     if (need > ctx->cap_mlp_scratch) {
         cudaFree(ctx->d_mlp_scratch);
-    cudaFree(ctx->d_proposals);
         ctx->d_mlp_scratch = nullptr;
         cudaError_t e = cudaMalloc(&ctx->d_mlp_scratch, need);
         if (e != cudaSuccess) { ctx->cap_mlp_scratch = 0; return cuda_fail(ctx, e, "cudaMalloc(mlp scratch)"); }
