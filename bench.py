@@ -235,6 +235,10 @@ def run_ours(args):
         manifolds = manifold_section(ctx, sc, names, algos, dpairs, douts, args, dev,
                                      pinned)
 
+    dynamics = None
+    if not args.no_dynamics:
+        dynamics = dynamics_section(ctx, args, dev, rank == 0 and world == 1 and not args.no_cpu)
+
     learned = None
     if not args.no_learned:
         learned = learned_axis_section(ctx, sc, args, dev)
@@ -249,7 +253,8 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "pairs_per_gpu": sc.n_pairs, "batches": names,
                        "seed": args.seed, "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"independent pair sets per rank x{world}"},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "manifolds": manifolds, "learned_axis": learned,
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "manifolds": manifolds, "dynamics": dynamics,
+            "learned_axis": learned,
             "gpu_launches": int(launches),
             "clocks": clocks, "batch_ms": {k: round(v, 4) for k, v in mean_batch.items()}}
     if rank == 0:
@@ -319,6 +324,70 @@ def manifold_section(ctx, sc, names, algos, dpairs, douts, args, dev, pinned):
         out["e2e_narrowphase_plus_manifolds"] = {"value": round(sc.n_pairs / dt, 1), "unit": UNIT,
                                                  "ms_per_step": round(dt * 1e3, 4),
                                                  "api": "rp3dg_narrowphase_manifolds_host (pinned host buffers)"}
+    return out
+
+
+DYNAMICS_FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "np_dynamics.npz")
+
+
+def dynamics_section(ctx, args, dev, with_cpu):
+    """Dynamics stage of a world step (inertia, velocities, contact solver
+    with 6 velocity iterations and split impulses, positions, state) for many
+    independent worlds in one call: the reference worlds captured in
+    tests/golden/np_dynamics.npz, replicated to args.dyn_worlds worlds.
+    Device time per stage with CUDA events; the C restatement on one host
+    core for the same worlds as the CPU figure."""
+    import torch
+    from reactphysics3d_b200 import dynamics as D
+    z = np.load(DYNAMICS_FIXTURE)
+    names = sorted({k.split("/")[0] for k in z.files})
+    caps = [{k.split("/", 1)[1]: z[k] for k in z.files if k.startswith(n + "/")} for n in names]
+    base = [D.world_from_capture(c) for c in caps]
+    reps = (args.dyn_worlds + len(base) - 1) // len(base)
+    worlds = (base * reps)[: args.dyn_worlds]
+    batch, _ = D.batch_worlds(worlds)
+    params = D.params_from_capture(caps[0])
+    cnt = batch.counts
+    stream = ctx.torch_stream()
+    # inputs are restored from a pristine device copy before every step
+    # (outside the timed events), so each step solves the captured state
+    src = D.DynWorld(batch.a, batch.nb_enabled, batch.nc_enabled, device=dev)
+    work = D.DynWorld(batch.a, batch.nb_enabled, batch.nc_enabled, device=dev)
+    steps = max(3, min(args.steps, 20))
+    evs = []
+    launches0 = ctx.kernel_launches()
+    with torch.cuda.stream(stream):
+        for s_ in range(steps + 2):
+            for k in work.a:
+                work.a[k].copy_(src.a[k])
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ctx.dynamics_step(params, work)
+            b.record(stream)
+            if s_ >= 2:
+                evs.append((a, b))
+        ctx.synchronize()
+    launches = (ctx.kernel_launches() - launches0) // (steps + 2)
+    ms = float(np.mean([x.elapsed_time(y) for x, y in evs]))
+    out = {"workload": f"{len(worlds)} worlds (reference captures of tests/golden/np_dynamics.npz, replicated)",
+           "bodies": cnt["bodies"], "manifolds": cnt["manifolds"], "points": cnt["points"], "islands": cnt["islands"],
+           "kernels_per_stage": int(launches), "ms_per_stage": round(ms, 4),
+           "world_steps_per_s": round(len(worlds) / (ms / 1e3), 1),
+           "bodies_per_s": round(cnt["bodies"] / (ms / 1e3), 1)}
+    if with_cpu:
+        import ctypes as C
+        sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests"))
+        import reflib
+        lib = C.CDLL(reflib.PORT_LIB)
+        D.bind(lib, "rp3do_dynamics_step")
+        n_cpu = max(len(base), len(worlds) // 16)
+        cb, _ = D.batch_worlds(worlds[:n_cpu])
+        t0 = time.perf_counter()
+        b_, c_, m_, p_, i_ = cb.structs()
+        lib.rp3do_dynamics_step(C.byref(params), C.byref(b_), C.byref(c_), C.byref(m_), C.byref(p_), C.byref(i_))
+        dt_cpu = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(n_cpu / dt_cpu, 1), "unit": "world-steps/s", "cores": 1, "kind": "port",
+                               "sample": f"{n_cpu} of the worlds, one stage, C restatement (oracle), one core"}
     return out
 
 
@@ -522,6 +591,8 @@ def main():
     ap.add_argument("--traffic-bytes", type=float, default=None)
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-manifolds", action="store_true")
+    ap.add_argument("--no-dynamics", action="store_true")
+    ap.add_argument("--dyn-worlds", type=int, default=4096)
     ap.add_argument("--learned-epochs", type=int, default=4)
     args = ap.parse_args()
     if args.impl == "reference":

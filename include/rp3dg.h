@@ -282,6 +282,103 @@ int rp3dg_reduce_contacts_device(rp3dg_ctx* ctx, const rp3dg_pair_batch* pairs, 
 int rp3dg_narrowphase_manifolds_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* pairs,
                                      const rp3dg_contact_batch* out, int clip_with_previous_axis, uint8_t* kept);
 
+/* ---- dynamics stage of a world step ------------------------------------ */
+
+/* The part of PhysicsWorld::update (src/engine/PhysicsWorld.cpp:239-307) that
+ * runs after the contacts are created:
+ *   updateBodiesInverseWorldInertiaTensors (:310-318,
+ *     RigidBody::computeWorldInertiaTensorInverse, RigidBody.h:246-262),
+ *   DynamicsSystem::integrateRigidBodiesVelocities (DynamicsSystem.cpp:117-183),
+ *   ContactSolverSystem::init / initializeForIsland / warmStart / solve x
+ *     iterations / storeImpulses (ContactSolverSystem.cpp:66-818),
+ *   DynamicsSystem::integrateRigidBodiesPositions and updateBodiesState
+ *     (DynamicsSystem.cpp:44-110),
+ * bit-identical to the reference's float build for worlds without joints.
+ *
+ * Bodies follow the reference's rigid-body component order: the first
+ * n_enabled are integrated; the others (static and sleeping bodies) are only
+ * read, through their velocities and world inverse inertia.  Islands are
+ * ranges of the manifold array (which is in the solver's order: islands in
+ * order); manifolds of different islands may share only bodies with zero
+ * inverse mass and zero inverse inertia (static or kinematic), which the
+ * solver never moves, so islands are solved in parallel.  The solver does not
+ * write the velocities of such bodies (the reference adds signed zeros to
+ * them, which can only turn a -0 component into +0). */
+typedef struct rp3dg_bodies {
+    uint32_t n;                          /* bodies */
+    uint32_t n_enabled;                  /* bodies [0, n_enabled) are integrated */
+    rp3dg_float4* position;              /* in/out: transform position (xyz) */
+    rp3dg_float4* orientation;           /* in/out: transform orientation (x, y, z, w) */
+    rp3dg_float4* com_world;             /* in/out: centre of mass, world frame */
+    const rp3dg_float4* com_local;       /* centre of mass, body frame */
+    rp3dg_float4* linear_velocity;       /* in/out */
+    rp3dg_float4* angular_velocity;      /* in/out */
+    const rp3dg_float4* force;           /* external force, world frame */
+    const rp3dg_float4* torque;          /* external torque, world frame */
+    const rp3dg_float4* inv_inertia_local; /* diagonal of the local inverse inertia tensor */
+    rp3dg_float4* inv_inertia_world;     /* in/out: 3 rows per body (row r of body i at 3*i+r);
+                                            written for enabled bodies, read for the others */
+    const rp3dg_float4* mass;            /* x mass, y inverse mass, z linear damping, w angular damping */
+    const rp3dg_float4* linear_lock;     /* linear lock-axis factors */
+    const rp3dg_float4* angular_lock;    /* angular lock-axis factors */
+    const uint8_t* gravity;              /* 1 = gravity applies to the body */
+} rp3dg_bodies;
+
+typedef struct rp3dg_colliders {
+    uint32_t n;                          /* colliders, component order */
+    uint32_t n_enabled;                  /* colliders [0, n_enabled) get new world transforms */
+    const int32_t* body;                 /* body index of each collider */
+    const rp3dg_float4* local_position;  /* local-to-body transform */
+    const rp3dg_float4* local_orientation;
+    rp3dg_float4* world_position;        /* in/out: local-to-world transform */
+    rp3dg_float4* world_orientation;
+    const rp3dg_float4* material;        /* x sqrt(friction coefficient) (Material::mFrictionCoefficientSqrt),
+                                            y bounciness */
+} rp3dg_colliders;
+
+typedef struct rp3dg_manifolds {
+    uint32_t n;                          /* contact manifolds, solver order */
+    const int32_t* ids;                  /* 4 per manifold: body1, body2, collider1, collider2 */
+    const uint32_t* point_start;         /* first contact point of the manifold */
+    const uint8_t* nb_points;            /* 1..4 */
+    rp3dg_float4* friction_vector1;      /* in/out (warm start / stored) */
+    rp3dg_float4* friction_vector2;      /* in/out */
+    rp3dg_float4* friction_impulse;      /* in/out: x friction 1, y friction 2, z twist */
+} rp3dg_manifolds;
+
+typedef struct rp3dg_points {
+    uint32_t n;
+    const rp3dg_float4* normal_depth;    /* world normal (body 1 -> body 2), penetration depth */
+    const rp3dg_float4* local1;          /* contact point, collider-1 frame */
+    const rp3dg_float4* local2;          /* contact point, collider-2 frame */
+    float* penetration_impulse;          /* in/out */
+    uint8_t* is_resting;                 /* in/out (1 after the step, as the reference sets it) */
+} rp3dg_points;
+
+typedef struct rp3dg_islands {
+    uint32_t n;
+    const uint32_t* manifold_start;      /* each island is manifolds [start, start + count) */
+    const uint32_t* manifold_count;
+} rp3dg_islands;
+
+typedef struct rp3dg_dynamics_params {
+    float dt;
+    float gravity[3];                    /* world gravity (WorldSettings::gravity) */
+    int32_t gravity_enabled;             /* PhysicsWorld::isGravityEnabled */
+    int32_t velocity_iterations;         /* WorldSettings::defaultVelocitySolverNbIterations (6) */
+    int32_t split_impulse;               /* ContactSolverSystem::isSplitImpulseActive (1) */
+    float restitution_velocity_threshold; /* WorldSettings::restitutionVelocityThreshold (0.5) */
+} rp3dg_dynamics_params;
+
+/* One dynamics stage on device arrays (asynchronous on the context stream). */
+int rp3dg_dynamics_step_device(rp3dg_ctx* ctx, const rp3dg_dynamics_params* params, const rp3dg_bodies* bodies,
+                               const rp3dg_colliders* colliders, const rp3dg_manifolds* manifolds,
+                               const rp3dg_points* points, const rp3dg_islands* islands);
+/* The same on host arrays (copied in and out, synchronous). */
+int rp3dg_dynamics_step_host(rp3dg_ctx* ctx, const rp3dg_dynamics_params* params, const rp3dg_bodies* bodies,
+                             const rp3dg_colliders* colliders, const rp3dg_manifolds* manifolds,
+                             const rp3dg_points* points, const rp3dg_islands* islands);
+
 /* Number of kernels this context launched so far (instrumentation; a
  * convex-polyhedron batch takes two). */
 uint64_t rp3dg_kernel_launches(const rp3dg_ctx* ctx);

@@ -10,8 +10,9 @@
 // Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load
 // the resulting oracle/_ref/librp3d_ref_*.so.
 // The manifold-reduction entry below calls two private members of
-// CollisionDetectionSystem directly; access is widened for this translation
-// unit only (the reference objects themselves are compiled unchanged).
+// CollisionDetectionSystem directly: this translation unit is compiled with
+// -fno-access-control (oracle/Makefile), which lifts access checks without
+// changing any class layout; the reference objects are compiled unchanged.
 #include <algorithm>
 #include <array>
 #include <atomic>
@@ -22,8 +23,6 @@
 #include <sstream>
 #include <string>
 #include <unordered_map>
-#define private public
-#define protected public
 #include <reactphysics3d/reactphysics3d.h>
 #include <reactphysics3d/collision/narrowphase/NarrowPhaseInfoBatch.h>
 #include <reactphysics3d/collision/narrowphase/SphereVsSphereAlgorithm.h>

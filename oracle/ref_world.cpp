@@ -1,0 +1,395 @@
+// Test infrastructure, not product code: reference worlds (ReactPhysics3D
+// v0.10.2, built from its own sources by oracle/Makefile) stepped by the
+// reference itself, with the dynamics stage of one step captured.
+//
+// ref_world_create builds a seeded scene (a jittered grid of boxes, spheres
+// and capsules with random sizes, orientations, materials, dampings, lock
+// factors, external forces and a few kinematic / gravity-free bodies above a
+// static ground box).  ref_world_step runs PhysicsWorld::update.
+// ref_world_capture runs one step by calling the phases of
+// PhysicsWorld::update (src/engine/PhysicsWorld.cpp:239-307) in the same order
+// and records, between createContacts/reportContacts and the end of
+// updateBodiesState, every input and output of the dynamics stage: the
+// enabled rigid-body and collider components, the contact manifolds and
+// points in the contact solver's order (islands in order, each island's
+// manifold range in order), the islands as manifold ranges, and the world
+// settings.  Private members are reached because this translation unit is
+// compiled with -fno-access-control (oracle/Makefile), which lifts access
+// checks without changing any class layout; the reference objects are
+// compiled unchanged.
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cassert>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <iostream>
+#include <limits>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <random>
+#include <set>
+#include <sstream>
+#include <string>
+#include <unordered_map>
+#include <utility>
+#include <vector>
+#include <reactphysics3d/reactphysics3d.h>
+
+using namespace reactphysics3d;
+
+namespace {
+
+struct Capture {
+    std::map<std::string, std::vector<uint8_t>> f;
+    template <class T>
+    void put(const std::string& name, const std::vector<T>& v) {
+        std::vector<uint8_t> b(v.size() * sizeof(T));
+        if (!v.empty()) std::memcpy(b.data(), v.data(), b.size());
+        f[name] = std::move(b);
+    }
+};
+
+struct World {
+    PhysicsCommon common;
+    PhysicsWorld* world = nullptr;
+    std::vector<RigidBody*> bodies;
+    Capture cap;
+};
+
+std::vector<std::unique_ptr<World>>& worlds() {
+    static std::vector<std::unique_ptr<World>> w;
+    return w;
+}
+
+void f4(std::vector<float>& out, const Vector3& v, float w = 0.0f) {
+    out.push_back(float(v.x)); out.push_back(float(v.y)); out.push_back(float(v.z)); out.push_back(w);
+}
+void q4(std::vector<float>& out, const Quaternion& q) {
+    out.push_back(float(q.x)); out.push_back(float(q.y)); out.push_back(float(q.z)); out.push_back(float(q.w));
+}
+
+// Uniform unit quaternion (Shoemake).
+Quaternion random_rotation(std::mt19937_64& rng) {
+    std::uniform_real_distribution<double> u(0.0, 1.0);
+    const double u1 = u(rng), u2 = u(rng), u3 = u(rng);
+    const double a = std::sqrt(1.0 - u1), b = std::sqrt(u1);
+    const double t1 = 2.0 * 3.14159265358979323846 * u2, t2 = 2.0 * 3.14159265358979323846 * u3;
+    Quaternion q(decimal(a * std::sin(t1)), decimal(a * std::cos(t1)), decimal(b * std::sin(t2)), decimal(b * std::cos(t2)));
+    q.normalize();
+    return q;
+}
+
+// Bodies and colliders of the enabled component ranges, as the dynamics
+// stage sees them.
+void capture_state(World& W, const std::string& pre, bool inputs) {
+    PhysicsWorld& w = *W.world;
+    RigidBodyComponents& rb = w.mRigidBodyComponents;
+    ColliderComponents& cc = w.mCollidersComponents;
+    TransformComponents& tc = w.mTransformComponents;
+    // every component: the solver also reads bodies outside the enabled range
+    // (static bodies are never enabled), through their constrained
+    // velocities and world inverse inertia
+    const uint32 nb = rb.getNbComponents();
+    std::vector<float> pos, ori, comw, coml, lv, av, force, torque, iil, mass, llock, alock, iiw, clv, cav, sv;
+    std::vector<uint8_t> grav;
+    for (uint32 i = 0; i < nb; i++) {
+        const Transform& t = tc.getTransform(rb.mBodiesEntities[i]);
+        f4(pos, t.getPosition());
+        q4(ori, t.getOrientation());
+        f4(comw, rb.mCentersOfMassWorld[i]);
+        f4(lv, rb.mLinearVelocities[i]);
+        f4(av, rb.mAngularVelocities[i]);
+        if (inputs) {
+            f4(coml, rb.mCentersOfMassLocal[i]);
+            f4(force, rb.mExternalForces[i]);
+            f4(torque, rb.mExternalTorques[i]);
+            f4(iil, rb.mInverseInertiaTensorsLocal[i]);
+            mass.push_back(float(rb.mMasses[i])); mass.push_back(float(rb.mInverseMasses[i]));
+            mass.push_back(float(rb.mLinearDampings[i])); mass.push_back(float(rb.mAngularDampings[i]));
+            f4(llock, rb.mLinearLockAxisFactors[i]);
+            f4(alock, rb.mAngularLockAxisFactors[i]);
+            grav.push_back(rb.mIsGravityEnabled[i] ? 1 : 0);
+            f4(clv, rb.mConstrainedLinearVelocities[i]);
+            f4(cav, rb.mConstrainedAngularVelocities[i]);
+            f4(sv, rb.mSplitLinearVelocities[i]);
+            f4(sv, rb.mSplitAngularVelocities[i]);
+            const Matrix3x3& m = rb.mInverseInertiaTensorsWorld[i];
+            for (int r = 0; r < 3; r++) f4(iiw, m[r]);
+        } else {
+            const Matrix3x3& m = rb.mInverseInertiaTensorsWorld[i];
+            for (int r = 0; r < 3; r++) f4(iiw, m[r]);
+        }
+    }
+    W.cap.put(pre + "body_position", pos);
+    W.cap.put(pre + "body_orientation", ori);
+    W.cap.put(pre + "body_com_world", comw);
+    W.cap.put(pre + "body_linear_velocity", lv);
+    W.cap.put(pre + "body_angular_velocity", av);
+    if (inputs) {
+        W.cap.put(pre + "body_com_local", coml);
+        W.cap.put(pre + "body_force", force);
+        W.cap.put(pre + "body_torque", torque);
+        W.cap.put(pre + "body_inv_inertia_local", iil);
+        W.cap.put(pre + "body_mass", mass);
+        W.cap.put(pre + "body_linear_lock", llock);
+        W.cap.put(pre + "body_angular_lock", alock);
+        W.cap.put(pre + "body_gravity", grav);
+        W.cap.put(pre + "body_constrained_linear_velocity", clv);
+        W.cap.put(pre + "body_constrained_angular_velocity", cav);
+        W.cap.put(pre + "body_split_velocity", sv);
+        W.cap.put(pre + "body_inv_inertia_world", iiw);
+        std::vector<uint32_t> ne = {rb.getNbEnabledComponents()};
+        W.cap.put(pre + "body_nb_enabled", ne);
+    } else {
+        W.cap.put(pre + "body_inv_inertia_world", iiw);
+    }
+    const uint32 nc = cc.getNbComponents();
+    std::vector<int32_t> cbody;
+    std::vector<float> clp, clo, cwp, cwo, cmat;
+    for (uint32 i = 0; i < nc; i++) {
+        const Transform& lw = cc.mLocalToWorldTransforms[i];
+        f4(cwp, lw.getPosition());
+        q4(cwo, lw.getOrientation());
+        if (inputs) {
+            cbody.push_back(int32_t(rb.getEntityIndex(cc.mBodiesEntities[i])));
+            const Transform& lb = cc.mLocalToBodyTransforms[i];
+            f4(clp, lb.getPosition());
+            q4(clo, lb.getOrientation());
+            const Material& m = cc.mMaterials[i];
+            cmat.push_back(float(m.getFrictionCoefficientSqrt()));
+            cmat.push_back(float(m.getBounciness()));
+            cmat.push_back(0.0f); cmat.push_back(0.0f);
+        }
+    }
+    W.cap.put(pre + "collider_world_position", cwp);
+    W.cap.put(pre + "collider_world_orientation", cwo);
+    if (inputs) {
+        W.cap.put(pre + "collider_body", cbody);
+        W.cap.put(pre + "collider_local_position", clp);
+        W.cap.put(pre + "collider_local_orientation", clo);
+        W.cap.put(pre + "collider_material", cmat);
+        std::vector<uint32_t> ne = {cc.getNbEnabledComponents()};
+        W.cap.put(pre + "collider_nb_enabled", ne);
+    }
+}
+
+// Manifolds in the solver's order: islands in order, each island's range.
+std::vector<uint32_t> solver_order(World& W) {
+    Islands& isl = W.world->mIslands;
+    std::vector<uint32_t> order;
+    for (uint32 i = 0; i < isl.getNbIslands(); i++)
+        for (uint32 m = isl.contactManifoldsIndices[i]; m < isl.contactManifoldsIndices[i] + isl.nbContactManifolds[i]; m++)
+            order.push_back(m);
+    return order;
+}
+
+void capture_contacts(World& W, const std::string& pre, const std::vector<uint32_t>& order, bool inputs) {
+    PhysicsWorld& w = *W.world;
+    Array<ContactManifold>& mans = *w.mCollisionDetection.mCurrentContactManifolds;
+    Array<ContactPoint>& pts = *w.mCollisionDetection.mCurrentContactPoints;
+    RigidBodyComponents& rb = w.mRigidBodyComponents;
+    ColliderComponents& cc = w.mCollidersComponents;
+    std::vector<int32_t> ids;
+    std::vector<uint32_t> pstart, src;
+    std::vector<uint8_t> npts, resting;
+    std::vector<float> fv1, fv2, fimp, nd, l1, l2, pimp;
+    for (uint32_t k = 0; k < order.size(); k++) {
+        const ContactManifold& m = mans[order[k]];
+        src.push_back(order[k]);
+        ids.push_back(int32_t(rb.getEntityIndex(m.bodyEntity1)));
+        ids.push_back(int32_t(rb.getEntityIndex(m.bodyEntity2)));
+        ids.push_back(int32_t(cc.getEntityIndex(m.colliderEntity1)));
+        ids.push_back(int32_t(cc.getEntityIndex(m.colliderEntity2)));
+        pstart.push_back(uint32_t(pimp.size()));
+        npts.push_back(m.nbContactPoints);
+        f4(fv1, m.frictionVector1);
+        f4(fv2, m.frictionVector2);
+        fimp.push_back(float(m.frictionImpulse1)); fimp.push_back(float(m.frictionImpulse2));
+        fimp.push_back(float(m.frictionTwistImpulse)); fimp.push_back(0.0f);
+        for (uint32 c = m.contactPointsIndex; c < m.contactPointsIndex + m.nbContactPoints; c++) {
+            const ContactPoint& p = pts[c];
+            f4(nd, p.getNormal(), float(p.getPenetrationDepth()));
+            f4(l1, p.getLocalPointOnShape1());
+            f4(l2, p.getLocalPointOnShape2());
+            pimp.push_back(float(p.getPenetrationImpulse()));
+            resting.push_back(p.getIsRestingContact() ? 1 : 0);
+        }
+    }
+    W.cap.put(pre + "manifold_friction_vector1", fv1);
+    W.cap.put(pre + "manifold_friction_vector2", fv2);
+    W.cap.put(pre + "manifold_friction_impulse", fimp);
+    W.cap.put(pre + "point_penetration_impulse", pimp);
+    W.cap.put(pre + "point_is_resting", resting);
+    if (inputs) {
+        W.cap.put(pre + "manifold_ids", ids);
+        W.cap.put(pre + "manifold_point_start", pstart);
+        W.cap.put(pre + "manifold_nb_points", npts);
+        W.cap.put(pre + "manifold_source", src);
+        W.cap.put(pre + "point_normal_depth", nd);
+        W.cap.put(pre + "point_local1", l1);
+        W.cap.put(pre + "point_local2", l2);
+        Islands& isl = w.mIslands;
+        std::vector<uint32_t> is, in;
+        uint32_t at = 0;
+        for (uint32 i = 0; i < isl.getNbIslands(); i++) {
+            is.push_back(at);
+            in.push_back(isl.nbContactManifolds[i]);
+            at += isl.nbContactManifolds[i];
+        }
+        W.cap.put(pre + "island_manifold_start", is);
+        W.cap.put(pre + "island_manifold_count", in);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// kind 0: boxes only; 1: boxes, spheres and capsules.  Returns a world id.
+int ref_world_create(int kind, uint64_t seed, int nx, int ny, int nz, float spacing, int variety) {
+    auto W = std::make_unique<World>();
+    PhysicsWorld::WorldSettings s;
+    W->world = W->common.createPhysicsWorld(s);
+    std::mt19937_64 rng(seed);
+    std::uniform_real_distribution<double> u(0.0, 1.0);
+    auto U = [&](double a, double b) { return decimal(a + (b - a) * u(rng)); };
+    // static ground box 50 x 0.5 x 50 (half-extents 25, 0.25, 25) with its top at y = 0
+    RigidBody* ground = W->world->createRigidBody(Transform(Vector3(0, decimal(-0.25), 0), Quaternion::identity()));
+    ground->setType(BodyType::STATIC);
+    Collider* gc = ground->addCollider(W->common.createBoxShape(Vector3(25, decimal(0.25), 25)), Transform::identity());
+    if (variety) gc->getMaterial().setFrictionCoefficient(decimal(0.6));
+    W->bodies.push_back(ground);
+    int count = 0;
+    for (int iy = 0; iy < ny; iy++)
+        for (int ix = 0; ix < nx; ix++)
+            for (int iz = 0; iz < nz; iz++) {
+                const Vector3 p(decimal((ix - 0.5 * (nx - 1)) * spacing) + U(-0.1, 0.1),
+                                decimal(1.0 + iy * spacing) + U(-0.1, 0.1),
+                                decimal((iz - 0.5 * (nz - 1)) * spacing) + U(-0.1, 0.1));
+                RigidBody* b = W->world->createRigidBody(Transform(p, random_rotation(rng)));
+                const int shape = kind == 0 ? 0 : int(u(rng) * 3.0);
+                CollisionShape* cs;
+                if (shape == 0) cs = W->common.createBoxShape(Vector3(U(0.25, 0.75), U(0.25, 0.75), U(0.25, 0.75)));
+                else if (shape == 1) cs = W->common.createSphereShape(U(0.2, 0.5));
+                else cs = W->common.createCapsuleShape(decimal(0.2), decimal(0.6));
+                Collider* c = b->addCollider(cs, Transform::identity());
+                if (variety) {
+                    c->getMaterial().setFrictionCoefficient(U(0.1, 1.0));
+                    c->getMaterial().setBounciness(U(0.0, 0.6));
+                }
+                b->updateMassPropertiesFromColliders();
+                if (variety) {
+                    const int k = count % 23;
+                    if (k == 3) b->setLinearDamping(U(0.0, 0.5));
+                    if (k == 4) b->setAngularDamping(U(0.0, 0.5));
+                    if (k == 5) b->setLinearLockAxisFactor(Vector3(1, 0, 1));
+                    if (k == 6) b->setAngularLockAxisFactor(Vector3(0, 1, 0));
+                    if (k == 7) b->enableGravity(false);
+                    if (k == 8) b->setLinearVelocity(Vector3(U(-2, 2), U(-2, 0), U(-2, 2)));
+                    if (k == 9) b->setAngularVelocity(Vector3(U(-3, 3), U(-3, 3), U(-3, 3)));
+                    if (k == 10) {
+                        b->setType(BodyType::KINEMATIC);
+                        b->setLinearVelocity(Vector3(U(-0.5, 0.5), 0, U(-0.5, 0.5)));
+                    }
+                }
+                W->bodies.push_back(b);
+                count++;
+            }
+    worlds().push_back(std::move(W));
+    return int(worlds().size()) - 1;
+}
+
+// External forces/torques on every 5th dynamic body (they are reset by each
+// update, so they are applied right before a step).
+int ref_world_apply_forces(int id, uint64_t seed) {
+    World& W = *worlds().at(size_t(id));
+    std::mt19937_64 rng(seed);
+    std::uniform_real_distribution<double> u(-1.0, 1.0);
+    for (size_t i = 1; i < W.bodies.size(); i += 5) {
+        RigidBody* b = W.bodies[i];
+        if (b->getType() != BodyType::DYNAMIC) continue;
+        b->applyWorldForceAtCenterOfMass(Vector3(decimal(20 * u(rng)), decimal(20 * u(rng)), decimal(20 * u(rng))));
+        b->applyLocalTorque(Vector3(decimal(5 * u(rng)), decimal(5 * u(rng)), decimal(5 * u(rng))));
+    }
+    return 0;
+}
+
+int ref_world_step(int id, float dt, int nsteps) {
+    World& W = *worlds().at(size_t(id));
+    for (int i = 0; i < nsteps; i++) W.world->update(decimal(dt));
+    return 0;
+}
+
+// One step, phase by phase in the order of PhysicsWorld::update, recording
+// the dynamics stage's inputs ("in_") and outputs ("out_").
+int ref_world_capture(int id, float dt) {
+    World& W = *worlds().at(size_t(id));
+    PhysicsWorld& w = *W.world;
+    W.cap.f.clear();
+    const decimal timeStep = decimal(dt);
+    w.mCollisionDetection.computeCollisionDetection();
+    w.createIslands();
+    w.mCollisionDetection.createContacts();
+    w.mCollisionDetection.reportContactsAndTriggers();
+
+    const std::vector<uint32_t> order = solver_order(W);
+    capture_state(W, "in_", true);
+    capture_contacts(W, "in_", order, true);
+    std::vector<float> params = {float(timeStep), float(w.mConfig.gravity.x), float(w.mConfig.gravity.y),
+                                 float(w.mConfig.gravity.z), w.mIsGravityEnabled ? 1.0f : 0.0f,
+                                 float(w.mNbVelocitySolverIterations), w.mContactSolverSystem.isSplitImpulseActive() ? 1.0f : 0.0f,
+                                 float(w.mContactSolverSystem.mRestitutionVelocityThreshold)};
+    W.cap.put("params", params);
+
+    w.updateBodiesInverseWorldInertiaTensors();
+    w.enableDisableJoints();
+    w.mDynamicsSystem.integrateRigidBodiesVelocities(timeStep);
+    w.solveContactsAndConstraints(timeStep);
+    w.mDynamicsSystem.integrateRigidBodiesPositions(timeStep, w.mContactSolverSystem.isSplitImpulseActive());
+    w.solvePositionCorrection();
+    w.mDynamicsSystem.updateBodiesState();
+
+    capture_state(W, "out_", false);
+    capture_contacts(W, "out_", order, false);
+
+    w.mCollisionDetection.updateColliders();
+    if (w.mIsSleepingEnabled) w.updateSleepingBodies(timeStep);
+    w.mDynamicsSystem.resetBodiesForceAndTorque();
+    w.mIslands.clear();
+    w.mProcessContactPairsOrderIslands.clear(true);
+    w.mMemoryManager.resetFrameAllocator();
+    return 0;
+}
+
+// Size in bytes of a captured field (-1 if absent) and a copy of it.
+long ref_world_field_size(int id, const char* name) {
+    World& W = *worlds().at(size_t(id));
+    auto it = W.cap.f.find(name);
+    return it == W.cap.f.end() ? -1 : long(it->second.size());
+}
+
+int ref_world_field(int id, const char* name, void* dst) {
+    World& W = *worlds().at(size_t(id));
+    auto it = W.cap.f.find(name);
+    if (it == W.cap.f.end()) return -1;
+    if (!it->second.empty()) std::memcpy(dst, it->second.data(), it->second.size());
+    return 0;
+}
+
+// Names of the captured fields, separated by spaces.
+int ref_world_field_names(int id, char* dst, int cap) {
+    World& W = *worlds().at(size_t(id));
+    std::string s;
+    for (auto& kv : W.cap.f) { s += kv.first; s += ' '; }
+    if (int(s.size()) + 1 > cap) return -1;
+    std::memcpy(dst, s.c_str(), s.size() + 1);
+    return 0;
+}
+
+void ref_world_destroy_all(void) { worlds().clear(); }
+
+}  // extern "C"

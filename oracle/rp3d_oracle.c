@@ -1677,3 +1677,393 @@ int rp3do_reduce_contacts(const rp3dg_pair_batch* p, const rp3dg_contact_batch* 
     }
     return 0;
 }
+
+/* ===================================================================== */
+/* Dynamics stage of a world step (PhysicsWorld.cpp:310-360,             */
+/* DynamicsSystem.cpp:44-183, ContactSolverSystem.cpp:66-818), restated  */
+/* phase by phase over the whole world, with the reference's sequential  */
+/* order: all islands' manifolds in one pass per phase.                  */
+/* ===================================================================== */
+
+typedef struct {
+    int b1, b2, nb;
+    float im1, im2, friction;
+    v3 lf1, lf2, af1, af2;
+    float I1[9], I2[9];
+    v3 normal, fp1, fp2, r1f, r2f, ofv1, ofv2, fv1, fv2, r1ct1, r1ct2, r2ct1, r2ct2;
+    float inv_f1, inv_f2, inv_tw, f1, f2, ftw;
+    uint32_t ext;        /* index of the external manifold */
+} DynMan;
+
+typedef struct {
+    v3 r1, r2, normal, i1, i2;
+    float depth, inv_mass, restitution_bias, impulse, split_impulse;
+    int resting;
+    uint32_t ext;        /* index of the external contact point */
+} DynPt;
+
+static v3 L4(rp3dg_float4 a) { return V(a.x, a.y, a.z); }
+static rp3dg_float4 S4(v3 a) { rp3dg_float4 r; r.x = a.x; r.y = a.y; r.z = a.z; r.w = 0.0f; return r; }
+/* Matrix3x3 * Vector3 (Matrix3x3.h:324-331) */
+static v3 m3v(const float* m, v3 v) {
+    return V(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[3] * v.x + m[4] * v.y + m[5] * v.z,
+             m[6] * v.x + m[7] * v.y + m[8] * v.z);
+}
+/* Quaternion::getMatrix (Quaternion.cpp:138-165) */
+static void q_matrix(quat q, float* r) {
+    float nQ = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w, s = 0.0f;
+    if (nQ > 0.0f) s = 2.0f / nQ;
+    float xs = q.x * s, ys = q.y * s, zs = q.z * s, wxs = q.w * xs, wys = q.w * ys, wzs = q.w * zs;
+    float xxs = q.x * xs, xys = q.x * ys, xzs = q.x * zs, yys = q.y * ys, yzs = q.y * zs, zzs = q.z * zs;
+    r[0] = 1.0f - yys - zzs; r[1] = xys - wzs; r[2] = xzs + wys;
+    r[3] = xys + wzs; r[4] = 1.0f - xxs - zzs; r[5] = yzs - wxs;
+    r[6] = xzs - wys; r[7] = yzs + wxs; r[8] = 1.0f - xxs - yys;
+}
+/* Matrix3x3 * Matrix3x3 (Matrix3x3.h:302-321) */
+static void m3m(const float* a, const float* b, float* o) {
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) o[3 * i + j] = a[3 * i] * b[j] + a[3 * i + 1] * b[3 + j] + a[3 * i + 2] * b[6 + j];
+}
+/* deltaV of ContactSolverSystem.cpp:196-201 */
+static v3 rel_vel(v3 v1, v3 w1, v3 v2, v3 w2, v3 r1, v3 r2) {
+    return V(v2.x + w2.y * r2.z - w2.z * r2.y - v1.x - w1.y * r1.z + w1.z * r1.y,
+             v2.y + w2.z * r2.x - w2.x * r2.z - v1.y - w1.z * r1.x + w1.x * r1.z,
+             v2.z + w2.x * r2.y - w2.y * r2.x - v1.z - w1.x * r1.y + w1.y * r1.x);
+}
+/* Vector3::getOneUnitOrthogonalVector (Vector3.cpp:46-64) */
+static v3 one_unit_orthogonal(v3 v) {
+    v3 a = V(fabsf(v.x), fabsf(v.y), fabsf(v.z));
+    int k = (a.x < a.y ? (a.x < a.z ? 0 : 2) : (a.y < a.z ? 1 : 2));
+    if (k == 0) return vdivs(V(0.0f, -v.z, v.y), sqrtf(v.y * v.y + v.z * v.z));
+    if (k == 1) return vdivs(V(-v.z, 0.0f, v.x), sqrtf(v.x * v.x + v.z * v.z));
+    return vdivs(V(-v.y, v.x, 0.0f), sqrtf(v.x * v.x + v.y * v.y));
+}
+/* v -= s * imp * lock (or +=), Vector3 operators */
+static v3 lin_sub(v3 v, float s, v3 imp, v3 lock) { return vsub(v, vcmul(vmul(imp, s), lock)); }
+static v3 lin_add(v3 v, float s, v3 imp, v3 lock) { return vadd(v, vcmul(vmul(imp, s), lock)); }
+
+int rp3do_dynamics_step(const rp3dg_dynamics_params* pr, const rp3dg_bodies* B, const rp3dg_colliders* Cl,
+                        const rp3dg_manifolds* M, const rp3dg_points* P, const rp3dg_islands* IS) {
+    const uint32_t nb = B->n, ne = B->n_enabled;
+    const float dt = pr->dt;
+    v3* cv = (v3*)calloc(nb ? nb : 1, sizeof(v3));
+    v3* cw = (v3*)calloc(nb ? nb : 1, sizeof(v3));
+    v3* sv = (v3*)calloc(nb ? nb : 1, sizeof(v3));
+    v3* sw = (v3*)calloc(nb ? nb : 1, sizeof(v3));
+    DynMan* man = (DynMan*)calloc(M->n ? M->n : 1, sizeof(DynMan));
+    DynPt* pt = (DynPt*)calloc(P->n ? P->n : 1, sizeof(DynPt));
+    if (!cv || !cw || !sv || !sw || !man || !pt) { free(cv); free(cw); free(sv); free(sw); free(man); free(pt); return RP3DG_ENOMEM; }
+    /* bodies outside the enabled range keep their stored velocities */
+    for (uint32_t i = ne; i < nb; i++) { cv[i] = L4(B->linear_velocity[i]); cw[i] = L4(B->angular_velocity[i]); }
+
+    /* updateBodiesInverseWorldInertiaTensors (PhysicsWorld.cpp:310-318) */
+    for (uint32_t i = 0; i < ne; i++) {
+        float R[9], D[9], W[9];
+        rp3dg_float4 o = B->orientation[i];
+        q_matrix(Q(o.x, o.y, o.z, o.w), R);
+        v3 inv = L4(B->inv_inertia_local[i]);
+        D[0] = R[0] * inv.x; D[1] = R[3] * inv.x; D[2] = R[6] * inv.x;
+        D[3] = R[1] * inv.y; D[4] = R[4] * inv.y; D[5] = R[7] * inv.y;
+        D[6] = R[2] * inv.z; D[7] = R[5] * inv.z; D[8] = R[8] * inv.z;
+        m3m(R, D, W);
+        for (int r = 0; r < 3; r++) {
+            rp3dg_float4 row; row.x = W[3 * r]; row.y = W[3 * r + 1]; row.z = W[3 * r + 2]; row.w = 0.0f;
+            B->inv_inertia_world[3 * i + r] = row;
+        }
+    }
+    /* integrateRigidBodiesVelocities (DynamicsSystem.cpp:117-183) */
+    for (uint32_t i = 0; i < ne; i++) {
+        const rp3dg_float4 m = B->mass[i];
+        const float* W = &B->inv_inertia_world[3 * i].x;
+        float I[9] = {W[0], W[1], W[2], W[4], W[5], W[6], W[8], W[9], W[10]};
+        v3 lf = L4(B->linear_lock[i]), af = L4(B->angular_lock[i]);
+        cv[i] = vadd(L4(B->linear_velocity[i]), vcmul(vmul(lf, dt * m.y), L4(B->force[i])));
+        cw[i] = vadd(L4(B->angular_velocity[i]), vcmul(vmul(af, dt), m3v(I, L4(B->torque[i]))));
+    }
+    if (pr->gravity_enabled)
+        for (uint32_t i = 0; i < ne; i++)
+            if (B->gravity[i]) {
+                const rp3dg_float4 m = B->mass[i];
+                v3 g = V(pr->gravity[0], pr->gravity[1], pr->gravity[2]);
+                cv[i] = vadd(cv[i], vcmul(vmul(vmul(L4(B->linear_lock[i]), dt * m.y), m.x), g));
+            }
+    for (uint32_t i = 0; i < ne; i++) {
+        const rp3dg_float4 m = B->mass[i];
+        float ld = 1.0f / (1.0f + m.z * dt), ad = 1.0f / (1.0f + m.w * dt);
+        cv[i] = vmul(cv[i], ld);
+        cw[i] = vmul(cw[i], ad);
+    }
+
+    /* ContactSolverSystem::init / initializeForIsland (:66-318) */
+    uint32_t nm = 0, np = 0;
+    for (uint32_t il = 0; il < IS->n; il++) {
+        for (uint32_t e = IS->manifold_start[il]; e < IS->manifold_start[il] + IS->manifold_count[il]; e++) {
+            DynMan* c = &man[nm];
+            const int32_t* id = &M->ids[4 * e];
+            const int b1 = id[0], b2 = id[1], c1 = id[2], c2 = id[3];
+            c->b1 = b1; c->b2 = b2; c->nb = M->nb_points[e]; c->ext = e;
+            v3 x1 = L4(B->com_world[b1]), x2 = L4(B->com_world[b2]);
+            for (int k = 0; k < 9; k++) {
+                c->I1[k] = (&B->inv_inertia_world[3 * b1].x)[(k / 3) * 4 + k % 3];
+                c->I2[k] = (&B->inv_inertia_world[3 * b2].x)[(k / 3) * 4 + k % 3];
+            }
+            c->im1 = B->mass[b1].y; c->im2 = B->mass[b2].y;
+            c->lf1 = L4(B->linear_lock[b1]); c->lf2 = L4(B->linear_lock[b2]);
+            c->af1 = L4(B->angular_lock[b1]); c->af2 = L4(B->angular_lock[b2]);
+            c->friction = Cl->material[c1].x * Cl->material[c2].x;
+            c->normal = V(0.0f, 0.0f, 0.0f); c->fp1 = V(0.0f, 0.0f, 0.0f); c->fp2 = V(0.0f, 0.0f, 0.0f);
+            v3 v1 = L4(B->linear_velocity[b1]), w1 = L4(B->angular_velocity[b1]);
+            v3 v2 = L4(B->linear_velocity[b2]), w2 = L4(B->angular_velocity[b2]);
+            rp3dg_float4 o1 = Cl->world_orientation[c1], o2 = Cl->world_orientation[c2];
+            xform t1 = X(L4(Cl->world_position[c1]), Q(o1.x, o1.y, o1.z, o1.w));
+            xform t2 = X(L4(Cl->world_position[c2]), Q(o2.x, o2.y, o2.z, o2.w));
+            for (uint32_t q = M->point_start[e]; q < M->point_start[e] + c->nb; q++) {
+                DynPt* p = &pt[np];
+                p->ext = q;
+                p->normal = L4(P->normal_depth[q]);
+                v3 p1 = xapply(t1, L4(P->local1[q])), p2 = xapply(t2, L4(P->local2[q]));
+                p->r1 = V(p1.x - x1.x, p1.y - x1.y, p1.z - x1.z);
+                p->r2 = V(p2.x - x2.x, p2.y - x2.y, p2.z - x2.z);
+                p->depth = P->normal_depth[q].w;
+                p->resting = P->is_resting[q];
+                P->is_resting[q] = 1;
+                p->impulse = P->penetration_impulse[q];
+                p->split_impulse = 0.0f;
+                c->fp1 = V(c->fp1.x + p1.x, c->fp1.y + p1.y, c->fp1.z + p1.z);
+                c->fp2 = V(c->fp2.x + p2.x, c->fp2.y + p2.y, c->fp2.z + p2.z);
+                v3 dv = rel_vel(v1, w1, v2, w2, p->r1, p->r2);
+                v3 r1n = vcross(p->r1, p->normal), r2n = vcross(p->r2, p->normal);
+                p->i1 = m3v(c->I1, r1n);
+                p->i2 = m3v(c->I2, r2n);
+                float mp = c->im1 + c->im2 + vdot(vcross(p->i1, p->r1), p->normal) + vdot(vcross(p->i2, p->r2), p->normal);
+                p->inv_mass = mp > 0.0f ? 1.0f / mp : 0.0f;
+                p->restitution_bias = 0.0f;
+                float dvn = dv.x * p->normal.x + dv.y * p->normal.y + dv.z * p->normal.z;
+                float b1r = Cl->material[c1].y, b2r = Cl->material[c2].y;
+                float rest = (b1r > b2r) ? b1r : b2r;
+                if (dvn < -pr->restitution_velocity_threshold) p->restitution_bias = rest * dvn;
+                c->normal = V(c->normal.x + p->normal.x, c->normal.y + p->normal.y, c->normal.z + p->normal.z);
+                np++;
+            }
+            c->fp1 = vdivs(c->fp1, (float)c->nb);
+            c->fp2 = vdivs(c->fp2, (float)c->nb);
+            c->r1f = V(c->fp1.x - x1.x, c->fp1.y - x1.y, c->fp1.z - x1.z);
+            c->r2f = V(c->fp2.x - x2.x, c->fp2.y - x2.y, c->fp2.z - x2.z);
+            c->ofv1 = L4(M->friction_vector1[e]);
+            c->ofv2 = L4(M->friction_vector2[e]);
+            c->f1 = M->friction_impulse[e].x; c->f2 = M->friction_impulse[e].y; c->ftw = M->friction_impulse[e].z;
+            c->normal = vnormalize(c->normal);
+            v3 dvf = rel_vel(v1, w1, v2, w2, c->r1f, c->r2f);
+            /* computeFrictionVectors (:789-818) */
+            v3 nv = vmul(c->normal, vdot(dvf, c->normal));
+            v3 tv = V(dvf.x - nv.x, dvf.y - nv.y, dvf.z - nv.z);
+            float lt = vlen(tv);
+            c->fv1 = lt > MACHINE_EPSILON ? vdivs(tv, lt) : one_unit_orthogonal(c->normal);
+            c->fv2 = vcross(c->normal, c->fv1);
+            c->r1ct1 = vcross(c->r1f, c->fv1); c->r1ct2 = vcross(c->r1f, c->fv2);
+            c->r2ct1 = vcross(c->r2f, c->fv1); c->r2ct2 = vcross(c->r2f, c->fv2);
+            float f1m = c->im1 + c->im2 + vdot(vcross(m3v(c->I1, c->r1ct1), c->r1f), c->fv1) +
+                        vdot(vcross(m3v(c->I2, c->r2ct1), c->r2f), c->fv1);
+            float f2m = c->im1 + c->im2 + vdot(vcross(m3v(c->I1, c->r1ct2), c->r1f), c->fv2) +
+                        vdot(vcross(m3v(c->I2, c->r2ct2), c->r2f), c->fv2);
+            float twm = vdot(c->normal, m3v(c->I1, c->normal)) + vdot(c->normal, m3v(c->I2, c->normal));
+            c->inv_f1 = f1m > 0.0f ? 1.0f / f1m : 0.0f;
+            c->inv_f2 = f2m > 0.0f ? 1.0f / f2m : 0.0f;
+            c->inv_tw = twm > 0.0f ? 1.0f / twm : 0.0f;
+            nm++;
+        }
+    }
+
+    /* warmStart (:324-476) */
+    uint32_t pi_ = 0;
+    for (uint32_t k = 0; k < nm; k++) {
+        DynMan* c = &man[k];
+        const int b1 = c->b1, b2 = c->b2;
+        int any = 0;
+        for (int i = 0; i < c->nb; i++, pi_++) {
+            DynPt* p = &pt[pi_];
+            if (p->resting) {
+                any = 1;
+                v3 ip = V(p->normal.x * p->impulse, p->normal.y * p->impulse, p->normal.z * p->impulse);
+                cv[b1].x -= c->im1 * ip.x * c->lf1.x; cv[b1].y -= c->im1 * ip.y * c->lf1.y; cv[b1].z -= c->im1 * ip.z * c->lf1.z;
+                cw[b1].x -= p->i1.x * c->af1.x * p->impulse; cw[b1].y -= p->i1.y * c->af1.y * p->impulse;
+                cw[b1].z -= p->i1.z * c->af1.z * p->impulse;
+                cv[b2].x += c->im2 * ip.x * c->lf2.x; cv[b2].y += c->im2 * ip.y * c->lf2.y; cv[b2].z += c->im2 * ip.z * c->lf2.z;
+                cw[b2].x += p->i2.x * c->af2.x * p->impulse; cw[b2].y += p->i2.y * c->af2.y * p->impulse;
+                cw[b2].z += p->i2.z * c->af2.z * p->impulse;
+            } else {
+                p->impulse = 0.0f;
+            }
+        }
+        if (any) {
+            v3 ofi = V(c->f1 * c->ofv1.x + c->f2 * c->ofv2.x, c->f1 * c->ofv1.y + c->f2 * c->ofv2.y,
+                       c->f1 * c->ofv1.z + c->f2 * c->ofv2.z);
+            c->f1 = vdot(ofi, c->fv1);
+            c->f2 = vdot(ofi, c->fv2);
+            v3 a1 = V(-c->r1ct1.x * c->f1, -c->r1ct1.y * c->f1, -c->r1ct1.z * c->f1);
+            v3 l2 = V(c->fv1.x * c->f1, c->fv1.y * c->f1, c->fv1.z * c->f1);
+            v3 a2 = V(c->r2ct1.x * c->f1, c->r2ct1.y * c->f1, c->r2ct1.z * c->f1);
+            cv[b1] = lin_sub(cv[b1], c->im1, l2, c->lf1);
+            cw[b1] = vadd(cw[b1], vcmul(c->af1, m3v(c->I1, a1)));
+            cv[b2] = lin_add(cv[b2], c->im2, l2, c->lf2);
+            cw[b2] = vadd(cw[b2], vcmul(c->af2, m3v(c->I2, a2)));
+            a1 = V(-c->r1ct2.x * c->f2, -c->r1ct2.y * c->f2, -c->r1ct2.z * c->f2);
+            l2 = V(c->fv2.x * c->f2, c->fv2.y * c->f2, c->fv2.z * c->f2);
+            a2 = V(c->r2ct2.x * c->f2, c->r2ct2.y * c->f2, c->r2ct2.z * c->f2);
+            cv[b1] = lin_sub(cv[b1], c->im1, l2, c->lf1);
+            cw[b1] = vadd(cw[b1], vcmul(c->af1, m3v(c->I1, a1)));
+            cv[b2] = lin_add(cv[b2], c->im2, l2, c->lf2);
+            cw[b2] = vadd(cw[b2], vcmul(c->af2, m3v(c->I2, a2)));
+            a1 = V(-c->normal.x * c->ftw, -c->normal.y * c->ftw, -c->normal.z * c->ftw);
+            a2 = V(c->normal.x * c->ftw, c->normal.y * c->ftw, c->normal.z * c->ftw);
+            cw[b1] = vadd(cw[b1], vcmul(c->af1, m3v(c->I1, a1)));
+            cw[b2] = vadd(cw[b2], vcmul(c->af2, m3v(c->I2, a2)));
+            cw[b1] = vsub(cw[b1], vcmul(c->af1, m3v(c->I1, a2)));
+            cw[b2] = vadd(cw[b2], vcmul(c->af2, m3v(c->I2, a2)));
+        } else {
+            c->f1 = 0.0f; c->f2 = 0.0f; c->ftw = 0.0f;
+        }
+    }
+
+    /* solve (:479-759), velocity iterations (PhysicsWorld.cpp:333-339) */
+    const float beta = pr->split_impulse ? 0.2f : 0.2f;   /* BETA_SPLIT_IMPULSE : BETA (:43-44) */
+    const float SLOP = 0.01f;                             /* :45 */
+    for (int it = 0; it < pr->velocity_iterations; it++) {
+        uint32_t q = 0;
+        for (uint32_t k = 0; k < nm; k++) {
+            DynMan* c = &man[k];
+            const int b1 = c->b1, b2 = c->b2;
+            float sum = 0.0f;
+            for (int i = 0; i < c->nb; i++, q++) {
+                DynPt* p = &pt[q];
+                v3 dv = rel_vel(cv[b1], cw[b1], cv[b2], cw[b2], p->r1, p->r2);
+                float Jv = dv.x * p->normal.x + dv.y * p->normal.y + dv.z * p->normal.z;
+                float bias = 0.0f;
+                if (p->depth > SLOP) bias = -(beta / dt) * fmax_std(0.0f, p->depth - SLOP);
+                float b = bias + p->restitution_bias;
+                float dl = pr->split_impulse ? -(Jv + p->restitution_bias) * p->inv_mass : -(Jv + b) * p->inv_mass;
+                float lt = p->impulse;
+                p->impulse = fmax_std(p->impulse + dl, 0.0f);
+                dl = p->impulse - lt;
+                v3 li = V(p->normal.x * dl, p->normal.y * dl, p->normal.z * dl);
+                cv[b1].x -= c->im1 * li.x * c->lf1.x; cv[b1].y -= c->im1 * li.y * c->lf1.y; cv[b1].z -= c->im1 * li.z * c->lf1.z;
+                cw[b1].x -= p->i1.x * c->af1.x * dl; cw[b1].y -= p->i1.y * c->af1.y * dl; cw[b1].z -= p->i1.z * c->af1.z * dl;
+                cv[b2].x += c->im2 * li.x * c->lf2.x; cv[b2].y += c->im2 * li.y * c->lf2.y; cv[b2].z += c->im2 * li.z * c->lf2.z;
+                cw[b2].x += p->i2.x * c->af2.x * dl; cw[b2].y += p->i2.y * c->af2.y * dl; cw[b2].z += p->i2.z * c->af2.z * dl;
+                sum += p->impulse;
+                if (pr->split_impulse) {
+                    v3 dvs = rel_vel(sv[b1], sw[b1], sv[b2], sw[b2], p->r1, p->r2);
+                    float Jvs = dvs.x * p->normal.x + dvs.y * p->normal.y + dvs.z * p->normal.z;
+                    float dls = -(Jvs + bias) * p->inv_mass;
+                    float lts = p->split_impulse;
+                    p->split_impulse = fmax_std(p->split_impulse + dls, 0.0f);
+                    dls = p->split_impulse - lts;
+                    v3 ls = V(p->normal.x * dls, p->normal.y * dls, p->normal.z * dls);
+                    sv[b1].x -= c->im1 * ls.x * c->lf1.x; sv[b1].y -= c->im1 * ls.y * c->lf1.y; sv[b1].z -= c->im1 * ls.z * c->lf1.z;
+                    sw[b1].x -= p->i1.x * c->af1.x * dls; sw[b1].y -= p->i1.y * c->af1.y * dls; sw[b1].z -= p->i1.z * c->af1.z * dls;
+                    sv[b2].x += c->im2 * ls.x * c->lf2.x; sv[b2].y += c->im2 * ls.y * c->lf2.y; sv[b2].z += c->im2 * ls.z * c->lf2.z;
+                    sw[b2].x += p->i2.x * c->af2.x * dls; sw[b2].y += p->i2.y * c->af2.y * dls; sw[b2].z += p->i2.z * c->af2.z * dls;
+                }
+            }
+            /* friction 1 */
+            {
+                v3 dv = rel_vel(cv[b1], cw[b1], cv[b2], cw[b2], c->r1f, c->r2f);
+                float Jv = dv.x * c->fv1.x + dv.y * c->fv1.y + dv.z * c->fv1.z;
+                float dl = -Jv * c->inv_f1, lim = c->friction * sum, lt = c->f1;
+                c->f1 = fmax_std(-lim, fmin_std(c->f1 + dl, lim));
+                dl = c->f1 - lt;
+                v3 a1 = V(-c->r1ct1.x * dl, -c->r1ct1.y * dl, -c->r1ct1.z * dl);
+                v3 l2 = V(c->fv1.x * dl, c->fv1.y * dl, c->fv1.z * dl);
+                v3 a2 = V(c->r2ct1.x * dl, c->r2ct1.y * dl, c->r2ct1.z * dl);
+                cv[b1].x -= c->im1 * l2.x * c->lf1.x; cv[b1].y -= c->im1 * l2.y * c->lf1.y; cv[b1].z -= c->im1 * l2.z * c->lf1.z;
+                v3 av1 = vcmul(c->af1, m3v(c->I1, a1));
+                cw[b1].x += av1.x; cw[b1].y += av1.y; cw[b1].z += av1.z;
+                cv[b2].x += c->im2 * l2.x * c->lf2.x; cv[b2].y += c->im2 * l2.y * c->lf2.y; cv[b2].z += c->im2 * l2.z * c->lf2.z;
+                v3 av2 = vcmul(c->af2, m3v(c->I2, a2));
+                cw[b2].x += av2.x; cw[b2].y += av2.y; cw[b2].z += av2.z;
+            }
+            /* friction 2 */
+            {
+                v3 dv = rel_vel(cv[b1], cw[b1], cv[b2], cw[b2], c->r1f, c->r2f);
+                float Jv = dv.x * c->fv2.x + dv.y * c->fv2.y + dv.z * c->fv2.z;
+                float dl = -Jv * c->inv_f2, lim = c->friction * sum, lt = c->f2;
+                c->f2 = fmax_std(-lim, fmin_std(c->f2 + dl, lim));
+                dl = c->f2 - lt;
+                v3 a1 = V(-c->r1ct2.x * dl, -c->r1ct2.y * dl, -c->r1ct2.z * dl);
+                v3 l2 = V(c->fv2.x * dl, c->fv2.y * dl, c->fv2.z * dl);
+                v3 a2 = V(c->r2ct2.x * dl, c->r2ct2.y * dl, c->r2ct2.z * dl);
+                cv[b1].x -= c->im1 * l2.x * c->lf1.x; cv[b1].y -= c->im1 * l2.y * c->lf1.y; cv[b1].z -= c->im1 * l2.z * c->lf1.z;
+                v3 av1 = vcmul(c->af1, m3v(c->I1, a1));
+                cw[b1].x += av1.x; cw[b1].y += av1.y; cw[b1].z += av1.z;
+                cv[b2].x += c->im2 * l2.x * c->lf2.x; cv[b2].y += c->im2 * l2.y * c->lf2.y; cv[b2].z += c->im2 * l2.z * c->lf2.z;
+                v3 av2 = vcmul(c->af2, m3v(c->I2, a2));
+                cw[b2].x += av2.x; cw[b2].y += av2.y; cw[b2].z += av2.z;
+            }
+            /* twist */
+            {
+                v3 dw = vsub(cw[b2], cw[b1]);
+                float Jv = dw.x * c->normal.x + dw.y * c->normal.y + dw.z * c->normal.z;
+                float dl = -Jv * c->inv_tw, lim = c->friction * sum, lt = c->ftw;
+                c->ftw = fmax_std(-lim, fmin_std(c->ftw + dl, lim));
+                dl = c->ftw - lt;
+                v3 a2 = V(c->normal.x * dl, c->normal.y * dl, c->normal.z * dl);
+                v3 av1 = vcmul(c->af1, m3v(c->I1, a2));
+                cw[b1].x -= av1.x; cw[b1].y -= av1.y; cw[b1].z -= av1.z;
+                v3 av2 = vcmul(c->af2, m3v(c->I2, a2));
+                cw[b2].x += av2.x; cw[b2].y += av2.y; cw[b2].z += av2.z;
+            }
+        }
+    }
+
+    /* storeImpulses (:763-785) */
+    {
+        uint32_t q = 0;
+        for (uint32_t k = 0; k < nm; k++) {
+            DynMan* c = &man[k];
+            for (int i = 0; i < c->nb; i++, q++) P->penetration_impulse[pt[q].ext] = pt[q].impulse;
+            rp3dg_float4 fi; fi.x = c->f1; fi.y = c->f2; fi.z = c->ftw; fi.w = 0.0f;
+            M->friction_impulse[c->ext] = fi;
+            M->friction_vector1[c->ext] = S4(c->fv1);
+            M->friction_vector2[c->ext] = S4(c->fv2);
+        }
+    }
+
+    /* integrateRigidBodiesPositions + updateBodiesState (DynamicsSystem.cpp:44-110) */
+    const float f = pr->split_impulse ? 1.0f : 0.0f;
+    quat* co = (quat*)calloc(ne ? ne : 1, sizeof(quat));
+    v3* cp = (v3*)calloc(ne ? ne : 1, sizeof(v3));
+    for (uint32_t i = 0; i < ne; i++) {
+        v3 nl = vadd(cv[i], vmul(sv[i], f)), na = vadd(cw[i], vmul(sw[i], f));
+        rp3dg_float4 o = B->orientation[i];
+        quat q = Q(o.x, o.y, o.z, o.w);
+        cp[i] = vadd(L4(B->com_world[i]), vmul(nl, dt));
+        quat d = qmul(Q(na.x, na.y, na.z, 0.0f), q);
+        d = Q(0.5f * d.x, 0.5f * d.y, 0.5f * d.z, 0.5f * d.w);
+        d = Q(dt * d.x, dt * d.y, dt * d.z, dt * d.w);
+        co[i] = Q(q.x + d.x, q.y + d.y, q.z + d.z, q.w + d.w);
+    }
+    for (uint32_t i = 0; i < ne; i++) {
+        B->linear_velocity[i] = S4(cv[i]);
+        B->angular_velocity[i] = S4(cw[i]);
+        B->com_world[i] = S4(cp[i]);
+        quat q = co[i];
+        float l = sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+        rp3dg_float4 o; o.x = q.x / l; o.y = q.y / l; o.z = q.z / l; o.w = q.w / l;
+        B->orientation[i] = o;
+    }
+    for (uint32_t i = 0; i < ne; i++) {
+        rp3dg_float4 o = B->orientation[i];
+        B->position[i] = S4(vsub(cp[i], qrot(Q(o.x, o.y, o.z, o.w), L4(B->com_local[i]))));
+    }
+    for (uint32_t i = 0; i < Cl->n_enabled; i++) {
+        int b = Cl->body[i];
+        rp3dg_float4 bo = B->orientation[b], lo = Cl->local_orientation[i];
+        xform t = xmul(X(L4(B->position[b]), Q(bo.x, bo.y, bo.z, bo.w)), X(L4(Cl->local_position[i]), Q(lo.x, lo.y, lo.z, lo.w)));
+        Cl->world_position[i] = S4(t.p);
+        rp3dg_float4 wq; wq.x = t.q.x; wq.y = t.q.y; wq.z = t.q.z; wq.w = t.q.w;
+        Cl->world_orientation[i] = wq;
+    }
+    free(co); free(cp);
+    free(cv); free(cw); free(sv); free(sw); free(man); free(pt);
+    return 0;
+}

@@ -35,6 +35,13 @@ int rp3do_narrowphase(int algorithm, const rp3dg_shape* shapes, uint32_t nb_shap
 /* Convex-pair manifold reduction (<= 4 points, de-duplicated), in place. */
 int rp3do_reduce_contacts(const rp3dg_pair_batch* pairs, const rp3dg_contact_batch* contacts, uint8_t* kept);
 
+/* Dynamics stage of a world step, same semantics as rp3dg_dynamics_step_host
+ * except that the velocities of read-only bodies receive the solver's
+ * signed-zero updates exactly as the reference's arrays do. */
+int rp3do_dynamics_step(const rp3dg_dynamics_params* params, const rp3dg_bodies* bodies,
+                        const rp3dg_colliders* colliders, const rp3dg_manifolds* manifolds,
+                        const rp3dg_points* points, const rp3dg_islands* islands);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,6 +18,7 @@
 
 #include "../../include/rp3dg.h"
 #include "contacts_launch.h"
+#include "dynamics_launch.h"
 #include "mlp_launch.h"
 #include "np_launch.h"
 #include "rp3dg_internal.h"
@@ -201,6 +202,12 @@ struct rp3dg_ctx {
     int mlp_step = 0;
     bool mlp_ready = false;
     bool learned_axis = false;
+    // dynamics stage: per-body velocity scratch and solver records
+    void* d_dyn = nullptr;
+    size_t cap_dyn = 0;
+    // staging buffers for rp3dg_dynamics_step_host
+    void* d_dyn_stage = nullptr;
+    size_t cap_dyn_stage = 0;
 };
 
 namespace {
@@ -324,6 +331,8 @@ void rp3dg_destroy(rp3dg_ctx* ctx) {
     cudaFree(ctx->d_mlp);
     cudaFree(ctx->d_mlp_scratch);
     cudaFree(ctx->d_proposals);
+    cudaFree(ctx->d_dyn);
+    cudaFree(ctx->d_dyn_stage);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -865,3 +874,185 @@ int rp3dg_learned_axis_stats(rp3dg_ctx* ctx, uint64_t* tested, uint64_t* confirm
 }
 
 }  // extern "C"
+
+// ---- dynamics stage ------------------------------------------------------
+
+namespace {
+
+int grow(rp3dg_ctx* ctx, void** buf, size_t* cap, size_t need, const char* what) {
+    if (need <= *cap) return 0;
+    cudaFree(*buf);
+    *buf = nullptr;
+    cudaError_t e = cudaMalloc(buf, need);
+    if (e != cudaSuccess) { *cap = 0; *buf = nullptr; return cuda_fail(ctx, e, what); }
+    *cap = need;
+    return 0;
+}
+
+int check_dynamics(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b, const rp3dg_colliders* c,
+                   const rp3dg_manifolds* m, const rp3dg_points* p, const rp3dg_islands* is) {
+    if (!ctx || !pr || !b || !c || !m || !p || !is) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (b->n_enabled > b->n || c->n_enabled > c->n) return fail(ctx, RP3DG_EINVAL, "n_enabled > n");
+    if (!(pr->dt > 0.0f) || pr->velocity_iterations < 0) return fail(ctx, RP3DG_EINVAL, "bad dt or iterations");
+    if (b->n && (!b->position || !b->orientation || !b->com_world || !b->com_local || !b->linear_velocity ||
+                 !b->angular_velocity || !b->force || !b->torque || !b->inv_inertia_local || !b->inv_inertia_world ||
+                 !b->mass || !b->linear_lock || !b->angular_lock || !b->gravity))
+        return fail(ctx, RP3DG_EINVAL, "null body array");
+    if (c->n && (!c->body || !c->local_position || !c->local_orientation || !c->world_position ||
+                 !c->world_orientation || !c->material))
+        return fail(ctx, RP3DG_EINVAL, "null collider array");
+    if (m->n && (!m->ids || !m->point_start || !m->nb_points || !m->friction_vector1 || !m->friction_vector2 ||
+                 !m->friction_impulse))
+        return fail(ctx, RP3DG_EINVAL, "null manifold array");
+    if (p->n && (!p->normal_depth || !p->local1 || !p->local2 || !p->penetration_impulse || !p->is_resting))
+        return fail(ctx, RP3DG_EINVAL, "null point array");
+    if (is->n && (!is->manifold_start || !is->manifold_count)) return fail(ctx, RP3DG_EINVAL, "null island array");
+    if (m->n && (!b->n || !c->n || !p->n)) return fail(ctx, RP3DG_EINVAL, "manifolds without bodies, colliders or points");
+    return 0;
+}
+
+}  // namespace
+
+int rp3dg_dynamics_step_device(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
+                               const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
+                               const rp3dg_islands* is) {
+    int rc = check_dynamics(ctx, pr, b, c, m, p, is);
+    if (rc) return rc;
+    const void* f16[] = {b->position, b->orientation, b->com_world, b->com_local, b->linear_velocity,
+                         b->angular_velocity, b->force, b->torque, b->inv_inertia_local, b->inv_inertia_world,
+                         b->mass, b->linear_lock, b->angular_lock, c->local_position, c->local_orientation,
+                         c->world_position, c->world_orientation, c->material, m->ids, m->friction_vector1,
+                         m->friction_vector2, m->friction_impulse, p->normal_depth, p->local1, p->local2};
+    for (const void* q : f16)
+        if (!aligned(q, 16)) return fail(ctx, RP3DG_EINVAL, "misaligned device array (float4 / int4 arrays need 16 bytes)");
+    const void* f4[] = {c->body, m->point_start, p->penetration_impulse, is->manifold_start, is->manifold_count};
+    for (const void* q : f4)
+        if (!aligned(q, 4)) return fail(ctx, RP3DG_EINVAL, "misaligned device array (32-bit arrays need 4 bytes)");
+    cudaSetDevice(ctx->device);
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t vel_bytes = al(size_t(b->n) * 16);
+    const size_t off_m = 4 * vel_bytes;
+    const size_t off_p = off_m + al(size_t(m->n) * sizeof(rp3dg::DynManifoldRec));
+    const size_t need = off_p + al(size_t(p->n) * sizeof(rp3dg::DynPointRec)) + 256;
+    rc = grow(ctx, &ctx->d_dyn, &ctx->cap_dyn, need, "cudaMalloc(dynamics scratch)");
+    if (rc) return rc;
+    char* s = static_cast<char*>(ctx->d_dyn);
+    rp3dg::DynArgs a;
+    a.dt = pr->dt; a.gx = pr->gravity[0]; a.gy = pr->gravity[1]; a.gz = pr->gravity[2];
+    a.gravity_enabled = pr->gravity_enabled; a.iterations = pr->velocity_iterations; a.split = pr->split_impulse ? 1 : 0;
+    a.restitution_threshold = pr->restitution_velocity_threshold;
+    a.nb = b->n; a.nb_enabled = b->n_enabled;
+    a.position = reinterpret_cast<float4*>(b->position);
+    a.orientation = reinterpret_cast<float4*>(b->orientation);
+    a.com_world = reinterpret_cast<float4*>(b->com_world);
+    a.com_local = reinterpret_cast<const float4*>(b->com_local);
+    a.lin_vel = reinterpret_cast<float4*>(b->linear_velocity);
+    a.ang_vel = reinterpret_cast<float4*>(b->angular_velocity);
+    a.force = reinterpret_cast<const float4*>(b->force);
+    a.torque = reinterpret_cast<const float4*>(b->torque);
+    a.iil = reinterpret_cast<const float4*>(b->inv_inertia_local);
+    a.iiw = reinterpret_cast<float4*>(b->inv_inertia_world);
+    a.mass = reinterpret_cast<const float4*>(b->mass);
+    a.llock = reinterpret_cast<const float4*>(b->linear_lock);
+    a.alock = reinterpret_cast<const float4*>(b->angular_lock);
+    a.gravity = b->gravity;
+    a.nc = c->n; a.nc_enabled = c->n_enabled;
+    a.c_body = c->body;
+    a.c_lpos = reinterpret_cast<const float4*>(c->local_position);
+    a.c_lori = reinterpret_cast<const float4*>(c->local_orientation);
+    a.c_wpos = reinterpret_cast<float4*>(c->world_position);
+    a.c_wori = reinterpret_cast<float4*>(c->world_orientation);
+    a.c_mat = reinterpret_cast<const float4*>(c->material);
+    a.nm = m->n; a.np = p->n; a.ni = is->n;
+    a.m_ids = reinterpret_cast<const int4*>(m->ids);
+    a.m_pstart = m->point_start;
+    a.m_npts = m->nb_points;
+    a.m_fv1 = reinterpret_cast<float4*>(m->friction_vector1);
+    a.m_fv2 = reinterpret_cast<float4*>(m->friction_vector2);
+    a.m_fimp = reinterpret_cast<float4*>(m->friction_impulse);
+    a.p_nd = reinterpret_cast<const float4*>(p->normal_depth);
+    a.p_l1 = reinterpret_cast<const float4*>(p->local1);
+    a.p_l2 = reinterpret_cast<const float4*>(p->local2);
+    a.p_impulse = p->penetration_impulse;
+    a.p_resting = p->is_resting;
+    a.i_start = is->manifold_start;
+    a.i_count = is->manifold_count;
+    a.error = ctx->d_error;
+    a.cv = reinterpret_cast<float4*>(s);
+    a.cw = reinterpret_cast<float4*>(s + vel_bytes);
+    a.sv = reinterpret_cast<float4*>(s + 2 * vel_bytes);
+    a.sw = reinterpret_cast<float4*>(s + 3 * vel_bytes);
+    a.mrec = reinterpret_cast<rp3dg::DynManifoldRec*>(s + off_m);
+    a.prec = reinterpret_cast<rp3dg::DynPointRec*>(s + off_p);
+    cudaError_t e = rp3dg::launch_dynamics(a, ctx->stream, &ctx->launches);
+    return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "dynamics launch");
+}
+
+int rp3dg_dynamics_step_host(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
+                             const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
+                             const rp3dg_islands* is) {
+    int rc = check_dynamics(ctx, pr, b, c, m, p, is);
+    if (rc) return rc;
+    // every array goes to one staging buffer (256-byte aligned slots); the
+    // ones the stage writes come back
+    struct Arr { const void* host; void* out; size_t bytes; size_t off; };
+    std::vector<Arr> arrs;
+    size_t off = 0;
+    auto add = [&](const void* host, size_t bytes, bool written) -> size_t {
+        Arr r{host, written ? const_cast<void*>(host) : nullptr, host ? bytes : 0, off};
+        off += (r.bytes + 255) & ~size_t(255);
+        arrs.push_back(r);
+        return arrs.size() - 1;
+    };
+    const size_t nb = b->n, nc = c->n, nm = m->n, np = p->n, ni = is->n;
+    const size_t i_pos = add(b->position, nb * 16, true), i_ori = add(b->orientation, nb * 16, true);
+    const size_t i_comw = add(b->com_world, nb * 16, true), i_coml = add(b->com_local, nb * 16, false);
+    const size_t i_lv = add(b->linear_velocity, nb * 16, true), i_av = add(b->angular_velocity, nb * 16, true);
+    const size_t i_f = add(b->force, nb * 16, false), i_t = add(b->torque, nb * 16, false);
+    const size_t i_iil = add(b->inv_inertia_local, nb * 16, false), i_iiw = add(b->inv_inertia_world, nb * 48, true);
+    const size_t i_mass = add(b->mass, nb * 16, false), i_ll = add(b->linear_lock, nb * 16, false);
+    const size_t i_al = add(b->angular_lock, nb * 16, false), i_g = add(b->gravity, nb, false);
+    const size_t i_cb = add(c->body, nc * 4, false), i_clp = add(c->local_position, nc * 16, false);
+    const size_t i_clo = add(c->local_orientation, nc * 16, false), i_cwp = add(c->world_position, nc * 16, true);
+    const size_t i_cwo = add(c->world_orientation, nc * 16, true), i_cm = add(c->material, nc * 16, false);
+    const size_t i_mid = add(m->ids, nm * 16, false), i_mps = add(m->point_start, nm * 4, false);
+    const size_t i_mnp = add(m->nb_points, nm, false), i_fv1 = add(m->friction_vector1, nm * 16, true);
+    const size_t i_fv2 = add(m->friction_vector2, nm * 16, true), i_fi = add(m->friction_impulse, nm * 16, true);
+    const size_t i_pnd = add(p->normal_depth, np * 16, false), i_pl1 = add(p->local1, np * 16, false);
+    const size_t i_pl2 = add(p->local2, np * 16, false), i_pi = add(p->penetration_impulse, np * 4, true);
+    const size_t i_pr = add(p->is_resting, np, true);
+    const size_t i_is = add(is->manifold_start, ni * 4, false), i_ic = add(is->manifold_count, ni * 4, false);
+    cudaSetDevice(ctx->device);
+    rc = grow(ctx, &ctx->d_dyn_stage, &ctx->cap_dyn_stage, off + 256, "cudaMalloc(dynamics staging)");
+    if (rc) return rc;
+    char* d = static_cast<char*>(ctx->d_dyn_stage);
+    cudaError_t e = cudaSuccess;
+    for (const Arr& r : arrs)
+        if (e == cudaSuccess && r.bytes) e = cudaMemcpyAsync(d + r.off, r.host, r.bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "upload dynamics arrays");
+    auto D = [&](size_t i) { return arrs[i].bytes ? static_cast<void*>(d + arrs[i].off) : nullptr; };
+    auto F = [&](size_t i) { return static_cast<rp3dg_float4*>(D(i)); };
+    rp3dg_bodies db = *b;
+    db.position = F(i_pos); db.orientation = F(i_ori); db.com_world = F(i_comw); db.com_local = F(i_coml);
+    db.linear_velocity = F(i_lv); db.angular_velocity = F(i_av); db.force = F(i_f); db.torque = F(i_t);
+    db.inv_inertia_local = F(i_iil); db.inv_inertia_world = F(i_iiw); db.mass = F(i_mass);
+    db.linear_lock = F(i_ll); db.angular_lock = F(i_al); db.gravity = static_cast<const uint8_t*>(D(i_g));
+    rp3dg_colliders dc = *c;
+    dc.body = static_cast<const int32_t*>(D(i_cb)); dc.local_position = F(i_clp); dc.local_orientation = F(i_clo);
+    dc.world_position = F(i_cwp); dc.world_orientation = F(i_cwo); dc.material = F(i_cm);
+    rp3dg_manifolds dm = *m;
+    dm.ids = static_cast<const int32_t*>(D(i_mid)); dm.point_start = static_cast<const uint32_t*>(D(i_mps));
+    dm.nb_points = static_cast<const uint8_t*>(D(i_mnp)); dm.friction_vector1 = F(i_fv1);
+    dm.friction_vector2 = F(i_fv2); dm.friction_impulse = F(i_fi);
+    rp3dg_points dp = *p;
+    dp.normal_depth = F(i_pnd); dp.local1 = F(i_pl1); dp.local2 = F(i_pl2);
+    dp.penetration_impulse = static_cast<float*>(D(i_pi)); dp.is_resting = static_cast<uint8_t*>(D(i_pr));
+    rp3dg_islands di = *is;
+    di.manifold_start = static_cast<const uint32_t*>(D(i_is)); di.manifold_count = static_cast<const uint32_t*>(D(i_ic));
+    rc = rp3dg_dynamics_step_device(ctx, pr, &db, &dc, &dm, &dp, &di);
+    if (rc) return rc;
+    for (const Arr& r : arrs)
+        if (e == cudaSuccess && r.out && r.bytes) e = cudaMemcpyAsync(r.out, d + r.off, r.bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "dynamics (host arrays)");
+}

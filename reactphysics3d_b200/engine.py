@@ -67,6 +67,10 @@ def load_library(path=LIB_PATH):
     L.rp3dg_reduce_contacts_device.argtypes = [P, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), P]
     L.rp3dg_narrowphase_manifolds_host.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch),
                                                    C.c_int, P]
+    from . import dynamics as DY
+    for fn in ("rp3dg_dynamics_step_host", "rp3dg_dynamics_step_device"):
+        getattr(L, fn).argtypes = [P, C.POINTER(DY.Params), C.POINTER(DY.Bodies), C.POINTER(DY.Colliders),
+                                   C.POINTER(DY.Manifolds), C.POINTER(DY.Points), C.POINTER(DY.Islands)]
     L.rp3dg_axis_mlp_init.argtypes = [P, C.c_uint64]
     L.rp3dg_axis_mlp_get_params.argtypes = [P, P]
     L.rp3dg_axis_mlp_set_params.argtypes = [P, P]
@@ -245,6 +249,22 @@ class Context:
         self._check(self.lib.rp3dg_narrowphase_manifolds_host(self.h, algo, C.byref(pb), C.byref(cb), int(clip),
                                                               None if kept is None else kept.ctypes.data))
         return out, kept
+
+    def dynamics_step(self, params, world):
+        """One dynamics stage (inertia, velocities, contact solver, positions,
+        state) on a reactphysics3d_b200.dynamics.DynWorld, in place: host
+        arrays through rp3dg_dynamics_step_host, CUDA tensors through
+        rp3dg_dynamics_step_device (asynchronous)."""
+        b, c, m, p, i = world.structs()
+        if world.device is None:
+            fn = self.lib.rp3dg_dynamics_step_host
+        else:
+            fn = self.lib.rp3dg_dynamics_step_device
+            self.order_in()
+        self._check(fn(self.h, C.byref(params), C.byref(b), C.byref(c), C.byref(m), C.byref(p), C.byref(i)))
+        if world.device is not None:
+            self.order_out()
+        return world
 
     def reduce_contacts_device(self, pairs, contacts, kept=None):
         """Convex-pair manifold reduction in place on DeviceContacts; kept is an

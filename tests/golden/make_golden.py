@@ -24,7 +24,16 @@ Writes:
                    removeDuplicatedContactPointsInManifold result ("red_"
                    arrays and the kept-slot table)
 
-`python tests/golden/make_golden.py manifold` rewrites np_manifold.npz only.
+  np_dynamics.npz  dynamics stage of a world step: for seeded reference
+                   worlds (oracle/ref_world.cpp: boxes, or boxes, spheres and
+                   capsules with random materials, dampings, lock factors,
+                   forces and kinematic bodies, on a static ground), the
+                   reference's own inputs and outputs of one step's
+                   inertia / velocity / contact-solver / position / state
+                   phases ("<case>/in_*", "<case>/out_*", "<case>/params")
+
+`python tests/golden/make_golden.py manifold` (or `dynamics`) rewrites that
+fixture only.
 """
 import json
 import os
@@ -145,7 +154,30 @@ def synthetic_manifolds(rng, n=512):
     return pairs, c
 
 
-def main(parts=("scene", "manifold")):
+# (kind, seed, steps before the captured one, grid nx, ny, nz)
+DYNAMICS_CASES = [(0, 1, 60, 4, 3, 4), (1, 3, 150, 4, 3, 4), (1, 5, 300, 4, 3, 4), (0, 6, 200, 8, 4, 8),
+                  (1, 4, 40, 4, 3, 4)]
+
+
+def dynamics_fixture():
+    d = {}
+    for kind, seed, steps, nx, ny, nz in DYNAMICS_CASES:
+        w = reflib.RefWorld(kind=kind, seed=seed, nx=nx, ny=ny, nz=nz)
+        w.step(n=steps)
+        w.apply_forces(seed + 1)
+        cap = w.capture()
+        name = f"k{kind}_s{seed}_t{steps}"
+        for k, v in cap.items():
+            d[name + "/" + k] = v
+        print(name, "bodies", len(cap["in_body_mass"]), "manifolds", len(cap["in_manifold_ids"]),
+              "points", len(cap["in_point_normal_depth"]), "islands", len(cap["in_island_manifold_start"]))
+    np.savez_compressed(os.path.join(HERE, "np_dynamics.npz"), **d)
+
+
+def main(parts=("scene", "manifold", "dynamics")):
+    if parts == ("dynamics",):
+        dynamics_fixture()
+        return
     ref = reflib.RefEngine("f32")
     verts, faces = ref.quickhull(scenes.icosphere42_points())
     if "scene" not in parts:
@@ -189,7 +221,9 @@ def main(parts=("scene", "manifold")):
     np.savez_compressed(os.path.join(HERE, "np_edge.npz"), **e)
     if "manifold" in parts:
         manifold_fixture(ref, verts, faces)
+    if "dynamics" in parts:
+        dynamics_fixture()
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("scene", "manifold"))
+    main(tuple(sys.argv[1:]) or ("scene", "manifold", "dynamics"))

@@ -206,3 +206,57 @@ def copy_contacts(c):
     for f in ("is_colliding", "nb_contacts", "normal_depth", "local1", "local2"):
         getattr(d, f)[...] = getattr(c, f)
     return d
+
+
+# dtype of each captured dynamics field of oracle/ref_world.cpp, by suffix
+_WORLD_DTYPES = {"body_gravity": np.uint8, "collider_body": np.int32, "manifold_ids": np.int32,
+                 "manifold_point_start": np.uint32, "manifold_nb_points": np.uint8, "manifold_source": np.uint32,
+                 "point_is_resting": np.uint8, "island_manifold_start": np.uint32,
+                 "island_manifold_count": np.uint32, "body_nb_enabled": np.uint32,
+                 "collider_nb_enabled": np.uint32}
+_WORLD_SHAPES = {"manifold_ids": (-1, 4), "point_penetration_impulse": (-1,), "body_inv_inertia_world": (-1, 3, 4),
+                 "body_split_velocity": (-1, 2, 4)}
+
+
+class RefWorld:
+    """A reference world (oracle/ref_world.cpp) stepped by the reference; one
+    step's dynamics stage can be captured as numpy arrays."""
+
+    def __init__(self, kind=1, seed=1, nx=4, ny=3, nz=4, spacing=1.6, variety=True, prec="f32"):
+        self.lib = C.CDLL(REF_LIB[prec])
+        L = self.lib
+        L.ref_world_create.argtypes = [C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int]
+        L.ref_world_apply_forces.argtypes = [C.c_int, C.c_uint64]
+        L.ref_world_step.argtypes = [C.c_int, C.c_float, C.c_int]
+        L.ref_world_capture.argtypes = [C.c_int, C.c_float]
+        L.ref_world_field_size.argtypes = [C.c_int, C.c_char_p]
+        L.ref_world_field_size.restype = C.c_long
+        L.ref_world_field.argtypes = [C.c_int, C.c_char_p, C.c_void_p]
+        L.ref_world_field_names.argtypes = [C.c_int, C.c_char_p, C.c_int]
+        self.id = L.ref_world_create(kind, seed, nx, ny, nz, spacing, int(variety))
+
+    def step(self, dt=1.0 / 60.0, n=1):
+        self.lib.ref_world_step(self.id, dt, n)
+
+    def apply_forces(self, seed):
+        self.lib.ref_world_apply_forces(self.id, seed)
+
+    def capture(self, dt=1.0 / 60.0):
+        """One step, phase by phase; returns {name: array} of the dynamics
+        stage's inputs (in_*), outputs (out_*) and params."""
+        assert self.lib.ref_world_capture(self.id, dt) == 0
+        buf = C.create_string_buffer(1 << 16)
+        assert self.lib.ref_world_field_names(self.id, buf, len(buf)) == 0
+        out = {}
+        for name in buf.value.decode().split():
+            size = self.lib.ref_world_field_size(self.id, name.encode())
+            suffix = name.split("_", 1)[1] if name.startswith(("in_", "out_")) else name
+            dt_ = _WORLD_DTYPES.get(suffix, np.float32)
+            a = np.zeros(size // np.dtype(dt_).itemsize, dt_)
+            assert self.lib.ref_world_field(self.id, name.encode(), a.ctypes.data) == 0
+            if suffix in _WORLD_SHAPES:
+                a = a.reshape(_WORLD_SHAPES[suffix])
+            elif dt_ == np.float32 and suffix != "params":
+                a = a.reshape(-1, 4)
+            out[name] = a
+        return out
