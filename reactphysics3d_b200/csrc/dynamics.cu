@@ -126,50 +126,59 @@ __global__ void __launch_bounds__(128) dyn_bodies_pre(const DynArgs a) {
     a.cw[i] = F4(cw);
 }
 
-RD void load_rows(const float4* rows, float* I) {
-    const float4 r0 = rows[0], r1 = rows[1], r2 = rows[2];
-    I[0] = r0.x; I[1] = r0.y; I[2] = r0.z;
-    I[3] = r1.x; I[4] = r1.y; I[5] = r1.z;
-    I[6] = r2.x; I[7] = r2.y; I[8] = r2.z;
-}
-
 RD bool is_fixed(const DynArgs& a, int32_t b) {
     if (uint32_t(b) >= a.nb_enabled) return true;
     const float4 il = a.iil[b];
     return a.mass[b].y == 0.0f && il.x == 0.0f && il.y == 0.0f && il.z == 0.0f;
 }
 
+RD float4 F4w(v3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
+
 // ---- kernel 2: ContactSolverSystem::initializeForIsland per manifold ------
-// (ContactSolverSystem.cpp:116-318)
+// (ContactSolverSystem.cpp:116-318).  Writes the manifold's solver record and
+// its points' records (layouts in dynamics_launch.h).
 __global__ void __launch_bounds__(128) dyn_manifold_init(const DynArgs a) {
     const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= a.nm) return;
-    DynManifoldRec& c = a.mrec[m];
+    float4* __restrict__ q = a.mrec[m].q;
     const int4 id = a.m_ids[m];
     const int32_t b1 = id.x, b2 = id.y;
     const uint32_t nb = a.m_npts[m], ps = a.m_pstart[m];
     if (uint32_t(b1) >= a.nb || uint32_t(b2) >= a.nb || b1 == b2 || uint32_t(id.z) >= a.nc ||
         uint32_t(id.w) >= a.nc || nb == 0 || nb > 4 || ps > a.np || nb > a.np - ps) {
         atomicOr(a.error, 4u);
-        c.b1 = 0; c.b2 = 0; c.nb = 0; c.pstart = 0; c.fixed_mask = 3.0f;  // solver skips it
+        q[DQ_IDS] = make_float4(__int_as_float(0), __int_as_float(0), __int_as_float(0), __int_as_float(0));
+        q[DQ_MASS] = make_float4(0.0f, 0.0f, 0.0f, 3.0f);  // no points: every pass skips it
         return;
     }
-    c.b1 = b1; c.b2 = b2; c.nb = int32_t(nb); c.pstart = int32_t(ps);
+    q[DQ_IDS] = make_float4(__int_as_float(b1), __int_as_float(b2), __int_as_float(int32_t(nb)), __int_as_float(int32_t(ps)));
     const v3 x1 = L3(a.com_world[b1]), x2 = L3(a.com_world[b2]);
-    load_rows(a.iiw + 3 * b1, c.I1);
-    load_rows(a.iiw + 3 * b2, c.I2);
-    c.im1 = a.mass[b1].y;
-    c.im2 = a.mass[b2].y;
-    S3(c.lf1, L3(a.llock[b1])); S3(c.lf2, L3(a.llock[b2]));
-    S3(c.alf1, L3(a.alock[b1])); S3(c.alf2, L3(a.alock[b2]));
-    c.fixed_mask = float((is_fixed(a, b1) ? 1 : 0) | (is_fixed(a, b2) ? 2 : 0));
+    float I1[9], I2[9];
+    {
+        const float4 r0 = a.iiw[3 * b1], r1 = a.iiw[3 * b1 + 1], r2 = a.iiw[3 * b1 + 2];
+        I1[0] = r0.x; I1[1] = r0.y; I1[2] = r0.z; I1[3] = r1.x; I1[4] = r1.y; I1[5] = r1.z;
+        I1[6] = r2.x; I1[7] = r2.y; I1[8] = r2.z;
+        q[DQ_I1 + 0] = r0; q[DQ_I1 + 1] = r1; q[DQ_I1 + 2] = r2;
+    }
+    {
+        const float4 r0 = a.iiw[3 * b2], r1 = a.iiw[3 * b2 + 1], r2 = a.iiw[3 * b2 + 2];
+        I2[0] = r0.x; I2[1] = r0.y; I2[2] = r0.z; I2[3] = r1.x; I2[4] = r1.y; I2[5] = r1.z;
+        I2[6] = r2.x; I2[7] = r2.y; I2[8] = r2.z;
+        q[DQ_I2 + 0] = r0; q[DQ_I2 + 1] = r1; q[DQ_I2 + 2] = r2;
+    }
+    const float im1 = a.mass[b1].y, im2 = a.mass[b2].y;
     const float4 mat1 = a.c_mat[id.z], mat2 = a.c_mat[id.w];
-    c.friction = mat1.x * mat2.x;                          // computeMixedFrictionCoefficient
-    const float restitution = (mat1.y > mat2.y) ? mat1.y : mat2.y;  // computeMixedRestitutionFactor
+    const float friction = mat1.x * mat2.x;                          // computeMixedFrictionCoefficient
+    const float restitution = (mat1.y > mat2.y) ? mat1.y : mat2.y;   // computeMixedRestitutionFactor
+    const float fixed = float((is_fixed(a, b1) ? 1 : 0) | (is_fixed(a, b2) ? 2 : 0));
+    q[DQ_MASS] = make_float4(im1, im2, friction, fixed);
+    q[DQ_LF1] = a.llock[b1]; q[DQ_LF2] = a.llock[b2];
+    q[DQ_AF1] = a.alock[b1]; q[DQ_AF2] = a.alock[b2];
     const v3 v1 = L3(a.lin_vel[b1]), w1 = L3(a.ang_vel[b1]);
     const v3 v2 = L3(a.lin_vel[b2]), w2 = L3(a.ang_vel[b2]);
-    const xform t1 = X(L3(a.c_wpos[id.z]), Q(a.c_wori[id.z].x, a.c_wori[id.z].y, a.c_wori[id.z].z, a.c_wori[id.z].w));
-    const xform t2 = X(L3(a.c_wpos[id.w]), Q(a.c_wori[id.w].x, a.c_wori[id.w].y, a.c_wori[id.w].z, a.c_wori[id.w].w));
+    const float4 o1 = a.c_wori[id.z], o2 = a.c_wori[id.w];
+    const xform t1 = X(L3(a.c_wpos[id.z]), Q(o1.x, o1.y, o1.z, o1.w));
+    const xform t2 = X(L3(a.c_wpos[id.w]), Q(o2.x, o2.y, o2.z, o2.w));
     v3 fp1 = V(0.0f, 0.0f, 0.0f), fp2 = V(0.0f, 0.0f, 0.0f), nsum = V(0.0f, 0.0f, 0.0f);
     for (uint32_t k = 0; k < nb; k++) {
         const uint32_t p = ps + k;
@@ -180,23 +189,24 @@ __global__ void __launch_bounds__(128) dyn_manifold_init(const DynArgs a) {
         const v3 p2 = xapply(t2, L3(a.p_l2[p]));
         const v3 r1 = V(p1.x - x1.x, p1.y - x1.y, p1.z - x1.z);
         const v3 r2 = V(p2.x - x2.x, p2.y - x2.y, p2.z - x2.z);
-        S3(r.r1, r1); S3(r.r2, r2); S3(r.normal, n);
-        r.depth = nd.w;
-        r.resting = a.p_resting[p];
+        const uint8_t resting = a.p_resting[p];
         a.p_resting[p] = 1;
-        r.impulse = a.p_impulse[p];
-        r.split_impulse = 0.0f;
         fp1 = V(fp1.x + p1.x, fp1.y + p1.y, fp1.z + p1.z);
         fp2 = V(fp2.x + p2.x, fp2.y + p2.y, fp2.z + p2.z);
         const v3 dv = rel_velocity(v1, w1, v2, w2, r1, r2);
         const v3 r1n = vcross(r1, n), r2n = vcross(r2, n);
-        const v3 i1 = mv(c.I1, r1n), i2 = mv(c.I2, r2n);
-        S3(r.i1, i1); S3(r.i2, i2);
-        const float mp = c.im1 + c.im2 + vdot(vcross(i1, r1), n) + vdot(vcross(i2, r2), n);
-        r.inv_mass = mp > 0.0f ? 1.0f / mp : 0.0f;
-        r.restitution_bias = 0.0f;
+        const v3 i1 = mv(I1, r1n), i2 = mv(I2, r2n);
+        const float mp = im1 + im2 + vdot(vcross(i1, r1), n) + vdot(vcross(i2, r2), n);
+        const float inv_mass = mp > 0.0f ? 1.0f / mp : 0.0f;
+        float bias = 0.0f;
         const float dvn = dv.x * n.x + dv.y * n.y + dv.z * n.z;
-        if (dvn < -a.restitution_threshold) r.restitution_bias = restitution * dvn;
+        if (dvn < -a.restitution_threshold) bias = restitution * dvn;
+        r.q[DP_R1] = F4w(r1, nd.w);
+        r.q[DP_R2] = F4w(r2, inv_mass);
+        r.q[DP_N] = F4w(n, bias);
+        r.q[DP_I1] = F4w(i1, 0.0f);
+        r.q[DP_I2] = F4w(i2, 0.0f);
+        r.mut = make_float4(a.p_impulse[p], 0.0f, resting ? 1.0f : 0.0f, 0.0f);
         nsum = V(nsum.x + n.x, nsum.y + n.y, nsum.z + n.z);
     }
     const float fnb = float(nb);
@@ -204,13 +214,11 @@ __global__ void __launch_bounds__(128) dyn_manifold_init(const DynArgs a) {
     fp2 = vdivs(fp2, fnb);
     const v3 r1f = V(fp1.x - x1.x, fp1.y - x1.y, fp1.z - x1.z);
     const v3 r2f = V(fp2.x - x2.x, fp2.y - x2.y, fp2.z - x2.z);
-    S3(c.r1f, r1f); S3(c.r2f, r2f);
-    S3(c.ofv1, L3(a.m_fv1[m]));
-    S3(c.ofv2, L3(a.m_fv2[m]));
+    q[DQ_OFV1] = a.m_fv1[m];
+    q[DQ_OFV2] = a.m_fv2[m];
     const float4 fi = a.m_fimp[m];
-    c.f1 = fi.x; c.f2 = fi.y; c.ftw = fi.z;
+    a.mrec[m].mut = make_float4(fi.x, fi.y, fi.z, 0.0f);
     const v3 n = vnormalize(nsum);
-    S3(c.normal, n);
     // computeFrictionVectors (:789-818)
     const v3 dvf = rel_velocity(v1, w1, v2, w2, r1f, r2f);
     const float dvfn = vdot(dvf, n);
@@ -219,33 +227,324 @@ __global__ void __launch_bounds__(128) dyn_manifold_init(const DynArgs a) {
     const float lt = vlen(tv);
     const v3 fv1 = lt > MACHINE_EPSILON ? vdivs(tv, lt) : unit_orthogonal(n);
     const v3 fv2 = vcross(n, fv1);
-    S3(c.fv1, fv1); S3(c.fv2, fv2);
     const v3 r1ct1 = vcross(r1f, fv1), r1ct2 = vcross(r1f, fv2);
     const v3 r2ct1 = vcross(r2f, fv1), r2ct2 = vcross(r2f, fv2);
-    S3(c.r1ct1, r1ct1); S3(c.r1ct2, r1ct2); S3(c.r2ct1, r2ct1); S3(c.r2ct2, r2ct2);
-    const float f1m = c.im1 + c.im2 + vdot(vcross(mv(c.I1, r1ct1), r1f), fv1) + vdot(vcross(mv(c.I2, r2ct1), r2f), fv1);
-    const float f2m = c.im1 + c.im2 + vdot(vcross(mv(c.I1, r1ct2), r1f), fv2) + vdot(vcross(mv(c.I2, r2ct2), r2f), fv2);
-    const float twm = vdot(n, mv(c.I1, n)) + vdot(n, mv(c.I2, n));
-    c.inv_f1 = f1m > 0.0f ? 1.0f / f1m : 0.0f;
-    c.inv_f2 = f2m > 0.0f ? 1.0f / f2m : 0.0f;
-    c.inv_tw = twm > 0.0f ? 1.0f / twm : 0.0f;
+    const float f1m = im1 + im2 + vdot(vcross(mv(I1, r1ct1), r1f), fv1) + vdot(vcross(mv(I2, r2ct1), r2f), fv1);
+    const float f2m = im1 + im2 + vdot(vcross(mv(I1, r1ct2), r1f), fv2) + vdot(vcross(mv(I2, r2ct2), r2f), fv2);
+    const float twm = vdot(n, mv(I1, n)) + vdot(n, mv(I2, n));
+    q[DQ_N] = F4w(n, twm > 0.0f ? 1.0f / twm : 0.0f);
+    q[DQ_R1F] = F4w(r1f, f1m > 0.0f ? 1.0f / f1m : 0.0f);
+    q[DQ_R2F] = F4w(r2f, f2m > 0.0f ? 1.0f / f2m : 0.0f);
+    q[DQ_FV1] = F4w(fv1, 0.0f);
+    q[DQ_FV2] = F4w(fv2, 0.0f);
+    q[DQ_R1CT1] = F4w(r1ct1, 0.0f);
+    q[DQ_R1CT2] = F4w(r1ct2, 0.0f);
+    q[DQ_R2CT1] = F4w(r2ct1, 0.0f);
+    q[DQ_R2CT2] = F4w(r2ct2, 0.0f);
 }
 
-// Body velocities of one island's thread (cached loads / stores; the two
-// bodies of a manifold are distinct).
-struct Vel {
-    v3 v1, w1, v2, w2;
+// A manifold's constant solver data in registers (one 16-byte load per row).
+struct Man {
+    int32_t b1, b2, nb, pstart;
+    float im1, im2, friction;
+    uint32_t fixed;
+    v3 lf1, lf2, af1, af2;
+    float I1[9], I2[9];
+    v3 n, r1f, r2f, fv1, fv2, r1ct1, r1ct2, r2ct1, r2ct2;
+    float inv_tw, inv_f1, inv_f2;
 };
 
-RD void apply_linear(v3& v, float im, v3 imp, const float* lf, float sign) {
-    // v -= im * imp * lf (sign -1) or v += ... (sign +1), per component
-    if (sign < 0.0f) v = V(v.x - im * imp.x * lf[0], v.y - im * imp.y * lf[1], v.z - im * imp.z * lf[2]);
-    else v = V(v.x + im * imp.x * lf[0], v.y + im * imp.y * lf[1], v.z + im * imp.z * lf[2]);
+RD void rows3(const float4* __restrict__ q, float* I) {
+    const float4 r0 = __ldg(q), r1 = __ldg(q + 1), r2 = __ldg(q + 2);
+    I[0] = r0.x; I[1] = r0.y; I[2] = r0.z; I[3] = r1.x; I[4] = r1.y; I[5] = r1.z;
+    I[6] = r2.x; I[7] = r2.y; I[8] = r2.z;
+}
+
+// The records are written by kernel 2 and only read here, so the read-only
+// data path may serve them.
+RD void load_man(const DynManifoldRec* __restrict__ rec, Man& c) {
+    const float4* __restrict__ q = rec->q;
+    const float4 ids = __ldg(q + DQ_IDS), ms = __ldg(q + DQ_MASS);
+    c.b1 = __float_as_int(ids.x); c.b2 = __float_as_int(ids.y);
+    c.nb = __float_as_int(ids.z); c.pstart = __float_as_int(ids.w);
+    c.im1 = ms.x; c.im2 = ms.y; c.friction = ms.z; c.fixed = uint32_t(ms.w);
+    c.lf1 = L3(__ldg(q + DQ_LF1)); c.lf2 = L3(__ldg(q + DQ_LF2));
+    c.af1 = L3(__ldg(q + DQ_AF1)); c.af2 = L3(__ldg(q + DQ_AF2));
+    rows3(q + DQ_I1, c.I1);
+    rows3(q + DQ_I2, c.I2);
+    const float4 n = __ldg(q + DQ_N), r1f = __ldg(q + DQ_R1F), r2f = __ldg(q + DQ_R2F);
+    c.n = L3(n); c.inv_tw = n.w;
+    c.r1f = L3(r1f); c.inv_f1 = r1f.w;
+    c.r2f = L3(r2f); c.inv_f2 = r2f.w;
+    c.fv1 = L3(__ldg(q + DQ_FV1)); c.fv2 = L3(__ldg(q + DQ_FV2));
+    c.r1ct1 = L3(__ldg(q + DQ_R1CT1)); c.r1ct2 = L3(__ldg(q + DQ_R1CT2));
+    c.r2ct1 = L3(__ldg(q + DQ_R2CT1)); c.r2ct2 = L3(__ldg(q + DQ_R2CT2));
+}
+
+struct Pt {
+    v3 r1, r2, n, i1, i2;
+    float depth, inv_mass, bias;
+};
+
+RD void load_pt(const DynPointRec* __restrict__ rec, Pt& p) {
+    const float4 a = __ldg(rec->q + DP_R1), b = __ldg(rec->q + DP_R2), c = __ldg(rec->q + DP_N);
+    p.r1 = L3(a); p.depth = a.w;
+    p.r2 = L3(b); p.inv_mass = b.w;
+    p.n = L3(c); p.bias = c.w;
+    p.i1 = L3(__ldg(rec->q + DP_I1));
+    p.i2 = L3(__ldg(rec->q + DP_I2));
+}
+
+// v -= im * imp * lock  /  v += im * imp * lock, per component (Vector3 operators)
+RD v3 lin_sub(v3 v, float im, v3 imp, v3 lf) {
+    return V(v.x - im * imp.x * lf.x, v.y - im * imp.y * lf.y, v.z - im * imp.z * lf.z);
+}
+RD v3 lin_add(v3 v, float im, v3 imp, v3 lf) {
+    return V(v.x + im * imp.x * lf.x, v.y + im * imp.y * lf.y, v.z + im * imp.z * lf.z);
+}
+// w -= i * af * s  /  w += i * af * s, per component (the point updates)
+RD v3 ang_sub(v3 w, v3 i, v3 af, float s) {
+    return V(w.x - i.x * af.x * s, w.y - i.y * af.y * s, w.z - i.z * af.z * s);
+}
+RD v3 ang_add(v3 w, v3 i, v3 af, float s) {
+    return V(w.x + i.x * af.x * s, w.y + i.y * af.y * s, w.z + i.z * af.z * s);
+}
+
+// Where the solver reads and writes the velocities (constrained and split)
+// of a manifold's two bodies: the global scratch arrays, or a warp's shared
+// memory copy for the movable bodies of a large island.
+struct BodyVel {
+    float4 *v1, *w1, *s1, *t1, *v2, *w2, *s2, *t2;
+};
+
+RD BodyVel vel_global(const DynArgs& a, int32_t b1, int32_t b2) {
+    BodyVel p;
+    p.v1 = a.cv + b1; p.w1 = a.cw + b1; p.s1 = a.sv + b1; p.t1 = a.sw + b1;
+    p.v2 = a.cv + b2; p.w2 = a.cw + b2; p.s2 = a.sv + b2; p.t2 = a.sw + b2;
+    return p;
+}
+
+// warmStart (:324-476) of one manifold: its two bodies' velocities are loaded,
+// updated in the reference's statement order and stored back (the two bodies
+// are distinct; fixed bodies are never stored).
+RD void warm_manifold(const DynArgs& a, uint32_t mi, const BodyVel& bv, int32_t nb, int32_t pstart) {
+    if (nb == 0) return;  // rejected by the manifold kernel
+    Man c;
+    load_man(a.mrec + mi, c);
+    const v3 o1 = L3(__ldg(a.mrec[mi].q + DQ_OFV1)), o2 = L3(__ldg(a.mrec[mi].q + DQ_OFV2));
+    float4 mut = a.mrec[mi].mut;
+    v3 v1 = L3(*bv.v1), w1 = L3(*bv.w1), v2 = L3(*bv.v2), w2 = L3(*bv.w2);
+    bool resting_any = false;
+    for (int k = 0; k < nb; k++) {
+        DynPointRec* pr = a.prec + pstart + k;
+        float4 pm = pr->mut;
+        if (pm.z != 0.0f) {
+            resting_any = true;
+            Pt p;
+            load_pt(pr, p);
+            const float pi = pm.x;
+            const v3 ip = V(p.n.x * pi, p.n.y * pi, p.n.z * pi);
+            v1 = lin_sub(v1, c.im1, ip, c.lf1);
+            w1 = ang_sub(w1, p.i1, c.af1, pi);
+            v2 = lin_add(v2, c.im2, ip, c.lf2);
+            w2 = ang_add(w2, p.i2, c.af2, pi);
+        } else {
+            pm.x = 0.0f;
+            pr->mut = pm;
+        }
+    }
+    float f1 = mut.x, f2 = mut.y, ftw = mut.z;
+    if (resting_any) {
+        const v3 ofi = V(f1 * o1.x + f2 * o2.x, f1 * o1.y + f2 * o2.y, f1 * o1.z + f2 * o2.z);
+        f1 = vdot(ofi, c.fv1);
+        f2 = vdot(ofi, c.fv2);
+        // first friction constraint
+        v3 ai1 = V(-c.r1ct1.x * f1, -c.r1ct1.y * f1, -c.r1ct1.z * f1);
+        v3 li2 = V(c.fv1.x * f1, c.fv1.y * f1, c.fv1.z * f1);
+        v3 ai2 = V(c.r2ct1.x * f1, c.r2ct1.y * f1, c.r2ct1.z * f1);
+        v1 = lin_sub(v1, c.im1, li2, c.lf1);
+        w1 = vadd(w1, vcmul(c.af1, mv(c.I1, ai1)));
+        v2 = lin_add(v2, c.im2, li2, c.lf2);
+        w2 = vadd(w2, vcmul(c.af2, mv(c.I2, ai2)));
+        // second friction constraint
+        ai1 = V(-c.r1ct2.x * f2, -c.r1ct2.y * f2, -c.r1ct2.z * f2);
+        li2 = V(c.fv2.x * f2, c.fv2.y * f2, c.fv2.z * f2);
+        ai2 = V(c.r2ct2.x * f2, c.r2ct2.y * f2, c.r2ct2.z * f2);
+        v1 = lin_sub(v1, c.im1, li2, c.lf1);
+        w1 = vadd(w1, vcmul(c.af1, mv(c.I1, ai1)));
+        v2 = lin_add(v2, c.im2, li2, c.lf2);
+        w2 = vadd(w2, vcmul(c.af2, mv(c.I2, ai2)));
+        // twist friction constraint (the reference applies the body-2
+        // angular impulse to both bodies a second time, :461-465)
+        ai1 = V(-c.n.x * ftw, -c.n.y * ftw, -c.n.z * ftw);
+        ai2 = V(c.n.x * ftw, c.n.y * ftw, c.n.z * ftw);
+        w1 = vadd(w1, vcmul(c.af1, mv(c.I1, ai1)));
+        w2 = vadd(w2, vcmul(c.af2, mv(c.I2, ai2)));
+        w1 = vsub(w1, vcmul(c.af1, mv(c.I1, ai2)));
+        w2 = vadd(w2, vcmul(c.af2, mv(c.I2, ai2)));
+    } else {
+        f1 = 0.0f; f2 = 0.0f; ftw = 0.0f;
+    }
+    a.mrec[mi].mut = make_float4(f1, f2, ftw, mut.w);
+    if (!(c.fixed & 1)) { *bv.v1 = F4(v1); *bv.w1 = F4(w1); }
+    if (!(c.fixed & 2)) { *bv.v2 = F4(v2); *bv.w2 = F4(w2); }
+}
+
+// One solve pass (:479-759) over one manifold.
+RD void solve_manifold(const DynArgs& a, uint32_t mi, float beta, const BodyVel& bv, int32_t nb, int32_t pstart) {
+    if (nb == 0) return;
+    Man c;
+    load_man(a.mrec + mi, c);
+    float4 mut = a.mrec[mi].mut;
+    v3 v1 = L3(*bv.v1), w1 = L3(*bv.w1), v2 = L3(*bv.v2), w2 = L3(*bv.w2);
+    v3 s1 = L3(*bv.s1), t1 = L3(*bv.t1), s2 = L3(*bv.s2), t2 = L3(*bv.t2);
+    float sum_pen = 0.0f;
+    for (int k = 0; k < nb; k++) {
+        DynPointRec* pr = a.prec + pstart + k;
+        Pt p;
+        load_pt(pr, p);
+        float4 pm = pr->mut;
+        const v3 n = p.n;
+        const v3 dv = rel_velocity(v1, w1, v2, w2, p.r1, p.r2);
+        const float Jv = dv.x * n.x + dv.y * n.y + dv.z * n.z;
+        float bias_pen = 0.0f;
+        if (p.depth > SLOP) {
+            const float excess = p.depth - SLOP;
+            bias_pen = -(beta / a.dt) * ((0.0f < excess) ? excess : 0.0f);
+        }
+        const float b = bias_pen + p.bias;
+        float dl = a.split ? -(Jv + p.bias) * p.inv_mass : -(Jv + b) * p.inv_mass;
+        const float lt = pm.x;
+        const float sum = pm.x + dl;
+        pm.x = (sum < 0.0f) ? 0.0f : sum;
+        dl = pm.x - lt;
+        const v3 li = V(n.x * dl, n.y * dl, n.z * dl);
+        v1 = lin_sub(v1, c.im1, li, c.lf1);
+        w1 = ang_sub(w1, p.i1, c.af1, dl);
+        v2 = lin_add(v2, c.im2, li, c.lf2);
+        w2 = ang_add(w2, p.i2, c.af2, dl);
+        sum_pen += pm.x;
+        if (a.split) {
+            const v3 dvs = rel_velocity(s1, t1, s2, t2, p.r1, p.r2);
+            const float Jvs = dvs.x * n.x + dvs.y * n.y + dvs.z * n.z;
+            float dls = -(Jvs + bias_pen) * p.inv_mass;
+            const float lts = pm.y;
+            const float ss = pm.y + dls;
+            pm.y = (ss < 0.0f) ? 0.0f : ss;
+            dls = pm.y - lts;
+            const v3 lis = V(n.x * dls, n.y * dls, n.z * dls);
+            s1 = lin_sub(s1, c.im1, lis, c.lf1);
+            t1 = ang_sub(t1, p.i1, c.af1, dls);
+            s2 = lin_add(s2, c.im2, lis, c.lf2);
+            t2 = ang_add(t2, p.i2, c.af2, dls);
+        }
+        pr->mut = pm;
+    }
+    float f1 = mut.x, f2 = mut.y, ftw = mut.z;
+    // first friction constraint
+    {
+        const v3 dv = rel_velocity(v1, w1, v2, w2, c.r1f, c.r2f);
+        const float Jv = dv.x * c.fv1.x + dv.y * c.fv1.y + dv.z * c.fv1.z;
+        float dl = -Jv * c.inv_f1;
+        const float limit = c.friction * sum_pen;
+        const float lt = f1;
+        f1 = smax(-limit, smin(f1 + dl, limit));
+        dl = f1 - lt;
+        const v3 ai1 = V(-c.r1ct1.x * dl, -c.r1ct1.y * dl, -c.r1ct1.z * dl);
+        const v3 li2 = V(c.fv1.x * dl, c.fv1.y * dl, c.fv1.z * dl);
+        const v3 ai2 = V(c.r2ct1.x * dl, c.r2ct1.y * dl, c.r2ct1.z * dl);
+        v1 = lin_sub(v1, c.im1, li2, c.lf1);
+        w1 = vadd(w1, vcmul(c.af1, mv(c.I1, ai1)));
+        v2 = lin_add(v2, c.im2, li2, c.lf2);
+        w2 = vadd(w2, vcmul(c.af2, mv(c.I2, ai2)));
+    }
+    // second friction constraint
+    {
+        const v3 dv = rel_velocity(v1, w1, v2, w2, c.r1f, c.r2f);
+        const float Jv = dv.x * c.fv2.x + dv.y * c.fv2.y + dv.z * c.fv2.z;
+        float dl = -Jv * c.inv_f2;
+        const float limit = c.friction * sum_pen;
+        const float lt = f2;
+        f2 = smax(-limit, smin(f2 + dl, limit));
+        dl = f2 - lt;
+        const v3 ai1 = V(-c.r1ct2.x * dl, -c.r1ct2.y * dl, -c.r1ct2.z * dl);
+        const v3 li2 = V(c.fv2.x * dl, c.fv2.y * dl, c.fv2.z * dl);
+        const v3 ai2 = V(c.r2ct2.x * dl, c.r2ct2.y * dl, c.r2ct2.z * dl);
+        v1 = lin_sub(v1, c.im1, li2, c.lf1);
+        w1 = vadd(w1, vcmul(c.af1, mv(c.I1, ai1)));
+        v2 = lin_add(v2, c.im2, li2, c.lf2);
+        w2 = vadd(w2, vcmul(c.af2, mv(c.I2, ai2)));
+    }
+    // twist friction constraint
+    {
+        const v3 dw = vsub(w2, w1);
+        const float Jv = dw.x * c.n.x + dw.y * c.n.y + dw.z * c.n.z;
+        float dl = -Jv * c.inv_tw;
+        const float limit = c.friction * sum_pen;
+        const float lt = ftw;
+        ftw = smax(-limit, smin(ftw + dl, limit));
+        dl = ftw - lt;
+        const v3 ai2 = V(c.n.x * dl, c.n.y * dl, c.n.z * dl);
+        w1 = vsub(w1, vcmul(c.af1, mv(c.I1, ai2)));
+        w2 = vadd(w2, vcmul(c.af2, mv(c.I2, ai2)));
+    }
+    a.mrec[mi].mut = make_float4(f1, f2, ftw, mut.w);
+    if (!(c.fixed & 1)) { *bv.v1 = F4(v1); *bv.w1 = F4(w1); *bv.s1 = F4(s1); *bv.t1 = F4(t1); }
+    if (!(c.fixed & 2)) { *bv.v2 = F4(v2); *bv.w2 = F4(w2); *bv.s2 = F4(s2); *bv.t2 = F4(t2); }
+}
+
+// storeImpulses (:763-785) of one manifold.
+RD void store_manifold(const DynArgs& a, uint32_t mi) {
+    Man c;
+    load_man(a.mrec + mi, c);
+    if (c.nb == 0) return;
+    for (int k = 0; k < c.nb; k++) a.p_impulse[c.pstart + k] = a.prec[c.pstart + k].mut.x;
+    const float4 mut = a.mrec[mi].mut;
+    a.m_fimp[mi] = make_float4(mut.x, mut.y, mut.z, 0.0f);
+    a.m_fv1[mi] = F4(c.fv1);
+    a.m_fv2[mi] = F4(c.fv2);
+}
+
+RD void man_bodies(const DynArgs& a, uint32_t mi, int32_t& b1, int32_t& b2, uint32_t& fixed, bool& valid) {
+    const float4 ids = __ldg(a.mrec[mi].q + DQ_IDS), ms = __ldg(a.mrec[mi].q + DQ_MASS);
+    b1 = __float_as_int(ids.x); b2 = __float_as_int(ids.y);
+    valid = __float_as_int(ids.z) != 0;
+    fixed = uint32_t(ms.w);
 }
 
 // ---- kernel 3: warm start, velocity iterations, stored impulses ----------
-// One thread per island (ContactSolverSystem.cpp:324-785).
-__global__ void __launch_bounds__(128) dyn_island_solve(const DynArgs a) {
+//
+// The reference runs the manifolds of an island strictly in order; manifold j
+// only reads and writes the velocities of its two bodies, and islands share
+// only fixed bodies (static or kinematic: never written here).  So islands
+// are independent, and inside an island any schedule that keeps, for every
+// movable body, the order of the manifolds touching it gives bit-identical
+// results.
+//
+// 3a: one thread per island runs islands of up to SMALL_ISLAND manifolds in
+//     the reference's order and queues the larger ones.
+// 3b: persistent warps take the queued islands.  Lane 0 gives each manifold a
+//     level (1 + the highest level of an earlier manifold sharing a movable
+//     body) and sorts the island's manifolds by level; every pass (warm
+//     start, each velocity iteration) then runs level after level, the
+//     manifolds of a level in parallel across the warp, __syncwarp (which
+//     orders the lanes' memory accesses) between levels.  An island of up to
+//     STAGE_MANIFOLDS manifolds and STAGE_BODIES movable bodies is staged in
+//     the warp's shared memory: its manifold table, the schedule (computed
+//     with a shared hash of body -> slot, last level) and the bodies'
+//     velocities.  Larger islands use the same schedule built in global
+//     scratch, with velocities in global memory.
+
+constexpr uint32_t SMALL_ISLAND = 8;
+constexpr uint32_t BIG_ISLAND = 64;   // queued first: the longest islands start first
+
+RD int4 man_ids(const DynArgs& a, uint32_t mi) {
+    const float4 q = __ldg(a.mrec[mi].q + DQ_IDS);
+    return make_int4(__float_as_int(q.x), __float_as_int(q.y), __float_as_int(q.z), __float_as_int(q.w));
+}
+RD uint32_t man_fixed(const DynArgs& a, uint32_t mi) { return uint32_t(__ldg(a.mrec[mi].q + DQ_MASS).w); }
+
+__global__ void __launch_bounds__(128) dyn_islands_small(const DynArgs a) {
     const uint32_t is = blockIdx.x * blockDim.x + threadIdx.x;
     if (is >= a.ni) return;
     const uint32_t m0 = a.i_start[is], cnt = a.i_count[is];
@@ -253,182 +552,223 @@ __global__ void __launch_bounds__(128) dyn_island_solve(const DynArgs a) {
         atomicOr(a.error, 4u);
         return;
     }
+    if (cnt == 0) return;
+    if (cnt > SMALL_ISLAND) {
+        // big islands fill the list from the front, the others from the back
+        if (cnt > BIG_ISLAND) a.large_list[atomicAdd(a.counters, 1u)] = is;
+        else a.large_list[a.ni - 1 - atomicAdd(a.counters + 2, 1u)] = is;
+        return;
+    }
     const uint32_t m1 = m0 + cnt;
-    float4* __restrict__ cv = a.cv;
-    float4* __restrict__ cw = a.cw;
-
-    // warmStart (:324-476)
     for (uint32_t mi = m0; mi < m1; mi++) {
-        DynManifoldRec& c = a.mrec[mi];
-        if (c.nb == 0) continue;  // rejected by the manifold kernel
-        const int32_t b1 = c.b1, b2 = c.b2;
-        const uint32_t fixed = uint32_t(c.fixed_mask);
-        v3 v1 = L3(cv[b1]), w1 = L3(cw[b1]), v2 = L3(cv[b2]), w2 = L3(cw[b2]);
-        bool resting_any = false;
-        for (int k = 0; k < c.nb; k++) {
-            DynPointRec& p = a.prec[c.pstart + k];
-            if (p.resting) {
-                resting_any = true;
-                const v3 n = A3(p.normal);
-                const float pi = p.impulse;
-                const v3 ip = V(n.x * pi, n.y * pi, n.z * pi);
-                apply_linear(v1, c.im1, ip, c.lf1, -1.0f);
-                w1 = V(w1.x - p.i1[0] * c.alf1[0] * pi, w1.y - p.i1[1] * c.alf1[1] * pi, w1.z - p.i1[2] * c.alf1[2] * pi);
-                apply_linear(v2, c.im2, ip, c.lf2, 1.0f);
-                w2 = V(w2.x + p.i2[0] * c.alf2[0] * pi, w2.y + p.i2[1] * c.alf2[1] * pi, w2.z + p.i2[2] * c.alf2[2] * pi);
-            } else {
-                p.impulse = 0.0f;
-            }
-        }
-        if (resting_any) {
-            const v3 o1 = A3(c.ofv1), o2 = A3(c.ofv2);
-            const v3 ofi = V(c.f1 * o1.x + c.f2 * o2.x, c.f1 * o1.y + c.f2 * o2.y, c.f1 * o1.z + c.f2 * o2.z);
-            c.f1 = vdot(ofi, A3(c.fv1));
-            c.f2 = vdot(ofi, A3(c.fv2));
-            // first friction constraint
-            v3 ai1 = V(-c.r1ct1[0] * c.f1, -c.r1ct1[1] * c.f1, -c.r1ct1[2] * c.f1);
-            v3 li2 = V(c.fv1[0] * c.f1, c.fv1[1] * c.f1, c.fv1[2] * c.f1);
-            v3 ai2 = V(c.r2ct1[0] * c.f1, c.r2ct1[1] * c.f1, c.r2ct1[2] * c.f1);
-            apply_linear(v1, c.im1, li2, c.lf1, -1.0f);
-            w1 = vadd(w1, vcmul(A3(c.alf1), mv(c.I1, ai1)));
-            apply_linear(v2, c.im2, li2, c.lf2, 1.0f);
-            w2 = vadd(w2, vcmul(A3(c.alf2), mv(c.I2, ai2)));
-            // second friction constraint
-            ai1 = V(-c.r1ct2[0] * c.f2, -c.r1ct2[1] * c.f2, -c.r1ct2[2] * c.f2);
-            li2 = V(c.fv2[0] * c.f2, c.fv2[1] * c.f2, c.fv2[2] * c.f2);
-            ai2 = V(c.r2ct2[0] * c.f2, c.r2ct2[1] * c.f2, c.r2ct2[2] * c.f2);
-            apply_linear(v1, c.im1, li2, c.lf1, -1.0f);
-            w1 = vadd(w1, vcmul(A3(c.alf1), mv(c.I1, ai1)));
-            apply_linear(v2, c.im2, li2, c.lf2, 1.0f);
-            w2 = vadd(w2, vcmul(A3(c.alf2), mv(c.I2, ai2)));
-            // twist friction constraint (the reference applies the body-2
-            // angular impulse to both bodies a second time, :461-465)
-            ai1 = V(-c.normal[0] * c.ftw, -c.normal[1] * c.ftw, -c.normal[2] * c.ftw);
-            ai2 = V(c.normal[0] * c.ftw, c.normal[1] * c.ftw, c.normal[2] * c.ftw);
-            w1 = vadd(w1, vcmul(A3(c.alf1), mv(c.I1, ai1)));
-            w2 = vadd(w2, vcmul(A3(c.alf2), mv(c.I2, ai2)));
-            w1 = vsub(w1, vcmul(A3(c.alf1), mv(c.I1, ai2)));
-            w2 = vadd(w2, vcmul(A3(c.alf2), mv(c.I2, ai2)));
-        } else {
-            c.f1 = 0.0f; c.f2 = 0.0f; c.ftw = 0.0f;
-        }
-        if (!(fixed & 1)) { cv[b1] = F4(v1); cw[b1] = F4(w1); }
-        if (!(fixed & 2)) { cv[b2] = F4(v2); cw[b2] = F4(w2); }
+        const int4 id = man_ids(a, mi);
+        warm_manifold(a, mi, vel_global(a, id.x, id.y), id.z, id.w);
     }
-
-    // solve (:479-759), iterations x island manifolds in order
     const float beta = a.split ? BETA_SPLIT_IMPULSE : BETA;
-    float4* __restrict__ sv = a.sv;
-    float4* __restrict__ sw = a.sw;
-    for (int it = 0; it < a.iterations; it++) {
+    for (int it = 0; it < a.iterations; it++)
         for (uint32_t mi = m0; mi < m1; mi++) {
-            DynManifoldRec& c = a.mrec[mi];
-            if (c.nb == 0) continue;
-            const int32_t b1 = c.b1, b2 = c.b2;
-            const uint32_t fixed = uint32_t(c.fixed_mask);
-            v3 v1 = L3(cv[b1]), w1 = L3(cw[b1]), v2 = L3(cv[b2]), w2 = L3(cw[b2]);
-            v3 s1 = L3(sv[b1]), t1 = L3(sw[b1]), s2 = L3(sv[b2]), t2 = L3(sw[b2]);
-            float sum_pen = 0.0f;
-            for (int k = 0; k < c.nb; k++) {
-                DynPointRec& p = a.prec[c.pstart + k];
-                const v3 n = A3(p.normal), r1 = A3(p.r1), r2 = A3(p.r2);
-                const v3 dv = rel_velocity(v1, w1, v2, w2, r1, r2);
-                const float Jv = dv.x * n.x + dv.y * n.y + dv.z * n.z;
-                float bias_pen = 0.0f;
-                if (p.depth > SLOP) {
-                    const float excess = p.depth - SLOP;
-                    bias_pen = -(beta / a.dt) * ((0.0f < excess) ? excess : 0.0f);
-                }
-                const float b = bias_pen + p.restitution_bias;
-                float dl = a.split ? -(Jv + p.restitution_bias) * p.inv_mass : -(Jv + b) * p.inv_mass;
-                const float lt = p.impulse;
-                const float sum = p.impulse + dl;
-                p.impulse = (sum < 0.0f) ? 0.0f : sum;
-                dl = p.impulse - lt;
-                const v3 li = V(n.x * dl, n.y * dl, n.z * dl);
-                apply_linear(v1, c.im1, li, c.lf1, -1.0f);
-                w1 = V(w1.x - p.i1[0] * c.alf1[0] * dl, w1.y - p.i1[1] * c.alf1[1] * dl, w1.z - p.i1[2] * c.alf1[2] * dl);
-                apply_linear(v2, c.im2, li, c.lf2, 1.0f);
-                w2 = V(w2.x + p.i2[0] * c.alf2[0] * dl, w2.y + p.i2[1] * c.alf2[1] * dl, w2.z + p.i2[2] * c.alf2[2] * dl);
-                sum_pen += p.impulse;
-                if (a.split) {
-                    const v3 dvs = rel_velocity(s1, t1, s2, t2, r1, r2);
-                    const float Jvs = dvs.x * n.x + dvs.y * n.y + dvs.z * n.z;
-                    float dls = -(Jvs + bias_pen) * p.inv_mass;
-                    const float lts = p.split_impulse;
-                    const float ss = p.split_impulse + dls;
-                    p.split_impulse = (ss < 0.0f) ? 0.0f : ss;
-                    dls = p.split_impulse - lts;
-                    const v3 lis = V(n.x * dls, n.y * dls, n.z * dls);
-                    apply_linear(s1, c.im1, lis, c.lf1, -1.0f);
-                    t1 = V(t1.x - p.i1[0] * c.alf1[0] * dls, t1.y - p.i1[1] * c.alf1[1] * dls,
-                           t1.z - p.i1[2] * c.alf1[2] * dls);
-                    apply_linear(s2, c.im2, lis, c.lf2, 1.0f);
-                    t2 = V(t2.x + p.i2[0] * c.alf2[0] * dls, t2.y + p.i2[1] * c.alf2[1] * dls,
-                           t2.z + p.i2[2] * c.alf2[2] * dls);
-                }
-            }
-            const v3 r1f = A3(c.r1f), r2f = A3(c.r2f);
-            // first friction constraint
-            {
-                const v3 dv = rel_velocity(v1, w1, v2, w2, r1f, r2f);
-                const float Jv = dv.x * c.fv1[0] + dv.y * c.fv1[1] + dv.z * c.fv1[2];
-                float dl = -Jv * c.inv_f1;
-                const float limit = c.friction * sum_pen;
-                const float lt = c.f1;
-                c.f1 = smax(-limit, smin(c.f1 + dl, limit));
-                dl = c.f1 - lt;
-                const v3 ai1 = V(-c.r1ct1[0] * dl, -c.r1ct1[1] * dl, -c.r1ct1[2] * dl);
-                const v3 li2 = V(c.fv1[0] * dl, c.fv1[1] * dl, c.fv1[2] * dl);
-                const v3 ai2 = V(c.r2ct1[0] * dl, c.r2ct1[1] * dl, c.r2ct1[2] * dl);
-                apply_linear(v1, c.im1, li2, c.lf1, -1.0f);
-                w1 = vadd(w1, vcmul(A3(c.alf1), mv(c.I1, ai1)));
-                apply_linear(v2, c.im2, li2, c.lf2, 1.0f);
-                w2 = vadd(w2, vcmul(A3(c.alf2), mv(c.I2, ai2)));
-            }
-            // second friction constraint
-            {
-                const v3 dv = rel_velocity(v1, w1, v2, w2, r1f, r2f);
-                const float Jv = dv.x * c.fv2[0] + dv.y * c.fv2[1] + dv.z * c.fv2[2];
-                float dl = -Jv * c.inv_f2;
-                const float limit = c.friction * sum_pen;
-                const float lt = c.f2;
-                c.f2 = smax(-limit, smin(c.f2 + dl, limit));
-                dl = c.f2 - lt;
-                const v3 ai1 = V(-c.r1ct2[0] * dl, -c.r1ct2[1] * dl, -c.r1ct2[2] * dl);
-                const v3 li2 = V(c.fv2[0] * dl, c.fv2[1] * dl, c.fv2[2] * dl);
-                const v3 ai2 = V(c.r2ct2[0] * dl, c.r2ct2[1] * dl, c.r2ct2[2] * dl);
-                apply_linear(v1, c.im1, li2, c.lf1, -1.0f);
-                w1 = vadd(w1, vcmul(A3(c.alf1), mv(c.I1, ai1)));
-                apply_linear(v2, c.im2, li2, c.lf2, 1.0f);
-                w2 = vadd(w2, vcmul(A3(c.alf2), mv(c.I2, ai2)));
-            }
-            // twist friction constraint
-            {
-                const v3 dw = vsub(w2, w1);
-                const float Jv = dw.x * c.normal[0] + dw.y * c.normal[1] + dw.z * c.normal[2];
-                float dl = -Jv * c.inv_tw;
-                const float limit = c.friction * sum_pen;
-                const float lt = c.ftw;
-                c.ftw = smax(-limit, smin(c.ftw + dl, limit));
-                dl = c.ftw - lt;
-                const v3 ai2 = V(c.normal[0] * dl, c.normal[1] * dl, c.normal[2] * dl);
-                w1 = vsub(w1, vcmul(A3(c.alf1), mv(c.I1, ai2)));
-                w2 = vadd(w2, vcmul(A3(c.alf2), mv(c.I2, ai2)));
-            }
-            if (!(fixed & 1)) { cv[b1] = F4(v1); cw[b1] = F4(w1); sv[b1] = F4(s1); sw[b1] = F4(t1); }
-            if (!(fixed & 2)) { cv[b2] = F4(v2); cw[b2] = F4(w2); sv[b2] = F4(s2); sw[b2] = F4(t2); }
+            const int4 id = man_ids(a, mi);
+            solve_manifold(a, mi, beta, vel_global(a, id.x, id.y), id.z, id.w);
+        }
+    for (uint32_t mi = m0; mi < m1; mi++) store_manifold(a, mi);
+}
+
+// Shared memory of one warp of kernel 3b.
+constexpr uint32_t STAGE_HASH = 2 * STAGE_BODIES;   // open addressing, load <= 1/2
+struct WarpStage {
+    float4 vel[4][STAGE_BODIES];        // constrained v, w and split v, w of the staged bodies
+    int4 man[STAGE_MANIFOLDS];          // body 1, body 2, points, first point
+    short2 slot[STAGE_MANIFOLDS];       // slot of body 1 / body 2 (-1: fixed body)
+    uint16_t order[STAGE_MANIFOLDS];    // island manifolds sorted by level
+    uint16_t lev[STAGE_MANIFOLDS];      // start of each level
+    uint16_t klev[STAGE_MANIFOLDS];     // level of each manifold
+    int32_t hkey[STAGE_HASH];           // body id (-1 empty)
+    uint32_t hval[STAGE_HASH];          // slot << 16 | last level
+    int32_t slot_body[STAGE_BODIES];    // body of each slot
+};
+static_assert(sizeof(WarpStage) <= LARGE_WARP_SMEM, "warp stage");
+
+// Slot and last level of a movable body (inserted on first use); false when
+// the island has more movable bodies than the stage holds.
+RD bool stage_body(WarpStage* st, int32_t b, uint32_t& nslots, uint32_t& idx) {
+    uint32_t h = (uint32_t(b) * 2654435761u) >> 23;   // 9 bits: STAGE_HASH = 512
+    for (uint32_t probe = 0; probe < STAGE_HASH; probe++, h = (h + 1) & (STAGE_HASH - 1)) {
+        const int32_t k = st->hkey[h];
+        if (k == b) { idx = h; return true; }
+        if (k < 0) {
+            if (nslots >= STAGE_BODIES) return false;
+            st->hkey[h] = b;
+            st->hval[h] = nslots << 16;
+            st->slot_body[nslots] = b;
+            nslots++;
+            idx = h;
+            return true;
         }
     }
+    return false;
+}
 
-    // storeImpulses (:763-785)
-    for (uint32_t mi = m0; mi < m1; mi++) {
-        const DynManifoldRec& c = a.mrec[mi];
-        if (c.nb == 0) continue;
-        for (int k = 0; k < c.nb; k++) a.p_impulse[c.pstart + k] = a.prec[c.pstart + k].impulse;
-        a.m_fimp[mi] = make_float4(c.f1, c.f2, c.ftw, 0.0f);
-        a.m_fv1[mi] = F4(A3(c.fv1));
-        a.m_fv2[mi] = F4(A3(c.fv2));
+// Schedule of a staged island in shared memory; false if it does not fit.
+RD bool schedule_staged(const DynArgs& a, uint32_t m0, uint32_t cnt, WarpStage* st, uint32_t lane,
+                        uint32_t& depth, uint32_t& nslots) {
+    for (uint32_t h = lane; h < STAGE_HASH; h += 32) st->hkey[h] = -1;
+    for (uint32_t k = lane; k < cnt; k += 32) {
+        int4 id = man_ids(a, m0 + k);
+        const uint32_t fixed = man_fixed(a, m0 + k);
+        // fixed bodies are marked by a negative id in the table
+        if (fixed & 1) id.x = -1 - id.x;
+        if (fixed & 2) id.y = -1 - id.y;
+        st->man[k] = id;
+    }
+    __syncwarp();
+    bool ok = true;
+    if (lane == 0) {
+        depth = 0;
+        nslots = 0;
+        for (uint32_t k = 0; k < cnt && ok; k++) {
+            const int4 id = st->man[k];
+            uint32_t L = 1;
+            short2 sl = make_short2(-1, -1);
+            if (id.z != 0) {
+                uint32_t h1 = 0, h2 = 0, l1 = 0, l2 = 0;
+                if (id.x >= 0) { ok = stage_body(st, id.x, nslots, h1); if (ok) { l1 = st->hval[h1] & 0xffffu; sl.x = short(st->hval[h1] >> 16); } }
+                if (ok && id.y >= 0) { ok = stage_body(st, id.y, nslots, h2); if (ok) { l2 = st->hval[h2] & 0xffffu; sl.y = short(st->hval[h2] >> 16); } }
+                if (!ok) break;
+                L = 1 + (l1 > l2 ? l1 : l2);
+                if (id.x >= 0) st->hval[h1] = (st->hval[h1] & 0xffff0000u) | L;
+                if (id.y >= 0) st->hval[h2] = (st->hval[h2] & 0xffff0000u) | L;
+            }
+            st->slot[k] = sl;
+            st->klev[k] = uint16_t(L);
+            depth = L > depth ? L : depth;
+        }
+        if (ok) {
+            for (uint32_t L = 0; L < depth; L++) st->lev[L] = 0;
+            for (uint32_t k = 0; k < cnt; k++) st->lev[st->klev[k] - 1]++;
+            uint32_t run = 0;
+            for (uint32_t L = 0; L < depth; L++) { run += st->lev[L]; st->lev[L] = uint16_t(run); }
+            for (uint32_t k = cnt; k-- > 0;) st->order[--st->lev[st->klev[k] - 1]] = uint16_t(k);
+        }
+    }
+    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+    depth = __shfl_sync(0xffffffffu, depth, 0);
+    nslots = __shfl_sync(0xffffffffu, nslots, 0);
+    __syncwarp();
+    return ok;
+}
+
+RD void solve_staged(const DynArgs& a, uint32_t m0, uint32_t cnt, WarpStage* st, uint32_t lane, uint32_t depth,
+                     uint32_t nslots) {
+    for (uint32_t s = lane; s < nslots; s += 32) {
+        const int32_t b = st->slot_body[s];
+        st->vel[0][s] = a.cv[b]; st->vel[1][s] = a.cw[b];
+        st->vel[2][s] = a.sv[b]; st->vel[3][s] = a.sw[b];
+    }
+    __syncwarp();
+    const float beta = a.split ? BETA_SPLIT_IMPULSE : BETA;
+    for (int pass = 0; pass <= a.iterations; pass++) {
+        for (uint32_t L = 0; L < depth; L++) {
+            const uint32_t b = st->lev[L];
+            const uint32_t e = (L + 1 < depth) ? st->lev[L + 1] : cnt;
+            for (uint32_t k = b + lane; k < e; k += 32) {
+                const uint32_t kk = st->order[k];
+                const int4 id = st->man[kk];
+                const short2 sl = st->slot[kk];
+                BodyVel bv;
+                if (sl.x >= 0) { bv.v1 = &st->vel[0][sl.x]; bv.w1 = &st->vel[1][sl.x]; bv.s1 = &st->vel[2][sl.x]; bv.t1 = &st->vel[3][sl.x]; }
+                else { const int32_t b1 = -1 - id.x; bv.v1 = a.cv + b1; bv.w1 = a.cw + b1; bv.s1 = a.sv + b1; bv.t1 = a.sw + b1; }
+                if (sl.y >= 0) { bv.v2 = &st->vel[0][sl.y]; bv.w2 = &st->vel[1][sl.y]; bv.s2 = &st->vel[2][sl.y]; bv.t2 = &st->vel[3][sl.y]; }
+                else { const int32_t b2 = -1 - id.y; bv.v2 = a.cv + b2; bv.w2 = a.cw + b2; bv.s2 = a.sv + b2; bv.t2 = a.sw + b2; }
+                if (pass == 0) warm_manifold(a, m0 + kk, bv, id.z, id.w);
+                else solve_manifold(a, m0 + kk, beta, bv, id.z, id.w);
+            }
+            __syncwarp();
+        }
+    }
+    for (uint32_t s = lane; s < nslots; s += 32) {
+        const int32_t b = st->slot_body[s];
+        a.cv[b] = st->vel[0][s]; a.cw[b] = st->vel[1][s];
+        a.sv[b] = st->vel[2][s]; a.sw[b] = st->vel[3][s];
+    }
+}
+
+// Islands too large for the stage: the same schedule in global scratch.
+RD void solve_global(const DynArgs& a, uint32_t m0, uint32_t cnt, uint32_t lane) {
+    uint32_t* __restrict__ ord = a.order + m0;
+    uint32_t* __restrict__ lev = a.level + m0;
+    uint32_t* __restrict__ blev = a.body_level;
+    for (uint32_t k = lane; k < cnt; k += 32) {
+        const int4 id = man_ids(a, m0 + k);
+        if (id.z == 0) continue;
+        const uint32_t fixed = man_fixed(a, m0 + k);
+        if (!(fixed & 1)) blev[id.x] = 0;
+        if (!(fixed & 2)) blev[id.y] = 0;
+    }
+    __syncwarp();
+    uint32_t depth = 0;
+    if (lane == 0) {
+        for (uint32_t k = 0; k < cnt; k++) {
+            const int4 id = man_ids(a, m0 + k);
+            uint32_t L = 1;
+            if (id.z != 0) {
+                const uint32_t fixed = man_fixed(a, m0 + k);
+                const uint32_t l1 = (fixed & 1) ? 0u : blev[id.x];
+                const uint32_t l2 = (fixed & 2) ? 0u : blev[id.y];
+                L = 1 + (l1 > l2 ? l1 : l2);
+                if (!(fixed & 1)) blev[id.x] = L;
+                if (!(fixed & 2)) blev[id.y] = L;
+            }
+            ord[k] = L;  // the level, until the scatter below
+            depth = L > depth ? L : depth;
+        }
+        for (uint32_t L = 0; L < depth; L++) lev[L] = 0;
+        for (uint32_t k = 0; k < cnt; k++) lev[ord[k] - 1]++;
+        uint32_t run = 0;
+        for (uint32_t L = 0; L < depth; L++) { run += lev[L]; lev[L] = run; }
+        // keep the levels in the records' spare word while scattering
+        for (uint32_t k = 0; k < cnt; k++) a.mrec[m0 + k].mut.w = __int_as_float(int32_t(ord[k]));
+        for (uint32_t k = cnt; k-- > 0;) {
+            const uint32_t L = uint32_t(__float_as_int(a.mrec[m0 + k].mut.w));
+            ord[--lev[L - 1]] = k;
+        }
+    }
+    depth = __shfl_sync(0xffffffffu, depth, 0);
+    __syncwarp();
+    const float beta = a.split ? BETA_SPLIT_IMPULSE : BETA;
+    for (int pass = 0; pass <= a.iterations; pass++) {
+        for (uint32_t L = 0; L < depth; L++) {
+            const uint32_t b = lev[L];
+            const uint32_t e = (L + 1 < depth) ? lev[L + 1] : cnt;
+            for (uint32_t k = b + lane; k < e; k += 32) {
+                const uint32_t mi = m0 + ord[k];
+                const int4 id = man_ids(a, mi);
+                if (pass == 0) warm_manifold(a, mi, vel_global(a, id.x, id.y), id.z, id.w);
+                else solve_manifold(a, mi, beta, vel_global(a, id.x, id.y), id.z, id.w);
+            }
+            __syncwarp();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(LARGE_WARPS * 32, 2) dyn_islands_large(const DynArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpStage* st = reinterpret_cast<WarpStage*>(smem_raw + size_t(wid) * LARGE_WARP_SMEM);
+    const uint32_t n_big = a.counters[0], n_mid = a.counters[2];
+    for (;;) {
+        uint32_t k = 0;
+        if (lane == 0) k = atomicAdd(a.counters + 1, 1u);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (k >= n_big + n_mid) break;
+        const uint32_t is = k < n_big ? a.large_list[k] : a.large_list[a.ni - 1 - (k - n_big)];
+        const uint32_t m0 = a.i_start[is], cnt = a.i_count[is];
+        uint32_t depth = 0, nslots = 0;
+        if (cnt <= STAGE_MANIFOLDS && schedule_staged(a, m0, cnt, st, lane, depth, nslots))
+            solve_staged(a, m0, cnt, st, lane, depth, nslots);
+        else
+            solve_global(a, m0, cnt, lane);
+        for (uint32_t j = lane; j < cnt; j += 32) store_manifold(a, m0 + j);
+        __syncwarp();
     }
 }
 
@@ -482,7 +822,15 @@ uint32_t blocks(uint32_t n) { return (n + 127) / 128; }
 cudaError_t launch_dynamics(const DynArgs& a, cudaStream_t s, uint64_t* launches) {
     if (a.nb) { dyn_bodies_pre<<<blocks(a.nb), 128, 0, s>>>(a); (*launches)++; }
     if (a.nm) { dyn_manifold_init<<<blocks(a.nm), 128, 0, s>>>(a); (*launches)++; }
-    if (a.ni) { dyn_island_solve<<<blocks(a.ni), 128, 0, s>>>(a); (*launches)++; }
+    if (a.ni) {
+        cudaMemsetAsync(a.counters, 0, 3 * sizeof(uint32_t), s);
+        dyn_islands_small<<<blocks(a.ni), 128, 0, s>>>(a);
+        (*launches)++;
+        const size_t smem = size_t(LARGE_WARPS) * LARGE_WARP_SMEM;
+        cudaFuncSetAttribute(dyn_islands_large, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        dyn_islands_large<<<a.large_ctas, LARGE_WARPS * 32, smem, s>>>(a);
+        (*launches)++;
+    }
     if (a.nb_enabled) { dyn_bodies_post<<<blocks(a.nb_enabled), 128, 0, s>>>(a); (*launches)++; }
     if (a.nc_enabled) { dyn_colliders<<<blocks(a.nc_enabled), 128, 0, s>>>(a); (*launches)++; }
     return cudaGetLastError();

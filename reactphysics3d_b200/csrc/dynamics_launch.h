@@ -8,32 +8,40 @@
 
 namespace rp3dg {
 
-// Per-manifold solver record (ContactManifoldSolver, ContactSolverSystem.h:
-// 153-260) and per-point record (ContactPointSolver, :85-135), in device
-// scratch; one thread touches a record at a time.
-struct DynManifoldRec {
-    int32_t b1, b2, nb, pstart;
-    float im1, im2, friction, fixed_mask;   // fixed_mask: bit0 body 1, bit1 body 2 never written
-    float lf1[3], lf2[3], alf1[3], alf2[3];
-    float I1[9], I2[9];
-    float normal[3];
-    float r1f[3], r2f[3];
-    float fv1[3], fv2[3];
-    float ofv1[3], ofv2[3];
-    float r1ct1[3], r1ct2[3], r2ct1[3], r2ct2[3];
-    float inv_f1, inv_f2, inv_tw;
-    float f1, f2, ftw;
-    float pad[2];
+// Per-manifold solver record (the data of ContactManifoldSolver,
+// ContactSolverSystem.h:153-260) and per-point record (ContactPointSolver,
+// :85-135) in device scratch, as rows of float4 so that the solver loads each
+// with one 16-byte access.  q[] is written once by the manifold kernel;
+// mut holds what the passes update.
+enum DynManifoldRow {
+    DQ_IDS = 0,     // body1, body2, number of points, first point (int bits)
+    DQ_MASS,        // inverse mass 1, inverse mass 2, friction coefficient, fixed mask (bit0 body1, bit1 body2)
+    DQ_LF1, DQ_LF2, DQ_AF1, DQ_AF2,   // linear / angular lock factors
+    DQ_I1, DQ_I2 = DQ_I1 + 3,          // world inverse inertia rows
+    DQ_N = DQ_I2 + 3,                  // normal, inverse twist friction mass
+    DQ_R1F, DQ_R2F,                    // friction point arms, inverse friction 1 / 2 masses
+    DQ_FV1, DQ_FV2,                    // friction vectors
+    DQ_R1CT1, DQ_R1CT2, DQ_R2CT1, DQ_R2CT2,
+    DQ_OFV1, DQ_OFV2,                  // previous friction vectors (warm start)
+    DQ_ROWS
+};
+struct __align__(16) DynManifoldRec {
+    float4 q[DQ_ROWS];
+    float4 mut;   // friction 1, friction 2, twist impulses; w: scheduling level
 };
 
-struct DynPointRec {
-    float r1[3], depth;
-    float r2[3], inv_mass;
-    float normal[3], restitution_bias;
-    float i1[3], impulse;
-    float i2[3], split_impulse;
-    uint32_t resting, pad[3];
+enum DynPointRow { DP_R1 = 0, DP_R2, DP_N, DP_I1, DP_I2, DP_ROWS };  // (r1, depth), (r2, inverse mass), (n, restitution bias)
+struct __align__(16) DynPointRec {
+    float4 q[DP_ROWS];
+    float4 mut;   // penetration impulse, split impulse, resting (1 / 0)
 };
+
+// Kernel 3b stages an island's schedule and its movable bodies' velocities
+// in the shared memory of the warp that solves it, when they fit.
+constexpr uint32_t STAGE_BODIES = 256;
+constexpr uint32_t STAGE_MANIFOLDS = 512;
+constexpr int LARGE_WARPS = 3;                 // warps per CTA of kernel 3b (2 CTAs per SM)
+constexpr size_t LARGE_WARP_SMEM = 34816;      // bytes of shared memory per warp
 
 struct DynArgs {
     // params
@@ -72,9 +80,16 @@ struct DynArgs {
     float4 *cv, *cw, *sv, *sw;
     DynManifoldRec* mrec;
     DynPointRec* prec;
+    uint32_t* level;       // nm: level starts per island (scratch)
+    uint32_t* order;       // nm: island manifolds sorted by level (scratch)
+    uint32_t* body_level;  // nb: last level of each movable body (scratch)
+    int32_t* body_slot;    // nb: shared-memory slot of each movable body (scratch)
+    uint32_t* counters;    // [0] big islands queued (front of large_list), [1] islands taken, [2] others queued (back)
+    uint32_t* large_list;  // ni: queued islands
+    uint32_t large_ctas;   // grid of kernel 3b (persistent)
 };
 
-// Launches the five kernels in order on stream s; *launches += 5.
+// Launches the kernels in order on stream s; *launches counts them.
 cudaError_t launch_dynamics(const DynArgs& a, cudaStream_t s, uint64_t* launches);
 
 }  // namespace rp3dg

@@ -933,7 +933,13 @@ int rp3dg_dynamics_step_device(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, 
     const size_t vel_bytes = al(size_t(b->n) * 16);
     const size_t off_m = 4 * vel_bytes;
     const size_t off_p = off_m + al(size_t(m->n) * sizeof(rp3dg::DynManifoldRec));
-    const size_t need = off_p + al(size_t(p->n) * sizeof(rp3dg::DynPointRec)) + 256;
+    const size_t off_lev = off_p + al(size_t(p->n) * sizeof(rp3dg::DynPointRec));
+    const size_t off_ord = off_lev + al(size_t(m->n) * 4);
+    const size_t off_blev = off_ord + al(size_t(m->n) * 4);
+    const size_t off_bslot = off_blev + al(size_t(b->n) * 4);
+    const size_t off_cnt = off_bslot + al(size_t(b->n) * 4);
+    const size_t off_list = off_cnt + 256;
+    const size_t need = off_list + al(size_t(is->n) * 4) + 256;
     rc = grow(ctx, &ctx->d_dyn, &ctx->cap_dyn, need, "cudaMalloc(dynamics scratch)");
     if (rc) return rc;
     char* s = static_cast<char*>(ctx->d_dyn);
@@ -984,6 +990,13 @@ int rp3dg_dynamics_step_device(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, 
     a.sw = reinterpret_cast<float4*>(s + 3 * vel_bytes);
     a.mrec = reinterpret_cast<rp3dg::DynManifoldRec*>(s + off_m);
     a.prec = reinterpret_cast<rp3dg::DynPointRec*>(s + off_p);
+    a.level = reinterpret_cast<uint32_t*>(s + off_lev);
+    a.order = reinterpret_cast<uint32_t*>(s + off_ord);
+    a.body_level = reinterpret_cast<uint32_t*>(s + off_blev);
+    a.body_slot = reinterpret_cast<int32_t*>(s + off_bslot);
+    a.counters = reinterpret_cast<uint32_t*>(s + off_cnt);
+    a.large_list = reinterpret_cast<uint32_t*>(s + off_list);
+    a.large_ctas = uint32_t(ctx->num_sms) * 2;
     cudaError_t e = rp3dg::launch_dynamics(a, ctx->stream, &ctx->launches);
     return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "dynamics launch");
 }
