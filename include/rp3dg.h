@@ -199,9 +199,12 @@ int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch
                            const rp3dg_contact_batch* out, int clip_with_previous_axis);
 
 /* Device-side error bits accumulated by the kernels since the last clear
- * (bit 0: a pair named a shape outside the shape table; such pairs are
- * reported as not colliding; bit 1: a GJK run hit the 1024-iteration safety
- * bound).  Synchronizes the context stream. */
+ * (bit 0: a pair or collider named a shape outside the shape table; such
+ * pairs are reported as not colliding; bit 1: a GJK run hit the
+ * 1024-iteration safety bound; bit 2: a dynamics-stage index or range was
+ * out of bounds and that manifold, island or collider was skipped; bit 3: a
+ * broad-phase group id was not below nb_groups).  Synchronizes the context
+ * stream. */
 int rp3dg_device_errors(rp3dg_ctx* ctx, uint32_t* flags, int clear);
 
 /* ---- learned separating-axis proposal ----------------------------------
@@ -378,6 +381,53 @@ int rp3dg_dynamics_step_device(rp3dg_ctx* ctx, const rp3dg_dynamics_params* para
 int rp3dg_dynamics_step_host(rp3dg_ctx* ctx, const rp3dg_dynamics_params* params, const rp3dg_bodies* bodies,
                              const rp3dg_colliders* colliders, const rp3dg_manifolds* manifolds,
                              const rp3dg_points* points, const rp3dg_islands* islands);
+
+/* ---- broad phase ------------------------------------------------------ */
+
+/* Colliders in the broad phase.  rp3dg_broadphase_update_device restates
+ * BroadPhaseSystem::updateCollidersComponents (src/systems/BroadPhaseSystem.cpp:
+ * 155-185): the world AABB of each collider from its shape
+ * (CollisionShape::computeTransformedAABB, CollisionShape.cpp:54-90; spheres
+ * SphereShape.cpp:49-58) and the fat-AABB update of
+ * DynamicAABBTree::updateObject (DynamicAABBTree.cpp:186-214: kept while it
+ * contains the new AABB, else the new AABB grown by 4% of its extent per
+ * side), bit-identical.  rp3dg_broadphase_pairs_device returns the set the
+ * reference's overlapping pairs hold after its broad phase
+ * (CollisionDetectionSystem::computeBroadPhase / updateOverlappingPairs /
+ * removeNonOverlappingPairs, CollisionDetectionSystem.cpp:103-343): every
+ * pair of colliders of different bodies in the same group whose fat AABBs
+ * overlap (AABB::testCollision, inclusive) and whose category / mask bits
+ * accept each other, as (lower, higher) collider index.  The reference's
+ * no-collision body pairs (joints with collision disabled) are not applied.
+ * The order of the pairs is deterministic but is not the reference's (which
+ * follows its tree). */
+typedef struct rp3dg_broadphase {
+    uint32_t n;                           /* colliders in the broad phase */
+    uint32_t n_update;                    /* colliders [0, n_update) get new AABBs (the enabled ones) */
+    uint32_t nb_groups;                   /* worlds; 0 or 1 = one world (group may be NULL) */
+    const int32_t* shape;                 /* shape-table index of each collider */
+    const int32_t* body;                  /* body of each collider */
+    const int32_t* group;                 /* world of each collider, 0..nb_groups-1, or NULL */
+    const uint16_t* category;             /* collision category bits, or NULL (0xffff) */
+    const uint16_t* mask;                 /* collide-with mask bits, or NULL (0xffff) */
+    const rp3dg_float4* world_position;   /* local-to-world transform of each collider */
+    const rp3dg_float4* world_orientation;
+    const uint8_t* force_reinsert;        /* the shape changed size, or NULL */
+    rp3dg_float4* fat_min;                /* in/out: fat AABB of each collider */
+    rp3dg_float4* fat_max;
+    uint8_t* moved;                       /* out, n_update: 1 = reinserted (BroadPhaseSystem::mMovedShapes) */
+} rp3dg_broadphase;
+
+int rp3dg_broadphase_update_device(rp3dg_ctx* ctx, const rp3dg_broadphase* bp);
+/* Pairs on device arrays: pairs (2 x capacity int32) receives up to capacity
+ * pairs; *count (device) the number found (may exceed capacity).  axis 0, 1
+ * or 2 is the sweep axis. */
+int rp3dg_broadphase_pairs_device(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, int axis, int32_t* pairs,
+                                  uint32_t capacity, uint32_t* count);
+/* The same on host arrays (fat_min, fat_max, body, group, category, mask);
+ * *count is written on the host.  Synchronous. */
+int rp3dg_broadphase_pairs_host(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, int axis, int32_t* pairs,
+                                uint32_t capacity, uint32_t* count);
 
 /* Number of kernels this context launched so far (instrumentation; a
  * convex-polyhedron batch takes two). */

@@ -245,11 +245,85 @@ void capture_contacts(World& W, const std::string& pre, const std::vector<uint32
     }
 }
 
+// Fat AABB of every collider component (zeros for colliders outside the
+// broad phase), by collider index.
+void capture_fat(World& W, const std::string& pre) {
+    PhysicsWorld& w = *W.world;
+    ColliderComponents& cc = w.mCollidersComponents;
+    const DynamicAABBTree& tree = w.mCollisionDetection.mBroadPhaseSystem.mDynamicAABBTree;
+    std::vector<float> mn, mx;
+    for (uint32 i = 0; i < cc.getNbComponents(); i++) {
+        const int32 id = cc.mBroadPhaseIds[i];
+        if (id >= 0) {
+            const AABB& a = tree.getFatAABB(id);
+            f4(mn, a.getMin()); f4(mx, a.getMax());
+        } else {
+            f4(mn, Vector3(0, 0, 0)); f4(mx, Vector3(0, 0, 0));
+        }
+    }
+    W.cap.put(pre + "fat_min", mn);
+    W.cap.put(pre + "fat_max", mx);
+}
+
+// Static broad-phase data of the colliders: shape (kind as in rp3dg.h: 0
+// sphere, 1 capsule, 2 box; params), local bounds, filter bits, broad-phase id.
+void capture_bp_static(World& W) {
+    PhysicsWorld& w = *W.world;
+    ColliderComponents& cc = w.mCollidersComponents;
+    std::vector<float> shape, lmin, lmax;
+    std::vector<int32_t> bits, bpid;
+    for (uint32 i = 0; i < cc.getNbComponents(); i++) {
+        const CollisionShape* cs = cc.mCollisionShapes[i];
+        float kind = -1, p0 = 0, p1 = 0, p2 = 0;
+        switch (cs->getName()) {
+            case CollisionShapeName::SPHERE: kind = 0; p0 = float(static_cast<const SphereShape*>(cs)->getRadius()); break;
+            case CollisionShapeName::CAPSULE:
+                kind = 1; p0 = float(static_cast<const CapsuleShape*>(cs)->getRadius());
+                p1 = float(static_cast<const CapsuleShape*>(cs)->mHalfHeight); break;
+            case CollisionShapeName::BOX: {
+                kind = 2; const Vector3 h = static_cast<const BoxShape*>(cs)->getHalfExtents();
+                p0 = float(h.x); p1 = float(h.y); p2 = float(h.z); break;
+            }
+            default: break;
+        }
+        shape.push_back(p0); shape.push_back(p1); shape.push_back(p2); shape.push_back(kind);
+        const AABB lb = cs->getLocalBounds();
+        f4(lmin, lb.getMin()); f4(lmax, lb.getMax());
+        bits.push_back(int32_t(cc.mCollisionCategoryBits[i]));
+        bits.push_back(int32_t(cc.mCollideWithMaskBits[i]));
+        bpid.push_back(cc.mBroadPhaseIds[i]);
+    }
+    W.cap.put("bp_shape", shape);
+    W.cap.put("bp_local_min", lmin);
+    W.cap.put("bp_local_max", lmax);
+    W.cap.put("bp_bits", bits);
+    W.cap.put("bp_id", bpid);
+}
+
+// Every overlapping pair (enabled and disabled arrays) as (lower, higher)
+// collider index.
+void capture_pairs(World& W, const std::string& name) {
+    PhysicsWorld& w = *W.world;
+    ColliderComponents& cc = w.mCollidersComponents;
+    OverlappingPairs& op = w.mCollisionDetection.mOverlappingPairs;
+    std::vector<int32_t> out;
+    auto add = [&](const OverlappingPairs::OverlappingPair& p) {
+        const int32_t a = int32_t(cc.getEntityIndex(p.collider1)), b = int32_t(cc.getEntityIndex(p.collider2));
+        out.push_back(a < b ? a : b);
+        out.push_back(a < b ? b : a);
+    };
+    for (uint32 i = 0; i < op.mConvexPairs.size(); i++) add(op.mConvexPairs[i]);
+    for (uint32 i = 0; i < op.mDisabledConvexPairs.size(); i++) add(op.mDisabledConvexPairs[i]);
+    W.cap.put(name, out);
+}
+
 }  // namespace
 
 extern "C" {
 
-// kind 0: boxes only; 1: boxes, spheres and capsules.  Returns a world id.
+// kind 0: boxes only; 1: boxes, spheres and capsules.  variety bit 0: random
+// materials, dampings, locks, kinematic bodies...; bit 1: collision filters.
+// Returns a world id.
 int ref_world_create(int kind, uint64_t seed, int nx, int ny, int nz, float spacing, int variety) {
     auto W = std::make_unique<World>();
     PhysicsWorld::WorldSettings s;
@@ -261,7 +335,7 @@ int ref_world_create(int kind, uint64_t seed, int nx, int ny, int nz, float spac
     RigidBody* ground = W->world->createRigidBody(Transform(Vector3(0, decimal(-0.25), 0), Quaternion::identity()));
     ground->setType(BodyType::STATIC);
     Collider* gc = ground->addCollider(W->common.createBoxShape(Vector3(25, decimal(0.25), 25)), Transform::identity());
-    if (variety) gc->getMaterial().setFrictionCoefficient(decimal(0.6));
+    if (variety & 1) gc->getMaterial().setFrictionCoefficient(decimal(0.6));
     W->bodies.push_back(ground);
     int count = 0;
     for (int iy = 0; iy < ny; iy++)
@@ -277,12 +351,12 @@ int ref_world_create(int kind, uint64_t seed, int nx, int ny, int nz, float spac
                 else if (shape == 1) cs = W->common.createSphereShape(U(0.2, 0.5));
                 else cs = W->common.createCapsuleShape(decimal(0.2), decimal(0.6));
                 Collider* c = b->addCollider(cs, Transform::identity());
-                if (variety) {
+                if (variety & 1) {
                     c->getMaterial().setFrictionCoefficient(U(0.1, 1.0));
                     c->getMaterial().setBounciness(U(0.0, 0.6));
                 }
                 b->updateMassPropertiesFromColliders();
-                if (variety) {
+                if (variety & 1) {
                     const int k = count % 23;
                     if (k == 3) b->setLinearDamping(U(0.0, 0.5));
                     if (k == 4) b->setAngularDamping(U(0.0, 0.5));
@@ -295,6 +369,11 @@ int ref_world_create(int kind, uint64_t seed, int nx, int ny, int nz, float spac
                         b->setType(BodyType::KINEMATIC);
                         b->setLinearVelocity(Vector3(U(-0.5, 0.5), 0, U(-0.5, 0.5)));
                     }
+                }
+                if (variety & 2) {
+                    // collision filtering: categories 1, 2, 4; every 3rd collider ignores category 2
+                    c->setCollisionCategoryBits((unsigned short)(1u << (count % 3)));
+                    if (count % 3 == 0) c->setCollideWithMaskBits((unsigned short)(0xffffu & ~2u));
                 }
                 W->bodies.push_back(b);
                 count++;
@@ -331,7 +410,10 @@ int ref_world_capture(int id, float dt) {
     PhysicsWorld& w = *W.world;
     W.cap.f.clear();
     const decimal timeStep = decimal(dt);
+    capture_bp_static(W);
+    capture_fat(W, "bp_start_");
     w.mCollisionDetection.computeCollisionDetection();
+    capture_pairs(W, "bp_pairs");
     w.createIslands();
     w.mCollisionDetection.createContacts();
     w.mCollisionDetection.reportContactsAndTriggers();
@@ -356,7 +438,18 @@ int ref_world_capture(int id, float dt) {
     capture_state(W, "out_", false);
     capture_contacts(W, "out_", order, false);
 
+    capture_fat(W, "bp_in_");
     w.mCollisionDetection.updateColliders();
+    capture_fat(W, "bp_out_");
+    {
+        // colliders reinserted by this update (BroadPhaseSystem::mMovedShapes)
+        ColliderComponents& cc = w.mCollidersComponents;
+        std::vector<uint8_t> moved(cc.getNbComponents(), 0);
+        const Set<int>& ms = w.mCollisionDetection.mBroadPhaseSystem.mMovedShapes;
+        for (uint32 i = 0; i < cc.getNbComponents(); i++)
+            if (cc.mBroadPhaseIds[i] >= 0 && ms.contains(cc.mBroadPhaseIds[i])) moved[i] = 1;
+        W.cap.put("bp_moved", moved);
+    }
     if (w.mIsSleepingEnabled) w.updateSleepingBodies(timeStep);
     w.mDynamicsSystem.resetBodiesForceAndTorque();
     w.mIslands.clear();

@@ -2067,3 +2067,82 @@ int rp3do_dynamics_step(const rp3dg_dynamics_params* pr, const rp3dg_bodies* B, 
     free(cv); free(cw); free(sv); free(sw); free(man); free(pt);
     return 0;
 }
+
+/* ===================================================================== */
+/* Broad phase: collider AABBs and fat AABBs (BroadPhaseSystem.cpp:       */
+/* 155-185, CollisionShape.cpp:54-90, SphereShape.cpp:49-58,              */
+/* DynamicAABBTree.cpp:186-214), and the overlapping-pair set             */
+/* (CollisionDetectionSystem.cpp:270-343 with DynamicAABBTree.cpp:589-638) */
+/* ===================================================================== */
+
+/* CollisionShape::getLocalBounds of the shape kinds of rp3dg.h */
+static void local_bounds(const rp3dg_shape* s, const float* mesh_bounds, v3* mn, v3* mx) {
+    const float* p = s->params;
+    switch (s->kind) {
+        case RP3DG_SHAPE_SPHERE: *mn = V(-p[0], -p[0], -p[0]); *mx = V(p[0], p[0], p[0]); break;
+        case RP3DG_SHAPE_CAPSULE: *mn = V(-p[0], -p[1] - p[0], -p[0]); *mx = V(p[0], p[1] + p[0], p[0]); break;
+        case RP3DG_SHAPE_BOX: *mn = V(-p[0], -p[1], -p[2]); *mx = V(p[0], p[1], p[2]); break;
+        default: *mn = V(mesh_bounds[0], mesh_bounds[1], mesh_bounds[2]); *mx = V(mesh_bounds[3], mesh_bounds[4], mesh_bounds[5]); break;
+    }
+}
+
+int rp3do_broadphase_update(const rp3dg_shape* shapes, const float* mesh_bounds, uint32_t n, const int32_t* shape,
+                            const rp3dg_float4* wpos, const rp3dg_float4* wori, const uint8_t* force,
+                            rp3dg_float4* fat_min, rp3dg_float4* fat_max, uint8_t* moved) {
+    for (uint32_t i = 0; i < n; i++) {
+        const rp3dg_shape* s = &shapes[shape[i]];
+        v3 t = L4(wpos[i]);
+        v3 amin, amax;
+        if (s->kind == RP3DG_SHAPE_SPHERE) {
+            v3 e = V(s->params[0], s->params[0], s->params[0]);
+            amin = vsub(t, e); amax = vadd(t, e);
+        } else {
+            v3 lmn, lmx;
+            local_bounds(s, mesh_bounds ? mesh_bounds + 6 * (s->mesh < 0 ? 0 : s->mesh) : NULL, &lmn, &lmx);
+            float m[9];
+            q_matrix(Q(wori[i].x, wori[i].y, wori[i].z, wori[i].w), m);
+            float rmin[3], rmax[3], tt[3] = {t.x, t.y, t.z}, bmin[3] = {lmn.x, lmn.y, lmn.z}, bmax[3] = {lmx.x, lmx.y, lmx.z};
+            for (int a = 0; a < 3; a++) {
+                rmin[a] = tt[a]; rmax[a] = tt[a];
+                for (int b = 0; b < 3; b++) {
+                    float e = m[3 * a + b] * bmin[b], f = m[3 * a + b] * bmax[b];
+                    if (e < f) { rmin[a] += e; rmax[a] += f; }
+                    else { rmin[a] += f; rmax[a] += e; }
+                }
+            }
+            amin = V(rmin[0], rmin[1], rmin[2]); amax = V(rmax[0], rmax[1], rmax[2]);
+        }
+        v3 fmn = L4(fat_min[i]), fmx = L4(fat_max[i]);
+        int inside = fmn.x <= amin.x && fmn.y <= amin.y && fmn.z <= amin.z &&
+                     fmx.x >= amax.x && fmx.y >= amax.y && fmx.z >= amax.z;
+        if ((!force || !force[i]) && inside) { moved[i] = 0; continue; }
+        v3 ext = vsub(amax, amin);
+        v3 gap = vmul(vmul(ext, 0.08f), 0.5f);   /* DYNAMIC_TREE_FAT_AABB_INFLATE_PERCENTAGE (configuration.h:131) */
+        fat_min[i] = S4(vsub(amin, gap));
+        fat_max[i] = S4(vadd(amax, gap));
+        moved[i] = 1;
+    }
+    return 0;
+}
+
+/* All pairs (i < j) whose fat AABBs overlap (AABB::testCollision, inclusive),
+ * of different bodies and the same group, passing the category / mask
+ * filter.  Writes up to cap pairs, returns the count (may exceed cap). */
+long rp3do_broadphase_pairs(uint32_t n, const rp3dg_float4* fat_min, const rp3dg_float4* fat_max, const int32_t* body,
+                            const int32_t* group, const uint16_t* category, const uint16_t* mask, int32_t* pairs,
+                            long cap) {
+    long count = 0;
+    for (uint32_t i = 0; i < n; i++)
+        for (uint32_t j = i + 1; j < n; j++) {
+            if (group && group[i] != group[j]) continue;
+            const rp3dg_float4 a0 = fat_min[i], a1 = fat_max[i], b0 = fat_min[j], b1 = fat_max[j];
+            if (a1.x < b0.x || b1.x < a0.x) continue;
+            if (a1.y < b0.y || b1.y < a0.y) continue;
+            if (a1.z < b0.z || b1.z < a0.z) continue;
+            if (body[i] == body[j]) continue;
+            if (category && mask && (!(mask[i] & category[j]) || !(category[i] & mask[j]))) continue;
+            if (count < cap) { pairs[2 * count] = (int32_t)i; pairs[2 * count + 1] = (int32_t)j; }
+            count++;
+        }
+    return count;
+}

@@ -42,6 +42,18 @@ int rp3do_dynamics_step(const rp3dg_dynamics_params* params, const rp3dg_bodies*
                         const rp3dg_colliders* colliders, const rp3dg_manifolds* manifolds,
                         const rp3dg_points* points, const rp3dg_islands* islands);
 
+/* Broad phase: world AABB of each collider from its shape and local-to-world
+ * transform, then the fat-AABB update (moved = reinserted); mesh_bounds holds
+ * 6 floats (min, max) per convex-mesh instance, scaled. */
+int rp3do_broadphase_update(const rp3dg_shape* shapes, const float* mesh_bounds, uint32_t n, const int32_t* shape,
+                            const rp3dg_float4* world_position, const rp3dg_float4* world_orientation,
+                            const uint8_t* force_reinsert, rp3dg_float4* fat_min, rp3dg_float4* fat_max,
+                            uint8_t* moved);
+/* Overlapping pairs (i < j) of fat AABBs, brute force. */
+long rp3do_broadphase_pairs(uint32_t n, const rp3dg_float4* fat_min, const rp3dg_float4* fat_max, const int32_t* body,
+                            const int32_t* group, const uint16_t* category, const uint16_t* mask, int32_t* pairs,
+                            long cap);
+
 #ifdef __cplusplus
 }
 #endif

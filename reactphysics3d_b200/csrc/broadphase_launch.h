@@ -1,0 +1,44 @@
+// Launch interface of the broad-phase kernels (broadphase.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/rp3dg.h"
+
+namespace rp3dg {
+
+struct BpArgs {
+    uint32_t n;           // colliders in the broad phase
+    uint32_t n_update;    // colliders [0, n_update) get new AABBs
+    uint32_t nb_shapes;
+    const rp3dg_shape* shapes;
+    const float4* bounds;   // 2 per shape: local bounds min, max (CollisionShape::getLocalBounds)
+    const int32_t* shape;
+    const float4 *wpos, *wori;
+    const uint8_t* force;
+    float4 *fat_min, *fat_max;
+    uint8_t* moved;
+    uint32_t* error;
+    // pair search
+    const int32_t* group;
+    const int32_t* body;
+    const uint16_t *category, *mask;
+    int group_bits;
+    unsigned long long *keys, *keys_tmp;
+    uint32_t *vals, *vals_tmp;
+    uint32_t* sort_hist;
+    float4 *s_lo, *s_hi;
+    int32_t* s_group;
+    uint32_t* pair_offset;
+    int32_t* pairs;
+    uint32_t capacity;
+    uint32_t* pair_count;
+};
+
+cudaError_t launch_bp_update(const BpArgs& a, cudaStream_t s, uint64_t* launches);
+cudaError_t launch_bp_pairs(const BpArgs& a, int axis, cudaStream_t s, uint64_t* launches);
+// uint32 words of sort histogram scratch for n keys
+size_t sort_scratch_words(uint32_t n);
+
+}  // namespace rp3dg

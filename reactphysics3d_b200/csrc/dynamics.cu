@@ -26,8 +26,6 @@ constexpr float SLOP = 0.01f;              // :45
 
 RD v3 L3(const float4 a) { return V(a.x, a.y, a.z); }
 RD float4 F4(v3 a, float w = 0.0f) { return make_float4(a.x, a.y, a.z, w); }
-RD v3 A3(const float* a) { return V(a[0], a[1], a[2]); }
-RD void S3(float* a, v3 v) { a[0] = v.x; a[1] = v.y; a[2] = v.z; }
 
 // Matrix3x3 * Vector3 (Matrix3x3.h:324-331), row-major m[9]
 RD v3 mv(const float* m, v3 v) {
@@ -503,13 +501,6 @@ RD void store_manifold(const DynArgs& a, uint32_t mi) {
     a.m_fimp[mi] = make_float4(mut.x, mut.y, mut.z, 0.0f);
     a.m_fv1[mi] = F4(c.fv1);
     a.m_fv2[mi] = F4(c.fv2);
-}
-
-RD void man_bodies(const DynArgs& a, uint32_t mi, int32_t& b1, int32_t& b2, uint32_t& fixed, bool& valid) {
-    const float4 ids = __ldg(a.mrec[mi].q + DQ_IDS), ms = __ldg(a.mrec[mi].q + DQ_MASS);
-    b1 = __float_as_int(ids.x); b2 = __float_as_int(ids.y);
-    valid = __float_as_int(ids.z) != 0;
-    fixed = uint32_t(ms.w);
 }
 
 // ---- kernel 3: warm start, velocity iterations, stored impulses ----------

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/rp3dg.h"
+#include "broadphase_launch.h"
 #include "contacts_launch.h"
 #include "dynamics_launch.h"
 #include "mlp_launch.h"
@@ -208,6 +209,14 @@ struct rp3dg_ctx {
     // staging buffers for rp3dg_dynamics_step_host
     void* d_dyn_stage = nullptr;
     size_t cap_dyn_stage = 0;
+    // broad phase: local bounds of every shape (min, max float4 pairs),
+    // pair-search scratch and host-call staging
+    float* d_shape_bounds = nullptr;
+    uint32_t cap_shape_bounds = 0;
+    void* d_bp = nullptr;
+    size_t cap_bp = 0;
+    void* d_bp_stage = nullptr;
+    size_t cap_bp_stage = 0;
 };
 
 namespace {
@@ -333,6 +342,9 @@ void rp3dg_destroy(rp3dg_ctx* ctx) {
     cudaFree(ctx->d_proposals);
     cudaFree(ctx->d_dyn);
     cudaFree(ctx->d_dyn_stage);
+    cudaFree(ctx->d_shape_bounds);
+    cudaFree(ctx->d_bp);
+    cudaFree(ctx->d_bp_stage);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -475,8 +487,45 @@ int rp3dg_set_shapes(rp3dg_ctx* ctx, const rp3dg_shape* shapes, uint32_t nb) {
         if (e != cudaSuccess) { ctx->cap_shapes = 0; return cuda_fail(ctx, e, "cudaMalloc(shapes)"); }
         ctx->cap_shapes = nb;
     }
+    // local bounds of every shape (CollisionShape::getLocalBounds): sphere
+    // (BoxShape.cpp:149-151, SphereShape.h:160-164, CapsuleShape.cpp:90-94),
+    // convex mesh: the mesh's vertex bounds (ConvexMesh.cpp:83-99) times the
+    // scale (ConvexMeshShape.cpp:208-212, AABB::applyScale)
+    std::vector<float> bounds(size_t(nb) * 8, 0.0f);
+    for (uint32_t i = 0; i < nb; i++) {
+        const rp3dg_shape& sh = shapes[i];
+        const float* p = sh.params;
+        float* b = &bounds[8 * size_t(i)];
+        switch (sh.kind) {
+            case RP3DG_SHAPE_SPHERE: b[0] = -p[0]; b[1] = -p[0]; b[2] = -p[0]; b[4] = p[0]; b[5] = p[0]; b[6] = p[0]; break;
+            case RP3DG_SHAPE_CAPSULE:
+                b[0] = -p[0]; b[1] = -p[1] - p[0]; b[2] = -p[0]; b[4] = p[0]; b[5] = p[1] + p[0]; b[6] = p[0]; break;
+            case RP3DG_SHAPE_BOX: b[0] = -p[0]; b[1] = -p[1]; b[2] = -p[2]; b[4] = p[0]; b[5] = p[1]; b[6] = p[2]; break;
+            default: {
+                const MeshInstance& in = ctx->instances[size_t(sh.mesh)];
+                const MeshTopo& m = ctx->meshes[size_t(in.mesh)];
+                float mn[3] = {m.verts[0], m.verts[1], m.verts[2]}, mx[3] = {mn[0], mn[1], mn[2]};
+                for (uint32_t v = 0; v < m.nv; v++)
+                    for (int k = 0; k < 3; k++) {
+                        const float x = m.verts[3 * v + k];
+                        if (x > mx[k]) mx[k] = x;
+                        if (x < mn[k]) mn[k] = x;
+                    }
+                for (int k = 0; k < 3; k++) { b[k] = mn[k] * in.scale[k]; b[4 + k] = mx[k] * in.scale[k]; }
+            }
+        }
+    }
+    if (nb > ctx->cap_shape_bounds) {
+        cudaFree(ctx->d_shape_bounds);
+        ctx->d_shape_bounds = nullptr;
+        cudaError_t e = cudaMalloc(&ctx->d_shape_bounds, bounds.size() * sizeof(float));
+        if (e != cudaSuccess) { ctx->cap_shape_bounds = 0; return cuda_fail(ctx, e, "cudaMalloc(shape bounds)"); }
+        ctx->cap_shape_bounds = nb;
+    }
     if (nb) {
         cudaError_t e = cudaMemcpyAsync(ctx->d_shapes, shapes, size_t(nb) * sizeof(rp3dg_shape), cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ctx->d_shape_bounds, bounds.data(), bounds.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "upload shapes");
     }
@@ -1068,4 +1117,152 @@ int rp3dg_dynamics_step_host(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, co
         if (e == cudaSuccess && r.out && r.bytes) e = cudaMemcpyAsync(r.out, d + r.off, r.bytes, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "dynamics (host arrays)");
+}
+
+// ---- broad phase -----------------------------------------------------------
+
+namespace {
+
+int check_bp(rp3dg_ctx* ctx, const rp3dg_broadphase* bp) {
+    if (!ctx || !bp) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (bp->n_update > bp->n) return fail(ctx, RP3DG_EINVAL, "n_update > n");
+    if (bp->nb_groups > 1 && !bp->group) return fail(ctx, RP3DG_EINVAL, "nb_groups > 1 needs group");
+    if (bp->n && (!bp->fat_min || !bp->fat_max)) return fail(ctx, RP3DG_EINVAL, "null fat AABB array");
+    if (!aligned(bp->fat_min, 16) || !aligned(bp->fat_max, 16) || !aligned(bp->world_position, 16) ||
+        !aligned(bp->world_orientation, 16) || !aligned(bp->shape, 4) || !aligned(bp->body, 4) ||
+        !aligned(bp->group, 4) || !aligned(bp->category, 2) || !aligned(bp->mask, 2))
+        return fail(ctx, RP3DG_EINVAL, "misaligned device array (float4 arrays need 16 bytes)");
+    return 0;
+}
+
+}  // namespace
+
+int rp3dg_broadphase_update_device(rp3dg_ctx* ctx, const rp3dg_broadphase* bp) {
+    int rc = check_bp(ctx, bp);
+    if (rc) return rc;
+    if (bp->n_update == 0) return 0;
+    if (!bp->shape || !bp->world_position || !bp->world_orientation || !bp->moved)
+        return fail(ctx, RP3DG_EINVAL, "null collider array");
+    if (!ctx->d_shapes || !ctx->d_shape_bounds) return fail(ctx, RP3DG_EINVAL, "no shape table (rp3dg_set_shapes)");
+    rp3dg::BpArgs a = {};
+    a.n = bp->n;
+    a.n_update = bp->n_update;
+    a.nb_shapes = ctx->nb_shapes;
+    a.shapes = ctx->d_shapes;
+    a.bounds = reinterpret_cast<const float4*>(ctx->d_shape_bounds);
+    a.shape = bp->shape;
+    a.wpos = reinterpret_cast<const float4*>(bp->world_position);
+    a.wori = reinterpret_cast<const float4*>(bp->world_orientation);
+    a.force = bp->force_reinsert;
+    a.fat_min = reinterpret_cast<float4*>(bp->fat_min);
+    a.fat_max = reinterpret_cast<float4*>(bp->fat_max);
+    a.moved = bp->moved;
+    a.error = ctx->d_error;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = rp3dg::launch_bp_update(a, ctx->stream, &ctx->launches);
+    return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "broad-phase update");
+}
+
+int rp3dg_broadphase_pairs_device(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, int axis, int32_t* pairs,
+                                  uint32_t capacity, uint32_t* count) {
+    int rc = check_bp(ctx, bp);
+    if (rc) return rc;
+    if (axis < 0 || axis > 2) return fail(ctx, RP3DG_EINVAL, "axis must be 0, 1 or 2");
+    if (!count || (capacity && !pairs)) return fail(ctx, RP3DG_EINVAL, "null output");
+    if (bp->n && !bp->body) return fail(ctx, RP3DG_EINVAL, "null body array");
+    if (!aligned(pairs, 4) || !aligned(count, 4)) return fail(ctx, RP3DG_EINVAL, "misaligned output");
+    const size_t n = bp->n;
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    size_t off = 0;
+    const size_t o_keys = off; off += al(n * 8);
+    const size_t o_keys2 = off; off += al(n * 8);
+    const size_t o_vals = off; off += al(n * 4);
+    const size_t o_vals2 = off; off += al(n * 4);
+    const size_t o_hist = off; off += al(rp3dg::sort_scratch_words(uint32_t(n)) * 4);
+    const size_t o_lo = off; off += al(n * 16);
+    const size_t o_hi = off; off += al(n * 16);
+    const size_t o_grp = off; off += al(n * 4);
+    const size_t o_poff = off; off += al(n * 4 + 4);
+    cudaSetDevice(ctx->device);
+    rc = grow(ctx, &ctx->d_bp, &ctx->cap_bp, off + 256, "cudaMalloc(broad-phase scratch)");
+    if (rc) return rc;
+    char* s = static_cast<char*>(ctx->d_bp);
+    rp3dg::BpArgs a = {};
+    a.n = bp->n;
+    a.fat_min = reinterpret_cast<float4*>(bp->fat_min);
+    a.fat_max = reinterpret_cast<float4*>(bp->fat_max);
+    a.group = bp->nb_groups > 1 ? bp->group : nullptr;
+    a.body = bp->body;
+    a.category = bp->category;
+    a.mask = bp->mask;
+    int bits = 0;
+    if (bp->nb_groups > 1) while (bits < 32 && (uint64_t(1) << bits) < bp->nb_groups) bits++;
+    a.group_bits = bits;
+    a.keys = reinterpret_cast<unsigned long long*>(s + o_keys);
+    a.keys_tmp = reinterpret_cast<unsigned long long*>(s + o_keys2);
+    a.vals = reinterpret_cast<uint32_t*>(s + o_vals);
+    a.vals_tmp = reinterpret_cast<uint32_t*>(s + o_vals2);
+    a.sort_hist = reinterpret_cast<uint32_t*>(s + o_hist);
+    a.s_lo = reinterpret_cast<float4*>(s + o_lo);
+    a.s_hi = reinterpret_cast<float4*>(s + o_hi);
+    a.s_group = reinterpret_cast<int32_t*>(s + o_grp);
+    a.pair_offset = reinterpret_cast<uint32_t*>(s + o_poff);
+    a.pairs = pairs;
+    a.capacity = capacity;
+    a.pair_count = count;
+    a.error = ctx->d_error;
+    cudaError_t e = rp3dg::launch_bp_pairs(a, axis, ctx->stream, &ctx->launches);
+    return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "broad-phase pairs");
+}
+
+int rp3dg_broadphase_pairs_host(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, int axis, int32_t* pairs,
+                                uint32_t capacity, uint32_t* count) {
+    if (!ctx || !bp || !count) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (bp->nb_groups > 1 && !bp->group) return fail(ctx, RP3DG_EINVAL, "nb_groups > 1 needs group");
+    const size_t n = bp->n;
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    size_t off = 0;
+    const size_t o_min = off; off += al(n * 16);
+    const size_t o_max = off; off += al(n * 16);
+    const size_t o_body = off; off += al(n * 4);
+    const size_t o_grp = off; off += al(n * 4);
+    const size_t o_cat = off; off += al(n * 2);
+    const size_t o_msk = off; off += al(n * 2);
+    const size_t o_cnt = off; off += 256;
+    const size_t o_pairs = off; off += al(size_t(capacity) * 8);
+    cudaSetDevice(ctx->device);
+    int rc = grow(ctx, &ctx->d_bp_stage, &ctx->cap_bp_stage, off + 256, "cudaMalloc(broad-phase staging)");
+    if (rc) return rc;
+    char* d = static_cast<char*>(ctx->d_bp_stage);
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaSuccess;
+    auto up = [&](size_t o, const void* src, size_t bytes) {
+        if (e == cudaSuccess && src && bytes) e = cudaMemcpyAsync(d + o, src, bytes, cudaMemcpyHostToDevice, s);
+    };
+    up(o_min, bp->fat_min, n * 16); up(o_max, bp->fat_max, n * 16);
+    up(o_body, bp->body, n * 4);
+    if (bp->nb_groups > 1) up(o_grp, bp->group, n * 4);
+    up(o_cat, bp->category, n * 2); up(o_msk, bp->mask, n * 2);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "upload broad-phase arrays");
+    rp3dg_broadphase dbp = *bp;
+    dbp.fat_min = reinterpret_cast<rp3dg_float4*>(d + o_min);
+    dbp.fat_max = reinterpret_cast<rp3dg_float4*>(d + o_max);
+    dbp.body = reinterpret_cast<const int32_t*>(d + o_body);
+    dbp.group = bp->nb_groups > 1 ? reinterpret_cast<const int32_t*>(d + o_grp) : nullptr;
+    dbp.category = bp->category ? reinterpret_cast<const uint16_t*>(d + o_cat) : nullptr;
+    dbp.mask = bp->mask ? reinterpret_cast<const uint16_t*>(d + o_msk) : nullptr;
+    dbp.shape = nullptr; dbp.world_position = nullptr; dbp.world_orientation = nullptr;
+    dbp.force_reinsert = nullptr; dbp.moved = nullptr;
+    uint32_t* dcount = reinterpret_cast<uint32_t*>(d + o_cnt);
+    int32_t* dpairs = reinterpret_cast<int32_t*>(d + o_pairs);
+    rc = rp3dg_broadphase_pairs_device(ctx, &dbp, axis, dpairs, capacity, dcount);
+    if (rc) return rc;
+    e = cudaMemcpyAsync(count, dcount, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && capacity && pairs) {
+        const size_t got = *count < capacity ? *count : capacity;
+        if (got) e = cudaMemcpyAsync(pairs, dpairs, got * 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "broad-phase pairs (host arrays)");
 }

@@ -67,6 +67,8 @@ def load_library(path=LIB_PATH):
     L.rp3dg_reduce_contacts_device.argtypes = [P, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), P]
     L.rp3dg_narrowphase_manifolds_host.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch),
                                                    C.c_int, P]
+    from . import broadphase as BP
+    BP.bind(L)
     from . import dynamics as DY
     for fn in ("rp3dg_dynamics_step_host", "rp3dg_dynamics_step_device"):
         getattr(L, fn).argtypes = [P, C.POINTER(DY.Params), C.POINTER(DY.Bodies), C.POINTER(DY.Colliders),
@@ -249,6 +251,30 @@ class Context:
         self._check(self.lib.rp3dg_narrowphase_manifolds_host(self.h, algo, C.byref(pb), C.byref(cb), int(clip),
                                                               None if kept is None else kept.ctypes.data))
         return out, kept
+
+    def broadphase_update(self, bp):
+        """Fat-AABB update on device arrays (reactphysics3d_b200.broadphase.make)."""
+        self.order_in()
+        self._check(self.lib.rp3dg_broadphase_update_device(self.h, C.byref(bp)))
+        self.order_out()
+
+    def broadphase_pairs(self, bp, capacity, axis=0, device=False):
+        """Overlapping pairs: (count, pairs (capacity x 2 int32)).  Host arrays
+        unless device is set (then pairs and the count are CUDA tensors)."""
+        if device:
+            import torch
+            pairs = torch.empty((max(capacity, 1), 2), dtype=torch.int32, device="cuda")
+            cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+            self.order_in()
+            self._check(self.lib.rp3dg_broadphase_pairs_device(self.h, C.byref(bp), axis, pairs.data_ptr(), capacity,
+                                                               cnt.data_ptr()))
+            self.order_out()
+            return cnt, pairs
+        pairs = np.zeros((max(capacity, 1), 2), np.int32)
+        cnt = C.c_uint32(0)
+        self._check(self.lib.rp3dg_broadphase_pairs_host(self.h, C.byref(bp), axis, pairs.ctypes.data, capacity,
+                                                         C.addressof(cnt)))
+        return int(cnt.value), pairs
 
     def dynamics_step(self, params, world):
         """One dynamics stage (inertia, velocities, contact solver, positions,

@@ -24,13 +24,17 @@ Writes:
                    removeDuplicatedContactPointsInManifold result ("red_"
                    arrays and the kept-slot table)
 
-  np_dynamics.npz  dynamics stage of a world step: for seeded reference
-                   worlds (oracle/ref_world.cpp: boxes, or boxes, spheres and
+  np_dynamics.npz  one captured step of seeded reference worlds
+                   (oracle/ref_world.cpp: boxes, or boxes, spheres and
                    capsules with random materials, dampings, lock factors,
-                   forces and kinematic bodies, on a static ground), the
-                   reference's own inputs and outputs of one step's
-                   inertia / velocity / contact-solver / position / state
-                   phases ("<case>/in_*", "<case>/out_*", "<case>/params")
+                   forces, kinematic bodies and collision filters, on a
+                   static ground): the reference's own inputs and outputs of
+                   the dynamics stage (inertia / velocities / contact solver /
+                   positions / state: "<case>/in_*", "<case>/out_*",
+                   "<case>/params") and of the broad phase (fat AABBs before
+                   and after the collider update, moved colliders, the
+                   overlapping pairs after the step's broad phase, shapes and
+                   filter bits: "<case>/bp_*")
 
 `python tests/golden/make_golden.py manifold` (or `dynamics`) rewrites that
 fixture only.
@@ -154,15 +158,17 @@ def synthetic_manifolds(rng, n=512):
     return pairs, c
 
 
-# (kind, seed, steps before the captured one, grid nx, ny, nz)
-DYNAMICS_CASES = [(0, 1, 60, 4, 3, 4), (1, 3, 150, 4, 3, 4), (1, 5, 300, 4, 3, 4), (0, 6, 200, 8, 4, 8),
-                  (1, 4, 40, 4, 3, 4)]
+# (kind, seed, steps before the captured one, grid nx, ny, nz, variety:
+# bit 0 random materials / dampings / locks / kinematic bodies, bit 1
+# collision category and mask filters)
+DYNAMICS_CASES = [(0, 1, 60, 4, 3, 4, 1), (1, 3, 150, 4, 3, 4, 1), (1, 5, 300, 4, 3, 4, 1), (0, 6, 200, 8, 4, 8, 1),
+                  (1, 4, 40, 4, 3, 4, 1), (1, 21, 100, 5, 3, 5, 3)]
 
 
 def dynamics_fixture():
     d = {}
-    for kind, seed, steps, nx, ny, nz in DYNAMICS_CASES:
-        w = reflib.RefWorld(kind=kind, seed=seed, nx=nx, ny=ny, nz=nz)
+    for kind, seed, steps, nx, ny, nz, variety in DYNAMICS_CASES:
+        w = reflib.RefWorld(kind=kind, seed=seed, nx=nx, ny=ny, nz=nz, variety=variety)
         w.step(n=steps)
         w.apply_forces(seed + 1)
         cap = w.capture()
