@@ -239,6 +239,11 @@ def run_ours(args):
     if not args.no_dynamics:
         dynamics = dynamics_section(ctx, args, dev, rank == 0 and world == 1 and not args.no_cpu)
 
+    broadphase = None
+    if not args.no_broadphase:
+        broadphase = broadphase_section(ctx, args, dev)
+        ctx.set_shapes(sc.shapes)   # the narrow-phase workload's table again
+
     learned = None
     if not args.no_learned:
         learned = learned_axis_section(ctx, sc, args, dev)
@@ -253,7 +258,7 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "pairs_per_gpu": sc.n_pairs, "batches": names,
                        "seed": args.seed, "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"independent pair sets per rank x{world}"},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "manifolds": manifolds, "dynamics": dynamics,
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "manifolds": manifolds, "dynamics": dynamics, "broadphase": broadphase,
             "learned_axis": learned,
             "gpu_launches": int(launches),
             "clocks": clocks, "batch_ms": {k: round(v, 4) for k, v in mean_batch.items()}}
@@ -389,6 +394,71 @@ def dynamics_section(ctx, args, dev, with_cpu):
         out["cpu_baseline"] = {"value": round(n_cpu / dt_cpu, 1), "unit": "world-steps/s", "cores": 1, "kind": "port",
                                "sample": f"{n_cpu} of the worlds, one stage, C restatement (oracle), one core"}
     return out
+
+
+def broadphase_section(ctx, args, dev):
+    """Broad phase of a single large world: 100,000 colliders (40% boxes, 30%
+    spheres, 30% capsules, sizes of the large-world workload) on a jittered
+    50 x 40 x 50 lattice with 1.5 m spacing, random orientations: the fat-AABB
+    update of every collider (after a small random displacement, so part of
+    them are reinserted) and the overlapping-pair search, device time with
+    CUDA events."""
+    import torch
+    from reactphysics3d_b200 import broadphase as BP
+    rng = np.random.default_rng(args.seed + 17)
+    nx, ny, nz = 50, 40, 50
+    n = nx * ny * nz
+    g = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"), -1).reshape(-1, 3)
+    pos = (g * 1.5 + rng.uniform(-0.1, 0.1, (n, 3))).astype(np.float32)
+    kind = rng.choice([2, 0, 1], size=n, p=[0.4, 0.3, 0.3]).astype(np.int32)
+    table = np.zeros(n, A.SHAPE_DTYPE)
+    table["kind"] = kind
+    table["params"][:, 0] = np.where(kind == 0, rng.uniform(0.2, 0.5, n), np.where(kind == 1, 0.2, rng.uniform(0.2, 0.6, n)))
+    table["params"][:, 1] = np.where(kind == 1, 0.3, rng.uniform(0.2, 0.6, n))
+    table["params"][:, 2] = rng.uniform(0.2, 0.6, n)
+    q = rng.normal(size=(n, 4)).astype(np.float32)
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    wpos = np.zeros((n, 4), np.float32); wpos[:, :3] = pos
+    ctx.set_shapes(table)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    shape, wp, wo = T(np.arange(n, dtype=np.int32)), T(wpos), T(q)
+    body = T(np.arange(n, dtype=np.int32))
+    fmin = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    fmax = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    moved = torch.zeros(n, dtype=torch.uint8, device=dev)
+    force = T(np.ones(n, np.uint8))
+    bp0 = BP.make(n, n, 0, shape=shape, body=body, world_position=wp, world_orientation=wo, force_reinsert=force,
+                  fat_min=fmin, fat_max=fmax, moved=moved)
+    ctx.broadphase_update(bp0)           # initial fat AABBs
+    wpos2 = wpos.copy()
+    wpos2[:, :3] += rng.normal(scale=0.02, size=(n, 3)).astype(np.float32)
+    wp2 = T(wpos2)
+    bp = BP.make(n, n, 0, shape=shape, body=body, world_position=wp2, world_orientation=wo, fat_min=fmin,
+                 fat_max=fmax, moved=moved)
+    fmin0, fmax0 = fmin.clone(), fmax.clone()
+    stream = ctx.torch_stream()
+    reps = max(3, min(args.steps, 20))
+    ev_u, ev_p = [], []
+    cap = 4 * n
+    with torch.cuda.stream(stream):
+        for r in range(reps + 2):
+            fmin.copy_(fmin0); fmax.copy_(fmax0)
+            a0, a1, a2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            a0.record(stream)
+            ctx.broadphase_update(bp)
+            a1.record(stream)
+            cnt, _ = ctx.broadphase_pairs(bp, cap, axis=0, device=True)
+            a2.record(stream)
+            if r >= 2:
+                ev_u.append((a0, a1)); ev_p.append((a1, a2))
+        ctx.synchronize()
+    tu = float(np.mean([x.elapsed_time(y) for x, y in ev_u]))
+    tp = float(np.mean([x.elapsed_time(y) for x, y in ev_p]))
+    return {"workload": "one world, 100,000 colliders (40% boxes, 30% spheres, 30% capsules) on a 50x40x50 "
+                        "lattice, 1.5 m spacing, 2 cm random displacement",
+            "colliders": n, "reinserted": int(moved.sum().item()), "pairs": int(cnt.item()),
+            "update_ms": round(tu, 4), "pairs_ms": round(tp, 4),
+            "colliders_per_s": round(n / ((tu + tp) / 1e3), 1)}
 
 
 def learned_axis_section(ctx, sc, args, dev):
@@ -592,6 +662,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-manifolds", action="store_true")
     ap.add_argument("--no-dynamics", action="store_true")
+    ap.add_argument("--no-broadphase", action="store_true")
     ap.add_argument("--dyn-worlds", type=int, default=4096)
     ap.add_argument("--learned-epochs", type=int, default=4)
     args = ap.parse_args()
