@@ -429,6 +429,117 @@ int rp3dg_broadphase_pairs_device(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, in
 int rp3dg_broadphase_pairs_host(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, int axis, int32_t* pairs,
                                 uint32_t capacity, uint32_t* count);
 
+/* ---- world step --------------------------------------------------------
+ * A physics world stepped like PhysicsWorld::update(decimal timeStep)
+ * (include/reactphysics3d/engine/PhysicsWorld.h:352, body
+ * src/engine/PhysicsWorld.cpp:239-307).  The floating-point work of a step
+ * runs on the GPU (world AABBs and the fat-AABB test of the broad phase, the
+ * narrow phase, the manifold step, warm starting, inertia, velocity
+ * integration, the contact solver, position integration); the host keeps the
+ * order-defining bookkeeping of the reference (its dynamic AABB tree topology,
+ * the moved-collider set, the persistent overlapping-pair arrays, contact-pair
+ * order, islands, component order and sleeping) so that every step processes
+ * pairs, contacts and constraints in the reference's own order and the results
+ * are the reference float build's, bit for bit.  Worlds without joints, with
+ * convex colliders (sphere, capsule, box, convex mesh), simulation colliders
+ * only (no triggers), are supported.
+ *
+ * rp3dg_world_create mirrors this sequence of reference calls, body by body:
+ *   b = world->createRigidBody(Transform(position, orientation));
+ *   for each collider c of the body, in order:
+ *       c = b->addCollider(shape, Transform(local position, local orientation));
+ *       c->getMaterial().setFrictionCoefficient / setBounciness / setMassDensity;
+ *       c->setCollisionCategoryBits(category); c->setCollideWithMaskBits(mask);
+ *   if (type == DYNAMIC) b->updateMassPropertiesFromColliders(); else b->setType(type);
+ *   b->setLinearDamping; setAngularDamping; setLinearLockAxisFactor;
+ *   setAngularLockAxisFactor; enableGravity; setIsAllowedToSleep;
+ *   if (type != STATIC) { b->setLinearVelocity; b->setAngularVelocity; }
+ * Colliders are given grouped by body, bodies in ascending order. */
+#define RP3DG_BODY_STATIC 0     /* BodyType::STATIC (RigidBody.h) */
+#define RP3DG_BODY_KINEMATIC 1
+#define RP3DG_BODY_DYNAMIC 2
+
+typedef struct rp3dg_world_settings {      /* PhysicsWorld::WorldSettings (PhysicsWorld.h:80-140) */
+    float gravity[3];                       /* (0, -9.81, 0) */
+    int32_t velocity_iterations;            /* defaultVelocitySolverNbIterations, 6 */
+    int32_t sleeping_enabled;               /* isSleepingEnabled, 1 */
+    float sleep_linear_velocity;            /* defaultSleepLinearVelocity, 0.02 */
+    float sleep_angular_velocity;           /* defaultSleepAngularVelocity, 3 degrees/s in rad/s */
+    float time_before_sleep;                /* defaultTimeBeforeSleep, 1 */
+    float restitution_velocity_threshold;   /* 0.5 */
+    float persistent_contact_distance_threshold; /* 0.03 */
+    float cos_angle_similar_contact_manifold;    /* 0.95 */
+} rp3dg_world_settings;
+
+typedef struct rp3dg_body_desc {
+    int32_t type;                  /* RP3DG_BODY_* */
+    float position[3];
+    float orientation[4];          /* unit quaternion (x, y, z, w) */
+    float linear_velocity[3];
+    float angular_velocity[3];
+    float linear_damping;
+    float angular_damping;
+    float linear_lock[3];          /* lock-axis factors, (1, 1, 1) = free */
+    float angular_lock[3];
+    int32_t gravity_enabled;
+    int32_t allowed_to_sleep;
+} rp3dg_body_desc;
+
+typedef struct rp3dg_collider_desc {
+    int32_t body;                  /* body index */
+    int32_t shape;                 /* index into the context's shape table */
+    float position[3];             /* local-to-body transform */
+    float orientation[4];
+    float friction;                /* Material::setFrictionCoefficient */
+    float bounciness;              /* Material::setBounciness */
+    float mass_density;            /* Material::setMassDensity */
+    uint16_t category;             /* collision category bits (0x0001 by default) */
+    uint16_t mask;                 /* collide-with mask bits (0xffff by default) */
+} rp3dg_collider_desc;
+
+typedef struct rp3dg_world rp3dg_world;
+
+typedef struct rp3dg_world_stats {
+    uint32_t overlapping_pairs;    /* enabled convex overlapping pairs after the broad phase */
+    uint32_t disabled_pairs;       /* pairs of two sleeping / static bodies */
+    uint32_t narrowphase_tests;    /* pairs tested by the narrow phase this step */
+    uint32_t contact_pairs;        /* colliding pairs */
+    uint32_t manifolds;            /* contact manifolds given to the solver */
+    uint32_t contact_points;
+    uint32_t islands;
+    uint32_t enabled_bodies;       /* awake non-static bodies after the step */
+    uint32_t moved_colliders;      /* colliders reinserted in the broad-phase tree by the step */
+    uint32_t reserved;
+} rp3dg_world_stats;
+
+/* Build a world on ctx's device (the shape table must be set).  The world
+ * keeps pointers to nothing the caller owns. */
+int rp3dg_world_create(rp3dg_ctx* ctx, const rp3dg_world_settings* settings, const rp3dg_body_desc* bodies,
+                       uint32_t nb_bodies, const rp3dg_collider_desc* colliders, uint32_t nb_colliders,
+                       rp3dg_world** out);
+void rp3dg_world_destroy(rp3dg_world* world);
+/* PhysicsWorld::update(dt): one step (synchronous). */
+int rp3dg_world_update(rp3dg_world* world, float dt);
+/* Body state in creation order (host arrays of nb_bodies rows, any may be
+ * NULL): position (x, y, z), orientation (x, y, z, w), linear and angular
+ * velocity (x, y, z), sleeping flag. */
+int rp3dg_world_get_bodies(rp3dg_world* world, float* position, float* orientation, float* linear_velocity,
+                           float* angular_velocity, uint8_t* sleeping);
+/* Overlapping-pair ids (pairNumbers of the two broad-phase ids,
+ * mathematics_functions.h:428-433) in the reference's array order: enabled
+ * pairs (OverlappingPairs::mConvexPairs) then disabled ones
+ * (mDisabledConvexPairs).  *n receives the total; at most capacity are
+ * written. */
+int rp3dg_world_get_pairs(rp3dg_world* world, uint64_t* pair_ids, uint32_t capacity, uint32_t* n);
+/* Contact manifolds of the last step in the solver's order: per manifold the
+ * creation indices of body 1 and body 2 and the number of points (host
+ * arrays, capacity rows); per point (capacity_points rows, may be NULL)
+ * normal + penetration depth and the two local points as float4. */
+int rp3dg_world_get_contacts(rp3dg_world* world, int32_t* body1, int32_t* body2, uint8_t* nb_points,
+                             uint32_t capacity, float* normal_depth, float* local1, float* local2,
+                             uint32_t capacity_points, uint32_t* nb_manifolds, uint32_t* nb_contact_points);
+int rp3dg_world_get_stats(rp3dg_world* world, rp3dg_world_stats* stats);
+
 /* Number of kernels this context launched so far (instrumentation; a
  * convex-polyhedron batch takes two). */
 uint64_t rp3dg_kernel_launches(const rp3dg_ctx* ctx);

@@ -39,6 +39,8 @@
 #include <vector>
 #include <reactphysics3d/reactphysics3d.h>
 
+#include "../include/rp3dg.h"
+
 using namespace reactphysics3d;
 
 namespace {
@@ -481,6 +483,130 @@ int ref_world_field_names(int id, char* dst, int cap) {
     if (int(s.size()) + 1 > cap) return -1;
     std::memcpy(dst, s.c_str(), s.size() + 1);
     return 0;
+}
+
+// ---- scenes described with the library's own world description -----------
+// ref_scene_create builds a reference world from the rp3dg_world_settings /
+// rp3dg_body_desc / rp3dg_collider_desc arrays that rp3dg_world_create takes,
+// with the call sequence documented there (include/rp3dg.h), so that both
+// engines start from identical worlds.  Convex meshes are not used here.
+int ref_scene_create(const rp3dg_world_settings* s, const rp3dg_shape* shapes, uint32_t nshapes,
+                     const rp3dg_body_desc* bd, uint32_t nb, const rp3dg_collider_desc* cd, uint32_t nc) {
+    auto W = std::make_unique<World>();
+    PhysicsWorld::WorldSettings ws;
+    ws.gravity = Vector3(s->gravity[0], s->gravity[1], s->gravity[2]);
+    ws.defaultVelocitySolverNbIterations = uint16(s->velocity_iterations);
+    ws.isSleepingEnabled = s->sleeping_enabled != 0;
+    ws.defaultSleepLinearVelocity = s->sleep_linear_velocity;
+    ws.defaultSleepAngularVelocity = s->sleep_angular_velocity;
+    ws.defaultTimeBeforeSleep = s->time_before_sleep;
+    ws.restitutionVelocityThreshold = s->restitution_velocity_threshold;
+    ws.persistentContactDistanceThreshold = s->persistent_contact_distance_threshold;
+    ws.cosAngleSimilarContactManifold = s->cos_angle_similar_contact_manifold;
+    W->world = W->common.createPhysicsWorld(ws);
+    std::vector<CollisionShape*> cs(nshapes, nullptr);
+    for (uint32_t i = 0; i < nshapes; i++) {
+        const rp3dg_shape& sh = shapes[i];
+        if (sh.kind == RP3DG_SHAPE_SPHERE) cs[i] = W->common.createSphereShape(sh.params[0]);
+        else if (sh.kind == RP3DG_SHAPE_CAPSULE) cs[i] = W->common.createCapsuleShape(sh.params[0], sh.params[1] * 2.0f);
+        else if (sh.kind == RP3DG_SHAPE_BOX) cs[i] = W->common.createBoxShape(Vector3(sh.params[0], sh.params[1], sh.params[2]));
+        else return -1;
+    }
+    uint32_t ci = 0;
+    for (uint32_t b = 0; b < nb; b++) {
+        const rp3dg_body_desc& d = bd[b];
+        RigidBody* body = W->world->createRigidBody(
+            Transform(Vector3(d.position[0], d.position[1], d.position[2]),
+                      Quaternion(d.orientation[0], d.orientation[1], d.orientation[2], d.orientation[3])));
+        while (ci < nc && uint32_t(cd[ci].body) == b) {
+            const rp3dg_collider_desc& c = cd[ci];
+            Collider* col = body->addCollider(cs[size_t(c.shape)],
+                Transform(Vector3(c.position[0], c.position[1], c.position[2]),
+                          Quaternion(c.orientation[0], c.orientation[1], c.orientation[2], c.orientation[3])));
+            col->getMaterial().setFrictionCoefficient(c.friction);
+            col->getMaterial().setBounciness(c.bounciness);
+            col->getMaterial().setMassDensity(c.mass_density);
+            col->setCollisionCategoryBits(c.category);
+            col->setCollideWithMaskBits(c.mask);
+            ci++;
+        }
+        if (d.type == RP3DG_BODY_DYNAMIC) body->updateMassPropertiesFromColliders();
+        else body->setType(d.type == RP3DG_BODY_STATIC ? BodyType::STATIC : BodyType::KINEMATIC);
+        body->setLinearDamping(d.linear_damping);
+        body->setAngularDamping(d.angular_damping);
+        body->setLinearLockAxisFactor(Vector3(d.linear_lock[0], d.linear_lock[1], d.linear_lock[2]));
+        body->setAngularLockAxisFactor(Vector3(d.angular_lock[0], d.angular_lock[1], d.angular_lock[2]));
+        body->enableGravity(d.gravity_enabled != 0);
+        body->setIsAllowedToSleep(d.allowed_to_sleep != 0);
+        if (d.type != RP3DG_BODY_STATIC) {
+            body->setLinearVelocity(Vector3(d.linear_velocity[0], d.linear_velocity[1], d.linear_velocity[2]));
+            body->setAngularVelocity(Vector3(d.angular_velocity[0], d.angular_velocity[1], d.angular_velocity[2]));
+        }
+        W->bodies.push_back(body);
+    }
+    worlds().push_back(std::move(W));
+    return int(worlds().size()) - 1;
+}
+
+// Body state in creation order.
+int ref_scene_bodies(int id, float* pos, float* ori, float* lv, float* av, uint8_t* sleeping) {
+    World& W = *worlds().at(size_t(id));
+    for (size_t i = 0; i < W.bodies.size(); i++) {
+        RigidBody* b = W.bodies[i];
+        const Transform& t = b->getTransform();
+        const Vector3 p = t.getPosition();
+        const Quaternion q = t.getOrientation();
+        const Vector3 v = b->getLinearVelocity(), a = b->getAngularVelocity();
+        if (pos) { pos[3 * i] = float(p.x); pos[3 * i + 1] = float(p.y); pos[3 * i + 2] = float(p.z); }
+        if (ori) { ori[4 * i] = float(q.x); ori[4 * i + 1] = float(q.y); ori[4 * i + 2] = float(q.z); ori[4 * i + 3] = float(q.w); }
+        if (lv) { lv[3 * i] = float(v.x); lv[3 * i + 1] = float(v.y); lv[3 * i + 2] = float(v.z); }
+        if (av) { av[3 * i] = float(a.x); av[3 * i + 1] = float(a.y); av[3 * i + 2] = float(a.z); }
+        if (sleeping) sleeping[i] = b->isSleeping() ? 1 : 0;
+    }
+    return int(W.bodies.size());
+}
+
+// Overlapping-pair ids in array order (enabled convex pairs, then disabled).
+long ref_scene_pairs(int id, uint64_t* out, long cap) {
+    World& W = *worlds().at(size_t(id));
+    OverlappingPairs& op = W.world->mCollisionDetection.mOverlappingPairs;
+    long k = 0;
+    for (uint64 i = 0; i < op.mConvexPairs.size(); i++, k++)
+        if (out && k < cap) out[k] = op.mConvexPairs[i].pairID;
+    for (uint64 i = 0; i < op.mDisabledConvexPairs.size(); i++, k++)
+        if (out && k < cap) out[k] = op.mDisabledConvexPairs[i].pairID;
+    return k;
+}
+
+// Contact manifolds of the last step in the solver's order: body creation
+// indices, point counts and the points (normal + depth, local points).
+long ref_scene_contacts(int id, int32_t* body1, int32_t* body2, uint8_t* npts, long cap, float* nd, float* l1,
+                        float* l2, long cap_points, long* nb_points) {
+    World& W = *worlds().at(size_t(id));
+    PhysicsWorld& w = *W.world;
+    std::unordered_map<uint32_t, int32_t> index;
+    for (size_t i = 0; i < W.bodies.size(); i++) index[W.bodies[i]->getEntity().id] = int32_t(i);
+    Array<ContactManifold>& mans = *w.mCollisionDetection.mCurrentContactManifolds;
+    Array<ContactPoint>& pts = *w.mCollisionDetection.mCurrentContactPoints;
+    long k = 0, p = 0;
+    for (uint64 m = 0; m < mans.size(); m++, k++) {
+        const ContactManifold& M = mans[m];
+        if (k < cap) {
+            if (body1) body1[k] = index[M.bodyEntity1.id];
+            if (body2) body2[k] = index[M.bodyEntity2.id];
+            if (npts) npts[k] = uint8_t(M.nbContactPoints);
+        }
+        for (uint32 c = M.contactPointsIndex; c < M.contactPointsIndex + M.nbContactPoints; c++, p++) {
+            if (p >= cap_points) continue;
+            const ContactPoint& P = pts[c];
+            const Vector3 n = P.getNormal(), a = P.getLocalPointOnShape1(), b = P.getLocalPointOnShape2();
+            if (nd) { nd[4 * p] = float(n.x); nd[4 * p + 1] = float(n.y); nd[4 * p + 2] = float(n.z); nd[4 * p + 3] = float(P.getPenetrationDepth()); }
+            if (l1) { l1[4 * p] = float(a.x); l1[4 * p + 1] = float(a.y); l1[4 * p + 2] = float(a.z); l1[4 * p + 3] = 0.0f; }
+            if (l2) { l2[4 * p] = float(b.x); l2[4 * p + 1] = float(b.y); l2[4 * p + 2] = float(b.z); l2[4 * p + 3] = 0.0f; }
+        }
+    }
+    if (nb_points) *nb_points = p;
+    return k;
 }
 
 void ref_world_destroy_all(void) { worlds().clear(); }

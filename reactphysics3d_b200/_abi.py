@@ -107,3 +107,66 @@ class HostContacts:
     def valid_mask(self):
         """Boolean [max_contacts, n] mask of the slots that hold a contact."""
         return np.arange(self.max_contacts)[:, None] < self.nb_contacts[None, :]
+
+
+# ---- world step (rp3dg_world_*) --------------------------------------------
+BODY_STATIC, BODY_KINEMATIC, BODY_DYNAMIC = 0, 1, 2
+
+WORLD_SETTINGS_DTYPE = np.dtype([
+    ("gravity", "<f4", (3,)), ("velocity_iterations", "<i4"), ("sleeping_enabled", "<i4"),
+    ("sleep_linear_velocity", "<f4"), ("sleep_angular_velocity", "<f4"), ("time_before_sleep", "<f4"),
+    ("restitution_velocity_threshold", "<f4"), ("persistent_contact_distance_threshold", "<f4"),
+    ("cos_angle_similar_contact_manifold", "<f4")])
+BODY_DESC_DTYPE = np.dtype([
+    ("type", "<i4"), ("position", "<f4", (3,)), ("orientation", "<f4", (4,)),
+    ("linear_velocity", "<f4", (3,)), ("angular_velocity", "<f4", (3,)),
+    ("linear_damping", "<f4"), ("angular_damping", "<f4"),
+    ("linear_lock", "<f4", (3,)), ("angular_lock", "<f4", (3,)),
+    ("gravity_enabled", "<i4"), ("allowed_to_sleep", "<i4")])
+COLLIDER_DESC_DTYPE = np.dtype([
+    ("body", "<i4"), ("shape", "<i4"), ("position", "<f4", (3,)), ("orientation", "<f4", (4,)),
+    ("friction", "<f4"), ("bounciness", "<f4"), ("mass_density", "<f4"),
+    ("category", "<u2"), ("mask", "<u2")])
+WORLD_STATS_DTYPE = np.dtype([(k, "<u4") for k in (
+    "overlapping_pairs", "disabled_pairs", "narrowphase_tests", "contact_pairs", "manifolds",
+    "contact_points", "islands", "enabled_bodies", "moved_colliders", "reserved")])
+assert WORLD_SETTINGS_DTYPE.itemsize == 44 and BODY_DESC_DTYPE.itemsize == 96
+assert COLLIDER_DESC_DTYPE.itemsize == 52 and WORLD_STATS_DTYPE.itemsize == 40
+
+
+def default_world_settings():
+    """PhysicsWorld::WorldSettings defaults (PhysicsWorld.h:122-138), float32."""
+    s = np.zeros(1, WORLD_SETTINGS_DTYPE)[0]
+    f = np.float32
+    s["gravity"] = (0.0, -9.81, 0.0)
+    s["velocity_iterations"] = 6
+    s["sleeping_enabled"] = 1
+    s["sleep_linear_velocity"] = f(0.02)
+    s["sleep_angular_velocity"] = f(3.0) * (f(3.141592653589) / f(180.0))
+    s["time_before_sleep"] = 1.0
+    s["restitution_velocity_threshold"] = f(0.5)
+    s["persistent_contact_distance_threshold"] = f(0.03)
+    s["cos_angle_similar_contact_manifold"] = f(0.95)
+    return s
+
+
+def body_descs(n):
+    b = np.zeros(n, BODY_DESC_DTYPE)
+    b["type"] = BODY_DYNAMIC
+    b["orientation"][:, 3] = 1.0
+    b["linear_lock"] = 1.0
+    b["angular_lock"] = 1.0
+    b["gravity_enabled"] = 1
+    b["allowed_to_sleep"] = 1
+    return b
+
+
+def collider_descs(n):
+    c = np.zeros(n, COLLIDER_DESC_DTYPE)
+    c["orientation"][:, 3] = 1.0
+    c["friction"] = np.float32(0.3)
+    c["bounciness"] = np.float32(0.5)
+    c["mass_density"] = 1.0
+    c["category"] = 1
+    c["mask"] = 0xFFFF
+    return c

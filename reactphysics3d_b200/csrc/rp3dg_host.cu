@@ -181,6 +181,7 @@ struct rp3dg_ctx {
     // shapes
     rp3dg_shape* d_shapes = nullptr;
     uint32_t nb_shapes = 0, cap_shapes = 0;
+    std::vector<rp3dg_shape> host_shapes;
     // convex meshes
     std::vector<MeshTopo> meshes;
     std::vector<MeshInstance> instances;
@@ -303,6 +304,15 @@ int upload_arena(rp3dg_ctx* ctx) {
 }
 
 }  // namespace
+
+// host copy of the shape table (world set-up reads it; C++ linkage)
+namespace rp3dg {
+int get_shapes_host(rp3dg_ctx* ctx, std::vector<rp3dg_shape>* out) {
+    if (!ctx || !out) return RP3DG_EINVAL;
+    *out = ctx->host_shapes;
+    return 0;
+}
+}  // namespace rp3dg
 
 extern "C" {
 
@@ -530,6 +540,7 @@ int rp3dg_set_shapes(rp3dg_ctx* ctx, const rp3dg_shape* shapes, uint32_t nb) {
         if (e != cudaSuccess) return cuda_fail(ctx, e, "upload shapes");
     }
     ctx->nb_shapes = nb;
+    ctx->host_shapes.assign(shapes, shapes + nb);
     return 0;
 }
 

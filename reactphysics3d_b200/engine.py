@@ -83,6 +83,15 @@ def load_library(path=LIB_PATH):
     L.rp3dg_axis_mlp_predict.argtypes = [P, P, C.c_uint32, P]
     L.rp3dg_set_learned_axis.argtypes = [P, C.c_int]
     L.rp3dg_learned_axis_stats.argtypes = [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_int]
+    L.rp3dg_world_create.argtypes = [P, P, P, C.c_uint32, P, C.c_uint32, C.POINTER(P)]
+    L.rp3dg_world_destroy.argtypes = [P]
+    L.rp3dg_world_destroy.restype = None
+    L.rp3dg_world_update.argtypes = [P, C.c_float]
+    L.rp3dg_world_get_bodies.argtypes = [P, P, P, P, P, P]
+    L.rp3dg_world_get_pairs.argtypes = [P, P, C.c_uint32, C.POINTER(C.c_uint32)]
+    L.rp3dg_world_get_contacts.argtypes = [P, P, P, P, C.c_uint32, P, P, P, C.c_uint32,
+                                           C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+    L.rp3dg_world_get_stats.argtypes = [P, P]
     _lib = L
     return L
 
@@ -410,3 +419,78 @@ def train_axis_mlp(ctx, mlp, x, y, epochs=4, batch=8192, lr=2e-3, seed=0, log=No
         if log:
             log(f"epoch {ep}: loss {losses[-1]:.4f}")
     return losses
+
+
+class World:
+    """A physics world stepped on the GPU (rp3dg_world_*): the drop-in for
+    PhysicsWorld::update.  `scene` is a scenes.WorldScene; the context's shape
+    table is replaced by the scene's."""
+
+    def __init__(self, ctx, scene):
+        self.ctx, self.lib = ctx, ctx.lib
+        ctx.set_shapes(scene.shapes)
+        self.nb = len(scene.bodies)
+        self._keep = (np.ascontiguousarray(scene.settings).copy(), np.ascontiguousarray(scene.bodies),
+                      np.ascontiguousarray(scene.colliders))
+        st, bd, cd = self._keep
+        h = C.c_void_p()
+        rc = self.lib.rp3dg_world_create(ctx.h, st.ctypes.data, bd.ctypes.data, len(bd), cd.ctypes.data, len(cd),
+                                         C.byref(h))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(ctx.h).decode())
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.rp3dg_world_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def update(self, dt=1.0 / 60.0, n=1):
+        for _ in range(n):
+            rc = self.lib.rp3dg_world_update(self.h, dt)
+            if rc != 0:
+                raise Rp3dgError(rc, "rp3dg_world_update failed (see stderr)")
+
+    def bodies(self):
+        """(position (n,3), orientation (n,4), linear velocity, angular velocity, sleeping) in creation order."""
+        n = self.nb
+        p, q = np.zeros((n, 3), np.float32), np.zeros((n, 4), np.float32)
+        lv, av = np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32)
+        sl = np.zeros(n, np.uint8)
+        rc = self.lib.rp3dg_world_get_bodies(self.h, p.ctypes.data, q.ctypes.data, lv.ctypes.data, av.ctypes.data,
+                                             sl.ctypes.data)
+        assert rc == 0, rc
+        return p, q, lv, av, sl
+
+    def pairs(self):
+        """Overlapping-pair ids in the reference's array order (enabled, then disabled)."""
+        n = C.c_uint32()
+        self.lib.rp3dg_world_get_pairs(self.h, None, 0, C.byref(n))
+        out = np.zeros(n.value, np.uint64)
+        self.lib.rp3dg_world_get_pairs(self.h, out.ctypes.data, n.value, C.byref(n))
+        return out
+
+    def contacts(self):
+        """Manifolds of the last step in solver order: body1, body2, point
+        counts, and per point normal|depth, local1, local2 (float4)."""
+        nm, npt = C.c_uint32(), C.c_uint32()
+        self.lib.rp3dg_world_get_contacts(self.h, None, None, None, 0, None, None, None, 0, C.byref(nm), C.byref(npt))
+        b1, b2 = np.zeros(nm.value, np.int32), np.zeros(nm.value, np.int32)
+        k = np.zeros(nm.value, np.uint8)
+        nd, l1, l2 = (np.zeros((npt.value, 4), np.float32) for _ in range(3))
+        rc = self.lib.rp3dg_world_get_contacts(self.h, b1.ctypes.data, b2.ctypes.data, k.ctypes.data, nm.value,
+                                               nd.ctypes.data, l1.ctypes.data, l2.ctypes.data, npt.value,
+                                               C.byref(nm), C.byref(npt))
+        assert rc == 0, rc
+        return b1, b2, k, nd, l1, l2
+
+    def stats(self):
+        s = np.zeros(1, A.WORLD_STATS_DTYPE)
+        self.lib.rp3dg_world_get_stats(self.h, s.ctypes.data)
+        return {k: int(s[k][0]) for k in A.WORLD_STATS_DTYPE.names if k != "reserved"}

@@ -179,3 +179,112 @@ def narrowphase_scene(total_pairs=TOTAL_PAIRS, seed=1234, names=BATCH_NAMES, pos
         base += 2 * n
     shapes = np.concatenate(all_shapes) if all_shapes else np.zeros(0, A.SHAPE_DTYPE)
     return NarrowphaseScene(shapes, batches, hull_vertices, hull_faces, seed)
+
+
+# ---- worlds ----------------------------------------------------------------
+
+class WorldScene:
+    """A world description: settings, shape table, bodies and colliders
+    (numpy structured arrays with the layouts of include/rp3dg.h)."""
+
+    def __init__(self, settings, shapes, bodies, colliders, name=""):
+        self.settings, self.shapes, self.bodies, self.colliders, self.name = settings, shapes, bodies, colliders, name
+
+
+def box_pile(nx=10, ny=10, nz=10, seed=1, spacing=2.0, base=2.0, jitter=0.1):
+    """The plain box pile: nx*ny*nz dynamic boxes (half-extents U[0.25, 0.75],
+    density 1, friction 0.3, bounciness 0) on a grid with `spacing` metres
+    between centres, the lowest layer at y = base, each centre jittered by
+    U[-jitter, jitter] per axis, uniform random orientations; they fall onto a
+    static ground box of half-extents 50 x 0.5 x 50 centred at y = 0.  Gravity
+    -9.81, default solver iterations, sleeping on.  Body 0 is the ground."""
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nz
+    shapes = np.zeros(n + 1, A.SHAPE_DTYPE)
+    shapes["kind"] = A.SHAPE_BOX
+    shapes["mesh"] = -1
+    shapes["params"][0, :3] = (50.0, 0.5, 50.0)
+    shapes["params"][1:, :3] = rng.uniform(0.25, 0.75, size=(n, 3)).astype(np.float32)
+    bodies = A.body_descs(n + 1)
+    bodies[0]["type"] = A.BODY_STATIC
+    iy, ix, iz = np.meshgrid(np.arange(ny), np.arange(nx), np.arange(nz), indexing="ij")
+    centre = np.stack([(ix.ravel() - 0.5 * (nx - 1)) * spacing, base + iy.ravel() * spacing,
+                       (iz.ravel() - 0.5 * (nz - 1)) * spacing], axis=1)
+    centre = centre + rng.uniform(-jitter, jitter, size=(n, 3))
+    bodies["position"][1:] = centre.astype(np.float32)
+    bodies["orientation"][1:] = random_quaternions(rng, n)
+    colliders = A.collider_descs(n + 1)
+    colliders["body"] = np.arange(n + 1)
+    colliders["shape"] = np.arange(n + 1)
+    colliders["friction"] = np.float32(0.3)
+    colliders["bounciness"] = 0.0
+    return WorldScene(A.default_world_settings(), shapes, bodies, colliders, f"box pile {n}")
+
+
+def mixed_world(nx=5, ny=4, nz=5, seed=2, spacing=1.6, variety=True):
+    """Boxes, spheres and capsules of random sizes on a jittered grid above a
+    static ground; with `variety`, random frictions and bounciness, dampings,
+    lock factors, a few kinematic and gravity-free bodies, initial velocities,
+    one body that may not sleep, and collision filters (categories 1, 2, 4;
+    every third collider ignores category 2)."""
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nz
+    kinds = rng.integers(0, 3, size=n)
+    shapes = np.zeros(n + 1, A.SHAPE_DTYPE)
+    shapes["mesh"] = -1
+    shapes[0]["kind"] = A.SHAPE_BOX
+    shapes["params"][0, :3] = (25.0, 0.25, 25.0)
+    for i, k in enumerate(kinds):
+        s = shapes[i + 1]
+        if k == 0:
+            s["kind"] = A.SHAPE_BOX
+            s["params"][:3] = rng.uniform(0.25, 0.6, 3)
+        elif k == 1:
+            s["kind"] = A.SHAPE_SPHERE
+            s["params"][0] = rng.uniform(0.2, 0.5)
+        else:
+            s["kind"] = A.SHAPE_CAPSULE
+            s["params"][:2] = (rng.uniform(0.15, 0.3), rng.uniform(0.2, 0.4))
+    bodies = A.body_descs(n + 1)
+    bodies[0]["type"] = A.BODY_STATIC
+    bodies[0]["position"] = (0.0, -0.25, 0.0)
+    iy, ix, iz = np.meshgrid(np.arange(ny), np.arange(nx), np.arange(nz), indexing="ij")
+    centre = np.stack([(ix.ravel() - 0.5 * (nx - 1)) * spacing, 1.0 + iy.ravel() * spacing,
+                       (iz.ravel() - 0.5 * (nz - 1)) * spacing], axis=1) + rng.uniform(-0.1, 0.1, size=(n, 3))
+    bodies["position"][1:] = centre.astype(np.float32)
+    bodies["orientation"][1:] = random_quaternions(rng, n)
+    colliders = A.collider_descs(n + 1)
+    colliders["body"] = np.arange(n + 1)
+    colliders["shape"] = np.arange(n + 1)
+    colliders["friction"] = np.float32(0.3)
+    colliders["bounciness"] = 0.0
+    if variety:
+        colliders["friction"][1:] = rng.uniform(0.1, 1.0, n).astype(np.float32)
+        colliders["bounciness"][1:] = rng.uniform(0.0, 0.6, n).astype(np.float32)
+        colliders["friction"][0] = np.float32(0.6)
+        for i in range(1, n + 1):
+            k = (i - 1) % 23
+            b = bodies[i]
+            if k == 3:
+                b["linear_damping"] = rng.uniform(0.0, 0.5)
+            elif k == 4:
+                b["angular_damping"] = rng.uniform(0.0, 0.5)
+            elif k == 5:
+                b["linear_lock"] = (1.0, 0.0, 1.0)
+            elif k == 6:
+                b["angular_lock"] = (0.0, 1.0, 0.0)
+            elif k == 7:
+                b["gravity_enabled"] = 0
+            elif k == 8:
+                b["linear_velocity"] = rng.uniform(-2, 2, 3) * np.array([1, 0.5, 1]) - np.array([0, 1, 0])
+            elif k == 9:
+                b["angular_velocity"] = rng.uniform(-3, 3, 3)
+            elif k == 10:
+                b["type"] = A.BODY_KINEMATIC
+                b["linear_velocity"] = (rng.uniform(-0.5, 0.5), 0.0, rng.uniform(-0.5, 0.5))
+            elif k == 11:
+                b["allowed_to_sleep"] = 0
+        c = np.arange(n)
+        colliders["category"][1:] = (1 << (c % 3)).astype(np.uint16)
+        colliders["mask"][1:] = np.where(c % 3 == 0, 0xFFFF & ~2, 0xFFFF).astype(np.uint16)
+    return WorldScene(A.default_world_settings(), shapes, bodies, colliders, f"mixed {n}")

@@ -261,3 +261,55 @@ class RefWorld:
                 a = a.reshape(-1, 4)
             out[name] = a
         return out
+
+
+class RefScene:
+    """A reference world built from a scenes.WorldScene (oracle/ref_world.cpp
+    ref_scene_create, the call sequence of rp3dg_world_create) and stepped by
+    PhysicsWorld::update."""
+
+    def __init__(self, scene, prec="f32"):
+        self.lib = C.CDLL(REF_LIB[prec])
+        L = self.lib
+        P = C.c_void_p
+        L.ref_scene_create.argtypes = [P, P, C.c_uint32, P, C.c_uint32, P, C.c_uint32]
+        L.ref_scene_bodies.argtypes = [C.c_int, P, P, P, P, P]
+        L.ref_scene_pairs.argtypes = [C.c_int, P, C.c_long]
+        L.ref_scene_pairs.restype = C.c_long
+        L.ref_scene_contacts.argtypes = [C.c_int, P, P, P, C.c_long, P, P, P, C.c_long, C.POINTER(C.c_long)]
+        L.ref_scene_contacts.restype = C.c_long
+        L.ref_world_step.argtypes = [C.c_int, C.c_float, C.c_int]
+        self._keep = (np.ascontiguousarray(scene.settings).copy(), np.ascontiguousarray(scene.shapes),
+                      np.ascontiguousarray(scene.bodies), np.ascontiguousarray(scene.colliders))
+        st, sh, bd, cd = self._keep
+        self.id = L.ref_scene_create(st.ctypes.data, sh.ctypes.data, len(sh), bd.ctypes.data, len(bd),
+                                     cd.ctypes.data, len(cd))
+        assert self.id >= 0
+        self.nb = len(bd)
+
+    def update(self, dt=1.0 / 60.0, n=1):
+        self.lib.ref_world_step(self.id, dt, n)
+
+    def bodies(self):
+        n = self.nb
+        p, q = np.zeros((n, 3), np.float32), np.zeros((n, 4), np.float32)
+        lv, av = np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32)
+        sl = np.zeros(n, np.uint8)
+        self.lib.ref_scene_bodies(self.id, p.ctypes.data, q.ctypes.data, lv.ctypes.data, av.ctypes.data, sl.ctypes.data)
+        return p, q, lv, av, sl
+
+    def pairs(self):
+        n = self.lib.ref_scene_pairs(self.id, None, 0)
+        out = np.zeros(n, np.uint64)
+        self.lib.ref_scene_pairs(self.id, out.ctypes.data, n)
+        return out
+
+    def contacts(self):
+        npt = C.c_long()
+        nm = self.lib.ref_scene_contacts(self.id, None, None, None, 0, None, None, None, 0, C.byref(npt))
+        b1, b2 = np.zeros(nm, np.int32), np.zeros(nm, np.int32)
+        k = np.zeros(nm, np.uint8)
+        nd, l1, l2 = (np.zeros((npt.value, 4), np.float32) for _ in range(3))
+        self.lib.ref_scene_contacts(self.id, b1.ctypes.data, b2.ctypes.data, k.ctypes.data, nm, nd.ctypes.data,
+                                    l1.ctypes.data, l2.ctypes.data, npt.value, C.byref(npt))
+        return b1, b2, k, nd, l1, l2
