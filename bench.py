@@ -244,6 +244,11 @@ def run_ours(args):
         broadphase = broadphase_section(ctx, args, dev)
         ctx.set_shapes(sc.shapes)   # the narrow-phase workload's table again
 
+    world_step = None
+    if not args.no_world:
+        world_step = world_section(ctx, args, rank == 0 and world == 1 and not args.no_cpu)
+        ctx.set_shapes(sc.shapes)
+
     learned = None
     if not args.no_learned:
         learned = learned_axis_section(ctx, sc, args, dev)
@@ -259,6 +264,7 @@ def run_ours(args):
                        "seed": args.seed, "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"independent pair sets per rank x{world}"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "manifolds": manifolds, "dynamics": dynamics, "broadphase": broadphase,
+            "world_step": world_step,
             "learned_axis": learned,
             "gpu_launches": int(launches),
             "clocks": clocks, "batch_ms": {k: round(v, 4) for k, v in mean_batch.items()}}
@@ -393,6 +399,64 @@ def dynamics_section(ctx, args, dev, with_cpu):
         dt_cpu = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": round(n_cpu / dt_cpu, 1), "unit": "world-steps/s", "cores": 1, "kind": "port",
                                "sample": f"{n_cpu} of the worlds, one stage, C restatement (oracle), one core"}
+    return out
+
+
+def world_section(ctx, args, with_cpu):
+    """The whole world step (PhysicsWorld::update) on the plain box pile:
+    1,000 dynamic boxes falling onto a static ground, 300 steps at 1/60 s,
+    through rp3dg_world_update (host API; synchronous, so wall-clock time is
+    the metric).  The reference engine (oracle/_ref, built from its sources)
+    steps the same world on one host core (it is single-threaded); the final
+    states are compared bit for bit, and both against the reference's FP64
+    build.  A second run with phase profiling gives the per-phase split."""
+    from reactphysics3d_b200 import engine
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import reflib
+    sc = scenes.box_pile()
+    n = args.world_steps
+    dt = float(np.float32(1.0 / 60.0))
+    w = engine.World(ctx, sc)
+    w.update(dt, 1)                  # first step: pair creation for every collider
+    launches0 = ctx.kernel_launches()
+    t0 = time.perf_counter()
+    w.update(dt, n - 1)
+    ctx.synchronize()
+    sec = time.perf_counter() - t0
+    launches = (ctx.kernel_launches() - launches0) / (n - 1)
+    st = w.stats()
+    ours = w.bodies()
+    w.close()
+    wp = engine.World(ctx, sc)
+    wp.set_profiling(True)
+    wp.update(dt, n)
+    phases = {k: round(v / n, 4) for k, v in wp.phase_times().items()}
+    wp.close()
+    out = {"workload": "plain box pile: 1,000 boxes (half-extents U[0.25,0.75], density 1, friction 0.3, "
+                       "restitution 0) on a 10x10x10 grid, 2 m spacing, lowest layer at y=2, +-0.1 m jitter, "
+                       "random orientations, static ground box 50x0.5x50 at y=0; 300 steps at 1/60 s, "
+                       "6 velocity iterations, sleeping on",
+           "steps": n, "world_steps_per_s": round((n - 1) / sec, 1), "ms_per_step": round(1e3 * sec / (n - 1), 4),
+           "kernels_per_step": round(launches, 1), "phase_ms_per_step": phases,
+           "final_stats": st, "api": "rp3dg_world_update"}
+    if with_cpu and reflib.have_ref("f32"):
+        r = reflib.RefScene(sc, "f32")
+        r.update(dt, 1)
+        t0 = time.perf_counter()
+        r.update(dt, n - 1)
+        rsec = time.perf_counter() - t0
+        ref = r.bodies()
+        out["cpu_baseline"] = {"value": round((n - 1) / rsec, 1), "unit": "world-steps/s", "cores": 1,
+                               "kind": "reference", "sample": f"the same world, steps 2-{n}, PhysicsWorld::update "
+                                                              "of the reference float build (single-threaded engine)"}
+        out["bit_identical_to_reference"] = all(np.array_equal(a, b) for a, b in zip(ours, ref))
+        if reflib.have_ref("f64"):
+            r64 = reflib.RefScene(sc, "f64")
+            r64.update(dt, n)
+            d = np.linalg.norm(ours[0].astype(np.float64) - r64.bodies()[0], axis=1)
+            out["fp64_position_deviation_m"] = {"median": round(float(np.median(d)), 5), "max": round(float(d.max()), 4),
+                                                "note": "same for the reference float build (bit-identical); "
+                                                        "a 1,000-body pile is chaotic"}
     return out
 
 
@@ -664,6 +728,8 @@ def main():
     ap.add_argument("--no-dynamics", action="store_true")
     ap.add_argument("--no-broadphase", action="store_true")
     ap.add_argument("--dyn-worlds", type=int, default=4096)
+    ap.add_argument("--no-world", action="store_true")
+    ap.add_argument("--world-steps", type=int, default=300)
     ap.add_argument("--learned-epochs", type=int, default=4)
     args = ap.parse_args()
     if args.impl == "reference":

@@ -539,6 +539,15 @@ int rp3dg_world_get_contacts(rp3dg_world* world, int32_t* body1, int32_t* body2,
                              uint32_t capacity, float* normal_depth, float* local1, float* local2,
                              uint32_t capacity_points, uint32_t* nb_manifolds, uint32_t* nb_contact_points);
 int rp3dg_world_get_stats(rp3dg_world* world, rp3dg_world_stats* stats);
+/* Phase profiling (instrumentation; no counterpart in the reference, whose
+ * profiler is a compile-time option): when enabled, each step drains the
+ * stream at phase boundaries and accumulates wall-clock milliseconds per
+ * phase: 0 broad phase (host), 1 middle phase (host), 2 narrow phase and
+ * manifold step (GPU), 3 contact pairs and islands (host), 4 contact packing
+ * and warm start (GPU), 5 dynamics stage (GPU), 6 collider update and tree
+ * reinsertion, 7 sleeping and end of step.  Enabling resets the counters. */
+int rp3dg_world_set_profiling(rp3dg_world* world, int enable);
+int rp3dg_world_get_phase_times(rp3dg_world* world, double* ms, uint32_t n);
 
 /* Number of kernels this context launched so far (instrumentation; a
  * convex-polyhedron batch takes two). */

@@ -312,6 +312,10 @@ int get_shapes_host(rp3dg_ctx* ctx, std::vector<rp3dg_shape>* out) {
     *out = ctx->host_shapes;
     return 0;
 }
+// error message of a world call, readable through rp3dg_last_error
+void set_error(rp3dg_ctx* ctx, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+}
 }  // namespace rp3dg
 
 extern "C" {

@@ -31,6 +31,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -44,6 +45,7 @@
 namespace rp3dg {
 // host copy of the context's shape table (rp3dg_host.cu)
 int get_shapes_host(rp3dg_ctx* ctx, std::vector<rp3dg_shape>* out);
+void set_error(rp3dg_ctx* ctx, const std::string& msg);
 }  // namespace rp3dg
 
 using rp3dg::order::Box;
@@ -495,6 +497,10 @@ struct rp3dg_world {
     std::vector<uint32_t> item_pair;  // index into pairs of each item
     std::vector<uint8_t> gravity;  // gravity flag by body id (re-uploaded after permutations)
     bool tables_dirty = true;
+    // phase profiling (rp3dg_world_set_profiling): cumulative ms per phase
+    bool profiling = false;
+    double phase_ms[8] = {};
+    std::chrono::steady_clock::time_point t_mark;
     rp3dg_world_stats stats{};
     std::string err;
 };
@@ -502,8 +508,14 @@ struct rp3dg_world {
 namespace {
 
 int wfail(rp3dg_world* w, int code, const std::string& msg) {
-    if (w) w->err = msg;
-    std::fprintf(stderr, "rp3dg world: %s\n", msg.c_str());
+    if (w) {
+        w->err = msg;
+        rp3dg::set_error(w->ctx, "world: " + msg);
+    }
+    return code;
+}
+int cfail(rp3dg_ctx* ctx, int code, const std::string& msg) {
+    rp3dg::set_error(ctx, "world: " + msg);
     return code;
 }
 int wcuda(rp3dg_world* w, cudaError_t e, const char* what) {
@@ -819,7 +831,7 @@ extern "C" {
 
 int rp3dg_world_create(rp3dg_ctx* ctx, const rp3dg_world_settings* s, const rp3dg_body_desc* bd, uint32_t nb,
                        const rp3dg_collider_desc* cd, uint32_t nc, rp3dg_world** out) {
-    if (!ctx || !s || !out || (nb && !bd) || (nc && !cd)) return wfail(nullptr, RP3DG_EINVAL, "null argument");
+    if (!ctx || !s || !out || (nb && !bd) || (nc && !cd)) return ctx ? cfail(ctx, RP3DG_EINVAL, "null argument") : RP3DG_EINVAL;
     *out = nullptr;
     // shape table (host copy)
     auto* w = new rp3dg_world();
@@ -830,22 +842,22 @@ int rp3dg_world_create(rp3dg_ctx* ctx, const rp3dg_world_settings* s, const rp3d
     w->nc = nc;
     if (rp3dg::get_shapes_host(ctx, &w->shapes) || w->shapes.empty()) {
         delete w;
-        return wfail(nullptr, RP3DG_EINVAL, "no shape table (rp3dg_set_shapes)");
+        return cfail(ctx, RP3DG_EINVAL, "no shape table (rp3dg_set_shapes)");
     }
     for (uint32_t i = 0; i < nc; i++) {
         if (cd[i].body < 0 || uint32_t(cd[i].body) >= nb || (i && cd[i].body < cd[i - 1].body)) {
             delete w;
-            return wfail(nullptr, RP3DG_EINVAL, "colliders must be grouped by body, bodies ascending");
+            return cfail(ctx, RP3DG_EINVAL, "colliders must be grouped by body, bodies ascending");
         }
         if (cd[i].shape < 0 || size_t(cd[i].shape) >= w->shapes.size()) {
             delete w;
-            return wfail(nullptr, RP3DG_EINVAL, "collider shape outside the shape table");
+            return cfail(ctx, RP3DG_EINVAL, "collider shape outside the shape table");
         }
     }
     for (uint32_t i = 0; i < nb; i++)
         if (bd[i].type < RP3DG_BODY_STATIC || bd[i].type > RP3DG_BODY_DYNAMIC) {
             delete w;
-            return wfail(nullptr, RP3DG_EINVAL, "bad body type");
+            return cfail(ctx, RP3DG_EINVAL, "bad body type");
         }
     w->bodies.resize(nb);
     w->colliders.resize(nc);
@@ -897,7 +909,7 @@ int rp3dg_world_create(rp3dg_ctx* ctx, const rp3dg_world_settings* s, const rp3d
                 float vol, in[3], m;
                 if (!shape_mass(w->shapes[size_t(cd[k].shape)], cd[k].mass_density, &vol, in, &m)) {
                     delete w;
-                    return wfail(nullptr, RP3DG_EINVAL, "mass properties of a convex-mesh collider are not supported");
+                    return cfail(ctx, RP3DG_EINVAL, "mass properties of a convex-mesh collider are not supported");
                 }
                 total += m;
                 for (int a = 0; a < 3; a++) com[a] += m * cd[k].position[a];
@@ -969,7 +981,7 @@ int rp3dg_world_create(rp3dg_ctx* ctx, const rp3dg_world_settings* s, const rp3d
     M((void**)&w->c_moved, nc);
     if (e != cudaSuccess) {
         rp3dg_world_destroy(w);
-        return wcuda(nullptr, e, "cudaMalloc(world)");
+        return cfail(ctx, RP3DG_ENOMEM, "cudaMalloc(world)");
     }
     w->dev_body_at = w->bcomp.at;
     w->dev_col_at = w->ccomp.at;
@@ -1026,7 +1038,7 @@ int rp3dg_world_create(rp3dg_ctx* ctx, const rp3dg_world_settings* s, const rp3d
         cudaFree(force);
         if (rc || e != cudaSuccess) {
             rp3dg_world_destroy(w);
-            return rc ? rc : wcuda(nullptr, e, "initial broad phase");
+            return rc ? rc : cfail(ctx, RP3DG_ECUDA, "initial broad phase");
         }
         w->bp_to_collider.clear();
         for (int c : creation_order) {
@@ -1070,9 +1082,20 @@ int rp3dg_world_update(rp3dg_world* w, float dt) {
     cudaStream_t st = w->stream;
     rp3dg_ctx* ctx = w->ctx;
     std::memset(&w->stats, 0, sizeof(w->stats));
+    // phase timer: with profiling on, the stream is drained at each mark so
+    // that GPU time is charged to the phase that queued it
+    auto mark = [&](int k) {
+        if (!w->profiling) return;
+        cudaStreamSynchronize(w->stream);
+        const auto now = std::chrono::steady_clock::now();
+        w->phase_ms[k] += std::chrono::duration<double, std::milli>(now - w->t_mark).count();
+        w->t_mark = now;
+    };
+    if (w->profiling) w->t_mark = std::chrono::steady_clock::now();
 
     // ---- computeCollisionDetection: broad phase (host order, GPU fat AABBs)
     broad_phase(w);
+    mark(0);
 
     // ---- middle phase: narrow-phase batches in pair-array order
     std::vector<int4> by_algo[NB_ALGOS];
@@ -1098,6 +1121,7 @@ int rp3dg_world_update(rp3dg_world* w, float dt) {
     w->stats.narrowphase_tests = T;
     w->stats.overlapping_pairs = uint32_t(w->pairs.size());
 
+    mark(1);
     int rc = ensure_pool(w);
     if (rc) return rc;
     if (!w->reset_slots.empty()) {
@@ -1105,7 +1129,6 @@ int rp3dg_world_update(rp3dg_world* w, float dt) {
         cudaMemcpyAsync(w->d_small, w->reset_slots.data(), w->reset_slots.size() * 4, cudaMemcpyHostToDevice, st);
         world_reset_cache<<<blocks(uint32_t(w->reset_slots.size())), 128, 0, st>>>(uint32_t(w->reset_slots.size()),
                                                                                  w->d_small, w->pool);
-        cudaStreamSynchronize(st);
         w->reset_slots.clear();
     }
     rc = sync_rows(w);
@@ -1178,6 +1201,7 @@ int rp3dg_world_update(rp3dg_world* w, float dt) {
             w->cpairs.push_back(c);
         }
     }
+    mark(2);
     // addContactPairsToBodies
     for (uint32_t p = 0; p < w->cpairs.size(); p++) {
         w->bodies[size_t(w->cpairs[p].b1)].contact_pairs.push_back(p);
@@ -1238,6 +1262,7 @@ int rp3dg_world_update(rp3dg_world* w, float dt) {
     }
     w->stats.islands = uint32_t(w->islands.size());
 
+    mark(3);
     // ---- createContacts: manifolds and points in island order
     rc = sync_rows(w);
     if (rc) return rc;
@@ -1332,6 +1357,7 @@ int rp3dg_world_update(rp3dg_world* w, float dt) {
         cudaMemcpyAsync(w->d_icount, w->h_icount, size_t(ni) * 4, cudaMemcpyHostToDevice, st);
     }
 
+    mark(4);
     // ---- dynamics stage (inertia, velocities, solver, positions, state)
     {
         rp3dg_dynamics_params pr{};
@@ -1376,6 +1402,7 @@ int rp3dg_world_update(rp3dg_world* w, float dt) {
         if (rc) return wfail(w, rc, std::string("dynamics: ") + rp3dg_last_error(ctx));
     }
 
+    mark(5);
     // ---- updateColliders: world AABBs, fat-AABB test, reinsertion flags
     const uint32_t ncu = w->ccomp.n_enabled, nbe = w->bcomp.n_enabled;
     const size_t step_bytes = size_t(ncu) + size_t(ncu) * 32 + size_t(nbe) * 32 + 64;
@@ -1421,6 +1448,7 @@ int rp3dg_world_update(rp3dg_world* w, float dt) {
     }
     w->stats.moved_colliders = nmoved;
 
+    mark(6);
     // ---- updateSleepingBodies (PhysicsWorld.cpp:871-926)
     if (w->set.sleeping_enabled) {
         // velocities by body id, read before any body falls asleep
@@ -1476,6 +1504,20 @@ int rp3dg_world_update(rp3dg_world* w, float dt) {
     w->cur_cb = 1 - w->cur_cb;
     w->stats.disabled_pairs = uint32_t(w->disabled.size());
     w->stats.enabled_bodies = w->bcomp.n_enabled;
+    mark(7);
+    return 0;
+}
+
+int rp3dg_world_set_profiling(rp3dg_world* w, int enable) {
+    if (!w) return RP3DG_EINVAL;
+    w->profiling = enable != 0;
+    for (double& t : w->phase_ms) t = 0.0;
+    return 0;
+}
+
+int rp3dg_world_get_phase_times(rp3dg_world* w, double* ms, uint32_t n) {
+    if (!w || !ms) return RP3DG_EINVAL;
+    for (uint32_t i = 0; i < n && i < 8; i++) ms[i] = w->phase_ms[i];
     return 0;
 }
 

@@ -92,6 +92,8 @@ def load_library(path=LIB_PATH):
     L.rp3dg_world_get_contacts.argtypes = [P, P, P, P, C.c_uint32, P, P, P, C.c_uint32,
                                            C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.rp3dg_world_get_stats.argtypes = [P, P]
+    L.rp3dg_world_set_profiling.argtypes = [P, C.c_int]
+    L.rp3dg_world_get_phase_times.argtypes = [P, P, C.c_uint32]
     _lib = L
     return L
 
@@ -455,7 +457,7 @@ class World:
         for _ in range(n):
             rc = self.lib.rp3dg_world_update(self.h, dt)
             if rc != 0:
-                raise Rp3dgError(rc, "rp3dg_world_update failed (see stderr)")
+                raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
 
     def bodies(self):
         """(position (n,3), orientation (n,4), linear velocity, angular velocity, sleeping) in creation order."""
@@ -489,6 +491,16 @@ class World:
                                                C.byref(nm), C.byref(npt))
         assert rc == 0, rc
         return b1, b2, k, nd, l1, l2
+
+    PHASES = ("broadphase", "middle", "narrow", "islands", "pack", "dynamics", "colliders", "sleeping")
+
+    def set_profiling(self, on=True):
+        self.lib.rp3dg_world_set_profiling(self.h, int(on))
+
+    def phase_times(self):
+        t = np.zeros(8, np.float64)
+        self.lib.rp3dg_world_get_phase_times(self.h, t.ctypes.data, 8)
+        return dict(zip(self.PHASES, t.tolist()))
 
     def stats(self):
         s = np.zeros(1, A.WORLD_STATS_DTYPE)

@@ -36,8 +36,17 @@ Writes:
                    overlapping pairs after the step's broad phase, shapes and
                    filter bits: "<case>/bp_*")
 
-`python tests/golden/make_golden.py manifold` (or `dynamics`) rewrites that
-fixture only.
+  world.npz        whole world steps of two seeded scenes (tests/worldio.py:
+                   a 125-box pile for 240 steps, a mixed world of boxes,
+                   spheres and capsules with materials, dampings, locks,
+                   kinematic / gravity-free bodies and filters for 200 steps)
+                   stepped by the reference's PhysicsWorld::update: per step
+                   the overlapping-pair ids in array order and the solver's
+                   manifolds (counts + 64-bit digests), and the body states
+                   at checkpoints, bit for bit
+
+`python tests/golden/make_golden.py manifold` (or `dynamics`, `world`)
+rewrites that fixture only.
 """
 import json
 import os
@@ -180,9 +189,23 @@ def dynamics_fixture():
     np.savez_compressed(os.path.join(HERE, "np_dynamics.npz"), **d)
 
 
-def main(parts=("scene", "manifold", "dynamics")):
+def world_fixture():
+    import worldio
+    d = {}
+    for name in worldio.WORLD_CASES:
+        sc, steps, every = worldio.make_scene(name)
+        t = worldio.trajectory(reflib.RefScene(sc), steps, every)
+        for k, v in t.items():
+            d[f"{name}/{k}"] = v
+    np.savez_compressed(os.path.join(HERE, "world.npz"), **d)
+
+
+def main(parts=("scene", "manifold", "dynamics", "world")):
     if parts == ("dynamics",):
         dynamics_fixture()
+        return
+    if parts == ("world",):
+        world_fixture()
         return
     ref = reflib.RefEngine("f32")
     verts, faces = ref.quickhull(scenes.icosphere42_points())
@@ -229,7 +252,9 @@ def main(parts=("scene", "manifold", "dynamics")):
         manifold_fixture(ref, verts, faces)
     if "dynamics" in parts:
         dynamics_fixture()
+    if "world" in parts:
+        world_fixture()
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("scene", "manifold", "dynamics"))
+    main(tuple(sys.argv[1:]) or ("scene", "manifold", "dynamics", "world"))

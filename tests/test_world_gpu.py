@@ -1,0 +1,88 @@
+"""World step on the GPU (rp3dg_world_*, the drop-in for PhysicsWorld::update)
+against the reference float build: every step's overlapping pairs in the
+reference's array order, the solver's contact manifolds and points, and the
+body states (positions, orientations, velocities, sleeping flags) must be
+bit-identical."""
+import os
+
+import numpy as np
+import pytest
+
+import reflib
+import worldio
+from reactphysics3d_b200 import _abi as A
+from reactphysics3d_b200 import engine, scenes
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "world.npz")
+
+
+@pytest.fixture(scope="module")
+def ctx(cuda_lib):
+    c = engine.Context(0)
+    yield c
+    c.close()
+
+
+def fixture(name):
+    z = np.load(GOLDEN)
+    return {k.split("/", 1)[1]: z[k] for k in z.files if k.startswith(name + "/")}
+
+
+@pytest.mark.parametrize("name", list(worldio.WORLD_CASES))
+def test_world_matches_reference_fixture(ctx, name):
+    sc, steps, every = worldio.make_scene(name)
+    w = engine.World(ctx, sc)
+    got = worldio.trajectory(w, steps, every)
+    exp = fixture(name)
+    assert worldio.first_mismatch(got, exp) is None, worldio.first_mismatch(got, exp)
+    for k in ("ckpt_pos", "ckpt_ori", "ckpt_lv", "ckpt_av", "ckpt_sleep"):
+        assert np.array_equal(got[k], exp[k]), k
+    w.close()
+
+
+@pytest.mark.skipif(not reflib.have_ref("f32"), reason="reference engine not built")
+def test_box_pile_1000_matches_reference_live(ctx):
+    """The full plain box pile (1,000 boxes, 300 steps at 1/60 s): pair
+    arrays, manifolds and final states bit-identical to the reference."""
+    sc = scenes.box_pile()
+    w, r = engine.World(ctx, sc), reflib.RefScene(sc)
+    for s in range(300):
+        w.update(float(worldio.DT))
+        r.update(float(worldio.DT))
+        if s % 25 == 24 or s == 299:
+            assert np.array_equal(w.pairs(), r.pairs()), s
+            cw, cr = w.contacts(), r.contacts()
+            for a, b in zip(cw, cr):
+                assert np.array_equal(a, b), s
+    for a, b in zip(w.bodies(), r.bodies()):
+        assert np.array_equal(a, b)
+    assert w.bodies()[4].sum() > 0      # some boxes asleep after 5 s
+    w.close()
+
+
+def test_world_create_rejects_bad_input(ctx):
+    sc = scenes.box_pile(2, 2, 2)
+    bad = scenes.WorldScene(sc.settings, sc.shapes, sc.bodies, sc.colliders[::-1].copy())
+    with pytest.raises(engine.Rp3dgError):
+        engine.World(ctx, bad)          # colliders not grouped by ascending body
+    bad = scenes.WorldScene(sc.settings, sc.shapes, sc.bodies, sc.colliders.copy())
+    bad.colliders["shape"][3] = len(sc.shapes) + 5
+    with pytest.raises(engine.Rp3dgError):
+        engine.World(ctx, bad)          # shape outside the table
+    w = engine.World(ctx, sc)
+    with pytest.raises(engine.Rp3dgError):
+        w.update(0.0)                    # dt must be positive
+    w.close()
+
+
+def test_world_stats_and_launches(ctx):
+    sc = scenes.box_pile(4, 4, 4, seed=2)
+    w = engine.World(ctx, sc)
+    l0 = ctx.kernel_launches()
+    w.update(float(worldio.DT), 90)
+    st = w.stats()
+    assert st["contact_pairs"] > 0 and st["manifolds"] == st["contact_pairs"]
+    assert st["overlapping_pairs"] >= st["contact_pairs"]
+    assert ctx.kernel_launches() - l0 >= 90 * 5
+    w.close()

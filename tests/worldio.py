@@ -1,0 +1,59 @@
+"""World trajectories in a compact, comparable form: per step the overlapping
+pair ids (in array order) and the solver's contact manifolds, each as a count
+and a 64-bit digest, plus the body state at checkpoints.  Used by the golden
+world fixture (tests/golden/make_golden.py world) and the world tests."""
+import hashlib
+
+import numpy as np
+
+from reactphysics3d_b200 import scenes
+
+# name -> (scene factory, kwargs, steps, checkpoint every)
+WORLD_CASES = {
+    "pile125": (scenes.box_pile, dict(nx=5, ny=5, nz=5, seed=3), 240, 60),
+    "mixed100": (scenes.mixed_world, dict(nx=5, ny=4, nz=5, seed=5), 200, 50),
+}
+DT = np.float32(1.0 / 60.0)
+
+
+def digest(*arrays):
+    h = hashlib.blake2b(digest_size=8)
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return np.frombuffer(h.digest(), dtype=np.uint64)[0]
+
+
+def make_scene(name):
+    f, kw, steps, every = WORLD_CASES[name]
+    return f(**kw), steps, every
+
+
+def trajectory(world, steps, every):
+    """Step `world` (engine.World or reflib.RefScene) and record the trace."""
+    rec = {k: [] for k in ("pair_n", "pair_h", "man_n", "pt_n", "man_h", "pt_h")}
+    ckpt = {k: [] for k in ("pos", "ori", "lv", "av", "sleep")}
+    for s in range(steps):
+        world.update(float(DT))
+        p = world.pairs()
+        b1, b2, k, nd, l1, l2 = world.contacts()
+        rec["pair_n"].append(len(p))
+        rec["pair_h"].append(digest(p))
+        rec["man_n"].append(len(b1))
+        rec["pt_n"].append(len(nd))
+        rec["man_h"].append(digest(b1, b2, k))
+        rec["pt_h"].append(digest(nd, l1, l2))
+        if (s + 1) % every == 0 or s + 1 == steps:
+            for key, v in zip(ckpt, world.bodies()):
+                ckpt[key].append(v)
+    out = {k: np.array(v, dtype=np.uint64 if k.endswith("_h") else np.int64) for k, v in rec.items()}
+    out.update({"ckpt_" + k: np.stack(v) for k, v in ckpt.items()})
+    return out
+
+
+def first_mismatch(got, exp):
+    """(step, field) of the first per-step difference, or None."""
+    for s in range(len(exp["pair_n"])):
+        for k in ("pair_n", "pair_h", "man_n", "pt_n", "man_h", "pt_h"):
+            if got[k][s] != exp[k][s]:
+                return s, k
+    return None
