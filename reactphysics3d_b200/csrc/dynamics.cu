@@ -12,6 +12,9 @@
 // reference's operand order; the library is built without FMA contraction,
 // so results are bit-identical to the reference's float build.
 #include <cuda_runtime.h>
+#ifdef RP3DG_PROFILE_GIANT
+#include <cstdio>
+#endif
 
 #include "dynamics_launch.h"
 #include "rp3dg_math.cuh"
@@ -252,45 +255,52 @@ struct Man {
     float inv_tw, inv_f1, inv_f2;
 };
 
+template <bool LDG>
+RD float4 ldq(const float4* p) { return LDG ? __ldg(p) : *p; }
+
+template <bool LDG>
 RD void rows3(const float4* __restrict__ q, float* I) {
-    const float4 r0 = __ldg(q), r1 = __ldg(q + 1), r2 = __ldg(q + 2);
+    const float4 r0 = ldq<LDG>(q), r1 = ldq<LDG>(q + 1), r2 = ldq<LDG>(q + 2);
     I[0] = r0.x; I[1] = r0.y; I[2] = r0.z; I[3] = r1.x; I[4] = r1.y; I[5] = r1.z;
     I[6] = r2.x; I[7] = r2.y; I[8] = r2.z;
 }
 
 // The records are written by kernel 2 and only read here, so the read-only
-// data path may serve them.
-RD void load_man(const DynManifoldRec* __restrict__ rec, Man& c) {
-    const float4* __restrict__ q = rec->q;
-    const float4 ids = __ldg(q + DQ_IDS), ms = __ldg(q + DQ_MASS);
+// data path may serve them (LDG); the giant-island kernel reads copies staged
+// in shared memory (generic loads).
+template <bool LDG = true>
+RD void load_man_q(const float4* __restrict__ q, Man& c) {
+    const float4 ids = ldq<LDG>(q + DQ_IDS), ms = ldq<LDG>(q + DQ_MASS);
     c.b1 = __float_as_int(ids.x); c.b2 = __float_as_int(ids.y);
     c.nb = __float_as_int(ids.z); c.pstart = __float_as_int(ids.w);
     c.im1 = ms.x; c.im2 = ms.y; c.friction = ms.z; c.fixed = uint32_t(ms.w);
-    c.lf1 = L3(__ldg(q + DQ_LF1)); c.lf2 = L3(__ldg(q + DQ_LF2));
-    c.af1 = L3(__ldg(q + DQ_AF1)); c.af2 = L3(__ldg(q + DQ_AF2));
-    rows3(q + DQ_I1, c.I1);
-    rows3(q + DQ_I2, c.I2);
-    const float4 n = __ldg(q + DQ_N), r1f = __ldg(q + DQ_R1F), r2f = __ldg(q + DQ_R2F);
+    c.lf1 = L3(ldq<LDG>(q + DQ_LF1)); c.lf2 = L3(ldq<LDG>(q + DQ_LF2));
+    c.af1 = L3(ldq<LDG>(q + DQ_AF1)); c.af2 = L3(ldq<LDG>(q + DQ_AF2));
+    rows3<LDG>(q + DQ_I1, c.I1);
+    rows3<LDG>(q + DQ_I2, c.I2);
+    const float4 n = ldq<LDG>(q + DQ_N), r1f = ldq<LDG>(q + DQ_R1F), r2f = ldq<LDG>(q + DQ_R2F);
     c.n = L3(n); c.inv_tw = n.w;
     c.r1f = L3(r1f); c.inv_f1 = r1f.w;
     c.r2f = L3(r2f); c.inv_f2 = r2f.w;
-    c.fv1 = L3(__ldg(q + DQ_FV1)); c.fv2 = L3(__ldg(q + DQ_FV2));
-    c.r1ct1 = L3(__ldg(q + DQ_R1CT1)); c.r1ct2 = L3(__ldg(q + DQ_R1CT2));
-    c.r2ct1 = L3(__ldg(q + DQ_R2CT1)); c.r2ct2 = L3(__ldg(q + DQ_R2CT2));
+    c.fv1 = L3(ldq<LDG>(q + DQ_FV1)); c.fv2 = L3(ldq<LDG>(q + DQ_FV2));
+    c.r1ct1 = L3(ldq<LDG>(q + DQ_R1CT1)); c.r1ct2 = L3(ldq<LDG>(q + DQ_R1CT2));
+    c.r2ct1 = L3(ldq<LDG>(q + DQ_R2CT1)); c.r2ct2 = L3(ldq<LDG>(q + DQ_R2CT2));
 }
+RD void load_man(const DynManifoldRec* __restrict__ rec, Man& c) { load_man_q<true>(rec->q, c); }
 
 struct Pt {
     v3 r1, r2, n, i1, i2;
     float depth, inv_mass, bias;
 };
 
-RD void load_pt(const DynPointRec* __restrict__ rec, Pt& p) {
-    const float4 a = __ldg(rec->q + DP_R1), b = __ldg(rec->q + DP_R2), c = __ldg(rec->q + DP_N);
+template <bool LDG = true>
+RD void load_pt_q(const float4* __restrict__ q, Pt& p) {
+    const float4 a = ldq<LDG>(q + DP_R1), b = ldq<LDG>(q + DP_R2), c = ldq<LDG>(q + DP_N);
     p.r1 = L3(a); p.depth = a.w;
     p.r2 = L3(b); p.inv_mass = b.w;
     p.n = L3(c); p.bias = c.w;
-    p.i1 = L3(__ldg(rec->q + DP_I1));
-    p.i2 = L3(__ldg(rec->q + DP_I2));
+    p.i1 = L3(ldq<LDG>(q + DP_I1));
+    p.i2 = L3(ldq<LDG>(q + DP_I2));
 }
 
 // v -= im * imp * lock  /  v += im * imp * lock, per component (Vector3 operators)
@@ -315,6 +325,28 @@ struct BodyVel {
     float4 *v1, *w1, *s1, *t1, *v2, *w2, *s2, *t2;
 };
 
+// Where the solver reads a manifold's constant rows and reads / writes its
+// impulses: the records in global memory, or copies in shared memory.
+// Point k's rows are at pq + k * pq_stride, its impulses at pmut + k * pmut_stride.
+struct RecSrc {
+    const float4* mq;
+    float4* mmut;
+    const float4* pq;
+    float4* pmut;
+    int pq_stride, pmut_stride;
+};
+constexpr int PREC_F4 = int(sizeof(DynPointRec) / sizeof(float4));
+RD RecSrc rec_global(const DynArgs& a, uint32_t mi, int32_t pstart) {
+    RecSrc r;
+    r.mq = a.mrec[mi].q;
+    r.mmut = &a.mrec[mi].mut;
+    r.pq = a.prec[pstart].q;
+    r.pmut = &a.prec[pstart].mut;
+    r.pq_stride = PREC_F4;
+    r.pmut_stride = PREC_F4;
+    return r;
+}
+
 RD BodyVel vel_global(const DynArgs& a, int32_t b1, int32_t b2) {
     BodyVel p;
     p.v1 = a.cv + b1; p.w1 = a.cw + b1; p.s1 = a.sv + b1; p.t1 = a.sw + b1;
@@ -325,21 +357,22 @@ RD BodyVel vel_global(const DynArgs& a, int32_t b1, int32_t b2) {
 // warmStart (:324-476) of one manifold: its two bodies' velocities are loaded,
 // updated in the reference's statement order and stored back (the two bodies
 // are distinct; fixed bodies are never stored).
-RD void warm_manifold(const DynArgs& a, uint32_t mi, const BodyVel& bv, int32_t nb, int32_t pstart) {
+template <bool LDG>
+RD void warm_core(const DynArgs& a, const RecSrc& r, const BodyVel& bv, int32_t nb) {
     if (nb == 0) return;  // rejected by the manifold kernel
     Man c;
-    load_man(a.mrec + mi, c);
-    const v3 o1 = L3(__ldg(a.mrec[mi].q + DQ_OFV1)), o2 = L3(__ldg(a.mrec[mi].q + DQ_OFV2));
-    float4 mut = a.mrec[mi].mut;
+    load_man_q<LDG>(r.mq, c);
+    const v3 o1 = L3(ldq<LDG>(r.mq + DQ_OFV1)), o2 = L3(ldq<LDG>(r.mq + DQ_OFV2));
+    float4 mut = *r.mmut;
     v3 v1 = L3(*bv.v1), w1 = L3(*bv.w1), v2 = L3(*bv.v2), w2 = L3(*bv.w2);
     bool resting_any = false;
     for (int k = 0; k < nb; k++) {
-        DynPointRec* pr = a.prec + pstart + k;
-        float4 pm = pr->mut;
+        float4* pmp = r.pmut + k * r.pmut_stride;
+        float4 pm = *pmp;
         if (pm.z != 0.0f) {
             resting_any = true;
             Pt p;
-            load_pt(pr, p);
+            load_pt_q<LDG>(r.pq + k * r.pq_stride, p);
             const float pi = pm.x;
             const v3 ip = V(p.n.x * pi, p.n.y * pi, p.n.z * pi);
             v1 = lin_sub(v1, c.im1, ip, c.lf1);
@@ -348,7 +381,7 @@ RD void warm_manifold(const DynArgs& a, uint32_t mi, const BodyVel& bv, int32_t 
             w2 = ang_add(w2, p.i2, c.af2, pi);
         } else {
             pm.x = 0.0f;
-            pr->mut = pm;
+            *pmp = pm;
         }
     }
     float f1 = mut.x, f2 = mut.y, ftw = mut.z;
@@ -383,25 +416,29 @@ RD void warm_manifold(const DynArgs& a, uint32_t mi, const BodyVel& bv, int32_t 
     } else {
         f1 = 0.0f; f2 = 0.0f; ftw = 0.0f;
     }
-    a.mrec[mi].mut = make_float4(f1, f2, ftw, mut.w);
+    *r.mmut = make_float4(f1, f2, ftw, mut.w);
     if (!(c.fixed & 1)) { *bv.v1 = F4(v1); *bv.w1 = F4(w1); }
     if (!(c.fixed & 2)) { *bv.v2 = F4(v2); *bv.w2 = F4(w2); }
 }
+RD void warm_manifold(const DynArgs& a, uint32_t mi, const BodyVel& bv, int32_t nb, int32_t pstart) {
+    warm_core<true>(a, rec_global(a, mi, pstart), bv, nb);
+}
 
 // One solve pass (:479-759) over one manifold.
-RD void solve_manifold(const DynArgs& a, uint32_t mi, float beta, const BodyVel& bv, int32_t nb, int32_t pstart) {
+template <bool LDG>
+RD void solve_core(const DynArgs& a, const RecSrc& r, float beta, const BodyVel& bv, int32_t nb) {
     if (nb == 0) return;
     Man c;
-    load_man(a.mrec + mi, c);
-    float4 mut = a.mrec[mi].mut;
+    load_man_q<LDG>(r.mq, c);
+    float4 mut = *r.mmut;
     v3 v1 = L3(*bv.v1), w1 = L3(*bv.w1), v2 = L3(*bv.v2), w2 = L3(*bv.w2);
     v3 s1 = L3(*bv.s1), t1 = L3(*bv.t1), s2 = L3(*bv.s2), t2 = L3(*bv.t2);
     float sum_pen = 0.0f;
     for (int k = 0; k < nb; k++) {
-        DynPointRec* pr = a.prec + pstart + k;
+        float4* pmp = r.pmut + k * r.pmut_stride;
         Pt p;
-        load_pt(pr, p);
-        float4 pm = pr->mut;
+        load_pt_q<LDG>(r.pq + k * r.pq_stride, p);
+        float4 pm = *pmp;
         const v3 n = p.n;
         const v3 dv = rel_velocity(v1, w1, v2, w2, p.r1, p.r2);
         const float Jv = dv.x * n.x + dv.y * n.y + dv.z * n.z;
@@ -436,7 +473,7 @@ RD void solve_manifold(const DynArgs& a, uint32_t mi, float beta, const BodyVel&
             s2 = lin_add(s2, c.im2, lis, c.lf2);
             t2 = ang_add(t2, p.i2, c.af2, dls);
         }
-        pr->mut = pm;
+        *pmp = pm;
     }
     float f1 = mut.x, f2 = mut.y, ftw = mut.z;
     // first friction constraint
@@ -486,9 +523,12 @@ RD void solve_manifold(const DynArgs& a, uint32_t mi, float beta, const BodyVel&
         w1 = vsub(w1, vcmul(c.af1, mv(c.I1, ai2)));
         w2 = vadd(w2, vcmul(c.af2, mv(c.I2, ai2)));
     }
-    a.mrec[mi].mut = make_float4(f1, f2, ftw, mut.w);
+    *r.mmut = make_float4(f1, f2, ftw, mut.w);
     if (!(c.fixed & 1)) { *bv.v1 = F4(v1); *bv.w1 = F4(w1); *bv.s1 = F4(s1); *bv.t1 = F4(t1); }
     if (!(c.fixed & 2)) { *bv.v2 = F4(v2); *bv.w2 = F4(w2); *bv.s2 = F4(s2); *bv.t2 = F4(t2); }
+}
+RD void solve_manifold(const DynArgs& a, uint32_t mi, float beta, const BodyVel& bv, int32_t nb, int32_t pstart) {
+    solve_core<true>(a, rec_global(a, mi, pstart), beta, bv, nb);
 }
 
 // storeImpulses (:763-785) of one manifold.
@@ -528,6 +568,9 @@ RD void store_manifold(const DynArgs& a, uint32_t mi) {
 
 constexpr uint32_t SMALL_ISLAND = 8;
 constexpr uint32_t BIG_ISLAND = 64;   // queued first: the longest islands start first
+// islands above this many manifolds go to kernel 3c (one CTA per island,
+// the island staged in up to the whole opt-in shared memory of a CTA)
+constexpr uint32_t GIANT_ISLAND = 256;
 
 RD int4 man_ids(const DynArgs& a, uint32_t mi) {
     const float4 q = __ldg(a.mrec[mi].q + DQ_IDS);
@@ -546,7 +589,8 @@ __global__ void __launch_bounds__(128) dyn_islands_small(const DynArgs a) {
     if (cnt == 0) return;
     if (cnt > SMALL_ISLAND) {
         // big islands fill the list from the front, the others from the back
-        if (cnt > BIG_ISLAND) a.large_list[atomicAdd(a.counters, 1u)] = is;
+        if (cnt > GIANT_ISLAND) a.giant_list[atomicAdd(a.counters + 3, 1u)] = is;
+        else if (cnt > BIG_ISLAND) a.large_list[atomicAdd(a.counters, 1u)] = is;
         else a.large_list[a.ni - 1 - atomicAdd(a.counters + 2, 1u)] = is;
         return;
     }
@@ -763,6 +807,303 @@ __global__ void __launch_bounds__(LARGE_WARPS * 32, 2) dyn_islands_large(const D
     }
 }
 
+
+// ---- kernel 3c: islands of more than GIANT_ISLAND manifolds --------------
+//
+// One CTA of two warps takes one island at a time with the CTA's whole opt-in
+// shared memory: the movable bodies' velocities, every manifold's and point's
+// impulses, the manifold table and the level schedule (built by lane 0 with a
+// shared hash of body -> slot, last level) stay on chip for the warm start and
+// all velocity iterations.  Warp 0 solves, level after level; warp 1 stages
+// the constant rows of the manifolds (and their points) of level t + 2 into a
+// three-level ring with cp.async, with a compact descriptor per manifold,
+// while warp 0 solves level t, so warp 0's time per level is its arithmetic.
+// The two warps meet at one named barrier per level.  The arithmetic is
+// warm_core / solve_core, the same as the other paths: only where the rows and
+// impulses live changes.  An island that does not fit falls back to the
+// schedule in global scratch (solve_global), run by warp 0.
+constexpr uint32_t GIANT_RING = 8;     // manifolds of a level staged (the first 8)
+constexpr uint32_t GIANT_LEVELS = 3;   // levels in the ring
+constexpr uint32_t GIANT_THREADS = 64;
+struct __align__(16) GiantSlot {
+    int4 desc;                         // slot 1 | slot 2 << 16 (0xffff: fixed), points, manifold (island index), first point
+    float4 mq[DQ_ROWS];
+    float4 pq[4 * PREC_F4];
+};
+
+RD void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+RD void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+RD void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+// named barrier 1 over both warps of the CTA
+RD void giant_bar() { asm volatile("bar.sync 1, %0;\n" ::"n"(GIANT_THREADS) : "memory"); }
+
+struct GiantStage {
+    float4 *vel, *mmut, *pmut;
+    GiantSlot* ring;
+    int32_t *hkey, *slot_body;
+    uint32_t* hval;
+    int2* man;             // body ids (fixed bodies as -1 - id)
+    short2* slot;          // staged slot of body 1 / body 2 (-1: fixed)
+    uint16_t *order, *klev, *lev;
+    uint32_t* pofs;        // first point of each manifold, relative to the island's first point
+    uint8_t* npt;
+    uint32_t H, nbmax;
+};
+
+RD bool giant_layout(const DynArgs& a, uint32_t cnt, uint32_t np, unsigned char* sm, GiantStage& g) {
+    if (cnt > 65535u) return false;
+    g.nbmax = 2 * cnt < a.nb ? 2 * cnt : a.nb;
+    if (g.nbmax > 32767u) return false;
+    g.H = 1;
+    while (g.H < 2 * g.nbmax) g.H <<= 1;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { const size_t o = off; off = (off + bytes + 15) & ~size_t(15); return sm + o; };
+    g.vel = reinterpret_cast<float4*>(take(size_t(4) * g.nbmax * 16));
+    g.mmut = reinterpret_cast<float4*>(take(size_t(cnt) * 16));
+    g.pmut = reinterpret_cast<float4*>(take(size_t(np) * 16));
+    g.ring = reinterpret_cast<GiantSlot*>(take(size_t(GIANT_LEVELS) * GIANT_RING * sizeof(GiantSlot)));
+    g.hkey = reinterpret_cast<int32_t*>(take(size_t(g.H) * 4));
+    g.hval = reinterpret_cast<uint32_t*>(take(size_t(g.H) * 4));
+    g.slot_body = reinterpret_cast<int32_t*>(take(size_t(g.nbmax) * 4));
+    g.man = reinterpret_cast<int2*>(take(size_t(cnt) * 8));
+    g.slot = reinterpret_cast<short2*>(take(size_t(cnt) * 4));
+    g.order = reinterpret_cast<uint16_t*>(take(size_t(cnt) * 2));
+    g.klev = reinterpret_cast<uint16_t*>(take(size_t(cnt) * 2));
+    g.lev = reinterpret_cast<uint16_t*>(take(size_t(cnt + 1) * 2));
+    g.pofs = reinterpret_cast<uint32_t*>(take(size_t(cnt) * 4));
+    g.npt = take(size_t(cnt));
+    return off <= a.giant_smem;
+}
+
+RD bool giant_body(GiantStage& g, int32_t b, uint32_t& nslots, uint32_t& idx) {
+    uint32_t h = (uint32_t(b) * 2654435761u) & (g.H - 1);
+    for (uint32_t probe = 0; probe < g.H; probe++, h = (h + 1) & (g.H - 1)) {
+        const int32_t k = g.hkey[h];
+        if (k == b) { idx = h; return true; }
+        if (k < 0) {
+            if (nslots >= g.nbmax) return false;
+            g.hkey[h] = b;
+            g.hval[h] = nslots << 16;
+            g.slot_body[nslots] = b;
+            nslots++;
+            idx = h;
+            return true;
+        }
+    }
+    return false;
+}
+
+// Stage and schedule an island (warp 0); false (nothing written to global
+// memory) when it does not fit or its points are not one contiguous range.
+RD bool giant_schedule(const DynArgs& a, uint32_t m0, uint32_t cnt, unsigned char* sm, GiantStage& g,
+                       uint32_t lane, uint32_t& depth, uint32_t& nslots, uint32_t& p0) {
+    const int4 f = man_ids(a, m0), l = man_ids(a, m0 + cnt - 1);
+    p0 = uint32_t(f.w);
+    const int64_t end = int64_t(l.w) + int64_t(l.z);
+    if (f.w < 0 || end < int64_t(p0) || end > int64_t(a.np)) return false;
+    const uint32_t np = uint32_t(end - int64_t(p0));
+    if (!giant_layout(a, cnt, np, sm, g)) return false;
+    for (uint32_t h = lane; h < g.H; h += 32) g.hkey[h] = -1;
+    for (uint32_t k = lane; k < cnt; k += 32) {
+        const int4 id = man_ids(a, m0 + k);
+        const uint32_t fixed = man_fixed(a, m0 + k);
+        g.man[k] = make_int2((fixed & 1) ? -1 - id.x : id.x, (fixed & 2) ? -1 - id.y : id.y);
+        g.pofs[k] = uint32_t(id.w) - p0;
+        g.npt[k] = uint8_t(id.z < 0 ? 0 : (id.z > 255 ? 255 : id.z));
+    }
+    __syncwarp();
+    bool ok = true;
+    if (lane == 0) {
+        depth = 0;
+        nslots = 0;
+        uint32_t expect = 0;
+        for (uint32_t k = 0; k < cnt && ok; k++) {
+            const int2 id = g.man[k];
+            if (g.pofs[k] != expect || g.npt[k] > 4) { ok = false; break; }
+            expect += g.npt[k];
+            uint32_t L = 1;
+            short2 sl = make_short2(-1, -1);
+            if (g.npt[k] != 0) {
+                uint32_t h1 = 0, h2 = 0, l1 = 0, l2 = 0;
+                if (id.x >= 0) { ok = giant_body(g, id.x, nslots, h1); if (ok) { l1 = g.hval[h1] & 0xffffu; sl.x = short(g.hval[h1] >> 16); } }
+                if (ok && id.y >= 0) { ok = giant_body(g, id.y, nslots, h2); if (ok) { l2 = g.hval[h2] & 0xffffu; sl.y = short(g.hval[h2] >> 16); } }
+                if (!ok) break;
+                L = 1 + (l1 > l2 ? l1 : l2);
+                if (id.x >= 0) g.hval[h1] = (g.hval[h1] & 0xffff0000u) | L;
+                if (id.y >= 0) g.hval[h2] = (g.hval[h2] & 0xffff0000u) | L;
+            }
+            g.slot[k] = sl;
+            g.klev[k] = uint16_t(L);
+            depth = L > depth ? L : depth;
+        }
+        if (ok && expect != np) ok = false;
+        if (ok) {
+            for (uint32_t L = 0; L <= depth; L++) g.lev[L] = 0;
+            for (uint32_t k = 0; k < cnt; k++) g.lev[g.klev[k] - 1]++;
+            uint32_t run = 0;
+            for (uint32_t L = 0; L < depth; L++) { run += g.lev[L]; g.lev[L] = uint16_t(run); }
+            g.lev[depth] = uint16_t(cnt);
+            for (uint32_t k = cnt; k-- > 0;) g.order[--g.lev[g.klev[k] - 1]] = uint16_t(k);
+        }
+    }
+    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+    depth = __shfl_sync(0xffffffffu, depth, 0);
+    nslots = __shfl_sync(0xffffffffu, nslots, 0);
+    __syncwarp();
+    return ok;
+}
+
+// Warp 1: stage level t (of the linearised passes x levels) into ring level t % 3.
+RD void giant_stage_level(const DynArgs& a, const GiantStage& g, uint32_t m0, uint32_t p0, uint32_t depth,
+                          uint32_t total, uint32_t t, uint32_t lane) {
+    if (t < total) {
+        const uint32_t L = t % depth;
+        const uint32_t j = g.lev[L] + lane;
+        if (lane < GIANT_RING && j < g.lev[L + 1]) {
+            const uint32_t kk = g.order[j];
+            GiantSlot* sl = g.ring + (t % GIANT_LEVELS) * GIANT_RING + lane;
+            const short2 bs = g.slot[kk];
+            const uint32_t np = g.npt[kk];
+            sl->desc = make_int4(int(uint32_t(uint16_t(bs.x)) | (uint32_t(uint16_t(bs.y)) << 16)), int(np), int(kk),
+                                 int(g.pofs[kk]));
+            const float4* src = a.mrec[m0 + kk].q;
+            for (int r = 0; r < DQ_ROWS; r++) cp_async16(&sl->mq[r], src + r);
+            const float4* ps = a.prec[p0 + g.pofs[kk]].q;
+            for (uint32_t r = 0; r < np * PREC_F4; r++) cp_async16(&sl->pq[r], ps + r);
+        }
+    }
+    cp_async_commit();
+}
+
+RD BodyVel giant_vel(const DynArgs& a, const GiantStage& g, int32_t s1, int32_t s2, int2 id) {
+    BodyVel bv;
+    const uint32_t n = g.nbmax;
+    if (s1 >= 0) { bv.v1 = g.vel + s1; bv.w1 = g.vel + n + s1; bv.s1 = g.vel + 2 * n + s1; bv.t1 = g.vel + 3 * n + s1; }
+    else { const int32_t b1 = -1 - id.x; bv.v1 = a.cv + b1; bv.w1 = a.cw + b1; bv.s1 = a.sv + b1; bv.t1 = a.sw + b1; }
+    if (s2 >= 0) { bv.v2 = g.vel + s2; bv.w2 = g.vel + n + s2; bv.s2 = g.vel + 2 * n + s2; bv.t2 = g.vel + 3 * n + s2; }
+    else { const int32_t b2 = -1 - id.y; bv.v2 = a.cv + b2; bv.w2 = a.cw + b2; bv.s2 = a.sv + b2; bv.t2 = a.sw + b2; }
+    return bv;
+}
+
+// Both warps: stage, solve and write back one island.
+RD void giant_solve(const DynArgs& a, uint32_t m0, uint32_t cnt, const GiantStage& g, uint32_t warp,
+                    uint32_t lane, uint32_t depth, uint32_t nslots, uint32_t p0) {
+    const uint32_t np = g.pofs[cnt - 1] + g.npt[cnt - 1];
+    const uint32_t tid = warp * 32 + lane;
+    for (uint32_t s = tid; s < nslots; s += GIANT_THREADS) {
+        const int32_t b = g.slot_body[s];
+        g.vel[s] = a.cv[b];
+        g.vel[g.nbmax + s] = a.cw[b];
+        g.vel[2 * g.nbmax + s] = a.sv[b];
+        g.vel[3 * g.nbmax + s] = a.sw[b];
+    }
+    for (uint32_t k = tid; k < cnt; k += GIANT_THREADS) g.mmut[k] = a.mrec[m0 + k].mut;
+    for (uint32_t p = tid; p < np; p += GIANT_THREADS) g.pmut[p] = a.prec[p0 + p].mut;
+    const uint32_t total = uint32_t(a.iterations + 1) * depth;
+    if (warp == 1) {
+        giant_stage_level(a, g, m0, p0, depth, total, 0, lane);
+        giant_stage_level(a, g, m0, p0, depth, total, 1, lane);
+        cp_async_wait<1>();
+        giant_bar();                       // level 0 staged, stage loads done
+        for (uint32_t t = 0; t < total; t++) {
+            giant_stage_level(a, g, m0, p0, depth, total, t + 2, lane);
+            cp_async_wait<1>();            // level t + 1 staged
+            giant_bar();                   // end of level t
+        }
+        cp_async_wait<0>();
+    } else {
+        const float beta = a.split ? BETA_SPLIT_IMPULSE : BETA;
+        giant_bar();
+        for (uint32_t t = 0; t < total; t++) {
+            const uint32_t L = t % depth;
+            const bool warm = t < depth;
+            const uint32_t b = g.lev[L], e = g.lev[L + 1];
+            if (lane < GIANT_RING && b + lane < e) {
+                const GiantSlot* sl = g.ring + (t % GIANT_LEVELS) * GIANT_RING + lane;
+                const int4 d = sl->desc;
+                const int32_t s1 = int32_t(int16_t(d.x & 0xffff)), s2 = int32_t(int16_t(uint32_t(d.x) >> 16));
+                const BodyVel bv = giant_vel(a, g, s1, s2, g.man[d.z]);
+                RecSrc r;
+                r.mq = sl->mq;
+                r.pq = sl->pq;
+                r.pq_stride = PREC_F4;
+                r.mmut = g.mmut + d.z;
+                r.pmut = g.pmut + d.w;
+                r.pmut_stride = 1;
+                if (warm) warm_core<false>(a, r, bv, d.y);
+                else solve_core<false>(a, r, beta, bv, d.y);
+            }
+            // manifolds of a level beyond the staged ones read their rows from global memory
+            for (uint32_t j = b + GIANT_RING + lane; j < e; j += 32) {
+                const uint32_t kk = g.order[j];
+                const short2 sl = g.slot[kk];
+                const BodyVel bv = giant_vel(a, g, sl.x, sl.y, g.man[kk]);
+                RecSrc r;
+                r.mq = a.mrec[m0 + kk].q;
+                r.pq = a.prec[p0 + g.pofs[kk]].q;
+                r.pq_stride = PREC_F4;
+                r.mmut = g.mmut + kk;
+                r.pmut = g.pmut + g.pofs[kk];
+                r.pmut_stride = 1;
+                if (warm) warm_core<true>(a, r, bv, g.npt[kk]);
+                else solve_core<true>(a, r, beta, bv, g.npt[kk]);
+            }
+            __syncwarp();
+            giant_bar();
+        }
+    }
+    __syncthreads();
+    for (uint32_t s = tid; s < nslots; s += GIANT_THREADS) {
+        const int32_t b = g.slot_body[s];
+        a.cv[b] = g.vel[s];
+        a.cw[b] = g.vel[g.nbmax + s];
+        a.sv[b] = g.vel[2 * g.nbmax + s];
+        a.sw[b] = g.vel[3 * g.nbmax + s];
+    }
+    for (uint32_t k = tid; k < cnt; k += GIANT_THREADS) a.mrec[m0 + k].mut = g.mmut[k];
+    for (uint32_t p = tid; p < np; p += GIANT_THREADS) a.prec[p0 + p].mut = g.pmut[p];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(GIANT_THREADS, 1) dyn_islands_giant(const DynArgs a) {
+    extern __shared__ __align__(16) unsigned char gsm[];
+    __shared__ uint32_t s_island, s_ok, s_depth, s_nslots, s_p0;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t n_giant = a.counters[3];
+    for (;;) {
+        if (threadIdx.x == 0) s_island = atomicAdd(a.counters + 4, 1u);
+        __syncthreads();
+        const uint32_t k = s_island;
+        if (k >= n_giant) break;
+        const uint32_t is = a.giant_list[k];
+        const uint32_t m0 = a.i_start[is], cnt = a.i_count[is];
+        GiantStage g;
+        if (warp == 0) {
+            uint32_t depth = 0, nslots = 0, p0 = 0;
+            const bool ok = giant_schedule(a, m0, cnt, gsm, g, lane, depth, nslots, p0);
+            if (lane == 0) { s_ok = ok ? 1u : 0u; s_depth = depth; s_nslots = nslots; s_p0 = p0; }
+        }
+        __syncthreads();
+        if (s_ok) {
+            if (warp == 1) {
+                // the same layout (a pure function of the island's sizes)
+                const int4 l = man_ids(a, m0 + cnt - 1);
+                giant_layout(a, cnt, uint32_t(int64_t(l.w) + int64_t(l.z) - int64_t(s_p0)), gsm, g);
+            }
+            giant_solve(a, m0, cnt, g, warp, lane, s_depth, s_nslots, s_p0);
+        } else if (warp == 0) {
+            solve_global(a, m0, cnt, lane);
+        }
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < cnt; j += GIANT_THREADS) store_manifold(a, m0 + j);
+        __syncthreads();
+    }
+}
+
 // ---- kernel 4: integrateRigidBodiesPositions + updateBodiesState ----------
 __global__ void __launch_bounds__(128) dyn_bodies_post(const DynArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -814,13 +1155,18 @@ cudaError_t launch_dynamics(const DynArgs& a, cudaStream_t s, uint64_t* launches
     if (a.nb) { dyn_bodies_pre<<<blocks(a.nb), 128, 0, s>>>(a); (*launches)++; }
     if (a.nm) { dyn_manifold_init<<<blocks(a.nm), 128, 0, s>>>(a); (*launches)++; }
     if (a.ni) {
-        cudaMemsetAsync(a.counters, 0, 3 * sizeof(uint32_t), s);
+        cudaMemsetAsync(a.counters, 0, 5 * sizeof(uint32_t), s);
         dyn_islands_small<<<blocks(a.ni), 128, 0, s>>>(a);
         (*launches)++;
         const size_t smem = size_t(LARGE_WARPS) * LARGE_WARP_SMEM;
         cudaFuncSetAttribute(dyn_islands_large, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         dyn_islands_large<<<a.large_ctas, LARGE_WARPS * 32, smem, s>>>(a);
         (*launches)++;
+        if (a.giant_smem) {
+            cudaFuncSetAttribute(dyn_islands_giant, cudaFuncAttributeMaxDynamicSharedMemorySize, int(a.giant_smem));
+            dyn_islands_giant<<<a.giant_ctas, GIANT_THREADS, a.giant_smem, s>>>(a);
+            (*launches)++;
+        }
     }
     if (a.nb_enabled) { dyn_bodies_post<<<blocks(a.nb_enabled), 128, 0, s>>>(a); (*launches)++; }
     if (a.nc_enabled) { dyn_colliders<<<blocks(a.nc_enabled), 128, 0, s>>>(a); (*launches)++; }

@@ -84,9 +84,13 @@ struct DynArgs {
     uint32_t* order;       // nm: island manifolds sorted by level (scratch)
     uint32_t* body_level;  // nb: last level of each movable body (scratch)
     int32_t* body_slot;    // nb: shared-memory slot of each movable body (scratch)
-    uint32_t* counters;    // [0] big islands queued (front of large_list), [1] islands taken, [2] others queued (back)
+    uint32_t* counters;    // [0] big islands queued (front of large_list), [1] islands taken, [2] others queued (back),
+                           // [3] giant islands queued, [4] giant islands taken
     uint32_t* large_list;  // ni: queued islands
+    uint32_t* giant_list;  // ni: islands for kernel 3c
     uint32_t large_ctas;   // grid of kernel 3b (persistent)
+    uint32_t giant_ctas;   // grid of kernel 3c (persistent, one warp per CTA)
+    uint32_t giant_smem;   // dynamic shared memory of a kernel-3c CTA (0: kernel 3c off)
 };
 
 // Launches the kernels in order on stream s; *launches counts them.

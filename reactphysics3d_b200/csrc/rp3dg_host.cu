@@ -175,6 +175,7 @@ BoxTables make_box_tables() {
 struct rp3dg_ctx {
     int device = 0;
     int num_sms = 148;
+    int smem_optin = 0;   // cudaDevAttrMaxSharedMemoryPerBlockOptin
     cudaStream_t stream = nullptr;
     std::string err;
     uint64_t launches = 0;
@@ -330,6 +331,7 @@ int rp3dg_create(int device, rp3dg_ctx** out) {
     ctx->device = device;
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_error, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_error, 0, sizeof(uint32_t), ctx->stream);
@@ -1003,7 +1005,8 @@ int rp3dg_dynamics_step_device(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, 
     const size_t off_bslot = off_blev + al(size_t(b->n) * 4);
     const size_t off_cnt = off_bslot + al(size_t(b->n) * 4);
     const size_t off_list = off_cnt + 256;
-    const size_t need = off_list + al(size_t(is->n) * 4) + 256;
+    const size_t off_giant = off_list + al(size_t(is->n) * 4);
+    const size_t need = off_giant + al(size_t(is->n) * 4) + 256;
     rc = grow(ctx, &ctx->d_dyn, &ctx->cap_dyn, need, "cudaMalloc(dynamics scratch)");
     if (rc) return rc;
     char* s = static_cast<char*>(ctx->d_dyn);
@@ -1060,7 +1063,11 @@ int rp3dg_dynamics_step_device(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, 
     a.body_slot = reinterpret_cast<int32_t*>(s + off_bslot);
     a.counters = reinterpret_cast<uint32_t*>(s + off_cnt);
     a.large_list = reinterpret_cast<uint32_t*>(s + off_list);
+    a.giant_list = reinterpret_cast<uint32_t*>(s + off_giant);
     a.large_ctas = uint32_t(ctx->num_sms) * 2;
+    a.giant_ctas = uint32_t(ctx->num_sms);
+    // the opt-in maximum less room for the kernel's static shared memory
+    a.giant_smem = ctx->smem_optin > 2048 ? uint32_t(ctx->smem_optin - 1024) : 0u;
     cudaError_t e = rp3dg::launch_dynamics(a, ctx->stream, &ctx->launches);
     return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "dynamics launch");
 }
