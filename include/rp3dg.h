@@ -539,6 +539,31 @@ int rp3dg_world_get_contacts(rp3dg_world* world, int32_t* body1, int32_t* body2,
                              uint32_t capacity, float* normal_depth, float* local1, float* local2,
                              uint32_t capacity_points, uint32_t* nb_manifolds, uint32_t* nb_contact_points);
 int rp3dg_world_get_stats(rp3dg_world* world, rp3dg_world_stats* stats);
+
+/* Many independent worlds stepped together (the batch of the many-worlds
+ * workload): nb_worlds worlds, world k made of bodies[body_offsets[k] ..
+ * body_offsets[k+1]) and colliders[collider_offsets[k] .. collider_offsets[k+1])
+ * (collider body indices local to the world), each built like
+ * rp3dg_world_create and each stepping exactly as its own PhysicsWorld would
+ * (bit-identical to a reference world per world).  One rp3dg_world_update
+ * steps every world; the GPU work of all worlds runs in shared launches and
+ * the order bookkeeping of the worlds on nb_threads host threads.  The
+ * returned handle works with rp3dg_world_update / _destroy / _get_stats /
+ * _set_profiling / _get_phase_times (rp3dg_world_get_bodies then returns all
+ * worlds' bodies, world after world); the calls below read one world.  No
+ * counterpart in the reference, where each world is its own PhysicsWorld. */
+int rp3dg_world_group_create(rp3dg_ctx* ctx, const rp3dg_world_settings* settings, uint32_t nb_worlds,
+                             const uint32_t* body_offsets, const rp3dg_body_desc* bodies,
+                             const uint32_t* collider_offsets, const rp3dg_collider_desc* colliders,
+                             int nb_threads, rp3dg_world** out);
+int rp3dg_world_group_get_bodies(rp3dg_world* group, uint32_t world, float* position, float* orientation,
+                                 float* linear_velocity, float* angular_velocity, uint8_t* sleeping);
+int rp3dg_world_group_get_pairs(rp3dg_world* group, uint32_t world, uint64_t* pair_ids, uint32_t capacity,
+                                uint32_t* n);
+int rp3dg_world_group_get_contacts(rp3dg_world* group, uint32_t world, int32_t* body1, int32_t* body2,
+                                   uint8_t* nb_points, uint32_t capacity, float* normal_depth, float* local1,
+                                   float* local2, uint32_t capacity_points, uint32_t* nb_manifolds,
+                                   uint32_t* nb_contact_points);
 /* Phase profiling (instrumentation; no counterpart in the reference, whose
  * profiler is a compile-time option): when enabled, each step drains the
  * stream at phase boundaries and accumulates wall-clock milliseconds per

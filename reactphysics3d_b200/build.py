@@ -18,13 +18,13 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 FP_FLAGS = ["--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-         "-Xcompiler", "-fPIC,-ffp-contract=off", "--shared", "-Xptxas", "-v"] + FP_FLAGS
+         "-Xcompiler", "-fPIC,-ffp-contract=off,-fopenmp", "--shared", "-Xptxas", "-v"] + FP_FLAGS
 
 
 def build(verbose=False, out=LIB, defines=()):
     os.makedirs(os.path.dirname(out), exist_ok=True)
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    cmd = [NVCC] + FLAGS + [f"-D{d}" for d in defines] + srcs + ["-o", out, "-lcudart"]
+    cmd = [NVCC] + FLAGS + [f"-D{d}" for d in defines] + srcs + ["-o", out, "-lcudart", "-lgomp"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)

@@ -41,6 +41,10 @@ RD void quat_matrix_bp(quat q, float* r) {
 __global__ void __launch_bounds__(128) bp_update_kernel(const BpArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n_update) return;
+    if (a.enabled && !a.enabled[i]) {
+        a.moved[i] = 0;
+        return;
+    }
     const int32_t si = a.shape[i];
     if (uint32_t(si) >= a.nb_shapes) {
         atomicOr(a.error, 1u);

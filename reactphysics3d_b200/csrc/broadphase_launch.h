@@ -11,6 +11,7 @@ namespace rp3dg {
 struct BpArgs {
     uint32_t n;           // colliders in the broad phase
     uint32_t n_update;    // colliders [0, n_update) get new AABBs
+    const uint8_t* enabled;  // or null; else only the flagged rows of [0, n_update)
     uint32_t nb_shapes;
     const rp3dg_shape* shapes;
     const float4* bounds;   // 2 per shape: local bounds min, max (CollisionShape::getLocalBounds)

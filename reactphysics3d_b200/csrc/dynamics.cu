@@ -85,6 +85,12 @@ RD v3 unit_orthogonal(v3 v) {
     return V(-v.y / l, v.x / l, 0.0f / l);
 }
 
+// Enabled bodies / colliders: the first nb_enabled / nc_enabled rows, or the
+// rows flagged in b_enabled / c_enabled when those are given (several worlds
+// in one batch, each with its own enabled range).
+RD bool body_enabled(const DynArgs& a, uint32_t i) { return a.b_enabled ? a.b_enabled[i] != 0 : i < a.nb_enabled; }
+RD bool collider_enabled(const DynArgs& a, uint32_t i) { return a.c_enabled ? a.c_enabled[i] != 0 : i < a.nc_enabled; }
+
 // ---- kernel 1: world inverse inertia + velocity integration --------------
 __global__ void __launch_bounds__(128) dyn_bodies_pre(const DynArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -92,7 +98,7 @@ __global__ void __launch_bounds__(128) dyn_bodies_pre(const DynArgs a) {
     const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     a.sv[i] = zero;
     a.sw[i] = zero;
-    if (i >= a.nb_enabled) {
+    if (!body_enabled(a, i)) {
         // read-only body: the solver sees its stored velocity
         a.cv[i] = a.lin_vel[i];
         a.cw[i] = a.ang_vel[i];
@@ -128,7 +134,7 @@ __global__ void __launch_bounds__(128) dyn_bodies_pre(const DynArgs a) {
 }
 
 RD bool is_fixed(const DynArgs& a, int32_t b) {
-    if (uint32_t(b) >= a.nb_enabled) return true;
+    if (uint32_t(b) >= a.nb || !body_enabled(a, uint32_t(b))) return true;
     const float4 il = a.iil[b];
     return a.mass[b].y == 0.0f && il.x == 0.0f && il.y == 0.0f && il.z == 0.0f;
 }
@@ -1107,7 +1113,7 @@ __global__ void __launch_bounds__(GIANT_THREADS, 1) dyn_islands_giant(const DynA
 // ---- kernel 4: integrateRigidBodiesPositions + updateBodiesState ----------
 __global__ void __launch_bounds__(128) dyn_bodies_post(const DynArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.nb_enabled) return;
+    if (i >= a.nb || !body_enabled(a, i)) return;
     const float dt = a.dt;
     const float f = a.split ? 1.0f : 0.0f;
     const v3 cv = L3(a.cv[i]), cw = L3(a.cw[i]);
@@ -1135,7 +1141,7 @@ __global__ void __launch_bounds__(128) dyn_bodies_post(const DynArgs a) {
 // ---- kernel 5: collider local-to-world transforms ------------------------
 __global__ void __launch_bounds__(128) dyn_colliders(const DynArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.nc_enabled) return;
+    if (i >= a.nc || !collider_enabled(a, i)) return;
     const int32_t b = a.c_body[i];
     if (uint32_t(b) >= a.nb) {
         atomicOr(a.error, 4u);
@@ -1168,8 +1174,9 @@ cudaError_t launch_dynamics(const DynArgs& a, cudaStream_t s, uint64_t* launches
             (*launches)++;
         }
     }
-    if (a.nb_enabled) { dyn_bodies_post<<<blocks(a.nb_enabled), 128, 0, s>>>(a); (*launches)++; }
-    if (a.nc_enabled) { dyn_colliders<<<blocks(a.nc_enabled), 128, 0, s>>>(a); (*launches)++; }
+    const uint32_t nbp = a.b_enabled ? a.nb : a.nb_enabled, ncp = a.c_enabled ? a.nc : a.nc_enabled;
+    if (nbp) { dyn_bodies_post<<<blocks(nbp), 128, 0, s>>>(a); (*launches)++; }
+    if (ncp) { dyn_colliders<<<blocks(ncp), 128, 0, s>>>(a); (*launches)++; }
     return cudaGetLastError();
 }
 

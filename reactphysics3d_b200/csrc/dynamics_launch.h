@@ -50,6 +50,7 @@ struct DynArgs {
     float restitution_threshold;
     // bodies
     uint32_t nb, nb_enabled;
+    const uint8_t* b_enabled;   // per-row enabled flag, or null: rows [0, nb_enabled)
     float4 *position, *orientation, *com_world;
     const float4* com_local;
     float4 *lin_vel, *ang_vel;
@@ -59,6 +60,7 @@ struct DynArgs {
     const uint8_t* gravity;
     // colliders
     uint32_t nc, nc_enabled;
+    const uint8_t* c_enabled;   // per-row enabled flag, or null: rows [0, nc_enabled)
     const int32_t* c_body;
     const float4 *c_lpos, *c_lori;
     float4 *c_wpos, *c_wori;

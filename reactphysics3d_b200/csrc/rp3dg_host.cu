@@ -306,6 +306,13 @@ int upload_arena(rp3dg_ctx* ctx) {
 
 }  // namespace
 
+namespace rp3dg {
+int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
+                        const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
+                        const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled);
+int broadphase_update_flags(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, const uint8_t* enabled);
+}  // namespace rp3dg
+
 // host copy of the shape table (world set-up reads it; C++ linkage)
 namespace rp3dg {
 int get_shapes_host(rp3dg_ctx* ctx, std::vector<rp3dg_shape>* out) {
@@ -982,6 +989,15 @@ int check_dynamics(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_
 int rp3dg_dynamics_step_device(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
                                const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
                                const rp3dg_islands* is) {
+    return rp3dg::dynamics_step_flags(ctx, pr, b, c, m, p, is, nullptr, nullptr);
+}
+
+namespace rp3dg {
+// The dynamics stage with the enabled bodies / colliders given as per-row
+// flags (several worlds in one batch) instead of a leading range.
+int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
+                        const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
+                        const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled) {
     int rc = check_dynamics(ctx, pr, b, c, m, p, is);
     if (rc) return rc;
     const void* f16[] = {b->position, b->orientation, b->com_world, b->com_local, b->linear_velocity,
@@ -1010,7 +1026,9 @@ int rp3dg_dynamics_step_device(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, 
     rc = grow(ctx, &ctx->d_dyn, &ctx->cap_dyn, need, "cudaMalloc(dynamics scratch)");
     if (rc) return rc;
     char* s = static_cast<char*>(ctx->d_dyn);
-    rp3dg::DynArgs a;
+    rp3dg::DynArgs a = {};
+    a.b_enabled = b_enabled;
+    a.c_enabled = c_enabled;
     a.dt = pr->dt; a.gx = pr->gravity[0]; a.gy = pr->gravity[1]; a.gz = pr->gravity[2];
     a.gravity_enabled = pr->gravity_enabled; a.iterations = pr->velocity_iterations; a.split = pr->split_impulse ? 1 : 0;
     a.restitution_threshold = pr->restitution_velocity_threshold;
@@ -1071,6 +1089,8 @@ int rp3dg_dynamics_step_device(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, 
     cudaError_t e = rp3dg::launch_dynamics(a, ctx->stream, &ctx->launches);
     return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "dynamics launch");
 }
+}  // namespace rp3dg
+
 
 int rp3dg_dynamics_step_host(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
                              const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
@@ -1160,6 +1180,12 @@ int check_bp(rp3dg_ctx* ctx, const rp3dg_broadphase* bp) {
 }  // namespace
 
 int rp3dg_broadphase_update_device(rp3dg_ctx* ctx, const rp3dg_broadphase* bp) {
+    return rp3dg::broadphase_update_flags(ctx, bp, nullptr);
+}
+
+namespace rp3dg {
+// The fat-AABB update of the flagged rows of [0, n_update) only.
+int broadphase_update_flags(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, const uint8_t* enabled) {
     int rc = check_bp(ctx, bp);
     if (rc) return rc;
     if (bp->n_update == 0) return 0;
@@ -1179,11 +1205,14 @@ int rp3dg_broadphase_update_device(rp3dg_ctx* ctx, const rp3dg_broadphase* bp) {
     a.fat_min = reinterpret_cast<float4*>(bp->fat_min);
     a.fat_max = reinterpret_cast<float4*>(bp->fat_max);
     a.moved = bp->moved;
+    a.enabled = enabled;
     a.error = ctx->d_error;
     cudaSetDevice(ctx->device);
     cudaError_t e = rp3dg::launch_bp_update(a, ctx->stream, &ctx->launches);
     return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "broad-phase update");
 }
+}  // namespace rp3dg
+
 
 int rp3dg_broadphase_pairs_device(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, int axis, int32_t* pairs,
                                   uint32_t capacity, uint32_t* count) {

@@ -28,9 +28,20 @@
 // narrow-phase outcome (colliding flag and kept point count per tested pair)
 // and, after the step, the broad-phase reinsertion flags, the new fat AABBs
 // and the velocities (sleep test).
+//
+// Many worlds step together as a group: each world keeps its own bookkeeping
+// (run for all worlds on the host threads, OpenMP) and its own rows of the
+// group's device arrays (bodies, colliders, cache slots), while every GPU
+// phase is one launch over all worlds: the narrow-phase batches hold the
+// pairs of all worlds (algorithm-major), the contact arrays and islands of
+// all worlds are packed back to back, and the dynamics stage and collider
+// update run on all rows, each world's enabled bodies and colliders given by
+// per-row flags.  A single world (rp3dg_world_create) is a group of one.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <cmath>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -43,9 +54,14 @@
 #include "world_order.h"
 
 namespace rp3dg {
-// host copy of the context's shape table (rp3dg_host.cu)
+// (rp3dg_host.cu) host copy of the context's shape table, error message, and
+// the dynamics stage / fat-AABB update with per-row enabled flags
 int get_shapes_host(rp3dg_ctx* ctx, std::vector<rp3dg_shape>* out);
 void set_error(rp3dg_ctx* ctx, const std::string& msg);
+int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
+                        const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
+                        const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled);
+int broadphase_update_flags(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, const uint8_t* enabled);
 }  // namespace rp3dg
 
 using rp3dg::order::Box;
@@ -258,7 +274,7 @@ uint32_t blocks(uint32_t n) { return (n + 127) / 128; }
 
 // Volume and local inertia tensor of a shape (BoxShape.h:233, BoxShape.cpp:53-59,
 // SphereShape.h:170-178, CapsuleShape.h:175-177, CapsuleShape.cpp:51-67).
-bool shape_mass(const rp3dg_shape& s, float mass_density, float* vol_out, float* inertia /*3*/, float* mass_out) {
+bool shape_mass(const rp3dg_shape& s, float mass_density, float* inertia /*3*/, float* mass_out) {
     const float PI = float(3.141592653589);
     float vol;
     if (s.kind == RP3DG_SHAPE_BOX) {
@@ -297,7 +313,6 @@ bool shape_mass(const rp3dg_shape& s, float mass_density, float* vol_out, float*
         inertia[1] = iy;
         inertia[2] = ixz;
     }
-    *vol_out = vol;
     *mass_out = mass;
     return true;
 }
@@ -348,10 +363,10 @@ struct ContactPairH {
     uint32_t item;       // global narrow-phase item
     uint32_t k;          // points after the manifold step
     bool in_island = false;
-    uint32_t manifold = 0, point = 0;  // indices in the packed arrays
+    uint32_t manifold = 0, point = 0;  // global indices in the packed arrays
 };
 struct IslandH {
-    uint32_t manifold_start = 0, manifold_count = 0;
+    uint32_t manifold_start = 0, manifold_count = 0;  // world-local manifold range
     std::vector<int> bodies;
 };
 
@@ -390,12 +405,11 @@ int host_grow(T** p, size_t* cap, size_t need) {
     return 0;
 }
 
-// Device columns of the rigid-body components (row = component slot).
+// Device columns of the rigid-body components (row = world's first row + component slot).
 enum BodyCol { BC_POS, BC_ORI, BC_COMW, BC_COML, BC_LV, BC_AV, BC_F, BC_T, BC_IIL, BC_MASS, BC_LLOCK, BC_ALOCK, BC_NCOL };
 enum ColCol { CC_LPOS, CC_LORI, CC_WPOS, CC_WORI, CC_MAT, CC_FMIN, CC_FMAX, CC_NCOL };
 
 struct ContactBuf {
-    size_t cap_m = 0, cap_p = 0;
     int4* ids = nullptr;
     uint32_t* pstart = nullptr;
     uint8_t* npts = nullptr;
@@ -427,16 +441,11 @@ struct ContactBuf {
     }
 };
 
-}  // namespace
-
-struct rp3dg_world {
-    rp3dg_ctx* ctx = nullptr;
-    cudaStream_t stream = nullptr;
-    rp3dg_world_settings set{};
-    uint32_t nb = 0, nc = 0;
+// One world's order bookkeeping (host) and its rows in the group's arrays.
+struct WorldH {
+    uint32_t nb = 0, nc = 0, b0 = 0, c0 = 0;  // bodies at rows [b0, b0 + nb), colliders [c0, c0 + nc)
     std::vector<BodyH> bodies;
     std::vector<ColliderH> colliders;
-    std::vector<rp3dg_shape> shapes;
     rp3dg::order::Comps bcomp, ccomp;
     rp3dg::order::Tree tree;
     rp3dg::order::IdSet moved;
@@ -445,30 +454,54 @@ struct rp3dg_world {
     std::vector<PairH> pairs, disabled;
     std::unordered_map<uint64_t, uint32_t> map_pairs, map_disabled;
     std::vector<int> free_cache;
-    uint32_t cache_next = 0;
     std::vector<int32_t> reset_slots;
-    // contacts of this step and the previous one
+    // contacts of this step and of the previous one
     std::vector<ContactPairH> cpairs, prev_cpairs;
     std::unordered_map<uint64_t, uint32_t> prev_map;
     std::vector<uint32_t> island_order;  // mProcessContactPairsOrderIslands
     std::vector<IslandH> islands;
-    // device rows currently in the order of these slot lists
-    std::vector<int> dev_body_at, dev_col_at;
+    std::vector<int> dev_body_at, dev_col_at;  // component order the device rows have
+    uint32_t dev_nb_en = ~0u, dev_nc_en = ~0u; // enabled counts the device flags hold
+    std::vector<uint8_t> gravity;              // by body id
+    // this step
+    std::vector<int4> items[NB_ALGOS];
+    std::vector<uint32_t> item_pair[NB_ALGOS];
+    uint32_t item_off[NB_ALGOS] = {};
+    uint32_t nm = 0, np = 0, man_base = 0, pt_base = 0, isl_base = 0;
+    std::vector<int> slept;                    // bodies put to sleep by this step
+    rp3dg_world_stats stats{};
+};
+
+}  // namespace
+
+struct rp3dg_world {
+    rp3dg_ctx* ctx = nullptr;
+    cudaStream_t stream = nullptr;
+    rp3dg_world_settings set{};
+    std::vector<rp3dg_shape> shapes;
+    std::vector<WorldH> worlds;
+    uint32_t NB = 0, NC = 0;  // rows of all worlds
+    int nthreads = 1;
+    std::atomic<uint32_t> cache_next{0};
     // device state
     float4* bcol[2][BC_NCOL] = {};
     float4* biiw[2] = {};
-    uint8_t* bgrav = nullptr;
+    uint8_t *bgrav = nullptr, *b_en = nullptr, *c_en = nullptr;
     float4* ccol[2][CC_NCOL] = {};
-    int32_t* c_body = nullptr;
-    int32_t* c_shape = nullptr;
+    int32_t *c_body = nullptr, *c_shape = nullptr;
     uint16_t *c_cat = nullptr, *c_mask = nullptr;
     uint8_t* c_moved = nullptr;
     int cur_b = 0, cur_c = 0;
     rp3dg_lastframe* pool = nullptr;
     size_t cap_pool = 0;
-    int32_t* d_small = nullptr;  // reset slots / permutation / rows
+    int32_t* d_small = nullptr;
     size_t cap_small = 0;
-    // narrow-phase step buffers (all batches concatenated)
+    bool tables_dirty = true;
+    // pinned host copies of the per-row tables and the row permutations
+    uint8_t *t_grav = nullptr, *t_ben = nullptr, *t_cen = nullptr;
+    int32_t *t_cbody = nullptr, *t_cshape = nullptr, *t_bperm = nullptr, *t_cperm = nullptr;
+    uint16_t *t_cat = nullptr, *t_mask = nullptr;
+    // narrow-phase step buffers (all batches of all worlds concatenated)
     size_t cap_items = 0;
     int4* d_items = nullptr;
     int32_t *d_s1 = nullptr, *d_s2 = nullptr;
@@ -476,50 +509,42 @@ struct rp3dg_world {
     uint8_t *d_rep = nullptr, *d_coll = nullptr, *d_nct = nullptr;
     rp3dg_lastframe* d_cache = nullptr;
     float4 *d_nd = nullptr, *d_l1 = nullptr, *d_l2 = nullptr;
-    // manifold packing inputs
-    size_t cap_m = 0;
+    uint32_t batch_start[NB_ALGOS + 1] = {};
+    // manifold packing
+    size_t cap_m = 0, cap_i = 0;
     int4 *d_mids = nullptr, *d_msrc = nullptr, *d_mprev = nullptr;
-    size_t cap_i = 0;
     uint32_t *d_istart = nullptr, *d_icount = nullptr;
     ContactBuf cbuf[2];
     int cur_cb = 0;
     // pinned host staging
-    size_t cap_hitems = 0, cap_hm = 0, cap_hi = 0, cap_hstep = 0;
+    size_t cap_hitems = 0, cap_hout = 0, cap_hm = 0, cap_hi = 0, cap_hstep = 0, cap_hreset = 0;
     int4* h_items = nullptr;
     uint8_t* h_out = nullptr;  // colliding flag, kept count
-    size_t cap_hout = 0;
     int4 *h_mids = nullptr, *h_msrc = nullptr, *h_mprev = nullptr;
     uint32_t *h_istart = nullptr, *h_icount = nullptr;
     uint8_t* h_step = nullptr;  // moved flags, fat AABBs, velocities after the step
-    // batches of this step
-    uint32_t batch_start[NB_ALGOS + 1] = {};
-    std::vector<int4> items;
-    std::vector<uint32_t> item_pair;  // index into pairs of each item
-    std::vector<uint8_t> gravity;  // gravity flag by body id (re-uploaded after permutations)
-    bool tables_dirty = true;
+    int32_t* h_reset = nullptr;
     // phase profiling (rp3dg_world_set_profiling): cumulative ms per phase
     bool profiling = false;
-    double phase_ms[8] = {};
+    double phase_ms[16] = {};
     std::chrono::steady_clock::time_point t_mark;
     rp3dg_world_stats stats{};
-    std::string err;
 };
 
 namespace {
 
-int wfail(rp3dg_world* w, int code, const std::string& msg) {
-    if (w) {
-        w->err = msg;
-        rp3dg::set_error(w->ctx, "world: " + msg);
-    }
+using Group = rp3dg_world;
+
+int wfail(Group* g, int code, const std::string& msg) {
+    if (g) rp3dg::set_error(g->ctx, "world: " + msg);
     return code;
 }
 int cfail(rp3dg_ctx* ctx, int code, const std::string& msg) {
     rp3dg::set_error(ctx, "world: " + msg);
     return code;
 }
-int wcuda(rp3dg_world* w, cudaError_t e, const char* what) {
-    return wfail(w, RP3DG_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+int wcuda(Group* g, cudaError_t e, const char* what) {
+    return wfail(g, RP3DG_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
 int shape_type_index(const rp3dg_shape& s) {
@@ -537,23 +562,24 @@ int select_algorithm(int t1, int t2) {
     return RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON;
 }
 
-int alloc_cache(rp3dg_world* w) {
-    int slot;
-    if (!w->free_cache.empty()) {
-        slot = w->free_cache.back();
-        w->free_cache.pop_back();
-    } else {
-        slot = int(w->cache_next++);
+// Cache slots: a world takes chunks of the group's pool and keeps a free list.
+int alloc_cache(Group* g, WorldH& w) {
+    if (w.free_cache.empty()) {
+        constexpr uint32_t CHUNK = 64;
+        const uint32_t base = g->cache_next.fetch_add(CHUNK);
+        for (uint32_t i = CHUNK; i-- > 0;) w.free_cache.push_back(int(base + i));
     }
-    w->reset_slots.push_back(slot);
+    const int slot = w.free_cache.back();
+    w.free_cache.pop_back();
+    w.reset_slots.push_back(slot);
     return slot;
 }
 
-PairH* find_pair(rp3dg_world* w, uint64_t id) {
-    auto it = w->map_pairs.find(id);
-    if (it != w->map_pairs.end()) return &w->pairs[it->second];
-    it = w->map_disabled.find(id);
-    if (it != w->map_disabled.end()) return &w->disabled[it->second];
+PairH* find_pair(WorldH& w, uint64_t id) {
+    auto it = w.map_pairs.find(id);
+    if (it != w.map_pairs.end()) return &w.pairs[it->second];
+    it = w.map_disabled.find(id);
+    if (it != w.map_disabled.end()) return &w.disabled[it->second];
     return nullptr;
 }
 
@@ -566,88 +592,88 @@ void remove_pair_at(std::vector<PairH>& arr, std::unordered_map<uint64_t, uint32
     arr.pop_back();
 }
 
-void remove_from_collider(rp3dg_world* w, int c, uint64_t id) {
-    auto& v = w->colliders[size_t(c)].pairs;
+void remove_from_collider(WorldH& w, int c, uint64_t id) {
+    auto& v = w.colliders[size_t(c)].pairs;
     auto it = std::find(v.begin(), v.end(), id);
     if (it != v.end()) v.erase(it);
 }
 
 // OverlappingPairs::addPair (OverlappingPairs.cpp:397-449), convex pairs
-void add_pair(rp3dg_world* w, int c1, int c2) {
-    const uint32_t b1 = uint32_t(w->colliders[size_t(c1)].bp), b2 = uint32_t(w->colliders[size_t(c2)].bp);
+void add_pair(Group* g, WorldH& w, int c1, int c2) {
+    const uint32_t b1 = uint32_t(w.colliders[size_t(c1)].bp), b2 = uint32_t(w.colliders[size_t(c2)].bp);
     PairH p;
     p.id = pair_number(std::max(b1, b2), std::min(b1, b2));
     p.bp1 = int(b1);
     p.bp2 = int(b2);
     p.c1 = c1;
     p.c2 = c2;
-    p.algo = select_algorithm(shape_type_index(w->shapes[size_t(w->colliders[size_t(c1)].shape)]),
-                              shape_type_index(w->shapes[size_t(w->colliders[size_t(c2)].shape)]));
+    p.algo = select_algorithm(shape_type_index(g->shapes[size_t(w.colliders[size_t(c1)].shape)]),
+                              shape_type_index(g->shapes[size_t(w.colliders[size_t(c2)].shape)]));
     p.enabled = true;
-    p.cache = alloc_cache(w);
-    w->map_pairs[p.id] = uint32_t(w->pairs.size());
-    w->pairs.push_back(p);
-    w->colliders[size_t(c1)].pairs.push_back(p.id);
-    w->colliders[size_t(c2)].pairs.push_back(p.id);
+    p.cache = alloc_cache(g, w);
+    w.map_pairs[p.id] = uint32_t(w.pairs.size());
+    w.pairs.push_back(p);
+    w.colliders[size_t(c1)].pairs.push_back(p.id);
+    w.colliders[size_t(c2)].pairs.push_back(p.id);
 }
 
 // removeConvexPairWithIndex(index, removeFromColliders = true)
-void remove_pair(rp3dg_world* w, uint32_t idx) {
-    PairH& p = w->pairs[idx];
+void remove_pair(WorldH& w, uint32_t idx) {
+    PairH& p = w.pairs[idx];
     remove_from_collider(w, p.c1, p.id);
     remove_from_collider(w, p.c2, p.id);
-    w->free_cache.push_back(p.cache);
-    remove_pair_at(w->pairs, w->map_pairs, idx);
+    w.free_cache.push_back(p.cache);
+    remove_pair_at(w.pairs, w.map_pairs, idx);
 }
 
 // disableConvexPairWithIndex / enableConvexPairWithIndex: the pair is
 // re-created in the other array with a fresh temporal-coherence record
-void disable_pair(rp3dg_world* w, uint64_t id) {
-    auto it = w->map_pairs.find(id);
-    if (it == w->map_pairs.end()) return;
+void disable_pair(Group* g, WorldH& w, uint64_t id) {
+    auto it = w.map_pairs.find(id);
+    if (it == w.map_pairs.end()) return;
     const uint32_t idx = it->second;
-    PairH np = w->pairs[idx];
+    PairH np = w.pairs[idx];
     np.enabled = false;
     np.need_test = false;
-    w->free_cache.push_back(np.cache);
-    np.cache = alloc_cache(w);
-    w->map_disabled[id] = uint32_t(w->disabled.size());
-    w->disabled.push_back(np);
-    remove_pair_at(w->pairs, w->map_pairs, idx);
+    w.free_cache.push_back(np.cache);
+    np.cache = alloc_cache(g, w);
+    w.map_disabled[id] = uint32_t(w.disabled.size());
+    w.disabled.push_back(np);
+    remove_pair_at(w.pairs, w.map_pairs, idx);
 }
-void enable_pair(rp3dg_world* w, uint64_t id) {
-    auto it = w->map_disabled.find(id);
-    if (it == w->map_disabled.end()) return;
+void enable_pair(Group* g, WorldH& w, uint64_t id) {
+    auto it = w.map_disabled.find(id);
+    if (it == w.map_disabled.end()) return;
     const uint32_t idx = it->second;
-    PairH np = w->disabled[idx];
+    PairH np = w.disabled[idx];
     np.enabled = true;
     np.need_test = false;
-    w->free_cache.push_back(np.cache);
-    np.cache = alloc_cache(w);
-    w->map_pairs[id] = uint32_t(w->pairs.size());
-    w->pairs.push_back(np);
-    remove_pair_at(w->disabled, w->map_disabled, idx);
+    w.free_cache.push_back(np.cache);
+    np.cache = alloc_cache(g, w);
+    w.map_pairs[id] = uint32_t(w.pairs.size());
+    w.pairs.push_back(np);
+    remove_pair_at(w.disabled, w.map_disabled, idx);
 }
 
 // BroadPhaseSystem::addMovedCollider + notifyOverlappingPairsToTestOverlap
-void add_moved(rp3dg_world* w, int c) {
-    w->moved.add(w->colliders[size_t(c)].bp);
-    for (uint64_t id : w->colliders[size_t(c)].pairs) {
+void add_moved(WorldH& w, int c) {
+    w.moved.add(w.colliders[size_t(c)].bp);
+    for (uint64_t id : w.colliders[size_t(c)].pairs) {
         PairH* p = find_pair(w, id);
         if (p) p->need_test = true;
     }
 }
 
 // PhysicsWorld::setBodyDisabled (PhysicsWorld.cpp:168-186)
-void set_body_disabled(rp3dg_world* w, int b, bool dis) {
-    if (w->bcomp.enabled(b) == !dis) return;
-    w->bcomp.set_disabled(b, dis);
-    for (int c : w->bodies[size_t(b)].colliders) w->ccomp.set_disabled(c, dis);
+void set_body_disabled(WorldH& w, int b, bool dis) {
+    if (w.bcomp.enabled(b) == !dis) return;
+    w.bcomp.set_disabled(b, dis);
+    for (int c : w.bodies[size_t(b)].colliders) w.ccomp.set_disabled(c, dis);
 }
 
 // RigidBody::setIsSleeping (RigidBody.cpp:1006-1057)
-void set_sleeping(rp3dg_world* w, int b, bool sleeping, std::vector<int32_t>* zero_rows) {
-    BodyH& B = w->bodies[size_t(b)];
+void set_sleeping(Group* g, WorldH& w, int b, bool sleeping) {
+    BodyH& B = w.bodies[size_t(b)];
     if (B.sleeping == sleeping) return;
     if (B.type == RP3DG_BODY_STATIC) return;
     if (sleeping) B.sleep_time = 0.0f;
@@ -657,22 +683,22 @@ void set_sleeping(rp3dg_world* w, int b, bool sleeping, std::vector<int32_t>* ze
     if (sleeping) {
         // checkForDisabledOverlappingPairs
         for (int c : B.colliders) {
-            const std::vector<uint64_t> ids = w->colliders[size_t(c)].pairs;
+            const std::vector<uint64_t> ids = w.colliders[size_t(c)].pairs;
             for (uint64_t id : ids) {
                 PairH* p = find_pair(w, id);
                 if (!p) continue;
-                const int o1 = w->colliders[size_t(p->c1)].body, o2 = w->colliders[size_t(p->c2)].body;
-                if (!w->bcomp.enabled(o1) && !w->bcomp.enabled(o2)) disable_pair(w, id);
+                const int o1 = w.colliders[size_t(p->c1)].body, o2 = w.colliders[size_t(p->c2)].body;
+                if (!w.bcomp.enabled(o1) && !w.bcomp.enabled(o2)) disable_pair(g, w, id);
             }
         }
-        zero_rows->push_back(b);
+        w.slept.push_back(b);
     } else {
         // enableOverlappingPairs + askForBroadPhaseCollisionCheck
         for (int c : B.colliders) {
-            const std::vector<uint64_t> ids = w->colliders[size_t(c)].pairs;
+            const std::vector<uint64_t> ids = w.colliders[size_t(c)].pairs;
             for (uint64_t id : ids) {
                 PairH* p = find_pair(w, id);
-                if (p && !p->enabled) enable_pair(w, id);
+                if (p && !p->enabled) enable_pair(g, w, id);
             }
         }
         for (int c : B.colliders) add_moved(w, c);
@@ -681,202 +707,443 @@ void set_sleeping(rp3dg_world* w, int b, bool sleeping, std::vector<int32_t>* ze
 
 // ---------------------------------------------------------------- phases
 
-// computeBroadPhase (CollisionDetectionSystem.cpp:103-167, 270-343)
-void broad_phase(rp3dg_world* w) {
+// computeBroadPhase (CollisionDetectionSystem.cpp:103-167, 270-343) and the
+// middle phase for convex pairs (:346-410): narrow-phase items in pair order.
+void broad_and_middle_phase(Group* g, WorldH& w) {
     std::vector<int32_t> shapes;
-    w->moved.to_array(shapes);
-    w->moved.clear();
+    w.moved.to_array(shapes);
+    w.moved.clear();
     std::vector<int> leaves, stack;
     for (int32_t s : shapes) {
         leaves.clear();
-        w->tree.query(w->tree.nodes[size_t(s)].box, leaves, stack);
+        w.tree.query(w.tree.nodes[size_t(s)].box, leaves, stack);
         for (int leaf : leaves) {
             if (leaf == s) continue;
-            const int c1 = w->bp_to_collider[size_t(s)], c2 = w->bp_to_collider[size_t(leaf)];
-            const ColliderH &C1 = w->colliders[size_t(c1)], &C2 = w->colliders[size_t(c2)];
+            const int c1 = w.bp_to_collider[size_t(s)], c2 = w.bp_to_collider[size_t(leaf)];
+            const ColliderH &C1 = w.colliders[size_t(c1)], &C2 = w.colliders[size_t(c2)];
             if (C1.body == C2.body) continue;
             const uint64_t id = pair_number(uint32_t(std::max(s, leaf)), uint32_t(std::min(s, leaf)));
             PairH* p = find_pair(w, id);
             if (!p) {
-                if ((C1.mask & C2.category) != 0 && (C1.category & C2.mask) != 0) add_pair(w, c1, c2);
+                if ((C1.mask & C2.category) != 0 && (C1.category & C2.mask) != 0) add_pair(g, w, c1, c2);
             } else {
                 p->need_test = false;
             }
         }
     }
     // removeNonOverlappingPairs
-    for (uint64_t i = 0; i < w->pairs.size(); i++) {
-        PairH& p = w->pairs[i];
+    for (uint64_t i = 0; i < w.pairs.size(); i++) {
+        PairH& p = w.pairs[i];
         if (!p.need_test) continue;
-        if (rp3dg::order::overlap(w->tree.nodes[size_t(p.bp1)].box, w->tree.nodes[size_t(p.bp2)].box)) {
+        if (rp3dg::order::overlap(w.tree.nodes[size_t(p.bp1)].box, w.tree.nodes[size_t(p.bp2)].box)) {
             p.need_test = false;
         } else {
             remove_pair(w, uint32_t(i));
             i--;
         }
     }
+    for (int a = 0; a < NB_ALGOS; a++) {
+        w.items[a].clear();
+        w.item_pair[a].clear();
+    }
+    // rows in the order the device will have after this step's row sync
+    for (uint32_t i = 0; i < w.pairs.size(); i++) {
+        PairH& p = w.pairs[i];
+        p.coll_curr = false;
+        const bool e1 = w.ccomp.enabled(p.c1), e2 = w.ccomp.enabled(p.c2);
+        if (!(e1 || e2)) continue;
+        const int a = p.algo - 1;
+        w.items[a].push_back(make_int4(int(w.c0) + w.ccomp.slot[size_t(p.c1)], int(w.c0) + w.ccomp.slot[size_t(p.c2)],
+                                       p.cache, 1));
+        w.item_pair[a].push_back(i);
+    }
 }
 
-int ensure_items(rp3dg_world* w, size_t n) {
-    if (n <= w->cap_items) return 0;
-    size_t c = std::max<size_t>(n, w->cap_items * 2);
+// processAllPotentialContacts' contact pairs (batch order), addContactPairsToBodies
+// and PhysicsWorld::createIslands (PhysicsWorld.cpp:695-866).
+void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint8_t* h_count) {
+    w.cpairs.clear();
+    for (int a = 0; a < NB_ALGOS; a++) {
+        const uint32_t base = g->batch_start[a] + w.item_off[a];
+        for (uint32_t i = 0; i < w.items[a].size(); i++) {
+            const uint32_t it = base + i;
+            if (!h_coll[it]) continue;
+            PairH& p = w.pairs[w.item_pair[a][i]];
+            p.coll_curr = true;
+            ContactPairH c;
+            c.id = p.id;
+            c.c1 = p.c1;
+            c.c2 = p.c2;
+            c.b1 = w.colliders[size_t(p.c1)].body;
+            c.b2 = w.colliders[size_t(p.c2)].body;
+            c.item = it;
+            c.k = h_count[it];
+            w.cpairs.push_back(c);
+        }
+    }
+    for (uint32_t p = 0; p < w.cpairs.size(); p++) {
+        w.bodies[size_t(w.cpairs[p].b1)].contact_pairs.push_back(p);
+        w.bodies[size_t(w.cpairs[p].b2)].contact_pairs.push_back(p);
+    }
+    w.island_order.clear();
+    w.islands.clear();
+    for (auto& B : w.bodies) B.in_island = false;
+    uint32_t total_manifolds = 0;
+    std::vector<int> stack, statics;
+    for (uint32_t s = 0; s < w.bcomp.n_enabled; s++) {
+        const int b0 = w.bcomp.at[s];
+        if (w.bodies[size_t(b0)].in_island) continue;
+        if (w.bodies[size_t(b0)].type == RP3DG_BODY_STATIC) continue;
+        stack.clear();
+        w.bodies[size_t(b0)].in_island = true;
+        stack.push_back(b0);
+        IslandH isl;
+        isl.manifold_start = total_manifolds;
+        const size_t isl_index = w.islands.size();
+        w.islands.push_back(isl);
+        while (!stack.empty()) {
+            const int b = stack.back();
+            stack.pop_back();
+            w.islands[isl_index].bodies.push_back(b);
+            set_sleeping(g, w, b, false);
+            if (w.bodies[size_t(b)].type == RP3DG_BODY_STATIC) {
+                statics.push_back(b);
+                continue;
+            }
+            for (uint32_t cpi : w.bodies[size_t(b)].contact_pairs) {
+                ContactPairH& cp = w.cpairs[cpi];
+                if (cp.in_island) continue;
+                cp.in_island = true;
+                const int other = cp.b1 == b ? cp.b2 : cp.b1;
+                if (w.bodies[size_t(other)].has_sim_collider) {
+                    w.island_order.push_back(cpi);
+                    total_manifolds += 1;
+                    w.islands[isl_index].manifold_count += 1;
+                    if (w.bodies[size_t(other)].in_island) continue;
+                    stack.push_back(other);
+                    w.bodies[size_t(other)].in_island = true;
+                }
+            }
+        }
+        for (int sb : statics) w.bodies[size_t(sb)].in_island = false;
+        statics.clear();
+    }
+    for (auto& cp : w.cpairs) {
+        w.bodies[size_t(cp.b1)].contact_pairs.clear();
+        w.bodies[size_t(cp.b2)].contact_pairs.clear();
+    }
+    w.nm = uint32_t(w.island_order.size());
+    w.np = 0;
+    for (uint32_t m = 0; m < w.nm; m++) w.np += w.cpairs[w.island_order[m]].k;
+}
+
+// createContacts' packing (CollisionDetectionSystem.cpp:906-975) and the
+// warm-start sources of initContactsWithPreviousOnes (:1069-1160).
+void fill_manifolds(Group* g, WorldH& w) {
+    uint32_t pt = w.pt_base;
+    for (uint32_t m = 0; m < w.nm; m++) {
+        ContactPairH& cp = w.cpairs[w.island_order[m]];
+        const uint32_t gm = w.man_base + m;
+        cp.manifold = gm;
+        cp.point = pt;
+        uint32_t a = 0;
+        while (cp.item >= g->batch_start[a + 1]) a++;
+        const uint32_t s0 = g->batch_start[a];
+        g->h_mids[gm] = make_int4(int(w.b0) + w.bcomp.slot[size_t(cp.b1)], int(w.b0) + w.bcomp.slot[size_t(cp.b2)],
+                                  int(w.c0) + w.ccomp.slot[size_t(cp.c1)], int(w.c0) + w.ccomp.slot[size_t(cp.c2)]);
+        g->h_msrc[gm] = make_int4(int(cp.item - s0), int(g->batch_start[a + 1] - s0), int(s0), int(pt));
+        auto it = w.prev_map.find(cp.id);
+        if (it != w.prev_map.end() && w.prev_cpairs[it->second].in_island) {
+            const ContactPairH& pc = w.prev_cpairs[it->second];
+            g->h_mprev[gm] = make_int4(int(pc.manifold), 1, int(pc.point), int(pc.k));
+        } else {
+            g->h_mprev[gm] = make_int4(-1, 0, 0, 0);
+        }
+        pt += cp.k;
+    }
+    for (uint32_t i = 0; i < w.islands.size(); i++) {
+        g->h_istart[w.isl_base + i] = w.man_base + w.islands[i].manifold_start;
+        g->h_icount[w.isl_base + i] = w.islands[i].manifold_count;
+    }
+    // computeMapPreviousContactPairs for the next step
+    w.prev_map.clear();
+    for (uint32_t i = 0; i < w.cpairs.size(); i++) w.prev_map[w.cpairs[i].id] = i;
+}
+
+// BroadPhaseSystem::updateColliders' reinsertions (enabled colliders in
+// component order) and PhysicsWorld::updateSleepingBodies (:871-926).
+void colliders_and_sleep(Group* g, WorldH& w, float dt, const uint8_t* h_moved, const float4* h_fmin,
+                         const float4* h_fmax, const float4* h_lv, const float4* h_av) {
+    uint32_t nmoved = 0;
+    for (uint32_t s = 0; s < w.ccomp.n_enabled; s++) {
+        const uint32_t r = w.c0 + s;
+        if (!h_moved[r]) continue;
+        const int c = w.ccomp.at[s];
+        Box box;
+        box.mn[0] = h_fmin[r].x; box.mn[1] = h_fmin[r].y; box.mn[2] = h_fmin[r].z;
+        box.mx[0] = h_fmax[r].x; box.mx[1] = h_fmax[r].y; box.mx[2] = h_fmax[r].z;
+        w.tree.reinsert(w.colliders[size_t(c)].bp, box);
+        add_moved(w, c);
+        nmoved++;
+    }
+    w.stats.moved_colliders = nmoved;
+    w.slept.clear();
+    if (g->set.sleeping_enabled) {
+        // velocities by body id (rows in the device order before any body falls asleep)
+        std::vector<float4> lv(w.nb), av(w.nb);
+        for (uint32_t s = 0; s < w.nb; s++) {
+            lv[size_t(w.dev_body_at[s])] = h_lv[w.b0 + s];
+            av[size_t(w.dev_body_at[s])] = h_av[w.b0 + s];
+        }
+        const float slv2 = g->set.sleep_linear_velocity * g->set.sleep_linear_velocity;
+        const float sav2 = g->set.sleep_angular_velocity * g->set.sleep_angular_velocity;
+        for (const IslandH& isl : w.islands) {
+            float min_sleep = 3.40282347e+38f;
+            for (int b : isl.bodies) {
+                BodyH& B = w.bodies[size_t(b)];
+                if (B.type == RP3DG_BODY_STATIC) continue;
+                const float4 l = lv[size_t(b)], a = av[size_t(b)];
+                if (l.x * l.x + l.y * l.y + l.z * l.z > slv2 || a.x * a.x + a.y * a.y + a.z * a.z > sav2 ||
+                    !B.allowed_sleep) {
+                    B.sleep_time = 0.0f;
+                    min_sleep = 0.0f;
+                } else {
+                    B.sleep_time += dt;
+                    if (B.sleep_time < min_sleep) min_sleep = B.sleep_time;
+                }
+            }
+            if (min_sleep >= g->set.time_before_sleep)
+                for (int b : isl.bodies) set_sleeping(g, w, b, true);
+        }
+    }
+    // collidingInPreviousFrame for the next step
+    for (auto& p : w.pairs) p.coll_prev = p.coll_curr;
+    w.prev_cpairs.swap(w.cpairs);
+    w.stats.disabled_pairs = uint32_t(w.disabled.size());
+    w.stats.enabled_bodies = w.bcomp.n_enabled;
+}
+
+int ensure_items(Group* g, size_t n) {
+    if (n <= g->cap_items) return 0;
+    size_t c = std::max<size_t>(n, g->cap_items * 2);
     c = std::max<size_t>(c, 256);
-    cudaFree(w->d_items); cudaFree(w->d_s1); cudaFree(w->d_s2); cudaFree(w->d_p1); cudaFree(w->d_r1);
-    cudaFree(w->d_p2); cudaFree(w->d_r2); cudaFree(w->d_rep); cudaFree(w->d_coll); cudaFree(w->d_nct);
-    cudaFree(w->d_cache); cudaFree(w->d_nd); cudaFree(w->d_l1); cudaFree(w->d_l2);
+    cudaFree(g->d_items); cudaFree(g->d_s1); cudaFree(g->d_s2); cudaFree(g->d_p1); cudaFree(g->d_r1);
+    cudaFree(g->d_p2); cudaFree(g->d_r2); cudaFree(g->d_rep); cudaFree(g->d_coll); cudaFree(g->d_nct);
+    cudaFree(g->d_cache); cudaFree(g->d_nd); cudaFree(g->d_l1); cudaFree(g->d_l2);
     cudaError_t e = cudaSuccess;
     auto M = [&](void** p, size_t b) { if (e == cudaSuccess) e = cudaMalloc(p, b); };
-    M((void**)&w->d_items, c * 16); M((void**)&w->d_s1, c * 4); M((void**)&w->d_s2, c * 4);
-    M((void**)&w->d_p1, c * 16); M((void**)&w->d_r1, c * 16); M((void**)&w->d_p2, c * 16); M((void**)&w->d_r2, c * 16);
-    M((void**)&w->d_rep, c); M((void**)&w->d_coll, c); M((void**)&w->d_nct, c);
-    M((void**)&w->d_cache, c * 16);
-    M((void**)&w->d_nd, c * 16 * MAXC); M((void**)&w->d_l1, c * 16 * MAXC); M((void**)&w->d_l2, c * 16 * MAXC);
-    if (e != cudaSuccess) { w->cap_items = 0; return wcuda(w, e, "cudaMalloc(narrow-phase step buffers)"); }
-    w->cap_items = c;
-    if (host_grow(&w->h_items, &w->cap_hitems, c) || host_grow(&w->h_out, &w->cap_hout, 2 * c))
-        return wfail(w, RP3DG_ENOMEM, "cudaMallocHost(step staging)");
+    M((void**)&g->d_items, c * 16); M((void**)&g->d_s1, c * 4); M((void**)&g->d_s2, c * 4);
+    M((void**)&g->d_p1, c * 16); M((void**)&g->d_r1, c * 16); M((void**)&g->d_p2, c * 16); M((void**)&g->d_r2, c * 16);
+    M((void**)&g->d_rep, c); M((void**)&g->d_coll, c); M((void**)&g->d_nct, c);
+    M((void**)&g->d_cache, c * 16);
+    M((void**)&g->d_nd, c * 16 * MAXC); M((void**)&g->d_l1, c * 16 * MAXC); M((void**)&g->d_l2, c * 16 * MAXC);
+    if (e != cudaSuccess) { g->cap_items = 0; return wcuda(g, e, "cudaMalloc(narrow-phase step buffers)"); }
+    g->cap_items = c;
+    if (host_grow(&g->h_items, &g->cap_hitems, c) || host_grow(&g->h_out, &g->cap_hout, 2 * c))
+        return wfail(g, RP3DG_ENOMEM, "cudaMallocHost(step staging)");
     return 0;
 }
 
-int ensure_pool(rp3dg_world* w) {
-    const size_t need = w->cache_next;
-    if (need <= w->cap_pool) return 0;
-    size_t c = std::max<size_t>(need, w->cap_pool * 2);
+int ensure_pool(Group* g) {
+    const size_t need = g->cache_next.load();
+    if (need <= g->cap_pool) return 0;
+    size_t c = std::max<size_t>(need, g->cap_pool * 2);
     c = std::max<size_t>(c, 1024);
     rp3dg_lastframe* np = nullptr;
     cudaError_t e = cudaMalloc(&np, c * sizeof(rp3dg_lastframe));
-    if (e != cudaSuccess) return wcuda(w, e, "cudaMalloc(cache pool)");
-    if (w->pool && w->cap_pool)
-        cudaMemcpyAsync(np, w->pool, w->cap_pool * sizeof(rp3dg_lastframe), cudaMemcpyDeviceToDevice, w->stream);
-    cudaStreamSynchronize(w->stream);
-    cudaFree(w->pool);
-    w->pool = np;
-    w->cap_pool = c;
+    if (e != cudaSuccess) return wcuda(g, e, "cudaMalloc(cache pool)");
+    if (g->pool && g->cap_pool)
+        cudaMemcpyAsync(np, g->pool, g->cap_pool * sizeof(rp3dg_lastframe), cudaMemcpyDeviceToDevice, g->stream);
+    cudaStreamSynchronize(g->stream);
+    cudaFree(g->pool);
+    g->pool = np;
+    g->cap_pool = c;
     return 0;
 }
 
-int ensure_small(rp3dg_world* w, size_t n) { return dev_grow(&w->d_small, &w->cap_small, n) ? wfail(w, RP3DG_ENOMEM, "cudaMalloc(small)") : 0; }
+int ensure_small(Group* g, size_t n) { return dev_grow(&g->d_small, &g->cap_small, n) ? wfail(g, RP3DG_ENOMEM, "cudaMalloc(small)") : 0; }
 
-// Device rows follow the host's component order: permute them when a sleep,
-// wake or type change moved components since the last step.
-int sync_rows(rp3dg_world* w) {
-    if (w->dev_body_at != w->bcomp.at) {
-        const uint32_t n = w->nb;
-        std::vector<int32_t> perm(n), inv(n);
-        for (uint32_t r = 0; r < n; r++) inv[size_t(w->dev_body_at[r])] = int32_t(r);
-        for (uint32_t r = 0; r < n; r++) perm[r] = inv[size_t(w->bcomp.at[r])];
-        if (ensure_small(w, n)) return RP3DG_ENOMEM;
-        cudaMemcpyAsync(w->d_small, perm.data(), n * 4, cudaMemcpyHostToDevice, w->stream);
-        PermArgs a{};
-        a.n = n;
-        a.perm = w->d_small;
-        const int s = w->cur_b, d = 1 - s;
-        for (int c = 0; c < BC_NCOL; c++) a.col[a.ncol++] = PermCol{w->bcol[s][c], w->bcol[d][c], 1};
-        a.col[a.ncol++] = PermCol{w->biiw[s], w->biiw[d], 3};
-        world_permute<<<blocks(n), 128, 0, w->stream>>>(a);
-        w->cur_b = d;
-        cudaStreamSynchronize(w->stream);
-        w->dev_body_at = w->bcomp.at;
-        w->tables_dirty = true;
+// Run f(world index) for every world on the group's host threads.
+template <class F>
+void for_worlds(Group* g, F f) {
+    const int n = int(g->worlds.size());
+    if (g->nthreads <= 1 || n <= 1) {
+        for (int i = 0; i < n; i++) f(i);
+        return;
     }
-    if (w->dev_col_at != w->ccomp.at) {
-        const uint32_t n = w->nc;
-        std::vector<int32_t> perm(n), inv(n);
-        for (uint32_t r = 0; r < n; r++) inv[size_t(w->dev_col_at[r])] = int32_t(r);
-        for (uint32_t r = 0; r < n; r++) perm[r] = inv[size_t(w->ccomp.at[r])];
-        if (ensure_small(w, n)) return RP3DG_ENOMEM;
-        cudaMemcpyAsync(w->d_small, perm.data(), n * 4, cudaMemcpyHostToDevice, w->stream);
+#pragma omp parallel for schedule(dynamic, 4) num_threads(g->nthreads)
+    for (int i = 0; i < n; i++) f(i);
+}
+
+// Host copies of the per-row tables (pinned), kept current world by world.
+void world_tables(Group* g, WorldH& w) {
+    for (uint32_t r = 0; r < w.nb; r++) {
+        g->t_grav[w.b0 + r] = w.gravity[size_t(w.bcomp.at[r])];
+        g->t_ben[w.b0 + r] = r < w.bcomp.n_enabled ? 1 : 0;
+    }
+    for (uint32_t r = 0; r < w.nc; r++) {
+        const ColliderH& C = w.colliders[size_t(w.ccomp.at[r])];
+        g->t_cbody[w.c0 + r] = int32_t(w.b0) + w.bcomp.slot[size_t(C.body)];
+        g->t_cshape[w.c0 + r] = C.shape;
+        g->t_cat[w.c0 + r] = C.category;
+        g->t_mask[w.c0 + r] = C.mask;
+        g->t_cen[w.c0 + r] = r < w.ccomp.n_enabled ? 1 : 0;
+    }
+}
+
+int ensure_tables(Group* g) {
+    if (g->t_grav) return 0;
+    const size_t nb = std::max<uint32_t>(g->NB, 1), nc = std::max<uint32_t>(g->NC, 1);
+    if (cudaMallocHost(&g->t_grav, nb) || cudaMallocHost(&g->t_ben, nb) || cudaMallocHost(&g->t_cen, nc) ||
+        cudaMallocHost(&g->t_cbody, nc * 4) || cudaMallocHost(&g->t_cshape, nc * 4) ||
+        cudaMallocHost(&g->t_cat, nc * 2) || cudaMallocHost(&g->t_mask, nc * 2) ||
+        cudaMallocHost(&g->t_bperm, nb * 4) || cudaMallocHost(&g->t_cperm, nc * 4))
+        return wfail(g, RP3DG_ENOMEM, "cudaMallocHost(row tables)");
+    for (uint32_t r = 0; r < g->NB; r++) g->t_bperm[r] = int32_t(r);
+    for (uint32_t r = 0; r < g->NC; r++) g->t_cperm[r] = int32_t(r);
+    return 0;
+}
+
+// Device rows follow the host's component order.  Worlds whose order changed
+// (a sleep, wake or type change moved components) or whose enabled counts
+// changed get their permutation segment and table rows rebuilt (in
+// parallel); one permutation kernel and one upload per table then cover all
+// rows.
+int sync_rows(Group* g) {
+    int rc = ensure_tables(g);
+    if (rc) return rc;
+    std::atomic<int> bchg{0}, cchg{0}, tchg{0};
+    for_worlds(g, [&](int k) {
+        WorldH& w = g->worlds[size_t(k)];
+        const bool bo = w.dev_body_at != w.bcomp.at, co = w.dev_col_at != w.ccomp.at;
+        const bool en = w.dev_nb_en != w.bcomp.n_enabled || w.dev_nc_en != w.ccomp.n_enabled;
+        if (bo) {
+            std::vector<int32_t> inv(w.nb);
+            for (uint32_t r = 0; r < w.nb; r++) inv[size_t(w.dev_body_at[r])] = int32_t(r);
+            for (uint32_t r = 0; r < w.nb; r++) g->t_bperm[w.b0 + r] = int32_t(w.b0) + inv[size_t(w.bcomp.at[r])];
+            w.dev_body_at = w.bcomp.at;
+            bchg = 1;
+        }
+        if (co) {
+            std::vector<int32_t> inv(w.nc);
+            for (uint32_t r = 0; r < w.nc; r++) inv[size_t(w.dev_col_at[r])] = int32_t(r);
+            for (uint32_t r = 0; r < w.nc; r++) g->t_cperm[w.c0 + r] = int32_t(w.c0) + inv[size_t(w.ccomp.at[r])];
+            w.dev_col_at = w.ccomp.at;
+            cchg = 1;
+        }
+        if (bo || co || en || g->tables_dirty) {
+            world_tables(g, w);
+            w.dev_nb_en = w.bcomp.n_enabled;
+            w.dev_nc_en = w.ccomp.n_enabled;
+            tchg = 1;
+        }
+    });
+    cudaStream_t st = g->stream;
+    if (bchg) {
+        if (ensure_small(g, g->NB)) return RP3DG_ENOMEM;
+        cudaMemcpyAsync(g->d_small, g->t_bperm, size_t(g->NB) * 4, cudaMemcpyHostToDevice, st);
         PermArgs a{};
-        a.n = n;
-        a.perm = w->d_small;
-        const int s = w->cur_c, d = 1 - s;
-        for (int c = 0; c < CC_NCOL; c++) a.col[a.ncol++] = PermCol{w->ccol[s][c], w->ccol[d][c], 1};
-        world_permute<<<blocks(n), 128, 0, w->stream>>>(a);
-        w->cur_c = d;
-        cudaStreamSynchronize(w->stream);
-        w->dev_col_at = w->ccomp.at;
-        w->tables_dirty = true;
+        a.n = g->NB;
+        a.perm = g->d_small;
+        const int s = g->cur_b, d = 1 - s;
+        for (int c = 0; c < BC_NCOL; c++) a.col[a.ncol++] = PermCol{g->bcol[s][c], g->bcol[d][c], 1};
+        a.col[a.ncol++] = PermCol{g->biiw[s], g->biiw[d], 3};
+        world_permute<<<blocks(g->NB), 128, 0, st>>>(a);
+        g->cur_b = d;
+    }
+    if (cchg) {
+        // the small buffer holds the body permutation until its kernel ran
+        cudaStreamSynchronize(st);
+        if (ensure_small(g, g->NC)) return RP3DG_ENOMEM;
+        cudaMemcpyAsync(g->d_small, g->t_cperm, size_t(g->NC) * 4, cudaMemcpyHostToDevice, st);
+        PermArgs a{};
+        a.n = g->NC;
+        a.perm = g->d_small;
+        const int s = g->cur_c, d = 1 - s;
+        for (int c = 0; c < CC_NCOL; c++) a.col[a.ncol++] = PermCol{g->ccol[s][c], g->ccol[d][c], 1};
+        world_permute<<<blocks(g->NC), 128, 0, st>>>(a);
+        g->cur_c = d;
+    }
+    if (tchg) {
+        cudaMemcpyAsync(g->bgrav, g->t_grav, g->NB, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->b_en, g->t_ben, g->NB, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->c_en, g->t_cen, g->NC, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->c_body, g->t_cbody, size_t(g->NC) * 4, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->c_shape, g->t_cshape, size_t(g->NC) * 4, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->c_cat, g->t_cat, size_t(g->NC) * 2, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->c_mask, g->t_mask, size_t(g->NC) * 2, cudaMemcpyHostToDevice, st);
+    }
+    g->tables_dirty = false;
+    // the host buffers are rewritten by the next sync: wait for the copies
+    if (bchg || cchg || tchg) {
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return wcuda(g, e, "row sync");
+        if (bchg)
+            for_worlds(g, [&](int k) {
+                const WorldH& w = g->worlds[size_t(k)];
+                for (uint32_t r = 0; r < w.nb; r++) g->t_bperm[w.b0 + r] = int32_t(w.b0 + r);
+            });
+        if (cchg)
+            for_worlds(g, [&](int k) {
+                const WorldH& w = g->worlds[size_t(k)];
+                for (uint32_t r = 0; r < w.nc; r++) g->t_cperm[w.c0 + r] = int32_t(w.c0 + r);
+            });
     }
     return 0;
 }
 
-// The per-row tables that are not float4 columns (gravity flag, collider body
-// row, shape, category, mask) are uploaded from host copies whenever the
-// component order changed.
-int upload_tables(rp3dg_world* w) {
-    if (!w->tables_dirty) return 0;
-    w->tables_dirty = false;
-    std::vector<uint8_t> g(w->nb);
-    for (uint32_t r = 0; r < w->nb; r++) g[r] = w->gravity[size_t(w->bcomp.at[r])];
-    std::vector<int32_t> cb(w->nc), cs(w->nc);
-    std::vector<uint16_t> cat(w->nc), mask(w->nc);
-    for (uint32_t r = 0; r < w->nc; r++) {
-        const ColliderH& C = w->colliders[size_t(w->ccomp.at[r])];
-        cb[r] = w->bcomp.slot[size_t(C.body)];
-        cs[r] = C.shape;
-        cat[r] = C.category;
-        mask[r] = C.mask;
+void destroy_group(Group* g) {
+    if (!g) return;
+    for (int k = 0; k < 2; k++) {
+        for (int c = 0; c < BC_NCOL; c++) cudaFree(g->bcol[k][c]);
+        cudaFree(g->biiw[k]);
+        for (int c = 0; c < CC_NCOL; c++) cudaFree(g->ccol[k][c]);
+        g->cbuf[k].release();
     }
-    cudaMemcpyAsync(w->bgrav, g.data(), w->nb, cudaMemcpyHostToDevice, w->stream);
-    cudaMemcpyAsync(w->c_body, cb.data(), size_t(w->nc) * 4, cudaMemcpyHostToDevice, w->stream);
-    cudaMemcpyAsync(w->c_shape, cs.data(), size_t(w->nc) * 4, cudaMemcpyHostToDevice, w->stream);
-    cudaMemcpyAsync(w->c_cat, cat.data(), size_t(w->nc) * 2, cudaMemcpyHostToDevice, w->stream);
-    cudaMemcpyAsync(w->c_mask, mask.data(), size_t(w->nc) * 2, cudaMemcpyHostToDevice, w->stream);
-    return cudaStreamSynchronize(w->stream) == cudaSuccess ? 0 : wfail(w, RP3DG_ECUDA, "table upload");
+    cudaFree(g->bgrav); cudaFree(g->b_en); cudaFree(g->c_en); cudaFree(g->c_body); cudaFree(g->c_shape);
+    cudaFree(g->c_cat); cudaFree(g->c_mask); cudaFree(g->c_moved); cudaFree(g->pool); cudaFree(g->d_small);
+    cudaFree(g->d_items); cudaFree(g->d_s1); cudaFree(g->d_s2); cudaFree(g->d_p1); cudaFree(g->d_r1);
+    cudaFree(g->d_p2); cudaFree(g->d_r2); cudaFree(g->d_rep); cudaFree(g->d_coll); cudaFree(g->d_nct);
+    cudaFree(g->d_cache); cudaFree(g->d_nd); cudaFree(g->d_l1); cudaFree(g->d_l2);
+    cudaFree(g->d_mids); cudaFree(g->d_msrc); cudaFree(g->d_mprev); cudaFree(g->d_istart); cudaFree(g->d_icount);
+    cudaFreeHost(g->h_items); cudaFreeHost(g->h_out); cudaFreeHost(g->h_mids); cudaFreeHost(g->h_msrc);
+    cudaFreeHost(g->h_mprev); cudaFreeHost(g->h_istart); cudaFreeHost(g->h_icount); cudaFreeHost(g->h_step);
+    cudaFreeHost(g->h_reset);
+    cudaFreeHost(g->t_grav); cudaFreeHost(g->t_ben); cudaFreeHost(g->t_cen); cudaFreeHost(g->t_cbody);
+    cudaFreeHost(g->t_cshape); cudaFreeHost(g->t_cat); cudaFreeHost(g->t_mask); cudaFreeHost(g->t_bperm);
+    cudaFreeHost(g->t_cperm);
+    delete g;
 }
 
-}  // namespace
-
-extern "C" {
-
-int rp3dg_world_create(rp3dg_ctx* ctx, const rp3dg_world_settings* s, const rp3dg_body_desc* bd, uint32_t nb,
-                       const rp3dg_collider_desc* cd, uint32_t nc, rp3dg_world** out) {
-    if (!ctx || !s || !out || (nb && !bd) || (nc && !cd)) return ctx ? cfail(ctx, RP3DG_EINVAL, "null argument") : RP3DG_EINVAL;
-    *out = nullptr;
-    // shape table (host copy)
-    auto* w = new rp3dg_world();
-    w->ctx = ctx;
-    w->stream = static_cast<cudaStream_t>(rp3dg_stream(ctx));
-    w->set = *s;
-    w->nb = nb;
-    w->nc = nc;
-    if (rp3dg::get_shapes_host(ctx, &w->shapes) || w->shapes.empty()) {
-        delete w;
-        return cfail(ctx, RP3DG_EINVAL, "no shape table (rp3dg_set_shapes)");
-    }
+// Replays rp3dg_world_create's call sequence for one world on the host
+// bookkeeping and fills that world's rows of the host columns.
+int build_world(Group* g, WorldH& w, const rp3dg_body_desc* bd, uint32_t nb, const rp3dg_collider_desc* cd,
+                uint32_t nc, std::vector<float4>* col, std::vector<float4>* ccols, std::vector<uint8_t>& dynamic,
+                std::vector<int>& creation_order) {
     for (uint32_t i = 0; i < nc; i++) {
-        if (cd[i].body < 0 || uint32_t(cd[i].body) >= nb || (i && cd[i].body < cd[i - 1].body)) {
-            delete w;
-            return cfail(ctx, RP3DG_EINVAL, "colliders must be grouped by body, bodies ascending");
-        }
-        if (cd[i].shape < 0 || size_t(cd[i].shape) >= w->shapes.size()) {
-            delete w;
-            return cfail(ctx, RP3DG_EINVAL, "collider shape outside the shape table");
-        }
+        if (cd[i].body < 0 || uint32_t(cd[i].body) >= nb || (i && cd[i].body < cd[i - 1].body))
+            return cfail(g->ctx, RP3DG_EINVAL, "colliders must be grouped by body, bodies ascending");
+        if (cd[i].shape < 0 || size_t(cd[i].shape) >= g->shapes.size())
+            return cfail(g->ctx, RP3DG_EINVAL, "collider shape outside the shape table");
     }
     for (uint32_t i = 0; i < nb; i++)
-        if (bd[i].type < RP3DG_BODY_STATIC || bd[i].type > RP3DG_BODY_DYNAMIC) {
-            delete w;
-            return cfail(ctx, RP3DG_EINVAL, "bad body type");
-        }
-    w->bodies.resize(nb);
-    w->colliders.resize(nc);
-    w->bcomp.reserve_ids(nb);
-    w->ccomp.reserve_ids(nc);
-    // host-side component data by id
-    std::vector<float4> col[BC_NCOL];
-    for (auto& v : col) v.assign(nb, make_float4(0.f, 0.f, 0.f, 0.f));
-    std::vector<uint8_t> dynamic(nb, 0), gravity(nb, 1);
-    std::vector<float4> ccols[CC_NCOL];
-    for (auto& v : ccols) v.assign(nc, make_float4(0.f, 0.f, 0.f, 0.f));
-    // replay the creation protocol on the component order (the tree comes
-    // after the fat AABBs are computed on the device, in the same order)
+        if (bd[i].type < RP3DG_BODY_STATIC || bd[i].type > RP3DG_BODY_DYNAMIC)
+            return cfail(g->ctx, RP3DG_EINVAL, "bad body type");
+    w.nb = nb;
+    w.nc = nc;
+    w.bodies.resize(nb);
+    w.colliders.resize(nc);
+    w.bcomp.reserve_ids(nb);
+    w.ccomp.reserve_ids(nc);
+    w.gravity.assign(nb, 1);
+    dynamic.assign(nb, 0);
+    for (int k = 0; k < BC_NCOL; k++) col[k].assign(nb, make_float4(0.f, 0.f, 0.f, 0.f));
+    for (int k = 0; k < CC_NCOL; k++) ccols[k].assign(nc, make_float4(0.f, 0.f, 0.f, 0.f));
     uint32_t ci = 0;
-    std::vector<int> creation_order;  // colliders in addCollider order
     for (uint32_t b = 0; b < nb; b++) {
         const rp3dg_body_desc& d = bd[b];
-        BodyH& B = w->bodies[b];
-        w->bcomp.add(int(b), false);  // createRigidBody: enabled, DYNAMIC
+        BodyH& B = w.bodies[b];
+        w.bcomp.add(int(b), false);  // createRigidBody: enabled, DYNAMIC
         col[BC_POS][b] = make_float4(d.position[0], d.position[1], d.position[2], 0.f);
         col[BC_ORI][b] = make_float4(d.orientation[0], d.orientation[1], d.orientation[2], d.orientation[3]);
         col[BC_MASS][b] = make_float4(1.0f, 1.0f, 0.0f, 0.0f);
@@ -886,17 +1153,17 @@ int rp3dg_world_create(rp3dg_ctx* ctx, const rp3dg_world_settings* s, const rp3d
         std::vector<uint32_t> mine;
         while (ci < nc && uint32_t(cd[ci].body) == b) {
             const rp3dg_collider_desc& c = cd[ci];
-            ColliderH& C = w->colliders[ci];
+            ColliderH& C = w.colliders[ci];
             C.body = int(b);
             C.shape = c.shape;
             C.category = c.category;
             C.mask = c.mask;
-            w->ccomp.add(int(ci), !w->bcomp.enabled(int(b)));
+            w.ccomp.add(int(ci), !w.bcomp.enabled(int(b)));
             B.colliders.push_back(int(ci));
             B.has_sim_collider = true;
             ccols[CC_LPOS][ci] = make_float4(c.position[0], c.position[1], c.position[2], 0.f);
             ccols[CC_LORI][ci] = make_float4(c.orientation[0], c.orientation[1], c.orientation[2], c.orientation[3]);
-            // Material::mFrictionCoefficientSqrt = sqrt(friction) (Material.h)
+            // Material::mFrictionCoefficientSqrt = sqrt(friction)
             ccols[CC_MAT][ci] = make_float4(std::sqrt(c.friction), c.bounciness, 0.f, 0.f);
             creation_order.push_back(int(ci));
             mine.push_back(ci);
@@ -906,11 +1173,9 @@ int rp3dg_world_create(rp3dg_ctx* ctx, const rp3dg_world_settings* s, const rp3d
             // updateMassPropertiesFromColliders (RigidBody.cpp:548-608)
             float total = 0.0f, com[3] = {0.f, 0.f, 0.f};
             for (uint32_t k : mine) {
-                float vol, in[3], m;
-                if (!shape_mass(w->shapes[size_t(cd[k].shape)], cd[k].mass_density, &vol, in, &m)) {
-                    delete w;
-                    return cfail(ctx, RP3DG_EINVAL, "mass properties of a convex-mesh collider are not supported");
-                }
+                float in[3], m;
+                if (!shape_mass(g->shapes[size_t(cd[k].shape)], cd[k].mass_density, in, &m))
+                    return cfail(g->ctx, RP3DG_EINVAL, "mass properties of a convex-mesh collider are not supported");
                 total += m;
                 for (int a = 0; a < 3; a++) com[a] += m * cd[k].position[a];
             }
@@ -919,8 +1184,8 @@ int rp3dg_world_create(rp3dg_ctx* ctx, const rp3dg_world_settings* s, const rp3d
             float tmp[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
             float total2 = 0.0f;
             for (uint32_t k : mine) {
-                float vol, in[3], m;
-                shape_mass(w->shapes[size_t(cd[k].shape)], cd[k].mass_density, &vol, in, &m);
+                float in[3], m;
+                shape_mass(g->shapes[size_t(cd[k].shape)], cd[k].mass_density, in, &m);
                 total2 += m;
                 float R[3][3], RT[3][3], I[3][3];
                 quat_matrix(cd[k].orientation, R);
@@ -957,554 +1222,583 @@ int rp3dg_world_create(rp3dg_ctx* ctx, const rp3dg_world_settings* s, const rp3d
         col[BC_MASS][b].w = d.angular_damping;
         col[BC_LLOCK][b] = make_float4(d.linear_lock[0], d.linear_lock[1], d.linear_lock[2], 0.f);
         col[BC_ALOCK][b] = make_float4(d.angular_lock[0], d.angular_lock[1], d.angular_lock[2], 0.f);
-        gravity[b] = d.gravity_enabled ? 1 : 0;
+        w.gravity[b] = d.gravity_enabled ? 1 : 0;
         B.allowed_sleep = d.allowed_to_sleep != 0;
         if (d.type != RP3DG_BODY_STATIC) {
             col[BC_LV][b] = make_float4(d.linear_velocity[0], d.linear_velocity[1], d.linear_velocity[2], 0.f);
             col[BC_AV][b] = make_float4(d.angular_velocity[0], d.angular_velocity[1], d.angular_velocity[2], 0.f);
         }
     }
-    w->gravity = gravity;
-    // device arrays in component order
-    cudaError_t e = cudaSuccess;
-    auto M = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(p, std::max<size_t>(bytes, 16)); };
-    for (int k = 0; k < 2; k++) {
-        for (int c = 0; c < BC_NCOL; c++) M((void**)&w->bcol[k][c], size_t(nb) * 16);
-        M((void**)&w->biiw[k], size_t(nb) * 48);
-        for (int c = 0; c < CC_NCOL; c++) M((void**)&w->ccol[k][c], size_t(nc) * 16);
-    }
-    M((void**)&w->bgrav, nb);
-    M((void**)&w->c_body, size_t(nc) * 4);
-    M((void**)&w->c_shape, size_t(nc) * 4);
-    M((void**)&w->c_cat, size_t(nc) * 2);
-    M((void**)&w->c_mask, size_t(nc) * 2);
-    M((void**)&w->c_moved, nc);
-    if (e != cudaSuccess) {
-        rp3dg_world_destroy(w);
-        return cfail(ctx, RP3DG_ENOMEM, "cudaMalloc(world)");
-    }
-    w->dev_body_at = w->bcomp.at;
-    w->dev_col_at = w->ccomp.at;
-    {
-        std::vector<float4> tmp(std::max(nb, nc));
-        for (int c = 0; c < BC_NCOL; c++) {
-            for (uint32_t r = 0; r < nb; r++) tmp[r] = col[c][size_t(w->bcomp.at[r])];
-            cudaMemcpyAsync(w->bcol[0][c], tmp.data(), size_t(nb) * 16, cudaMemcpyHostToDevice, w->stream);
-            cudaStreamSynchronize(w->stream);
-        }
-        cudaMemsetAsync(w->biiw[0], 0, size_t(nb) * 48, w->stream);
-        for (int c = 0; c < CC_NCOL; c++) {
-            for (uint32_t r = 0; r < nc; r++) tmp[r] = ccols[c][size_t(w->ccomp.at[r])];
-            cudaMemcpyAsync(w->ccol[0][c], tmp.data(), size_t(nc) * 16, cudaMemcpyHostToDevice, w->stream);
-            cudaStreamSynchronize(w->stream);
-        }
-        std::vector<uint8_t> dyn(nb);
-        for (uint32_t r = 0; r < nb; r++) dyn[r] = dynamic[size_t(w->bcomp.at[r])];
-        uint8_t* d_dyn = nullptr;
-        cudaMalloc(&d_dyn, std::max<uint32_t>(nb, 1));
-        cudaMemcpyAsync(d_dyn, dyn.data(), nb, cudaMemcpyHostToDevice, w->stream);
-        w->tables_dirty = true;
-        int rc = upload_tables(w);
-        if (rc) { cudaFree(d_dyn); rp3dg_world_destroy(w); return rc; }
-        const uint32_t n = std::max(nb, nc);
-        if (n)
-            world_setup<<<blocks(n), 128, 0, w->stream>>>(nb, w->bcol[0][BC_POS], w->bcol[0][BC_ORI], w->bcol[0][BC_COML],
-                                                          w->bcol[0][BC_COMW], d_dyn, nc, w->c_body, w->ccol[0][CC_LPOS],
-                                                          w->ccol[0][CC_LORI], w->ccol[0][CC_WPOS], w->ccol[0][CC_WORI]);
-        cudaStreamSynchronize(w->stream);
-        cudaFree(d_dyn);
-    }
-    // initial fat AABBs of every collider (addCollider -> addObject)
-    if (nc) {
-        uint8_t* force = nullptr;
-        cudaMalloc(&force, nc);
-        cudaMemsetAsync(force, 1, nc, w->stream);
-        rp3dg_broadphase bp{};
-        bp.n = nc;
-        bp.n_update = nc;
-        bp.shape = w->c_shape;
-        bp.body = w->c_body;
-        bp.world_position = reinterpret_cast<rp3dg_float4*>(w->ccol[0][CC_WPOS]);
-        bp.world_orientation = reinterpret_cast<rp3dg_float4*>(w->ccol[0][CC_WORI]);
-        bp.force_reinsert = force;
-        bp.fat_min = reinterpret_cast<rp3dg_float4*>(w->ccol[0][CC_FMIN]);
-        bp.fat_max = reinterpret_cast<rp3dg_float4*>(w->ccol[0][CC_FMAX]);
-        bp.moved = w->c_moved;
-        int rc = rp3dg_broadphase_update_device(ctx, &bp);
-        std::vector<float4> fmin(nc), fmax(nc);
-        cudaMemcpyAsync(fmin.data(), w->ccol[0][CC_FMIN], size_t(nc) * 16, cudaMemcpyDeviceToHost, w->stream);
-        cudaMemcpyAsync(fmax.data(), w->ccol[0][CC_FMAX], size_t(nc) * 16, cudaMemcpyDeviceToHost, w->stream);
-        e = cudaStreamSynchronize(w->stream);
-        cudaFree(force);
-        if (rc || e != cudaSuccess) {
-            rp3dg_world_destroy(w);
-            return rc ? rc : cfail(ctx, RP3DG_ECUDA, "initial broad phase");
-        }
-        w->bp_to_collider.clear();
-        for (int c : creation_order) {
-            const uint32_t r = uint32_t(w->ccomp.slot[size_t(c)]);
-            Box box;
-            box.mn[0] = fmin[r].x; box.mn[1] = fmin[r].y; box.mn[2] = fmin[r].z;
-            box.mx[0] = fmax[r].x; box.mx[1] = fmax[r].y; box.mx[2] = fmax[r].z;
-            const int id = w->tree.add_object(box, c);
-            w->colliders[size_t(c)].bp = id;
-            if (size_t(id) >= w->bp_to_collider.size()) w->bp_to_collider.resize(size_t(id) + 1, -1);
-            w->bp_to_collider[size_t(id)] = c;
-            w->moved.add(id);
-        }
-    }
-    *out = w;
+    w.dev_body_at = w.bcomp.at;
+    w.dev_col_at = w.ccomp.at;
     return 0;
 }
 
-void rp3dg_world_destroy(rp3dg_world* w) {
-    if (!w) return;
-    for (int k = 0; k < 2; k++) {
-        for (int c = 0; c < BC_NCOL; c++) cudaFree(w->bcol[k][c]);
-        cudaFree(w->biiw[k]);
-        for (int c = 0; c < CC_NCOL; c++) cudaFree(w->ccol[k][c]);
-        w->cbuf[k].release();
+int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds, const uint32_t* boff,
+                 const rp3dg_body_desc* bd, const uint32_t* coff, const rp3dg_collider_desc* cd, int nthreads,
+                 Group** out) {
+    if (!ctx || !s || !out || !boff || !coff) return ctx ? cfail(ctx, RP3DG_EINVAL, "null argument") : RP3DG_EINVAL;
+    *out = nullptr;
+    auto* g = new Group();
+    g->ctx = ctx;
+    g->stream = static_cast<cudaStream_t>(rp3dg_stream(ctx));
+    g->set = *s;
+    g->nthreads = nthreads > 0 ? nthreads : 1;
+    if (rp3dg::get_shapes_host(ctx, &g->shapes) || g->shapes.empty()) {
+        destroy_group(g);
+        return cfail(ctx, RP3DG_EINVAL, "no shape table (rp3dg_set_shapes)");
     }
-    cudaFree(w->bgrav); cudaFree(w->c_body); cudaFree(w->c_shape); cudaFree(w->c_cat); cudaFree(w->c_mask);
-    cudaFree(w->c_moved); cudaFree(w->pool); cudaFree(w->d_small);
-    cudaFree(w->d_items); cudaFree(w->d_s1); cudaFree(w->d_s2); cudaFree(w->d_p1); cudaFree(w->d_r1);
-    cudaFree(w->d_p2); cudaFree(w->d_r2); cudaFree(w->d_rep); cudaFree(w->d_coll); cudaFree(w->d_nct);
-    cudaFree(w->d_cache); cudaFree(w->d_nd); cudaFree(w->d_l1); cudaFree(w->d_l2);
-    cudaFree(w->d_mids); cudaFree(w->d_msrc); cudaFree(w->d_mprev); cudaFree(w->d_istart); cudaFree(w->d_icount);
-    cudaFreeHost(w->h_items); cudaFreeHost(w->h_out); cudaFreeHost(w->h_mids); cudaFreeHost(w->h_msrc);
-    cudaFreeHost(w->h_mprev); cudaFreeHost(w->h_istart); cudaFreeHost(w->h_icount); cudaFreeHost(w->h_step);
-    delete w;
+    if (nworlds == 0) {
+        destroy_group(g);
+        return cfail(ctx, RP3DG_EINVAL, "no world");
+    }
+    g->worlds.resize(nworlds);
+    std::vector<float4> col[BC_NCOL], ccols[CC_NCOL];
+    std::vector<float4> wcol[BC_NCOL], wccols[CC_NCOL];
+    std::vector<uint8_t> dyn_all, dyn;
+    std::vector<std::vector<int>> orders(nworlds);
+    uint32_t NB = 0, NC = 0;
+    for (uint32_t k = 0; k < nworlds; k++) {
+        if (boff[k + 1] < boff[k] || coff[k + 1] < coff[k]) {
+            destroy_group(g);
+            return cfail(ctx, RP3DG_EINVAL, "world offsets must not decrease");
+        }
+        WorldH& w = g->worlds[k];
+        w.b0 = NB;
+        w.c0 = NC;
+        int rc = build_world(g, w, bd + boff[k], boff[k + 1] - boff[k], cd + coff[k], coff[k + 1] - coff[k], wcol,
+                             wccols, dyn, orders[k]);
+        if (rc) {
+            destroy_group(g);
+            return rc;
+        }
+        // host columns in component order
+        for (int c = 0; c < BC_NCOL; c++)
+            for (uint32_t r = 0; r < w.nb; r++) col[c].push_back(wcol[c][size_t(w.bcomp.at[r])]);
+        for (uint32_t r = 0; r < w.nb; r++) dyn_all.push_back(dyn[size_t(w.bcomp.at[r])]);
+        for (int c = 0; c < CC_NCOL; c++)
+            for (uint32_t r = 0; r < w.nc; r++) ccols[c].push_back(wccols[c][size_t(w.ccomp.at[r])]);
+        NB += w.nb;
+        NC += w.nc;
+    }
+    g->NB = NB;
+    g->NC = NC;
+    cudaError_t e = cudaSuccess;
+    auto M = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(p, std::max<size_t>(bytes, 16)); };
+    for (int k = 0; k < 2; k++) {
+        for (int c = 0; c < BC_NCOL; c++) M((void**)&g->bcol[k][c], size_t(NB) * 16);
+        M((void**)&g->biiw[k], size_t(NB) * 48);
+        for (int c = 0; c < CC_NCOL; c++) M((void**)&g->ccol[k][c], size_t(NC) * 16);
+    }
+    M((void**)&g->bgrav, NB); M((void**)&g->b_en, NB); M((void**)&g->c_en, NC);
+    M((void**)&g->c_body, size_t(NC) * 4); M((void**)&g->c_shape, size_t(NC) * 4);
+    M((void**)&g->c_cat, size_t(NC) * 2); M((void**)&g->c_mask, size_t(NC) * 2); M((void**)&g->c_moved, NC);
+    uint8_t* d_dyn = nullptr;
+    M((void**)&d_dyn, NB);
+    if (e != cudaSuccess) {
+        cudaFree(d_dyn);
+        destroy_group(g);
+        return cfail(ctx, RP3DG_ENOMEM, "cudaMalloc(world)");
+    }
+    for (int c = 0; c < BC_NCOL; c++)
+        if (NB) cudaMemcpyAsync(g->bcol[0][c], col[c].data(), size_t(NB) * 16, cudaMemcpyHostToDevice, g->stream);
+    cudaMemsetAsync(g->biiw[0], 0, size_t(NB) * 48, g->stream);
+    for (int c = 0; c < CC_NCOL; c++)
+        if (NC) cudaMemcpyAsync(g->ccol[0][c], ccols[c].data(), size_t(NC) * 16, cudaMemcpyHostToDevice, g->stream);
+    if (NB) cudaMemcpyAsync(d_dyn, dyn_all.data(), NB, cudaMemcpyHostToDevice, g->stream);
+    g->tables_dirty = true;
+    int rc = sync_rows(g);
+    if (rc) {
+        cudaFree(d_dyn);
+        destroy_group(g);
+        return rc;
+    }
+    const uint32_t n = std::max(NB, NC);
+    if (n)
+        world_setup<<<blocks(n), 128, 0, g->stream>>>(NB, g->bcol[0][BC_POS], g->bcol[0][BC_ORI], g->bcol[0][BC_COML],
+                                                      g->bcol[0][BC_COMW], d_dyn, NC, g->c_body, g->ccol[0][CC_LPOS],
+                                                      g->ccol[0][CC_LORI], g->ccol[0][CC_WPOS], g->ccol[0][CC_WORI]);
+    e = cudaStreamSynchronize(g->stream);
+    cudaFree(d_dyn);
+    if (e != cudaSuccess) {
+        destroy_group(g);
+        return cfail(ctx, RP3DG_ECUDA, "world set-up kernel");
+    }
+    // initial fat AABBs of every collider (addCollider -> addObject)
+    if (NC) {
+        uint8_t* force = nullptr;
+        cudaMalloc(&force, NC);
+        cudaMemsetAsync(force, 1, NC, g->stream);
+        rp3dg_broadphase bp{};
+        bp.n = NC;
+        bp.n_update = NC;
+        bp.shape = g->c_shape;
+        bp.body = g->c_body;
+        bp.world_position = reinterpret_cast<rp3dg_float4*>(g->ccol[0][CC_WPOS]);
+        bp.world_orientation = reinterpret_cast<rp3dg_float4*>(g->ccol[0][CC_WORI]);
+        bp.force_reinsert = force;
+        bp.fat_min = reinterpret_cast<rp3dg_float4*>(g->ccol[0][CC_FMIN]);
+        bp.fat_max = reinterpret_cast<rp3dg_float4*>(g->ccol[0][CC_FMAX]);
+        bp.moved = g->c_moved;
+        rc = rp3dg_broadphase_update_device(ctx, &bp);
+        std::vector<float4> fmin(NC), fmax(NC);
+        cudaMemcpyAsync(fmin.data(), g->ccol[0][CC_FMIN], size_t(NC) * 16, cudaMemcpyDeviceToHost, g->stream);
+        cudaMemcpyAsync(fmax.data(), g->ccol[0][CC_FMAX], size_t(NC) * 16, cudaMemcpyDeviceToHost, g->stream);
+        e = cudaStreamSynchronize(g->stream);
+        cudaFree(force);
+        if (rc || e != cudaSuccess) {
+            destroy_group(g);
+            return rc ? rc : cfail(ctx, RP3DG_ECUDA, "initial broad phase");
+        }
+        for (uint32_t k = 0; k < nworlds; k++) {
+            WorldH& w = g->worlds[k];
+            for (int c : orders[k]) {
+                const uint32_t r = w.c0 + uint32_t(w.ccomp.slot[size_t(c)]);
+                Box box;
+                box.mn[0] = fmin[r].x; box.mn[1] = fmin[r].y; box.mn[2] = fmin[r].z;
+                box.mx[0] = fmax[r].x; box.mx[1] = fmax[r].y; box.mx[2] = fmax[r].z;
+                const int id = w.tree.add_object(box, c);
+                w.colliders[size_t(c)].bp = id;
+                if (size_t(id) >= w.bp_to_collider.size()) w.bp_to_collider.resize(size_t(id) + 1, -1);
+                w.bp_to_collider[size_t(id)] = c;
+                w.moved.add(id);
+            }
+        }
+    }
+    *out = g;
+    return 0;
 }
 
-int rp3dg_world_update(rp3dg_world* w, float dt) {
-    if (!w) return RP3DG_EINVAL;
-    if (!(dt > 0.0f)) return wfail(w, RP3DG_EINVAL, "dt must be positive");
-    cudaStream_t st = w->stream;
-    rp3dg_ctx* ctx = w->ctx;
-    std::memset(&w->stats, 0, sizeof(w->stats));
+int update_group(Group* g, float dt) {
+    if (!g) return RP3DG_EINVAL;
+    if (!(dt > 0.0f)) return wfail(g, RP3DG_EINVAL, "dt must be positive");
+    cudaStream_t st = g->stream;
+    rp3dg_ctx* ctx = g->ctx;
+    std::memset(&g->stats, 0, sizeof(g->stats));
     // phase timer: with profiling on, the stream is drained at each mark so
     // that GPU time is charged to the phase that queued it
     auto mark = [&](int k) {
-        if (!w->profiling) return;
-        cudaStreamSynchronize(w->stream);
+        if (!g->profiling) return;
+        cudaStreamSynchronize(st);
         const auto now = std::chrono::steady_clock::now();
-        w->phase_ms[k] += std::chrono::duration<double, std::milli>(now - w->t_mark).count();
-        w->t_mark = now;
+        g->phase_ms[k] += std::chrono::duration<double, std::milli>(now - g->t_mark).count();
+        g->t_mark = now;
     };
-    if (w->profiling) w->t_mark = std::chrono::steady_clock::now();
+    if (g->profiling) g->t_mark = std::chrono::steady_clock::now();
 
-    // ---- computeCollisionDetection: broad phase (host order, GPU fat AABBs)
-    broad_phase(w);
+    // ---- broad phase and middle phase of every world (host order, GPU fat AABBs)
+    for_worlds(g, [&](int k) { broad_and_middle_phase(g, g->worlds[size_t(k)]); });
     mark(0);
-
-    // ---- middle phase: narrow-phase batches in pair-array order
-    std::vector<int4> by_algo[NB_ALGOS];
-    std::vector<uint32_t> pair_of[NB_ALGOS];
-    for (uint32_t i = 0; i < w->pairs.size(); i++) {
-        PairH& p = w->pairs[i];
-        p.coll_curr = false;
-        const bool e1 = w->ccomp.enabled(p.c1), e2 = w->ccomp.enabled(p.c2);
-        if (!(e1 || e2)) continue;
-        const int a = p.algo - 1;
-        by_algo[a].push_back(make_int4(w->ccomp.slot[size_t(p.c1)], w->ccomp.slot[size_t(p.c2)], p.cache, 1));
-        pair_of[a].push_back(i);
-    }
-    w->items.clear();
-    w->item_pair.clear();
+    // batches: algorithm-major, worlds in order inside a batch
+    // sub-phase marks of phase 1 (8..12)
+    auto sub = [&](int k) {
+        if (!g->profiling) return;
+        cudaStreamSynchronize(st);
+        const auto now = std::chrono::steady_clock::now();
+        g->phase_ms[k] += std::chrono::duration<double, std::milli>(now - g->t_mark).count();
+        g->t_mark = now;
+    };
+    uint32_t T = 0;
     for (int a = 0; a < NB_ALGOS; a++) {
-        w->batch_start[a] = uint32_t(w->items.size());
-        w->items.insert(w->items.end(), by_algo[a].begin(), by_algo[a].end());
-        w->item_pair.insert(w->item_pair.end(), pair_of[a].begin(), pair_of[a].end());
+        g->batch_start[a] = T;
+        for (WorldH& w : g->worlds) {
+            w.item_off[a] = T - g->batch_start[a];
+            T += uint32_t(w.items[a].size());
+        }
     }
-    w->batch_start[NB_ALGOS] = uint32_t(w->items.size());
-    const uint32_t T = uint32_t(w->items.size());
-    w->stats.narrowphase_tests = T;
-    w->stats.overlapping_pairs = uint32_t(w->pairs.size());
-
-    mark(1);
-    int rc = ensure_pool(w);
+    g->batch_start[NB_ALGOS] = T;
+    g->stats.narrowphase_tests = T;
+    int rc = ensure_pool(g);
     if (rc) return rc;
-    if (!w->reset_slots.empty()) {
-        if (ensure_small(w, w->reset_slots.size())) return RP3DG_ENOMEM;
-        cudaMemcpyAsync(w->d_small, w->reset_slots.data(), w->reset_slots.size() * 4, cudaMemcpyHostToDevice, st);
-        world_reset_cache<<<blocks(uint32_t(w->reset_slots.size())), 128, 0, st>>>(uint32_t(w->reset_slots.size()),
-                                                                                 w->d_small, w->pool);
-        w->reset_slots.clear();
+    sub(8);
+    size_t nreset = 0;
+    for (WorldH& w : g->worlds) nreset += w.reset_slots.size();
+    if (nreset) {
+        if (host_grow(&g->h_reset, &g->cap_hreset, nreset) || dev_grow(&g->d_small, &g->cap_small, nreset))
+            return wfail(g, RP3DG_ENOMEM, "allocation of cache resets");
+        size_t o = 0;
+        for (WorldH& w : g->worlds) {
+            std::memcpy(g->h_reset + o, w.reset_slots.data(), w.reset_slots.size() * 4);
+            o += w.reset_slots.size();
+            w.reset_slots.clear();
+        }
+        cudaMemcpyAsync(g->d_small, g->h_reset, nreset * 4, cudaMemcpyHostToDevice, st);
+        world_reset_cache<<<blocks(uint32_t(nreset)), 128, 0, st>>>(uint32_t(nreset), g->d_small, g->pool);
     }
-    rc = sync_rows(w);
+    sub(9);
+    rc = sync_rows(g);
     if (rc) return rc;
-    rc = upload_tables(w);
-    if (rc) return rc;
-    const int cb = w->cur_b, cc = w->cur_c;
-
-    w->cpairs.clear();
+    sub(10);
     if (T) {
-        rc = ensure_items(w, T);
+        rc = ensure_items(g, T);
         if (rc) return rc;
-        std::memcpy(w->h_items, w->items.data(), size_t(T) * 16);
-        cudaMemcpyAsync(w->d_items, w->h_items, size_t(T) * 16, cudaMemcpyHostToDevice, st);
-        GatherArgs g;
-        g.n = T;
-        g.items = w->d_items;
-        g.c_shape = w->c_shape;
-        g.c_wpos = w->ccol[cc][CC_WPOS];
-        g.c_wori = w->ccol[cc][CC_WORI];
-        g.pool = w->pool;
-        g.s1 = w->d_s1; g.s2 = w->d_s2;
-        g.p1 = w->d_p1; g.r1 = w->d_r1; g.p2 = w->d_p2; g.r2 = w->d_r2;
-        g.report = w->d_rep;
-        g.cache = w->d_cache;
-        world_gather_batch<<<blocks(T), 128, 0, st>>>(g);
+    }
+    sub(12);
+    for_worlds(g, [&](int k) {
+        WorldH& w = g->worlds[size_t(k)];
+        for (int a = 0; a < NB_ALGOS; a++)
+            if (!w.items[a].empty())
+                std::memcpy(g->h_items + g->batch_start[a] + w.item_off[a], w.items[a].data(), w.items[a].size() * 16);
+    });
+    mark(1);
+    const int cc = g->cur_c;
+    if (T) {
+        cudaMemcpyAsync(g->d_items, g->h_items, size_t(T) * 16, cudaMemcpyHostToDevice, st);
+        GatherArgs ga;
+        ga.n = T;
+        ga.items = g->d_items;
+        ga.c_shape = g->c_shape;
+        ga.c_wpos = g->ccol[cc][CC_WPOS];
+        ga.c_wori = g->ccol[cc][CC_WORI];
+        ga.pool = g->pool;
+        ga.s1 = g->d_s1; ga.s2 = g->d_s2;
+        ga.p1 = g->d_p1; ga.r1 = g->d_r1; ga.p2 = g->d_p2; ga.r2 = g->d_r2;
+        ga.report = g->d_rep;
+        ga.cache = g->d_cache;
+        world_gather_batch<<<blocks(T), 128, 0, st>>>(ga);
         // ---- narrow phase + manifold step, one call per algorithm batch
         for (int a = 0; a < NB_ALGOS; a++) {
-            const uint32_t s0 = w->batch_start[a], n = w->batch_start[a + 1] - s0;
+            const uint32_t s0 = g->batch_start[a], n = g->batch_start[a + 1] - s0;
             if (!n) continue;
             rp3dg_pair_batch pb{};
             pb.n = n;
-            pb.shape1 = w->d_s1 + s0; pb.shape2 = w->d_s2 + s0;
-            pb.pos1 = reinterpret_cast<rp3dg_float4*>(w->d_p1 + s0);
-            pb.rot1 = reinterpret_cast<rp3dg_float4*>(w->d_r1 + s0);
-            pb.pos2 = reinterpret_cast<rp3dg_float4*>(w->d_p2 + s0);
-            pb.rot2 = reinterpret_cast<rp3dg_float4*>(w->d_r2 + s0);
-            pb.report_contacts = w->d_rep + s0;
-            pb.cache = w->d_cache + s0;
+            pb.shape1 = g->d_s1 + s0; pb.shape2 = g->d_s2 + s0;
+            pb.pos1 = reinterpret_cast<rp3dg_float4*>(g->d_p1 + s0);
+            pb.rot1 = reinterpret_cast<rp3dg_float4*>(g->d_r1 + s0);
+            pb.pos2 = reinterpret_cast<rp3dg_float4*>(g->d_p2 + s0);
+            pb.rot2 = reinterpret_cast<rp3dg_float4*>(g->d_r2 + s0);
+            pb.report_contacts = g->d_rep + s0;
+            pb.cache = g->d_cache + s0;
             rp3dg_contact_batch cbt{};
-            cbt.is_colliding = w->d_coll + s0;
-            cbt.nb_contacts = w->d_nct + s0;
-            cbt.normal_depth = reinterpret_cast<rp3dg_float4*>(w->d_nd + size_t(s0) * MAXC);
-            cbt.local1 = reinterpret_cast<rp3dg_float4*>(w->d_l1 + size_t(s0) * MAXC);
-            cbt.local2 = reinterpret_cast<rp3dg_float4*>(w->d_l2 + size_t(s0) * MAXC);
+            cbt.is_colliding = g->d_coll + s0;
+            cbt.nb_contacts = g->d_nct + s0;
+            cbt.normal_depth = reinterpret_cast<rp3dg_float4*>(g->d_nd + size_t(s0) * MAXC);
+            cbt.local1 = reinterpret_cast<rp3dg_float4*>(g->d_l1 + size_t(s0) * MAXC);
+            cbt.local2 = reinterpret_cast<rp3dg_float4*>(g->d_l2 + size_t(s0) * MAXC);
             cbt.max_contacts = MAXC;
             rc = rp3dg_narrowphase_device(ctx, a + 1, &pb, &cbt, 1);
-            if (rc) return wfail(w, rc, std::string("narrow phase: ") + rp3dg_last_error(ctx));
+            if (rc) return rc;
             rc = rp3dg_reduce_contacts_device(ctx, &pb, &cbt, nullptr);
-            if (rc) return wfail(w, rc, std::string("manifold step: ") + rp3dg_last_error(ctx));
+            if (rc) return rc;
         }
-        world_scatter_cache<<<blocks(T), 128, 0, st>>>(T, w->d_items, w->d_cache, w->pool);
-        cudaMemcpyAsync(w->h_out, w->d_coll, T, cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(w->h_out + T, w->d_nct, T, cudaMemcpyDeviceToHost, st);
+        world_scatter_cache<<<blocks(T), 128, 0, st>>>(T, g->d_items, g->d_cache, g->pool);
+        cudaMemcpyAsync(g->h_out, g->d_coll, T, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(g->h_out + T, g->d_nct, T, cudaMemcpyDeviceToHost, st);
         cudaError_t e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return wcuda(w, e, "narrow phase");
-        // ---- processAllPotentialContacts: contact pairs in batch order
-        for (uint32_t it = 0; it < T; it++) {
-            if (!w->h_out[it]) continue;
-            PairH& p = w->pairs[w->item_pair[it]];
-            p.coll_curr = true;
-            ContactPairH c;
-            c.id = p.id;
-            c.c1 = p.c1;
-            c.c2 = p.c2;
-            c.b1 = w->colliders[size_t(p.c1)].body;
-            c.b2 = w->colliders[size_t(p.c2)].body;
-            c.item = it;
-            c.k = w->h_out[T + it];
-            w->cpairs.push_back(c);
-        }
+        if (e != cudaSuccess) return wcuda(g, e, "narrow phase");
     }
     mark(2);
-    // addContactPairsToBodies
-    for (uint32_t p = 0; p < w->cpairs.size(); p++) {
-        w->bodies[size_t(w->cpairs[p].b1)].contact_pairs.push_back(p);
-        w->bodies[size_t(w->cpairs[p].b2)].contact_pairs.push_back(p);
+    // ---- contact pairs and islands of every world
+    const uint8_t* h_coll = g->h_out;
+    const uint8_t* h_count = g->h_out + T;
+    for_worlds(g, [&](int k) { contacts_and_islands(g, g->worlds[size_t(k)], h_coll, h_count); });
+    uint32_t NM = 0, NP = 0, NI = 0;
+    for (WorldH& w : g->worlds) {
+        w.man_base = NM;
+        w.pt_base = NP;
+        w.isl_base = NI;
+        NM += w.nm;
+        NP += w.np;
+        NI += uint32_t(w.islands.size());
+        g->stats.contact_pairs += uint32_t(w.cpairs.size());
     }
-    w->stats.contact_pairs = uint32_t(w->cpairs.size());
-
-    // ---- createIslands (PhysicsWorld.cpp:695-866)
-    std::vector<int32_t> zero_rows;
-    w->island_order.clear();
-    w->islands.clear();
-    for (auto& B : w->bodies) B.in_island = false;
-    {
-        uint32_t total_manifolds = 0;
-        std::vector<int> stack, statics;
-        for (uint32_t s = 0; s < w->bcomp.n_enabled; s++) {
-            const int b0 = w->bcomp.at[s];
-            if (w->bodies[size_t(b0)].in_island) continue;
-            if (w->bodies[size_t(b0)].type == RP3DG_BODY_STATIC) continue;
-            stack.clear();
-            w->bodies[size_t(b0)].in_island = true;
-            stack.push_back(b0);
-            IslandH isl;
-            isl.manifold_start = total_manifolds;
-            const size_t isl_index = w->islands.size();
-            w->islands.push_back(isl);
-            while (!stack.empty()) {
-                const int b = stack.back();
-                stack.pop_back();
-                w->islands[isl_index].bodies.push_back(b);
-                set_sleeping(w, b, false, &zero_rows);
-                if (w->bodies[size_t(b)].type == RP3DG_BODY_STATIC) {
-                    statics.push_back(b);
-                    continue;
-                }
-                for (uint32_t cpi : w->bodies[size_t(b)].contact_pairs) {
-                    ContactPairH& cp = w->cpairs[cpi];
-                    if (cp.in_island) continue;
-                    cp.in_island = true;
-                    const int other = cp.b1 == b ? cp.b2 : cp.b1;
-                    if (w->bodies[size_t(other)].has_sim_collider) {
-                        w->island_order.push_back(cpi);
-                        total_manifolds += 1;
-                        w->islands[isl_index].manifold_count += 1;
-                        if (w->bodies[size_t(other)].in_island) continue;
-                        stack.push_back(other);
-                        w->bodies[size_t(other)].in_island = true;
-                    }
-                }
-            }
-            for (int sb : statics) w->bodies[size_t(sb)].in_island = false;
-            statics.clear();
-        }
-        for (auto& cp : w->cpairs) {
-            w->bodies[size_t(cp.b1)].contact_pairs.clear();
-            w->bodies[size_t(cp.b2)].contact_pairs.clear();
-        }
+    g->stats.manifolds = NM;
+    g->stats.contact_points = NP;
+    g->stats.islands = NI;
+    if (g->cap_hm < NM || !g->h_mids) {
+        const size_t cap = std::max<size_t>(size_t(NM) * 2, 64);
+        cudaFreeHost(g->h_mids); cudaFreeHost(g->h_msrc); cudaFreeHost(g->h_mprev);
+        cudaFree(g->d_mids); cudaFree(g->d_msrc); cudaFree(g->d_mprev);
+        g->h_mids = g->h_msrc = g->h_mprev = nullptr;
+        g->d_mids = g->d_msrc = g->d_mprev = nullptr;
+        g->cap_hm = 0;
+        if (cudaMallocHost(&g->h_mids, cap * 16) || cudaMallocHost(&g->h_msrc, cap * 16) ||
+            cudaMallocHost(&g->h_mprev, cap * 16) || cudaMalloc(&g->d_mids, cap * 16) ||
+            cudaMalloc(&g->d_msrc, cap * 16) || cudaMalloc(&g->d_mprev, cap * 16))
+            return wfail(g, RP3DG_ENOMEM, "allocation of manifold staging");
+        g->cap_hm = cap;
     }
-    w->stats.islands = uint32_t(w->islands.size());
-
+    if (g->cap_hi < NI || !g->h_istart) {
+        const size_t cap = std::max<size_t>(size_t(NI) * 2, 64);
+        cudaFreeHost(g->h_istart); cudaFreeHost(g->h_icount); cudaFree(g->d_istart); cudaFree(g->d_icount);
+        g->h_istart = g->h_icount = nullptr;
+        g->d_istart = g->d_icount = nullptr;
+        g->cap_hi = 0;
+        if (cudaMallocHost(&g->h_istart, cap * 4) || cudaMallocHost(&g->h_icount, cap * 4) ||
+            cudaMalloc(&g->d_istart, cap * 4) || cudaMalloc(&g->d_icount, cap * 4))
+            return wfail(g, RP3DG_ENOMEM, "allocation of island arrays");
+        g->cap_hi = cap;
+    }
     mark(3);
-    // ---- createContacts: manifolds and points in island order
-    rc = sync_rows(w);
+    // rows may have moved (bodies woken by the islands): sync before packing ids
+    rc = sync_rows(g);
     if (rc) return rc;
-    rc = upload_tables(w);
-    if (rc) return rc;
-    const int bc = w->cur_b, ccur = w->cur_c;
-    ContactBuf& CB = w->cbuf[w->cur_cb];
-    ContactBuf& PB = w->cbuf[1 - w->cur_cb];
-    const uint32_t nm = uint32_t(w->island_order.size());
-    uint32_t np = 0;
-    {
-        if (dev_grow(&w->d_mids, &w->cap_m, std::max<uint32_t>(nm, 1))) return wfail(w, RP3DG_ENOMEM, "cudaMalloc");
-        if (w->cap_hm < nm || !w->h_mids) {
-            size_t cap = std::max<size_t>(nm, 64);
-            cudaFreeHost(w->h_mids); cudaFreeHost(w->h_msrc); cudaFreeHost(w->h_mprev);
-            cudaFree(w->d_msrc); cudaFree(w->d_mprev);
-            cudaFree(w->d_mids);
-            w->cap_m = 0;
-            if (cudaMallocHost(&w->h_mids, cap * 16) || cudaMallocHost(&w->h_msrc, cap * 16) ||
-                cudaMallocHost(&w->h_mprev, cap * 16) || cudaMalloc(&w->d_mids, cap * 16) ||
-                cudaMalloc(&w->d_msrc, cap * 16) || cudaMalloc(&w->d_mprev, cap * 16))
-                return wfail(w, RP3DG_ENOMEM, "allocation of manifold staging");
-            w->cap_hm = cap;
-            w->cap_m = cap;
-        }
-        for (uint32_t m = 0; m < nm; m++) {
-            ContactPairH& cp = w->cpairs[w->island_order[m]];
-            cp.manifold = m;
-            cp.point = np;
-            uint32_t a = 0;
-            while (cp.item >= w->batch_start[a + 1]) a++;
-            const uint32_t s0 = w->batch_start[a];
-            w->h_mids[m] = make_int4(w->bcomp.slot[size_t(cp.b1)], w->bcomp.slot[size_t(cp.b2)],
-                                     w->ccomp.slot[size_t(cp.c1)], w->ccomp.slot[size_t(cp.c2)]);
-            w->h_msrc[m] = make_int4(int(cp.item - s0), int(w->batch_start[a + 1] - s0), int(s0), int(np));
-            auto it = w->prev_map.find(cp.id);
-            if (it != w->prev_map.end() && w->prev_cpairs[it->second].in_island) {
-                const ContactPairH& pc = w->prev_cpairs[it->second];
-                w->h_mprev[m] = make_int4(int(pc.manifold), 1, int(pc.point), int(pc.k));
-            } else {
-                w->h_mprev[m] = make_int4(-1, 0, 0, 0);
-            }
-            np += cp.k;
-        }
-        if (CB.ensure(std::max<uint32_t>(nm, 1), std::max<uint32_t>(np, 1))) return wfail(w, RP3DG_ENOMEM, "cudaMalloc(contacts)");
-        if (nm) {
-            cudaMemcpyAsync(w->d_mids, w->h_mids, size_t(nm) * 16, cudaMemcpyHostToDevice, st);
-            cudaMemcpyAsync(w->d_msrc, w->h_msrc, size_t(nm) * 16, cudaMemcpyHostToDevice, st);
-            cudaMemcpyAsync(w->d_mprev, w->h_mprev, size_t(nm) * 16, cudaMemcpyHostToDevice, st);
-            PackArgs a;
-            a.nm = nm;
-            a.ids = w->d_mids;
-            a.src = w->d_msrc;
-            a.prev = w->d_mprev;
-            a.kept_count = w->d_nct;
-            a.b_nd = w->d_nd; a.b_l1 = w->d_l1; a.b_l2 = w->d_l2;
-            a.cos_similar = w->set.cos_angle_similar_contact_manifold;
-            a.persist2 = w->set.persistent_contact_distance_threshold * w->set.persistent_contact_distance_threshold;
-            a.pm_pstart = PB.pstart; a.pm_fv1 = PB.fv1; a.pm_fv2 = PB.fv2; a.pm_fimp = PB.fimp;
-            a.pp_nd = PB.nd; a.pp_l1 = PB.l1; a.pp_imp = PB.imp; a.pp_rest = PB.rest;
-            a.m_ids = CB.ids; a.m_pstart = CB.pstart; a.m_npts = CB.npts;
-            a.m_fv1 = CB.fv1; a.m_fv2 = CB.fv2; a.m_fimp = CB.fimp;
-            a.p_nd = CB.nd; a.p_l1 = CB.l1; a.p_l2 = CB.l2; a.p_imp = CB.imp; a.p_rest = CB.rest;
-            world_pack_contacts<<<blocks(nm), 128, 0, st>>>(a);
-        }
+    for_worlds(g, [&](int k) { fill_manifolds(g, g->worlds[size_t(k)]); });
+    const int bc = g->cur_b, ccur = g->cur_c;
+    ContactBuf& CB = g->cbuf[g->cur_cb];
+    ContactBuf& PB = g->cbuf[1 - g->cur_cb];
+    if (CB.ensure(std::max<uint32_t>(NM, 1), std::max<uint32_t>(NP, 1))) return wfail(g, RP3DG_ENOMEM, "cudaMalloc(contacts)");
+    if (NM) {
+        cudaMemcpyAsync(g->d_mids, g->h_mids, size_t(NM) * 16, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->d_msrc, g->h_msrc, size_t(NM) * 16, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->d_mprev, g->h_mprev, size_t(NM) * 16, cudaMemcpyHostToDevice, st);
+        PackArgs a;
+        a.nm = NM;
+        a.ids = g->d_mids;
+        a.src = g->d_msrc;
+        a.prev = g->d_mprev;
+        a.kept_count = g->d_nct;
+        a.b_nd = g->d_nd; a.b_l1 = g->d_l1; a.b_l2 = g->d_l2;
+        a.cos_similar = g->set.cos_angle_similar_contact_manifold;
+        a.persist2 = g->set.persistent_contact_distance_threshold * g->set.persistent_contact_distance_threshold;
+        a.pm_pstart = PB.pstart; a.pm_fv1 = PB.fv1; a.pm_fv2 = PB.fv2; a.pm_fimp = PB.fimp;
+        a.pp_nd = PB.nd; a.pp_l1 = PB.l1; a.pp_imp = PB.imp; a.pp_rest = PB.rest;
+        a.m_ids = CB.ids; a.m_pstart = CB.pstart; a.m_npts = CB.npts;
+        a.m_fv1 = CB.fv1; a.m_fv2 = CB.fv2; a.m_fimp = CB.fimp;
+        a.p_nd = CB.nd; a.p_l1 = CB.l1; a.p_l2 = CB.l2; a.p_imp = CB.imp; a.p_rest = CB.rest;
+        world_pack_contacts<<<blocks(NM), 128, 0, st>>>(a);
     }
-    CB.nm = nm;
-    CB.np = np;
-    w->stats.manifolds = nm;
-    w->stats.contact_points = np;
-    // computeMapPreviousContactPairs for the next step
-    w->prev_map.clear();
-    for (uint32_t i = 0; i < w->cpairs.size(); i++) w->prev_map[w->cpairs[i].id] = i;
-
-    // islands as manifold ranges
-    const uint32_t ni = uint32_t(w->islands.size());
-    if (w->cap_hi < ni || !w->h_istart) {
-        size_t cap = std::max<size_t>(ni, 64);
-        cudaFreeHost(w->h_istart); cudaFreeHost(w->h_icount); cudaFree(w->d_istart); cudaFree(w->d_icount);
-        if (cudaMallocHost(&w->h_istart, cap * 4) || cudaMallocHost(&w->h_icount, cap * 4) ||
-            cudaMalloc(&w->d_istart, cap * 4) || cudaMalloc(&w->d_icount, cap * 4))
-            return wfail(w, RP3DG_ENOMEM, "allocation of island arrays");
-        w->cap_hi = cap;
-        w->cap_i = cap;
+    CB.nm = NM;
+    CB.np = NP;
+    if (NI) {
+        cudaMemcpyAsync(g->d_istart, g->h_istart, size_t(NI) * 4, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->d_icount, g->h_icount, size_t(NI) * 4, cudaMemcpyHostToDevice, st);
     }
-    for (uint32_t i = 0; i < ni; i++) {
-        w->h_istart[i] = w->islands[i].manifold_start;
-        w->h_icount[i] = w->islands[i].manifold_count;
-    }
-    if (ni) {
-        cudaMemcpyAsync(w->d_istart, w->h_istart, size_t(ni) * 4, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(w->d_icount, w->h_icount, size_t(ni) * 4, cudaMemcpyHostToDevice, st);
-    }
-
     mark(4);
     // ---- dynamics stage (inertia, velocities, solver, positions, state)
     {
         rp3dg_dynamics_params pr{};
         pr.dt = dt;
-        pr.gravity[0] = w->set.gravity[0]; pr.gravity[1] = w->set.gravity[1]; pr.gravity[2] = w->set.gravity[2];
+        pr.gravity[0] = g->set.gravity[0]; pr.gravity[1] = g->set.gravity[1]; pr.gravity[2] = g->set.gravity[2];
         pr.gravity_enabled = 1;
-        pr.velocity_iterations = w->set.velocity_iterations;
+        pr.velocity_iterations = g->set.velocity_iterations;
         pr.split_impulse = 1;
-        pr.restitution_velocity_threshold = w->set.restitution_velocity_threshold;
-        rp3dg_bodies B{};
-        B.n = w->nb;
-        B.n_enabled = w->bcomp.n_enabled;
+        pr.restitution_velocity_threshold = g->set.restitution_velocity_threshold;
         auto F = [](float4* p) { return reinterpret_cast<rp3dg_float4*>(p); };
-        B.position = F(w->bcol[bc][BC_POS]); B.orientation = F(w->bcol[bc][BC_ORI]);
-        B.com_world = F(w->bcol[bc][BC_COMW]); B.com_local = F(w->bcol[bc][BC_COML]);
-        B.linear_velocity = F(w->bcol[bc][BC_LV]); B.angular_velocity = F(w->bcol[bc][BC_AV]);
-        B.force = F(w->bcol[bc][BC_F]); B.torque = F(w->bcol[bc][BC_T]);
-        B.inv_inertia_local = F(w->bcol[bc][BC_IIL]); B.inv_inertia_world = F(w->biiw[bc]);
-        B.mass = F(w->bcol[bc][BC_MASS]); B.linear_lock = F(w->bcol[bc][BC_LLOCK]); B.angular_lock = F(w->bcol[bc][BC_ALOCK]);
-        B.gravity = w->bgrav;
+        rp3dg_bodies B{};
+        B.n = g->NB;
+        B.n_enabled = 0;  // per-row flags
+        B.position = F(g->bcol[bc][BC_POS]); B.orientation = F(g->bcol[bc][BC_ORI]);
+        B.com_world = F(g->bcol[bc][BC_COMW]); B.com_local = F(g->bcol[bc][BC_COML]);
+        B.linear_velocity = F(g->bcol[bc][BC_LV]); B.angular_velocity = F(g->bcol[bc][BC_AV]);
+        B.force = F(g->bcol[bc][BC_F]); B.torque = F(g->bcol[bc][BC_T]);
+        B.inv_inertia_local = F(g->bcol[bc][BC_IIL]); B.inv_inertia_world = F(g->biiw[bc]);
+        B.mass = F(g->bcol[bc][BC_MASS]); B.linear_lock = F(g->bcol[bc][BC_LLOCK]); B.angular_lock = F(g->bcol[bc][BC_ALOCK]);
+        B.gravity = g->bgrav;
         rp3dg_colliders C{};
-        C.n = w->nc;
-        C.n_enabled = w->ccomp.n_enabled;
-        C.body = w->c_body;
-        C.local_position = F(w->ccol[ccur][CC_LPOS]); C.local_orientation = F(w->ccol[ccur][CC_LORI]);
-        C.world_position = F(w->ccol[ccur][CC_WPOS]); C.world_orientation = F(w->ccol[ccur][CC_WORI]);
-        C.material = F(w->ccol[ccur][CC_MAT]);
+        C.n = g->NC;
+        C.n_enabled = 0;
+        C.body = g->c_body;
+        C.local_position = F(g->ccol[ccur][CC_LPOS]); C.local_orientation = F(g->ccol[ccur][CC_LORI]);
+        C.world_position = F(g->ccol[ccur][CC_WPOS]); C.world_orientation = F(g->ccol[ccur][CC_WORI]);
+        C.material = F(g->ccol[ccur][CC_MAT]);
         rp3dg_manifolds Mf{};
-        Mf.n = nm;
+        Mf.n = NM;
         Mf.ids = reinterpret_cast<int32_t*>(CB.ids);
         Mf.point_start = CB.pstart; Mf.nb_points = CB.npts;
         Mf.friction_vector1 = F(CB.fv1); Mf.friction_vector2 = F(CB.fv2); Mf.friction_impulse = F(CB.fimp);
         rp3dg_points P{};
-        P.n = np;
+        P.n = NP;
         P.normal_depth = F(CB.nd); P.local1 = F(CB.l1); P.local2 = F(CB.l2);
         P.penetration_impulse = CB.imp; P.is_resting = CB.rest;
         rp3dg_islands I{};
-        I.n = ni;
-        I.manifold_start = w->d_istart;
-        I.manifold_count = w->d_icount;
-        rc = rp3dg_dynamics_step_device(ctx, &pr, &B, &C, &Mf, &P, &I);
-        if (rc) return wfail(w, rc, std::string("dynamics: ") + rp3dg_last_error(ctx));
+        I.n = NI;
+        I.manifold_start = g->d_istart;
+        I.manifold_count = g->d_icount;
+        rc = rp3dg::dynamics_step_flags(ctx, &pr, &B, &C, &Mf, &P, &I, g->b_en, g->c_en);
+        if (rc) return rc;
     }
-
     mark(5);
     // ---- updateColliders: world AABBs, fat-AABB test, reinsertion flags
-    const uint32_t ncu = w->ccomp.n_enabled, nbe = w->bcomp.n_enabled;
-    const size_t step_bytes = size_t(ncu) + size_t(ncu) * 32 + size_t(nbe) * 32 + 64;
-    if (host_grow(&w->h_step, &w->cap_hstep, step_bytes)) return wfail(w, RP3DG_ENOMEM, "cudaMallocHost(step)");
-    uint8_t* h_moved = w->h_step;
-    float4* h_fmin = reinterpret_cast<float4*>(w->h_step + ((size_t(ncu) + 15) & ~size_t(15)));
-    float4* h_fmax = h_fmin + ncu;
-    float4* h_lv = h_fmax + ncu;
-    float4* h_av = h_lv + nbe;
-    if (ncu) {
+    const size_t step_bytes = ((size_t(g->NC) + 15) & ~size_t(15)) + size_t(g->NC) * 32 + size_t(g->NB) * 32 + 64;
+    if (host_grow(&g->h_step, &g->cap_hstep, step_bytes)) return wfail(g, RP3DG_ENOMEM, "cudaMallocHost(step)");
+    uint8_t* h_moved = g->h_step;
+    float4* h_fmin = reinterpret_cast<float4*>(g->h_step + ((size_t(g->NC) + 15) & ~size_t(15)));
+    float4* h_fmax = h_fmin + g->NC;
+    float4* h_lv = h_fmax + g->NC;
+    float4* h_av = h_lv + g->NB;
+    if (g->NC) {
         rp3dg_broadphase bp{};
-        bp.n = w->nc;
-        bp.n_update = ncu;
-        bp.shape = w->c_shape;
-        bp.body = w->c_body;
-        bp.world_position = reinterpret_cast<rp3dg_float4*>(w->ccol[ccur][CC_WPOS]);
-        bp.world_orientation = reinterpret_cast<rp3dg_float4*>(w->ccol[ccur][CC_WORI]);
-        bp.fat_min = reinterpret_cast<rp3dg_float4*>(w->ccol[ccur][CC_FMIN]);
-        bp.fat_max = reinterpret_cast<rp3dg_float4*>(w->ccol[ccur][CC_FMAX]);
-        bp.moved = w->c_moved;
-        rc = rp3dg_broadphase_update_device(ctx, &bp);
-        if (rc) return wfail(w, rc, std::string("broad-phase update: ") + rp3dg_last_error(ctx));
-        cudaMemcpyAsync(h_moved, w->c_moved, ncu, cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(h_fmin, w->ccol[ccur][CC_FMIN], size_t(ncu) * 16, cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(h_fmax, w->ccol[ccur][CC_FMAX], size_t(ncu) * 16, cudaMemcpyDeviceToHost, st);
+        bp.n = g->NC;
+        bp.n_update = g->NC;
+        bp.shape = g->c_shape;
+        bp.body = g->c_body;
+        bp.world_position = reinterpret_cast<rp3dg_float4*>(g->ccol[ccur][CC_WPOS]);
+        bp.world_orientation = reinterpret_cast<rp3dg_float4*>(g->ccol[ccur][CC_WORI]);
+        bp.fat_min = reinterpret_cast<rp3dg_float4*>(g->ccol[ccur][CC_FMIN]);
+        bp.fat_max = reinterpret_cast<rp3dg_float4*>(g->ccol[ccur][CC_FMAX]);
+        bp.moved = g->c_moved;
+        rc = rp3dg::broadphase_update_flags(ctx, &bp, g->c_en);
+        if (rc) return rc;
+        cudaMemcpyAsync(h_moved, g->c_moved, g->NC, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(h_fmin, g->ccol[ccur][CC_FMIN], size_t(g->NC) * 16, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(h_fmax, g->ccol[ccur][CC_FMAX], size_t(g->NC) * 16, cudaMemcpyDeviceToHost, st);
     }
-    if (w->set.sleeping_enabled && nbe) {
-        cudaMemcpyAsync(h_lv, w->bcol[bc][BC_LV], size_t(nbe) * 16, cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(h_av, w->bcol[bc][BC_AV], size_t(nbe) * 16, cudaMemcpyDeviceToHost, st);
+    if (g->set.sleeping_enabled && g->NB) {
+        cudaMemcpyAsync(h_lv, g->bcol[bc][BC_LV], size_t(g->NB) * 16, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(h_av, g->bcol[bc][BC_AV], size_t(g->NB) * 16, cudaMemcpyDeviceToHost, st);
     }
     cudaError_t e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return wcuda(w, e, "step");
-    uint32_t nmoved = 0;
-    for (uint32_t r = 0; r < ncu; r++) {
-        if (!h_moved[r]) continue;
-        const int c = w->ccomp.at[r];
-        Box box;
-        box.mn[0] = h_fmin[r].x; box.mn[1] = h_fmin[r].y; box.mn[2] = h_fmin[r].z;
-        box.mx[0] = h_fmax[r].x; box.mx[1] = h_fmax[r].y; box.mx[2] = h_fmax[r].z;
-        w->tree.reinsert(w->colliders[size_t(c)].bp, box);
-        add_moved(w, c);
-        nmoved++;
-    }
-    w->stats.moved_colliders = nmoved;
-
+    if (e != cudaSuccess) return wcuda(g, e, "step");
     mark(6);
-    // ---- updateSleepingBodies (PhysicsWorld.cpp:871-926)
-    if (w->set.sleeping_enabled) {
-        // velocities by body id, read before any body falls asleep
-        std::vector<float4> lv(w->nb), av(w->nb);
-        for (uint32_t r = 0; r < nbe; r++) {
-            lv[size_t(w->bcomp.at[r])] = h_lv[r];
-            av[size_t(w->bcomp.at[r])] = h_av[r];
-        }
-        const float slv2 = w->set.sleep_linear_velocity * w->set.sleep_linear_velocity;
-        const float sav2 = w->set.sleep_angular_velocity * w->set.sleep_angular_velocity;
-        for (const IslandH& isl : w->islands) {
-            float min_sleep = 3.40282347e+38f;
-            for (int b : isl.bodies) {
-                BodyH& B = w->bodies[size_t(b)];
-                if (B.type == RP3DG_BODY_STATIC) continue;
-                const float4 l = lv[size_t(b)], a = av[size_t(b)];
-                if (l.x * l.x + l.y * l.y + l.z * l.z > slv2 || a.x * a.x + a.y * a.y + a.z * a.z > sav2 ||
-                    !B.allowed_sleep) {
-                    B.sleep_time = 0.0f;
-                    min_sleep = 0.0f;
-                } else {
-                    B.sleep_time += dt;
-                    if (B.sleep_time < min_sleep) min_sleep = B.sleep_time;
-                }
-            }
-            if (min_sleep >= w->set.time_before_sleep)
-                for (int b : isl.bodies) set_sleeping(w, b, true, &zero_rows);
-        }
-    }
+    // ---- reinsertions and sleeping of every world
+    for_worlds(g, [&](int k) { colliders_and_sleep(g, g->worlds[size_t(k)], dt, h_moved, h_fmin, h_fmax, h_lv, h_av); });
     // velocities / forces of bodies put to sleep (rows in the current device order)
-    if (!zero_rows.empty()) {
-        std::vector<int32_t> rows, row_of(w->nb);
-        for (uint32_t r = 0; r < w->nb; r++) row_of[size_t(w->dev_body_at[r])] = int32_t(r);
-        for (int b : zero_rows)
-            if (w->bodies[size_t(b)].sleeping) rows.push_back(row_of[size_t(b)]);
-        if (!rows.empty()) {
-            if (ensure_small(w, rows.size())) return RP3DG_ENOMEM;
-            cudaMemcpyAsync(w->d_small, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice, st);
-            world_zero_rows<<<blocks(uint32_t(rows.size())), 128, 0, st>>>(uint32_t(rows.size()), w->d_small,
-                                                                           w->bcol[bc][BC_LV], w->bcol[bc][BC_AV],
-                                                                           w->bcol[bc][BC_F], w->bcol[bc][BC_T]);
-        }
+    std::vector<int32_t> rows;
+    for (WorldH& w : g->worlds) {
+        if (w.slept.empty()) continue;
+        std::vector<int32_t> row_of(w.nb);
+        for (uint32_t r = 0; r < w.nb; r++) row_of[size_t(w.dev_body_at[r])] = int32_t(w.b0 + r);
+        for (int b : w.slept)
+            if (w.bodies[size_t(b)].sleeping) rows.push_back(row_of[size_t(b)]);
+    }
+    if (!rows.empty()) {
+        if (ensure_small(g, rows.size())) return RP3DG_ENOMEM;
+        cudaMemcpyAsync(g->d_small, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice, st);
+        world_zero_rows<<<blocks(uint32_t(rows.size())), 128, 0, st>>>(uint32_t(rows.size()), g->d_small,
+                                                                       g->bcol[bc][BC_LV], g->bcol[bc][BC_AV],
+                                                                       g->bcol[bc][BC_F], g->bcol[bc][BC_T]);
     }
     // resetBodiesForceAndTorque
-    cudaMemsetAsync(w->bcol[bc][BC_F], 0, size_t(w->nb) * 16, st);
-    cudaMemsetAsync(w->bcol[bc][BC_T], 0, size_t(w->nb) * 16, st);
+    cudaMemsetAsync(g->bcol[bc][BC_F], 0, size_t(g->NB) * 16, st);
+    cudaMemsetAsync(g->bcol[bc][BC_T], 0, size_t(g->NB) * 16, st);
     e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return wcuda(w, e, "end of step");
-    // collidingInPreviousFrame for the next step (updateCollidingInPreviousFrame
-    // runs in reportContactsAndTriggers)
-    for (auto& p : w->pairs) p.coll_prev = p.coll_curr;
-    w->prev_cpairs.swap(w->cpairs);
-    w->cur_cb = 1 - w->cur_cb;
-    w->stats.disabled_pairs = uint32_t(w->disabled.size());
-    w->stats.enabled_bodies = w->bcomp.n_enabled;
+    if (e != cudaSuccess) return wcuda(g, e, "end of step");
+    g->cur_cb = 1 - g->cur_cb;
+    for (WorldH& w : g->worlds) {
+        g->stats.overlapping_pairs += uint32_t(w.pairs.size());
+        g->stats.disabled_pairs += w.stats.disabled_pairs;
+        g->stats.enabled_bodies += w.stats.enabled_bodies;
+        g->stats.moved_colliders += w.stats.moved_colliders;
+    }
     mark(7);
+    return 0;
+}
+
+int read_bodies(Group* g, uint32_t world, bool all, float* position, float* orientation, float* linear_velocity,
+                float* angular_velocity, uint8_t* sleeping) {
+    const uint32_t n = g->NB;
+    std::vector<float4> p(n), q(n), lv(n), av(n);
+    const int b = g->cur_b;
+    cudaMemcpyAsync(p.data(), g->bcol[b][BC_POS], size_t(n) * 16, cudaMemcpyDeviceToHost, g->stream);
+    cudaMemcpyAsync(q.data(), g->bcol[b][BC_ORI], size_t(n) * 16, cudaMemcpyDeviceToHost, g->stream);
+    cudaMemcpyAsync(lv.data(), g->bcol[b][BC_LV], size_t(n) * 16, cudaMemcpyDeviceToHost, g->stream);
+    cudaMemcpyAsync(av.data(), g->bcol[b][BC_AV], size_t(n) * 16, cudaMemcpyDeviceToHost, g->stream);
+    cudaError_t e = cudaStreamSynchronize(g->stream);
+    if (e != cudaSuccess) return wcuda(g, e, "read bodies");
+    uint32_t out_base = 0;
+    for (uint32_t k = 0; k < g->worlds.size(); k++) {
+        const WorldH& w = g->worlds[k];
+        if (!all && k != world) continue;
+        for (uint32_t r = 0; r < w.nb; r++) {
+            const size_t id = out_base + size_t(w.dev_body_at[r]);
+            const uint32_t row = w.b0 + r;
+            if (position) { position[3 * id] = p[row].x; position[3 * id + 1] = p[row].y; position[3 * id + 2] = p[row].z; }
+            if (orientation) {
+                orientation[4 * id] = q[row].x; orientation[4 * id + 1] = q[row].y;
+                orientation[4 * id + 2] = q[row].z; orientation[4 * id + 3] = q[row].w;
+            }
+            if (linear_velocity) {
+                linear_velocity[3 * id] = lv[row].x; linear_velocity[3 * id + 1] = lv[row].y; linear_velocity[3 * id + 2] = lv[row].z;
+            }
+            if (angular_velocity) {
+                angular_velocity[3 * id] = av[row].x; angular_velocity[3 * id + 1] = av[row].y; angular_velocity[3 * id + 2] = av[row].z;
+            }
+            if (sleeping) sleeping[id] = w.bodies[size_t(w.dev_body_at[r])].sleeping ? 1 : 0;
+        }
+        if (all) out_base += w.nb;
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rp3dg_world_create(rp3dg_ctx* ctx, const rp3dg_world_settings* s, const rp3dg_body_desc* bd, uint32_t nb,
+                       const rp3dg_collider_desc* cd, uint32_t nc, rp3dg_world** out) {
+    if ((nb && !bd) || (nc && !cd)) return ctx ? cfail(ctx, RP3DG_EINVAL, "null argument") : RP3DG_EINVAL;
+    const uint32_t boff[2] = {0, nb}, coff[2] = {0, nc};
+    return create_group(ctx, s, 1, boff, bd, coff, cd, 1, out);
+}
+
+int rp3dg_world_group_create(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nb_worlds,
+                             const uint32_t* body_offsets, const rp3dg_body_desc* bodies,
+                             const uint32_t* collider_offsets, const rp3dg_collider_desc* colliders, int nb_threads,
+                             rp3dg_world** out) {
+    if (nb_worlds && (!bodies || !colliders)) return ctx ? cfail(ctx, RP3DG_EINVAL, "null argument") : RP3DG_EINVAL;
+    return create_group(ctx, s, nb_worlds, body_offsets, bodies, collider_offsets, colliders, nb_threads, out);
+}
+
+void rp3dg_world_destroy(rp3dg_world* w) { destroy_group(w); }
+
+int rp3dg_world_update(rp3dg_world* w, float dt) { return update_group(w, dt); }
+
+int rp3dg_world_get_bodies(rp3dg_world* w, float* position, float* orientation, float* linear_velocity,
+                           float* angular_velocity, uint8_t* sleeping) {
+    if (!w) return RP3DG_EINVAL;
+    return read_bodies(w, 0, true, position, orientation, linear_velocity, angular_velocity, sleeping);
+}
+
+int rp3dg_world_group_get_bodies(rp3dg_world* w, uint32_t world, float* position, float* orientation,
+                                 float* linear_velocity, float* angular_velocity, uint8_t* sleeping) {
+    if (!w || world >= w->worlds.size()) return RP3DG_EINVAL;
+    return read_bodies(w, world, false, position, orientation, linear_velocity, angular_velocity, sleeping);
+}
+
+int rp3dg_world_group_get_pairs(rp3dg_world* g, uint32_t world, uint64_t* ids, uint32_t capacity, uint32_t* n) {
+    if (!g || !n || world >= g->worlds.size()) return RP3DG_EINVAL;
+    const WorldH& w = g->worlds[world];
+    uint32_t k = 0;
+    for (const auto& p : w.pairs) { if (ids && k < capacity) ids[k] = p.id; k++; }
+    for (const auto& p : w.disabled) { if (ids && k < capacity) ids[k] = p.id; k++; }
+    *n = k;
+    return 0;
+}
+
+int rp3dg_world_get_pairs(rp3dg_world* w, uint64_t* ids, uint32_t capacity, uint32_t* n) {
+    return rp3dg_world_group_get_pairs(w, 0, ids, capacity, n);
+}
+
+int rp3dg_world_group_get_contacts(rp3dg_world* g, uint32_t world, int32_t* body1, int32_t* body2, uint8_t* nb_points,
+                                   uint32_t capacity, float* normal_depth, float* local1, float* local2,
+                                   uint32_t capacity_points, uint32_t* nb_manifolds, uint32_t* nb_contact_points) {
+    if (!g || world >= g->worlds.size()) return RP3DG_EINVAL;
+    // the arrays of the last step are the "previous" buffer after the swap
+    const ContactBuf& B = g->cbuf[1 - g->cur_cb];
+    const WorldH& w = g->worlds[world];
+    const std::vector<ContactPairH>& cps = w.prev_cpairs;
+    if (nb_manifolds) *nb_manifolds = w.nm;
+    if (nb_contact_points) *nb_contact_points = w.np;
+    std::vector<uint32_t> order(w.nm);
+    for (uint32_t i = 0; i < cps.size(); i++)
+        if (cps[i].in_island) order[cps[i].manifold - w.man_base] = i;
+    for (uint32_t m = 0; m < w.nm && m < capacity; m++) {
+        const ContactPairH& c = cps[order[m]];
+        if (body1) body1[m] = c.b1;
+        if (body2) body2[m] = c.b2;
+        if (nb_points) nb_points[m] = uint8_t(c.k);
+    }
+    const uint32_t np = std::min(w.np, capacity_points);
+    if (np) {
+        if (normal_depth) cudaMemcpyAsync(normal_depth, B.nd + w.pt_base, size_t(np) * 16, cudaMemcpyDeviceToHost, g->stream);
+        if (local1) cudaMemcpyAsync(local1, B.l1 + w.pt_base, size_t(np) * 16, cudaMemcpyDeviceToHost, g->stream);
+        if (local2) cudaMemcpyAsync(local2, B.l2 + w.pt_base, size_t(np) * 16, cudaMemcpyDeviceToHost, g->stream);
+    }
+    cudaError_t e = cudaStreamSynchronize(g->stream);
+    return e == cudaSuccess ? 0 : wcuda(g, e, "read contacts");
+}
+
+int rp3dg_world_get_contacts(rp3dg_world* w, int32_t* body1, int32_t* body2, uint8_t* nb_points, uint32_t capacity,
+                             float* normal_depth, float* local1, float* local2, uint32_t capacity_points,
+                             uint32_t* nb_manifolds, uint32_t* nb_contact_points) {
+    return rp3dg_world_group_get_contacts(w, 0, body1, body2, nb_points, capacity, normal_depth, local1, local2,
+                                          capacity_points, nb_manifolds, nb_contact_points);
+}
+
+int rp3dg_world_get_stats(rp3dg_world* w, rp3dg_world_stats* s) {
+    if (!w || !s) return RP3DG_EINVAL;
+    *s = w->stats;
     return 0;
 }
 
@@ -1517,80 +1811,7 @@ int rp3dg_world_set_profiling(rp3dg_world* w, int enable) {
 
 int rp3dg_world_get_phase_times(rp3dg_world* w, double* ms, uint32_t n) {
     if (!w || !ms) return RP3DG_EINVAL;
-    for (uint32_t i = 0; i < n && i < 8; i++) ms[i] = w->phase_ms[i];
-    return 0;
-}
-
-int rp3dg_world_get_bodies(rp3dg_world* w, float* position, float* orientation, float* linear_velocity,
-                           float* angular_velocity, uint8_t* sleeping) {
-    if (!w) return RP3DG_EINVAL;
-    const uint32_t n = w->nb;
-    std::vector<float4> p(n), q(n), lv(n), av(n);
-    const int b = w->cur_b;
-    cudaMemcpyAsync(p.data(), w->bcol[b][BC_POS], size_t(n) * 16, cudaMemcpyDeviceToHost, w->stream);
-    cudaMemcpyAsync(q.data(), w->bcol[b][BC_ORI], size_t(n) * 16, cudaMemcpyDeviceToHost, w->stream);
-    cudaMemcpyAsync(lv.data(), w->bcol[b][BC_LV], size_t(n) * 16, cudaMemcpyDeviceToHost, w->stream);
-    cudaMemcpyAsync(av.data(), w->bcol[b][BC_AV], size_t(n) * 16, cudaMemcpyDeviceToHost, w->stream);
-    cudaError_t e = cudaStreamSynchronize(w->stream);
-    if (e != cudaSuccess) return wcuda(w, e, "read bodies");
-    for (uint32_t r = 0; r < n; r++) {
-        const size_t id = size_t(w->dev_body_at[r]);
-        if (position) { position[3 * id] = p[r].x; position[3 * id + 1] = p[r].y; position[3 * id + 2] = p[r].z; }
-        if (orientation) {
-            orientation[4 * id] = q[r].x; orientation[4 * id + 1] = q[r].y;
-            orientation[4 * id + 2] = q[r].z; orientation[4 * id + 3] = q[r].w;
-        }
-        if (linear_velocity) {
-            linear_velocity[3 * id] = lv[r].x; linear_velocity[3 * id + 1] = lv[r].y; linear_velocity[3 * id + 2] = lv[r].z;
-        }
-        if (angular_velocity) {
-            angular_velocity[3 * id] = av[r].x; angular_velocity[3 * id + 1] = av[r].y; angular_velocity[3 * id + 2] = av[r].z;
-        }
-        if (sleeping) sleeping[id] = w->bodies[id].sleeping ? 1 : 0;
-    }
-    return 0;
-}
-
-int rp3dg_world_get_pairs(rp3dg_world* w, uint64_t* ids, uint32_t capacity, uint32_t* n) {
-    if (!w || !n) return RP3DG_EINVAL;
-    uint32_t k = 0;
-    for (const auto& p : w->pairs) { if (ids && k < capacity) ids[k] = p.id; k++; }
-    for (const auto& p : w->disabled) { if (ids && k < capacity) ids[k] = p.id; k++; }
-    *n = k;
-    return 0;
-}
-
-int rp3dg_world_get_contacts(rp3dg_world* w, int32_t* body1, int32_t* body2, uint8_t* nb_points, uint32_t capacity,
-                             float* normal_depth, float* local1, float* local2, uint32_t capacity_points,
-                             uint32_t* nb_manifolds, uint32_t* nb_contact_points) {
-    if (!w) return RP3DG_EINVAL;
-    // the arrays of the last step are the "previous" buffer after the swap
-    const ContactBuf& B = w->cbuf[1 - w->cur_cb];
-    const std::vector<ContactPairH>& cps = w->prev_cpairs;
-    if (nb_manifolds) *nb_manifolds = B.nm;
-    if (nb_contact_points) *nb_contact_points = B.np;
-    std::vector<uint32_t> order(B.nm);
-    for (uint32_t i = 0; i < cps.size(); i++)
-        if (cps[i].in_island) order[cps[i].manifold] = i;
-    for (uint32_t m = 0; m < B.nm && m < capacity; m++) {
-        const ContactPairH& c = cps[order[m]];
-        if (body1) body1[m] = c.b1;
-        if (body2) body2[m] = c.b2;
-        if (nb_points) nb_points[m] = uint8_t(c.k);
-    }
-    const uint32_t np = std::min(B.np, capacity_points);
-    if (np) {
-        if (normal_depth) cudaMemcpyAsync(normal_depth, B.nd, size_t(np) * 16, cudaMemcpyDeviceToHost, w->stream);
-        if (local1) cudaMemcpyAsync(local1, B.l1, size_t(np) * 16, cudaMemcpyDeviceToHost, w->stream);
-        if (local2) cudaMemcpyAsync(local2, B.l2, size_t(np) * 16, cudaMemcpyDeviceToHost, w->stream);
-    }
-    cudaError_t e = cudaStreamSynchronize(w->stream);
-    return e == cudaSuccess ? 0 : wcuda(w, e, "read contacts");
-}
-
-int rp3dg_world_get_stats(rp3dg_world* w, rp3dg_world_stats* s) {
-    if (!w || !s) return RP3DG_EINVAL;
-    *s = w->stats;
+    for (uint32_t i = 0; i < n && i < 16; i++) ms[i] = w->phase_ms[i];
     return 0;
 }
 

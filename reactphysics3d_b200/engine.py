@@ -93,6 +93,11 @@ def load_library(path=LIB_PATH):
                                            C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.rp3dg_world_get_stats.argtypes = [P, P]
     L.rp3dg_world_set_profiling.argtypes = [P, C.c_int]
+    L.rp3dg_world_group_create.argtypes = [P, P, C.c_uint32, P, P, P, P, C.c_int, C.POINTER(P)]
+    L.rp3dg_world_group_get_bodies.argtypes = [P, C.c_uint32, P, P, P, P, P]
+    L.rp3dg_world_group_get_pairs.argtypes = [P, C.c_uint32, P, C.c_uint32, C.POINTER(C.c_uint32)]
+    L.rp3dg_world_group_get_contacts.argtypes = [P, C.c_uint32, P, P, P, C.c_uint32, P, P, P, C.c_uint32,
+                                                 C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.rp3dg_world_get_phase_times.argtypes = [P, P, C.c_uint32]
     _lib = L
     return L
@@ -492,17 +497,75 @@ class World:
         assert rc == 0, rc
         return b1, b2, k, nd, l1, l2
 
-    PHASES = ("broadphase", "middle", "narrow", "islands", "pack", "dynamics", "colliders", "sleeping")
+    PHASES = ("broadphase", "middle", "narrow", "islands", "pack", "dynamics", "colliders", "sleeping",
+              "m.pool", "m.resets", "m.rows", "m.tables", "m.items")
 
     def set_profiling(self, on=True):
         self.lib.rp3dg_world_set_profiling(self.h, int(on))
 
     def phase_times(self):
-        t = np.zeros(8, np.float64)
-        self.lib.rp3dg_world_get_phase_times(self.h, t.ctypes.data, 8)
-        return dict(zip(self.PHASES, t.tolist()))
+        t = np.zeros(16, np.float64)
+        self.lib.rp3dg_world_get_phase_times(self.h, t.ctypes.data, 16)
+        return {k: v for k, v in zip(self.PHASES, t.tolist()) if v or not k.startswith("m.")}
 
     def stats(self):
         s = np.zeros(1, A.WORLD_STATS_DTYPE)
         self.lib.rp3dg_world_get_stats(self.h, s.ctypes.data)
         return {k: int(s[k][0]) for k in A.WORLD_STATS_DTYPE.names if k != "reserved"}
+
+
+class WorldGroup(World):
+    """Many independent worlds stepped together (rp3dg_world_group_*).  All
+    scenes must share one shape table (scenes.merge_shapes builds it); world k
+    is then read with bodies(k) / pairs(k) / contacts(k)."""
+
+    def __init__(self, ctx, scenes_, shapes, threads=None):
+        self.ctx, self.lib = ctx, ctx.lib
+        ctx.set_shapes(shapes)
+        threads = threads or (os.cpu_count() or 1)
+        bodies = np.concatenate([s.bodies for s in scenes_])
+        colliders = np.concatenate([s.colliders for s in scenes_])
+        boff = np.concatenate([[0], np.cumsum([len(s.bodies) for s in scenes_])]).astype(np.uint32)
+        coff = np.concatenate([[0], np.cumsum([len(s.colliders) for s in scenes_])]).astype(np.uint32)
+        self.sizes = [len(s.bodies) for s in scenes_]
+        self.nb = int(boff[-1])
+        self._keep = (np.ascontiguousarray(scenes_[0].settings).copy(), bodies, colliders, boff, coff)
+        st = self._keep[0]
+        h = C.c_void_p()
+        rc = self.lib.rp3dg_world_group_create(ctx.h, st.ctypes.data, len(scenes_), boff.ctypes.data, bodies.ctypes.data,
+                                               coff.ctypes.data, colliders.ctypes.data, int(threads), C.byref(h))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(ctx.h).decode())
+        self.h = h
+
+    def bodies(self, world=None):
+        if world is None:
+            return super().bodies()
+        n = self.sizes[world]
+        p, q = np.zeros((n, 3), np.float32), np.zeros((n, 4), np.float32)
+        lv, av = np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32)
+        sl = np.zeros(n, np.uint8)
+        rc = self.lib.rp3dg_world_group_get_bodies(self.h, world, p.ctypes.data, q.ctypes.data, lv.ctypes.data,
+                                                   av.ctypes.data, sl.ctypes.data)
+        assert rc == 0, rc
+        return p, q, lv, av, sl
+
+    def pairs(self, world=0):
+        n = C.c_uint32()
+        self.lib.rp3dg_world_group_get_pairs(self.h, world, None, 0, C.byref(n))
+        out = np.zeros(n.value, np.uint64)
+        self.lib.rp3dg_world_group_get_pairs(self.h, world, out.ctypes.data, n.value, C.byref(n))
+        return out
+
+    def contacts(self, world=0):
+        nm, npt = C.c_uint32(), C.c_uint32()
+        self.lib.rp3dg_world_group_get_contacts(self.h, world, None, None, None, 0, None, None, None, 0,
+                                                C.byref(nm), C.byref(npt))
+        b1, b2 = np.zeros(nm.value, np.int32), np.zeros(nm.value, np.int32)
+        k = np.zeros(nm.value, np.uint8)
+        nd, l1, l2 = (np.zeros((npt.value, 4), np.float32) for _ in range(3))
+        rc = self.lib.rp3dg_world_group_get_contacts(self.h, world, b1.ctypes.data, b2.ctypes.data, k.ctypes.data,
+                                                     nm.value, nd.ctypes.data, l1.ctypes.data, l2.ctypes.data,
+                                                     npt.value, C.byref(nm), C.byref(npt))
+        assert rc == 0, rc
+        return b1, b2, k, nd, l1, l2

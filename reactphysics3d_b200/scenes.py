@@ -288,3 +288,53 @@ def mixed_world(nx=5, ny=4, nz=5, seed=2, spacing=1.6, variety=True):
         colliders["category"][1:] = (1 << (c % 3)).astype(np.uint16)
         colliders["mask"][1:] = np.where(c % 3 == 0, 0xFFFF & ~2, 0xFFFF).astype(np.uint16)
     return WorldScene(A.default_world_settings(), shapes, bodies, colliders, f"mixed {n}")
+
+
+def merge_shapes(scenes_):
+    """One shape table for several world scenes: the scenes' tables
+    concatenated, each scene's collider shape indices shifted (returns the
+    table and new scenes; the inputs are not modified)."""
+    tables, out, base = [], [], 0
+    for s in scenes_:
+        c = s.colliders.copy()
+        c["shape"] += base
+        out.append(WorldScene(s.settings, s.shapes, s.bodies, c, s.name))
+        tables.append(s.shapes)
+        base += len(s.shapes)
+    return np.concatenate(tables), out
+
+
+def many_worlds(n_worlds=4096, seed=7, min_bodies=20, max_bodies=200, spacing=1.2, merge=True):
+    """The many-worlds batch (boxes and spheres): n_worlds independent worlds
+    with U[min_bodies, max_bodies] dynamic bodies each (half boxes with
+    half-extents U[0.2, 1], half spheres with radius U[0.2, 1]), stacked on a
+    jittered square grid above a static ground box, random orientations.
+    Returns (shape table, list of WorldScene) with merge, else the scenes with
+    their own shape tables."""
+    rng = np.random.default_rng(seed)
+    scenes_ = []
+    for k in range(n_worlds):
+        n = int(rng.integers(min_bodies, max_bodies + 1))
+        shapes = np.zeros(n + 1, A.SHAPE_DTYPE)
+        shapes["mesh"] = -1
+        shapes[0]["kind"] = A.SHAPE_BOX
+        shapes["params"][0, :3] = (25.0, 0.5, 25.0)
+        kinds = rng.integers(0, 2, n)
+        shapes["kind"][1:] = np.where(kinds == 0, A.SHAPE_BOX, A.SHAPE_SPHERE)
+        shapes["params"][1:, :3] = rng.uniform(0.2, 1.0, size=(n, 3)).astype(np.float32)
+        side = int(np.ceil(np.sqrt(n / 4.0)))
+        idx = np.arange(n)
+        gx, gz, gy = idx % side, (idx // side) % side, idx // (side * side)
+        centre = np.stack([(gx - 0.5 * (side - 1)) * 2.2 * spacing, 1.5 + gy * 2.2 * spacing,
+                           (gz - 0.5 * (side - 1)) * 2.2 * spacing], axis=1) + rng.uniform(-0.1, 0.1, (n, 3))
+        bodies = A.body_descs(n + 1)
+        bodies[0]["type"] = A.BODY_STATIC
+        bodies["position"][1:] = centre.astype(np.float32)
+        bodies["orientation"][1:] = random_quaternions(rng, n)
+        colliders = A.collider_descs(n + 1)
+        colliders["body"] = np.arange(n + 1)
+        colliders["shape"] = np.arange(n + 1)
+        colliders["friction"] = np.float32(0.3)
+        colliders["bounciness"] = 0.0
+        scenes_.append(WorldScene(A.default_world_settings(), shapes, bodies, colliders, f"world {k} ({n} bodies)"))
+    return merge_shapes(scenes_) if merge else scenes_

@@ -86,3 +86,29 @@ def test_world_stats_and_launches(ctx):
     assert st["overlapping_pairs"] >= st["contact_pairs"]
     assert ctx.kernel_launches() - l0 >= 90 * 5
     w.close()
+
+
+@pytest.mark.skipif(not reflib.have_ref("f32"), reason="reference engine not built")
+def test_world_group_matches_each_reference_world(ctx):
+    """Worlds of different kinds and sizes stepped together in one group (and
+    on several host threads) each stay bit-identical to their own reference
+    world: pair arrays, manifolds and states at every step."""
+    parts = [scenes.mixed_world(4, 3, 4, seed=11), scenes.box_pile(3, 4, 3, seed=12),
+             scenes.mixed_world(3, 3, 3, seed=13, variety=False)]
+    many = scenes.many_worlds(3, seed=14, min_bodies=20, max_bodies=60, merge=False)
+    shapes, merged = scenes.merge_shapes(parts + many)
+    g = engine.WorldGroup(ctx, merged, shapes, threads=4)
+    refs = [reflib.RefScene(s) for s in parts + many]
+    for step in range(150):
+        g.update(float(worldio.DT))
+        for k, r in enumerate(refs):
+            r.update(float(worldio.DT))
+            if step % 10 == 9:
+                assert np.array_equal(g.pairs(k), r.pairs()), (step, k)
+                for a, b in zip(g.contacts(k), r.contacts()):
+                    assert np.array_equal(a, b), (step, k)
+                for a, b in zip(g.bodies(k), r.bodies()):
+                    assert np.array_equal(a, b), (step, k)
+    st = g.stats()
+    assert st["manifolds"] > 0
+    g.close()
