@@ -249,6 +249,11 @@ def run_ours(args):
         world_step = world_section(ctx, args, rank == 0 and world == 1 and not args.no_cpu)
         ctx.set_shapes(sc.shapes)
 
+    worlds = None
+    if not args.no_worlds:
+        worlds = many_worlds_section(ctx, args, rank == 0 and world == 1 and not args.no_cpu)
+        ctx.set_shapes(sc.shapes)
+
     learned = None
     if not args.no_learned:
         learned = learned_axis_section(ctx, sc, args, dev)
@@ -264,7 +269,7 @@ def run_ours(args):
                        "seed": args.seed, "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"independent pair sets per rank x{world}"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "manifolds": manifolds, "dynamics": dynamics, "broadphase": broadphase,
-            "world_step": world_step,
+            "world_step": world_step, "many_worlds": worlds,
             "learned_axis": learned,
             "gpu_launches": int(launches),
             "clocks": clocks, "batch_ms": {k: round(v, 4) for k, v in mean_batch.items()}}
@@ -457,6 +462,70 @@ def world_section(ctx, args, with_cpu):
             out["fp64_position_deviation_m"] = {"median": round(float(np.median(d)), 5), "max": round(float(d.max()), 4),
                                                 "note": "same for the reference float build (bit-identical); "
                                                         "a 1,000-body pile is chaotic"}
+    return out
+
+
+def many_worlds_section(ctx, args, with_cpu):
+    """Many independent worlds stepped together: 4,096 worlds of U[20, 200]
+    dynamic boxes and spheres (sizes U[0.2, 1]) falling onto a static ground
+    each (scenes.many_worlds; no ragdolls: joints are not built), dt 1/120,
+    through one rp3dg_world_update per step of the whole group (wall clock,
+    synchronous).  60 untimed steps, then 60 timed.  The reference engine
+    steps a sample of the same worlds over the same steps on every host core
+    (one PhysicsWorld per thread at a time, its own PhysicsCommon each), and
+    the sampled worlds' final states are compared bit for bit."""
+    from reactphysics3d_b200 import engine
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import reflib
+    n = args.n_worlds
+    dt = float(np.float32(1.0 / 120.0))
+    warm, timed = 60, 60
+    shapes, scs = scenes.many_worlds(n, seed=args.seed)
+    threads = os.cpu_count() or 1
+    g = engine.WorldGroup(ctx, scs, shapes, threads=threads)
+    g.update(dt, warm)
+    launches0 = ctx.kernel_launches()
+    t0 = time.perf_counter()
+    g.update(dt, timed)
+    sec = time.perf_counter() - t0
+    launches = (ctx.kernel_launches() - launches0) / timed
+    st = g.stats()
+    g.set_profiling(True)
+    g.update(dt, 5)
+    phases = {k: round(v / 5, 3) for k, v in g.phase_times().items() if not k.startswith("m.")}
+    out = {"workload": f"{n} independent worlds, U[20,200] boxes and spheres each (sizes U[0.2,1]) above a static "
+                       "ground box, random orientations, dt 1/120; steps 61-120 timed",
+           "worlds": n, "bodies": int(sum(len(s_.bodies) for s_ in scs)),
+           "world_steps_per_s": round(n * timed / sec, 1), "ms_per_step": round(1e3 * sec / timed, 3),
+           "kernels_per_step": round(launches, 1), "host_threads": threads, "phase_ms_per_step": phases,
+           "stats_at_step_120": st, "api": "rp3dg_world_update (world group)"}
+    if with_cpu and reflib.have_ref("f32"):
+        raw = scenes.many_worlds(n, seed=args.seed, merge=False)
+        sample = list(range(0, n, max(1, n // (8 * threads))))[: 8 * threads]
+        refs = [reflib.RefScene(raw[k]) for k in sample]
+        # warm-up steps on all threads, then the timed steps
+        def run(idx, steps):
+            for i in idx:
+                refs[i].update(dt, steps)
+        chunks = [list(range(t, len(refs), threads)) for t in range(threads)]
+        ths = [threading.Thread(target=run, args=(c, warm)) for c in chunks]
+        [t_.start() for t_ in ths]
+        [t_.join() for t_ in ths]
+        t0 = time.perf_counter()
+        ths = [threading.Thread(target=run, args=(c, timed)) for c in chunks]
+        [t_.start() for t_ in ths]
+        [t_.join() for t_ in ths]
+        rsec = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(len(refs) * timed / rsec, 1), "unit": "world-steps/s", "cores": threads,
+                               "kind": "reference",
+                               "sample": f"{len(refs)} of the worlds, steps 61-120, PhysicsWorld::update of the "
+                                         "reference float build, one world per thread at a time"}
+        same = True
+        for j, k in enumerate(sample[:16]):
+            refs[j].update(dt, 5)   # the group ran 5 more (profiled) steps
+            same &= all(np.array_equal(a, b) for a, b in zip(g.bodies(k), refs[j].bodies()))
+        out["bit_identical_sample"] = bool(same)
+    g.close()
     return out
 
 
@@ -729,6 +798,8 @@ def main():
     ap.add_argument("--no-broadphase", action="store_true")
     ap.add_argument("--dyn-worlds", type=int, default=4096)
     ap.add_argument("--no-world", action="store_true")
+    ap.add_argument("--no-worlds", action="store_true")
+    ap.add_argument("--n-worlds", type=int, default=4096)
     ap.add_argument("--world-steps", type=int, default=300)
     ap.add_argument("--learned-epochs", type=int, default=4)
     args = ap.parse_args()
