@@ -442,7 +442,7 @@ int rp3dg_broadphase_pairs_host(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, int 
  * pairs, contacts and constraints in the reference's own order and the results
  * are the reference float build's, bit for bit.  Worlds without joints, with
  * convex colliders (sphere, capsule, box, convex mesh), simulation colliders
- * only (no triggers), are supported.
+ * only (no triggers), with ball-and-socket and hinge joints, are supported.
  *
  * rp3dg_world_create mirrors this sequence of reference calls, body by body:
  *   b = world->createRigidBody(Transform(position, orientation));
@@ -469,6 +469,7 @@ typedef struct rp3dg_world_settings {      /* PhysicsWorld::WorldSettings (Physi
     float restitution_velocity_threshold;   /* 0.5 */
     float persistent_contact_distance_threshold; /* 0.03 */
     float cos_angle_similar_contact_manifold;    /* 0.95 */
+    int32_t position_iterations;            /* defaultPositionSolverNbIterations, 3 (joints) */
 } rp3dg_world_settings;
 
 typedef struct rp3dg_body_desc {
@@ -497,6 +498,27 @@ typedef struct rp3dg_collider_desc {
     uint16_t mask;                 /* collide-with mask bits (0xffff by default) */
 } rp3dg_collider_desc;
 
+/* A joint, as PhysicsWorld::createJoint(JointInfo) (PhysicsWorld.cpp) creates
+ * it from a BallAndSocketJointInfo / HingeJointInfo with world-space anchor
+ * (and hinge axis), followed for a ball-and-socket joint with a cone limit by
+ * joint->enableConeLimit(true) and joint->setConeLimitHalfAngle(angle).  Only
+ * the NON_LINEAR_GAUSS_SEIDEL position correction (the default) is built. */
+#define RP3DG_JOINT_BALL_AND_SOCKET 0
+#define RP3DG_JOINT_HINGE 1
+typedef struct rp3dg_joint_desc {
+    int32_t type;                  /* RP3DG_JOINT_* */
+    int32_t body1, body2;          /* body indices of the world */
+    float anchor[3];               /* anchor point, world space, at creation */
+    float axis[3];                 /* hinge: rotation axis, world space */
+    int32_t collision_enabled;     /* JointInfo::isCollisionEnabled (0: the two bodies never collide) */
+    int32_t cone_limit_enabled;    /* ball-and-socket */
+    float cone_half_angle;         /* ball-and-socket, radians (PI by default) */
+    int32_t limit_enabled;         /* hinge */
+    float min_angle, max_angle;    /* hinge limits, radians (-1, 1 when disabled, the reference's defaults) */
+    int32_t motor_enabled;         /* hinge */
+    float motor_speed, max_motor_torque;
+} rp3dg_joint_desc;
+
 typedef struct rp3dg_world rp3dg_world;
 
 typedef struct rp3dg_world_stats {
@@ -518,6 +540,11 @@ int rp3dg_world_create(rp3dg_ctx* ctx, const rp3dg_world_settings* settings, con
                        uint32_t nb_bodies, const rp3dg_collider_desc* colliders, uint32_t nb_colliders,
                        rp3dg_world** out);
 void rp3dg_world_destroy(rp3dg_world* world);
+/* createJoint for each of the n joints, in order; before the first update.
+ * The joints are solved in islands with their bodies, warm-started, with
+ * the reference's velocity solve and non-linear Gauss-Seidel position
+ * correction (SolveBallAndSocketJointSystem.cpp, SolveHingeJointSystem.cpp). */
+int rp3dg_world_add_joints(rp3dg_world* world, const rp3dg_joint_desc* joints, uint32_t n);
 /* PhysicsWorld::update(dt): one step (synchronous). */
 int rp3dg_world_update(rp3dg_world* world, float dt);
 /* Body state in creation order (host arrays of nb_bodies rows, any may be
@@ -556,6 +583,7 @@ int rp3dg_world_group_create(rp3dg_ctx* ctx, const rp3dg_world_settings* setting
                              const uint32_t* body_offsets, const rp3dg_body_desc* bodies,
                              const uint32_t* collider_offsets, const rp3dg_collider_desc* colliders,
                              int nb_threads, rp3dg_world** out);
+int rp3dg_world_group_add_joints(rp3dg_world* group, uint32_t world, const rp3dg_joint_desc* joints, uint32_t n);
 int rp3dg_world_group_get_bodies(rp3dg_world* group, uint32_t world, float* position, float* orientation,
                                  float* linear_velocity, float* angular_velocity, uint8_t* sleeping);
 int rp3dg_world_group_get_pairs(rp3dg_world* group, uint32_t world, uint64_t* pair_ids, uint32_t capacity,

@@ -503,6 +503,7 @@ int ref_scene_create(const rp3dg_world_settings* s, const rp3dg_shape* shapes, u
     ws.restitutionVelocityThreshold = s->restitution_velocity_threshold;
     ws.persistentContactDistanceThreshold = s->persistent_contact_distance_threshold;
     ws.cosAngleSimilarContactManifold = s->cos_angle_similar_contact_manifold;
+    ws.defaultPositionSolverNbIterations = uint16(s->position_iterations);
     W->world = W->common.createPhysicsWorld(ws);
     std::vector<CollisionShape*> cs(nshapes, nullptr);
     for (uint32_t i = 0; i < nshapes; i++) {
@@ -546,6 +547,37 @@ int ref_scene_create(const rp3dg_world_settings* s, const rp3dg_shape* shapes, u
     }
     worlds().push_back(std::move(W));
     return int(worlds().size()) - 1;
+}
+
+// createJoint for each description, in order (rp3dg_world_add_joints).
+int ref_scene_add_joints(int id, const rp3dg_joint_desc* jd, uint32_t n) {
+    World& W = *worlds().at(size_t(id));
+    for (uint32_t i = 0; i < n; i++) {
+        const rp3dg_joint_desc& d = jd[i];
+        RigidBody* b1 = W.bodies.at(size_t(d.body1));
+        RigidBody* b2 = W.bodies.at(size_t(d.body2));
+        const Vector3 anchor(d.anchor[0], d.anchor[1], d.anchor[2]);
+        if (d.type == RP3DG_JOINT_BALL_AND_SOCKET) {
+            BallAndSocketJointInfo info(b1, b2, anchor);
+            info.isCollisionEnabled = d.collision_enabled != 0;
+            auto* j = static_cast<BallAndSocketJoint*>(W.world->createJoint(info));
+            if (d.cone_limit_enabled) {
+                j->enableConeLimit(true);
+                j->setConeLimitHalfAngle(d.cone_half_angle);
+            }
+        } else {
+            HingeJointInfo info(b1, b2, anchor, Vector3(d.axis[0], d.axis[1], d.axis[2]));
+            info.isCollisionEnabled = d.collision_enabled != 0;
+            info.isLimitEnabled = d.limit_enabled != 0;
+            info.minAngleLimit = d.min_angle;
+            info.maxAngleLimit = d.max_angle;
+            info.isMotorEnabled = d.motor_enabled != 0;
+            info.motorSpeed = d.motor_speed;
+            info.maxMotorTorque = d.max_motor_torque;
+            W.world->createJoint(info);
+        }
+    }
+    return 0;
 }
 
 // Body state in creation order.

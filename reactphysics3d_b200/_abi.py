@@ -116,7 +116,7 @@ WORLD_SETTINGS_DTYPE = np.dtype([
     ("gravity", "<f4", (3,)), ("velocity_iterations", "<i4"), ("sleeping_enabled", "<i4"),
     ("sleep_linear_velocity", "<f4"), ("sleep_angular_velocity", "<f4"), ("time_before_sleep", "<f4"),
     ("restitution_velocity_threshold", "<f4"), ("persistent_contact_distance_threshold", "<f4"),
-    ("cos_angle_similar_contact_manifold", "<f4")])
+    ("cos_angle_similar_contact_manifold", "<f4"), ("position_iterations", "<i4")])
 BODY_DESC_DTYPE = np.dtype([
     ("type", "<i4"), ("position", "<f4", (3,)), ("orientation", "<f4", (4,)),
     ("linear_velocity", "<f4", (3,)), ("angular_velocity", "<f4", (3,)),
@@ -130,7 +130,14 @@ COLLIDER_DESC_DTYPE = np.dtype([
 WORLD_STATS_DTYPE = np.dtype([(k, "<u4") for k in (
     "overlapping_pairs", "disabled_pairs", "narrowphase_tests", "contact_pairs", "manifolds",
     "contact_points", "islands", "enabled_bodies", "moved_colliders", "reserved")])
-assert WORLD_SETTINGS_DTYPE.itemsize == 44 and BODY_DESC_DTYPE.itemsize == 96
+JOINT_BALL_AND_SOCKET, JOINT_HINGE = 0, 1
+JOINT_DESC_DTYPE = np.dtype([
+    ("type", "<i4"), ("body1", "<i4"), ("body2", "<i4"), ("anchor", "<f4", (3,)), ("axis", "<f4", (3,)),
+    ("collision_enabled", "<i4"), ("cone_limit_enabled", "<i4"), ("cone_half_angle", "<f4"),
+    ("limit_enabled", "<i4"), ("min_angle", "<f4"), ("max_angle", "<f4"),
+    ("motor_enabled", "<i4"), ("motor_speed", "<f4"), ("max_motor_torque", "<f4")])
+assert JOINT_DESC_DTYPE.itemsize == 72
+assert WORLD_SETTINGS_DTYPE.itemsize == 48 and BODY_DESC_DTYPE.itemsize == 96
 assert COLLIDER_DESC_DTYPE.itemsize == 52 and WORLD_STATS_DTYPE.itemsize == 40
 
 
@@ -147,7 +154,19 @@ def default_world_settings():
     s["restitution_velocity_threshold"] = f(0.5)
     s["persistent_contact_distance_threshold"] = f(0.03)
     s["cos_angle_similar_contact_manifold"] = f(0.95)
+    s["position_iterations"] = 3
     return s
+
+
+def joint_descs(n):
+    """JointInfo defaults: collision enabled, no cone limit (half angle PI),
+    hinge limits off (-1, 1), no motor."""
+    j = np.zeros(n, JOINT_DESC_DTYPE)
+    j["collision_enabled"] = 1
+    j["cone_half_angle"] = np.float32(3.141592653589)
+    j["min_angle"] = -1.0
+    j["max_angle"] = 1.0
+    return j
 
 
 def body_descs(n):

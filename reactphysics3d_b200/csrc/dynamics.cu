@@ -592,6 +592,7 @@ __global__ void __launch_bounds__(128) dyn_islands_small(const DynArgs a) {
         atomicOr(a.error, 4u);
         return;
     }
+    if (a.i_jcount && a.i_jcount[is]) return;  // kernel 3d
     if (cnt == 0) return;
     if (cnt > SMALL_ISLAND) {
         // big islands fill the list from the front, the others from the back
@@ -813,6 +814,75 @@ __global__ void __launch_bounds__(LARGE_WARPS * 32, 2) dyn_islands_large(const D
     }
 }
 
+
+}  // namespace
+}  // namespace rp3dg
+#include "joints.cuh"
+namespace rp3dg {
+namespace {
+
+// ---- kernel 3d: islands with joints --------------------------------------
+//
+// One thread per island, in the reference's order: the contact warm start
+// (ContactSolverSystem::init), the joints' warm start
+// (ConstraintSolverSystem::initialize: ball-and-socket, then hinge), then per
+// velocity iteration the joints (solveVelocityConstraints) before the
+// contacts (ContactSolverSystem::solve), and storeImpulses.
+__global__ void __launch_bounds__(128) dyn_joints_init(const DynArgs a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < a.nj) joint_init(a, a.j_list[i]);
+}
+
+__global__ void __launch_bounds__(64) dyn_islands_joint(const DynArgs a) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.nji) return;
+    const uint32_t is = a.ji_island[k];
+    const uint32_t m0 = a.i_start[is], cnt = a.i_count[is];
+    const uint32_t j0 = a.i_jstart[is], jn = a.i_jcount[is];
+    if (m0 > a.nm || cnt > a.nm - m0 || j0 > a.nj || jn > a.nj - j0) {
+        atomicOr(a.error, 4u);
+        return;
+    }
+    for (uint32_t mi = m0; mi < m0 + cnt; mi++) {
+        const int4 id = man_ids(a, mi);
+        warm_manifold(a, mi, vel_global(a, id.x, id.y), id.z, id.w);
+    }
+    for (uint32_t j = j0; j < j0 + jn; j++) joint_warm(a, a.j_list[j]);
+    const float beta = a.split ? BETA_SPLIT_IMPULSE : BETA;
+    for (int it = 0; it < a.iterations; it++) {
+        for (uint32_t j = j0; j < j0 + jn; j++) joint_solve(a, a.j_list[j]);
+        for (uint32_t mi = m0; mi < m0 + cnt; mi++) {
+            const int4 id = man_ids(a, mi);
+            solve_manifold(a, mi, beta, vel_global(a, id.x, id.y), id.z, id.w);
+        }
+    }
+    for (uint32_t mi = m0; mi < m0 + cnt; mi++) store_manifold(a, mi);
+}
+
+// ---- kernel 4b: position correction of the joints (solvePositionCorrection,
+// PhysicsWorld.cpp:348-360) and updateBodiesState (DynamicsSystem.cpp:74-110)
+// of the islands with joints.
+__global__ void __launch_bounds__(64) dyn_joints_position(const DynArgs a) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.nji) return;
+    const uint32_t is = a.ji_island[k];
+    const uint32_t j0 = a.i_jstart[is], jn = a.i_jcount[is];
+    if (j0 > a.nj || jn > a.nj - j0) return;
+    for (int it = 0; it < a.position_iterations; it++)
+        for (uint32_t j = j0; j < j0 + jn; j++) joint_position(a, a.j_list[j]);
+    for (uint32_t r = a.ji_bstart[k]; r < a.ji_bstart[k] + a.ji_bcount[k]; r++) {
+        const int32_t i = a.ji_rows[r];
+        const v3 cp = L3(a.xc[i]);
+        const float4 c4 = a.qc[i];
+        const quat co = Q(c4.x, c4.y, c4.z, c4.w);
+        a.com_world[i] = F4(cp);
+        const float len = sqrtf(co.x * co.x + co.y * co.y + co.z * co.z + co.w * co.w);
+        const quat u = Q(co.x / len, co.y / len, co.z / len, co.w / len);
+        a.orientation[i] = make_float4(u.x, u.y, u.z, u.w);
+        const v3 rr = qrot(u, L3(a.com_local[i]));
+        a.position[i] = F4(V(cp.x - rr.x, cp.y - rr.y, cp.z - rr.z));
+    }
+}
 
 // ---- kernel 3c: islands of more than GIANT_ISLAND manifolds --------------
 //
@@ -1127,6 +1197,11 @@ __global__ void __launch_bounds__(128) dyn_bodies_post(const DynArgs a) {
     const quat dq = qmul(Q(na.x, na.y, na.z, 0.0f), q);
     const quat sq = Q(dt * (0.5f * dq.x), dt * (0.5f * dq.y), dt * (0.5f * dq.z), dt * (0.5f * dq.w));
     const quat co = Q(q.x + sq.x, q.y + sq.y, q.z + sq.z, q.w + sq.w);
+    if (a.xc) {
+        // mConstrainedPositions / mConstrainedOrientations, read by the joints' position correction
+        a.xc[i] = F4(cp);
+        a.qc[i] = make_float4(co.x, co.y, co.z, co.w);
+    }
     // updateBodiesState
     a.lin_vel[i] = F4(cv);
     a.ang_vel[i] = F4(cw);
@@ -1160,6 +1235,7 @@ uint32_t blocks(uint32_t n) { return (n + 127) / 128; }
 cudaError_t launch_dynamics(const DynArgs& a, cudaStream_t s, uint64_t* launches) {
     if (a.nb) { dyn_bodies_pre<<<blocks(a.nb), 128, 0, s>>>(a); (*launches)++; }
     if (a.nm) { dyn_manifold_init<<<blocks(a.nm), 128, 0, s>>>(a); (*launches)++; }
+    if (a.nj) { dyn_joints_init<<<blocks(a.nj), 128, 0, s>>>(a); (*launches)++; }
     if (a.ni) {
         cudaMemsetAsync(a.counters, 0, 5 * sizeof(uint32_t), s);
         dyn_islands_small<<<blocks(a.ni), 128, 0, s>>>(a);
@@ -1173,9 +1249,11 @@ cudaError_t launch_dynamics(const DynArgs& a, cudaStream_t s, uint64_t* launches
             dyn_islands_giant<<<a.giant_ctas, GIANT_THREADS, a.giant_smem, s>>>(a);
             (*launches)++;
         }
+        if (a.nji) { dyn_islands_joint<<<(a.nji + 63) / 64, 64, 0, s>>>(a); (*launches)++; }
     }
     const uint32_t nbp = a.b_enabled ? a.nb : a.nb_enabled, ncp = a.c_enabled ? a.nc : a.nc_enabled;
     if (nbp) { dyn_bodies_post<<<blocks(nbp), 128, 0, s>>>(a); (*launches)++; }
+    if (a.nji) { dyn_joints_position<<<(a.nji + 63) / 64, 64, 0, s>>>(a); (*launches)++; }
     if (ncp) { dyn_colliders<<<blocks(ncp), 128, 0, s>>>(a); (*launches)++; }
     return cudaGetLastError();
 }

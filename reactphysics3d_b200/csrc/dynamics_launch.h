@@ -36,6 +36,30 @@ struct __align__(16) DynPointRec {
     float4 mut;   // penetration impulse, split impulse, resting (1 / 0)
 };
 
+// Per-joint record (joints.cuh): constant rows set on creation (type and
+// flags, local anchors, local hinge axes, inverse initial orientation
+// difference, limits / motor parameters), accumulated impulses and limit
+// state carried from step to step, and the rows initBeforeSolve computes.
+enum JointRow {
+    JR_HDR = 0,     // x type (0 ball-and-socket, 1 hinge), y flags (int bits)
+    JR_LA1, JR_LA2, // local anchor points
+    JR_AX1, JR_AX2, // hinge: local axes
+    JR_QINV,        // hinge: inverse initial orientation difference (quaternion)
+    JR_PARAM,       // x cone half angle, y lower limit, z upper limit, w motor speed
+    JR_PARAM2,      // x max motor torque
+    JR_IMP,         // ball-and-socket impulse / hinge translation impulse
+    JR_IMP2,        // hinge: rotation impulse x, y, lower-limit impulse, upper-limit impulse
+    JR_STATE,       // ball-and-socket: cone impulse, cone violated; hinge: lower / upper violated, motor impulse
+    JR_R1, JR_R2,
+    JR_I1, JR_I2 = JR_I1 + 3, JR_K = JR_I2 + 3, JR_ACB = JR_K + 3,
+    JR_A1, JR_B2A1, JR_C2A1, JR_KROT, JR_MISC,
+    JR_ROWS
+};
+enum JointFlags { JF_CONE = 1, JF_LIMIT = 2, JF_MOTOR = 4 };
+struct __align__(16) JointRec {
+    float4 q[JR_ROWS];
+};
+
 // Kernel 3b stages an island's schedule and its movable bodies' velocities
 // in the shared memory of the warp that solves it, when they fit.
 constexpr uint32_t STAGE_BODIES = 256;
@@ -91,8 +115,40 @@ struct DynArgs {
     uint32_t* large_list;  // ni: queued islands
     uint32_t* giant_list;  // ni: islands for kernel 3c
     uint32_t large_ctas;   // grid of kernel 3b (persistent)
+    // joints (nj = 0: none).  j_list holds this step's enabled joints island
+    // by island, each island's ball-and-socket joints then hinge joints in
+    // component order: record index, body 1 row, body 2 row, bit 0 / bit 1 =
+    // body 1 / body 2 dynamic.  Islands with joints (i_jcount > 0) are solved
+    // by kernel 3d; after the position integration kernel 4b runs the
+    // position correction of their joints and updates their bodies' state.
+    uint32_t nj;
+    const int4* j_list;
+    JointRec* j_rec;
+    const uint32_t* i_jstart;
+    const uint32_t* i_jcount;
+    uint32_t nji;               // islands with joints
+    const uint32_t* ji_island;  // their island indices
+    const uint32_t* ji_bstart;  // and their enabled bodies' rows: ji_rows[ji_bstart[k] .. + ji_bcount[k])
+    const uint32_t* ji_bcount;
+    const int32_t* ji_rows;
+    float4* xc;                 // constrained positions (centres of mass), all rows, kept between steps
+    float4* qc;                 // constrained orientations, all rows
+    int32_t position_iterations;
     uint32_t giant_ctas;   // grid of kernel 3c (persistent, one warp per CTA)
     uint32_t giant_smem;   // dynamic shared memory of a kernel-3c CTA (0: kernel 3c off)
+};
+
+// The joint part of a dynamics stage (see DynArgs).
+struct DynJoints {
+    uint32_t nj;
+    const int4* j_list;
+    JointRec* j_rec;
+    const uint32_t *i_jstart, *i_jcount;
+    uint32_t nji;
+    const uint32_t *ji_island, *ji_bstart, *ji_bcount;
+    const int32_t* ji_rows;
+    float4 *xc, *qc;
+    int32_t position_iterations;
 };
 
 // Launches the kernels in order on stream s; *launches counts them.

@@ -309,7 +309,8 @@ int upload_arena(rp3dg_ctx* ctx) {
 namespace rp3dg {
 int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
                         const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
-                        const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled);
+                        const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled,
+                        const DynJoints* joints = nullptr);
 int broadphase_update_flags(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, const uint8_t* enabled);
 }  // namespace rp3dg
 
@@ -997,7 +998,8 @@ namespace rp3dg {
 // flags (several worlds in one batch) instead of a leading range.
 int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
                         const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
-                        const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled) {
+                        const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled,
+                        const DynJoints* joints) {
     int rc = check_dynamics(ctx, pr, b, c, m, p, is);
     if (rc) return rc;
     const void* f16[] = {b->position, b->orientation, b->com_world, b->com_local, b->linear_velocity,
@@ -1029,6 +1031,14 @@ int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const r
     rp3dg::DynArgs a = {};
     a.b_enabled = b_enabled;
     a.c_enabled = c_enabled;
+    if (joints && joints->nj) {
+        a.nj = joints->nj; a.j_list = joints->j_list; a.j_rec = joints->j_rec;
+        a.i_jstart = joints->i_jstart; a.i_jcount = joints->i_jcount;
+        a.nji = joints->nji; a.ji_island = joints->ji_island; a.ji_bstart = joints->ji_bstart;
+        a.ji_bcount = joints->ji_bcount; a.ji_rows = joints->ji_rows;
+        a.xc = joints->xc; a.qc = joints->qc;
+        a.position_iterations = joints->position_iterations;
+    }
     a.dt = pr->dt; a.gx = pr->gravity[0]; a.gy = pr->gravity[1]; a.gz = pr->gravity[2];
     a.gravity_enabled = pr->gravity_enabled; a.iterations = pr->velocity_iterations; a.split = pr->split_impulse ? 1 : 0;
     a.restitution_threshold = pr->restitution_velocity_threshold;

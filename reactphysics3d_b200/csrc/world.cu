@@ -49,7 +49,10 @@
 #include <unordered_map>
 #include <vector>
 
+#include <set>
+
 #include "../../include/rp3dg.h"
+#include "dynamics_launch.h"
 #include "rp3dg_math.cuh"
 #include "world_order.h"
 
@@ -60,7 +63,8 @@ int get_shapes_host(rp3dg_ctx* ctx, std::vector<rp3dg_shape>* out);
 void set_error(rp3dg_ctx* ctx, const std::string& msg);
 int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
                         const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
-                        const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled);
+                        const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled,
+                        const DynJoints* joints);
 int broadphase_update_flags(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, const uint8_t* enabled);
 }  // namespace rp3dg
 
@@ -339,8 +343,15 @@ struct BodyH {
     bool in_island = false;
     bool has_sim_collider = false;
     float sleep_time = 0.0f;
+    int island = -1;               // island of this step (non-static bodies)
     std::vector<int> colliders;
     std::vector<uint32_t> contact_pairs;
+    std::vector<int> joints;       // RigidBodyComponents::mJoints (creation order)
+};
+struct JointH {
+    int type = 0;
+    int b1 = -1, b2 = -1;
+    bool in_island = false;
 };
 struct ColliderH {
     int body = -1;
@@ -369,6 +380,12 @@ struct IslandH {
     uint32_t manifold_start = 0, manifold_count = 0;  // world-local manifold range
     std::vector<int> bodies;
 };
+
+inline float __int_as_float_host(int v) {
+    float f;
+    std::memcpy(&f, &v, 4);
+    return f;
+}
 
 // pairNumbers (mathematics_functions.h:428-433)
 inline uint64_t pair_number(uint32_t a, uint32_t b) {
@@ -406,7 +423,8 @@ int host_grow(T** p, size_t* cap, size_t need) {
 }
 
 // Device columns of the rigid-body components (row = world's first row + component slot).
-enum BodyCol { BC_POS, BC_ORI, BC_COMW, BC_COML, BC_LV, BC_AV, BC_F, BC_T, BC_IIL, BC_MASS, BC_LLOCK, BC_ALOCK, BC_NCOL };
+enum BodyCol { BC_POS, BC_ORI, BC_COMW, BC_COML, BC_LV, BC_AV, BC_F, BC_T, BC_IIL, BC_MASS, BC_LLOCK, BC_ALOCK,
+               BC_XC, BC_QC, BC_NCOL };  // XC / QC: constrained position / orientation (joints)
 enum ColCol { CC_LPOS, CC_LORI, CC_WPOS, CC_WORI, CC_MAT, CC_FMIN, CC_FMAX, CC_NCOL };
 
 struct ContactBuf {
@@ -463,6 +481,18 @@ struct WorldH {
     std::vector<int> dev_body_at, dev_col_at;  // component order the device rows have
     uint32_t dev_nb_en = ~0u, dev_nc_en = ~0u; // enabled counts the device flags hold
     std::vector<uint8_t> gravity;              // by body id
+    // joints: JointComponents and the per-type components (order), the pairs
+    // of bodies that must not collide, the first record of this world
+    std::vector<JointH> joints;
+    rp3dg::order::Comps jcomp, bscomp, hcomp;
+    std::set<std::pair<int, int>> nocollide;
+    uint32_t jbase = 0;
+    struct Pose { float p[3], q[4]; };
+    std::vector<Pose> init_pose;               // transforms at creation (joint anchors)
+    std::vector<int4> jlist;                   // this step's joints, island by island (record, rows, flags)
+    std::vector<uint32_t> isl_jstart, isl_jcount;
+    uint32_t jl_base = 0;
+    bool stepped = false;
     // this step
     std::vector<int4> items[NB_ALGOS];
     std::vector<uint32_t> item_pair[NB_ALGOS];
@@ -516,12 +546,22 @@ struct rp3dg_world {
     uint32_t *d_istart = nullptr, *d_icount = nullptr;
     ContactBuf cbuf[2];
     int cur_cb = 0;
+    // joints: records by global joint index, per-step lists
+    rp3dg::JointRec* j_rec = nullptr;
+    uint32_t nj_total = 0;
+    size_t cap_jrec = 0;
+    int4* d_jlist = nullptr;
+    uint32_t *d_ijstart = nullptr, *d_ijcount = nullptr, *d_jiisl = nullptr, *d_jibstart = nullptr, *d_jibcount = nullptr;
+    int32_t* d_jirows = nullptr;
+    size_t cap_jl = 0, cap_ji = 0, cap_jbs = 0, cap_jbc = 0, cap_jr = 0;
     // pinned host staging
     size_t cap_hitems = 0, cap_hout = 0, cap_hm = 0, cap_hi = 0, cap_hstep = 0, cap_hreset = 0;
     int4* h_items = nullptr;
     uint8_t* h_out = nullptr;  // colliding flag, kept count
     int4 *h_mids = nullptr, *h_msrc = nullptr, *h_mprev = nullptr;
-    uint32_t *h_istart = nullptr, *h_icount = nullptr;
+    uint32_t *h_istart = nullptr, *h_icount = nullptr, *h_ijstart = nullptr, *h_ijcount = nullptr;
+    int4* h_jlist = nullptr;
+    size_t cap_hjl = 0;
     uint8_t* h_step = nullptr;  // moved flags, fat AABBs, velocities after the step
     int32_t* h_reset = nullptr;
     // phase profiling (rp3dg_world_set_profiling): cumulative ms per phase
@@ -722,6 +762,9 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
             const int c1 = w.bp_to_collider[size_t(s)], c2 = w.bp_to_collider[size_t(leaf)];
             const ColliderH &C1 = w.colliders[size_t(c1)], &C2 = w.colliders[size_t(c2)];
             if (C1.body == C2.body) continue;
+            if (!w.nocollide.empty() &&
+                w.nocollide.count(std::make_pair(std::min(C1.body, C2.body), std::max(C1.body, C2.body))))
+                continue;
             const uint64_t id = pair_number(uint32_t(std::max(s, leaf)), uint32_t(std::min(s, leaf)));
             PairH* p = find_pair(w, id);
             if (!p) {
@@ -787,7 +830,11 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
     }
     w.island_order.clear();
     w.islands.clear();
-    for (auto& B : w.bodies) B.in_island = false;
+    for (auto& B : w.bodies) {
+        B.in_island = false;
+        B.island = -1;
+    }
+    for (auto& J : w.joints) J.in_island = false;
     uint32_t total_manifolds = 0;
     std::vector<int> stack, statics;
     for (uint32_t s = 0; s < w.bcomp.n_enabled; s++) {
@@ -810,6 +857,7 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
                 statics.push_back(b);
                 continue;
             }
+            w.bodies[size_t(b)].island = int(isl_index);
             for (uint32_t cpi : w.bodies[size_t(b)].contact_pairs) {
                 ContactPairH& cp = w.cpairs[cpi];
                 if (cp.in_island) continue;
@@ -824,6 +872,16 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
                     w.bodies[size_t(other)].in_island = true;
                 }
             }
+            // the body's joints (PhysicsWorld.cpp:822-844)
+            for (int j : w.bodies[size_t(b)].joints) {
+                JointH& J = w.joints[size_t(j)];
+                if (J.in_island) continue;
+                J.in_island = true;
+                const int other = J.b1 == b ? J.b2 : J.b1;
+                if (w.bodies[size_t(other)].in_island) continue;
+                stack.push_back(other);
+                w.bodies[size_t(other)].in_island = true;
+            }
         }
         for (int sb : statics) w.bodies[size_t(sb)].in_island = false;
         statics.clear();
@@ -835,6 +893,45 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
     w.nm = uint32_t(w.island_order.size());
     w.np = 0;
     for (uint32_t m = 0; m < w.nm; m++) w.np += w.cpairs[w.island_order[m]].k;
+    // PhysicsWorld::enableDisableJoints (:363-393): a joint is enabled while
+    // one of its bodies is
+    if (!w.joints.empty()) {
+        const std::vector<int> order = w.jcomp.at;
+        for (int j : order) {
+            const JointH& J = w.joints[size_t(j)];
+            const bool dis = !w.bcomp.enabled(J.b1) && !w.bcomp.enabled(J.b2);
+            if (w.jcomp.enabled(j) == !dis) continue;
+            w.jcomp.set_disabled(j, dis);
+            (J.type == RP3DG_JOINT_BALL_AND_SOCKET ? w.bscomp : w.hcomp).set_disabled(j, dis);
+        }
+    }
+    // the enabled joints island by island: ball-and-socket then hinge, each in
+    // component order (the order the constraint solver visits them)
+    w.jlist.clear();
+    w.isl_jstart.assign(w.islands.size(), 0);
+    w.isl_jcount.assign(w.islands.size(), 0);
+    if (!w.joints.empty()) {
+        std::vector<std::vector<int>> per(w.islands.size());
+        for (rp3dg::order::Comps* cmp : {&w.bscomp, &w.hcomp})
+            for (uint32_t s = 0; s < cmp->n_enabled; s++) {
+                const int j = cmp->at[s];
+                const JointH& J = w.joints[size_t(j)];
+                const int isl = w.bodies[size_t(J.b1)].type != RP3DG_BODY_STATIC ? w.bodies[size_t(J.b1)].island
+                                                                                  : w.bodies[size_t(J.b2)].island;
+                if (isl >= 0) per[size_t(isl)].push_back(j);
+            }
+        for (size_t i = 0; i < per.size(); i++) {
+            w.isl_jstart[i] = uint32_t(w.jlist.size());
+            w.isl_jcount[i] = uint32_t(per[i].size());
+            for (int j : per[i]) {
+                const JointH& J = w.joints[size_t(j)];
+                const int flags = (w.bodies[size_t(J.b1)].type == RP3DG_BODY_DYNAMIC ? 1 : 0) |
+                                  (w.bodies[size_t(J.b2)].type == RP3DG_BODY_DYNAMIC ? 2 : 0);
+                // rows filled in fill_manifolds (after the row sync)
+                w.jlist.push_back(make_int4(int(w.jbase) + j, J.b1, J.b2, flags));
+            }
+        }
+    }
 }
 
 // createContacts' packing (CollisionDetectionSystem.cpp:906-975) and the
@@ -864,6 +961,14 @@ void fill_manifolds(Group* g, WorldH& w) {
     for (uint32_t i = 0; i < w.islands.size(); i++) {
         g->h_istart[w.isl_base + i] = w.man_base + w.islands[i].manifold_start;
         g->h_icount[w.isl_base + i] = w.islands[i].manifold_count;
+        g->h_ijstart[w.isl_base + i] = w.jl_base + w.isl_jstart[i];
+        g->h_ijcount[w.isl_base + i] = w.isl_jcount[i];
+    }
+    for (size_t k = 0; k < w.jlist.size(); k++) {
+        int4 e = w.jlist[k];
+        e.y = int(w.b0) + w.bcomp.slot[size_t(e.y)];
+        e.z = int(w.b0) + w.bcomp.slot[size_t(e.z)];
+        g->h_jlist[w.jl_base + k] = e;
     }
     // computeMapPreviousContactPairs for the next step
     w.prev_map.clear();
@@ -1108,7 +1213,10 @@ void destroy_group(Group* g) {
     cudaFree(g->d_mids); cudaFree(g->d_msrc); cudaFree(g->d_mprev); cudaFree(g->d_istart); cudaFree(g->d_icount);
     cudaFreeHost(g->h_items); cudaFreeHost(g->h_out); cudaFreeHost(g->h_mids); cudaFreeHost(g->h_msrc);
     cudaFreeHost(g->h_mprev); cudaFreeHost(g->h_istart); cudaFreeHost(g->h_icount); cudaFreeHost(g->h_step);
+    cudaFreeHost(g->h_ijstart); cudaFreeHost(g->h_ijcount); cudaFreeHost(g->h_jlist);
     cudaFreeHost(g->h_reset);
+    cudaFree(g->j_rec); cudaFree(g->d_jlist); cudaFree(g->d_ijstart); cudaFree(g->d_ijcount); cudaFree(g->d_jiisl);
+    cudaFree(g->d_jibstart); cudaFree(g->d_jibcount); cudaFree(g->d_jirows);
     cudaFreeHost(g->t_grav); cudaFreeHost(g->t_ben); cudaFreeHost(g->t_cen); cudaFreeHost(g->t_cbody);
     cudaFreeHost(g->t_cshape); cudaFreeHost(g->t_cat); cudaFreeHost(g->t_mask); cudaFreeHost(g->t_bperm);
     cudaFreeHost(g->t_cperm);
@@ -1318,11 +1426,26 @@ int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds
         world_setup<<<blocks(n), 128, 0, g->stream>>>(NB, g->bcol[0][BC_POS], g->bcol[0][BC_ORI], g->bcol[0][BC_COML],
                                                       g->bcol[0][BC_COMW], d_dyn, NC, g->c_body, g->ccol[0][CC_LPOS],
                                                       g->ccol[0][CC_LORI], g->ccol[0][CC_WPOS], g->ccol[0][CC_WORI]);
+    // constrained position / orientation: the centre of mass and orientation
+    // (setType(STATIC) sets them from the transform, RigidBody.cpp:80-82)
+    if (NB) {
+        cudaMemcpyAsync(g->bcol[0][BC_XC], g->bcol[0][BC_COMW], size_t(NB) * 16, cudaMemcpyDeviceToDevice, g->stream);
+        cudaMemcpyAsync(g->bcol[0][BC_QC], g->bcol[0][BC_ORI], size_t(NB) * 16, cudaMemcpyDeviceToDevice, g->stream);
+    }
     e = cudaStreamSynchronize(g->stream);
     cudaFree(d_dyn);
     if (e != cudaSuccess) {
         destroy_group(g);
         return cfail(ctx, RP3DG_ECUDA, "world set-up kernel");
+    }
+    for (uint32_t k = 0; k < nworlds; k++) {
+        WorldH& w = g->worlds[k];
+        const rp3dg_body_desc* d = bd + boff[k];
+        w.init_pose.resize(w.nb);
+        for (uint32_t b = 0; b < w.nb; b++) {
+            w.init_pose[b].p[0] = d[b].position[0]; w.init_pose[b].p[1] = d[b].position[1]; w.init_pose[b].p[2] = d[b].position[2];
+            for (int c = 0; c < 4; c++) w.init_pose[b].q[c] = d[b].orientation[c];
+        }
     }
     // initial fat AABBs of every collider (addCollider -> addObject)
     if (NC) {
@@ -1521,20 +1644,60 @@ int update_group(Group* g, float dt) {
     if (g->cap_hi < NI || !g->h_istart) {
         const size_t cap = std::max<size_t>(size_t(NI) * 2, 64);
         cudaFreeHost(g->h_istart); cudaFreeHost(g->h_icount); cudaFree(g->d_istart); cudaFree(g->d_icount);
-        g->h_istart = g->h_icount = nullptr;
-        g->d_istart = g->d_icount = nullptr;
+        cudaFreeHost(g->h_ijstart); cudaFreeHost(g->h_ijcount); cudaFree(g->d_ijstart); cudaFree(g->d_ijcount);
+        g->h_istart = g->h_icount = g->h_ijstart = g->h_ijcount = nullptr;
+        g->d_istart = g->d_icount = g->d_ijstart = g->d_ijcount = nullptr;
         g->cap_hi = 0;
         if (cudaMallocHost(&g->h_istart, cap * 4) || cudaMallocHost(&g->h_icount, cap * 4) ||
-            cudaMalloc(&g->d_istart, cap * 4) || cudaMalloc(&g->d_icount, cap * 4))
+            cudaMalloc(&g->d_istart, cap * 4) || cudaMalloc(&g->d_icount, cap * 4) ||
+            cudaMallocHost(&g->h_ijstart, cap * 4) || cudaMallocHost(&g->h_ijcount, cap * 4) ||
+            cudaMalloc(&g->d_ijstart, cap * 4) || cudaMalloc(&g->d_ijcount, cap * 4))
             return wfail(g, RP3DG_ENOMEM, "allocation of island arrays");
         g->cap_hi = cap;
     }
+    // joints of every world, back to back
+    uint32_t NJ = 0;
+    for (WorldH& w : g->worlds) {
+        w.jl_base = NJ;
+        NJ += uint32_t(w.jlist.size());
+    }
+    if (NJ && (host_grow(&g->h_jlist, &g->cap_hjl, NJ) || dev_grow(&g->d_jlist, &g->cap_jl, NJ)))
+        return wfail(g, RP3DG_ENOMEM, "allocation of joint lists");
     mark(3);
     // rows may have moved (bodies woken by the islands): sync before packing ids
     rc = sync_rows(g);
     if (rc) return rc;
     for_worlds(g, [&](int k) { fill_manifolds(g, g->worlds[size_t(k)]); });
     const int bc = g->cur_b, ccur = g->cur_c;
+    // islands with joints and their enabled bodies' rows (for the position correction)
+    std::vector<uint32_t> ji_island, ji_bstart, ji_bcount;
+    std::vector<int32_t> ji_rows;
+    if (NJ) {
+        for (WorldH& w : g->worlds)
+            for (uint32_t i = 0; i < w.islands.size(); i++) {
+                if (!w.isl_jcount[i]) continue;
+                ji_island.push_back(w.isl_base + i);
+                ji_bstart.push_back(uint32_t(ji_rows.size()));
+                for (int b : w.islands[i].bodies)
+                    if (w.bodies[size_t(b)].type != RP3DG_BODY_STATIC) ji_rows.push_back(int32_t(w.b0) + w.bcomp.slot[size_t(b)]);
+                ji_bcount.push_back(uint32_t(ji_rows.size()) - ji_bstart.back());
+            }
+        if (dev_grow(&g->d_jiisl, &g->cap_ji, ji_island.size() + 1) ||
+            dev_grow(&g->d_jibstart, &g->cap_jbs, ji_island.size() + 1) ||
+            dev_grow(&g->d_jibcount, &g->cap_jbc, ji_island.size() + 1) ||
+            dev_grow(&g->d_jirows, &g->cap_jr, ji_rows.size() + 1))
+            return wfail(g, RP3DG_ENOMEM, "allocation of joint islands");
+        cudaMemcpyAsync(g->d_jlist, g->h_jlist, size_t(NJ) * 16, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->d_ijstart, g->h_ijstart, size_t(NI) * 4, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->d_ijcount, g->h_ijcount, size_t(NI) * 4, cudaMemcpyHostToDevice, st);
+        if (!ji_island.empty()) {
+            cudaMemcpyAsync(g->d_jiisl, ji_island.data(), ji_island.size() * 4, cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(g->d_jibstart, ji_bstart.data(), ji_bstart.size() * 4, cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(g->d_jibcount, ji_bcount.data(), ji_bcount.size() * 4, cudaMemcpyHostToDevice, st);
+        }
+        if (!ji_rows.empty())
+            cudaMemcpyAsync(g->d_jirows, ji_rows.data(), ji_rows.size() * 4, cudaMemcpyHostToDevice, st);
+    }
     ContactBuf& CB = g->cbuf[g->cur_cb];
     ContactBuf& PB = g->cbuf[1 - g->cur_cb];
     if (CB.ensure(std::max<uint32_t>(NM, 1), std::max<uint32_t>(NP, 1))) return wfail(g, RP3DG_ENOMEM, "cudaMalloc(contacts)");
@@ -1605,8 +1768,26 @@ int update_group(Group* g, float dt) {
         I.n = NI;
         I.manifold_start = g->d_istart;
         I.manifold_count = g->d_icount;
-        rc = rp3dg::dynamics_step_flags(ctx, &pr, &B, &C, &Mf, &P, &I, g->b_en, g->c_en);
+        rp3dg::DynJoints J{};
+        if (NJ) {
+            J.nj = NJ;
+            J.j_list = g->d_jlist;
+            J.j_rec = g->j_rec;
+            J.i_jstart = g->d_ijstart;
+            J.i_jcount = g->d_ijcount;
+            J.nji = uint32_t(ji_island.size());
+            J.ji_island = g->d_jiisl;
+            J.ji_bstart = g->d_jibstart;
+            J.ji_bcount = g->d_jibcount;
+            J.ji_rows = g->d_jirows;
+            J.xc = g->bcol[bc][BC_XC];
+            J.qc = g->bcol[bc][BC_QC];
+            J.position_iterations = g->set.position_iterations;
+        }
+        rc = rp3dg::dynamics_step_flags(ctx, &pr, &B, &C, &Mf, &P, &I, g->b_en, g->c_en, NJ ? &J : nullptr);
         if (rc) return rc;
+        // the pageable joint-island vectors are read by the copies above
+        if (NJ) cudaStreamSynchronize(st);
     }
     mark(5);
     // ---- updateColliders: world AABBs, fat-AABB test, reinsertion flags
@@ -1666,12 +1847,133 @@ int update_group(Group* g, float dt) {
     if (e != cudaSuccess) return wcuda(g, e, "end of step");
     g->cur_cb = 1 - g->cur_cb;
     for (WorldH& w : g->worlds) {
+        w.stepped = true;
         g->stats.overlapping_pairs += uint32_t(w.pairs.size());
         g->stats.disabled_pairs += w.stats.disabled_pairs;
         g->stats.enabled_bodies += w.stats.enabled_bodies;
         g->stats.moved_colliders += w.stats.moved_colliders;
     }
     mark(7);
+    return 0;
+}
+
+// Host quaternion / vector arithmetic with the reference's expression trees
+// (Quaternion.h:349-378, Vector3.h:219-227), for the joints' local frames.
+struct HQ { float x, y, z, w; };
+HQ hq_mul(HQ a, HQ b) {
+    return {a.w * b.x + b.w * a.x + a.y * b.z - a.z * b.y, a.w * b.y + b.w * a.y + a.z * b.x - a.x * b.z,
+            a.w * b.z + b.w * a.z + a.x * b.y - a.y * b.x, a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z};
+}
+void hq_rot(HQ q, const float* p, float* out) {
+    const float prodX = q.w * p[0] + q.y * p[2] - q.z * p[1];
+    const float prodY = q.w * p[1] + q.z * p[0] - q.x * p[2];
+    const float prodZ = q.w * p[2] + q.x * p[1] - q.y * p[0];
+    const float prodW = -q.x * p[0] - q.y * p[1] - q.z * p[2];
+    out[0] = q.w * prodX - prodY * q.z + prodZ * q.y - prodW * q.x;
+    out[1] = q.w * prodY - prodZ * q.x + prodX * q.z - prodW * q.y;
+    out[2] = q.w * prodZ - prodX * q.y + prodY * q.x - prodW * q.z;
+}
+void hv_normalize(float* v) {
+    const float l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    if (l < 1.1920928955078125e-07f) return;
+    v[0] /= l; v[1] /= l; v[2] /= l;
+}
+// transform.getInverse() * point (Transform.h:162-195)
+void inv_apply(const float* p, HQ q, const float* point, float* out) {
+    const HQ iq{-q.x, -q.y, -q.z, q.w};
+    const float np[3] = {-p[0], -p[1], -p[2]};
+    float t[3], r[3];
+    hq_rot(iq, np, t);
+    hq_rot(iq, point, r);
+    out[0] = r[0] + t[0]; out[1] = r[1] + t[1]; out[2] = r[2] + t[2];
+}
+
+int add_joints(Group* g, uint32_t world, const rp3dg_joint_desc* jd, uint32_t n) {
+    if (world >= g->worlds.size() || (n && !jd)) return wfail(g, RP3DG_EINVAL, "bad joint arguments");
+    WorldH& w = g->worlds[world];
+    if (w.stepped) return wfail(g, RP3DG_EINVAL, "joints must be added before the first update");
+    if (!w.joints.empty()) return wfail(g, RP3DG_EINVAL, "joints of a world are added in one call");
+    if (world + 1 < g->worlds.size())
+        for (uint32_t k = world + 1; k < g->worlds.size(); k++)
+            if (!g->worlds[k].joints.empty()) return wfail(g, RP3DG_EINVAL, "add the joints of the worlds in order");
+    for (uint32_t i = 0; i < n; i++) {
+        const rp3dg_joint_desc& d = jd[i];
+        if (d.type != RP3DG_JOINT_BALL_AND_SOCKET && d.type != RP3DG_JOINT_HINGE)
+            return wfail(g, RP3DG_EINVAL, "bad joint type");
+        if (d.body1 < 0 || d.body2 < 0 || uint32_t(d.body1) >= w.nb || uint32_t(d.body2) >= w.nb || d.body1 == d.body2)
+            return wfail(g, RP3DG_EINVAL, "bad joint bodies");
+    }
+    std::vector<rp3dg::JointRec> recs(n);
+    w.jbase = g->nj_total;
+    w.joints.resize(n);
+    w.jcomp.reserve_ids(n);
+    w.bscomp.reserve_ids(n);
+    w.hcomp.reserve_ids(n);
+    for (uint32_t j = 0; j < n; j++) {
+        const rp3dg_joint_desc& d = jd[j];
+        JointH& J = w.joints[j];
+        J.type = d.type;
+        J.b1 = d.body1;
+        J.b2 = d.body2;
+        const bool dis = !w.bcomp.enabled(J.b1) && !w.bcomp.enabled(J.b2);
+        (d.type == RP3DG_JOINT_BALL_AND_SOCKET ? w.bscomp : w.hcomp).add(int(j), dis);
+        w.jcomp.add(int(j), dis);
+        if (!d.collision_enabled) w.nocollide.insert(std::make_pair(std::min(J.b1, J.b2), std::max(J.b1, J.b2)));
+        w.bodies[size_t(J.b1)].joints.push_back(int(j));
+        w.bodies[size_t(J.b2)].joints.push_back(int(j));
+        const auto& P1 = w.init_pose[size_t(J.b1)];
+        const auto& P2 = w.init_pose[size_t(J.b2)];
+        const HQ q1{P1.q[0], P1.q[1], P1.q[2], P1.q[3]}, q2{P2.q[0], P2.q[1], P2.q[2], P2.q[3]};
+        float la1[3], la2[3];
+        inv_apply(P1.p, q1, d.anchor, la1);
+        inv_apply(P2.p, q2, d.anchor, la2);
+        float4* q = recs[j].q;
+        for (int r = 0; r < rp3dg::JR_ROWS; r++) q[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+        int flags = 0;
+        if (d.type == RP3DG_JOINT_BALL_AND_SOCKET && d.cone_limit_enabled) flags |= rp3dg::JF_CONE;
+        if (d.type == RP3DG_JOINT_HINGE && d.limit_enabled) flags |= rp3dg::JF_LIMIT;
+        if (d.type == RP3DG_JOINT_HINGE && d.motor_enabled) flags |= rp3dg::JF_MOTOR;
+        q[rp3dg::JR_HDR] = make_float4(__int_as_float_host(d.type), __int_as_float_host(flags), 0.f, 0.f);
+        q[rp3dg::JR_LA1] = make_float4(la1[0], la1[1], la1[2], 0.f);
+        q[rp3dg::JR_LA2] = make_float4(la2[0], la2[1], la2[2], 0.f);
+        if (d.type == RP3DG_JOINT_HINGE) {
+            float ax1[3], ax2[3];
+            hq_rot(HQ{-q1.x, -q1.y, -q1.z, q1.w}, d.axis, ax1);
+            hq_rot(HQ{-q2.x, -q2.y, -q2.z, q2.w}, d.axis, ax2);
+            hv_normalize(ax1);
+            hv_normalize(ax2);
+            HQ qd = hq_mul(q2, HQ{-q1.x, -q1.y, -q1.z, q1.w});
+            const float l = std::sqrt(qd.x * qd.x + qd.y * qd.y + qd.z * qd.z + qd.w * qd.w);
+            qd = HQ{qd.x / l, qd.y / l, qd.z / l, qd.w / l};
+            q[rp3dg::JR_AX1] = make_float4(ax1[0], ax1[1], ax1[2], 0.f);
+            q[rp3dg::JR_AX2] = make_float4(ax2[0], ax2[1], ax2[2], 0.f);
+            q[rp3dg::JR_QINV] = make_float4(-qd.x, -qd.y, -qd.z, qd.w);
+            q[rp3dg::JR_PARAM] = make_float4(0.f, d.min_angle, d.max_angle, d.motor_speed);
+            q[rp3dg::JR_PARAM2] = make_float4(d.max_motor_torque, 0.f, 0.f, 0.f);
+        } else {
+            q[rp3dg::JR_PARAM] = make_float4(d.cone_limit_enabled ? d.cone_half_angle : float(3.141592653589), 0.f, 0.f, 0.f);
+        }
+    }
+    // records: the group's array grows (existing records copied)
+    const size_t need = size_t(g->nj_total) + n;
+    if (need > g->cap_jrec) {
+        rp3dg::JointRec* nr = nullptr;
+        const size_t cap = std::max<size_t>(need, g->cap_jrec * 2);
+        if (cudaMalloc(&nr, cap * sizeof(rp3dg::JointRec)) != cudaSuccess)
+            return wfail(g, RP3DG_ENOMEM, "cudaMalloc(joint records)");
+        if (g->nj_total)
+            cudaMemcpyAsync(nr, g->j_rec, size_t(g->nj_total) * sizeof(rp3dg::JointRec), cudaMemcpyDeviceToDevice, g->stream);
+        cudaStreamSynchronize(g->stream);
+        cudaFree(g->j_rec);
+        g->j_rec = nr;
+        g->cap_jrec = cap;
+    }
+    if (n)
+        cudaMemcpyAsync(g->j_rec + g->nj_total, recs.data(), size_t(n) * sizeof(rp3dg::JointRec), cudaMemcpyHostToDevice,
+                        g->stream);
+    cudaError_t e = cudaStreamSynchronize(g->stream);
+    if (e != cudaSuccess) return wcuda(g, e, "joint records");
+    g->nj_total += n;
     return 0;
 }
 
@@ -1731,6 +2033,16 @@ int rp3dg_world_group_create(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint
 }
 
 void rp3dg_world_destroy(rp3dg_world* w) { destroy_group(w); }
+
+int rp3dg_world_add_joints(rp3dg_world* w, const rp3dg_joint_desc* joints, uint32_t n) {
+    if (!w) return RP3DG_EINVAL;
+    return add_joints(w, 0, joints, n);
+}
+
+int rp3dg_world_group_add_joints(rp3dg_world* w, uint32_t world, const rp3dg_joint_desc* joints, uint32_t n) {
+    if (!w) return RP3DG_EINVAL;
+    return add_joints(w, world, joints, n);
+}
 
 int rp3dg_world_update(rp3dg_world* w, float dt) { return update_group(w, dt); }
 

@@ -93,6 +93,8 @@ def load_library(path=LIB_PATH):
                                            C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.rp3dg_world_get_stats.argtypes = [P, P]
     L.rp3dg_world_set_profiling.argtypes = [P, C.c_int]
+    L.rp3dg_world_add_joints.argtypes = [P, P, C.c_uint32]
+    L.rp3dg_world_group_add_joints.argtypes = [P, C.c_uint32, P, C.c_uint32]
     L.rp3dg_world_group_create.argtypes = [P, P, C.c_uint32, P, P, P, P, C.c_int, C.POINTER(P)]
     L.rp3dg_world_group_get_bodies.argtypes = [P, C.c_uint32, P, P, P, P, P]
     L.rp3dg_world_group_get_pairs.argtypes = [P, C.c_uint32, P, C.c_uint32, C.POINTER(C.c_uint32)]
@@ -446,6 +448,8 @@ class World:
         if rc != 0:
             raise Rp3dgError(rc, self.lib.rp3dg_last_error(ctx.h).decode())
         self.h = h
+        if getattr(scene, "joints", None) is not None and len(scene.joints):
+            self.add_joints(scene.joints)
 
     def close(self):
         if self.h:
@@ -457,6 +461,16 @@ class World:
             self.close()
         except Exception:
             pass
+
+    def add_joints(self, joints, world=None):
+        """createJoint for each row of `joints` (A.JOINT_DESC_DTYPE), before the first update."""
+        j = np.ascontiguousarray(joints)
+        if world is None:
+            rc = self.lib.rp3dg_world_add_joints(self.h, j.ctypes.data, len(j))
+        else:
+            rc = self.lib.rp3dg_world_group_add_joints(self.h, int(world), j.ctypes.data, len(j))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
 
     def update(self, dt=1.0 / 60.0, n=1):
         for _ in range(n):
@@ -537,6 +551,9 @@ class WorldGroup(World):
         if rc != 0:
             raise Rp3dgError(rc, self.lib.rp3dg_last_error(ctx.h).decode())
         self.h = h
+        for k, sc in enumerate(scenes_):
+            if getattr(sc, "joints", None) is not None and len(sc.joints):
+                self.add_joints(sc.joints, world=k)
 
     def bodies(self, world=None):
         if world is None:

@@ -184,11 +184,12 @@ def narrowphase_scene(total_pairs=TOTAL_PAIRS, seed=1234, names=BATCH_NAMES, pos
 # ---- worlds ----------------------------------------------------------------
 
 class WorldScene:
-    """A world description: settings, shape table, bodies and colliders
-    (numpy structured arrays with the layouts of include/rp3dg.h)."""
+    """A world description: settings, shape table, bodies, colliders and
+    joints (numpy structured arrays with the layouts of include/rp3dg.h)."""
 
-    def __init__(self, settings, shapes, bodies, colliders, name=""):
+    def __init__(self, settings, shapes, bodies, colliders, name="", joints=None):
         self.settings, self.shapes, self.bodies, self.colliders, self.name = settings, shapes, bodies, colliders, name
+        self.joints = joints
 
 
 def box_pile(nx=10, ny=10, nz=10, seed=1, spacing=2.0, base=2.0, jitter=0.1):
@@ -298,17 +299,21 @@ def merge_shapes(scenes_):
     for s in scenes_:
         c = s.colliders.copy()
         c["shape"] += base
-        out.append(WorldScene(s.settings, s.shapes, s.bodies, c, s.name))
+        out.append(WorldScene(s.settings, s.shapes, s.bodies, c, s.name, getattr(s, "joints", None)))
         tables.append(s.shapes)
         base += len(s.shapes)
     return np.concatenate(tables), out
 
 
-def many_worlds(n_worlds=4096, seed=7, min_bodies=20, max_bodies=200, spacing=1.2, merge=True):
-    """The many-worlds batch (boxes and spheres): n_worlds independent worlds
-    with U[min_bodies, max_bodies] dynamic bodies each (half boxes with
-    half-extents U[0.2, 1], half spheres with radius U[0.2, 1]), stacked on a
-    jittered square grid above a static ground box, random orientations.
+def many_worlds(n_worlds=4096, seed=7, min_bodies=20, max_bodies=200, spacing=1.2, merge=True, ragdolls=(1, 4),
+                limits=True):
+    """The many-worlds batch: n_worlds independent worlds with
+    U[min_bodies, max_bodies] dynamic bodies each (half boxes with half-extents
+    U[0.2, 1], half spheres with radius U[0.2, 1]) stacked on a jittered
+    square grid above a static ground box, random orientations, and
+    U[ragdolls] ragdolls (ragdoll_world's 15-capsule skeleton, 10
+    ball-and-socket + 4 hinge joints, 60-degree cones and +-60-degree hinge
+    limits with `limits`) above the stack.
     Returns (shape table, list of WorldScene) with merge, else the scenes with
     their own shape tables."""
     rng = np.random.default_rng(seed)
@@ -327,14 +332,139 @@ def many_worlds(n_worlds=4096, seed=7, min_bodies=20, max_bodies=200, spacing=1.
         gx, gz, gy = idx % side, (idx // side) % side, idx // (side * side)
         centre = np.stack([(gx - 0.5 * (side - 1)) * 2.2 * spacing, 1.5 + gy * 2.2 * spacing,
                            (gz - 0.5 * (side - 1)) * 2.2 * spacing], axis=1) + rng.uniform(-0.1, 0.1, (n, 3))
-        bodies = A.body_descs(n + 1)
+        nr = int(rng.integers(ragdolls[0], ragdolls[1] + 1)) if ragdolls else 0
+        nparts = len(RAGDOLL_PARTS)
+        shapes = np.concatenate([shapes, np.zeros(nr * nparts, A.SHAPE_DTYPE)])
+        shapes["mesh"][n + 1:] = -1
+        bodies = A.body_descs(n + 1 + nr * nparts)
         bodies[0]["type"] = A.BODY_STATIC
-        bodies["position"][1:] = centre.astype(np.float32)
-        bodies["orientation"][1:] = random_quaternions(rng, n)
-        colliders = A.collider_descs(n + 1)
-        colliders["body"] = np.arange(n + 1)
-        colliders["shape"] = np.arange(n + 1)
+        bodies["position"][1:n + 1] = centre.astype(np.float32)
+        bodies["orientation"][1:n + 1] = random_quaternions(rng, n)
+        top = float(centre[:, 1].max()) + 2.5
+        joints = []
+        b = n + 1
+        for r in range(nr):
+            base = np.array([(r - 0.5 * (nr - 1)) * 3.0, top, 0.0]) + rng.uniform(-0.2, 0.2, 3)
+            params, centres, q, js = _ragdoll(rng, b, base, limits)
+            shapes["kind"][b:b + nparts] = A.SHAPE_CAPSULE
+            shapes["params"][b:b + nparts, :2] = params
+            bodies["position"][b:b + nparts] = centres.astype(np.float32)
+            bodies["orientation"][b:b + nparts] = np.asarray(q, dtype=np.float32)
+            joints += js
+            b += nparts
+        nt = len(bodies)
+        colliders = A.collider_descs(nt)
+        colliders["body"] = np.arange(nt)
+        colliders["shape"] = np.arange(nt)
         colliders["friction"] = np.float32(0.3)
         colliders["bounciness"] = 0.0
-        scenes_.append(WorldScene(A.default_world_settings(), shapes, bodies, colliders, f"world {k} ({n} bodies)"))
+        scenes_.append(WorldScene(A.default_world_settings(), shapes, bodies, colliders,
+                                  f"world {k} ({n} bodies, {nr} ragdolls)",
+                                  np.array(joints, dtype=A.JOINT_DESC_DTYPE) if joints else None))
     return merge_shapes(scenes_) if merge else scenes_
+
+
+# 15-part skeleton: (name, parent index, offset of the part's centre from the
+# parent's centre in the ragdoll frame, joint: "ball" or "hinge")
+RAGDOLL_PARTS = (
+    ("pelvis", -1, (0.0, 0.0, 0.0), None),
+    ("spine", 0, (0.0, 0.35, 0.0), "ball"),
+    ("chest", 1, (0.0, 0.35, 0.0), "ball"),
+    ("neck", 2, (0.0, 0.3, 0.0), "ball"),
+    ("head", 3, (0.0, 0.25, 0.0), "ball"),
+    ("l_upper_arm", 2, (0.35, 0.1, 0.0), "ball"),
+    ("l_forearm", 5, (0.4, 0.0, 0.0), "hinge"),
+    ("l_hand", 6, (0.3, 0.0, 0.0), "ball"),
+    ("r_upper_arm", 2, (-0.35, 0.1, 0.0), "ball"),
+    ("r_forearm", 8, (-0.4, 0.0, 0.0), "hinge"),
+    ("r_hand", 9, (-0.3, 0.0, 0.0), "ball"),
+    ("l_thigh", 0, (0.15, -0.45, 0.0), "ball"),
+    ("l_shin", 11, (0.0, -0.5, 0.0), "hinge"),
+    ("r_thigh", 0, (-0.15, -0.45, 0.0), "ball"),
+    ("r_shin", 13, (0.0, -0.5, 0.0), "hinge"),
+)
+
+
+def _rotate(q, v):
+    """Rotate vectors v (n, 3) by the unit quaternion q (x, y, z, w), float64."""
+    x, y, z, w = q
+    u = np.array([x, y, z])
+    v = np.asarray(v, dtype=np.float64)
+    return v + 2.0 * np.cross(u, np.cross(u, v) + w * v)
+
+
+def _ragdoll(rng, first, base, limits):
+    """One ragdoll whose first body index is `first`, centred at `base` with a
+    random orientation: (capsule params (15, 2), centres (15, 3), orientation,
+    joint records)."""
+    nparts = len(RAGDOLL_PARTS)
+    q = random_quaternions(rng, 1)[0].astype(np.float64)
+    centres = np.zeros((nparts, 3))
+    for i, (_, parent, off, _) in enumerate(RAGDOLL_PARTS):
+        centres[i] = (centres[parent] if parent >= 0 else 0.0) + np.array(off)
+    world_c = _rotate(q, centres) + base
+    params = np.stack([rng.uniform(0.08, 0.15, nparts), rng.uniform(0.1, 0.3, nparts)], axis=1)
+    joints = []
+    for i, (_, parent, _, kind) in enumerate(RAGDOLL_PARTS):
+        if parent < 0:
+            continue
+        j = A.joint_descs(1)[0]
+        j["type"] = A.JOINT_HINGE if kind == "hinge" else A.JOINT_BALL_AND_SOCKET
+        j["body1"], j["body2"] = first + parent, first + i
+        j["anchor"] = (0.5 * (world_c[parent] + world_c[i])).astype(np.float32)
+        j["axis"] = _rotate(q, np.array([[0.0, 0.0, 1.0]]))[0].astype(np.float32)
+        j["collision_enabled"] = 0
+        if limits:
+            if kind == "hinge":
+                j["limit_enabled"] = 1
+                j["min_angle"] = np.float32(-np.pi / 3)
+                j["max_angle"] = np.float32(np.pi / 3)
+            else:
+                j["cone_limit_enabled"] = 1
+                j["cone_half_angle"] = np.float32(np.pi / 3)
+        joints.append(j)
+    return params, world_c, q, joints
+
+
+def ragdoll_world(n_ragdolls=2, seed=21, limits=True, boxes=0):
+    """Ragdolls (15 capsules each: radius U[0.08, 0.15], half-height
+    U[0.1, 0.3]; 10 ball-and-socket and 4 hinge joints in a tree, the bodies
+    a joint connects not colliding with each other, as in the reference
+    testbed's ragdoll scene) dropped with random orientations onto a static
+    ground box, optionally with a few boxes.  With limits, the ball-and-socket
+    joints have a 60-degree cone and the hinges (elbows, knees) +-60 degrees
+    (tolerance-level parity: the reference computes these angles with
+    acos / atan2)."""
+    rng = np.random.default_rng(seed)
+    nparts = len(RAGDOLL_PARTS)
+    n = 1 + n_ragdolls * nparts + boxes
+    shapes = np.zeros(n, A.SHAPE_DTYPE)
+    shapes["mesh"] = -1
+    shapes[0]["kind"] = A.SHAPE_BOX
+    shapes["params"][0, :3] = (25.0, 0.5, 25.0)
+    bodies = A.body_descs(n)
+    bodies[0]["type"] = A.BODY_STATIC
+    joints = []
+    b = 1
+    for r in range(n_ragdolls):
+        base = np.array([(r % 4) * 3.0 - 4.5, 2.5 + 1.0 * (r // 4), (r // 4) * 2.0 - 2.0]) + rng.uniform(-0.2, 0.2, 3)
+        params, centres, q, js = _ragdoll(rng, b, base, limits)
+        shapes["kind"][b:b + nparts] = A.SHAPE_CAPSULE
+        shapes["params"][b:b + nparts, :2] = params
+        bodies["position"][b:b + nparts] = centres.astype(np.float32)
+        bodies["orientation"][b:b + nparts] = np.asarray(q, dtype=np.float32)
+        joints += js
+        b += nparts
+    for k in range(boxes):
+        shapes[b]["kind"] = A.SHAPE_BOX
+        shapes[b]["params"][:3] = rng.uniform(0.2, 0.5, 3)
+        bodies[b]["position"] = (rng.uniform(-4, 4), 0.8 + 0.6 * k, rng.uniform(-3, 3))
+        bodies[b]["orientation"] = random_quaternions(rng, 1)[0]
+        b += 1
+    colliders = A.collider_descs(n)
+    colliders["body"] = np.arange(n)
+    colliders["shape"] = np.arange(n)
+    colliders["friction"] = np.float32(0.3)
+    colliders["bounciness"] = 0.0
+    return WorldScene(A.default_world_settings(), shapes, bodies, colliders,
+                      f"ragdolls {n_ragdolls}", np.array(joints, dtype=A.JOINT_DESC_DTYPE))

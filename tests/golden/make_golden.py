@@ -39,7 +39,9 @@ Writes:
   world.npz        whole world steps of two seeded scenes (tests/worldio.py:
                    a 125-box pile for 240 steps, a mixed world of boxes,
                    spheres and capsules with materials, dampings, locks,
-                   kinematic / gravity-free bodies and filters for 200 steps)
+                   kinematic / gravity-free bodies and filters for 200 steps,
+                   four ragdolls of ball-and-socket and hinge joints without
+                   limits with six boxes for 240 steps)
                    stepped by the reference's PhysicsWorld::update: per step
                    the overlapping-pair ids in array order and the solver's
                    manifolds (counts + 64-bit digests), and the body states

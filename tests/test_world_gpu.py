@@ -94,8 +94,9 @@ def test_world_group_matches_each_reference_world(ctx):
     on several host threads) each stay bit-identical to their own reference
     world: pair arrays, manifolds and states at every step."""
     parts = [scenes.mixed_world(4, 3, 4, seed=11), scenes.box_pile(3, 4, 3, seed=12),
+             scenes.ragdoll_world(2, seed=15, limits=False, boxes=3),
              scenes.mixed_world(3, 3, 3, seed=13, variety=False)]
-    many = scenes.many_worlds(3, seed=14, min_bodies=20, max_bodies=60, merge=False)
+    many = scenes.many_worlds(3, seed=14, min_bodies=20, max_bodies=60, merge=False, limits=False)
     shapes, merged = scenes.merge_shapes(parts + many)
     g = engine.WorldGroup(ctx, merged, shapes, threads=4)
     refs = [reflib.RefScene(s) for s in parts + many]
@@ -112,3 +113,30 @@ def test_world_group_matches_each_reference_world(ctx):
     st = g.stats()
     assert st["manifolds"] > 0
     g.close()
+
+
+@pytest.mark.skipif(not (reflib.have_ref("f32") and reflib.have_ref("f64")), reason="reference engine not built")
+def test_ragdolls_with_limits_stay_within_tolerance(ctx):
+    """Cone and hinge limits go through acos / atan2, whose last bit differs
+    between CUDA and the host C library, so ragdolls with limits are compared
+    within a tolerance, the one the reference itself shows between its float
+    and double builds: over the first 30 steps (the limits engage, the bodies
+    hit the ground and each other) the largest position difference from the
+    float reference stays within the largest difference between the
+    reference's float and double builds; after 240 steps every body rests
+    above the ground."""
+    sc = scenes.ragdoll_world(4, seed=29, limits=True, boxes=4)
+    w, r, r64 = engine.World(ctx, sc), reflib.RefScene(sc), reflib.RefScene(sc, "f64")
+    ours, spread = 0.0, 0.0
+    for s in range(240):
+        w.update(float(worldio.DT))
+        r.update(float(worldio.DT))
+        if s < 30:
+            r64.update(float(worldio.DT))
+            pr = r.bodies()[0].astype(np.float64)
+            ours = max(ours, float(np.abs(w.bodies()[0] - pr).max()))
+            spread = max(spread, float(np.abs(r64.bodies()[0] - pr).max()))
+    assert ours <= max(spread, 1e-5), (ours, spread)
+    pw, pr = w.bodies()[0], r.bodies()[0]
+    assert (pw[1:, 1] > 0.45).all() and (pr[1:, 1] > 0.45).all()
+    w.close()

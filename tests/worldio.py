@@ -12,6 +12,7 @@ from reactphysics3d_b200 import scenes
 WORLD_CASES = {
     "pile125": (scenes.box_pile, dict(nx=5, ny=5, nz=5, seed=3), 240, 60),
     "mixed100": (scenes.mixed_world, dict(nx=5, ny=4, nz=5, seed=5), 200, 50),
+    "ragdolls4": (scenes.ragdoll_world, dict(n_ragdolls=4, seed=23, limits=False, boxes=6), 240, 60),
 }
 DT = np.float32(1.0 / 60.0)
 
