@@ -55,7 +55,8 @@ enum rp3dg_shape_kind {
     RP3DG_SHAPE_SPHERE = 0,
     RP3DG_SHAPE_CAPSULE = 1,
     RP3DG_SHAPE_BOX = 2,
-    RP3DG_SHAPE_CONVEX_MESH = 3
+    RP3DG_SHAPE_CONVEX_MESH = 3,
+    RP3DG_SHAPE_HEIGHTFIELD = 4   /* CONCAVE_SHAPE / HEIGHTFIELD */
 };
 
 /* Narrow-phase algorithms, same numbering as the reference's
@@ -79,7 +80,10 @@ typedef struct rp3dg_float4 { float x, y, z, w; } rp3dg_float4;
  *                  CapsuleShape.cpp:41, and getHeight() = 2 * halfHeight)
  *   box:          params = (halfExtent.x, .y, .z, 0)
  *   convex mesh:  params unused; mesh = index returned by
- *                 rp3dg_create_convex_mesh_shape (mesh + scale instance) */
+ *                 rp3dg_create_convex_mesh_shape (mesh + scale instance)
+ *   height field: params unused; mesh = index returned by
+ *                 rp3dg_create_heightfield (a concave shape: it collides
+ *                 only inside a world, through the middle phase) */
 typedef struct rp3dg_shape {
     float params[4];
     int32_t kind;
@@ -176,6 +180,19 @@ int rp3dg_get_convex_mesh_tables(rp3dg_ctx* ctx, int32_t instance_id,
                                  uint32_t* nb_vertices, uint32_t* nb_faces, uint32_t* nb_half_edges,
                                  uint32_t* half_edges, float* face_normals, uint32_t* face_edge,
                                  float* centroid, uint32_t capacity_half_edges, uint32_t capacity_faces);
+
+/* Height field + height-field shape: replaces
+ * PhysicsCommon::createHeightField(nbGridColumns, nbGridRows, data,
+ * HeightDataType::HEIGHT_FLOAT_TYPE, messages) (HeightField::init,
+ * HeightField.cpp:47-90) followed by PhysicsCommon::createHeightFieldShape(
+ * heightField, scaling) (HeightFieldShape.cpp:40-43).  heights holds
+ * nb_columns * nb_rows floats, heights[y * nb_columns + x]; grid column x lies
+ * along local X, row y along local Z, one unit apart before scaling, and the
+ * local bounds are centred on the origin.  nb_columns and nb_rows must be at
+ * least 2 (the reference's init fails otherwise).  Returns the id to store in
+ * rp3dg_shape.mesh with kind RP3DG_SHAPE_HEIGHTFIELD. */
+int rp3dg_create_heightfield(rp3dg_ctx* ctx, uint32_t nb_columns, uint32_t nb_rows, const float* heights,
+                             float sx, float sy, float sz, int32_t* heightfield_id);
 
 /* Replace the context's shape table (device copy of `shapes`). */
 int rp3dg_set_shapes(rp3dg_ctx* ctx, const rp3dg_shape* shapes, uint32_t nb_shapes);
@@ -554,8 +571,9 @@ int rp3dg_world_get_bodies(rp3dg_world* world, float* position, float* orientati
                            float* angular_velocity, uint8_t* sleeping);
 /* Overlapping-pair ids (pairNumbers of the two broad-phase ids,
  * mathematics_functions.h:428-433) in the reference's array order: enabled
- * pairs (OverlappingPairs::mConvexPairs) then disabled ones
- * (mDisabledConvexPairs).  *n receives the total; at most capacity are
+ * convex pairs (OverlappingPairs::mConvexPairs), disabled ones
+ * (mDisabledConvexPairs), then the convex vs concave pairs (mConcavePairs,
+ * mDisabledConcavePairs).  *n receives the total; at most capacity are
  * written. */
 int rp3dg_world_get_pairs(rp3dg_world* world, uint64_t* pair_ids, uint32_t capacity, uint32_t* n);
 /* Contact manifolds of the last step in the solver's order: per manifold the

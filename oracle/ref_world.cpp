@@ -486,10 +486,33 @@ int ref_world_field_names(int id, char* dst, int cap) {
 }
 
 // ---- scenes described with the library's own world description -----------
+// Height fields named by rp3dg_shape.mesh (kind RP3DG_SHAPE_HEIGHTFIELD):
+// registered here with the arguments of rp3dg_create_heightfield, then built
+// by ref_scene_create with PhysicsCommon::createHeightField (float heights)
+// and createHeightFieldShape(scale).
+struct HeightFieldSpec {
+    int ncol, nrow;
+    std::vector<float> heights;
+    float scale[3];
+};
+static std::vector<HeightFieldSpec>& heightfields() {
+    static std::vector<HeightFieldSpec> h;
+    return h;
+}
 // ref_scene_create builds a reference world from the rp3dg_world_settings /
 // rp3dg_body_desc / rp3dg_collider_desc arrays that rp3dg_world_create takes,
 // with the call sequence documented there (include/rp3dg.h), so that both
 // engines start from identical worlds.  Convex meshes are not used here.
+int ref_heightfield_register(uint32_t ncol, uint32_t nrow, const float* heights, float sx, float sy, float sz) {
+    HeightFieldSpec h;
+    h.ncol = int(ncol);
+    h.nrow = int(nrow);
+    h.heights.assign(heights, heights + size_t(ncol) * nrow);
+    h.scale[0] = sx; h.scale[1] = sy; h.scale[2] = sz;
+    heightfields().push_back(h);
+    return int(heightfields().size()) - 1;
+}
+
 int ref_scene_create(const rp3dg_world_settings* s, const rp3dg_shape* shapes, uint32_t nshapes,
                      const rp3dg_body_desc* bd, uint32_t nb, const rp3dg_collider_desc* cd, uint32_t nc) {
     auto W = std::make_unique<World>();
@@ -511,6 +534,15 @@ int ref_scene_create(const rp3dg_world_settings* s, const rp3dg_shape* shapes, u
         if (sh.kind == RP3DG_SHAPE_SPHERE) cs[i] = W->common.createSphereShape(sh.params[0]);
         else if (sh.kind == RP3DG_SHAPE_CAPSULE) cs[i] = W->common.createCapsuleShape(sh.params[0], sh.params[1] * 2.0f);
         else if (sh.kind == RP3DG_SHAPE_BOX) cs[i] = W->common.createBoxShape(Vector3(sh.params[0], sh.params[1], sh.params[2]));
+        else if (sh.kind == RP3DG_SHAPE_HEIGHTFIELD) {
+            if (sh.mesh < 0 || size_t(sh.mesh) >= heightfields().size()) return -1;
+            const HeightFieldSpec& h = heightfields()[size_t(sh.mesh)];
+            std::vector<Message> messages;
+            HeightField* hf = W->common.createHeightField(h.ncol, h.nrow, h.heights.data(),
+                                                          HeightField::HeightDataType::HEIGHT_FLOAT_TYPE, messages);
+            if (!hf) return -1;
+            cs[i] = W->common.createHeightFieldShape(hf, Vector3(h.scale[0], h.scale[1], h.scale[2]));
+        }
         else return -1;
     }
     uint32_t ci = 0;
@@ -607,6 +639,10 @@ long ref_scene_pairs(int id, uint64_t* out, long cap) {
         if (out && k < cap) out[k] = op.mConvexPairs[i].pairID;
     for (uint64 i = 0; i < op.mDisabledConvexPairs.size(); i++, k++)
         if (out && k < cap) out[k] = op.mDisabledConvexPairs[i].pairID;
+    for (uint64 i = 0; i < op.mConcavePairs.size(); i++, k++)
+        if (out && k < cap) out[k] = op.mConcavePairs[i].pairID;
+    for (uint64 i = 0; i < op.mDisabledConcavePairs.size(); i++, k++)
+        if (out && k < cap) out[k] = op.mDisabledConcavePairs[i].pairID;
     return k;
 }
 

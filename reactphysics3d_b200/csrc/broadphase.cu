@@ -18,24 +18,11 @@
 
 #include "broadphase_launch.h"
 #include "rp3dg_math.cuh"
+#include "shape_aabb.cuh"
 
 namespace rp3dg {
 
 namespace {
-
-// Quaternion::getMatrix (src/mathematics/Quaternion.cpp:138-165)
-RD void quat_matrix_bp(quat q, float* r) {
-    const float nQ = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
-    float s = 0.0f;
-    if (nQ > 0.0f) s = 2.0f / nQ;
-    const float xs = q.x * s, ys = q.y * s, zs = q.z * s;
-    const float wxs = q.w * xs, wys = q.w * ys, wzs = q.w * zs;
-    const float xxs = q.x * xs, xys = q.x * ys, xzs = q.x * zs;
-    const float yys = q.y * ys, yzs = q.y * zs, zzs = q.z * zs;
-    r[0] = 1.0f - yys - zzs; r[1] = xys - wzs;        r[2] = xzs + wys;
-    r[3] = xys + wzs;        r[4] = 1.0f - xxs - zzs; r[5] = yzs - wxs;
-    r[6] = xzs - wys;        r[7] = yzs + wxs;        r[8] = 1.0f - xxs - yys;
-}
 
 // ---- world AABB + fat AABB update, one collider per thread --------------
 __global__ void __launch_bounds__(128) bp_update_kernel(const BpArgs a) {
@@ -53,34 +40,9 @@ __global__ void __launch_bounds__(128) bp_update_kernel(const BpArgs a) {
     }
     const rp3dg_shape s = a.shapes[si];
     const float4 p4 = a.wpos[i], q4 = a.wori[i];
-    const v3 t = V(p4.x, p4.y, p4.z);
     v3 amin, amax;
-    if (s.kind == RP3DG_SHAPE_SPHERE) {
-        // SphereShape::computeTransformedAABB: position -/+ (margin, margin, margin)
-        const float r = s.params[0];
-        amin = V(t.x - r, t.y - r, t.z - r);
-        amax = V(t.x + r, t.y + r, t.z + r);
-    } else {
-        const float4 lo = a.bounds[2 * si], hi = a.bounds[2 * si + 1];
-        const float bmin[3] = {lo.x, lo.y, lo.z}, bmax[3] = {hi.x, hi.y, hi.z}, tt[3] = {t.x, t.y, t.z};
-        float m[9];
-        quat_matrix_bp(Q(q4.x, q4.y, q4.z, q4.w), m);
-        float rmin[3], rmax[3];
-#pragma unroll
-        for (int r = 0; r < 3; r++) {
-            rmin[r] = tt[r];
-            rmax[r] = tt[r];
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const float e = m[3 * r + c] * bmin[c];
-                const float f = m[3 * r + c] * bmax[c];
-                if (e < f) { rmin[r] += e; rmax[r] += f; }
-                else { rmin[r] += f; rmax[r] += e; }
-            }
-        }
-        amin = V(rmin[0], rmin[1], rmin[2]);
-        amax = V(rmax[0], rmax[1], rmax[2]);
-    }
+    shape_transformed_aabb(s.kind, s.params[0], a.bounds[2 * si], a.bounds[2 * si + 1],
+                           X(V(p4.x, p4.y, p4.z), Q(q4.x, q4.y, q4.z, q4.w)), amin, amax);
     // DynamicAABBTree::updateObject: keep the fat AABB while it contains the
     // new one (AABB::contains), else inflate the new one by 4% of its extent
     // on each side (DYNAMIC_TREE_FAT_AABB_INFLATE_PERCENTAGE 0.08 x 0.5)

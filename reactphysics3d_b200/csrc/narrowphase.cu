@@ -52,6 +52,23 @@ RD ShapeRec load_shape(const rp3dg_shape* shapes, int32_t idx) {
     return s;
 }
 
+// The shape kinds an algorithm batch accepts (CollisionDispatch::selectAlgorithm,
+// CollisionDispatch.cpp:80-115); any other pair is reported as a bad shape.
+RD bool is_poly_kind(int k) { return k == RP3DG_SHAPE_BOX || k == RP3DG_SHAPE_CONVEX_MESH; }
+RD bool kinds_match(int algo, int k1, int k2) {
+    switch (algo) {
+        case RP3DG_ALGO_SPHERE_VS_SPHERE: return k1 == RP3DG_SHAPE_SPHERE && k2 == RP3DG_SHAPE_SPHERE;
+        case RP3DG_ALGO_SPHERE_VS_CAPSULE:
+            return (k1 == RP3DG_SHAPE_SPHERE && k2 == RP3DG_SHAPE_CAPSULE) || (k1 == RP3DG_SHAPE_CAPSULE && k2 == RP3DG_SHAPE_SPHERE);
+        case RP3DG_ALGO_CAPSULE_VS_CAPSULE: return k1 == RP3DG_SHAPE_CAPSULE && k2 == RP3DG_SHAPE_CAPSULE;
+        case RP3DG_ALGO_SPHERE_VS_CONVEX_POLYHEDRON:
+            return (k1 == RP3DG_SHAPE_SPHERE && is_poly_kind(k2)) || (is_poly_kind(k1) && k2 == RP3DG_SHAPE_SPHERE);
+        case RP3DG_ALGO_CAPSULE_VS_CONVEX_POLYHEDRON:
+            return (k1 == RP3DG_SHAPE_CAPSULE && is_poly_kind(k2)) || (is_poly_kind(k1) && k2 == RP3DG_SHAPE_CAPSULE);
+        default: return is_poly_kind(k1) && is_poly_kind(k2);
+    }
+}
+
 RD MeshPoly mesh_poly(const uint32_t* words, int32_t inst) {
     MeshPoly m;
     m.h = reinterpret_cast<const MeshHdr*>(words) + inst;
@@ -98,6 +115,8 @@ RD void load_item(const NpArgs& a, uint32_t i, Item& it) {
     it.out.count = 0;
     it.out.first_normal = V(0.0f, 0.0f, 0.0f);
     it.out.first_depth = 0.0f;
+    it.tri_side = 0;
+    it.tri = nullptr;
 }
 
 RD void store_item(const NpArgs& a, uint32_t i, const Item& it) {
@@ -129,6 +148,14 @@ RD uint32_t process_pair(const NpArgs& a, uint32_t i, const BoxTables* box, cons
     }
     const ShapeRec s1 = load_shape(a.shapes, i1);
     const ShapeRec s2 = load_shape(a.shapes, i2);
+    if (!kinds_match(ALGO, s1.kind, s2.kind)) {
+        // a pair the algorithm does not handle (a concave shape has no pair
+        // test of its own: it goes through the middle phase's triangles)
+        a.is_colliding[i] = 0;
+        a.nb_contacts[i] = 0;
+        atomicOr(a.error, 1u);
+        return 0;
+    }
     Item it;
     load_item(a, i, it);
     it.proposal = proposal;
@@ -170,6 +197,61 @@ RD uint32_t process_pair(const NpArgs& a, uint32_t i, const BoxTables* box, cons
     return (it.proposal_tested ? 1u : 0u) | (it.proposal_confirmed ? 2u : 0u);
 }
 
+// One triangle test of a convex vs concave pair (the narrow-phase input that
+// computeConvexVsConcaveMiddlePhase creates per overlapping triangle,
+// CollisionDetectionSystem.cpp:522-615): the convex shape comes from the
+// shape table, the TriangleShape from args.tri.
+template <int ALGO>
+RD void process_tri(const NpArgs& a, uint32_t i, const BoxTables* box, const uint32_t* mesh_words) {
+    const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
+    const bool tri1 = i1 < 0;
+    const int32_t ci = tri1 ? i2 : i1;
+    bool ok = (i1 < 0) != (i2 < 0) && uint32_t(ci) < a.nb_shapes;
+    ShapeRec cs;
+    if (ok) {
+        cs = load_shape(a.shapes, ci);
+        ok = ALGO == RP3DG_ALGO_SPHERE_VS_CONVEX_POLYHEDRON    ? cs.kind == RP3DG_SHAPE_SPHERE
+             : ALGO == RP3DG_ALGO_CAPSULE_VS_CONVEX_POLYHEDRON ? cs.kind == RP3DG_SHAPE_CAPSULE
+                                                               : is_poly_kind(cs.kind);
+    }
+    if (!ok) {
+        a.is_colliding[i] = 0;
+        a.nb_contacts[i] = 0;
+        atomicOr(a.error, 1u);
+        return;
+    }
+    TriPoly tp;
+    const float4 f0 = a.tri[i], f1 = a.tri[size_t(a.n) + i], f2 = a.tri[2 * size_t(a.n) + i];
+    const float4 f3 = a.tri[3 * size_t(a.n) + i], f4 = a.tri[4 * size_t(a.n) + i];
+    tp.p0 = V(f0.x, f0.y, f0.z);
+    tp.p1 = V(f1.x, f1.y, f1.z);
+    tp.p2 = V(f2.x, f2.y, f2.z);
+    tp.n = V(f3.x, f3.y, f3.z);
+    tp.vn0 = tp.vn1 = tp.vn2 = V(f4.x, f4.y, f4.z);
+    tp.t = box;
+    Item it;
+    load_item(a, i, it);
+    it.tri_side = tri1 ? 1u : 2u;
+    it.tri = &tp;
+    if (ALGO == RP3DG_ALGO_SPHERE_VS_CONVEX_POLYHEDRON) {
+        sphere_poly(it, !tri1, SphereS{cs.params.x}, tp);
+    } else if (ALGO == RP3DG_ALGO_CAPSULE_VS_CONVEX_POLYHEDRON) {
+        capsule_poly(it, !tri1, CapsuleS{cs.params.x, cs.params.y}, tp);
+    } else {
+        if (cs.kind == RP3DG_SHAPE_BOX) {
+            if (tri1) sat_poly_poly(it, tp, box_poly(cs, box), a.clip);
+            else sat_poly_poly(it, box_poly(cs, box), tp, a.clip);
+        } else {
+            if (tri1) sat_poly_poly(it, tp, mesh_poly(mesh_words, cs.mesh), a.clip);
+            else sat_poly_poly(it, mesh_poly(mesh_words, cs.mesh), tp, a.clip);
+        }
+        // ConvexPolyhedronVsConvexPolyhedronAlgorithm.cpp:53-61
+        it.lf.set(RP3DG_LF_WAS_USING_SAT, true);
+        it.lf.set(RP3DG_LF_WAS_USING_GJK, false);
+    }
+    store_item(a, i, it);
+}
+
 // Convex polyhedron vs convex polyhedron, one warp per pair.
 RD uint32_t process_pair_warp(const NpArgs& a, uint32_t i, int lane, const BoxTables* box, const uint32_t* mesh_words,
                               WarpScratch& stage, uint32_t proposal) {
@@ -184,6 +266,14 @@ RD uint32_t process_pair_warp(const NpArgs& a, uint32_t i, int lane, const BoxTa
     }
     const ShapeRec s1 = load_shape(a.shapes, i1);
     const ShapeRec s2 = load_shape(a.shapes, i2);
+    if (!kinds_match(RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON, s1.kind, s2.kind)) {
+        if (lane == 0) {
+            a.is_colliding[i] = 0;
+            a.nb_contacts[i] = 0;
+            atomicOr(a.error, 1u);
+        }
+        return 0;
+    }
     Item it;
     load_item(a, i, it);
     it.proposal = proposal;
@@ -206,6 +296,7 @@ RD void pair_features(const NpArgs& a, uint32_t i, const BoxTables* box, const u
     const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
     if (uint32_t(i1) >= a.nb_shapes || uint32_t(i2) >= a.nb_shapes) return;
     const ShapeRec s1 = load_shape(a.shapes, i1), s2 = load_shape(a.shapes, i2);
+    if (!is_poly_kind(s1.kind) || !is_poly_kind(s2.kind)) return;
     const float4 p1 = a.pos1[i], q1 = a.rot1[i], p2 = a.pos2[i], q2 = a.rot2[i];
     const xform t1 = X(V(p1.x, p1.y, p1.z), Q(q1.x, q1.y, q1.z, q1.w));
     const xform t2 = X(V(p2.x, p2.y, p2.z), Q(q2.x, q2.y, q2.z, q2.w));
@@ -298,6 +389,51 @@ __global__ void __launch_bounds__(NP_BLOCK, MinBlocks<ALGO>::value) narrowphase_
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride)
             process_pair<ALGO>(a, i, &s_box, mesh_words);
     }
+}
+
+template <int ALGO>
+__global__ void __launch_bounds__(NP_BLOCK, NP_MIN_BLOCKS) narrowphase_tri_kernel(const NpArgs a) {
+    extern __shared__ uint32_t s_mesh[];
+    __shared__ BoxTables s_box;
+    const uint32_t* mesh_words = a.mesh_words;
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&c_box_tables);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&s_box);
+        for (uint32_t k = threadIdx.x; k < sizeof(BoxTables) / 4; k += blockDim.x) dst[k] = src[k];
+        if (a.stage_mesh) {
+            for (uint32_t k = threadIdx.x; k < a.mesh_nwords; k += blockDim.x) s_mesh[k] = __ldg(a.mesh_words + k);
+            mesh_words = s_mesh;
+        }
+        __syncthreads();
+    }
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride)
+        process_tri<ALGO>(a, i, &s_box, mesh_words);
+}
+
+cudaError_t launch_narrowphase_tri(int algo, const NpArgs& args, int num_sms, cudaStream_t stream) {
+    if (args.n == 0) return cudaSuccess;
+    const void* k = algo == RP3DG_ALGO_SPHERE_VS_CONVEX_POLYHEDRON
+                        ? reinterpret_cast<const void*>(&narrowphase_tri_kernel<RP3DG_ALGO_SPHERE_VS_CONVEX_POLYHEDRON>)
+                    : algo == RP3DG_ALGO_CAPSULE_VS_CONVEX_POLYHEDRON
+                        ? reinterpret_cast<const void*>(&narrowphase_tri_kernel<RP3DG_ALGO_CAPSULE_VS_CONVEX_POLYHEDRON>)
+                    : algo == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON
+                        ? reinterpret_cast<const void*>(&narrowphase_tri_kernel<RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON>)
+                        : nullptr;
+    if (!k || !args.tri) return cudaErrorInvalidValue;
+    const size_t smem = args.stage_mesh ? size_t(args.mesh_nwords) * 4 : 0;
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, k);
+    if (e != cudaSuccess) return e;
+    if (smem > 0 && fa.sharedSizeBytes + smem > 48 * 1024) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+    }
+    const uint32_t blocks_needed = (args.n + NP_BLOCK - 1) / NP_BLOCK;
+    const uint32_t cap = uint32_t(num_sms) * 16u;
+    const uint32_t blocks = blocks_needed < cap ? blocks_needed : cap;
+    void* params[] = {const_cast<NpArgs*>(&args)};
+    return cudaLaunchKernel(k, dim3(blocks), dim3(NP_BLOCK), params, smem, stream);
 }
 
 // Learned proposals of a polyhedron batch: per tile of 32 pairs the warp

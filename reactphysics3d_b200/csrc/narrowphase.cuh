@@ -123,6 +123,54 @@ struct MeshPoly {
     }
 };
 
+// TriangleShape (TriangleShape.h/.cpp): a two-faced convex polyhedron with
+// margin 0; its topology is the shared triangle half-edge table.
+struct TriPoly {
+    v3 p0, p1, p2;       // mPoints
+    v3 n;                // mNormal: cross product of the edges, normalize()d
+    v3 vn0, vn1, vn2;    // mVerticesNormals
+    const BoxTables* t;
+    RD float margin() const { return 0.0f; }
+    RD uint32_t nfaces() const { return 2; }
+    RD uint32_t nhe() const { return 6; }
+    RD hedge edge(uint32_t e) const {
+        const uint8_t* c = t->tri_edges[e];
+        hedge h; h.vertex = c[0]; h.twin = c[1]; h.face = c[2]; h.next = c[3];
+        return h;
+    }
+    RD uint32_t face_edge(uint32_t f) const { return t->tri_face_edge[f]; }
+    RD uint32_t face_count(uint32_t) const { return 3; }
+    // faces (0, 1, 2) and (0, 2, 1)
+    RD uint32_t face_vertex(uint32_t f, uint32_t i) const { return (f == 0 || i == 0) ? i : 3u - i; }
+    RD v3 vertex(uint32_t v) const { return v == 0 ? p0 : (v == 1 ? p1 : p2); }
+    // TriangleShape::getFaceNormal (TriangleShape.h:262-266)
+    RD v3 normal(uint32_t f) const { return f == 0 ? n : vneg(n); }
+    // TriangleShape::getCentroid (TriangleShape.h:269-271)
+    RD v3 centroid() const { return vdivs(vadd(vadd(p0, p1), p2), 3.0f); }
+    // TriangleShape::getLocalSupportPointWithoutMargin (TriangleShape.h:193-197) with
+    // Vector3::getMaxAxis (Vector3.h:240-242)
+    RD v3 support(v3 d) const {
+        const float x = vdot(d, p0), y = vdot(d, p1), z = vdot(d, p2);
+        const int k = x < y ? (y < z ? 2 : 1) : (x < z ? 2 : 0);
+        return vertex(uint32_t(k));
+    }
+    // computeBarycentricCoordinatesInTriangle (mathematics_functions.h:203-219)
+    // and computeSmoothLocalContactNormalForTriangle (TriangleShape.h:309-337)
+    RD v3 smooth_normal(v3 p) const {
+        const v3 e0 = vsub(p1, p0), e1 = vsub(p2, p0), e2 = vsub(p, p0);
+        const float d00 = vdot(e0, e0), d01 = vdot(e0, e1), d11 = vdot(e1, e1);
+        const float d20 = vdot(e2, e0), d21 = vdot(e2, e1);
+        const float denom = d00 * d11 - d01 * d01;
+        const float v = (d11 * d20 - d01 * d21) / denom;
+        const float w = (d00 * d21 - d01 * d20) / denom;
+        const float u = 1.0f - v - w;
+        if (u > MACHINE_EPSILON && v > MACHINE_EPSILON && w > MACHINE_EPSILON) return n;
+        const v3 in = vadd(vadd(vmul(vn0, u), vmul(vn1, v)), vmul(vn2, w));
+        if (vlen2(in) < MACHINE_EPSILON) return n;
+        return vunit(in);
+    }
+};
+
 // ConvexPolyhedronShape::findMostAntiParallelFace (ConvexPolyhedronShape.h:105-123)
 template <class P>
 RD uint32_t most_antiparallel_face(const P& p, v3 dir) {
@@ -181,7 +229,40 @@ struct Item {
     bool proposal_tested, proposal_confirmed;
     LastFrame lf;
     ContactSink out;
+    uint32_t tri_side;        // 0: no triangle, 1: shape 1 is the triangle, 2: shape 2
+    const TriPoly* tri;
 };
+
+// TriangleShape::computeSmoothTriangleMeshContact (TriangleShape.h:342-365) and
+// computeSmoothMeshContact (TriangleShape.cpp:90-115): the contact normal
+// becomes the triangle's smooth normal at the contact point, oriented like the
+// penetration axis, and the other shape's point is re-projected from it.
+RD void smooth_triangle_contact(const Item& it, v3& nrm, float depth, v3& p1, v3& p2) {
+    const bool tri1 = it.tri_side == 1;
+    const v3 lpTri = tri1 ? p1 : p2;
+    const xform triToWorld = tri1 ? it.t1 : it.t2;
+    const xform worldToOther = tri1 ? xinv(it.t2) : xinv(it.t1);
+    v3 ln = it.tri->smooth_normal(lpTri);
+    v3 wn = qrot(triToWorld.q, ln);
+    const v3 penAxis = tri1 ? nrm : vneg(nrm);
+    if (vdot(wn, penAxis) < 0.0f) {
+        wn = vneg(wn);
+        ln = vneg(ln);
+    }
+    nrm = tri1 ? wn : vneg(wn);
+    const v3 otherTri = vsub(lpTri, vmul(ln, depth));
+    const v3 other = xapply(xmul(worldToOther, triToWorld), otherTri);
+    if (tri1) p2 = other;
+    else p1 = other;
+}
+
+// A contact of the GJK / SAT algorithms: smoothed first when one shape is a
+// triangle (every addContactPoint of GJKAlgorithm.cpp and SATAlgorithm.cpp is
+// preceded by computeSmoothTriangleMeshContact on the same arguments).
+RD void emit(Item& it, v3& nrm, float depth, v3 p1, v3 p2, bool write = true) {
+    if (it.tri_side) smooth_triangle_contact(it, nrm, depth, p1, p2);
+    it.out.add(nrm, depth, p1, p2, write);
+}
 
 // ---------------------------------------------------------------------------
 // SphereVsSphereAlgorithm::testCollision (SphereVsSphereAlgorithm.cpp:34-113)
@@ -586,7 +667,10 @@ RD int gjk(Item& it, const S1& s1, const S2& s2) {
         const float depth = margin - dist;
         if (depth <= 0.0f) return GJK_SEPARATED;
         if (vlen2(normal) < MACHINE_EPSILON) return GJK_SEPARATED;
-        if (it.report) it.out.add(normal, depth, pA, pB);
+        if (it.report) {
+            v3 nrm = normal;
+            emit(it, nrm, depth, pA, pB);
+        }
         return GJK_COLLIDE_IN_MARGIN;
     }
     return GJK_INTERPENETRATE;
@@ -618,8 +702,8 @@ RD void sat_sphere_poly(Item& it, bool sphere1, SphereS sph, const P& poly) {
         const v3 mnw = qrot(p2w.q, mn);
         const v3 psph = qrot(xinv(s2w).q, vmul(vneg(mnw), sph.r));
         const v3 ppoly = vadd(center, vmul(mn, minDepth - sph.r));
-        const v3 nw = sphere1 ? vneg(mnw) : mnw;
-        it.out.add(nw, minDepth, sphere1 ? psph : ppoly, sphere1 ? ppoly : psph);
+        v3 nw = sphere1 ? vneg(mnw) : mnw;
+        emit(it, nw, minDepth, sphere1 ? psph : ppoly, sphere1 ? ppoly : psph);
     }
     it.colliding = true;
 }
@@ -681,7 +765,9 @@ RD bool capsule_poly_face_contacts(uint32_t refFace, float capR, const P& poly, 
             found = true;
             const v3 pPoly = vadd(c, delta);
             const v3 pCap = vsub(xapply(p2c, c), vmul(sepAxisCap, capR));
-            it.out.add(nw, depth, cap1 ? pCap : pPoly, cap1 ? pPoly : pCap);
+            // normalWorld is a reference parameter there: a smoothed normal
+            // carries into the next clipped point
+            emit(it, nw, depth, cap1 ? pCap : pPoly, cap1 ? pPoly : pCap);
         }
     }
     return found;
@@ -746,7 +832,7 @@ RD bool sat_capsule_poly(Item& it, bool cap1, CapsuleS cap, const P& poly) {
         v3 cpSeg, cpEdge;
         closest_points_segments(segAp, segBp, sepE1, sepE2, cpSeg, cpEdge);
         const v3 pCap = vsub(xapply(p2c, cpSeg), vmul(sepAxis, cap.r));
-        it.out.add(nw, minDepth, cap1 ? pCap : cpEdge, cap1 ? cpEdge : pCap);
+        emit(it, nw, minDepth, cap1 ? pCap : cpEdge, cap1 ? cpEdge : pCap);
     }
     return true;
 }
@@ -821,11 +907,13 @@ RD bool edges_minkowski(const Edge1Gauss& g, const P2& p2, const hedge& e2, uint
     return edges_minkowski(g, p2, e2);
 }
 
-// computeDistanceBetweenEdges (SATAlgorithm.cpp:1040-1083); shape 1 is never a triangle here
-RD float sat_edge_distance(v3 e1A, v3 e2A, v3 c1, v3 d1, v3 d2, v3& outAxis) {
+// computeDistanceBetweenEdges (SATAlgorithm.cpp:1040-1083): when shape 1 is a
+// triangle the axis is oriented with shape 2's centroid c2 instead of c1
+RD float sat_edge_distance(v3 e1A, v3 e2A, v3 c1, v3 d1, v3 d2, v3& outAxis, bool tri1 = false,
+                           v3 c2 = V(0.0f, 0.0f, 0.0f)) {
     if (are_parallel(d1, d2)) return DECIMAL_LARGEST;
     v3 axis = vunit(vcross(d1, d2));
-    const float dp = vdot(axis, vsub(c1, e1A));
+    const float dp = tri1 ? vdot(axis, vsub(e2A, c2)) : vdot(axis, vsub(c1, e1A));
     if (dp > 0.0f) axis = vneg(axis);
     outAxis = axis;
     return -vdot(axis, vsub(e2A, e1A));
@@ -898,7 +986,8 @@ RD bool face_contacts(bool ref1, const PR& refP, const PI& incP, const xform& r2
             if (it.report) {
                 const v3 pInc = xapply(r2i, clipped[i]);
                 const v3 pRef = project_onto_plane(clipped[i], axisR, refV);
-                it.out.add(nw, depth, ref1 ? pRef : pInc, ref1 ? pInc : pRef);
+                v3 onw = nw;  // outWorldNormal: a copy per clipped point
+                emit(it, onw, depth, ref1 ? pRef : pInc, ref1 ? pInc : pRef);
             }
         }
     }
@@ -914,10 +1003,14 @@ RD bool poly_face_contacts(bool ref1, const P1& p1, const P2& p2, const xform& p
 
 template <class P> struct IsBox { static constexpr bool value = false; };
 template <> struct IsBox<BoxPoly> { static constexpr bool value = true; };
+template <class P> struct IsTri { static constexpr bool value = false; };
+template <> struct IsTri<TriPoly> { static constexpr bool value = true; };
 RD const BoxTables* box_tables_of(const BoxPoly& b, const BoxPoly&) { return b.t; }
 RD const BoxTables* box_tables_of(const BoxPoly& b, const MeshPoly&) { return b.t; }
 RD const BoxTables* box_tables_of(const MeshPoly&, const BoxPoly& b) { return b.t; }
 RD const BoxTables* box_tables_of(const MeshPoly&, const MeshPoly&) { return nullptr; }
+template <class P1, class P2>
+RD const BoxTables* box_tables_of(const P1&, const P2&) { return nullptr; }
 
 // ---------------------------------------------------------------------------
 // exact confirmation of a proposed feature
@@ -1020,7 +1113,8 @@ RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
             if (edges_minkowski(edge1_gauss(p1, e1, p1to2), p2, e2, lf.sat_e2)) {
                 v3 axis;
                 const v3 c1 = xapply(p1to2, p1.centroid());
-                const float d = sat_edge_distance(e1A, e2A, c1, d1, d2, axis);
+                const float d = sat_edge_distance(e1A, e2A, c1, d1, d2, axis, IsTri<P1>::value,
+                                                  IsTri<P1>::value ? p2.centroid() : V(0.0f, 0.0f, 0.0f));
                 if (!wasColliding && d <= 0.0f) return;
                 if (wasColliding && clipPrev && d > 0.0f && d < DECIMAL_LARGEST) {
                     v3 cp1, cp2;
@@ -1029,7 +1123,10 @@ RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
                     const float t1 = vdot(vsub(cp1, e2A), d2) / l2;
                     const float t2 = vdot(vsub(cp2, e1A), d1) / l1;
                     if (t1 >= 0.0f && t1 <= 1.0f && t2 >= 0.0f && t2 <= 1.0f) {
-                        if (it.report) it.out.add(qrot(it.t2.q, axis), d, xapply(p2to1, cp1), cp2);
+                        if (it.report) {
+                            v3 nw = qrot(it.t2.q, axis);
+                            emit(it, nw, d, xapply(p2to1, cp1), cp2);
+                        }
                         it.colliding = true;
                         return;
                     }
@@ -1081,7 +1178,8 @@ RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
                 const v3 e2A = p2.vertex(e2.vertex);
                 const v3 e2B = p2.vertex(p2.edge(e2.next).vertex);
                 v3 axis;
-                const float d = sat_edge_distance(e1A, e2A, c1, dir1, vsub(e2B, e2A), axis);
+                const float d = sat_edge_distance(e1A, e2A, c1, dir1, vsub(e2B, e2A), axis, IsTri<P1>::value,
+                                                  IsTri<P1>::value ? p2.centroid() : V(0.0f, 0.0f, 0.0f));
                 if (d <= 0.0f) {
                     lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, false);
                     lf.sat_e1 = i; lf.sat_e2 = j;
@@ -1102,7 +1200,8 @@ RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
         if (it.report) {
             v3 cp1, cp2;
             closest_points_segments(sE1A, sE1B, sE2A, sE2B, cp1, cp2);
-            it.out.add(qrot(it.t2.q, minEdgeAxis), minDepth, xapply(p2to1, cp1), cp2);
+            v3 nw = qrot(it.t2.q, minEdgeAxis);
+            emit(it, nw, minDepth, xapply(p2to1, cp1), cp2);
         }
         lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, false);
         lf.sat_e1 = minE1; lf.sat_e2 = minE2;

@@ -39,11 +39,17 @@ struct NpArgs {
     const void* mlp;                 // packed MLP weights (MlpPacked), read by narrowphase_propose
     const uint8_t* proposals;        // per-pair learned proposal (15 = none) or nullptr
     unsigned long long* mlp_stats;   // [0] proposals tested, [1] confirmed
+    // triangle tests (launch_narrowphase_tri): the triangle side of a test has
+    // shape index -1; 5 float4 per test, slot-major (k * n + i): the three
+    // vertices, the face normal and the vertex normal shared by the vertices
+    const float4* tri;
 };
 
 void upload_box_tables(const BoxTables& t, cudaStream_t s);
 // Launches the kernels of one algorithm batch; *launches receives how many.
 cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaStream_t stream, int* launches);
+// Triangle tests of one algorithm batch (4, 5 or 6), one test per thread.
+cudaError_t launch_narrowphase_tri(int algo, const NpArgs& args, int num_sms, cudaStream_t stream);
 // Learned proposals of a polyhedron batch (args.mlp must be set).
 cudaError_t launch_narrowphase_propose(const NpArgs& args, uint8_t* proposals, int num_sms, cudaStream_t stream);
 

@@ -167,6 +167,20 @@ BoxTables make_box_tables() {
         const int k = t.gauss[e][0] & 3;
         if (fillc[k] < 4) t.axis_edges[k][fillc[k]++] = uint8_t(e);
     }
+    // PhysicsCommon::initTriangleShapeHalfEdgeStructure (reference
+    // src/engine/PhysicsCommon.cpp:111-130): the two faces of a triangle
+    static const uint32_t tri_faces[6] = {0, 1, 2, 0, 2, 1};
+    std::vector<uint32_t> tfs = {0, 3}, tfc = {3, 3}, tfv(tri_faces, tri_faces + 6), tfe;
+    std::vector<HalfEdge> tedges;
+    compute_half_edges(tfs, tfc, tfv, 3, tedges, tfe);
+    for (int e = 0; e < 6; e++) {
+        t.tri_edges[e][0] = uint8_t(tedges[e].vertex);
+        t.tri_edges[e][1] = uint8_t(tedges[e].twin);
+        t.tri_edges[e][2] = uint8_t(tedges[e].face);
+        t.tri_edges[e][3] = uint8_t(tedges[e].next);
+    }
+    t.tri_face_edge[0] = uint8_t(tfe[0]);
+    t.tri_face_edge[1] = uint8_t(tfe[1]);
     return t;
 }
 
@@ -219,6 +233,8 @@ struct rp3dg_ctx {
     size_t cap_bp = 0;
     void* d_bp_stage = nullptr;
     size_t cap_bp_stage = 0;
+    // height fields (device heights in HfDesc::heights)
+    std::vector<rp3dg::HfDesc> hfields;
 };
 
 namespace {
@@ -321,6 +337,19 @@ int get_shapes_host(rp3dg_ctx* ctx, std::vector<rp3dg_shape>* out) {
     *out = ctx->host_shapes;
     return 0;
 }
+// the device shape table and its local bounds (2 float4 per shape)
+int get_shape_device(rp3dg_ctx* ctx, const rp3dg_shape** shapes, const float4** bounds) {
+    if (!ctx) return RP3DG_EINVAL;
+    *shapes = ctx->d_shapes;
+    *bounds = reinterpret_cast<const float4*>(ctx->d_shape_bounds);
+    return 0;
+}
+// a height field of the context (world set-up and middle phase)
+int get_heightfield(rp3dg_ctx* ctx, int32_t id, HfDesc* out) {
+    if (!ctx || !out || id < 0 || size_t(id) >= ctx->hfields.size()) return RP3DG_EINVAL;
+    *out = ctx->hfields[size_t(id)];
+    return 0;
+}
 // error message of a world call, readable through rp3dg_last_error
 void set_error(rp3dg_ctx* ctx, const std::string& msg) {
     if (ctx) ctx->err = msg;
@@ -369,6 +398,7 @@ void rp3dg_destroy(rp3dg_ctx* ctx) {
     cudaFree(ctx->d_shape_bounds);
     cudaFree(ctx->d_bp);
     cudaFree(ctx->d_bp_stage);
+    for (auto& h : ctx->hfields) cudaFree(const_cast<float*>(h.heights));
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -495,11 +525,55 @@ int rp3dg_get_convex_mesh_tables(rp3dg_ctx* ctx, int32_t instance_id, uint32_t* 
     return 0;
 }
 
+int rp3dg_create_heightfield(rp3dg_ctx* ctx, uint32_t nb_columns, uint32_t nb_rows, const float* heights,
+                             float sx, float sy, float sz, int32_t* heightfield_id) {
+    if (!ctx || !heights || !heightfield_id) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (nb_columns < 2 || nb_rows < 2)
+        return fail(ctx, RP3DG_EINVAL, "the number of grid columns and grid rows must be at least two");
+    if (size_t(nb_columns) * nb_rows > (size_t(1) << 30)) return fail(ctx, RP3DG_EINVAL, "height field too large");
+    if (!(sx > 0.0f) || !(sy > 0.0f) || !(sz > 0.0f)) return fail(ctx, RP3DG_EINVAL, "scale must be positive");
+    const size_t n = size_t(nb_columns) * nb_rows;
+    // HeightField::copyData (HeightField.cpp:93-133): minimum and maximum
+    // over the grid, then the height origin
+    float mn = heights[0], mx = heights[0];
+    for (uint32_t x = 0; x < nb_columns; x++)
+        for (uint32_t y = 0; y < nb_rows; y++) {
+            const float h = heights[size_t(y) * nb_columns + x];
+            if (!(h == h)) return fail(ctx, RP3DG_EINVAL, "height is NaN");
+            if (h < mn) mn = h;
+            if (h > mx) mx = h;
+        }
+    rp3dg::HfDesc d{};
+    d.ncol = nb_columns;
+    d.nrow = nb_rows;
+    d.width = float(nb_columns - 1);
+    d.length = float(nb_rows - 1);
+    d.origin = -(mx - mn) * 0.5f - mn;
+    // HeightField::init (:72-79): local bounds centred on the origin
+    const float halfHeight = (mx - mn) * 0.5f;
+    d.bmin[0] = -d.width * 0.5f; d.bmin[1] = -halfHeight; d.bmin[2] = -d.length * 0.5f;
+    d.bmax[0] = d.width * 0.5f;  d.bmax[1] = halfHeight;  d.bmax[2] = d.length * 0.5f;
+    d.scale[0] = sx; d.scale[1] = sy; d.scale[2] = sz;
+    cudaSetDevice(ctx->device);
+    float* dh = nullptr;
+    cudaError_t e = cudaMalloc(&dh, n * sizeof(float));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc(heights)");
+    e = cudaMemcpyAsync(dh, heights, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) { cudaFree(dh); return cuda_fail(ctx, e, "upload heights"); }
+    d.heights = dh;
+    *heightfield_id = int32_t(ctx->hfields.size());
+    ctx->hfields.push_back(d);
+    return 0;
+}
+
 int rp3dg_set_shapes(rp3dg_ctx* ctx, const rp3dg_shape* shapes, uint32_t nb) {
     if (!ctx || (!shapes && nb)) return fail(ctx, RP3DG_EINVAL, "null argument");
     for (uint32_t i = 0; i < nb; i++) {
         const rp3dg_shape& s = shapes[i];
-        if (s.kind < RP3DG_SHAPE_SPHERE || s.kind > RP3DG_SHAPE_CONVEX_MESH) return fail(ctx, RP3DG_EINVAL, "unknown shape kind");
+        if (s.kind < RP3DG_SHAPE_SPHERE || s.kind > RP3DG_SHAPE_HEIGHTFIELD) return fail(ctx, RP3DG_EINVAL, "unknown shape kind");
+        if (s.kind == RP3DG_SHAPE_HEIGHTFIELD && (s.mesh < 0 || size_t(s.mesh) >= ctx->hfields.size()))
+            return fail(ctx, RP3DG_EINVAL, "shape refers to an unknown height field");
         if (s.kind == RP3DG_SHAPE_CONVEX_MESH && (s.mesh < 0 || size_t(s.mesh) >= ctx->instances.size()))
             return fail(ctx, RP3DG_EINVAL, "shape refers to an unknown convex mesh instance");
     }
@@ -525,6 +599,12 @@ int rp3dg_set_shapes(rp3dg_ctx* ctx, const rp3dg_shape* shapes, uint32_t nb) {
             case RP3DG_SHAPE_CAPSULE:
                 b[0] = -p[0]; b[1] = -p[1] - p[0]; b[2] = -p[0]; b[4] = p[0]; b[5] = p[1] + p[0]; b[6] = p[0]; break;
             case RP3DG_SHAPE_BOX: b[0] = -p[0]; b[1] = -p[1]; b[2] = -p[2]; b[4] = p[0]; b[5] = p[1]; b[6] = p[2]; break;
+            case RP3DG_SHAPE_HEIGHTFIELD: {
+                // HeightFieldShape::getLocalBounds (HeightFieldShape.cpp:46-50): bounds * scale
+                const rp3dg::HfDesc& h = ctx->hfields[size_t(sh.mesh)];
+                for (int k = 0; k < 3; k++) { b[k] = h.bmin[k] * h.scale[k]; b[4 + k] = h.bmax[k] * h.scale[k]; }
+                break;
+            }
             default: {
                 const MeshInstance& in = ctx->instances[size_t(sh.mesh)];
                 const MeshTopo& m = ctx->meshes[size_t(in.mesh)];
@@ -600,6 +680,7 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
     a.mlp = learned ? static_cast<const void*>(mlp_packed(ctx)) : nullptr;
     a.mlp_stats = learned ? mlp_stats(ctx) : nullptr;
     a.proposals = nullptr;
+    a.tri = nullptr;
     cudaSetDevice(ctx->device);
     if (learned) {
         // one proposal byte per pair, in a buffer that grows with the batch
@@ -948,6 +1029,48 @@ int rp3dg_learned_axis_stats(rp3dg_ctx* ctx, uint64_t* tested, uint64_t* confirm
 }
 
 }  // extern "C"
+
+namespace rp3dg {
+// Triangle tests of one algorithm batch of the world step (device arrays,
+// asynchronous): like rp3dg_narrowphase_device, with the TriangleShape of
+// each test in tri (the triangle side has shape index -1).
+int narrowphase_tri_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3dg_contact_batch* out,
+                           const float4* tri) {
+    if (!ctx || !p || !out || !tri) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (algorithm < RP3DG_ALGO_SPHERE_VS_CONVEX_POLYHEDRON || algorithm > RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON)
+        return fail(ctx, RP3DG_EINVAL, "triangle tests need a convex-polyhedron algorithm");
+    if (p->n == 0) return 0;
+    if (!ctx->d_shapes) return fail(ctx, RP3DG_EINVAL, "no shape table (rp3dg_set_shapes)");
+    NpArgs a;
+    a.n = p->n;
+    a.nb_shapes = ctx->nb_shapes;
+    a.error = ctx->d_error;
+    a.max_contacts = out->max_contacts;
+    a.clip = 1;
+    a.mesh_nwords = uint32_t(ctx->arena.size());
+    a.mesh_words = ctx->d_arena;
+    a.stage_mesh = (a.mesh_nwords > 0 && size_t(a.mesh_nwords) * 4 <= MESH_STAGE_MAX_BYTES) ? 1 : 0;
+    a.shapes = ctx->d_shapes;
+    a.shape1 = p->shape1; a.shape2 = p->shape2;
+    a.pos1 = reinterpret_cast<const float4*>(p->pos1); a.rot1 = reinterpret_cast<const float4*>(p->rot1);
+    a.pos2 = reinterpret_cast<const float4*>(p->pos2); a.rot2 = reinterpret_cast<const float4*>(p->rot2);
+    a.report = p->report_contacts;
+    a.cache = p->cache;
+    a.is_colliding = out->is_colliding;
+    a.nb_contacts = out->nb_contacts;
+    a.normal_depth = reinterpret_cast<float4*>(out->normal_depth);
+    a.local1 = reinterpret_cast<float4*>(out->local1);
+    a.local2 = reinterpret_cast<float4*>(out->local2);
+    a.mlp = nullptr;
+    a.mlp_stats = nullptr;
+    a.proposals = nullptr;
+    a.tri = tri;
+    cudaError_t e = launch_narrowphase_tri(algorithm, a, ctx->num_sms, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "triangle narrow-phase launch");
+    ctx->launches++;
+    return 0;
+}
+}  // namespace rp3dg
 
 // ---- dynamics stage ------------------------------------------------------
 

@@ -43,6 +43,21 @@ struct BoxTables {
     uint8_t pad[2];
     uint8_t gauss[24][4];
     uint8_t axis_edges[3][4];  // even half-edges along x, y, z (increasing index)
+    // TriangleShape topology (PhysicsCommon::initTriangleShapeHalfEdgeStructure):
+    // faces (0, 1, 2) and (0, 2, 1)
+    uint8_t tri_edges[6][4];   // vertex, twin, face, next
+    uint8_t tri_face_edge[2];
+    uint8_t pad2[2];
+};
+
+// A height field (HeightField + HeightFieldShape scale) as the middle phase
+// reads it: heights[y * ncol + x], unscaled local bounds, height origin.
+struct HfDesc {
+    uint32_t ncol, nrow;
+    float width, length, origin;
+    float bmin[3], bmax[3];
+    float scale[3];
+    const float* heights;  // device
 };
 
 }  // namespace rp3dg

@@ -53,6 +53,7 @@
 
 #include "../../include/rp3dg.h"
 #include "dynamics_launch.h"
+#include "hf_launch.h"
 #include "rp3dg_math.cuh"
 #include "world_order.h"
 
@@ -66,6 +67,12 @@ int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const r
                         const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled,
                         const DynJoints* joints);
 int broadphase_update_flags(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, const uint8_t* enabled);
+// height fields, the shape table and its local bounds on the device, and the
+// triangle tests of convex vs concave pairs
+int get_heightfield(rp3dg_ctx* ctx, int32_t id, HfDesc* out);
+int get_shape_device(rp3dg_ctx* ctx, const rp3dg_shape** shapes, const float4** bounds);
+int narrowphase_tri_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3dg_contact_batch* out,
+                           const float4* tri);
 }  // namespace rp3dg
 
 using rp3dg::order::Box;
@@ -130,10 +137,12 @@ __global__ void __launch_bounds__(128) world_reset_cache(uint32_t n, const int32
 struct PackArgs {
     uint32_t nm;
     const int4* ids;            // body1 row, body2 row, collider1 row, collider2 row
-    const int4* src;            // x item index inside its batch, y batch size, z batch first item, w first point
+    const int4* src;            // x item index inside its batch, y batch size, z batch first item, w first point;
+                                // concave manifolds: x first point in c_*, y = -1, z points, w first point
     const int4* prev;           // previous pair's manifold start, count, point start, count (x < 0: none)
     const uint8_t* kept_count;  // points kept by the manifold step, per item
     const float4 *b_nd, *b_l1, *b_l2;  // narrow-phase outputs, slot-major per batch (16 slots)
+    const float4 *c_nd, *c_l1, *c_l2;  // manifolds of convex vs concave pairs (4 x 4 points per pair)
     float cos_similar, persist2;
     // previous step's manifolds and points (after storeImpulses)
     const uint32_t* pm_pstart;
@@ -152,29 +161,36 @@ struct PackArgs {
 };
 
 // createContacts (CollisionDetectionSystem.cpp:906-960) + the warm start of
-// initContactsWithPreviousOnes (:1069-1160) for convex pairs: one manifold
-// per contact pair, one thread per manifold.
+// initContactsWithPreviousOnes (:1069-1160): one thread per manifold; a
+// convex pair has one manifold (its narrow-phase slots), a convex vs concave
+// pair up to four (from the concave manifold step).
 __global__ void __launch_bounds__(128) world_pack_contacts(const PackArgs a) {
     const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= a.nm) return;
     const int4 s = a.src[m];
-    const uint32_t item = uint32_t(s.z + s.x);
-    const uint32_t k = a.kept_count[item];
+    const bool concave = s.y < 0;
+    const uint32_t k = concave ? uint32_t(s.z) : a.kept_count[uint32_t(s.z + s.x)];
     const uint32_t ps = uint32_t(s.w);
-    const uint32_t base = uint32_t(s.z) * MAXC;  // batch region start (float4 units)
+    const uint32_t base = concave ? 0u : uint32_t(s.z) * MAXC;  // batch region start (float4 units)
     a.m_ids[m] = a.ids[m];
     a.m_pstart[m] = ps;
     a.m_npts[m] = uint8_t(k);
     for (uint32_t c = 0; c < k; c++) {
-        const uint32_t src = base + c * uint32_t(s.y) + uint32_t(s.x);
-        a.p_nd[ps + c] = a.b_nd[src];
-        a.p_l1[ps + c] = a.b_l1[src];
-        a.p_l2[ps + c] = a.b_l2[src];
+        if (concave) {
+            a.p_nd[ps + c] = a.c_nd[uint32_t(s.x) + c];
+            a.p_l1[ps + c] = a.c_l1[uint32_t(s.x) + c];
+            a.p_l2[ps + c] = a.c_l2[uint32_t(s.x) + c];
+        } else {
+            const uint32_t src = base + c * uint32_t(s.y) + uint32_t(s.x);
+            a.p_nd[ps + c] = a.b_nd[src];
+            a.p_l1[ps + c] = a.b_l1[src];
+            a.p_l2[ps + c] = a.b_l2[src];
+        }
     }
     float4 fv1 = make_float4(0.f, 0.f, 0.f, 0.f), fv2 = fv1, fimp = fv1;
     const int4 pv = a.prev[m];
     if (pv.x >= 0 && k > 0) {
-        const float4 cn = a.b_nd[base + uint32_t(s.x)];
+        const float4 cn = concave ? a.c_nd[uint32_t(s.x)] : a.b_nd[base + uint32_t(s.x)];
         for (int p = pv.x; p < pv.x + pv.y; p++) {
             const float4 pn = a.pp_nd[a.pm_pstart[p]];
             // previousNormal.dot(currentNormal) >= cosAngleSimilarContactManifold
@@ -356,6 +372,8 @@ struct JointH {
 struct ColliderH {
     int body = -1;
     int shape = -1;
+    bool convex = true;  // CollisionShape::isConvex (a height field is not)
+    int hf = -1;         // height-field id of a concave collider
     int bp = -1;  // broad-phase id (tree leaf)
     uint16_t category = 1, mask = 0xffff;
     std::vector<uint64_t> pairs;  // ColliderComponents::mOverlappingPairs
@@ -367,12 +385,21 @@ struct PairH {
     int algo = 0;
     bool need_test = false, coll_prev = false, coll_curr = false, enabled = true;
     int cache = -1;  // slot of its LastFrameCollisionInfo in the device pool
+    // convex vs concave pairs (ConcaveOverlappingPair): which shape is convex,
+    // and the per-triangle records of the last step that tested the pair
+    // (valid only for the step right after it: the others are obsolete)
+    bool concave = false, shape1_convex = true, rec_valid = false;
+    int rec_start = -1;
+    int4 rec_rect = {0, 0, 0, 0};
 };
 struct ContactPairH {
     uint64_t id;
     int b1, b2, c1, c2;
-    uint32_t item;       // global narrow-phase item
-    uint32_t k;          // points after the manifold step
+    uint32_t item;       // global narrow-phase item (convex pair) or concave item
+    bool concave = false;
+    uint32_t nman = 1;   // manifolds (a convex pair has one)
+    uint32_t npts = 0;   // points per manifold, one byte each
+    uint32_t k;          // points of all its manifolds after the manifold step
     bool in_island = false;
     uint32_t manifold = 0, point = 0;  // global indices in the packed arrays
 };
@@ -468,9 +495,10 @@ struct WorldH {
     rp3dg::order::Tree tree;
     rp3dg::order::IdSet moved;
     std::vector<int> bp_to_collider;
-    // overlapping pairs (OverlappingPairs::mConvexPairs / mDisabledConvexPairs)
-    std::vector<PairH> pairs, disabled;
-    std::unordered_map<uint64_t, uint32_t> map_pairs, map_disabled;
+    // overlapping pairs (OverlappingPairs::mConvexPairs / mDisabledConvexPairs,
+    // mConcavePairs / mDisabledConcavePairs)
+    std::vector<PairH> pairs, disabled, concave, concave_dis;
+    std::unordered_map<uint64_t, uint32_t> map_pairs, map_disabled, map_concave, map_concave_dis;
     std::vector<int> free_cache;
     std::vector<int32_t> reset_slots;
     // contacts of this step and of the previous one
@@ -497,6 +525,10 @@ struct WorldH {
     std::vector<int4> items[NB_ALGOS];
     std::vector<uint32_t> item_pair[NB_ALGOS];
     uint32_t item_off[NB_ALGOS] = {};
+    // convex vs concave pairs of the middle phase (hf_launch.h items)
+    std::vector<int4> hitems[NB_ALGOS];
+    std::vector<uint32_t> hitem_pair[NB_ALGOS];
+    uint32_t hitem_off[NB_ALGOS] = {};
     uint32_t nm = 0, np = 0, man_base = 0, pt_base = 0, isl_base = 0;
     std::vector<int> slept;                    // bodies put to sleep by this step
     rp3dg_world_stats stats{};
@@ -540,6 +572,26 @@ struct rp3dg_world {
     rp3dg_lastframe* d_cache = nullptr;
     float4 *d_nd = nullptr, *d_l1 = nullptr, *d_l2 = nullptr;
     uint32_t batch_start[NB_ALGOS + 1] = {};
+    // convex vs concave pairs: items (algorithm-major like the batches), their
+    // triangle tests, and the per-triangle records of this step and the last
+    uint32_t hitem_start[NB_ALGOS + 1] = {};
+    uint32_t htest_start[NB_ALGOS + 1] = {};
+    rp3dg::HfDesc* d_hf = nullptr;
+    uint32_t n_hf = 0;
+    size_t cap_hitem = 0, cap_htest = 0, cap_hc[2] = {0, 0};
+    int4 *h_hitems = nullptr, *d_hitems = nullptr, *h_hrect = nullptr, *d_hrect = nullptr;
+    uint32_t *h_hstart = nullptr, *d_hstart = nullptr;
+    int32_t *h_hpstart = nullptr, *d_hpstart = nullptr;
+    int4 *h_hprect = nullptr, *d_hprect = nullptr, *h_hbatch = nullptr, *d_hbatch = nullptr;
+    uint8_t *h_hout = nullptr, *d_hout = nullptr;  // colliding (n), manifolds (n), points per manifold (4n)
+    float4 *d_hond = nullptr, *d_hol1 = nullptr, *d_hol2 = nullptr;
+    int32_t *d_ts1 = nullptr, *d_ts2 = nullptr;
+    float4 *d_tp1 = nullptr, *d_tr1 = nullptr, *d_tp2 = nullptr, *d_tr2 = nullptr;
+    uint8_t *d_trep = nullptr, *d_tcoll = nullptr, *d_tnct = nullptr, *d_tmid = nullptr;
+    float4 *d_tnd = nullptr, *d_tl1 = nullptr, *d_tl2 = nullptr, *d_tri = nullptr;
+    rp3dg_lastframe* d_tcache[2] = {nullptr, nullptr};
+    int cur_tc = 0;
+    cudaEvent_t ev_rect = nullptr;
     // manifold packing
     size_t cap_m = 0, cap_i = 0;
     int4 *d_mids = nullptr, *d_msrc = nullptr, *d_mprev = nullptr;
@@ -615,11 +667,16 @@ int alloc_cache(Group* g, WorldH& w) {
     return slot;
 }
 
+// OverlappingPairs::getOverlappingPair
 PairH* find_pair(WorldH& w, uint64_t id) {
     auto it = w.map_pairs.find(id);
     if (it != w.map_pairs.end()) return &w.pairs[it->second];
+    it = w.map_concave.find(id);
+    if (it != w.map_concave.end()) return &w.concave[it->second];
     it = w.map_disabled.find(id);
     if (it != w.map_disabled.end()) return &w.disabled[it->second];
+    it = w.map_concave_dis.find(id);
+    if (it != w.map_concave_dis.end()) return &w.concave_dis[it->second];
     return nullptr;
 }
 
@@ -638,21 +695,32 @@ void remove_from_collider(WorldH& w, int c, uint64_t id) {
     if (it != v.end()) v.erase(it);
 }
 
-// OverlappingPairs::addPair (OverlappingPairs.cpp:397-449), convex pairs
+// OverlappingPairs::addPair (OverlappingPairs.cpp:397-449): a convex pair, or
+// a convex vs concave pair whose algorithm is the convex shape's against a
+// CONVEX_POLYHEDRON (the triangles)
 void add_pair(Group* g, WorldH& w, int c1, int c2) {
-    const uint32_t b1 = uint32_t(w.colliders[size_t(c1)].bp), b2 = uint32_t(w.colliders[size_t(c2)].bp);
+    const ColliderH &C1 = w.colliders[size_t(c1)], &C2 = w.colliders[size_t(c2)];
+    const uint32_t b1 = uint32_t(C1.bp), b2 = uint32_t(C2.bp);
     PairH p;
     p.id = pair_number(std::max(b1, b2), std::min(b1, b2));
     p.bp1 = int(b1);
     p.bp2 = int(b2);
     p.c1 = c1;
     p.c2 = c2;
-    p.algo = select_algorithm(shape_type_index(g->shapes[size_t(w.colliders[size_t(c1)].shape)]),
-                              shape_type_index(g->shapes[size_t(w.colliders[size_t(c2)].shape)]));
     p.enabled = true;
-    p.cache = alloc_cache(g, w);
-    w.map_pairs[p.id] = uint32_t(w.pairs.size());
-    w.pairs.push_back(p);
+    if (C1.convex && C2.convex) {
+        p.algo = select_algorithm(shape_type_index(g->shapes[size_t(C1.shape)]),
+                                  shape_type_index(g->shapes[size_t(C2.shape)]));
+        p.cache = alloc_cache(g, w);
+        w.map_pairs[p.id] = uint32_t(w.pairs.size());
+        w.pairs.push_back(p);
+    } else {
+        p.concave = true;
+        p.shape1_convex = C1.convex;
+        p.algo = select_algorithm(shape_type_index(g->shapes[size_t(C1.convex ? C1.shape : C2.shape)]), 2);
+        w.map_concave[p.id] = uint32_t(w.concave.size());
+        w.concave.push_back(p);
+    }
     w.colliders[size_t(c1)].pairs.push_back(p.id);
     w.colliders[size_t(c2)].pairs.push_back(p.id);
 }
@@ -666,11 +734,33 @@ void remove_pair(WorldH& w, uint32_t idx) {
     remove_pair_at(w.pairs, w.map_pairs, idx);
 }
 
+// removeConcavePairWithIndex(index, removeFromColliders = true): its
+// per-triangle records go with it
+void remove_concave_pair(WorldH& w, uint32_t idx) {
+    PairH& p = w.concave[idx];
+    remove_from_collider(w, p.c1, p.id);
+    remove_from_collider(w, p.c2, p.id);
+    remove_pair_at(w.concave, w.map_concave, idx);
+}
+
 // disableConvexPairWithIndex / enableConvexPairWithIndex: the pair is
 // re-created in the other array with a fresh temporal-coherence record
 void disable_pair(Group* g, WorldH& w, uint64_t id) {
     auto it = w.map_pairs.find(id);
-    if (it == w.map_pairs.end()) return;
+    if (it == w.map_pairs.end()) {
+        // disableConcavePairWithIndex: re-created without records
+        auto ic = w.map_concave.find(id);
+        if (ic == w.map_concave.end()) return;
+        const uint32_t idx = ic->second;
+        PairH np = w.concave[idx];
+        np.enabled = false;
+        np.need_test = false;
+        np.rec_valid = false;
+        w.map_concave_dis[id] = uint32_t(w.concave_dis.size());
+        w.concave_dis.push_back(np);
+        remove_pair_at(w.concave, w.map_concave, idx);
+        return;
+    }
     const uint32_t idx = it->second;
     PairH np = w.pairs[idx];
     np.enabled = false;
@@ -683,7 +773,20 @@ void disable_pair(Group* g, WorldH& w, uint64_t id) {
 }
 void enable_pair(Group* g, WorldH& w, uint64_t id) {
     auto it = w.map_disabled.find(id);
-    if (it == w.map_disabled.end()) return;
+    if (it == w.map_disabled.end()) {
+        // enableConcavePairWithIndex
+        auto ic = w.map_concave_dis.find(id);
+        if (ic == w.map_concave_dis.end()) return;
+        const uint32_t idx = ic->second;
+        PairH np = w.concave_dis[idx];
+        np.enabled = true;
+        np.need_test = false;
+        np.rec_valid = false;
+        w.map_concave[id] = uint32_t(w.concave.size());
+        w.concave.push_back(np);
+        remove_pair_at(w.concave_dis, w.map_concave_dis, idx);
+        return;
+    }
     const uint32_t idx = it->second;
     PairH np = w.disabled[idx];
     np.enabled = true;
@@ -768,7 +871,8 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
             const uint64_t id = pair_number(uint32_t(std::max(s, leaf)), uint32_t(std::min(s, leaf)));
             PairH* p = find_pair(w, id);
             if (!p) {
-                if ((C1.mask & C2.category) != 0 && (C1.category & C2.mask) != 0) add_pair(g, w, c1, c2);
+                if ((C1.mask & C2.category) != 0 && (C1.category & C2.mask) != 0 && (C1.convex || C2.convex))
+                    add_pair(g, w, c1, c2);
             } else {
                 p->need_test = false;
             }
@@ -785,9 +889,21 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
             i--;
         }
     }
+    for (uint64_t i = 0; i < w.concave.size(); i++) {
+        PairH& p = w.concave[i];
+        if (!p.need_test) continue;
+        if (rp3dg::order::overlap(w.tree.nodes[size_t(p.bp1)].box, w.tree.nodes[size_t(p.bp2)].box)) {
+            p.need_test = false;
+        } else {
+            remove_concave_pair(w, uint32_t(i));
+            i--;
+        }
+    }
     for (int a = 0; a < NB_ALGOS; a++) {
         w.items[a].clear();
         w.item_pair[a].clear();
+        w.hitems[a].clear();
+        w.hitem_pair[a].clear();
     }
     // rows in the order the device will have after this step's row sync
     for (uint32_t i = 0; i < w.pairs.size(); i++) {
@@ -800,12 +916,31 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
                                        p.cache, 1));
         w.item_pair[a].push_back(i);
     }
+    // convex vs concave pairs (computeMiddlePhase :412-456): a pair that is
+    // not tested this step loses its per-triangle records
+    for (uint32_t i = 0; i < w.concave.size(); i++) {
+        PairH& p = w.concave[i];
+        p.coll_curr = false;
+        const bool e1 = w.ccomp.enabled(p.c1), e2 = w.ccomp.enabled(p.c2);
+        if (!(e1 || e2)) {
+            p.rec_valid = false;
+            continue;
+        }
+        const int cv = p.shape1_convex ? p.c1 : p.c2, cc = p.shape1_convex ? p.c2 : p.c1;
+        const int a = p.algo - 1;
+        w.hitems[a].push_back(make_int4(int(w.c0) + w.ccomp.slot[size_t(cv)], int(w.c0) + w.ccomp.slot[size_t(cc)],
+                                        w.colliders[size_t(cc)].hf, p.shape1_convex ? HF_SHAPE1_CONVEX : 0));
+        w.hitem_pair[a].push_back(i);
+    }
 }
 
 // processAllPotentialContacts' contact pairs (batch order), addContactPairsToBodies
 // and PhysicsWorld::createIslands (PhysicsWorld.cpp:695-866).
-void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint8_t* h_count) {
+void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint8_t* h_count, const uint8_t* h_hcoll,
+                          const uint8_t* h_hnman, const uint8_t* h_hnpts) {
     w.cpairs.clear();
+    // batch by batch; inside a batch the convex pairs' tests come first, then
+    // the triangles of the concave pairs (computeMiddlePhase's order)
     for (int a = 0; a < NB_ALGOS; a++) {
         const uint32_t base = g->batch_start[a] + w.item_off[a];
         for (uint32_t i = 0; i < w.items[a].size(); i++) {
@@ -821,6 +956,30 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
             c.b2 = w.colliders[size_t(p.c2)].body;
             c.item = it;
             c.k = h_count[it];
+            c.npts = c.k;
+            w.cpairs.push_back(c);
+        }
+        const uint32_t hbase = g->hitem_start[a] + w.hitem_off[a];
+        for (uint32_t i = 0; i < w.hitems[a].size(); i++) {
+            const uint32_t it = hbase + i;
+            if (!h_hcoll[it]) continue;
+            PairH& p = w.concave[w.hitem_pair[a][i]];
+            p.coll_curr = true;
+            ContactPairH c;
+            c.id = p.id;
+            c.c1 = p.c1;
+            c.c2 = p.c2;
+            c.b1 = w.colliders[size_t(p.c1)].body;
+            c.b2 = w.colliders[size_t(p.c2)].body;
+            c.item = it;
+            c.concave = true;
+            c.nman = h_hnman[it];
+            c.k = 0;
+            c.npts = 0;
+            for (uint32_t m = 0; m < c.nman; m++) {
+                c.k += h_hnpts[4 * size_t(it) + m];
+                c.npts |= uint32_t(h_hnpts[4 * size_t(it) + m]) << (8 * m);
+            }
             w.cpairs.push_back(c);
         }
     }
@@ -865,8 +1024,8 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
                 const int other = cp.b1 == b ? cp.b2 : cp.b1;
                 if (w.bodies[size_t(other)].has_sim_collider) {
                     w.island_order.push_back(cpi);
-                    total_manifolds += 1;
-                    w.islands[isl_index].manifold_count += 1;
+                    total_manifolds += cp.nman;
+                    w.islands[isl_index].manifold_count += cp.nman;
                     if (w.bodies[size_t(other)].in_island) continue;
                     stack.push_back(other);
                     w.bodies[size_t(other)].in_island = true;
@@ -890,9 +1049,9 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
         w.bodies[size_t(cp.b1)].contact_pairs.clear();
         w.bodies[size_t(cp.b2)].contact_pairs.clear();
     }
-    w.nm = uint32_t(w.island_order.size());
+    w.nm = total_manifolds;
     w.np = 0;
-    for (uint32_t m = 0; m < w.nm; m++) w.np += w.cpairs[w.island_order[m]].k;
+    for (uint32_t m = 0; m < w.island_order.size(); m++) w.np += w.cpairs[w.island_order[m]].k;
     // PhysicsWorld::enableDisableJoints (:363-393): a joint is enabled while
     // one of its bodies is
     if (!w.joints.empty()) {
@@ -938,25 +1097,38 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
 // warm-start sources of initContactsWithPreviousOnes (:1069-1160).
 void fill_manifolds(Group* g, WorldH& w) {
     uint32_t pt = w.pt_base;
-    for (uint32_t m = 0; m < w.nm; m++) {
-        ContactPairH& cp = w.cpairs[w.island_order[m]];
-        const uint32_t gm = w.man_base + m;
+    uint32_t gm = w.man_base;
+    for (uint32_t o = 0; o < w.island_order.size(); o++) {
+        ContactPairH& cp = w.cpairs[w.island_order[o]];
         cp.manifold = gm;
         cp.point = pt;
-        uint32_t a = 0;
-        while (cp.item >= g->batch_start[a + 1]) a++;
-        const uint32_t s0 = g->batch_start[a];
-        g->h_mids[gm] = make_int4(int(w.b0) + w.bcomp.slot[size_t(cp.b1)], int(w.b0) + w.bcomp.slot[size_t(cp.b2)],
-                                  int(w.c0) + w.ccomp.slot[size_t(cp.c1)], int(w.c0) + w.ccomp.slot[size_t(cp.c2)]);
-        g->h_msrc[gm] = make_int4(int(cp.item - s0), int(g->batch_start[a + 1] - s0), int(s0), int(pt));
+        const int4 ids = make_int4(int(w.b0) + w.bcomp.slot[size_t(cp.b1)], int(w.b0) + w.bcomp.slot[size_t(cp.b2)],
+                                   int(w.c0) + w.ccomp.slot[size_t(cp.c1)], int(w.c0) + w.ccomp.slot[size_t(cp.c2)]);
+        int4 prev = make_int4(-1, 0, 0, 0);
         auto it = w.prev_map.find(cp.id);
         if (it != w.prev_map.end() && w.prev_cpairs[it->second].in_island) {
             const ContactPairH& pc = w.prev_cpairs[it->second];
-            g->h_mprev[gm] = make_int4(int(pc.manifold), 1, int(pc.point), int(pc.k));
-        } else {
-            g->h_mprev[gm] = make_int4(-1, 0, 0, 0);
+            prev = make_int4(int(pc.manifold), int(pc.nman), int(pc.point), int(pc.k));
         }
-        pt += cp.k;
+        if (!cp.concave) {
+            uint32_t a = 0;
+            while (cp.item >= g->batch_start[a + 1]) a++;
+            const uint32_t s0 = g->batch_start[a];
+            g->h_mids[gm] = ids;
+            g->h_msrc[gm] = make_int4(int(cp.item - s0), int(g->batch_start[a + 1] - s0), int(s0), int(pt));
+            g->h_mprev[gm] = prev;
+            gm++;
+            pt += cp.k;
+        } else {
+            for (uint32_t m = 0; m < cp.nman; m++) {
+                const uint32_t km = (cp.npts >> (8 * m)) & 0xffu;
+                g->h_mids[gm] = ids;
+                g->h_msrc[gm] = make_int4(int(cp.item * HF_OUT_POINTS + 4 * m), -1, int(km), int(pt));
+                g->h_mprev[gm] = prev;
+                gm++;
+                pt += km;
+            }
+        }
     }
     for (uint32_t i = 0; i < w.islands.size(); i++) {
         g->h_istart[w.isl_base + i] = w.man_base + w.islands[i].manifold_start;
@@ -1023,8 +1195,9 @@ void colliders_and_sleep(Group* g, WorldH& w, float dt, const uint8_t* h_moved, 
     }
     // collidingInPreviousFrame for the next step
     for (auto& p : w.pairs) p.coll_prev = p.coll_curr;
+    for (auto& p : w.concave) p.coll_prev = p.coll_curr;
     w.prev_cpairs.swap(w.cpairs);
-    w.stats.disabled_pairs = uint32_t(w.disabled.size());
+    w.stats.disabled_pairs = uint32_t(w.disabled.size() + w.concave_dis.size());
     w.stats.enabled_bodies = w.bcomp.n_enabled;
 }
 
@@ -1067,6 +1240,60 @@ int ensure_pool(Group* g) {
 }
 
 int ensure_small(Group* g, size_t n) { return dev_grow(&g->d_small, &g->cap_small, n) ? wfail(g, RP3DG_ENOMEM, "cudaMalloc(small)") : 0; }
+
+// Per-item arrays of the convex vs concave pairs (pinned staging + device).
+int ensure_hitems(Group* g, size_t n) {
+    if (n <= g->cap_hitem && g->h_hitems) return 0;
+    const size_t c = std::max<size_t>(std::max<size_t>(n, g->cap_hitem * 2), 64);
+    cudaFreeHost(g->h_hitems); cudaFreeHost(g->h_hrect); cudaFreeHost(g->h_hstart); cudaFreeHost(g->h_hpstart);
+    cudaFreeHost(g->h_hprect); cudaFreeHost(g->h_hbatch); cudaFreeHost(g->h_hout);
+    cudaFree(g->d_hitems); cudaFree(g->d_hrect); cudaFree(g->d_hstart); cudaFree(g->d_hpstart); cudaFree(g->d_hprect);
+    cudaFree(g->d_hbatch); cudaFree(g->d_hout); cudaFree(g->d_hond); cudaFree(g->d_hol1); cudaFree(g->d_hol2);
+    g->h_hitems = g->h_hrect = g->h_hprect = g->h_hbatch = nullptr;
+    g->h_hstart = nullptr; g->h_hpstart = nullptr; g->h_hout = nullptr;
+    g->d_hitems = g->d_hrect = g->d_hprect = g->d_hbatch = nullptr;
+    g->d_hstart = nullptr; g->d_hpstart = nullptr; g->d_hout = nullptr;
+    g->d_hond = g->d_hol1 = g->d_hol2 = nullptr;
+    g->cap_hitem = 0;
+    bool ok = true;
+    auto H = [&](void** p, size_t b) { if (ok && cudaMallocHost(p, b) != cudaSuccess) ok = false; };
+    auto D = [&](void** p, size_t b) { if (ok && cudaMalloc(p, b) != cudaSuccess) ok = false; };
+    H((void**)&g->h_hitems, c * 16); H((void**)&g->h_hrect, c * 16); H((void**)&g->h_hstart, (c + 1) * 4);
+    H((void**)&g->h_hpstart, c * 4); H((void**)&g->h_hprect, c * 16); H((void**)&g->h_hbatch, c * 16);
+    H((void**)&g->h_hout, c * 6);
+    D((void**)&g->d_hitems, c * 16); D((void**)&g->d_hrect, c * 16); D((void**)&g->d_hstart, (c + 1) * 4);
+    D((void**)&g->d_hpstart, c * 4); D((void**)&g->d_hprect, c * 16); D((void**)&g->d_hbatch, c * 16);
+    D((void**)&g->d_hout, c * 6);
+    D((void**)&g->d_hond, c * HF_OUT_POINTS * 16); D((void**)&g->d_hol1, c * HF_OUT_POINTS * 16);
+    D((void**)&g->d_hol2, c * HF_OUT_POINTS * 16);
+    if (!ok) return wfail(g, RP3DG_ENOMEM, "allocation of concave-pair arrays");
+    g->cap_hitem = c;
+    return 0;
+}
+
+// Per-test arrays of the triangle tests; the record buffer of this step
+// (the previous step's buffer is kept as it is).
+int ensure_htests(Group* g, size_t n) {
+    n = std::max<size_t>(n, 1);
+    if (dev_grow(&g->d_tcache[g->cur_tc], &g->cap_hc[g->cur_tc], n))
+        return wfail(g, RP3DG_ENOMEM, "cudaMalloc(triangle records)");
+    if (n <= g->cap_htest) return 0;
+    const size_t c = std::max<size_t>(std::max<size_t>(n, g->cap_htest * 2), 256);
+    cudaFree(g->d_ts1); cudaFree(g->d_ts2); cudaFree(g->d_tp1); cudaFree(g->d_tr1); cudaFree(g->d_tp2);
+    cudaFree(g->d_tr2); cudaFree(g->d_trep); cudaFree(g->d_tcoll); cudaFree(g->d_tnct); cudaFree(g->d_tmid);
+    cudaFree(g->d_tnd); cudaFree(g->d_tl1); cudaFree(g->d_tl2); cudaFree(g->d_tri);
+    g->cap_htest = 0;
+    cudaError_t e = cudaSuccess;
+    auto M = [&](void** p, size_t b) { if (e == cudaSuccess) e = cudaMalloc(p, b); };
+    M((void**)&g->d_ts1, c * 4); M((void**)&g->d_ts2, c * 4);
+    M((void**)&g->d_tp1, c * 16); M((void**)&g->d_tr1, c * 16); M((void**)&g->d_tp2, c * 16); M((void**)&g->d_tr2, c * 16);
+    M((void**)&g->d_trep, c); M((void**)&g->d_tcoll, c); M((void**)&g->d_tnct, c); M((void**)&g->d_tmid, c * MAXC);
+    M((void**)&g->d_tnd, c * 16 * MAXC); M((void**)&g->d_tl1, c * 16 * MAXC); M((void**)&g->d_tl2, c * 16 * MAXC);
+    M((void**)&g->d_tri, c * 16 * 5);
+    if (e != cudaSuccess) return wcuda(g, e, "cudaMalloc(triangle tests)");
+    g->cap_htest = c;
+    return 0;
+}
 
 // Run f(world index) for every world on the group's host threads.
 template <class F>
@@ -1217,6 +1444,15 @@ void destroy_group(Group* g) {
     cudaFreeHost(g->h_reset);
     cudaFree(g->j_rec); cudaFree(g->d_jlist); cudaFree(g->d_ijstart); cudaFree(g->d_ijcount); cudaFree(g->d_jiisl);
     cudaFree(g->d_jibstart); cudaFree(g->d_jibcount); cudaFree(g->d_jirows);
+    cudaFreeHost(g->h_hitems); cudaFreeHost(g->h_hrect); cudaFreeHost(g->h_hstart); cudaFreeHost(g->h_hpstart);
+    cudaFreeHost(g->h_hprect); cudaFreeHost(g->h_hbatch); cudaFreeHost(g->h_hout);
+    cudaFree(g->d_hitems); cudaFree(g->d_hrect); cudaFree(g->d_hstart); cudaFree(g->d_hpstart); cudaFree(g->d_hprect);
+    cudaFree(g->d_hbatch); cudaFree(g->d_hout); cudaFree(g->d_hond); cudaFree(g->d_hol1); cudaFree(g->d_hol2);
+    cudaFree(g->d_ts1); cudaFree(g->d_ts2); cudaFree(g->d_tp1); cudaFree(g->d_tr1); cudaFree(g->d_tp2);
+    cudaFree(g->d_tr2); cudaFree(g->d_trep); cudaFree(g->d_tcoll); cudaFree(g->d_tnct); cudaFree(g->d_tmid);
+    cudaFree(g->d_tnd); cudaFree(g->d_tl1); cudaFree(g->d_tl2); cudaFree(g->d_tri);
+    cudaFree(g->d_tcache[0]); cudaFree(g->d_tcache[1]); cudaFree(g->d_hf);
+    if (g->ev_rect) cudaEventDestroy(g->ev_rect);
     cudaFreeHost(g->t_grav); cudaFreeHost(g->t_ben); cudaFreeHost(g->t_cen); cudaFreeHost(g->t_cbody);
     cudaFreeHost(g->t_cshape); cudaFreeHost(g->t_cat); cudaFreeHost(g->t_mask); cudaFreeHost(g->t_bperm);
     cudaFreeHost(g->t_cperm);
@@ -1237,6 +1473,9 @@ int build_world(Group* g, WorldH& w, const rp3dg_body_desc* bd, uint32_t nb, con
     for (uint32_t i = 0; i < nb; i++)
         if (bd[i].type < RP3DG_BODY_STATIC || bd[i].type > RP3DG_BODY_DYNAMIC)
             return cfail(g->ctx, RP3DG_EINVAL, "bad body type");
+    for (uint32_t i = 0; i < nc; i++)
+        if (g->shapes[size_t(cd[i].shape)].kind == RP3DG_SHAPE_HEIGHTFIELD && bd[cd[i].body].type != RP3DG_BODY_STATIC)
+            return cfail(g->ctx, RP3DG_EINVAL, "a height-field collider must belong to a static body");
     w.nb = nb;
     w.nc = nc;
     w.bodies.resize(nb);
@@ -1264,6 +1503,8 @@ int build_world(Group* g, WorldH& w, const rp3dg_body_desc* bd, uint32_t nb, con
             ColliderH& C = w.colliders[ci];
             C.body = int(b);
             C.shape = c.shape;
+            C.convex = g->shapes[size_t(c.shape)].kind != RP3DG_SHAPE_HEIGHTFIELD;
+            C.hf = C.convex ? -1 : g->shapes[size_t(c.shape)].mesh;
             C.category = c.category;
             C.mask = c.mask;
             w.ccomp.add(int(ci), !w.bcomp.enabled(int(b)));
@@ -1359,6 +1600,27 @@ int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds
     if (nworlds == 0) {
         destroy_group(g);
         return cfail(ctx, RP3DG_EINVAL, "no world");
+    }
+    // height fields named by the shape table, by id
+    {
+        std::vector<rp3dg::HfDesc> hfs;
+        for (const rp3dg_shape& sh : g->shapes) {
+            if (sh.kind != RP3DG_SHAPE_HEIGHTFIELD) continue;
+            if (size_t(sh.mesh) >= hfs.size()) hfs.resize(size_t(sh.mesh) + 1, rp3dg::HfDesc{});
+            if (rp3dg::get_heightfield(ctx, sh.mesh, &hfs[size_t(sh.mesh)])) {
+                destroy_group(g);
+                return cfail(ctx, RP3DG_EINVAL, "shape refers to an unknown height field");
+            }
+        }
+        if (!hfs.empty()) {
+            g->n_hf = uint32_t(hfs.size());
+            if (cudaMalloc(&g->d_hf, hfs.size() * sizeof(rp3dg::HfDesc)) != cudaSuccess ||
+                cudaMemcpy(g->d_hf, hfs.data(), hfs.size() * sizeof(rp3dg::HfDesc), cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaEventCreateWithFlags(&g->ev_rect, cudaEventDisableTiming) != cudaSuccess) {
+                destroy_group(g);
+                return cfail(ctx, RP3DG_ENOMEM, "height-field tables");
+            }
+        }
     }
     g->worlds.resize(nworlds);
     std::vector<float4> col[BC_NCOL], ccols[CC_NCOL];
@@ -1531,6 +1793,16 @@ int update_group(Group* g, float dt) {
     }
     g->batch_start[NB_ALGOS] = T;
     g->stats.narrowphase_tests = T;
+    // convex vs concave pairs, laid out the same way
+    uint32_t CI = 0;
+    for (int a = 0; a < NB_ALGOS; a++) {
+        g->hitem_start[a] = CI;
+        for (WorldH& w : g->worlds) {
+            w.hitem_off[a] = CI - g->hitem_start[a];
+            CI += uint32_t(w.hitems[a].size());
+        }
+    }
+    g->hitem_start[NB_ALGOS] = CI;
     int rc = ensure_pool(g);
     if (rc) return rc;
     sub(8);
@@ -1563,8 +1835,39 @@ int update_group(Group* g, float dt) {
             if (!w.items[a].empty())
                 std::memcpy(g->h_items + g->batch_start[a] + w.item_off[a], w.items[a].data(), w.items[a].size() * 16);
     });
-    mark(1);
     const int cc = g->cur_c;
+    // ---- middle phase of the convex vs concave pairs: the cell rectangle of
+    // each pair first (read back while the convex pairs' narrow phase runs)
+    if (CI) {
+        rc = ensure_hitems(g, CI);
+        if (rc) return rc;
+        for_worlds(g, [&](int k) {
+            WorldH& w = g->worlds[size_t(k)];
+            for (int a = 0; a < NB_ALGOS; a++)
+                if (!w.hitems[a].empty())
+                    std::memcpy(g->h_hitems + g->hitem_start[a] + w.hitem_off[a], w.hitems[a].data(),
+                                w.hitems[a].size() * 16);
+        });
+        const rp3dg_shape* d_shapes = nullptr;
+        const float4* d_bounds = nullptr;
+        rp3dg::get_shape_device(ctx, &d_shapes, &d_bounds);
+        cudaMemcpyAsync(g->d_hitems, g->h_hitems, size_t(CI) * 16, cudaMemcpyHostToDevice, st);
+        HfRectArgs ra;
+        ra.n = CI;
+        ra.items = g->d_hitems;
+        ra.c_shape = g->c_shape;
+        ra.shapes = d_shapes;
+        ra.bounds = d_bounds;
+        ra.c_wpos = g->ccol[cc][CC_WPOS];
+        ra.c_wori = g->ccol[cc][CC_WORI];
+        ra.hf = g->d_hf;
+        ra.rect = g->d_hrect;
+        cudaError_t e = launch_hf_rects(ra, st);
+        if (e != cudaSuccess) return wcuda(g, e, "height-field middle phase");
+        cudaMemcpyAsync(g->h_hrect, g->d_hrect, size_t(CI) * 16, cudaMemcpyDeviceToHost, st);
+        cudaEventRecord(g->ev_rect, st);
+    }
+    mark(1);
     if (T) {
         cudaMemcpyAsync(g->d_items, g->h_items, size_t(T) * 16, cudaMemcpyHostToDevice, st);
         GatherArgs ga;
@@ -1607,6 +1910,117 @@ int update_group(Group* g, float dt) {
         world_scatter_cache<<<blocks(T), 128, 0, st>>>(T, g->d_items, g->d_cache, g->pool);
         cudaMemcpyAsync(g->h_out, g->d_coll, T, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(g->h_out + T, g->d_nct, T, cudaMemcpyDeviceToHost, st);
+    }
+    // ---- triangle tests of the convex vs concave pairs and their manifolds
+    if (CI) {
+        cudaError_t e = cudaEventSynchronize(g->ev_rect);
+        if (e != cudaSuccess) return wcuda(g, e, "height-field middle phase");
+        // HeightField::computeOverlappingTriangles: two triangles per cell of
+        // [iMin, iMax) x [jMin, jMax); tests algorithm-major like the items
+        uint32_t TC = 0;
+        for (int a = 0; a < NB_ALGOS; a++) {
+            g->htest_start[a] = TC;
+            for (uint32_t ci = g->hitem_start[a]; ci < g->hitem_start[a + 1]; ci++) {
+                const int4 r = g->h_hrect[ci];
+                g->h_hstart[ci] = TC;
+                if (r.y > r.x && r.w > r.z) TC += 2u * uint32_t(r.y - r.x) * uint32_t(r.w - r.z);
+            }
+        }
+        g->htest_start[NB_ALGOS] = TC;
+        g->h_hstart[CI] = TC;
+        g->stats.narrowphase_tests += TC;
+        // per item: its batch, and the records of the step before (the pair
+        // keeps them only if that step tested it)
+        for (int a = 0; a < NB_ALGOS; a++) {
+            const int4 batch = make_int4(int(g->htest_start[a]), int(g->htest_start[a + 1] - g->htest_start[a]), 0, 0);
+            for (WorldH& w : g->worlds) {
+                const uint32_t base = g->hitem_start[a] + w.hitem_off[a];
+                for (uint32_t i = 0; i < w.hitems[a].size(); i++) {
+                    const uint32_t ci = base + i;
+                    PairH& p = w.concave[w.hitem_pair[a][i]];
+                    g->h_hbatch[ci] = batch;
+                    g->h_hpstart[ci] = p.rec_valid ? p.rec_start : -1;
+                    g->h_hprect[ci] = p.rec_rect;
+                    p.rec_valid = true;
+                    p.rec_start = int(g->h_hstart[ci]);
+                    p.rec_rect = g->h_hrect[ci];
+                }
+            }
+        }
+        rc = ensure_htests(g, TC);
+        if (rc) return rc;
+        cudaMemcpyAsync(g->d_hstart, g->h_hstart, size_t(CI + 1) * 4, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->d_hbatch, g->h_hbatch, size_t(CI) * 16, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->d_hpstart, g->h_hpstart, size_t(CI) * 4, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->d_hprect, g->h_hprect, size_t(CI) * 16, cudaMemcpyHostToDevice, st);
+        const int cur = g->cur_tc;
+        if (TC) {
+            HfTestArgs ta;
+            ta.n_items = CI;
+            ta.n_tests = TC;
+            ta.items = g->d_hitems;
+            ta.rect = g->d_hrect;
+            ta.start = g->d_hstart;
+            ta.batch = g->d_hbatch;
+            ta.prev_start = g->d_hpstart;
+            ta.prev_rect = g->d_hprect;
+            ta.c_shape = g->c_shape;
+            ta.c_wpos = g->ccol[cc][CC_WPOS];
+            ta.c_wori = g->ccol[cc][CC_WORI];
+            ta.hf = g->d_hf;
+            ta.prev_cache = g->d_tcache[1 - cur];
+            ta.s1 = g->d_ts1; ta.s2 = g->d_ts2;
+            ta.p1 = g->d_tp1; ta.r1 = g->d_tr1; ta.p2 = g->d_tp2; ta.r2 = g->d_tr2;
+            ta.report = g->d_trep;
+            ta.cache = g->d_tcache[cur];
+            ta.tri = g->d_tri;
+            e = launch_hf_tests(ta, st);
+            if (e != cudaSuccess) return wcuda(g, e, "height-field triangles");
+            for (int a = 0; a < NB_ALGOS; a++) {
+                const uint32_t s0 = g->htest_start[a], n = g->htest_start[a + 1] - s0;
+                if (!n) continue;
+                rp3dg_pair_batch pb{};
+                pb.n = n;
+                pb.shape1 = g->d_ts1 + s0; pb.shape2 = g->d_ts2 + s0;
+                pb.pos1 = reinterpret_cast<rp3dg_float4*>(g->d_tp1 + s0);
+                pb.rot1 = reinterpret_cast<rp3dg_float4*>(g->d_tr1 + s0);
+                pb.pos2 = reinterpret_cast<rp3dg_float4*>(g->d_tp2 + s0);
+                pb.rot2 = reinterpret_cast<rp3dg_float4*>(g->d_tr2 + s0);
+                pb.report_contacts = g->d_trep + s0;
+                pb.cache = g->d_tcache[cur] + s0;
+                rp3dg_contact_batch cbt{};
+                cbt.is_colliding = g->d_tcoll + s0;
+                cbt.nb_contacts = g->d_tnct + s0;
+                cbt.normal_depth = reinterpret_cast<rp3dg_float4*>(g->d_tnd + size_t(s0) * MAXC);
+                cbt.local1 = reinterpret_cast<rp3dg_float4*>(g->d_tl1 + size_t(s0) * MAXC);
+                cbt.local2 = reinterpret_cast<rp3dg_float4*>(g->d_tl2 + size_t(s0) * MAXC);
+                cbt.max_contacts = MAXC;
+                rc = rp3dg::narrowphase_tri_device(ctx, a + 1, &pb, &cbt, g->d_tri + 5 * size_t(s0));
+                if (rc) return rc;
+            }
+        }
+        HfManifoldArgs ma;
+        ma.n_items = CI;
+        ma.items = g->d_hitems;
+        ma.start = g->d_hstart;
+        ma.batch = g->d_hbatch;
+        ma.c_wori = g->ccol[cc][CC_WORI];
+        ma.cos_similar = g->set.cos_angle_similar_contact_manifold;
+        ma.is_colliding = g->d_tcoll;
+        ma.nb_contacts = g->d_tnct;
+        ma.nd = g->d_tnd; ma.l1 = g->d_tl1; ma.l2 = g->d_tl2;
+        ma.cache = g->d_tcache[cur];
+        ma.mid = g->d_tmid;
+        ma.out_coll = g->d_hout;
+        ma.out_nman = g->d_hout + CI;
+        ma.out_npts = reinterpret_cast<uchar4*>(g->d_hout + 2 * size_t(CI));
+        ma.out_nd = g->d_hond; ma.out_l1 = g->d_hol1; ma.out_l2 = g->d_hol2;
+        e = launch_hf_manifolds(ma, st);
+        if (e != cudaSuccess) return wcuda(g, e, "concave manifolds");
+        cudaMemcpyAsync(g->h_hout, g->d_hout, size_t(CI) * 6, cudaMemcpyDeviceToHost, st);
+    }
+    g->cur_tc = 1 - g->cur_tc;
+    if (T || CI) {
         cudaError_t e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return wcuda(g, e, "narrow phase");
     }
@@ -1614,7 +2028,12 @@ int update_group(Group* g, float dt) {
     // ---- contact pairs and islands of every world
     const uint8_t* h_coll = g->h_out;
     const uint8_t* h_count = g->h_out + T;
-    for_worlds(g, [&](int k) { contacts_and_islands(g, g->worlds[size_t(k)], h_coll, h_count); });
+    const uint8_t* h_hcoll = g->h_hout;
+    const uint8_t* h_hnman = g->h_hout + CI;
+    const uint8_t* h_hnpts = g->h_hout + 2 * size_t(CI);
+    for_worlds(g, [&](int k) {
+        contacts_and_islands(g, g->worlds[size_t(k)], h_coll, h_count, h_hcoll, h_hnman, h_hnpts);
+    });
     uint32_t NM = 0, NP = 0, NI = 0;
     for (WorldH& w : g->worlds) {
         w.man_base = NM;
@@ -1712,6 +2131,7 @@ int update_group(Group* g, float dt) {
         a.prev = g->d_mprev;
         a.kept_count = g->d_nct;
         a.b_nd = g->d_nd; a.b_l1 = g->d_l1; a.b_l2 = g->d_l2;
+        a.c_nd = g->d_hond; a.c_l1 = g->d_hol1; a.c_l2 = g->d_hol2;
         a.cos_similar = g->set.cos_angle_similar_contact_manifold;
         a.persist2 = g->set.persistent_contact_distance_threshold * g->set.persistent_contact_distance_threshold;
         a.pm_pstart = PB.pstart; a.pm_fv1 = PB.fv1; a.pm_fv2 = PB.fv2; a.pm_fimp = PB.fimp;
@@ -1848,7 +2268,7 @@ int update_group(Group* g, float dt) {
     g->cur_cb = 1 - g->cur_cb;
     for (WorldH& w : g->worlds) {
         w.stepped = true;
-        g->stats.overlapping_pairs += uint32_t(w.pairs.size());
+        g->stats.overlapping_pairs += uint32_t(w.pairs.size() + w.concave.size());
         g->stats.disabled_pairs += w.stats.disabled_pairs;
         g->stats.enabled_bodies += w.stats.enabled_bodies;
         g->stats.moved_colliders += w.stats.moved_colliders;
@@ -2064,6 +2484,8 @@ int rp3dg_world_group_get_pairs(rp3dg_world* g, uint32_t world, uint64_t* ids, u
     uint32_t k = 0;
     for (const auto& p : w.pairs) { if (ids && k < capacity) ids[k] = p.id; k++; }
     for (const auto& p : w.disabled) { if (ids && k < capacity) ids[k] = p.id; k++; }
+    for (const auto& p : w.concave) { if (ids && k < capacity) ids[k] = p.id; k++; }
+    for (const auto& p : w.concave_dis) { if (ids && k < capacity) ids[k] = p.id; k++; }
     *n = k;
     return 0;
 }

@@ -61,6 +61,8 @@ def load_library(path=LIB_PATH):
                                                  C.POINTER(C.c_int32)]
     L.rp3dg_get_convex_mesh_tables.argtypes = [P, C.c_int32] + [P] * 7 + [C.c_uint32, C.c_uint32]
     L.rp3dg_set_shapes.argtypes = [P, P, C.c_uint32]
+    L.rp3dg_create_heightfield.argtypes = [P, C.c_uint32, C.c_uint32, P, C.c_float, C.c_float, C.c_float,
+                                           C.POINTER(C.c_int32)]
     L.rp3dg_device_errors.argtypes = [P, C.POINTER(C.c_uint32), C.c_int]
     L.rp3dg_narrowphase_device.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_int]
     L.rp3dg_narrowphase_host.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_int]
@@ -236,6 +238,28 @@ class Context:
         out = C.c_int32()
         self._check(self.lib.rp3dg_create_convex_mesh_shape(self.h, mesh, *map(float, scale), C.byref(out)))
         return out.value
+
+    def create_heightfield(self, heights, scale=(1.0, 1.0, 1.0)):
+        """Height field from an (nb_rows, nb_columns) float32 grid (row y
+        along local Z, column x along local X); returns the id for
+        rp3dg_shape.mesh with kind SHAPE_HEIGHTFIELD."""
+        h = np.ascontiguousarray(heights, dtype=np.float32)
+        assert h.ndim == 2
+        out = C.c_int32()
+        self._check(self.lib.rp3dg_create_heightfield(self.h, h.shape[1], h.shape[0], h.ctypes.data,
+                                                      *map(float, scale), C.byref(out)))
+        return out.value
+
+    def scene_shapes(self, scene):
+        """The scene's shape table with its height fields created in this
+        context (scene.heightfields: list of (heights, scale); a height-field
+        shape's mesh field indexes that list)."""
+        shapes = np.array(scene.shapes, copy=True)
+        hfs = getattr(scene, "heightfields", None) or []
+        ids = [self.create_heightfield(h, s) for (h, s) in hfs]
+        for i in np.nonzero(shapes["kind"] == A.SHAPE_HEIGHTFIELD)[0]:
+            shapes["mesh"][i] = ids[int(shapes["mesh"][i])]
+        return shapes
 
     def mesh_tables(self, instance, cap=4096):
         nv, nf, nh = C.c_uint32(), C.c_uint32(), C.c_uint32()
@@ -437,7 +461,7 @@ class World:
 
     def __init__(self, ctx, scene):
         self.ctx, self.lib = ctx, ctx.lib
-        ctx.set_shapes(scene.shapes)
+        ctx.set_shapes(ctx.scene_shapes(scene))
         self.nb = len(scene.bodies)
         self._keep = (np.ascontiguousarray(scene.settings).copy(), np.ascontiguousarray(scene.bodies),
                       np.ascontiguousarray(scene.colliders))

@@ -187,9 +187,12 @@ class WorldScene:
     """A world description: settings, shape table, bodies, colliders and
     joints (numpy structured arrays with the layouts of include/rp3dg.h)."""
 
-    def __init__(self, settings, shapes, bodies, colliders, name="", joints=None):
+    def __init__(self, settings, shapes, bodies, colliders, name="", joints=None, heightfields=None):
         self.settings, self.shapes, self.bodies, self.colliders, self.name = settings, shapes, bodies, colliders, name
         self.joints = joints
+        # height fields: list of (heights (nb_rows, nb_columns) float32, scale);
+        # a SHAPE_HEIGHTFIELD shape's mesh field indexes this list
+        self.heightfields = heightfields or []
 
 
 def box_pile(nx=10, ny=10, nz=10, seed=1, spacing=2.0, base=2.0, jitter=0.1):
@@ -468,3 +471,79 @@ def ragdoll_world(n_ragdolls=2, seed=21, limits=True, boxes=0):
     colliders["bounciness"] = 0.0
     return WorldScene(A.default_world_settings(), shapes, bodies, colliders,
                       f"ragdolls {n_ragdolls}", np.array(joints, dtype=A.JOINT_DESC_DTYPE))
+
+
+def sine_heights(cols, rows, seed=3, n_waves=8, amplitude=2.0, k_range=(0.05, 0.5), cell=1.0):
+    """A height grid (rows, cols) of `n_waves` sines with random directions,
+    wave numbers |k| in k_range (rad per metre) and phases, whose amplitudes
+    sum to `amplitude` metres; computed in float64, stored as float32."""
+    rng = np.random.default_rng(seed)
+    x = np.arange(cols) * cell
+    z = np.arange(rows) * cell
+    X, Z = np.meshgrid(x, z)
+    h = np.zeros((rows, cols))
+    for _ in range(n_waves):
+        k = rng.uniform(*k_range)
+        th = rng.uniform(0.0, 2.0 * np.pi)
+        ph = rng.uniform(0.0, 2.0 * np.pi)
+        h += (amplitude / n_waves) * np.sin(k * (np.cos(th) * X + np.sin(th) * Z) + ph)
+    return h.astype(np.float32)
+
+
+def heightfield_world(n_bodies=1000, cols=64, rows=64, cell=1.0, seed=5, spacing=1.5, amplitude=2.0,
+                      sleeping=True, y_scale=1.0, terrain_position=(0.0, 0.0, 0.0), terrain_orientation=None):
+    """Bodies over a static height-field terrain: n_bodies dynamic bodies,
+    40% boxes (half-extents U[0.2, 0.6]), 30% spheres (radius U[0.2, 0.5]),
+    30% capsules (radius 0.2, half-height 0.3), on a jittered 3-D lattice with
+    `spacing` metres between centres above a cols x rows height field of
+    `cell`-metre cells whose heights are sine_heights (total amplitude
+    `amplitude`).  Body 0 is the terrain (a static body at the origin whose
+    collider is the height field, scaled by (cell, y_scale, cell), placed at
+    terrain_position with terrain_orientation (x, y, z, w), identity by
+    default).  Density 1, friction 0.3, gravity -9.81."""
+    rng = np.random.default_rng(seed)
+    heights = sine_heights(cols, rows, seed=seed + 1000, amplitude=amplitude, cell=cell)
+    n = n_bodies
+    shapes = np.zeros(n + 1, A.SHAPE_DTYPE)
+    shapes["mesh"] = -1
+    shapes[0]["kind"] = A.SHAPE_HEIGHTFIELD
+    shapes[0]["mesh"] = 0
+    u = rng.uniform(size=n)
+    kinds = np.where(u < 0.4, A.SHAPE_BOX, np.where(u < 0.7, A.SHAPE_SPHERE, A.SHAPE_CAPSULE))
+    shapes["kind"][1:] = kinds
+    box = kinds == A.SHAPE_BOX
+    sph = kinds == A.SHAPE_SPHERE
+    cap = kinds == A.SHAPE_CAPSULE
+    p = shapes["params"][1:]
+    p[box, :3] = rng.uniform(0.2, 0.6, size=(int(box.sum()), 3))
+    p[sph, 0] = rng.uniform(0.2, 0.5, size=int(sph.sum()))
+    p[cap, 0] = 0.2
+    p[cap, 1] = 0.3
+    shapes["params"][1:] = p
+    bodies = A.body_descs(n + 1)
+    bodies[0]["type"] = A.BODY_STATIC
+    bodies[0]["position"] = terrain_position
+    if terrain_orientation is not None:
+        bodies[0]["orientation"] = terrain_orientation
+    # lattice over the terrain, 1 m inside its border, layers upwards
+    width, length = (cols - 1) * cell, (rows - 1) * cell
+    nx = max(1, int((width - 2.0) // spacing) + 1)
+    nz = max(1, int((length - 2.0) // spacing) + 1)
+    per_layer = nx * nz
+    idx = np.arange(n)
+    iy, rem = idx // per_layer, idx % per_layer
+    ix, iz = rem % nx, rem // nx
+    top = float(heights.max() - heights.min()) * 0.5 * y_scale + float(terrain_position[1])
+    centre = np.stack([(ix - 0.5 * (nx - 1)) * spacing, top + 1.5 + iy * spacing,
+                       (iz - 0.5 * (nz - 1)) * spacing], axis=1) + rng.uniform(-0.1, 0.1, size=(n, 3))
+    bodies["position"][1:] = centre.astype(np.float32)
+    bodies["orientation"][1:] = random_quaternions(rng, n)
+    colliders = A.collider_descs(n + 1)
+    colliders["body"] = np.arange(n + 1)
+    colliders["shape"] = np.arange(n + 1)
+    colliders["friction"] = np.float32(0.3)
+    colliders["bounciness"] = 0.0
+    settings = A.default_world_settings()
+    settings["sleeping_enabled"] = 1 if sleeping else 0
+    return WorldScene(settings, shapes, bodies, colliders, f"heightfield {cols}x{rows} + {n}",
+                      heightfields=[(heights, (cell, y_scale, cell))])

@@ -280,7 +280,17 @@ class RefScene:
         L.ref_scene_contacts.restype = C.c_long
         L.ref_world_step.argtypes = [C.c_int, C.c_float, C.c_int]
         L.ref_scene_add_joints.argtypes = [C.c_int, P, C.c_uint32]
-        self._keep = (np.ascontiguousarray(scene.settings).copy(), np.ascontiguousarray(scene.shapes),
+        L.ref_heightfield_register.argtypes = [C.c_uint32, C.c_uint32, P, C.c_float, C.c_float, C.c_float]
+        # height fields of the scene registered with the harness; the shape
+        # table's mesh field then names the harness's ids
+        shapes = np.array(scene.shapes, copy=True)
+        hf_ids = []
+        for heights, scale in getattr(scene, "heightfields", None) or []:
+            h = np.ascontiguousarray(heights, dtype=np.float32)
+            hf_ids.append(L.ref_heightfield_register(h.shape[1], h.shape[0], h.ctypes.data, *map(float, scale)))
+        for i in np.nonzero(shapes["kind"] == A.SHAPE_HEIGHTFIELD)[0]:
+            shapes["mesh"][i] = hf_ids[int(shapes["mesh"][i])]
+        self._keep = (np.ascontiguousarray(scene.settings).copy(), np.ascontiguousarray(shapes),
                       np.ascontiguousarray(scene.bodies), np.ascontiguousarray(scene.colliders))
         st, sh, bd, cd = self._keep
         self.id = L.ref_scene_create(st.ctypes.data, sh.ctypes.data, len(sh), bd.ctypes.data, len(bd),

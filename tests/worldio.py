@@ -13,6 +13,13 @@ WORLD_CASES = {
     "pile125": (scenes.box_pile, dict(nx=5, ny=5, nz=5, seed=3), 240, 60),
     "mixed100": (scenes.mixed_world, dict(nx=5, ny=4, nz=5, seed=5), 200, 50),
     "ragdolls4": (scenes.ragdoll_world, dict(n_ragdolls=4, seed=23, limits=False, boxes=6), 240, 60),
+    # boxes, spheres and capsules falling onto a height-field terrain
+    "terrain60": (scenes.heightfield_world, dict(n_bodies=60, cols=24, rows=24, seed=11), 240, 60),
+    # a scaled terrain on a tilted, shifted static body
+    "terrain_tilt": (scenes.heightfield_world,
+                     dict(n_bodies=40, cols=18, rows=21, cell=1.25, y_scale=0.7, seed=12,
+                          terrain_position=(0.5, -0.3, 0.25),
+                          terrain_orientation=(0.0499792, 0.0, 0.0299875, 0.9983002)), 200, 50),
 }
 DT = np.float32(1.0 / 60.0)
 
