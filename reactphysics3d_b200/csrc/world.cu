@@ -583,7 +583,7 @@ struct rp3dg_world {
     uint32_t *h_hstart = nullptr, *d_hstart = nullptr;
     int32_t *h_hpstart = nullptr, *d_hpstart = nullptr;
     int4 *h_hprect = nullptr, *d_hprect = nullptr, *h_hbatch = nullptr, *d_hbatch = nullptr;
-    uint8_t *h_hout = nullptr, *d_hout = nullptr;  // colliding (n), manifolds (n), points per manifold (4n)
+    uint8_t *h_hout = nullptr, *d_hout = nullptr;  // points per manifold (4n, uchar4), colliding (n), manifolds (n)
     float4 *d_hond = nullptr, *d_hol1 = nullptr, *d_hol2 = nullptr;
     int32_t *d_ts1 = nullptr, *d_ts2 = nullptr;
     float4 *d_tp1 = nullptr, *d_tr1 = nullptr, *d_tp2 = nullptr, *d_tr2 = nullptr;
@@ -2011,9 +2011,10 @@ int update_group(Group* g, float dt) {
         ma.nd = g->d_tnd; ma.l1 = g->d_tl1; ma.l2 = g->d_tl2;
         ma.cache = g->d_tcache[cur];
         ma.mid = g->d_tmid;
-        ma.out_coll = g->d_hout;
-        ma.out_nman = g->d_hout + CI;
-        ma.out_npts = reinterpret_cast<uchar4*>(g->d_hout + 2 * size_t(CI));
+        // the uchar4 counts first: 4-byte aligned whatever CI is
+        ma.out_npts = reinterpret_cast<uchar4*>(g->d_hout);
+        ma.out_coll = g->d_hout + 4 * size_t(CI);
+        ma.out_nman = g->d_hout + 5 * size_t(CI);
         ma.out_nd = g->d_hond; ma.out_l1 = g->d_hol1; ma.out_l2 = g->d_hol2;
         e = launch_hf_manifolds(ma, st);
         if (e != cudaSuccess) return wcuda(g, e, "concave manifolds");
@@ -2028,9 +2029,9 @@ int update_group(Group* g, float dt) {
     // ---- contact pairs and islands of every world
     const uint8_t* h_coll = g->h_out;
     const uint8_t* h_count = g->h_out + T;
-    const uint8_t* h_hcoll = g->h_hout;
-    const uint8_t* h_hnman = g->h_hout + CI;
-    const uint8_t* h_hnpts = g->h_hout + 2 * size_t(CI);
+    const uint8_t* h_hnpts = g->h_hout;
+    const uint8_t* h_hcoll = g->h_hout + 4 * size_t(CI);
+    const uint8_t* h_hnman = g->h_hout + 5 * size_t(CI);
     for_worlds(g, [&](int k) {
         contacts_and_islands(g, g->worlds[size_t(k)], h_coll, h_count, h_hcoll, h_hnman, h_hnpts);
     });
@@ -2504,14 +2505,17 @@ int rp3dg_world_group_get_contacts(rp3dg_world* g, uint32_t world, int32_t* body
     const std::vector<ContactPairH>& cps = w.prev_cpairs;
     if (nb_manifolds) *nb_manifolds = w.nm;
     if (nb_contact_points) *nb_contact_points = w.np;
-    std::vector<uint32_t> order(w.nm);
+    // manifold -> (contact pair, manifold of the pair): a convex vs concave
+    // pair owns up to four consecutive manifolds
+    std::vector<std::pair<uint32_t, uint32_t>> order(w.nm, std::make_pair(0u, 0u));
     for (uint32_t i = 0; i < cps.size(); i++)
-        if (cps[i].in_island) order[cps[i].manifold - w.man_base] = i;
+        if (cps[i].in_island)
+            for (uint32_t q = 0; q < cps[i].nman; q++) order[cps[i].manifold - w.man_base + q] = std::make_pair(i, q);
     for (uint32_t m = 0; m < w.nm && m < capacity; m++) {
-        const ContactPairH& c = cps[order[m]];
+        const ContactPairH& c = cps[order[m].first];
         if (body1) body1[m] = c.b1;
         if (body2) body2[m] = c.b2;
-        if (nb_points) nb_points[m] = uint8_t(c.k);
+        if (nb_points) nb_points[m] = uint8_t(c.concave ? (c.npts >> (8 * order[m].second)) & 0xffu : c.k);
     }
     const uint32_t np = std::min(w.np, capacity_points);
     if (np) {

@@ -61,6 +61,45 @@ def test_box_pile_1000_matches_reference_live(ctx):
     w.close()
 
 
+@pytest.mark.skipif(not reflib.have_ref("f32"), reason="reference engine not built")
+def test_terrain_world_matches_reference_live(ctx):
+    """400 boxes, spheres and capsules falling onto a 40 x 40 height field
+    (300 steps at 1/60 s): the convex vs concave pairs, their triangle tests
+    and up to four manifolds per pair give pair arrays, manifolds, points
+    and final states bit-identical to the reference."""
+    sc = scenes.heightfield_world(n_bodies=400, cols=40, rows=40, seed=21)
+    w, r = engine.World(ctx, sc), reflib.RefScene(sc)
+    multi = 0
+    for s in range(300):
+        w.update(float(worldio.DT))
+        r.update(float(worldio.DT))
+        if s % 25 == 24 or s == 299:
+            assert np.array_equal(w.pairs(), r.pairs()), s
+            cw, cr = w.contacts(), r.contacts()
+            for a, b in zip(cw, cr):
+                assert np.array_equal(a, b), s
+            b1, b2 = cw[0], cw[1]
+            keys = b1.astype(np.int64) * 100000 + b2
+            multi = max(multi, len(keys) - len(np.unique(keys)))
+    for a, b in zip(w.bodies(), r.bodies()):
+        assert np.array_equal(a, b)
+    assert multi > 0                    # some terrain pairs carried several manifolds
+    assert w.bodies()[4].sum() > 0      # bodies come to rest on the terrain
+    w.close()
+
+
+def test_heightfield_rejects_bad_input(ctx):
+    with pytest.raises(engine.Rp3dgError):
+        ctx.create_heightfield(np.zeros((1, 5), np.float32))          # fewer than two rows
+    with pytest.raises(engine.Rp3dgError):
+        ctx.create_heightfield(np.zeros((4, 4), np.float32), scale=(1.0, 0.0, 1.0))
+    sc = scenes.heightfield_world(n_bodies=4, cols=8, rows=8)
+    bad = scenes.WorldScene(sc.settings, sc.shapes, sc.bodies.copy(), sc.colliders, heightfields=sc.heightfields)
+    bad.bodies["type"][0] = A.BODY_DYNAMIC
+    with pytest.raises(engine.Rp3dgError):
+        engine.World(ctx, bad)          # a height field must be on a static body
+
+
 def test_world_create_rejects_bad_input(ctx):
     sc = scenes.box_pile(2, 2, 2)
     bad = scenes.WorldScene(sc.settings, sc.shapes, sc.bodies, sc.colliders[::-1].copy())
