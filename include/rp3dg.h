@@ -539,9 +539,9 @@ typedef struct rp3dg_joint_desc {
 typedef struct rp3dg_world rp3dg_world;
 
 typedef struct rp3dg_world_stats {
-    uint32_t overlapping_pairs;    /* enabled convex overlapping pairs after the broad phase */
+    uint32_t overlapping_pairs;    /* enabled overlapping pairs (convex and convex vs concave) after the broad phase */
     uint32_t disabled_pairs;       /* pairs of two sleeping / static bodies */
-    uint32_t narrowphase_tests;    /* pairs tested by the narrow phase this step */
+    uint32_t narrowphase_tests;    /* narrow-phase tests this step (pairs and height-field triangles) */
     uint32_t contact_pairs;        /* colliding pairs */
     uint32_t manifolds;            /* contact manifolds given to the solver */
     uint32_t contact_points;

@@ -1145,6 +1145,187 @@ RD void giant_solve(const DynArgs& a, uint32_t m0, uint32_t cnt, const GiantStag
     __syncthreads();
 }
 
+// ---- islands too large for shared memory: streamed ---------------------
+//
+// The level schedule is built by warp 0 in global scratch, 32 manifolds at a
+// time: the lanes load their manifolds' bodies and the bodies' last levels in
+// parallel, then a 32-step shuffle scan settles the dependencies inside the
+// chunk in manifold order (a manifold's level is one more than the latest
+// level of its movable bodies, exactly as the sequential rule).  A stable
+// counting sort by level follows (histogram, scan, scatter with per-level
+// ranks from __match_any_sync).  The solve is the giant pipeline with the
+// island state left in global memory: warp 1 stages the constant rows of up
+// to 32 manifolds per level two levels ahead, warp 0 solves each level from
+// the ring with the velocities and impulses read from and written to global
+// memory; both warps meet at the named barrier once per level.
+constexpr uint32_t STREAM_RING = 32;
+
+// Warp 0: levels and the level-ordered manifolds of an island.  Writes
+// a.order[m0 + i] (island-relative manifold indices in level order) and
+// a.level[m0 + L] = end of level L in that order; returns the depth.
+RD uint32_t stream_schedule(const DynArgs& a, uint32_t m0, uint32_t cnt, uint32_t lane) {
+    uint32_t* __restrict__ ord = a.order + m0;
+    uint32_t* __restrict__ lev = a.level + m0;
+    uint32_t* __restrict__ blev = a.body_level;
+    for (uint32_t k = lane; k < cnt; k += 32) {
+        const int4 id = man_ids(a, m0 + k);
+        if (id.z == 0) continue;
+        const uint32_t fixed = man_fixed(a, m0 + k);
+        if (!(fixed & 1)) blev[id.x] = 0;
+        if (!(fixed & 2)) blev[id.y] = 0;
+    }
+    __syncwarp();
+    uint32_t depth = 0;
+    for (uint32_t base = 0; base < cnt; base += 32) {
+        const uint32_t k = base + lane;
+        int32_t b1 = -1, b2 = -1;
+        if (k < cnt) {
+            const int4 id = man_ids(a, m0 + k);
+            if (id.z != 0) {
+                const uint32_t fixed = man_fixed(a, m0 + k);
+                b1 = (fixed & 1) ? -1 : id.x;
+                b2 = (fixed & 2) ? -1 : id.y;
+            }
+        }
+        uint32_t l1 = b1 >= 0 ? blev[b1] : 0u, l2 = b2 >= 0 ? blev[b2] : 0u, L = 1;
+        bool last1 = true, last2 = true;
+        for (uint32_t j = 0; j < 32; j++) {
+            if (lane == j) L = 1 + (l1 > l2 ? l1 : l2);
+            const uint32_t Lj = __shfl_sync(0xffffffffu, L, int(j));
+            const int32_t c1 = __shfl_sync(0xffffffffu, b1, int(j)), c2 = __shfl_sync(0xffffffffu, b2, int(j));
+            const bool m1 = b1 >= 0 && (b1 == c1 || b1 == c2), m2 = b2 >= 0 && (b2 == c1 || b2 == c2);
+            if (lane > j) {
+                if (m1) l1 = Lj;
+                if (m2) l2 = Lj;
+            } else if (lane < j) {
+                if (m1) last1 = false;
+                if (m2) last2 = false;
+            }
+        }
+        if (k < cnt) {
+            if (b1 >= 0 && last1) blev[b1] = L;
+            if (b2 >= 0 && last2) blev[b2] = L;
+            // the level, kept in the record's spare word until the scatter
+            a.mrec[m0 + k].mut.w = __int_as_float(int32_t(L));
+            depth = L > depth ? L : depth;
+        }
+        __syncwarp();
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const uint32_t d = __shfl_xor_sync(0xffffffffu, depth, o);
+        depth = d > depth ? d : depth;
+    }
+    // counting sort by level, stable in manifold order
+    for (uint32_t L = lane; L < depth; L += 32) lev[L] = 0;
+    __syncwarp();
+    for (uint32_t k = lane; k < cnt; k += 32)
+        atomicAdd(lev + (uint32_t(__float_as_int(a.mrec[m0 + k].mut.w)) - 1), 1u);
+    __syncwarp();
+    uint32_t run = 0;
+    for (uint32_t base = 0; base < depth; base += 32) {
+        const uint32_t L = base + lane;
+        const uint32_t v = L < depth ? lev[L] : 0u;
+        uint32_t inc = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= uint32_t(o)) inc += t;
+        }
+        if (L < depth) lev[L] = run + inc - v;   // first position of level L
+        run += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    __syncwarp();
+    const uint32_t lt = (1u << lane) - 1u;
+    for (uint32_t base = 0; base < cnt; base += 32) {
+        const uint32_t k = base + lane;
+        const uint32_t L = k < cnt ? uint32_t(__float_as_int(a.mrec[m0 + k].mut.w)) : 0u;
+        const uint32_t key = k < cnt ? L : (0x80000000u | lane);
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        const uint32_t pos = k < cnt ? lev[L - 1] + uint32_t(__popc(peers & lt)) : 0u;
+        __syncwarp();
+        if (k < cnt) {
+            ord[pos] = k;
+            // the lowest lane of a level advances its cursor past the chunk's peers
+            if ((peers & lt) == 0) lev[L - 1] += uint32_t(__popc(peers));
+        }
+        __syncwarp();
+    }
+    // lev[L] is now the end of level L
+    return depth;
+}
+
+// Warp 1: stage the manifolds of linearised level t (passes x levels).
+RD void stream_stage_level(const DynArgs& a, GiantSlot* ring, uint32_t m0, uint32_t depth, uint32_t total,
+                           uint32_t t, uint32_t lane) {
+    if (t < total) {
+        const uint32_t L = t % depth;
+        const uint32_t b = L ? a.level[m0 + L - 1] : 0u, e = a.level[m0 + L];
+        const uint32_t j = b + lane;
+        if (lane < STREAM_RING && j < e) {
+            const uint32_t kk = a.order[m0 + j];
+            const int4 id = man_ids(a, m0 + kk);
+            const uint32_t np = id.z < 0 ? 0u : (id.z > 4 ? 4u : uint32_t(id.z));
+            GiantSlot* sl = ring + (t % GIANT_LEVELS) * STREAM_RING + lane;
+            sl->desc = make_int4(0, int(np), int(kk), id.w);
+            const float4* src = a.mrec[m0 + kk].q;
+            for (int r = 0; r < DQ_ROWS; r++) cp_async16(&sl->mq[r], src + r);
+            const float4* ps = a.prec[id.w].q;
+            for (uint32_t r = 0; r < np * PREC_F4; r++) cp_async16(&sl->pq[r], ps + r);
+        }
+    }
+    cp_async_commit();
+}
+
+// Both warps: warm start and velocity iterations of a scheduled island.
+RD void stream_solve(const DynArgs& a, uint32_t m0, GiantSlot* ring, uint32_t warp, uint32_t lane, uint32_t depth) {
+    const uint32_t total = uint32_t(a.iterations + 1) * depth;
+    if (warp == 1) {
+        stream_stage_level(a, ring, m0, depth, total, 0, lane);
+        stream_stage_level(a, ring, m0, depth, total, 1, lane);
+        cp_async_wait<1>();
+        giant_bar();
+        for (uint32_t t = 0; t < total; t++) {
+            stream_stage_level(a, ring, m0, depth, total, t + 2, lane);
+            cp_async_wait<1>();
+            giant_bar();
+        }
+        cp_async_wait<0>();
+    } else {
+        const float beta = a.split ? BETA_SPLIT_IMPULSE : BETA;
+        giant_bar();
+        for (uint32_t t = 0; t < total; t++) {
+            const uint32_t L = t % depth;
+            const bool warm = t < depth;
+            const uint32_t b = L ? a.level[m0 + L - 1] : 0u, e = a.level[m0 + L];
+            if (lane < STREAM_RING && b + lane < e) {
+                const GiantSlot* sl = ring + (t % GIANT_LEVELS) * STREAM_RING + lane;
+                const int4 d = sl->desc;
+                const float4 ids = sl->mq[DQ_IDS];
+                const BodyVel bv = vel_global(a, __float_as_int(ids.x), __float_as_int(ids.y));
+                RecSrc r;
+                r.mq = sl->mq;
+                r.pq = sl->pq;
+                r.pq_stride = PREC_F4;
+                r.mmut = &a.mrec[m0 + uint32_t(d.z)].mut;
+                r.pmut = &a.prec[d.w].mut;
+                r.pmut_stride = PREC_F4;
+                if (warm) warm_core<false>(a, r, bv, d.y);
+                else solve_core<false>(a, r, beta, bv, d.y);
+            }
+            // manifolds of a level beyond the ring read their rows from global memory
+            for (uint32_t j = b + STREAM_RING + lane; j < e; j += 32) {
+                const uint32_t mi = m0 + a.order[m0 + j];
+                const int4 id = man_ids(a, mi);
+                const BodyVel bv = vel_global(a, id.x, id.y);
+                if (warm) warm_core<true>(a, rec_global(a, mi, id.w), bv, id.z);
+                else solve_core<true>(a, rec_global(a, mi, id.w), beta, bv, id.z);
+            }
+            __syncwarp();
+            giant_bar();
+        }
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(GIANT_THREADS, 1) dyn_islands_giant(const DynArgs a) {
     extern __shared__ __align__(16) unsigned char gsm[];
     __shared__ uint32_t s_island, s_ok, s_depth, s_nslots, s_p0;
@@ -1171,6 +1352,13 @@ __global__ void __launch_bounds__(GIANT_THREADS, 1) dyn_islands_giant(const DynA
                 giant_layout(a, cnt, uint32_t(int64_t(l.w) + int64_t(l.z) - int64_t(s_p0)), gsm, g);
             }
             giant_solve(a, m0, cnt, g, warp, lane, s_depth, s_nslots, s_p0);
+        } else if (size_t(GIANT_LEVELS) * STREAM_RING * sizeof(GiantSlot) <= a.giant_smem) {
+            if (warp == 0) {
+                const uint32_t depth = stream_schedule(a, m0, cnt, lane);
+                if (lane == 0) s_depth = depth;
+            }
+            __syncthreads();
+            stream_solve(a, m0, reinterpret_cast<GiantSlot*>(gsm), warp, lane, s_depth);
         } else if (warp == 0) {
             solve_global(a, m0, cnt, lane);
         }

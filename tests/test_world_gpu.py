@@ -88,6 +88,53 @@ def test_terrain_world_matches_reference_live(ctx):
     w.close()
 
 
+def largest_island(b1, b2, static=(0,)):
+    """Manifolds of the largest island (connected through movable bodies)."""
+    par = {}
+
+    def find(x):
+        while par.get(x, x) != x:
+            x = par[x]
+        return x
+
+    for a, b in zip(b1.tolist(), b2.tolist()):
+        if a in static or b in static:
+            continue
+        ra, rb = find(a), find(b)
+        if ra != rb:
+            par[ra] = rb
+    sizes = {}
+    for a, b in zip(b1.tolist(), b2.tolist()):
+        r = find(a if a not in static else b)
+        sizes[r] = sizes.get(r, 0) + 1
+    return max(sizes.values()) if sizes else 0
+
+
+@pytest.mark.skipif(not reflib.have_ref("f32"), reason="reference engine not built")
+def test_island_beyond_shared_memory_matches_reference(ctx):
+    """2,500 bodies piling on a 36 x 36 height field form one island of
+    thousands of manifolds, too large for a CTA's shared memory: its level
+    schedule is built in global memory and its rows are streamed through the
+    staging ring.  Pairs, manifolds, points and states stay bit-identical to
+    the reference."""
+    sc = scenes.heightfield_world(n_bodies=2500, cols=36, rows=36, seed=31)
+    w, r = engine.World(ctx, sc), reflib.RefScene(sc)
+    big = 0
+    for s in range(150):
+        w.update(float(worldio.DT))
+        r.update(float(worldio.DT))
+        if s >= 90 and (s % 10 == 9 or s == 149):
+            assert np.array_equal(w.pairs(), r.pairs()), s
+            cw, cr = w.contacts(), r.contacts()
+            for a, b in zip(cw, cr):
+                assert np.array_equal(a, b), s
+            big = max(big, largest_island(cw[0], cw[1]))
+    for a, b in zip(w.bodies(), r.bodies()):
+        assert np.array_equal(a, b)
+    assert big >= 2000, big
+    w.close()
+
+
 def test_heightfield_rejects_bad_input(ctx):
     with pytest.raises(engine.Rp3dgError):
         ctx.create_heightfield(np.zeros((1, 5), np.float32))          # fewer than two rows
