@@ -616,8 +616,17 @@ int rp3dg_world_group_get_contacts(rp3dg_world* group, uint32_t world, int32_t* 
  * phase: 0 broad phase (host), 1 middle phase (host), 2 narrow phase and
  * manifold step (GPU), 3 contact pairs and islands (host), 4 contact packing
  * and warm start (GPU), 5 dynamics stage (GPU), 6 collider update and tree
- * reinsertion, 7 sleeping and end of step.  Enabling resets the counters. */
+ * reinsertion, 7 sleeping and end of step; 8-12 parts of the middle phase,
+ * 13-15 parts of the broad phase (tree queries, pair removal, narrow-phase
+ * items).  Enabling resets the counters. */
 int rp3dg_world_set_profiling(rp3dg_world* world, int enable);
+/* Host threads of a world's bookkeeping (no counterpart in the reference,
+ * whose update runs on one thread).  A group spreads its worlds over them; a
+ * single world runs its broad-phase tree queries on them (the tree does not
+ * change while it is queried, and the pairs are still processed in the
+ * moved set's order, so results do not depend on the count).  A world from
+ * rp3dg_world_create starts with 1. */
+int rp3dg_world_set_threads(rp3dg_world* world, int threads);
 int rp3dg_world_get_phase_times(rp3dg_world* world, double* ms, uint32_t n);
 
 /* Number of kernels this context launched so far (instrumentation; a

@@ -51,6 +51,8 @@
 
 #include <set>
 
+#include <omp.h>
+
 #include "../../include/rp3dg.h"
 #include "dynamics_launch.h"
 #include "hf_launch.h"
@@ -449,6 +451,54 @@ int host_grow(T** p, size_t* cap, size_t need) {
     return 0;
 }
 
+// Pair id -> index map for the previous step's contact pairs
+// (mPreviousMapPairIdToContactPairIndex): open addressing with linear
+// probing over a power-of-two table that is kept from step to step, so
+// rebuilding it allocates nothing once it has grown.
+struct FlatMap {
+    static constexpr uint64_t EMPTY = ~uint64_t(0);
+    std::vector<uint64_t> keys;
+    std::vector<uint32_t> vals;
+    uint32_t mask = 0, n = 0;
+    static uint32_t hash(uint64_t k) {
+        k ^= k >> 33;
+        k *= 0xff51afd7ed558ccdull;
+        k ^= k >> 33;
+        return uint32_t(k);
+    }
+    void clear_for(size_t count) {
+        size_t cap = 16;
+        while (cap < 2 * count) cap <<= 1;
+        if (cap != keys.size()) {
+            keys.assign(cap, EMPTY);
+            vals.assign(cap, 0);
+        } else {
+            std::fill(keys.begin(), keys.end(), EMPTY);
+        }
+        mask = uint32_t(cap - 1);
+        n = 0;
+    }
+    void put(uint64_t k, uint32_t v) {
+        uint32_t h = hash(k) & mask;
+        while (keys[h] != EMPTY && keys[h] != k) h = (h + 1) & mask;
+        if (keys[h] == EMPTY) n++;
+        keys[h] = k;
+        vals[h] = v;
+    }
+    bool get(uint64_t k, uint32_t& v) const {
+        if (keys.empty()) return false;
+        uint32_t h = hash(k) & mask;
+        while (keys[h] != EMPTY) {
+            if (keys[h] == k) {
+                v = vals[h];
+                return true;
+            }
+            h = (h + 1) & mask;
+        }
+        return false;
+    }
+};
+
 // Device columns of the rigid-body components (row = world's first row + component slot).
 enum BodyCol { BC_POS, BC_ORI, BC_COMW, BC_COML, BC_LV, BC_AV, BC_F, BC_T, BC_IIL, BC_MASS, BC_LLOCK, BC_ALOCK,
                BC_XC, BC_QC, BC_NCOL };  // XC / QC: constrained position / orientation (joints)
@@ -503,7 +553,7 @@ struct WorldH {
     std::vector<int32_t> reset_slots;
     // contacts of this step and of the previous one
     std::vector<ContactPairH> cpairs, prev_cpairs;
-    std::unordered_map<uint64_t, uint32_t> prev_map;
+    FlatMap prev_map;
     std::vector<uint32_t> island_order;  // mProcessContactPairsOrderIslands
     std::vector<IslandH> islands;
     std::vector<int> dev_body_at, dev_col_at;  // component order the device rows have
@@ -530,6 +580,11 @@ struct WorldH {
     std::vector<uint32_t> hitem_pair[NB_ALGOS];
     uint32_t hitem_off[NB_ALGOS] = {};
     uint32_t nm = 0, np = 0, man_base = 0, pt_base = 0, isl_base = 0;
+    double prof_bp[3] = {0.0, 0.0, 0.0};       // broad phase: queries, pair removal, narrow-phase items (ms)
+    // tree queries of the moved colliders run on several threads: leaves per
+    // thread buffer, and per moved collider (thread, first leaf, count)
+    std::vector<std::vector<int>> q_buf;
+    std::vector<int4> q_pos;
     std::vector<int> slept;                    // bodies put to sleep by this step
     rp3dg_world_stats stats{};
 };
@@ -853,14 +908,36 @@ void set_sleeping(Group* g, WorldH& w, int b, bool sleeping) {
 // computeBroadPhase (CollisionDetectionSystem.cpp:103-167, 270-343) and the
 // middle phase for convex pairs (:346-410): narrow-phase items in pair order.
 void broad_and_middle_phase(Group* g, WorldH& w) {
+    using clk = std::chrono::steady_clock;
+    const auto t0 = g->profiling ? clk::now() : clk::time_point();
     std::vector<int32_t> shapes;
     w.moved.to_array(shapes);
     w.moved.clear();
-    std::vector<int> leaves, stack;
-    for (int32_t s : shapes) {
-        leaves.clear();
-        w.tree.query(w.tree.nodes[size_t(s)].box, leaves, stack);
-        for (int leaf : leaves) {
+    // reportAllShapesOverlappingWithShapes: the tree does not change during
+    // the queries, so with a single world on the group's threads they run in
+    // parallel; the pairs are then processed in the moved set's order
+    const int nt = (g->nthreads > 1 && g->worlds.size() == 1 && shapes.size() >= 256) ? g->nthreads : 1;
+    if (int(w.q_buf.size()) < nt) w.q_buf.resize(size_t(nt));
+    w.q_pos.resize(shapes.size());
+#pragma omp parallel num_threads(nt) if (nt > 1)
+    {
+        const int t = omp_get_thread_num();
+        std::vector<int>& buf = w.q_buf[size_t(t)];
+        buf.clear();
+        std::vector<int> stack;
+#pragma omp for schedule(static)
+        for (long i = 0; i < long(shapes.size()); i++) {
+            const size_t o = buf.size();
+            w.tree.query(w.tree.nodes[size_t(shapes[size_t(i)])].box, buf, stack);
+            w.q_pos[size_t(i)] = make_int4(t, int(o), int(buf.size() - o), 0);
+        }
+    }
+    for (size_t i = 0; i < shapes.size(); i++) {
+        const int32_t s = shapes[i];
+        const int4 qp = w.q_pos[i];
+        const int* leaves = w.q_buf[size_t(qp.x)].data() + qp.y;
+        for (int li = 0; li < qp.z; li++) {
+            const int leaf = leaves[li];
             if (leaf == s) continue;
             const int c1 = w.bp_to_collider[size_t(s)], c2 = w.bp_to_collider[size_t(leaf)];
             const ColliderH &C1 = w.colliders[size_t(c1)], &C2 = w.colliders[size_t(c2)];
@@ -878,6 +955,7 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
             }
         }
     }
+    const auto t1 = g->profiling ? clk::now() : clk::time_point();
     // removeNonOverlappingPairs
     for (uint64_t i = 0; i < w.pairs.size(); i++) {
         PairH& p = w.pairs[i];
@@ -899,6 +977,7 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
             i--;
         }
     }
+    const auto t2 = g->profiling ? clk::now() : clk::time_point();
     for (int a = 0; a < NB_ALGOS; a++) {
         w.items[a].clear();
         w.item_pair[a].clear();
@@ -931,6 +1010,12 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
         w.hitems[a].push_back(make_int4(int(w.c0) + w.ccomp.slot[size_t(cv)], int(w.c0) + w.ccomp.slot[size_t(cc)],
                                         w.colliders[size_t(cc)].hf, p.shape1_convex ? HF_SHAPE1_CONVEX : 0));
         w.hitem_pair[a].push_back(i);
+    }
+    if (g->profiling) {
+        const auto t3 = clk::now();
+        w.prof_bp[0] += std::chrono::duration<double, std::milli>(t1 - t0).count();
+        w.prof_bp[1] += std::chrono::duration<double, std::milli>(t2 - t1).count();
+        w.prof_bp[2] += std::chrono::duration<double, std::milli>(t3 - t2).count();
     }
 }
 
@@ -1105,9 +1190,9 @@ void fill_manifolds(Group* g, WorldH& w) {
         const int4 ids = make_int4(int(w.b0) + w.bcomp.slot[size_t(cp.b1)], int(w.b0) + w.bcomp.slot[size_t(cp.b2)],
                                    int(w.c0) + w.ccomp.slot[size_t(cp.c1)], int(w.c0) + w.ccomp.slot[size_t(cp.c2)]);
         int4 prev = make_int4(-1, 0, 0, 0);
-        auto it = w.prev_map.find(cp.id);
-        if (it != w.prev_map.end() && w.prev_cpairs[it->second].in_island) {
-            const ContactPairH& pc = w.prev_cpairs[it->second];
+        uint32_t pi = 0;
+        if (w.prev_map.get(cp.id, pi) && w.prev_cpairs[pi].in_island) {
+            const ContactPairH& pc = w.prev_cpairs[pi];
             prev = make_int4(int(pc.manifold), int(pc.nman), int(pc.point), int(pc.k));
         }
         if (!cp.concave) {
@@ -1143,8 +1228,8 @@ void fill_manifolds(Group* g, WorldH& w) {
         g->h_jlist[w.jl_base + k] = e;
     }
     // computeMapPreviousContactPairs for the next step
-    w.prev_map.clear();
-    for (uint32_t i = 0; i < w.cpairs.size(); i++) w.prev_map[w.cpairs[i].id] = i;
+    w.prev_map.clear_for(w.cpairs.size());
+    for (uint32_t i = 0; i < w.cpairs.size(); i++) w.prev_map.put(w.cpairs[i].id, i);
 }
 
 // BroadPhaseSystem::updateColliders' reinsertions (enabled colliders in
@@ -1774,6 +1859,14 @@ int update_group(Group* g, float dt) {
     // ---- broad phase and middle phase of every world (host order, GPU fat AABBs)
     for_worlds(g, [&](int k) { broad_and_middle_phase(g, g->worlds[size_t(k)]); });
     mark(0);
+    if (g->profiling) {
+        // broad-phase sub-phases summed over the worlds (13..15)
+        for (WorldH& w : g->worlds)
+            for (int q = 0; q < 3; q++) {
+                g->phase_ms[13 + q] += w.prof_bp[q];
+                w.prof_bp[q] = 0.0;
+            }
+    }
     // batches: algorithm-major, worlds in order inside a batch
     // sub-phase marks of phase 1 (8..12)
     auto sub = [&](int k) {
@@ -2537,6 +2630,12 @@ int rp3dg_world_get_contacts(rp3dg_world* w, int32_t* body1, int32_t* body2, uin
 int rp3dg_world_get_stats(rp3dg_world* w, rp3dg_world_stats* s) {
     if (!w || !s) return RP3DG_EINVAL;
     *s = w->stats;
+    return 0;
+}
+
+int rp3dg_world_set_threads(rp3dg_world* w, int threads) {
+    if (!w || threads < 1) return RP3DG_EINVAL;
+    w->nthreads = threads;
     return 0;
 }
 

@@ -95,6 +95,7 @@ def load_library(path=LIB_PATH):
                                            C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.rp3dg_world_get_stats.argtypes = [P, P]
     L.rp3dg_world_set_profiling.argtypes = [P, C.c_int]
+    L.rp3dg_world_set_threads.argtypes = [P, C.c_int]
     L.rp3dg_world_add_joints.argtypes = [P, P, C.c_uint32]
     L.rp3dg_world_group_add_joints.argtypes = [P, C.c_uint32, P, C.c_uint32]
     L.rp3dg_world_group_create.argtypes = [P, P, C.c_uint32, P, P, P, P, C.c_int, C.POINTER(P)]
@@ -459,7 +460,7 @@ class World:
     PhysicsWorld::update.  `scene` is a scenes.WorldScene; the context's shape
     table is replaced by the scene's."""
 
-    def __init__(self, ctx, scene):
+    def __init__(self, ctx, scene, threads=None):
         self.ctx, self.lib = ctx, ctx.lib
         ctx.set_shapes(ctx.scene_shapes(scene))
         self.nb = len(scene.bodies)
@@ -472,6 +473,7 @@ class World:
         if rc != 0:
             raise Rp3dgError(rc, self.lib.rp3dg_last_error(ctx.h).decode())
         self.h = h
+        self.set_threads(threads or (os.cpu_count() or 1))
         if getattr(scene, "joints", None) is not None and len(scene.joints):
             self.add_joints(scene.joints)
 
@@ -536,7 +538,13 @@ class World:
         return b1, b2, k, nd, l1, l2
 
     PHASES = ("broadphase", "middle", "narrow", "islands", "pack", "dynamics", "colliders", "sleeping",
-              "m.pool", "m.resets", "m.rows", "m.tables", "m.items")
+              "m.pool", "m.resets", "m.rows", "m.tables", "m.items", "b.queries", "b.remove", "b.items")
+
+    def set_threads(self, n):
+        """Host threads of the world's bookkeeping (results do not depend on it)."""
+        rc = self.lib.rp3dg_world_set_threads(self.h, int(n))
+        if rc != 0:
+            raise Rp3dgError(rc, "bad thread count")
 
     def set_profiling(self, on=True):
         self.lib.rp3dg_world_set_profiling(self.h, int(on))
