@@ -249,6 +249,11 @@ def run_ours(args):
         world_step = world_section(ctx, args, rank == 0 and world == 1 and not args.no_cpu)
         ctx.set_shapes(sc.shapes)
 
+    terrain = None
+    if not args.no_terrain:
+        terrain = terrain_section(ctx, args, rank == 0 and world == 1 and not args.no_cpu)
+        ctx.set_shapes(sc.shapes)
+
     worlds = None
     if not args.no_worlds:
         worlds = many_worlds_section(ctx, args, rank == 0 and world == 1 and not args.no_cpu)
@@ -269,7 +274,7 @@ def run_ours(args):
                        "seed": args.seed, "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"independent pair sets per rank x{world}"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "manifolds": manifolds, "dynamics": dynamics, "broadphase": broadphase,
-            "world_step": world_step, "many_worlds": worlds,
+            "world_step": world_step, "terrain_world": terrain, "many_worlds": worlds,
             "learned_axis": learned,
             "gpu_launches": int(launches),
             "clocks": clocks, "batch_ms": {k: round(v, 4) for k, v in mean_batch.items()}}
@@ -543,6 +548,64 @@ def many_worlds_section(ctx, args, with_cpu):
     return out
 
 
+def terrain_section(ctx, args, with_cpu):
+    """The single large world: 100,000 bodies (40% boxes with half-extents
+    U[0.2,0.6], 30% spheres with radius U[0.2,0.5], 30% capsules of radius
+    0.2 and half-height 0.3) on a jittered 3-D lattice with 1.5 m spacing above
+    a 256 x 256-cell height field of 1 m cells whose heights are a seeded sum
+    of 8 sines (wave numbers in [0.05, 0.5] rad/m, total amplitude 2 m),
+    stepped at 1/60 s through rp3dg_world_update (wall clock, synchronous).
+    Steps 2-21 (the bodies fall, the first ones land) are timed on both
+    engines, the reference on one host core (it is single-threaded), and the
+    states after step 21 compared bit for bit; the GPU then continues to step
+    60 and times steps 61-80, when most bodies rest on the terrain and on each
+    other (the contact-heavy regime: ~2 million triangle tests, ~10^5
+    manifolds, one island of ~10^5 manifolds)."""
+    from reactphysics3d_b200 import engine
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import reflib
+    n_bodies = args.terrain_bodies
+    sc = scenes.heightfield_world(n_bodies=n_bodies, cols=257, rows=257, seed=5)
+    dt = float(np.float32(1.0 / 60.0))
+    w = engine.World(ctx, sc)
+    w.update(dt, 1)
+    t0 = time.perf_counter()
+    w.update(dt, 20)
+    sec_early = time.perf_counter() - t0
+    ours21 = w.bodies()
+    st21 = w.stats()
+    w.update(dt, 39)
+    launches0 = ctx.kernel_launches()
+    t0 = time.perf_counter()
+    w.update(dt, 20)
+    sec = time.perf_counter() - t0
+    launches = (ctx.kernel_launches() - launches0) / 20
+    st = w.stats()
+    w.set_profiling(True)
+    w.update(dt, 3)
+    phases = {k: round(v / 3, 3) for k, v in w.phase_times().items() if not k.startswith("m.")}
+    w.close()
+    out = {"workload": f"{n_bodies:,} bodies (40% boxes, 30% spheres, 30% capsules) on a 1.5 m jittered lattice above a "
+                       "256x256-cell height field (1 m cells, 8 seeded sines, amplitude 2 m), dt 1/60; "
+                       "steps 61-80 timed",
+           "bodies": n_bodies, "world_steps_per_s": round(20 / sec, 3), "ms_per_step": round(1e3 * sec / 20, 2),
+           "kernels_per_step": round(launches, 1), "host_threads": os.cpu_count() or 1,
+           "phase_ms_per_step": phases, "stats_at_step_80": st,
+           "early_steps_2_21": {"world_steps_per_s": round(20 / sec_early, 3), "stats_at_step_21": st21},
+           "api": "rp3dg_world_update"}
+    if with_cpu and reflib.have_ref("f32"):
+        r = reflib.RefScene(sc, "f32")
+        r.update(dt, 1)
+        t0 = time.perf_counter()
+        r.update(dt, 20)
+        rsec = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(20 / rsec, 3), "unit": "world-steps/s", "cores": 1, "kind": "reference",
+                               "sample": "the same world, steps 2-21, PhysicsWorld::update of the reference float "
+                                         "build (single-threaded engine); compare early_steps_2_21"}
+        out["bit_identical_to_reference_at_step_21"] = all(np.array_equal(a, b) for a, b in zip(ours21, r.bodies()))
+    return out
+
+
 def broadphase_section(ctx, args, dev):
     """Broad phase of a single large world: 100,000 colliders (40% boxes, 30%
     spheres, 30% capsules, sizes of the large-world workload) on a jittered
@@ -813,6 +876,8 @@ def main():
     ap.add_argument("--dyn-worlds", type=int, default=4096)
     ap.add_argument("--no-world", action="store_true")
     ap.add_argument("--no-worlds", action="store_true")
+    ap.add_argument("--no-terrain", action="store_true")
+    ap.add_argument("--terrain-bodies", type=int, default=100000)
     ap.add_argument("--n-worlds", type=int, default=4096)
     ap.add_argument("--world-steps", type=int, default=300)
     ap.add_argument("--learned-epochs", type=int, default=4)

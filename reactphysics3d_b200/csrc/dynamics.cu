@@ -363,7 +363,37 @@ RD BodyVel vel_global(const DynArgs& a, int32_t b1, int32_t b2) {
 // warmStart (:324-476) of one manifold: its two bodies' velocities are loaded,
 // updated in the reference's statement order and stored back (the two bodies
 // are distinct; fixed bodies are never stored).
-template <bool LDG>
+// A manifold's point impulses held in four registers (PRE cores): loaded
+// together before the points are solved and stored after, so that copies in
+// global memory cost one round trip; points beyond four (none after the
+// manifold step) are read and written in place.
+RD void pmv_load(const RecSrc& r, int nb, float4& p0, float4& p1, float4& p2, float4& p3) {
+    if (nb > 0) p0 = r.pmut[0];
+    if (nb > 1) p1 = r.pmut[r.pmut_stride];
+    if (nb > 2) p2 = r.pmut[2 * r.pmut_stride];
+    if (nb > 3) p3 = r.pmut[3 * r.pmut_stride];
+}
+RD void pmv_store(const RecSrc& r, int nb, const float4& p0, const float4& p1, const float4& p2, const float4& p3) {
+    if (nb > 0) r.pmut[0] = p0;
+    if (nb > 1) r.pmut[r.pmut_stride] = p1;
+    if (nb > 2) r.pmut[2 * r.pmut_stride] = p2;
+    if (nb > 3) r.pmut[3 * r.pmut_stride] = p3;
+}
+template <bool PRE>
+RD float4 pm_get(const RecSrc& r, int k, const float4& p0, const float4& p1, const float4& p2, const float4& p3) {
+    if (!PRE) return r.pmut[k * r.pmut_stride];
+    return k == 0 ? p0 : k == 1 ? p1 : k == 2 ? p2 : k == 3 ? p3 : r.pmut[k * r.pmut_stride];
+}
+template <bool PRE>
+RD void pm_set(const RecSrc& r, int k, const float4& v, float4& p0, float4& p1, float4& p2, float4& p3) {
+    if (!PRE || k > 3) { r.pmut[k * r.pmut_stride] = v; return; }
+    if (k == 0) p0 = v;
+    else if (k == 1) p1 = v;
+    else if (k == 2) p2 = v;
+    else p3 = v;
+}
+
+template <bool LDG, bool PRE = false>
 RD void warm_core(const DynArgs& a, const RecSrc& r, const BodyVel& bv, int32_t nb) {
     if (nb == 0) return;  // rejected by the manifold kernel
     Man c;
@@ -371,10 +401,11 @@ RD void warm_core(const DynArgs& a, const RecSrc& r, const BodyVel& bv, int32_t 
     const v3 o1 = L3(ldq<LDG>(r.mq + DQ_OFV1)), o2 = L3(ldq<LDG>(r.mq + DQ_OFV2));
     float4 mut = *r.mmut;
     v3 v1 = L3(*bv.v1), w1 = L3(*bv.w1), v2 = L3(*bv.v2), w2 = L3(*bv.w2);
+    float4 pv0, pv1, pv2, pv3;
+    if (PRE) pmv_load(r, nb, pv0, pv1, pv2, pv3);
     bool resting_any = false;
     for (int k = 0; k < nb; k++) {
-        float4* pmp = r.pmut + k * r.pmut_stride;
-        float4 pm = *pmp;
+        float4 pm = pm_get<PRE>(r, k, pv0, pv1, pv2, pv3);
         if (pm.z != 0.0f) {
             resting_any = true;
             Pt p;
@@ -387,9 +418,10 @@ RD void warm_core(const DynArgs& a, const RecSrc& r, const BodyVel& bv, int32_t 
             w2 = ang_add(w2, p.i2, c.af2, pi);
         } else {
             pm.x = 0.0f;
-            *pmp = pm;
+            pm_set<PRE>(r, k, pm, pv0, pv1, pv2, pv3);
         }
     }
+    if (PRE) pmv_store(r, nb, pv0, pv1, pv2, pv3);
     float f1 = mut.x, f2 = mut.y, ftw = mut.z;
     if (resting_any) {
         const v3 ofi = V(f1 * o1.x + f2 * o2.x, f1 * o1.y + f2 * o2.y, f1 * o1.z + f2 * o2.z);
@@ -431,7 +463,7 @@ RD void warm_manifold(const DynArgs& a, uint32_t mi, const BodyVel& bv, int32_t 
 }
 
 // One solve pass (:479-759) over one manifold.
-template <bool LDG>
+template <bool LDG, bool PRE = false>
 RD void solve_core(const DynArgs& a, const RecSrc& r, float beta, const BodyVel& bv, int32_t nb) {
     if (nb == 0) return;
     Man c;
@@ -439,12 +471,13 @@ RD void solve_core(const DynArgs& a, const RecSrc& r, float beta, const BodyVel&
     float4 mut = *r.mmut;
     v3 v1 = L3(*bv.v1), w1 = L3(*bv.w1), v2 = L3(*bv.v2), w2 = L3(*bv.w2);
     v3 s1 = L3(*bv.s1), t1 = L3(*bv.t1), s2 = L3(*bv.s2), t2 = L3(*bv.t2);
+    float4 pv0, pv1, pv2, pv3;
+    if (PRE) pmv_load(r, nb, pv0, pv1, pv2, pv3);
     float sum_pen = 0.0f;
     for (int k = 0; k < nb; k++) {
-        float4* pmp = r.pmut + k * r.pmut_stride;
         Pt p;
         load_pt_q<LDG>(r.pq + k * r.pq_stride, p);
-        float4 pm = *pmp;
+        float4 pm = pm_get<PRE>(r, k, pv0, pv1, pv2, pv3);
         const v3 n = p.n;
         const v3 dv = rel_velocity(v1, w1, v2, w2, p.r1, p.r2);
         const float Jv = dv.x * n.x + dv.y * n.y + dv.z * n.z;
@@ -479,8 +512,9 @@ RD void solve_core(const DynArgs& a, const RecSrc& r, float beta, const BodyVel&
             s2 = lin_add(s2, c.im2, lis, c.lf2);
             t2 = ang_add(t2, p.i2, c.af2, dls);
         }
-        *pmp = pm;
+        pm_set<PRE>(r, k, pm, pv0, pv1, pv2, pv3);
     }
+    if (PRE) pmv_store(r, nb, pv0, pv1, pv2, pv3);
     float f1 = mut.x, f2 = mut.y, ftw = mut.z;
     // first friction constraint
     {
@@ -1253,38 +1287,69 @@ RD uint32_t stream_schedule(const DynArgs& a, uint32_t m0, uint32_t cnt, uint32_
     return depth;
 }
 
-// Warp 1: stage the manifolds of linearised level t (passes x levels).
-RD void stream_stage_level(const DynArgs& a, GiantSlot* ring, uint32_t m0, uint32_t depth, uint32_t total,
-                           uint32_t t, uint32_t lane) {
-    if (t < total) {
-        const uint32_t L = t % depth;
-        const uint32_t b = L ? a.level[m0 + L - 1] : 0u, e = a.level[m0 + L];
-        const uint32_t j = b + lane;
-        if (lane < STREAM_RING && j < e) {
-            const uint32_t kk = a.order[m0 + j];
-            const int4 id = man_ids(a, m0 + kk);
-            const uint32_t np = id.z < 0 ? 0u : (id.z > 4 ? 4u : uint32_t(id.z));
-            GiantSlot* sl = ring + (t % GIANT_LEVELS) * STREAM_RING + lane;
-            sl->desc = make_int4(0, int(np), int(kk), id.w);
-            const float4* src = a.mrec[m0 + kk].q;
+// Warp 1's staging pipeline: for linearised level x (passes x levels) it
+// loads the level's bounds three steps ahead, the lanes' manifold indices two
+// steps ahead and their id rows one step ahead, and issues the cp.async
+// copies of the rows at x, so that no stage waits on a load issued in the
+// same step; the registers then shift by one level.
+struct StreamPipe {
+    int2 b0, b1, b2;   // bounds of levels x, x + 1, x + 2
+    uint32_t k0, k1;   // the lane's manifold of levels x, x + 1 (~0u: none)
+    int4 i0;           // the id row of k0
+};
+RD int2 stream_bounds(const DynArgs& a, uint32_t m0, uint32_t depth, int64_t total, int64_t x) {
+    if (x < 0 || x >= total) return make_int2(0, 0);
+    const uint32_t L = uint32_t(x) % depth;
+    return make_int2(int(L ? a.level[m0 + L - 1] : 0u), int(a.level[m0 + L]));
+}
+RD uint32_t stream_kk(const DynArgs& a, uint32_t m0, int2 bd, uint32_t lane) {
+    const uint32_t j = uint32_t(bd.x) + lane;
+    return (lane < STREAM_RING && j < uint32_t(bd.y)) ? a.order[m0 + j] : ~0u;
+}
+
+// One pipeline step for level x (negative in the prologue: loads only); the
+// header of level x (its bounds) goes to hdr[x % 3] for warp 0.
+RD void stream_stage_step(const DynArgs& a, GiantSlot* ring, int2* hdr, StreamPipe& P, uint32_t m0, uint32_t depth,
+                          int64_t total, int64_t x, uint32_t lane) {
+    const int2 nb3 = stream_bounds(a, m0, depth, total, x + 3);
+    const uint32_t nk2 = stream_kk(a, m0, P.b2, lane);
+    int4 ni1 = make_int4(0, 0, 0, 0);
+    if (P.k1 != ~0u) ni1 = man_ids(a, m0 + P.k1);
+    if (x >= 0 && x < total) {
+        if (lane == 0) hdr[uint32_t(x) % GIANT_LEVELS] = P.b0;
+        if (P.k0 != ~0u) {
+            const uint32_t np = P.i0.z < 0 ? 0u : (P.i0.z > 4 ? 4u : uint32_t(P.i0.z));
+            GiantSlot* sl = ring + (uint32_t(x) % GIANT_LEVELS) * STREAM_RING + lane;
+            sl->desc = make_int4(0, int(np), int(P.k0), P.i0.w);
+            const float4* src = a.mrec[m0 + P.k0].q;
             for (int r = 0; r < DQ_ROWS; r++) cp_async16(&sl->mq[r], src + r);
-            const float4* ps = a.prec[id.w].q;
+            const float4* ps = a.prec[P.i0.w].q;
             for (uint32_t r = 0; r < np * PREC_F4; r++) cp_async16(&sl->pq[r], ps + r);
         }
     }
-    cp_async_commit();
+    if (x >= 0) cp_async_commit();
+    P.b0 = P.b1;
+    P.b1 = P.b2;
+    P.b2 = nb3;
+    P.k0 = P.k1;
+    P.k1 = nk2;
+    P.i0 = ni1;
 }
 
 // Both warps: warm start and velocity iterations of a scheduled island.
 RD void stream_solve(const DynArgs& a, uint32_t m0, GiantSlot* ring, uint32_t warp, uint32_t lane, uint32_t depth) {
     const uint32_t total = uint32_t(a.iterations + 1) * depth;
+    int2* hdr = reinterpret_cast<int2*>(ring + GIANT_LEVELS * STREAM_RING);
     if (warp == 1) {
-        stream_stage_level(a, ring, m0, depth, total, 0, lane);
-        stream_stage_level(a, ring, m0, depth, total, 1, lane);
+        StreamPipe P;
+        P.b0 = P.b1 = P.b2 = make_int2(0, 0);
+        P.k0 = P.k1 = ~0u;
+        P.i0 = make_int4(0, 0, 0, 0);
+        for (int64_t x = -3; x <= 1; x++) stream_stage_step(a, ring, hdr, P, m0, depth, total, x, lane);
         cp_async_wait<1>();
         giant_bar();
         for (uint32_t t = 0; t < total; t++) {
-            stream_stage_level(a, ring, m0, depth, total, t + 2, lane);
+            stream_stage_step(a, ring, hdr, P, m0, depth, total, int64_t(t) + 2, lane);
             cp_async_wait<1>();
             giant_bar();
         }
@@ -1293,9 +1358,9 @@ RD void stream_solve(const DynArgs& a, uint32_t m0, GiantSlot* ring, uint32_t wa
         const float beta = a.split ? BETA_SPLIT_IMPULSE : BETA;
         giant_bar();
         for (uint32_t t = 0; t < total; t++) {
-            const uint32_t L = t % depth;
             const bool warm = t < depth;
-            const uint32_t b = L ? a.level[m0 + L - 1] : 0u, e = a.level[m0 + L];
+            const int2 bd = hdr[t % GIANT_LEVELS];
+            const uint32_t b = uint32_t(bd.x), e = uint32_t(bd.y);
             if (lane < STREAM_RING && b + lane < e) {
                 const GiantSlot* sl = ring + (t % GIANT_LEVELS) * STREAM_RING + lane;
                 const int4 d = sl->desc;
@@ -1308,16 +1373,16 @@ RD void stream_solve(const DynArgs& a, uint32_t m0, GiantSlot* ring, uint32_t wa
                 r.mmut = &a.mrec[m0 + uint32_t(d.z)].mut;
                 r.pmut = &a.prec[d.w].mut;
                 r.pmut_stride = PREC_F4;
-                if (warm) warm_core<false>(a, r, bv, d.y);
-                else solve_core<false>(a, r, beta, bv, d.y);
+                if (warm) warm_core<false, true>(a, r, bv, d.y);
+                else solve_core<false, true>(a, r, beta, bv, d.y);
             }
             // manifolds of a level beyond the ring read their rows from global memory
             for (uint32_t j = b + STREAM_RING + lane; j < e; j += 32) {
                 const uint32_t mi = m0 + a.order[m0 + j];
                 const int4 id = man_ids(a, mi);
                 const BodyVel bv = vel_global(a, id.x, id.y);
-                if (warm) warm_core<true>(a, rec_global(a, mi, id.w), bv, id.z);
-                else solve_core<true>(a, rec_global(a, mi, id.w), beta, bv, id.z);
+                if (warm) warm_core<true, true>(a, rec_global(a, mi, id.w), bv, id.z);
+                else solve_core<true, true>(a, rec_global(a, mi, id.w), beta, bv, id.z);
             }
             __syncwarp();
             giant_bar();
@@ -1352,17 +1417,39 @@ __global__ void __launch_bounds__(GIANT_THREADS, 1) dyn_islands_giant(const DynA
                 giant_layout(a, cnt, uint32_t(int64_t(l.w) + int64_t(l.z) - int64_t(s_p0)), gsm, g);
             }
             giant_solve(a, m0, cnt, g, warp, lane, s_depth, s_nslots, s_p0);
-        } else if (size_t(GIANT_LEVELS) * STREAM_RING * sizeof(GiantSlot) <= a.giant_smem) {
-            if (warp == 0) {
-                const uint32_t depth = stream_schedule(a, m0, cnt, lane);
-                if (lane == 0) s_depth = depth;
-            }
+        } else if (size_t(GIANT_LEVELS) * STREAM_RING * sizeof(GiantSlot) + GIANT_LEVELS * sizeof(int2) <= a.giant_smem) {
+            // streamed by dyn_islands_stream (queued at the back of giant_list)
+            if (threadIdx.x == 0) a.giant_list[a.ni - 1 - atomicAdd(a.counters + 5, 1u)] = is;
             __syncthreads();
-            stream_solve(a, m0, reinterpret_cast<GiantSlot*>(gsm), warp, lane, s_depth);
+            continue;
         } else if (warp == 0) {
             solve_global(a, m0, cnt, lane);
         }
         __syncthreads();
+        for (uint32_t j = threadIdx.x; j < cnt; j += GIANT_THREADS) store_manifold(a, m0 + j);
+        __syncthreads();
+    }
+}
+
+// ---- kernel 3d: islands streamed through global memory -------------------
+__global__ void __launch_bounds__(GIANT_THREADS, 1) dyn_islands_stream(const DynArgs a) {
+    extern __shared__ __align__(16) unsigned char ssm[];
+    __shared__ uint32_t s_island, s_depth;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t n_stream = a.counters[5];
+    for (;;) {
+        if (threadIdx.x == 0) s_island = atomicAdd(a.counters + 6, 1u);
+        __syncthreads();
+        const uint32_t k = s_island;
+        if (k >= n_stream) break;
+        const uint32_t is = a.giant_list[a.ni - 1 - k];
+        const uint32_t m0 = a.i_start[is], cnt = a.i_count[is];
+        if (warp == 0) {
+            const uint32_t depth = stream_schedule(a, m0, cnt, lane);
+            if (lane == 0) s_depth = depth;
+        }
+        __syncthreads();
+        stream_solve(a, m0, reinterpret_cast<GiantSlot*>(ssm), warp, lane, s_depth);
         for (uint32_t j = threadIdx.x; j < cnt; j += GIANT_THREADS) store_manifold(a, m0 + j);
         __syncthreads();
     }
@@ -1425,7 +1512,7 @@ cudaError_t launch_dynamics(const DynArgs& a, cudaStream_t s, uint64_t* launches
     if (a.nm) { dyn_manifold_init<<<blocks(a.nm), 128, 0, s>>>(a); (*launches)++; }
     if (a.nj) { dyn_joints_init<<<blocks(a.nj), 128, 0, s>>>(a); (*launches)++; }
     if (a.ni) {
-        cudaMemsetAsync(a.counters, 0, 5 * sizeof(uint32_t), s);
+        cudaMemsetAsync(a.counters, 0, 7 * sizeof(uint32_t), s);
         dyn_islands_small<<<blocks(a.ni), 128, 0, s>>>(a);
         (*launches)++;
         const size_t smem = size_t(LARGE_WARPS) * LARGE_WARP_SMEM;
@@ -1435,6 +1522,10 @@ cudaError_t launch_dynamics(const DynArgs& a, cudaStream_t s, uint64_t* launches
         if (a.giant_smem) {
             cudaFuncSetAttribute(dyn_islands_giant, cudaFuncAttributeMaxDynamicSharedMemorySize, int(a.giant_smem));
             dyn_islands_giant<<<a.giant_ctas, GIANT_THREADS, a.giant_smem, s>>>(a);
+            (*launches)++;
+            const size_t ring = size_t(GIANT_LEVELS) * STREAM_RING * sizeof(GiantSlot) + GIANT_LEVELS * sizeof(int2);
+            cudaFuncSetAttribute(dyn_islands_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ring));
+            dyn_islands_stream<<<a.giant_ctas, GIANT_THREADS, ring, s>>>(a);
             (*launches)++;
         }
         if (a.nji) { dyn_islands_joint<<<(a.nji + 63) / 64, 64, 0, s>>>(a); (*launches)++; }

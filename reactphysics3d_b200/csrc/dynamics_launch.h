@@ -111,7 +111,8 @@ struct DynArgs {
     uint32_t* body_level;  // nb: last level of each movable body (scratch)
     int32_t* body_slot;    // nb: shared-memory slot of each movable body (scratch)
     uint32_t* counters;    // [0] big islands queued (front of large_list), [1] islands taken, [2] others queued (back),
-                           // [3] giant islands queued, [4] giant islands taken
+                           // [3] giant islands queued, [4] giant islands taken,
+                           // [5] streamed islands queued (back of giant_list), [6] streamed islands taken
     uint32_t* large_list;  // ni: queued islands
     uint32_t* giant_list;  // ni: islands for kernel 3c
     uint32_t large_ctas;   // grid of kernel 3b (persistent)
