@@ -290,6 +290,60 @@ __global__ void __launch_bounds__(128) world_zero_rows(uint32_t n, const int32_t
     torque[r] = z;
 }
 
+// reportAllShapesOverlappingWithShapes on the GPU for worlds with many moved
+// colliders: one thread per moved collider runs the tree's stack query (same
+// visiting order as DynamicAABBTree::reportAllShapesOverlappingWithAABB,
+// DynamicAABBTree.cpp:589-638) over a copy of the host tree's nodes, counts
+// its leaves, reserves a contiguous block and writes them in that order.
+constexpr int TREE_STACK = 96;
+constexpr size_t TREE_GPU_MIN_QUERIES = 4096;
+__global__ void __launch_bounds__(128) world_tree_query(const rp3dg::order::Tree::Node* __restrict__ nodes, int root,
+                                                        const int32_t* __restrict__ queries, uint32_t n, int2* out_pos,
+                                                        int32_t* leaves, uint32_t cap, uint32_t* counter,
+                                                        uint32_t* flags) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const rp3dg::order::Box q = nodes[queries[i]].box;
+    int stack[TREE_STACK];
+    auto visit = [&](int32_t* out, uint32_t& cnt) -> bool {
+        int sp = 0;
+        stack[sp++] = root;
+        while (sp > 0) {
+            const int id = stack[--sp];
+            if (id < 0) continue;
+            const rp3dg::order::Box b = nodes[id].box;
+            // AABB::testCollision (inclusive)
+            if (q.mx[0] < b.mn[0] || b.mx[0] < q.mn[0] || q.mx[1] < b.mn[1] || b.mx[1] < q.mn[1] ||
+                q.mx[2] < b.mn[2] || b.mx[2] < q.mn[2])
+                continue;
+            if (nodes[id].height == 0) {
+                if (out) out[cnt] = id;
+                cnt++;
+            } else {
+                if (sp + 2 > TREE_STACK) return false;
+                stack[sp++] = nodes[id].child[0];
+                stack[sp++] = nodes[id].child[1];
+            }
+        }
+        return true;
+    };
+    uint32_t cnt = 0;
+    if (!visit(nullptr, cnt)) {
+        atomicOr(flags, 1u);
+        out_pos[i] = make_int2(-1, 0);
+        return;
+    }
+    const uint32_t off = atomicAdd(counter, cnt);
+    if (off + cnt > cap) {
+        atomicOr(flags, 2u);
+        out_pos[i] = make_int2(-1, int(cnt));
+        return;
+    }
+    uint32_t w = 0;
+    visit(leaves + off, w);
+    out_pos[i] = make_int2(int(off), int(cnt));
+}
+
 uint32_t blocks(uint32_t n) { return (n + 127) / 128; }
 
 // ------------------------------------------------------------------ host
@@ -647,6 +701,12 @@ struct rp3dg_world {
     rp3dg_lastframe* d_tcache[2] = {nullptr, nullptr};
     int cur_tc = 0;
     cudaEvent_t ev_rect = nullptr;
+    // broad-phase tree queries on the GPU (worlds with many moved colliders)
+    rp3dg::order::Tree::Node *h_tnodes = nullptr, *d_tnodes = nullptr;
+    size_t cap_tnodes = 0, cap_tq = 0, cap_tleaves = 0, cap_tpos = 0, cap_tcnt = 0;
+    int32_t *h_tq = nullptr, *d_tq = nullptr, *h_tleaves = nullptr, *d_tleaves = nullptr;
+    int2 *h_tpos = nullptr, *d_tpos = nullptr;
+    uint32_t *h_tcnt = nullptr, *d_tcnt = nullptr;   // [0] leaves reserved, [1] flags
     // manifold packing
     size_t cap_m = 0, cap_i = 0;
     int4 *d_mids = nullptr, *d_msrc = nullptr, *d_mprev = nullptr;
@@ -905,6 +965,59 @@ void set_sleeping(Group* g, WorldH& w, int b, bool sleeping) {
 
 // ---------------------------------------------------------------- phases
 
+// Pinned host and device copies of one array, grown together.
+template <class T>
+bool pair_grow(T** h, T** d, size_t* cap, size_t need) {
+    if (need <= *cap && *h && *d) return true;
+    const size_t n = std::max<size_t>(std::max<size_t>(need, *cap * 2), 256);
+    cudaFreeHost(*h);
+    cudaFree(*d);
+    *h = nullptr;
+    *d = nullptr;
+    *cap = 0;
+    if (cudaMallocHost(reinterpret_cast<void**>(h), n * sizeof(T)) != cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void**>(d), n * sizeof(T)) != cudaSuccess)
+        return false;
+    *cap = n;
+    return true;
+}
+
+// The moved colliders' tree queries on the GPU: the leaves of query i are
+// h_tleaves[pos.x, pos.x + pos.y) (pos = h_tpos[i]) in the host query's
+// order.  False when a buffer cannot be had or a query needs a deeper stack
+// (the caller then queries on the host).
+bool tree_queries_gpu(Group* g, WorldH& w, const std::vector<int32_t>& shapes) {
+    const size_t nn = w.tree.nodes.size(), nq = shapes.size();
+    cudaStream_t st = g->stream;
+    if (!pair_grow(&g->h_tnodes, &g->d_tnodes, &g->cap_tnodes, nn) || !pair_grow(&g->h_tq, &g->d_tq, &g->cap_tq, nq) ||
+        !pair_grow(&g->h_tpos, &g->d_tpos, &g->cap_tpos, nq) ||
+        !pair_grow(&g->h_tcnt, &g->d_tcnt, &g->cap_tcnt, 2) ||
+        !pair_grow(&g->h_tleaves, &g->d_tleaves, &g->cap_tleaves, 8 * nq))
+        return false;
+    std::memcpy(g->h_tnodes, w.tree.nodes.data(), nn * sizeof(rp3dg::order::Tree::Node));
+    std::memcpy(g->h_tq, shapes.data(), nq * 4);
+    cudaMemcpyAsync(g->d_tnodes, g->h_tnodes, nn * sizeof(rp3dg::order::Tree::Node), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(g->d_tq, g->h_tq, nq * 4, cudaMemcpyHostToDevice, st);
+    for (int attempt = 0; attempt < 2; attempt++) {
+        cudaMemsetAsync(g->d_tcnt, 0, 8, st);
+        world_tree_query<<<blocks(uint32_t(nq)), 128, 0, st>>>(g->d_tnodes, w.tree.root, g->d_tq, uint32_t(nq),
+                                                               g->d_tpos, g->d_tleaves, uint32_t(g->cap_tleaves),
+                                                               g->d_tcnt, g->d_tcnt + 1);
+        cudaMemcpyAsync(g->h_tcnt, g->d_tcnt, 8, cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) return false;
+        const uint32_t total = g->h_tcnt[0], flags = g->h_tcnt[1];
+        if (flags & 1u) return false;
+        if (flags & 2u) {
+            if (attempt || !pair_grow(&g->h_tleaves, &g->d_tleaves, &g->cap_tleaves, size_t(total) + 1024)) return false;
+            continue;
+        }
+        cudaMemcpyAsync(g->h_tpos, g->d_tpos, nq * sizeof(int2), cudaMemcpyDeviceToHost, st);
+        if (total) cudaMemcpyAsync(g->h_tleaves, g->d_tleaves, size_t(total) * 4, cudaMemcpyDeviceToHost, st);
+        return cudaStreamSynchronize(st) == cudaSuccess;
+    }
+    return false;
+}
+
 // computeBroadPhase (CollisionDetectionSystem.cpp:103-167, 270-343) and the
 // middle phase for convex pairs (:346-410): narrow-phase items in pair order.
 void broad_and_middle_phase(Group* g, WorldH& w) {
@@ -917,10 +1030,12 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
     // the queries, so with a single world on the group's threads they run in
     // parallel; the pairs are then processed in the moved set's order
     const int nt = (g->nthreads > 1 && g->worlds.size() == 1 && shapes.size() >= 256) ? g->nthreads : 1;
+    // a single world with many moved colliders queries on the GPU
+    const bool gpu = g->worlds.size() == 1 && shapes.size() >= TREE_GPU_MIN_QUERIES && tree_queries_gpu(g, w, shapes);
     if (int(w.q_buf.size()) < nt) w.q_buf.resize(size_t(nt));
     w.q_pos.resize(shapes.size());
-#pragma omp parallel num_threads(nt) if (nt > 1)
-    {
+#pragma omp parallel num_threads(nt) if (nt > 1 && !gpu)
+    if (!gpu) {
         const int t = omp_get_thread_num();
         std::vector<int>& buf = w.q_buf[size_t(t)];
         buf.clear();
@@ -934,9 +1049,18 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
     }
     for (size_t i = 0; i < shapes.size(); i++) {
         const int32_t s = shapes[i];
-        const int4 qp = w.q_pos[i];
-        const int* leaves = w.q_buf[size_t(qp.x)].data() + qp.y;
-        for (int li = 0; li < qp.z; li++) {
+        const int* leaves;
+        int nleaf;
+        if (gpu) {
+            const int2 tp = g->h_tpos[i];
+            leaves = g->h_tleaves + tp.x;
+            nleaf = tp.y;
+        } else {
+            const int4 qp = w.q_pos[i];
+            leaves = w.q_buf[size_t(qp.x)].data() + qp.y;
+            nleaf = qp.z;
+        }
+        for (int li = 0; li < nleaf; li++) {
             const int leaf = leaves[li];
             if (leaf == s) continue;
             const int c1 = w.bp_to_collider[size_t(s)], c2 = w.bp_to_collider[size_t(leaf)];
@@ -1537,6 +1661,9 @@ void destroy_group(Group* g) {
     cudaFree(g->d_tr2); cudaFree(g->d_trep); cudaFree(g->d_tcoll); cudaFree(g->d_tnct); cudaFree(g->d_tmid);
     cudaFree(g->d_tnd); cudaFree(g->d_tl1); cudaFree(g->d_tl2); cudaFree(g->d_tri);
     cudaFree(g->d_tcache[0]); cudaFree(g->d_tcache[1]); cudaFree(g->d_hf);
+    cudaFreeHost(g->h_tnodes); cudaFree(g->d_tnodes); cudaFreeHost(g->h_tq); cudaFree(g->d_tq);
+    cudaFreeHost(g->h_tleaves); cudaFree(g->d_tleaves); cudaFreeHost(g->h_tpos); cudaFree(g->d_tpos);
+    cudaFreeHost(g->h_tcnt); cudaFree(g->d_tcnt);
     if (g->ev_rect) cudaEventDestroy(g->ev_rect);
     cudaFreeHost(g->t_grav); cudaFreeHost(g->t_ben); cudaFreeHost(g->t_cen); cudaFreeHost(g->t_cbody);
     cudaFreeHost(g->t_cshape); cudaFreeHost(g->t_cat); cudaFreeHost(g->t_mask); cudaFreeHost(g->t_bperm);
