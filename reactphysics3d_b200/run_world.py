@@ -1,0 +1,65 @@
+"""Step one of the generated worlds on the GPU and print its statistics.
+
+    python -m reactphysics3d_b200.run_world terrain --bodies 100000 --cols 257 --steps 156
+    python -m reactphysics3d_b200.run_world pile --steps 300 --phases
+
+Scenes: `pile` (scenes.box_pile), `mixed` (scenes.mixed_world), `terrain`
+(scenes.heightfield_world: --bodies bodies over a --cols x --cols height
+field), `ragdolls` (scenes.ragdoll_world).  The world is created, stepped
+--steps times at --dt and synchronised; nothing else is launched, so kernel
+launch counts (for a profiler's skip / count options) follow from the step
+count.  --phases prints the per-phase host / device times per step
+(rp3dg_world_set_profiling) of the last --phase-steps steps.
+"""
+import argparse
+import json
+import time
+
+from . import engine, scenes
+
+
+def make_scene(args):
+    if args.scene == "pile":
+        return scenes.box_pile(seed=args.seed if args.seed is not None else 1)
+    if args.scene == "mixed":
+        return scenes.mixed_world(seed=args.seed if args.seed is not None else 2)
+    if args.scene == "ragdolls":
+        return scenes.ragdoll_world(n_ragdolls=args.bodies or 8, seed=args.seed if args.seed is not None else 23)
+    n = args.bodies or 100000
+    seed = args.seed if args.seed is not None else (31 if n < 50000 else 5)
+    return scenes.heightfield_world(n_bodies=n, cols=args.cols, rows=args.cols, seed=seed)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("scene", choices=["pile", "mixed", "terrain", "ragdolls"])
+    ap.add_argument("--bodies", type=int, default=None)
+    ap.add_argument("--cols", type=int, default=257)
+    ap.add_argument("--seed", type=int, default=None)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--dt", type=float, default=1.0 / 60.0)
+    ap.add_argument("--threads", type=int, default=None)
+    ap.add_argument("--phases", action="store_true")
+    ap.add_argument("--phase-steps", type=int, default=5)
+    args = ap.parse_args()
+    sc = make_scene(args)
+    ctx = engine.Context(0)
+    w = engine.World(ctx, sc, threads=args.threads)
+    n_plain = args.steps - (min(args.phase_steps, args.steps) if args.phases else 0)
+    t0 = time.perf_counter()
+    w.update(args.dt, n_plain)
+    ctx.synchronize()
+    sec = time.perf_counter() - t0
+    out = {"scene": sc.name, "steps": args.steps, "ms_per_step": round(1e3 * sec / max(n_plain, 1), 3),
+           "stats": w.stats()}
+    if args.phases and args.steps > n_plain:
+        w.set_profiling(True)
+        w.update(args.dt, args.steps - n_plain)
+        out["phase_ms_per_step"] = {k: round(v / (args.steps - n_plain), 3) for k, v in w.phase_times().items()}
+    print(json.dumps(out))
+    w.close()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()
