@@ -38,6 +38,12 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
 
+# Measured DRAM traffic per pair of a batch (both of its launches), from
+# profiles/narrowphase_kernel6_kernel7_262k.md: hull-box 2.76 + 5.28 MB,
+# box-box 5.85 + 2.77 MB, over 37,449 pairs each.
+TRAFFIC_PER_PAIR = {"hull_box": (2.76e6 + 5.26e6 + 0.02e6) / 37449, "box_box": (5.54e6 + 0.31e6 + 2.77e6) / 37449}
+
+
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
@@ -192,6 +198,12 @@ def run_ours(args):
                         "FP32 CUDA-core peak is in MEASURED_PEAKS.json"}
     if args.traffic_bytes:
         roofline["traffic"] = args.traffic_bytes
+    elif dom in TRAFFIC_PER_PAIR:
+        # DRAM bytes (read + write) of the batch's launches from an ncu capture
+        # of the 262,144-pair case, scaled by the pairs of this launch
+        roofline["traffic"] = round(TRAFFIC_PER_PAIR[dom] * n_dom)
+        roofline["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 262,144-pair case "
+                                      "(profiles/narrowphase_kernel6_kernel7_262k.md), scaled by pairs")
 
     # ---- end to end through the host-memory C-ABI call -------------------
     e2e, pinned = None, None
