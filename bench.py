@@ -38,9 +38,10 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
 
-# Measured DRAM traffic per pair of a batch (both of its launches), from
-# profiles/narrowphase_kernel6_kernel7_262k.md: hull-box 2.76 + 5.28 MB,
-# box-box 5.85 + 2.77 MB, over 37,449 pairs each.
+# Measured DRAM traffic per pair of a batch (both of its launches): ncu
+# dram__bytes_read.sum + dram__bytes_write.sum of `python bench.py --pairs
+# 262144 --steps 2 --warmup 1 --no-cpu --no-e2e --no-learned` (37,449 pairs
+# per batch): hull-box 2.76 + 5.28 MB, box-box 5.85 + 2.77 MB.
 TRAFFIC_PER_PAIR = {"hull_box": (2.76e6 + 5.26e6 + 0.02e6) / 37449, "box_box": (5.54e6 + 0.31e6 + 2.77e6) / 37449}
 
 
@@ -202,8 +203,8 @@ def run_ours(args):
         # DRAM bytes (read + write) of the batch's launches from an ncu capture
         # of the 262,144-pair case, scaled by the pairs of this launch
         roofline["traffic"] = round(TRAFFIC_PER_PAIR[dom] * n_dom)
-        roofline["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 262,144-pair case "
-                                      "(profiles/narrowphase_kernel6_kernel7_262k.md), scaled by pairs")
+        roofline["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the same batch in the "
+                                      "262,144-pair case (37,449 pairs), scaled by pairs")
 
     # ---- end to end through the host-memory C-ABI call -------------------
     e2e, pinned = None, None
