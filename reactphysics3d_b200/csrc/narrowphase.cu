@@ -344,8 +344,9 @@ __global__ void __launch_bounds__(NP_BLOCK, MinBlocks<ALGO>::value) narrowphase_
         const uint32_t nwarps = gridDim.x * (NP_BLOCK / 32);
         uint32_t tested = 0, confirmed = 0;
         for (uint32_t tile = blockIdx.x * (NP_BLOCK / 32) + warp; tile * 32u < a.n; tile += nwarps) {
-            const uint32_t i = tile * 32u + lane;
-            bool boxbox = i >= a.n;  // lanes past the end do not force the warp path
+            const uint32_t t = tile * 32u + lane;
+            const uint32_t i = (a.perm && t < a.n) ? a.perm[t] : t;
+            bool boxbox = t >= a.n;  // lanes past the end do not force the warp path
             if (i < a.n) {
                 const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
                 if (uint32_t(i1) < a.nb_shapes && uint32_t(i2) < a.nb_shapes) {
@@ -359,20 +360,21 @@ __global__ void __launch_bounds__(NP_BLOCK, MinBlocks<ALGO>::value) narrowphase_
             uint32_t proposal = MLP_NO_PROPOSAL;
             if (a.proposals) {
                 // learned proposals written by narrowphase_propose for this batch
-                proposal = i < a.n ? a.proposals[i] : uint32_t(MLP_NO_PROPOSAL);
+                proposal = t < a.n ? a.proposals[i] : uint32_t(MLP_NO_PROPOSAL);
                 if (proposal >= MLP_OUT) proposal = MLP_NO_PROPOSAL;
                 ws.cls[lane] = proposal;
                 __syncwarp();
             }
             if (ALGO == ALGO_POLY_PER_THREAD) {
                 uint32_t r = 0;
-                if (i < a.n) r = process_pair<RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON>(a, i, &s_box, mesh_words, proposal);
+                if (t < a.n) r = process_pair<RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON>(a, i, &s_box, mesh_words, proposal);
                 tested += __popc(__ballot_sync(FULL_MASK, r & 1u));
                 confirmed += __popc(__ballot_sync(FULL_MASK, (r & 2u) != 0));
             } else {
                 const uint32_t cnt = a.n - tile * 32u < 32u ? a.n - tile * 32u : 32u;
                 for (uint32_t l = 0; l < cnt; l++) {
-                    const uint32_t r = process_pair_warp(a, tile * 32u + l, lane, &s_box, mesh_words, ws,
+                    const uint32_t tl = tile * 32u + l;
+                    const uint32_t r = process_pair_warp(a, a.perm ? a.perm[tl] : tl, lane, &s_box, mesh_words, ws,
                                                          a.proposals ? ws.cls[l] : uint32_t(MLP_NO_PROPOSAL));
                     tested += r & 1u;
                     confirmed += (r >> 1) & 1u;
@@ -461,6 +463,66 @@ __global__ void __launch_bounds__(NP_BLOCK) narrowphase_propose(const NpArgs a, 
         if (i < a.n) proposals[i] = uint8_t(c);
         __syncwarp();
     }
+}
+
+// Counting sort of a polyhedron batch's pairs by learned class, so that a
+// tile of 32 pairs holds pairs of one class: the predicted-colliding pairs
+// (class 15: full SAT and clipping) share tiles, and pairs whose proposal
+// the exact test confirms share tiles and finish together.  Only the order in
+// which the pairs are processed changes (each pair writes its own slots), so
+// the results do not depend on it; the order inside a class follows the
+// atomics.  Rank of class c: 15 first, then 0..14.
+__device__ __forceinline__ uint32_t class_rank(uint32_t c) { return c >= 15u ? 0u : c + 1u; }
+__global__ void __launch_bounds__(256) partition_count(const NpArgs a, const uint8_t* __restrict__ cls,
+                                                       uint32_t* __restrict__ counts) {
+    const uint32_t n = a.n;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = i < n ? class_rank(cls[i]) : 16u;
+    // a batch with a convex mesh keeps its order: its pairs go one per warp,
+    // where grouping gains nothing
+    if (i < n) {
+        const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
+        const bool box = uint32_t(i1) < a.nb_shapes && uint32_t(i2) < a.nb_shapes &&
+                         load_shape(a.shapes, i1).kind == RP3DG_SHAPE_BOX && load_shape(a.shapes, i2).kind == RP3DG_SHAPE_BOX;
+        if (!box) counts[31] = 1u;
+    }
+    const uint32_t peers = __match_any_sync(0xffffffffu, r);
+    const uint32_t lane = threadIdx.x & 31u;
+    if (r < 16u && (peers & ((1u << lane) - 1u)) == 0) atomicAdd(counts + r, uint32_t(__popc(peers)));
+}
+__global__ void __launch_bounds__(256) partition_scatter(const uint8_t* __restrict__ cls, uint32_t n,
+                                                         uint32_t* __restrict__ counts, uint32_t* __restrict__ perm) {
+    __shared__ uint32_t base[16];
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int k = 0; k < 16; k++) { base[k] = run; run += counts[k]; }
+    }
+    __syncthreads();
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (counts[31]) {
+        if (i < n) perm[i] = i;
+        return;
+    }
+    const uint32_t r = i < n ? class_rank(cls[i]) : 16u;
+    const uint32_t peers = __match_any_sync(0xffffffffu, r);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t rank = uint32_t(__popc(peers & ((1u << lane) - 1u)));
+    const uint32_t leader = uint32_t(__ffs(peers)) - 1u;
+    uint32_t off = 0;
+    if (r < 16u && lane == leader) off = atomicAdd(counts + 16 + r, uint32_t(__popc(peers)));
+    off = __shfl_sync(0xffffffffu, off, int(leader));
+    if (r < 16u) perm[base[r] + off + rank] = i;
+}
+cudaError_t launch_partition_by_class(const NpArgs& a, const uint8_t* cls, uint32_t* counts, uint32_t* perm,
+                                      cudaStream_t stream) {
+    const uint32_t n = a.n;
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(counts, 0, 32 * sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    const uint32_t nb = (n + 255) / 256;
+    partition_count<<<nb, 256, 0, stream>>>(a, cls, counts);
+    partition_scatter<<<nb, 256, 0, stream>>>(cls, n, counts, perm);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_narrowphase_propose(const NpArgs& args, uint8_t* proposals, int num_sms, cudaStream_t stream) {

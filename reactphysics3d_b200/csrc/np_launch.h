@@ -43,11 +43,20 @@ struct NpArgs {
     // shape index -1; 5 float4 per test, slot-major (k * n + i): the three
     // vertices, the face normal and the vertex normal shared by the vertices
     const float4* tri;
+    // polyhedron batches: the order in which the tiles take the pairs (thread
+    // t of the batch processes pair perm[t]) or nullptr for 0..n-1
+    const uint32_t* perm;
 };
 
 void upload_box_tables(const BoxTables& t, cudaStream_t s);
 // Launches the kernels of one algorithm batch; *launches receives how many.
 cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaStream_t stream, int* launches);
+// Pairs of an all-box polyhedron batch grouped by their learned class
+// (colliding first, then the proposed features): perm receives the order
+// (the identity when a pair holds a convex mesh); counts is scratch for 32
+// words.
+cudaError_t launch_partition_by_class(const NpArgs& a, const uint8_t* cls, uint32_t* counts, uint32_t* perm,
+                                      cudaStream_t stream);
 // Triangle tests of one algorithm batch (4, 5 or 6), one test per thread.
 cudaError_t launch_narrowphase_tri(int algo, const NpArgs& args, int num_sms, cudaStream_t stream);
 // Learned proposals of a polyhedron batch (args.mlp must be set).

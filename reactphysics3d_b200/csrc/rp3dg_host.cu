@@ -215,6 +215,8 @@ struct rp3dg_ctx {
     float* d_mlp_scratch = nullptr;
     uint8_t* d_proposals = nullptr;
     uint32_t cap_proposals = 0;
+    uint32_t* d_perm = nullptr;     // pair order of a learned batch, then 32 counters
+    uint32_t cap_perm = 0;
     size_t cap_mlp_scratch = 0;
     int mlp_step = 0;
     bool mlp_ready = false;
@@ -393,6 +395,7 @@ void rp3dg_destroy(rp3dg_ctx* ctx) {
     cudaFree(ctx->d_mlp);
     cudaFree(ctx->d_mlp_scratch);
     cudaFree(ctx->d_proposals);
+    cudaFree(ctx->d_perm);
     cudaFree(ctx->d_dyn);
     cudaFree(ctx->d_dyn_stage);
     cudaFree(ctx->d_shape_bounds);
@@ -681,6 +684,7 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
     a.mlp_stats = learned ? mlp_stats(ctx) : nullptr;
     a.proposals = nullptr;
     a.tri = nullptr;
+    a.perm = nullptr;
     cudaSetDevice(ctx->device);
     if (learned) {
         // one proposal byte per pair, in a buffer that grows with the batch
@@ -695,6 +699,18 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
         if (e != cudaSuccess) return cuda_fail(ctx, e, "learned proposals");
         ctx->launches++;
         a.proposals = ctx->d_proposals;
+        // tiles of one learned class each (the order only, not the results)
+        if (p->n > ctx->cap_perm) {
+            cudaFree(ctx->d_perm);
+            ctx->d_perm = nullptr;
+            e = cudaMalloc(&ctx->d_perm, (size_t(p->n) + 32) * sizeof(uint32_t));
+            if (e != cudaSuccess) { ctx->cap_perm = 0; return cuda_fail(ctx, e, "cudaMalloc(pair order)"); }
+            ctx->cap_perm = p->n;
+        }
+        e = rp3dg::launch_partition_by_class(a, ctx->d_proposals, ctx->d_perm + p->n, ctx->d_perm, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "learned grouping");
+        ctx->launches += 2;
+        a.perm = ctx->d_perm;
     }
     int launched = 0;
     cudaError_t e = rp3dg::launch_narrowphase(algorithm, a, ctx->num_sms, ctx->stream, &launched);
@@ -1065,6 +1081,7 @@ int narrowphase_tri_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch
     a.mlp_stats = nullptr;
     a.proposals = nullptr;
     a.tri = tri;
+    a.perm = nullptr;
     cudaError_t e = launch_narrowphase_tri(algorithm, a, ctx->num_sms, ctx->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "triangle narrow-phase launch");
     ctx->launches++;
