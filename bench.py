@@ -502,7 +502,9 @@ def many_worlds_section(ctx, args, with_cpu):
     shapes, scs = scenes.many_worlds(n, seed=args.seed)
     threads = os.cpu_count() or 1
     g = engine.WorldGroup(ctx, scs, shapes, threads=threads)
+    g.autotune(rounds=2)             # 18 of the warm-up steps: island scheduling (results unchanged)
     g.update(dt, warm)
+    tuning = g.tuning()
     launches0 = ctx.kernel_launches()
     t0 = time.perf_counter()
     g.update(dt, timed)
@@ -518,6 +520,7 @@ def many_worlds_section(ctx, args, with_cpu):
            "worlds": n, "bodies": int(sum(len(s_.bodies) for s_ in scs)),
            "world_steps_per_s": round(n * timed / sec, 1), "ms_per_step": round(1e3 * sec / timed, 3),
            "kernels_per_step": round(launches, 1), "host_threads": threads, "phase_ms_per_step": phases,
+           "autotuned_scheduling": tuning,
            "stats_at_step_120": st, "api": "rp3dg_world_update (world group)"}
     if with_cpu and reflib.have_ref("f32"):
         raw = scenes.many_worlds(n, seed=args.seed, merge=False)

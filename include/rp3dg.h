@@ -627,6 +627,18 @@ int rp3dg_world_set_profiling(rp3dg_world* world, int enable);
  * moved set's order, so results do not depend on the count).  A world from
  * rp3dg_world_create starts with 1. */
 int rp3dg_world_set_threads(rp3dg_world* world, int threads);
+/* Autotuner of the dynamics stage's island scheduling (no counterpart in the
+ * reference): over the next steps, candidate settings of one parameter at a
+ * time are tried on successive steps, `rounds` steps each, and timed with
+ * CUDA events around the stage (per manifold); the fastest is kept.  The
+ * parameters (islands of up to small_max manifolds: one thread each; above
+ * giant_min: one CTA each; persistent CTAs per SM of the warp-per-island
+ * kernel: large_per_sm) only decide which kernel takes which island, so
+ * results are identical for every candidate.  The tuning takes
+ * 9 x rounds steps. */
+int rp3dg_world_autotune(rp3dg_world* world, int rounds);
+/* out[0..3] = small_max, giant_min, large_per_sm, 1 while tuning. */
+int rp3dg_world_get_tuning(rp3dg_world* world, uint32_t* out);
 int rp3dg_world_get_phase_times(rp3dg_world* world, double* ms, uint32_t n);
 
 /* Number of kernels this context launched so far (instrumentation; a

@@ -592,7 +592,7 @@ RD void store_manifold(const DynArgs& a, uint32_t mi) {
 // movable body, the order of the manifolds touching it gives bit-identical
 // results.
 //
-// 3a: one thread per island runs islands of up to SMALL_ISLAND manifolds in
+// 3a: one thread per island runs islands of up to small_max manifolds in
 //     the reference's order and queues the larger ones.
 // 3b: persistent warps take the queued islands.  Lane 0 gives each manifold a
 //     level (1 + the highest level of an earlier manifold sharing a movable
@@ -606,11 +606,10 @@ RD void store_manifold(const DynArgs& a, uint32_t mi) {
 //     velocities.  Larger islands use the same schedule built in global
 //     scratch, with velocities in global memory.
 
-constexpr uint32_t SMALL_ISLAND = 8;
+// (a.small_max, 8 by default, and a.giant_min, 256 by default: islands above
+// it go to kernel 3c, one CTA per island, the island staged in up to the
+// whole opt-in shared memory of a CTA; both come from DynTuning)
 constexpr uint32_t BIG_ISLAND = 64;   // queued first: the longest islands start first
-// islands above this many manifolds go to kernel 3c (one CTA per island,
-// the island staged in up to the whole opt-in shared memory of a CTA)
-constexpr uint32_t GIANT_ISLAND = 256;
 
 RD int4 man_ids(const DynArgs& a, uint32_t mi) {
     const float4 q = __ldg(a.mrec[mi].q + DQ_IDS);
@@ -628,9 +627,9 @@ __global__ void __launch_bounds__(128) dyn_islands_small(const DynArgs a) {
     }
     if (a.i_jcount && a.i_jcount[is]) return;  // kernel 3d
     if (cnt == 0) return;
-    if (cnt > SMALL_ISLAND) {
+    if (cnt > a.small_max) {
         // big islands fill the list from the front, the others from the back
-        if (cnt > GIANT_ISLAND) a.giant_list[atomicAdd(a.counters + 3, 1u)] = is;
+        if (cnt > a.giant_min) a.giant_list[atomicAdd(a.counters + 3, 1u)] = is;
         else if (cnt > BIG_ISLAND) a.large_list[atomicAdd(a.counters, 1u)] = is;
         else a.large_list[a.ni - 1 - atomicAdd(a.counters + 2, 1u)] = is;
         return;
@@ -918,7 +917,7 @@ __global__ void __launch_bounds__(64) dyn_joints_position(const DynArgs a) {
     }
 }
 
-// ---- kernel 3c: islands of more than GIANT_ISLAND manifolds --------------
+// ---- kernel 3c: islands of more than giant_min manifolds -----------------
 //
 // One CTA of two warps takes one island at a time with the CTA's whole opt-in
 // shared memory: the movable bodies' velocities, every manifold's and point's

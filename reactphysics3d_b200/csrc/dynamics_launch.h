@@ -116,6 +116,8 @@ struct DynArgs {
     uint32_t* large_list;  // ni: queued islands
     uint32_t* giant_list;  // ni: islands for kernel 3c
     uint32_t large_ctas;   // grid of kernel 3b (persistent)
+    uint32_t small_max;    // islands of up to this many manifolds: one thread each (kernel 3a)
+    uint32_t giant_min;    // islands above this many manifolds: one CTA each (kernel 3c)
     // joints (nj = 0: none).  j_list holds this step's enabled joints island
     // by island, each island's ball-and-socket joints then hinge joints in
     // component order: record index, body 1 row, body 2 row, bit 0 / bit 1 =
@@ -150,6 +152,13 @@ struct DynJoints {
     const int32_t* ji_rows;
     float4 *xc, *qc;
     int32_t position_iterations;
+};
+
+// Scheduling of the islands over the kernels (results do not depend on it):
+// thread-per-island limit, one-CTA-per-island threshold and persistent CTAs
+// per SM of the warp-per-island kernel.
+struct DynTuning {
+    uint32_t small_max = 8, giant_min = 256, large_per_sm = 2;
 };
 
 // Launches the kernels in order on stream s; *launches counts them.

@@ -328,7 +328,7 @@ namespace rp3dg {
 int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
                         const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
                         const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled,
-                        const DynJoints* joints = nullptr);
+                        const DynJoints* joints = nullptr, const DynTuning* tune = nullptr);
 int broadphase_update_flags(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, const uint8_t* enabled);
 }  // namespace rp3dg
 
@@ -1139,7 +1139,7 @@ namespace rp3dg {
 int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
                         const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
                         const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled,
-                        const DynJoints* joints) {
+                        const DynJoints* joints, const DynTuning* tune) {
     int rc = check_dynamics(ctx, pr, b, c, m, p, is);
     if (rc) return rc;
     const void* f16[] = {b->position, b->orientation, b->com_world, b->com_local, b->linear_velocity,
@@ -1232,7 +1232,11 @@ int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const r
     a.counters = reinterpret_cast<uint32_t*>(s + off_cnt);
     a.large_list = reinterpret_cast<uint32_t*>(s + off_list);
     a.giant_list = reinterpret_cast<uint32_t*>(s + off_giant);
-    a.large_ctas = uint32_t(ctx->num_sms) * 2;
+    const rp3dg::DynTuning tdef{};
+    const rp3dg::DynTuning& tn = tune ? *tune : tdef;
+    a.large_ctas = uint32_t(ctx->num_sms) * (tn.large_per_sm ? tn.large_per_sm : 1u);
+    a.small_max = tn.small_max;
+    a.giant_min = tn.giant_min;
     a.giant_ctas = uint32_t(ctx->num_sms);
     // the opt-in maximum less room for the kernel's static shared memory
     a.giant_smem = ctx->smem_optin > 2048 ? uint32_t(ctx->smem_optin - 1024) : 0u;

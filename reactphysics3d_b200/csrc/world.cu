@@ -67,7 +67,7 @@ void set_error(rp3dg_ctx* ctx, const std::string& msg);
 int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
                         const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
                         const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled,
-                        const DynJoints* joints);
+                        const DynJoints* joints, const DynTuning* tune);
 int broadphase_update_flags(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, const uint8_t* enabled);
 // height fields, the shape table and its local bounds on the device, and the
 // triangle tests of convex vs concave pairs
@@ -701,6 +701,19 @@ struct rp3dg_world {
     rp3dg_lastframe* d_tcache[2] = {nullptr, nullptr};
     int cur_tc = 0;
     cudaEvent_t ev_rect = nullptr;
+    // island scheduling and its autotuner: candidates are tried on successive
+    // steps (round robin, `rounds` times each), timed with CUDA events around
+    // the dynamics stage per manifold, one parameter after the other
+    rp3dg::DynTuning tune{};
+    struct Tuner {
+        bool active = false;
+        int phase = 0, rounds = 2, idx = 0;
+        std::vector<rp3dg::DynTuning> cands;
+        std::vector<std::vector<float>> score;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        bool timed = false;
+        uint32_t nm = 0;
+    } tuner;
     // broad-phase tree queries on the GPU (worlds with many moved colliders)
     rp3dg::order::Tree::Node *h_tnodes = nullptr, *d_tnodes = nullptr;
     size_t cap_tnodes = 0, cap_tq = 0, cap_tleaves = 0, cap_tpos = 0, cap_tcnt = 0;
@@ -1661,6 +1674,8 @@ void destroy_group(Group* g) {
     cudaFree(g->d_tr2); cudaFree(g->d_trep); cudaFree(g->d_tcoll); cudaFree(g->d_tnct); cudaFree(g->d_tmid);
     cudaFree(g->d_tnd); cudaFree(g->d_tl1); cudaFree(g->d_tl2); cudaFree(g->d_tri);
     cudaFree(g->d_tcache[0]); cudaFree(g->d_tcache[1]); cudaFree(g->d_hf);
+    if (g->tuner.e0) cudaEventDestroy(g->tuner.e0);
+    if (g->tuner.e1) cudaEventDestroy(g->tuner.e1);
     cudaFreeHost(g->h_tnodes); cudaFree(g->d_tnodes); cudaFreeHost(g->h_tq); cudaFree(g->d_tq);
     cudaFreeHost(g->h_tleaves); cudaFree(g->d_tleaves); cudaFreeHost(g->h_tpos); cudaFree(g->d_tpos);
     cudaFreeHost(g->h_tcnt); cudaFree(g->d_tcnt);
@@ -1965,6 +1980,8 @@ int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds
     *out = g;
     return 0;
 }
+
+void tuner_step(Group* g);
 
 int update_group(Group* g, float dt) {
     if (!g) return RP3DG_EINVAL;
@@ -2425,8 +2442,18 @@ int update_group(Group* g, float dt) {
             J.qc = g->bcol[bc][BC_QC];
             J.position_iterations = g->set.position_iterations;
         }
-        rc = rp3dg::dynamics_step_flags(ctx, &pr, &B, &C, &Mf, &P, &I, g->b_en, g->c_en, NJ ? &J : nullptr);
+        // the candidate of this step while the autotuner runs
+        Group::Tuner& tu = g->tuner;
+        const bool tuning = tu.active && !tu.cands.empty();
+        const rp3dg::DynTuning tn = tuning ? tu.cands[size_t(tu.idx) % tu.cands.size()] : g->tune;
+        if (tuning) cudaEventRecord(tu.e0, st);
+        rc = rp3dg::dynamics_step_flags(ctx, &pr, &B, &C, &Mf, &P, &I, g->b_en, g->c_en, NJ ? &J : nullptr, &tn);
         if (rc) return rc;
+        if (tuning) {
+            cudaEventRecord(tu.e1, st);
+            tu.timed = true;
+            tu.nm = NM;
+        }
         // the pageable joint-island vectors are read by the copies above
         if (NJ) cudaStreamSynchronize(st);
     }
@@ -2486,6 +2513,7 @@ int update_group(Group* g, float dt) {
     cudaMemsetAsync(g->bcol[bc][BC_T], 0, size_t(g->NB) * 16, st);
     e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return wcuda(g, e, "end of step");
+    tuner_step(g);
     g->cur_cb = 1 - g->cur_cb;
     for (WorldH& w : g->worlds) {
         w.stepped = true;
@@ -2496,6 +2524,46 @@ int update_group(Group* g, float dt) {
     }
     mark(7);
     return 0;
+}
+
+// The candidates of one autotuner phase: the current scheduling with one
+// parameter varied (0: thread-per-island limit, 1: one-CTA-per-island
+// threshold, 2: warp-kernel CTAs per SM).
+std::vector<rp3dg::DynTuning> tuner_candidates(const rp3dg::DynTuning& base, int phase) {
+    std::vector<rp3dg::DynTuning> c;
+    const uint32_t small[] = {4, 8, 16, 32}, giant[] = {128, 256, 512}, per_sm[] = {1, 2};
+    if (phase == 0) for (uint32_t v : small) { rp3dg::DynTuning t = base; t.small_max = v; c.push_back(t); }
+    if (phase == 1) for (uint32_t v : giant) { rp3dg::DynTuning t = base; t.giant_min = v; c.push_back(t); }
+    if (phase == 2) for (uint32_t v : per_sm) { rp3dg::DynTuning t = base; t.large_per_sm = v; c.push_back(t); }
+    return c;
+}
+
+// After a step's end: record the timed candidate; at the end of a phase keep
+// the candidate with the lowest median time per manifold and start the next.
+void tuner_step(Group* g) {
+    Group::Tuner& tu = g->tuner;
+    if (!tu.active || !tu.timed) return;
+    tu.timed = false;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, tu.e0, tu.e1) != cudaSuccess) return;
+    const size_t k = size_t(tu.idx) % tu.cands.size();
+    tu.score[k].push_back(ms / float(std::max<uint32_t>(tu.nm, 1)));
+    tu.idx++;
+    if (size_t(tu.idx) < tu.cands.size() * size_t(tu.rounds)) return;
+    size_t best = 0;
+    float best_t = 3.4e38f;
+    for (size_t i = 0; i < tu.cands.size(); i++) {
+        std::vector<float> v = tu.score[i];
+        std::sort(v.begin(), v.end());
+        const float med = v.empty() ? 3.4e38f : v[v.size() / 2];
+        if (med < best_t) { best_t = med; best = i; }
+    }
+    g->tune = tu.cands[best];
+    tu.phase++;
+    tu.idx = 0;
+    tu.cands = tuner_candidates(g->tune, tu.phase);
+    tu.score.assign(tu.cands.size(), std::vector<float>());
+    if (tu.cands.empty()) tu.active = false;
 }
 
 // Host quaternion / vector arithmetic with the reference's expression trees
@@ -2757,6 +2825,30 @@ int rp3dg_world_get_contacts(rp3dg_world* w, int32_t* body1, int32_t* body2, uin
 int rp3dg_world_get_stats(rp3dg_world* w, rp3dg_world_stats* s) {
     if (!w || !s) return RP3DG_EINVAL;
     *s = w->stats;
+    return 0;
+}
+
+int rp3dg_world_autotune(rp3dg_world* w, int rounds) {
+    if (!w || rounds < 1) return RP3DG_EINVAL;
+    Group::Tuner& tu = w->tuner;
+    if (!tu.e0 && (cudaEventCreate(&tu.e0) != cudaSuccess || cudaEventCreate(&tu.e1) != cudaSuccess))
+        return wfail(w, RP3DG_ECUDA, "cudaEventCreate(autotuner)");
+    tu.active = true;
+    tu.rounds = rounds;
+    tu.phase = 0;
+    tu.idx = 0;
+    tu.timed = false;
+    tu.cands = tuner_candidates(w->tune, 0);
+    tu.score.assign(tu.cands.size(), std::vector<float>());
+    return 0;
+}
+
+int rp3dg_world_get_tuning(rp3dg_world* w, uint32_t* out) {
+    if (!w || !out) return RP3DG_EINVAL;
+    out[0] = w->tune.small_max;
+    out[1] = w->tune.giant_min;
+    out[2] = w->tune.large_per_sm;
+    out[3] = w->tuner.active ? 1u : 0u;
     return 0;
 }
 

@@ -96,6 +96,8 @@ def load_library(path=LIB_PATH):
     L.rp3dg_world_get_stats.argtypes = [P, P]
     L.rp3dg_world_set_profiling.argtypes = [P, C.c_int]
     L.rp3dg_world_set_threads.argtypes = [P, C.c_int]
+    L.rp3dg_world_autotune.argtypes = [P, C.c_int]
+    L.rp3dg_world_get_tuning.argtypes = [P, P]
     L.rp3dg_world_add_joints.argtypes = [P, P, C.c_uint32]
     L.rp3dg_world_group_add_joints.argtypes = [P, C.c_uint32, P, C.c_uint32]
     L.rp3dg_world_group_create.argtypes = [P, P, C.c_uint32, P, P, P, P, C.c_int, C.POINTER(P)]
@@ -545,6 +547,17 @@ class World:
         rc = self.lib.rp3dg_world_set_threads(self.h, int(n))
         if rc != 0:
             raise Rp3dgError(rc, "bad thread count")
+
+    def autotune(self, rounds=2):
+        """Tune the island scheduling over the next 9 * rounds steps (results unchanged)."""
+        rc = self.lib.rp3dg_world_autotune(self.h, int(rounds))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+
+    def tuning(self):
+        t = np.zeros(4, np.uint32)
+        self.lib.rp3dg_world_get_tuning(self.h, t.ctypes.data)
+        return {"small_max": int(t[0]), "giant_min": int(t[1]), "large_per_sm": int(t[2]), "tuning": bool(t[3])}
 
     def set_profiling(self, on=True):
         self.lib.rp3dg_world_set_profiling(self.h, int(on))

@@ -223,6 +223,29 @@ def test_world_group_matches_each_reference_world(ctx):
     g.close()
 
 
+def test_autotuned_scheduling_gives_identical_results(ctx):
+    """The autotuner varies which kernel takes which island and how many
+    persistent CTAs run; the results must not depend on it: a group tuned
+    over its first steps ends bit-identical to the same group untuned, and
+    the chosen setting is one of the candidates."""
+    shapes, scs = scenes.many_worlds(96, seed=21, min_bodies=20, max_bodies=200, ragdolls=(1, 2), limits=True)
+    a = engine.WorldGroup(ctx, scs, shapes, threads=4)
+    b = engine.WorldGroup(ctx, scs, shapes, threads=4)
+    a.autotune(rounds=1)
+    assert a.tuning()["tuning"]
+    for _ in range(40):
+        a.update(float(worldio.DT))
+        b.update(float(worldio.DT))
+    t = a.tuning()
+    assert not t["tuning"]
+    assert t["small_max"] in (4, 8, 16, 32) and t["giant_min"] in (128, 256, 512) and t["large_per_sm"] in (1, 2)
+    for k in range(len(scs)):
+        for x, y in zip(a.bodies(k), b.bodies(k)):
+            assert np.array_equal(x, y), k
+    a.close()
+    b.close()
+
+
 @pytest.mark.skipif(not (reflib.have_ref("f32") and reflib.have_ref("f64")), reason="reference engine not built")
 def test_ragdolls_with_limits_stay_within_tolerance(ctx):
     """Cone and hinge limits go through acos / atan2, whose last bit differs
