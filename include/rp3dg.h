@@ -457,9 +457,10 @@ int rp3dg_broadphase_pairs_host(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, int 
  * the moved-collider set, the persistent overlapping-pair arrays, contact-pair
  * order, islands, component order and sleeping) so that every step processes
  * pairs, contacts and constraints in the reference's own order and the results
- * are the reference float build's, bit for bit.  Worlds without joints, with
- * convex colliders (sphere, capsule, box, convex mesh), simulation colliders
- * only (no triggers), with ball-and-socket and hinge joints, are supported.
+ * are the reference float build's, bit for bit.  Worlds with convex
+ * colliders (sphere, capsule, box, convex mesh) and height fields, simulation
+ * colliders only (no triggers), with ball-and-socket, hinge, fixed and slider
+ * joints, are supported.
  *
  * rp3dg_world_create mirrors this sequence of reference calls, body by body:
  *   b = world->createRigidBody(Transform(position, orientation));
@@ -515,25 +516,31 @@ typedef struct rp3dg_collider_desc {
     uint16_t mask;                 /* collide-with mask bits (0xffff by default) */
 } rp3dg_collider_desc;
 
-/* A joint, as PhysicsWorld::createJoint(JointInfo) (PhysicsWorld.cpp) creates
- * it from a BallAndSocketJointInfo / HingeJointInfo with world-space anchor
- * (and hinge axis), followed for a ball-and-socket joint with a cone limit by
+/* A joint, as PhysicsWorld::createJoint(JointInfo) (PhysicsWorld.cpp:467-580)
+ * creates it from a BallAndSocketJointInfo / HingeJointInfo / FixedJointInfo /
+ * SliderJointInfo with a world-space anchor (and hinge or slider axis),
+ * followed for a ball-and-socket joint with a cone limit by
  * joint->enableConeLimit(true) and joint->setConeLimitHalfAngle(angle).  Only
- * the NON_LINEAR_GAUSS_SEIDEL position correction (the default) is built. */
+ * the NON_LINEAR_GAUSS_SEIDEL position correction (the default) is built.
+ * The hinge and slider joints share the limit and motor fields: angles in
+ * radians and a torque for a hinge, translations along the axis and a force
+ * for a slider (minTranslationLimit, maxTranslationLimit, maxMotorForce). */
 #define RP3DG_JOINT_BALL_AND_SOCKET 0
 #define RP3DG_JOINT_HINGE 1
+#define RP3DG_JOINT_FIXED 2
+#define RP3DG_JOINT_SLIDER 3
 typedef struct rp3dg_joint_desc {
     int32_t type;                  /* RP3DG_JOINT_* */
     int32_t body1, body2;          /* body indices of the world */
     float anchor[3];               /* anchor point, world space, at creation */
-    float axis[3];                 /* hinge: rotation axis, world space */
+    float axis[3];                 /* hinge: rotation axis; slider: sliding axis; world space */
     int32_t collision_enabled;     /* JointInfo::isCollisionEnabled (0: the two bodies never collide) */
     int32_t cone_limit_enabled;    /* ball-and-socket */
     float cone_half_angle;         /* ball-and-socket, radians (PI by default) */
-    int32_t limit_enabled;         /* hinge */
-    float min_angle, max_angle;    /* hinge limits, radians (-1, 1 when disabled, the reference's defaults) */
-    int32_t motor_enabled;         /* hinge */
-    float motor_speed, max_motor_torque;
+    int32_t limit_enabled;         /* hinge, slider */
+    float min_angle, max_angle;    /* hinge: angle limits, radians; slider: translation limits (-1, 1 when disabled, the reference's defaults) */
+    int32_t motor_enabled;         /* hinge, slider */
+    float motor_speed, max_motor_torque;  /* hinge: rad/s, N m; slider: m/s, N (maxMotorForce) */
 } rp3dg_joint_desc;
 
 typedef struct rp3dg_world rp3dg_world;
@@ -560,8 +567,15 @@ void rp3dg_world_destroy(rp3dg_world* world);
 /* createJoint for each of the n joints, in order; before the first update.
  * The joints are solved in islands with their bodies, warm-started, with
  * the reference's velocity solve and non-linear Gauss-Seidel position
- * correction (SolveBallAndSocketJointSystem.cpp, SolveHingeJointSystem.cpp). */
+ * correction (SolveBallAndSocketJointSystem.cpp, SolveFixedJointSystem.cpp,
+ * SolveHingeJointSystem.cpp, SolveSliderJointSystem.cpp). */
 int rp3dg_world_add_joints(rp3dg_world* world, const rp3dg_joint_desc* joints, uint32_t n);
+/* HingeJoint::setMotorSpeed / SliderJoint::setMotorSpeed (HingeJoint.cpp:168,
+ * SliderJoint.cpp:210) between updates, on joint `joint` (index in the order
+ * the joints were added) of world `world` (0 for rp3dg_world_create, the
+ * group index otherwise): a changed speed wakes the joint's two bodies.
+ * RP3DG_EINVAL for a ball-and-socket or fixed joint. */
+int rp3dg_world_set_motor_speed(rp3dg_world* world, uint32_t world_index, uint32_t joint, float speed);
 /* PhysicsWorld::update(dt): one step (synchronous). */
 int rp3dg_world_update(rp3dg_world* world, float dt);
 /* Body state in creation order (host arrays of nb_bodies rows, any may be

@@ -59,6 +59,7 @@ struct World {
     PhysicsCommon common;
     PhysicsWorld* world = nullptr;
     std::vector<RigidBody*> bodies;
+    std::vector<Joint*> joints;  // in creation order
     Capture cap;
 };
 
@@ -593,10 +594,25 @@ int ref_scene_add_joints(int id, const rp3dg_joint_desc* jd, uint32_t n) {
             BallAndSocketJointInfo info(b1, b2, anchor);
             info.isCollisionEnabled = d.collision_enabled != 0;
             auto* j = static_cast<BallAndSocketJoint*>(W.world->createJoint(info));
+            W.joints.push_back(j);
             if (d.cone_limit_enabled) {
                 j->enableConeLimit(true);
                 j->setConeLimitHalfAngle(d.cone_half_angle);
             }
+        } else if (d.type == RP3DG_JOINT_FIXED) {
+            FixedJointInfo info(b1, b2, anchor);
+            info.isCollisionEnabled = d.collision_enabled != 0;
+            W.joints.push_back(W.world->createJoint(info));
+        } else if (d.type == RP3DG_JOINT_SLIDER) {
+            SliderJointInfo info(b1, b2, anchor, Vector3(d.axis[0], d.axis[1], d.axis[2]));
+            info.isCollisionEnabled = d.collision_enabled != 0;
+            info.isLimitEnabled = d.limit_enabled != 0;
+            info.minTranslationLimit = d.min_angle;
+            info.maxTranslationLimit = d.max_angle;
+            info.isMotorEnabled = d.motor_enabled != 0;
+            info.motorSpeed = d.motor_speed;
+            info.maxMotorForce = d.max_motor_torque;
+            W.joints.push_back(W.world->createJoint(info));
         } else {
             HingeJointInfo info(b1, b2, anchor, Vector3(d.axis[0], d.axis[1], d.axis[2]));
             info.isCollisionEnabled = d.collision_enabled != 0;
@@ -606,10 +622,25 @@ int ref_scene_add_joints(int id, const rp3dg_joint_desc* jd, uint32_t n) {
             info.isMotorEnabled = d.motor_enabled != 0;
             info.motorSpeed = d.motor_speed;
             info.maxMotorTorque = d.max_motor_torque;
-            W.world->createJoint(info);
+            W.joints.push_back(W.world->createJoint(info));
         }
     }
     return 0;
+}
+
+// HingeJoint::setMotorSpeed / SliderJoint::setMotorSpeed on joint k.
+int ref_scene_set_motor_speed(int id, uint32_t k, float speed) {
+    World& W = *worlds().at(size_t(id));
+    Joint* j = W.joints.at(size_t(k));
+    if (auto* h = dynamic_cast<HingeJoint*>(j)) {
+        h->setMotorSpeed(speed);
+        return 0;
+    }
+    if (auto* sl = dynamic_cast<SliderJoint*>(j)) {
+        sl->setMotorSpeed(speed);
+        return 0;
+    }
+    return -1;
 }
 
 // Body state in creation order.

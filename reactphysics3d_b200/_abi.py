@@ -130,7 +130,7 @@ COLLIDER_DESC_DTYPE = np.dtype([
 WORLD_STATS_DTYPE = np.dtype([(k, "<u4") for k in (
     "overlapping_pairs", "disabled_pairs", "narrowphase_tests", "contact_pairs", "manifolds",
     "contact_points", "islands", "enabled_bodies", "moved_colliders", "reserved")])
-JOINT_BALL_AND_SOCKET, JOINT_HINGE = 0, 1
+JOINT_BALL_AND_SOCKET, JOINT_HINGE, JOINT_FIXED, JOINT_SLIDER = 0, 1, 2, 3
 JOINT_DESC_DTYPE = np.dtype([
     ("type", "<i4"), ("body1", "<i4"), ("body2", "<i4"), ("anchor", "<f4", (3,)), ("axis", "<f4", (3,)),
     ("collision_enabled", "<i4"), ("cone_limit_enabled", "<i4"), ("cone_half_angle", "<f4"),
@@ -160,7 +160,7 @@ def default_world_settings():
 
 def joint_descs(n):
     """JointInfo defaults: collision enabled, no cone limit (half angle PI),
-    hinge limits off (-1, 1), no motor."""
+    hinge / slider limits off (-1, 1), no motor."""
     j = np.zeros(n, JOINT_DESC_DTYPE)
     j["collision_enabled"] = 1
     j["cone_half_angle"] = np.float32(3.141592653589)

@@ -37,22 +37,33 @@ struct __align__(16) DynPointRec {
 };
 
 // Per-joint record (joints.cuh): constant rows set on creation (type and
-// flags, local anchors, local hinge axes, inverse initial orientation
-// difference, limits / motor parameters), accumulated impulses and limit
-// state carried from step to step, and the rows initBeforeSolve computes.
+// flags, local anchors, local hinge / slider axes, inverse initial
+// orientation difference, limits / motor parameters), accumulated impulses
+// and limit state carried from step to step, and the rows initBeforeSolve
+// computes.
 enum JointRow {
-    JR_HDR = 0,     // x type (0 ball-and-socket, 1 hinge), y flags (int bits)
+    JR_HDR = 0,     // x type (RP3DG_JOINT_*), y flags (int bits)
     JR_LA1, JR_LA2, // local anchor points
-    JR_AX1, JR_AX2, // hinge: local axes
-    JR_QINV,        // hinge: inverse initial orientation difference (quaternion)
+    JR_AX1, JR_AX2, // hinge: local axes; slider: local axis of body 1 (AX1)
+    JR_QINV,        // hinge, fixed, slider: inverse initial orientation difference (quaternion)
     JR_PARAM,       // x cone half angle, y lower limit, z upper limit, w motor speed
-    JR_PARAM2,      // x max motor torque
-    JR_IMP,         // ball-and-socket impulse / hinge translation impulse
-    JR_IMP2,        // hinge: rotation impulse x, y, lower-limit impulse, upper-limit impulse
-    JR_STATE,       // ball-and-socket: cone impulse, cone violated; hinge: lower / upper violated, motor impulse
+    JR_PARAM2,      // x max motor torque (hinge) / force (slider)
+    JR_IMP,         // ball-and-socket impulse / hinge, fixed translation impulse /
+                    // slider: translation impulse x, y, lower-limit impulse, upper-limit impulse
+    JR_IMP2,        // hinge: rotation impulse x, y, lower-limit impulse, upper-limit impulse;
+                    // fixed, slider: rotation impulse
+    JR_STATE,       // ball-and-socket: cone impulse, cone violated;
+                    // hinge, slider: lower / upper violated, motor impulse
     JR_R1, JR_R2,
     JR_I1, JR_I2 = JR_I1 + 3, JR_K = JR_I2 + 3, JR_ACB = JR_K + 3,
-    JR_A1, JR_B2A1, JR_C2A1, JR_KROT, JR_MISC,
+    JR_A1,          // hinge / slider axis in world space
+    JR_B2A1, JR_C2A1,
+    JR_KROT,        // 2x2 inverse mass: hinge rotation, slider translation
+    JR_MISC,        // x inverse mass of the limits (and of the hinge motor), y slider motor inverse mass
+    JR_KR3,         // fixed, slider: 3x3 rotation inverse mass (3 rows)
+    JR_N1 = JR_KR3 + 3, JR_N2,             // slider: the two axes orthogonal to the slider axis
+    JR_R2N1, JR_R2N2, JR_R2A,              // slider: r2 x n1, r2 x n2, r2 x axis
+    JR_R1N1, JR_R1N2, JR_R1A,              // slider: (r1 + u) x n1, x n2, x axis
     JR_ROWS
 };
 enum JointFlags { JF_CONE = 1, JF_LIMIT = 2, JF_MOTOR = 4 };
@@ -119,8 +130,8 @@ struct DynArgs {
     uint32_t small_max;    // islands of up to this many manifolds: one thread each (kernel 3a)
     uint32_t giant_min;    // islands above this many manifolds: one CTA each (kernel 3c)
     // joints (nj = 0: none).  j_list holds this step's enabled joints island
-    // by island, each island's ball-and-socket joints then hinge joints in
-    // component order: record index, body 1 row, body 2 row, bit 0 / bit 1 =
+    // by island, each island's ball-and-socket, fixed, hinge then slider
+    // joints, each type in component order: record index, body 1 row, body 2 row, bit 0 / bit 1 =
     // body 1 / body 2 dynamic.  Islands with joints (i_jcount > 0) are solved
     // by kernel 3d; after the position integration kernel 4b runs the
     // position correction of their joints and updates their bodies' state.

@@ -1,6 +1,8 @@
 // Joints of the dynamics stage: ball-and-socket (SolveBallAndSocketJointSystem,
-// reference src/systems/SolveBallAndSocketJointSystem.cpp) and hinge
-// (SolveHingeJointSystem, src/systems/SolveHingeJointSystem.cpp): the per-step
+// reference src/systems/SolveBallAndSocketJointSystem.cpp), hinge
+// (src/systems/SolveHingeJointSystem.cpp), fixed
+// (src/systems/SolveFixedJointSystem.cpp) and slider
+// (src/systems/SolveSliderJointSystem.cpp): the per-step
 // initialisation (initBeforeSolve), warm start, velocity solve and the
 // non-linear Gauss-Seidel position correction, one joint at a time, with the
 // reference's float expression trees (Matrix3x3 / Matrix2x2 / Quaternion /
@@ -173,10 +175,425 @@ RD JBody jbody(const DynArgs& a, int32_t b, bool dynamic) {
     return r;
 }
 
+// --- fixed joint (SolveFixedJointSystem.cpp) ------------------------------
+constexpr uint32_t JT_FIXED = 2, JT_SLIDER = 3;
+
+// 3x3 rotation inverse mass: I1 + I2, inverted when its determinant is not
+// tiny and a body is dynamic, else left as the sum (the reference keeps it).
+RD M3 rotation_inverse_mass(const M3& I1, const M3& I2, bool dyn, bool* ok) {
+    M3 K = m3_add(I1, I2);
+    const float det = m3_det(K);
+    *ok = fabsf(det) > MACHINE_EPSILON;
+    if (*ok && dyn) K = m3_inverse(K, det);
+    return K;
+}
+// 2 * (q2 * qinv0 * q1^-1).getVectorV() (SolveFixedJointSystem.cpp:419-421)
+RD v3 rotation_error(quat q1, quat q2, float4 f0) {
+    const quat e = qmul(qmul(q2, Q(f0.x, f0.y, f0.z, f0.w)), qinv(q1));
+    return V(2.0f * e.x, 2.0f * e.y, 2.0f * e.z);
+}
+
+// initBeforeSolve (:49-133)
+RD void fixed_init(const DynArgs& a, const int4 e) {
+    float4* q = a.j_rec[e.x].q;
+    const int32_t b1 = e.y, b2 = e.z;
+    const bool dyn = (e.w & 3) != 0;
+    const M3 I1 = iiw_of(a, b1), I2 = iiw_of(a, b2);
+    st3(q + JR_I1, I1);
+    st3(q + JR_I2, I2);
+    const float4 o1 = a.orientation[b1], o2 = a.orientation[b2];
+    const quat q1 = Q(o1.x, o1.y, o1.z, o1.w), q2 = Q(o2.x, o2.y, o2.z, o2.w);
+    const v3 r1 = qrot(q1, vsub(L3v(q[JR_LA1]), L3v(a.com_local[b1])));
+    const v3 r2 = qrot(q2, vsub(L3v(q[JR_LA2]), L3v(a.com_local[b2])));
+    q[JR_R1] = F4v(r1);
+    q[JR_R2] = F4v(r2);
+    const M3 K = joint_mass_matrix(a.mass[b1].y + a.mass[b2].y, m3_skew(r1), I1, m3_skew(r2), I2);
+    M3 Kinv = m3_zero();
+    const float det = m3_det(K);
+    if (fabsf(det) > MACHINE_EPSILON && dyn) Kinv = m3_inverse(K, det);
+    st3(q + JR_K, Kinv);
+    bool ok;
+    st3(q + JR_KR3, rotation_inverse_mass(I1, I2, dyn, &ok));
+}
+
+// warmstart (:136-186)
+RD void fixed_warm(const DynArgs& a, const int4 e) {
+    float4* q = a.j_rec[e.x].q;
+    const JBody B1 = jbody(a, e.y, false), B2 = jbody(a, e.z, false);
+    v3 v1 = L3v(a.cv[e.y]), w1 = L3v(a.cw[e.y]), v2 = L3v(a.cv[e.z]), w2 = L3v(a.cw[e.z]);
+    const M3 I1 = ld3(q + JR_I1), I2 = ld3(q + JR_I2);
+    const v3 r1 = L3v(q[JR_R1]), r2 = L3v(q[JR_R2]);
+    const v3 it = L3v(q[JR_IMP]), ir = L3v(q[JR_IMP2]);
+    v3 ang1 = vcross(it, r1);
+    ang1 = v3add(ang1, vneg(ir));
+    v1 = v3add(v1, lin(B1.im, B1.lf, vneg(it)));
+    w1 = v3add(w1, vcmul(B1.af, m3_mulv(I1, ang1)));
+    v3 ang2 = vneg(vcross(it, r2));
+    ang2 = v3add(ang2, ir);
+    v2 = v3add(v2, lin(B2.im, B2.lf, it));
+    w2 = v3add(w2, vcmul(B2.af, m3_mulv(I2, ang2)));
+    a.cv[e.y] = F4v(v1); a.cw[e.y] = F4v(w1);
+    a.cv[e.z] = F4v(v2); a.cw[e.z] = F4v(w2);
+}
+
+// solveVelocityConstraint (:189-262)
+RD void fixed_solve(const DynArgs& a, const int4 e) {
+    float4* q = a.j_rec[e.x].q;
+    const JBody B1 = jbody(a, e.y, false), B2 = jbody(a, e.z, false);
+    v3 v1 = L3v(a.cv[e.y]), w1 = L3v(a.cw[e.y]), v2 = L3v(a.cv[e.z]), w2 = L3v(a.cw[e.z]);
+    const M3 I1 = ld3(q + JR_I1), I2 = ld3(q + JR_I2);
+    const v3 r1 = L3v(q[JR_R1]), r2 = L3v(q[JR_R2]);
+    // translation: Jv = v2 + w2 x r2 - v1 - w1 x r1
+    const v3 Jt = vsub(vsub(v3add(v2, vcross(w2, r2)), v1), vcross(w1, r1));
+    const v3 dl = m3_mulv(ld3(q + JR_K), vsub(vneg(Jt), V(0.0f, 0.0f, 0.0f)));
+    q[JR_IMP] = F4v(v3add(L3v(q[JR_IMP]), dl));
+    v1 = v3add(v1, lin(B1.im, B1.lf, vneg(dl)));
+    w1 = v3add(w1, vcmul(B1.af, m3_mulv(I1, vcross(dl, r1))));
+    v2 = v3add(v2, lin(B2.im, B2.lf, dl));
+    w2 = v3add(w2, vcmul(B2.af, m3_mulv(I2, vneg(vcross(dl, r2)))));
+    // rotation: Jv = w2 - w1
+    const v3 Jr = vsub(w2, w1);
+    const v3 dr = m3_mulv(ld3(q + JR_KR3), vsub(vneg(Jr), V(0.0f, 0.0f, 0.0f)));
+    q[JR_IMP2] = F4v(v3add(L3v(q[JR_IMP2]), dr));
+    w1 = v3add(w1, vcmul(B1.af, m3_mulv(I1, vneg(dr))));
+    w2 = v3add(w2, vcmul(B2.af, m3_mulv(I2, dr)));
+    a.cv[e.y] = F4v(v1); a.cw[e.y] = F4v(w1);
+    a.cv[e.z] = F4v(v2); a.cw[e.z] = F4v(w2);
+}
+
+// solvePositionConstraint, NON_LINEAR_GAUSS_SEIDEL (:265-447)
+RD void fixed_position(const DynArgs& a, const int4 e) {
+    float4* q = a.j_rec[e.x].q;
+    const bool dyn = (e.w & 3) != 0;
+    const JBody B1 = jbody(a, e.y, false), B2 = jbody(a, e.z, false);
+    const float4 t1 = a.qc[e.y], t2 = a.qc[e.z];
+    quat q1 = Q(t1.x, t1.y, t1.z, t1.w), q2 = Q(t2.x, t2.y, t2.z, t2.w);
+    float R[9];
+    M3 I1, I2;
+    quat_matrix(q1, R);
+    world_inertia(R, L3v(a.iil[e.y]), I1.m);
+    quat_matrix(q2, R);
+    world_inertia(R, L3v(a.iil[e.z]), I2.m);
+    st3(q + JR_I1, I1);
+    st3(q + JR_I2, I2);
+    const v3 r1 = qrot(q1, vsub(L3v(q[JR_LA1]), L3v(a.com_local[e.y])));
+    const v3 r2 = qrot(q2, vsub(L3v(q[JR_LA2]), L3v(a.com_local[e.z])));
+    q[JR_R1] = F4v(r1);
+    q[JR_R2] = F4v(r2);
+    v3 x1 = L3v(a.xc[e.y]), x2 = L3v(a.xc[e.z]);
+    const M3 K = joint_mass_matrix(B1.im + B2.im, m3_skew(r1), I1, m3_skew(r2), I2);
+    M3 Kinv = m3_zero();
+    const float det = m3_det(K);
+    if (fabsf(det) > MACHINE_EPSILON) {
+        if (dyn) Kinv = m3_inverse(K, det);
+        const v3 err = vsub(vsub(v3add(x2, r2), x1), r1);
+        const v3 lam = m3_mulv(Kinv, vneg(err));
+        x1 = v3add(x1, lin(B1.im, B1.lf, vneg(lam)));
+        q1 = q_add_rot(q1, vcmul(B1.af, m3_mulv(I1, vcross(lam, r1))));
+        x2 = v3add(x2, lin(B2.im, B2.lf, lam));
+        q2 = q_add_rot(q2, vcmul(B2.af, m3_mulv(I2, vneg(vcross(lam, r2)))));
+    }
+    st3(q + JR_K, Kinv);
+    bool ok;
+    const M3 KR = rotation_inverse_mass(I1, I2, dyn, &ok);
+    if (ok) {
+        const v3 lam = m3_mulv(KR, vneg(rotation_error(q1, q2, q[JR_QINV])));
+        q1 = q_add_rot(q1, vcmul(B1.af, m3_mulv(I1, vneg(lam))));
+        q2 = q_add_rot(q2, vcmul(B2.af, m3_mulv(I2, lam)));
+    }
+    st3(q + JR_KR3, KR);
+    a.xc[e.y] = F4v(x1);
+    a.xc[e.z] = F4v(x2);
+    a.qc[e.y] = make_float4(q1.x, q1.y, q1.z, q1.w);
+    a.qc[e.z] = make_float4(q2.x, q2.y, q2.z, q2.w);
+}
+
+// --- slider joint (SolveSliderJointSystem.cpp) ----------------------------
+RD v3 comb(float s, v3 a, float t, v3 b) {  // a * s + b * t
+    return v3add(sv(s, a), sv(t, b));
+}
+RD v3 comb_neg(float s, v3 a, float t, v3 b) {  // -a * s - b * t
+    return vsub(sv(s, vneg(a)), sv(t, b));
+}
+// el11 .. el22 of the 2x2 translation mass matrix and its inverse (zero when
+// the determinant is tiny or no body is dynamic), :141-160 / :455-474.
+RD float4 slider_translation_inverse(float sum_im, const M3& I1, const M3& I2, v3 r1n1, v3 r1n2, v3 r2n1, v3 r2n2,
+                                     bool dyn, bool* ok) {
+    const v3 i1n1 = m3_mulv(I1, r1n1), i1n2 = m3_mulv(I1, r1n2);
+    const v3 i2n1 = m3_mulv(I2, r2n1), i2n2 = m3_mulv(I2, r2n2);
+    const float e11 = sum_im + vdot(r1n1, i1n1) + vdot(r2n1, i2n1);
+    const float e12 = vdot(r1n1, i1n2) + vdot(r2n1, i2n2);
+    const float e21 = vdot(r1n2, i1n1) + vdot(r2n2, i2n1);
+    const float e22 = sum_im + vdot(r1n2, i1n2) + vdot(r2n2, i2n2);
+    const float d = e11 * e22 - e21 * e12;
+    *ok = fabsf(d) > MACHINE_EPSILON;
+    if (*ok && dyn) {
+        const float inv = 1.0f / d;
+        return make_float4(e22 * inv, -e12 * inv, -e21 * inv, e11 * inv);
+    }
+    return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+// 1 / (im1 + im2 + (r1+u)xa . I1 (r1+u)xa + r2xa . I2 r2xa), or 0
+RD float slider_limit_inverse(float im1, float im2, const M3& I1, const M3& I2, v3 r1a, v3 r2a) {
+    float k = im1 + im2 + vdot(r1a, m3_mulv(I1, r1a)) + vdot(r2a, m3_mulv(I2, r2a));
+    return (k > 0.0f) ? 1.0f / k : 0.0f;
+}
+
+// initBeforeSolve (:49-170).  The limit's inverse mass is computed from the
+// r2 x axis row before this step's value replaces it (the reference reads
+// mR2CrossSliderAxis ahead of its update).
+RD void slider_init(const DynArgs& a, const int4 e) {
+    float4* q = a.j_rec[e.x].q;
+    const int32_t b1 = e.y, b2 = e.z;
+    const bool dyn = (e.w & 3) != 0;
+    const uint32_t flags = uint32_t(__float_as_int(q[JR_HDR].y));
+    const M3 I1 = iiw_of(a, b1), I2 = iiw_of(a, b2);
+    st3(q + JR_I1, I1);
+    st3(q + JR_I2, I2);
+    const float4 o1 = a.orientation[b1], o2 = a.orientation[b2];
+    const quat q1 = Q(o1.x, o1.y, o1.z, o1.w), q2 = Q(o2.x, o2.y, o2.z, o2.w);
+    const v3 r1 = qrot(q1, vsub(L3v(q[JR_LA1]), L3v(a.com_local[b1])));
+    const v3 r2 = qrot(q2, vsub(L3v(q[JR_LA2]), L3v(a.com_local[b2])));
+    q[JR_R1] = F4v(r1);
+    q[JR_R2] = F4v(r2);
+    const v3 ax = vnormalize(qrot(q1, L3v(q[JR_AX1])));
+    const v3 n1 = unit_orthogonal(ax);
+    const v3 n2 = vcross(ax, n1);
+    const v3 x1 = L3v(a.com_world[b1]), x2 = L3v(a.com_world[b2]);
+    const v3 u = vsub(vsub(v3add(x2, r2), x1), r1);
+    const v3 r1u = v3add(r1, u);
+    const v3 r1n1 = vcross(r1u, n1), r1n2 = vcross(r1u, n2), r1a = vcross(r1u, ax);
+    const float4 par = q[JR_PARAM];
+    const float ud = vdot(u, ax);
+    const float lerr = ud - par.y, uerr = par.z - ud;
+    float4 st = q[JR_STATE], imp = q[JR_IMP], misc = q[JR_MISC];
+    const bool oldl = st.x != 0.0f, lv = lerr <= 0.0f;
+    st.x = lv ? 1.0f : 0.0f;
+    if (!lv || lv != oldl) imp.z = 0.0f;
+    const bool oldu = st.y != 0.0f, uv = uerr <= 0.0f;
+    st.y = uv ? 1.0f : 0.0f;
+    if (!uv || uv != oldu) imp.w = 0.0f;
+    const float im1 = a.mass[b1].y, im2 = a.mass[b2].y;
+    if ((flags & JF_LIMIT) && (lv || uv)) misc.x = slider_limit_inverse(im1, im2, I1, I2, r1a, L3v(q[JR_R2A]));
+    const v3 r2n1 = vcross(r2, n1), r2n2 = vcross(r2, n2), r2a = vcross(r2, ax);
+    bool ok;
+    q[JR_KROT] = slider_translation_inverse(im1 + im2, I1, I2, r1n1, r1n2, r2n1, r2n2, dyn, &ok);
+    st3(q + JR_KR3, rotation_inverse_mass(I1, I2, dyn, &ok));
+    if (flags & JF_MOTOR) {
+        const float s = im1 + im2;
+        misc.y = (s > 0.0f) ? 1.0f / s : 0.0f;
+    }
+    q[JR_A1] = F4v(ax);
+    q[JR_N1] = F4v(n1);
+    q[JR_N2] = F4v(n2);
+    q[JR_R1N1] = F4v(r1n1);
+    q[JR_R1N2] = F4v(r1n2);
+    q[JR_R1A] = F4v(r1a);
+    q[JR_R2N1] = F4v(r2n1);
+    q[JR_R2N2] = F4v(r2n2);
+    q[JR_R2A] = F4v(r2a);
+    q[JR_STATE] = st;
+    q[JR_IMP] = imp;
+    q[JR_MISC] = misc;
+}
+
+// warmstart (:173-248)
+RD void slider_warm(const DynArgs& a, const int4 e) {
+    float4* q = a.j_rec[e.x].q;
+    const JBody B1 = jbody(a, e.y, false), B2 = jbody(a, e.z, false);
+    v3 v1 = L3v(a.cv[e.y]), w1 = L3v(a.cw[e.y]), v2 = L3v(a.cv[e.z]), w2 = L3v(a.cw[e.z]);
+    const M3 I1 = ld3(q + JR_I1), I2 = ld3(q + JR_I2);
+    const v3 ax = L3v(q[JR_A1]), n1 = L3v(q[JR_N1]), n2 = L3v(q[JR_N2]);
+    const float4 imp = q[JR_IMP];
+    const v3 ir = L3v(q[JR_IMP2]);
+    const float il = imp.w - imp.z;
+    const v3 lim = sv(il, ax);
+    const v3 mot = sv(q[JR_STATE].z, ax);
+    v3 lin1 = comb_neg(imp.x, n1, imp.y, n2);
+    v3 ang1 = comb_neg(imp.x, L3v(q[JR_R1N1]), imp.y, L3v(q[JR_R1N2]));
+    ang1 = v3add(ang1, vneg(ir));
+    lin1 = v3add(lin1, lim);
+    ang1 = v3add(ang1, sv(il, L3v(q[JR_R1A])));
+    lin1 = v3add(lin1, mot);
+    v1 = v3add(v1, lin(B1.im, B1.lf, lin1));
+    w1 = v3add(w1, vcmul(B1.af, m3_mulv(I1, ang1)));
+    v3 lin2 = comb(imp.x, n1, imp.y, n2);
+    v3 ang2 = comb(imp.x, L3v(q[JR_R2N1]), imp.y, L3v(q[JR_R2N2]));
+    ang2 = v3add(ang2, ir);
+    lin2 = v3add(lin2, vneg(lim));
+    ang2 = v3add(ang2, sv(-il, L3v(q[JR_R2A])));
+    lin2 = v3add(lin2, vneg(mot));
+    v2 = v3add(v2, lin(B2.im, B2.lf, lin2));
+    w2 = v3add(w2, vcmul(B2.af, m3_mulv(I2, ang2)));
+    a.cv[e.y] = F4v(v1); a.cw[e.y] = F4v(w1);
+    a.cv[e.z] = F4v(v2); a.cw[e.z] = F4v(w2);
+}
+
+// solveVelocityConstraint (:251-415)
+RD void slider_solve(const DynArgs& a, const int4 e) {
+    float4* q = a.j_rec[e.x].q;
+    const uint32_t flags = uint32_t(__float_as_int(q[JR_HDR].y));
+    const JBody B1 = jbody(a, e.y, false), B2 = jbody(a, e.z, false);
+    v3 v1 = L3v(a.cv[e.y]), w1 = L3v(a.cw[e.y]), v2 = L3v(a.cv[e.z]), w2 = L3v(a.cw[e.z]);
+    const M3 I1 = ld3(q + JR_I1), I2 = ld3(q + JR_I2);
+    const v3 ax = L3v(q[JR_A1]), n1 = L3v(q[JR_N1]), n2 = L3v(q[JR_N2]);
+    const v3 r2n1 = L3v(q[JR_R2N1]), r2n2 = L3v(q[JR_R2N2]), r2a = L3v(q[JR_R2A]);
+    const v3 r1n1 = L3v(q[JR_R1N1]), r1n2 = L3v(q[JR_R1N2]), r1a = L3v(q[JR_R1A]);
+    float4 imp = q[JR_IMP], st = q[JR_STATE];
+    const float4 misc = q[JR_MISC];
+    if (flags & JF_LIMIT) {
+        if (st.x != 0.0f) {
+            const float Jv = vdot(ax, v2) + vdot(r2a, w2) - vdot(ax, v1) - vdot(r1a, w1);
+            float dl = misc.x * (-Jv - 0.0f);
+            const float lt = imp.z;
+            imp.z = smax(imp.z + dl, 0.0f);
+            dl = imp.z - lt;
+            v1 = v3add(v1, lin(B1.im, B1.lf, sv(-dl, ax)));
+            w1 = v3add(w1, vcmul(B1.af, m3_mulv(I1, sv(-dl, r1a))));
+            v2 = v3add(v2, lin(B2.im, B2.lf, sv(dl, ax)));
+            w2 = v3add(w2, vcmul(B2.af, m3_mulv(I2, sv(dl, r2a))));
+        }
+        if (st.y != 0.0f) {
+            const float Jv = vdot(ax, v1) + vdot(r1a, w1) - vdot(ax, v2) - vdot(r2a, w2);
+            float dl = misc.x * (-Jv - 0.0f);
+            const float lt = imp.w;
+            imp.w = smax(imp.w + dl, 0.0f);
+            dl = imp.w - lt;
+            v1 = v3add(v1, lin(B1.im, B1.lf, sv(dl, ax)));
+            w1 = v3add(w1, vcmul(B1.af, m3_mulv(I1, sv(dl, r1a))));
+            v2 = v3add(v2, lin(B2.im, B2.lf, sv(-dl, ax)));
+            w2 = v3add(w2, vcmul(B2.af, m3_mulv(I2, sv(-dl, r2a))));
+        }
+    }
+    if (flags & JF_MOTOR) {
+        const float Jv = vdot(ax, v1) - vdot(ax, v2);
+        const float maxi = q[JR_PARAM2].x * a.dt;
+        float dl = misc.y * (-Jv - q[JR_PARAM].w);
+        const float lt = st.z;
+        st.z = sclamp(st.z + dl, -maxi, maxi);
+        dl = st.z - lt;
+        v1 = v3add(v1, lin(B1.im, B1.lf, sv(dl, ax)));
+        v2 = v3add(v2, lin(B2.im, B2.lf, sv(-dl, ax)));
+    }
+    // rotation: Jv = w2 - w1
+    const v3 dr = m3_mulv(ld3(q + JR_KR3), vsub(vneg(vsub(w2, w1)), V(0.0f, 0.0f, 0.0f)));
+    q[JR_IMP2] = F4v(v3add(L3v(q[JR_IMP2]), dr));
+    w1 = v3add(w1, vcmul(B1.af, m3_mulv(I1, vneg(dr))));
+    w2 = v3add(w2, vcmul(B2.af, m3_mulv(I2, dr)));
+    // translation along n1, n2
+    const float el1 = -vdot(n1, v1) - vdot(w1, r1n1) + vdot(n1, v2) + vdot(w2, r2n1);
+    const float el2 = -vdot(n2, v1) - vdot(w1, r1n2) + vdot(n2, v2) + vdot(w2, r2n2);
+    const float4 kt = q[JR_KROT];
+    const float rx = -el1 - 0.0f, ry = -el2 - 0.0f;
+    const float dx = kt.x * rx + kt.y * ry, dy = kt.z * rx + kt.w * ry;
+    imp.x = imp.x + dx;
+    imp.y = imp.y + dy;
+    const v3 lin1 = comb_neg(dx, n1, dy, n2);
+    v1 = v3add(v1, lin(B1.im, B1.lf, lin1));
+    w1 = v3add(w1, vcmul(B1.af, m3_mulv(I1, comb_neg(dx, r1n1, dy, r1n2))));
+    v2 = v3add(v2, lin(B2.im, B2.lf, vneg(lin1)));
+    w2 = v3add(w2, vcmul(B2.af, m3_mulv(I2, comb(dx, r2n1, dy, r2n2))));
+    q[JR_IMP] = imp;
+    q[JR_STATE] = st;
+    a.cv[e.y] = F4v(v1); a.cw[e.y] = F4v(w1);
+    a.cv[e.z] = F4v(v2); a.cw[e.z] = F4v(w2);
+}
+
+// solvePositionConstraint, NON_LINEAR_GAUSS_SEIDEL (:418-596).  The
+// translation error is the one measured before the limit corrections.
+RD void slider_position(const DynArgs& a, const int4 e) {
+    float4* q = a.j_rec[e.x].q;
+    const uint32_t flags = uint32_t(__float_as_int(q[JR_HDR].y));
+    const bool dyn = (e.w & 3) != 0;
+    const JBody B1 = jbody(a, e.y, false), B2 = jbody(a, e.z, false);
+    const float4 t1 = a.qc[e.y], t2 = a.qc[e.z];
+    quat q1 = Q(t1.x, t1.y, t1.z, t1.w), q2 = Q(t2.x, t2.y, t2.z, t2.w);
+    float R[9];
+    M3 I1, I2;
+    quat_matrix(q1, R);
+    world_inertia(R, L3v(a.iil[e.y]), I1.m);
+    quat_matrix(q2, R);
+    world_inertia(R, L3v(a.iil[e.z]), I2.m);
+    st3(q + JR_I1, I1);
+    st3(q + JR_I2, I2);
+    const v3 r1 = qrot(q1, vsub(L3v(q[JR_LA1]), L3v(a.com_local[e.y])));
+    const v3 r2 = qrot(q2, vsub(L3v(q[JR_LA2]), L3v(a.com_local[e.z])));
+    q[JR_R1] = F4v(r1);
+    q[JR_R2] = F4v(r2);
+    v3 x1 = L3v(a.xc[e.y]), x2 = L3v(a.xc[e.z]);
+    const v3 u = vsub(vsub(v3add(x2, r2), x1), r1);
+    const v3 ax = vnormalize(qrot(q1, L3v(q[JR_AX1])));
+    const v3 n1 = unit_orthogonal(ax);
+    const v3 n2 = vcross(ax, n1);
+    const float4 par = q[JR_PARAM];
+    const float ud = vdot(u, ax);
+    float4 st = q[JR_STATE], misc = q[JR_MISC];
+    st.x = (ud - par.y <= 0.0f) ? 1.0f : 0.0f;
+    st.y = (par.z - ud <= 0.0f) ? 1.0f : 0.0f;
+    const v3 r2n1 = vcross(r2, n1), r2n2 = vcross(r2, n2), r2a = vcross(r2, ax);
+    const v3 r1u = v3add(r1, u);
+    const v3 r1n1 = vcross(r1u, n1), r1n2 = vcross(r1u, n2), r1a = vcross(r1u, ax);
+    if (flags & JF_LIMIT) {
+        if (st.x != 0.0f || st.y != 0.0f) misc.x = slider_limit_inverse(B1.im, B2.im, I1, I2, r1a, r2a);
+        if (st.x != 0.0f) {
+            const v3 uu = vsub(vsub(v3add(x2, r2), x1), r1);
+            const float lam = misc.x * (-(vdot(uu, ax) - par.y));
+            x1 = v3add(x1, lin(B1.im, B1.lf, sv(-lam, ax)));
+            q1 = q_add_rot(q1, vcmul(B1.af, m3_mulv(I1, sv(-lam, r1a))));
+            x2 = v3add(x2, lin(B2.im, B2.lf, sv(lam, ax)));
+            q2 = q_add_rot(q2, vcmul(B2.af, m3_mulv(I2, sv(lam, r2a))));
+        }
+        if (st.y != 0.0f) {
+            const v3 uu = vsub(vsub(v3add(x2, r2), x1), r1);
+            const float lam = misc.x * (-(par.z - vdot(uu, ax)));
+            x1 = v3add(x1, lin(B1.im, B1.lf, sv(lam, ax)));
+            q1 = q_add_rot(q1, vcmul(B1.af, m3_mulv(I1, sv(lam, r1a))));
+            x2 = v3add(x2, lin(B2.im, B2.lf, sv(-lam, ax)));
+            q2 = q_add_rot(q2, vcmul(B2.af, m3_mulv(I2, sv(-lam, r2a))));
+        }
+    }
+    bool ok;
+    const M3 KR = rotation_inverse_mass(I1, I2, dyn, &ok);
+    if (ok) {
+        const v3 lam = m3_mulv(KR, vneg(rotation_error(q1, q2, q[JR_QINV])));
+        q1 = q_add_rot(q1, vcmul(B1.af, m3_mulv(I1, vneg(lam))));
+        q2 = q_add_rot(q2, vcmul(B2.af, m3_mulv(I2, lam)));
+    }
+    st3(q + JR_KR3, KR);
+    const float4 kt = slider_translation_inverse(B1.im + B2.im, I1, I2, r1n1, r1n2, r2n1, r2n2, dyn, &ok);
+    if (ok) {
+        const float ex = -vdot(u, n1), ey = -vdot(u, n2);
+        const float lx = kt.x * ex + kt.y * ey, ly = kt.z * ex + kt.w * ey;
+        x1 = v3add(x1, lin(B1.im, B1.lf, comb_neg(lx, n1, ly, n2)));
+        q1 = q_add_rot(q1, vcmul(B1.af, m3_mulv(I1, comb_neg(lx, r1n1, ly, r1n2))));
+        x2 = v3add(x2, lin(B2.im, B2.lf, comb(lx, n1, ly, n2)));
+        q2 = q_add_rot(q2, vcmul(B2.af, m3_mulv(I2, comb(lx, r2n1, ly, r2n2))));
+    }
+    q[JR_KROT] = kt;
+    q[JR_A1] = F4v(ax);
+    q[JR_N1] = F4v(n1);
+    q[JR_N2] = F4v(n2);
+    q[JR_R1N1] = F4v(r1n1);
+    q[JR_R1N2] = F4v(r1n2);
+    q[JR_R1A] = F4v(r1a);
+    q[JR_R2N1] = F4v(r2n1);
+    q[JR_R2N2] = F4v(r2n2);
+    q[JR_R2A] = F4v(r2a);
+    q[JR_STATE] = st;
+    q[JR_MISC] = misc;
+    a.xc[e.y] = F4v(x1);
+    a.xc[e.z] = F4v(x2);
+    a.qc[e.y] = make_float4(q1.x, q1.y, q1.z, q1.w);
+    a.qc[e.z] = make_float4(q2.x, q2.y, q2.z, q2.w);
+}
+
 // initBeforeSolve of one joint (BallAndSocket :49-136, Hinge :48-214).
 RD void joint_init(const DynArgs& a, const int4 e) {
     JointRec* R = a.j_rec + e.x;
     float4* q = R->q;
+    const uint32_t jt = uint32_t(__float_as_int(q[JR_HDR].x));
+    if (jt == JT_FIXED) return fixed_init(a, e);
+    if (jt == JT_SLIDER) return slider_init(a, e);
     const int32_t b1 = e.y, b2 = e.z;
     const bool dyn1 = (e.w & 1) != 0, dyn2 = (e.w & 2) != 0;
     const uint32_t type = uint32_t(__float_as_int(q[JR_HDR].x));
@@ -262,6 +679,8 @@ RD void joint_init(const DynArgs& a, const int4 e) {
 RD void joint_warm(const DynArgs& a, const int4 e) {
     float4* q = a.j_rec[e.x].q;
     const uint32_t type = uint32_t(__float_as_int(q[JR_HDR].x));
+    if (type == JT_FIXED) return fixed_warm(a, e);
+    if (type == JT_SLIDER) return slider_warm(a, e);
     const JBody B1 = jbody(a, e.y, false), B2 = jbody(a, e.z, false);
     v3 v1 = L3v(a.cv[e.y]), w1 = L3v(a.cw[e.y]), v2 = L3v(a.cv[e.z]), w2 = L3v(a.cw[e.z]);
     const M3 I1 = ld3(q + JR_I1), I2 = ld3(q + JR_I2);
@@ -308,6 +727,8 @@ RD void joint_warm(const DynArgs& a, const int4 e) {
 RD void joint_solve(const DynArgs& a, const int4 e) {
     float4* q = a.j_rec[e.x].q;
     const uint32_t type = uint32_t(__float_as_int(q[JR_HDR].x));
+    if (type == JT_FIXED) return fixed_solve(a, e);
+    if (type == JT_SLIDER) return slider_solve(a, e);
     const uint32_t flags = uint32_t(__float_as_int(q[JR_HDR].y));
     const JBody B1 = jbody(a, e.y, false), B2 = jbody(a, e.z, false);
     v3 v1 = L3v(a.cv[e.y]), w1 = L3v(a.cw[e.y]), v2 = L3v(a.cv[e.z]), w2 = L3v(a.cw[e.z]);
@@ -405,6 +826,8 @@ RD void joint_solve(const DynArgs& a, const int4 e) {
 RD void joint_position(const DynArgs& a, const int4 e) {
     float4* q = a.j_rec[e.x].q;
     const uint32_t type = uint32_t(__float_as_int(q[JR_HDR].x));
+    if (type == JT_FIXED) return fixed_position(a, e);
+    if (type == JT_SLIDER) return slider_position(a, e);
     const uint32_t flags = uint32_t(__float_as_int(q[JR_HDR].y));
     const bool dyn1 = (e.w & 1) != 0, dyn2 = (e.w & 2) != 0;
     const JBody B1 = jbody(a, e.y, dyn1), B2 = jbody(a, e.z, dyn2);

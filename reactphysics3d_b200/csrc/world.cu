@@ -424,6 +424,7 @@ struct JointH {
     int type = 0;
     int b1 = -1, b2 = -1;
     bool in_island = false;
+    float motor_speed = 0.0f;  // hinge / slider (the record's copy is on the device)
 };
 struct ColliderH {
     int body = -1;
@@ -616,7 +617,7 @@ struct WorldH {
     // joints: JointComponents and the per-type components (order), the pairs
     // of bodies that must not collide, the first record of this world
     std::vector<JointH> joints;
-    rp3dg::order::Comps jcomp, bscomp, hcomp;
+    rp3dg::order::Comps jcomp, bscomp, fcomp, hcomp, scomp;  // JointComponents, then one per joint type
     std::set<std::pair<int, int>> nocollide;
     uint32_t jbase = 0;
     struct Pose { float p[3], q[4]; };
@@ -642,6 +643,17 @@ struct WorldH {
     std::vector<int> slept;                    // bodies put to sleep by this step
     rp3dg_world_stats stats{};
 };
+
+// The per-type joint components (BallAndSocketJointComponents, ...,
+// SliderJointComponents) of a joint type.
+rp3dg::order::Comps& joint_type_comps(WorldH& w, int type) {
+    switch (type) {
+        case RP3DG_JOINT_BALL_AND_SOCKET: return w.bscomp;
+        case RP3DG_JOINT_FIXED: return w.fcomp;
+        case RP3DG_JOINT_HINGE: return w.hcomp;
+        default: return w.scomp;
+    }
+}
 
 }  // namespace
 
@@ -1283,17 +1295,18 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
             const bool dis = !w.bcomp.enabled(J.b1) && !w.bcomp.enabled(J.b2);
             if (w.jcomp.enabled(j) == !dis) continue;
             w.jcomp.set_disabled(j, dis);
-            (J.type == RP3DG_JOINT_BALL_AND_SOCKET ? w.bscomp : w.hcomp).set_disabled(j, dis);
+            joint_type_comps(w, J.type).set_disabled(j, dis);
         }
     }
-    // the enabled joints island by island: ball-and-socket then hinge, each in
-    // component order (the order the constraint solver visits them)
+    // the enabled joints island by island: ball-and-socket, fixed, hinge then
+    // slider, each in component order (the order the constraint solver visits
+    // them, ConstraintSolverSystem.cpp:60-113)
     w.jlist.clear();
     w.isl_jstart.assign(w.islands.size(), 0);
     w.isl_jcount.assign(w.islands.size(), 0);
     if (!w.joints.empty()) {
         std::vector<std::vector<int>> per(w.islands.size());
-        for (rp3dg::order::Comps* cmp : {&w.bscomp, &w.hcomp})
+        for (rp3dg::order::Comps* cmp : {&w.bscomp, &w.fcomp, &w.hcomp, &w.scomp})
             for (uint32_t s = 0; s < cmp->n_enabled; s++) {
                 const int j = cmp->at[s];
                 const JointH& J = w.joints[size_t(j)];
@@ -2607,7 +2620,8 @@ int add_joints(Group* g, uint32_t world, const rp3dg_joint_desc* jd, uint32_t n)
             if (!g->worlds[k].joints.empty()) return wfail(g, RP3DG_EINVAL, "add the joints of the worlds in order");
     for (uint32_t i = 0; i < n; i++) {
         const rp3dg_joint_desc& d = jd[i];
-        if (d.type != RP3DG_JOINT_BALL_AND_SOCKET && d.type != RP3DG_JOINT_HINGE)
+        if (d.type != RP3DG_JOINT_BALL_AND_SOCKET && d.type != RP3DG_JOINT_HINGE && d.type != RP3DG_JOINT_FIXED &&
+            d.type != RP3DG_JOINT_SLIDER)
             return wfail(g, RP3DG_EINVAL, "bad joint type");
         if (d.body1 < 0 || d.body2 < 0 || uint32_t(d.body1) >= w.nb || uint32_t(d.body2) >= w.nb || d.body1 == d.body2)
             return wfail(g, RP3DG_EINVAL, "bad joint bodies");
@@ -2617,15 +2631,18 @@ int add_joints(Group* g, uint32_t world, const rp3dg_joint_desc* jd, uint32_t n)
     w.joints.resize(n);
     w.jcomp.reserve_ids(n);
     w.bscomp.reserve_ids(n);
+    w.fcomp.reserve_ids(n);
     w.hcomp.reserve_ids(n);
+    w.scomp.reserve_ids(n);
     for (uint32_t j = 0; j < n; j++) {
         const rp3dg_joint_desc& d = jd[j];
         JointH& J = w.joints[j];
         J.type = d.type;
         J.b1 = d.body1;
         J.b2 = d.body2;
+        J.motor_speed = d.motor_speed;
         const bool dis = !w.bcomp.enabled(J.b1) && !w.bcomp.enabled(J.b2);
-        (d.type == RP3DG_JOINT_BALL_AND_SOCKET ? w.bscomp : w.hcomp).add(int(j), dis);
+        joint_type_comps(w, d.type).add(int(j), dis);
         w.jcomp.add(int(j), dis);
         if (!d.collision_enabled) w.nocollide.insert(std::make_pair(std::min(J.b1, J.b2), std::max(J.b1, J.b2)));
         w.bodies[size_t(J.b1)].joints.push_back(int(j));
@@ -2640,8 +2657,9 @@ int add_joints(Group* g, uint32_t world, const rp3dg_joint_desc* jd, uint32_t n)
         for (int r = 0; r < rp3dg::JR_ROWS; r++) q[r] = make_float4(0.f, 0.f, 0.f, 0.f);
         int flags = 0;
         if (d.type == RP3DG_JOINT_BALL_AND_SOCKET && d.cone_limit_enabled) flags |= rp3dg::JF_CONE;
-        if (d.type == RP3DG_JOINT_HINGE && d.limit_enabled) flags |= rp3dg::JF_LIMIT;
-        if (d.type == RP3DG_JOINT_HINGE && d.motor_enabled) flags |= rp3dg::JF_MOTOR;
+        const bool limited = d.type == RP3DG_JOINT_HINGE || d.type == RP3DG_JOINT_SLIDER;
+        if (limited && d.limit_enabled) flags |= rp3dg::JF_LIMIT;
+        if (limited && d.motor_enabled) flags |= rp3dg::JF_MOTOR;
         q[rp3dg::JR_HDR] = make_float4(__int_as_float_host(d.type), __int_as_float_host(flags), 0.f, 0.f);
         q[rp3dg::JR_LA1] = make_float4(la1[0], la1[1], la1[2], 0.f);
         q[rp3dg::JR_LA2] = make_float4(la2[0], la2[1], la2[2], 0.f);
@@ -2659,8 +2677,22 @@ int add_joints(Group* g, uint32_t world, const rp3dg_joint_desc* jd, uint32_t n)
             q[rp3dg::JR_QINV] = make_float4(-qd.x, -qd.y, -qd.z, qd.w);
             q[rp3dg::JR_PARAM] = make_float4(0.f, d.min_angle, d.max_angle, d.motor_speed);
             q[rp3dg::JR_PARAM2] = make_float4(d.max_motor_torque, 0.f, 0.f, 0.f);
-        } else {
+        } else if (d.type == RP3DG_JOINT_BALL_AND_SOCKET) {
             q[rp3dg::JR_PARAM] = make_float4(d.cone_limit_enabled ? d.cone_half_angle : float(3.141592653589), 0.f, 0.f, 0.f);
+        } else {
+            // FixedJoint / SliderJoint constructors (FixedJoint.cpp:35-58,
+            // SliderJoint.cpp:37-72): inverse initial orientation difference
+            // q2^-1 * q1, and the slider axis in body 1's frame, normalised
+            const HQ qd = hq_mul(HQ{-q2.x, -q2.y, -q2.z, q2.w}, q1);
+            q[rp3dg::JR_QINV] = make_float4(qd.x, qd.y, qd.z, qd.w);
+            if (d.type == RP3DG_JOINT_SLIDER) {
+                float ax1[3];
+                hq_rot(HQ{-q1.x, -q1.y, -q1.z, q1.w}, d.axis, ax1);
+                hv_normalize(ax1);
+                q[rp3dg::JR_AX1] = make_float4(ax1[0], ax1[1], ax1[2], 0.f);
+                q[rp3dg::JR_PARAM] = make_float4(0.f, d.min_angle, d.max_angle, d.motor_speed);
+                q[rp3dg::JR_PARAM2] = make_float4(d.max_motor_torque, 0.f, 0.f, 0.f);
+            }
         }
     }
     // records: the group's array grows (existing records copied)
@@ -2751,6 +2783,28 @@ int rp3dg_world_add_joints(rp3dg_world* w, const rp3dg_joint_desc* joints, uint3
 int rp3dg_world_group_add_joints(rp3dg_world* w, uint32_t world, const rp3dg_joint_desc* joints, uint32_t n) {
     if (!w) return RP3DG_EINVAL;
     return add_joints(w, world, joints, n);
+}
+
+// HingeJoint::setMotorSpeed / SliderJoint::setMotorSpeed (HingeJoint.cpp:168-177,
+// SliderJoint.cpp:210-219): a new speed is stored and wakes the joint's two
+// bodies (Joint::awakeBodies, Joint.cpp:74-86).
+int rp3dg_world_set_motor_speed(rp3dg_world* g, uint32_t world, uint32_t joint, float speed) {
+    if (!g) return RP3DG_EINVAL;
+    if (world >= g->worlds.size() || joint >= g->worlds[world].joints.size())
+        return wfail(g, RP3DG_EINVAL, "bad world or joint index");
+    WorldH& w = g->worlds[world];
+    JointH& J = w.joints[joint];
+    if (J.type != RP3DG_JOINT_HINGE && J.type != RP3DG_JOINT_SLIDER)
+        return wfail(g, RP3DG_EINVAL, "only hinge and slider joints have a motor");
+    if (speed == J.motor_speed) return 0;
+    J.motor_speed = speed;
+    float4* row = g->j_rec[w.jbase + joint].q + rp3dg::JR_PARAM;
+    cudaError_t e = cudaMemcpyAsync(reinterpret_cast<char*>(row) + 3 * sizeof(float), &J.motor_speed, sizeof(float),
+                                    cudaMemcpyHostToDevice, g->stream);
+    if (e != cudaSuccess) return wcuda(g, e, "motor speed");
+    set_sleeping(g, w, J.b1, false);
+    set_sleeping(g, w, J.b2, false);
+    return sync_rows(g);
 }
 
 int rp3dg_world_update(rp3dg_world* w, float dt) { return update_group(w, dt); }

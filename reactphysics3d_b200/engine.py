@@ -100,6 +100,7 @@ def load_library(path=LIB_PATH):
     L.rp3dg_world_get_tuning.argtypes = [P, P]
     L.rp3dg_world_add_joints.argtypes = [P, P, C.c_uint32]
     L.rp3dg_world_group_add_joints.argtypes = [P, C.c_uint32, P, C.c_uint32]
+    L.rp3dg_world_set_motor_speed.argtypes = [P, C.c_uint32, C.c_uint32, C.c_float]
     L.rp3dg_world_group_create.argtypes = [P, P, C.c_uint32, P, P, P, P, C.c_int, C.POINTER(P)]
     L.rp3dg_world_group_get_bodies.argtypes = [P, C.c_uint32, P, P, P, P, P]
     L.rp3dg_world_group_get_pairs.argtypes = [P, C.c_uint32, P, C.c_uint32, C.POINTER(C.c_uint32)]
@@ -497,6 +498,13 @@ class World:
             rc = self.lib.rp3dg_world_add_joints(self.h, j.ctypes.data, len(j))
         else:
             rc = self.lib.rp3dg_world_group_add_joints(self.h, int(world), j.ctypes.data, len(j))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+
+    def set_motor_speed(self, joint, speed, world=0):
+        """HingeJoint / SliderJoint::setMotorSpeed on joint `joint` (creation
+        order) of world `world`; a changed speed wakes the joint's bodies."""
+        rc = self.lib.rp3dg_world_set_motor_speed(self.h, int(world), int(joint), float(speed))
         if rc != 0:
             raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
 

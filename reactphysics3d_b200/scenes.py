@@ -473,6 +473,101 @@ def ragdoll_world(n_ragdolls=2, seed=21, limits=True, boxes=0):
                       f"ragdolls {n_ragdolls}", np.array(joints, dtype=A.JOINT_DESC_DTYPE))
 
 
+def _yaw_quaternion(angle):
+    return np.array([0.0, np.sin(0.5 * angle), 0.0, np.cos(0.5 * angle)])
+
+
+def mechanism_world(n_mechanisms=1, seed=31, spacing=20.0, speeds=(-2.0, 2.0)):
+    """Copies of the reference testbed's joints scene (testbed/scenes/joints/
+    JointsScene.cpp) on one static floor, each turned by a random yaw about
+    its centre: a chain of 7 unit boxes hanging from a static box by 6
+    ball-and-socket joints; a dynamic box (1.5 x 4 x 1.5) on a slider joint
+    over a static box (2 x 4 x 2), translation limits +-1.7 and a motor
+    (random speed in `speeds`, max force 10000); a propeller box (10 x 1 x 1)
+    on a motorised hinge (-PI / 2 rad/s, max torque 60) above the sliding box;
+    and two boxes (1.5 cubed) welded to the propeller's ends by fixed joints.
+    The bodies a joint connects do not collide; boxes have bounciness 0.4,
+    chain boxes angular damping 0.2.  The mechanisms sit on a square grid
+    `spacing` metres apart on a floor 0.5 m thick."""
+    rng = np.random.default_rng(seed)
+    side = int(np.ceil(np.sqrt(n_mechanisms)))
+    half_floor = 0.5 * side * spacing + 5.0
+    # (half extents, centre, static) of one mechanism's bodies, in its frame
+    parts = [((0.5, 0.5, 0.5), (0.0, 15.0 - 1.5 * i, 5.0), i == 0) for i in range(7)]
+    parts += [((1.0, 2.0, 1.0), (0.0, 2.1, 0.0), True), ((0.75, 2.0, 0.75), (0.0, 4.2, 0.0), False),
+              ((5.0, 0.5, 0.5), (0.0, 7.0, 0.0), False),
+              ((0.75, 0.75, 0.75), (5.0, 7.0, 0.0), False), ((0.75, 0.75, 0.75), (-5.0, 7.0, 0.0), False)]
+    per = len(parts)
+    n = 1 + n_mechanisms * per
+    shapes = np.zeros(n, A.SHAPE_DTYPE)
+    shapes["mesh"] = -1
+    shapes["kind"] = A.SHAPE_BOX
+    shapes["params"][0, :3] = (half_floor, 0.25, half_floor)
+    bodies = A.body_descs(n)
+    bodies[0]["type"] = A.BODY_STATIC
+    colliders = A.collider_descs(n)
+    colliders["body"] = np.arange(n)
+    colliders["shape"] = np.arange(n)
+    colliders["bounciness"] = np.float32(0.4)
+    colliders[0]["bounciness"] = np.float32(0.3)
+    joints = []
+    for m in range(n_mechanisms):
+        b = 1 + m * per
+        origin = np.array([(m % side - 0.5 * (side - 1)) * spacing, 0.0, (m // side - 0.5 * (side - 1)) * spacing])
+        q = _yaw_quaternion(rng.uniform(0.0, 2.0 * np.pi))
+        centres = _rotate(q, np.array([c for _, c, _ in parts])) + origin
+        c32 = centres.astype(np.float32)
+        for k, (he, _, static) in enumerate(parts):
+            shapes["params"][b + k, :3] = he
+            bodies[b + k]["position"] = c32[k]
+            bodies[b + k]["orientation"] = q.astype(np.float32)
+            if static:
+                bodies[b + k]["type"] = A.BODY_STATIC
+            if k < 7:
+                bodies[b + k]["angular_damping"] = np.float32(0.2)
+
+        def joint(kind, i1, i2, anchor, axis=None):
+            j = A.joint_descs(1)[0]
+            j["type"] = kind
+            j["body1"], j["body2"] = b + i1, b + i2
+            j["anchor"] = np.asarray(anchor, dtype=np.float32)
+            if axis is not None:
+                j["axis"] = np.asarray(axis, dtype=np.float32)
+            return j
+        for i in range(6):
+            j = joint(A.JOINT_BALL_AND_SOCKET, i, i + 1, 0.5 * (c32[i].astype(np.float64) + c32[i + 1]))
+            joints.append(j)
+        j = joint(A.JOINT_SLIDER, 7, 8, np.float32(0.5) * (c32[8] + c32[7]), c32[8] - c32[7])
+        j["collision_enabled"] = 0
+        j["limit_enabled"] = 1
+        j["min_angle"], j["max_angle"] = np.float32(-1.7), np.float32(1.7)
+        j["motor_enabled"] = 1
+        j["motor_speed"] = np.float32(rng.uniform(*speeds))
+        j["max_motor_torque"] = np.float32(10000.0)
+        joints.append(j)
+        j = joint(A.JOINT_HINGE, 9, 8, 0.5 * (c32[8].astype(np.float64) + c32[9]), _rotate(q, [[0.0, 1.0, 0.0]])[0])
+        j["collision_enabled"] = 0
+        j["motor_enabled"] = 1
+        j["motor_speed"] = -np.float32(0.5) * np.float32(3.141592653589)
+        j["max_motor_torque"] = np.float32(60.0)
+        joints.append(j)
+        for k in (10, 11):
+            j = joint(A.JOINT_FIXED, k, 9, c32[k])
+            j["collision_enabled"] = 0
+            joints.append(j)
+    return WorldScene(A.default_world_settings(), shapes, bodies, colliders, f"mechanisms {n_mechanisms}",
+                      np.array(joints, dtype=A.JOINT_DESC_DTYPE))
+
+
+def mechanism_motor_speeds(n_mechanisms, step, dt=1.0 / 60.0):
+    """The slider motor speeds before update `step` (0-based) of
+    mechanism_world: (joint index, speed) pairs, speed 2 cos(1.5 t + m) m/s at
+    elapsed time t = step * dt for mechanism m, as the testbed's joints scene
+    drives its slider (JointsScene::updatePhysics)."""
+    t = step * float(dt)
+    return [(10 * m + 6, np.float32(2.0 * np.cos(1.5 * t + m))) for m in range(n_mechanisms)]
+
+
 def sine_heights(cols, rows, seed=3, n_waves=8, amplitude=2.0, k_range=(0.05, 0.5), cell=1.0):
     """A height grid (rows, cols) of `n_waves` sines with random directions,
     wave numbers |k| in k_range (rad per metre) and phases, whose amplitudes

@@ -196,7 +196,7 @@ def world_fixture():
     d = {}
     for name in worldio.WORLD_CASES:
         sc, steps, every = worldio.make_scene(name)
-        t = worldio.trajectory(reflib.RefScene(sc), steps, every)
+        t = worldio.trajectory(reflib.RefScene(sc), steps, every, worldio.DRIVERS.get(name))
         for k, v in t.items():
             d[f"{name}/{k}"] = v
     np.savez_compressed(os.path.join(HERE, "world.npz"), **d)

@@ -280,6 +280,7 @@ class RefScene:
         L.ref_scene_contacts.restype = C.c_long
         L.ref_world_step.argtypes = [C.c_int, C.c_float, C.c_int]
         L.ref_scene_add_joints.argtypes = [C.c_int, P, C.c_uint32]
+        L.ref_scene_set_motor_speed.argtypes = [C.c_int, C.c_uint32, C.c_float]
         L.ref_heightfield_register.argtypes = [C.c_uint32, C.c_uint32, P, C.c_float, C.c_float, C.c_float]
         # height fields of the scene registered with the harness; the shape
         # table's mesh field then names the harness's ids
@@ -304,6 +305,9 @@ class RefScene:
 
     def update(self, dt=1.0 / 60.0, n=1):
         self.lib.ref_world_step(self.id, dt, n)
+
+    def set_motor_speed(self, joint, speed):
+        assert self.lib.ref_scene_set_motor_speed(self.id, int(joint), float(speed)) == 0
 
     def bodies(self):
         n = self.nb

@@ -23,7 +23,7 @@ def fixture(name):
 @pytest.mark.parametrize("name", list(worldio.WORLD_CASES))
 def test_reference_reproduces_world_fixture(name):
     sc, steps, every = worldio.make_scene(name)
-    got = worldio.trajectory(reflib.RefScene(sc), steps, every)
+    got = worldio.trajectory(reflib.RefScene(sc), steps, every, worldio.DRIVERS.get(name))
     exp = fixture(name)
     assert worldio.first_mismatch(got, exp) is None
     for k in ("ckpt_pos", "ckpt_ori", "ckpt_lv", "ckpt_av", "ckpt_sleep"):

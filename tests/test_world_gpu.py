@@ -33,7 +33,7 @@ def fixture(name):
 def test_world_matches_reference_fixture(ctx, name):
     sc, steps, every = worldio.make_scene(name)
     w = engine.World(ctx, sc)
-    got = worldio.trajectory(w, steps, every)
+    got = worldio.trajectory(w, steps, every, worldio.DRIVERS.get(name))
     exp = fixture(name)
     assert worldio.first_mismatch(got, exp) is None, worldio.first_mismatch(got, exp)
     for k in ("ckpt_pos", "ckpt_ori", "ckpt_lv", "ckpt_av", "ckpt_sleep"):
@@ -270,4 +270,77 @@ def test_ragdolls_with_limits_stay_within_tolerance(ctx):
     assert ours <= max(spread, 1e-5), (ours, spread)
     pw, pr = w.bodies()[0], r.bodies()[0]
     assert (pw[1:, 1] > 0.45).all() and (pr[1:, 1] > 0.45).all()
+    w.close()
+
+
+def _slider_translations(bodies, n):
+    """Translation of each mechanism's sliding box along its slider from the
+    creation offset (positions of bodies 8 and 9 of each 12-body mechanism)."""
+    p = bodies[0].astype(np.float64)
+    return np.array([p[9 + 12 * m, 1] - p[8 + 12 * m, 1] - 2.1 for m in range(n)])
+
+
+@pytest.mark.skipif(not reflib.have_ref("f32"), reason="reference engine not built")
+def test_mechanisms_match_reference_live(ctx):
+    """Fixed and slider joints (translation limits, a motor whose speed is set
+    before every step) next to ball-and-socket chains and motorised hinges:
+    36 copies of the testbed's joints scene stay bit-identical to the float
+    reference for 300 steps (pairs, manifolds and states every 10 steps), and
+    the sliders reach both of their limits."""
+    n = 36
+    sc = scenes.mechanism_world(n, seed=37)
+    w, r = engine.World(ctx, sc), reflib.RefScene(sc)
+    lo, hi = np.inf, -np.inf
+    for s in range(300):
+        for j, v in scenes.mechanism_motor_speeds(n, s, worldio.DT):
+            w.set_motor_speed(j, v)
+            r.set_motor_speed(j, v)
+        w.update(float(worldio.DT))
+        r.update(float(worldio.DT))
+        if s % 10 == 9:
+            assert np.array_equal(w.pairs(), r.pairs()), s
+            for a, b in zip(w.contacts(), r.contacts()):
+                assert np.array_equal(a, b), s
+            for a, b in zip(w.bodies(), r.bodies()):
+                assert np.array_equal(a, b), s
+            u = _slider_translations(r.bodies(), n)
+            lo, hi = min(lo, u.min()), max(hi, u.max())
+    assert lo < -1.6 and hi > 1.6, (lo, hi)
+    w.close()
+
+
+@pytest.mark.skipif(not reflib.have_ref("f32"), reason="reference engine not built")
+def test_mechanism_group_matches_reference_worlds(ctx):
+    """Mechanism worlds in one group, motor speeds set per world: each world
+    stays bit-identical to its own reference world."""
+    parts = [scenes.mechanism_world(k, seed=40 + k) for k in (1, 3, 2)]
+    shapes, merged = scenes.merge_shapes(parts)
+    g = engine.WorldGroup(ctx, merged, shapes, threads=2)
+    refs = [reflib.RefScene(s) for s in parts]
+    for s in range(150):
+        for k, (part, r) in enumerate(zip((1, 3, 2), refs)):
+            for j, v in scenes.mechanism_motor_speeds(part, s, worldio.DT):
+                g.set_motor_speed(j, v, world=k)
+                r.set_motor_speed(j, v)
+        g.update(float(worldio.DT))
+        for k, r in enumerate(refs):
+            r.update(float(worldio.DT))
+            if s % 10 == 9:
+                for a, b in zip(g.bodies(k), r.bodies()):
+                    assert np.array_equal(a, b), (s, k)
+    g.close()
+
+
+def test_motor_speed_rejects_bad_joints(ctx):
+    sc = scenes.mechanism_world(1)
+    w = engine.World(ctx, sc)
+    with pytest.raises(engine.Rp3dgError):
+        w.set_motor_speed(0, 1.0)        # a ball-and-socket joint has no motor
+    with pytest.raises(engine.Rp3dgError):
+        w.set_motor_speed(8, 1.0)        # nor has a fixed joint
+    with pytest.raises(engine.Rp3dgError):
+        w.set_motor_speed(len(sc.joints), 1.0)
+    w.set_motor_speed(6, 0.5)            # the slider
+    w.set_motor_speed(7, -1.0)           # the hinge
+    w.update(float(worldio.DT))
     w.close()

@@ -20,8 +20,16 @@ WORLD_CASES = {
                      dict(n_bodies=40, cols=18, rows=21, cell=1.25, y_scale=0.7, seed=12,
                           terrain_position=(0.5, -0.3, 0.25),
                           terrain_orientation=(0.0499792, 0.0, 0.0299875, 0.9983002)), 200, 50),
+    # the testbed's joints scene: ball-and-socket chain, motorised slider
+    # with limits, motorised hinge, fixed joints; slider speeds set every step
+    "mechanisms4": (scenes.mechanism_world, dict(n_mechanisms=4, seed=31), 240, 60),
 }
 DT = np.float32(1.0 / 60.0)
+# cases whose joints' motors are driven between steps: name -> f(world, step)
+DRIVERS = {
+    "mechanisms4": lambda world, step: [world.set_motor_speed(j, v)
+                                        for j, v in scenes.mechanism_motor_speeds(4, step, DT)],
+}
 
 
 def digest(*arrays):
@@ -36,11 +44,14 @@ def make_scene(name):
     return f(**kw), steps, every
 
 
-def trajectory(world, steps, every):
-    """Step `world` (engine.World or reflib.RefScene) and record the trace."""
+def trajectory(world, steps, every, driver=None):
+    """Step `world` (engine.World or reflib.RefScene) and record the trace;
+    driver(world, step) runs before each update."""
     rec = {k: [] for k in ("pair_n", "pair_h", "man_n", "pt_n", "man_h", "pt_h")}
     ckpt = {k: [] for k in ("pos", "ori", "lv", "av", "sleep")}
     for s in range(steps):
+        if driver is not None:
+            driver(world, s)
         world.update(float(DT))
         p = world.pairs()
         b1, b2, k, nd, l1, l2 = world.contacts()
