@@ -599,6 +599,51 @@ int rp3dg_world_get_contacts(rp3dg_world* world, int32_t* body1, int32_t* body2,
                              uint32_t capacity_points, uint32_t* nb_manifolds, uint32_t* nb_contact_points);
 int rp3dg_world_get_stats(rp3dg_world* world, rp3dg_world_stats* stats);
 
+/* PhysicsWorld::raycast(ray, callback, raycastWithCategoryMaskBits)
+ * (PhysicsWorld.h:486-490) for a batch of rays, each traced as the reference
+ * traces one: DynamicAABBTree::raycast (DynamicAABBTree.cpp:684-747) over the
+ * world's broad-phase tree in its stack order, the category filter
+ * (BroadPhaseSystem.cpp:224-240), Collider::raycast into the collider's local
+ * space (Collider.cpp:173-192) and the shape's raycast (SphereShape.cpp:61,
+ * CapsuleShape.cpp:97, BoxShape.cpp:62, ConvexMeshShape.cpp:107,
+ * HeightFieldShape.cpp:76 with HeightField.cpp:258-361 and
+ * TriangleShape.cpp:143), with one of three RaycastCallback behaviours:
+ *   CLOSEST  notifyRaycastHit returns hitFraction (the ray is clipped to each
+ *            hit; the last hit reported is the result)
+ *   ANY      returns 0 (the first hit in traversal order stops the ray)
+ *   ALL      returns 1 (every hit is reported, in traversal order)
+ * The world's state is the one after its last update. */
+#define RP3DG_RAYCAST_CLOSEST 0
+#define RP3DG_RAYCAST_ANY 1
+#define RP3DG_RAYCAST_ALL 2
+typedef struct rp3dg_ray {
+    float point1[3];               /* Ray::point1, world space */
+    float point2[3];               /* Ray::point2 */
+    float max_fraction;            /* Ray::maxFraction (1 by default) */
+    uint32_t category_mask;        /* raycastWithCategoryMaskBits (0xFFFF by default) */
+} rp3dg_ray;
+typedef struct rp3dg_raycast_hit { /* RaycastInfo */
+    float world_point[3];
+    float world_normal[3];
+    float hit_fraction;
+    int32_t body;                  /* creation index of the body */
+    int32_t collider;              /* creation index of the collider */
+    int32_t flags;                 /* bit 0: a height-field walk stopped at its cell limit (where the
+                                      reference's walk does not end: a ray with an exactly zero z
+                                      direction entering on a cell boundary) */
+} rp3dg_raycast_hit;
+/* n rays of world `world_index` (0 for rp3dg_world_create): hits holds
+ * max_hits records per ray (ray i at hits[i * max_hits]), nb_hits[i] the
+ * number of hits the callback received (it may exceed max_hits in ALL mode;
+ * CLOSEST and ANY keep one record, the last received).  Host arrays. */
+int rp3dg_world_raycast(rp3dg_world* world, uint32_t world_index, const rp3dg_ray* rays, uint32_t n, int32_t mode,
+                        uint32_t max_hits, rp3dg_raycast_hit* hits, uint32_t* nb_hits);
+/* The same with device arrays; returns when the results are written.
+ * kernel_ms (may be NULL) receives the traversal kernel's duration. */
+int rp3dg_world_raycast_device(rp3dg_world* world, uint32_t world_index, const rp3dg_ray* rays, uint32_t n,
+                               int32_t mode, uint32_t max_hits, rp3dg_raycast_hit* hits, uint32_t* nb_hits,
+                               float* kernel_ms);
+
 /* Many independent worlds stepped together (the batch of the many-worlds
  * workload): nb_worlds worlds, world k made of bodies[body_offsets[k] ..
  * body_offsets[k+1]) and colliders[collider_offsets[k] .. collider_offsets[k+1])

@@ -60,6 +60,7 @@ struct World {
     PhysicsWorld* world = nullptr;
     std::vector<RigidBody*> bodies;
     std::vector<Joint*> joints;  // in creation order
+    std::vector<Collider*> colliders;  // in creation order
     Capture cap;
 };
 
@@ -500,10 +501,42 @@ static std::vector<HeightFieldSpec>& heightfields() {
     static std::vector<HeightFieldSpec> h;
     return h;
 }
+// Convex meshes for world scenes (shape kind RP3DG_SHAPE_CONVEX_MESH, the
+// shape's mesh field naming the id returned here): ref_scene_create builds
+// each with PhysicsCommon::createConvexMesh(PolygonVertexArray) and
+// createConvexMeshShape(mesh, scale) in the world's PhysicsCommon.
+struct ConvexSpec {
+    std::vector<float> vertices;
+    std::vector<uint32_t> indices;
+    std::vector<PolygonVertexArray::PolygonFace> faces;
+    float scale[3];
+};
+static std::vector<ConvexSpec>& convex_specs() {
+    static std::vector<ConvexSpec> c;
+    return c;
+}
+int ref_convex_register(const float* vertices, uint32_t nv, const uint32_t* face_indices, const uint32_t* face_sizes,
+                        uint32_t nf, float sx, float sy, float sz) {
+    ConvexSpec c;
+    c.vertices.assign(vertices, vertices + 3 * size_t(nv));
+    uint32_t total = 0;
+    for (uint32_t f = 0; f < nf; f++) {
+        PolygonVertexArray::PolygonFace pf;
+        pf.nbVertices = face_sizes[f];
+        pf.indexBase = total;
+        c.faces.push_back(pf);
+        total += face_sizes[f];
+    }
+    c.indices.assign(face_indices, face_indices + total);
+    c.scale[0] = sx; c.scale[1] = sy; c.scale[2] = sz;
+    convex_specs().push_back(std::move(c));
+    return int(convex_specs().size()) - 1;
+}
+
 // ref_scene_create builds a reference world from the rp3dg_world_settings /
 // rp3dg_body_desc / rp3dg_collider_desc arrays that rp3dg_world_create takes,
 // with the call sequence documented there (include/rp3dg.h), so that both
-// engines start from identical worlds.  Convex meshes are not used here.
+// engines start from identical worlds.
 int ref_heightfield_register(uint32_t ncol, uint32_t nrow, const float* heights, float sx, float sy, float sz) {
     HeightFieldSpec h;
     h.ncol = int(ncol);
@@ -544,6 +577,18 @@ int ref_scene_create(const rp3dg_world_settings* s, const rp3dg_shape* shapes, u
             if (!hf) return -1;
             cs[i] = W->common.createHeightFieldShape(hf, Vector3(h.scale[0], h.scale[1], h.scale[2]));
         }
+        else if (sh.kind == RP3DG_SHAPE_CONVEX_MESH) {
+            if (sh.mesh < 0 || size_t(sh.mesh) >= convex_specs().size()) return -1;
+            ConvexSpec& c = convex_specs()[size_t(sh.mesh)];
+            PolygonVertexArray pva(uint32(c.vertices.size() / 3), c.vertices.data(), 3 * sizeof(float),
+                                   c.indices.data(), sizeof(uint32_t), uint32(c.faces.size()), c.faces.data(),
+                                   PolygonVertexArray::VertexDataType::VERTEX_FLOAT_TYPE,
+                                   PolygonVertexArray::IndexDataType::INDEX_INTEGER_TYPE);
+            std::vector<Message> messages;
+            ConvexMesh* mesh = W->common.createConvexMesh(pva, messages);
+            if (!mesh) return -1;
+            cs[i] = W->common.createConvexMeshShape(mesh, Vector3(c.scale[0], c.scale[1], c.scale[2]));
+        }
         else return -1;
     }
     uint32_t ci = 0;
@@ -562,6 +607,7 @@ int ref_scene_create(const rp3dg_world_settings* s, const rp3dg_shape* shapes, u
             col->getMaterial().setMassDensity(c.mass_density);
             col->setCollisionCategoryBits(c.category);
             col->setCollideWithMaskBits(c.mask);
+            W->colliders.push_back(col);
             ci++;
         }
         if (d.type == RP3DG_BODY_DYNAMIC) body->updateMassPropertiesFromColliders();
@@ -624,6 +670,57 @@ int ref_scene_add_joints(int id, const rp3dg_joint_desc* jd, uint32_t n) {
             info.maxMotorTorque = d.max_motor_torque;
             W.joints.push_back(W.world->createJoint(info));
         }
+    }
+    return 0;
+}
+
+// PhysicsWorld::raycast for each ray with a RaycastCallback that keeps the
+// last hit and returns its hitFraction (mode 0), returns 0 after the first
+// hit (mode 1) or records every hit and returns 1 (mode 2); hits as
+// rp3dg_raycast_hit (flags 0), max_hits records per ray, counts per ray.
+struct RayRecorder : public RaycastCallback {
+    int mode = 0;
+    uint32_t max_hits = 1, count = 0;
+    rp3dg_raycast_hit* out = nullptr;
+    const std::unordered_map<const void*, int32_t>* bindex = nullptr;
+    const std::unordered_map<const void*, int32_t>* cindex = nullptr;
+    decimal notifyRaycastHit(const RaycastInfo& info) override {
+        rp3dg_raycast_hit h{};
+        h.world_point[0] = float(info.worldPoint.x); h.world_point[1] = float(info.worldPoint.y);
+        h.world_point[2] = float(info.worldPoint.z);
+        h.world_normal[0] = float(info.worldNormal.x); h.world_normal[1] = float(info.worldNormal.y);
+        h.world_normal[2] = float(info.worldNormal.z);
+        h.hit_fraction = float(info.hitFraction);
+        h.body = bindex->at(static_cast<const void*>(info.body));
+        h.collider = cindex->at(static_cast<const void*>(info.collider));
+        if (mode == 2) {
+            if (count < max_hits) out[count] = h;
+        } else if (max_hits) {
+            out[0] = h;
+        }
+        count++;
+        return mode == 0 ? info.hitFraction : (mode == 1 ? decimal(0.0) : decimal(1.0));
+    }
+};
+int ref_scene_raycast(int id, const rp3dg_ray* rays, uint32_t n, int mode, uint32_t max_hits, rp3dg_raycast_hit* hits,
+                      uint32_t* counts) {
+    World& W = *worlds().at(size_t(id));
+    std::unordered_map<const void*, int32_t> bindex, cindex;
+    for (size_t i = 0; i < W.bodies.size(); i++) bindex[static_cast<const void*>(static_cast<Body*>(W.bodies[i]))] = int32_t(i);
+    for (size_t i = 0; i < W.colliders.size(); i++) cindex[static_cast<const void*>(W.colliders[i])] = int32_t(i);
+    RayRecorder cb;
+    cb.mode = mode;
+    cb.max_hits = max_hits;
+    cb.bindex = &bindex;
+    cb.cindex = &cindex;
+    for (uint32_t i = 0; i < n; i++) {
+        const rp3dg_ray& r = rays[i];
+        cb.count = 0;
+        cb.out = hits + size_t(i) * max_hits;
+        Ray ray(Vector3(r.point1[0], r.point1[1], r.point1[2]), Vector3(r.point2[0], r.point2[1], r.point2[2]),
+                r.max_fraction);
+        W.world->raycast(ray, &cb, static_cast<unsigned short>(r.category_mask));
+        counts[i] = cb.count;
     }
     return 0;
 }

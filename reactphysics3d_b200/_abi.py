@@ -137,6 +137,12 @@ JOINT_DESC_DTYPE = np.dtype([
     ("limit_enabled", "<i4"), ("min_angle", "<f4"), ("max_angle", "<f4"),
     ("motor_enabled", "<i4"), ("motor_speed", "<f4"), ("max_motor_torque", "<f4")])
 assert JOINT_DESC_DTYPE.itemsize == 72
+RAYCAST_CLOSEST, RAYCAST_ANY, RAYCAST_ALL = 0, 1, 2
+RAY_DTYPE = np.dtype([("point1", "<f4", (3,)), ("point2", "<f4", (3,)), ("max_fraction", "<f4"),
+                      ("category_mask", "<u4")])
+RAYCAST_HIT_DTYPE = np.dtype([("world_point", "<f4", (3,)), ("world_normal", "<f4", (3,)), ("hit_fraction", "<f4"),
+                              ("body", "<i4"), ("collider", "<i4"), ("flags", "<i4")])
+assert RAY_DTYPE.itemsize == 32 and RAYCAST_HIT_DTYPE.itemsize == 40
 assert WORLD_SETTINGS_DTYPE.itemsize == 48 and BODY_DESC_DTYPE.itemsize == 96
 assert COLLIDER_DESC_DTYPE.itemsize == 52 and WORLD_STATS_DTYPE.itemsize == 40
 
@@ -156,6 +162,14 @@ def default_world_settings():
     s["cos_angle_similar_contact_manifold"] = f(0.95)
     s["position_iterations"] = 3
     return s
+
+
+def rays(n):
+    """Ray defaults: maxFraction 1, category mask 0xFFFF."""
+    r = np.zeros(n, RAY_DTYPE)
+    r["max_fraction"] = 1.0
+    r["category_mask"] = 0xFFFF
+    return r
 
 
 def joint_descs(n):

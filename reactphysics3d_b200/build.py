@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "librp3dg.so")
-SOURCES = ["rp3dg_host.cu", "narrowphase.cu", "axis_mlp.cu", "contacts.cu", "dynamics.cu", "broadphase.cu", "world.cu", "heightfield.cu"]
+SOURCES = ["rp3dg_host.cu", "narrowphase.cu", "axis_mlp.cu", "contacts.cu", "dynamics.cu", "broadphase.cu", "world.cu", "heightfield.cu", "raycast.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 FP_FLAGS = ["--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]

@@ -1,0 +1,42 @@
+// Launch interface of the batched world raycast (raycast.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/rp3dg.h"
+#include "rp3dg_internal.h"
+
+namespace rp3dg {
+
+// One node of the world's dynamic AABB tree, as the ray traversal reads it:
+// lo = (fat AABB min, child 0), hi = (fat AABB max, child 1), the children as
+// int bits (-1: none).  A leaf has child 0 = -2 - collider index.
+struct __align__(16) RayNode {
+    float4 lo, hi;
+};
+
+// Per collider (creation order): x device row of its world transform,
+// y body index, z shape index, w collision category bits.
+struct RayArgs {
+    const RayNode* nodes;
+    int32_t root;
+    const int4* colliders;
+    const float4* c_wpos;          // collider local-to-world position, by row
+    const float4* c_wori;          // and orientation
+    const rp3dg_shape* shapes;
+    const uint32_t* mesh_words;    // convex mesh arena
+    const HfDesc* hfields;         // height fields of the context, by id
+    uint32_t nb_hfields;
+    const rp3dg_ray* rays;
+    uint32_t n;
+    int32_t mode;                  // RP3DG_RAYCAST_*
+    uint32_t max_hits;
+    rp3dg_raycast_hit* hits;       // n * max_hits
+    uint32_t* nb_hits;             // n
+    uint32_t* error;               // bit 0: a traversal stack overflowed
+};
+
+cudaError_t launch_world_raycast(const RayArgs& a, cudaStream_t stream);
+
+}  // namespace rp3dg

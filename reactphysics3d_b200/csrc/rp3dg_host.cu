@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <cfloat>
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -36,7 +37,10 @@ struct MeshTopo {
     std::vector<uint32_t> face_start, face_count, face_verts, face_edge;
     std::vector<HalfEdge> edges;
     std::vector<float> normals;  // nf*3 (unit, unscaled mesh)
+    std::vector<float> area2;    // nf: length of the Newell normal (twice the face area)
     float centroid[3] = {0, 0, 0};
+    float bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};  // ConvexMesh::mBounds
+    float volume = 0.0f;                             // ConvexMesh::mVolume
     uint32_t nv = 0, nf = 0;
 };
 
@@ -346,6 +350,29 @@ int get_shape_device(rp3dg_ctx* ctx, const rp3dg_shape** shapes, const float4** 
     *bounds = reinterpret_cast<const float4*>(ctx->d_shape_bounds);
     return 0;
 }
+// all height fields of the context, by id, and the device convex-mesh arena
+// (world raycasts)
+int get_heightfields(rp3dg_ctx* ctx, std::vector<HfDesc>* out) {
+    if (!ctx || !out) return RP3DG_EINVAL;
+    *out = ctx->hfields;
+    return 0;
+}
+// ConvexMeshShape::getVolume (ConvexMeshShape.h:230-232) and the extents of
+// ConvexMesh::getLocalInertiaTensor (ConvexMesh.h:200-211): volume * sx * sy
+// * sz, and 0.5 * scale * (bounds max - bounds min)
+int get_mesh_mass(rp3dg_ctx* ctx, int32_t instance, float* volume, float* extent) {
+    if (!ctx || instance < 0 || size_t(instance) >= ctx->instances.size()) return RP3DG_EINVAL;
+    const MeshInstance& in = ctx->instances[size_t(instance)];
+    const MeshTopo& m = ctx->meshes[size_t(in.mesh)];
+    *volume = m.volume * in.scale[0] * in.scale[1] * in.scale[2];
+    for (int a = 0; a < 3; a++) extent[a] = (0.5f * in.scale[a]) * (m.bmax[a] - m.bmin[a]);
+    return 0;
+}
+int get_mesh_arena_device(rp3dg_ctx* ctx, const uint32_t** words) {
+    if (!ctx || !words) return RP3DG_EINVAL;
+    *words = ctx->d_arena;
+    return 0;
+}
 // a height field of the context (world set-up and middle phase)
 int get_heightfield(rp3dg_ctx* ctx, int32_t id, HfDesc* out) {
     if (!ctx || !out || id < 0 || size_t(id) >= ctx->hfields.size()) return RP3DG_EINVAL;
@@ -469,6 +496,27 @@ int rp3dg_create_convex_mesh(rp3dg_ctx* ctx, const float* vertices, uint32_t nv,
         const float len = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
         if (!(len > FLT_EPSILON)) return fail(ctx, RP3DG_EINVAL, "face with zero area");
         m.normals[3 * f] = n[0] / len; m.normals[3 * f + 1] = n[1] / len; m.normals[3 * f + 2] = n[2] / len;
+        m.area2.push_back(len);
+    }
+    // bounds: ConvexMesh::copyVertices (AABB::inflateWithPoint over the vertices)
+    for (int a = 0; a < 3; a++) m.bmin[a] = m.bmax[a] = m.verts[size_t(a)];
+    for (uint32_t i = 0; i < nv; i++)
+        for (int a = 0; a < 3; a++) {
+            const float v = m.verts[3 * i + a];
+            m.bmin[a] = std::min(m.bmin[a], v);
+            m.bmax[a] = std::max(m.bmax[a], v);
+        }
+    // ConvexMesh::computeVolume (ConvexMesh.cpp:248-264): sum over the faces of
+    // (first vertex . unit normal) * (Newell normal length * 0.5), |sum| / 3
+    {
+        float sum = 0.0f;
+        for (uint32_t f = 0; f < nf; f++) {
+            const float area = m.area2[f] * 0.5f;
+            const float* v = &m.verts[3 * m.face_verts[m.face_start[f]]];
+            const float* n = &m.normals[3 * f];
+            sum += (v[0] * n[0] + v[1] * n[1] + v[2] * n[2]) * area;
+        }
+        m.volume = std::fabs(sum) / 3.0f;
     }
     ctx->meshes.push_back(std::move(m));
     *mesh_id = int32_t(ctx->meshes.size() - 1);

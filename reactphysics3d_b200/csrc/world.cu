@@ -56,6 +56,7 @@
 #include "../../include/rp3dg.h"
 #include "dynamics_launch.h"
 #include "hf_launch.h"
+#include "raycast_launch.h"
 #include "rp3dg_math.cuh"
 #include "world_order.h"
 
@@ -72,6 +73,9 @@ int broadphase_update_flags(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, const ui
 // height fields, the shape table and its local bounds on the device, and the
 // triangle tests of convex vs concave pairs
 int get_heightfield(rp3dg_ctx* ctx, int32_t id, HfDesc* out);
+int get_heightfields(rp3dg_ctx* ctx, std::vector<HfDesc>* out);
+int get_mesh_arena_device(rp3dg_ctx* ctx, const uint32_t** words);
+int get_mesh_mass(rp3dg_ctx* ctx, int32_t instance, float* volume, float* extent);
 int get_shape_device(rp3dg_ctx* ctx, const rp3dg_shape** shapes, const float4** bounds);
 int narrowphase_tri_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3dg_contact_batch* out,
                            const float4* tri);
@@ -350,9 +354,23 @@ uint32_t blocks(uint32_t n) { return (n + 127) / 128; }
 
 // Volume and local inertia tensor of a shape (BoxShape.h:233, BoxShape.cpp:53-59,
 // SphereShape.h:170-178, CapsuleShape.h:175-177, CapsuleShape.cpp:51-67).
-bool shape_mass(const rp3dg_shape& s, float mass_density, float* inertia /*3*/, float* mass_out) {
+bool shape_mass(rp3dg_ctx* ctx, const rp3dg_shape& s, float mass_density, float* inertia /*3*/, float* mass_out) {
     const float PI = float(3.141592653589);
     float vol;
+    if (s.kind == RP3DG_SHAPE_CONVEX_MESH) {
+        // ConvexMeshShape::getVolume and ConvexMesh::getLocalInertiaTensor: the
+        // inertia of the box of the scaled bounds
+        float ext[3];
+        if (rp3dg::get_mesh_mass(ctx, s.mesh, &vol, ext)) return false;
+        const float mass = vol * mass_density;
+        const float factor = (1.0f / 3.0f) * mass;
+        const float xs = ext[0] * ext[0], ys = ext[1] * ext[1], zs = ext[2] * ext[2];
+        inertia[0] = factor * (ys + zs);
+        inertia[1] = factor * (xs + zs);
+        inertia[2] = factor * (xs + ys);
+        *mass_out = mass;
+        return true;
+    }
     if (s.kind == RP3DG_SHAPE_BOX) {
         vol = 8.0f * s.params[0] * s.params[1] * s.params[2];
     } else if (s.kind == RP3DG_SHAPE_SPHERE) {
@@ -732,6 +750,20 @@ struct rp3dg_world {
     int32_t *h_tq = nullptr, *d_tq = nullptr, *h_tleaves = nullptr, *d_tleaves = nullptr;
     int2 *h_tpos = nullptr, *d_tpos = nullptr;
     uint32_t *h_tcnt = nullptr, *d_tcnt = nullptr;   // [0] leaves reserved, [1] flags
+    // world raycasts: the tree's nodes and the collider table as the ray
+    // kernel reads them (rebuilt when the world state changed), rays and hits
+    uint64_t state_version = 1;      // bumped by every update and between-step change
+    uint64_t ray_version = 0;        // state the ray tables were built for
+    uint32_t ray_world = 0;
+    rp3dg::RayNode *h_rnodes = nullptr, *d_rnodes = nullptr;
+    int4 *h_rcols = nullptr, *d_rcols = nullptr;
+    size_t cap_rnodes = 0, cap_rcols = 0, cap_rhf = 0, cap_rays = 0, cap_rhits = 0, cap_rcount = 0;
+    rp3dg::HfDesc* d_rhf = nullptr;
+    uint32_t nb_rhf = 0;
+    rp3dg_ray* d_rays = nullptr;
+    rp3dg_raycast_hit* d_rhits = nullptr;
+    uint32_t* d_rcount = nullptr;    // n counts, then the error word
+    cudaEvent_t ev_r0 = nullptr, ev_r1 = nullptr;
     // manifold packing
     size_t cap_m = 0, cap_i = 0;
     int4 *d_mids = nullptr, *d_msrc = nullptr, *d_mprev = nullptr;
@@ -1692,6 +1724,10 @@ void destroy_group(Group* g) {
     cudaFreeHost(g->h_tnodes); cudaFree(g->d_tnodes); cudaFreeHost(g->h_tq); cudaFree(g->d_tq);
     cudaFreeHost(g->h_tleaves); cudaFree(g->d_tleaves); cudaFreeHost(g->h_tpos); cudaFree(g->d_tpos);
     cudaFreeHost(g->h_tcnt); cudaFree(g->d_tcnt);
+    cudaFreeHost(g->h_rnodes); cudaFree(g->d_rnodes); cudaFreeHost(g->h_rcols); cudaFree(g->d_rcols);
+    cudaFree(g->d_rhf); cudaFree(g->d_rays); cudaFree(g->d_rhits); cudaFree(g->d_rcount);
+    if (g->ev_r0) cudaEventDestroy(g->ev_r0);
+    if (g->ev_r1) cudaEventDestroy(g->ev_r1);
     if (g->ev_rect) cudaEventDestroy(g->ev_rect);
     cudaFreeHost(g->t_grav); cudaFreeHost(g->t_ben); cudaFreeHost(g->t_cen); cudaFreeHost(g->t_cbody);
     cudaFreeHost(g->t_cshape); cudaFreeHost(g->t_cat); cudaFreeHost(g->t_mask); cudaFreeHost(g->t_bperm);
@@ -1763,8 +1799,8 @@ int build_world(Group* g, WorldH& w, const rp3dg_body_desc* bd, uint32_t nb, con
             float total = 0.0f, com[3] = {0.f, 0.f, 0.f};
             for (uint32_t k : mine) {
                 float in[3], m;
-                if (!shape_mass(g->shapes[size_t(cd[k].shape)], cd[k].mass_density, in, &m))
-                    return cfail(g->ctx, RP3DG_EINVAL, "mass properties of a convex-mesh collider are not supported");
+                if (!shape_mass(g->ctx, g->shapes[size_t(cd[k].shape)], cd[k].mass_density, in, &m))
+                    return cfail(g->ctx, RP3DG_EINVAL, "mass properties of a concave or unknown collider shape");
                 total += m;
                 for (int a = 0; a < 3; a++) com[a] += m * cd[k].position[a];
             }
@@ -1774,7 +1810,7 @@ int build_world(Group* g, WorldH& w, const rp3dg_body_desc* bd, uint32_t nb, con
             float total2 = 0.0f;
             for (uint32_t k : mine) {
                 float in[3], m;
-                shape_mass(g->shapes[size_t(cd[k].shape)], cd[k].mass_density, in, &m);
+                shape_mass(g->ctx, g->shapes[size_t(cd[k].shape)], cd[k].mass_density, in, &m);
                 total2 += m;
                 float R[3][3], RT[3][3], I[3][3];
                 quat_matrix(cd[k].orientation, R);
@@ -1999,6 +2035,7 @@ void tuner_step(Group* g);
 int update_group(Group* g, float dt) {
     if (!g) return RP3DG_EINVAL;
     if (!(dt > 0.0f)) return wfail(g, RP3DG_EINVAL, "dt must be positive");
+    g->state_version++;
     cudaStream_t st = g->stream;
     rp3dg_ctx* ctx = g->ctx;
     std::memset(&g->stats, 0, sizeof(g->stats));
@@ -2804,7 +2841,133 @@ int rp3dg_world_set_motor_speed(rp3dg_world* g, uint32_t world, uint32_t joint, 
     if (e != cudaSuccess) return wcuda(g, e, "motor speed");
     set_sleeping(g, w, J.b1, false);
     set_sleeping(g, w, J.b2, false);
+    g->state_version++;
     return sync_rows(g);
+}
+
+// The ray kernel's view of world `world`: the broad-phase tree's nodes
+// (children, fat AABBs, leaves as collider indices) and per collider its
+// transform row, body, shape and category bits; rebuilt when the state
+// changed since the last build.
+int ray_tables(Group* g, uint32_t world) {
+    if (g->ray_version == g->state_version && g->ray_world == world && g->d_rnodes) return 0;
+    int rc = sync_rows(g);
+    if (rc) return rc;
+    WorldH& w = g->worlds[world];
+    const size_t nn = std::max<size_t>(w.tree.nodes.size(), 1);
+    const size_t nc = std::max<size_t>(w.colliders.size(), 1);
+    if (!pair_grow(&g->h_rnodes, &g->d_rnodes, &g->cap_rnodes, nn) ||
+        !pair_grow(&g->h_rcols, &g->d_rcols, &g->cap_rcols, nc))
+        return wfail(g, RP3DG_ENOMEM, "allocation of raycast tables");
+    for (size_t k = 0; k < w.tree.nodes.size(); k++) {
+        const rp3dg::order::Tree::Node& N = w.tree.nodes[k];
+        rp3dg::RayNode& R = g->h_rnodes[k];
+        const bool leaf = N.height == 0;
+        const int c0 = leaf ? -2 - N.data : N.child[0];
+        const int c1 = leaf ? -1 : N.child[1];
+        R.lo = make_float4(N.box.mn[0], N.box.mn[1], N.box.mn[2], __int_as_float_host(c0));
+        R.hi = make_float4(N.box.mx[0], N.box.mx[1], N.box.mx[2], __int_as_float_host(c1));
+    }
+    for (size_t c = 0; c < w.colliders.size(); c++) {
+        const ColliderH& C = w.colliders[c];
+        g->h_rcols[c] = make_int4(int(w.c0) + w.ccomp.slot[c], C.body, C.shape, int(C.category));
+    }
+    std::vector<rp3dg::HfDesc> hf;
+    rp3dg::get_heightfields(g->ctx, &hf);
+    if (!hf.empty() && dev_grow(&g->d_rhf, &g->cap_rhf, hf.size()))
+        return wfail(g, RP3DG_ENOMEM, "allocation of raycast tables");
+    cudaStream_t st = g->stream;
+    cudaMemcpyAsync(g->d_rnodes, g->h_rnodes, w.tree.nodes.size() * sizeof(rp3dg::RayNode), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(g->d_rcols, g->h_rcols, w.colliders.size() * sizeof(int4), cudaMemcpyHostToDevice, st);
+    if (!hf.empty())
+        cudaMemcpyAsync(g->d_rhf, hf.data(), hf.size() * sizeof(rp3dg::HfDesc), cudaMemcpyHostToDevice, st);
+    g->nb_rhf = uint32_t(hf.size());
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return wcuda(g, e, "raycast tables");
+    g->ray_version = g->state_version;
+    g->ray_world = world;
+    return 0;
+}
+
+// Rays, hits and counts in device memory (on the world's stream).
+int raycast_device(Group* g, uint32_t world, const rp3dg_ray* rays, uint32_t n, int32_t mode, uint32_t max_hits,
+                   rp3dg_raycast_hit* hits, uint32_t* nb_hits, float* kernel_ms) {
+    int rc = ray_tables(g, world);
+    if (rc) return rc;
+    if (dev_grow(&g->d_rcount, &g->cap_rcount, 1))
+        return wfail(g, RP3DG_ENOMEM, "allocation of the raycast error word");
+    if (!g->ev_r0 && (cudaEventCreate(&g->ev_r0) != cudaSuccess || cudaEventCreate(&g->ev_r1) != cudaSuccess))
+        return wfail(g, RP3DG_ECUDA, "cudaEventCreate(raycast)");
+    cudaStream_t st = g->stream;
+    WorldH& w = g->worlds[world];
+    rp3dg::RayArgs a{};
+    a.nodes = g->d_rnodes;
+    a.root = w.tree.root;
+    a.colliders = g->d_rcols;
+    a.c_wpos = g->ccol[g->cur_c][CC_WPOS];
+    a.c_wori = g->ccol[g->cur_c][CC_WORI];
+    const float4* bounds = nullptr;
+    rp3dg::get_shape_device(g->ctx, &a.shapes, &bounds);
+    rp3dg::get_mesh_arena_device(g->ctx, &a.mesh_words);
+    a.hfields = g->d_rhf;
+    a.nb_hfields = g->nb_rhf;
+    a.rays = rays;
+    a.n = n;
+    a.mode = mode;
+    a.max_hits = max_hits;
+    a.hits = hits;
+    a.nb_hits = nb_hits;
+    a.error = g->d_rcount;
+    cudaMemsetAsync(g->d_rcount, 0, sizeof(uint32_t), st);
+    cudaEventRecord(g->ev_r0, st);
+    cudaError_t e = rp3dg::launch_world_raycast(a, st);
+    cudaEventRecord(g->ev_r1, st);
+    if (e != cudaSuccess) return wcuda(g, e, "raycast kernel");
+    uint32_t err = 0;
+    cudaMemcpyAsync(&err, g->d_rcount, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return wcuda(g, e, "raycast");
+    if (kernel_ms) cudaEventElapsedTime(kernel_ms, g->ev_r0, g->ev_r1);
+    if (err & 1u) return wfail(g, RP3DG_ECAPACITY, "raycast: tree deeper than the traversal stack");
+    return 0;
+}
+
+int raycast_args(Group* g, uint32_t world, const void* rays, uint32_t n, int32_t mode, uint32_t max_hits,
+                 const void* hits, const void* nb_hits) {
+    if (!g) return RP3DG_EINVAL;
+    if (world >= g->worlds.size()) return wfail(g, RP3DG_EINVAL, "bad world index");
+    if (mode != RP3DG_RAYCAST_CLOSEST && mode != RP3DG_RAYCAST_ANY && mode != RP3DG_RAYCAST_ALL)
+        return wfail(g, RP3DG_EINVAL, "bad raycast mode");
+    if (n && (!rays || !nb_hits || (max_hits && !hits))) return wfail(g, RP3DG_EINVAL, "null raycast array");
+    return 0;
+}
+
+int rp3dg_world_raycast_device(rp3dg_world* g, uint32_t world, const rp3dg_ray* rays, uint32_t n, int32_t mode,
+                               uint32_t max_hits, rp3dg_raycast_hit* hits, uint32_t* nb_hits, float* kernel_ms) {
+    int rc = raycast_args(g, world, rays, n, mode, max_hits, hits, nb_hits);
+    if (rc || n == 0) return rc;
+    return raycast_device(g, world, rays, n, mode, max_hits, hits, nb_hits, kernel_ms);
+}
+
+int rp3dg_world_raycast(rp3dg_world* g, uint32_t world, const rp3dg_ray* rays, uint32_t n, int32_t mode,
+                        uint32_t max_hits, rp3dg_raycast_hit* hits, uint32_t* nb_hits) {
+    int rc = raycast_args(g, world, rays, n, mode, max_hits, hits, nb_hits);
+    if (rc || n == 0) return rc;
+    const size_t nh = size_t(n) * max_hits;
+    if (dev_grow(&g->d_rays, &g->cap_rays, n) || dev_grow(&g->d_rhits, &g->cap_rhits, std::max<size_t>(nh, 1)) ||
+        dev_grow(&g->d_rcount, &g->cap_rcount, size_t(n) + 1))
+        return wfail(g, RP3DG_ENOMEM, "allocation of raycast buffers");
+    cudaStream_t st = g->stream;
+    cudaMemcpyAsync(g->d_rays, rays, size_t(n) * sizeof(rp3dg_ray), cudaMemcpyHostToDevice, st);
+    // the error word sits after the counts
+    uint32_t* counts = g->d_rcount + 1;
+    rc = raycast_device(g, world, g->d_rays, n, mode, max_hits, g->d_rhits, counts, nullptr);
+    if (rc) return rc;
+    if (nh) cudaMemcpyAsync(hits, g->d_rhits, nh * sizeof(rp3dg_raycast_hit), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(nb_hits, counts, size_t(n) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return wcuda(g, e, "raycast results");
+    return 0;
 }
 
 int rp3dg_world_update(rp3dg_world* w, float dt) { return update_group(w, dt); }

@@ -101,6 +101,9 @@ def load_library(path=LIB_PATH):
     L.rp3dg_world_add_joints.argtypes = [P, P, C.c_uint32]
     L.rp3dg_world_group_add_joints.argtypes = [P, C.c_uint32, P, C.c_uint32]
     L.rp3dg_world_set_motor_speed.argtypes = [P, C.c_uint32, C.c_uint32, C.c_float]
+    L.rp3dg_world_raycast.argtypes = [P, C.c_uint32, P, C.c_uint32, C.c_int32, C.c_uint32, P, P]
+    L.rp3dg_world_raycast_device.argtypes = [P, C.c_uint32, P, C.c_uint32, C.c_int32, C.c_uint32, P, P,
+                                             C.POINTER(C.c_float)]
     L.rp3dg_world_group_create.argtypes = [P, P, C.c_uint32, P, P, P, P, C.c_int, C.POINTER(P)]
     L.rp3dg_world_group_get_bodies.argtypes = [P, C.c_uint32, P, P, P, P, P]
     L.rp3dg_world_group_get_pairs.argtypes = [P, C.c_uint32, P, C.c_uint32, C.POINTER(C.c_uint32)]
@@ -263,6 +266,12 @@ class Context:
         ids = [self.create_heightfield(h, s) for (h, s) in hfs]
         for i in np.nonzero(shapes["kind"] == A.SHAPE_HEIGHTFIELD)[0]:
             shapes["mesh"][i] = ids[int(shapes["mesh"][i])]
+        # convex meshes (scene.convex_meshes: list of (vertices, faces, scale);
+        # a convex-mesh shape's mesh field indexes that list)
+        cms = getattr(scene, "convex_meshes", None) or []
+        inst = [self.create_convex_mesh_shape(self.create_convex_mesh(v, f), s) for (v, f, s) in cms]
+        for i in np.nonzero(shapes["kind"] == A.SHAPE_CONVEX_MESH)[0]:
+            shapes["mesh"][i] = inst[int(shapes["mesh"][i])]
         return shapes
 
     def mesh_tables(self, instance, cap=4096):
@@ -501,6 +510,30 @@ class World:
         if rc != 0:
             raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
 
+    def raycast(self, rays, mode=A.RAYCAST_CLOSEST, max_hits=1, world=0):
+        """PhysicsWorld::raycast for each row of `rays` (A.RAY_DTYPE) with the
+        CLOSEST / ANY / ALL callback: (hits (n, max_hits) A.RAYCAST_HIT_DTYPE,
+        hit counts (n,))."""
+        r = np.ascontiguousarray(rays, dtype=A.RAY_DTYPE)
+        n = len(r)
+        hits = np.zeros((n, max_hits), A.RAYCAST_HIT_DTYPE)
+        counts = np.zeros(n, np.uint32)
+        rc = self.lib.rp3dg_world_raycast(self.h, int(world), r.ctypes.data, n, int(mode), int(max_hits),
+                                          hits.ctypes.data, counts.ctypes.data)
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+        return hits, counts
+
+    def raycast_device(self, rays_ptr, n, hits_ptr, counts_ptr, mode=A.RAYCAST_CLOSEST, max_hits=1, world=0):
+        """The raycast on device arrays (raw pointers); returns the traversal
+        kernel's duration in ms."""
+        ms = C.c_float()
+        rc = self.lib.rp3dg_world_raycast_device(self.h, int(world), rays_ptr, int(n), int(mode), int(max_hits),
+                                                 hits_ptr, counts_ptr, C.byref(ms))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+        return ms.value
+
     def set_motor_speed(self, joint, speed, world=0):
         """HingeJoint / SliderJoint::setMotorSpeed on joint `joint` (creation
         order) of world `world`; a changed speed wakes the joint's bodies."""
@@ -588,6 +621,17 @@ class WorldGroup(World):
 
     def __init__(self, ctx, scenes_, shapes, threads=None):
         self.ctx, self.lib = ctx, ctx.lib
+        if any(getattr(s, "heightfields", None) or getattr(s, "convex_meshes", None) for s in scenes_):
+            # the table is the scenes' tables back to back (scenes.merge_shapes):
+            # each segment gets its scene's height fields and convex meshes
+            shapes = np.array(shapes, copy=True)
+            base = 0
+            for s in scenes_:
+                seg = ctx.scene_shapes(s)
+                shapes[base:base + len(seg)] = seg
+                base += len(seg)
+            if base != len(shapes):
+                raise ValueError("height fields or convex meshes need the table of scenes.merge_shapes")
         ctx.set_shapes(shapes)
         threads = threads or (os.cpu_count() or 1)
         bodies = np.concatenate([s.bodies for s in scenes_])

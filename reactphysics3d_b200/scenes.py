@@ -187,12 +187,16 @@ class WorldScene:
     """A world description: settings, shape table, bodies, colliders and
     joints (numpy structured arrays with the layouts of include/rp3dg.h)."""
 
-    def __init__(self, settings, shapes, bodies, colliders, name="", joints=None, heightfields=None):
+    def __init__(self, settings, shapes, bodies, colliders, name="", joints=None, heightfields=None,
+                 convex_meshes=None):
         self.settings, self.shapes, self.bodies, self.colliders, self.name = settings, shapes, bodies, colliders, name
         self.joints = joints
         # height fields: list of (heights (nb_rows, nb_columns) float32, scale);
         # a SHAPE_HEIGHTFIELD shape's mesh field indexes this list
         self.heightfields = heightfields or []
+        # convex meshes: list of (vertices (n, 3), polygon faces, scale); a
+        # SHAPE_CONVEX_MESH shape's mesh field indexes this list
+        self.convex_meshes = convex_meshes or []
 
 
 def box_pile(nx=10, ny=10, nz=10, seed=1, spacing=2.0, base=2.0, jitter=0.1):
@@ -223,6 +227,77 @@ def box_pile(nx=10, ny=10, nz=10, seed=1, spacing=2.0, base=2.0, jitter=0.1):
     colliders["friction"] = np.float32(0.3)
     colliders["bounciness"] = 0.0
     return WorldScene(A.default_world_settings(), shapes, bodies, colliders, f"box pile {n}")
+
+
+def hull_world(nx=5, ny=3, nz=5, seed=9, spacing=1.8):
+    """Convex hulls (the reference QuickHull of icosphere42_points(), at
+    scale 0.6 and at the non-uniform scale (0.7, 0.45, 0.55)), boxes, spheres
+    and capsules of random sizes on a jittered grid above a static ground box,
+    random orientations; collision categories 1 and 2 alternate."""
+    rng = np.random.default_rng(seed)
+    verts, faces = load_hull()
+    n = nx * ny * nz
+    kinds = rng.integers(0, 5, size=n)
+    shapes = np.zeros(n + 1, A.SHAPE_DTYPE)
+    shapes["mesh"] = -1
+    shapes[0]["kind"] = A.SHAPE_BOX
+    shapes["params"][0, :3] = (20.0, 0.5, 20.0)
+    for i, k in enumerate(kinds):
+        sh = shapes[i + 1]
+        if k <= 1:
+            sh["kind"] = A.SHAPE_CONVEX_MESH
+            sh["mesh"] = int(k)
+        elif k == 2:
+            sh["kind"] = A.SHAPE_BOX
+            sh["params"][:3] = rng.uniform(0.25, 0.6, 3)
+        elif k == 3:
+            sh["kind"] = A.SHAPE_SPHERE
+            sh["params"][0] = rng.uniform(0.2, 0.5)
+        else:
+            sh["kind"] = A.SHAPE_CAPSULE
+            sh["params"][:2] = (rng.uniform(0.15, 0.3), rng.uniform(0.2, 0.4))
+    bodies = A.body_descs(n + 1)
+    bodies[0]["type"] = A.BODY_STATIC
+    bodies[0]["position"] = (0.0, -0.5, 0.0)
+    iy, ix, iz = np.meshgrid(np.arange(ny), np.arange(nx), np.arange(nz), indexing="ij")
+    centre = np.stack([(ix.ravel() - 0.5 * (nx - 1)) * spacing, 1.0 + iy.ravel() * spacing,
+                       (iz.ravel() - 0.5 * (nz - 1)) * spacing], axis=1) + rng.uniform(-0.1, 0.1, size=(n, 3))
+    bodies["position"][1:] = centre.astype(np.float32)
+    bodies["orientation"][1:] = random_quaternions(rng, n)
+    colliders = A.collider_descs(n + 1)
+    colliders["body"] = np.arange(n + 1)
+    colliders["shape"] = np.arange(n + 1)
+    colliders["friction"] = np.float32(0.4)
+    colliders["bounciness"] = 0.0
+    colliders["category"][1:] = (1 + (np.arange(n) % 2)).astype(np.uint16)
+    return WorldScene(A.default_world_settings(), shapes, bodies, colliders, f"hulls {n}",
+                      convex_meshes=[(verts, faces, (0.6, 0.6, 0.6)), (verts, faces, (0.7, 0.45, 0.55))])
+
+
+def world_rays(n, lo, hi, seed=0, down=0.5, max_fraction=1.0, masks=(0xFFFF,)):
+    """n rays (A.RAY_DTYPE) for a scene inside the box [lo, hi]: a `down`
+    share cast from above the box straight through it with a small random
+    tilt, the others between two uniform points of the box grown by a tenth
+    of its size; ray k takes category mask masks[k % len(masks)]."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.asarray(lo, np.float64), np.asarray(hi, np.float64)
+    size = hi - lo
+    r = A.rays(n)
+    nd = int(n * down)
+    p = rng.uniform(lo, hi, size=(nd, 3))
+    top = np.array([0.0, hi[1] + 0.5 * size[1] + 1.0, 0.0])
+    a = p.copy()
+    a[:, 1] = top[1]
+    b = p + rng.uniform(-0.05, 0.05, size=(nd, 3)) * size
+    b[:, 1] = lo[1] - 0.5 * size[1] - 1.0
+    grow = 0.1 * size
+    a2 = rng.uniform(lo - grow, hi + grow, size=(n - nd, 3))
+    b2 = rng.uniform(lo - grow, hi + grow, size=(n - nd, 3))
+    r["point1"] = np.concatenate([a, a2]).astype(np.float32)
+    r["point2"] = np.concatenate([b, b2]).astype(np.float32)
+    r["max_fraction"] = np.float32(max_fraction)
+    r["category_mask"] = np.asarray(masks, np.uint32)[np.arange(n) % len(masks)]
+    return r
 
 
 def mixed_world(nx=5, ny=4, nz=5, seed=2, spacing=1.6, variety=True):
@@ -302,7 +377,8 @@ def merge_shapes(scenes_):
     for s in scenes_:
         c = s.colliders.copy()
         c["shape"] += base
-        out.append(WorldScene(s.settings, s.shapes, s.bodies, c, s.name, getattr(s, "joints", None)))
+        out.append(WorldScene(s.settings, s.shapes, s.bodies, c, s.name, getattr(s, "joints", None),
+                              getattr(s, "heightfields", None), getattr(s, "convex_meshes", None)))
         tables.append(s.shapes)
         base += len(s.shapes)
     return np.concatenate(tables), out

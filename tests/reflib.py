@@ -281,6 +281,8 @@ class RefScene:
         L.ref_world_step.argtypes = [C.c_int, C.c_float, C.c_int]
         L.ref_scene_add_joints.argtypes = [C.c_int, P, C.c_uint32]
         L.ref_scene_set_motor_speed.argtypes = [C.c_int, C.c_uint32, C.c_float]
+        L.ref_scene_raycast.argtypes = [C.c_int, P, C.c_uint32, C.c_int, C.c_uint32, P, P]
+        L.ref_convex_register.argtypes = [P, C.c_uint32, P, P, C.c_uint32, C.c_float, C.c_float, C.c_float]
         L.ref_heightfield_register.argtypes = [C.c_uint32, C.c_uint32, P, C.c_float, C.c_float, C.c_float]
         # height fields of the scene registered with the harness; the shape
         # table's mesh field then names the harness's ids
@@ -291,6 +293,15 @@ class RefScene:
             hf_ids.append(L.ref_heightfield_register(h.shape[1], h.shape[0], h.ctypes.data, *map(float, scale)))
         for i in np.nonzero(shapes["kind"] == A.SHAPE_HEIGHTFIELD)[0]:
             shapes["mesh"][i] = hf_ids[int(shapes["mesh"][i])]
+        cm_ids = []
+        for v, faces, scale in getattr(scene, "convex_meshes", None) or []:
+            v = np.ascontiguousarray(v, dtype=np.float32)
+            idx = np.ascontiguousarray(np.concatenate([np.asarray(f, np.uint32) for f in faces]), dtype=np.uint32)
+            sizes = np.array([len(f) for f in faces], dtype=np.uint32)
+            cm_ids.append(L.ref_convex_register(v.ctypes.data, len(v), idx.ctypes.data, sizes.ctypes.data,
+                                                len(faces), *map(float, scale)))
+        for i in np.nonzero(shapes["kind"] == A.SHAPE_CONVEX_MESH)[0]:
+            shapes["mesh"][i] = cm_ids[int(shapes["mesh"][i])]
         self._keep = (np.ascontiguousarray(scene.settings).copy(), np.ascontiguousarray(shapes),
                       np.ascontiguousarray(scene.bodies), np.ascontiguousarray(scene.colliders))
         st, sh, bd, cd = self._keep
@@ -305,6 +316,15 @@ class RefScene:
 
     def update(self, dt=1.0 / 60.0, n=1):
         self.lib.ref_world_step(self.id, dt, n)
+
+    def raycast(self, rays, mode=A.RAYCAST_CLOSEST, max_hits=1):
+        r = np.ascontiguousarray(rays, dtype=A.RAY_DTYPE)
+        n = len(r)
+        hits = np.zeros((n, max_hits), A.RAYCAST_HIT_DTYPE)
+        counts = np.zeros(n, np.uint32)
+        assert self.lib.ref_scene_raycast(self.id, r.ctypes.data, n, int(mode), int(max_hits), hits.ctypes.data,
+                                          counts.ctypes.data) == 0
+        return hits, counts
 
     def set_motor_speed(self, joint, speed):
         assert self.lib.ref_scene_set_motor_speed(self.id, int(joint), float(speed)) == 0

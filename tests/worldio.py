@@ -20,6 +20,8 @@ WORLD_CASES = {
                      dict(n_bodies=40, cols=18, rows=21, cell=1.25, y_scale=0.7, seed=12,
                           terrain_position=(0.5, -0.3, 0.25),
                           terrain_orientation=(0.0499792, 0.0, 0.0299875, 0.9983002)), 200, 50),
+    # convex hulls (two scales) with boxes, spheres and capsules
+    "hulls75": (scenes.hull_world, dict(nx=5, ny=3, nz=5, seed=9), 240, 60),
     # the testbed's joints scene: ball-and-socket chain, motorised slider
     # with limits, motorised hinge, fixed joints; slider speeds set every step
     "mechanisms4": (scenes.mechanism_world, dict(n_mechanisms=4, seed=31), 240, 60),
