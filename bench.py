@@ -590,6 +590,8 @@ def terrain_section(ctx, args, with_cpu):
     sec_early = time.perf_counter() - t0
     ours21 = w.bodies()
     st21 = w.stats()
+    rays = scenes.terrain_rays(sc, args.rays)
+    ray_out, ray_hits = raycast_measure(ctx, w, rays)
     w.update(dt, 39)
     launches0 = ctx.kernel_launches()
     t0 = time.perf_counter()
@@ -619,7 +621,49 @@ def terrain_section(ctx, args, with_cpu):
                                "sample": "the same world, steps 2-21, PhysicsWorld::update of the reference float "
                                          "build (single-threaded engine); compare early_steps_2_21"}
         out["bit_identical_to_reference_at_step_21"] = all(np.array_equal(a, b) for a, b in zip(ours21, r.bodies()))
+        # the reference's PhysicsWorld::raycast on a sample of the same rays,
+        # same state (step 21); its hits compared with the GPU's bit for bit
+        ns = min(len(rays), args.ray_sample)
+        t0 = time.perf_counter()
+        rh, rc = r.raycast(rays[:ns], A.RAYCAST_CLOSEST, 1)
+        rsec = time.perf_counter() - t0
+        gh, gc = ray_hits
+        ray_out["cpu_baseline"] = {"value": round(ns / rsec, 1), "unit": "rays/s", "cores": 1, "kind": "reference",
+                                   "sample": f"the first {ns:,} rays, PhysicsWorld::raycast with a closest-hit "
+                                             "callback, reference float build, one host core"}
+        k = gc[:ns] > 0
+        ray_out["bit_identical_to_reference_sample"] = bool(np.array_equal(gc[:ns], rc) and
+                                                            gh[:ns][k].tobytes() == rh[k].tobytes())
+    out["raycast_at_step_21"] = ray_out
     return out
+
+
+def raycast_measure(ctx, w, rays, reps=5):
+    """rp3dg_world_raycast_device on device-resident rays (kernel time by CUDA
+    events, after a first call that also builds the tree tables) and
+    rp3dg_world_raycast on host arrays (wall clock, copies included)."""
+    import torch
+    dev = torch.device("cuda", 0)
+    n = len(rays)
+    d_rays = torch.from_numpy(rays.view(np.uint8)).to(dev)
+    d_hits = torch.empty(n * A.RAYCAST_HIT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    d_cnt = torch.empty(n, dtype=torch.int32, device=dev)
+    t0 = time.perf_counter()
+    w.raycast_device(d_rays.data_ptr(), n, d_hits.data_ptr(), d_cnt.data_ptr())
+    first = time.perf_counter() - t0
+    ms = [w.raycast_device(d_rays.data_ptr(), n, d_hits.data_ptr(), d_cnt.data_ptr()) for _ in range(reps)]
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        hits, counts = w.raycast(rays, A.RAYCAST_CLOSEST, 1)
+    e2e = (time.perf_counter() - t0) / reps
+    kms = float(np.median(ms))
+    out = {"rays": n, "mode": "closest hit", "rays_per_s": round(n / (kms * 1e-3), 1), "kernel_ms": round(kms, 3),
+           "first_call_ms": round(1e3 * first, 3),
+           "e2e": {"rays_per_s": round(n / e2e, 1), "ms": round(1e3 * e2e, 3),
+                   "h2d_bytes": int(rays.nbytes), "d2h_bytes": int(hits.nbytes + counts.nbytes)},
+           "hit_rays": int((counts > 0).sum()),
+           "api": "rp3dg_world_raycast_device / rp3dg_world_raycast"}
+    return out, (hits[:, 0], counts)
 
 
 def broadphase_section(ctx, args, dev):
@@ -894,6 +938,8 @@ def main():
     ap.add_argument("--no-worlds", action="store_true")
     ap.add_argument("--no-terrain", action="store_true")
     ap.add_argument("--terrain-bodies", type=int, default=100000)
+    ap.add_argument("--rays", type=int, default=1 << 20)
+    ap.add_argument("--ray-sample", type=int, default=20000)
     ap.add_argument("--n-worlds", type=int, default=4096)
     ap.add_argument("--world-steps", type=int, default=300)
     ap.add_argument("--learned-epochs", type=int, default=4)

@@ -2,6 +2,7 @@
 
     python -m reactphysics3d_b200.run_world terrain --bodies 100000 --cols 257 --steps 156
     python -m reactphysics3d_b200.run_world pile --steps 300 --phases
+    python -m reactphysics3d_b200.run_world terrain --bodies 20000 --steps 21 --rays 1048576
 
 Scenes: `pile` (scenes.box_pile), `mixed` (scenes.mixed_world), `terrain`
 (scenes.heightfield_world: --bodies bodies over a --cols x --cols height
@@ -9,7 +10,10 @@ field), `ragdolls` (scenes.ragdoll_world).  The world is created, stepped
 --steps times at --dt and synchronised; nothing else is launched, so kernel
 launch counts (for a profiler's skip / count options) follow from the step
 count.  --phases prints the per-phase host / device times per step
-(rp3dg_world_set_profiling) of the last --phase-steps steps.
+(rp3dg_world_set_profiling) of the last --phase-steps steps.  --rays casts
+that many rays (scenes.terrain_rays for a terrain, closest hit) --ray-reps
+times through rp3dg_world_raycast after the steps (one raycast kernel launch
+each).
 """
 import argparse
 import json
@@ -41,6 +45,8 @@ def main():
     ap.add_argument("--threads", type=int, default=None)
     ap.add_argument("--phases", action="store_true")
     ap.add_argument("--phase-steps", type=int, default=5)
+    ap.add_argument("--rays", type=int, default=0)
+    ap.add_argument("--ray-reps", type=int, default=1)
     args = ap.parse_args()
     sc = make_scene(args)
     ctx = engine.Context(0)
@@ -56,6 +62,15 @@ def main():
         w.set_profiling(True)
         w.update(args.dt, args.steps - n_plain)
         out["phase_ms_per_step"] = {k: round(v / (args.steps - n_plain), 3) for k, v in w.phase_times().items()}
+    if args.rays:
+        if not sc.heightfields:
+            raise SystemExit("--rays needs the terrain scene")
+        rays = scenes.terrain_rays(sc, args.rays)
+        t0 = time.perf_counter()
+        for _ in range(args.ray_reps):
+            hits, counts = w.raycast(rays)
+        out["raycast"] = {"rays": args.rays, "reps": args.ray_reps, "hit_rays": int((counts > 0).sum()),
+                          "ms_per_call": round(1e3 * (time.perf_counter() - t0) / args.ray_reps, 3)}
     print(json.dumps(out))
     w.close()
     ctx.close()

@@ -300,6 +300,29 @@ def world_rays(n, lo, hi, seed=0, down=0.5, max_fraction=1.0, masks=(0xFFFF,)):
     return r
 
 
+def terrain_rays(sc, n, seed=41):
+    """Rays over the large world: half cast from 5 m above the highest body
+    straight down (a random tilt of up to 2% of the footprint), half between
+    two uniform points of the world's box (which walk the height field's
+    grid when they reach the terrain)."""
+    p = sc.bodies["position"][1:]
+    half = 0.5 * (np.array(sc.heightfields[0][0].shape[::-1]) - 1)   # (x, z) half-extents of the field
+    lo = np.array([-half[0], -4.0, -half[1]])
+    hi = np.array([half[0], float(p[:, 1].max()) + 5.0, half[1]])
+    rng = np.random.default_rng(seed)
+    r = A.rays(n)
+    nd = n // 2
+    a = rng.uniform(lo, hi, size=(nd, 3))
+    a[:, 1] = hi[1]
+    b = a + rng.uniform(-0.02, 0.02, size=(nd, 3)) * (hi - lo)
+    b[:, 1] = lo[1]
+    a2 = rng.uniform(lo, hi, size=(n - nd, 3))
+    b2 = rng.uniform(lo, hi, size=(n - nd, 3))
+    r["point1"] = np.concatenate([a, a2]).astype(np.float32)
+    r["point2"] = np.concatenate([b, b2]).astype(np.float32)
+    return r
+
+
 def mixed_world(nx=5, ny=4, nz=5, seed=2, spacing=1.6, variety=True):
     """Boxes, spheres and capsules of random sizes on a jittered grid above a
     static ground; with `variety`, random frictions and bounciness, dampings,
