@@ -599,6 +599,33 @@ int rp3dg_world_get_contacts(rp3dg_world* world, int32_t* body1, int32_t* body2,
                              uint32_t capacity_points, uint32_t* nb_manifolds, uint32_t* nb_contact_points);
 int rp3dg_world_get_stats(rp3dg_world* world, rp3dg_world_stats* stats);
 
+/* The contact events of the last update, as EventListener::onContact
+ * receives them (CollisionDetectionSystem::reportContacts,
+ * CollisionDetectionSystem.cpp:1729-1738, and CollisionCallback::CallbackData,
+ * CollisionCallback.cpp:79-134): the update's contact pairs in their creation
+ * order, then the lost contact pairs (pairs that touched in the previous
+ * frame and were removed by the broad phase or no longer touch).  Each event
+ * has ContactPair::getEventType's type and, for a contact pair of an island,
+ * its contact points (world normal and penetration depth, local points on
+ * the two colliders; a pair outside the islands and a lost pair have none),
+ * copied into the points arrays from `first_point`. */
+#define RP3DG_CONTACT_START 0
+#define RP3DG_CONTACT_STAY 1
+#define RP3DG_CONTACT_EXIT 2
+typedef struct rp3dg_contact_event {
+    int32_t body1, body2;          /* creation indices */
+    int32_t collider1, collider2;  /* creation indices */
+    int32_t type;                  /* RP3DG_CONTACT_* */
+    uint32_t first_point;          /* index of its first point in the points arrays */
+    uint32_t nb_points;            /* ContactPair::getNbContactPoints */
+} rp3dg_contact_event;
+/* Host arrays with room for `capacity` events and `capacity_points` points
+ * (float4 rows: normal + depth, local point 1, local point 2; any may be
+ * NULL); the counts are written even when the arrays are short. */
+int rp3dg_world_get_contact_events(rp3dg_world* world, uint32_t world_index, rp3dg_contact_event* events,
+                                   uint32_t capacity, float* normal_depth, float* local1, float* local2,
+                                   uint32_t capacity_points, uint32_t* nb_events, uint32_t* nb_points);
+
 /* PhysicsWorld::raycast(ray, callback, raycastWithCategoryMaskBits)
  * (PhysicsWorld.h:486-490) for a batch of rays, each traced as the reference
  * traces one: DynamicAABBTree::raycast (DynamicAABBTree.cpp:684-747) over the

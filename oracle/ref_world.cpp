@@ -55,12 +55,52 @@ struct Capture {
     }
 };
 
+// The contact events of the last update (EventListener::onContact), in the
+// rp3dg_contact_event layout: body and collider creation indices, event type,
+// first point and point count, and the points (normal + depth, local points).
+struct EventRecorder : public EventListener {
+    const std::vector<RigidBody*>* bodies = nullptr;
+    const std::vector<Collider*>* colliders = nullptr;
+    std::vector<rp3dg_contact_event> events;
+    std::vector<float> nd, l1, l2;
+    void clear() { events.clear(); nd.clear(); l1.clear(); l2.clear(); }
+    void onContact(const CollisionCallback::CallbackData& data) override {
+        std::unordered_map<const void*, int32_t> bi, ci;
+        for (size_t i = 0; i < bodies->size(); i++) bi[static_cast<const void*>(static_cast<Body*>((*bodies)[i]))] = int32_t(i);
+        for (size_t i = 0; i < colliders->size(); i++) ci[static_cast<const void*>((*colliders)[i])] = int32_t(i);
+        for (uint32 k = 0; k < data.getNbContactPairs(); k++) {
+            const CollisionCallback::ContactPair pair = data.getContactPair(k);
+            rp3dg_contact_event ev{};
+            ev.body1 = bi.at(static_cast<const void*>(pair.getBody1()));
+            ev.body2 = bi.at(static_cast<const void*>(pair.getBody2()));
+            ev.collider1 = ci.at(static_cast<const void*>(pair.getCollider1()));
+            ev.collider2 = ci.at(static_cast<const void*>(pair.getCollider2()));
+            const auto t = pair.getEventType();
+            ev.type = t == CollisionCallback::ContactPair::EventType::ContactStart ? 0
+                    : (t == CollisionCallback::ContactPair::EventType::ContactStay ? 1 : 2);
+            ev.first_point = uint32_t(nd.size() / 4);
+            ev.nb_points = pair.getNbContactPoints();
+            for (uint32 c = 0; c < pair.getNbContactPoints(); c++) {
+                const CollisionCallback::ContactPoint cp = pair.getContactPoint(c);
+                const Vector3 n = cp.getWorldNormal(), a = cp.getLocalPointOnCollider1(), b = cp.getLocalPointOnCollider2();
+                const float v[12] = {float(n.x), float(n.y), float(n.z), float(cp.getPenetrationDepth()),
+                                     float(a.x), float(a.y), float(a.z), 0.0f, float(b.x), float(b.y), float(b.z), 0.0f};
+                nd.insert(nd.end(), v, v + 4);
+                l1.insert(l1.end(), v + 4, v + 8);
+                l2.insert(l2.end(), v + 8, v + 12);
+            }
+            events.push_back(ev);
+        }
+    }
+};
+
 struct World {
     PhysicsCommon common;
     PhysicsWorld* world = nullptr;
     std::vector<RigidBody*> bodies;
     std::vector<Joint*> joints;  // in creation order
     std::vector<Collider*> colliders;  // in creation order
+    EventRecorder recorder;
     Capture cap;
 };
 
@@ -403,7 +443,25 @@ int ref_world_apply_forces(int id, uint64_t seed) {
 
 int ref_world_step(int id, float dt, int nsteps) {
     World& W = *worlds().at(size_t(id));
-    for (int i = 0; i < nsteps; i++) W.world->update(decimal(dt));
+    for (int i = 0; i < nsteps; i++) {
+        W.recorder.clear();
+        W.world->update(decimal(dt));
+    }
+    return 0;
+}
+
+// The contact events of the last update (counts always written).
+int ref_scene_events(int id, rp3dg_contact_event* events, uint32_t cap, float* nd, float* l1, float* l2,
+                     uint32_t cap_points, uint32_t* nb_events, uint32_t* nb_points) {
+    World& W = *worlds().at(size_t(id));
+    const EventRecorder& R = W.recorder;
+    *nb_events = uint32_t(R.events.size());
+    *nb_points = uint32_t(R.nd.size() / 4);
+    for (size_t k = 0; k < R.events.size() && k < cap; k++) events[k] = R.events[k];
+    const size_t np = std::min<size_t>(R.nd.size() / 4, cap_points);
+    if (nd) std::memcpy(nd, R.nd.data(), np * 16);
+    if (l1) std::memcpy(l1, R.l1.data(), np * 16);
+    if (l2) std::memcpy(l2, R.l2.data(), np * 16);
     return 0;
 }
 
@@ -562,6 +620,9 @@ int ref_scene_create(const rp3dg_world_settings* s, const rp3dg_shape* shapes, u
     ws.cosAngleSimilarContactManifold = s->cos_angle_similar_contact_manifold;
     ws.defaultPositionSolverNbIterations = uint16(s->position_iterations);
     W->world = W->common.createPhysicsWorld(ws);
+    W->recorder.bodies = &W->bodies;
+    W->recorder.colliders = &W->colliders;
+    W->world->setEventListener(&W->recorder);
     std::vector<CollisionShape*> cs(nshapes, nullptr);
     for (uint32_t i = 0; i < nshapes; i++) {
         const rp3dg_shape& sh = shapes[i];

@@ -137,6 +137,10 @@ JOINT_DESC_DTYPE = np.dtype([
     ("limit_enabled", "<i4"), ("min_angle", "<f4"), ("max_angle", "<f4"),
     ("motor_enabled", "<i4"), ("motor_speed", "<f4"), ("max_motor_torque", "<f4")])
 assert JOINT_DESC_DTYPE.itemsize == 72
+CONTACT_START, CONTACT_STAY, CONTACT_EXIT = 0, 1, 2
+CONTACT_EVENT_DTYPE = np.dtype([("body1", "<i4"), ("body2", "<i4"), ("collider1", "<i4"), ("collider2", "<i4"),
+                                ("type", "<i4"), ("first_point", "<u4"), ("nb_points", "<u4")])
+assert CONTACT_EVENT_DTYPE.itemsize == 28
 RAYCAST_CLOSEST, RAYCAST_ANY, RAYCAST_ALL = 0, 1, 2
 RAY_DTYPE = np.dtype([("point1", "<f4", (3,)), ("point2", "<f4", (3,)), ("max_fraction", "<f4"),
                       ("category_mask", "<u4")])

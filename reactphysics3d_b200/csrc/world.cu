@@ -476,6 +476,7 @@ struct ContactPairH {
     uint32_t npts = 0;   // points per manifold, one byte each
     uint32_t k;          // points of all its manifolds after the manifold step
     bool in_island = false;
+    bool prev = false;   // ContactPair::collidingInPreviousFrame (the overlapping pair's, at creation)
     uint32_t manifold = 0, point = 0;  // global indices in the packed arrays
 };
 struct IslandH {
@@ -626,6 +627,7 @@ struct WorldH {
     std::vector<int32_t> reset_slots;
     // contacts of this step and of the previous one
     std::vector<ContactPairH> cpairs, prev_cpairs;
+    std::vector<ContactPairH> lost;            // this step's lost contact pairs (mLostContactPairs)
     FlatMap prev_map;
     std::vector<uint32_t> island_order;  // mProcessContactPairsOrderIslands
     std::vector<IslandH> islands;
@@ -897,6 +899,19 @@ void add_pair(Group* g, WorldH& w, int c1, int c2) {
     w.colliders[size_t(c2)].pairs.push_back(p.id);
 }
 
+// CollisionDetectionSystem::addLostContactPair (CollisionDetectionSystem.cpp:220-236)
+void add_lost(WorldH& w, const PairH& p) {
+    ContactPairH c;
+    c.id = p.id;
+    c.c1 = p.c1;
+    c.c2 = p.c2;
+    c.b1 = w.colliders[size_t(p.c1)].body;
+    c.b2 = w.colliders[size_t(p.c2)].body;
+    c.prev = true;
+    c.k = 0;
+    w.lost.push_back(c);
+}
+
 // removeConvexPairWithIndex(index, removeFromColliders = true)
 void remove_pair(WorldH& w, uint32_t idx) {
     PairH& p = w.pairs[idx];
@@ -1137,13 +1152,16 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
         }
     }
     const auto t1 = g->profiling ? clk::now() : clk::time_point();
-    // removeNonOverlappingPairs
+    // removeNonOverlappingPairs; a pair removed while it was colliding in
+    // the previous frame becomes a lost contact pair (addLostContactPair)
+    w.lost.clear();
     for (uint64_t i = 0; i < w.pairs.size(); i++) {
         PairH& p = w.pairs[i];
         if (!p.need_test) continue;
         if (rp3dg::order::overlap(w.tree.nodes[size_t(p.bp1)].box, w.tree.nodes[size_t(p.bp2)].box)) {
             p.need_test = false;
         } else {
+            if (p.coll_prev) add_lost(w, p);
             remove_pair(w, uint32_t(i));
             i--;
         }
@@ -1154,6 +1172,7 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
         if (rp3dg::order::overlap(w.tree.nodes[size_t(p.bp1)].box, w.tree.nodes[size_t(p.bp2)].box)) {
             p.need_test = false;
         } else {
+            if (p.coll_prev) add_lost(w, p);
             remove_concave_pair(w, uint32_t(i));
             i--;
         }
@@ -1215,6 +1234,7 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
             PairH& p = w.pairs[w.item_pair[a][i]];
             p.coll_curr = true;
             ContactPairH c;
+            c.prev = p.coll_prev;
             c.id = p.id;
             c.c1 = p.c1;
             c.c2 = p.c2;
@@ -1232,6 +1252,7 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
             PairH& p = w.concave[w.hitem_pair[a][i]];
             p.coll_curr = true;
             ContactPairH c;
+            c.prev = p.coll_prev;
             c.id = p.id;
             c.c1 = p.c1;
             c.c2 = p.c2;
@@ -1249,6 +1270,12 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
             w.cpairs.push_back(c);
         }
     }
+    // computeLostContactPairs (CollisionDetectionSystem.cpp:978-1011): pairs
+    // colliding in the previous frame and not in this one, convex then concave
+    for (const PairH& p : w.pairs)
+        if (p.coll_prev && !p.coll_curr) add_lost(w, p);
+    for (const PairH& p : w.concave)
+        if (p.coll_prev && !p.coll_curr) add_lost(w, p);
     for (uint32_t p = 0; p < w.cpairs.size(); p++) {
         w.bodies[size_t(w.cpairs[p].b1)].contact_pairs.push_back(p);
         w.bodies[size_t(w.cpairs[p].b2)].contact_pairs.push_back(p);
@@ -3030,6 +3057,59 @@ int rp3dg_world_group_get_contacts(rp3dg_world* g, uint32_t world, int32_t* body
     }
     cudaError_t e = cudaStreamSynchronize(g->stream);
     return e == cudaSuccess ? 0 : wcuda(g, e, "read contacts");
+}
+
+int rp3dg_world_get_contact_events(rp3dg_world* g, uint32_t world, rp3dg_contact_event* events, uint32_t capacity,
+                                   float* normal_depth, float* local1, float* local2, uint32_t capacity_points,
+                                   uint32_t* nb_events, uint32_t* nb_points) {
+    if (!g || world >= g->worlds.size() || (capacity && !events)) return RP3DG_EINVAL;
+    const ContactBuf& B = g->cbuf[1 - g->cur_cb];
+    const WorldH& w = g->worlds[world];
+    const std::vector<ContactPairH>& cps = w.prev_cpairs;
+    const uint32_t ne = uint32_t(cps.size() + w.lost.size());
+    uint32_t np = 0;
+    for (const ContactPairH& c : cps)
+        if (c.in_island) np += c.k;
+    if (nb_events) *nb_events = ne;
+    if (nb_points) *nb_points = np;
+    // the step's packed points of this world, then gathered pair by pair
+    std::vector<float4> nd, l1, l2;
+    const bool want = capacity_points && (normal_depth || local1 || local2) && w.np;
+    if (want) {
+        nd.resize(w.np);
+        l1.resize(w.np);
+        l2.resize(w.np);
+        cudaMemcpyAsync(nd.data(), B.nd + w.pt_base, size_t(w.np) * 16, cudaMemcpyDeviceToHost, g->stream);
+        cudaMemcpyAsync(l1.data(), B.l1 + w.pt_base, size_t(w.np) * 16, cudaMemcpyDeviceToHost, g->stream);
+        cudaMemcpyAsync(l2.data(), B.l2 + w.pt_base, size_t(w.np) * 16, cudaMemcpyDeviceToHost, g->stream);
+        cudaError_t e = cudaStreamSynchronize(g->stream);
+        if (e != cudaSuccess) return wcuda(g, e, "read contact events");
+    }
+    uint32_t k = 0, pt = 0;
+    auto emit = [&](const ContactPairH& c, int type, bool points) {
+        const uint32_t n = points ? c.k : 0u;
+        if (k < capacity) {
+            rp3dg_contact_event& ev = events[k];
+            ev.body1 = c.b1;
+            ev.body2 = c.b2;
+            ev.collider1 = c.c1;
+            ev.collider2 = c.c2;
+            ev.type = type;
+            ev.first_point = pt;
+            ev.nb_points = n;
+        }
+        for (uint32_t i = 0; i < n; i++, pt++) {
+            if (!want || pt >= capacity_points) continue;
+            const uint32_t src = c.point - w.pt_base + i;
+            if (normal_depth) std::memcpy(normal_depth + 4 * size_t(pt), &nd[src], 16);
+            if (local1) std::memcpy(local1 + 4 * size_t(pt), &l1[src], 16);
+            if (local2) std::memcpy(local2 + 4 * size_t(pt), &l2[src], 16);
+        }
+        k++;
+    };
+    for (const ContactPairH& c : cps) emit(c, c.prev ? RP3DG_CONTACT_STAY : RP3DG_CONTACT_START, c.in_island);
+    for (const ContactPairH& c : w.lost) emit(c, RP3DG_CONTACT_EXIT, false);
+    return 0;
 }
 
 int rp3dg_world_get_contacts(rp3dg_world* w, int32_t* body1, int32_t* body2, uint8_t* nb_points, uint32_t capacity,

@@ -101,6 +101,8 @@ def load_library(path=LIB_PATH):
     L.rp3dg_world_add_joints.argtypes = [P, P, C.c_uint32]
     L.rp3dg_world_group_add_joints.argtypes = [P, C.c_uint32, P, C.c_uint32]
     L.rp3dg_world_set_motor_speed.argtypes = [P, C.c_uint32, C.c_uint32, C.c_float]
+    L.rp3dg_world_get_contact_events.argtypes = [P, C.c_uint32, P, C.c_uint32, P, P, P, C.c_uint32,
+                                                 C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.rp3dg_world_raycast.argtypes = [P, C.c_uint32, P, C.c_uint32, C.c_int32, C.c_uint32, P, P]
     L.rp3dg_world_raycast_device.argtypes = [P, C.c_uint32, P, C.c_uint32, C.c_int32, C.c_uint32, P, P,
                                              C.POINTER(C.c_float)]
@@ -509,6 +511,24 @@ class World:
             rc = self.lib.rp3dg_world_group_add_joints(self.h, int(world), j.ctypes.data, len(j))
         if rc != 0:
             raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+
+    def contact_events(self, world=0):
+        """EventListener::onContact of the last update: (events
+        A.CONTACT_EVENT_DTYPE, normal + depth (n, 4), local points 1, local
+        points 2)."""
+        ne, npt = C.c_uint32(), C.c_uint32()
+        rc = self.lib.rp3dg_world_get_contact_events(self.h, int(world), None, 0, None, None, None, 0,
+                                                     C.byref(ne), C.byref(npt))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+        ev = np.zeros(ne.value, A.CONTACT_EVENT_DTYPE)
+        nd, l1, l2 = (np.zeros((npt.value, 4), np.float32) for _ in range(3))
+        rc = self.lib.rp3dg_world_get_contact_events(self.h, int(world), ev.ctypes.data, len(ev), nd.ctypes.data,
+                                                     l1.ctypes.data, l2.ctypes.data, len(nd), C.byref(ne),
+                                                     C.byref(npt))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+        return ev, nd, l1, l2
 
     def raycast(self, rays, mode=A.RAYCAST_CLOSEST, max_hits=1, world=0):
         """PhysicsWorld::raycast for each row of `rays` (A.RAY_DTYPE) with the

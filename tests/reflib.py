@@ -282,6 +282,7 @@ class RefScene:
         L.ref_scene_add_joints.argtypes = [C.c_int, P, C.c_uint32]
         L.ref_scene_set_motor_speed.argtypes = [C.c_int, C.c_uint32, C.c_float]
         L.ref_scene_raycast.argtypes = [C.c_int, P, C.c_uint32, C.c_int, C.c_uint32, P, P]
+        L.ref_scene_events.argtypes = [C.c_int, P, C.c_uint32, P, P, P, C.c_uint32, P, P]
         L.ref_convex_register.argtypes = [P, C.c_uint32, P, P, C.c_uint32, C.c_float, C.c_float, C.c_float]
         L.ref_heightfield_register.argtypes = [C.c_uint32, C.c_uint32, P, C.c_float, C.c_float, C.c_float]
         # height fields of the scene registered with the harness; the shape
@@ -316,6 +317,15 @@ class RefScene:
 
     def update(self, dt=1.0 / 60.0, n=1):
         self.lib.ref_world_step(self.id, dt, n)
+
+    def contact_events(self):
+        ne, npt = C.c_uint32(), C.c_uint32()
+        self.lib.ref_scene_events(self.id, None, 0, None, None, None, 0, C.byref(ne), C.byref(npt))
+        ev = np.zeros(ne.value, A.CONTACT_EVENT_DTYPE)
+        nd, l1, l2 = (np.zeros((npt.value, 4), np.float32) for _ in range(3))
+        self.lib.ref_scene_events(self.id, ev.ctypes.data, len(ev), nd.ctypes.data, l1.ctypes.data, l2.ctypes.data,
+                                  len(nd), C.byref(ne), C.byref(npt))
+        return ev, nd, l1, l2
 
     def raycast(self, rays, mode=A.RAYCAST_CLOSEST, max_hits=1):
         r = np.ascontiguousarray(rays, dtype=A.RAY_DTYPE)

@@ -344,3 +344,37 @@ def test_motor_speed_rejects_bad_joints(ctx):
     w.set_motor_speed(7, -1.0)           # the hinge
     w.update(float(worldio.DT))
     w.close()
+
+
+@pytest.mark.skipif(not reflib.have_ref("f32"), reason="reference engine not built")
+@pytest.mark.parametrize("name,make,steps", [
+    ("mixed", lambda: scenes.mixed_world(5, 4, 5, seed=5), 300),
+    ("hulls", lambda: scenes.hull_world(4, 3, 4, seed=44), 200),
+    ("terrain", lambda: scenes.heightfield_world(n_bodies=80, cols=20, rows=20, seed=45), 200),
+    ("mechanisms", lambda: scenes.mechanism_world(4, seed=46), 200),
+])
+def test_contact_events_match_reference(ctx, name, make, steps):
+    """EventListener::onContact after every update: the contact pairs in
+    creation order with ContactStart / ContactStay, then the lost pairs with
+    ContactExit (removed by the broad phase or no longer touching), and each
+    pair's contact points, bit-identical to the reference; every kind of
+    event occurs (in the mechanisms, whose joined bodies do not collide,
+    contacts are rare)."""
+    sc = make()
+    w, r = engine.World(ctx, sc), reflib.RefScene(sc)
+    seen = np.zeros(3, np.int64)
+    for s in range(steps):
+        if name == "mechanisms":
+            for j, v in scenes.mechanism_motor_speeds(4, s, worldio.DT):
+                w.set_motor_speed(j, v)
+                r.set_motor_speed(j, v)
+        w.update(float(worldio.DT))
+        r.update(float(worldio.DT))
+        got, exp = w.contact_events(), r.contact_events()
+        assert got[0].tobytes() == exp[0].tobytes(), (s, len(got[0]), len(exp[0]))
+        for a, b in zip(got[1:], exp[1:]):
+            assert np.array_equal(a, b), s
+        seen += np.bincount(got[0]["type"], minlength=3)[:3]
+    # joint-connected bodies do not collide: the mechanisms touch rarely
+    assert (seen > 0).all() if name != "mechanisms" else seen.sum() > 0, seen
+    w.close()
