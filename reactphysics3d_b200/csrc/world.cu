@@ -481,7 +481,7 @@ struct ContactPairH {
 };
 struct IslandH {
     uint32_t manifold_start = 0, manifold_count = 0;  // world-local manifold range
-    std::vector<int> bodies;
+    uint32_t body_start = 0, body_count = 0;          // its bodies: WorldH::isl_bodies[start, start + count)
 };
 
 inline float __int_as_float_host(int v) {
@@ -628,6 +628,8 @@ struct WorldH {
     // contacts of this step and of the previous one
     std::vector<ContactPairH> cpairs, prev_cpairs;
     std::vector<ContactPairH> lost;            // this step's lost contact pairs (mLostContactPairs)
+    std::vector<int> isl_bodies;               // the islands' bodies, island after island
+    std::vector<float4> sleep_lv, sleep_av;    // the sleep test's velocities by body id (reused)
     FlatMap prev_map;
     std::vector<uint32_t> island_order;  // mProcessContactPairsOrderIslands
     std::vector<IslandH> islands;
@@ -1282,6 +1284,7 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
     }
     w.island_order.clear();
     w.islands.clear();
+    w.isl_bodies.clear();
     for (auto& B : w.bodies) {
         B.in_island = false;
         B.island = -1;
@@ -1298,12 +1301,14 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
         stack.push_back(b0);
         IslandH isl;
         isl.manifold_start = total_manifolds;
+        isl.body_start = uint32_t(w.isl_bodies.size());
         const size_t isl_index = w.islands.size();
         w.islands.push_back(isl);
         while (!stack.empty()) {
             const int b = stack.back();
             stack.pop_back();
-            w.islands[isl_index].bodies.push_back(b);
+            w.isl_bodies.push_back(b);
+            w.islands[isl_index].body_count++;
             set_sleeping(g, w, b, false);
             if (w.bodies[size_t(b)].type == RP3DG_BODY_STATIC) {
                 statics.push_back(b);
@@ -1461,7 +1466,10 @@ void colliders_and_sleep(Group* g, WorldH& w, float dt, const uint8_t* h_moved, 
     w.slept.clear();
     if (g->set.sleeping_enabled) {
         // velocities by body id (rows in the device order before any body falls asleep)
-        std::vector<float4> lv(w.nb), av(w.nb);
+        std::vector<float4>& lv = w.sleep_lv;
+        std::vector<float4>& av = w.sleep_av;
+        lv.resize(w.nb);
+        av.resize(w.nb);
         for (uint32_t s = 0; s < w.nb; s++) {
             lv[size_t(w.dev_body_at[s])] = h_lv[w.b0 + s];
             av[size_t(w.dev_body_at[s])] = h_av[w.b0 + s];
@@ -1470,7 +1478,8 @@ void colliders_and_sleep(Group* g, WorldH& w, float dt, const uint8_t* h_moved, 
         const float sav2 = g->set.sleep_angular_velocity * g->set.sleep_angular_velocity;
         for (const IslandH& isl : w.islands) {
             float min_sleep = 3.40282347e+38f;
-            for (int b : isl.bodies) {
+            for (uint32_t ib = isl.body_start; ib < isl.body_start + isl.body_count; ib++) {
+                const int b = w.isl_bodies[ib];
                 BodyH& B = w.bodies[size_t(b)];
                 if (B.type == RP3DG_BODY_STATIC) continue;
                 const float4 l = lv[size_t(b)], a = av[size_t(b)];
@@ -1484,7 +1493,8 @@ void colliders_and_sleep(Group* g, WorldH& w, float dt, const uint8_t* h_moved, 
                 }
             }
             if (min_sleep >= g->set.time_before_sleep)
-                for (int b : isl.bodies) set_sleeping(g, w, b, true);
+                for (uint32_t ib = isl.body_start; ib < isl.body_start + isl.body_count; ib++)
+                    set_sleeping(g, w, w.isl_bodies[ib], true);
         }
     }
     // collidingInPreviousFrame for the next step
@@ -2412,8 +2422,10 @@ int update_group(Group* g, float dt) {
                 if (!w.isl_jcount[i]) continue;
                 ji_island.push_back(w.isl_base + i);
                 ji_bstart.push_back(uint32_t(ji_rows.size()));
-                for (int b : w.islands[i].bodies)
+                for (uint32_t ib = w.islands[i].body_start; ib < w.islands[i].body_start + w.islands[i].body_count; ib++) {
+                    const int b = w.isl_bodies[ib];
                     if (w.bodies[size_t(b)].type != RP3DG_BODY_STATIC) ji_rows.push_back(int32_t(w.b0) + w.bcomp.slot[size_t(b)]);
+                }
                 ji_bcount.push_back(uint32_t(ji_rows.size()) - ji_bstart.back());
             }
         if (dev_grow(&g->d_jiisl, &g->cap_ji, ji_island.size() + 1) ||
