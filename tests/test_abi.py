@@ -44,3 +44,39 @@ def test_null_arguments_are_rejected(cuda_lib):
     assert L.rp3dg_narrowphase_device(None, 1, None, None, 1) == engine.RP3DG_EINVAL
     assert L.rp3dg_narrowphase_host(None, 1, None, None, 1) == engine.RP3DG_EINVAL
     assert L.rp3dg_set_shapes(None, None, 0) == engine.RP3DG_EINVAL
+
+
+def test_struct_layouts_match_the_python_dtypes(tmp_path):
+    """The public structs as a C compiler lays them out from include/rp3dg.h
+    (sizes and field offsets) are the numpy dtypes the Python side uses."""
+    import shutil
+    import subprocess
+
+    import numpy as np
+
+    from reactphysics3d_b200 import _abi as A
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    structs = {"rp3dg_joint_desc": A.JOINT_DESC_DTYPE, "rp3dg_ray": A.RAY_DTYPE,
+               "rp3dg_raycast_hit": A.RAYCAST_HIT_DTYPE, "rp3dg_contact_event": A.CONTACT_EVENT_DTYPE,
+               "rp3dg_world_settings": A.WORLD_SETTINGS_DTYPE, "rp3dg_body_desc": A.BODY_DESC_DTYPE,
+               "rp3dg_collider_desc": A.COLLIDER_DESC_DTYPE, "rp3dg_world_stats": A.WORLD_STATS_DTYPE}
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{os.path.join(root, "include", "rp3dg.h")}"',
+             "int main(void) {"]
+    for name, dt in structs.items():
+        lines.append(f'    printf("{name} %zu\\n", sizeof({name}));')
+        for f in dt.names:
+            lines.append(f'    printf("{name}.{f} %zu\\n", offsetof({name}, {f}));')
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, str(src), "-o", str(exe)], check=True)
+    got = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                          check=True).stdout.splitlines())
+    for name, dt in structs.items():
+        assert int(got[name]) == dt.itemsize, name
+        for f in dt.names:
+            assert int(got[f"{name}.{f}"]) == dt.fields[f][1], (name, f)
