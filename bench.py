@@ -27,6 +27,7 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+T_START = time.perf_counter()
 
 from reactphysics3d_b200 import _abi as A  # noqa: E402
 from reactphysics3d_b200 import scenes  # noqa: E402
@@ -243,42 +244,52 @@ def run_ours(args):
                "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_s * 1e3, 4),
                "api": "rp3dg_narrowphase_host (pinned host buffers)"}
 
-    manifolds = None
-    if not args.no_manifolds:
-        manifolds = manifold_section(ctx, sc, names, algos, dpairs, douts, args, dev,
-                                     pinned)
+    # ---- the headline's CPU baseline, then the other sections --------------
+    # Every section below is guarded: an exception or the time budget records
+    # {"error": ...} / {"skipped": ...} in its place instead of losing the
+    # headline line.  A section that ends in a collective (many worlds) runs
+    # on every rank; the single-world sections are replicas, run by rank 0.
+    t_bench0 = T_START
+    sections = {}
+    solo = rank == 0
+    cpu_ok = rank == 0 and not args.no_cpu
 
-    dynamics = None
-    if not args.no_dynamics:
-        dynamics = dynamics_section(ctx, args, dev, rank == 0 and world == 1 and not args.no_cpu)
-
-    broadphase = None
-    if not args.no_broadphase:
-        broadphase = broadphase_section(ctx, args, dev)
+    def section(name, enabled, fn, every_rank=False):
+        if not enabled:
+            return None
+        if not (every_rank or solo):
+            return None
+        left = args.budget_s - (time.perf_counter() - t_bench0)
+        if left < 0 and not every_rank:
+            sections[name] = {"skipped": f"time budget of {args.budget_s:.0f} s spent before this section"}
+            return sections[name]
+        t0 = time.perf_counter()
+        try:
+            r = fn()
+        except Exception as e:  # recorded, never fatal for the headline
+            r = {"error": f"{type(e).__name__}: {str(e)[:400]}"}
+        if isinstance(r, dict):
+            r["section_seconds"] = round(time.perf_counter() - t0, 2)
+        sections[name] = r
         ctx.set_shapes(sc.shapes)   # the narrow-phase workload's table again
+        return r
 
-    world_step = None
-    if not args.no_world:
-        world_step = world_section(ctx, args, rank == 0 and world == 1 and not args.no_cpu)
-        ctx.set_shapes(sc.shapes)
-
-    terrain = None
-    if not args.no_terrain:
-        terrain = terrain_section(ctx, args, rank == 0 and world == 1 and not args.no_cpu)
-        ctx.set_shapes(sc.shapes)
-
-    worlds = None
-    if not args.no_worlds:
-        worlds = many_worlds_section(ctx, args, rank == 0 and world == 1 and not args.no_cpu)
-        ctx.set_shapes(sc.shapes)
-
-    learned = None
-    if not args.no_learned:
-        learned = learned_axis_section(ctx, sc, args, dev)
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(sc, args)
+    cpu = section("cpu_baseline", cpu_ok and world == 1, lambda: cpu_baseline(sc, args))
+    sections.pop("cpu_baseline", None)
+    section("fp32_roofline", not args.no_fp32, lambda: fp32_section(ctx, sc, names, algos, dpairs, douts, mean_batch,
+                                                                   args, dev, roofline))
+    section("fp64_error", not args.no_cpu and not args.no_fp64, lambda: fp64_error_section(ctx, sc, names, algos, args, dev))
+    section("manifolds", not args.no_manifolds,
+            lambda: manifold_section(ctx, sc, names, algos, dpairs, douts, args, dev, pinned))
+    section("dynamics", not args.no_dynamics, lambda: dynamics_section(ctx, args, dev, cpu_ok and world == 1))
+    section("broadphase", not args.no_broadphase, lambda: broadphase_section(ctx, args, dev))
+    section("world_step", not args.no_world, lambda: world_section(ctx, args, cpu_ok))
+    section("many_worlds", not args.no_worlds, lambda: many_worlds_section(ctx, args, cpu_ok, rank, world),
+            every_rank=True)
+    section("learned_axis", not args.no_learned, lambda: learned_axis_section(ctx, sc, args, dev))
+    section("many_worlds_1000_steps", not args.no_worlds and world == 1,
+            lambda: worlds_long_section(ctx, args, cpu_ok))
+    section("terrain_world", not args.no_terrain, lambda: terrain_section(ctx, args, cpu_ok))
 
     line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
@@ -286,18 +297,69 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "pairs_per_gpu": sc.n_pairs, "batches": names,
                        "seed": args.seed, "l2": "flushed between steps (256 MB write)",
                        "parallelism": f"independent pair sets per rank x{world}"},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "manifolds": manifolds, "dynamics": dynamics, "broadphase": broadphase,
-            "world_step": world_step, "terrain_world": terrain, "many_worlds": worlds,
-            "learned_axis": learned,
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
             "gpu_launches": int(launches),
             "clocks": clocks, "batch_ms": {k: round(v, 4) for k, v in mean_batch.items()}}
+    line.update(sections)
+    line["bench_seconds"] = round(time.perf_counter() - t_bench0, 1)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    ctx.close()
+    try:
+        ctx.close()
+    except Exception:
+        pass
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+
+
+def fp64_error_section(ctx, sc, names, algos, args, dev):
+    """Error of the GPU's FP32 contacts against the reference's double build
+    (IS_RP3D_DOUBLE_PRECISION_ENABLED, oracle/_ref/librp3d_ref_f64.so) on the
+    first args.fp64_sample pairs of every batch, fresh caches: the share of
+    pairs on the same path (same colliding flag and contact count), then per
+    contact the largest component error of the normal, the depth error and
+    the largest component error of the two local points (metres), median and
+    max.  The same sample through the reference's float build is checked
+    bit for bit against the GPU, so these errors are the reference's own
+    FP32 errors."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import reflib
+    if not (reflib.have_ref("f64") and reflib.have_ref("f32")):
+        return {"skipped": "reference builds (oracle/_ref) absent"}
+    r32, r64 = reflib.RefEngine("f32"), reflib.RefEngine("f64")
+    for e in (r32, r64):
+        m = e.create_convex_mesh(sc.hull_vertices, sc.hull_faces)
+        e.create_convex_mesh_shape(m)
+    threads = _threads()
+    res, identical = {}, True
+    worst = {"normal": 0.0, "depth": 0.0, "point": 0.0}
+    for nm in names:
+        algo, pairs = sc.batches[nm]
+        k = min(pairs.n, args.fp64_sample)
+        ours = ctx.narrowphase_host(algo, pairs.slice(0, k))
+        f32, _ = r32.narrowphase(algo, sc.shapes, pairs.slice(0, k), nthreads=threads)
+        f64, _ = r64.narrowphase(algo, sc.shapes, pairs.slice(0, k), nthreads=threads)
+        identical &= all(v == 0 for v in reflib.compare_contacts(ours, f32, k).values())
+        same = (ours.is_colliding == f64.is_colliding) & (ours.nb_contacts == f64.nb_contacts)
+        mask = ours.valid_mask() & same[None, :]
+        nd = np.abs(ours.normal_depth.astype(np.float64) - f64.normal_depth)[mask]
+        pt = np.maximum(np.abs(ours.local1.astype(np.float64) - f64.local1)[mask][:, :3].max(1),
+                        np.abs(ours.local2.astype(np.float64) - f64.local2)[mask][:, :3].max(1))
+        ne, de = nd[:, :3].max(1) if len(nd) else np.zeros(1), nd[:, 3] if len(nd) else np.zeros(1)
+        pt = pt if len(pt) else np.zeros(1)
+        q = lambda v: {"median": float(f"{np.median(v):.3g}"), "max": float(f"{v.max():.3g}")}
+        res[nm] = {"pairs": k, "same_path": round(float(same.mean()), 6), "contacts": int(mask.sum()),
+                   "normal": q(ne), "depth_m": q(de), "local_point_m": q(pt)}
+        worst["normal"] = max(worst["normal"], float(ne.max()))
+        worst["depth"] = max(worst["depth"], float(de.max()))
+        worst["point"] = max(worst["point"], float(pt.max()))
+    return {"oracle": "reference double build (IS_RP3D_DOUBLE_PRECISION_ENABLED), outputs rounded to float",
+            "sample": f"first {args.fp64_sample} pairs of every batch, fresh caches", "batches": res,
+            "max_error": {k: float(f"{v:.3g}") for k, v in worst.items()},
+            "tolerance": {"normal": 1e-3, "depth_m": 1e-4, "local_point_m": 1e-3, "same_path": 0.999},
+            "bit_identical_to_reference_f32_on_sample": bool(identical)}
 
 
 def manifold_section(ctx, sc, names, algos, dpairs, douts, args, dev, pinned):
@@ -483,33 +545,47 @@ def world_section(ctx, args, with_cpu):
     return out
 
 
-def many_worlds_section(ctx, args, with_cpu):
+def many_worlds_section(ctx, args, with_cpu, rank=0, world=1):
     """Many independent worlds stepped together: 4,096 worlds of U[20, 200]
     dynamic boxes and spheres (sizes U[0.2, 1]) and 1-4 ragdolls (15 capsules,
     10 ball-and-socket + 4 hinge joints, 60-degree cones, +-60-degree hinge
     limits) falling onto a static ground each (scenes.many_worlds), dt 1/120,
     through one rp3dg_world_update per step of the whole group (wall clock,
-    synchronous).  60 untimed steps, then 60 timed.  The reference engine
+    synchronous).  60 untimed steps, then 60 timed.  With N ranks the worlds
+    are split into N contiguous blocks balanced by body count
+    (reactphysics3d_b200.shard), each rank steps its block with
+    cpu_count // N host threads, and the time is the slowest rank's (strong
+    scaling: the 4,096 worlds are the whole job).  The reference engine
     steps a sample of the same worlds over the same steps on every host core
     (one PhysicsWorld per thread at a time, its own PhysicsCommon each), and
     the sampled worlds' final states are compared bit for bit."""
-    from reactphysics3d_b200 import engine
+    from reactphysics3d_b200 import engine, shard
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import reflib
     n = args.n_worlds
     dt = float(np.float32(1.0 / 120.0))
     warm, timed = 60, 60
-    shapes, scs = scenes.many_worlds(n, seed=args.seed)
-    threads = os.cpu_count() or 1
-    g = engine.WorldGroup(ctx, scs, shapes, threads=threads)
-    g.autotune(rounds=2)             # 18 of the warm-up steps: island scheduling (results unchanged)
-    g.update(dt, warm)
-    tuning = g.tuning()
-    launches0 = ctx.kernel_launches()
-    t0 = time.perf_counter()
-    g.update(dt, timed)
-    sec = time.perf_counter() - t0
-    launches = (ctx.kernel_launches() - launches0) / timed
+    raw_all = scenes.many_worlds(n, seed=args.seed, merge=False)
+    lo, hi = shard.rank_block([len(s_.bodies) for s_ in raw_all], rank, world)
+    shapes, scs = scenes.merge_shapes(raw_all[lo:hi])
+    threads = max(1, (os.cpu_count() or 1) // world)
+    ok, err = True, None
+    try:
+        g = engine.WorldGroup(ctx, scs, shapes, threads=threads)
+        g.autotune(rounds=2)             # 18 of the warm-up steps: island scheduling (results unchanged)
+        g.update(dt, warm)
+        tuning = g.tuning()
+        launches0 = ctx.kernel_launches()
+        t0 = time.perf_counter()
+        g.update(dt, timed)
+        sec = time.perf_counter() - t0
+        launches = (ctx.kernel_launches() - launches0) / timed
+    except Exception as e:   # every rank still takes part in the gather below
+        ok, err, sec = False, f"{type(e).__name__}: {str(e)[:300]}", float("inf")
+    sec_all = shard.max_over_ranks(sec)
+    all_ok = all(shard.gather_objects(ok))
+    if not all_ok:
+        return {"error": err or "another rank failed", "rank_block": [lo, hi]}
     st = g.stats()
     g.set_profiling(True)
     g.update(dt, 5)
@@ -517,14 +593,17 @@ def many_worlds_section(ctx, args, with_cpu):
     out = {"workload": f"{n} independent worlds, U[20,200] boxes and spheres each (sizes U[0.2,1]) and 1-4 ragdolls "
                        "(15 capsules, 10 ball-and-socket + 4 hinge joints, 60-degree cones, +-60-degree hinge limits) "
                        "above a static ground box, random orientations, dt 1/120; steps 61-120 timed",
-           "worlds": n, "bodies": int(sum(len(s_.bodies) for s_ in scs)),
-           "world_steps_per_s": round(n * timed / sec, 1), "ms_per_step": round(1e3 * sec / timed, 3),
-           "kernels_per_step": round(launches, 1), "host_threads": threads, "phase_ms_per_step": phases,
-           "autotuned_scheduling": tuning,
+           "worlds": n, "bodies": int(sum(len(s_.bodies) for s_ in raw_all)),
+           "world_steps_per_s": round(n * timed / sec_all, 1), "ms_per_step": round(1e3 * sec_all / timed, 3),
+           "ranks": world, "scaling": "strong (the worlds are split over the ranks)",
+           "rank0_block": [lo, hi], "kernels_per_step": round(launches, 1), "host_threads_per_rank": threads,
+           "phase_ms_per_step": phases, "autotuned_scheduling": tuning,
            "stats_at_step_120": st, "api": "rp3dg_world_update (world group)"}
     if with_cpu and reflib.have_ref("f32"):
-        raw = scenes.many_worlds(n, seed=args.seed, merge=False)
-        sample = list(range(0, n, max(1, n // (8 * threads))))[: 8 * threads]
+        raw = raw_all[lo:hi]
+        threads = _threads()
+        nn = len(raw)
+        sample = list(range(0, nn, max(1, nn // (8 * threads))))[: 8 * threads]
         refs = [reflib.RefScene(raw[k]) for k in sample]
         # warm-up steps on all threads, then the timed steps
         def run(idx, steps):
@@ -599,6 +678,7 @@ def terrain_section(ctx, args, with_cpu):
     sec = time.perf_counter() - t0
     launches = (ctx.kernel_launches() - launches0) / 20
     st = w.stats()
+    ours80 = w.bodies()
     w.set_profiling(True)
     w.update(dt, 3)
     phases = {k: round(v / 3, 3) for k, v in w.phase_times().items() if not k.startswith("m.")}
@@ -634,8 +714,74 @@ def terrain_section(ctx, args, with_cpu):
         k = gc[:ns] > 0
         ray_out["bit_identical_to_reference_sample"] = bool(np.array_equal(gc[:ns], rc) and
                                                             gh[:ns][k].tobytes() == rh[k].tobytes())
+        # after the landing: the reference continues to step 80 (~10^5
+        # manifolds, one large island) and its states are compared again
+        n_ref = args.terrain_ref_steps
+        if n_ref > 21:
+            t0 = time.perf_counter()
+            r.update(dt, min(n_ref, 80) - 21)
+            out["reference_steps_22_to_80_seconds"] = round(time.perf_counter() - t0, 1)
+            out["bit_identical_to_reference_at_step_80"] = all(np.array_equal(a, b)
+                                                               for a, b in zip(ours80, r.bodies()))
     out["raycast_at_step_21"] = ray_out
     return out
+
+
+def worlds_long_section(ctx, args, with_cpu):
+    """Parity of the many-worlds workload over its full length: a sample of
+    its worlds (every (n / sample)-th world of the same seeded batch) stepped
+    as one group for args.worlds_long_steps steps at 1/120 s, then every
+    sampled world's body states compared with the reference's float build
+    (bit for bit; ragdoll cone / hinge limits use acos / atan2, whose last bit
+    differs between CUDA and the host C library, so a world whose limits
+    engaged is held to a tolerance instead) and with the reference's double
+    build, whose distance to the float build is the spread the tolerance is
+    stated against."""
+    from reactphysics3d_b200 import engine
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import reflib
+    if not (with_cpu and reflib.have_ref("f32") and reflib.have_ref("f64")):
+        return {"skipped": "reference builds (oracle/_ref) absent or CPU legs disabled"}
+    n, ns, steps = args.n_worlds, args.worlds_long_sample, args.worlds_long_steps
+    dt = float(np.float32(1.0 / 120.0))
+    raw = scenes.many_worlds(n, seed=args.seed, merge=False)
+    idx = list(range(0, n, max(1, n // ns)))[:ns]
+    shapes, scs = scenes.merge_shapes([raw[k] for k in idx])
+    threads = _threads()
+    g = engine.WorldGroup(ctx, scs, shapes, threads=threads)
+    t0 = time.perf_counter()
+    g.update(dt, steps)
+    gpu_s = time.perf_counter() - t0
+    ours = [g.bodies(j) for j in range(len(idx))]
+    g.close()
+    refs = {p: [reflib.RefScene(raw[k], p) for k in idx] for p in ("f32", "f64")}
+
+    def run(chunk):
+        for p, j in chunk:
+            refs[p][j].update(dt, steps)
+    jobs = [(p, j) for p in ("f32", "f64") for j in range(len(idx))]
+    ths = [threading.Thread(target=run, args=(jobs[t::threads],)) for t in range(threads)]
+    t0 = time.perf_counter()
+    [t_.start() for t_ in ths]
+    [t_.join() for t_ in ths]
+    ref_s = time.perf_counter() - t0
+    same, within, dev_max, spread_max = 0, 0, 0.0, 0.0
+    for j in range(len(idx)):
+        a = refs["f32"][j].bodies()
+        if all(np.array_equal(x, y) for x, y in zip(ours[j], a)):
+            same += 1
+        p32 = a[0].astype(np.float64)
+        dev = float(np.abs(ours[j][0].astype(np.float64) - p32).max())
+        spread = float(np.abs(refs["f64"][j].bodies()[0] - p32).max())
+        within += dev <= spread
+        dev_max, spread_max = max(dev_max, dev), max(spread_max, spread)
+    return {"workload": f"{len(idx)} of the {n} many-worlds worlds (every {max(1, n // ns)}-th), {steps} steps at "
+                        "1/120 s as one group",
+            "worlds": len(idx), "steps": steps, "gpu_seconds": round(gpu_s, 2),
+            "reference_seconds_f32_and_f64": round(ref_s, 2), "reference_threads": threads,
+            "bit_identical_worlds": same, "worlds_within_fp32_fp64_spread": int(within),
+            "max_position_deviation_m": float(f"{dev_max:.3g}"),
+            "max_reference_fp32_vs_fp64_deviation_m": float(f"{spread_max:.3g}")}
 
 
 def raycast_measure(ctx, w, rays, reps=5):
@@ -866,6 +1012,10 @@ def _threads():
         return os.cpu_count() or 1
 
 
+def fp32_section(ctx, sc, names, algos, dpairs, douts, mean_batch, args, dev, roofline):
+    return {"skipped": "event-counting build not present"}
+
+
 def cpu_baseline(sc, args, sample_frac=None, repeats=1):
     """Time the reference engine's algorithms on the host cores over a bounded
     sample (every batch cut to the same fraction) of the workload."""
@@ -899,13 +1049,19 @@ def run_reference(args):
     sc = scenes.narrowphase_scene(total_pairs=args.pairs, seed=args.seed)
     vals = []
     base = None
-    for s in range(args.warmup + args.steps):
+    # each step is one pass of the reference's algorithms over the sample; the
+    # value is the median over the (at least 5) timed steps, which damps the
+    # load of other processes on the shared host
+    steps = max(5, args.steps)
+    for s in range(args.warmup + steps):
         r = cpu_baseline(sc, args, repeats=1)
         if s >= args.warmup:
             vals.append(r["value"])
             base = r
-    value = float(np.mean(vals))
+    value = float(np.median(vals))
     base["value"] = round(value, 1)
+    base["steps_timed"] = steps
+    base["spread"] = {"min": round(min(vals), 1), "max": round(max(vals), 1)}
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * args.pairs / value, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -943,7 +1099,27 @@ def main():
     ap.add_argument("--n-worlds", type=int, default=4096)
     ap.add_argument("--world-steps", type=int, default=300)
     ap.add_argument("--learned-epochs", type=int, default=4)
+    ap.add_argument("--budget-s", type=float, default=1500.0,
+                    help="sections that would start after this many seconds are skipped (recorded as such)")
+    ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--fp64-sample", type=int, default=20000)
+    ap.add_argument("--terrain-ref-steps", type=int, default=80,
+                    help="the reference steps the large world this far and its states are compared with the GPU's")
+    ap.add_argument("--worlds-long-steps", type=int, default=1000)
+    ap.add_argument("--worlds-long-sample", type=int, default=64)
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: start the ranks through torch's launcher
+        # (rendezvous on the loopback address) and pass every argument on
+        import socket
+        s = socket.socket()
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+        s.close()
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+        sys.exit(subprocess.run(cmd).returncode)
     if args.impl == "reference":
         run_reference(args)
     else:
