@@ -1013,7 +1013,45 @@ def _threads():
 
 
 def fp32_section(ctx, sc, names, algos, dpairs, douts, mean_batch, args, dev, roofline):
-    return {"skipped": "event-counting build not present"}
+    """FP32 roofline of every batch: the batch's inputs go once through the
+    event-counting build of the kernels (rp3dg_narrowphase_count_events,
+    untimed), the path events times the static op table
+    (reactphysics3d_b200.roofline) give the reference's FP32 operations for
+    those pairs, and dividing by the batch's timed device time gives the
+    achieved rate.  The peak is this device's multiply + add rate measured by
+    the library's microkernel (the kernels are compiled without FMA
+    contraction, so fused multiply-adds are not available to them); the FMA
+    rate is reported beside it.  The headline roofline becomes the dominant
+    batch's FP32 roofline, with its HBM figures kept under "hbm"."""
+    from reactphysics3d_b200 import engine
+    from reactphysics3d_b200 import roofline as RF
+    peak = ctx.measure_fp32_peak(fused=False) / 1e12
+    peak_fma = ctx.measure_fp32_peak(fused=True) / 1e12
+    per, tot_ops, tot_ms = {}, 0.0, 0.0
+    for nm in names:
+        scratch = engine.DeviceContacts(dpairs[nm].n, device=dev)
+        ev = ctx.narrowphase_count_events(algos[nm], dpairs[nm], scratch)
+        ops = RF.fp32_ops(algos[nm], ev)
+        ms = mean_batch[nm]
+        per[nm] = {"fp32_ops": round(ops), "ops_per_pair": round(ops / dpairs[nm].n, 1), "kernel_ms": round(ms, 4),
+                   "achieved_tflops": round(ops / (ms * 1e-3) / 1e12, 3),
+                   "frac": round(ops / (ms * 1e-3) / 1e12 / peak, 4), "events": RF.named(ev)}
+        tot_ops += ops
+        tot_ms += ms
+    dom = max(mean_batch, key=mean_batch.get)
+    hbm = {k: roofline[k] for k in ("bound", "achieved", "peak", "unit", "frac", "peak_source") if k in roofline}
+    d = per[dom]
+    roofline.update({"bound": "fp32", "achieved": d["achieved_tflops"], "peak": round(peak, 2), "unit": "TFLOP/s",
+                     "frac": d["frac"], "peak_source": "measured: rp3dg_measure_fp32_peak, separate FP32 multiplies "
+                                                       "and adds (the kernels' arithmetic: no FMA contraction)",
+                     "fma_peak": round(peak_fma, 2), "frac_of_fma_peak": round(d["achieved_tflops"] / peak_fma, 4),
+                     "algorithmic_flops": "reference code-path operations: path events x static op table "
+                                          "(reactphysics3d_b200/roofline.py)",
+                     "hbm": hbm,
+                     "whole_step": {"achieved_tflops": round(tot_ops / (tot_ms * 1e-3) / 1e12, 3),
+                                    "frac": round(tot_ops / (tot_ms * 1e-3) / 1e12 / peak, 4)}})
+    roofline.pop("note", None)
+    return {"peak_tflops_mul_add": round(peak, 2), "peak_tflops_fma": round(peak_fma, 2), "batches": per}
 
 
 def cpu_baseline(sc, args, sample_frac=None, repeats=1):

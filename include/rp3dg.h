@@ -215,6 +215,36 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
 int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* pairs,
                            const rp3dg_contact_batch* out, int clip_with_previous_axis);
 
+/* Measurement entry point, no counterpart in the reference engine: runs
+ * the same batch as rp3dg_narrowphase_device through the event-counting
+ * build of the kernels (same results, slower) and returns, in events[0..
+ * RP3DG_NP_EVENTS-1], how many times the pairs' code paths executed each
+ * step of the reference's algorithms: 0 polyhedron-pair transforms, 1 face
+ * test, 2 box support, 3 convex-mesh support vertex, 4 triangle support,
+ * 5 capsule support, 6 polyhedron-1 edge, 7 Gauss-map test, 8 edge distance,
+ * 9 face-clipping set-up, 10 anti-parallel face candidate, 11 incident
+ * vertex, 12 clipping plane, 13 clipped input vertex, 14 plane-segment
+ * intersection, 15 clipped-vertex depth, 16 face contact, 17 edge contact,
+ * 18 GJK set-up, 19 GJK iteration, 20-22 simplex closest point (2, 3, 4
+ * points), 23 GJK contact, 24 SAT sphere face, 25 SAT sphere contact,
+ * 26 SAT capsule face, 27 SAT capsule edge, 28 capsule edge axis, 29 capsule
+ * clipping plane, 30 closed-form pair test, 31 closed-form contact,
+ * 32 in-margin capsule face, 33 triangle smooth normal; 34-39 zero.
+ * Learned proposals are not used.  Synchronizes the context stream. */
+#define RP3DG_NP_EVENTS 40
+int rp3dg_narrowphase_count_events(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* pairs,
+                                   const rp3dg_contact_batch* out, int clip_with_previous_axis,
+                                   unsigned long long* events);
+
+/* Measurement entry point, no counterpart in the reference engine: FP32
+ * throughput of the device in operations per second, measured with a
+ * microkernel of independent chains timed with CUDA events (best of five
+ * launches after a warm-up).  fused = 0: separate multiplies and adds
+ * (round-to-nearest intrinsics, the arithmetic the narrow-phase kernels are
+ * compiled to: no contraction); fused = 1: fused multiply-adds counted as two
+ * operations.  Touches no clock or power setting. */
+int rp3dg_measure_fp32_peak(int device, int fused, double* ops_per_second);
+
 /* Device-side error bits accumulated by the kernels since the last clear
  * (bit 0: a pair or collider named a shape outside the shape table; such
  * pairs are reported as not colliding; bit 1: a GJK run hit the

@@ -117,10 +117,16 @@ RD void load_item(const NpArgs& a, uint32_t i, Item& it) {
     it.out.first_depth = 0.0f;
     it.tri_side = 0;
     it.tri = nullptr;
+    NP_EV_ONLY(for (uint32_t e = 0; e < NP_EVENT_COUNT; e++) it.ev[e] = 0u;)
 }
 
 RD void store_item(const NpArgs& a, uint32_t i, const Item& it) {
     if (it.gjk_capped) atomicOr(a.error, 2u);
+#ifdef RP3DG_COUNT_EVENTS
+    if (a.events)
+        for (uint32_t e = 0; e < NP_EVENT_USED; e++)
+            if (it.ev[e]) atomicAdd(a.events + e, (unsigned long long)it.ev[e]);
+#endif
     a.is_colliding[i] = it.colliding ? 1 : 0;
     a.nb_contacts[i] = uint8_t(it.out.count < a.max_contacts ? it.out.count : a.max_contacts);
     if (a.cache) {
@@ -599,3 +605,18 @@ static cudaError_t launch_one(int algo, const NpArgs& args, int num_sms, cudaStr
 }
 
 }  // namespace rp3dg
+
+#ifdef RP3DG_COUNT_EVENTS
+// Entry points of the event-counting build (this file compiled a second time
+// by narrowphase_events.cu, which renames the namespace); args points to an
+// NpArgs of the same layout with `events` set.
+cudaError_t rp3dg_events_launch_narrowphase(int algo, const void* args, int num_sms, cudaStream_t stream, int* launches) {
+    return rp3dg::launch_narrowphase(algo, *static_cast<const rp3dg::NpArgs*>(args), num_sms, stream, launches);
+}
+cudaError_t rp3dg_events_launch_narrowphase_tri(int algo, const void* args, int num_sms, cudaStream_t stream) {
+    return rp3dg::launch_narrowphase_tri(algo, *static_cast<const rp3dg::NpArgs*>(args), num_sms, stream);
+}
+void rp3dg_events_upload_box_tables(const void* t, cudaStream_t stream) {
+    rp3dg::upload_box_tables(*static_cast<const rp3dg::BoxTables*>(t), stream);
+}
+#endif

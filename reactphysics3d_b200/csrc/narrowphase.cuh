@@ -231,7 +231,33 @@ struct Item {
     ContactSink out;
     uint32_t tri_side;        // 0: no triangle, 1: shape 1 is the triangle, 2: shape 2
     const TriPoly* tri;
+#ifdef RP3DG_COUNT_EVENTS
+    uint32_t ev[NP_EVENT_COUNT];  // path events of this pair (NpEvent)
+#endif
 };
+
+// Path events: only the event-counting build (RP3DG_COUNT_EVENTS) keeps them;
+// in the product build NP_EV expands to nothing and its arguments are never
+// evaluated, so the timed kernels are unchanged.
+#ifdef RP3DG_COUNT_EVENTS
+#define NP_EV(it, e, k) ((it).ev[(e)] += uint32_t(k))
+#define NP_EV_ONLY(...) __VA_ARGS__
+#else
+#define NP_EV(it, e, k) ((void)0)
+#define NP_EV_ONLY(...)
+#endif
+// the support-point step of each shape kind, k times
+RD void ev_support(Item& it, const SphereS&, uint32_t k = 1) { (void)it; (void)k; }
+RD void ev_support(Item& it, const CapsuleS&, uint32_t k = 1) { (void)it; (void)k; NP_EV(it, EV_SUPPORT_CAPSULE, k); }
+RD void ev_support(Item& it, const BoxPoly&, uint32_t k = 1) { (void)it; (void)k; NP_EV(it, EV_SUPPORT_BOX, k); }
+RD void ev_support(Item& it, const MeshPoly& m, uint32_t k = 1) { (void)it; (void)m; (void)k; NP_EV(it, EV_SUPPORT_VERTEX, k * m.h->nv); }
+RD void ev_support(Item& it, const TriPoly&, uint32_t k = 1) { (void)it; (void)k; NP_EV(it, EV_SUPPORT_TRI, k); }
+// k face tests of testFacesDirectionPolyhedronVsPolyhedron against `other`
+template <class P>
+RD void ev_face_tests(Item& it, const P& other, uint32_t k) {
+    NP_EV(it, EV_FACE_TEST, k);
+    ev_support(it, other, k);
+}
 
 // TriangleShape::computeSmoothTriangleMeshContact (TriangleShape.h:342-365) and
 // computeSmoothMeshContact (TriangleShape.cpp:90-115): the contact normal
@@ -260,6 +286,7 @@ RD void smooth_triangle_contact(const Item& it, v3& nrm, float depth, v3& p1, v3
 // triangle (every addContactPoint of GJKAlgorithm.cpp and SATAlgorithm.cpp is
 // preceded by computeSmoothTriangleMeshContact on the same arguments).
 RD void emit(Item& it, v3& nrm, float depth, v3 p1, v3 p2, bool write = true) {
+    if (it.tri_side) NP_EV(it, EV_TRI_SMOOTH, 1);
     if (it.tri_side) smooth_triangle_contact(it, nrm, depth, p1, p2);
     it.out.add(nrm, depth, p1, p2, write);
 }
@@ -268,6 +295,7 @@ RD void emit(Item& it, v3& nrm, float depth, v3 p1, v3 p2, bool write = true) {
 // SphereVsSphereAlgorithm::testCollision (SphereVsSphereAlgorithm.cpp:34-113)
 // ---------------------------------------------------------------------------
 RD void sphere_sphere(Item& it, float r1, float r2) {
+    NP_EV(it, EV_CLOSED_FORM, 1);
     const xform t1 = it.t1, t2 = it.t2;
     const v3 d = vsub(t2.p, t1.p);
     const float d2 = vlen2(d);
@@ -288,6 +316,7 @@ RD void sphere_sphere(Item& it, float r1, float r2) {
                     p1 = vmul(qrot(i1.q, n), r1);
                     p2 = vmul(qrot(i2.q, n), r2);
                 }
+                NP_EV(it, EV_CLOSED_FORM_CONTACT, 1);
                 it.out.add(n, depth, p1, p2);
             }
             it.colliding = true;
@@ -297,6 +326,7 @@ RD void sphere_sphere(Item& it, float r1, float r2) {
 
 // SphereVsCapsuleAlgorithm::testCollision (SphereVsCapsuleAlgorithm.cpp:38-152)
 RD void sphere_capsule(Item& it, bool sphere1, SphereS sph, CapsuleS cap) {
+    NP_EV(it, EV_CLOSED_FORM, 1);
     const float capHeight = cap.hh + cap.hh;
     const float sr = sph.r, cr = cap.r;
     const xform s2w = sphere1 ? it.t1 : it.t2;
@@ -331,6 +361,7 @@ RD void sphere_capsule(Item& it, bool sphere1, SphereS sph, CapsuleS cap) {
                 pcap = vsub(center, vmul(ncap, cr));
             }
             if (depth <= 0.0f) return;
+            NP_EV(it, EV_CLOSED_FORM_CONTACT, 1);
             it.out.add(nw, depth, sphere1 ? psph : pcap, sphere1 ? pcap : psph);
         }
         it.colliding = true;
@@ -339,6 +370,7 @@ RD void sphere_capsule(Item& it, bool sphere1, SphereS sph, CapsuleS cap) {
 
 // CapsuleVsCapsuleAlgorithm::testCollision (CapsuleVsCapsuleAlgorithm.cpp:37-243)
 RD void capsule_capsule(Item& it, CapsuleS c1, CapsuleS c2) {
+    NP_EV(it, EV_CLOSED_FORM, 1);
     const xform c1to2 = xmul(xinv(it.t2), it.t1);
     const float h1 = c1.hh + c1.hh, h2 = c2.hh + c2.hh;
     const float r1 = c1.r, r2 = c2.r;
@@ -382,6 +414,7 @@ RD void capsule_capsule(Item& it, CapsuleS c1, CapsuleS c2) {
                 const v3 pB2 = vsub(clipB, vmul(n2, r2));
                 const float depth = sum - perp;
                 const v3 nw = qrot(it.t2.q, n2);
+                NP_EV(it, EV_CLOSED_FORM_CONTACT, 2);
                 it.out.add(nw, depth, pA1, pA2);
                 it.out.add(nw, depth, pB1, pB2);
             }
@@ -395,6 +428,7 @@ RD void capsule_capsule(Item& it, CapsuleS c1, CapsuleS c2) {
     const float dist2 = vlen2(d);
     if (dist2 < sum * sum) {
         if (it.report) {
+            NP_EV(it, EV_CLOSED_FORM_CONTACT, 1);
             if (dist2 > MACHINE_EPSILON) {
                 const float dist = sqrtf(dist2);
                 d = vdivs(d, dist);
@@ -618,6 +652,7 @@ enum GjkResult { GJK_SEPARATED = 0, GJK_COLLIDE_IN_MARGIN = 1, GJK_INTERPENETRAT
 
 template <class S1, class S2>
 RD int gjk(Item& it, const S1& s1, const S2& s2) {
+    NP_EV(it, EV_GJK_SETUP, 1);
     const xform t1 = it.t1, t2 = it.t2;
     const xform b2to1 = xmul(xinv(t1), t2);
     const quat rotToB2 = qmul(qinv(t2.q), t1.q);
@@ -635,6 +670,9 @@ RD int gjk(Item& it, const S1& s1, const S2& s2) {
         // Safety bound only: the reference loop has no cap and converges in a
         // handful of iterations; a pair that reaches the bound is flagged.
         if (++iterations > GJK_MAX_ITERATIONS) { it.gjk_capped = true; contactFound = true; break; }
+        NP_EV(it, EV_GJK_ITER, 1);
+        ev_support(it, s1);
+        ev_support(it, s2);
         const v3 suppA = s1.support(vneg(v));
         const v3 suppB = xapply(b2to1, s2.support(qrot(rotToB2, v)));
         const v3 w = vsub(suppA, suppB);
@@ -646,6 +684,7 @@ RD int gjk(Item& it, const S1& s1, const S2& s2) {
         if (sx.contains(w) || distSquare - vDotw <= distSquare * REL_ERROR_SQUARE) { contactFound = true; break; }
         sx.add(w, suppA, suppB);
         if (sx.affinely_dependent()) { contactFound = true; break; }
+        NP_EV(it, sx.n == 2 ? EV_SX_SEG : sx.n == 3 ? EV_SX_TRI : EV_SX_TET, sx.n >= 2 ? 1 : 0);
         const bool ok = sx_recompute(sx);
         v = sx.cp;
         if (!ok) { contactFound = true; break; }
@@ -667,6 +706,7 @@ RD int gjk(Item& it, const S1& s1, const S2& s2) {
         const float depth = margin - dist;
         if (depth <= 0.0f) return GJK_SEPARATED;
         if (vlen2(normal) < MACHINE_EPSILON) return GJK_SEPARATED;
+        NP_EV(it, EV_GJK_CONTACT, 1);
         if (it.report) {
             v3 nrm = normal;
             emit(it, nrm, depth, pA, pB);
@@ -693,11 +733,13 @@ RD void sat_sphere_poly(Item& it, bool sphere1, SphereS sph, const P& poly) {
     const uint32_t nf = poly.nfaces();
     for (uint32_t f = 0; f < nf; f++) {
         const v3 n = poly.normal(f);
+        NP_EV(it, EV_SPHERE_FACE, 1);
         const float depth = vdot(vsub(poly.vertex(poly.face_vertex(f, 0)), center), n) + sph.r;
         if (depth <= 0.0f) return;
         if (depth < minDepth) { minDepth = depth; minFace = f; }
     }
     if (it.report) {
+        NP_EV(it, EV_SPHERE_POLY_CONTACT, 1);
         const v3 mn = poly.normal(minFace);
         const v3 mnw = qrot(p2w.q, mn);
         const v3 psph = qrot(xinv(s2w).q, vmul(vneg(mnw), sph.r));
@@ -729,6 +771,7 @@ RD bool capsule_poly_face_contacts(uint32_t refFace, float capR, const P& poly, 
         const v3 v2 = poly.vertex(tw.vertex);
         const v3 pn = vcross(fn, vsub(v2, v1));
         const v3 pp = poly.vertex(ed.vertex);
+        NP_EV(it, EV_CAPSULE_CLIP, 1);
         if (firstPlane) { plane0 = pp; firstPlane = false; }
         if (nin != 0) {
             v3 o0 = V(0.0f, 0.0f, 0.0f), o1 = V(0.0f, 0.0f, 0.0f);
@@ -792,6 +835,7 @@ RD bool sat_capsule_poly(Item& it, bool cap1, CapsuleS cap, const P& poly) {
     const uint32_t nf = poly.nfaces();
     for (uint32_t f = 0; f < nf; f++) {
         const v3 fnc = qrot(p2c.q, poly.normal(f));
+        NP_EV(it, EV_CAPSULE_FACE, 1);
         const v3 sp = cap.support_margin(vneg(fnc));
         const v3 pf = xapply(p2c, poly.vertex(poly.face_vertex(f, 0)));
         const float depth = vdot(vsub(pf, sp), fnc);
@@ -807,7 +851,9 @@ RD bool sat_capsule_poly(Item& it, bool cap1, CapsuleS cap, const P& poly) {
         const hedge tw = poly.edge(ed.twin);
         const v3 n1 = qrot(p2c.q, poly.normal(ed.face));
         const v3 n2 = qrot(p2c.q, poly.normal(tw.face));
+        NP_EV(it, EV_CAPSULE_EDGE, 1);
         if (vdot(segAxis, n1) * vdot(segAxis, n2) < 0.0f) {
+            NP_EV(it, EV_CAPSULE_EDGE_AXIS, 1);
             float depth = DECIMAL_LARGEST;
             v3 axis = vcross(segAxis, edirc);
             if (vlen2(axis) >= 0.00001f) {
@@ -920,7 +966,7 @@ RD float sat_edge_distance(v3 e1A, v3 e2A, v3 c1, v3 d1, v3 d2, v3& outAxis, boo
 }
 
 // clipPolygonWithPlane (mathematics_functions.h:332-393)
-RD uint32_t clip_polygon(const v3* in, uint32_t nin, v3 pp, v3 pn, v3* out) {
+RD uint32_t clip_polygon(const v3* in, uint32_t nin, v3 pp, v3 pn, v3* out, uint32_t* ninter = nullptr) {
     uint32_t no = 0;
     uint32_t vs = nin - 1;
     const float pnpp = vdot(pn, pp);
@@ -931,11 +977,13 @@ RD uint32_t clip_polygon(const v3* in, uint32_t nin, v3 pp, v3 pn, v3* out) {
         // writes are bounded by CLIP_MAX; a convex face never reaches it
         if (ven >= 0.0f) {
             if (vsn < 0.0f) {
+                if (ninter) ++*ninter;
                 const float t = plane_segment_intersection(a, b, pnpp, pn);
                 if (no < CLIP_MAX) out[no++] = (t >= 0.0f && t <= 1.0f) ? vadd(a, vmul(vsub(b, a), t)) : b;
             }
             if (no < CLIP_MAX) out[no++] = b;
         } else if (vsn >= 0.0f) {
+            if (ninter) ++*ninter;
             const float t = plane_segment_intersection(a, b, -pnpp, vneg(pn));
             if (no < CLIP_MAX) out[no++] = (t >= 0.0f && t <= 1.0f) ? vadd(a, vmul(vsub(b, a), t)) : a;
         }
@@ -954,6 +1002,10 @@ RD bool face_contacts(bool ref1, const PR& refP, const PI& incP, const xform& r2
     const v3 nw = ref1 ? qrot(it.t1.q, axisR) : vneg(qrot(it.t2.q, axisR));
     const uint32_t incFace = most_antiparallel_face(incP, axisI);
     const uint32_t nInc = incP.face_count(incFace);
+    NP_EV(it, EV_CLIP_SETUP, 1);
+    NP_EV(it, EV_ANTIPARALLEL, incP.nfaces());
+    NP_EV(it, EV_INC_VERTEX, nInc < CLIP_MAX ? nInc : CLIP_MAX);
+    NP_EV_ONLY(uint32_t ninter = 0;)
     v3 buf1[CLIP_MAX], buf2[CLIP_MAX];
     uint32_t n1 = 0, n2 = 0;
     for (uint32_t i = 0; i < nInc && i < CLIP_MAX; i++) buf1[n1++] = xapply(i2r, incP.vertex(incP.face_vertex(incFace, i)));
@@ -967,8 +1019,15 @@ RD bool face_contacts(bool ref1, const PR& refP, const PI& incP, const xform& r2
         const hedge nxt = refP.edge(cur.next);
         const v3 ev2 = refP.vertex(nxt.vertex);
         const v3 pn = vcross(axisR, vsub(ev2, ev1));
+        NP_EV(it, EV_CLIP_PLANE, 1);
+        NP_EV(it, EV_CLIP_VERTEX, v1in ? n1 : n2);
+#ifdef RP3DG_COUNT_EVENTS
+        if (v1in) n2 = clip_polygon(buf1, n1, ev1, pn, buf2, &ninter);
+        else n1 = clip_polygon(buf2, n2, ev1, pn, buf1, &ninter);
+#else
         if (v1in) n2 = clip_polygon(buf1, n1, ev1, pn, buf2);
         else n1 = clip_polygon(buf2, n2, ev1, pn, buf1);
+#endif
         curIdx = cur.next;
         cur = nxt;
         ev1 = ev2;
@@ -979,11 +1038,14 @@ RD bool face_contacts(bool ref1, const PR& refP, const PI& incP, const xform& r2
     const uint32_t nClip = v1in ? n2 : n1;
     const v3 refV = refP.vertex(refP.edge(firstEdge).vertex);
     bool found = false;
+    NP_EV(it, EV_CLIP_INTERSECT, ninter);
+    NP_EV(it, EV_CLIP_DEPTH, nClip);
     for (uint32_t i = 0; i < nClip; i++) {
         const float depth = vdot(vsub(refV, clipped[i]), axisR);
         if (depth > 0.0f) {
             found = true;
             if (it.report) {
+                NP_EV(it, EV_CONTACT, 1);
                 const v3 pInc = xapply(r2i, clipped[i]);
                 const v3 pRef = project_onto_plane(clipped[i], axisR, refV);
                 v3 onw = nw;  // outWorldNormal: a copy per clipped point
@@ -1078,6 +1140,7 @@ RD bool confirm_proposal(uint32_t cls, const P1& p1, const P2& p2, const xform& 
 // testCollisionConvexPolyhedronVsConvexPolyhedron (SATAlgorithm.cpp:485-889)
 template <class P1, class P2>
 RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
+    NP_EV(it, EV_POLY_SETUP, 1);
     const xform p1to2 = xmul(xinv(it.t2), it.t1);
     const xform p2to1 = xinv(p1to2);
     LastFrame& lf = it.lf;
@@ -1092,6 +1155,8 @@ RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
         if (lf.has(RP3DG_LF_SAT_FACE_POLY1) || lf.has(RP3DG_LF_SAT_FACE_POLY2)) {
             const bool face1 = lf.has(RP3DG_LF_SAT_FACE_POLY1);
             const float d = face1 ? sat_single_face(p1, p2, p1to2, lf.sat_face) : sat_single_face(p2, p1, p2to1, lf.sat_face);
+            if (face1) ev_face_tests(it, p2, 1);
+            else ev_face_tests(it, p1, 1);
             if (!wasColliding && d <= 0.0f) return;
             if (wasColliding && clipPrev && d > 0.0f) {
                 if (poly_face_contacts(face1, p1, p2, p1to2, p2to1, lf.sat_face, it)) {
@@ -1110,7 +1175,10 @@ RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
             const v3 e2A = p2.vertex(e2.vertex);
             const v3 e2B = p2.vertex(p2.edge(e2.next).vertex);
             const v3 d2 = vsub(e2B, e2A);
+            NP_EV(it, EV_EDGE1, 1);
+            NP_EV(it, EV_GAUSS, 1);
             if (edges_minkowski(edge1_gauss(p1, e1, p1to2), p2, e2, lf.sat_e2)) {
+                NP_EV(it, EV_EDGE_DIST, 1);
                 v3 axis;
                 const v3 c1 = xapply(p1to2, p1.centroid());
                 const float d = sat_edge_distance(e1A, e2A, c1, d1, d2, axis, IsTri<P1>::value,
@@ -1122,6 +1190,7 @@ RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
                     const float l1 = vlen2(d1), l2 = vlen2(d2);
                     const float t1 = vdot(vsub(cp1, e2A), d2) / l2;
                     const float t2 = vdot(vsub(cp2, e1A), d1) / l1;
+                    NP_EV(it, EV_EDGE_CONTACT, 1);
                     if (t1 >= 0.0f && t1 <= 1.0f && t2 >= 0.0f && t2 <= 1.0f) {
                         if (it.report) {
                             v3 nw = qrot(it.t2.q, axis);
@@ -1148,11 +1217,13 @@ RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
     bool isFace1;
     uint32_t f1 = 0, f2 = 0;
     const float d1 = sat_faces(p1, p2, p1to2, f1);
+    ev_face_tests(it, p2, d1 <= 0.0f ? f1 + 1 : p1.nfaces());
     if (d1 <= 0.0f) {
         lf.set(RP3DG_LF_SAT_FACE_POLY1, true); lf.set(RP3DG_LF_SAT_FACE_POLY2, false); lf.sat_face = f1;
         return;
     }
     const float d2 = sat_faces(p2, p1, p2to1, f2);
+    ev_face_tests(it, p1, d2 <= 0.0f ? f2 + 1 : p2.nfaces());
     if (d2 <= 0.0f) {
         lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, true); lf.sat_face = f2;
         return;
@@ -1172,9 +1243,12 @@ RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
         const v3 e1B = xapply(p1to2, p1.vertex(p1.edge(e1.next).vertex));
         const v3 dir1 = vsub(e1B, e1A);
         const Edge1Gauss g = edge1_gauss(p1, e1, p1to2);
+        NP_EV(it, EV_EDGE1, 1);
         for (uint32_t j = 0; j < nhe2; j += 2) {
             const hedge e2 = p2.edge(j);
+            NP_EV(it, EV_GAUSS, 1);
             if (edges_minkowski(g, p2, e2, j)) {
+                NP_EV(it, EV_EDGE_DIST, 1);
                 const v3 e2A = p2.vertex(e2.vertex);
                 const v3 e2B = p2.vertex(p2.edge(e2.next).vertex);
                 v3 axis;
@@ -1198,6 +1272,7 @@ RD void sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev) {
         if (!found) return;
     } else {
         if (it.report) {
+            NP_EV(it, EV_EDGE_CONTACT, 1);
             v3 cp1, cp2;
             closest_points_segments(sE1A, sE1B, sE2A, sE2B, cp1, cp2);
             v3 nw = qrot(it.t2.q, minEdgeAxis);
@@ -1244,6 +1319,7 @@ RD void capsule_poly(Item& it, bool cap1, CapsuleS cap, const P& poly) {
             const uint32_t nf = poly.nfaces();
             for (uint32_t f = 0; f < nf; f++) {
                 const v3 fn = poly.normal(f);
+                NP_EV(it, EV_CAPSULE_GJK_FACE, 1);
                 v3 fnw = qrot(p2w.q, fn);
                 const bool inDir = vdot(fnw, cn) > 0.0f;
                 const bool inContactDir = (cap1 && !inDir) || (!cap1 && inDir);
@@ -1478,6 +1554,9 @@ RD bool warp_face_contacts(bool ref1, const PR& refP, const PI& incP, const xfor
     const uint32_t incFace = warp_most_antiparallel_face(incP, axisI, lane);
     uint32_t n = incP.face_count(incFace);
     if (n > CLIP_MAX) n = CLIP_MAX;
+    NP_EV(it, EV_CLIP_SETUP, 1);
+    NP_EV(it, EV_ANTIPARALLEL, incP.nfaces());
+    NP_EV(it, EV_INC_VERTEX, n);
     v3 P = V(0.0f, 0.0f, 0.0f);
     if (uint32_t(lane) < n) P = xapply(i2r, incP.vertex(incP.face_vertex(incFace, lane)));
     const uint32_t firstEdge = refP.face_edge(minFace);
@@ -1490,6 +1569,8 @@ RD bool warp_face_contacts(bool ref1, const PR& refP, const PI& incP, const xfor
         const v3 pn = vcross(axisR, vsub(ev2, ev1));
         const float pnpp = vdot(pn, ev1);
         const bool active = uint32_t(lane) < n;
+        NP_EV(it, EV_CLIP_PLANE, 1);
+        NP_EV(it, EV_CLIP_VERTEX, n);
         const float ven = active ? vdot(vsub(P, ev1), pn) : 0.0f;
         const int src = lane == 0 ? int(n) - 1 : lane - 1;
         const v3 S = V(__shfl_sync(FULL_MASK, P.x, src), __shfl_sync(FULL_MASK, P.y, src), __shfl_sync(FULL_MASK, P.z, src));
@@ -1513,6 +1594,7 @@ RD bool warp_face_contacts(bool ref1, const PR& refP, const PI& incP, const xfor
                 cnt = 1;
             }
         }
+        NP_EV(it, EV_CLIP_INTERSECT, __popc(__ballot_sync(FULL_MASK, active && (ven >= 0.0f) != (vsn >= 0.0f))));
         uint32_t total;
         const uint32_t pos = warp_exclusive_scan(cnt, lane, total);
         __syncwarp();
@@ -1531,6 +1613,8 @@ RD bool warp_face_contacts(bool ref1, const PR& refP, const PI& incP, const xfor
     const float depth = active ? vdot(vsub(refV, P), axisR) : 0.0f;
     const bool hit = active && depth > 0.0f;
     const unsigned mask = __ballot_sync(FULL_MASK, hit);
+    NP_EV(it, EV_CLIP_DEPTH, n);
+    if (it.report) NP_EV(it, EV_CONTACT, __popc(mask));
     if (mask && it.report) {
         const uint32_t slot = it.out.count + __popc(mask & ((1u << lane) - 1u));
         if (hit && slot < MAX_CONTACTS) {
@@ -1628,6 +1712,7 @@ struct EdgePairWalker<BoxPoly> {
 // Every lane holds the same pair state; contacts and outputs are produced by lane 0.
 template <class P1, class P2>
 RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, int lane, WarpScratch& ws) {
+    NP_EV(it, EV_POLY_SETUP, 1);
     Edge1Stage* stage = ws.stage;
     PhaseTimer timer(lane);
     const xform p1to2 = xmul(xinv(it.t2), it.t1);
@@ -1642,6 +1727,8 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
         if (lf.has(RP3DG_LF_SAT_FACE_POLY1) || lf.has(RP3DG_LF_SAT_FACE_POLY2)) {
             const bool face1 = lf.has(RP3DG_LF_SAT_FACE_POLY1);
             const float d = face1 ? sat_single_face(p1, p2, p1to2, lf.sat_face) : sat_single_face(p2, p1, p2to1, lf.sat_face);
+            if (face1) ev_face_tests(it, p2, 1);
+            else ev_face_tests(it, p1, 1);
             if (!wasColliding && d <= 0.0f) return;
             if (wasColliding && clipPrev && d > 0.0f) {
                 const bool found = warp_poly_face_contacts(face1, p1, p2, p1to2, p2to1, lf.sat_face, it, lane, ws.poly);
@@ -1661,7 +1748,10 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
             const v3 e2A = p2.vertex(e2.vertex);
             const v3 e2B = p2.vertex(p2.edge(e2.next).vertex);
             const v3 d2 = vsub(e2B, e2A);
+            NP_EV(it, EV_EDGE1, 1);
+            NP_EV(it, EV_GAUSS, 1);
             if (edges_minkowski(edge1_gauss(p1, e1, p1to2), p2, e2, lf.sat_e2)) {
+                NP_EV(it, EV_EDGE_DIST, 1);
                 v3 axis;
                 const v3 c1 = xapply(p1to2, p1.centroid());
                 const float d = sat_edge_distance(e1A, e2A, c1, d1, d2, axis);
@@ -1672,6 +1762,7 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
                     const float l1 = vlen2(d1), l2 = vlen2(d2);
                     const float t1 = vdot(vsub(cp1, e2A), d2) / l2;
                     const float t2 = vdot(vsub(cp2, e1A), d1) / l1;
+                    NP_EV(it, EV_EDGE_CONTACT, 1);
                     if (t1 >= 0.0f && t1 <= 1.0f && t2 >= 0.0f && t2 <= 1.0f) {
                         if (it.report) it.out.add(qrot(it.t2.q, axis), d, xapply(p2to1, cp1), cp2, lane == 0);
                         it.colliding = true;
@@ -1692,12 +1783,14 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
     timer.mark(0);
     uint32_t f1 = 0, f2 = 0;
     const float d1 = warp_sat_faces(p1, p2, p1to2, f1, lane);
+    ev_face_tests(it, p2, d1 <= 0.0f ? f1 + 1 : p1.nfaces());
     timer.mark(1);
     if (d1 <= 0.0f) {
         lf.set(RP3DG_LF_SAT_FACE_POLY1, true); lf.set(RP3DG_LF_SAT_FACE_POLY2, false); lf.sat_face = f1;
         return;
     }
     const float d2 = warp_sat_faces(p2, p1, p2to1, f2, lane);
+    ev_face_tests(it, p1, d2 <= 0.0f ? f2 + 1 : p2.nfaces());
     timer.mark(2);
     if (d2 <= 0.0f) {
         lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, true); lf.sat_face = f2;
@@ -1737,6 +1830,7 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
     // first arg-min are those of the sequential loop.
     uint32_t ncand = 0;
     bool separated = false;
+    NP_EV_ONLY(uint32_t cand_before = 0;)
     EdgePairWalker<P2> walk(p2, n2h, lane);
     for (uint32_t base = 0; base < total || ncand > 0;) {
         if (EdgePairWalker<P2>::UNROLL > 1 && base < total && ncand + 32 * EdgePairWalker<P2>::UNROLL <= WARP_CAND_CAP) {
@@ -1789,6 +1883,10 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
             if (sep) {
                 const uint32_t first = __shfl_sync(FULL_MASK, idx, __ffs(sep) - 1);
                 const uint32_t fi = first / n2h;
+                // the reference's loop stops at this pair
+                NP_EV(it, EV_EDGE1, fi + 1);
+                NP_EV(it, EV_GAUSS, first + 1);
+                NP_EV(it, EV_EDGE_DIST, cand_before + c0 + uint32_t(__ffs(sep)));
                 lf.set(RP3DG_LF_SAT_FACE_POLY1, false); lf.set(RP3DG_LF_SAT_FACE_POLY2, false);
                 lf.sat_e1 = 2 * fi;
                 lf.sat_e2 = 2 * (first - fi * n2h);
@@ -1799,8 +1897,12 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
         }
         __syncwarp();
         if (separated) return;
+        NP_EV_ONLY(cand_before += ncand;)
         ncand = 0;
     }
+    NP_EV(it, EV_EDGE1, n1h);
+    NP_EV(it, EV_GAUSS, total);
+    NP_EV(it, EV_EDGE_DIST, cand_before);
     warp_argmin(best, bestIdx);
     __syncwarp();
     timer.mark(4);
@@ -1813,6 +1915,7 @@ RD void warp_sat_poly_poly(Item& it, const P1& p1, const P2& p2, bool clipPrev, 
     } else {
         const uint32_t ih = bestIdx / n2h, jh = bestIdx - ih * n2h;
         if (it.report) {
+            NP_EV(it, EV_EDGE_CONTACT, 1);
             const hedge e1 = p1.edge(2 * ih);
             const v3 e1A = xapply(p1to2, p1.vertex(e1.vertex));
             const v3 e1B = xapply(p1to2, p1.vertex(p1.edge(e1.next).vertex));

@@ -46,6 +46,9 @@ struct NpArgs {
     // polyhedron batches: the order in which the tiles take the pairs (thread
     // t of the batch processes pair perm[t]) or nullptr for 0..n-1
     const uint32_t* perm;
+    // event-counting build only: NP_EVENT_COUNT counters (NpEvent order) the
+    // kernels add each pair's path events to; ignored by the product kernels
+    unsigned long long* events = nullptr;
 };
 
 void upload_box_tables(const BoxTables& t, cudaStream_t s);
@@ -63,3 +66,10 @@ cudaError_t launch_narrowphase_tri(int algo, const NpArgs& args, int num_sms, cu
 cudaError_t launch_narrowphase_propose(const NpArgs& args, uint8_t* proposals, int num_sms, cudaStream_t stream);
 
 }  // namespace rp3dg
+
+// The event-counting build of the narrow-phase kernels (narrowphase_events.cu):
+// the same launches as rp3dg::launch_narrowphase / launch_narrowphase_tri /
+// upload_box_tables, for an rp3dg::NpArgs whose `events` is set.
+cudaError_t rp3dg_events_launch_narrowphase(int algo, const void* args, int num_sms, cudaStream_t stream, int* launches);
+cudaError_t rp3dg_events_launch_narrowphase_tri(int algo, const void* args, int num_sms, cudaStream_t stream);
+void rp3dg_events_upload_box_tables(const void* t, cudaStream_t stream);

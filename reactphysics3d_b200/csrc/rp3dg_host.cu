@@ -209,6 +209,8 @@ struct rp3dg_ctx {
     size_t cap_arena = 0;
     // device error word written by the kernels (bit 0: a pair named a shape outside the table)
     uint32_t* d_error = nullptr;
+    // path-event counters of rp3dg_narrowphase_count_events (NP_EVENT_COUNT words)
+    unsigned long long* d_events = nullptr;
     // staging buffers for rp3dg_narrowphase_host
     void* d_stage = nullptr;
     size_t cap_stage = 0;
@@ -404,6 +406,7 @@ int rp3dg_create(int device, rp3dg_ctx** out) {
     if (e != cudaSuccess) { delete ctx; return RP3DG_ECUDA; }
     const BoxTables t = make_box_tables();
     rp3dg::upload_box_tables(t, ctx->stream);
+    rp3dg_events_upload_box_tables(&t, ctx->stream);
     rp3dg::upload_mlp_box_tables(t, ctx->stream);
     e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) { cudaStreamDestroy(ctx->stream); delete ctx; return RP3DG_ECUDA; }
@@ -419,6 +422,7 @@ void rp3dg_destroy(rp3dg_ctx* ctx) {
     cudaFree(ctx->d_arena);
     cudaFree(ctx->d_stage);
     cudaFree(ctx->d_error);
+    cudaFree(ctx->d_events);
     cudaFree(ctx->d_mlp);
     cudaFree(ctx->d_mlp_scratch);
     cudaFree(ctx->d_proposals);
@@ -689,12 +693,15 @@ int rp3dg_set_shapes(rp3dg_ctx* ctx, const rp3dg_shape* shapes, uint32_t nb) {
     return 0;
 }
 
-int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3dg_contact_batch* out,
-                             int clip_with_previous_axis) {
+namespace {
+// Checks of a device-array narrow-phase call and the kernel arguments it gives
+// (learned proposals off); returns 0 or an error code, 1 for an empty batch.
+int np_args(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3dg_contact_batch* out,
+            int clip_with_previous_axis, rp3dg::NpArgs& a) {
     if (!ctx || !p || !out) return fail(ctx, RP3DG_EINVAL, "null argument");
     if (algorithm < RP3DG_ALGO_SPHERE_VS_SPHERE || algorithm > RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON)
         return fail(ctx, RP3DG_EINVAL, "unknown algorithm");
-    if (p->n == 0) return 0;
+    if (p->n == 0) return 1;
     if (!p->shape1 || !p->shape2 || !p->pos1 || !p->rot1 || !p->pos2 || !p->rot2)
         return fail(ctx, RP3DG_EINVAL, "null pair array");
     if (!out->is_colliding || !out->nb_contacts || !out->normal_depth || !out->local1 || !out->local2)
@@ -706,7 +713,6 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
         !aligned(p->cache, 16) || !aligned(out->normal_depth, 16) || !aligned(out->local1, 16) ||
         !aligned(out->local2, 16) || !aligned(p->shape1, 4) || !aligned(p->shape2, 4))
         return fail(ctx, RP3DG_EINVAL, "misaligned device array (float4 and cache arrays need 16 bytes, shape ids 4)");
-    rp3dg::NpArgs a;
     a.n = p->n;
     a.nb_shapes = ctx->nb_shapes;
     a.error = ctx->d_error;
@@ -727,12 +733,24 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
     a.normal_depth = reinterpret_cast<float4*>(out->normal_depth);
     a.local1 = reinterpret_cast<float4*>(out->local1);
     a.local2 = reinterpret_cast<float4*>(out->local2);
-    const bool learned = ctx->learned_axis && ctx->mlp_ready && algorithm == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON;
-    a.mlp = learned ? static_cast<const void*>(mlp_packed(ctx)) : nullptr;
-    a.mlp_stats = learned ? mlp_stats(ctx) : nullptr;
+    a.mlp = nullptr;
+    a.mlp_stats = nullptr;
     a.proposals = nullptr;
     a.tri = nullptr;
     a.perm = nullptr;
+    a.events = nullptr;
+    return 0;
+}
+}  // namespace
+
+int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3dg_contact_batch* out,
+                             int clip_with_previous_axis) {
+    rp3dg::NpArgs a;
+    const int rc = np_args(ctx, algorithm, p, out, clip_with_previous_axis, a);
+    if (rc != 0) return rc > 0 ? 0 : rc;
+    const bool learned = ctx->learned_axis && ctx->mlp_ready && algorithm == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON;
+    a.mlp = learned ? static_cast<const void*>(mlp_packed(ctx)) : nullptr;
+    a.mlp_stats = learned ? mlp_stats(ctx) : nullptr;
     cudaSetDevice(ctx->device);
     if (learned) {
         // one proposal byte per pair, in a buffer that grows with the batch
@@ -764,6 +782,32 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
     cudaError_t e = rp3dg::launch_narrowphase(algorithm, a, ctx->num_sms, ctx->stream, &launched);
     ctx->launches += uint64_t(launched);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "narrowphase launch");
+    return 0;
+}
+
+int rp3dg_narrowphase_count_events(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p,
+                                   const rp3dg_contact_batch* out, int clip_with_previous_axis,
+                                   unsigned long long* events) {
+    if (!events) return fail(ctx, RP3DG_EINVAL, "null events array");
+    for (int k = 0; k < RP3DG_NP_EVENTS; k++) events[k] = 0;
+    rp3dg::NpArgs a;
+    const int rc = np_args(ctx, algorithm, p, out, clip_with_previous_axis, a);
+    if (rc != 0) return rc > 0 ? 0 : rc;
+    static_assert(RP3DG_NP_EVENTS == rp3dg::NP_EVENT_COUNT, "event array size");
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaSuccess;
+    if (!ctx->d_events) e = cudaMalloc(&ctx->d_events, RP3DG_NP_EVENTS * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_events, 0, RP3DG_NP_EVENTS * sizeof(unsigned long long), ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "event counters");
+    a.events = ctx->d_events;
+    int launched = 0;
+    e = rp3dg_events_launch_narrowphase(algorithm, &a, ctx->num_sms, ctx->stream, &launched);
+    ctx->launches += uint64_t(launched);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(events, ctx->d_events, RP3DG_NP_EVENTS * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "narrowphase (event counting)");
     return 0;
 }
 

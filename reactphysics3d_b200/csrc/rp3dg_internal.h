@@ -50,6 +50,50 @@ struct BoxTables {
     uint8_t pad2[2];
 };
 
+// Steps of the reference's narrow-phase code paths, counted per batch by the
+// event-counting build of the kernels (RP3DG_COUNT_EVENTS): each event is one
+// execution of a fixed piece of the reference's arithmetic, so the FP32
+// operations of a batch are the event counts times a static per-event op
+// table.  The order is part of the C ABI (rp3dg_narrowphase_count_events).
+enum NpEvent : uint32_t {
+    EV_POLY_SETUP = 0,     // SAT polyhedron pair: both relative transforms (SATAlgorithm.cpp:502-503)
+    EV_FACE_TEST,          // testSingleFaceDirectionPolyhedronVsPolyhedron without the support (:1087-1110)
+    EV_SUPPORT_BOX,        // BoxShape::getLocalSupportPointWithoutMargin
+    EV_SUPPORT_VERTEX,     // one vertex of ConvexMeshShape::getLocalSupportPointWithoutMargin
+    EV_SUPPORT_TRI,        // TriangleShape::getLocalSupportPointWithoutMargin
+    EV_SUPPORT_CAPSULE,    // CapsuleShape::getLocalSupportPointWithoutMargin
+    EV_EDGE1,              // edge of polyhedron 1 in polyhedron-2 space (:749-755)
+    EV_GAUSS,              // edge-2 direction + testEdgesBuildMinkowskiFace (:763-769, :1146-1191)
+    EV_EDGE_DIST,          // centroid + computeDistanceBetweenEdges + comparisons (:771-809, :1040-1083)
+    EV_CLIP_SETUP,         // computePolyhedronVsPolyhedronFaceContactPoints: axes (:921-928)
+    EV_ANTIPARALLEL,       // one face of findMostAntiParallelFace (ConvexPolyhedronShape.h:105-123)
+    EV_INC_VERTEX,         // incident face vertex into reference space (:945-948)
+    EV_CLIP_PLANE,         // one reference-face side plane + clipPolygonWithPlane set-up (:958-965, mathematics_functions.h:339-343)
+    EV_CLIP_VERTEX,        // one input vertex of clipPolygonWithPlane (mathematics_functions.h:346-392)
+    EV_CLIP_INTERSECT,     // one computePlaneSegmentIntersection + interpolation
+    EV_CLIP_DEPTH,         // depth of one clipped vertex (:1000-1002)
+    EV_CONTACT,            // one face contact: incident point + projection (:1007-1013)
+    EV_EDGE_CONTACT,       // edge-edge contact: closest points, transforms (:853-864)
+    EV_GJK_SETUP,          // GJKAlgorithm::testCollision transforms (GJKAlgorithm.cpp:79-92)
+    EV_GJK_ITER,           // one GJK iteration without supports and simplex (:118-190)
+    EV_SX_SEG,             // VoronoiSimplex closest point, 2 points (VoronoiSimplex.cpp:304-331)
+    EV_SX_TRI,             // 3 points (:336-451)
+    EV_SX_TET,             // 4 points (:456-575)
+    EV_GJK_CONTACT,        // GJK contact in margin (GJKAlgorithm.cpp:196-233)
+    EV_SPHERE_FACE,        // one face of the SAT sphere test (SATAlgorithm.cpp:82-95, :147-162)
+    EV_SPHERE_POLY_CONTACT,// SAT sphere contact (:100-140)
+    EV_CAPSULE_FACE,       // one face of the SAT capsule test (:197-211, :357-376)
+    EV_CAPSULE_EDGE,       // one edge of the SAT capsule test, Minkowski-face check (:218-236, :476-482)
+    EV_CAPSULE_EDGE_AXIS,  // its edge vs inner-segment depth (:322-354)
+    EV_CAPSULE_CLIP,       // one side plane of computeCapsulePolyhedronFaceContactPoints (:381-470)
+    EV_CLOSED_FORM,        // sphere-sphere / sphere-capsule / capsule-capsule: one whole pair test
+    EV_CLOSED_FORM_CONTACT,// ... and one of its contacts
+    EV_CAPSULE_GJK_FACE,   // one face of the in-margin capsule face search (CapsuleVsConvexPolyhedronAlgorithm.cpp:104-160)
+    EV_TRI_SMOOTH,         // one smooth-normal correction of a triangle contact (TriangleShape.h:309-365)
+    NP_EVENT_USED,
+    NP_EVENT_COUNT = 40    // slots of the C ABI array (the rest stay zero)
+};
+
 // A height field (HeightField + HeightFieldShape scale) as the middle phase
 // reads it: heights[y * ncol + x], unscaled local bounds, height origin.
 struct HfDesc {

@@ -21,6 +21,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "librp3dg.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "rp3dg.h")
 
 RP3DG_OK, RP3DG_EINVAL, RP3DG_ECUDA, RP3DG_ENOMEM, RP3DG_ECAPACITY, RP3DG_ENODEV = 0, -1, -2, -3, -4, -5
+NP_EVENTS = 40  # RP3DG_NP_EVENTS
 
 _lib = None
 
@@ -66,6 +67,9 @@ def load_library(path=LIB_PATH):
     L.rp3dg_device_errors.argtypes = [P, C.POINTER(C.c_uint32), C.c_int]
     L.rp3dg_narrowphase_device.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_int]
     L.rp3dg_narrowphase_host.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_int]
+    L.rp3dg_narrowphase_count_events.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch),
+                                                 C.c_int, C.POINTER(C.c_ulonglong)]
+    L.rp3dg_measure_fp32_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.rp3dg_reduce_contacts_device.argtypes = [P, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), P]
     L.rp3dg_narrowphase_manifolds_host.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch),
                                                    C.c_int, P]
@@ -358,6 +362,22 @@ class Context:
                                                           None if kept is None else kept.data_ptr()))
         self.order_out()
         return contacts
+
+    def narrowphase_count_events(self, algo, pairs, out, clip=True):
+        """Run a device batch through the event-counting build of the kernels;
+        returns the RP3DG_NP_EVENTS path-event counts (numpy uint64)."""
+        ev = (C.c_ulonglong * NP_EVENTS)()
+        pb, cb = pairs.struct(), out.struct()
+        self._check(self.lib.rp3dg_narrowphase_count_events(self.h, int(algo), C.byref(pb), C.byref(cb), int(clip), ev))
+        return np.array(ev[:], dtype=np.uint64)
+
+    def measure_fp32_peak(self, fused=False):
+        """FP32 operations per second of this context's device (microkernel,
+        CUDA events): separate multiplies and adds, or fused multiply-adds
+        counted as two operations."""
+        v = C.c_double()
+        self._check(self.lib.rp3dg_measure_fp32_peak(self.device, int(bool(fused)), C.byref(v)))
+        return v.value
 
     def narrowphase_device(self, algo, pairs, out, clip=True):
         """Asynchronous on the context stream, ordered after torch's current
