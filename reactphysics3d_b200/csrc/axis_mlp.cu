@@ -326,7 +326,19 @@ std::mutex g_noalloc_mutex;
 }  // namespace
 
 // Device address of the scratch array on the current device, looked up once
-// per device (the host-side name of the array is not a device address).
+// per device (the host-side name of the array is not a device address).  The
+// address belongs to the device's current context: a process that resets the
+// device (cudaDeviceReset) while the library is loaded gets a new module
+// image, so the cached address is dropped whenever a call fails and the next
+// call looks it up again; callers that reset a device must not have a call of
+// this entry point in flight on it.
+static void noalloc_forget() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    g_noalloc_ptr[dev] = nullptr;
+}
+
 static cudaError_t noalloc_scratch(float** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -351,15 +363,17 @@ cudaError_t launch_mlp_grads_noalloc(const float* params, const float* x, const 
     if (e != cudaSuccess) return e;
     float* loss_word = scratch + size_t(MLP_NOALLOC_MAX_SAMPLES) * MLP_SCRATCH_ROW;
     e = cudaMemsetAsync(loss_word, 0, sizeof(float), s);
-    if (e != cudaSuccess) return e;
+    if (e != cudaSuccess) { noalloc_forget(); return e; }
     mlp_forward_backward<<<(n + 127) / 128, 128, 0, s>>>(params, x, y, n, scratch, loss_word);
     mlp_weight_grads<<<(MLP_NPARAMS + 127) / 128, 128, 0, s>>>(x, scratch, n, grads);
     e = cudaGetLastError();
-    if (e != cudaSuccess || !loss_host) return e;
+    if (e != cudaSuccess) { noalloc_forget(); return e; }
+    if (!loss_host) return e;
     float sum = 0.0f;
     e = cudaMemcpyAsync(&sum, loss_word, sizeof(float), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e == cudaSuccess) *loss_host = sum / float(n);
+    else noalloc_forget();
     return e;
 }
 

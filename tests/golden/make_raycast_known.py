@@ -9,6 +9,8 @@ checks them, the expected hit fraction and hit point.  Writes
 tests/golden/raycast_known.json.
 
     python tests/golden/make_raycast_known.py [path/to/reference]
+
+(the path defaults to the RP3D_REFERENCE environment variable)
 """
 import json
 import os
@@ -16,7 +18,7 @@ import re
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RP3D_REFERENCE", "")
 SRC = os.path.join(REF, "test", "tests", "collision", "TestRaycast.h")
 TESTS = {"box": "testBox", "sphere": "testSphere", "capsule": "testCapsule",
          "convex_mesh": "testConvexMesh", "heightfield": "testHeightField"}

@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 import reflib
+from reactphysics3d_b200 import _abi as A
 from reactphysics3d_b200 import engine, scenes
 
 TOL = {"normal": 1e-3, "depth": 1e-4, "point": 1e-3, "same_path": 0.999}
@@ -27,21 +28,26 @@ def setup():
     sc = scenes.narrowphase_scene(total_pairs=7 * 4000, seed=2024)
     ctx = engine.Context(0)
     r32, r64 = reflib.RefEngine("f32"), reflib.RefEngine("f64")
-    for e in (ctx, r32, r64):
-        m = e.create_convex_mesh(sc.hull_vertices, sc.hull_faces)
-        e.create_convex_mesh_shape(m)
-    ctx.set_shapes(sc.shapes)
-    yield sc, ctx, r32, r64
+    tables = {}
+    for name, e in (("gpu", ctx), ("f32", r32), ("f64", r64)):
+        inst = e.create_convex_mesh_shape(e.create_convex_mesh(sc.hull_vertices, sc.hull_faces))
+        # the reference harness keeps meshes for the whole process: rename
+        # instance 0 of the workload's table to the id this registration got
+        s = np.array(sc.shapes, copy=True)
+        s["mesh"][s["kind"] == A.SHAPE_CONVEX_MESH] = inst
+        tables[name] = s
+    ctx.set_shapes(tables["gpu"])
+    yield sc, ctx, r32, r64, tables
     ctx.close()
 
 
 @pytest.mark.parametrize("name", scenes.BATCH_NAMES)
 def test_error_against_double_build(setup, name):
-    sc, ctx, r32, r64 = setup
+    sc, ctx, r32, r64, tables = setup
     algo, pairs = sc.batches[name]
     ours = ctx.narrowphase_host(algo, pairs.slice(0, pairs.n))
-    f32, _ = r32.narrowphase(algo, sc.shapes, pairs.slice(0, pairs.n), nthreads=4)
-    f64, _ = r64.narrowphase(algo, sc.shapes, pairs.slice(0, pairs.n), nthreads=4)
+    f32, _ = r32.narrowphase(algo, tables["f32"], pairs.slice(0, pairs.n), nthreads=4)
+    f64, _ = r64.narrowphase(algo, tables["f64"], pairs.slice(0, pairs.n), nthreads=4)
     assert all(v == 0 for v in reflib.compare_contacts(ours, f32, pairs.n).values())
     same = (ours.is_colliding == f64.is_colliding) & (ours.nb_contacts == f64.nb_contacts)
     assert same.mean() >= TOL["same_path"], same.mean()

@@ -24,16 +24,27 @@ def _assert_same(got, exp, cache_got=None, cache_exp=None, what=""):
 
 
 def _register_hulls(e):
+    """The unscaled and the scaled hull instance (ids 0 and 1 in a fresh
+    context); returns their ids."""
     v, f = edgecases.load_hull()
     m = e.create_convex_mesh(v, f)
-    assert e.create_convex_mesh_shape(m) == 0
-    assert e.create_convex_mesh_shape(m, edgecases.HULL_SCALE) == 1
+    return e.create_convex_mesh_shape(m), e.create_convex_mesh_shape(m, edgecases.HULL_SCALE)
+
+
+def _remap_meshes(shapes, ids):
+    """The shape table with convex-mesh instance k renamed ids[k] (the
+    reference harness keeps its meshes for the whole process, so its ids
+    depend on what ran before)."""
+    s = np.array(shapes, copy=True)
+    conv = s["kind"] == A.SHAPE_CONVEX_MESH
+    s["mesh"][conv] = np.asarray(ids)[s["mesh"][conv]]
+    return s
 
 
 @pytest.fixture(scope="module")
 def ctx(cuda_lib):
     c = engine.Context(0)
-    _register_hulls(c)
+    assert _register_hulls(c) == (0, 1)
     yield c
     c.close()
 
@@ -41,7 +52,7 @@ def ctx(cuda_lib):
 @pytest.fixture(scope="module")
 def port_hulls(port):
     port.lib.rp3do_reset()
-    _register_hulls(port)
+    assert _register_hulls(port) == (0, 1)
     return port
 
 
@@ -97,13 +108,14 @@ def test_gpu_matches_oracle_two_frames(ctx, port_hulls, seed):
 @pytest.mark.skipif(not reflib.have_ref("f32"), reason="reference build oracle/_ref not present")
 def test_gpu_matches_reference_build(ctx):
     ref = reflib.RefEngine("f32")
-    _register_hulls(ref)
+    ref_shapes = None
     sc = scenes.narrowphase_scene(total_pairs=7 * 2048, seed=77, hull=edgecases.load_hull())
+    ref_shapes = _remap_meshes(sc.shapes, _register_hulls(ref))
     ctx.set_shapes(sc.shapes)
     for name, (algo, pairs) in sc.batches.items():
         pairs.cache = A.fresh_cache(pairs.n)
         pr, pg = pairs.slice(0, pairs.n), pairs.slice(0, pairs.n)
-        a, _ = ref.narrowphase(algo, sc.shapes, pr)
+        a, _ = ref.narrowphase(algo, ref_shapes, pr)
         g = ctx.narrowphase_host(algo, pg)
         _assert_same(g, a, pg.cache, pr.cache, name)
 
