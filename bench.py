@@ -290,6 +290,8 @@ def run_ours(args):
     section("many_worlds_1000_steps", not args.no_worlds and world == 1,
             lambda: worlds_long_section(ctx, args, cpu_ok))
     section("terrain_world", not args.no_terrain, lambda: terrain_section(ctx, args, cpu_ok))
+    section("graph_coloured_solver", not args.no_terrain and not args.no_colored,
+            lambda: colored_solver_section(ctx, args))
 
     line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
@@ -727,6 +729,52 @@ def terrain_section(ctx, args, with_cpu):
     return out
 
 
+def colored_solver_section(ctx, args):
+    """The graph-coloured contact solver (RP3DG_SOLVER_GRAPH_COLORED, not the
+    drop-in) against the exact-order solver on the 100,000-body terrain world:
+    each solver steps its own copy of the world to args.colored_steps (the
+    bodies settle into one island of ~10^5 manifolds), the last 20 steps are
+    timed, and every step records the velocity constraint residual over the
+    contact points and the bodies' kinetic + potential energy."""
+    from reactphysics3d_b200 import engine
+    n_bodies = args.terrain_bodies
+    sc = scenes.heightfield_world(n_bodies=n_bodies, cols=257, rows=257, seed=5)
+    dt = float(np.float32(1.0 / 60.0))
+    steps = args.colored_steps
+    out = {"workload": f"{n_bodies:,}-body terrain world (as terrain_world), steps 1-{steps}, last 20 timed",
+           "note": "the graph-coloured solver changes the constraint order, so its results differ from the "
+                   "reference's; it is reported by residual and energy beside the exact (drop-in) solver"}
+    for name, solver in (("exact", engine.SOLVER_EXACT), ("graph_coloured", engine.SOLVER_GRAPH_COLORED)):
+        w = engine.World(ctx, sc)
+        w.set_solver(solver, True)
+        trace = []
+        for s_ in range(steps - 20):
+            w.update(dt)
+            trace.append(w.solver_stats())
+        t0 = time.perf_counter()
+        for s_ in range(20):
+            w.update(dt)
+            trace.append(w.solver_stats())
+        sec = time.perf_counter() - t0
+        w.set_profiling(True)
+        w.update(dt, 2)
+        ph = w.phase_times()
+        st = w.stats()
+        w.close()
+        e = np.array([t["kinetic_energy"] + t["potential_energy"] for t in trace])
+        res = np.array([t["residual_rms"] for t in trace[-20:]])
+        out[name] = {"world_steps_per_s": round(20 / sec, 3), "ms_per_step": round(1e3 * sec / 20, 2),
+                     "dynamics_ms_per_step": round(ph.get("dynamics", 0.0) / 2, 3),
+                     "residual_rms_last20": float(f"{res.mean():.4g}"),
+                     "residual_max_last20": float(f"{max(t['residual_max'] for t in trace[-20:]):.4g}"),
+                     "energy_J": {f"step_{k}": round(float(e[k - 1]), 1) for k in (1, steps // 2, steps)},
+                     "kinetic_energy_J_last": round(float(trace[-1]["kinetic_energy"]), 2),
+                     "largest_energy_rise_J_per_step": round(float(np.max(np.diff(e))) if len(e) > 1 else 0.0, 3),
+                     "colors_last": int(trace[-1]["colors"]), "islands": st["islands"],
+                     "manifolds": st["manifolds"]}
+    return out
+
+
 def worlds_long_section(ctx, args, with_cpu):
     """Parity of the many-worlds workload over its full length: a sample of
     its worlds (every (n / sample)-th world of the same seeded batch) stepped
@@ -854,27 +902,37 @@ def broadphase_section(ctx, args, dev):
     fmin0, fmax0 = fmin.clone(), fmax.clone()
     stream = ctx.torch_stream()
     reps = max(3, min(args.steps, 20))
-    ev_u, ev_p = [], []
     cap = 4 * n
-    with torch.cuda.stream(stream):
-        for r in range(reps + 2):
-            fmin.copy_(fmin0); fmax.copy_(fmax0)
-            a0, a1, a2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-            a0.record(stream)
-            ctx.broadphase_update(bp)
-            a1.record(stream)
-            cnt, _ = ctx.broadphase_pairs(bp, cap, axis=0, device=True)
-            a2.record(stream)
-            if r >= 2:
-                ev_u.append((a0, a1)); ev_p.append((a1, a2))
-        ctx.synchronize()
-    tu = float(np.mean([x.elapsed_time(y) for x, y in ev_u]))
-    tp = float(np.mean([x.elapsed_time(y) for x, y in ev_p]))
+    res = {}
+    for method, axis in (("lbvh", -1), ("sweep_x", 0)):
+        ev_u, ev_p = [], []
+        with torch.cuda.stream(stream):
+            for r in range(reps + 2):
+                fmin.copy_(fmin0); fmax.copy_(fmax0)
+                a0, a1, a2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+                a0.record(stream)
+                ctx.broadphase_update(bp)
+                a1.record(stream)
+                cnt, pairs = ctx.broadphase_pairs(bp, cap, axis=axis, device=True)
+                a2.record(stream)
+                if r >= 2:
+                    ev_u.append((a0, a1)); ev_p.append((a1, a2))
+            ctx.synchronize()
+        c = int(cnt.item())
+        pr = pairs[:c].cpu().numpy().astype(np.int64)
+        res[method] = {"pairs": c, "update_ms": float(np.mean([x.elapsed_time(y) for x, y in ev_u])),
+                       "pairs_ms": float(np.mean([x.elapsed_time(y) for x, y in ev_p])),
+                       "set": np.sort(pr[:, 0] * n + pr[:, 1])}
+    lb, sw = res["lbvh"], res["sweep_x"]
+    tu, tp = lb["update_ms"], lb["pairs_ms"]
     return {"workload": "one world, 100,000 colliders (40% boxes, 30% spheres, 30% capsules) on a 50x40x50 "
                         "lattice, 1.5 m spacing, 2 cm random displacement",
-            "colliders": n, "reinserted": int(moved.sum().item()), "pairs": int(cnt.item()),
+            "colliders": n, "reinserted": int(moved.sum().item()), "pairs": lb["pairs"],
+            "method": "LBVH (Morton keys, Karras tree, refit, warp-cooperative traversal)",
             "update_ms": round(tu, 4), "pairs_ms": round(tp, 4),
-            "colliders_per_s": round(n / ((tu + tp) / 1e3), 1)}
+            "colliders_per_s": round(n / ((tu + tp) / 1e3), 1),
+            "sweep_and_prune_pairs_ms": round(sw["pairs_ms"], 4),
+            "same_pair_set_as_sweep": bool(np.array_equal(lb["set"], sw["set"]))}
 
 
 def learned_axis_section(ctx, sc, args, dev):
@@ -1144,6 +1202,8 @@ def main():
     ap.add_argument("--fp64-sample", type=int, default=20000)
     ap.add_argument("--terrain-ref-steps", type=int, default=80,
                     help="the reference steps the large world this far and its states are compared with the GPU's")
+    ap.add_argument("--no-colored", action="store_true")
+    ap.add_argument("--colored-steps", type=int, default=200)
     ap.add_argument("--worlds-long-steps", type=int, default=1000)
     ap.add_argument("--worlds-long-sample", type=int, default=64)
     args = ap.parse_args()

@@ -447,7 +447,11 @@ int rp3dg_dynamics_step_host(rp3dg_ctx* ctx, const rp3dg_dynamics_params* params
  * accept each other, as (lower, higher) collider index.  The reference's
  * no-collision body pairs (joints with collision disabled) are not applied.
  * The order of the pairs is deterministic but is not the reference's (which
- * follows its tree). */
+ * follows its tree).  The search is a linear BVH (axis RP3DG_BROADPHASE_LBVH:
+ * Morton-sorted fat-AABB centres, group in the high key bits, Karras tree,
+ * bottom-up refit, warp-cooperative traversal) or a sort and sweep along
+ * axis 0, 1 or 2; both return the same set. */
+#define RP3DG_BROADPHASE_LBVH (-1)
 typedef struct rp3dg_broadphase {
     uint32_t n;                           /* colliders in the broad phase */
     uint32_t n_update;                    /* colliders [0, n_update) get new AABBs (the enabled ones) */
@@ -467,8 +471,10 @@ typedef struct rp3dg_broadphase {
 
 int rp3dg_broadphase_update_device(rp3dg_ctx* ctx, const rp3dg_broadphase* bp);
 /* Pairs on device arrays: pairs (2 x capacity int32) receives up to capacity
- * pairs; *count (device) the number found (may exceed capacity).  axis 0, 1
- * or 2 is the sweep axis. */
+ * pairs; *count (device) the number found (may exceed capacity).  axis:
+ * RP3DG_BROADPHASE_LBVH (-1) for the LBVH, 0, 1 or 2 for the sweep axis.
+ * Device error bit 4 is set if an LBVH traversal ran out of stack (not
+ * reachable: the tree of 96-bit keys is at most 96 levels deep). */
 int rp3dg_broadphase_pairs_device(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, int axis, int32_t* pairs,
                                   uint32_t capacity, uint32_t* count);
 /* The same on host arrays (fat_min, fat_max, body, group, category, mask);
@@ -628,6 +634,32 @@ int rp3dg_world_get_contacts(rp3dg_world* world, int32_t* body1, int32_t* body2,
                              uint32_t capacity, float* normal_depth, float* local1, float* local2,
                              uint32_t capacity_points, uint32_t* nb_manifolds, uint32_t* nb_contact_points);
 int rp3dg_world_get_stats(rp3dg_world* world, rp3dg_world_stats* stats);
+
+/* Contact solver of the world step.  RP3DG_SOLVER_EXACT (the default) is the
+ * drop-in: ContactSolverSystem::solve (ContactSolverSystem.cpp:479-759) in
+ * the reference's constraint order, bit-identical.  RP3DG_SOLVER_GRAPH_COLORED
+ * has no counterpart in the reference and is not a drop-in: the manifolds'
+ * conflict graph (manifolds sharing a movable body) is coloured on the GPU
+ * and every pass runs colour after colour, the manifolds of a colour in
+ * parallel, with the reference's per-manifold arithmetic; the order differs,
+ * so the results do (worlds with joints keep the exact solver).  With stats,
+ * each step records the velocity constraint residual over the contact points
+ * after the last iteration and the bodies' energies after the step. */
+#define RP3DG_SOLVER_EXACT 0
+#define RP3DG_SOLVER_GRAPH_COLORED 1
+typedef struct rp3dg_solver_stats {
+    double residual_rms;      /* over the contact points: |n.dv| where the impulse is positive, else max(0, -n.dv) */
+    double residual_max;
+    double kinetic_energy;    /* sum of 1/2 m v^2 + 1/2 w.I.w over the enabled dynamic bodies */
+    double potential_energy;  /* sum of -m g.x over the same bodies */
+    uint32_t contact_points;
+    uint32_t colors;          /* graph-coloured solver: colours used, colouring rounds */
+    uint32_t coloring_rounds;
+    uint32_t reserved;
+} rp3dg_solver_stats;
+int rp3dg_world_set_solver(rp3dg_world* world, int solver, int stats);
+/* Statistics of the last step (zero before a step with stats on). */
+int rp3dg_world_get_solver_stats(rp3dg_world* world, rp3dg_solver_stats* out);
 
 /* The contact events of the last update, as EventListener::onContact
  * receives them (CollisionDetectionSystem::reportContacts,

@@ -35,11 +35,22 @@ struct BpArgs {
     int32_t* pairs;
     uint32_t capacity;
     uint32_t* pair_count;
+    // LBVH (sweep axis < 0): centre bounds (6 words), per internal node its
+    // children, sorted range, box and visit counter, per node its parent
+    uint32_t* lbvh_bounds;
+    int2* lbvh_child;
+    int2* lbvh_range;
+    int32_t* lbvh_parent;     // 2n - 1 entries
+    uint32_t* lbvh_visits;
+    float4 *lbvh_nlo, *lbvh_nhi;
 };
 
 cudaError_t launch_bp_update(const BpArgs& a, cudaStream_t s, uint64_t* launches);
+// axis 0, 1, 2: sort and sweep along that axis; axis < 0: LBVH
 cudaError_t launch_bp_pairs(const BpArgs& a, int axis, cudaStream_t s, uint64_t* launches);
 // uint32 words of sort histogram scratch for n keys
 size_t sort_scratch_words(uint32_t n);
+// Exclusive scan of n words in place (one CTA); *total (device, or null) gets the sum.
+cudaError_t launch_exclusive_scan(uint32_t* v, uint32_t n, uint32_t* total, cudaStream_t s);
 
 }  // namespace rp3dg

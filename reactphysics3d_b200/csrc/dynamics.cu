@@ -16,6 +16,7 @@
 #include <cstdio>
 #endif
 
+#include "broadphase_launch.h"
 #include "dynamics_launch.h"
 #include "rp3dg_math.cuh"
 
@@ -1504,13 +1505,257 @@ __global__ void __launch_bounds__(128) dyn_colliders(const DynArgs a) {
 
 uint32_t blocks(uint32_t n) { return (n + 127) / 128; }
 
+// ---- graph-coloured solver -------------------------------------------------
+//
+// Not the drop-in (the drop-in is the exact-order solver above): for very
+// large worlds, where one island of 10^5 manifolds is a chain of 10^4
+// dependency levels, the manifolds' conflict graph (two manifolds conflict
+// when they share a movable body) is coloured on the GPU and every pass (warm
+// start, each velocity iteration) runs colour after colour, the manifolds of
+// one colour in parallel.  No two manifolds of a colour share a movable body,
+// so each manifold still reads the latest velocities of its bodies and the
+// per-manifold arithmetic is the reference's (ContactSolverSystem.cpp:
+// 324-759); only the order of the manifolds differs, so the results differ
+// from the reference's and the solver is reported by its constraint residual
+// and energy, next to the exact solver on the same world.
+//
+// Colouring: speculative greedy rounds.  Each uncoloured manifold takes the
+// lowest colour none of its coloured neighbours has; of two neighbours that
+// took the same colour in a round, the one with the lower index keeps it and
+// the other tries again in the next round.  Decisions depend on the previous
+// round only, so the colouring is deterministic.
+constexpr uint8_t NO_COLOR = 0xff;
+
+RD uint32_t movable_mask(const DynArgs& a, uint32_t mi) { return ~man_fixed(a, mi) & 3u; }
+
+__global__ void __launch_bounds__(128) color_degree(const DynArgs a, uint32_t* __restrict__ deg) {
+    const uint32_t mi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mi >= a.nm) return;
+    const int4 id = man_ids(a, mi);
+    const uint32_t mv = movable_mask(a, mi);
+    if (mv & 1u) atomicAdd(deg + id.x, 1u);
+    if (mv & 2u) atomicAdd(deg + id.y, 1u);
+}
+
+__global__ void __launch_bounds__(128) color_adjacency(const DynArgs a, const uint32_t* __restrict__ start,
+                                                       uint32_t* __restrict__ fill, uint32_t* __restrict__ adj) {
+    const uint32_t mi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mi >= a.nm) return;
+    const int4 id = man_ids(a, mi);
+    const uint32_t mv = movable_mask(a, mi);
+    if (mv & 1u) adj[start[id.x] + atomicAdd(fill + id.x, 1u)] = mi;
+    if (mv & 2u) adj[start[id.y] + atomicAdd(fill + id.y, 1u)] = mi;
+}
+
+__global__ void __launch_bounds__(128) color_tentative(const DynArgs a, ColorScratch c) {
+    const uint32_t mi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mi >= a.nm) return;
+    if (c.color[mi] != NO_COLOR) { c.tent[mi] = NO_COLOR; return; }
+    const int4 id = man_ids(a, mi);
+    const uint32_t mv = movable_mask(a, mi);
+    unsigned long long used[2] = {0ull, 0ull};
+    for (int side = 0; side < 2; side++) {
+        if (!(mv & (1u << side))) continue;
+        const int32_t b = side ? id.y : id.x;
+        for (uint32_t k = c.start[b]; k < c.start[b + 1]; k++) {
+            const uint8_t nc = c.color[c.adj[k]];
+            if (nc != NO_COLOR) used[nc >> 6] |= 1ull << (nc & 63u);
+        }
+    }
+    uint8_t t = NO_COLOR;
+    if (~used[0]) t = uint8_t(__ffsll(static_cast<long long>(~used[0])) - 1);
+    else if (~used[1]) t = uint8_t(64 + __ffsll(static_cast<long long>(~used[1])) - 1);
+    c.tent[mi] = t;   // NO_COLOR: every colour is taken (the caller falls back)
+}
+
+__global__ void __launch_bounds__(128) color_resolve(const DynArgs a, ColorScratch c) {
+    const uint32_t mi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mi >= a.nm) return;
+    const uint8_t t = c.tent[mi];
+    if (t == NO_COLOR) {
+        if (c.color[mi] == NO_COLOR) atomicAdd(c.count + COLOR_MAX, 1u);
+        return;
+    }
+    const int4 id = man_ids(a, mi);
+    const uint32_t mv = movable_mask(a, mi);
+    for (int side = 0; side < 2; side++) {
+        if (!(mv & (1u << side))) continue;
+        const int32_t b = side ? id.y : id.x;
+        for (uint32_t k = c.start[b]; k < c.start[b + 1]; k++) {
+            const uint32_t n = c.adj[k];
+            if (n < mi && c.tent[n] == t) {
+                atomicAdd(c.count + COLOR_MAX, 1u);
+                return;
+            }
+        }
+    }
+    c.color[mi] = t;
+}
+
+__global__ void __launch_bounds__(128) color_count(const DynArgs a, ColorScratch c) {
+    const uint32_t mi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mi < a.nm) atomicAdd(c.count + c.color[mi], 1u);
+}
+
+// Manifolds grouped by colour (the order inside a colour does not matter:
+// its manifolds share no movable body).
+__global__ void __launch_bounds__(128) color_scatter(const DynArgs a, ColorScratch c) {
+    const uint32_t mi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mi < a.nm) c.order[atomicAdd(c.offset + c.color[mi], 1u)] = mi;
+}
+
+template <int PASS>   // 0 warm start, 1 velocity iteration
+__global__ void __launch_bounds__(128) colored_pass(const DynArgs a, const uint32_t* __restrict__ order, uint32_t off,
+                                                    uint32_t cnt, float beta) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= cnt) return;
+    const uint32_t mi = order[off + k];
+    const int4 id = man_ids(a, mi);
+    if (PASS == 0) warm_manifold(a, mi, vel_global(a, id.x, id.y), id.z, id.w);
+    else solve_manifold(a, mi, beta, vel_global(a, id.x, id.y), id.z, id.w);
+}
+
+__global__ void __launch_bounds__(128) colored_store(const DynArgs a) {
+    const uint32_t mi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (mi < a.nm) store_manifold(a, mi);
+}
+
+// Velocity constraint residual of every contact point after the solve, on
+// the constrained velocities (either solver).
+__global__ void __launch_bounds__(128) solver_residual(const DynArgs a) {
+    const uint32_t mi = blockIdx.x * blockDim.x + threadIdx.x;
+    float sq = 0.0f, mx = 0.0f;
+    uint32_t np = 0;
+    if (mi < a.nm) {
+        const int4 id = man_ids(a, mi);
+        const v3 v1 = L3(a.cv[id.x]), w1 = L3(a.cw[id.x]), v2 = L3(a.cv[id.y]), w2 = L3(a.cw[id.y]);
+        for (int k = 0; k < id.z; k++) {
+            const DynPointRec& pr = a.prec[id.w + k];
+            const v3 r1 = L3(pr.q[DP_R1]), r2 = L3(pr.q[DP_R2]), n = L3(pr.q[DP_N]);
+            const float jv = vdot(rel_velocity(v1, w1, v2, w2, r1, r2), n);
+            const float lambda = pr.mut.x;
+            const float r = lambda > 0.0f ? fabsf(jv) : (jv < 0.0f ? -jv : 0.0f);
+            sq += r * r;
+            mx = fmaxf(mx, r);
+            np++;
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        sq += __shfl_xor_sync(0xffffffffu, sq, o);
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        np += __shfl_xor_sync(0xffffffffu, np, o);
+    }
+    if ((threadIdx.x & 31u) == 0 && np) {
+        atomicAdd(&a.stats->residual_sq_sum, double(sq));
+        atomicMax(&a.stats->residual_max_bits, __float_as_uint(mx));
+        atomicAdd(&a.stats->points, np);
+    }
+}
+
+// Energies of the enabled dynamic bodies after the stage.
+__global__ void __launch_bounds__(128) body_energy(const DynArgs a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ke = 0.0, pe = 0.0;
+    if (i < a.nb && body_enabled(a, i)) {
+        const float4 m = a.mass[i];   // mass, inverse mass, dampings
+        if (m.y > 0.0f) {
+            const v3 v = L3(a.lin_vel[i]), w = L3(a.ang_vel[i]);
+            const float4 o = a.orientation[i];
+            const v3 wl = qrot(qinv(Q(o.x, o.y, o.z, o.w)), w);   // angular velocity in the body frame
+            const v3 ii = L3(a.iil[i]);
+            double rot = 0.0;
+            if (ii.x > 0.0f) rot += double(wl.x) * wl.x / ii.x;
+            if (ii.y > 0.0f) rot += double(wl.y) * wl.y / ii.y;
+            if (ii.z > 0.0f) rot += double(wl.z) * wl.z / ii.z;
+            ke = 0.5 * double(m.x) * (double(v.x) * v.x + double(v.y) * v.y + double(v.z) * v.z) + 0.5 * rot;
+            if (a.gravity_enabled && a.gravity[i]) {
+                const float4 x = a.com_world[i];
+                pe = -double(m.x) * (double(a.gx) * x.x + double(a.gy) * x.y + double(a.gz) * x.z);
+            }
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        ke += __shfl_xor_sync(0xffffffffu, ke, o);
+        pe += __shfl_xor_sync(0xffffffffu, pe, o);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        atomicAdd(&a.stats->kinetic, ke);
+        atomicAdd(&a.stats->potential, pe);
+    }
+}
+
+// Colours every manifold and runs the passes; false when the colouring does
+// not finish (every colour taken around some manifold, or too many rounds):
+// the caller then runs the exact solver.  Synchronizes the stream.
+bool colored_islands(const DynArgs& a, cudaStream_t s, uint64_t* launches) {
+    ColorScratch c = *a.color;
+    const uint32_t nm = a.nm;
+    cudaMemsetAsync(c.start, 0, (size_t(a.nb) + 1) * 4, s);
+    cudaMemsetAsync(c.fill, 0, size_t(a.nb) * 4, s);
+    cudaMemsetAsync(c.color, NO_COLOR, nm, s);
+    color_degree<<<blocks(nm), 128, 0, s>>>(a, c.start);
+    launch_exclusive_scan(c.start, a.nb + 1, nullptr, s);
+    color_adjacency<<<blocks(nm), 128, 0, s>>>(a, c.start, c.fill, c.adj);
+    *launches += 3;
+    uint32_t rounds = 0, remaining = nm;
+    while (remaining > 0) {
+        if (++rounds > 64) return false;
+        cudaMemsetAsync(c.count + COLOR_MAX, 0, 4, s);
+        color_tentative<<<blocks(nm), 128, 0, s>>>(a, c);
+        color_resolve<<<blocks(nm), 128, 0, s>>>(a, c);
+        *launches += 2;
+        if (cudaMemcpyAsync(&remaining, c.count + COLOR_MAX, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return false;
+        // (a manifold whose neighbours hold every colour never gets one: the
+        // round limit ends the loop)
+    }
+    uint32_t cnt[COLOR_MAX];
+    cudaMemsetAsync(c.count, 0, COLOR_MAX * 4, s);
+    color_count<<<blocks(nm), 128, 0, s>>>(a, c);
+    *launches += 1;
+    if (cudaMemcpyAsync(cnt, c.count, sizeof(cnt), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return false;
+    uint32_t off[COLOR_MAX], ncol = 0, run = 0;
+    for (uint32_t k = 0; k < COLOR_MAX; k++) {
+        off[k] = run;
+        run += cnt[k];
+        if (cnt[k]) ncol = k + 1;
+    }
+    cudaMemcpyAsync(c.offset, off, sizeof(off), cudaMemcpyHostToDevice, s);
+    color_scatter<<<blocks(nm), 128, 0, s>>>(a, c);
+    *launches += 1;
+    const float beta = a.split ? BETA_SPLIT_IMPULSE : BETA;
+    for (uint32_t k = 0; k < ncol; k++)
+        if (cnt[k]) { colored_pass<0><<<blocks(cnt[k]), 128, 0, s>>>(a, c.order, off[k], cnt[k], beta); (*launches)++; }
+    for (int it = 0; it < a.iterations; it++)
+        for (uint32_t k = 0; k < ncol; k++)
+            if (cnt[k]) { colored_pass<1><<<blocks(cnt[k]), 128, 0, s>>>(a, c.order, off[k], cnt[k], beta); (*launches)++; }
+    colored_store<<<blocks(nm), 128, 0, s>>>(a);
+    (*launches)++;
+    if (a.stats) {
+        uint32_t cr[2] = {ncol, rounds};
+        cudaMemcpyAsync(&a.stats->colors, cr, sizeof(cr), cudaMemcpyHostToDevice, s);
+        // the pageable source is read before the function returns
+        cudaStreamSynchronize(s);
+    }
+    return true;
+}
+
 }  // namespace
 
 cudaError_t launch_dynamics(const DynArgs& a, cudaStream_t s, uint64_t* launches) {
     if (a.nb) { dyn_bodies_pre<<<blocks(a.nb), 128, 0, s>>>(a); (*launches)++; }
     if (a.nm) { dyn_manifold_init<<<blocks(a.nm), 128, 0, s>>>(a); (*launches)++; }
     if (a.nj) { dyn_joints_init<<<blocks(a.nj), 128, 0, s>>>(a); (*launches)++; }
-    if (a.ni) {
+    if (a.stats) cudaMemsetAsync(a.stats, 0, sizeof(SolverStats), s);
+    // the graph-coloured solver takes every island when the stage has no
+    // joints (joint islands keep the exact order); it falls back to the exact
+    // solver if the colouring does not finish
+    bool colored_done = false;
+    if (a.colored && a.color && a.nj == 0 && a.nm) colored_done = colored_islands(a, s, launches);
+    if (a.ni && !colored_done) {
         cudaMemsetAsync(a.counters, 0, 7 * sizeof(uint32_t), s);
         dyn_islands_small<<<blocks(a.ni), 128, 0, s>>>(a);
         (*launches)++;
@@ -1529,8 +1774,10 @@ cudaError_t launch_dynamics(const DynArgs& a, cudaStream_t s, uint64_t* launches
         }
         if (a.nji) { dyn_islands_joint<<<(a.nji + 63) / 64, 64, 0, s>>>(a); (*launches)++; }
     }
+    if (a.stats && a.nm) { solver_residual<<<blocks(a.nm), 128, 0, s>>>(a); (*launches)++; }
     const uint32_t nbp = a.b_enabled ? a.nb : a.nb_enabled, ncp = a.c_enabled ? a.nc : a.nc_enabled;
     if (nbp) { dyn_bodies_post<<<blocks(nbp), 128, 0, s>>>(a); (*launches)++; }
+    if (a.stats && a.nb) { body_energy<<<blocks(a.nb), 128, 0, s>>>(a); (*launches)++; }
     if (a.nji) { dyn_joints_position<<<(a.nji + 63) / 64, 64, 0, s>>>(a); (*launches)++; }
     if (ncp) { dyn_colliders<<<blocks(ncp), 128, 0, s>>>(a); (*launches)++; }
     return cudaGetLastError();

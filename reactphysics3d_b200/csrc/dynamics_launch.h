@@ -36,6 +36,34 @@ struct __align__(16) DynPointRec {
     float4 mut;   // penetration impulse, split impulse, resting (1 / 0)
 };
 
+// Statistics of one dynamics stage for a solver comparison: the velocity
+// constraint residual over the contact points after the last iteration (per
+// point |n . dv| when its accumulated impulse is positive, else the
+// approaching speed max(0, -n . dv)), and the bodies' energies after the
+// stage (kinetic: translational + rotational; potential: -m g . x).
+struct SolverStats {
+    double residual_sq_sum;
+    double kinetic;
+    double potential;
+    uint32_t residual_max_bits;   // float bits of the largest residual (non-negative)
+    uint32_t points;
+    uint32_t colors;              // graph-coloured solver: colours and colouring rounds
+    uint32_t rounds;
+};
+
+// Scratch of the graph-coloured solver (sized by the caller).
+struct ColorScratch {
+    uint32_t* start;     // nb + 1: first adjacency entry of each body
+    uint32_t* fill;      // nb
+    uint32_t* adj;       // 2 nm: manifolds of each movable body
+    uint8_t* color;      // nm
+    uint8_t* tent;       // nm
+    uint32_t* count;     // COLOR_MAX + 2: manifolds per colour, then [COLOR_MAX] remaining, [COLOR_MAX + 1] spare
+    uint32_t* offset;    // COLOR_MAX
+    uint32_t* order;     // nm: manifolds sorted by colour
+};
+constexpr uint32_t COLOR_MAX = 128;
+
 // Per-joint record (joints.cuh): constant rows set on creation (type and
 // flags, local anchors, local hinge / slider axes, inverse initial
 // orientation difference, limits / motor parameters), accumulated impulses
@@ -150,6 +178,11 @@ struct DynArgs {
     int32_t position_iterations;
     uint32_t giant_ctas;   // grid of kernel 3c (persistent, one warp per CTA)
     uint32_t giant_smem;   // dynamic shared memory of a kernel-3c CTA (0: kernel 3c off)
+    // graph-coloured solver (not the drop-in: see launch_dynamics) and the
+    // solver statistics of the stage (either solver), when set
+    int32_t colored;
+    struct SolverStats* stats;
+    ColorScratch* color;
 };
 
 // The joint part of a dynamics stage (see DynArgs).
@@ -170,6 +203,14 @@ struct DynJoints {
 // per SM of the warp-per-island kernel.
 struct DynTuning {
     uint32_t small_max = 8, giant_min = 256, large_per_sm = 2;
+};
+
+// Solver choice of a dynamics stage: the exact-order solver (the drop-in) or
+// the graph-coloured one, and where the stage's statistics go (device, or
+// null for none).
+struct DynSolver {
+    int colored = 0;
+    SolverStats* stats = nullptr;
 };
 
 // Launches the kernels in order on stream s; *launches counts them.

@@ -334,7 +334,8 @@ namespace rp3dg {
 int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
                         const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
                         const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled,
-                        const DynJoints* joints = nullptr, const DynTuning* tune = nullptr);
+                        const DynJoints* joints = nullptr, const DynTuning* tune = nullptr,
+                        const DynSolver* solver = nullptr);
 int broadphase_update_flags(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, const uint8_t* enabled);
 }  // namespace rp3dg
 
@@ -1231,7 +1232,7 @@ namespace rp3dg {
 int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
                         const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
                         const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled,
-                        const DynJoints* joints, const DynTuning* tune) {
+                        const DynJoints* joints, const DynTuning* tune, const DynSolver* solver) {
     int rc = check_dynamics(ctx, pr, b, c, m, p, is);
     if (rc) return rc;
     const void* f16[] = {b->position, b->orientation, b->com_world, b->com_local, b->linear_velocity,
@@ -1256,7 +1257,17 @@ int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const r
     const size_t off_cnt = off_bslot + al(size_t(b->n) * 4);
     const size_t off_list = off_cnt + 256;
     const size_t off_giant = off_list + al(size_t(is->n) * 4);
-    const size_t need = off_giant + al(size_t(is->n) * 4) + 256;
+    size_t need = off_giant + al(size_t(is->n) * 4) + 256;
+    // graph-coloured solver scratch
+    const bool colored = solver && solver->colored;
+    const size_t o_cstart = need; if (colored) need += al((size_t(b->n) + 1) * 4);
+    const size_t o_cfill = need; if (colored) need += al(size_t(b->n) * 4);
+    const size_t o_cadj = need; if (colored) need += al(size_t(m->n) * 8);
+    const size_t o_ccol = need; if (colored) need += al(size_t(m->n));
+    const size_t o_ctent = need; if (colored) need += al(size_t(m->n));
+    const size_t o_ccnt = need; if (colored) need += al((rp3dg::COLOR_MAX + 2) * 4);
+    const size_t o_coff = need; if (colored) need += al(rp3dg::COLOR_MAX * 4);
+    const size_t o_cord = need; if (colored) need += al(size_t(m->n) * 4);
     rc = grow(ctx, &ctx->d_dyn, &ctx->cap_dyn, need, "cudaMalloc(dynamics scratch)");
     if (rc) return rc;
     char* s = static_cast<char*>(ctx->d_dyn);
@@ -1332,6 +1343,20 @@ int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const r
     a.giant_ctas = uint32_t(ctx->num_sms);
     // the opt-in maximum less room for the kernel's static shared memory
     a.giant_smem = ctx->smem_optin > 2048 ? uint32_t(ctx->smem_optin - 1024) : 0u;
+    rp3dg::ColorScratch cs{};
+    if (colored) {
+        cs.start = reinterpret_cast<uint32_t*>(s + o_cstart);
+        cs.fill = reinterpret_cast<uint32_t*>(s + o_cfill);
+        cs.adj = reinterpret_cast<uint32_t*>(s + o_cadj);
+        cs.color = reinterpret_cast<uint8_t*>(s + o_ccol);
+        cs.tent = reinterpret_cast<uint8_t*>(s + o_ctent);
+        cs.count = reinterpret_cast<uint32_t*>(s + o_ccnt);
+        cs.offset = reinterpret_cast<uint32_t*>(s + o_coff);
+        cs.order = reinterpret_cast<uint32_t*>(s + o_cord);
+        a.colored = 1;
+        a.color = &cs;
+    }
+    a.stats = solver ? solver->stats : nullptr;
     cudaError_t e = rp3dg::launch_dynamics(a, ctx->stream, &ctx->launches);
     return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "dynamics launch");
 }
@@ -1464,7 +1489,7 @@ int rp3dg_broadphase_pairs_device(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, in
                                   uint32_t capacity, uint32_t* count) {
     int rc = check_bp(ctx, bp);
     if (rc) return rc;
-    if (axis < 0 || axis > 2) return fail(ctx, RP3DG_EINVAL, "axis must be 0, 1 or 2");
+    if (axis < RP3DG_BROADPHASE_LBVH || axis > 2) return fail(ctx, RP3DG_EINVAL, "axis must be -1 (LBVH), 0, 1 or 2");
     if (!count || (capacity && !pairs)) return fail(ctx, RP3DG_EINVAL, "null output");
     if (bp->n && !bp->body) return fail(ctx, RP3DG_EINVAL, "null body array");
     if (!aligned(pairs, 4) || !aligned(count, 4)) return fail(ctx, RP3DG_EINVAL, "misaligned output");
@@ -1480,6 +1505,14 @@ int rp3dg_broadphase_pairs_device(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, in
     const size_t o_hi = off; off += al(n * 16);
     const size_t o_grp = off; off += al(n * 4);
     const size_t o_poff = off; off += al(n * 4 + 4);
+    const bool lbvh = axis == RP3DG_BROADPHASE_LBVH;
+    const size_t o_lb = off; off += lbvh ? al(8 * 4) : 0;
+    const size_t o_lchild = off; off += lbvh ? al(n * 8) : 0;
+    const size_t o_lrange = off; off += lbvh ? al(n * 8) : 0;
+    const size_t o_lparent = off; off += lbvh ? al(2 * n * 4) : 0;
+    const size_t o_lvisit = off; off += lbvh ? al(n * 4) : 0;
+    const size_t o_lnlo = off; off += lbvh ? al(n * 16) : 0;
+    const size_t o_lnhi = off; off += lbvh ? al(n * 16) : 0;
     cudaSetDevice(ctx->device);
     rc = grow(ctx, &ctx->d_bp, &ctx->cap_bp, off + 256, "cudaMalloc(broad-phase scratch)");
     if (rc) return rc;
@@ -1508,6 +1541,15 @@ int rp3dg_broadphase_pairs_device(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, in
     a.capacity = capacity;
     a.pair_count = count;
     a.error = ctx->d_error;
+    if (lbvh) {
+        a.lbvh_bounds = reinterpret_cast<uint32_t*>(s + o_lb);
+        a.lbvh_child = reinterpret_cast<int2*>(s + o_lchild);
+        a.lbvh_range = reinterpret_cast<int2*>(s + o_lrange);
+        a.lbvh_parent = reinterpret_cast<int32_t*>(s + o_lparent);
+        a.lbvh_visits = reinterpret_cast<uint32_t*>(s + o_lvisit);
+        a.lbvh_nlo = reinterpret_cast<float4*>(s + o_lnlo);
+        a.lbvh_nhi = reinterpret_cast<float4*>(s + o_lnhi);
+    }
     cudaError_t e = rp3dg::launch_bp_pairs(a, axis, ctx->stream, &ctx->launches);
     return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "broad-phase pairs");
 }

@@ -68,7 +68,7 @@ void set_error(rp3dg_ctx* ctx, const std::string& msg);
 int dynamics_step_flags(rp3dg_ctx* ctx, const rp3dg_dynamics_params* pr, const rp3dg_bodies* b,
                         const rp3dg_colliders* c, const rp3dg_manifolds* m, const rp3dg_points* p,
                         const rp3dg_islands* is, const uint8_t* b_enabled, const uint8_t* c_enabled,
-                        const DynJoints* joints, const DynTuning* tune);
+                        const DynJoints* joints, const DynTuning* tune, const DynSolver* solver);
 int broadphase_update_flags(rp3dg_ctx* ctx, const rp3dg_broadphase* bp, const uint8_t* enabled);
 // height fields, the shape table and its local bounds on the device, and the
 // triangle tests of convex vs concave pairs
@@ -792,6 +792,11 @@ struct rp3dg_world {
     size_t cap_hjl = 0;
     uint8_t* h_step = nullptr;  // moved flags, fat AABBs, velocities after the step
     int32_t* h_reset = nullptr;
+    // solver (rp3dg_world_set_solver): 0 exact order, 1 graph-coloured;
+    // with stats, each step's solver statistics in d_solver_stats
+    int solver = 0;
+    bool solver_stats = false;
+    rp3dg::SolverStats* d_solver_stats = nullptr;
     // phase profiling (rp3dg_world_set_profiling): cumulative ms per phase
     bool profiling = false;
     double phase_ms[16] = {};
@@ -1748,6 +1753,7 @@ void destroy_group(Group* g) {
     cudaFreeHost(g->h_reset);
     cudaFree(g->j_rec); cudaFree(g->d_jlist); cudaFree(g->d_ijstart); cudaFree(g->d_ijcount); cudaFree(g->d_jiisl);
     cudaFree(g->d_jibstart); cudaFree(g->d_jibcount); cudaFree(g->d_jirows);
+    cudaFree(g->d_solver_stats);
     cudaFreeHost(g->h_hitems); cudaFreeHost(g->h_hrect); cudaFreeHost(g->h_hstart); cudaFreeHost(g->h_hpstart);
     cudaFreeHost(g->h_hprect); cudaFreeHost(g->h_hbatch); cudaFreeHost(g->h_hout);
     cudaFree(g->d_hitems); cudaFree(g->d_hrect); cudaFree(g->d_hstart); cudaFree(g->d_hpstart); cudaFree(g->d_hprect);
@@ -2536,7 +2542,11 @@ int update_group(Group* g, float dt) {
         const bool tuning = tu.active && !tu.cands.empty();
         const rp3dg::DynTuning tn = tuning ? tu.cands[size_t(tu.idx) % tu.cands.size()] : g->tune;
         if (tuning) cudaEventRecord(tu.e0, st);
-        rc = rp3dg::dynamics_step_flags(ctx, &pr, &B, &C, &Mf, &P, &I, g->b_en, g->c_en, NJ ? &J : nullptr, &tn);
+        rp3dg::DynSolver sol;
+        sol.colored = g->solver;
+        sol.stats = g->solver_stats ? g->d_solver_stats : nullptr;
+        rc = rp3dg::dynamics_step_flags(ctx, &pr, &B, &C, &Mf, &P, &I, g->b_en, g->c_en, NJ ? &J : nullptr, &tn,
+                                        &sol);
         if (rc) return rc;
         if (tuning) {
             cudaEventRecord(tu.e1, st);
@@ -3164,6 +3174,40 @@ int rp3dg_world_get_tuning(rp3dg_world* w, uint32_t* out) {
 int rp3dg_world_set_threads(rp3dg_world* w, int threads) {
     if (!w || threads < 1) return RP3DG_EINVAL;
     w->nthreads = threads;
+    return 0;
+}
+
+int rp3dg_world_set_solver(rp3dg_world* w, int solver, int stats) {
+    if (!w || (solver != RP3DG_SOLVER_EXACT && solver != RP3DG_SOLVER_GRAPH_COLORED)) return RP3DG_EINVAL;
+    if (stats && !w->d_solver_stats) {
+        if (cudaMalloc(&w->d_solver_stats, sizeof(rp3dg::SolverStats)) != cudaSuccess) {
+            w->d_solver_stats = nullptr;
+            return wfail(w, RP3DG_ENOMEM, "cudaMalloc(solver statistics)");
+        }
+        cudaMemset(w->d_solver_stats, 0, sizeof(rp3dg::SolverStats));
+    }
+    w->solver = solver;
+    w->solver_stats = stats != 0;
+    return 0;
+}
+
+int rp3dg_world_get_solver_stats(rp3dg_world* w, rp3dg_solver_stats* out) {
+    if (!w || !out) return RP3DG_EINVAL;
+    std::memset(out, 0, sizeof(*out));
+    if (!w->d_solver_stats) return 0;
+    rp3dg::SolverStats st;
+    cudaError_t e = cudaMemcpyAsync(&st, w->d_solver_stats, sizeof(st), cudaMemcpyDeviceToHost, w->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+    if (e != cudaSuccess) return wfail(w, RP3DG_ECUDA, "solver statistics");
+    float mx;
+    std::memcpy(&mx, &st.residual_max_bits, 4);
+    out->residual_rms = st.points ? std::sqrt(st.residual_sq_sum / double(st.points)) : 0.0;
+    out->residual_max = mx;
+    out->kinetic_energy = st.kinetic;
+    out->potential_energy = st.potential;
+    out->contact_points = st.points;
+    out->colors = st.colors;
+    out->coloring_rounds = st.rounds;
     return 0;
 }
 

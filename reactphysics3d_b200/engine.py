@@ -26,6 +26,16 @@ NP_EVENTS = 40  # RP3DG_NP_EVENTS
 _lib = None
 
 
+SOLVER_EXACT, SOLVER_GRAPH_COLORED = 0, 1
+
+
+class SolverStats(C.Structure):
+    """rp3dg_solver_stats (include/rp3dg.h)."""
+    _fields_ = [("residual_rms", C.c_double), ("residual_max", C.c_double), ("kinetic_energy", C.c_double),
+                ("potential_energy", C.c_double), ("contact_points", C.c_uint32), ("colors", C.c_uint32),
+                ("coloring_rounds", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class Rp3dgError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"rp3dg error {code}: {msg}")
@@ -116,6 +126,8 @@ def load_library(path=LIB_PATH):
     L.rp3dg_world_group_get_contacts.argtypes = [P, C.c_uint32, P, P, P, C.c_uint32, P, P, P, C.c_uint32,
                                                  C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.rp3dg_world_get_phase_times.argtypes = [P, P, C.c_uint32]
+    L.rp3dg_world_set_solver.argtypes = [P, C.c_int, C.c_int]
+    L.rp3dg_world_get_solver_stats.argtypes = [P, C.POINTER(SolverStats)]
     _lib = L
     return L
 
@@ -319,7 +331,7 @@ class Context:
         self._check(self.lib.rp3dg_broadphase_update_device(self.h, C.byref(bp)))
         self.order_out()
 
-    def broadphase_pairs(self, bp, capacity, axis=0, device=False):
+    def broadphase_pairs(self, bp, capacity, axis=-1, device=False):
         """Overlapping pairs: (count, pairs (capacity x 2 int32)).  Host arrays
         unless device is set (then pairs and the count are CUDA tensors)."""
         if device:
@@ -639,6 +651,21 @@ class World:
         t = np.zeros(4, np.uint32)
         self.lib.rp3dg_world_get_tuning(self.h, t.ctypes.data)
         return {"small_max": int(t[0]), "giant_min": int(t[1]), "large_per_sm": int(t[2]), "tuning": bool(t[3])}
+
+    def set_solver(self, solver=SOLVER_EXACT, stats=False):
+        """RP3DG_SOLVER_EXACT (the drop-in) or RP3DG_SOLVER_GRAPH_COLORED; with
+        stats, every step records the solver statistics."""
+        rc = self.lib.rp3dg_world_set_solver(self.h, int(solver), int(bool(stats)))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+
+    def solver_stats(self):
+        """The last step's solver statistics as a dict."""
+        st = SolverStats()
+        rc = self.lib.rp3dg_world_get_solver_stats(self.h, C.byref(st))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+        return {f: getattr(st, f) for f, _ in SolverStats._fields_ if f != "reserved"}
 
     def set_profiling(self, on=True):
         self.lib.rp3dg_world_set_profiling(self.h, int(on))

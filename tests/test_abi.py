@@ -62,12 +62,18 @@ def test_struct_layouts_match_the_python_dtypes(tmp_path):
                "rp3dg_raycast_hit": A.RAYCAST_HIT_DTYPE, "rp3dg_contact_event": A.CONTACT_EVENT_DTYPE,
                "rp3dg_world_settings": A.WORLD_SETTINGS_DTYPE, "rp3dg_body_desc": A.BODY_DESC_DTYPE,
                "rp3dg_collider_desc": A.COLLIDER_DESC_DTYPE, "rp3dg_world_stats": A.WORLD_STATS_DTYPE}
+    # ctypes structures of the bindings, as (size, {field: offset})
+    from reactphysics3d_b200 import broadphase as BP
+    ctypes_structs = {"rp3dg_solver_stats": engine.SolverStats, "rp3dg_broadphase": BP.BroadPhase}
+    layouts = {name: (dt.itemsize, {f: dt.fields[f][1] for f in dt.names}) for name, dt in structs.items()}
+    layouts.update({name: (C.sizeof(st), {f: getattr(st, f).offset for f, _ in st._fields_})
+                    for name, st in ctypes_structs.items()})
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{os.path.join(root, "include", "rp3dg.h")}"',
              "int main(void) {"]
-    for name, dt in structs.items():
+    for name, (size, fields) in layouts.items():
         lines.append(f'    printf("{name} %zu\\n", sizeof({name}));')
-        for f in dt.names:
+        for f in fields:
             lines.append(f'    printf("{name}.{f} %zu\\n", offsetof({name}, {f}));')
     lines += ["    return 0;", "}"]
     src = tmp_path / "layout.c"
@@ -76,7 +82,7 @@ def test_struct_layouts_match_the_python_dtypes(tmp_path):
     subprocess.run([cc, str(src), "-o", str(exe)], check=True)
     got = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], capture_output=True, text=True,
                                                           check=True).stdout.splitlines())
-    for name, dt in structs.items():
-        assert int(got[name]) == dt.itemsize, name
-        for f in dt.names:
-            assert int(got[f"{name}.{f}"]) == dt.fields[f][1], (name, f)
+    for name, (size, fields) in layouts.items():
+        assert int(got[name]) == size, name
+        for f, off in fields.items():
+            assert int(got[f"{name}.{f}"]) == off, (name, f)

@@ -1,8 +1,8 @@
 """Broad phase on the GPU (rp3dg_broadphase_update_device,
 rp3dg_broadphase_pairs_device / _host) against the reference's own broad
 phase (committed fixture): bit-exact fat AABBs and reinsertions, identical
-pair sets; random AABB sets against the brute-force oracle on every sweep
-axis; thousands of worlds as groups."""
+pair sets; random AABB sets against the brute-force oracle with the LBVH and
+on every sweep axis; thousands of worlds as groups."""
 import numpy as np
 import pytest
 import torch
@@ -55,7 +55,7 @@ def test_gpu_pairs_match_reference(ctx, fixture, api):
     for n in dynio.cases(fixture):
         p = bpio.pairs_case(dynio.capture(fixture, n))
         m = len(p["body"])
-        for axis in (0, 1, 2):
+        for axis in (-1, 0, 1, 2):
             if api == "host":
                 bp = BP.make(m, 0, 0, body=p["body"], category=p["category"], mask=p["mask"], fat_min=p["fat_min"],
                              fat_max=p["fat_max"])
@@ -91,7 +91,7 @@ def test_gpu_pairs_random_vs_oracle(ctx, port, seed, n, groups):
     keep = [T(a) for a in (body, cat, msk, mn, mx)] + ([T(grp)] if groups else [None])
     bp = BP.make(n, 0, groups, body=keep[0], category=keep[1], mask=keep[2], fat_min=keep[3], fat_max=keep[4],
                  group=keep[5])
-    for axis in (0, 1, 2):
+    for axis in (-1, 0, 1, 2):
         c, pr = ctx.broadphase_pairs(bp, len(exp) + 16, axis=axis, device=True)
         ctx.synchronize()
         cnt = int(c.item())
@@ -122,11 +122,12 @@ def test_gpu_pairs_many_worlds(ctx, fixture):
     keep = [T(arr[k]) for k in ("body", "category", "mask", "fat_min", "fat_max")] + [T(np.concatenate(group))]
     bp = BP.make(off, 0, 4096, body=keep[0], category=keep[1], mask=keep[2], fat_min=keep[3], fat_max=keep[4],
                  group=keep[5])
-    c, pr = ctx.broadphase_pairs(bp, len(expected) + 16, axis=0, device=True)
-    ctx.synchronize()
-    cnt = int(c.item())
-    assert cnt == len(expected)
-    assert bpio.pair_set(pr.cpu().numpy(), cnt) == expected
+    for axis in (-1, 0):
+        c, pr = ctx.broadphase_pairs(bp, len(expected) + 16, axis=axis, device=True)
+        ctx.synchronize()
+        cnt = int(c.item())
+        assert cnt == len(expected)
+        assert bpio.pair_set(pr.cpu().numpy(), cnt) == expected
 
 
 def test_gpu_broadphase_errors(ctx):
@@ -134,5 +135,10 @@ def test_gpu_broadphase_errors(ctx):
     bp = BP.make(1, 0, 0, body=np.zeros(1, np.int32), fat_min=z, fat_max=z)
     with pytest.raises(engine.Rp3dgError):
         ctx.broadphase_pairs(bp, 4, axis=3)
-    cnt, _ = ctx.broadphase_pairs(BP.make(0, 0, 0), 4)
-    assert cnt == 0
+    with pytest.raises(engine.Rp3dgError):
+        ctx.broadphase_pairs(bp, 4, axis=-2)
+    for axis in (-1, 0):
+        cnt, _ = ctx.broadphase_pairs(BP.make(0, 0, 0), 4, axis=axis)
+        assert cnt == 0
+        cnt, _ = ctx.broadphase_pairs(bp, 4, axis=axis)   # one collider: no pair
+        assert cnt == 0
