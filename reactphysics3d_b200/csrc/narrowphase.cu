@@ -349,6 +349,33 @@ __global__ void __launch_bounds__(NP_BLOCK, MinBlocks<ALGO>::value) narrowphase_
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const uint32_t nwarps = gridDim.x * (NP_BLOCK / 32);
         uint32_t tested = 0, confirmed = 0;
+        if (ALGO == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON && a.tiles) {
+            // persistent warps over the pairs of the tiles the thread-per-pair
+            // launch left (listed by it, in any order): one pair at a time, so
+            // the launch ends within one pair's time of its average
+            const uint32_t total = 32u * __ldcg(a.work);
+            WarpScratch& ws = s_stage[warp];
+            for (;;) {
+                uint32_t k = 0;
+                if (lane == 0) k = atomicAdd(a.work + 1, 1u);
+                k = __shfl_sync(FULL_MASK, k, 0);
+                if (k >= total) break;
+                const uint32_t t = a.tiles[k >> 5] * 32u + (k & 31u);
+                if (t >= a.n) continue;
+                const uint32_t i = a.perm ? a.perm[t] : t;
+                uint32_t proposal = a.proposals ? uint32_t(a.proposals[i]) : uint32_t(MLP_NO_PROPOSAL);
+                if (proposal >= MLP_OUT) proposal = MLP_NO_PROPOSAL;
+                const uint32_t r = process_pair_warp(a, i, lane, &s_box, mesh_words, ws, proposal);
+                tested += r & 1u;
+                confirmed += (r >> 1) & 1u;
+                __syncwarp();
+            }
+            if (a.mlp_stats && lane == 0 && tested) {
+                atomicAdd(&a.mlp_stats[0], (unsigned long long)tested);
+                atomicAdd(&a.mlp_stats[1], (unsigned long long)confirmed);
+            }
+            return;
+        }
         for (uint32_t tile = blockIdx.x * (NP_BLOCK / 32) + warp; tile * 32u < a.n; tile += nwarps) {
             const uint32_t t = tile * 32u + lane;
             const uint32_t i = (a.perm && t < a.n) ? a.perm[t] : t;
@@ -361,6 +388,7 @@ __global__ void __launch_bounds__(NP_BLOCK, MinBlocks<ALGO>::value) narrowphase_
                 }
             }
             const bool all_box = __all_sync(FULL_MASK, boxbox);
+            if (ALGO == ALGO_POLY_PER_THREAD && !all_box && a.tiles && lane == 0) a.tiles[atomicAdd(a.work, 1u)] = tile;
             if ((ALGO == ALGO_POLY_PER_THREAD) != all_box) continue;  // the other launch takes this tile
             WarpScratch& ws = s_stage[warp];
             uint32_t proposal = MLP_NO_PROPOSAL;
@@ -575,6 +603,10 @@ cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaSt
     *launches = 0;
     if (args.n == 0) return cudaSuccess;
     if (algo == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON) {
+        if (args.tiles) {
+            cudaError_t e = cudaMemsetAsync(args.work, 0, 2 * sizeof(uint32_t), stream);
+            if (e != cudaSuccess) return e;
+        }
         cudaError_t e = launch_one(ALGO_POLY_PER_THREAD, args, num_sms, stream);
         if (e != cudaSuccess) return e;
         ++*launches;
@@ -599,7 +631,15 @@ static cudaError_t launch_one(int algo, const NpArgs& args, int num_sms, cudaStr
     const uint32_t blocks_needed = (args.n + NP_BLOCK - 1) / NP_BLOCK;
     // Enough CTAs to fill every SM several times; the grid-stride loop covers the rest.
     const uint32_t cap = uint32_t(num_sms) * 16u;
-    const uint32_t blocks = blocks_needed < cap ? blocks_needed : cap;
+    uint32_t blocks = blocks_needed < cap ? blocks_needed : cap;
+    if (algo == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON && args.tiles) {
+        // persistent: the CTAs that fit on the device at once
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NP_BLOCK, smem);
+        if (e != cudaSuccess) return e;
+        const uint32_t resident = uint32_t(num_sms) * uint32_t(per_sm > 0 ? per_sm : 1);
+        blocks = blocks_needed < resident ? blocks_needed : resident;
+    }
     void* params[] = {const_cast<NpArgs*>(&args)};
     return cudaLaunchKernel(k, dim3(blocks), dim3(NP_BLOCK), params, smem, stream);
 }

@@ -792,7 +792,17 @@ RD bool capsule_poly_face_contacts(uint32_t refFace, float capR, const P& poly, 
                 o0 = a;
                 no = 1;
                 const float t = plane_segment_intersection(a, b, -vdot(pn, pp), vneg(pn));
-                if (t >= 0.0f && t <= 1.0f) { o1 = vadd(a, vmul(vsub(b, a), t)); no = 2; }
+                if (t >= 0.0f && t <= 1.0f) {
+                    o1 = vadd(a, vmul(vsub(b, a), t));
+                    no = 2;
+                } else {
+                    // the segment is nearly parallel to the plane (t = -1): the
+                    // reference keeps one vertex, and its next plane reads the
+                    // array's second slot past its size, which still holds this
+                    // plane's second vertex (Array::operator= clears and re-adds,
+                    // Array.h:470-482): the segment goes on unchanged
+                    o1 = b;
+                }
             }
             in0 = o0; in1 = o1; nin = no;
         }
@@ -1545,8 +1555,16 @@ RD uint32_t warp_exclusive_scan(uint32_t v, int lane, uint32_t& total) {
 // of the counts), which is exactly the sequential output order.  Vertex dot
 // products are the same expressions as in the sequential pass.  Contacts are
 // appended in clipped-vertex order.  All lanes return the same value.
+// Functions a pair runs at most once or twice (the clipping of the contact
+// face) may be kept out of line to shrink the instruction footprint of the
+// warp-per-pair kernel (RP3DG_NP_COLD_NOINLINE, a build option).
+#ifdef RP3DG_NP_COLD_NOINLINE
+#define RD_COLD __device__ __noinline__
+#else
+#define RD_COLD RD
+#endif
 template <class PR, class PI>
-RD bool warp_face_contacts(bool ref1, const PR& refP, const PI& incP, const xform& r2i, const xform& i2r,
+RD_COLD bool warp_face_contacts(bool ref1, const PR& refP, const PI& incP, const xform& r2i, const xform& i2r,
                            uint32_t minFace, Item& it, int lane, v3* poly) {
     const v3 axisR = refP.normal(minFace);
     const v3 axisI = qrot(r2i.q, axisR);

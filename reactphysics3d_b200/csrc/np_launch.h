@@ -49,6 +49,12 @@ struct NpArgs {
     // event-counting build only: NP_EVENT_COUNT counters (NpEvent order) the
     // kernels add each pair's path events to; ignored by the product kernels
     unsigned long long* events = nullptr;
+    // polyhedron batches, when set: the thread-per-pair launch appends every
+    // tile it leaves to the warp-per-pair launch to `tiles` (count in
+    // work[0]); the warp-per-pair launch is then persistent and its warps take
+    // those tiles' pairs one at a time (counter work[1])
+    uint32_t* tiles = nullptr;
+    uint32_t* work = nullptr;
 };
 
 void upload_box_tables(const BoxTables& t, cudaStream_t s);

@@ -211,6 +211,9 @@ struct rp3dg_ctx {
     uint32_t* d_error = nullptr;
     // path-event counters of rp3dg_narrowphase_count_events (NP_EVENT_COUNT words)
     unsigned long long* d_events = nullptr;
+    // polyhedron batches: tiles for the warp-per-pair launch and two counters
+    uint32_t* d_tiles = nullptr;
+    size_t cap_tiles = 0;
     // staging buffers for rp3dg_narrowphase_host
     void* d_stage = nullptr;
     size_t cap_stage = 0;
@@ -424,6 +427,7 @@ void rp3dg_destroy(rp3dg_ctx* ctx) {
     cudaFree(ctx->d_stage);
     cudaFree(ctx->d_error);
     cudaFree(ctx->d_events);
+    cudaFree(ctx->d_tiles);
     cudaFree(ctx->d_mlp);
     cudaFree(ctx->d_mlp_scratch);
     cudaFree(ctx->d_proposals);
@@ -695,6 +699,8 @@ int rp3dg_set_shapes(rp3dg_ctx* ctx, const rp3dg_shape* shapes, uint32_t nb) {
 }
 
 namespace {
+int grow(rp3dg_ctx* ctx, void** buf, size_t* cap, size_t need, const char* what);
+
 // Checks of a device-array narrow-phase call and the kernel arguments it gives
 // (learned proposals off); returns 0 or an error code, 1 for an empty batch.
 int np_args(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3dg_contact_batch* out,
@@ -740,6 +746,18 @@ int np_args(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3d
     a.tri = nullptr;
     a.perm = nullptr;
     a.events = nullptr;
+    a.tiles = nullptr;
+    a.work = nullptr;
+    if (algorithm == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON) {
+        // tile list (one word per tile of 32 pairs) and its two counters
+        const size_t words = (size_t(p->n) + 31) / 32 + 2;
+        cudaSetDevice(ctx->device);
+        const int rc = grow(ctx, reinterpret_cast<void**>(&ctx->d_tiles), &ctx->cap_tiles, words * 4,
+                            "cudaMalloc(polyhedron tiles)");
+        if (rc) return rc;
+        a.work = ctx->d_tiles;
+        a.tiles = ctx->d_tiles + 2;
+    }
     return 0;
 }
 }  // namespace

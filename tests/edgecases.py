@@ -156,3 +156,37 @@ def load_hull():
     with open(os.path.join(HERE, "golden", "hull42.json")) as fh:
         d = json.load(fh)
     return np.array(d["vertices"], np.float32), [list(map(int, f)) for f in d["faces"]]
+
+
+def grazing_capsule_batch(n=4096, seed=0):
+    """Capsules (CAP_A) lying on the top face of a box (BOX_A, half extents
+    1 x 0.5 x 0.75) with their axis almost parallel to one of the face's
+    edges and crossing that edge's side plane at a grazing angle, so that
+    |n . (b - a)| is below the 1e-4 parallel threshold of
+    computePlaneSegmentIntersection and clipSegmentWithPlanes
+    (mathematics_functions.h:256-326) takes its one-vertex branch; shallow
+    (GJK in margin) and deep (SAT) contacts, both shape orders."""
+    rng = np.random.default_rng(seed)
+    rows = []
+    he = (1.0, 0.5, 0.75)
+    for k in range(n):
+        along_z = k % 2 == 0
+        eps = rng.uniform(-4e-5, 4e-5)
+        off = rng.uniform(-2e-5, 2e-5)
+        depth = rng.uniform(0.01, 0.25) if k % 4 < 2 else rng.uniform(0.31, 0.45)
+        y = he[1] + 0.3 - depth
+        side = 1.0 if rng.random() < 0.5 else -1.0
+        if along_z:
+            # axis (local y) -> world z, then a tiny turn about y
+            q = qmul(qaxis((0, 1, 0), math.degrees(eps)), qaxis((1, 0, 0), 90.0))
+            pos = (side * he[0] + off, y, rng.uniform(-0.1, 0.1))
+        else:
+            q = qmul(qaxis((0, 1, 0), math.degrees(eps)), qaxis((0, 0, 1), 90.0))
+            pos = (rng.uniform(-0.1, 0.1), y, side * he[2] + off)
+        spin = qaxis((0, 1, 0), rng.uniform(0, 360))   # about the capsule's own axis
+        qc = qmul(q, spin)
+        if k % 8 < 4:
+            rows.append((CAP_A, BOX_A, pos, qc, (0.0, 0.0, 0.0), I))
+        else:
+            rows.append((BOX_A, CAP_A, (0.0, 0.0, 0.0), I, pos, qc))
+    return batch(rows)

@@ -177,3 +177,21 @@ def test_full_size_scene_properties(ctx, port_hulls):
         nd = h1.normal_depth[m]
         assert np.all(nd[:, 3] > 0)
         assert np.allclose(np.linalg.norm(nd[:, :3], axis=1), 1.0, atol=1e-4)
+
+
+def test_grazing_capsule_clip_matches_oracle(ctx, port_hulls):
+    """Capsules on a box face almost parallel to one of its edges, crossing
+    the edge's side plane at a grazing angle: clipSegmentWithPlanes keeps one
+    vertex and its next plane reads the array's stale second slot (the
+    previous second vertex); the GPU reproduces it."""
+    sh = edgecases.shape_table()
+    ctx.set_shapes(sh)
+    b = edgecases.grazing_capsule_batch(4096, seed=5)
+    exp, _ = port_hulls.narrowphase(A.ALGO_CAPSULE_VS_CONVEX_POLYHEDRON, sh, b.slice(0, b.n))
+    got = ctx.narrowphase_host(A.ALGO_CAPSULE_VS_CONVEX_POLYHEDRON, b.slice(0, b.n))
+    _assert_same(got, exp, what="grazing capsules")
+    if reflib.have_ref("f32"):
+        ref = reflib.RefEngine("f32")
+        a, _ = ref.narrowphase(A.ALGO_CAPSULE_VS_CONVEX_POLYHEDRON, _remap_meshes(sh, _register_hulls(ref)),
+                               b.slice(0, b.n))
+        _assert_same(got, a, what="grazing capsules vs reference")

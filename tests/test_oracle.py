@@ -102,3 +102,24 @@ def test_planted_mistake_is_caught(port_hulls):
     k = int(np.argmax(got.nb_contacts > 0))
     got.normal_depth[0, k, 3] = np.nextafter(got.normal_depth[0, k, 3], np.float32(np.inf))
     assert reflib.compare_contacts(got, exp, exp.n)["normal_depth"] == 1
+
+
+@pytest.mark.skipif(not reflib.have_ref("f32"), reason="reference build oracle/_ref not present")
+def test_grazing_capsule_clip_matches_reference(port):
+    """clipSegmentWithPlanes' one-vertex branch (segment nearly parallel to a
+    side plane): the next plane reads the array's stale second slot."""
+    ref = reflib.RefEngine("f32")
+    sh = edgecases.shape_table()
+    ids = []
+    for e in (ref, port):
+        if e is port:
+            port.lib.rp3do_reset()
+        v, f = edgecases.load_hull()
+        m = e.create_convex_mesh(v, f)
+        ids.append((e.create_convex_mesh_shape(m), e.create_convex_mesh_shape(m, edgecases.HULL_SCALE)))
+    b = edgecases.grazing_capsule_batch(4096, seed=5)
+    a, _ = ref.narrowphase(A.ALGO_CAPSULE_VS_CONVEX_POLYHEDRON, sh, b.slice(0, b.n))
+    c, _ = port.narrowphase(A.ALGO_CAPSULE_VS_CONVEX_POLYHEDRON, sh, b.slice(0, b.n))
+    assert reflib.compare_contacts(c, a, b.n) == {k: 0 for k in ("is_colliding", "nb_contacts", "normal_depth",
+                                                                  "local1", "local2")}
+    assert (a.nb_contacts == 1).sum() > 100 and (a.nb_contacts == 2).sum() > 100
