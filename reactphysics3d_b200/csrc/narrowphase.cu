@@ -472,33 +472,6 @@ cudaError_t launch_narrowphase_tri(int algo, const NpArgs& args, int num_sms, cu
     return cudaLaunchKernel(k, dim3(blocks), dim3(NP_BLOCK), params, smem, stream);
 }
 
-// Learned proposals of a polyhedron batch: per tile of 32 pairs the warp
-// computes the features and runs the MLP on the bf16 tensor cores; one class
-// byte per pair (15 = none).
-__global__ void __launch_bounds__(NP_BLOCK) narrowphase_propose(const NpArgs a, uint8_t* __restrict__ proposals) {
-    __shared__ float s_feat[NP_BLOCK / 32][32][MLP_KPAD];
-    __shared__ uint32_t s_cls[NP_BLOCK / 32][32];
-    __shared__ BoxTables s_box;
-    {
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(&c_box_tables);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(&s_box);
-        for (uint32_t k = threadIdx.x; k < sizeof(BoxTables) / 4; k += blockDim.x) dst[k] = src[k];
-        __syncthreads();
-    }
-    const MlpPacked& w = *static_cast<const MlpPacked*>(a.mlp);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t nwarps = gridDim.x * (NP_BLOCK / 32);
-    for (uint32_t tile = blockIdx.x * (NP_BLOCK / 32) + warp; tile * 32u < a.n; tile += nwarps) {
-        const uint32_t i = tile * 32u + lane;
-        pair_features(a, i, &s_box, a.mesh_words, s_feat[warp][lane]);
-        __syncwarp();
-        uint32_t c = mlp_infer_tile(s_feat[warp], w, lane, s_cls[warp]);
-        if (c >= MLP_OUT) c = MLP_NO_PROPOSAL;
-        if (i < a.n) proposals[i] = uint8_t(c);
-        __syncwarp();
-    }
-}
-
 // Counting sort of a polyhedron batch's pairs by learned class, so that a
 // tile of 32 pairs holds pairs of one class: the predicted-colliding pairs
 // (class 15: full SAT and clipping) share tiles, and pairs whose proposal
@@ -559,11 +532,73 @@ cudaError_t launch_partition_by_class(const NpArgs& a, const uint8_t* cls, uint3
     return cudaGetLastError();
 }
 
-cudaError_t launch_narrowphase_propose(const NpArgs& args, uint8_t* proposals, int num_sms, cudaStream_t stream) {
+// Classification of a polyhedron batch before its SAT kernels, per tile of
+// 32 pairs (one warp):
+//   - the geometric class of a box-box pair: its inscribed spheres overlap
+//     (certainly colliding: full SAT and clipping), its bounding spheres are
+//     apart (certainly separated: a face test ends it), or neither;
+//   - with the learned proposal on, the warp also computes the pairs'
+//     features and runs the MLP on the bf16 tensor cores (mma.sync
+//     m16n8k16, 112 MMAs per tile) and writes each pair's proposed feature
+//     (15 = none) to `proposals`, which the SAT kernels test exactly.
+// `key` receives the order class that partition_count / partition_scatter
+// sort by (class 15 first, then 0..14): plain SAT groups certainly colliding
+// (15), uncertain (0) and certainly separated (1) pairs; the learned path
+// groups by proposal, with the pairs it proposes nothing for among the
+// colliding ones unless they are certainly separated.  Only the order in
+// which the pairs are processed depends on the key.
+RD uint8_t box_pair_class(const NpArgs& a, uint32_t i) {
+    if (i >= a.n) return 0;
+    const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
+    if (uint32_t(i1) >= a.nb_shapes || uint32_t(i2) >= a.nb_shapes) return 0;
+    const ShapeRec r1 = load_shape(a.shapes, i1), r2 = load_shape(a.shapes, i2);
+    if (r1.kind != RP3DG_SHAPE_BOX || r2.kind != RP3DG_SHAPE_BOX) return 0;
+    const float4 p1 = a.pos1[i], p2 = a.pos2[i];
+    const float dx = p2.x - p1.x, dy = p2.y - p1.y, dz = p2.z - p1.z;
+    const float d2 = dx * dx + dy * dy + dz * dz;
+    const float4 h1 = r1.params, h2 = r2.params;
+    const float R = sqrtf(h1.x * h1.x + h1.y * h1.y + h1.z * h1.z) + sqrtf(h2.x * h2.x + h2.y * h2.y + h2.z * h2.z);
+    const float r = fminf(h1.x, fminf(h1.y, h1.z)) + fminf(h2.x, fminf(h2.y, h2.z));
+    return d2 > R * R * 1.0001f ? 1 : (d2 < r * r * 0.9999f ? 15 : 0);
+}
+
+__global__ void __launch_bounds__(NP_BLOCK) classify_pairs(const NpArgs a, uint8_t* __restrict__ key,
+                                                           uint8_t* __restrict__ proposals) {
+    __shared__ float s_feat[NP_BLOCK / 32][32][MLP_KPAD];
+    __shared__ uint32_t s_cls[NP_BLOCK / 32][32];
+    __shared__ BoxTables s_box;
+    const bool learned = a.mlp != nullptr && proposals != nullptr;
+    if (learned) {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&c_box_tables);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&s_box);
+        for (uint32_t k = threadIdx.x; k < sizeof(BoxTables) / 4; k += blockDim.x) dst[k] = src[k];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t nwarps = gridDim.x * (NP_BLOCK / 32);
+    for (uint32_t tile = blockIdx.x * (NP_BLOCK / 32) + warp; tile * 32u < a.n; tile += nwarps) {
+        const uint32_t i = tile * 32u + lane;
+        const uint8_t geo = box_pair_class(a, i);
+        uint8_t k = geo;
+        if (learned) {
+            pair_features(a, i, &s_box, a.mesh_words, s_feat[warp][lane]);
+            __syncwarp();
+            uint32_t c = mlp_infer_tile(s_feat[warp], *static_cast<const MlpPacked*>(a.mlp), lane, s_cls[warp]);
+            if (c >= MLP_OUT) c = MLP_NO_PROPOSAL;
+            if (i < a.n) proposals[i] = uint8_t(c);
+            k = (geo == 15 || c >= 15) ? (geo == 1 ? uint8_t(1) : uint8_t(15)) : uint8_t(c);
+            __syncwarp();
+        }
+        if (i < a.n) key[i] = k;
+    }
+}
+
+cudaError_t launch_classify_pairs(const NpArgs& args, uint8_t* key, uint8_t* proposals, int num_sms,
+                                  cudaStream_t stream) {
     if (args.n == 0) return cudaSuccess;
     const uint32_t blocks_needed = (args.n + NP_BLOCK - 1) / NP_BLOCK;
     const uint32_t cap = uint32_t(num_sms) * 16u;
-    narrowphase_propose<<<blocks_needed < cap ? blocks_needed : cap, NP_BLOCK, 0, stream>>>(args, proposals);
+    classify_pairs<<<blocks_needed < cap ? blocks_needed : cap, NP_BLOCK, 0, stream>>>(args, key, proposals);
     return cudaGetLastError();
 }
 

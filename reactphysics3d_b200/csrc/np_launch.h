@@ -66,10 +66,13 @@ cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaSt
 // words.
 cudaError_t launch_partition_by_class(const NpArgs& a, const uint8_t* cls, uint32_t* counts, uint32_t* perm,
                                       cudaStream_t stream);
+// Order key of every pair of a polyhedron batch (launch_partition_by_class
+// then sorts by it) and, with args.mlp set and proposals non-null, the
+// learned proposal of every pair (MLP inference on the tensor cores).
+cudaError_t launch_classify_pairs(const NpArgs& a, uint8_t* key, uint8_t* proposals, int num_sms, cudaStream_t stream);
 // Triangle tests of one algorithm batch (4, 5 or 6), one test per thread.
 cudaError_t launch_narrowphase_tri(int algo, const NpArgs& args, int num_sms, cudaStream_t stream);
-// Learned proposals of a polyhedron batch (args.mlp must be set).
-cudaError_t launch_narrowphase_propose(const NpArgs& args, uint8_t* proposals, int num_sms, cudaStream_t stream);
+
 
 }  // namespace rp3dg
 

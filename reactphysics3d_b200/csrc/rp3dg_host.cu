@@ -700,6 +700,8 @@ int rp3dg_set_shapes(rp3dg_ctx* ctx, const rp3dg_shape* shapes, uint32_t nb) {
 
 namespace {
 int grow(rp3dg_ctx* ctx, void** buf, size_t* cap, size_t need, const char* what);
+// polyhedron batches of at least this many pairs are grouped by class
+constexpr uint32_t NP_GROUP_MIN_PAIRS = 4096;
 
 // Checks of a device-array narrow-phase call and the kernel arguments it gives
 // (learned proposals off); returns 0 or an error code, 1 for an empty batch.
@@ -771,19 +773,26 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
     a.mlp = learned ? static_cast<const void*>(mlp_packed(ctx)) : nullptr;
     a.mlp_stats = learned ? mlp_stats(ctx) : nullptr;
     cudaSetDevice(ctx->device);
-    if (learned) {
-        // one proposal byte per pair, in a buffer that grows with the batch
+    // plain SAT on a large polyhedron batch: pairs grouped by a geometric
+    // class so that the thread-per-pair kernel's tiles are homogeneous
+    const bool grouped = !learned && algorithm == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON &&
+                         p->n >= NP_GROUP_MIN_PAIRS;
+    if (learned || grouped) {
+        // an order key and a proposal byte per pair, in a buffer that grows
+        // with the batch
         if (p->n > ctx->cap_proposals) {
             cudaFree(ctx->d_proposals);
             ctx->d_proposals = nullptr;
-            cudaError_t e = cudaMalloc(&ctx->d_proposals, p->n);
+            cudaError_t e = cudaMalloc(&ctx->d_proposals, 2 * size_t(p->n));
             if (e != cudaSuccess) { ctx->cap_proposals = 0; return cuda_fail(ctx, e, "cudaMalloc(proposals)"); }
             ctx->cap_proposals = p->n;
         }
-        cudaError_t e = rp3dg::launch_narrowphase_propose(a, ctx->d_proposals, ctx->num_sms, ctx->stream);
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "learned proposals");
+        uint8_t* key = ctx->d_proposals;
+        uint8_t* prop = ctx->d_proposals + p->n;
+        cudaError_t e = rp3dg::launch_classify_pairs(a, key, learned ? prop : nullptr, ctx->num_sms, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "pair classes");
         ctx->launches++;
-        a.proposals = ctx->d_proposals;
+        if (learned) a.proposals = prop;
         // tiles of one learned class each (the order only, not the results)
         if (p->n > ctx->cap_perm) {
             cudaFree(ctx->d_perm);
@@ -792,8 +801,8 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
             if (e != cudaSuccess) { ctx->cap_perm = 0; return cuda_fail(ctx, e, "cudaMalloc(pair order)"); }
             ctx->cap_perm = p->n;
         }
-        e = rp3dg::launch_partition_by_class(a, ctx->d_proposals, ctx->d_perm + p->n, ctx->d_perm, ctx->stream);
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "learned grouping");
+        e = rp3dg::launch_partition_by_class(a, key, ctx->d_perm + p->n, ctx->d_perm, ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "pair grouping");
         ctx->launches += 2;
         a.perm = ctx->d_perm;
     }
