@@ -550,7 +550,14 @@ typedef struct rp3dg_collider_desc {
     float mass_density;            /* Material::setMassDensity */
     uint16_t category;             /* collision category bits (0x0001 by default) */
     uint16_t mask;                 /* collide-with mask bits (0xffff by default) */
+    uint32_t flags;                /* RP3DG_COLLIDER_TRIGGER: Collider::setIsTrigger(true) after creation */
 } rp3dg_collider_desc;
+/* A trigger collider (Collider::setIsTrigger, Collider.cpp:250-257) is not a
+ * simulation collider: its pairs are tested without contact points, a
+ * colliding one becomes a contact pair that no island takes, and the world
+ * reports it through rp3dg_world_get_trigger_events instead of the contact
+ * events.  It still counts for the body's mass properties. */
+#define RP3DG_COLLIDER_TRIGGER 1u
 
 /* A joint, as PhysicsWorld::createJoint(JointInfo) (PhysicsWorld.cpp:467-580)
  * creates it from a BallAndSocketJointInfo / HingeJointInfo / FixedJointInfo /
@@ -687,6 +694,16 @@ typedef struct rp3dg_contact_event {
 int rp3dg_world_get_contact_events(rp3dg_world* world, uint32_t world_index, rp3dg_contact_event* events,
                                    uint32_t capacity, float* normal_depth, float* local1, float* local2,
                                    uint32_t capacity_points, uint32_t* nb_events, uint32_t* nb_points);
+
+/* The trigger events of the last update: EventListener::onTrigger through
+ * CollisionDetectionSystem::reportTriggers (CollisionDetectionSystem.cpp:
+ * 1745-1757) and OverlapCallback::CallbackData (OverlapCallback.cpp:70-92):
+ * the contact pairs of trigger colliders in creation order (type
+ * RP3DG_CONTACT_START for OverlapStart, RP3DG_CONTACT_STAY for OverlapStay),
+ * then the lost ones (RP3DG_CONTACT_EXIT for OverlapExit); no points.  The
+ * contact events leave trigger pairs out (CollisionCallback.cpp:84-103). */
+int rp3dg_world_get_trigger_events(rp3dg_world* world, uint32_t world_index, rp3dg_contact_event* events,
+                                   uint32_t capacity, uint32_t* nb_events);
 
 /* PhysicsWorld::raycast(ray, callback, raycastWithCategoryMaskBits)
  * (PhysicsWorld.h:486-490) for a batch of rays, each traced as the reference

@@ -62,8 +62,26 @@ struct EventRecorder : public EventListener {
     const std::vector<RigidBody*>* bodies = nullptr;
     const std::vector<Collider*>* colliders = nullptr;
     std::vector<rp3dg_contact_event> events;
+    std::vector<rp3dg_contact_event> triggers;   // EventListener::onTrigger, no points
     std::vector<float> nd, l1, l2;
-    void clear() { events.clear(); nd.clear(); l1.clear(); l2.clear(); }
+    void clear() { events.clear(); triggers.clear(); nd.clear(); l1.clear(); l2.clear(); }
+    void onTrigger(const OverlapCallback::CallbackData& data) override {
+        std::unordered_map<const void*, int32_t> bi, ci;
+        for (size_t i = 0; i < bodies->size(); i++) bi[static_cast<const void*>(static_cast<Body*>((*bodies)[i]))] = int32_t(i);
+        for (size_t i = 0; i < colliders->size(); i++) ci[static_cast<const void*>((*colliders)[i])] = int32_t(i);
+        for (uint32 k = 0; k < data.getNbOverlappingPairs(); k++) {
+            const OverlapCallback::OverlapPair pair = data.getOverlappingPair(k);
+            rp3dg_contact_event ev{};
+            ev.body1 = bi.at(static_cast<const void*>(pair.getBody1()));
+            ev.body2 = bi.at(static_cast<const void*>(pair.getBody2()));
+            ev.collider1 = ci.at(static_cast<const void*>(pair.getCollider1()));
+            ev.collider2 = ci.at(static_cast<const void*>(pair.getCollider2()));
+            const auto t = pair.getEventType();
+            ev.type = t == OverlapCallback::OverlapPair::EventType::OverlapStart ? 0
+                    : (t == OverlapCallback::OverlapPair::EventType::OverlapStay ? 1 : 2);
+            triggers.push_back(ev);
+        }
+    }
     void onContact(const CollisionCallback::CallbackData& data) override {
         std::unordered_map<const void*, int32_t> bi, ci;
         for (size_t i = 0; i < bodies->size(); i++) bi[static_cast<const void*>(static_cast<Body*>((*bodies)[i]))] = int32_t(i);
@@ -450,6 +468,15 @@ int ref_world_step(int id, float dt, int nsteps) {
     return 0;
 }
 
+// The trigger events of the last update (EventListener::onTrigger).
+int ref_scene_trigger_events(int id, rp3dg_contact_event* events, uint32_t cap, uint32_t* nb_events) {
+    World& W = *worlds().at(size_t(id));
+    const EventRecorder& R = W.recorder;
+    *nb_events = uint32_t(R.triggers.size());
+    for (size_t k = 0; k < R.triggers.size() && k < cap; k++) events[k] = R.triggers[k];
+    return 0;
+}
+
 // The contact events of the last update (counts always written).
 int ref_scene_events(int id, rp3dg_contact_event* events, uint32_t cap, float* nd, float* l1, float* l2,
                      uint32_t cap_points, uint32_t* nb_events, uint32_t* nb_points) {
@@ -668,6 +695,7 @@ int ref_scene_create(const rp3dg_world_settings* s, const rp3dg_shape* shapes, u
             col->getMaterial().setMassDensity(c.mass_density);
             col->setCollisionCategoryBits(c.category);
             col->setCollideWithMaskBits(c.mask);
+            if (c.flags & RP3DG_COLLIDER_TRIGGER) col->setIsTrigger(true);
             W->colliders.push_back(col);
             ci++;
         }

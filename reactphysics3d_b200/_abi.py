@@ -126,7 +126,8 @@ BODY_DESC_DTYPE = np.dtype([
 COLLIDER_DESC_DTYPE = np.dtype([
     ("body", "<i4"), ("shape", "<i4"), ("position", "<f4", (3,)), ("orientation", "<f4", (4,)),
     ("friction", "<f4"), ("bounciness", "<f4"), ("mass_density", "<f4"),
-    ("category", "<u2"), ("mask", "<u2")])
+    ("category", "<u2"), ("mask", "<u2"), ("flags", "<u4")])
+COLLIDER_TRIGGER = 1
 WORLD_STATS_DTYPE = np.dtype([(k, "<u4") for k in (
     "overlapping_pairs", "disabled_pairs", "narrowphase_tests", "contact_pairs", "manifolds",
     "contact_points", "islands", "enabled_bodies", "moved_colliders", "reserved")])
@@ -148,7 +149,7 @@ RAYCAST_HIT_DTYPE = np.dtype([("world_point", "<f4", (3,)), ("world_normal", "<f
                               ("body", "<i4"), ("collider", "<i4"), ("flags", "<i4")])
 assert RAY_DTYPE.itemsize == 32 and RAYCAST_HIT_DTYPE.itemsize == 40
 assert WORLD_SETTINGS_DTYPE.itemsize == 48 and BODY_DESC_DTYPE.itemsize == 96
-assert COLLIDER_DESC_DTYPE.itemsize == 52 and WORLD_STATS_DTYPE.itemsize == 40
+assert COLLIDER_DESC_DTYPE.itemsize == 56 and WORLD_STATS_DTYPE.itemsize == 40
 
 
 def default_world_settings():

@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(128) hf_tests_kernel(const HfTestArgs a) {
     a.r1[t] = a.c_wori[row1];
     a.p2[t] = a.c_wpos[row2];
     a.r2[t] = a.c_wori[row2];
-    a.report[t] = 1;
+    a.report[t] = (it.w & HF_NO_REPORT) ? 0 : 1;
     // the record of this triangle: kept from the previous step when the
     // triangle was tested then, else a new LastFrameCollisionInfo
     // (OverlappingPairs.h:86-91)

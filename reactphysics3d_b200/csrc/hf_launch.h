@@ -13,6 +13,7 @@ namespace rp3dg {
 //   item = (convex collider row, concave collider row, height-field id,
 //           flags: bit 0 = shape 1 is the convex one)
 constexpr int HF_SHAPE1_CONVEX = 1;
+constexpr int HF_NO_REPORT = 2;   // a collider of the pair is a trigger: no contact points
 constexpr uint32_t HF_MAX_MANIFOLDS = 4;   // NB_MAX_CONTACT_MANIFOLDS (configuration.h:137)
 constexpr uint32_t HF_OUT_POINTS = 16;     // 4 manifolds x 4 points per pair
 

@@ -451,6 +451,7 @@ struct ColliderH {
     int hf = -1;         // height-field id of a concave collider
     int bp = -1;  // broad-phase id (tree leaf)
     uint16_t category = 1, mask = 0xffff;
+    bool trigger = false;  // Collider::setIsTrigger: not a simulation collider
     std::vector<uint64_t> pairs;  // ColliderComponents::mOverlappingPairs
 };
 struct PairH {
@@ -477,6 +478,7 @@ struct ContactPairH {
     uint32_t k;          // points of all its manifolds after the manifold step
     bool in_island = false;
     bool prev = false;   // ContactPair::collidingInPreviousFrame (the overlapping pair's, at creation)
+    bool trigger = false;  // ContactPair::isTrigger: one collider is a trigger (no points, no island)
     uint32_t manifold = 0, point = 0;  // global indices in the packed arrays
 };
 struct IslandH {
@@ -916,6 +918,7 @@ void add_lost(WorldH& w, const PairH& p) {
     c.b2 = w.colliders[size_t(p.c2)].body;
     c.prev = true;
     c.k = 0;
+    c.trigger = w.colliders[size_t(p.c1)].trigger || w.colliders[size_t(p.c2)].trigger;
     w.lost.push_back(c);
 }
 
@@ -1198,8 +1201,10 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
         const bool e1 = w.ccomp.enabled(p.c1), e2 = w.ccomp.enabled(p.c2);
         if (!(e1 || e2)) continue;
         const int a = p.algo - 1;
+        // reportContacts is off when a collider is a trigger (:402)
+        const bool trig = w.colliders[size_t(p.c1)].trigger || w.colliders[size_t(p.c2)].trigger;
         w.items[a].push_back(make_int4(int(w.c0) + w.ccomp.slot[size_t(p.c1)], int(w.c0) + w.ccomp.slot[size_t(p.c2)],
-                                       p.cache, 1));
+                                       p.cache, trig ? 0 : 1));
         w.item_pair[a].push_back(i);
     }
     // convex vs concave pairs (computeMiddlePhase :412-456): a pair that is
@@ -1214,8 +1219,10 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
         }
         const int cv = p.shape1_convex ? p.c1 : p.c2, cc = p.shape1_convex ? p.c2 : p.c1;
         const int a = p.algo - 1;
+        const bool trig = w.colliders[size_t(p.c1)].trigger || w.colliders[size_t(p.c2)].trigger;
         w.hitems[a].push_back(make_int4(int(w.c0) + w.ccomp.slot[size_t(cv)], int(w.c0) + w.ccomp.slot[size_t(cc)],
-                                        w.colliders[size_t(cc)].hf, p.shape1_convex ? HF_SHAPE1_CONVEX : 0));
+                                        w.colliders[size_t(cc)].hf,
+                                        (p.shape1_convex ? HF_SHAPE1_CONVEX : 0) | (trig ? HF_NO_REPORT : 0)));
         w.hitem_pair[a].push_back(i);
     }
     if (g->profiling) {
@@ -1250,6 +1257,8 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
             c.item = it;
             c.k = h_count[it];
             c.npts = c.k;
+            c.trigger = w.colliders[size_t(p.c1)].trigger || w.colliders[size_t(p.c2)].trigger;
+            if (c.trigger) c.nman = 0;   // a trigger pair has no contact points, so no manifold
             w.cpairs.push_back(c);
         }
         const uint32_t hbase = g->hitem_start[a] + w.hitem_off[a];
@@ -1267,7 +1276,8 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
             c.b2 = w.colliders[size_t(p.c2)].body;
             c.item = it;
             c.concave = true;
-            c.nman = h_hnman[it];
+            c.trigger = w.colliders[size_t(p.c1)].trigger || w.colliders[size_t(p.c2)].trigger;
+            c.nman = c.trigger ? 0u : h_hnman[it];
             c.k = 0;
             c.npts = 0;
             for (uint32_t m = 0; m < c.nman; m++) {
@@ -1324,6 +1334,8 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
                 ContactPairH& cp = w.cpairs[cpi];
                 if (cp.in_island) continue;
                 cp.in_island = true;
+                // both colliders must be simulation colliders (:788-790)
+                if (cp.trigger) continue;
                 const int other = cp.b1 == b ? cp.b2 : cp.b1;
                 if (w.bodies[size_t(other)].has_sim_collider) {
                     w.island_order.push_back(cpi);
@@ -1826,9 +1838,13 @@ int build_world(Group* g, WorldH& w, const rp3dg_body_desc* bd, uint32_t nb, con
             C.hf = C.convex ? -1 : g->shapes[size_t(c.shape)].mesh;
             C.category = c.category;
             C.mask = c.mask;
+            // addCollider, then setIsTrigger(true): the collider stops being a
+            // simulation collider and the body keeps one only if another
+            // collider is (Collider.cpp:250-257, Body::updateHasSimulationCollider)
+            C.trigger = (c.flags & RP3DG_COLLIDER_TRIGGER) != 0;
             w.ccomp.add(int(ci), !w.bcomp.enabled(int(b)));
             B.colliders.push_back(int(ci));
-            B.has_sim_collider = true;
+            if (!C.trigger) B.has_sim_collider = true;
             ccols[CC_LPOS][ci] = make_float4(c.position[0], c.position[1], c.position[2], 0.f);
             ccols[CC_LORI][ci] = make_float4(c.orientation[0], c.orientation[1], c.orientation[2], c.orientation[3]);
             // Material::mFrictionCoefficientSqrt = sqrt(friction)
@@ -3088,10 +3104,14 @@ int rp3dg_world_get_contact_events(rp3dg_world* g, uint32_t world, rp3dg_contact
     const ContactBuf& B = g->cbuf[1 - g->cur_cb];
     const WorldH& w = g->worlds[world];
     const std::vector<ContactPairH>& cps = w.prev_cpairs;
-    const uint32_t ne = uint32_t(cps.size() + w.lost.size());
-    uint32_t np = 0;
+    // CollisionCallback::CallbackData keeps the pairs that are not triggers
+    uint32_t ne = 0, np = 0;
     for (const ContactPairH& c : cps)
-        if (c.in_island) np += c.k;
+        if (!c.trigger) {
+            ne++;
+            if (c.in_island) np += c.k;
+        }
+    for (const ContactPairH& c : w.lost) ne += c.trigger ? 0u : 1u;
     if (nb_events) *nb_events = ne;
     if (nb_points) *nb_points = np;
     // the step's packed points of this world, then gathered pair by pair
@@ -3129,8 +3149,38 @@ int rp3dg_world_get_contact_events(rp3dg_world* g, uint32_t world, rp3dg_contact
         }
         k++;
     };
-    for (const ContactPairH& c : cps) emit(c, c.prev ? RP3DG_CONTACT_STAY : RP3DG_CONTACT_START, c.in_island);
-    for (const ContactPairH& c : w.lost) emit(c, RP3DG_CONTACT_EXIT, false);
+    for (const ContactPairH& c : cps)
+        if (!c.trigger) emit(c, c.prev ? RP3DG_CONTACT_STAY : RP3DG_CONTACT_START, c.in_island);
+    for (const ContactPairH& c : w.lost)
+        if (!c.trigger) emit(c, RP3DG_CONTACT_EXIT, false);
+    return 0;
+}
+
+int rp3dg_world_get_trigger_events(rp3dg_world* g, uint32_t world, rp3dg_contact_event* events, uint32_t capacity,
+                                   uint32_t* nb_events) {
+    if (!g || world >= g->worlds.size() || (capacity && !events)) return RP3DG_EINVAL;
+    const WorldH& w = g->worlds[world];
+    uint32_t k = 0;
+    auto emit = [&](const ContactPairH& c, int type) {
+        if (k < capacity) {
+            rp3dg_contact_event& ev = events[k];
+            ev.body1 = c.b1;
+            ev.body2 = c.b2;
+            ev.collider1 = c.c1;
+            ev.collider2 = c.c2;
+            ev.type = type;
+            ev.first_point = 0;
+            ev.nb_points = 0;
+        }
+        k++;
+    };
+    // OverlapCallback::CallbackData with onlyReportTriggers: the trigger
+    // contact pairs, then the lost trigger pairs
+    for (const ContactPairH& c : w.prev_cpairs)
+        if (c.trigger) emit(c, c.prev ? RP3DG_CONTACT_STAY : RP3DG_CONTACT_START);
+    for (const ContactPairH& c : w.lost)
+        if (c.trigger) emit(c, RP3DG_CONTACT_EXIT);
+    if (nb_events) *nb_events = k;
     return 0;
 }
 

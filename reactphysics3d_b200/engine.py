@@ -117,6 +117,7 @@ def load_library(path=LIB_PATH):
     L.rp3dg_world_set_motor_speed.argtypes = [P, C.c_uint32, C.c_uint32, C.c_float]
     L.rp3dg_world_get_contact_events.argtypes = [P, C.c_uint32, P, C.c_uint32, P, P, P, C.c_uint32,
                                                  C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+    L.rp3dg_world_get_trigger_events.argtypes = [P, C.c_uint32, P, C.c_uint32, C.POINTER(C.c_uint32)]
     L.rp3dg_world_raycast.argtypes = [P, C.c_uint32, P, C.c_uint32, C.c_int32, C.c_uint32, P, P]
     L.rp3dg_world_raycast_device.argtypes = [P, C.c_uint32, P, C.c_uint32, C.c_int32, C.c_uint32, P, P,
                                              C.POINTER(C.c_float)]
@@ -561,6 +562,20 @@ class World:
         if rc != 0:
             raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
         return ev, nd, l1, l2
+
+    def trigger_events(self, world=0):
+        """The trigger events of the last update (structured array of
+        A.CONTACT_EVENT_DTYPE, no points)."""
+        n = C.c_uint32()
+        rc = self.lib.rp3dg_world_get_trigger_events(self.h, int(world), None, 0, C.byref(n))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+        ev = np.zeros(n.value, A.CONTACT_EVENT_DTYPE)
+        rc = self.lib.rp3dg_world_get_trigger_events(self.h, int(world), ev.ctypes.data if len(ev) else None, len(ev),
+                                                     C.byref(n))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+        return ev
 
     def raycast(self, rays, mode=A.RAYCAST_CLOSEST, max_hits=1, world=0):
         """PhysicsWorld::raycast for each row of `rays` (A.RAY_DTYPE) with the

@@ -741,3 +741,29 @@ def heightfield_world(n_bodies=1000, cols=64, rows=64, cell=1.0, seed=5, spacing
     settings["sleeping_enabled"] = 1 if sleeping else 0
     return WorldScene(settings, shapes, bodies, colliders, f"heightfield {cols}x{rows} + {n}",
                       heightfields=[(heights, (cell, y_scale, cell))])
+
+
+def with_triggers(scene, every=6, zones=((0.0, 2.0, 0.0, 2.5, 0.6, 2.5), (-3.0, 4.5, 1.0, 1.5, 1.5, 1.5))):
+    """A copy of `scene` with trigger colliders (Collider::setIsTrigger): every
+    `every`-th dynamic body's collider becomes a trigger (the body keeps its
+    mass, falls through everything and reports overlaps), and static trigger
+    boxes are added as sensor zones, one per (x, y, z, half-extent x, y, z)."""
+    shapes = np.concatenate([scene.shapes, np.zeros(len(zones), A.SHAPE_DTYPE)])
+    bodies = np.concatenate([scene.bodies, A.body_descs(len(zones))])
+    colliders = np.concatenate([scene.colliders, A.collider_descs(len(zones))])
+    dyn = np.flatnonzero(scene.bodies["type"] == A.BODY_DYNAMIC)
+    for b in dyn[::every]:
+        colliders["flags"][np.flatnonzero(scene.colliders["body"] == b)] |= A.COLLIDER_TRIGGER
+    ns, nb, nc = len(scene.shapes), len(scene.bodies), len(scene.colliders)
+    for k, (x, y, z, hx, hy, hz) in enumerate(zones):
+        shapes["kind"][ns + k] = A.SHAPE_BOX
+        shapes["mesh"][ns + k] = -1
+        shapes["params"][ns + k, :3] = (hx, hy, hz)
+        bodies["type"][nb + k] = A.BODY_STATIC
+        bodies["position"][nb + k] = (x, y, z)
+        colliders["body"][nc + k] = nb + k
+        colliders["shape"][nc + k] = ns + k
+        colliders["flags"][nc + k] = A.COLLIDER_TRIGGER
+    return WorldScene(scene.settings, shapes, bodies, colliders, scene.name + " with triggers",
+                      getattr(scene, "joints", None), getattr(scene, "heightfields", None),
+                      getattr(scene, "convex_meshes", None))

@@ -283,6 +283,7 @@ class RefScene:
         L.ref_scene_set_motor_speed.argtypes = [C.c_int, C.c_uint32, C.c_float]
         L.ref_scene_raycast.argtypes = [C.c_int, P, C.c_uint32, C.c_int, C.c_uint32, P, P]
         L.ref_scene_events.argtypes = [C.c_int, P, C.c_uint32, P, P, P, C.c_uint32, P, P]
+        L.ref_scene_trigger_events.argtypes = [C.c_int, P, C.c_uint32, P]
         L.ref_convex_register.argtypes = [P, C.c_uint32, P, P, C.c_uint32, C.c_float, C.c_float, C.c_float]
         L.ref_heightfield_register.argtypes = [C.c_uint32, C.c_uint32, P, C.c_float, C.c_float, C.c_float]
         # height fields of the scene registered with the harness; the shape
@@ -326,6 +327,13 @@ class RefScene:
         self.lib.ref_scene_events(self.id, ev.ctypes.data, len(ev), nd.ctypes.data, l1.ctypes.data, l2.ctypes.data,
                                   len(nd), C.byref(ne), C.byref(npt))
         return ev, nd, l1, l2
+
+    def trigger_events(self):
+        n = C.c_uint32()
+        self.lib.ref_scene_trigger_events(self.id, None, 0, C.byref(n))
+        ev = np.zeros(n.value, A.CONTACT_EVENT_DTYPE)
+        self.lib.ref_scene_trigger_events(self.id, ev.ctypes.data if len(ev) else None, len(ev), C.byref(n))
+        return ev
 
     def raycast(self, rays, mode=A.RAYCAST_CLOSEST, max_hits=1):
         r = np.ascontiguousarray(rays, dtype=A.RAY_DTYPE)
