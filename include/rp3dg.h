@@ -56,7 +56,8 @@ enum rp3dg_shape_kind {
     RP3DG_SHAPE_CAPSULE = 1,
     RP3DG_SHAPE_BOX = 2,
     RP3DG_SHAPE_CONVEX_MESH = 3,
-    RP3DG_SHAPE_HEIGHTFIELD = 4   /* CONCAVE_SHAPE / HEIGHTFIELD */
+    RP3DG_SHAPE_HEIGHTFIELD = 4,  /* CONCAVE_SHAPE / HEIGHTFIELD */
+    RP3DG_SHAPE_CONCAVE_MESH = 5  /* CONCAVE_SHAPE / TRIANGLE_MESH */
 };
 
 /* Narrow-phase algorithms, same numbering as the reference's
@@ -83,7 +84,10 @@ typedef struct rp3dg_float4 { float x, y, z, w; } rp3dg_float4;
  *                 rp3dg_create_convex_mesh_shape (mesh + scale instance)
  *   height field: params unused; mesh = index returned by
  *                 rp3dg_create_heightfield (a concave shape: it collides
- *                 only inside a world, through the middle phase) */
+ *                 only inside a world, through the middle phase)
+ *   concave mesh: params unused; mesh = index returned by
+ *                 rp3dg_create_concave_mesh_shape (concave, like a height
+ *                 field) */
 typedef struct rp3dg_shape {
     float params[4];
     int32_t kind;
@@ -193,6 +197,31 @@ int rp3dg_get_convex_mesh_tables(rp3dg_ctx* ctx, int32_t instance_id,
  * rp3dg_shape.mesh with kind RP3DG_SHAPE_HEIGHTFIELD. */
 int rp3dg_create_heightfield(rp3dg_ctx* ctx, uint32_t nb_columns, uint32_t nb_rows, const float* heights,
                              float sx, float sy, float sz, int32_t* heightfield_id);
+
+/* Triangle mesh: replaces PhysicsCommon::createTriangleMesh(
+ * TriangleVertexArray(nb_vertices, vertices, 12, nb_triangles, indices, 12,
+ * VERTEX_FLOAT_TYPE, INDEX_INTEGER_TYPE[, normals, 12, NORMAL_FLOAT_TYPE]),
+ * messages) (TriangleMesh::init, TriangleMesh.cpp:42-67): triangles of
+ * almost zero area or with an almost zero edge dropped, unused vertices
+ * removed (:91-240), angle-weighted vertex normals when `normals` is NULL
+ * (:277-333), and the DynamicAABBTree of the triangles built on the host by
+ * inserting them in order (:242-266).  vertices: nb_vertices * 3 floats;
+ * indices: 3 per triangle.  RP3DG_EINVAL where the reference's mesh is
+ * invalid (an index out of range, no triangle left, a normal too short). */
+int rp3dg_create_triangle_mesh(rp3dg_ctx* ctx, const float* vertices, uint32_t nb_vertices, const uint32_t* indices,
+                               uint32_t nb_triangles, const float* normals, int32_t* mesh_id);
+/* Concave mesh shape = triangle mesh + scale: replaces
+ * PhysicsCommon::createConcaveMeshShape(TriangleMesh*, const Vector3& scaling)
+ * (scaled vertex normals ConcaveMeshShape.cpp:56-76).  Returns the instance
+ * id to store in rp3dg_shape.mesh with kind RP3DG_SHAPE_CONCAVE_MESH. */
+int rp3dg_create_concave_mesh_shape(rp3dg_ctx* ctx, int32_t mesh_id, float sx, float sy, float sz,
+                                    int32_t* instance_id);
+/* Read back a triangle mesh as built (for parity checks): its vertices and
+ * vertex normals (3 floats each) and triangles (3 indices), up to the
+ * capacities; the counts are always written. */
+int rp3dg_get_triangle_mesh(rp3dg_ctx* ctx, int32_t mesh_id, uint32_t* nb_vertices, uint32_t* nb_triangles,
+                            float* vertices, float* normals, uint32_t* triangles, uint32_t capacity_vertices,
+                            uint32_t capacity_triangles);
 
 /* Replace the context's shape table (device copy of `shapes`). */
 int rp3dg_set_shapes(rp3dg_ctx* ctx, const rp3dg_shape* shapes, uint32_t nb_shapes);
@@ -704,6 +733,53 @@ int rp3dg_world_get_contact_events(rp3dg_world* world, uint32_t world_index, rp3
  * contact events leave trigger pairs out (CollisionCallback.cpp:84-103). */
 int rp3dg_world_get_trigger_events(rp3dg_world* world, uint32_t world_index, rp3dg_contact_event* events,
                                    uint32_t capacity, uint32_t* nb_events);
+
+/* Debug rendering (DebugRenderer, src/utils/DebugRenderer.cpp) as headless
+ * buffers: the items of DebugRenderer::DebugItem (DebugRenderer.h:73-91). */
+#define RP3DG_DEBUG_COLLIDER_AABB            0x01u
+#define RP3DG_DEBUG_COLLIDER_BROADPHASE_AABB 0x02u
+#define RP3DG_DEBUG_COLLISION_SHAPE          0x04u
+#define RP3DG_DEBUG_CONTACT_POINT            0x08u
+#define RP3DG_DEBUG_CONTACT_NORMAL           0x10u
+#define RP3DG_DEBUG_COLLISION_SHAPE_NORMAL   0x20u
+/* DebugRenderer::DebugLine and DebugTriangle (DebugRenderer.h:95-146):
+ * points and 0xRRGGBB colours, the same 32- and 48-byte layouts. */
+typedef struct rp3dg_debug_line {
+    float p1[3];
+    uint32_t color1;
+    float p2[3];
+    uint32_t color2;
+} rp3dg_debug_line;
+typedef struct rp3dg_debug_triangle {
+    float p1[3];
+    uint32_t color1;
+    float p2[3];
+    uint32_t color2;
+    float p3[3];
+    uint32_t color3;
+} rp3dg_debug_triangle;
+/* PhysicsWorld::setIsDebugRenderingEnabled(items != 0) with
+ * DebugRenderer::setIsDebugItemDisplayed(item, true) for each RP3DG_DEBUG_*
+ * bit of `items` (every world of a group).  From the next update on, each
+ * update ends with the primitives of DebugRenderer::onContact (a sphere of
+ * radius 0.1 and a 1 m normal per contact point of the update's contact
+ * pairs, DebugRenderer.cpp:530-560) followed by those of
+ * computeDebugRenderingPrimitives (DebugRenderer.cpp:482-527: per body with
+ * debug enabled, per collider, its AABB, fat broad-phase AABB and shape
+ * triangles and face normals), with the default colours, computed on the GPU
+ * in the reference's order and arithmetic. */
+int rp3dg_world_set_debug_rendering(rp3dg_world* world, uint32_t items);
+/* Body::setIsDebugEnabled (Body.cpp:509-512; false for a new body) for body
+ * `body` of world `world_index`, or for every body of it when body < 0. */
+int rp3dg_world_set_body_debug(rp3dg_world* world, uint32_t world_index, int32_t body, int enabled);
+/* DebugRenderer::getLinesArray / getTrianglesArray after the last update of
+ * world `world_index`: up to cap_lines lines and cap_triangles triangles
+ * into `lines` / `triangles` (host memory, or device memory of the world's
+ * device when `device` is non-zero; either may be NULL with capacity 0); the
+ * counts are written even when the arrays are short. */
+int rp3dg_world_get_debug_primitives(rp3dg_world* world, uint32_t world_index, rp3dg_debug_line* lines,
+                                     uint32_t cap_lines, rp3dg_debug_triangle* triangles, uint32_t cap_triangles,
+                                     uint32_t* nb_lines, uint32_t* nb_triangles, int device);
 
 /* PhysicsWorld::raycast(ray, callback, raycastWithCategoryMaskBits)
  * (PhysicsWorld.h:486-490) for a batch of rays, each traced as the reference

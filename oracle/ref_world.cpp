@@ -632,6 +632,48 @@ int ref_heightfield_register(uint32_t ncol, uint32_t nrow, const float* heights,
     return int(heightfields().size()) - 1;
 }
 
+// PhysicsWorld::setIsDebugRenderingEnabled(items != 0) and
+// DebugRenderer::setIsDebugItemDisplayed for the six DebugItem bits.
+int ref_scene_set_debug(int id, uint32_t items) {
+    World& W = *worlds().at(size_t(id));
+    W.world->setIsDebugRenderingEnabled(items != 0);
+    DebugRenderer& r = W.world->getDebugRenderer();
+    for (uint32_t bit = 1; bit <= 32; bit <<= 1)
+        r.setIsDebugItemDisplayed(static_cast<DebugRenderer::DebugItem>(bit), (items & bit) != 0);
+    return 0;
+}
+
+// Body::setIsDebugEnabled for one body (body >= 0) or all of them.
+int ref_scene_set_body_debug(int id, int body, int enabled) {
+    World& W = *worlds().at(size_t(id));
+    for (size_t b = 0; b < W.bodies.size(); b++)
+        if (body < 0 || size_t(body) == b) W.bodies[b]->setIsDebugEnabled(enabled != 0);
+    return 0;
+}
+
+// DebugRenderer::getLinesArray / getTrianglesArray of the last update
+// (counts always written), converted field by field to the C-ABI structs.
+int ref_scene_debug_primitives(int id, rp3dg_debug_line* lines, uint32_t cap_lines, rp3dg_debug_triangle* tris,
+                               uint32_t cap_tris, uint32_t* nb_lines, uint32_t* nb_tris) {
+    World& W = *worlds().at(size_t(id));
+    DebugRenderer& r = W.world->getDebugRenderer();
+    *nb_lines = r.getNbLines();
+    *nb_tris = r.getNbTriangles();
+    auto put = [](float* o, const Vector3& v) { o[0] = float(v.x); o[1] = float(v.y); o[2] = float(v.z); };
+    const DebugRenderer::DebugLine* L = r.getLinesArray();
+    for (uint32_t k = 0; k < r.getNbLines() && k < cap_lines; k++) {
+        put(lines[k].p1, L[k].point1); lines[k].color1 = L[k].color1;
+        put(lines[k].p2, L[k].point2); lines[k].color2 = L[k].color2;
+    }
+    const DebugRenderer::DebugTriangle* T = r.getTrianglesArray();
+    for (uint32_t k = 0; k < r.getNbTriangles() && k < cap_tris; k++) {
+        put(tris[k].p1, T[k].point1); tris[k].color1 = T[k].color1;
+        put(tris[k].p2, T[k].point2); tris[k].color2 = T[k].color2;
+        put(tris[k].p3, T[k].point3); tris[k].color3 = T[k].color3;
+    }
+    return 0;
+}
+
 int ref_scene_create(const rp3dg_world_settings* s, const rp3dg_shape* shapes, uint32_t nshapes,
                      const rp3dg_body_desc* bd, uint32_t nb, const rp3dg_collider_desc* cd, uint32_t nc) {
     auto W = std::make_unique<World>();

@@ -148,6 +148,14 @@ RAY_DTYPE = np.dtype([("point1", "<f4", (3,)), ("point2", "<f4", (3,)), ("max_fr
 RAYCAST_HIT_DTYPE = np.dtype([("world_point", "<f4", (3,)), ("world_normal", "<f4", (3,)), ("hit_fraction", "<f4"),
                               ("body", "<i4"), ("collider", "<i4"), ("flags", "<i4")])
 assert RAY_DTYPE.itemsize == 32 and RAYCAST_HIT_DTYPE.itemsize == 40
+# DebugRenderer::DebugItem bits and DebugLine / DebugTriangle
+DEBUG_COLLIDER_AABB, DEBUG_COLLIDER_BROADPHASE_AABB, DEBUG_COLLISION_SHAPE = 0x01, 0x02, 0x04
+DEBUG_CONTACT_POINT, DEBUG_CONTACT_NORMAL, DEBUG_COLLISION_SHAPE_NORMAL = 0x08, 0x10, 0x20
+DEBUG_ALL = 0x3f
+DEBUG_LINE_DTYPE = np.dtype([("p1", "<f4", (3,)), ("color1", "<u4"), ("p2", "<f4", (3,)), ("color2", "<u4")])
+DEBUG_TRIANGLE_DTYPE = np.dtype([("p1", "<f4", (3,)), ("color1", "<u4"), ("p2", "<f4", (3,)), ("color2", "<u4"),
+                                 ("p3", "<f4", (3,)), ("color3", "<u4")])
+assert DEBUG_LINE_DTYPE.itemsize == 32 and DEBUG_TRIANGLE_DTYPE.itemsize == 48
 assert WORLD_SETTINGS_DTYPE.itemsize == 48 and BODY_DESC_DTYPE.itemsize == 96
 assert COLLIDER_DESC_DTYPE.itemsize == 56 and WORLD_STATS_DTYPE.itemsize == 40
 

@@ -21,7 +21,7 @@ LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "librp3dg.so")
 OBJDIR = os.path.join(HERE, "_build")
 SOURCES = ["rp3dg_host.cu", "narrowphase.cu", "narrowphase_events.cu", "peak.cu", "axis_mlp.cu", "contacts.cu", "dynamics.cu",
-           "broadphase.cu", "world.cu", "heightfield.cu", "raycast.cu"]
+           "broadphase.cu", "world.cu", "heightfield.cu", "raycast.cu", "debug.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 FP_FLAGS = ["--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]

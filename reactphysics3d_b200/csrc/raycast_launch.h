@@ -9,13 +9,8 @@
 
 namespace rp3dg {
 
-// One node of the world's dynamic AABB tree, as the ray traversal reads it:
-// lo = (fat AABB min, child 0), hi = (fat AABB max, child 1), the children as
-// int bits (-1: none).  A leaf has child 0 = -2 - collider index.
-struct __align__(16) RayNode {
-    float4 lo, hi;
-};
-
+// The world's dynamic AABB tree as RayNode records (rp3dg_internal.h): a
+// leaf has child 0 = -2 - collider index.
 // Per collider (creation order): x device row of its world transform,
 // y body index, z shape index, w collision category bits.
 struct RayArgs {

@@ -24,6 +24,7 @@
 #include "mlp_launch.h"
 #include "np_launch.h"
 #include "rp3dg_internal.h"
+#include "world_order.h"
 
 using rp3dg::BoxTables;
 using rp3dg::MeshHdr;
@@ -42,6 +43,17 @@ struct MeshTopo {
     float bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};  // ConvexMesh::mBounds
     float volume = 0.0f;                             // ConvexMesh::mVolume
     uint32_t nv = 0, nf = 0;
+};
+
+// TriangleMesh (TriangleMesh.h): the vertices and vertex normals left after
+// the unused ones were removed, the kept triangles, and the DynamicAABBTree
+// of the triangles as RayNode records
+struct TriMesh {
+    std::vector<float> verts, normals;   // 3 per vertex
+    std::vector<uint32_t> tris;          // 3 per triangle
+    std::vector<rp3dg::RayNode> nodes;
+    int32_t root = -1;
+    float bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};  // getBounds: the root's AABB
 };
 
 struct MeshInstance {
@@ -246,6 +258,10 @@ struct rp3dg_ctx {
     size_t cap_bp_stage = 0;
     // height fields (device heights in HfDesc::heights)
     std::vector<rp3dg::HfDesc> hfields;
+    // triangle meshes and concave mesh shape instances (device arrays in
+    // each CmDesc)
+    std::vector<TriMesh> trimeshes;
+    std::vector<rp3dg::CmDesc> cmeshes;
 };
 
 namespace {
@@ -374,9 +390,22 @@ int get_mesh_mass(rp3dg_ctx* ctx, int32_t instance, float* volume, float* extent
     for (int a = 0; a < 3; a++) extent[a] = (0.5f * in.scale[a]) * (m.bmax[a] - m.bmin[a]);
     return 0;
 }
+// face vertex counts of a convex-mesh instance (debug rendering)
+int get_mesh_face_counts(rp3dg_ctx* ctx, int32_t instance, std::vector<uint32_t>* counts) {
+    if (!ctx || !counts || instance < 0 || size_t(instance) >= ctx->instances.size()) return RP3DG_EINVAL;
+    const MeshTopo& m = ctx->meshes[size_t(ctx->instances[size_t(instance)].mesh)];
+    *counts = m.face_count;
+    return 0;
+}
 int get_mesh_arena_device(rp3dg_ctx* ctx, const uint32_t** words) {
     if (!ctx || !words) return RP3DG_EINVAL;
     *words = ctx->d_arena;
+    return 0;
+}
+// all concave mesh shape instances of the context, by id
+int get_cmeshes(rp3dg_ctx* ctx, std::vector<CmDesc>* out) {
+    if (!ctx || !out) return RP3DG_EINVAL;
+    *out = ctx->cmeshes;
     return 0;
 }
 // a height field of the context (world set-up and middle phase)
@@ -438,6 +467,12 @@ void rp3dg_destroy(rp3dg_ctx* ctx) {
     cudaFree(ctx->d_bp);
     cudaFree(ctx->d_bp_stage);
     for (auto& h : ctx->hfields) cudaFree(const_cast<float*>(h.heights));
+    for (auto& c : ctx->cmeshes) {
+        cudaFree(const_cast<uint32_t*>(c.tris));
+        cudaFree(const_cast<float*>(c.sverts));
+        cudaFree(const_cast<float*>(c.snormals));
+        cudaFree(const_cast<rp3dg::RayNode*>(c.nodes));
+    }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -627,11 +662,272 @@ int rp3dg_create_heightfield(rp3dg_ctx* ctx, uint32_t nb_columns, uint32_t nb_ro
     return 0;
 }
 
+namespace {
+float vlen3(const float* a) { return std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]); }
+float vdot3(const float* a, const float* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+void vsub3(const float* a, const float* b, float* o) { o[0] = a[0] - b[0]; o[1] = a[1] - b[1]; o[2] = a[2] - b[2]; }
+void vcross3(const float* a, const float* b, float* o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+// Vector3::normalize (Vector3.h:219-227): three divisions, short vectors kept
+void vnormalize3(float* a) {
+    const float l = vlen3(a);
+    if (l < FLT_EPSILON) return;
+    a[0] /= l;
+    a[1] /= l;
+    a[2] /= l;
+}
+float as_float(int v) {
+    float f;
+    std::memcpy(&f, &v, 4);
+    return f;
+}
+}  // namespace
+
+int rp3dg_create_triangle_mesh(rp3dg_ctx* ctx, const float* vertices, uint32_t nv, const uint32_t* indices,
+                               uint32_t nt, const float* normals, int32_t* mesh_id) {
+    if (!ctx || !vertices || !indices || !mesh_id) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (nv == 0 || nt == 0) return fail(ctx, RP3DG_EINVAL, "a triangle mesh needs vertices and triangles");
+    // TriangleMesh::computeEpsilon (TriangleMesh.cpp:70-88)
+    float mx[3] = {0.0f, 0.0f, 0.0f};
+    for (uint32_t i = 0; i < nv; i++)
+        for (int k = 0; k < 3; k++) {
+            const float a = std::fabs(vertices[3 * size_t(i) + k]);
+            if (a > mx[k]) mx[k] = a;
+        }
+    const float eps = 3 * (mx[0] + mx[1] + mx[2]) * FLT_EPSILON;
+    const float eps2 = eps * eps;
+    // copyData (:91-214): the triangles of non-zero area and edges, their
+    // vertices (and given normals) stored at the user's vertex indices
+    TriMesh m;
+    m.verts.assign(3 * size_t(nv), 0.0f);
+    m.normals.assign(3 * size_t(nv), 0.0f);
+    std::vector<uint8_t> used(nv, 0);
+    bool valid = true;
+    std::string why;
+    for (uint32_t i = 0; i < nt; i++) {
+        const uint32_t* id = indices + 3 * size_t(i);
+        bool face_ok = true;
+        for (int v = 0; v < 3; v++)
+            if (id[v] >= nv) {
+                face_ok = false;
+                valid = false;
+                why = "the face with index " + std::to_string(i) + " has a vertex index out of range";
+            }
+        if (!face_ok) continue;
+        const float* v1 = vertices + 3 * size_t(id[0]);
+        const float* v2 = vertices + 3 * size_t(id[1]);
+        const float* v3 = vertices + 3 * size_t(id[2]);
+        float e31[3], e21[3], fn[3], e32[3], e13[3];
+        vsub3(v3, v1, e31);
+        vsub3(v2, v1, e21);
+        vcross3(e31, e21, fn);
+        const bool zero_area = vdot3(fn, fn) < eps2;
+        vsub3(v3, v2, e32);
+        vsub3(v1, v3, e13);
+        const bool zero_edge = vdot3(e21, e21) < eps2 || vdot3(e32, e32) < eps2 || vdot3(e13, e13) < eps2;
+        if (zero_area || zero_edge) continue;
+        float vn[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        if (normals)
+            for (int v = 0; v < 3; v++) {
+                for (int k = 0; k < 3; k++) vn[v][k] = normals[3 * size_t(id[v]) + k];
+                if (vdot3(vn[v], vn[v]) < eps2) {
+                    valid = false;
+                    why = "the provided normal of a vertex is too small";
+                }
+            }
+        const float* vp[3] = {v1, v2, v3};
+        for (int v = 0; v < 3; v++) {
+            for (int k = 0; k < 3; k++) {
+                m.normals[3 * size_t(id[v]) + k] = vn[v][k];
+                m.verts[3 * size_t(id[v]) + k] = vp[v][k];
+            }
+            m.tris.push_back(id[v]);
+            used[id[v]] = 1;
+        }
+    }
+    // removeUnusedVertices (:217-240): every unused vertex but the first is
+    // removed and the later indices shift down
+    std::vector<uint32_t> shift(nv, 0);
+    std::vector<float> kv, kn;
+    uint32_t removed = 0;
+    for (uint32_t i = 0; i < nv; i++) {
+        shift[i] = removed;
+        if (i > 0 && !used[i]) {
+            removed++;
+            continue;
+        }
+        for (int k = 0; k < 3; k++) {
+            kv.push_back(m.verts[3 * size_t(i) + k]);
+            kn.push_back(m.normals[3 * size_t(i) + k]);
+        }
+    }
+    for (uint32_t& t : m.tris) t -= shift[t];
+    m.verts.swap(kv);
+    m.normals.swap(kn);
+    if (m.tris.empty()) {
+        valid = false;
+        why = "the mesh does not have any valid triangle faces";
+    }
+    if (!valid) return fail(ctx, RP3DG_EINVAL, "triangle mesh: " + why);
+    const uint32_t nkept = uint32_t(m.tris.size() / 3), nvk = uint32_t(m.verts.size() / 3);
+    // computeVerticesNormals (:277-333): angle-weighted face normals
+    if (!normals) {
+        for (uint32_t f = 0; f < nkept; f++) {
+            const float* tv[3] = {&m.verts[3 * size_t(m.tris[3 * f])], &m.verts[3 * size_t(m.tris[3 * f + 1])],
+                                  &m.verts[3 * size_t(m.tris[3 * f + 2])]};
+            float d[3];
+            float len[3];
+            vsub3(tv[1], tv[0], d);
+            len[0] = vlen3(d);
+            vsub3(tv[2], tv[1], d);
+            len[1] = vlen3(d);
+            vsub3(tv[0], tv[2], d);
+            len[2] = vlen3(d);
+            for (uint32_t v = 0; v < 3; v++) {
+                const uint32_t prev = v == 0 ? 2 : v - 1, next = v == 2 ? 0 : v + 1;
+                float a[3], b[3], n[3];
+                vsub3(tv[next], tv[v], a);
+                vsub3(tv[prev], tv[v], b);
+                const float dp = vdot3(a, b);
+                const float lab = len[prev] * len[v];
+                float cosA = dp / lab;
+                cosA = (cosA < 0.0f) ? 0.0f : cosA;   // std::max(cosA, 0)
+                cosA = (1.0f < cosA) ? 1.0f : cosA;   // std::min(cosA, 1)
+                const float angle = std::acos(cosA);
+                vcross3(a, b, n);
+                vnormalize3(n);
+                float* acc = &m.normals[3 * size_t(m.tris[3 * f + v])];
+                for (int k = 0; k < 3; k++) acc[k] += angle * n[k];
+            }
+        }
+        for (uint32_t v = 0; v < nvk; v++) vnormalize3(&m.normals[3 * size_t(v)]);
+    }
+    // initBVHTree (:242-266): the triangles' AABBs (AABB::createAABBForTriangle,
+    // AABB.h:260-282) inserted in order into a tree without fattening
+    rp3dg::order::Tree tree;
+    for (uint32_t f = 0; f < nkept; f++) {
+        const float* p0 = &m.verts[3 * size_t(m.tris[3 * f])];
+        const float* p1 = &m.verts[3 * size_t(m.tris[3 * f + 1])];
+        const float* p2 = &m.verts[3 * size_t(m.tris[3 * f + 2])];
+        rp3dg::order::Box b;
+        for (int k = 0; k < 3; k++) {
+            b.mn[k] = p0[k];
+            b.mx[k] = p0[k];
+            if (p1[k] < b.mn[k]) b.mn[k] = p1[k];
+        }
+        for (int k = 0; k < 3; k++)
+            if (p2[k] < b.mn[k]) b.mn[k] = p2[k];
+        for (int k = 0; k < 3; k++)
+            if (p1[k] > b.mx[k]) b.mx[k] = p1[k];
+        for (int k = 0; k < 3; k++)
+            if (p2[k] > b.mx[k]) b.mx[k] = p2[k];
+        tree.add_object(b, int(f));
+    }
+    m.nodes.resize(tree.nodes.size());
+    for (size_t k = 0; k < tree.nodes.size(); k++) {
+        const rp3dg::order::Tree::Node& N = tree.nodes[k];
+        const bool leaf = N.height == 0;
+        const int c0 = leaf ? -2 - N.data : N.child[0];
+        const int c1 = leaf ? -1 : N.child[1];
+        m.nodes[k].lo = make_float4(N.box.mn[0], N.box.mn[1], N.box.mn[2], as_float(c0));
+        m.nodes[k].hi = make_float4(N.box.mx[0], N.box.mx[1], N.box.mx[2], as_float(c1));
+    }
+    m.root = tree.root;
+    for (int k = 0; k < 3; k++) {
+        m.bmin[k] = tree.nodes[size_t(tree.root)].box.mn[k];
+        m.bmax[k] = tree.nodes[size_t(tree.root)].box.mx[k];
+    }
+    *mesh_id = int32_t(ctx->trimeshes.size());
+    ctx->trimeshes.push_back(std::move(m));
+    return 0;
+}
+
+int rp3dg_create_concave_mesh_shape(rp3dg_ctx* ctx, int32_t mesh_id, float sx, float sy, float sz,
+                                    int32_t* instance_id) {
+    if (!ctx || !instance_id) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (mesh_id < 0 || size_t(mesh_id) >= ctx->trimeshes.size()) return fail(ctx, RP3DG_EINVAL, "unknown triangle mesh");
+    if (!(sx > 0.0f) || !(sy > 0.0f) || !(sz > 0.0f)) return fail(ctx, RP3DG_EINVAL, "scale must be positive");
+    const TriMesh& m = ctx->trimeshes[size_t(mesh_id)];
+    const uint32_t nv = uint32_t(m.verts.size() / 3), nt = uint32_t(m.tris.size() / 3);
+    const float sc[3] = {sx, sy, sz};
+    // getTriangleVertices (ConcaveMeshShape.cpp:79-89): vertex * scale;
+    // computeScaledVerticesNormals (:56-76): Vector3(1.0 / scale) * normal,
+    // divided by its length
+    std::vector<float> sv(3 * size_t(nv)), sn(3 * size_t(nv));
+    const float inv_d[3] = {float(1.0 / double(sx)), float(1.0 / double(sy)), float(1.0 / double(sz))};
+    for (uint32_t v = 0; v < nv; v++) {
+        float n[3];
+        for (int k = 0; k < 3; k++) {
+            sv[3 * size_t(v) + k] = m.verts[3 * size_t(v) + k] * sc[k];
+            n[k] = inv_d[k] * m.normals[3 * size_t(v) + k];
+        }
+        const float l = vlen3(n);
+        for (int k = 0; k < 3; k++) sn[3 * size_t(v) + k] = n[k] / l;
+    }
+    rp3dg::CmDesc d{};
+    d.nv = nv;
+    d.nt = nt;
+    d.root = m.root;
+    d.mesh = uint32_t(mesh_id);
+    for (int k = 0; k < 3; k++) {
+        d.scale[k] = sc[k];
+        d.inv_scale[k] = 1.0f / sc[k];
+    }
+    cudaSetDevice(ctx->device);
+    uint32_t* dt = nullptr;
+    float *dv = nullptr, *dn = nullptr;
+    rp3dg::RayNode* dnodes = nullptr;
+    cudaError_t e = cudaMalloc(&dt, m.tris.size() * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&dv, sv.size() * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&dn, sn.size() * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&dnodes, m.nodes.size() * sizeof(rp3dg::RayNode));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dt, m.tris.data(), m.tris.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dv, sv.data(), sv.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dn, sn.data(), sn.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dnodes, m.nodes.data(), m.nodes.size() * sizeof(rp3dg::RayNode), cudaMemcpyHostToDevice,
+                            ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(dt);
+        cudaFree(dv);
+        cudaFree(dn);
+        cudaFree(dnodes);
+        return cuda_fail(ctx, e, "upload concave mesh");
+    }
+    d.tris = dt;
+    d.sverts = dv;
+    d.snormals = dn;
+    d.nodes = dnodes;
+    *instance_id = int32_t(ctx->cmeshes.size());
+    ctx->cmeshes.push_back(d);
+    return 0;
+}
+
+int rp3dg_get_triangle_mesh(rp3dg_ctx* ctx, int32_t mesh_id, uint32_t* nb_vertices, uint32_t* nb_triangles,
+                            float* vertices, float* normals, uint32_t* triangles, uint32_t cap_v, uint32_t cap_t) {
+    if (!ctx || !nb_vertices || !nb_triangles) return fail(ctx, RP3DG_EINVAL, "null argument");
+    if (mesh_id < 0 || size_t(mesh_id) >= ctx->trimeshes.size()) return fail(ctx, RP3DG_EINVAL, "unknown triangle mesh");
+    const TriMesh& m = ctx->trimeshes[size_t(mesh_id)];
+    *nb_vertices = uint32_t(m.verts.size() / 3);
+    *nb_triangles = uint32_t(m.tris.size() / 3);
+    const size_t nv = std::min<size_t>(*nb_vertices, cap_v), nt = std::min<size_t>(*nb_triangles, cap_t);
+    if (vertices) std::memcpy(vertices, m.verts.data(), nv * 12);
+    if (normals) std::memcpy(normals, m.normals.data(), nv * 12);
+    if (triangles) std::memcpy(triangles, m.tris.data(), nt * 12);
+    return 0;
+}
+
 int rp3dg_set_shapes(rp3dg_ctx* ctx, const rp3dg_shape* shapes, uint32_t nb) {
     if (!ctx || (!shapes && nb)) return fail(ctx, RP3DG_EINVAL, "null argument");
     for (uint32_t i = 0; i < nb; i++) {
         const rp3dg_shape& s = shapes[i];
-        if (s.kind < RP3DG_SHAPE_SPHERE || s.kind > RP3DG_SHAPE_HEIGHTFIELD) return fail(ctx, RP3DG_EINVAL, "unknown shape kind");
+        if (s.kind < RP3DG_SHAPE_SPHERE || s.kind > RP3DG_SHAPE_CONCAVE_MESH) return fail(ctx, RP3DG_EINVAL, "unknown shape kind");
+        if (s.kind == RP3DG_SHAPE_CONCAVE_MESH && (s.mesh < 0 || size_t(s.mesh) >= ctx->cmeshes.size()))
+            return fail(ctx, RP3DG_EINVAL, "shape refers to an unknown concave mesh instance");
         if (s.kind == RP3DG_SHAPE_HEIGHTFIELD && (s.mesh < 0 || size_t(s.mesh) >= ctx->hfields.size()))
             return fail(ctx, RP3DG_EINVAL, "shape refers to an unknown height field");
         if (s.kind == RP3DG_SHAPE_CONVEX_MESH && (s.mesh < 0 || size_t(s.mesh) >= ctx->instances.size()))
@@ -663,6 +959,14 @@ int rp3dg_set_shapes(rp3dg_ctx* ctx, const rp3dg_shape* shapes, uint32_t nb) {
                 // HeightFieldShape::getLocalBounds (HeightFieldShape.cpp:46-50): bounds * scale
                 const rp3dg::HfDesc& h = ctx->hfields[size_t(sh.mesh)];
                 for (int k = 0; k < 3; k++) { b[k] = h.bmin[k] * h.scale[k]; b[4 + k] = h.bmax[k] * h.scale[k]; }
+                break;
+            }
+            case RP3DG_SHAPE_CONCAVE_MESH: {
+                // ConcaveMeshShape::getLocalBounds (ConcaveMeshShape.cpp:276-285):
+                // the triangle tree's root AABB * scale
+                const rp3dg::CmDesc& c = ctx->cmeshes[size_t(sh.mesh)];
+                const TriMesh& m = ctx->trimeshes[size_t(c.mesh)];
+                for (int k = 0; k < 3; k++) { b[k] = m.bmin[k] * c.scale[k]; b[4 + k] = m.bmax[k] * c.scale[k]; }
                 break;
             }
             default: {

@@ -1,5 +1,7 @@
 // Layouts shared by the host runtime and the kernels.
 #pragma once
+#include <vector_types.h>
+
 #include <cstdint>
 
 namespace rp3dg {
@@ -102,6 +104,27 @@ struct HfDesc {
     float bmin[3], bmax[3];
     float scale[3];
     const float* heights;  // device
+};
+
+// One node of a DynamicAABBTree as the GPU traversals read it: lo = (AABB
+// min, child 0), hi = (AABB max, child 1), the children as int bits (-1:
+// none).  A leaf has child 0 = -2 - its data (collider or triangle index).
+struct __align__(16) RayNode {
+    float4 lo, hi;
+};
+
+// A concave mesh shape (ConcaveMeshShape over a TriangleMesh, with its
+// scale) as the middle phase, the raycasts and the debug renderer read it.
+struct CmDesc {
+    uint32_t nv, nt;
+    int32_t root;             // root node of the triangle tree (-1: empty)
+    uint32_t mesh;            // the triangle mesh's id
+    float scale[3];
+    float inv_scale[3];       // decimal(1.0) / scale per axis
+    const uint32_t* tris;     // device: 3 vertex indices per triangle
+    const float* sverts;      // device: 3 floats per vertex, vertex * scale
+    const float* snormals;    // device: 3 floats per vertex, scaled vertex normals
+    const RayNode* nodes;     // device: the mesh's DynamicAABBTree over the unscaled triangles
 };
 
 }  // namespace rp3dg

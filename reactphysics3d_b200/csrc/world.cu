@@ -54,6 +54,7 @@
 #include <omp.h>
 
 #include "../../include/rp3dg.h"
+#include "debug_launch.h"
 #include "dynamics_launch.h"
 #include "hf_launch.h"
 #include "raycast_launch.h"
@@ -76,6 +77,7 @@ int get_heightfield(rp3dg_ctx* ctx, int32_t id, HfDesc* out);
 int get_heightfields(rp3dg_ctx* ctx, std::vector<HfDesc>* out);
 int get_mesh_arena_device(rp3dg_ctx* ctx, const uint32_t** words);
 int get_mesh_mass(rp3dg_ctx* ctx, int32_t instance, float* volume, float* extent);
+int get_mesh_face_counts(rp3dg_ctx* ctx, int32_t instance, std::vector<uint32_t>* counts);
 int get_shape_device(rp3dg_ctx* ctx, const rp3dg_shape** shapes, const float4** bounds);
 int narrowphase_tri_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3dg_contact_batch* out,
                            const float4* tri);
@@ -650,6 +652,10 @@ struct WorldH {
     std::vector<uint32_t> isl_jstart, isl_jcount;
     uint32_t jl_base = 0;
     bool stepped = false;
+    // Body::mIsDebugEnabled by body id, and where the last update's debug
+    // primitives of this world start in the group's buffers
+    std::vector<uint8_t> body_debug;
+    uint32_t dbg_line0 = 0, dbg_nl = 0, dbg_tri0 = 0, dbg_nt = 0;
     // this step
     std::vector<int4> items[NB_ALGOS];
     std::vector<uint32_t> item_pair[NB_ALGOS];
@@ -799,6 +805,17 @@ struct rp3dg_world {
     int solver = 0;
     bool solver_stats = false;
     rp3dg::SolverStats* d_solver_stats = nullptr;
+    // debug rendering (rp3dg_world_set_debug_rendering): the items shown,
+    // the collider transforms before the integration of the last update
+    // (world positions then orientations, NC rows each) and that update's
+    // primitives, world after world
+    uint32_t debug_items = 0;
+    float4* d_dbg_snap = nullptr;
+    rp3dg_debug_line* d_dbg_lines = nullptr;
+    rp3dg_debug_triangle* d_dbg_tris = nullptr;
+    rp3dg::DebugJob* d_dbg_jobs = nullptr;
+    int4* d_dbg_points = nullptr;
+    size_t cap_dbg_snap = 0, cap_dbg_lines = 0, cap_dbg_tris = 0, cap_dbg_jobs = 0, cap_dbg_points = 0;
     // phase profiling (rp3dg_world_set_profiling): cumulative ms per phase
     bool profiling = false;
     double phase_ms[16] = {};
@@ -1745,6 +1762,105 @@ int sync_rows(Group* g) {
     return 0;
 }
 
+// DebugRenderer at the end of PhysicsWorld::update (PhysicsWorld.cpp:248-303):
+// the contact primitives of DebugRenderer::onContact, from the contact pairs
+// of the update that are not triggers (CollisionCallback.cpp:84-103), then
+// computeDebugRenderingPrimitives over the bodies in creation order
+// (DebugRenderer.cpp:482-527), every world after the other.  The host lays
+// out the offsets; debug.cu writes the primitives.
+int debug_primitives(Group* g) {
+    const uint32_t items = g->debug_items;
+    if (!items) return 0;
+    const bool cpt = (items & RP3DG_DEBUG_CONTACT_POINT) != 0, cno = (items & RP3DG_DEBUG_CONTACT_NORMAL) != 0;
+    std::vector<rp3dg::DebugJob> jobs;
+    std::vector<int4> points;
+    std::unordered_map<int32_t, std::vector<uint32_t>> faces;
+    uint32_t nl = 0, nt = 0;
+    for (WorldH& w : g->worlds) {
+        w.dbg_line0 = nl;
+        w.dbg_tri0 = nt;
+        std::vector<int32_t> row_of(w.nc);
+        for (uint32_t r = 0; r < w.nc; r++) row_of[size_t(w.dev_col_at[r])] = int32_t(w.c0 + r);
+        if (cpt || cno)
+            for (const ContactPairH& c : w.prev_cpairs) {
+                if (c.trigger || !c.in_island) continue;
+                for (uint32_t i = 0; i < c.k; i++) {
+                    points.push_back(make_int4(row_of[size_t(c.c1)], int(c.point + i), int(nl), int(nt)));
+                    nl += cno ? 1u : 0u;
+                    nt += cpt ? rp3dg::DEBUG_SPHERE_TRIS : 0u;
+                }
+            }
+        for (uint32_t b = 0; b < w.nb; b++) {
+            if (!w.body_debug[b]) continue;
+            for (int c : w.bodies[b].colliders) {
+                const int si = w.colliders[size_t(c)].shape;
+                const rp3dg_shape& sh = g->shapes[size_t(si)];
+                const uint32_t* fc = nullptr;
+                uint32_t nf = 0, hc = 0, hr = 0;
+                if (sh.kind == RP3DG_SHAPE_CONVEX_MESH) {
+                    auto it = faces.find(sh.mesh);
+                    if (it == faces.end()) {
+                        std::vector<uint32_t> v;
+                        if (rp3dg::get_mesh_face_counts(g->ctx, sh.mesh, &v))
+                            return wfail(g, RP3DG_EINVAL, "debug rendering: unknown convex mesh");
+                        it = faces.emplace(sh.mesh, std::move(v)).first;
+                    }
+                    fc = it->second.data();
+                    nf = uint32_t(it->second.size());
+                } else if (sh.kind == RP3DG_SHAPE_HEIGHTFIELD) {
+                    rp3dg::HfDesc h;
+                    if (rp3dg::get_heightfield(g->ctx, sh.mesh, &h))
+                        return wfail(g, RP3DG_EINVAL, "debug rendering: unknown height field");
+                    hc = h.ncol;
+                    hr = h.nrow;
+                }
+                uint32_t l = 0, t = 0;
+                rp3dg::debug_collider_counts(items, sh.kind, fc, nf, hc, hr, &l, &t);
+                if (l || t) jobs.push_back(rp3dg::DebugJob{row_of[size_t(c)], si, nl, nt});
+                nl += l;
+                nt += t;
+            }
+        }
+        w.dbg_nl = nl - w.dbg_line0;
+        w.dbg_nt = nt - w.dbg_tri0;
+    }
+    if (dev_grow(&g->d_dbg_lines, &g->cap_dbg_lines, std::max<size_t>(nl, 1)) ||
+        dev_grow(&g->d_dbg_tris, &g->cap_dbg_tris, std::max<size_t>(nt, 1)) ||
+        dev_grow(&g->d_dbg_jobs, &g->cap_dbg_jobs, std::max<size_t>(jobs.size(), 1)) ||
+        dev_grow(&g->d_dbg_points, &g->cap_dbg_points, std::max<size_t>(points.size(), 1)))
+        return wfail(g, RP3DG_ENOMEM, "cudaMalloc(debug primitives)");
+    if (jobs.empty() && points.empty()) return 0;
+    cudaStream_t st = g->stream;
+    if (!jobs.empty())
+        cudaMemcpyAsync(g->d_dbg_jobs, jobs.data(), jobs.size() * sizeof(rp3dg::DebugJob), cudaMemcpyHostToDevice, st);
+    if (!points.empty())
+        cudaMemcpyAsync(g->d_dbg_points, points.data(), points.size() * sizeof(int4), cudaMemcpyHostToDevice, st);
+    rp3dg::DebugArgs a{};
+    a.items = items;
+    a.n_jobs = uint32_t(jobs.size());
+    a.jobs = g->d_dbg_jobs;
+    a.wpos = g->ccol[g->cur_c][CC_WPOS];
+    a.wori = g->ccol[g->cur_c][CC_WORI];
+    a.fmin = g->ccol[g->cur_c][CC_FMIN];
+    a.fmax = g->ccol[g->cur_c][CC_FMAX];
+    rp3dg::get_shape_device(g->ctx, &a.shapes, &a.bounds);
+    rp3dg::get_mesh_arena_device(g->ctx, &a.mesh_words);
+    a.hf = g->d_hf;
+    a.n_points = uint32_t(points.size());
+    a.points = g->d_dbg_points;
+    a.snap_wpos = g->d_dbg_snap;
+    a.snap_wori = g->d_dbg_snap ? g->d_dbg_snap + g->NC : nullptr;
+    const ContactBuf& B = g->cbuf[1 - g->cur_cb];
+    a.nd = B.nd;
+    a.l1 = B.l1;
+    a.lines = g->d_dbg_lines;
+    a.tris = g->d_dbg_tris;
+    rp3dg::make_debug_trig(&a.trig);
+    cudaError_t e = rp3dg::launch_debug(a, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? 0 : wcuda(g, e, "debug primitives");
+}
+
 void destroy_group(Group* g) {
     if (!g) return;
     for (int k = 0; k < 2; k++) {
@@ -1774,6 +1890,8 @@ void destroy_group(Group* g) {
     cudaFree(g->d_tr2); cudaFree(g->d_trep); cudaFree(g->d_tcoll); cudaFree(g->d_tnct); cudaFree(g->d_tmid);
     cudaFree(g->d_tnd); cudaFree(g->d_tl1); cudaFree(g->d_tl2); cudaFree(g->d_tri);
     cudaFree(g->d_tcache[0]); cudaFree(g->d_tcache[1]); cudaFree(g->d_hf);
+    cudaFree(g->d_dbg_snap); cudaFree(g->d_dbg_lines); cudaFree(g->d_dbg_tris); cudaFree(g->d_dbg_jobs);
+    cudaFree(g->d_dbg_points);
     if (g->tuner.e0) cudaEventDestroy(g->tuner.e0);
     if (g->tuner.e1) cudaEventDestroy(g->tuner.e1);
     cudaFreeHost(g->h_tnodes); cudaFree(g->d_tnodes); cudaFreeHost(g->h_tq); cudaFree(g->d_tq);
@@ -1814,6 +1932,7 @@ int build_world(Group* g, WorldH& w, const rp3dg_body_desc* bd, uint32_t nb, con
     w.bcomp.reserve_ids(nb);
     w.ccomp.reserve_ids(nc);
     w.gravity.assign(nb, 1);
+    w.body_debug.assign(nb, 0);
     dynamic.assign(nb, 0);
     for (int k = 0; k < BC_NCOL; k++) col[k].assign(nb, make_float4(0.f, 0.f, 0.f, 0.f));
     for (int k = 0; k < CC_NCOL; k++) ccols[k].assign(nc, make_float4(0.f, 0.f, 0.f, 0.f));
@@ -2497,6 +2616,15 @@ int update_group(Group* g, float dt) {
         cudaMemcpyAsync(g->d_icount, g->h_icount, size_t(NI) * 4, cudaMemcpyHostToDevice, st);
     }
     mark(4);
+    // DebugRenderer::onContact runs before the integration: keep the
+    // collider transforms it reads
+    if ((g->debug_items & (RP3DG_DEBUG_CONTACT_POINT | RP3DG_DEBUG_CONTACT_NORMAL)) && g->NC) {
+        if (dev_grow(&g->d_dbg_snap, &g->cap_dbg_snap, 2 * size_t(g->NC)))
+            return wfail(g, RP3DG_ENOMEM, "cudaMalloc(debug snapshot)");
+        cudaMemcpyAsync(g->d_dbg_snap, g->ccol[ccur][CC_WPOS], size_t(g->NC) * 16, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(g->d_dbg_snap + g->NC, g->ccol[ccur][CC_WORI], size_t(g->NC) * 16, cudaMemcpyDeviceToDevice,
+                        st);
+    }
     // ---- dynamics stage (inertia, velocities, solver, positions, state)
     {
         rp3dg_dynamics_params pr{};
@@ -2630,6 +2758,8 @@ int update_group(Group* g, float dt) {
     if (e != cudaSuccess) return wcuda(g, e, "end of step");
     tuner_step(g);
     g->cur_cb = 1 - g->cur_cb;
+    rc = debug_primitives(g);
+    if (rc) return rc;
     for (WorldH& w : g->worlds) {
         w.stepped = true;
         g->stats.overlapping_pairs += uint32_t(w.pairs.size() + w.concave.size());
@@ -3182,6 +3312,37 @@ int rp3dg_world_get_trigger_events(rp3dg_world* g, uint32_t world, rp3dg_contact
         if (c.trigger) emit(c, RP3DG_CONTACT_EXIT);
     if (nb_events) *nb_events = k;
     return 0;
+}
+
+int rp3dg_world_set_debug_rendering(rp3dg_world* g, uint32_t items) {
+    if (!g || (items & ~0x3fu)) return RP3DG_EINVAL;
+    // disabled, the renderer is no longer reset: the last primitives stay
+    g->debug_items = items;
+    return 0;
+}
+
+int rp3dg_world_set_body_debug(rp3dg_world* g, uint32_t world, int32_t body, int enabled) {
+    if (!g || world >= g->worlds.size()) return RP3DG_EINVAL;
+    WorldH& w = g->worlds[world];
+    if (body >= int32_t(w.nb)) return RP3DG_EINVAL;
+    if (body < 0) std::fill(w.body_debug.begin(), w.body_debug.end(), uint8_t(enabled ? 1 : 0));
+    else w.body_debug[size_t(body)] = enabled ? 1 : 0;
+    return 0;
+}
+
+int rp3dg_world_get_debug_primitives(rp3dg_world* g, uint32_t world, rp3dg_debug_line* lines, uint32_t cap_lines,
+                                     rp3dg_debug_triangle* tris, uint32_t cap_tris, uint32_t* nb_lines,
+                                     uint32_t* nb_tris, int device) {
+    if (!g || world >= g->worlds.size() || (cap_lines && !lines) || (cap_tris && !tris)) return RP3DG_EINVAL;
+    const WorldH& w = g->worlds[world];
+    if (nb_lines) *nb_lines = w.dbg_nl;
+    if (nb_tris) *nb_tris = w.dbg_nt;
+    const uint32_t nl = std::min(w.dbg_nl, cap_lines), nt = std::min(w.dbg_nt, cap_tris);
+    const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (nl) cudaMemcpyAsync(lines, g->d_dbg_lines + w.dbg_line0, size_t(nl) * sizeof(rp3dg_debug_line), kind, g->stream);
+    if (nt) cudaMemcpyAsync(tris, g->d_dbg_tris + w.dbg_tri0, size_t(nt) * sizeof(rp3dg_debug_triangle), kind, g->stream);
+    cudaError_t e = cudaStreamSynchronize(g->stream);
+    return e == cudaSuccess ? 0 : wcuda(g, e, "read debug primitives");
 }
 
 int rp3dg_world_get_contacts(rp3dg_world* w, int32_t* body1, int32_t* body2, uint8_t* nb_points, uint32_t capacity,

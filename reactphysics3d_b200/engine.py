@@ -118,6 +118,10 @@ def load_library(path=LIB_PATH):
     L.rp3dg_world_get_contact_events.argtypes = [P, C.c_uint32, P, C.c_uint32, P, P, P, C.c_uint32,
                                                  C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.rp3dg_world_get_trigger_events.argtypes = [P, C.c_uint32, P, C.c_uint32, C.POINTER(C.c_uint32)]
+    L.rp3dg_world_set_debug_rendering.argtypes = [P, C.c_uint32]
+    L.rp3dg_world_set_body_debug.argtypes = [P, C.c_uint32, C.c_int32, C.c_int]
+    L.rp3dg_world_get_debug_primitives.argtypes = [P, C.c_uint32, P, C.c_uint32, P, C.c_uint32,
+                                                   C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_int]
     L.rp3dg_world_raycast.argtypes = [P, C.c_uint32, P, C.c_uint32, C.c_int32, C.c_uint32, P, P]
     L.rp3dg_world_raycast_device.argtypes = [P, C.c_uint32, P, C.c_uint32, C.c_int32, C.c_uint32, P, P,
                                              C.POINTER(C.c_float)]
@@ -576,6 +580,35 @@ class World:
         if rc != 0:
             raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
         return ev
+
+    def set_debug_rendering(self, items=A.DEBUG_ALL):
+        """PhysicsWorld::setIsDebugRenderingEnabled(items != 0) with the
+        DebugRenderer items of `items` (A.DEBUG_* bits) displayed."""
+        rc = self.lib.rp3dg_world_set_debug_rendering(self.h, int(items))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+
+    def set_body_debug(self, body=-1, enabled=True, world=0):
+        """Body::setIsDebugEnabled for one body, or every body (body < 0)."""
+        rc = self.lib.rp3dg_world_set_body_debug(self.h, int(world), int(body), int(bool(enabled)))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+
+    def debug_primitives(self, world=0):
+        """DebugRenderer's lines and triangles after the last update
+        (structured arrays of A.DEBUG_LINE_DTYPE / A.DEBUG_TRIANGLE_DTYPE)."""
+        nl, nt = C.c_uint32(), C.c_uint32()
+        rc = self.lib.rp3dg_world_get_debug_primitives(self.h, int(world), None, 0, None, 0, C.byref(nl), C.byref(nt), 0)
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+        lines = np.zeros(nl.value, A.DEBUG_LINE_DTYPE)
+        tris = np.zeros(nt.value, A.DEBUG_TRIANGLE_DTYPE)
+        rc = self.lib.rp3dg_world_get_debug_primitives(self.h, int(world), lines.ctypes.data if len(lines) else None,
+                                                       len(lines), tris.ctypes.data if len(tris) else None, len(tris),
+                                                       C.byref(nl), C.byref(nt), 0)
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+        return lines, tris
 
     def raycast(self, rays, mode=A.RAYCAST_CLOSEST, max_hits=1, world=0):
         """PhysicsWorld::raycast for each row of `rays` (A.RAY_DTYPE) with the

@@ -284,6 +284,9 @@ class RefScene:
         L.ref_scene_raycast.argtypes = [C.c_int, P, C.c_uint32, C.c_int, C.c_uint32, P, P]
         L.ref_scene_events.argtypes = [C.c_int, P, C.c_uint32, P, P, P, C.c_uint32, P, P]
         L.ref_scene_trigger_events.argtypes = [C.c_int, P, C.c_uint32, P]
+        L.ref_scene_set_debug.argtypes = [C.c_int, C.c_uint32]
+        L.ref_scene_set_body_debug.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.ref_scene_debug_primitives.argtypes = [C.c_int, P, C.c_uint32, P, C.c_uint32, P, P]
         L.ref_convex_register.argtypes = [P, C.c_uint32, P, P, C.c_uint32, C.c_float, C.c_float, C.c_float]
         L.ref_heightfield_register.argtypes = [C.c_uint32, C.c_uint32, P, C.c_float, C.c_float, C.c_float]
         # height fields of the scene registered with the harness; the shape
@@ -334,6 +337,21 @@ class RefScene:
         ev = np.zeros(n.value, A.CONTACT_EVENT_DTYPE)
         self.lib.ref_scene_trigger_events(self.id, ev.ctypes.data if len(ev) else None, len(ev), C.byref(n))
         return ev
+
+    def set_debug_rendering(self, items=A.DEBUG_ALL):
+        self.lib.ref_scene_set_debug(self.id, int(items))
+
+    def set_body_debug(self, body=-1, enabled=True):
+        self.lib.ref_scene_set_body_debug(self.id, int(body), int(bool(enabled)))
+
+    def debug_primitives(self):
+        nl, nt = C.c_uint32(), C.c_uint32()
+        self.lib.ref_scene_debug_primitives(self.id, None, 0, None, 0, C.byref(nl), C.byref(nt))
+        lines = np.zeros(nl.value, A.DEBUG_LINE_DTYPE)
+        tris = np.zeros(nt.value, A.DEBUG_TRIANGLE_DTYPE)
+        self.lib.ref_scene_debug_primitives(self.id, lines.ctypes.data if len(lines) else None, len(lines),
+                                            tris.ctypes.data if len(tris) else None, len(tris), C.byref(nl), C.byref(nt))
+        return lines, tris
 
     def raycast(self, rays, mode=A.RAYCAST_CLOSEST, max_hits=1):
         r = np.ascontiguousarray(rays, dtype=A.RAY_DTYPE)
