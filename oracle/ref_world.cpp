@@ -600,6 +600,65 @@ static std::vector<ConvexSpec>& convex_specs() {
     static std::vector<ConvexSpec> c;
     return c;
 }
+// A triangle mesh and its concave-mesh-shape scale, registered for
+// ref_scene_create (rp3dg_shape.mesh names this id for RP3DG_SHAPE_CONCAVE_MESH).
+struct ConcaveSpec {
+    std::vector<float> vertices, normals;   // normals empty: computed by TriangleMesh::init
+    std::vector<uint32_t> indices;
+    float scale[3];
+};
+static std::vector<ConcaveSpec>& concave_specs() {
+    static std::vector<ConcaveSpec> c;
+    return c;
+}
+int ref_concave_register(const float* vertices, uint32_t nv, const uint32_t* indices, uint32_t nt,
+                         const float* normals, float sx, float sy, float sz) {
+    ConcaveSpec c;
+    c.vertices.assign(vertices, vertices + 3 * size_t(nv));
+    if (normals) c.normals.assign(normals, normals + 3 * size_t(nv));
+    c.indices.assign(indices, indices + 3 * size_t(nt));
+    c.scale[0] = sx; c.scale[1] = sy; c.scale[2] = sz;
+    concave_specs().push_back(std::move(c));
+    return int(concave_specs().size()) - 1;
+}
+
+// The TriangleMesh of a registered spec as the reference builds it: vertices,
+// vertex normals, triangles (counts always written; -1 when it is invalid).
+int ref_concave_mesh_data(int id, float* vertices, float* normals, uint32_t* triangles, uint32_t cap_v, uint32_t cap_t,
+                          uint32_t* nv, uint32_t* nt) {
+    ConcaveSpec& c = concave_specs().at(size_t(id));
+    PhysicsCommon common;
+    const uint32 n = uint32(c.vertices.size() / 3), m = uint32(c.indices.size() / 3);
+    std::unique_ptr<TriangleVertexArray> tva;
+    if (c.normals.empty())
+        tva.reset(new TriangleVertexArray(n, c.vertices.data(), 3 * sizeof(float), m, c.indices.data(),
+                                          3 * sizeof(uint32_t), TriangleVertexArray::VertexDataType::VERTEX_FLOAT_TYPE,
+                                          TriangleVertexArray::IndexDataType::INDEX_INTEGER_TYPE));
+    else
+        tva.reset(new TriangleVertexArray(n, c.vertices.data(), 3 * sizeof(float), c.normals.data(), 3 * sizeof(float),
+                                          m, c.indices.data(), 3 * sizeof(uint32_t),
+                                          TriangleVertexArray::VertexDataType::VERTEX_FLOAT_TYPE,
+                                          TriangleVertexArray::NormalDataType::NORMAL_FLOAT_TYPE,
+                                          TriangleVertexArray::IndexDataType::INDEX_INTEGER_TYPE));
+    std::vector<Message> messages;
+    TriangleMesh* mesh = common.createTriangleMesh(*tva, messages);
+    if (!mesh) return -1;
+    *nv = mesh->getNbVertices();
+    *nt = mesh->getNbTriangles();
+    for (uint32_t v = 0; v < *nv && v < cap_v; v++) {
+        const Vector3& p = mesh->getVertex(v);
+        const Vector3& q = mesh->getVertexNormal(v);
+        vertices[3 * v] = float(p.x); vertices[3 * v + 1] = float(p.y); vertices[3 * v + 2] = float(p.z);
+        normals[3 * v] = float(q.x); normals[3 * v + 1] = float(q.y); normals[3 * v + 2] = float(q.z);
+    }
+    for (uint32_t t = 0; t < *nt && t < cap_t; t++) {
+        uint32 a, b, d;
+        mesh->getTriangleVerticesIndices(t, a, b, d);
+        triangles[3 * t] = a; triangles[3 * t + 1] = b; triangles[3 * t + 2] = d;
+    }
+    return 0;
+}
+
 int ref_convex_register(const float* vertices, uint32_t nv, const uint32_t* face_indices, const uint32_t* face_sizes,
                         uint32_t nf, float sx, float sy, float sz) {
     ConvexSpec c;
@@ -706,6 +765,27 @@ int ref_scene_create(const rp3dg_world_settings* s, const rp3dg_shape* shapes, u
                                                           HeightField::HeightDataType::HEIGHT_FLOAT_TYPE, messages);
             if (!hf) return -1;
             cs[i] = W->common.createHeightFieldShape(hf, Vector3(h.scale[0], h.scale[1], h.scale[2]));
+        }
+        else if (sh.kind == RP3DG_SHAPE_CONCAVE_MESH) {
+            if (sh.mesh < 0 || size_t(sh.mesh) >= concave_specs().size()) return -1;
+            ConcaveSpec& c = concave_specs()[size_t(sh.mesh)];
+            const uint32 n = uint32(c.vertices.size() / 3), m = uint32(c.indices.size() / 3);
+            std::unique_ptr<TriangleVertexArray> tva;
+            if (c.normals.empty())
+                tva.reset(new TriangleVertexArray(n, c.vertices.data(), 3 * sizeof(float), m, c.indices.data(),
+                                                  3 * sizeof(uint32_t),
+                                                  TriangleVertexArray::VertexDataType::VERTEX_FLOAT_TYPE,
+                                                  TriangleVertexArray::IndexDataType::INDEX_INTEGER_TYPE));
+            else
+                tva.reset(new TriangleVertexArray(n, c.vertices.data(), 3 * sizeof(float), c.normals.data(),
+                                                  3 * sizeof(float), m, c.indices.data(), 3 * sizeof(uint32_t),
+                                                  TriangleVertexArray::VertexDataType::VERTEX_FLOAT_TYPE,
+                                                  TriangleVertexArray::NormalDataType::NORMAL_FLOAT_TYPE,
+                                                  TriangleVertexArray::IndexDataType::INDEX_INTEGER_TYPE));
+            std::vector<Message> messages;
+            TriangleMesh* mesh = W->common.createTriangleMesh(*tva, messages);
+            if (!mesh) return -1;
+            cs[i] = W->common.createConcaveMeshShape(mesh, Vector3(c.scale[0], c.scale[1], c.scale[2]));
         }
         else if (sh.kind == RP3DG_SHAPE_CONVEX_MESH) {
             if (sh.mesh < 0 || size_t(sh.mesh) >= convex_specs().size()) return -1;

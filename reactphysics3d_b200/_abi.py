@@ -11,7 +11,7 @@ import numpy as np
 
 MAX_CONTACTS = 16  # NB_MAX_CONTACT_POINTS_IN_NARROWPHASE_INFO (configuration.h:109)
 
-SHAPE_SPHERE, SHAPE_CAPSULE, SHAPE_BOX, SHAPE_CONVEX_MESH, SHAPE_HEIGHTFIELD = 0, 1, 2, 3, 4
+SHAPE_SPHERE, SHAPE_CAPSULE, SHAPE_BOX, SHAPE_CONVEX_MESH, SHAPE_HEIGHTFIELD, SHAPE_CONCAVE_MESH = 0, 1, 2, 3, 4, 5
 
 ALGO_NONE = 0
 ALGO_SPHERE_VS_SPHERE = 1

@@ -38,7 +38,8 @@ void make_debug_trig(DebugTrig* t) {
 }
 
 void debug_collider_counts(uint32_t items, int kind, const uint32_t* face_counts, uint32_t nfaces, uint32_t hf_cols,
-                           uint32_t hf_rows, uint32_t* lines, uint32_t* tris) {
+                           uint32_t hf_rows, uint32_t cm_vertices, uint32_t cm_triangles, uint32_t* lines,
+                           uint32_t* tris) {
     uint32_t l = 0, t = 0;
     if (items & RP3DG_DEBUG_COLLIDER_AABB) l += 12;
     if (items & RP3DG_DEBUG_COLLIDER_BROADPHASE_AABB) l += 12;
@@ -56,6 +57,10 @@ void debug_collider_counts(uint32_t items, int kind, const uint32_t* face_counts
                 for (uint32_t f = 0; f < nfaces; f++)
                     if (shape && face_counts[f] >= 3) t += face_counts[f] - 2;
                 if (normal) l += nfaces;
+                break;
+            case RP3DG_SHAPE_CONCAVE_MESH:
+                if (shape) t += cm_triangles;
+                if (normal) l += cm_vertices;
                 break;
             case RP3DG_SHAPE_HEIGHTFIELD: {
                 const uint32_t cells = (hf_cols > 1 && hf_rows > 1) ? (hf_cols - 1) * (hf_rows - 1) : 0u;
@@ -305,6 +310,26 @@ __global__ void __launch_bounds__(128) debug_colliders(const DebugArgs a) {
                     put_line(a.lines + line++, centroid, normalPoint, COLOR_SHAPE_NORMAL);
                 }
             }
+            break;
+        }
+        case RP3DG_SHAPE_CONCAVE_MESH: {
+            // drawConcaveMeshShape (:350-383): every triangle (scaled vertices),
+            // then a normal line per vertex
+            const CmDesc cm = a.cm[sh.mesh];
+            auto ld = [](const float* p, uint32_t v) { return V(p[3 * v], p[3 * v + 1], p[3 * v + 2]); };
+            if (shape)
+                for (uint32_t k = tid; k < cm.nt; k += nt) {
+                    const v3 p0 = xapply(T, ld(cm.sverts, cm.tris[3 * k]));
+                    const v3 p1 = xapply(T, ld(cm.sverts, cm.tris[3 * k + 1]));
+                    const v3 p2 = xapply(T, ld(cm.sverts, cm.tris[3 * k + 2]));
+                    put_tri(a.tris + J.tri + k, p0, p1, p2, COLOR_SHAPE);
+                }
+            if (normal)
+                for (uint32_t v = tid; v < cm.nv; v += nt) {
+                    const v3 vertex = xapply(T, ld(cm.sverts, v));
+                    const v3 n = qrot(T.q, ld(cm.snormals, v));
+                    put_line(a.lines + line + v, vertex, vadd(vertex, V(n.x * 1.0f, n.y * 1.0f, n.z * 1.0f)), COLOR_SHAPE_NORMAL);
+                }
             break;
         }
         case RP3DG_SHAPE_HEIGHTFIELD: {

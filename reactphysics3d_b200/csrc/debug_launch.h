@@ -41,6 +41,7 @@ struct DebugArgs {
     const float4* bounds;              // 2 per shape: local bounds min, max
     const uint32_t* mesh_words;
     const HfDesc* hf;
+    const CmDesc* cm;
     // contact points: x collider-1 row in the snapshot taken before the
     // step's integration, y packed point index, z first line, w first triangle
     uint32_t n_points;
@@ -55,9 +56,10 @@ struct DebugArgs {
 
 // Number of lines and triangles one collider adds (host side, same rules as
 // the kernels): kind, mesh face vertex counts (convex mesh), height-field
-// size.
+// size, concave mesh vertices and triangles.
 void debug_collider_counts(uint32_t items, int kind, const uint32_t* face_counts, uint32_t nfaces, uint32_t hf_cols,
-                           uint32_t hf_rows, uint32_t* lines, uint32_t* tris);
+                           uint32_t hf_rows, uint32_t cm_vertices, uint32_t cm_triangles, uint32_t* lines,
+                           uint32_t* tris);
 constexpr uint32_t DEBUG_SPHERE_TRIS = 324;   // 18 x (9 + 9)
 
 cudaError_t launch_debug(const DebugArgs& a, cudaStream_t s);

@@ -9,6 +9,11 @@
 //                 src/collision/shapes/HeightFieldShape.cpp:53-63;
 //                 HeightField::computeMinMaxGridCoordinates,
 //                 src/collision/HeightField.cpp:220-253)
+//   concave meshes: the convex AABB without the mesh's scale queried
+//                 against the mesh's triangle tree (ConcaveMeshShape::
+//                 computeOverlappingTriangles, src/collision/shapes/
+//                 ConcaveMeshShape.cpp:135-175): counted by hf_rects, listed
+//                 in query order by hf_list
 //   hf_tests:     one narrow-phase test per triangle of the rectangle, two
 //                 per cell in (i, j) order (HeightField::computeOverlappingTriangles,
 //                 HeightField.cpp:139-216; TriangleShape constructor,
@@ -46,20 +51,66 @@ RD int clamp_int(int v, int lo, int hi) {                        // clamp (mathe
     return hi < m ? hi : m;
 }
 
+// The convex collider's AABB in the concave shape's local space
+// (computeConvexVsConcaveMiddlePhase: convexShape->computeTransformedAABB of
+// convexToConcaveTransform = concave^-1 * convex).
+RD void convex_aabb_in_concave(const int4 it, const int32_t* c_shape, const rp3dg_shape* shapes,
+                               const float4* bounds, const float4* c_wpos, const float4* c_wori, v3& amin,
+                               v3& amax) {
+    const float4 pv = c_wpos[it.x], qv = c_wori[it.x], pc = c_wpos[it.y], qc = c_wori[it.y];
+    const xform tConvex = X(V(pv.x, pv.y, pv.z), Q(qv.x, qv.y, qv.z, qv.w));
+    const xform tConcave = X(V(pc.x, pc.y, pc.z), Q(qc.x, qc.y, qc.z, qc.w));
+    const xform c2c = xmul(xinv(tConcave), tConvex);
+    const int32_t si = c_shape[it.x];
+    const rp3dg_shape s = shapes[si];
+    shape_transformed_aabb(s.kind, s.params[0], bounds[2 * si], bounds[2 * si + 1], c2c, amin, amax);
+}
+
+// ConcaveMeshShape::computeOverlappingTriangles (ConcaveMeshShape.cpp:135-175)
+// over DynamicAABBTree::reportAllShapesOverlappingWithAABB (DynamicAABBTree.cpp:
+// 641-681): the AABB without the mesh's scale (AABB::applyScale by
+// decimal(1.0) / scale), then the leaves whose AABB it touches (inclusive
+// test), children[1] popped before children[0].  `emit(k, triangle)` sees
+// them in that order; returns the count, or -1 when the stack overflowed.
+template <class F>
+RD int mesh_query(const CmDesc& cm, v3 amin, v3 amax, F emit) {
+    const v3 mn = V(amin.x * cm.inv_scale[0], amin.y * cm.inv_scale[1], amin.z * cm.inv_scale[2]);
+    const v3 mx = V(amax.x * cm.inv_scale[0], amax.y * cm.inv_scale[1], amax.z * cm.inv_scale[2]);
+    int stack[MESH_STACK];
+    int sp = 0, count = 0;
+    stack[sp++] = cm.root;
+    while (sp > 0) {
+        const int id = stack[--sp];
+        if (id < 0) continue;
+        const float4 lo = __ldg(&cm.nodes[id].lo), hi = __ldg(&cm.nodes[id].hi);
+        // AABB::testCollision (AABB.h:179-187)
+        if (mx.x < lo.x || hi.x < mn.x || mx.y < lo.y || hi.y < mn.y || mx.z < lo.z || hi.z < mn.z) continue;
+        const int c0 = __float_as_int(lo.w);
+        if (c0 <= -2) {
+            emit(count, -2 - c0);
+            count++;
+        } else {
+            if (sp + 2 > MESH_STACK) return -1;
+            stack[sp++] = c0;
+            stack[sp++] = __float_as_int(hi.w);
+        }
+    }
+    return count;
+}
+
 __global__ void __launch_bounds__(128) hf_rects_kernel(const HfRectArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const int4 it = a.items[i];
-    const HfDesc hf = a.hf[it.z];
-    const float4 pv = a.c_wpos[it.x], qv = a.c_wori[it.x], pc = a.c_wpos[it.y], qc = a.c_wori[it.y];
-    const xform tConvex = X(V(pv.x, pv.y, pv.z), Q(qv.x, qv.y, qv.z, qv.w));
-    const xform tConcave = X(V(pc.x, pc.y, pc.z), Q(qc.x, qc.y, qc.z, qc.w));
-    // convexToConcaveTransform = concave^-1 * convex
-    const xform c2c = xmul(xinv(tConcave), tConvex);
-    const int32_t si = a.c_shape[it.x];
-    const rp3dg_shape s = a.shapes[si];
     v3 amin, amax;
-    shape_transformed_aabb(s.kind, s.params[0], a.bounds[2 * si], a.bounds[2 * si + 1], c2c, amin, amax);
+    convex_aabb_in_concave(it, a.c_shape, a.shapes, a.bounds, a.c_wpos, a.c_wori, amin, amax);
+    if (it.w & HF_MESH) {
+        const int n = mesh_query(a.cm[it.z], amin, amax, [](int, int) {});
+        if (n < 0) atomicOr(a.error, 2u);
+        a.rect[i] = make_int4(0, n < 0 ? 0 : n, 0, 1);
+        return;
+    }
+    const HfDesc hf = a.hf[it.z];
     // HeightFieldShape::computeOverlappingTriangles: the AABB without the scale
     const v3 inv = V(1.0f / hf.scale[0], 1.0f / hf.scale[1], 1.0f / hf.scale[2]);
     const float mn[3] = {amin.x * inv.x, amin.y * inv.y, amin.z * inv.z};
@@ -90,6 +141,21 @@ RD v3 hf_vertex(const HfDesc& h, uint32_t x, uint32_t y) {
     return V(v.x * h.scale[0], v.y * h.scale[1], v.z * h.scale[2]);
 }
 
+__global__ void __launch_bounds__(128) hf_list_kernel(const HfListArgs a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int4 it = a.items[i];
+    if (!(it.w & HF_MESH)) return;
+    v3 amin, amax;
+    convex_aabb_in_concave(it, a.c_shape, a.shapes, a.bounds, a.c_wpos, a.c_wori, amin, amax);
+    int32_t* out = a.tri_id + a.start[i];
+    const uint32_t room = a.start[i + 1] - a.start[i];
+    const int n = mesh_query(a.cm[it.z], amin, amax, [&](int k, int tri) {
+        if (uint32_t(k) < room) out[k] = tri;
+    });
+    if (n < 0 || uint32_t(n) != room) atomicOr(a.error, 2u);
+}
+
 __global__ void __launch_bounds__(128) hf_tests_kernel(const HfTestArgs a) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.n_tests) return;
@@ -104,25 +170,55 @@ __global__ void __launch_bounds__(128) hf_tests_kernel(const HfTestArgs a) {
     const int4 it = a.items[ci];
     const int4 r = a.rect[ci];
     const uint32_t local = t - a.start[ci];
-    const uint32_t nj = uint32_t(r.w - r.z);
-    const uint32_t cell = local >> 1, k = local & 1u;
-    const uint32_t i = uint32_t(r.x) + cell / nj, j = uint32_t(r.z) + cell % nj;
-    const HfDesc hf = a.hf[it.z];
-    const v3 q1 = hf_vertex(hf, i, j), q2 = hf_vertex(hf, i, j + 1);
-    const v3 q3 = hf_vertex(hf, i + 1, j), q4 = hf_vertex(hf, i + 1, j + 1);
-    // first triangle (p1, p2, p3), second (p3, p2, p4); vertex normals are the
-    // face normal by getUnit(), the shape's own normal by normalize()
-    const v3 v0 = k == 0 ? q1 : q3, v1 = q2, v2 = k == 0 ? q3 : q4;
-    const v3 c = vcross(vsub(v1, v0), vsub(v2, v0));
-    const v3 vn = vunit(c), fn = vnormalize(c);
+    const bool mesh = (it.w & HF_MESH) != 0;
+    v3 v0, v1, v2, vn0, vn1, vn2;
+    uint32_t i = 0, j = 0, k = 0;
+    int32_t tri = -1;
+    if (mesh) {
+        // ConcaveMeshShape::getTriangleVertices / getTriangleVerticesNormals
+        // (ConcaveMeshShape.cpp:79-104): scaled vertices, scaled vertex normals
+        const CmDesc cm = a.cm[it.z];
+        tri = a.tri_id[t];
+        if (tri < 0 || uint32_t(tri) >= cm.nt) {
+            atomicOr(a.error, 2u);
+            tri = 0;
+        }
+        const uint32_t i0 = __ldg(cm.tris + 3 * tri), i1 = __ldg(cm.tris + 3 * tri + 1), i2 = __ldg(cm.tris + 3 * tri + 2);
+        auto ld = [](const float* p, uint32_t v) { return V(__ldg(p + 3 * v), __ldg(p + 3 * v + 1), __ldg(p + 3 * v + 2)); };
+        v0 = ld(cm.sverts, i0);
+        v1 = ld(cm.sverts, i1);
+        v2 = ld(cm.sverts, i2);
+        vn0 = ld(cm.snormals, i0);
+        vn1 = ld(cm.snormals, i1);
+        vn2 = ld(cm.snormals, i2);
+    } else {
+        const uint32_t nj = uint32_t(r.w - r.z);
+        const uint32_t cell = local >> 1;
+        k = local & 1u;
+        i = uint32_t(r.x) + cell / nj;
+        j = uint32_t(r.z) + cell % nj;
+        const HfDesc hf = a.hf[it.z];
+        const v3 q1 = hf_vertex(hf, i, j), q2 = hf_vertex(hf, i, j + 1);
+        const v3 q3 = hf_vertex(hf, i + 1, j), q4 = hf_vertex(hf, i + 1, j + 1);
+        // first triangle (p1, p2, p3), second (p3, p2, p4); the vertex normals
+        // are the face normal by getUnit()
+        v0 = k == 0 ? q1 : q3;
+        v1 = q2;
+        v2 = k == 0 ? q3 : q4;
+        vn0 = vn1 = vn2 = vunit(vcross(vsub(v1, v0), vsub(v2, v0)));
+    }
+    // TriangleShape's own normal (TriangleShape.cpp:40-60): normalize()
+    const v3 fn = vnormalize(vcross(vsub(v1, v0), vsub(v2, v0)));
     const int4 b = a.batch[ci];
     const size_t n = size_t(b.y);
-    float4* tr = a.tri + 5 * size_t(b.x) + (t - uint32_t(b.x));
+    float4* tr = a.tri + TRI_REC * size_t(b.x) + (t - uint32_t(b.x));
     tr[0] = make_float4(v0.x, v0.y, v0.z, 0.0f);
     tr[n] = make_float4(v1.x, v1.y, v1.z, 0.0f);
     tr[2 * n] = make_float4(v2.x, v2.y, v2.z, 0.0f);
     tr[3 * n] = make_float4(fn.x, fn.y, fn.z, 0.0f);
-    tr[4 * n] = make_float4(vn.x, vn.y, vn.z, 0.0f);
+    tr[4 * n] = make_float4(vn0.x, vn0.y, vn0.z, 0.0f);
+    tr[5 * n] = make_float4(vn1.x, vn1.y, vn1.z, 0.0f);
+    tr[6 * n] = make_float4(vn2.x, vn2.y, vn2.z, 0.0f);
     const bool convex1 = (it.w & HF_SHAPE1_CONVEX) != 0;
     const int32_t sc = a.c_shape[it.x];
     const int row1 = convex1 ? it.x : it.y, row2 = convex1 ? it.y : it.x;
@@ -138,9 +234,19 @@ __global__ void __launch_bounds__(128) hf_tests_kernel(const HfTestArgs a) {
     // (OverlappingPairs.h:86-91)
     const int32_t ps = a.prev_start[ci];
     const int4 pr = a.prev_rect[ci];
-    if (ps >= 0 && int(i) >= pr.x && int(i) < pr.y && int(j) >= pr.z && int(j) < pr.w) {
-        const uint32_t pl = ((i - uint32_t(pr.x)) * uint32_t(pr.w - pr.z) + (j - uint32_t(pr.z))) * 2u + k;
-        a.cache[t] = a.prev_cache[uint32_t(ps) + pl];
+    int32_t pl = -1;
+    if (ps >= 0 && mesh) {
+        // the previous step's tests of this pair, in their query order
+        for (int32_t q = 0; q < pr.y; q++)
+            if (a.prev_tri_id[ps + q] == tri) {
+                pl = q;
+                break;
+            }
+    } else if (ps >= 0 && int(i) >= pr.x && int(i) < pr.y && int(j) >= pr.z && int(j) < pr.w) {
+        pl = int32_t(((i - uint32_t(pr.x)) * uint32_t(pr.w - pr.z) + (j - uint32_t(pr.z))) * 2u + k);
+    }
+    if (pl >= 0) {
+        a.cache[t] = a.prev_cache[uint32_t(ps) + uint32_t(pl)];
     } else {
         rp3dg_lastframe f;
         f.gjk_axis[0] = 0.0f;
@@ -270,6 +376,12 @@ __global__ void __launch_bounds__(128) hf_manifolds_kernel(const HfManifoldArgs 
 cudaError_t launch_hf_rects(const HfRectArgs& a, cudaStream_t s) {
     if (a.n == 0) return cudaSuccess;
     hf_rects_kernel<<<(a.n + 127) / 128, 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hf_list(const HfListArgs& a, cudaStream_t s) {
+    if (a.n == 0) return cudaSuccess;
+    hf_list_kernel<<<(a.n + 127) / 128, 128, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -229,11 +229,14 @@ RD void process_tri(const NpArgs& a, uint32_t i, const BoxTables* box, const uin
     TriPoly tp;
     const float4 f0 = a.tri[i], f1 = a.tri[size_t(a.n) + i], f2 = a.tri[2 * size_t(a.n) + i];
     const float4 f3 = a.tri[3 * size_t(a.n) + i], f4 = a.tri[4 * size_t(a.n) + i];
+    const float4 f5 = a.tri[5 * size_t(a.n) + i], f6 = a.tri[6 * size_t(a.n) + i];
     tp.p0 = V(f0.x, f0.y, f0.z);
     tp.p1 = V(f1.x, f1.y, f1.z);
     tp.p2 = V(f2.x, f2.y, f2.z);
     tp.n = V(f3.x, f3.y, f3.z);
-    tp.vn0 = tp.vn1 = tp.vn2 = V(f4.x, f4.y, f4.z);
+    tp.vn0 = V(f4.x, f4.y, f4.z);
+    tp.vn1 = V(f5.x, f5.y, f5.z);
+    tp.vn2 = V(f6.x, f6.y, f6.z);
     tp.t = box;
     Item it;
     load_item(a, i, it);

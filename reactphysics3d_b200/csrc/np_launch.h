@@ -40,8 +40,8 @@ struct NpArgs {
     const uint8_t* proposals;        // per-pair learned proposal (15 = none) or nullptr
     unsigned long long* mlp_stats;   // [0] proposals tested, [1] confirmed
     // triangle tests (launch_narrowphase_tri): the triangle side of a test has
-    // shape index -1; 5 float4 per test, slot-major (k * n + i): the three
-    // vertices, the face normal and the vertex normal shared by the vertices
+    // shape index -1; 7 float4 per test, slot-major (k * n + i): the three
+    // vertices, the face normal and the three vertex normals
     const float4* tri;
     // polyhedron batches: the order in which the tiles take the pairs (thread
     // t of the batch processes pair perm[t]) or nullptr for 0..n-1

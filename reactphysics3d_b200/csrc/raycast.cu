@@ -345,6 +345,54 @@ RD bool ray_heightfield(v3 p1, v3 p2, float maxf, const HfDesc& H, LocalHit& h, 
     return hit;
 }
 
+// ConcaveMeshShape::raycast (ConcaveMeshShape.cpp:179-274): the ray without
+// the mesh's scale walks the mesh's tree (DynamicAABBTree::raycast,
+// DynamicAABBTree.cpp:684-747, whose callback collects every leaf it reaches
+// and returns the ray's maxFraction, so the walk is never clipped), then each
+// collected triangle, scaled, is tested in that order against the unscaled
+// ray (TriangleShape::raycast, FRONT side), a hit at a fraction <= the
+// smallest so far replacing the current one.
+constexpr int MESH_RAY_STACK = 64;
+__device__ __noinline__ bool ray_concave_mesh(v3 p1, v3 p2, float maxf, const CmDesc& cm, LocalHit& h, bool* overflow) {
+    const v3 is = V(cm.inv_scale[0], cm.inv_scale[1], cm.inv_scale[2]);
+    const v3 s1 = vcmul(p1, is), s2 = vcmul(p2, is);
+    const v3 d = vsub(s2, s1);
+    const v3 dinv = V(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    float smallest = maxf;
+    bool hit = false;
+    int stack[MESH_RAY_STACK];
+    int sp = 0;
+    stack[sp++] = cm.root;
+    while (sp > 0) {
+        const int id = stack[--sp];
+        if (id < 0) continue;
+        const float4 lo = __ldg(&cm.nodes[id].lo), hi = __ldg(&cm.nodes[id].hi);
+        if (!ray_aabb(lo, hi, s1, dinv, maxf)) continue;
+        const int c0 = __float_as_int(lo.w);
+        if (c0 <= -2) {
+            const uint32_t tri = uint32_t(-2 - c0);
+            const uint32_t i0 = __ldg(cm.tris + 3 * tri), i1 = __ldg(cm.tris + 3 * tri + 1), i2 = __ldg(cm.tris + 3 * tri + 2);
+            auto ld = [&](uint32_t v) { return V(__ldg(cm.sverts + 3 * v), __ldg(cm.sverts + 3 * v + 1), __ldg(cm.sverts + 3 * v + 2)); };
+            LocalHit th;
+            if (ray_triangle(p1, p2, maxf, ld(i0), ld(i1), ld(i2), th) && th.fraction <= smallest) {
+                h = th;
+                smallest = th.fraction;
+                hit = true;
+            }
+            // the callback's answer is the ray's maxFraction: 0 ends the walk
+            if (maxf == 0.0f) break;
+        } else {
+            if (sp + 2 > MESH_RAY_STACK) {
+                *overflow = true;
+                break;
+            }
+            stack[sp++] = c0;
+            stack[sp++] = __float_as_int(hi.w);
+        }
+    }
+    return hit;
+}
+
 // Collider::raycast: the ray into the collider's local space
 // (localToWorld.getInverse() * point), the shape's raycast, the hit point and
 // the rotated, normalised normal back in world space.
@@ -372,6 +420,13 @@ RD bool collider_raycast(const RayArgs& a, int4 col, v3 p1, v3 p2, float maxf, L
             hit = ray_heightfield(vcmul(l1, is), vcmul(l2, is), maxf, H, h, &limit);
             if (hit) h.point = vcmul(h.point, V(H.scale[0], H.scale[1], H.scale[2]));
             if (limit) *flags |= 1;
+            break;
+        }
+        case RP3DG_SHAPE_CONCAVE_MESH: {
+            if (s.mesh < 0 || uint32_t(s.mesh) >= a.nb_cmeshes) break;
+            bool overflow = false;
+            hit = ray_concave_mesh(l1, l2, maxf, a.cmeshes[s.mesh], h, &overflow);
+            if (overflow) atomicOr(a.error, 1u);
             break;
         }
         default: break;

@@ -23,13 +23,15 @@ struct RayArgs {
     const uint32_t* mesh_words;    // convex mesh arena
     const HfDesc* hfields;         // height fields of the context, by id
     uint32_t nb_hfields;
+    const CmDesc* cmeshes;         // concave mesh instances of the context, by id
+    uint32_t nb_cmeshes;
     const rp3dg_ray* rays;
     uint32_t n;
     int32_t mode;                  // RP3DG_RAYCAST_*
     uint32_t max_hits;
     rp3dg_raycast_hit* hits;       // n * max_hits
     uint32_t* nb_hits;             // n
-    uint32_t* error;               // bit 0: a traversal stack overflowed
+    uint32_t* error;               // bit 0: a traversal stack overflowed (world or mesh tree)
 };
 
 cudaError_t launch_world_raycast(const RayArgs& a, cudaStream_t stream);

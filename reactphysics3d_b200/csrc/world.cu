@@ -78,6 +78,7 @@ int get_heightfields(rp3dg_ctx* ctx, std::vector<HfDesc>* out);
 int get_mesh_arena_device(rp3dg_ctx* ctx, const uint32_t** words);
 int get_mesh_mass(rp3dg_ctx* ctx, int32_t instance, float* volume, float* extent);
 int get_mesh_face_counts(rp3dg_ctx* ctx, int32_t instance, std::vector<uint32_t>* counts);
+int get_cmeshes(rp3dg_ctx* ctx, std::vector<CmDesc>* out);
 int get_shape_device(rp3dg_ctx* ctx, const rp3dg_shape** shapes, const float4** bounds);
 int narrowphase_tri_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3dg_contact_batch* out,
                            const float4* tri);
@@ -449,8 +450,9 @@ struct JointH {
 struct ColliderH {
     int body = -1;
     int shape = -1;
-    bool convex = true;  // CollisionShape::isConvex (a height field is not)
-    int hf = -1;         // height-field id of a concave collider
+    bool convex = true;  // CollisionShape::isConvex (height fields and concave meshes are not)
+    bool mesh = false;   // a concave collider's shape is a triangle mesh (not a height field)
+    int hf = -1;         // height-field or concave-mesh id of a concave collider
     int bp = -1;  // broad-phase id (tree leaf)
     uint16_t category = 1, mask = 0xffff;
     bool trigger = false;  // Collider::setIsTrigger: not a simulation collider
@@ -729,6 +731,11 @@ struct rp3dg_world {
     uint32_t htest_start[NB_ALGOS + 1] = {};
     rp3dg::HfDesc* d_hf = nullptr;
     uint32_t n_hf = 0;
+    rp3dg::CmDesc* d_cm = nullptr;      // concave mesh instances of the context, by id
+    uint32_t n_cm = 0;
+    int32_t* d_ttri[2] = {nullptr, nullptr};   // per triangle test of a mesh item: its triangle (this step, the last)
+    size_t cap_ttri[2] = {0, 0};
+    uint32_t *d_herr = nullptr, *h_herr = nullptr;   // middle-phase error word (bit 1: mesh query stack overflow)
     size_t cap_hitem = 0, cap_htest = 0, cap_hc[2] = {0, 0};
     int4 *h_hitems = nullptr, *d_hitems = nullptr, *h_hrect = nullptr, *d_hrect = nullptr;
     uint32_t *h_hstart = nullptr, *d_hstart = nullptr;
@@ -1239,7 +1246,8 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
         const bool trig = w.colliders[size_t(p.c1)].trigger || w.colliders[size_t(p.c2)].trigger;
         w.hitems[a].push_back(make_int4(int(w.c0) + w.ccomp.slot[size_t(cv)], int(w.c0) + w.ccomp.slot[size_t(cc)],
                                         w.colliders[size_t(cc)].hf,
-                                        (p.shape1_convex ? HF_SHAPE1_CONVEX : 0) | (trig ? HF_NO_REPORT : 0)));
+                                        (p.shape1_convex ? HF_SHAPE1_CONVEX : 0) | (trig ? HF_NO_REPORT : 0) |
+                                            (w.colliders[size_t(cc)].mesh ? HF_MESH : 0)));
         w.hitem_pair[a].push_back(i);
     }
     if (g->profiling) {
@@ -1613,7 +1621,8 @@ int ensure_hitems(Group* g, size_t n) {
 // (the previous step's buffer is kept as it is).
 int ensure_htests(Group* g, size_t n) {
     n = std::max<size_t>(n, 1);
-    if (dev_grow(&g->d_tcache[g->cur_tc], &g->cap_hc[g->cur_tc], n))
+    if (dev_grow(&g->d_tcache[g->cur_tc], &g->cap_hc[g->cur_tc], n) ||
+        dev_grow(&g->d_ttri[g->cur_tc], &g->cap_ttri[g->cur_tc], n))
         return wfail(g, RP3DG_ENOMEM, "cudaMalloc(triangle records)");
     if (n <= g->cap_htest) return 0;
     const size_t c = std::max<size_t>(std::max<size_t>(n, g->cap_htest * 2), 256);
@@ -1627,7 +1636,7 @@ int ensure_htests(Group* g, size_t n) {
     M((void**)&g->d_tp1, c * 16); M((void**)&g->d_tr1, c * 16); M((void**)&g->d_tp2, c * 16); M((void**)&g->d_tr2, c * 16);
     M((void**)&g->d_trep, c); M((void**)&g->d_tcoll, c); M((void**)&g->d_tnct, c); M((void**)&g->d_tmid, c * MAXC);
     M((void**)&g->d_tnd, c * 16 * MAXC); M((void**)&g->d_tl1, c * 16 * MAXC); M((void**)&g->d_tl2, c * 16 * MAXC);
-    M((void**)&g->d_tri, c * 16 * 5);
+    M((void**)&g->d_tri, c * 16 * rp3dg::TRI_REC);
     if (e != cudaSuccess) return wcuda(g, e, "cudaMalloc(triangle tests)");
     g->cap_htest = c;
     return 0;
@@ -1775,6 +1784,8 @@ int debug_primitives(Group* g) {
     std::vector<rp3dg::DebugJob> jobs;
     std::vector<int4> points;
     std::unordered_map<int32_t, std::vector<uint32_t>> faces;
+    std::vector<rp3dg::CmDesc> cms;
+    rp3dg::get_cmeshes(g->ctx, &cms);
     uint32_t nl = 0, nt = 0;
     for (WorldH& w : g->worlds) {
         w.dbg_line0 = nl;
@@ -1796,7 +1807,7 @@ int debug_primitives(Group* g) {
                 const int si = w.colliders[size_t(c)].shape;
                 const rp3dg_shape& sh = g->shapes[size_t(si)];
                 const uint32_t* fc = nullptr;
-                uint32_t nf = 0, hc = 0, hr = 0;
+                uint32_t nf = 0, hc = 0, hr = 0, cv = 0, ct = 0;
                 if (sh.kind == RP3DG_SHAPE_CONVEX_MESH) {
                     auto it = faces.find(sh.mesh);
                     if (it == faces.end()) {
@@ -1813,9 +1824,14 @@ int debug_primitives(Group* g) {
                         return wfail(g, RP3DG_EINVAL, "debug rendering: unknown height field");
                     hc = h.ncol;
                     hr = h.nrow;
+                } else if (sh.kind == RP3DG_SHAPE_CONCAVE_MESH) {
+                    if (sh.mesh < 0 || uint32_t(sh.mesh) >= g->n_cm)
+                        return wfail(g, RP3DG_EINVAL, "debug rendering: unknown concave mesh");
+                    cv = cms[size_t(sh.mesh)].nv;
+                    ct = cms[size_t(sh.mesh)].nt;
                 }
                 uint32_t l = 0, t = 0;
-                rp3dg::debug_collider_counts(items, sh.kind, fc, nf, hc, hr, &l, &t);
+                rp3dg::debug_collider_counts(items, sh.kind, fc, nf, hc, hr, cv, ct, &l, &t);
                 if (l || t) jobs.push_back(rp3dg::DebugJob{row_of[size_t(c)], si, nl, nt});
                 nl += l;
                 nt += t;
@@ -1846,6 +1862,7 @@ int debug_primitives(Group* g) {
     rp3dg::get_shape_device(g->ctx, &a.shapes, &a.bounds);
     rp3dg::get_mesh_arena_device(g->ctx, &a.mesh_words);
     a.hf = g->d_hf;
+    a.cm = g->d_cm;
     a.n_points = uint32_t(points.size());
     a.points = g->d_dbg_points;
     a.snap_wpos = g->d_dbg_snap;
@@ -1890,6 +1907,7 @@ void destroy_group(Group* g) {
     cudaFree(g->d_tr2); cudaFree(g->d_trep); cudaFree(g->d_tcoll); cudaFree(g->d_tnct); cudaFree(g->d_tmid);
     cudaFree(g->d_tnd); cudaFree(g->d_tl1); cudaFree(g->d_tl2); cudaFree(g->d_tri);
     cudaFree(g->d_tcache[0]); cudaFree(g->d_tcache[1]); cudaFree(g->d_hf);
+    cudaFree(g->d_cm); cudaFree(g->d_ttri[0]); cudaFree(g->d_ttri[1]); cudaFree(g->d_herr); cudaFreeHost(g->h_herr);
     cudaFree(g->d_dbg_snap); cudaFree(g->d_dbg_lines); cudaFree(g->d_dbg_tris); cudaFree(g->d_dbg_jobs);
     cudaFree(g->d_dbg_points);
     if (g->tuner.e0) cudaEventDestroy(g->tuner.e0);
@@ -1953,7 +1971,9 @@ int build_world(Group* g, WorldH& w, const rp3dg_body_desc* bd, uint32_t nb, con
             ColliderH& C = w.colliders[ci];
             C.body = int(b);
             C.shape = c.shape;
-            C.convex = g->shapes[size_t(c.shape)].kind != RP3DG_SHAPE_HEIGHTFIELD;
+            const int kind = g->shapes[size_t(c.shape)].kind;
+            C.convex = kind != RP3DG_SHAPE_HEIGHTFIELD && kind != RP3DG_SHAPE_CONCAVE_MESH;
+            C.mesh = kind == RP3DG_SHAPE_CONCAVE_MESH;
             C.hf = C.convex ? -1 : g->shapes[size_t(c.shape)].mesh;
             C.category = c.category;
             C.mask = c.mask;
@@ -2055,6 +2075,21 @@ int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds
         destroy_group(g);
         return cfail(ctx, RP3DG_EINVAL, "no world");
     }
+    // concave mesh instances of the context, by id, and the middle phase's error word
+    {
+        std::vector<rp3dg::CmDesc> cms;
+        rp3dg::get_cmeshes(ctx, &cms);
+        if ((!cms.empty() && (cudaMalloc(&g->d_cm, cms.size() * sizeof(rp3dg::CmDesc)) != cudaSuccess ||
+                              cudaMemcpy(g->d_cm, cms.data(), cms.size() * sizeof(rp3dg::CmDesc),
+                                         cudaMemcpyHostToDevice) != cudaSuccess)) ||
+            cudaMalloc(&g->d_herr, 4) != cudaSuccess || cudaMemset(g->d_herr, 0, 4) != cudaSuccess ||
+            cudaMallocHost(&g->h_herr, 4) != cudaSuccess) {
+            destroy_group(g);
+            return cfail(ctx, RP3DG_ENOMEM, "concave-mesh tables");
+        }
+        *g->h_herr = 0;
+        g->n_cm = uint32_t(cms.size());
+    }
     // height fields named by the shape table, by id
     {
         std::vector<rp3dg::HfDesc> hfs;
@@ -2069,12 +2104,16 @@ int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds
         if (!hfs.empty()) {
             g->n_hf = uint32_t(hfs.size());
             if (cudaMalloc(&g->d_hf, hfs.size() * sizeof(rp3dg::HfDesc)) != cudaSuccess ||
-                cudaMemcpy(g->d_hf, hfs.data(), hfs.size() * sizeof(rp3dg::HfDesc), cudaMemcpyHostToDevice) != cudaSuccess ||
-                cudaEventCreateWithFlags(&g->ev_rect, cudaEventDisableTiming) != cudaSuccess) {
+                cudaMemcpy(g->d_hf, hfs.data(), hfs.size() * sizeof(rp3dg::HfDesc), cudaMemcpyHostToDevice) != cudaSuccess) {
                 destroy_group(g);
                 return cfail(ctx, RP3DG_ENOMEM, "height-field tables");
             }
         }
+    }
+    // the event after the concave pairs' rectangles / mesh counts are read back
+    if (cudaEventCreateWithFlags(&g->ev_rect, cudaEventDisableTiming) != cudaSuccess) {
+        destroy_group(g);
+        return cfail(ctx, RP3DG_ENOMEM, "middle-phase event");
     }
     g->worlds.resize(nworlds);
     std::vector<float4> col[BC_NCOL], ccols[CC_NCOL];
@@ -2326,10 +2365,13 @@ int update_group(Group* g, float dt) {
         ra.c_wpos = g->ccol[cc][CC_WPOS];
         ra.c_wori = g->ccol[cc][CC_WORI];
         ra.hf = g->d_hf;
+        ra.cm = g->d_cm;
         ra.rect = g->d_hrect;
+        ra.error = g->d_herr;
         cudaError_t e = launch_hf_rects(ra, st);
         if (e != cudaSuccess) return wcuda(g, e, "height-field middle phase");
         cudaMemcpyAsync(g->h_hrect, g->d_hrect, size_t(CI) * 16, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(g->h_herr, g->d_herr, 4, cudaMemcpyDeviceToHost, st);
         cudaEventRecord(g->ev_rect, st);
     }
     mark(1);
@@ -2380,15 +2422,23 @@ int update_group(Group* g, float dt) {
     if (CI) {
         cudaError_t e = cudaEventSynchronize(g->ev_rect);
         if (e != cudaSuccess) return wcuda(g, e, "height-field middle phase");
+        if (*g->h_herr) return wfail(g, RP3DG_ECAPACITY, "concave mesh middle phase: tree deeper than the query stack");
         // HeightField::computeOverlappingTriangles: two triangles per cell of
-        // [iMin, iMax) x [jMin, jMax); tests algorithm-major like the items
+        // [iMin, iMax) x [jMin, jMax); a concave mesh: the triangles its tree
+        // query found; tests algorithm-major like the items
         uint32_t TC = 0;
+        bool any_mesh = false;
         for (int a = 0; a < NB_ALGOS; a++) {
             g->htest_start[a] = TC;
             for (uint32_t ci = g->hitem_start[a]; ci < g->hitem_start[a + 1]; ci++) {
                 const int4 r = g->h_hrect[ci];
                 g->h_hstart[ci] = TC;
-                if (r.y > r.x && r.w > r.z) TC += 2u * uint32_t(r.y - r.x) * uint32_t(r.w - r.z);
+                if (g->h_hitems[ci].w & HF_MESH) {
+                    any_mesh = true;
+                    TC += uint32_t(r.y);
+                } else if (r.y > r.x && r.w > r.z) {
+                    TC += 2u * uint32_t(r.y - r.x) * uint32_t(r.w - r.z);
+                }
             }
         }
         g->htest_start[NB_ALGOS] = TC;
@@ -2419,6 +2469,25 @@ int update_group(Group* g, float dt) {
         cudaMemcpyAsync(g->d_hpstart, g->h_hpstart, size_t(CI) * 4, cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(g->d_hprect, g->h_hprect, size_t(CI) * 16, cudaMemcpyHostToDevice, st);
         const int cur = g->cur_tc;
+        if (TC && any_mesh) {
+            const rp3dg_shape* d_shapes = nullptr;
+            const float4* d_bounds = nullptr;
+            rp3dg::get_shape_device(ctx, &d_shapes, &d_bounds);
+            HfListArgs la;
+            la.n = CI;
+            la.items = g->d_hitems;
+            la.start = g->d_hstart;
+            la.c_shape = g->c_shape;
+            la.shapes = d_shapes;
+            la.bounds = d_bounds;
+            la.c_wpos = g->ccol[cc][CC_WPOS];
+            la.c_wori = g->ccol[cc][CC_WORI];
+            la.cm = g->d_cm;
+            la.tri_id = g->d_ttri[cur];
+            la.error = g->d_herr;
+            e = launch_hf_list(la, st);
+            if (e != cudaSuccess) return wcuda(g, e, "concave mesh triangles");
+        }
         if (TC) {
             HfTestArgs ta;
             ta.n_items = CI;
@@ -2433,6 +2502,10 @@ int update_group(Group* g, float dt) {
             ta.c_wpos = g->ccol[cc][CC_WPOS];
             ta.c_wori = g->ccol[cc][CC_WORI];
             ta.hf = g->d_hf;
+            ta.cm = g->d_cm;
+            ta.tri_id = g->d_ttri[cur];
+            ta.prev_tri_id = g->d_ttri[1 - cur];
+            ta.error = g->d_herr;
             ta.prev_cache = g->d_tcache[1 - cur];
             ta.s1 = g->d_ts1; ta.s2 = g->d_ts2;
             ta.p1 = g->d_tp1; ta.r1 = g->d_tr1; ta.p2 = g->d_tp2; ta.r2 = g->d_tr2;
@@ -2460,7 +2533,7 @@ int update_group(Group* g, float dt) {
                 cbt.local1 = reinterpret_cast<rp3dg_float4*>(g->d_tl1 + size_t(s0) * MAXC);
                 cbt.local2 = reinterpret_cast<rp3dg_float4*>(g->d_tl2 + size_t(s0) * MAXC);
                 cbt.max_contacts = MAXC;
-                rc = rp3dg::narrowphase_tri_device(ctx, a + 1, &pb, &cbt, g->d_tri + 5 * size_t(s0));
+                rc = rp3dg::narrowphase_tri_device(ctx, a + 1, &pb, &cbt, g->d_tri + rp3dg::TRI_REC * size_t(s0));
                 if (rc) return rc;
             }
         }
@@ -2484,11 +2557,13 @@ int update_group(Group* g, float dt) {
         e = launch_hf_manifolds(ma, st);
         if (e != cudaSuccess) return wcuda(g, e, "concave manifolds");
         cudaMemcpyAsync(g->h_hout, g->d_hout, size_t(CI) * 6, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(g->h_herr, g->d_herr, 4, cudaMemcpyDeviceToHost, st);
     }
     g->cur_tc = 1 - g->cur_tc;
     if (T || CI) {
         cudaError_t e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return wcuda(g, e, "narrow phase");
+        if (CI && *g->h_herr) return wfail(g, RP3DG_ECAPACITY, "concave mesh middle phase: inconsistent triangle lists");
     }
     mark(2);
     // ---- contact pairs and islands of every world
@@ -3106,6 +3181,8 @@ int raycast_device(Group* g, uint32_t world, const rp3dg_ray* rays, uint32_t n, 
     rp3dg::get_mesh_arena_device(g->ctx, &a.mesh_words);
     a.hfields = g->d_rhf;
     a.nb_hfields = g->nb_rhf;
+    a.cmeshes = g->d_cm;
+    a.nb_cmeshes = g->n_cm;
     a.rays = rays;
     a.n = n;
     a.mode = mode;

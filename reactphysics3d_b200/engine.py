@@ -74,6 +74,11 @@ def load_library(path=LIB_PATH):
     L.rp3dg_set_shapes.argtypes = [P, P, C.c_uint32]
     L.rp3dg_create_heightfield.argtypes = [P, C.c_uint32, C.c_uint32, P, C.c_float, C.c_float, C.c_float,
                                            C.POINTER(C.c_int32)]
+    L.rp3dg_create_triangle_mesh.argtypes = [P, P, C.c_uint32, P, C.c_uint32, P, C.POINTER(C.c_int32)]
+    L.rp3dg_create_concave_mesh_shape.argtypes = [P, C.c_int32, C.c_float, C.c_float, C.c_float,
+                                                  C.POINTER(C.c_int32)]
+    L.rp3dg_get_triangle_mesh.argtypes = [P, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), P, P, P,
+                                          C.c_uint32, C.c_uint32]
     L.rp3dg_device_errors.argtypes = [P, C.POINTER(C.c_uint32), C.c_int]
     L.rp3dg_narrowphase_device.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_int]
     L.rp3dg_narrowphase_host.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_int]
@@ -280,6 +285,36 @@ class Context:
                                                       *map(float, scale), C.byref(out)))
         return out.value
 
+    def create_triangle_mesh(self, vertices, triangles, normals=None):
+        """PhysicsCommon::createTriangleMesh over float vertices (n, 3),
+        uint32 triangles (m, 3) and optional vertex normals (n, 3); returns
+        the mesh id."""
+        v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+        n = None if normals is None else np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3)
+        out = C.c_int32()
+        self._check(self.lib.rp3dg_create_triangle_mesh(self.h, v.ctypes.data, len(v), t.ctypes.data, len(t),
+                                                        None if n is None else n.ctypes.data, C.byref(out)))
+        return out.value
+
+    def create_concave_mesh_shape(self, mesh, scale=(1.0, 1.0, 1.0)):
+        """PhysicsCommon::createConcaveMeshShape; returns the instance id for
+        rp3dg_shape.mesh with kind SHAPE_CONCAVE_MESH."""
+        out = C.c_int32()
+        self._check(self.lib.rp3dg_create_concave_mesh_shape(self.h, mesh, *map(float, scale), C.byref(out)))
+        return out.value
+
+    def triangle_mesh(self, mesh):
+        """The mesh as built: (vertices (n, 3), vertex normals (n, 3), triangles (m, 3))."""
+        nv, nt = C.c_uint32(), C.c_uint32()
+        self._check(self.lib.rp3dg_get_triangle_mesh(self.h, mesh, C.byref(nv), C.byref(nt), None, None, None, 0, 0))
+        v = np.zeros((nv.value, 3), np.float32)
+        n = np.zeros((nv.value, 3), np.float32)
+        t = np.zeros((nt.value, 3), np.uint32)
+        self._check(self.lib.rp3dg_get_triangle_mesh(self.h, mesh, C.byref(nv), C.byref(nt), v.ctypes.data,
+                                                     n.ctypes.data, t.ctypes.data, len(v), len(t)))
+        return v, n, t
+
     def scene_shapes(self, scene):
         """The scene's shape table with its height fields created in this
         context (scene.heightfields: list of (heights, scale); a height-field
@@ -295,6 +330,13 @@ class Context:
         inst = [self.create_convex_mesh_shape(self.create_convex_mesh(v, f), s) for (v, f, s) in cms]
         for i in np.nonzero(shapes["kind"] == A.SHAPE_CONVEX_MESH)[0]:
             shapes["mesh"][i] = inst[int(shapes["mesh"][i])]
+        # concave meshes (scene.concave_meshes: list of (vertices, triangles,
+        # normals or None, scale); a concave-mesh shape's mesh field indexes
+        # that list)
+        ccs = getattr(scene, "concave_meshes", None) or []
+        cinst = [self.create_concave_mesh_shape(self.create_triangle_mesh(v, t, n), s) for (v, t, n, s) in ccs]
+        for i in np.nonzero(shapes["kind"] == A.SHAPE_CONCAVE_MESH)[0]:
+            shapes["mesh"][i] = cinst[int(shapes["mesh"][i])]
         return shapes
 
     def mesh_tables(self, instance, cap=4096):
@@ -736,7 +778,8 @@ class WorldGroup(World):
 
     def __init__(self, ctx, scenes_, shapes, threads=None):
         self.ctx, self.lib = ctx, ctx.lib
-        if any(getattr(s, "heightfields", None) or getattr(s, "convex_meshes", None) for s in scenes_):
+        if any(getattr(s, "heightfields", None) or getattr(s, "convex_meshes", None) or
+               getattr(s, "concave_meshes", None) for s in scenes_):
             # the table is the scenes' tables back to back (scenes.merge_shapes):
             # each segment gets its scene's height fields and convex meshes
             shapes = np.array(shapes, copy=True)

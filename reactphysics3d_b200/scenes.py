@@ -188,7 +188,7 @@ class WorldScene:
     joints (numpy structured arrays with the layouts of include/rp3dg.h)."""
 
     def __init__(self, settings, shapes, bodies, colliders, name="", joints=None, heightfields=None,
-                 convex_meshes=None):
+                 convex_meshes=None, concave_meshes=None):
         self.settings, self.shapes, self.bodies, self.colliders, self.name = settings, shapes, bodies, colliders, name
         self.joints = joints
         # height fields: list of (heights (nb_rows, nb_columns) float32, scale);
@@ -197,6 +197,10 @@ class WorldScene:
         # convex meshes: list of (vertices (n, 3), polygon faces, scale); a
         # SHAPE_CONVEX_MESH shape's mesh field indexes this list
         self.convex_meshes = convex_meshes or []
+        # concave meshes: list of (vertices (n, 3), triangles (m, 3), vertex
+        # normals (n, 3) or None, scale); a SHAPE_CONCAVE_MESH shape's mesh
+        # field indexes this list
+        self.concave_meshes = concave_meshes or []
 
 
 def box_pile(nx=10, ny=10, nz=10, seed=1, spacing=2.0, base=2.0, jitter=0.1):
@@ -401,7 +405,8 @@ def merge_shapes(scenes_):
         c = s.colliders.copy()
         c["shape"] += base
         out.append(WorldScene(s.settings, s.shapes, s.bodies, c, s.name, getattr(s, "joints", None),
-                              getattr(s, "heightfields", None), getattr(s, "convex_meshes", None)))
+                              getattr(s, "heightfields", None), getattr(s, "convex_meshes", None),
+                              getattr(s, "concave_meshes", None)))
         tables.append(s.shapes)
         base += len(s.shapes)
     return np.concatenate(tables), out
@@ -766,4 +771,104 @@ def with_triggers(scene, every=6, zones=((0.0, 2.0, 0.0, 2.5, 0.6, 2.5), (-3.0, 
         colliders["flags"][nc + k] = A.COLLIDER_TRIGGER
     return WorldScene(scene.settings, shapes, bodies, colliders, scene.name + " with triggers",
                       getattr(scene, "joints", None), getattr(scene, "heightfields", None),
-                      getattr(scene, "convex_meshes", None))
+                      getattr(scene, "convex_meshes", None), getattr(scene, "concave_meshes", None))
+
+
+def terrain_mesh(cols=24, rows=24, cell=1.0, seed=61, amplitude=2.0, jitter=0.2):
+    """A triangle-mesh terrain: a cols x rows grid of vertices at
+    sine_heights, x and z jittered by up to `jitter` cells, two triangles per
+    cell wound upwards (the height field's (p1, p2, p3), (p3, p2, p4) order),
+    the diagonal alternating from cell to cell; plus what
+    TriangleMesh::init must clean up: an unused vertex in the middle of the
+    array and two degenerate triangles (a repeated index, a zero-length
+    edge).  Returns (vertices (n, 3) float32, triangles (m, 3) uint32)."""
+    rng = np.random.default_rng(seed)
+    h = sine_heights(cols, rows, seed=seed + 1000, amplitude=amplitude, cell=cell)
+    I, J = np.meshgrid(np.arange(cols), np.arange(rows), indexing="ij")
+    x = (I - 0.5 * (cols - 1)) * cell + rng.uniform(-jitter, jitter, I.shape) * cell
+    z = (J - 0.5 * (rows - 1)) * cell + rng.uniform(-jitter, jitter, I.shape) * cell
+    y = h.T   # h is (rows, cols): row j along z, column i along x
+    verts = np.stack([x, y, z], axis=-1).reshape(-1, 3).astype(np.float32)
+    vid = lambda i, j: i * rows + j
+    tris = []
+    for i in range(cols - 1):
+        for j in range(rows - 1):
+            p1, p2, p3, p4 = vid(i, j), vid(i, j + 1), vid(i + 1, j), vid(i + 1, j + 1)
+            if (i + j) % 2 == 0:
+                tris += [(p1, p2, p3), (p3, p2, p4)]
+            else:
+                tris += [(p1, p2, p4), (p1, p4, p3)]
+    # an unused vertex in the middle, shifting the later indices
+    mid = len(verts) // 2
+    verts = np.concatenate([verts[:mid], np.array([[0.0, 50.0, 0.0]], np.float32), verts[mid:]])
+    tris = [tuple(v + (v >= mid) for v in t) for t in tris]
+    tris.insert(len(tris) // 3, (tris[0][0], tris[0][0], tris[0][1]))   # zero-length edge
+    tris.append((tris[5][1], tris[5][2], tris[5][2]))
+    return verts, np.array(tris, np.uint32)
+
+
+def concave_mesh_world(n_bodies=300, cols=24, rows=24, cell=1.0, seed=61, spacing=1.5, amplitude=2.0, hulls=True,
+                       scale=(1.0, 1.0, 1.0), normals=False, terrain_orientation=None, sleeping=True):
+    """Bodies over a static concave-mesh terrain (terrain_mesh, scaled by
+    `scale`; vertex normals computed by TriangleMesh::init, or given as the
+    normalised up vector when `normals`): n_bodies dynamic bodies, boxes,
+    spheres and capsules (and convex hulls when `hulls`) on a jittered
+    lattice above the terrain.  Body 0 is the terrain, static at the origin
+    with terrain_orientation (x, y, z, w), identity by default."""
+    rng = np.random.default_rng(seed)
+    verts, tris = terrain_mesh(cols, rows, cell, seed, amplitude)
+    vn = None
+    if normals:
+        vn = np.tile(np.array([[0.0, 1.0, 0.0]], np.float32), (len(verts), 1))
+        vn[:, 0] = rng.uniform(-0.2, 0.2, len(verts))
+        vn /= np.linalg.norm(vn, axis=1, keepdims=True)
+        vn = vn.astype(np.float32)
+    n = n_bodies
+    shapes = np.zeros(n + 1, A.SHAPE_DTYPE)
+    shapes["mesh"] = -1
+    shapes[0]["kind"] = A.SHAPE_CONCAVE_MESH
+    shapes[0]["mesh"] = 0
+    kinds = rng.integers(0, 5 if hulls else 3, size=n)
+    convex = []
+    if hulls:
+        hv, hf = load_hull()
+        convex = [(hv, hf, (0.5, 0.5, 0.5)), (hv, hf, (0.6, 0.4, 0.5))]
+    for i, k in enumerate(kinds):
+        sh = shapes[i + 1]
+        if k == 0:
+            sh["kind"] = A.SHAPE_BOX
+            sh["params"][:3] = rng.uniform(0.2, 0.5, 3)
+        elif k == 1:
+            sh["kind"] = A.SHAPE_SPHERE
+            sh["params"][0] = rng.uniform(0.2, 0.45)
+        elif k == 2:
+            sh["kind"] = A.SHAPE_CAPSULE
+            sh["params"][:2] = (rng.uniform(0.15, 0.25), rng.uniform(0.2, 0.35))
+        else:
+            sh["kind"] = A.SHAPE_CONVEX_MESH
+            sh["mesh"] = int(k - 3)
+    bodies = A.body_descs(n + 1)
+    bodies[0]["type"] = A.BODY_STATIC
+    if terrain_orientation is not None:
+        bodies[0]["orientation"] = terrain_orientation
+    width, length = (cols - 1) * cell * scale[0], (rows - 1) * cell * scale[2]
+    nx = max(1, int((width - 3.0) // spacing) + 1)
+    nz = max(1, int((length - 3.0) // spacing) + 1)
+    per_layer = nx * nz
+    idx = np.arange(n)
+    iy, rem = idx // per_layer, idx % per_layer
+    ix, iz = rem % nx, rem // nx
+    top = float(verts[:, 1][verts[:, 1] < 40.0].max()) * scale[1]
+    centre = np.stack([(ix - 0.5 * (nx - 1)) * spacing, top + 1.5 + iy * spacing,
+                       (iz - 0.5 * (nz - 1)) * spacing], axis=1) + rng.uniform(-0.1, 0.1, size=(n, 3))
+    bodies["position"][1:] = centre.astype(np.float32)
+    bodies["orientation"][1:] = random_quaternions(rng, n)
+    colliders = A.collider_descs(n + 1)
+    colliders["body"] = np.arange(n + 1)
+    colliders["shape"] = np.arange(n + 1)
+    colliders["friction"] = np.float32(0.4)
+    colliders["bounciness"] = 0.0
+    settings = A.default_world_settings()
+    settings["sleeping_enabled"] = 1 if sleeping else 0
+    return WorldScene(settings, shapes, bodies, colliders, f"concave mesh {cols}x{rows} + {n}",
+                      convex_meshes=convex, concave_meshes=[(verts, tris, vn, tuple(map(float, scale)))])

@@ -263,6 +263,33 @@ class RefWorld:
         return out
 
 
+def concave_register(L, vertices, triangles, normals, scale):
+    """Register a triangle mesh + scale with the reference harness; returns its id."""
+    v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+    n = None if normals is None else np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3)
+    return L.ref_concave_register(v.ctypes.data, len(v), t.ctypes.data, len(t), None if n is None else n.ctypes.data,
+                                  *map(float, scale))
+
+
+def ref_triangle_mesh(vertices, triangles, normals=None, prec="f32"):
+    """TriangleMesh of the reference build over these arrays: (vertices,
+    vertex normals, triangles), or None where the reference rejects it."""
+    L = C.CDLL(REF_LIB[prec])
+    P = C.c_void_p
+    L.ref_concave_register.argtypes = [P, C.c_uint32, P, C.c_uint32, P, C.c_float, C.c_float, C.c_float]
+    L.ref_concave_mesh_data.argtypes = [C.c_int, P, P, P, C.c_uint32, C.c_uint32, P, P]
+    cid = concave_register(L, vertices, triangles, normals, (1.0, 1.0, 1.0))
+    nv, nt = C.c_uint32(), C.c_uint32()
+    if L.ref_concave_mesh_data(cid, None, None, None, 0, 0, C.byref(nv), C.byref(nt)) != 0:
+        return None
+    v = np.zeros((nv.value, 3), np.float32)
+    n = np.zeros((nv.value, 3), np.float32)
+    t = np.zeros((nt.value, 3), np.uint32)
+    L.ref_concave_mesh_data(cid, v.ctypes.data, n.ctypes.data, t.ctypes.data, len(v), len(t), C.byref(nv), C.byref(nt))
+    return v, n, t
+
+
 class RefScene:
     """A reference world built from a scenes.WorldScene (oracle/ref_world.cpp
     ref_scene_create, the call sequence of rp3dg_world_create) and stepped by
@@ -289,6 +316,7 @@ class RefScene:
         L.ref_scene_debug_primitives.argtypes = [C.c_int, P, C.c_uint32, P, C.c_uint32, P, P]
         L.ref_convex_register.argtypes = [P, C.c_uint32, P, P, C.c_uint32, C.c_float, C.c_float, C.c_float]
         L.ref_heightfield_register.argtypes = [C.c_uint32, C.c_uint32, P, C.c_float, C.c_float, C.c_float]
+        L.ref_concave_register.argtypes = [P, C.c_uint32, P, C.c_uint32, P, C.c_float, C.c_float, C.c_float]
         # height fields of the scene registered with the harness; the shape
         # table's mesh field then names the harness's ids
         shapes = np.array(scene.shapes, copy=True)
@@ -307,6 +335,9 @@ class RefScene:
                                                 len(faces), *map(float, scale)))
         for i in np.nonzero(shapes["kind"] == A.SHAPE_CONVEX_MESH)[0]:
             shapes["mesh"][i] = cm_ids[int(shapes["mesh"][i])]
+        cc_ids = [concave_register(L, *m) for m in getattr(scene, "concave_meshes", None) or []]
+        for i in np.nonzero(shapes["kind"] == A.SHAPE_CONCAVE_MESH)[0]:
+            shapes["mesh"][i] = cc_ids[int(shapes["mesh"][i])]
         self._keep = (np.ascontiguousarray(scene.settings).copy(), np.ascontiguousarray(shapes),
                       np.ascontiguousarray(scene.bodies), np.ascontiguousarray(scene.colliders))
         st, sh, bd, cd = self._keep

@@ -2,9 +2,10 @@
 after every update the lines and triangles of DebugRenderer::onContact and
 computeDebugRenderingPrimitives (src/utils/DebugRenderer.cpp:482-560) are
 bit-identical to the reference engine's getLinesArray / getTrianglesArray,
-on worlds of boxes, spheres and capsules, of convex meshes, and on a height
-field; with every item shown on every body, and with a subset of the items
-on a subset of the bodies switched on, changed and off between updates."""
+on worlds of boxes, spheres and capsules, of convex meshes, on a height
+field and on a concave mesh; with every item shown on every body, and with
+a subset of the items on a subset of the bodies switched on, changed and
+off between updates."""
 import numpy as np
 import pytest
 
@@ -43,6 +44,8 @@ SCENES = [
     ("mixed", lambda: scenes.mixed_world(nx=3, ny=3, nz=3, seed=5, variety=True), 90),
     ("hulls", lambda: scenes.hull_world(3, 2, 3, seed=44), 90),
     ("terrain", lambda: scenes.heightfield_world(n_bodies=40, cols=12, rows=12, seed=45), 90),
+    ("concave_mesh", lambda: scenes.concave_mesh_world(n_bodies=40, cols=10, rows=10, seed=46, scale=(1.2, 1.0, 0.9)),
+     90),
 ]
 
 
