@@ -539,23 +539,25 @@ cudaError_t launch_partition_by_class(const NpArgs& a, const uint8_t* cls, uint3
 // 32 pairs (one warp):
 //   - the geometric class of a box-box pair: its inscribed spheres overlap
 //     (certainly colliding: full SAT and clipping), its bounding spheres are
-//     apart (certainly separated: a face test ends it), or neither;
+//     apart (certainly separated: a face test ends it), or neither, in which
+//     case a valid last-frame record predicts it (was colliding / separated
+//     by a SAT axis); a pair with a mesh gets its own class, so that box
+//     tiles stay all-box for the thread-per-pair kernel;
 //   - with the learned proposal on, the warp also computes the pairs'
 //     features and runs the MLP on the bf16 tensor cores (mma.sync
 //     m16n8k16, 112 MMAs per tile) and writes each pair's proposed feature
 //     (15 = none) to `proposals`, which the SAT kernels test exactly.
 // `key` receives the order class that partition_count / partition_scatter
-// sort by (class 15 first, then 0..14): plain SAT groups certainly colliding
-// (15), uncertain (0) and certainly separated (1) pairs; the learned path
-// groups by proposal, with the pairs it proposes nothing for among the
-// colliding ones unless they are certainly separated.  Only the order in
-// which the pairs are processed depends on the key.
+// sort by (class 15 first, then 0..14): certainly colliding (15), uncertain
+// (0), certainly separated (1) and mesh pairs (2); the learned proposals do
+// not change the order.  Only the order in which the pairs are processed
+// depends on the key.
 RD uint8_t box_pair_class(const NpArgs& a, uint32_t i) {
     if (i >= a.n) return 0;
     const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
     if (uint32_t(i1) >= a.nb_shapes || uint32_t(i2) >= a.nb_shapes) return 0;
     const ShapeRec r1 = load_shape(a.shapes, i1), r2 = load_shape(a.shapes, i2);
-    if (r1.kind != RP3DG_SHAPE_BOX || r2.kind != RP3DG_SHAPE_BOX) return 0;
+    if (r1.kind != RP3DG_SHAPE_BOX || r2.kind != RP3DG_SHAPE_BOX) return 2;   // a mesh pair: its own tiles
     const float4 p1 = a.pos1[i], p2 = a.pos2[i];
     const float dx = p2.x - p1.x, dy = p2.y - p1.y, dz = p2.z - p1.z;
     const float d2 = dx * dx + dy * dy + dz * dz;
@@ -581,16 +583,35 @@ __global__ void __launch_bounds__(NP_BLOCK) classify_pairs(const NpArgs a, uint8
     const uint32_t nwarps = gridDim.x * (NP_BLOCK / 32);
     for (uint32_t tile = blockIdx.x * (NP_BLOCK / 32) + warp; tile * 32u < a.n; tile += nwarps) {
         const uint32_t i = tile * 32u + lane;
-        const uint8_t geo = box_pair_class(a, i);
+        uint8_t geo = box_pair_class(a, i);
+        // an uncertain box pair with a last-frame record follows last
+        // frame's outcome: colliding pairs clip, SAT-separated ones usually
+        // end at the remembered axis
+        if (geo == 0 && i < a.n && a.cache) {
+            const uint8_t f = a.cache[i].flags;
+            if (f & RP3DG_LF_IS_VALID) geo = (f & RP3DG_LF_WAS_COLLIDING) ? 15 : ((f & RP3DG_LF_WAS_USING_SAT) ? 1 : 0);
+        }
         uint8_t k = geo;
         if (learned) {
-            pair_features(a, i, &s_box, a.mesh_words, s_feat[warp][lane]);
-            __syncwarp();
-            uint32_t c = mlp_infer_tile(s_feat[warp], *static_cast<const MlpPacked*>(a.mlp), lane, s_cls[warp]);
-            if (c >= MLP_OUT) c = MLP_NO_PROPOSAL;
+            // a proposal is only looked at where the full SAT starts: not for
+            // pairs that certainly collide or are certainly apart (geometric
+            // class), nor, mostly, for pairs whose SAT cache from the last
+            // frame is tested first; a tile none of whose pairs needs one
+            // skips the features and the MLP
+            bool need = i < a.n && (geo == 0 || geo == 2);
+            if (need && a.cache) {
+                const uint8_t f = a.cache[i].flags;
+                if ((f & RP3DG_LF_IS_VALID) && (f & RP3DG_LF_WAS_USING_SAT)) need = false;
+            }
+            uint32_t c = MLP_NO_PROPOSAL;
+            if (__any_sync(0xffffffffu, need)) {
+                pair_features(a, i, &s_box, a.mesh_words, s_feat[warp][lane]);
+                __syncwarp();
+                c = mlp_infer_tile(s_feat[warp], *static_cast<const MlpPacked*>(a.mlp), lane, s_cls[warp]);
+                if (c >= MLP_OUT || !need) c = MLP_NO_PROPOSAL;
+                __syncwarp();
+            }
             if (i < a.n) proposals[i] = uint8_t(c);
-            k = (geo == 15 || c >= 15) ? (geo == 1 ? uint8_t(1) : uint8_t(15)) : uint8_t(c);
-            __syncwarp();
         }
         if (i < a.n) key[i] = k;
     }

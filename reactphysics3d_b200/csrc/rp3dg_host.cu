@@ -1085,11 +1085,12 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
         // an order key and a proposal byte per pair, in a buffer that grows
         // with the batch
         if (p->n > ctx->cap_proposals) {
+            const uint32_t c = std::max(p->n, 2 * ctx->cap_proposals);
             cudaFree(ctx->d_proposals);
             ctx->d_proposals = nullptr;
-            cudaError_t e = cudaMalloc(&ctx->d_proposals, 2 * size_t(p->n));
+            cudaError_t e = cudaMalloc(&ctx->d_proposals, 2 * size_t(c));
             if (e != cudaSuccess) { ctx->cap_proposals = 0; return cuda_fail(ctx, e, "cudaMalloc(proposals)"); }
-            ctx->cap_proposals = p->n;
+            ctx->cap_proposals = c;
         }
         uint8_t* key = ctx->d_proposals;
         uint8_t* prop = ctx->d_proposals + p->n;
@@ -1099,11 +1100,12 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
         if (learned) a.proposals = prop;
         // tiles of one learned class each (the order only, not the results)
         if (p->n > ctx->cap_perm) {
+            const uint32_t c = std::max(p->n, 2 * ctx->cap_perm);
             cudaFree(ctx->d_perm);
             ctx->d_perm = nullptr;
-            e = cudaMalloc(&ctx->d_perm, (size_t(p->n) + 32) * sizeof(uint32_t));
+            e = cudaMalloc(&ctx->d_perm, (size_t(c) + 32) * sizeof(uint32_t));
             if (e != cudaSuccess) { ctx->cap_perm = 0; return cuda_fail(ctx, e, "cudaMalloc(pair order)"); }
-            ctx->cap_perm = p->n;
+            ctx->cap_perm = c;
         }
         e = rp3dg::launch_partition_by_class(a, key, ctx->d_perm + p->n, ctx->d_perm, ctx->stream);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "pair grouping");
@@ -1517,13 +1519,16 @@ int narrowphase_tri_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch
 
 namespace {
 
+// Device scratch that only grows, doubling, so that a world whose sizes creep
+// up step after step reallocates (a cudaFree waits for the device) rarely.
 int grow(rp3dg_ctx* ctx, void** buf, size_t* cap, size_t need, const char* what) {
     if (need <= *cap) return 0;
+    const size_t n = std::max(need, 2 * *cap);
     cudaFree(*buf);
     *buf = nullptr;
-    cudaError_t e = cudaMalloc(buf, need);
+    cudaError_t e = cudaMalloc(buf, n);
     if (e != cudaSuccess) { *cap = 0; *buf = nullptr; return cuda_fail(ctx, e, what); }
-    *cap = need;
+    *cap = n;
     return 0;
 }
 

@@ -2243,6 +2243,14 @@ int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds
             }
         }
     }
+    // the narrow phase's step buffers sized up front for twice as many convex
+    // pairs as colliders: growing them later frees and maps hundreds of MB
+    // (16 contact slots per pair), which stalls the step that does it
+    rc = ensure_items(g, 2 * size_t(g->NC) + 1024);
+    if (rc) {
+        destroy_group(g);
+        return rc;
+    }
     *out = g;
     return 0;
 }
