@@ -193,7 +193,9 @@ def run_ours(args):
     hbm_peak, peak_src = peaks()
     achieved = alg_bytes / (mean_batch[dom] / 1e3) / 1e9
     share = {nm: round(mean_batch[nm] / sum(mean_batch.values()), 4) for nm in names}
-    roofline = {"bound": "hbm", "kernel": f"narrowphase_kernel<{algos[dom]}> ({dom})", "achieved": round(achieved, 2),
+    label = ("narrowphase_kernel<7> + narrowphase_warp_kernel<mesh-box>" if algos[dom] == 6
+             else f"narrowphase_kernel<{algos[dom]}>")
+    roofline = {"bound": "hbm", "kernel": f"{label} ({dom})", "achieved": round(achieved, 2),
                 "peak": hbm_peak, "unit": "GB/s", "frac": round(achieved / hbm_peak, 5), "traffic": None,
                 "peak_source": peak_src, "kernel_ms": round(mean_batch[dom], 4), "share": share,
                 "note": "FP32 SAT/GJK kernels are issue/latency-bound; HBM fraction is reported because no "

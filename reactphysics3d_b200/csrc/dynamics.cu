@@ -1568,6 +1568,19 @@ __global__ void __launch_bounds__(128) color_tentative(const DynArgs a, ColorScr
     c.tent[mi] = t;   // NO_COLOR: every colour is taken (the caller falls back)
 }
 
+// Priority of a manifold in the conflict resolution: a hash of its index
+// (ties by index).  Index order itself follows the islands, i.e. space, so a
+// pile would chain "lower index wins" decisions over hundreds of rounds; a
+// hashed order resolves every round's conflicts independently of position
+// (a few rounds to colour the 100k-body terrain's island).
+RD uint64_t color_priority(uint32_t mi) {
+    uint32_t h = mi * 0x9E3779B1u;
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    return (uint64_t(h) << 32) | mi;
+}
+
 __global__ void __launch_bounds__(128) color_resolve(const DynArgs a, ColorScratch c) {
     const uint32_t mi = blockIdx.x * blockDim.x + threadIdx.x;
     if (mi >= a.nm) return;
@@ -1583,7 +1596,7 @@ __global__ void __launch_bounds__(128) color_resolve(const DynArgs a, ColorScrat
         const int32_t b = side ? id.y : id.x;
         for (uint32_t k = c.start[b]; k < c.start[b + 1]; k++) {
             const uint32_t n = c.adj[k];
-            if (n < mi && c.tent[n] == t) {
+            if (n != mi && c.tent[n] == t && color_priority(n) < color_priority(mi)) {
                 atomicAdd(c.count + COLOR_MAX, 1u);
                 return;
             }
@@ -1699,7 +1712,7 @@ bool colored_islands(const DynArgs& a, cudaStream_t s, uint64_t* launches) {
     *launches += 3;
     uint32_t rounds = 0, remaining = nm;
     while (remaining > 0) {
-        if (++rounds > 64) return false;
+        if (++rounds > 256) return false;
         cudaMemsetAsync(c.count + COLOR_MAX, 0, 4, s);
         color_tentative<<<blocks(nm), 128, 0, s>>>(a, c);
         color_resolve<<<blocks(nm), 128, 0, s>>>(a, c);

@@ -11,12 +11,15 @@
 
 // Kernel tuning knobs (compile time): resident CTAs per SM requested from the
 // register allocator, for the closed-form/GJK kernels, the warp-per-pair
-// polyhedron kernel and the thread-per-pair polyhedron kernel.
+// polyhedron kernels (one per shape combination, each with one SAT
+// instantiation: 5 CTAs of 96 registers without spills, 7% faster on the
+// hull-box batch than 4 CTAs) and the thread-per-pair polyhedron kernel
+// (box-box only: 103 registers at 4 CTAs; at 5 it spills and is slower).
 #ifndef RP3DG_NP_MIN_BLOCKS
 #define RP3DG_NP_MIN_BLOCKS 4
 #endif
 #ifndef RP3DG_NP_MIN_BLOCKS_POLY_WARP
-#define RP3DG_NP_MIN_BLOCKS_POLY_WARP 4
+#define RP3DG_NP_MIN_BLOCKS_POLY_WARP 5
 #endif
 #ifndef RP3DG_NP_MIN_BLOCKS_POLY_THREAD
 #define RP3DG_NP_MIN_BLOCKS_POLY_THREAD 4
@@ -154,7 +157,8 @@ RD uint32_t process_pair(const NpArgs& a, uint32_t i, const BoxTables* box, cons
     }
     const ShapeRec s1 = load_shape(a.shapes, i1);
     const ShapeRec s2 = load_shape(a.shapes, i2);
-    if (!kinds_match(ALGO, s1.kind, s2.kind)) {
+    constexpr int CHECK = ALGO == ALGO_POLY_PER_THREAD ? int(RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON) : ALGO;
+    if (!kinds_match(CHECK, s1.kind, s2.kind)) {
         // a pair the algorithm does not handle (a concave shape has no pair
         // test of its own: it goes through the middle phase's triangles)
         a.is_colliding[i] = 0;
@@ -188,6 +192,11 @@ RD uint32_t process_pair(const NpArgs& a, uint32_t i, const BoxTables* box, cons
         const CapsuleS cap{cs.params.x, cs.params.y};
         if (ps.kind == RP3DG_SHAPE_BOX) capsule_poly(it, cap1, cap, box_poly(ps, box));
         else capsule_poly(it, cap1, cap, mesh_poly(mesh_words, ps.mesh));
+    } else if (ALGO == ALGO_POLY_PER_THREAD) {
+        // the thread-per-pair launch is given box-box pairs only
+        sat_poly_poly(it, box_poly(s1, box), box_poly(s2, box), a.clip);
+        it.lf.set(RP3DG_LF_WAS_USING_SAT, true);
+        it.lf.set(RP3DG_LF_WAS_USING_GJK, false);
     } else {
         const bool b1 = s1.kind == RP3DG_SHAPE_BOX, b2 = s2.kind == RP3DG_SHAPE_BOX;
         if (b1 && b2) sat_poly_poly(it, box_poly(s1, box), box_poly(s2, box), a.clip);
@@ -261,7 +270,14 @@ RD void process_tri(const NpArgs& a, uint32_t i, const BoxTables* box, const uin
     store_item(a, i, it);
 }
 
-// Convex polyhedron vs convex polyhedron, one warp per pair.
+// Shape combinations of the polyhedron pairs a warp-per-pair launch takes:
+// each launch is compiled for one, so it carries one SAT instantiation
+// (fewer registers, a smaller code footprint)
+constexpr int COMBO_MESH_BOX = 1, COMBO_BOX_MESH = 2, COMBO_MESH_MESH = 3;
+
+// Convex polyhedron vs convex polyhedron, one warp per pair, for pairs of
+// shape combination COMBO.
+template <int COMBO>
 RD uint32_t process_pair_warp(const NpArgs& a, uint32_t i, int lane, const BoxTables* box, const uint32_t* mesh_words,
                               WarpScratch& stage, uint32_t proposal) {
     const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
@@ -286,11 +302,12 @@ RD uint32_t process_pair_warp(const NpArgs& a, uint32_t i, int lane, const BoxTa
     Item it;
     load_item(a, i, it);
     it.proposal = proposal;
-    const bool b1 = s1.kind == RP3DG_SHAPE_BOX, b2 = s2.kind == RP3DG_SHAPE_BOX;
-    if (b1 && b2) warp_sat_poly_poly(it, box_poly(s1, box), box_poly(s2, box), a.clip, lane, stage);
-    else if (!b1 && b2) warp_sat_poly_poly(it, mesh_poly(mesh_words, s1.mesh), box_poly(s2, box), a.clip, lane, stage);
-    else if (b1 && !b2) warp_sat_poly_poly(it, box_poly(s1, box), mesh_poly(mesh_words, s2.mesh), a.clip, lane, stage);
-    else warp_sat_poly_poly(it, mesh_poly(mesh_words, s1.mesh), mesh_poly(mesh_words, s2.mesh), a.clip, lane, stage);
+    if constexpr (COMBO == COMBO_MESH_BOX)
+        warp_sat_poly_poly(it, mesh_poly(mesh_words, s1.mesh), box_poly(s2, box), a.clip, lane, stage);
+    else if constexpr (COMBO == COMBO_BOX_MESH)
+        warp_sat_poly_poly(it, box_poly(s1, box), mesh_poly(mesh_words, s2.mesh), a.clip, lane, stage);
+    else
+        warp_sat_poly_poly(it, mesh_poly(mesh_words, s1.mesh), mesh_poly(mesh_words, s2.mesh), a.clip, lane, stage);
     // ConvexPolyhedronVsConvexPolyhedronAlgorithm.cpp:53-61
     it.lf.set(RP3DG_LF_WAS_USING_SAT, true);
     it.lf.set(RP3DG_LF_WAS_USING_GJK, false);
@@ -341,83 +358,48 @@ __global__ void __launch_bounds__(NP_BLOCK, MinBlocks<ALGO>::value) narrowphase_
         }
         __syncthreads();
     }
-    if constexpr (ALGO == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON || ALGO == ALGO_POLY_PER_THREAD) {
-        // Polyhedron pairs are split by tiles of 32 consecutive pairs: a tile
-        // whose pairs are all box-box (12 x 12 edge pairs) is done one pair per
-        // thread by the ALGO_POLY_PER_THREAD launch; any other tile (it holds a
-        // convex mesh, up to 128 x 128 edge pairs) is done one pair at a time
-        // by a whole warp in the ALGO 6 launch.  Both launches read the same
-        // tiles, so every pair is processed exactly once.
-        __shared__ WarpScratch s_stage[NP_BLOCK / 32];
+    if constexpr (ALGO == ALGO_POLY_PER_THREAD) {
+        // Polyhedron pairs by tiles of 32 (in the class order of the pair
+        // order perm): the box-box pairs of a tile (12 x 12 edge pairs) are
+        // done one per thread here; a pair with a convex mesh (up to 128 x 128
+        // edge pairs) is appended to the list of its shape combination, which
+        // a warp-per-pair launch of that combination then takes.
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const uint32_t nwarps = gridDim.x * (NP_BLOCK / 32);
         uint32_t tested = 0, confirmed = 0;
-        if (ALGO == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON && a.tiles) {
-            // persistent warps over the pairs of the tiles the thread-per-pair
-            // launch left (listed by it, in any order): one pair at a time, so
-            // the launch ends within one pair's time of its average
-            const uint32_t total = 32u * __ldcg(a.work);
-            WarpScratch& ws = s_stage[warp];
-            for (;;) {
-                uint32_t k = 0;
-                if (lane == 0) k = atomicAdd(a.work + 1, 1u);
-                k = __shfl_sync(FULL_MASK, k, 0);
-                if (k >= total) break;
-                const uint32_t t = a.tiles[k >> 5] * 32u + (k & 31u);
-                if (t >= a.n) continue;
-                const uint32_t i = a.perm ? a.perm[t] : t;
-                uint32_t proposal = a.proposals ? uint32_t(a.proposals[i]) : uint32_t(MLP_NO_PROPOSAL);
-                if (proposal >= MLP_OUT) proposal = MLP_NO_PROPOSAL;
-                const uint32_t r = process_pair_warp(a, i, lane, &s_box, mesh_words, ws, proposal);
-                tested += r & 1u;
-                confirmed += (r >> 1) & 1u;
-                __syncwarp();
-            }
-            if (a.mlp_stats && lane == 0 && tested) {
-                atomicAdd(&a.mlp_stats[0], (unsigned long long)tested);
-                atomicAdd(&a.mlp_stats[1], (unsigned long long)confirmed);
-            }
-            return;
-        }
         for (uint32_t tile = blockIdx.x * (NP_BLOCK / 32) + warp; tile * 32u < a.n; tile += nwarps) {
             const uint32_t t = tile * 32u + lane;
             const uint32_t i = (a.perm && t < a.n) ? a.perm[t] : t;
-            bool boxbox = t >= a.n;  // lanes past the end do not force the warp path
-            if (i < a.n) {
+            int combo = 0;   // box-box, or a pair whose check fails in process_pair
+            if (t < a.n) {
                 const int32_t i1 = a.shape1[i], i2 = a.shape2[i];
                 if (uint32_t(i1) < a.nb_shapes && uint32_t(i2) < a.nb_shapes) {
                     const ShapeRec r1 = load_shape(a.shapes, i1), r2 = load_shape(a.shapes, i2);
-                    boxbox = r1.kind == RP3DG_SHAPE_BOX && r2.kind == RP3DG_SHAPE_BOX;
+                    if (is_poly_kind(r1.kind) && is_poly_kind(r2.kind)) {
+                        const bool b1 = r1.kind == RP3DG_SHAPE_BOX, b2 = r2.kind == RP3DG_SHAPE_BOX;
+                        combo = (b1 && b2) ? 0 : (!b1 && b2) ? COMBO_MESH_BOX : (b1 ? COMBO_BOX_MESH : COMBO_MESH_MESH);
+                    }
                 }
             }
-            const bool all_box = __all_sync(FULL_MASK, boxbox);
-            if (ALGO == ALGO_POLY_PER_THREAD && !all_box && a.tiles && lane == 0) a.tiles[atomicAdd(a.work, 1u)] = tile;
-            if ((ALGO == ALGO_POLY_PER_THREAD) != all_box) continue;  // the other launch takes this tile
-            WarpScratch& ws = s_stage[warp];
+            for (int c = COMBO_MESH_BOX; c <= COMBO_MESH_MESH; c++) {
+                const uint32_t m = __ballot_sync(FULL_MASK, combo == c);
+                if (!m) continue;
+                const int leader = __ffs(m) - 1;
+                uint32_t base = 0;
+                if (lane == leader) base = atomicAdd(a.work + (c - 1), uint32_t(__popc(m)));
+                base = __shfl_sync(FULL_MASK, base, leader);
+                if (combo == c) a.plist[size_t(c - 1) * a.n + base + uint32_t(__popc(m & ((1u << lane) - 1u)))] = i;
+            }
             uint32_t proposal = MLP_NO_PROPOSAL;
-            if (a.proposals) {
-                // learned proposals written by narrowphase_propose for this batch
-                proposal = t < a.n ? a.proposals[i] : uint32_t(MLP_NO_PROPOSAL);
+            if (a.proposals && t < a.n) {
+                proposal = a.proposals[i];
                 if (proposal >= MLP_OUT) proposal = MLP_NO_PROPOSAL;
-                ws.cls[lane] = proposal;
-                __syncwarp();
             }
-            if (ALGO == ALGO_POLY_PER_THREAD) {
-                uint32_t r = 0;
-                if (t < a.n) r = process_pair<RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON>(a, i, &s_box, mesh_words, proposal);
-                tested += __popc(__ballot_sync(FULL_MASK, r & 1u));
-                confirmed += __popc(__ballot_sync(FULL_MASK, (r & 2u) != 0));
-            } else {
-                const uint32_t cnt = a.n - tile * 32u < 32u ? a.n - tile * 32u : 32u;
-                for (uint32_t l = 0; l < cnt; l++) {
-                    const uint32_t tl = tile * 32u + l;
-                    const uint32_t r = process_pair_warp(a, a.perm ? a.perm[tl] : tl, lane, &s_box, mesh_words, ws,
-                                                         a.proposals ? ws.cls[l] : uint32_t(MLP_NO_PROPOSAL));
-                    tested += r & 1u;
-                    confirmed += (r >> 1) & 1u;
-                }
-            }
-            __syncwarp();
+            uint32_t r = 0;
+            if (t < a.n && combo == 0)
+                r = process_pair<ALGO_POLY_PER_THREAD>(a, i, &s_box, mesh_words, proposal);
+            tested += __popc(__ballot_sync(FULL_MASK, r & 1u));
+            confirmed += __popc(__ballot_sync(FULL_MASK, (r & 2u) != 0));
         }
         if (a.mlp_stats && lane == 0 && tested) {
             atomicAdd(&a.mlp_stats[0], (unsigned long long)tested);
@@ -427,6 +409,52 @@ __global__ void __launch_bounds__(NP_BLOCK, MinBlocks<ALGO>::value) narrowphase_
         const uint32_t stride = gridDim.x * blockDim.x;
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride)
             process_pair<ALGO>(a, i, &s_box, mesh_words);
+    }
+}
+
+// The pairs with a convex mesh of one shape combination, listed by the
+// thread-per-pair launch: persistent warps take them one at a time (so the
+// launch ends within one pair's time of its average), faces over lanes
+// (ballot / arg-min), edge staging in shared memory, the Gauss-map pass and
+// the edge distances 32 at a time, warp-parallel clipping.
+template <int COMBO>
+__global__ void __launch_bounds__(NP_BLOCK, NP_MIN_BLOCKS_POLY_WARP) narrowphase_warp_kernel(const NpArgs a) {
+    extern __shared__ uint32_t s_mesh[];
+    __shared__ BoxTables s_box;
+    __shared__ WarpScratch s_stage[NP_BLOCK / 32];
+    const uint32_t total = __ldcg(a.work + (COMBO - 1));
+    if (total == 0) return;   // uniform: nothing of this combination in the batch
+    const uint32_t* mesh_words = a.mesh_words;
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&c_box_tables);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&s_box);
+        for (uint32_t k = threadIdx.x; k < sizeof(BoxTables) / 4; k += blockDim.x) dst[k] = src[k];
+        if (a.stage_mesh) {
+            for (uint32_t k = threadIdx.x; k < a.mesh_nwords; k += blockDim.x) s_mesh[k] = __ldg(a.mesh_words + k);
+            mesh_words = s_mesh;
+        }
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpScratch& ws = s_stage[warp];
+    const uint32_t* list = a.plist + size_t(COMBO - 1) * a.n;
+    uint32_t tested = 0, confirmed = 0;
+    for (;;) {
+        uint32_t k = 0;
+        if (lane == 0) k = atomicAdd(a.work + 3 + (COMBO - 1), 1u);
+        k = __shfl_sync(FULL_MASK, k, 0);
+        if (k >= total) break;
+        const uint32_t i = list[k];
+        uint32_t proposal = a.proposals ? uint32_t(a.proposals[i]) : uint32_t(MLP_NO_PROPOSAL);
+        if (proposal >= MLP_OUT) proposal = MLP_NO_PROPOSAL;
+        const uint32_t r = process_pair_warp<COMBO>(a, i, lane, &s_box, mesh_words, ws, proposal);
+        tested += r & 1u;
+        confirmed += (r >> 1) & 1u;
+        __syncwarp();
+    }
+    if (a.mlp_stats && lane == 0 && tested) {
+        atomicAdd(&a.mlp_stats[0], (unsigned long long)tested);
+        atomicAdd(&a.mlp_stats[1], (unsigned long long)confirmed);
     }
 }
 
@@ -633,7 +661,9 @@ static const void* kernel_ptr(int algo) {
         case 3: return reinterpret_cast<const void*>(&narrowphase_kernel<3>);
         case 4: return reinterpret_cast<const void*>(&narrowphase_kernel<4>);
         case 5: return reinterpret_cast<const void*>(&narrowphase_kernel<5>);
-        case 6: return reinterpret_cast<const void*>(&narrowphase_kernel<6>);
+        case 8 + COMBO_MESH_BOX: return reinterpret_cast<const void*>(&narrowphase_warp_kernel<COMBO_MESH_BOX>);
+        case 8 + COMBO_BOX_MESH: return reinterpret_cast<const void*>(&narrowphase_warp_kernel<COMBO_BOX_MESH>);
+        case 8 + COMBO_MESH_MESH: return reinterpret_cast<const void*>(&narrowphase_warp_kernel<COMBO_MESH_MESH>);
         case ALGO_POLY_PER_THREAD: return reinterpret_cast<const void*>(&narrowphase_kernel<ALGO_POLY_PER_THREAD>);
     }
     return nullptr;
@@ -662,13 +692,20 @@ cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaSt
     *launches = 0;
     if (args.n == 0) return cudaSuccess;
     if (algo == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON) {
-        if (args.tiles) {
-            cudaError_t e = cudaMemsetAsync(args.work, 0, 2 * sizeof(uint32_t), stream);
-            if (e != cudaSuccess) return e;
-        }
-        cudaError_t e = launch_one(ALGO_POLY_PER_THREAD, args, num_sms, stream);
+        // the thread-per-pair launch (box-box pairs, and the lists of the
+        // mesh pairs), then one warp-per-pair launch per shape combination
+        if (!args.plist || !args.work) return cudaErrorInvalidValue;
+        cudaError_t e = cudaMemsetAsync(args.work, 0, 6 * sizeof(uint32_t), stream);
+        if (e != cudaSuccess) return e;
+        e = launch_one(ALGO_POLY_PER_THREAD, args, num_sms, stream);
         if (e != cudaSuccess) return e;
         ++*launches;
+        for (int c = COMBO_MESH_BOX; c <= COMBO_MESH_MESH; c++) {
+            e = launch_one(8 + c, args, num_sms, stream);
+            if (e != cudaSuccess) return e;
+            ++*launches;
+        }
+        return cudaSuccess;
     }
     cudaError_t e = launch_one(algo, args, num_sms, stream);
     if (e == cudaSuccess) ++*launches;
@@ -678,6 +715,7 @@ cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaSt
 static cudaError_t launch_one(int algo, const NpArgs& args, int num_sms, cudaStream_t stream) {
     const void* k = kernel_ptr(algo);
     if (!k) return cudaErrorInvalidValue;
+    const bool warp_list = algo > 8;   // narrowphase_warp_kernel<algo - 8>
     size_t smem = (args.stage_mesh && algo != ALGO_POLY_PER_THREAD) ? size_t(args.mesh_nwords) * 4 : 0;
     cudaFuncAttributes fa;
     cudaError_t e = cudaFuncGetAttributes(&fa, k);
@@ -691,7 +729,7 @@ static cudaError_t launch_one(int algo, const NpArgs& args, int num_sms, cudaStr
     // Enough CTAs to fill every SM several times; the grid-stride loop covers the rest.
     const uint32_t cap = uint32_t(num_sms) * 16u;
     uint32_t blocks = blocks_needed < cap ? blocks_needed : cap;
-    if (algo == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON && args.tiles) {
+    if (warp_list) {
         // persistent: the CTAs that fit on the device at once
         int per_sm = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NP_BLOCK, smem);

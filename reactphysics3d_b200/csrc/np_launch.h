@@ -49,11 +49,13 @@ struct NpArgs {
     // event-counting build only: NP_EVENT_COUNT counters (NpEvent order) the
     // kernels add each pair's path events to; ignored by the product kernels
     unsigned long long* events = nullptr;
-    // polyhedron batches, when set: the thread-per-pair launch appends every
-    // tile it leaves to the warp-per-pair launch to `tiles` (count in
-    // work[0]); the warp-per-pair launch is then persistent and its warps take
-    // those tiles' pairs one at a time (counter work[1])
-    uint32_t* tiles = nullptr;
+    // polyhedron batches (required): the thread-per-pair launch does the
+    // box-box pairs and appends each pair with a convex mesh to the list of
+    // its shape combination c (mesh-box 1, box-mesh 2, mesh-mesh 3) at
+    // plist[(c - 1) * n + k], counted in work[c - 1]; the persistent
+    // warp-per-pair launch of combination c takes them one at a time
+    // (counter work[3 + c - 1])
+    uint32_t* plist = nullptr;
     uint32_t* work = nullptr;
 };
 

@@ -223,9 +223,9 @@ struct rp3dg_ctx {
     uint32_t* d_error = nullptr;
     // path-event counters of rp3dg_narrowphase_count_events (NP_EVENT_COUNT words)
     unsigned long long* d_events = nullptr;
-    // polyhedron batches: tiles for the warp-per-pair launch and two counters
-    uint32_t* d_tiles = nullptr;
-    size_t cap_tiles = 0;
+    // polyhedron batches: the lists of mesh pairs by shape combination and their counters
+    uint32_t* d_plist = nullptr;
+    size_t cap_plist = 0;
     // staging buffers for rp3dg_narrowphase_host
     void* d_stage = nullptr;
     size_t cap_stage = 0;
@@ -456,7 +456,7 @@ void rp3dg_destroy(rp3dg_ctx* ctx) {
     cudaFree(ctx->d_stage);
     cudaFree(ctx->d_error);
     cudaFree(ctx->d_events);
-    cudaFree(ctx->d_tiles);
+    cudaFree(ctx->d_plist);
     cudaFree(ctx->d_mlp);
     cudaFree(ctx->d_mlp_scratch);
     cudaFree(ctx->d_proposals);
@@ -1052,17 +1052,17 @@ int np_args(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p, const rp3d
     a.tri = nullptr;
     a.perm = nullptr;
     a.events = nullptr;
-    a.tiles = nullptr;
+    a.plist = nullptr;
     a.work = nullptr;
     if (algorithm == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON) {
-        // tile list (one word per tile of 32 pairs) and its two counters
-        const size_t words = (size_t(p->n) + 31) / 32 + 2;
+        // the mesh pairs' lists (three of n words) after their six counters
+        const size_t words = 3 * size_t(p->n) + 8;
         cudaSetDevice(ctx->device);
-        const int rc = grow(ctx, reinterpret_cast<void**>(&ctx->d_tiles), &ctx->cap_tiles, words * 4,
-                            "cudaMalloc(polyhedron tiles)");
+        const int rc = grow(ctx, reinterpret_cast<void**>(&ctx->d_plist), &ctx->cap_plist, words * 4,
+                            "cudaMalloc(polyhedron pair lists)");
         if (rc) return rc;
-        a.work = ctx->d_tiles;
-        a.tiles = ctx->d_tiles + 2;
+        a.work = ctx->d_plist;
+        a.plist = ctx->d_plist + 8;
     }
     return 0;
 }

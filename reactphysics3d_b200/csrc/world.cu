@@ -1568,8 +1568,8 @@ int ensure_items(Group* g, size_t n) {
     return 0;
 }
 
-int ensure_pool(Group* g) {
-    const size_t need = g->cache_next.load();
+int ensure_pool(Group* g, size_t reserve = 0) {
+    const size_t need = std::max<size_t>(g->cache_next.load(), reserve);
     if (need <= g->cap_pool) return 0;
     size_t c = std::max<size_t>(need, g->cap_pool * 2);
     c = std::max<size_t>(c, 1024);
@@ -2057,6 +2057,8 @@ int build_world(Group* g, WorldH& w, const rp3dg_body_desc* bd, uint32_t nb, con
     return 0;
 }
 
+int ensure_manifold_staging(Group* g, uint32_t NM, uint32_t NI);
+
 int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds, const uint32_t* boff,
                  const rp3dg_body_desc* bd, const uint32_t* coff, const rp3dg_collider_desc* cd, int nthreads,
                  Group** out) {
@@ -2247,11 +2249,50 @@ int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds
     // pairs as colliders: growing them later frees and maps hundreds of MB
     // (16 contact slots per pair), which stalls the step that does it
     rc = ensure_items(g, 2 * size_t(g->NC) + 1024);
+    // and, for the same reason, the manifold staging, the island arrays and
+    // both contact buffers for as many manifolds as colliders (two points each)
+    if (!rc) rc = ensure_manifold_staging(g, g->NC, g->NC / 2 + 64);
+    if (!rc) rc = ensure_pool(g, 2 * size_t(g->NC) + 1024);
+    if (!rc && (g->cbuf[0].ensure(g->NC + 64, 2 * g->NC + 64) || g->cbuf[1].ensure(g->NC + 64, 2 * g->NC + 64)))
+        rc = wfail(g, RP3DG_ENOMEM, "cudaMalloc(contacts)");
     if (rc) {
         destroy_group(g);
         return rc;
     }
     *out = g;
+    return 0;
+}
+
+// Manifold staging (ids, sources, previous manifolds) and island arrays of a
+// step, grown to twice what is needed.
+int ensure_manifold_staging(Group* g, uint32_t NM, uint32_t NI) {
+    if (g->cap_hm < NM || !g->h_mids) {
+        const size_t cap = std::max<size_t>(size_t(NM) * 2, 64);
+        cudaFreeHost(g->h_mids); cudaFreeHost(g->h_msrc); cudaFreeHost(g->h_mprev);
+        cudaFree(g->d_mids); cudaFree(g->d_msrc); cudaFree(g->d_mprev);
+        g->h_mids = g->h_msrc = g->h_mprev = nullptr;
+        g->d_mids = g->d_msrc = g->d_mprev = nullptr;
+        g->cap_hm = 0;
+        if (cudaMallocHost(&g->h_mids, cap * 16) || cudaMallocHost(&g->h_msrc, cap * 16) ||
+            cudaMallocHost(&g->h_mprev, cap * 16) || cudaMalloc(&g->d_mids, cap * 16) ||
+            cudaMalloc(&g->d_msrc, cap * 16) || cudaMalloc(&g->d_mprev, cap * 16))
+            return wfail(g, RP3DG_ENOMEM, "allocation of manifold staging");
+        g->cap_hm = cap;
+    }
+    if (g->cap_hi < NI || !g->h_istart) {
+        const size_t cap = std::max<size_t>(size_t(NI) * 2, 64);
+        cudaFreeHost(g->h_istart); cudaFreeHost(g->h_icount); cudaFree(g->d_istart); cudaFree(g->d_icount);
+        cudaFreeHost(g->h_ijstart); cudaFreeHost(g->h_ijcount); cudaFree(g->d_ijstart); cudaFree(g->d_ijcount);
+        g->h_istart = g->h_icount = g->h_ijstart = g->h_ijcount = nullptr;
+        g->d_istart = g->d_icount = g->d_ijstart = g->d_ijcount = nullptr;
+        g->cap_hi = 0;
+        if (cudaMallocHost(&g->h_istart, cap * 4) || cudaMallocHost(&g->h_icount, cap * 4) ||
+            cudaMalloc(&g->d_istart, cap * 4) || cudaMalloc(&g->d_icount, cap * 4) ||
+            cudaMallocHost(&g->h_ijstart, cap * 4) || cudaMallocHost(&g->h_ijcount, cap * 4) ||
+            cudaMalloc(&g->d_ijstart, cap * 4) || cudaMalloc(&g->d_ijcount, cap * 4))
+            return wfail(g, RP3DG_ENOMEM, "allocation of island arrays");
+        g->cap_hi = cap;
+    }
     return 0;
 }
 
@@ -2596,33 +2637,8 @@ int update_group(Group* g, float dt) {
     g->stats.manifolds = NM;
     g->stats.contact_points = NP;
     g->stats.islands = NI;
-    if (g->cap_hm < NM || !g->h_mids) {
-        const size_t cap = std::max<size_t>(size_t(NM) * 2, 64);
-        cudaFreeHost(g->h_mids); cudaFreeHost(g->h_msrc); cudaFreeHost(g->h_mprev);
-        cudaFree(g->d_mids); cudaFree(g->d_msrc); cudaFree(g->d_mprev);
-        g->h_mids = g->h_msrc = g->h_mprev = nullptr;
-        g->d_mids = g->d_msrc = g->d_mprev = nullptr;
-        g->cap_hm = 0;
-        if (cudaMallocHost(&g->h_mids, cap * 16) || cudaMallocHost(&g->h_msrc, cap * 16) ||
-            cudaMallocHost(&g->h_mprev, cap * 16) || cudaMalloc(&g->d_mids, cap * 16) ||
-            cudaMalloc(&g->d_msrc, cap * 16) || cudaMalloc(&g->d_mprev, cap * 16))
-            return wfail(g, RP3DG_ENOMEM, "allocation of manifold staging");
-        g->cap_hm = cap;
-    }
-    if (g->cap_hi < NI || !g->h_istart) {
-        const size_t cap = std::max<size_t>(size_t(NI) * 2, 64);
-        cudaFreeHost(g->h_istart); cudaFreeHost(g->h_icount); cudaFree(g->d_istart); cudaFree(g->d_icount);
-        cudaFreeHost(g->h_ijstart); cudaFreeHost(g->h_ijcount); cudaFree(g->d_ijstart); cudaFree(g->d_ijcount);
-        g->h_istart = g->h_icount = g->h_ijstart = g->h_ijcount = nullptr;
-        g->d_istart = g->d_icount = g->d_ijstart = g->d_ijcount = nullptr;
-        g->cap_hi = 0;
-        if (cudaMallocHost(&g->h_istart, cap * 4) || cudaMallocHost(&g->h_icount, cap * 4) ||
-            cudaMalloc(&g->d_istart, cap * 4) || cudaMalloc(&g->d_icount, cap * 4) ||
-            cudaMallocHost(&g->h_ijstart, cap * 4) || cudaMallocHost(&g->h_ijcount, cap * 4) ||
-            cudaMalloc(&g->d_ijstart, cap * 4) || cudaMalloc(&g->d_ijcount, cap * 4))
-            return wfail(g, RP3DG_ENOMEM, "allocation of island arrays");
-        g->cap_hi = cap;
-    }
+    rc = ensure_manifold_staging(g, NM, NI);
+    if (rc) return rc;
     // joints of every world, back to back
     uint32_t NJ = 0;
     for (WorldH& w : g->worlds) {
