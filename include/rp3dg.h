@@ -244,6 +244,22 @@ int rp3dg_narrowphase_device(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_bat
 int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* pairs,
                            const rp3dg_contact_batch* out, int clip_with_previous_axis);
 
+/* The whole narrow phase of a step on host arrays: replaces
+ * CollisionDetectionSystem::testNarrowPhaseCollision(NarrowPhaseInput&)
+ * (CollisionDetectionSystem.cpp:618-660), which runs the batches of a
+ * NarrowPhaseInput (NarrowPhaseInput.h:52-160) one algorithm after the
+ * other.  Batch b (algorithms[b], pairs[b], outs[b]) gives the results of
+ * rp3dg_narrowphase_host on it; the batches overlap on the device: the
+ * upload of one batch runs during the kernels of the one before, and each
+ * batch's results go back while the next one computes.  Outputs in
+ * page-locked host memory are written by the device directly, the contact
+ * slots k < nb_contacts[i] only (the others are left untouched); other
+ * outputs are copied back as rp3dg_narrowphase_host copies them.
+ * Synchronizes before returning. */
+int rp3dg_narrowphase_input_host(rp3dg_ctx* ctx, uint32_t nb_batches, const int32_t* algorithms,
+                                 const rp3dg_pair_batch* pairs, const rp3dg_contact_batch* outs,
+                                 int clip_with_previous_axis);
+
 /* Measurement entry point, no counterpart in the reference engine: runs
  * the same batch as rp3dg_narrowphase_device through the event-counting
  * build of the kernels (same results, slower) and returns, in events[0..

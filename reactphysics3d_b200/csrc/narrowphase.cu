@@ -645,6 +645,30 @@ __global__ void __launch_bounds__(NP_BLOCK) classify_pairs(const NpArgs a, uint8
     }
 }
 
+__global__ void __launch_bounds__(256) publish_contacts(const PublishArgs a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    a.h_col[i] = a.d_col[i];
+    const uint8_t c = a.d_nb[i];
+    a.h_nb[i] = c;
+    if (a.h_cache) {
+        const uint4 v = *reinterpret_cast<const uint4*>(a.d_cache + i);
+        *reinterpret_cast<uint4*>(a.h_cache + i) = v;
+    }
+    for (uint32_t k = 0; k < c; k++) {
+        const size_t o = size_t(k) * a.n + i;
+        a.h_nd[o] = a.d_nd[o];
+        a.h_l1[o] = a.d_l1[o];
+        a.h_l2[o] = a.d_l2[o];
+    }
+}
+
+cudaError_t launch_publish_contacts(const PublishArgs& a, cudaStream_t s) {
+    if (a.n == 0) return cudaSuccess;
+    publish_contacts<<<(a.n + 255) / 256, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_classify_pairs(const NpArgs& args, uint8_t* key, uint8_t* proposals, int num_sms,
                                   cudaStream_t stream) {
     if (args.n == 0) return cudaSuccess;

@@ -60,6 +60,21 @@ struct NpArgs {
 };
 
 void upload_box_tables(const BoxTables& t, cudaStream_t s);
+
+// A batch's results from device arrays into host-accessible memory
+// (page-locked, written over the bus by the kernel): flags, counts, the
+// cache when given, and the contact slots k < nb_contacts[i] (slot-major,
+// n pairs per slot, like the device arrays).
+struct PublishArgs {
+    uint32_t n;
+    const uint8_t *d_col, *d_nb;
+    const float4 *d_nd, *d_l1, *d_l2;
+    const rp3dg_lastframe* d_cache;
+    uint8_t *h_col, *h_nb;
+    float4 *h_nd, *h_l1, *h_l2;
+    rp3dg_lastframe* h_cache;
+};
+cudaError_t launch_publish_contacts(const PublishArgs& a, cudaStream_t s);
 // Launches the kernels of one algorithm batch; *launches receives how many.
 cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaStream_t stream, int* launches);
 // Pairs of an all-box polyhedron batch grouped by their learned class

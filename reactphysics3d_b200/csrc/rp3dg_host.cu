@@ -229,6 +229,12 @@ struct rp3dg_ctx {
     // staging buffers for rp3dg_narrowphase_host
     void* d_stage = nullptr;
     size_t cap_stage = 0;
+    // rp3dg_narrowphase_input_host: staging of all batches, an upload and a
+    // result stream beside the compute stream, and two events per batch
+    void* d_istage = nullptr;
+    size_t cap_istage = 0;
+    cudaStream_t s_up = nullptr, s_pub = nullptr;
+    std::vector<cudaEvent_t> events;
     // learned separating-axis MLP: one device block holding the fp32
     // parameters, Adam moments, gradients, packed bf16 fragments, loss word
     // and proposal counters; training scratch grows with the batch
@@ -454,6 +460,10 @@ void rp3dg_destroy(rp3dg_ctx* ctx) {
     cudaFree(ctx->d_shapes);
     cudaFree(ctx->d_arena);
     cudaFree(ctx->d_stage);
+    cudaFree(ctx->d_istage);
+    if (ctx->s_up) cudaStreamDestroy(ctx->s_up);
+    if (ctx->s_pub) cudaStreamDestroy(ctx->s_pub);
+    for (cudaEvent_t ev : ctx->events) cudaEventDestroy(ev);
     cudaFree(ctx->d_error);
     cudaFree(ctx->d_events);
     cudaFree(ctx->d_plist);
@@ -1274,6 +1284,164 @@ int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch
 int rp3dg_narrowphase_manifolds_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch* p,
                                      const rp3dg_contact_batch* out, int clip_with_previous_axis, uint8_t* kept) {
     return narrowphase_host_impl(ctx, algorithm, p, out, clip_with_previous_axis, true, kept);
+}
+
+namespace {
+// Host memory the device can write directly (page-locked and mapped, which
+// unified addressing gives every page-locked allocation).
+bool device_writable_host(const void* p) {
+    if (!p) return true;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost && at.devicePointer == p;
+}
+}  // namespace
+
+int rp3dg_narrowphase_input_host(rp3dg_ctx* ctx, uint32_t nb, const int32_t* algos, const rp3dg_pair_batch* P,
+                                 const rp3dg_contact_batch* O, int clip) {
+    if (!ctx || (nb && (!algos || !P || !O))) return fail(ctx, RP3DG_EINVAL, "null argument");
+    struct Lay {
+        size_t s1, s2, p1, r1, p2, r2, rep, cache, col, nbc, nd, l1, l2;
+        bool pub;
+    };
+    std::vector<Lay> L(nb);
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    size_t off = 0;
+    for (uint32_t b = 0; b < nb; b++) {
+        const rp3dg_pair_batch& p = P[b];
+        const rp3dg_contact_batch& o = O[b];
+        if (p.n == 0) continue;
+        if (!p.shape1 || !p.shape2 || !p.pos1 || !p.rot1 || !p.pos2 || !p.rot2)
+            return fail(ctx, RP3DG_EINVAL, "null pair array");
+        if (!o.is_colliding || !o.nb_contacts || !o.normal_depth || !o.local1 || !o.local2)
+            return fail(ctx, RP3DG_EINVAL, "null contact array");
+        if (o.max_contacts < 1 || o.max_contacts > RP3DG_MAX_CONTACTS_PER_PAIR)
+            return fail(ctx, RP3DG_EINVAL, "max_contacts must be in 1..16");
+        const size_t n = p.n, mc = o.max_contacts;
+        Lay& l = L[b];
+        l.s1 = off; off += al(n * 4);
+        l.s2 = off; off += al(n * 4);
+        l.p1 = off; off += al(n * 16);
+        l.r1 = off; off += al(n * 16);
+        l.p2 = off; off += al(n * 16);
+        l.r2 = off; off += al(n * 16);
+        l.rep = off; off += p.report_contacts ? al(n) : 0;
+        l.cache = off; off += p.cache ? al(n * sizeof(rp3dg_lastframe)) : 0;
+        l.col = off; off += al(n);
+        l.nbc = off; off += al(n);
+        l.nd = off; off += al(n * mc * 16);
+        l.l1 = off; off += al(n * mc * 16);
+        l.l2 = off; off += al(n * mc * 16);
+        l.pub = device_writable_host(o.is_colliding) && device_writable_host(o.nb_contacts) &&
+                device_writable_host(o.normal_depth) && device_writable_host(o.local1) &&
+                device_writable_host(o.local2) && device_writable_host(p.cache) && aligned(o.normal_depth, 16) &&
+                aligned(o.local1, 16) && aligned(o.local2, 16) && (!p.cache || aligned(p.cache, 16));
+    }
+    cudaSetDevice(ctx->device);
+    int rc = grow(ctx, &ctx->d_istage, &ctx->cap_istage, std::max<size_t>(off, 256), "cudaMalloc(narrow-phase input)");
+    if (rc) return rc;
+    cudaError_t e = cudaSuccess;
+    if (!ctx->s_up) e = cudaStreamCreateWithFlags(&ctx->s_up, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !ctx->s_pub) e = cudaStreamCreateWithFlags(&ctx->s_pub, cudaStreamNonBlocking);
+    while (e == cudaSuccess && ctx->events.size() < 2 * size_t(nb)) {
+        cudaEvent_t ev;
+        e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) ctx->events.push_back(ev);
+    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "narrow-phase input streams");
+    char* base = static_cast<char*>(ctx->d_istage);
+    // the batches one after the other: upload (s_up), kernels (context
+    // stream), results (s_pub); each stream waits on the stage before it
+    for (uint32_t b = 0; b < nb && rc == 0 && e == cudaSuccess; b++) {
+        const rp3dg_pair_batch& p = P[b];
+        const rp3dg_contact_batch& o = O[b];
+        if (p.n == 0) continue;
+        const Lay& l = L[b];
+        const size_t n = p.n;
+        auto up = [&](size_t at, const void* src, size_t bytes) {
+            if (e == cudaSuccess && src) e = cudaMemcpyAsync(base + at, src, bytes, cudaMemcpyHostToDevice, ctx->s_up);
+        };
+        up(l.s1, p.shape1, n * 4); up(l.s2, p.shape2, n * 4);
+        up(l.p1, p.pos1, n * 16); up(l.r1, p.rot1, n * 16);
+        up(l.p2, p.pos2, n * 16); up(l.r2, p.rot2, n * 16);
+        up(l.rep, p.report_contacts, n);
+        up(l.cache, p.cache, n * sizeof(rp3dg_lastframe));
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->events[2 * b], ctx->s_up);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->events[2 * b], 0);
+        if (e != cudaSuccess) break;
+        rp3dg_pair_batch dp;
+        dp.n = p.n;
+        dp.shape1 = reinterpret_cast<const int32_t*>(base + l.s1);
+        dp.shape2 = reinterpret_cast<const int32_t*>(base + l.s2);
+        dp.pos1 = reinterpret_cast<const rp3dg_float4*>(base + l.p1);
+        dp.rot1 = reinterpret_cast<const rp3dg_float4*>(base + l.r1);
+        dp.pos2 = reinterpret_cast<const rp3dg_float4*>(base + l.p2);
+        dp.rot2 = reinterpret_cast<const rp3dg_float4*>(base + l.r2);
+        dp.report_contacts = p.report_contacts ? reinterpret_cast<const uint8_t*>(base + l.rep) : nullptr;
+        dp.cache = p.cache ? reinterpret_cast<rp3dg_lastframe*>(base + l.cache) : nullptr;
+        rp3dg_contact_batch dout;
+        dout.is_colliding = reinterpret_cast<uint8_t*>(base + l.col);
+        dout.nb_contacts = reinterpret_cast<uint8_t*>(base + l.nbc);
+        dout.normal_depth = reinterpret_cast<rp3dg_float4*>(base + l.nd);
+        dout.local1 = reinterpret_cast<rp3dg_float4*>(base + l.l1);
+        dout.local2 = reinterpret_cast<rp3dg_float4*>(base + l.l2);
+        dout.max_contacts = o.max_contacts;
+        rc = rp3dg_narrowphase_device(ctx, algos[b], &dp, &dout, clip);
+        if (rc) break;
+        e = cudaEventRecord(ctx->events[2 * b + 1], ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->s_pub, ctx->events[2 * b + 1], 0);
+        if (e != cudaSuccess) break;
+        if (l.pub) {
+            rp3dg::PublishArgs pa;
+            pa.n = p.n;
+            pa.d_col = dout.is_colliding; pa.d_nb = dout.nb_contacts;
+            pa.d_nd = reinterpret_cast<const float4*>(dout.normal_depth);
+            pa.d_l1 = reinterpret_cast<const float4*>(dout.local1);
+            pa.d_l2 = reinterpret_cast<const float4*>(dout.local2);
+            pa.d_cache = dp.cache;
+            pa.h_col = o.is_colliding; pa.h_nb = o.nb_contacts;
+            pa.h_nd = reinterpret_cast<float4*>(o.normal_depth);
+            pa.h_l1 = reinterpret_cast<float4*>(o.local1);
+            pa.h_l2 = reinterpret_cast<float4*>(o.local2);
+            pa.h_cache = p.cache;
+            e = rp3dg::launch_publish_contacts(pa, ctx->s_pub);
+            ctx->launches++;
+        } else {
+            e = cudaMemcpyAsync(o.is_colliding, base + l.col, n, cudaMemcpyDeviceToHost, ctx->s_pub);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(o.nb_contacts, base + l.nbc, n, cudaMemcpyDeviceToHost, ctx->s_pub);
+            if (e == cudaSuccess && p.cache)
+                e = cudaMemcpyAsync(p.cache, base + l.cache, n * sizeof(rp3dg_lastframe), cudaMemcpyDeviceToHost,
+                                    ctx->s_pub);
+        }
+    }
+    // every stream drained before returning (also after an error)
+    const cudaError_t e1 = cudaStreamSynchronize(ctx->s_up);
+    const cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+    const cudaError_t e3 = cudaStreamSynchronize(ctx->s_pub);
+    if (rc) return rc;
+    if (e == cudaSuccess) e = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "narrow-phase input (host arrays)");
+    // the batches whose outputs are pageable: their used contact slots
+    for (uint32_t b = 0; b < nb; b++) {
+        const rp3dg_pair_batch& p = P[b];
+        const rp3dg_contact_batch& o = O[b];
+        if (p.n == 0 || L[b].pub) continue;
+        const size_t n = p.n;
+        uint32_t used = 0;
+        for (size_t i = 0; i < n; i++) used = o.nb_contacts[i] > used ? o.nb_contacts[i] : used;
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(o.normal_depth, base + L[b].nd, n * used * 16, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(o.local1, base + L[b].l1, n * used * 16, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(o.local2, base + L[b].l2, n * used * 16, cudaMemcpyDeviceToHost, ctx->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "narrow-phase input (host arrays)");
 }
 
 namespace {

@@ -82,6 +82,7 @@ def load_library(path=LIB_PATH):
     L.rp3dg_device_errors.argtypes = [P, C.POINTER(C.c_uint32), C.c_int]
     L.rp3dg_narrowphase_device.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_int]
     L.rp3dg_narrowphase_host.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch), C.c_int]
+    L.rp3dg_narrowphase_input_host.argtypes = [P, C.c_uint32, P, P, P, C.c_int]
     L.rp3dg_narrowphase_count_events.argtypes = [P, C.c_int, C.POINTER(A.PairBatch), C.POINTER(A.ContactBatch),
                                                  C.c_int, C.POINTER(C.c_ulonglong)]
     L.rp3dg_measure_fp32_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
@@ -362,6 +363,19 @@ class Context:
         pb, cb = pairs.struct(), out.struct()
         self._check(self.lib.rp3dg_narrowphase_host(self.h, int(algo), C.byref(pb), C.byref(cb), int(clip)))
         return out
+
+    def narrowphase_input_host(self, batches, clip=True):
+        """testNarrowPhaseCollision over a whole NarrowPhaseInput: `batches` is
+        a list of (algorithm, HostPairs, HostContacts or None); the batches
+        run overlapped (rp3dg_narrowphase_input_host); returns the outputs."""
+        outs = [o if o is not None else A.HostContacts(p.n) for (_, p, o) in batches]
+        n = len(batches)
+        algos = (C.c_int32 * n)(*[int(a) for (a, _, _) in batches])
+        pbs = (A.PairBatch * n)(*[p.struct() for (_, p, _) in batches])
+        cbs = (A.ContactBatch * n)(*[o.struct() for o in outs])
+        self._check(self.lib.rp3dg_narrowphase_input_host(self.h, n, C.addressof(algos), C.addressof(pbs),
+                                                          C.addressof(cbs), int(clip)))
+        return outs
 
     def narrowphase_manifolds_host(self, algo, pairs, out=None, clip=True, want_kept=True):
         """Narrow phase + manifold reduction on host arrays; returns (out, kept)."""

@@ -195,3 +195,45 @@ def test_grazing_capsule_clip_matches_oracle(ctx, port_hulls):
         a, _ = ref.narrowphase(A.ALGO_CAPSULE_VS_CONVEX_POLYHEDRON, _remap_meshes(sh, _register_hulls(ref)),
                                b.slice(0, b.n))
         _assert_same(got, a, what="grazing capsules vs reference")
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_narrowphase_input_matches_per_batch_calls(ctx, pinned):
+    """rp3dg_narrowphase_input_host (all batches overlapped, results written
+    straight into page-locked outputs) gives, batch by batch, the results and
+    caches of rp3dg_narrowphase_host, on two frames (fresh caches, then moved
+    poses with the first frame's caches)."""
+    import torch
+    sc = scenes.narrowphase_scene(total_pairs=7 * 6000, seed=321, hull=edgecases.load_hull())
+    ctx.set_shapes(sc.shapes)
+    rng = np.random.default_rng(4)
+
+    def pin(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy() if pinned else a.copy()
+
+    def outs_for(n):
+        o = A.HostContacts(n)
+        for f in ("is_colliding", "nb_contacts", "normal_depth", "local1", "local2"):
+            setattr(o, f, pin(getattr(o, f)))
+        return o
+
+    frames = []
+    for name, (algo, pairs) in sc.batches.items():
+        pairs.cache = A.fresh_cache(pairs.n)
+        frames.append((name, algo, pairs))
+    for frame in range(2):
+        ref, batches = [], []
+        for name, algo, pairs in frames:
+            pr = pairs.slice(0, pairs.n)
+            pb = A.HostPairs(pin(pairs.shape1), pin(pairs.shape2), pin(pairs.pos1), pin(pairs.rot1),
+                             pin(pairs.pos2), pin(pairs.rot2), None, pin(pairs.cache))
+            ref.append((ctx.narrowphase_host(algo, pr), pr.cache))
+            batches.append((algo, pb, outs_for(pairs.n)))
+        got = ctx.narrowphase_input_host(batches)
+        for (name, _, _), (exp, cache_exp), g, (_, pb, _) in zip(frames, ref, got, batches):
+            _assert_same(g, exp, pb.cache, cache_exp, f"{name} frame {frame + 1} pinned={pinned}")
+        # the next frame: moved poses, the caches the reference's collision
+        # detection leaves
+        frames = [(name, algo, reflib.perturb_pairs(pairs, rng)) for name, algo, pairs in frames]
+        for k, (name, algo, pairs) in enumerate(frames):
+            pairs.cache = reflib.next_frame_cache(ref[k][1], ref[k][0])
