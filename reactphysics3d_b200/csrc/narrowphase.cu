@@ -749,7 +749,8 @@ static cudaError_t launch_one(int algo, const NpArgs& args, int num_sms, cudaStr
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
     }
-    const uint32_t blocks_needed = (args.n + NP_BLOCK - 1) / NP_BLOCK;
+    // a warp-per-pair launch can use a warp per pair (4 per CTA), the others a thread
+    const uint32_t blocks_needed = warp_list ? (args.n + 3) / 4 : (args.n + NP_BLOCK - 1) / NP_BLOCK;
     // Enough CTAs to fill every SM several times; the grid-stride loop covers the rest.
     const uint32_t cap = uint32_t(num_sms) * 16u;
     uint32_t blocks = blocks_needed < cap ? blocks_needed : cap;

@@ -29,9 +29,15 @@ def test_library_loads(cuda_lib):
         assert hasattr(L, s)
 
 
-@pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES", None) is None and
-                    subprocess.run(["nvidia-smi"], capture_output=True).returncode == 0,
-                    reason="a GPU is present")
+def _gpu_present():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return subprocess.run(["nvidia-smi"], capture_output=True).returncode == 0
+
+
+@pytest.mark.skipif(_gpu_present(), reason="a GPU is present")
 def test_no_gpu_no_context(cuda_lib):
     L = engine.load_library(cuda_lib)
     h = C.c_void_p()

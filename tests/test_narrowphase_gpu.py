@@ -209,7 +209,11 @@ def test_narrowphase_input_matches_per_batch_calls(ctx, pinned):
     rng = np.random.default_rng(4)
 
     def pin(a):
-        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy() if pinned else a.copy()
+        a = np.ascontiguousarray(a)
+        if not pinned:
+            return a.copy()
+        b = torch.from_numpy(a.view(np.uint8).reshape(-1)).pin_memory().numpy()
+        return b.view(a.dtype).reshape(a.shape)
 
     def outs_for(n):
         o = A.HostContacts(n)
