@@ -736,18 +736,42 @@ cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaSt
     return e;
 }
 
+// Per kernel: its static shared memory, the dynamic size its opt-in was set
+// for, and its resident CTAs per SM for that size (queried once: the
+// queries cost more host time than a launch).
+struct LaunchCache {
+    bool known = false;
+    size_t static_smem = 0, smem = ~size_t(0);
+    int per_sm = 0;
+};
+
 static cudaError_t launch_one(int algo, const NpArgs& args, int num_sms, cudaStream_t stream) {
     const void* k = kernel_ptr(algo);
     if (!k) return cudaErrorInvalidValue;
     const bool warp_list = algo > 8;   // narrowphase_warp_kernel<algo - 8>
     size_t smem = (args.stage_mesh && algo != ALGO_POLY_PER_THREAD) ? size_t(args.mesh_nwords) * 4 : 0;
-    cudaFuncAttributes fa;
-    cudaError_t e = cudaFuncGetAttributes(&fa, k);
-    if (e != cudaSuccess) return e;
-    // static + dynamic shared memory above 48 KB needs the opt-in attribute
-    if (smem > 0 && fa.sharedSizeBytes + smem > 48 * 1024) {
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    static thread_local LaunchCache cache[16];
+    LaunchCache& lc = cache[algo & 15];
+    cudaError_t e = cudaSuccess;
+    if (!lc.known) {
+        cudaFuncAttributes fa;
+        e = cudaFuncGetAttributes(&fa, k);
         if (e != cudaSuccess) return e;
+        lc.static_smem = fa.sharedSizeBytes;
+        lc.known = true;
+    }
+    if (lc.smem != smem) {
+        // static + dynamic shared memory above 48 KB needs the opt-in attribute
+        if (smem > 0 && lc.static_smem + smem > 48 * 1024) {
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            if (e != cudaSuccess) return e;
+        }
+        lc.per_sm = 0;
+        if (warp_list) {
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lc.per_sm, k, NP_BLOCK, smem);
+            if (e != cudaSuccess) return e;
+        }
+        lc.smem = smem;
     }
     // a warp-per-pair launch can use a warp per pair (4 per CTA), the others a thread
     const uint32_t blocks_needed = warp_list ? (args.n + 3) / 4 : (args.n + NP_BLOCK - 1) / NP_BLOCK;
@@ -756,10 +780,7 @@ static cudaError_t launch_one(int algo, const NpArgs& args, int num_sms, cudaStr
     uint32_t blocks = blocks_needed < cap ? blocks_needed : cap;
     if (warp_list) {
         // persistent: the CTAs that fit on the device at once
-        int per_sm = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NP_BLOCK, smem);
-        if (e != cudaSuccess) return e;
-        const uint32_t resident = uint32_t(num_sms) * uint32_t(per_sm > 0 ? per_sm : 1);
+        const uint32_t resident = uint32_t(num_sms) * uint32_t(lc.per_sm > 0 ? lc.per_sm : 1);
         blocks = blocks_needed < resident ? blocks_needed : resident;
     }
     void* params[] = {const_cast<NpArgs*>(&args)};

@@ -1354,8 +1354,29 @@ int rp3dg_narrowphase_input_host(rp3dg_ctx* ctx, uint32_t nb, const int32_t* alg
     if (e != cudaSuccess) return cuda_fail(ctx, e, "narrow-phase input streams");
     char* base = static_cast<char*>(ctx->d_istage);
     // the batches one after the other: upload (s_up), kernels (context
-    // stream), results (s_pub); each stream waits on the stage before it
-    for (uint32_t b = 0; b < nb && rc == 0 && e == cudaSuccess; b++) {
+    // stream), results (s_pub); each stream waits on the stage before it.
+    // The batches are independent, so they go in order of decreasing
+    // estimated kernel time: the long polyhedron batches compute while the
+    // others upload.
+    std::vector<uint32_t> order(nb);
+    for (uint32_t b = 0; b < nb; b++) order[b] = b;
+    auto cost = [&](uint32_t b) {
+        static const double per_pair[7] = {0.0, 1.0, 1.0, 1.2, 4.0, 8.0, 20.0};
+        const int a = algos[b];
+        double c = (a >= 1 && a <= 6 ? per_pair[a] : 1.0) * double(P[b].n);
+        // a polyhedron batch whose first pair has a convex mesh: hull work
+        if (a == RP3DG_ALGO_CONVEX_POLYHEDRON_VS_CONVEX_POLYHEDRON && P[b].n) {
+            const int32_t s1 = P[b].shape1[0], s2 = P[b].shape2[0];
+            const size_t ns = ctx->host_shapes.size();
+            if ((s1 >= 0 && size_t(s1) < ns && ctx->host_shapes[size_t(s1)].kind == RP3DG_SHAPE_CONVEX_MESH) ||
+                (s2 >= 0 && size_t(s2) < ns && ctx->host_shapes[size_t(s2)].kind == RP3DG_SHAPE_CONVEX_MESH))
+                c *= 3.0;
+        }
+        return c;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return cost(x) > cost(y); });
+    for (uint32_t ob = 0; ob < nb && rc == 0 && e == cudaSuccess; ob++) {
+        const uint32_t b = order[ob];
         const rp3dg_pair_batch& p = P[b];
         const rp3dg_contact_batch& o = O[b];
         if (p.n == 0) continue;
