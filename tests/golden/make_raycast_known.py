@@ -1,7 +1,7 @@
 """Known-answer raycast cases read from the reference's own raycast test.
 
 Parses test/tests/collision/TestRaycast.h of the reference (as text) for the
-box, sphere, capsule, convex-mesh and height-field tests: the body and shape
+box, sphere, capsule, convex-mesh, concave-mesh and height-field tests: the body and shape
 transforms of the test fixture, the shapes, every ray the tests cast through
 PhysicsWorld::raycast (endpoints in the shape's local space, the ray's
 maxFraction) with the expected outcome (hit or miss) and, where the test
@@ -21,7 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RP3D_REFERENCE", "")
 SRC = os.path.join(REF, "test", "tests", "collision", "TestRaycast.h")
 TESTS = {"box": "testBox", "sphere": "testSphere", "capsule": "testCapsule",
-         "convex_mesh": "testConvexMesh", "heightfield": "testHeightField"}
+         "convex_mesh": "testConvexMesh", "concave_mesh": "testConcaveMesh", "heightfield": "testHeightField"}
 
 NUM = r"-?\d+(?:\.\d+)?"
 
@@ -79,11 +79,13 @@ def main():
     idx = {int(i): int(v) for i, v in re.findall(r"mConvexMeshIndices\[(\d+)\] = (\d+);", shapes)}
     v = [verts[i] for i in range(len(verts))]
     ix = [idx[i] for i in range(len(idx))]
+    cverts = [nums(m) for m in re.findall(r"mConcaveMeshVertices\.push_back\(Vector3\(([^)]*)\)\);", text)]
+    cidx = [int(m) for m in re.findall(r"mConcaveMeshIndices\.push_back\((\d+)\);", text)]
     hf = re.search(r"mHeightFieldData\[i\] = (" + NUM + r");", text)
     hfc = re.search(r"createHeightField\((\d+), (\d+),", text)
     out = {
         "source": "reference test/tests/collision/TestRaycast.h (setUp, testBox, testSphere, testCapsule, "
-                  "testConvexMesh, testHeightField), parsed by tests/golden/make_raycast_known.py",
+                  "testConvexMesh, testConcaveMesh, testHeightField), parsed by tests/golden/make_raycast_known.py",
         # Quaternion::fromEulerAngles arguments of the fixture (radians, as multiples of PI)
         "body_position": pos, "body_euler_pi": [1 / 5, 1 / 6, 1 / 7],
         "shape_position": shape_pos, "shape_euler_pi": [3 / 6, -1 / 8, 1 / 3],
@@ -92,6 +94,8 @@ def main():
         "capsule": nums(re.search(r"createCapsuleShape\(([^)]*)\)", shapes).group(1)),
         "convex_vertices": [v[3 * k:3 * k + 3] for k in range(len(v) // 3)],
         "convex_faces": [ix[4 * f:4 * f + 4] for f in range(len(ix) // 4)],
+        "concave_vertices": cverts,
+        "concave_triangles": [cidx[3 * t:3 * t + 3] for t in range(len(cidx) // 3)],
         "heightfield": {"columns": int(hfc.group(1)), "rows": int(hfc.group(2)), "height": float(hf.group(1))},
         "cases": {},
     }

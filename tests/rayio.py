@@ -38,7 +38,7 @@ def known_world(k, shape):
     sq = euler_quaternion(*(np.pi * np.array(k["shape_euler_pi"])))
     shapes = np.zeros(1, A.SHAPE_DTYPE)
     shapes["mesh"] = -1
-    hfs, cms = [], []
+    hfs, cms, ccs = [], [], []
     if shape == "box":
         shapes[0]["kind"] = A.SHAPE_BOX
         shapes[0]["params"][:3] = k["box_half_extents"]
@@ -53,6 +53,11 @@ def known_world(k, shape):
         shapes[0]["kind"] = A.SHAPE_CONVEX_MESH
         shapes[0]["mesh"] = 0
         cms = [(np.array(k["convex_vertices"], np.float32), k["convex_faces"], (1.0, 1.0, 1.0))]
+    elif shape == "concave_mesh":
+        shapes[0]["kind"] = A.SHAPE_CONCAVE_MESH
+        shapes[0]["mesh"] = 0
+        ccs = [(np.array(k["concave_vertices"], np.float32), np.array(k["concave_triangles"], np.uint32), None,
+                (1.0, 1.0, 1.0))]
     else:
         hf = k["heightfield"]
         shapes[0]["kind"] = A.SHAPE_HEIGHTFIELD
@@ -66,7 +71,7 @@ def known_world(k, shape):
     colliders[0]["position"] = np.float32(k["shape_position"])
     colliders[0]["orientation"] = sq.astype(np.float32)
     sc = scenes.WorldScene(A.default_world_settings(), shapes, bodies, colliders, f"raycast {shape}",
-                           heightfields=hfs, convex_meshes=cms)
+                           heightfields=hfs, convex_meshes=cms, concave_meshes=ccs)
     bq32, sq32 = bodies[0]["orientation"].astype(np.float64), colliders[0]["orientation"].astype(np.float64)
 
     def to_world(p):

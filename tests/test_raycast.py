@@ -7,7 +7,7 @@ import rayio
 import reflib
 from reactphysics3d_b200 import _abi as A
 
-SHAPES = ("box", "sphere", "capsule", "convex_mesh", "heightfield")
+SHAPES = ("box", "sphere", "capsule", "convex_mesh", "concave_mesh", "heightfield")
 
 
 @pytest.mark.skipif(not reflib.have_ref("f32"), reason="reference engine not built (make -C oracle ref)")

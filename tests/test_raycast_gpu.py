@@ -34,7 +34,7 @@ def _compare(w, r, rays, world=0):
 
 
 @needs_ref
-@pytest.mark.parametrize("shape", ("box", "sphere", "capsule", "convex_mesh", "heightfield"))
+@pytest.mark.parametrize("shape", ("box", "sphere", "capsule", "convex_mesh", "concave_mesh", "heightfield"))
 def test_raycast_known_answers(ctx, shape):
     """The reference test's rays against one shape: bit-identical to the
     reference in all modes, and its expected hits, fractions and points."""
