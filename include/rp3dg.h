@@ -884,6 +884,17 @@ int rp3dg_world_set_profiling(rp3dg_world* world, int enable);
  * moved set's order, so results do not depend on the count).  A world from
  * rp3dg_world_create starts with 1. */
 int rp3dg_world_set_threads(rp3dg_world* world, int threads);
+/* Where the broad-phase trees of a world's bookkeeping live (no counterpart
+ * in the reference).  With device trees, every world's DynamicAABBTree
+ * (DynamicAABBTree.cpp:219-638) sits in one device pool: the reinsertions of
+ * the moved colliders run on the GPU, one thread per world in the
+ * reference's order, and the moved colliders' queries one thread per query;
+ * the host keeps the moved set, the leaves' boxes and the pairs, and copies
+ * a world's tree back before a world raycast reads it.  Results are
+ * identical either way.  A group of 2 or more worlds of at most 8192
+ * colliders each starts with device trees, any other world with host trees. */
+int rp3dg_world_set_device_trees(rp3dg_world* world, int enable);
+int rp3dg_world_get_device_trees(rp3dg_world* world, int* enabled);
 /* Autotuner of the dynamics stage's island scheduling (no counterpart in the
  * reference): over the next steps, candidate settings of one parameter at a
  * time are tried on successive steps, `rounds` steps each, and timed with

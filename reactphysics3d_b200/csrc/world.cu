@@ -297,20 +297,21 @@ __global__ void __launch_bounds__(128) world_zero_rows(uint32_t n, const int32_t
     torque[r] = z;
 }
 
-// reportAllShapesOverlappingWithShapes on the GPU for worlds with many moved
-// colliders: one thread per moved collider runs the tree's stack query (same
-// visiting order as DynamicAABBTree::reportAllShapesOverlappingWithAABB,
-// DynamicAABBTree.cpp:589-638) over a copy of the host tree's nodes, counts
-// its leaves, reserves a contiguous block and writes them in that order.
+// reportAllShapesOverlappingWithShapes on the GPU: one thread per moved
+// collider runs the tree's stack query (same visiting order as
+// DynamicAABBTree::reportAllShapesOverlappingWithAABB, DynamicAABBTree.cpp:
+// 589-638), counts its leaves, reserves a contiguous block and writes them in
+// that order.  A single world with many moved colliders queries a copy of its
+// host tree; a world group queries the device trees of its worlds.
 constexpr int TREE_STACK = 96;
 constexpr size_t TREE_GPU_MIN_QUERIES = 4096;
-__global__ void __launch_bounds__(128) world_tree_query(const rp3dg::order::Tree::Node* __restrict__ nodes, int root,
-                                                        const int32_t* __restrict__ queries, uint32_t n, int2* out_pos,
-                                                        int32_t* leaves, uint32_t cap, uint32_t* counter,
-                                                        uint32_t* flags) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const rp3dg::order::Box q = nodes[queries[i]].box;
+constexpr size_t DEV_TREE_MAX_COLLIDERS = 8192;   // largest world of a group created with device trees
+using TreeNode = rp3dg::order::TreeNode;
+
+__device__ __forceinline__ void tree_query_one(const TreeNode* __restrict__ nodes, int root, int leaf, uint32_t i,
+                                               int2* out_pos, int32_t* leaves, uint32_t cap, uint32_t* counter,
+                                               uint32_t* flags) {
+    const rp3dg::order::Box q = nodes[leaf].box;
     int stack[TREE_STACK];
     auto visit = [&](int32_t* out, uint32_t& cnt) -> bool {
         int sp = 0;
@@ -349,6 +350,84 @@ __global__ void __launch_bounds__(128) world_tree_query(const rp3dg::order::Tree
     uint32_t w = 0;
     visit(leaves + off, w);
     out_pos[i] = make_int2(int(off), int(cnt));
+}
+
+__global__ void __launch_bounds__(128) world_tree_query(const TreeNode* __restrict__ nodes, int root,
+                                                        const int32_t* __restrict__ queries, uint32_t n, int2* out_pos,
+                                                        int32_t* leaves, uint32_t cap, uint32_t* counter,
+                                                        uint32_t* flags) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    tree_query_one(nodes, root, queries[i], i, out_pos, leaves, cap, counter, flags);
+}
+
+// A world group's trees: world k's nodes are pool[base[k], base[k] + hdr[k].w),
+// hdr[k] = (root, first free node, nodes in use, nodes).  Query i is
+// (world, leaf); the moved colliders of a world are consecutive, so the
+// threads of a warp mostly walk the same tree.
+__global__ void __launch_bounds__(128) world_tree_query_group(const TreeNode* __restrict__ pool,
+                                                              const uint32_t* __restrict__ base,
+                                                              const int4* __restrict__ hdr,
+                                                              const int2* __restrict__ queries, uint32_t n,
+                                                              int2* out_pos, int32_t* leaves, uint32_t cap,
+                                                              uint32_t* counter, uint32_t* flags) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int2 q = queries[i];
+    const int4 h = hdr[q.x];
+    if (q.y < 0 || q.y >= h.w) {
+        atomicOr(flags, 1u);
+        out_pos[i] = make_int2(-1, 0);
+        return;
+    }
+    tree_query_one(pool + base[q.x], h.x, q.y, i, out_pos, leaves, cap, counter, flags);
+}
+
+// DynamicAABBTree::updateObject's reinsertions (DynamicAABBTree.cpp:186-214,
+// removeLeafNode :348-412, insertLeafNode :219-345, balanceSubTreeAtNode
+// :420-586) of a world group's moved colliders: one warp per world, its
+// first lane replaying the world's reinsertions in collider-component order
+// (the order of BroadPhaseSystem::updateCollidersComponents) on the world's
+// device tree.  job j = (leaf, row of the collider's new fat AABB).
+struct TreeReinsertArgs {
+    uint32_t nworlds;
+    TreeNode* pool;
+    const uint32_t* base;
+    int4* hdr;
+    const uint32_t* job_start;   // nworlds + 1
+    const int2* jobs;
+    const float4 *fmin, *fmax;
+    uint32_t* error;             // bit 1: a tree would have had to grow; bit 2: a leaf out of range
+};
+__global__ void __launch_bounds__(128) world_tree_reinsert(const TreeReinsertArgs a) {
+    const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (k >= a.nworlds || (threadIdx.x & 31) != 0) return;
+    const uint32_t j0 = a.job_start[k], j1 = a.job_start[k + 1];
+    if (j0 == j1) return;
+    const int4 h = a.hdr[k];
+    rp3dg::order::DevTree t;
+    t.nodes.p = a.pool + a.base[k];
+    t.nodes.n = h.w;
+    t.root = h.x;
+    t.free_id = h.y;
+    t.nb_nodes = h.z;
+    for (uint32_t j = j0; j < j1; j++) {
+        const int2 job = a.jobs[j];
+        if (job.x < 0 || job.x >= h.w) {
+            atomicOr(a.error, 2u);
+            break;
+        }
+        const float4 mn = a.fmin[job.y], mx = a.fmax[job.y];
+        rp3dg::order::Box b;
+        b.mn[0] = mn.x; b.mn[1] = mn.y; b.mn[2] = mn.z;
+        b.mx[0] = mx.x; b.mx[1] = mx.y; b.mx[2] = mx.z;
+        t.reinsert(job.x, b);
+        if (t.failed) {
+            atomicOr(a.error, 1u);
+            break;
+        }
+    }
+    a.hdr[k] = make_int4(t.root, t.free_id, t.nb_nodes, t.nodes.n);
 }
 
 uint32_t blocks(uint32_t n) { return (n + 127) / 128; }
@@ -672,6 +751,13 @@ struct WorldH {
     // thread buffer, and per moved collider (thread, first leaf, count)
     std::vector<std::vector<int>> q_buf;
     std::vector<int4> q_pos;
+    std::vector<int32_t> q_shapes;             // this step's moved colliders in the moved set's order
+    uint32_t q_off = 0;                        // their first query in the group's device query list
+    // device tree of a world group: this step's reinsertions (leaf, row) and
+    // whether the host tree's inner nodes are older than the device's (the
+    // host keeps the leaves' boxes current either way)
+    std::vector<int2> reins;
+    bool tree_stale = false;
     std::vector<int> slept;                    // bodies put to sleep by this step
     rp3dg_world_stats stats{};
 };
@@ -764,11 +850,24 @@ struct rp3dg_world {
         uint32_t nm = 0;
     } tuner;
     // broad-phase tree queries on the GPU (worlds with many moved colliders)
-    rp3dg::order::Tree::Node *h_tnodes = nullptr, *d_tnodes = nullptr;
+    TreeNode *h_tnodes = nullptr, *d_tnodes = nullptr;
     size_t cap_tnodes = 0, cap_tq = 0, cap_tleaves = 0, cap_tpos = 0, cap_tcnt = 0;
     int32_t *h_tq = nullptr, *d_tq = nullptr, *h_tleaves = nullptr, *d_tleaves = nullptr;
     int2 *h_tpos = nullptr, *d_tpos = nullptr;
-    uint32_t *h_tcnt = nullptr, *d_tcnt = nullptr;   // [0] leaves reserved, [1] flags
+    uint32_t *h_tcnt = nullptr, *d_tcnt = nullptr;   // [0] leaves reserved, [1] flags, [2] reinsertion errors
+    // world groups: every world's broad-phase tree in one device pool (world
+    // k's nodes from tree_base[k], header root / free node / nodes in use /
+    // nodes), reinserted and queried on the GPU; the host replica keeps the
+    // moved set, the leaves' boxes and the pairs
+    bool dev_tree = false;
+    TreeNode* d_tree = nullptr;
+    uint32_t* d_tree_base = nullptr;
+    int4* d_tree_hdr = nullptr;
+    std::vector<uint32_t> tree_base;
+    size_t cap_tjobs = 0, cap_tjoff = 0, cap_gq = 0;
+    int2 *h_tjobs = nullptr, *d_tjobs = nullptr;     // reinsertions (leaf, row), world after world
+    uint32_t *h_tjoff = nullptr, *d_tjoff = nullptr; // first reinsertion of each world
+    int2 *h_gq = nullptr, *d_gq = nullptr;           // queries (world, leaf)
     // world raycasts: the tree's nodes and the collider table as the ray
     // kernel reads them (rebuilt when the world state changed), rays and hits
     uint64_t state_version = 1;      // bumped by every update and between-step change
@@ -1100,9 +1199,9 @@ bool tree_queries_gpu(Group* g, WorldH& w, const std::vector<int32_t>& shapes) {
         !pair_grow(&g->h_tcnt, &g->d_tcnt, &g->cap_tcnt, 2) ||
         !pair_grow(&g->h_tleaves, &g->d_tleaves, &g->cap_tleaves, 8 * nq))
         return false;
-    std::memcpy(g->h_tnodes, w.tree.nodes.data(), nn * sizeof(rp3dg::order::Tree::Node));
+    std::memcpy(g->h_tnodes, w.tree.nodes.data(), nn * sizeof(TreeNode));
     std::memcpy(g->h_tq, shapes.data(), nq * 4);
-    cudaMemcpyAsync(g->d_tnodes, g->h_tnodes, nn * sizeof(rp3dg::order::Tree::Node), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(g->d_tnodes, g->h_tnodes, nn * sizeof(TreeNode), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(g->d_tq, g->h_tq, nq * 4, cudaMemcpyHostToDevice, st);
     for (int attempt = 0; attempt < 2; attempt++) {
         cudaMemsetAsync(g->d_tcnt, 0, 8, st);
@@ -1129,15 +1228,21 @@ bool tree_queries_gpu(Group* g, WorldH& w, const std::vector<int32_t>& shapes) {
 void broad_and_middle_phase(Group* g, WorldH& w) {
     using clk = std::chrono::steady_clock;
     const auto t0 = g->profiling ? clk::now() : clk::time_point();
-    std::vector<int32_t> shapes;
-    w.moved.to_array(shapes);
-    w.moved.clear();
+    // with device trees the group's queries ran before (tree_queries_group)
+    const bool dev = g->dev_tree;
+    std::vector<int32_t>& shapes = w.q_shapes;
+    if (!dev) {
+        w.moved.to_array(shapes);
+        w.moved.clear();
+    }
     // reportAllShapesOverlappingWithShapes: the tree does not change during
     // the queries, so with a single world on the group's threads they run in
     // parallel; the pairs are then processed in the moved set's order
-    const int nt = (g->nthreads > 1 && g->worlds.size() == 1 && shapes.size() >= 256) ? g->nthreads : 1;
+    const int nt = (!dev && g->nthreads > 1 && g->worlds.size() == 1 && shapes.size() >= 256) ? g->nthreads : 1;
     // a single world with many moved colliders queries on the GPU
-    const bool gpu = g->worlds.size() == 1 && shapes.size() >= TREE_GPU_MIN_QUERIES && tree_queries_gpu(g, w, shapes);
+    const bool gpu = dev || (g->worlds.size() == 1 && shapes.size() >= TREE_GPU_MIN_QUERIES &&
+                             tree_queries_gpu(g, w, shapes));
+    const uint32_t qbase = dev ? w.q_off : 0;
     if (int(w.q_buf.size()) < nt) w.q_buf.resize(size_t(nt));
     w.q_pos.resize(shapes.size());
 #pragma omp parallel num_threads(nt) if (nt > 1 && !gpu)
@@ -1158,7 +1263,7 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
         const int* leaves;
         int nleaf;
         if (gpu) {
-            const int2 tp = g->h_tpos[i];
+            const int2 tp = g->h_tpos[qbase + i];
             leaves = g->h_tleaves + tp.x;
             nleaf = tp.y;
         } else {
@@ -1493,6 +1598,7 @@ void fill_manifolds(Group* g, WorldH& w) {
 void colliders_and_sleep(Group* g, WorldH& w, float dt, const uint8_t* h_moved, const float4* h_fmin,
                          const float4* h_fmax, const float4* h_lv, const float4* h_av) {
     uint32_t nmoved = 0;
+    w.reins.clear();
     for (uint32_t s = 0; s < w.ccomp.n_enabled; s++) {
         const uint32_t r = w.c0 + s;
         if (!h_moved[r]) continue;
@@ -1500,7 +1606,15 @@ void colliders_and_sleep(Group* g, WorldH& w, float dt, const uint8_t* h_moved, 
         Box box;
         box.mn[0] = h_fmin[r].x; box.mn[1] = h_fmin[r].y; box.mn[2] = h_fmin[r].z;
         box.mx[0] = h_fmax[r].x; box.mx[1] = h_fmax[r].y; box.mx[2] = h_fmax[r].z;
-        w.tree.reinsert(w.colliders[size_t(c)].bp, box);
+        const int bp = w.colliders[size_t(c)].bp;
+        if (g->dev_tree) {
+            // the device tree reinserts (reinsert_on_device); the host keeps the leaf's box
+            w.tree.nodes[size_t(bp)].box = box;
+            w.reins.push_back(make_int2(bp, int(r)));
+            w.tree_stale = true;
+        } else {
+            w.tree.reinsert(bp, box);
+        }
         add_moved(w, c);
         nmoved++;
     }
@@ -1652,6 +1766,155 @@ void for_worlds(Group* g, F f) {
     }
 #pragma omp parallel for schedule(dynamic, 4) num_threads(g->nthreads)
     for (int i = 0; i < n; i++) f(i);
+}
+
+// ---- device trees of a world group
+
+// Copies every world's host tree into the group's device pool (each world's
+// node array as it is: a reinsertion frees one node before it takes one, so
+// a tree never grows after its colliders were added).
+int upload_trees(Group* g) {
+    const size_t nw = g->worlds.size();
+    g->tree_base.assign(nw, 0);
+    size_t total = 0;
+    for (size_t k = 0; k < nw; k++) {
+        g->tree_base[k] = uint32_t(total);
+        total += g->worlds[k].tree.nodes.size();
+    }
+    if (total >= (size_t(1) << 31)) return wfail(g, RP3DG_EINVAL, "world group trees too large for the device pool");
+    cudaFree(g->d_tree);
+    cudaFree(g->d_tree_base);
+    cudaFree(g->d_tree_hdr);
+    g->d_tree = nullptr;
+    g->d_tree_base = nullptr;
+    g->d_tree_hdr = nullptr;
+    if (cudaMalloc(&g->d_tree, std::max<size_t>(total, 1) * sizeof(TreeNode)) != cudaSuccess ||
+        cudaMalloc(&g->d_tree_base, std::max<size_t>(nw, 1) * 4) != cudaSuccess ||
+        cudaMalloc(&g->d_tree_hdr, std::max<size_t>(nw, 1) * sizeof(int4)) != cudaSuccess ||
+        !pair_grow(&g->h_tcnt, &g->d_tcnt, &g->cap_tcnt, 4))
+        return wfail(g, RP3DG_ENOMEM, "cudaMalloc(device trees)");
+    std::vector<TreeNode> nodes(total);
+    std::vector<int4> hdr(nw);
+    for (size_t k = 0; k < nw; k++) {
+        const rp3dg::order::Tree& t = g->worlds[k].tree;
+        std::copy(t.nodes.begin(), t.nodes.end(), nodes.begin() + g->tree_base[k]);
+        hdr[k] = make_int4(t.root, t.free_id, t.nb_nodes, int(t.nodes.size()));
+        g->worlds[k].tree_stale = false;
+    }
+    cudaStream_t st = g->stream;
+    cudaMemcpyAsync(g->d_tree, nodes.data(), total * sizeof(TreeNode), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(g->d_tree_base, g->tree_base.data(), nw * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(g->d_tree_hdr, hdr.data(), nw * sizeof(int4), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(g->d_tcnt, 0, 16, st);
+    const cudaError_t e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? 0 : wcuda(g, e, "upload of the device trees");
+}
+
+// Brings world k's host tree up to date with its device tree (before a host
+// reader of the inner nodes: world raycasts, switching the device trees off).
+int download_tree(Group* g, uint32_t k) {
+    WorldH& w = g->worlds[k];
+    if (!g->dev_tree || !w.tree_stale) return 0;
+    cudaStream_t st = g->stream;
+    int4 h;
+    cudaMemcpyAsync(&h, g->d_tree_hdr + k, sizeof(int4), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return wcuda(g, e, "download of a device tree");
+    if (h.w != int(w.tree.nodes.size())) return wfail(g, RP3DG_EINVAL, "device tree size changed");
+    cudaMemcpyAsync(w.tree.nodes.data(), g->d_tree + g->tree_base[k], size_t(h.w) * sizeof(TreeNode),
+                    cudaMemcpyDeviceToHost, st);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return wcuda(g, e, "download of a device tree");
+    w.tree.root = h.x;
+    w.tree.free_id = h.y;
+    w.tree.nb_nodes = h.z;
+    w.tree_stale = false;
+    return 0;
+}
+
+// Queues this step's reinsertions of every world (WorldH::reins) on the
+// device trees; fmin / fmax are the fat AABBs by row of the step.
+int reinsert_on_device(Group* g, const float4* fmin, const float4* fmax) {
+    const size_t nw = g->worlds.size();
+    if (!pair_grow(&g->h_tjoff, &g->d_tjoff, &g->cap_tjoff, nw + 1)) return wfail(g, RP3DG_ENOMEM, "cudaMalloc(tree jobs)");
+    size_t total = 0;
+    for (size_t k = 0; k < nw; k++) {
+        g->h_tjoff[k] = uint32_t(total);
+        total += g->worlds[k].reins.size();
+    }
+    g->h_tjoff[nw] = uint32_t(total);
+    if (!total) return 0;
+    if (!pair_grow(&g->h_tjobs, &g->d_tjobs, &g->cap_tjobs, total)) return wfail(g, RP3DG_ENOMEM, "cudaMalloc(tree jobs)");
+    for_worlds(g, [&](int k) {
+        const std::vector<int2>& r = g->worlds[size_t(k)].reins;
+        if (!r.empty()) std::memcpy(g->h_tjobs + g->h_tjoff[k], r.data(), r.size() * sizeof(int2));
+    });
+    cudaStream_t st = g->stream;
+    cudaMemcpyAsync(g->d_tjoff, g->h_tjoff, (nw + 1) * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(g->d_tjobs, g->h_tjobs, total * sizeof(int2), cudaMemcpyHostToDevice, st);
+    TreeReinsertArgs a{};
+    a.nworlds = uint32_t(nw);
+    a.pool = g->d_tree;
+    a.base = g->d_tree_base;
+    a.hdr = g->d_tree_hdr;
+    a.job_start = g->d_tjoff;
+    a.jobs = g->d_tjobs;
+    a.fmin = fmin;
+    a.fmax = fmax;
+    a.error = g->d_tcnt + 2;
+    world_tree_reinsert<<<uint32_t((nw * 32 + 127) / 128), 128, 0, st>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : wcuda(g, e, "tree reinsertion launch");
+}
+
+// The moved colliders' queries of every world on the device trees: world
+// k's leaves of its i-th moved collider are h_tleaves[h_tpos[q_off + i]].
+int tree_queries_group(Group* g) {
+    const size_t nw = g->worlds.size();
+    for_worlds(g, [&](int k) {
+        WorldH& w = g->worlds[size_t(k)];
+        w.moved.to_array(w.q_shapes);
+        w.moved.clear();
+    });
+    size_t nq = 0;
+    for (WorldH& w : g->worlds) {
+        w.q_off = uint32_t(nq);
+        nq += w.q_shapes.size();
+    }
+    if (!pair_grow(&g->h_gq, &g->d_gq, &g->cap_gq, std::max<size_t>(nq, 1)) ||
+        !pair_grow(&g->h_tpos, &g->d_tpos, &g->cap_tpos, std::max<size_t>(nq, 1)) ||
+        !pair_grow(&g->h_tcnt, &g->d_tcnt, &g->cap_tcnt, 4) ||
+        !pair_grow(&g->h_tleaves, &g->d_tleaves, &g->cap_tleaves, 8 * nq))
+        return wfail(g, RP3DG_ENOMEM, "cudaMalloc(tree queries)");
+    for_worlds(g, [&](int k) {
+        const WorldH& w = g->worlds[size_t(k)];
+        for (size_t i = 0; i < w.q_shapes.size(); i++) g->h_gq[w.q_off + i] = make_int2(k, w.q_shapes[i]);
+    });
+    cudaStream_t st = g->stream;
+    if (nq) cudaMemcpyAsync(g->d_gq, g->h_gq, nq * sizeof(int2), cudaMemcpyHostToDevice, st);
+    for (int attempt = 0; attempt < 2; attempt++) {
+        cudaMemsetAsync(g->d_tcnt, 0, 8, st);
+        if (nq)
+            world_tree_query_group<<<blocks(uint32_t(nq)), 128, 0, st>>>(
+                g->d_tree, g->d_tree_base, g->d_tree_hdr, g->d_gq, uint32_t(nq), g->d_tpos, g->d_tleaves,
+                uint32_t(g->cap_tleaves), g->d_tcnt, g->d_tcnt + 1);
+        cudaMemcpyAsync(g->h_tcnt, g->d_tcnt, 16, cudaMemcpyDeviceToHost, st);
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return wcuda(g, e, "tree queries");
+        const uint32_t total = g->h_tcnt[0], flags = g->h_tcnt[1];
+        if (g->h_tcnt[2]) return wfail(g, RP3DG_ECUDA, "device tree reinsertion failed");
+        if (flags & 1u) return wfail(g, RP3DG_ECUDA, "device tree query: stack overflow or leaf out of range");
+        if (flags & 2u) {
+            if (attempt || !pair_grow(&g->h_tleaves, &g->d_tleaves, &g->cap_tleaves, size_t(total) + 1024))
+                return wfail(g, RP3DG_ENOMEM, "cudaMalloc(tree query leaves)");
+            continue;
+        }
+        if (nq) cudaMemcpyAsync(g->h_tpos, g->d_tpos, nq * sizeof(int2), cudaMemcpyDeviceToHost, st);
+        if (total) cudaMemcpyAsync(g->h_tleaves, g->d_tleaves, size_t(total) * 4, cudaMemcpyDeviceToHost, st);
+        e = cudaStreamSynchronize(st);
+        return e == cudaSuccess ? 0 : wcuda(g, e, "tree queries");
+    }
+    return wfail(g, RP3DG_ECUDA, "tree queries");
 }
 
 // Host copies of the per-row tables (pinned), kept current world by world.
@@ -1915,6 +2178,9 @@ void destroy_group(Group* g) {
     cudaFreeHost(g->h_tnodes); cudaFree(g->d_tnodes); cudaFreeHost(g->h_tq); cudaFree(g->d_tq);
     cudaFreeHost(g->h_tleaves); cudaFree(g->d_tleaves); cudaFreeHost(g->h_tpos); cudaFree(g->d_tpos);
     cudaFreeHost(g->h_tcnt); cudaFree(g->d_tcnt);
+    cudaFree(g->d_tree); cudaFree(g->d_tree_base); cudaFree(g->d_tree_hdr);
+    cudaFreeHost(g->h_tjobs); cudaFree(g->d_tjobs); cudaFreeHost(g->h_tjoff); cudaFree(g->d_tjoff);
+    cudaFreeHost(g->h_gq); cudaFree(g->d_gq);
     cudaFreeHost(g->h_rnodes); cudaFree(g->d_rnodes); cudaFreeHost(g->h_rcols); cudaFree(g->d_rcols);
     cudaFree(g->d_rhf); cudaFree(g->d_rays); cudaFree(g->d_rhits); cudaFree(g->d_rcount);
     if (g->ev_r0) cudaEventDestroy(g->ev_r0);
@@ -2255,6 +2521,17 @@ int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds
     if (!rc) rc = ensure_pool(g, 2 * size_t(g->NC) + 1024);
     if (!rc && (g->cbuf[0].ensure(g->NC + 64, 2 * g->NC + 64) || g->cbuf[1].ensure(g->NC + 64, 2 * g->NC + 64)))
         rc = wfail(g, RP3DG_ENOMEM, "cudaMalloc(contacts)");
+    // a group of small worlds keeps its trees on the device (one GPU thread
+    // per world replays that world's reinsertions); one large world keeps its
+    // tree on the host, whose sequential reinsertions are faster there
+    if (!rc && nworlds >= 2) {
+        size_t most = 0;
+        for (const WorldH& w : g->worlds) most = std::max(most, w.colliders.size());
+        if (most <= DEV_TREE_MAX_COLLIDERS) {
+            rc = upload_trees(g);
+            g->dev_tree = rc == 0;
+        }
+    }
     if (rc) {
         destroy_group(g);
         return rc;
@@ -2317,6 +2594,10 @@ int update_group(Group* g, float dt) {
     if (g->profiling) g->t_mark = std::chrono::steady_clock::now();
 
     // ---- broad phase and middle phase of every world (host order, GPU fat AABBs)
+    if (g->dev_tree) {
+        const int rq = tree_queries_group(g);
+        if (rq) return rq;
+    }
     for_worlds(g, [&](int k) { broad_and_middle_phase(g, g->worlds[size_t(k)]); });
     mark(0);
     if (g->profiling) {
@@ -2855,6 +3136,12 @@ int update_group(Group* g, float dt) {
     cudaMemsetAsync(g->bcol[bc][BC_T], 0, size_t(g->NB) * 16, st);
     e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return wcuda(g, e, "end of step");
+    // the device trees' reinsertions run while the host returns; the next
+    // step's queries (same stream) wait for them
+    if (g->dev_tree) {
+        rc = reinsert_on_device(g, g->ccol[ccur][CC_FMIN], g->ccol[ccur][CC_FMAX]);
+        if (rc) return rc;
+    }
     tuner_step(g);
     g->cur_cb = 1 - g->cur_cb;
     rc = debug_primitives(g);
@@ -3146,6 +3433,7 @@ int rp3dg_world_set_motor_speed(rp3dg_world* g, uint32_t world, uint32_t joint, 
 int ray_tables(Group* g, uint32_t world) {
     if (g->ray_version == g->state_version && g->ray_world == world && g->d_rnodes) return 0;
     int rc = sync_rows(g);
+    if (!rc) rc = download_tree(g, world);
     if (rc) return rc;
     WorldH& w = g->worlds[world];
     const size_t nn = std::max<size_t>(w.tree.nodes.size(), 1);
@@ -3480,6 +3768,29 @@ int rp3dg_world_get_tuning(rp3dg_world* w, uint32_t* out) {
     out[1] = w->tune.giant_min;
     out[2] = w->tune.large_per_sm;
     out[3] = w->tuner.active ? 1u : 0u;
+    return 0;
+}
+
+int rp3dg_world_set_device_trees(rp3dg_world* g, int enable) {
+    if (!g) return RP3DG_EINVAL;
+    if (bool(enable) == g->dev_tree) return 0;
+    if (enable) {
+        const int rc = upload_trees(g);
+        if (rc) return rc;
+        g->dev_tree = true;
+        return 0;
+    }
+    for (uint32_t k = 0; k < uint32_t(g->worlds.size()); k++) {
+        const int rc = download_tree(g, k);
+        if (rc) return rc;
+    }
+    g->dev_tree = false;
+    return 0;
+}
+
+int rp3dg_world_get_device_trees(rp3dg_world* g, int* enabled) {
+    if (!g || !enabled) return RP3DG_EINVAL;
+    *enabled = g->dev_tree ? 1 : 0;
     return 0;
 }
 

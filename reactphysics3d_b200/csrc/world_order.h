@@ -20,13 +20,26 @@
 //          by moving or swapping with the first disabled / last enabled one.
 //
 // Fat AABBs enter the tree as computed on the GPU (bit-identical to the
-// reference's); the host only merges them (min/max) and compares volumes,
+// reference's); the tree only merges them (min/max) and compares volumes,
 // with the reference's float expressions.
+//
+// The tree's insertion, removal and rotations are written once (TreeT) for
+// two node stores: a growing host vector (Tree, the host replica) and a
+// fixed device span (DevTree, one world's tree in a world group's device
+// pool, updated by one GPU thread per world).
 #pragma once
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <vector>
+
+#if defined(__CUDACC__)
+#define ORDER_HD __host__ __device__
+#define ORDER_NO_EXEC_CHECK _Pragma("nv_exec_check_disable")
+#else
+#define ORDER_HD
+#define ORDER_NO_EXEC_CHECK
+#endif
 
 namespace rp3dg {
 namespace order {
@@ -36,11 +49,11 @@ struct Box {
 };
 
 // std::min / std::max as the reference's AABB code uses them (signed zeros)
-inline float rmin(float a, float b) { return (b < a) ? b : a; }
-inline float rmax(float a, float b) { return (a < b) ? b : a; }
+ORDER_HD inline float rmin(float a, float b) { return (b < a) ? b : a; }
+ORDER_HD inline float rmax(float a, float b) { return (a < b) ? b : a; }
 
 // AABB::mergeTwoAABBs (AABB.h:235-243)
-inline Box merge(const Box& a, const Box& b) {
+ORDER_HD inline Box merge(const Box& a, const Box& b) {
     Box r;
     for (int k = 0; k < 3; k++) {
         r.mn[k] = rmin(a.mn[k], b.mn[k]);
@@ -49,55 +62,71 @@ inline Box merge(const Box& a, const Box& b) {
     return r;
 }
 // AABB::getVolume (AABB.h:190-193)
-inline float volume(const Box& a) {
+ORDER_HD inline float volume(const Box& a) {
     const float dx = a.mx[0] - a.mn[0], dy = a.mx[1] - a.mn[1], dz = a.mx[2] - a.mn[2];
     return dx * dy * dz;
 }
 // AABB::testCollision, inclusive (AABB.h:179-187)
-inline bool overlap(const Box& a, const Box& b) {
+ORDER_HD inline bool overlap(const Box& a, const Box& b) {
     for (int k = 0; k < 3; k++)
         if (a.mx[k] < b.mn[k] || b.mx[k] < a.mn[k]) return false;
     return true;
 }
 
-struct Tree {
+// One node of DynamicAABBTree (TreeNode, 48 bytes so that a device thread
+// reads it as three 16-byte words).
+struct alignas(16) TreeNode {
+    int parent = -1;    // parentID, or nextNodeID while the node is free
+    int child[2] = {-1, -1};
+    int height = -1;    // 0 = leaf, -1 = free
+    Box box{};
+    int data = -1;      // collider id of a leaf
+    int unused = 0;
+};
+static_assert(sizeof(TreeNode) == 48, "tree node layout");
+
+// DynamicAABBTree::allocateNode's growth (double the array, chain the new
+// nodes into the free list): the host vector grows; a device span cannot.
+inline bool grow_nodes(std::vector<TreeNode>& nodes, int nb_nodes, int& free_id) {
+    const int old = int(nodes.size());
+    nodes.resize(size_t(old) * 2);
+    for (int i = nb_nodes; i < int(nodes.size()) - 1; i++) {
+        nodes[size_t(i)].parent = i + 1;
+        nodes[size_t(i)].height = -1;
+    }
+    nodes.back().parent = -1;
+    nodes.back().height = -1;
+    free_id = nb_nodes;
+    return true;
+}
+
+// One world's nodes in device memory: n nodes, no growth.
+struct NodeSpan {
+    TreeNode* p = nullptr;
+    int n = 0;
+    ORDER_HD TreeNode& operator[](int i) const { return p[i]; }
+    ORDER_HD int size() const { return n; }
+};
+ORDER_HD inline bool grow_nodes(NodeSpan&, int, int&) { return false; }
+
+template <class Nodes>
+struct TreeT {
     static constexpr int NIL = -1;
-    struct Node {
-        int parent = NIL;   // parentID, or nextNodeID while the node is free
-        int child[2] = {NIL, NIL};
-        int height = -1;    // 0 = leaf, -1 = free
-        int data = -1;      // collider id of a leaf
-        Box box{};
-    };
-    std::vector<Node> nodes;
+    using Node = TreeNode;
+    Nodes nodes;
     int root = NIL;
     int free_id = 0;
     int nb_nodes = 0;
+    bool failed = false;   // a device tree that would have had to grow
 
-    Tree() { init(); }
+    ORDER_NO_EXEC_CHECK
+    ORDER_HD bool leaf(int id) const { return nodes[id].height == 0; }
 
-    // DynamicAABBTree::init (GLOBAL_ALIGNMENT = 16 nodes to start with)
-    void init() {
-        nodes.assign(16, Node());
-        for (int i = 0; i < 15; i++) nodes[i].parent = i + 1;
-        nodes[15].parent = NIL;
-        root = NIL;
-        free_id = 0;
-        nb_nodes = 0;
-    }
-    bool leaf(int id) const { return nodes[id].height == 0; }
-
-    int alloc() {
-        if (free_id == NIL) {
-            const int old = int(nodes.size());
-            nodes.resize(size_t(old) * 2);
-            for (int i = nb_nodes; i < int(nodes.size()) - 1; i++) {
-                nodes[i].parent = i + 1;
-                nodes[i].height = -1;
-            }
-            nodes.back().parent = NIL;
-            nodes.back().height = -1;
-            free_id = nb_nodes;
+    ORDER_NO_EXEC_CHECK
+    ORDER_HD int alloc() {
+        if (free_id == NIL && !grow_nodes(nodes, nb_nodes, free_id)) {
+            failed = true;
+            return NIL;
         }
         const int id = free_id;
         free_id = nodes[id].parent;
@@ -106,14 +135,16 @@ struct Tree {
         nb_nodes++;
         return id;
     }
-    void release(int id) {
+    ORDER_NO_EXEC_CHECK
+    ORDER_HD void release(int id) {
         nodes[id].parent = free_id;
         nodes[id].height = -1;
         free_id = id;
         nb_nodes--;
     }
 
-    int balance(int a_id) {
+    ORDER_NO_EXEC_CHECK
+    ORDER_HD int balance(int a_id) {
         Node* A = &nodes[a_id];
         if (A->height == 0 || A->height < 2) return a_id;
         const int b_id = A->child[0], c_id = A->child[1];
@@ -187,7 +218,8 @@ struct Tree {
         return a_id;
     }
 
-    void refit_up(int cur) {
+    ORDER_NO_EXEC_CHECK
+    ORDER_HD void refit_up(int cur) {
         while (cur != NIL) {
             cur = balance(cur);
             const int l = nodes[cur].child[0], r = nodes[cur].child[1];
@@ -197,7 +229,8 @@ struct Tree {
         }
     }
 
-    void insert_leaf(int id) {
+    ORDER_NO_EXEC_CHECK
+    ORDER_HD void insert_leaf(int id) {
         if (root == NIL) {
             root = id;
             nodes[id].parent = NIL;
@@ -224,6 +257,7 @@ struct Tree {
         const int sib = cur;
         const int old_parent = nodes[sib].parent;
         const int np = alloc();
+        if (np == NIL) return;
         nodes[np].parent = old_parent;
         nodes[np].box = merge(nodes[sib].box, nb);
         nodes[np].height = nodes[sib].height + 1;
@@ -240,7 +274,8 @@ struct Tree {
         refit_up(nodes[id].parent);
     }
 
-    void remove_leaf(int id) {
+    ORDER_NO_EXEC_CHECK
+    ORDER_HD void remove_leaf(int id) {
         if (root == id) {
             root = NIL;
             return;
@@ -261,20 +296,37 @@ struct Tree {
         }
     }
 
-    // addObject with the fat AABB already inflated (addObjectInternal)
-    int add_object(const Box& fat, int data) {
-        const int id = alloc();
-        nodes[id].box = fat;
-        nodes[id].height = 0;
-        nodes[id].data = data;
-        insert_leaf(id);
-        return id;
-    }
     // updateObject after the fat-AABB test failed (the new fat AABB given)
-    void reinsert(int id, const Box& fat) {
+    ORDER_NO_EXEC_CHECK
+    ORDER_HD void reinsert(int id, const Box& fat) {
         remove_leaf(id);
         nodes[id].box = fat;
         insert_leaf(id);
+    }
+};
+
+// The host replica: nodes in a vector that grows as the reference's array.
+struct Tree : TreeT<std::vector<TreeNode>> {
+    Tree() { init(); }
+
+    // DynamicAABBTree::init (GLOBAL_ALIGNMENT = 16 nodes to start with)
+    void init() {
+        nodes.assign(16, Node());
+        for (int i = 0; i < 15; i++) nodes[size_t(i)].parent = i + 1;
+        nodes[15].parent = NIL;
+        root = NIL;
+        free_id = 0;
+        nb_nodes = 0;
+    }
+
+    // addObject with the fat AABB already inflated (addObjectInternal)
+    int add_object(const Box& fat, int data) {
+        const int id = alloc();
+        nodes[size_t(id)].box = fat;
+        nodes[size_t(id)].height = 0;
+        nodes[size_t(id)].data = data;
+        insert_leaf(id);
+        return id;
     }
 
     // reportAllShapesOverlappingWithShapes for one shape: leaves in the
@@ -286,7 +338,7 @@ struct Tree {
             const int id = stack.back();
             stack.pop_back();
             if (id == NIL) continue;
-            const Node& n = nodes[id];
+            const Node& n = nodes[size_t(id)];
             if (overlap(box, n.box)) {
                 if (n.height == 0) {
                     out.push_back(id);
@@ -298,6 +350,9 @@ struct Tree {
         }
     }
 };
+
+// One world's tree in a world group's device pool.
+using DevTree = TreeT<NodeSpan>;
 
 // Set<int32> with std::hash<int32> (identity).
 struct IdSet {

@@ -116,6 +116,8 @@ def load_library(path=LIB_PATH):
     L.rp3dg_world_get_stats.argtypes = [P, P]
     L.rp3dg_world_set_profiling.argtypes = [P, C.c_int]
     L.rp3dg_world_set_threads.argtypes = [P, C.c_int]
+    L.rp3dg_world_set_device_trees.argtypes = [P, C.c_int]
+    L.rp3dg_world_get_device_trees.argtypes = [P, P]
     L.rp3dg_world_autotune.argtypes = [P, C.c_int]
     L.rp3dg_world_get_tuning.argtypes = [P, P]
     L.rp3dg_world_add_joints.argtypes = [P, P, C.c_uint32]
@@ -755,6 +757,19 @@ class World:
         t = np.zeros(4, np.uint32)
         self.lib.rp3dg_world_get_tuning(self.h, t.ctypes.data)
         return {"small_max": int(t[0]), "giant_min": int(t[1]), "large_per_sm": int(t[2]), "tuning": bool(t[3])}
+
+    def set_device_trees(self, enable=True):
+        """Keep the worlds' broad-phase trees on the device (reinsertions and
+        queries on the GPU) or on the host; results are identical."""
+        rc = self.lib.rp3dg_world_set_device_trees(self.h, int(bool(enable)))
+        if rc != 0:
+            raise Rp3dgError(rc, self.lib.rp3dg_last_error(self.ctx.h).decode())
+
+    @property
+    def device_trees(self):
+        v = C.c_int(0)
+        self.lib.rp3dg_world_get_device_trees(self.h, C.byref(v))
+        return bool(v.value)
 
     def set_solver(self, solver=SOLVER_EXACT, stats=False):
         """RP3DG_SOLVER_EXACT (the drop-in) or RP3DG_SOLVER_GRAPH_COLORED; with

@@ -246,6 +246,44 @@ def test_autotuned_scheduling_gives_identical_results(ctx):
     b.close()
 
 
+def test_device_trees_give_identical_results(ctx):
+    """A world group keeps its broad-phase trees on the device (reinsertions
+    one GPU thread per world, queries one thread per moved collider); the
+    same group with host trees, and one switched between the two every few
+    steps, end with the same pairs, contacts and states at every checkpoint,
+    and world raycasts (which copy a world's device tree back) hit the same
+    colliders at the same points."""
+    shapes, scs = scenes.many_worlds(96, seed=23, min_bodies=20, max_bodies=200, ragdolls=(1, 2), limits=True)
+    a = engine.WorldGroup(ctx, scs, shapes, threads=4)
+    b = engine.WorldGroup(ctx, scs, shapes, threads=4)
+    c = engine.WorldGroup(ctx, scs, shapes, threads=4)
+    assert a.device_trees and b.device_trees
+    b.set_device_trees(False)
+    assert not b.device_trees
+    rays = scenes.world_rays(4000, (-12, -0.5, -12), (12, 8, 12), seed=5, masks=(0xFFFF,))
+    for step in range(60):
+        for g in (a, b, c):
+            g.update(float(worldio.DT))
+        if step % 7 == 3:
+            c.set_device_trees(not c.device_trees)
+        if step % 15 == 14:
+            for k in (0, 17, 50, 95):
+                pa = a.pairs(k)
+                assert np.array_equal(pa, b.pairs(k)) and np.array_equal(pa, c.pairs(k)), (step, k)
+                for x, y, z in zip(a.contacts(k), b.contacts(k), c.contacts(k)):
+                    assert np.array_equal(x, y) and np.array_equal(x, z), (step, k)
+                for x, y in zip(a.bodies(k), b.bodies(k)):
+                    assert np.array_equal(x, y), (step, k)
+                ha, na = a.raycast(rays, A.RAYCAST_ALL, 4, world=k)
+                hb, nb = b.raycast(rays, A.RAYCAST_ALL, 4, world=k)
+                assert np.array_equal(na, nb) and np.array_equal(ha, hb), (step, k)
+    assert a.stats()["overlapping_pairs"] > 0
+    one = engine.World(ctx, scs[0])
+    assert not one.device_trees
+    for g in (a, b, c, one):
+        g.close()
+
+
 @pytest.mark.skipif(not (reflib.have_ref("f32") and reflib.have_ref("f64")), reason="reference engine not built")
 def test_ragdolls_with_limits_stay_within_tolerance(ctx):
     """Cone and hinge limits go through acos / atan2, whose last bit differs
