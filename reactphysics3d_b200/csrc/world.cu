@@ -658,6 +658,76 @@ struct FlatMap {
     }
 };
 
+// Pair id -> index in its pair array (OverlappingPairs' mMapConvexPairIdToPairIndex
+// and the three other maps; only looked up, never iterated, so its order is
+// free): open addressing with linear probing, deletion by backward shift,
+// at most half full.  find / end / operator[] / erase as std::unordered_map.
+struct PairMap {
+    static constexpr uint64_t EMPTY = ~uint64_t(0);
+    struct Entry {
+        uint64_t first = EMPTY;
+        uint32_t second = 0;
+    };
+    std::vector<Entry> slots;
+    uint32_t mask = 0;
+    size_t n = 0;
+
+    static uint32_t hash(uint64_t k) {
+        k ^= k >> 33;
+        k *= 0xff51afd7ed558ccdull;
+        k ^= k >> 33;
+        return uint32_t(k);
+    }
+    Entry* end() const { return nullptr; }
+    Entry* find(uint64_t k) {
+        if (!n) return nullptr;
+        for (uint32_t h = hash(k) & mask;; h = (h + 1) & mask) {
+            if (slots[h].first == k) return &slots[h];
+            if (slots[h].first == EMPTY) return nullptr;
+        }
+    }
+    void rehash(size_t cap) {
+        std::vector<Entry> old;
+        old.swap(slots);
+        slots.assign(cap, Entry());
+        mask = uint32_t(cap - 1);
+        for (const Entry& e : old)
+            if (e.first != EMPTY) {
+                uint32_t h = hash(e.first) & mask;
+                while (slots[h].first != EMPTY) h = (h + 1) & mask;
+                slots[h] = e;
+            }
+    }
+    uint32_t& operator[](uint64_t k) {
+        if (2 * (n + 1) > slots.size()) rehash(std::max<size_t>(16, 2 * slots.size()));
+        uint32_t h = hash(k) & mask;
+        while (slots[h].first != EMPTY && slots[h].first != k) h = (h + 1) & mask;
+        if (slots[h].first == EMPTY) {
+            slots[h].first = k;
+            slots[h].second = 0;
+            n++;
+        }
+        return slots[h].second;
+    }
+    void erase(uint64_t k) {
+        Entry* e = find(k);
+        if (!e) return;
+        uint32_t i = uint32_t(e - slots.data()), j = i;
+        for (;;) {
+            j = (j + 1) & mask;
+            if (slots[j].first == EMPTY) break;
+            const uint32_t home = hash(slots[j].first) & mask;
+            // the entry at j stays where it is if its home lies cyclically in (i, j]
+            const bool stays = i <= j ? (i < home && home <= j) : (i < home || home <= j);
+            if (stays) continue;
+            slots[i] = slots[j];
+            i = j;
+        }
+        slots[i] = Entry();
+        n--;
+    }
+};
+
 // Device columns of the rigid-body components (row = world's first row + component slot).
 enum BodyCol { BC_POS, BC_ORI, BC_COMW, BC_COML, BC_LV, BC_AV, BC_F, BC_T, BC_IIL, BC_MASS, BC_LLOCK, BC_ALOCK,
                BC_XC, BC_QC, BC_NCOL };  // XC / QC: constrained position / orientation (joints)
@@ -707,7 +777,7 @@ struct WorldH {
     // overlapping pairs (OverlappingPairs::mConvexPairs / mDisabledConvexPairs,
     // mConcavePairs / mDisabledConcavePairs)
     std::vector<PairH> pairs, disabled, concave, concave_dis;
-    std::unordered_map<uint64_t, uint32_t> map_pairs, map_disabled, map_concave, map_concave_dis;
+    PairMap map_pairs, map_disabled, map_concave, map_concave_dis;
     std::vector<int> free_cache;
     std::vector<int32_t> reset_slots;
     // contacts of this step and of the previous one
@@ -732,6 +802,11 @@ struct WorldH {
     std::vector<int4> jlist;                   // this step's joints, island by island (record, rows, flags)
     std::vector<uint32_t> isl_jstart, isl_jcount;
     uint32_t jl_base = 0;
+    // islands with joints (group island index), their enabled non-static
+    // bodies' rows, and where they go in the group's lists
+    std::vector<uint32_t> ji_isl, ji_bcount;
+    std::vector<int32_t> ji_rows;
+    uint32_t ji_off = 0, ji_row_off = 0;
     bool stepped = false;
     // Body::mIsDebugEnabled by body id, and where the last update's debug
     // primitives of this world start in the group's buffers
@@ -987,7 +1062,7 @@ PairH* find_pair(WorldH& w, uint64_t id) {
 }
 
 // swap-remove from a pair array keeping its id map (removeConvexPairWithIndex)
-void remove_pair_at(std::vector<PairH>& arr, std::unordered_map<uint64_t, uint32_t>& map, uint32_t idx) {
+void remove_pair_at(std::vector<PairH>& arr, PairMap& map, uint32_t idx) {
     map.erase(arr[idx].id);
     const uint32_t last = uint32_t(arr.size()) - 1;
     if (arr.size() > 1 && idx < last) map[arr[last].id] = idx;
@@ -1588,6 +1663,22 @@ void fill_manifolds(Group* g, WorldH& w) {
         e.z = int(w.b0) + w.bcomp.slot[size_t(e.z)];
         g->h_jlist[w.jl_base + k] = e;
     }
+    // islands with joints and their bodies' rows (the joints' position correction)
+    w.ji_isl.clear();
+    w.ji_bcount.clear();
+    w.ji_rows.clear();
+    if (!w.jlist.empty())
+        for (uint32_t i = 0; i < w.islands.size(); i++) {
+            if (!w.isl_jcount[i]) continue;
+            w.ji_isl.push_back(w.isl_base + i);
+            const uint32_t r0 = uint32_t(w.ji_rows.size());
+            for (uint32_t ib = w.islands[i].body_start; ib < w.islands[i].body_start + w.islands[i].body_count; ib++) {
+                const int b = w.isl_bodies[ib];
+                if (w.bodies[size_t(b)].type != RP3DG_BODY_STATIC)
+                    w.ji_rows.push_back(int32_t(w.b0) + w.bcomp.slot[size_t(b)]);
+            }
+            w.ji_bcount.push_back(uint32_t(w.ji_rows.size()) - r0);
+        }
     // computeMapPreviousContactPairs for the next step
     w.prev_map.clear_for(w.cpairs.size());
     for (uint32_t i = 0; i < w.cpairs.size(); i++) w.prev_map.put(w.cpairs[i].id, i);
@@ -2938,17 +3029,30 @@ int update_group(Group* g, float dt) {
     std::vector<uint32_t> ji_island, ji_bstart, ji_bcount;
     std::vector<int32_t> ji_rows;
     if (NJ) {
-        for (WorldH& w : g->worlds)
-            for (uint32_t i = 0; i < w.islands.size(); i++) {
-                if (!w.isl_jcount[i]) continue;
-                ji_island.push_back(w.isl_base + i);
-                ji_bstart.push_back(uint32_t(ji_rows.size()));
-                for (uint32_t ib = w.islands[i].body_start; ib < w.islands[i].body_start + w.islands[i].body_count; ib++) {
-                    const int b = w.isl_bodies[ib];
-                    if (w.bodies[size_t(b)].type != RP3DG_BODY_STATIC) ji_rows.push_back(int32_t(w.b0) + w.bcomp.slot[size_t(b)]);
-                }
-                ji_bcount.push_back(uint32_t(ji_rows.size()) - ji_bstart.back());
+        // the worlds' lists (fill_manifolds) back to back
+        size_t nisl = 0, nrows = 0;
+        for (WorldH& w : g->worlds) {
+            w.ji_off = uint32_t(nisl);
+            w.ji_row_off = uint32_t(nrows);
+            nisl += w.ji_isl.size();
+            nrows += w.ji_rows.size();
+        }
+        ji_island.resize(nisl);
+        ji_bstart.resize(nisl);
+        ji_bcount.resize(nisl);
+        ji_rows.resize(nrows);
+        for_worlds(g, [&](int k) {
+            const WorldH& w = g->worlds[size_t(k)];
+            uint32_t r = w.ji_row_off;
+            for (size_t i = 0; i < w.ji_isl.size(); i++) {
+                ji_island[w.ji_off + i] = w.ji_isl[i];
+                ji_bstart[w.ji_off + i] = r;
+                ji_bcount[w.ji_off + i] = w.ji_bcount[i];
+                r += w.ji_bcount[i];
             }
+            if (!w.ji_rows.empty())
+                std::memcpy(ji_rows.data() + w.ji_row_off, w.ji_rows.data(), w.ji_rows.size() * 4);
+        });
         if (dev_grow(&g->d_jiisl, &g->cap_ji, ji_island.size() + 1) ||
             dev_grow(&g->d_jibstart, &g->cap_jbs, ji_island.size() + 1) ||
             dev_grow(&g->d_jibcount, &g->cap_jbc, ji_island.size() + 1) ||
