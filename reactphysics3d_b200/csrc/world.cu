@@ -385,25 +385,27 @@ __global__ void __launch_bounds__(128) world_tree_query_group(const TreeNode* __
 
 // DynamicAABBTree::updateObject's reinsertions (DynamicAABBTree.cpp:186-214,
 // removeLeafNode :348-412, insertLeafNode :219-345, balanceSubTreeAtNode
-// :420-586) of a world group's moved colliders: one warp per world, its
-// first lane replaying the world's reinsertions in collider-component order
-// (the order of BroadPhaseSystem::updateCollidersComponents) on the world's
-// device tree.  job j = (leaf, row of the collider's new fat AABB).
+// :420-586) of a world group's moved colliders: one warp per world.  The
+// warp reads the world's collider rows 32 at a time (component order, the
+// enabled ones first: the order of BroadPhaseSystem::updateCollidersComponents)
+// and its first lane replays the reinsertions of the moved ones on the
+// world's device tree, in that order.
 struct TreeReinsertArgs {
     uint32_t nworlds;
     TreeNode* pool;
     const uint32_t* base;
     int4* hdr;
-    const uint32_t* job_start;   // nworlds + 1
-    const int2* jobs;
+    const uint2* rows;           // per world: first collider row, colliders
+    const uint8_t *enabled, *moved;
+    const int32_t* leaf;         // per row: the collider's tree leaf
     const float4 *fmin, *fmax;
     uint32_t* error;             // bit 1: a tree would have had to grow; bit 2: a leaf out of range
 };
 __global__ void __launch_bounds__(128) world_tree_reinsert(const TreeReinsertArgs a) {
     const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (k >= a.nworlds || (threadIdx.x & 31) != 0) return;
-    const uint32_t j0 = a.job_start[k], j1 = a.job_start[k + 1];
-    if (j0 == j1) return;
+    const uint32_t lane = threadIdx.x & 31;
+    if (k >= a.nworlds) return;
+    const uint2 rows = a.rows[k];
     const int4 h = a.hdr[k];
     rp3dg::order::DevTree t;
     t.nodes.p = a.pool + a.base[k];
@@ -411,23 +413,47 @@ __global__ void __launch_bounds__(128) world_tree_reinsert(const TreeReinsertArg
     t.root = h.x;
     t.free_id = h.y;
     t.nb_nodes = h.z;
-    for (uint32_t j = j0; j < j1; j++) {
-        const int2 job = a.jobs[j];
-        if (job.x < 0 || job.x >= h.w) {
-            atomicOr(a.error, 2u);
-            break;
+    bool changed = false, stop = false;
+    for (uint32_t r0 = rows.x; r0 < rows.x + rows.y && !stop; r0 += 32) {
+        const uint32_t r = r0 + lane;
+        const bool in = r < rows.x + rows.y;
+        const bool en = in && a.enabled[r];
+        const bool mv = en && a.moved[r];
+        const unsigned ben = __ballot_sync(0xffffffffu, en);
+        unsigned bmv = __ballot_sync(0xffffffffu, mv);
+        // the enabled rows come first: the first disabled one ends them
+        const unsigned nen = ~ben & ((r0 + 32 <= rows.x + rows.y) ? 0xffffffffu : ((1u << (rows.x + rows.y - r0)) - 1u));
+        if (nen) {
+            bmv &= (1u << (__ffs(nen) - 1)) - 1u;
+            stop = true;
         }
-        const float4 mn = a.fmin[job.y], mx = a.fmax[job.y];
-        rp3dg::order::Box b;
-        b.mn[0] = mn.x; b.mn[1] = mn.y; b.mn[2] = mn.z;
-        b.mx[0] = mx.x; b.mx[1] = mx.y; b.mx[2] = mx.z;
-        t.reinsert(job.x, b);
-        if (t.failed) {
-            atomicOr(a.error, 1u);
-            break;
+        if (lane == 0) {
+            while (bmv) {
+                const int b = __ffs(bmv) - 1;
+                bmv &= bmv - 1;
+                const uint32_t rr = r0 + uint32_t(b);
+                const int id = a.leaf[rr];
+                if (id < 0 || id >= h.w) {
+                    atomicOr(a.error, 2u);
+                    stop = true;
+                    break;
+                }
+                const float4 mn = a.fmin[rr], mx = a.fmax[rr];
+                rp3dg::order::Box box;
+                box.mn[0] = mn.x; box.mn[1] = mn.y; box.mn[2] = mn.z;
+                box.mx[0] = mx.x; box.mx[1] = mx.y; box.mx[2] = mx.z;
+                t.reinsert(id, box);
+                changed = true;
+                if (t.failed) {
+                    atomicOr(a.error, 1u);
+                    stop = true;
+                    break;
+                }
+            }
         }
+        stop = __shfl_sync(0xffffffffu, stop, 0);
     }
-    a.hdr[k] = make_int4(t.root, t.free_id, t.nb_nodes, t.nodes.n);
+    if (lane == 0 && changed) a.hdr[k] = make_int4(t.root, t.free_id, t.nb_nodes, t.nodes.n);
 }
 
 uint32_t blocks(uint32_t n) { return (n + 127) / 128; }
@@ -828,10 +854,8 @@ struct WorldH {
     std::vector<int4> q_pos;
     std::vector<int32_t> q_shapes;             // this step's moved colliders in the moved set's order
     uint32_t q_off = 0;                        // their first query in the group's device query list
-    // device tree of a world group: this step's reinsertions (leaf, row) and
-    // whether the host tree's inner nodes are older than the device's (the
-    // host keeps the leaves' boxes current either way)
-    std::vector<int2> reins;
+    // device tree of a world group: whether the host tree's inner nodes are
+    // older than the device's (the host keeps the leaves' boxes current)
     bool tree_stale = false;
     std::vector<int> slept;                    // bodies put to sleep by this step
     rp3dg_world_stats stats{};
@@ -864,7 +888,7 @@ struct rp3dg_world {
     float4* biiw[2] = {};
     uint8_t *bgrav = nullptr, *b_en = nullptr, *c_en = nullptr;
     float4* ccol[2][CC_NCOL] = {};
-    int32_t *c_body = nullptr, *c_shape = nullptr;
+    int32_t *c_body = nullptr, *c_shape = nullptr, *c_leaf = nullptr;   // c_leaf: the collider's tree leaf
     uint16_t *c_cat = nullptr, *c_mask = nullptr;
     uint8_t* c_moved = nullptr;
     int cur_b = 0, cur_c = 0;
@@ -875,7 +899,7 @@ struct rp3dg_world {
     bool tables_dirty = true;
     // pinned host copies of the per-row tables and the row permutations
     uint8_t *t_grav = nullptr, *t_ben = nullptr, *t_cen = nullptr;
-    int32_t *t_cbody = nullptr, *t_cshape = nullptr, *t_bperm = nullptr, *t_cperm = nullptr;
+    int32_t *t_cbody = nullptr, *t_cshape = nullptr, *t_cleaf = nullptr, *t_bperm = nullptr, *t_cperm = nullptr;
     uint16_t *t_cat = nullptr, *t_mask = nullptr;
     // narrow-phase step buffers (all batches of all worlds concatenated)
     size_t cap_items = 0;
@@ -938,11 +962,11 @@ struct rp3dg_world {
     TreeNode* d_tree = nullptr;
     uint32_t* d_tree_base = nullptr;
     int4* d_tree_hdr = nullptr;
+    uint2* d_tree_rows = nullptr;                    // per world: first collider row, colliders
     std::vector<uint32_t> tree_base;
-    size_t cap_tjobs = 0, cap_tjoff = 0, cap_gq = 0;
-    int2 *h_tjobs = nullptr, *d_tjobs = nullptr;     // reinsertions (leaf, row), world after world
-    uint32_t *h_tjoff = nullptr, *d_tjoff = nullptr; // first reinsertion of each world
+    size_t cap_gq = 0;
     int2 *h_gq = nullptr, *d_gq = nullptr;           // queries (world, leaf)
+    cudaEvent_t ev_step_copy = nullptr;              // the step's moved flags and fat AABBs are on the host
     // world raycasts: the tree's nodes and the collider table as the ray
     // kernel reads them (rebuilt when the world state changed), rays and hits
     uint64_t state_version = 1;      // bumped by every update and between-step change
@@ -1689,7 +1713,6 @@ void fill_manifolds(Group* g, WorldH& w) {
 void colliders_and_sleep(Group* g, WorldH& w, float dt, const uint8_t* h_moved, const float4* h_fmin,
                          const float4* h_fmax, const float4* h_lv, const float4* h_av) {
     uint32_t nmoved = 0;
-    w.reins.clear();
     for (uint32_t s = 0; s < w.ccomp.n_enabled; s++) {
         const uint32_t r = w.c0 + s;
         if (!h_moved[r]) continue;
@@ -1701,7 +1724,6 @@ void colliders_and_sleep(Group* g, WorldH& w, float dt, const uint8_t* h_moved, 
         if (g->dev_tree) {
             // the device tree reinserts (reinsert_on_device); the host keeps the leaf's box
             w.tree.nodes[size_t(bp)].box = box;
-            w.reins.push_back(make_int2(bp, int(r)));
             w.tree_stale = true;
         } else {
             w.tree.reinsert(bp, box);
@@ -1876,26 +1898,34 @@ int upload_trees(Group* g) {
     cudaFree(g->d_tree);
     cudaFree(g->d_tree_base);
     cudaFree(g->d_tree_hdr);
+    cudaFree(g->d_tree_rows);
     g->d_tree = nullptr;
     g->d_tree_base = nullptr;
     g->d_tree_hdr = nullptr;
+    g->d_tree_rows = nullptr;
     if (cudaMalloc(&g->d_tree, std::max<size_t>(total, 1) * sizeof(TreeNode)) != cudaSuccess ||
         cudaMalloc(&g->d_tree_base, std::max<size_t>(nw, 1) * 4) != cudaSuccess ||
         cudaMalloc(&g->d_tree_hdr, std::max<size_t>(nw, 1) * sizeof(int4)) != cudaSuccess ||
+        cudaMalloc(&g->d_tree_rows, std::max<size_t>(nw, 1) * sizeof(uint2)) != cudaSuccess ||
         !pair_grow(&g->h_tcnt, &g->d_tcnt, &g->cap_tcnt, 4))
         return wfail(g, RP3DG_ENOMEM, "cudaMalloc(device trees)");
+    if (!g->ev_step_copy && cudaEventCreateWithFlags(&g->ev_step_copy, cudaEventDisableTiming) != cudaSuccess)
+        return wfail(g, RP3DG_ECUDA, "cudaEventCreate(step copies)");
     std::vector<TreeNode> nodes(total);
     std::vector<int4> hdr(nw);
+    std::vector<uint2> rows(nw);
     for (size_t k = 0; k < nw; k++) {
         const rp3dg::order::Tree& t = g->worlds[k].tree;
         std::copy(t.nodes.begin(), t.nodes.end(), nodes.begin() + g->tree_base[k]);
         hdr[k] = make_int4(t.root, t.free_id, t.nb_nodes, int(t.nodes.size()));
+        rows[k] = make_uint2(g->worlds[k].c0, g->worlds[k].nc);
         g->worlds[k].tree_stale = false;
     }
     cudaStream_t st = g->stream;
     cudaMemcpyAsync(g->d_tree, nodes.data(), total * sizeof(TreeNode), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(g->d_tree_base, g->tree_base.data(), nw * 4, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(g->d_tree_hdr, hdr.data(), nw * sizeof(int4), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(g->d_tree_rows, rows.data(), nw * sizeof(uint2), cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(g->d_tcnt, 0, 16, st);
     const cudaError_t e = cudaStreamSynchronize(st);
     return e == cudaSuccess ? 0 : wcuda(g, e, "upload of the device trees");
@@ -1923,37 +1953,25 @@ int download_tree(Group* g, uint32_t k) {
     return 0;
 }
 
-// Queues this step's reinsertions of every world (WorldH::reins) on the
-// device trees; fmin / fmax are the fat AABBs by row of the step.
-int reinsert_on_device(Group* g, const float4* fmin, const float4* fmax) {
+// Queues the reinsertions of every world's moved colliders on the device
+// trees (the step's moved flags and fat AABBs by row, rows as the last row
+// sync left them).
+int reinsert_on_device(Group* g, const uint8_t* moved, const float4* fmin, const float4* fmax) {
     const size_t nw = g->worlds.size();
-    if (!pair_grow(&g->h_tjoff, &g->d_tjoff, &g->cap_tjoff, nw + 1)) return wfail(g, RP3DG_ENOMEM, "cudaMalloc(tree jobs)");
-    size_t total = 0;
-    for (size_t k = 0; k < nw; k++) {
-        g->h_tjoff[k] = uint32_t(total);
-        total += g->worlds[k].reins.size();
-    }
-    g->h_tjoff[nw] = uint32_t(total);
-    if (!total) return 0;
-    if (!pair_grow(&g->h_tjobs, &g->d_tjobs, &g->cap_tjobs, total)) return wfail(g, RP3DG_ENOMEM, "cudaMalloc(tree jobs)");
-    for_worlds(g, [&](int k) {
-        const std::vector<int2>& r = g->worlds[size_t(k)].reins;
-        if (!r.empty()) std::memcpy(g->h_tjobs + g->h_tjoff[k], r.data(), r.size() * sizeof(int2));
-    });
-    cudaStream_t st = g->stream;
-    cudaMemcpyAsync(g->d_tjoff, g->h_tjoff, (nw + 1) * 4, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(g->d_tjobs, g->h_tjobs, total * sizeof(int2), cudaMemcpyHostToDevice, st);
+    if (!nw) return 0;
     TreeReinsertArgs a{};
     a.nworlds = uint32_t(nw);
     a.pool = g->d_tree;
     a.base = g->d_tree_base;
     a.hdr = g->d_tree_hdr;
-    a.job_start = g->d_tjoff;
-    a.jobs = g->d_tjobs;
+    a.rows = g->d_tree_rows;
+    a.enabled = g->c_en;
+    a.moved = moved;
+    a.leaf = g->c_leaf;
     a.fmin = fmin;
     a.fmax = fmax;
     a.error = g->d_tcnt + 2;
-    world_tree_reinsert<<<uint32_t((nw * 32 + 127) / 128), 128, 0, st>>>(a);
+    world_tree_reinsert<<<uint32_t((nw * 32 + 127) / 128), 128, 0, g->stream>>>(a);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : wcuda(g, e, "tree reinsertion launch");
 }
@@ -2018,6 +2036,7 @@ void world_tables(Group* g, WorldH& w) {
         const ColliderH& C = w.colliders[size_t(w.ccomp.at[r])];
         g->t_cbody[w.c0 + r] = int32_t(w.b0) + w.bcomp.slot[size_t(C.body)];
         g->t_cshape[w.c0 + r] = C.shape;
+        g->t_cleaf[w.c0 + r] = C.bp;
         g->t_cat[w.c0 + r] = C.category;
         g->t_mask[w.c0 + r] = C.mask;
         g->t_cen[w.c0 + r] = r < w.ccomp.n_enabled ? 1 : 0;
@@ -2028,7 +2047,7 @@ int ensure_tables(Group* g) {
     if (g->t_grav) return 0;
     const size_t nb = std::max<uint32_t>(g->NB, 1), nc = std::max<uint32_t>(g->NC, 1);
     if (cudaMallocHost(&g->t_grav, nb) || cudaMallocHost(&g->t_ben, nb) || cudaMallocHost(&g->t_cen, nc) ||
-        cudaMallocHost(&g->t_cbody, nc * 4) || cudaMallocHost(&g->t_cshape, nc * 4) ||
+        cudaMallocHost(&g->t_cbody, nc * 4) || cudaMallocHost(&g->t_cshape, nc * 4) || cudaMallocHost(&g->t_cleaf, nc * 4) ||
         cudaMallocHost(&g->t_cat, nc * 2) || cudaMallocHost(&g->t_mask, nc * 2) ||
         cudaMallocHost(&g->t_bperm, nb * 4) || cudaMallocHost(&g->t_cperm, nc * 4))
         return wfail(g, RP3DG_ENOMEM, "cudaMallocHost(row tables)");
@@ -2102,6 +2121,7 @@ int sync_rows(Group* g) {
         cudaMemcpyAsync(g->b_en, g->t_ben, g->NB, cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(g->c_en, g->t_cen, g->NC, cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(g->c_body, g->t_cbody, size_t(g->NC) * 4, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(g->c_leaf, g->t_cleaf, size_t(g->NC) * 4, cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(g->c_shape, g->t_cshape, size_t(g->NC) * 4, cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(g->c_cat, g->t_cat, size_t(g->NC) * 2, cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(g->c_mask, g->t_mask, size_t(g->NC) * 2, cudaMemcpyHostToDevice, st);
@@ -2241,6 +2261,8 @@ void destroy_group(Group* g) {
         g->cbuf[k].release();
     }
     cudaFree(g->bgrav); cudaFree(g->b_en); cudaFree(g->c_en); cudaFree(g->c_body); cudaFree(g->c_shape);
+    cudaFree(g->c_leaf); cudaFreeHost(g->t_cleaf); cudaFree(g->d_tree_rows);
+    if (g->ev_step_copy) cudaEventDestroy(g->ev_step_copy);
     cudaFree(g->c_cat); cudaFree(g->c_mask); cudaFree(g->c_moved); cudaFree(g->pool); cudaFree(g->d_small);
     cudaFree(g->d_items); cudaFree(g->d_s1); cudaFree(g->d_s2); cudaFree(g->d_p1); cudaFree(g->d_r1);
     cudaFree(g->d_p2); cudaFree(g->d_r2); cudaFree(g->d_rep); cudaFree(g->d_coll); cudaFree(g->d_nct);
@@ -2270,7 +2292,6 @@ void destroy_group(Group* g) {
     cudaFreeHost(g->h_tleaves); cudaFree(g->d_tleaves); cudaFreeHost(g->h_tpos); cudaFree(g->d_tpos);
     cudaFreeHost(g->h_tcnt); cudaFree(g->d_tcnt);
     cudaFree(g->d_tree); cudaFree(g->d_tree_base); cudaFree(g->d_tree_hdr);
-    cudaFreeHost(g->h_tjobs); cudaFree(g->d_tjobs); cudaFreeHost(g->h_tjoff); cudaFree(g->d_tjoff);
     cudaFreeHost(g->h_gq); cudaFree(g->d_gq);
     cudaFreeHost(g->h_rnodes); cudaFree(g->d_rnodes); cudaFreeHost(g->h_rcols); cudaFree(g->d_rcols);
     cudaFree(g->d_rhf); cudaFree(g->d_rays); cudaFree(g->d_rhits); cudaFree(g->d_rcount);
@@ -2513,7 +2534,7 @@ int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds
         for (int c = 0; c < CC_NCOL; c++) M((void**)&g->ccol[k][c], size_t(NC) * 16);
     }
     M((void**)&g->bgrav, NB); M((void**)&g->b_en, NB); M((void**)&g->c_en, NC);
-    M((void**)&g->c_body, size_t(NC) * 4); M((void**)&g->c_shape, size_t(NC) * 4);
+    M((void**)&g->c_body, size_t(NC) * 4); M((void**)&g->c_shape, size_t(NC) * 4); M((void**)&g->c_leaf, size_t(NC) * 4);
     M((void**)&g->c_cat, size_t(NC) * 2); M((void**)&g->c_mask, size_t(NC) * 2); M((void**)&g->c_moved, NC);
     uint8_t* d_dyn = nullptr;
     M((void**)&d_dyn, NB);
@@ -2601,6 +2622,8 @@ int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds
                 w.moved.add(id);
             }
         }
+        // the row tables now hold each collider's tree leaf at the next sync
+        g->tables_dirty = true;
     }
     // the narrow phase's step buffers sized up front for twice as many convex
     // pairs as colliders: growing them later frees and maps hundreds of MB
@@ -3214,7 +3237,17 @@ int update_group(Group* g, float dt) {
         cudaMemcpyAsync(h_lv, g->bcol[bc][BC_LV], size_t(g->NB) * 16, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(h_av, g->bcol[bc][BC_AV], size_t(g->NB) * 16, cudaMemcpyDeviceToHost, st);
     }
-    cudaError_t e = cudaStreamSynchronize(st);
+    cudaError_t e;
+    if (g->dev_tree && g->NC) {
+        // the device trees' reinsertions run while the host does the sleep
+        // bookkeeping below (the next step's queries wait for them)
+        cudaEventRecord(g->ev_step_copy, st);
+        rc = reinsert_on_device(g, g->c_moved, g->ccol[ccur][CC_FMIN], g->ccol[ccur][CC_FMAX]);
+        if (rc) return rc;
+        e = cudaEventSynchronize(g->ev_step_copy);
+    } else {
+        e = cudaStreamSynchronize(st);
+    }
     if (e != cudaSuccess) return wcuda(g, e, "step");
     mark(6);
     // ---- reinsertions and sleeping of every world
@@ -3240,12 +3273,6 @@ int update_group(Group* g, float dt) {
     cudaMemsetAsync(g->bcol[bc][BC_T], 0, size_t(g->NB) * 16, st);
     e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return wcuda(g, e, "end of step");
-    // the device trees' reinsertions run while the host returns; the next
-    // step's queries (same stream) wait for them
-    if (g->dev_tree) {
-        rc = reinsert_on_device(g, g->ccol[ccur][CC_FMIN], g->ccol[ccur][CC_FMAX]);
-        if (rc) return rc;
-    }
     tuner_step(g);
     g->cur_cb = 1 - g->cur_cb;
     rc = debug_primitives(g);
