@@ -576,7 +576,8 @@ def many_worlds_section(ctx, args, with_cpu, rank=0, world=1):
     10 ball-and-socket + 4 hinge joints, 60-degree cones, +-60-degree hinge
     limits) falling onto a static ground each (scenes.many_worlds), dt 1/120,
     through one rp3dg_world_update per step of the whole group (wall clock,
-    synchronous).  60 untimed steps, then 60 timed.  With N ranks the worlds
+    synchronous; the worlds' broad-phase trees are on the device, their
+    reinsertions and queries on the GPU).  60 untimed steps, then 60 timed.  With N ranks the worlds
     are split into N contiguous blocks balanced by body count
     (reactphysics3d_b200.shard), each rank steps its block with
     cpu_count // N host threads, and the time is the slowest rank's (strong
@@ -629,6 +630,7 @@ def many_worlds_section(ctx, args, with_cpu, rank=0, world=1):
            "ranks": world, "scaling": "strong (the worlds are split over the ranks)",
            "rank0_block": [lo, hi], "kernels_per_step": round(launches, 1), "host_threads_per_rank": threads,
            "phase_ms_per_step": phases, "autotuned_scheduling": tuning,
+           "device_trees": g.device_trees,
            "stats_at_step_120": st, "api": "rp3dg_world_update (world group)"}
     if with_cpu and reflib.have_ref("f32"):
         raw = raw_all[lo:hi]

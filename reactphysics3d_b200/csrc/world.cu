@@ -49,7 +49,6 @@
 #include <unordered_map>
 #include <vector>
 
-#include <set>
 
 #include <omp.h>
 
@@ -705,6 +704,7 @@ struct PairMap {
         return uint32_t(k);
     }
     Entry* end() const { return nullptr; }
+    bool empty() const { return n == 0; }
     Entry* find(uint64_t k) {
         if (!n) return nullptr;
         for (uint32_t h = hash(k) & mask;; h = (h + 1) & mask) {
@@ -753,6 +753,10 @@ struct PairMap {
         n--;
     }
 };
+
+inline uint64_t body_pair_key(int a, int b) {
+    return (uint64_t(uint32_t(std::min(a, b))) << 32) | uint32_t(std::max(a, b));
+}
 
 // Device columns of the rigid-body components (row = world's first row + component slot).
 enum BodyCol { BC_POS, BC_ORI, BC_COMW, BC_COML, BC_LV, BC_AV, BC_F, BC_T, BC_IIL, BC_MASS, BC_LLOCK, BC_ALOCK,
@@ -821,7 +825,7 @@ struct WorldH {
     // of bodies that must not collide, the first record of this world
     std::vector<JointH> joints;
     rp3dg::order::Comps jcomp, bscomp, fcomp, hcomp, scomp;  // JointComponents, then one per joint type
-    std::set<std::pair<int, int>> nocollide;
+    PairMap nocollide;   // body pairs (smaller id << 32 | larger id) joined by a joint without collision
     uint32_t jbase = 0;
     struct Pose { float p[3], q[4]; };
     std::vector<Pose> init_pose;               // transforms at creation (joint anchors)
@@ -1376,8 +1380,7 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
             const int c1 = w.bp_to_collider[size_t(s)], c2 = w.bp_to_collider[size_t(leaf)];
             const ColliderH &C1 = w.colliders[size_t(c1)], &C2 = w.colliders[size_t(c2)];
             if (C1.body == C2.body) continue;
-            if (!w.nocollide.empty() &&
-                w.nocollide.count(std::make_pair(std::min(C1.body, C2.body), std::max(C1.body, C2.body))))
+            if (!w.nocollide.empty() && w.nocollide.find(body_pair_key(C1.body, C2.body)))
                 continue;
             const uint64_t id = pair_number(uint32_t(std::max(s, leaf)), uint32_t(std::min(s, leaf)));
             PairH* p = find_pair(w, id);
@@ -3393,7 +3396,7 @@ int add_joints(Group* g, uint32_t world, const rp3dg_joint_desc* jd, uint32_t n)
         const bool dis = !w.bcomp.enabled(J.b1) && !w.bcomp.enabled(J.b2);
         joint_type_comps(w, d.type).add(int(j), dis);
         w.jcomp.add(int(j), dis);
-        if (!d.collision_enabled) w.nocollide.insert(std::make_pair(std::min(J.b1, J.b2), std::max(J.b1, J.b2)));
+        if (!d.collision_enabled) w.nocollide[body_pair_key(J.b1, J.b2)] = 1;
         w.bodies[size_t(J.b1)].joints.push_back(int(j));
         w.bodies[size_t(J.b2)].joints.push_back(int(j));
         const auto& P1 = w.init_pose[size_t(J.b1)];
