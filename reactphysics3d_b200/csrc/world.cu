@@ -831,6 +831,9 @@ struct WorldH {
     std::vector<Pose> init_pose;               // transforms at creation (joint anchors)
     std::vector<int4> jlist;                   // this step's joints, island by island (record, rows, flags)
     std::vector<uint32_t> isl_jstart, isl_jcount;
+    std::vector<int2> jvisit;                  // scratch: (joint, island) in visiting order
+    std::vector<int> dfs_stack, dfs_statics;   // scratch of the island search
+    std::vector<uint32_t> jfill;               // scratch: next slot of each island's joints
     uint32_t jl_base = 0;
     // islands with joints (group island index), their enabled non-static
     // bodies' rows, and where they go in the group's lists
@@ -1538,7 +1541,9 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
     }
     for (auto& J : w.joints) J.in_island = false;
     uint32_t total_manifolds = 0;
-    std::vector<int> stack, statics;
+    std::vector<int>& stack = w.dfs_stack;
+    std::vector<int>& statics = w.dfs_statics;
+    statics.clear();
     for (uint32_t s = 0; s < w.bcomp.n_enabled; s++) {
         const int b0 = w.bcomp.at[s];
         if (w.bodies[size_t(b0)].in_island) continue;
@@ -1618,25 +1623,34 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
     w.isl_jstart.assign(w.islands.size(), 0);
     w.isl_jcount.assign(w.islands.size(), 0);
     if (!w.joints.empty()) {
-        std::vector<std::vector<int>> per(w.islands.size());
+        // (joint, island) in visiting order, then a stable counting sort by island
+        std::vector<int2>& jv = w.jvisit;
+        jv.clear();
         for (rp3dg::order::Comps* cmp : {&w.bscomp, &w.fcomp, &w.hcomp, &w.scomp})
             for (uint32_t s = 0; s < cmp->n_enabled; s++) {
                 const int j = cmp->at[s];
                 const JointH& J = w.joints[size_t(j)];
                 const int isl = w.bodies[size_t(J.b1)].type != RP3DG_BODY_STATIC ? w.bodies[size_t(J.b1)].island
                                                                                   : w.bodies[size_t(J.b2)].island;
-                if (isl >= 0) per[size_t(isl)].push_back(j);
+                if (isl >= 0) {
+                    jv.push_back(make_int2(j, isl));
+                    w.isl_jcount[size_t(isl)]++;
+                }
             }
-        for (size_t i = 0; i < per.size(); i++) {
-            w.isl_jstart[i] = uint32_t(w.jlist.size());
-            w.isl_jcount[i] = uint32_t(per[i].size());
-            for (int j : per[i]) {
-                const JointH& J = w.joints[size_t(j)];
-                const int flags = (w.bodies[size_t(J.b1)].type == RP3DG_BODY_DYNAMIC ? 1 : 0) |
-                                  (w.bodies[size_t(J.b2)].type == RP3DG_BODY_DYNAMIC ? 2 : 0);
-                // rows filled in fill_manifolds (after the row sync)
-                w.jlist.push_back(make_int4(int(w.jbase) + j, J.b1, J.b2, flags));
-            }
+        uint32_t run = 0;
+        for (size_t i = 0; i < w.islands.size(); i++) {
+            w.isl_jstart[i] = run;
+            run += w.isl_jcount[i];
+        }
+        w.jlist.resize(jv.size());
+        std::vector<uint32_t>& fill = w.jfill;
+        fill.assign(w.isl_jstart.begin(), w.isl_jstart.end());
+        for (const int2 e : jv) {
+            const JointH& J = w.joints[size_t(e.x)];
+            const int flags = (w.bodies[size_t(J.b1)].type == RP3DG_BODY_DYNAMIC ? 1 : 0) |
+                              (w.bodies[size_t(J.b2)].type == RP3DG_BODY_DYNAMIC ? 2 : 0);
+            // rows filled in fill_manifolds (after the row sync)
+            w.jlist[fill[size_t(e.y)]++] = make_int4(int(w.jbase) + e.x, J.b1, J.b2, flags);
         }
     }
 }
