@@ -21,6 +21,7 @@
 #include <array>
 #include <atomic>
 #include <cassert>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -516,6 +517,8 @@ int ref_world_capture(int id, float dt) {
                                  float(w.mContactSolverSystem.mRestitutionVelocityThreshold)};
     W.cap.put("params", params);
 
+    // the dynamics stage, timed (the CPU figure of the same stage on the GPU)
+    const auto t_dyn = std::chrono::steady_clock::now();
     w.updateBodiesInverseWorldInertiaTensors();
     w.enableDisableJoints();
     w.mDynamicsSystem.integrateRigidBodiesVelocities(timeStep);
@@ -523,6 +526,8 @@ int ref_world_capture(int id, float dt) {
     w.mDynamicsSystem.integrateRigidBodiesPositions(timeStep, w.mContactSolverSystem.isSplitImpulseActive());
     w.solvePositionCorrection();
     w.mDynamicsSystem.updateBodiesState();
+    W.cap.put("dyn_seconds",
+              std::vector<double>{std::chrono::duration<double>(std::chrono::steady_clock::now() - t_dyn).count()});
 
     capture_state(W, "out_", false);
     capture_contacts(W, "out_", order, false);

@@ -214,7 +214,7 @@ _WORLD_DTYPES = {"body_gravity": np.uint8, "collider_body": np.int32, "manifold_
                  "point_is_resting": np.uint8, "island_manifold_start": np.uint32,
                  "island_manifold_count": np.uint32, "body_nb_enabled": np.uint32,
                  "collider_nb_enabled": np.uint32, "bp_pairs": np.int32, "bp_bits": np.int32, "bp_id": np.int32,
-                 "bp_moved": np.uint8}
+                 "bp_moved": np.uint8, "dyn_seconds": np.float64}
 _WORLD_SHAPES = {"manifold_ids": (-1, 4), "bp_pairs": (-1, 2), "bp_bits": (-1, 2), "point_penetration_impulse": (-1,), "body_inv_inertia_world": (-1, 3, 4),
                  "body_split_velocity": (-1, 2, 4)}
 
