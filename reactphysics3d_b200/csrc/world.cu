@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(128) world_tree_query(const TreeNode* __restri
 }
 
 // A world group's trees: world k's nodes are pool[base[k], base[k] + hdr[k].w),
-// hdr[k] = (root, first free node, nodes in use, nodes).  Query i is
+// hdr[k] = (root, first free node, nodes in use, nodes held).  Query i is
 // (world, leaf); the moved colliders of a world are consecutive, so the
 // threads of a warp mostly walk the same tree.
 __global__ void __launch_bounds__(128) world_tree_query_group(const TreeNode* __restrict__ pool,
@@ -963,7 +963,7 @@ struct rp3dg_world {
     uint32_t *h_tcnt = nullptr, *d_tcnt = nullptr;   // [0] leaves reserved, [1] flags, [2] reinsertion errors
     // world groups: every world's broad-phase tree in one device pool (world
     // k's nodes from tree_base[k], header root / free node / nodes in use /
-    // nodes), reinserted and queried on the GPU; the host replica keeps the
+    // nodes held), reinserted and queried on the GPU; the host replica keeps the
     // moved set, the leaves' boxes and the pairs
     bool dev_tree = false;
     TreeNode* d_tree = nullptr;
@@ -1900,16 +1900,23 @@ void for_worlds(Group* g, F f) {
 
 // ---- device trees of a world group
 
-// Copies every world's host tree into the group's device pool (each world's
-// node array as it is: a reinsertion frees one node before it takes one, so
-// a tree never grows after its colliders were added).
+// Nodes of a world's tree that its device copy holds: a reinsertion frees
+// one node (its leaf's parent) and then takes that same node back, so a tree
+// never grows after its colliders were added and only the nodes below the
+// first never-used one (nodes in use, plus the free list's head) are ever
+// read or written; the rest of the host array stays as it is.
+int device_tree_nodes(const rp3dg::order::Tree& t) {
+    return std::min<int>(int(t.nodes.size()), t.nb_nodes + 1);
+}
+
+// Copies every world's host tree into the group's device pool.
 int upload_trees(Group* g) {
     const size_t nw = g->worlds.size();
     g->tree_base.assign(nw, 0);
     size_t total = 0;
     for (size_t k = 0; k < nw; k++) {
         g->tree_base[k] = uint32_t(total);
-        total += g->worlds[k].tree.nodes.size();
+        total += size_t(device_tree_nodes(g->worlds[k].tree));
     }
     if (total >= (size_t(1) << 31)) return wfail(g, RP3DG_EINVAL, "world group trees too large for the device pool");
     cudaFree(g->d_tree);
@@ -1933,8 +1940,9 @@ int upload_trees(Group* g) {
     std::vector<uint2> rows(nw);
     for (size_t k = 0; k < nw; k++) {
         const rp3dg::order::Tree& t = g->worlds[k].tree;
-        std::copy(t.nodes.begin(), t.nodes.end(), nodes.begin() + g->tree_base[k]);
-        hdr[k] = make_int4(t.root, t.free_id, t.nb_nodes, int(t.nodes.size()));
+        const int n = device_tree_nodes(t);
+        std::copy(t.nodes.begin(), t.nodes.begin() + n, nodes.begin() + g->tree_base[k]);
+        hdr[k] = make_int4(t.root, t.free_id, t.nb_nodes, n);
         rows[k] = make_uint2(g->worlds[k].c0, g->worlds[k].nc);
         g->worlds[k].tree_stale = false;
     }
@@ -1958,7 +1966,8 @@ int download_tree(Group* g, uint32_t k) {
     cudaMemcpyAsync(&h, g->d_tree_hdr + k, sizeof(int4), cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return wcuda(g, e, "download of a device tree");
-    if (h.w != int(w.tree.nodes.size())) return wfail(g, RP3DG_EINVAL, "device tree size changed");
+    if (h.w != device_tree_nodes(w.tree) || h.z != w.tree.nb_nodes)
+        return wfail(g, RP3DG_EINVAL, "device tree size changed");
     cudaMemcpyAsync(w.tree.nodes.data(), g->d_tree + g->tree_base[k], size_t(h.w) * sizeof(TreeNode),
                     cudaMemcpyDeviceToHost, st);
     e = cudaStreamSynchronize(st);

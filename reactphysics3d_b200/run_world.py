@@ -3,10 +3,13 @@
     python -m reactphysics3d_b200.run_world terrain --bodies 100000 --cols 257 --steps 156
     python -m reactphysics3d_b200.run_world pile --steps 300 --phases
     python -m reactphysics3d_b200.run_world terrain --bodies 20000 --steps 21 --rays 1048576
+    python -m reactphysics3d_b200.run_world worlds --worlds 4096 --dt 0.008333334 --steps 70 --phases
 
 Scenes: `pile` (scenes.box_pile), `mixed` (scenes.mixed_world), `terrain`
 (scenes.heightfield_world: --bodies bodies over a --cols x --cols height
-field), `ragdolls` (scenes.ragdoll_world).  The world is created, stepped
+field), `ragdolls` (scenes.ragdoll_world), `worlds` (--worlds independent
+worlds of scenes.many_worlds stepped as one group, rp3dg_world_group_create;
+--host-trees keeps their broad-phase trees on the host).  The world is created, stepped
 --steps times at --dt and synchronised; nothing else is launched, so kernel
 launch counts (for a profiler's skip / count options) follow from the step
 count.  --phases prints the per-phase host / device times per step
@@ -36,7 +39,9 @@ def make_scene(args):
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("scene", choices=["pile", "mixed", "terrain", "ragdolls"])
+    ap.add_argument("scene", choices=["pile", "mixed", "terrain", "ragdolls", "worlds"])
+    ap.add_argument("--worlds", type=int, default=4096)
+    ap.add_argument("--host-trees", action="store_true")
     ap.add_argument("--bodies", type=int, default=None)
     ap.add_argument("--cols", type=int, default=257)
     ap.add_argument("--seed", type=int, default=None)
@@ -48,16 +53,25 @@ def main():
     ap.add_argument("--rays", type=int, default=0)
     ap.add_argument("--ray-reps", type=int, default=1)
     args = ap.parse_args()
-    sc = make_scene(args)
     ctx = engine.Context(0)
-    w = engine.World(ctx, sc, threads=args.threads)
+    if args.scene == "worlds":
+        shapes, scs = scenes.many_worlds(args.worlds, seed=args.seed if args.seed is not None else 7)
+        w = engine.WorldGroup(ctx, scs, shapes, threads=args.threads)
+        if args.host_trees:
+            w.set_device_trees(False)
+        sc = scs[0]
+    else:
+        sc = make_scene(args)
+        w = engine.World(ctx, sc, threads=args.threads)
     n_plain = args.steps - (min(args.phase_steps, args.steps) if args.phases else 0)
     t0 = time.perf_counter()
     w.update(args.dt, n_plain)
     ctx.synchronize()
     sec = time.perf_counter() - t0
-    out = {"scene": sc.name, "steps": args.steps, "ms_per_step": round(1e3 * sec / max(n_plain, 1), 3),
-           "stats": w.stats()}
+    out = {"scene": f"{args.worlds} worlds" if args.scene == "worlds" else sc.name, "steps": args.steps,
+           "ms_per_step": round(1e3 * sec / max(n_plain, 1), 3), "stats": w.stats()}
+    if args.scene == "worlds":
+        out["device_trees"] = w.device_trees
     if args.phases and args.steps > n_plain:
         w.set_profiling(True)
         w.update(args.dt, args.steps - n_plain)
