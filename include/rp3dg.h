@@ -251,11 +251,12 @@ int rp3dg_narrowphase_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_pair_batch
  * other.  Batch b (algorithms[b], pairs[b], outs[b]) gives the results of
  * rp3dg_narrowphase_host on it; the batches overlap on the device: the
  * upload of one batch runs during the kernels of the one before, and each
- * batch's results go back while the next one computes.  Outputs in
- * page-locked host memory are written by the device directly, the contact
- * slots k < nb_contacts[i] only (the others are left untouched); other
- * outputs are copied back as rp3dg_narrowphase_host copies them.
- * Synchronizes before returning. */
+ * batch's results go back while the next one computes.  The device packs a
+ * batch's contacts densely (no gaps for pairs without contacts), the packed
+ * records and the flags and counts come back as plain copies, and the host
+ * threads write the contact slots k < nb_contacts[i] of the caller's arrays
+ * (the other slots are left untouched), so the outputs may be in pageable
+ * or page-locked memory.  Synchronizes before returning. */
 int rp3dg_narrowphase_input_host(rp3dg_ctx* ctx, uint32_t nb_batches, const int32_t* algorithms,
                                  const rp3dg_pair_batch* pairs, const rp3dg_contact_batch* outs,
                                  int clip_with_previous_axis);

@@ -645,27 +645,49 @@ __global__ void __launch_bounds__(NP_BLOCK) classify_pairs(const NpArgs a, uint8
     }
 }
 
-__global__ void __launch_bounds__(256) publish_contacts(const PublishArgs a) {
+// One warp per 32 pairs: an inclusive scan of the counts, one atomic for
+// the group's first record, then the warp writes its records as one
+// contiguous run (lane l the float4s l, l + 32, ...), so that records in
+// page-locked host memory go over the bus in full-width writes.  Float4 j
+// of the run belongs to record r = j / 3 of the lane whose inclusive count
+// is the first above r.
+__global__ void __launch_bounds__(256) compact_contacts(const CompactArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    a.h_col[i] = a.d_col[i];
-    const uint8_t c = a.d_nb[i];
-    a.h_nb[i] = c;
-    if (a.h_cache) {
-        const uint4 v = *reinterpret_cast<const uint4*>(a.d_cache + i);
-        *reinterpret_cast<uint4*>(a.h_cache + i) = v;
+    const uint32_t lane = threadIdx.x & 31u, group = i >> 5;
+    if ((group << 5) >= a.n) return;   // whole warps leave together
+    const uint32_t c = i < a.n ? a.nb[i] : 0u;
+    uint32_t incl = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= uint32_t(d)) incl += v;
     }
-    for (uint32_t k = 0; k < c; k++) {
-        const size_t o = size_t(k) * a.n + i;
-        a.h_nd[o] = a.d_nd[o];
-        a.h_l1[o] = a.d_l1[o];
-        a.h_l2[o] = a.d_l2[o];
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    uint32_t start = 0;
+    if (lane == 0) {
+        start = total ? atomicAdd(a.counter, total) : 0u;
+        a.warp_start[group] = start;
+    }
+    start = __shfl_sync(0xffffffffu, start, 0);
+    float4* dst = a.records + 3 * size_t(start);
+    const uint32_t excl = incl - c;
+    for (uint32_t j0 = 0; j0 < 3 * total; j0 += 32) {
+        const uint32_t j = j0 + lane, r = j / 3u, part = j - 3u * r;
+        uint32_t p = 0;
+#pragma unroll
+        for (uint32_t step = 16; step > 0; step >>= 1)
+            if (__shfl_sync(0xffffffffu, incl, int(p + step - 1)) <= r) p += step;
+        const uint32_t k = r - __shfl_sync(0xffffffffu, excl, int(p));
+        if (j < 3 * total) {
+            const size_t o = size_t(k) * a.n + (size_t(group) << 5) + p;
+            dst[j] = part == 0 ? a.nd[o] : (part == 1 ? a.l1[o] : a.l2[o]);
+        }
     }
 }
 
-cudaError_t launch_publish_contacts(const PublishArgs& a, cudaStream_t s) {
+cudaError_t launch_compact_contacts(const CompactArgs& a, cudaStream_t s) {
     if (a.n == 0) return cudaSuccess;
-    publish_contacts<<<(a.n + 255) / 256, 256, 0, s>>>(a);
+    compact_contacts<<<(a.n + 255) / 256, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -61,20 +61,20 @@ struct NpArgs {
 
 void upload_box_tables(const BoxTables& t, cudaStream_t s);
 
-// A batch's results from device arrays into host-accessible memory
-// (page-locked, written over the bus by the kernel): flags, counts, the
-// cache when given, and the contact slots k < nb_contacts[i] (slot-major,
-// n pairs per slot, like the device arrays).
-struct PublishArgs {
+// A batch's contacts packed densely for the copy to the host: the pairs in
+// groups of 32 (group g = pairs 32g .. 32g + 31); group g's contacts are
+// records warp_start[g] ... in pair order, slot order inside a pair, each
+// record three float4 (normal and depth, local point 1, local point 2).
+// *counter (zeroed before) ends as the number of records.
+struct CompactArgs {
     uint32_t n;
-    const uint8_t *d_col, *d_nb;
-    const float4 *d_nd, *d_l1, *d_l2;
-    const rp3dg_lastframe* d_cache;
-    uint8_t *h_col, *h_nb;
-    float4 *h_nd, *h_l1, *h_l2;
-    rp3dg_lastframe* h_cache;
+    const uint8_t* nb;                    // contacts per pair
+    const float4 *nd, *l1, *l2;           // slot-major, n pairs per slot
+    float4* records;                      // 3 per record
+    uint32_t* warp_start;                 // (n + 31) / 32
+    uint32_t* counter;
 };
-cudaError_t launch_publish_contacts(const PublishArgs& a, cudaStream_t s);
+cudaError_t launch_compact_contacts(const CompactArgs& a, cudaStream_t s);
 // Launches the kernels of one algorithm batch; *launches receives how many.
 cudaError_t launch_narrowphase(int algo, const NpArgs& args, int num_sms, cudaStream_t stream, int* launches);
 // Pairs of an all-box polyhedron batch grouped by their learned class

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <cfloat>
+#include <cstdlib>
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -229,12 +230,19 @@ struct rp3dg_ctx {
     // staging buffers for rp3dg_narrowphase_host
     void* d_stage = nullptr;
     size_t cap_stage = 0;
-    // rp3dg_narrowphase_input_host: staging of all batches, an upload and a
-    // result stream beside the compute stream, and two events per batch
+    // rp3dg_narrowphase_input_host: device staging of all batches; an
+    // upload stream, a stream for each batch's flags / counts / record
+    // count and one for its packed contacts beside the compute stream; four
+    // events per batch; page-locked host staging of the flags, counts and
+    // caches (h_imeta), of the packed contacts copied with the flags
+    // (h_ispec) and of those copied once their count is known (h_irec)
     void* d_istage = nullptr;
     size_t cap_istage = 0;
-    cudaStream_t s_up = nullptr, s_pub = nullptr;
+    cudaStream_t s_up = nullptr, s_pub = nullptr, s_rec = nullptr;
     std::vector<cudaEvent_t> events;
+    void *h_imeta = nullptr, *h_irec = nullptr, *h_ispec = nullptr;
+    size_t cap_imeta = 0, cap_irec = 0, cap_ispec = 0;
+    std::vector<uint32_t> last_pairs, last_records;   // per batch position: the last call's pairs and records
     // learned separating-axis MLP: one device block holding the fp32
     // parameters, Adam moments, gradients, packed bf16 fragments, loss word
     // and proposal counters; training scratch grows with the batch
@@ -463,6 +471,10 @@ void rp3dg_destroy(rp3dg_ctx* ctx) {
     cudaFree(ctx->d_istage);
     if (ctx->s_up) cudaStreamDestroy(ctx->s_up);
     if (ctx->s_pub) cudaStreamDestroy(ctx->s_pub);
+    if (ctx->s_rec) cudaStreamDestroy(ctx->s_rec);
+    cudaFreeHost(ctx->h_imeta);
+    cudaFreeHost(ctx->h_irec);
+    cudaFreeHost(ctx->h_ispec);
     for (cudaEvent_t ev : ctx->events) cudaEventDestroy(ev);
     cudaFree(ctx->d_error);
     cudaFree(ctx->d_events);
@@ -1014,6 +1026,7 @@ int rp3dg_set_shapes(rp3dg_ctx* ctx, const rp3dg_shape* shapes, uint32_t nb) {
 
 namespace {
 int grow(rp3dg_ctx* ctx, void** buf, size_t* cap, size_t need, const char* what);
+int grow_pinned(rp3dg_ctx* ctx, void** buf, size_t* cap, size_t need, const char* what);
 // polyhedron batches of at least this many pairs are grouped by class
 constexpr uint32_t NP_GROUP_MIN_PAIRS = 4096;
 
@@ -1286,30 +1299,30 @@ int rp3dg_narrowphase_manifolds_host(rp3dg_ctx* ctx, int algorithm, const rp3dg_
     return narrowphase_host_impl(ctx, algorithm, p, out, clip_with_previous_axis, true, kept);
 }
 
-namespace {
-// Host memory the device can write directly (page-locked and mapped, which
-// unified addressing gives every page-locked allocation).
-bool device_writable_host(const void* p) {
-    if (!p) return true;
-    cudaPointerAttributes at;
-    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return at.type == cudaMemoryTypeHost && at.devicePointer == p;
-}
-}  // namespace
-
 int rp3dg_narrowphase_input_host(rp3dg_ctx* ctx, uint32_t nb, const int32_t* algos, const rp3dg_pair_batch* P,
                                  const rp3dg_contact_batch* O, int clip) {
     if (!ctx || (nb && (!algos || !P || !O))) return fail(ctx, RP3DG_EINVAL, "null argument");
+    // device staging of a batch: its inputs, then one block of flags, counts,
+    // group starts and the record count (copied to the host in one piece),
+    // the slot-major contacts and the packed records; host staging: that
+    // block and the cache, then the records.  A batch whose pair count is
+    // the one of the same batch in the last call expects about as many
+    // records as then: that many (plus an eighth and 64) are copied back
+    // right after the flags, without waiting for the count; a batch with
+    // more records, or none expected, is copied once its count is known.
     struct Lay {
-        size_t s1, s2, p1, r1, p2, r2, rep, cache, col, nbc, nd, l1, l2;
-        bool pub;
+        size_t s1, s2, p1, r1, p2, r2, rep, cache, col, nbc, ws, cnt, meta, nd, l1, l2, rec;
+        size_t h_meta, h_cache, h_rec, h_spec;
+        uint32_t groups, expect;
+        bool spec;
     };
     std::vector<Lay> L(nb);
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-    size_t off = 0;
+    size_t off = 0, hoff = 0, hspec = 0;
+    if (ctx->last_pairs.size() != nb) {
+        ctx->last_pairs.assign(nb, 0);
+        ctx->last_records.assign(nb, 0);
+    }
     for (uint32_t b = 0; b < nb; b++) {
         const rp3dg_pair_batch& p = P[b];
         const rp3dg_contact_batch& o = O[b];
@@ -1322,6 +1335,7 @@ int rp3dg_narrowphase_input_host(rp3dg_ctx* ctx, uint32_t nb, const int32_t* alg
             return fail(ctx, RP3DG_EINVAL, "max_contacts must be in 1..16");
         const size_t n = p.n, mc = o.max_contacts;
         Lay& l = L[b];
+        l.groups = uint32_t((n + 31) / 32);
         l.s1 = off; off += al(n * 4);
         l.s2 = off; off += al(n * 4);
         l.p1 = off; off += al(n * 16);
@@ -1330,31 +1344,48 @@ int rp3dg_narrowphase_input_host(rp3dg_ctx* ctx, uint32_t nb, const int32_t* alg
         l.r2 = off; off += al(n * 16);
         l.rep = off; off += p.report_contacts ? al(n) : 0;
         l.cache = off; off += p.cache ? al(n * sizeof(rp3dg_lastframe)) : 0;
-        l.col = off; off += al(n);
-        l.nbc = off; off += al(n);
+        l.col = off;
+        l.nbc = l.col + al(n);
+        l.ws = l.nbc + al(n);
+        l.cnt = l.ws + al(size_t(l.groups) * 4);
+        l.meta = l.cnt + 4 - l.col;
+        off = l.col + al(l.meta);
         l.nd = off; off += al(n * mc * 16);
         l.l1 = off; off += al(n * mc * 16);
         l.l2 = off; off += al(n * mc * 16);
-        l.pub = device_writable_host(o.is_colliding) && device_writable_host(o.nb_contacts) &&
-                device_writable_host(o.normal_depth) && device_writable_host(o.local1) &&
-                device_writable_host(o.local2) && device_writable_host(p.cache) && aligned(o.normal_depth, 16) &&
-                aligned(o.local1, 16) && aligned(o.local2, 16) && (!p.cache || aligned(p.cache, 16));
+        l.rec = off; off += al(n * mc * 48);
+        l.h_meta = hoff; hoff += al(l.meta);
+        l.h_cache = hoff; hoff += p.cache ? al(n * sizeof(rp3dg_lastframe)) : 0;
+        l.h_rec = 0;
+        l.spec = false;
+        l.expect = 0;
+        if (ctx->last_pairs[b] == p.n && ctx->last_records[b])
+            l.expect = uint32_t(std::min<size_t>(size_t(ctx->last_records[b]) + ctx->last_records[b] / 8 + 64, n * mc));
+        l.h_spec = hspec;
+        hspec += al(size_t(l.expect) * 48);
     }
     cudaSetDevice(ctx->device);
     int rc = grow(ctx, &ctx->d_istage, &ctx->cap_istage, std::max<size_t>(off, 256), "cudaMalloc(narrow-phase input)");
+    if (!rc) rc = grow_pinned(ctx, &ctx->h_imeta, &ctx->cap_imeta, std::max<size_t>(hoff, 256), "cudaMallocHost(narrow-phase results)");
+    if (!rc && hspec)
+        rc = grow_pinned(ctx, &ctx->h_ispec, &ctx->cap_ispec, hspec, "cudaMallocHost(narrow-phase contacts)");
     if (rc) return rc;
     cudaError_t e = cudaSuccess;
     if (!ctx->s_up) e = cudaStreamCreateWithFlags(&ctx->s_up, cudaStreamNonBlocking);
     if (e == cudaSuccess && !ctx->s_pub) e = cudaStreamCreateWithFlags(&ctx->s_pub, cudaStreamNonBlocking);
-    while (e == cudaSuccess && ctx->events.size() < 2 * size_t(nb)) {
+    if (e == cudaSuccess && !ctx->s_rec) e = cudaStreamCreateWithFlags(&ctx->s_rec, cudaStreamNonBlocking);
+    while (e == cudaSuccess && ctx->events.size() < 4 * size_t(nb)) {
         cudaEvent_t ev;
         e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
         if (e == cudaSuccess) ctx->events.push_back(ev);
     }
     if (e != cudaSuccess) return cuda_fail(ctx, e, "narrow-phase input streams");
     char* base = static_cast<char*>(ctx->d_istage);
-    // the batches one after the other: upload (s_up), kernels (context
-    // stream), results (s_pub); each stream waits on the stage before it.
+    char* hmeta = static_cast<char*>(ctx->h_imeta);
+    cudaEvent_t* ev_up = ctx->events.data();
+    cudaEvent_t* ev_comp = ev_up + nb;
+    cudaEvent_t* ev_meta = ev_comp + nb;
+    cudaEvent_t* ev_rec = ev_meta + nb;
     // The batches are independent, so they go in order of decreasing
     // estimated kernel time: the long polyhedron batches compute while the
     // others upload.
@@ -1375,6 +1406,10 @@ int rp3dg_narrowphase_input_host(rp3dg_ctx* ctx, uint32_t nb, const int32_t* alg
         return c;
     };
     std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return cost(x) > cost(y); });
+    // 1. every batch: upload (s_up), kernels and the packing of its contacts
+    // (context stream), its flags / counts / group starts / record count and
+    // cache to the host (s_pub); each stream waits on the stage before it
+    uint32_t queued = 0;
     for (uint32_t ob = 0; ob < nb && rc == 0 && e == cudaSuccess; ob++) {
         const uint32_t b = order[ob];
         const rp3dg_pair_batch& p = P[b];
@@ -1390,8 +1425,8 @@ int rp3dg_narrowphase_input_host(rp3dg_ctx* ctx, uint32_t nb, const int32_t* alg
         up(l.p2, p.pos2, n * 16); up(l.r2, p.rot2, n * 16);
         up(l.rep, p.report_contacts, n);
         up(l.cache, p.cache, n * sizeof(rp3dg_lastframe));
-        if (e == cudaSuccess) e = cudaEventRecord(ctx->events[2 * b], ctx->s_up);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->events[2 * b], 0);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_up[b], ctx->s_up);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ev_up[b], 0);
         if (e != cudaSuccess) break;
         rp3dg_pair_batch dp;
         dp.n = p.n;
@@ -1412,55 +1447,135 @@ int rp3dg_narrowphase_input_host(rp3dg_ctx* ctx, uint32_t nb, const int32_t* alg
         dout.max_contacts = o.max_contacts;
         rc = rp3dg_narrowphase_device(ctx, algos[b], &dp, &dout, clip);
         if (rc) break;
-        e = cudaEventRecord(ctx->events[2 * b + 1], ctx->stream);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->s_pub, ctx->events[2 * b + 1], 0);
-        if (e != cudaSuccess) break;
-        if (l.pub) {
-            rp3dg::PublishArgs pa;
-            pa.n = p.n;
-            pa.d_col = dout.is_colliding; pa.d_nb = dout.nb_contacts;
-            pa.d_nd = reinterpret_cast<const float4*>(dout.normal_depth);
-            pa.d_l1 = reinterpret_cast<const float4*>(dout.local1);
-            pa.d_l2 = reinterpret_cast<const float4*>(dout.local2);
-            pa.d_cache = dp.cache;
-            pa.h_col = o.is_colliding; pa.h_nb = o.nb_contacts;
-            pa.h_nd = reinterpret_cast<float4*>(o.normal_depth);
-            pa.h_l1 = reinterpret_cast<float4*>(o.local1);
-            pa.h_l2 = reinterpret_cast<float4*>(o.local2);
-            pa.h_cache = p.cache;
-            e = rp3dg::launch_publish_contacts(pa, ctx->s_pub);
-            ctx->launches++;
-        } else {
-            e = cudaMemcpyAsync(o.is_colliding, base + l.col, n, cudaMemcpyDeviceToHost, ctx->s_pub);
-            if (e == cudaSuccess) e = cudaMemcpyAsync(o.nb_contacts, base + l.nbc, n, cudaMemcpyDeviceToHost, ctx->s_pub);
-            if (e == cudaSuccess && p.cache)
-                e = cudaMemcpyAsync(p.cache, base + l.cache, n * sizeof(rp3dg_lastframe), cudaMemcpyDeviceToHost,
-                                    ctx->s_pub);
+        rp3dg::CompactArgs ca;
+        ca.n = p.n;
+        ca.nb = dout.nb_contacts;
+        ca.nd = reinterpret_cast<const float4*>(dout.normal_depth);
+        ca.l1 = reinterpret_cast<const float4*>(dout.local1);
+        ca.l2 = reinterpret_cast<const float4*>(dout.local2);
+        ca.records = reinterpret_cast<float4*>(base + l.rec);
+        ca.warp_start = reinterpret_cast<uint32_t*>(base + l.ws);
+        ca.counter = reinterpret_cast<uint32_t*>(base + l.cnt);
+        e = cudaMemsetAsync(ca.counter, 0, 4, ctx->stream);
+        if (e == cudaSuccess) e = rp3dg::launch_compact_contacts(ca, ctx->stream);
+        ctx->launches++;
+        if (e == cudaSuccess) e = cudaEventRecord(ev_comp[b], ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->s_pub, ev_comp[b], 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hmeta + l.h_meta, base + l.col, l.meta, cudaMemcpyDeviceToHost, ctx->s_pub);
+        if (e == cudaSuccess && p.cache)
+            e = cudaMemcpyAsync(hmeta + l.h_cache, base + l.cache, n * sizeof(rp3dg_lastframe), cudaMemcpyDeviceToHost,
+                                ctx->s_pub);
+        if (e == cudaSuccess && l.expect)
+            e = cudaMemcpyAsync(static_cast<char*>(ctx->h_ispec) + l.h_spec, base + l.rec, size_t(l.expect) * 48,
+                                cudaMemcpyDeviceToHost, ctx->s_pub);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_meta[b], ctx->s_pub);
+        queued = ob + 1;
+    }
+    // 2. as each batch's count arrives: its records to the host (s_rec), and
+    // the batches whose records are in scattered into the caller's arrays on
+    // the host threads while the later batches are still on the GPU
+    auto scatter = [&](uint32_t b) {
+        const rp3dg_pair_batch& p = P[b];
+        const rp3dg_contact_batch& o = O[b];
+        const Lay& l = L[b];
+        const size_t n = p.n;
+        const uint8_t* col = reinterpret_cast<const uint8_t*>(hmeta + l.h_meta);
+        const uint8_t* cnt = col + (l.nbc - l.col);
+        const uint32_t* ws = reinterpret_cast<const uint32_t*>(col + (l.ws - l.col));
+        // the caller's arrays need only 4-byte alignment: plain struct copies
+        const rp3dg_float4* rec = reinterpret_cast<const rp3dg_float4*>(
+            l.spec ? static_cast<char*>(ctx->h_ispec) + l.h_spec : static_cast<char*>(ctx->h_irec) + l.h_rec);
+        std::memcpy(o.is_colliding, col, n);
+        std::memcpy(o.nb_contacts, cnt, n);
+        if (p.cache) std::memcpy(p.cache, hmeta + l.h_cache, n * sizeof(rp3dg_lastframe));
+        rp3dg_float4* nd = o.normal_depth;
+        rp3dg_float4* l1 = o.local1;
+        rp3dg_float4* l2 = o.local2;
+        const long groups = long(l.groups);
+#pragma omp parallel for schedule(static) if (groups >= 2048)
+        for (long g = 0; g < groups; g++) {
+            size_t r = ws[g];
+            const size_t i1 = std::min(n, size_t(g + 1) * 32);
+            for (size_t i = size_t(g) * 32; i < i1; i++)
+                for (uint32_t k = 0; k < cnt[i]; k++, r++) {
+                    const size_t at = size_t(k) * n + i;
+                    nd[at] = rec[3 * r];
+                    l1[at] = rec[3 * r + 1];
+                    l2[at] = rec[3 * r + 2];
+                }
         }
+    };
+    std::vector<uint32_t> pending;   // records on their way, in order
+    size_t rec_used = 0;
+    for (uint32_t ob = 0; ob < queued && rc == 0 && e == cudaSuccess; ob++) {
+        const uint32_t b = order[ob];
+        if (P[b].n == 0) continue;
+        Lay& l = L[b];
+        e = cudaEventSynchronize(ev_meta[b]);
+        if (e != cudaSuccess) break;
+        uint32_t total = 0;
+        std::memcpy(&total, hmeta + l.h_meta + (l.cnt - l.col), 4);
+        if (size_t(total) > size_t(P[b].n) * O[b].max_contacts) {
+            rc = fail(ctx, RP3DG_ECUDA, "narrow-phase contact count out of range");
+            break;
+        }
+        ctx->last_pairs[b] = P[b].n;
+        ctx->last_records[b] = total;
+        l.spec = total <= l.expect;
+        if (l.spec) {
+            // the records came back with the flags
+            scatter(b);
+            continue;
+        }
+        const size_t need = al(size_t(total) * 48);
+        if (rec_used + need > ctx->cap_irec) {
+            // the pending batches are finished first; then the staging grows
+            for (uint32_t q : pending) {
+                e = cudaEventSynchronize(ev_rec[q]);
+                if (e != cudaSuccess) break;
+                scatter(q);
+            }
+            pending.clear();
+            rec_used = 0;
+            if (e != cudaSuccess) break;
+            rc = grow_pinned(ctx, &ctx->h_irec, &ctx->cap_irec, std::max<size_t>(need, 256),
+                             "cudaMallocHost(narrow-phase contacts)");
+            if (rc) break;
+        }
+        l.h_rec = rec_used;
+        rec_used += need;
+        if (total)
+            e = cudaMemcpyAsync(static_cast<char*>(ctx->h_irec) + l.h_rec, base + l.rec, size_t(total) * 48,
+                                cudaMemcpyDeviceToHost, ctx->s_rec);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_rec[b], ctx->s_rec);
+        if (e != cudaSuccess) break;
+        while (!pending.empty()) {
+            const cudaError_t q = cudaEventQuery(ev_rec[pending.front()]);
+            if (q == cudaErrorNotReady) {
+                (void)cudaGetLastError();   // not an error: the copy is still running
+                break;
+            }
+            if (q != cudaSuccess) {
+                e = q;
+                break;
+            }
+            scatter(pending.front());
+            pending.erase(pending.begin());
+        }
+        pending.push_back(b);
+    }
+    for (uint32_t q : pending) {
+        if (rc || e != cudaSuccess) break;
+        e = cudaEventSynchronize(ev_rec[q]);
+        if (e == cudaSuccess) scatter(q);
     }
     // every stream drained before returning (also after an error)
     const cudaError_t e1 = cudaStreamSynchronize(ctx->s_up);
     const cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
     const cudaError_t e3 = cudaStreamSynchronize(ctx->s_pub);
+    const cudaError_t e4 = cudaStreamSynchronize(ctx->s_rec);
     if (rc) return rc;
-    if (e == cudaSuccess) e = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "narrow-phase input (host arrays)");
-    // the batches whose outputs are pageable: their used contact slots
-    for (uint32_t b = 0; b < nb; b++) {
-        const rp3dg_pair_batch& p = P[b];
-        const rp3dg_contact_batch& o = O[b];
-        if (p.n == 0 || L[b].pub) continue;
-        const size_t n = p.n;
-        uint32_t used = 0;
-        for (size_t i = 0; i < n; i++) used = o.nb_contacts[i] > used ? o.nb_contacts[i] : used;
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(o.normal_depth, base + L[b].nd, n * used * 16, cudaMemcpyDeviceToHost, ctx->stream);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(o.local1, base + L[b].l1, n * used * 16, cudaMemcpyDeviceToHost, ctx->stream);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(o.local2, base + L[b].l2, n * used * 16, cudaMemcpyDeviceToHost, ctx->stream);
-    }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : (e3 != cudaSuccess ? e3 : e4));
     if (e == cudaSuccess) e = cudaGetLastError();
     return e == cudaSuccess ? 0 : cuda_fail(ctx, e, "narrow-phase input (host arrays)");
 }
@@ -1716,6 +1831,18 @@ int grow(rp3dg_ctx* ctx, void** buf, size_t* cap, size_t need, const char* what)
     cudaFree(*buf);
     *buf = nullptr;
     cudaError_t e = cudaMalloc(buf, n);
+    if (e != cudaSuccess) { *cap = 0; *buf = nullptr; return cuda_fail(ctx, e, what); }
+    *cap = n;
+    return 0;
+}
+
+// The same for page-locked host memory (old contents are not kept).
+int grow_pinned(rp3dg_ctx* ctx, void** buf, size_t* cap, size_t need, const char* what) {
+    if (need <= *cap) return 0;
+    const size_t n = std::max(need, 2 * *cap);
+    cudaFreeHost(*buf);
+    *buf = nullptr;
+    cudaError_t e = cudaMallocHost(buf, n);
     if (e != cudaSuccess) { *cap = 0; *buf = nullptr; return cuda_fail(ctx, e, what); }
     *cap = n;
     return 0;

@@ -199,10 +199,13 @@ def test_grazing_capsule_clip_matches_oracle(ctx, port_hulls):
 
 @pytest.mark.parametrize("pinned", [False, True])
 def test_narrowphase_input_matches_per_batch_calls(ctx, pinned):
-    """rp3dg_narrowphase_input_host (all batches overlapped, results written
-    straight into page-locked outputs) gives, batch by batch, the results and
-    caches of rp3dg_narrowphase_host, on two frames (fresh caches, then moved
-    poses with the first frame's caches)."""
+    """rp3dg_narrowphase_input_host (all batches overlapped, contacts packed
+    on the device and scattered into the outputs on the host) gives, batch by
+    batch, the results and caches of rp3dg_narrowphase_host, on three frames
+    (fresh caches, then moved poses with the previous frame's caches): the
+    first call copies each batch's contacts back once their count is known,
+    the later ones copy the expected number with the flags and fall back to
+    the first way for a batch with more contacts than expected."""
     import torch
     sc = scenes.narrowphase_scene(total_pairs=7 * 6000, seed=321, hull=edgecases.load_hull())
     ctx.set_shapes(sc.shapes)
@@ -225,7 +228,7 @@ def test_narrowphase_input_matches_per_batch_calls(ctx, pinned):
     for name, (algo, pairs) in sc.batches.items():
         pairs.cache = A.fresh_cache(pairs.n)
         frames.append((name, algo, pairs))
-    for frame in range(2):
+    for frame in range(3):
         ref, batches = [], []
         for name, algo, pairs in frames:
             pr = pairs.slice(0, pairs.n)
