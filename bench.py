@@ -698,8 +698,57 @@ def many_worlds_section(ctx, args, with_cpu, rank=0, world=1):
                                  "whose last bit differs between CUDA and the host C library, so worlds whose limits "
                                  "engage are tolerance-level (worlds without limits are bit-identical: "
                                  "tests/test_world_gpu.py)"}
+    digest = [np.asarray(g.bodies(k)[0], np.float64).sum() for k in range(0, hi - lo, 97)]
     g.close()
+    if world == 1:
+        try:
+            out["two_groups_in_flight"] = _two_groups(raw_all, dt, warm, timed, digest)
+        except Exception as e:
+            out["two_groups_in_flight"] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
     return out
+
+
+def _two_groups(raw, dt, warm, timed, digest):
+    """The same worlds as two groups (halves balanced by body count), each on
+    its own context and half the host threads, stepped from two host threads
+    at once: one group's host bookkeeping runs while the other's kernels do.
+    Same steps (autotuning, warm-up, timed, 5 more) as the single group, whose
+    sampled final positions they must reproduce."""
+    import threading
+    from reactphysics3d_b200 import engine, shard
+    n = len(raw)
+    blocks = [shard.rank_block([len(s_.bodies) for s_ in raw], r, 2) for r in range(2)]
+    threads = max(1, (os.cpu_count() or 2) // 2)
+    parts = []
+    for lo, hi in blocks:
+        c = engine.Context(0)
+        shapes, scs = scenes.merge_shapes(raw[lo:hi])
+        g = engine.WorldGroup(c, scs, shapes, threads=threads)
+        g.autotune(rounds=2)
+        parts.append((c, g, lo, hi))
+
+    def run(steps):
+        ths = [threading.Thread(target=g.update, args=(dt, steps)) for _, g, _, _ in parts]
+        t0 = time.perf_counter()
+        [t_.start() for t_ in ths]
+        [t_.join() for t_ in ths]
+        return time.perf_counter() - t0
+    run(warm)
+    sec = run(timed)
+    run(5)
+    got = []
+    for k in range(0, n, 97):
+        for _, g, lo, hi in parts:
+            if lo <= k < hi:
+                got.append(np.asarray(g.bodies(k - lo)[0], np.float64).sum())
+    for c, g, _, _ in parts:
+        g.close()
+        c.close()
+    return {"world_steps_per_s": round(n * timed / sec, 1), "ms_per_step": round(1e3 * sec / timed, 3),
+            "groups": 2, "host_threads_per_group": threads,
+            "same_states_as_one_group": bool(np.array_equal(np.asarray(got), np.asarray(digest))),
+            "note": "not a library mode: two rp3dg_world_update calls in flight from two host threads, one "
+                    "context each; the timed region is the same 60 steps of all worlds"}
 
 
 def terrain_section(ctx, args, with_cpu):
