@@ -561,13 +561,18 @@ struct ColliderH {
     uint16_t category = 1, mask = 0xffff;
     bool trigger = false;  // Collider::setIsTrigger: not a simulation collider
     std::vector<uint64_t> pairs;  // ColliderComponents::mOverlappingPairs
+    uint64_t moved_at = 0;        // the world clock when it last joined the moved set
 };
 struct PairH {
     uint64_t id = 0;
     int bp1 = -1, bp2 = -1;
     int c1 = -1, c2 = -1;  // collider ids
     int algo = 0;
-    bool need_test = false, coll_prev = false, coll_curr = false, enabled = true;
+    // OverlappingPair::mNeedToTestOverlap, kept as the world clock's value
+    // when it was last cleared: it is set while a collider of the pair has
+    // moved since then (need_test below)
+    uint64_t reset_at = 0;
+    bool coll_prev = false, coll_curr = false, enabled = true;
     int cache = -1;  // slot of its LastFrameCollisionInfo in the device pool
     // convex vs concave pairs (ConcaveOverlappingPair): which shape is convex,
     // and the per-triangle records of the last step that tested the pair
@@ -803,6 +808,10 @@ struct WorldH {
     rp3dg::order::Comps bcomp, ccomp;
     rp3dg::order::Tree tree;
     rp3dg::order::IdSet moved;
+    // askForBroadPhaseCollisionCheck marks every pair of a moved collider for
+    // the overlap test; instead of visiting them, each mark and each clear
+    // takes the next value of this clock (ColliderH::moved_at, PairH::reset_at)
+    uint64_t clock = 0;
     std::vector<int> bp_to_collider;
     // overlapping pairs (OverlappingPairs::mConvexPairs / mDisabledConvexPairs,
     // mConcavePairs / mDisabledConcavePairs)
@@ -1115,6 +1124,7 @@ void add_pair(Group* g, WorldH& w, int c1, int c2) {
     const uint32_t b1 = uint32_t(C1.bp), b2 = uint32_t(C2.bp);
     PairH p;
     p.id = pair_number(std::max(b1, b2), std::min(b1, b2));
+    p.reset_at = ++w.clock;
     p.bp1 = int(b1);
     p.bp2 = int(b2);
     p.c1 = c1;
@@ -1180,7 +1190,7 @@ void disable_pair(Group* g, WorldH& w, uint64_t id) {
         const uint32_t idx = ic->second;
         PairH np = w.concave[idx];
         np.enabled = false;
-        np.need_test = false;
+        np.reset_at = ++w.clock;
         np.rec_valid = false;
         w.map_concave_dis[id] = uint32_t(w.concave_dis.size());
         w.concave_dis.push_back(np);
@@ -1190,7 +1200,7 @@ void disable_pair(Group* g, WorldH& w, uint64_t id) {
     const uint32_t idx = it->second;
     PairH np = w.pairs[idx];
     np.enabled = false;
-    np.need_test = false;
+    np.reset_at = ++w.clock;
     w.free_cache.push_back(np.cache);
     np.cache = alloc_cache(g, w);
     w.map_disabled[id] = uint32_t(w.disabled.size());
@@ -1206,7 +1216,7 @@ void enable_pair(Group* g, WorldH& w, uint64_t id) {
         const uint32_t idx = ic->second;
         PairH np = w.concave_dis[idx];
         np.enabled = true;
-        np.need_test = false;
+        np.reset_at = ++w.clock;
         np.rec_valid = false;
         w.map_concave[id] = uint32_t(w.concave.size());
         w.concave.push_back(np);
@@ -1216,7 +1226,7 @@ void enable_pair(Group* g, WorldH& w, uint64_t id) {
     const uint32_t idx = it->second;
     PairH np = w.disabled[idx];
     np.enabled = true;
-    np.need_test = false;
+    np.reset_at = ++w.clock;
     w.free_cache.push_back(np.cache);
     np.cache = alloc_cache(g, w);
     w.map_pairs[id] = uint32_t(w.pairs.size());
@@ -1227,10 +1237,12 @@ void enable_pair(Group* g, WorldH& w, uint64_t id) {
 // BroadPhaseSystem::addMovedCollider + notifyOverlappingPairsToTestOverlap
 void add_moved(WorldH& w, int c) {
     w.moved.add(w.colliders[size_t(c)].bp);
-    for (uint64_t id : w.colliders[size_t(c)].pairs) {
-        PairH* p = find_pair(w, id);
-        if (p) p->need_test = true;
-    }
+    w.colliders[size_t(c)].moved_at = ++w.clock;
+}
+
+// OverlappingPair::needToTestOverlap
+bool need_test(const WorldH& w, const PairH& p) {
+    return w.colliders[size_t(p.c1)].moved_at > p.reset_at || w.colliders[size_t(p.c2)].moved_at > p.reset_at;
 }
 
 // PhysicsWorld::setBodyDisabled (PhysicsWorld.cpp:168-186)
@@ -1391,7 +1403,7 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
                 if ((C1.mask & C2.category) != 0 && (C1.category & C2.mask) != 0 && (C1.convex || C2.convex))
                     add_pair(g, w, c1, c2);
             } else {
-                p->need_test = false;
+                p->reset_at = ++w.clock;
             }
         }
     }
@@ -1401,9 +1413,9 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
     w.lost.clear();
     for (uint64_t i = 0; i < w.pairs.size(); i++) {
         PairH& p = w.pairs[i];
-        if (!p.need_test) continue;
+        if (!need_test(w, p)) continue;
         if (rp3dg::order::overlap(w.tree.nodes[size_t(p.bp1)].box, w.tree.nodes[size_t(p.bp2)].box)) {
-            p.need_test = false;
+            p.reset_at = ++w.clock;
         } else {
             if (p.coll_prev) add_lost(w, p);
             remove_pair(w, uint32_t(i));
@@ -1412,9 +1424,9 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
     }
     for (uint64_t i = 0; i < w.concave.size(); i++) {
         PairH& p = w.concave[i];
-        if (!p.need_test) continue;
+        if (!need_test(w, p)) continue;
         if (rp3dg::order::overlap(w.tree.nodes[size_t(p.bp1)].box, w.tree.nodes[size_t(p.bp2)].box)) {
-            p.need_test = false;
+            p.reset_at = ++w.clock;
         } else {
             if (p.coll_prev) add_lost(w, p);
             remove_concave_pair(w, uint32_t(i));

@@ -284,6 +284,36 @@ def test_device_trees_give_identical_results(ctx):
         g.close()
 
 
+def test_groups_on_two_contexts_step_concurrently(ctx):
+    """Two world groups, each on its own context, stepped at the same time
+    from two host threads (the library's host bookkeeping and its streams
+    are per context), end bit-identical to one group holding all the
+    worlds."""
+    import threading
+    raw = scenes.many_worlds(64, seed=29, min_bodies=20, max_bodies=120, ragdolls=(1, 2), merge=False)
+    shapes, scs = scenes.merge_shapes(raw)
+    one = engine.WorldGroup(ctx, scs, shapes, threads=4)
+    parts = []
+    for lo, hi in ((0, 30), (30, 64)):
+        c = engine.Context(0)
+        sh, sc = scenes.merge_shapes(raw[lo:hi])
+        parts.append((c, engine.WorldGroup(c, sc, sh, threads=2), lo))
+    dt = float(worldio.DT)
+    ths = [threading.Thread(target=g.update, args=(dt, 80)) for _, g, _ in parts]
+    [t.start() for t in ths]
+    one.update(dt, 80)
+    [t.join() for t in ths]
+    for k in range(64):
+        c, g, lo = parts[0] if k < 30 else parts[1]
+        for x, y in zip(one.bodies(k), g.bodies(k - lo)):
+            assert np.array_equal(x, y), k
+        assert np.array_equal(one.pairs(k), g.pairs(k - lo)), k
+    one.close()
+    for c, g, _ in parts:
+        g.close()
+        c.close()
+
+
 @pytest.mark.skipif(not (reflib.have_ref("f32") and reflib.have_ref("f64")), reason="reference engine not built")
 def test_ragdolls_with_limits_stay_within_tolerance(ctx):
     """Cone and hinge limits go through acos / atan2, whose last bit differs
