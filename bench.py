@@ -222,7 +222,8 @@ def run_ours(args):
                 setattr(ho, f, torch.from_numpy(getattr(ho, f)).pin_memory().numpy())
             pinned[nm] = (pp, ho)
         # the whole narrow-phase input per call (testNarrowPhaseCollision):
-        # the batches overlap, results are written into the pinned outputs
+        # the batches overlap, the contacts come back packed and the library's
+        # host threads write them into the outputs
         step_batches = [(algos[nm], pinned[nm][0], pinned[nm][1]) for nm in names]
         for _ in range(max(1, args.warmup)):
             ctx.narrowphase_input_host(step_batches)
