@@ -688,76 +688,8 @@ struct FlatMap {
     }
 };
 
-// Pair id -> index in its pair array (OverlappingPairs' mMapConvexPairIdToPairIndex
-// and the three other maps; only looked up, never iterated, so its order is
-// free): open addressing with linear probing, deletion by backward shift,
-// at most half full.  find / end / operator[] / erase as std::unordered_map.
-struct PairMap {
-    static constexpr uint64_t EMPTY = ~uint64_t(0);
-    struct Entry {
-        uint64_t first = EMPTY;
-        uint32_t second = 0;
-    };
-    std::vector<Entry> slots;
-    uint32_t mask = 0;
-    size_t n = 0;
+using rp3dg::order::PairMap;
 
-    static uint32_t hash(uint64_t k) {
-        k ^= k >> 33;
-        k *= 0xff51afd7ed558ccdull;
-        k ^= k >> 33;
-        return uint32_t(k);
-    }
-    Entry* end() const { return nullptr; }
-    bool empty() const { return n == 0; }
-    Entry* find(uint64_t k) {
-        if (!n) return nullptr;
-        for (uint32_t h = hash(k) & mask;; h = (h + 1) & mask) {
-            if (slots[h].first == k) return &slots[h];
-            if (slots[h].first == EMPTY) return nullptr;
-        }
-    }
-    void rehash(size_t cap) {
-        std::vector<Entry> old;
-        old.swap(slots);
-        slots.assign(cap, Entry());
-        mask = uint32_t(cap - 1);
-        for (const Entry& e : old)
-            if (e.first != EMPTY) {
-                uint32_t h = hash(e.first) & mask;
-                while (slots[h].first != EMPTY) h = (h + 1) & mask;
-                slots[h] = e;
-            }
-    }
-    uint32_t& operator[](uint64_t k) {
-        if (2 * (n + 1) > slots.size()) rehash(std::max<size_t>(16, 2 * slots.size()));
-        uint32_t h = hash(k) & mask;
-        while (slots[h].first != EMPTY && slots[h].first != k) h = (h + 1) & mask;
-        if (slots[h].first == EMPTY) {
-            slots[h].first = k;
-            slots[h].second = 0;
-            n++;
-        }
-        return slots[h].second;
-    }
-    void erase(uint64_t k) {
-        Entry* e = find(k);
-        if (!e) return;
-        uint32_t i = uint32_t(e - slots.data()), j = i;
-        for (;;) {
-            j = (j + 1) & mask;
-            if (slots[j].first == EMPTY) break;
-            const uint32_t home = hash(slots[j].first) & mask;
-            // the entry at j stays where it is if its home lies cyclically in (i, j]
-            const bool stays = i <= j ? (i < home && home <= j) : (i < home || home <= j);
-            if (stays) continue;
-            slots[i] = slots[j];
-            i = j;
-        }
-        slots[i] = Entry();
-        n--;
-    }
-};
 
 inline uint64_t body_pair_key(int a, int b) {
     return (uint64_t(uint32_t(std::min(a, b))) << 32) | uint32_t(std::max(a, b));

@@ -15,6 +15,8 @@
 //          buckets, identity hash, new entries at the head of their bucket
 //          chain, rehash on growth, iteration bucket by bucket (:119-170,
 //          :263-341, :380-420, :475-484, :571-600).
+//   PairMap  the id-to-index maps of OverlappingPairs (a flat hash table;
+//          lookups only, so its own order never shows).
 //   Comps  component order of Components (src/components/Components.cpp:
 //          67-193): enabled components first, additions and enable/disable
 //          by moving or swapping with the first disabled / last enabled one.
@@ -28,6 +30,7 @@
 // fixed device span (DevTree, one world's tree in a world group's device
 // pool, updated by one GPU thread per world).
 #pragma once
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -432,6 +435,77 @@ struct IdSet {
         out.clear();
         for (uint64_t i = 0; i < hash_size; i++)
             for (uint64_t e = buckets[i]; e != INVALID; e = next[e]) out.push_back(entries[e]);
+    }
+};
+
+// Pair id -> index in its pair array (OverlappingPairs' mMapConvexPairIdToPairIndex
+// and the three other maps; only looked up, never iterated, so its order is
+// free): open addressing with linear probing, deletion by backward shift,
+// at most half full.  find / end / operator[] / erase as std::unordered_map.
+struct PairMap {
+    static constexpr uint64_t EMPTY = ~uint64_t(0);
+    struct Entry {
+        uint64_t first = EMPTY;
+        uint32_t second = 0;
+    };
+    std::vector<Entry> slots;
+    uint32_t mask = 0;
+    size_t n = 0;
+
+    static uint32_t hash(uint64_t k) {
+        k ^= k >> 33;
+        k *= 0xff51afd7ed558ccdull;
+        k ^= k >> 33;
+        return uint32_t(k);
+    }
+    Entry* end() const { return nullptr; }
+    bool empty() const { return n == 0; }
+    Entry* find(uint64_t k) {
+        if (!n) return nullptr;
+        for (uint32_t h = hash(k) & mask;; h = (h + 1) & mask) {
+            if (slots[h].first == k) return &slots[h];
+            if (slots[h].first == EMPTY) return nullptr;
+        }
+    }
+    void rehash(size_t cap) {
+        std::vector<Entry> old;
+        old.swap(slots);
+        slots.assign(cap, Entry());
+        mask = uint32_t(cap - 1);
+        for (const Entry& e : old)
+            if (e.first != EMPTY) {
+                uint32_t h = hash(e.first) & mask;
+                while (slots[h].first != EMPTY) h = (h + 1) & mask;
+                slots[h] = e;
+            }
+    }
+    uint32_t& operator[](uint64_t k) {
+        if (2 * (n + 1) > slots.size()) rehash(std::max<size_t>(16, 2 * slots.size()));
+        uint32_t h = hash(k) & mask;
+        while (slots[h].first != EMPTY && slots[h].first != k) h = (h + 1) & mask;
+        if (slots[h].first == EMPTY) {
+            slots[h].first = k;
+            slots[h].second = 0;
+            n++;
+        }
+        return slots[h].second;
+    }
+    void erase(uint64_t k) {
+        Entry* e = find(k);
+        if (!e) return;
+        uint32_t i = uint32_t(e - slots.data()), j = i;
+        for (;;) {
+            j = (j + 1) & mask;
+            if (slots[j].first == EMPTY) break;
+            const uint32_t home = hash(slots[j].first) & mask;
+            // the entry at j stays where it is if its home lies cyclically in (i, j]
+            const bool stays = i <= j ? (i < home && home <= j) : (i < home || home <= j);
+            if (stays) continue;
+            slots[i] = slots[j];
+            i = j;
+        }
+        slots[i] = Entry();
+        n--;
     }
 };
 
