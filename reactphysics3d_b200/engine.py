@@ -370,14 +370,29 @@ class Context:
         """testNarrowPhaseCollision over a whole NarrowPhaseInput: `batches` is
         a list of (algorithm, HostPairs, HostContacts or None); the batches
         run overlapped (rp3dg_narrowphase_input_host); returns the outputs."""
+        return self.narrowphase_input_call(batches, clip)()
+
+    def narrowphase_input_call(self, batches, clip=True):
+        """The same call prepared once for fixed host arrays (their contents
+        may change between runs): returns a function that makes one
+        rp3dg_narrowphase_input_host call and returns the outputs, without
+        rebuilding the batch descriptors each time."""
         outs = [o if o is not None else A.HostContacts(p.n) for (_, p, o) in batches]
         n = len(batches)
         algos = (C.c_int32 * n)(*[int(a) for (a, _, _) in batches])
         pbs = (A.PairBatch * n)(*[p.struct() for (_, p, _) in batches])
         cbs = (A.ContactBatch * n)(*[o.struct() for o in outs])
-        self._check(self.lib.rp3dg_narrowphase_input_host(self.h, n, C.addressof(algos), C.addressof(pbs),
-                                                          C.addressof(cbs), int(clip)))
-        return outs
+        fn, h, args = self.lib.rp3dg_narrowphase_input_host, self.h, (C.addressof(algos), C.addressof(pbs),
+                                                                       C.addressof(cbs), int(clip))
+        keep = (algos, pbs, cbs, batches)
+
+        def run():
+            rc = fn(h, n, *args)
+            if rc != 0:
+                self._check(rc)
+            return outs
+        run.keep = keep
+        return run
 
     def narrowphase_manifolds_host(self, algo, pairs, out=None, clip=True, want_kept=True):
         """Narrow phase + manifold reduction on host arrays; returns (out, kept)."""
