@@ -801,6 +801,11 @@ struct WorldH {
     std::vector<std::vector<int>> q_buf;
     std::vector<int4> q_pos;
     std::vector<int32_t> q_shapes;             // this step's moved colliders in the moved set's order
+    // one large world's candidate pairs: first candidate of each moved
+    // collider, class (0 filtered, 1 existing, 2 new) and existing pair
+    std::vector<size_t> c_start;
+    std::vector<uint8_t> c_code;
+    std::vector<PairH*> c_found;
     uint32_t q_off = 0;                        // their first query in the group's device query list
     // device tree of a world group: whether the host tree's inner nodes are
     // older than the device's (the host keeps the leaves' boxes current)
@@ -1308,34 +1313,90 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
             w.q_pos[size_t(i)] = make_int4(t, int(o), int(buf.size() - o), 0);
         }
     }
-    for (size_t i = 0; i < shapes.size(); i++) {
-        const int32_t s = shapes[i];
-        const int* leaves;
-        int nleaf;
+    auto leaves_of = [&](size_t i, const int** leaves, int* nleaf) {
         if (gpu) {
             const int2 tp = g->h_tpos[qbase + i];
-            leaves = g->h_tleaves + tp.x;
-            nleaf = tp.y;
+            *leaves = g->h_tleaves + tp.x;
+            *nleaf = tp.y;
         } else {
             const int4 qp = w.q_pos[i];
-            leaves = w.q_buf[size_t(qp.x)].data() + qp.y;
-            nleaf = qp.z;
+            *leaves = w.q_buf[size_t(qp.x)].data() + qp.y;
+            *nleaf = qp.z;
         }
-        for (int li = 0; li < nleaf; li++) {
-            const int leaf = leaves[li];
-            if (leaf == s) continue;
-            const int c1 = w.bp_to_collider[size_t(s)], c2 = w.bp_to_collider[size_t(leaf)];
-            const ColliderH &C1 = w.colliders[size_t(c1)], &C2 = w.colliders[size_t(c2)];
-            if (C1.body == C2.body) continue;
-            if (!w.nocollide.empty() && w.nocollide.find(body_pair_key(C1.body, C2.body)))
-                continue;
-            const uint64_t id = pair_number(uint32_t(std::max(s, leaf)), uint32_t(std::min(s, leaf)));
-            PairH* p = find_pair(w, id);
-            if (!p) {
-                if ((C1.mask & C2.category) != 0 && (C1.category & C2.mask) != 0 && (C1.convex || C2.convex))
-                    add_pair(g, w, c1, c2);
-            } else {
-                p->reset_at = ++w.clock;
+    };
+    // a candidate pair of the queries: 0 filtered out, 1 an existing pair, 2 new
+    auto classify = [&](int32_t s, int leaf, PairH** found) -> uint8_t {
+        if (leaf == s) return 0;
+        const int c1 = w.bp_to_collider[size_t(s)], c2 = w.bp_to_collider[size_t(leaf)];
+        const ColliderH &C1 = w.colliders[size_t(c1)], &C2 = w.colliders[size_t(c2)];
+        if (C1.body == C2.body) return 0;
+        if (!w.nocollide.empty() && w.nocollide.find(body_pair_key(C1.body, C2.body))) return 0;
+        *found = find_pair(w, pair_number(uint32_t(std::max(s, leaf)), uint32_t(std::min(s, leaf))));
+        return *found ? 1 : 2;
+    };
+    auto add_new = [&](int32_t s, int leaf) {
+        const uint64_t id = pair_number(uint32_t(std::max(s, leaf)), uint32_t(std::min(s, leaf)));
+        PairH* p = find_pair(w, id);
+        if (p) {
+            p->reset_at = ++w.clock;
+            return;
+        }
+        const int c1 = w.bp_to_collider[size_t(s)], c2 = w.bp_to_collider[size_t(leaf)];
+        const ColliderH &C1 = w.colliders[size_t(c1)], &C2 = w.colliders[size_t(c2)];
+        if ((C1.mask & C2.category) != 0 && (C1.category & C2.mask) != 0 && (C1.convex || C2.convex))
+            add_pair(g, w, c1, c2);
+    };
+    if (g->worlds.size() == 1 && g->nthreads > 1 && shapes.size() >= 256) {
+        // one large world: the candidates are classified on the group's
+        // threads (lookups only), the existing pairs' marks cleared (all
+        // with one clock value: every mark this clears is older), and only
+        // the new ones are added in the moved set's order, each looked up
+        // again so that a pair met twice is added once
+        size_t total = 0;
+        w.c_start.resize(shapes.size() + 1);
+        for (size_t i = 0; i < shapes.size(); i++) {
+            const int* lv;
+            int nl;
+            leaves_of(i, &lv, &nl);
+            w.c_start[i] = total;
+            total += size_t(nl);
+        }
+        w.c_start[shapes.size()] = total;
+        w.c_code.resize(total);
+        w.c_found.resize(total);
+#pragma omp parallel for schedule(dynamic, 64) num_threads(g->nthreads)
+        for (long i = 0; i < long(shapes.size()); i++) {
+            const int* lv;
+            int nl;
+            leaves_of(size_t(i), &lv, &nl);
+            const size_t o = w.c_start[size_t(i)];
+            for (int li = 0; li < nl; li++) {
+                PairH* f = nullptr;
+                w.c_code[o + size_t(li)] = classify(shapes[size_t(i)], lv[li], &f);
+                w.c_found[o + size_t(li)] = f;
+            }
+        }
+        const uint64_t stamp = ++w.clock;
+        for (size_t j = 0; j < total; j++)
+            if (w.c_code[j] == 1) w.c_found[j]->reset_at = stamp;
+        for (size_t i = 0; i < shapes.size(); i++) {
+            const int* lv;
+            int nl;
+            leaves_of(i, &lv, &nl);
+            const size_t o = w.c_start[i];
+            for (int li = 0; li < nl; li++)
+                if (w.c_code[o + size_t(li)] == 2) add_new(shapes[i], lv[li]);
+        }
+    } else {
+        for (size_t i = 0; i < shapes.size(); i++) {
+            const int* lv;
+            int nl;
+            leaves_of(i, &lv, &nl);
+            for (int li = 0; li < nl; li++) {
+                PairH* f = nullptr;
+                const uint8_t code = classify(shapes[i], lv[li], &f);
+                if (code == 1) f->reset_at = ++w.clock;
+                else if (code == 2) add_new(shapes[i], lv[li]);
             }
         }
     }
