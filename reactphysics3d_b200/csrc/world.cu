@@ -2657,14 +2657,17 @@ int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds
         g->tables_dirty = true;
     }
     // the narrow phase's step buffers sized up front for twice as many convex
-    // pairs as colliders: growing them later frees and maps hundreds of MB
+    // pairs as colliders (four times for a single world: a resting 100,000-
+    // body world has ~3.5): growing them later frees and maps hundreds of MB
     // (16 contact slots per pair), which stalls the step that does it
-    rc = ensure_items(g, 2 * size_t(g->NC) + 1024);
+    rc = ensure_items(g, (nworlds == 1 ? 4 : 2) * size_t(g->NC) + 1024);
     // and, for the same reason, the manifold staging, the island arrays and
-    // both contact buffers for as many manifolds as colliders (two points each)
+    // both contact buffers for twice as many manifolds as colliders (two
+    // points each: a resting 100,000-body world has ~1.25 manifolds and ~2
+    // points per collider)
     if (!rc) rc = ensure_manifold_staging(g, g->NC, g->NC / 2 + 64);
     if (!rc) rc = ensure_pool(g, 2 * size_t(g->NC) + 1024);
-    if (!rc && (g->cbuf[0].ensure(g->NC + 64, 2 * g->NC + 64) || g->cbuf[1].ensure(g->NC + 64, 2 * g->NC + 64)))
+    if (!rc && (g->cbuf[0].ensure(2 * g->NC + 64, 4 * g->NC + 64) || g->cbuf[1].ensure(2 * g->NC + 64, 4 * g->NC + 64)))
         rc = wfail(g, RP3DG_ENOMEM, "cudaMalloc(contacts)");
     // a group of small worlds keeps its trees on the device (one GPU thread
     // per world replays that world's reinsertions); one large world keeps its
