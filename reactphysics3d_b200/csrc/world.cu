@@ -284,6 +284,19 @@ __global__ void __launch_bounds__(128) world_setup(uint32_t nb, const float4* po
 
 // setIsSleeping(true): velocities, forces and torques of the listed rows set
 // to zero (RigidBody.cpp:1040-1046).
+// The velocity condition of the sleep test (updateSleepingBodies,
+// PhysicsWorld.cpp:889-893) for every body row: 1 when the squared linear or
+// angular speed is above its threshold (the host's float expressions), so
+// that the host reads one byte per body instead of both velocities.
+__global__ void __launch_bounds__(128) world_sleep_fast(uint32_t n, const float4* __restrict__ lv,
+                                                        const float4* __restrict__ av, float slv2, float sav2,
+                                                        uint8_t* __restrict__ fast) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 l = lv[i], a = av[i];
+    fast[i] = (l.x * l.x + l.y * l.y + l.z * l.z > slv2 || a.x * a.x + a.y * a.y + a.z * a.z > sav2) ? 1 : 0;
+}
+
 __global__ void __launch_bounds__(128) world_zero_rows(uint32_t n, const int32_t* rows, float4* lv, float4* av,
                                                        float4* force, float4* torque) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -755,7 +768,7 @@ struct WorldH {
     std::vector<ContactPairH> cpairs, prev_cpairs;
     std::vector<ContactPairH> lost;            // this step's lost contact pairs (mLostContactPairs)
     std::vector<int> isl_bodies;               // the islands' bodies, island after island
-    std::vector<float4> sleep_lv, sleep_av;    // the sleep test's velocities by body id (reused)
+    std::vector<uint8_t> sleep_fast;           // the sleep test's velocity condition by body id (reused)
     FlatMap prev_map;
     std::vector<uint32_t> island_order;  // mProcessContactPairsOrderIslands
     std::vector<IslandH> islands;
@@ -849,6 +862,8 @@ struct rp3dg_world {
     size_t cap_pool = 0;
     int32_t* d_small = nullptr;
     size_t cap_small = 0;
+    uint8_t* d_fast = nullptr;     // the sleep test's velocity condition by body row (world_sleep_fast)
+    size_t cap_fast = 0;
     bool tables_dirty = true;
     // pinned host copies of the per-row tables and the row permutations
     uint8_t *t_grav = nullptr, *t_ben = nullptr, *t_cen = nullptr;
@@ -1733,7 +1748,7 @@ void fill_manifolds(Group* g, WorldH& w) {
 // BroadPhaseSystem::updateColliders' reinsertions (enabled colliders in
 // component order) and PhysicsWorld::updateSleepingBodies (:871-926).
 void colliders_and_sleep(Group* g, WorldH& w, float dt, const uint8_t* h_moved, const float4* h_fmin,
-                         const float4* h_fmax, const float4* h_lv, const float4* h_av) {
+                         const float4* h_fmax, const uint8_t* h_fast) {
     uint32_t nmoved = 0;
     for (uint32_t s = 0; s < w.ccomp.n_enabled; s++) {
         const uint32_t r = w.c0 + s;
@@ -1756,26 +1771,18 @@ void colliders_and_sleep(Group* g, WorldH& w, float dt, const uint8_t* h_moved, 
     w.stats.moved_colliders = nmoved;
     w.slept.clear();
     if (g->set.sleeping_enabled) {
-        // velocities by body id (rows in the device order before any body falls asleep)
-        std::vector<float4>& lv = w.sleep_lv;
-        std::vector<float4>& av = w.sleep_av;
-        lv.resize(w.nb);
-        av.resize(w.nb);
-        for (uint32_t s = 0; s < w.nb; s++) {
-            lv[size_t(w.dev_body_at[s])] = h_lv[w.b0 + s];
-            av[size_t(w.dev_body_at[s])] = h_av[w.b0 + s];
-        }
-        const float slv2 = g->set.sleep_linear_velocity * g->set.sleep_linear_velocity;
-        const float sav2 = g->set.sleep_angular_velocity * g->set.sleep_angular_velocity;
+        // the velocity condition by body id (world_sleep_fast, rows in the
+        // device order before any body falls asleep)
+        std::vector<uint8_t>& fast = w.sleep_fast;
+        fast.resize(w.nb);
+        for (uint32_t s = 0; s < w.nb; s++) fast[size_t(w.dev_body_at[s])] = h_fast[w.b0 + s];
         for (const IslandH& isl : w.islands) {
             float min_sleep = 3.40282347e+38f;
             for (uint32_t ib = isl.body_start; ib < isl.body_start + isl.body_count; ib++) {
                 const int b = w.isl_bodies[ib];
                 BodyH& B = w.bodies[size_t(b)];
                 if (B.type == RP3DG_BODY_STATIC) continue;
-                const float4 l = lv[size_t(b)], a = av[size_t(b)];
-                if (l.x * l.x + l.y * l.y + l.z * l.z > slv2 || a.x * a.x + a.y * a.y + a.z * a.z > sav2 ||
-                    !B.allowed_sleep) {
+                if (fast[size_t(b)] || !B.allowed_sleep) {
                     B.sleep_time = 0.0f;
                     min_sleep = 0.0f;
                 } else {
@@ -2292,7 +2299,7 @@ void destroy_group(Group* g) {
         g->cbuf[k].release();
     }
     cudaFree(g->bgrav); cudaFree(g->b_en); cudaFree(g->c_en); cudaFree(g->c_body); cudaFree(g->c_shape);
-    cudaFree(g->c_leaf); cudaFreeHost(g->t_cleaf); cudaFree(g->d_tree_rows);
+    cudaFree(g->c_leaf); cudaFreeHost(g->t_cleaf); cudaFree(g->d_tree_rows); cudaFree(g->d_fast);
     if (g->ev_step_copy) cudaEventDestroy(g->ev_step_copy);
     cudaFree(g->c_cat); cudaFree(g->c_mask); cudaFree(g->c_moved); cudaFree(g->pool); cudaFree(g->d_small);
     cudaFree(g->d_items); cudaFree(g->d_s1); cudaFree(g->d_s2); cudaFree(g->d_p1); cudaFree(g->d_r1);
@@ -3243,13 +3250,12 @@ int update_group(Group* g, float dt) {
     }
     mark(5);
     // ---- updateColliders: world AABBs, fat-AABB test, reinsertion flags
-    const size_t step_bytes = ((size_t(g->NC) + 15) & ~size_t(15)) + size_t(g->NC) * 32 + size_t(g->NB) * 32 + 64;
+    const size_t step_bytes = ((size_t(g->NC) + 15) & ~size_t(15)) + size_t(g->NC) * 32 + size_t(g->NB) + 64;
     if (host_grow(&g->h_step, &g->cap_hstep, step_bytes)) return wfail(g, RP3DG_ENOMEM, "cudaMallocHost(step)");
     uint8_t* h_moved = g->h_step;
     float4* h_fmin = reinterpret_cast<float4*>(g->h_step + ((size_t(g->NC) + 15) & ~size_t(15)));
     float4* h_fmax = h_fmin + g->NC;
-    float4* h_lv = h_fmax + g->NC;
-    float4* h_av = h_lv + g->NB;
+    uint8_t* h_fast = reinterpret_cast<uint8_t*>(h_fmax + g->NC);
     if (g->NC) {
         rp3dg_broadphase bp{};
         bp.n = g->NC;
@@ -3268,8 +3274,11 @@ int update_group(Group* g, float dt) {
         cudaMemcpyAsync(h_fmax, g->ccol[ccur][CC_FMAX], size_t(g->NC) * 16, cudaMemcpyDeviceToHost, st);
     }
     if (g->set.sleeping_enabled && g->NB) {
-        cudaMemcpyAsync(h_lv, g->bcol[bc][BC_LV], size_t(g->NB) * 16, cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(h_av, g->bcol[bc][BC_AV], size_t(g->NB) * 16, cudaMemcpyDeviceToHost, st);
+        if (dev_grow(&g->d_fast, &g->cap_fast, g->NB)) return wfail(g, RP3DG_ENOMEM, "cudaMalloc(sleep test)");
+        world_sleep_fast<<<blocks(g->NB), 128, 0, st>>>(
+            g->NB, g->bcol[bc][BC_LV], g->bcol[bc][BC_AV], g->set.sleep_linear_velocity * g->set.sleep_linear_velocity,
+            g->set.sleep_angular_velocity * g->set.sleep_angular_velocity, g->d_fast);
+        cudaMemcpyAsync(h_fast, g->d_fast, g->NB, cudaMemcpyDeviceToHost, st);
     }
     cudaError_t e;
     if (g->dev_tree && g->NC) {
@@ -3285,7 +3294,7 @@ int update_group(Group* g, float dt) {
     if (e != cudaSuccess) return wcuda(g, e, "step");
     mark(6);
     // ---- reinsertions and sleeping of every world
-    for_worlds(g, [&](int k) { colliders_and_sleep(g, g->worlds[size_t(k)], dt, h_moved, h_fmin, h_fmax, h_lv, h_av); });
+    for_worlds(g, [&](int k) { colliders_and_sleep(g, g->worlds[size_t(k)], dt, h_moved, h_fmin, h_fmax, h_fast); });
     // velocities / forces of bodies put to sleep (rows in the current device order)
     std::vector<int32_t> rows;
     for (WorldH& w : g->worlds) {
