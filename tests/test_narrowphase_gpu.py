@@ -197,6 +197,32 @@ def test_grazing_capsule_clip_matches_oracle(ctx, port_hulls):
         _assert_same(got, a, what="grazing capsules vs reference")
 
 
+def test_narrowphase_input_small_slots_and_empty_batches(ctx):
+    """rp3dg_narrowphase_input_host with batches of 4 and 8 contact slots per
+    pair, an empty batch and a batch with report_contacts off for half its
+    pairs: each batch's results equal those of rp3dg_narrowphase_host on it
+    (two calls, so the second copies the expected number of contacts)."""
+    sc = scenes.narrowphase_scene(total_pairs=7 * 3000, seed=77, hull=edgecases.load_hull())
+    ctx.set_shapes(sc.shapes)
+    for call in range(2):
+        batches, refs = [], []
+        for k, (name, (algo, pairs)) in enumerate(sc.batches.items()):
+            n = 0 if k == 2 else pairs.n
+            pr = pairs.slice(0, n)
+            if k == 4:
+                pr.report = (np.arange(n) % 2).astype(np.uint8)
+            mc = (4, 8, 16)[k % 3]
+            exp = ctx.narrowphase_host(algo, pr.slice(0, n), A.HostContacts(n, mc)) if n else None
+            batches.append((algo, pr, A.HostContacts(n, mc)))
+            refs.append(exp)
+        got = ctx.narrowphase_input_host(batches)
+        for (algo, pr, _), g, exp in zip(batches, got, refs):
+            if exp is None:
+                assert g.n == 0
+                continue
+            _assert_same(g, exp, what=f"algo {algo} slots {g.max_contacts} call {call}")
+
+
 @pytest.mark.parametrize("pinned", [False, True])
 def test_narrowphase_input_matches_per_batch_calls(ctx, pinned):
     """rp3dg_narrowphase_input_host (all batches overlapped, contacts packed
