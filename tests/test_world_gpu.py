@@ -8,6 +8,7 @@ import os
 import numpy as np
 import pytest
 
+import rayio
 import reflib
 import worldio
 from reactphysics3d_b200 import _abi as A
@@ -58,6 +59,35 @@ def test_box_pile_1000_matches_reference_live(ctx):
     for a, b in zip(w.bodies(), r.bodies()):
         assert np.array_equal(a, b)
     assert w.bodies()[4].sum() > 0      # some boxes asleep after 5 s
+    w.close()
+
+
+@pytest.mark.skipif(not reflib.have_ref("f32"), reason="reference engine not built")
+def test_single_world_with_device_tree_matches_reference(ctx):
+    """A single world switched to a device tree (one GPU thread replaying
+    all its reinsertions) and back to the host tree mid-run: the 1,000-box
+    pile's pairs, manifolds and states stay bit-identical to the reference,
+    and world raycasts (which copy the device tree back) hit what the
+    reference hits."""
+    sc = scenes.box_pile()
+    w, r = engine.World(ctx, sc), reflib.RefScene(sc)
+    assert not w.device_trees
+    w.set_device_trees(True)
+    rays = scenes.world_rays(3000, (-12, -0.5, -12), (12, 12, 12), seed=8, masks=(0xFFFF,))
+    for s in range(160):
+        if s == 120:
+            w.set_device_trees(False)
+        w.update(float(worldio.DT))
+        r.update(float(worldio.DT))
+        if s % 40 == 39:
+            assert np.array_equal(w.pairs(), r.pairs()), s
+            for a, b in zip(w.contacts(), r.contacts()):
+                assert np.array_equal(a, b), s
+            hw, nw = w.raycast(rays, A.RAYCAST_ALL, 4)
+            hr, nr = r.raycast(rays, A.RAYCAST_ALL, 4)
+            assert rayio.same_hits((hw, nw), (hr, nr)), s
+    for a, b in zip(w.bodies(), r.bodies()):
+        assert np.array_equal(a, b)
     w.close()
 
 
