@@ -555,7 +555,6 @@ struct BodyH {
     float sleep_time = 0.0f;
     int island = -1;               // island of this step (non-static bodies)
     std::vector<int> colliders;
-    std::vector<uint32_t> contact_pairs;
     std::vector<int> joints;       // RigidBodyComponents::mJoints (creation order)
 };
 struct JointH {
@@ -787,6 +786,7 @@ struct WorldH {
     std::vector<uint32_t> isl_jstart, isl_jcount;
     std::vector<int2> jvisit;                  // scratch: (joint, island) in visiting order
     std::vector<int> dfs_stack, dfs_statics;   // scratch of the island search
+    std::vector<uint32_t> cp_start, cp_list, cp_fill;   // this step's contact pairs by body (see contacts_and_islands)
     std::vector<uint32_t> jfill;               // scratch: next slot of each island's joints
     uint32_t jl_base = 0;
     // islands with joints (group island index), their enabled non-static
@@ -1548,9 +1548,24 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
         if (p.coll_prev && !p.coll_curr) add_lost(w, p);
     for (const PairH& p : w.concave)
         if (p.coll_prev && !p.coll_curr) add_lost(w, p);
-    for (uint32_t p = 0; p < w.cpairs.size(); p++) {
-        w.bodies[size_t(w.cpairs[p].b1)].contact_pairs.push_back(p);
-        w.bodies[size_t(w.cpairs[p].b2)].contact_pairs.push_back(p);
+    // each body's contact pairs in creation order (RigidBodyComponents'
+    // contact pair lists), as one array per world: body b's are
+    // cp_list[cp_start[b], cp_start[b + 1])
+    {
+        std::vector<uint32_t>& cs = w.cp_start;
+        cs.assign(w.bodies.size() + 1, 0);
+        for (const ContactPairH& c : w.cpairs) {
+            cs[size_t(c.b1) + 1]++;
+            cs[size_t(c.b2) + 1]++;
+        }
+        for (size_t b = 0; b < w.bodies.size(); b++) cs[b + 1] += cs[b];
+        w.cp_list.resize(2 * w.cpairs.size());
+        std::vector<uint32_t>& fill = w.cp_fill;
+        fill.assign(cs.begin(), cs.end() - 1);
+        for (uint32_t p = 0; p < w.cpairs.size(); p++) {
+            w.cp_list[fill[size_t(w.cpairs[p].b1)]++] = p;
+            w.cp_list[fill[size_t(w.cpairs[p].b2)]++] = p;
+        }
     }
     w.island_order.clear();
     w.islands.clear();
@@ -1587,7 +1602,8 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
                 continue;
             }
             w.bodies[size_t(b)].island = int(isl_index);
-            for (uint32_t cpi : w.bodies[size_t(b)].contact_pairs) {
+            for (uint32_t k = w.cp_start[size_t(b)]; k < w.cp_start[size_t(b) + 1]; k++) {
+                const uint32_t cpi = w.cp_list[k];
                 ContactPairH& cp = w.cpairs[cpi];
                 if (cp.in_island) continue;
                 cp.in_island = true;
@@ -1616,10 +1632,6 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
         }
         for (int sb : statics) w.bodies[size_t(sb)].in_island = false;
         statics.clear();
-    }
-    for (auto& cp : w.cpairs) {
-        w.bodies[size_t(cp.b1)].contact_pairs.clear();
-        w.bodies[size_t(cp.b2)].contact_pairs.clear();
     }
     w.nm = total_manifolds;
     w.np = 0;
