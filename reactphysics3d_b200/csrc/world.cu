@@ -550,10 +550,8 @@ struct BodyH {
     int type = RP3DG_BODY_DYNAMIC;
     bool sleeping = false;
     bool allowed_sleep = true;
-    bool in_island = false;
     bool has_sim_collider = false;
     float sleep_time = 0.0f;
-    int island = -1;               // island of this step (non-static bodies)
     std::vector<int> colliders;
     std::vector<int> joints;       // RigidBodyComponents::mJoints (creation order)
 };
@@ -787,6 +785,8 @@ struct WorldH {
     std::vector<int2> jvisit;                  // scratch: (joint, island) in visiting order
     std::vector<int> dfs_stack, dfs_statics;   // scratch of the island search
     std::vector<uint32_t> cp_start, cp_list, cp_fill;   // this step's contact pairs by body (see contacts_and_islands)
+    std::vector<uint8_t> b_in_island;          // the island search's marks by body id
+    std::vector<int> b_island;                 // this step's island of each non-static body (-1: none)
     std::vector<uint32_t> jfill;               // scratch: next slot of each island's joints
     uint32_t jl_base = 0;
     // islands with joints (group island index), their enabled non-static
@@ -1570,10 +1570,12 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
     w.island_order.clear();
     w.islands.clear();
     w.isl_bodies.clear();
-    for (auto& B : w.bodies) {
-        B.in_island = false;
-        B.island = -1;
-    }
+    // the search's per-body marks, in arrays of their own (cheaper to reset
+    // and to test than the body records)
+    std::vector<uint8_t>& in_island = w.b_in_island;
+    std::vector<int>& island_of = w.b_island;
+    in_island.assign(w.bodies.size(), 0);
+    island_of.assign(w.bodies.size(), -1);
     for (auto& J : w.joints) J.in_island = false;
     uint32_t total_manifolds = 0;
     std::vector<int>& stack = w.dfs_stack;
@@ -1581,10 +1583,10 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
     statics.clear();
     for (uint32_t s = 0; s < w.bcomp.n_enabled; s++) {
         const int b0 = w.bcomp.at[s];
-        if (w.bodies[size_t(b0)].in_island) continue;
+        if (in_island[size_t(b0)]) continue;
         if (w.bodies[size_t(b0)].type == RP3DG_BODY_STATIC) continue;
         stack.clear();
-        w.bodies[size_t(b0)].in_island = true;
+        in_island[size_t(b0)] = true;
         stack.push_back(b0);
         IslandH isl;
         isl.manifold_start = total_manifolds;
@@ -1601,7 +1603,7 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
                 statics.push_back(b);
                 continue;
             }
-            w.bodies[size_t(b)].island = int(isl_index);
+            island_of[size_t(b)] = int(isl_index);
             for (uint32_t k = w.cp_start[size_t(b)]; k < w.cp_start[size_t(b) + 1]; k++) {
                 const uint32_t cpi = w.cp_list[k];
                 ContactPairH& cp = w.cpairs[cpi];
@@ -1614,9 +1616,9 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
                     w.island_order.push_back(cpi);
                     total_manifolds += cp.nman;
                     w.islands[isl_index].manifold_count += cp.nman;
-                    if (w.bodies[size_t(other)].in_island) continue;
+                    if (in_island[size_t(other)]) continue;
                     stack.push_back(other);
-                    w.bodies[size_t(other)].in_island = true;
+                    in_island[size_t(other)] = 1;
                 }
             }
             // the body's joints (PhysicsWorld.cpp:822-844)
@@ -1625,12 +1627,12 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
                 if (J.in_island) continue;
                 J.in_island = true;
                 const int other = J.b1 == b ? J.b2 : J.b1;
-                if (w.bodies[size_t(other)].in_island) continue;
+                if (in_island[size_t(other)]) continue;
                 stack.push_back(other);
-                w.bodies[size_t(other)].in_island = true;
+                in_island[size_t(other)] = true;
             }
         }
-        for (int sb : statics) w.bodies[size_t(sb)].in_island = false;
+        for (int sb : statics) in_island[size_t(sb)] = 0;
         statics.clear();
     }
     w.nm = total_manifolds;
@@ -1662,8 +1664,8 @@ void contacts_and_islands(Group* g, WorldH& w, const uint8_t* h_coll, const uint
             for (uint32_t s = 0; s < cmp->n_enabled; s++) {
                 const int j = cmp->at[s];
                 const JointH& J = w.joints[size_t(j)];
-                const int isl = w.bodies[size_t(J.b1)].type != RP3DG_BODY_STATIC ? w.bodies[size_t(J.b1)].island
-                                                                                  : w.bodies[size_t(J.b2)].island;
+                const int isl = w.bodies[size_t(J.b1)].type != RP3DG_BODY_STATIC ? w.b_island[size_t(J.b1)]
+                                                                                  : w.b_island[size_t(J.b2)];
                 if (isl >= 0) {
                     jv.push_back(make_int2(j, isl));
                     w.isl_jcount[size_t(isl)]++;
