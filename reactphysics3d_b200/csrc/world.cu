@@ -742,6 +742,13 @@ struct ContactBuf {
     }
 };
 
+// A tree leaf's collider as the broad phase's candidate filter reads it
+// (its body, collision category and mask never change after creation).
+struct LeafInfo {
+    int32_t body = -1;
+    uint16_t category = 0, mask = 0;
+};
+
 // One world's order bookkeeping (host) and its rows in the group's arrays.
 struct WorldH {
     uint32_t nb = 0, nc = 0, b0 = 0, c0 = 0;  // bodies at rows [b0, b0 + nb), colliders [c0, c0 + nc)
@@ -755,6 +762,7 @@ struct WorldH {
     // takes the next value of this clock (ColliderH::moved_at, PairH::reset_at)
     uint64_t clock = 0;
     std::vector<int> bp_to_collider;
+    std::vector<LeafInfo> leaf_info;   // by tree leaf: what the broad phase's pair filter reads of its collider
     // overlapping pairs (OverlappingPairs::mConvexPairs / mDisabledConvexPairs,
     // mConcavePairs / mDisabledConcavePairs)
     std::vector<PairH> pairs, disabled, concave, concave_dis;
@@ -1342,10 +1350,9 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
     // a candidate pair of the queries: 0 filtered out, 1 an existing pair, 2 new
     auto classify = [&](int32_t s, int leaf, PairH** found) -> uint8_t {
         if (leaf == s) return 0;
-        const int c1 = w.bp_to_collider[size_t(s)], c2 = w.bp_to_collider[size_t(leaf)];
-        const ColliderH &C1 = w.colliders[size_t(c1)], &C2 = w.colliders[size_t(c2)];
-        if (C1.body == C2.body) return 0;
-        if (!w.nocollide.empty() && w.nocollide.find(body_pair_key(C1.body, C2.body))) return 0;
+        const LeafInfo &L1 = w.leaf_info[size_t(s)], &L2 = w.leaf_info[size_t(leaf)];
+        if (L1.body == L2.body) return 0;
+        if (!w.nocollide.empty() && w.nocollide.find(body_pair_key(L1.body, L2.body))) return 0;
         *found = find_pair(w, pair_number(uint32_t(std::max(s, leaf)), uint32_t(std::min(s, leaf))));
         return *found ? 1 : 2;
     };
@@ -2672,6 +2679,14 @@ int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds
                 if (size_t(id) >= w.bp_to_collider.size()) w.bp_to_collider.resize(size_t(id) + 1, -1);
                 w.bp_to_collider[size_t(id)] = c;
                 w.moved.add(id);
+            }
+            // the filter fields of each leaf's collider, side by side
+            w.leaf_info.assign(w.bp_to_collider.size(), LeafInfo{});
+            for (size_t id = 0; id < w.bp_to_collider.size(); id++) {
+                const int c = w.bp_to_collider[id];
+                if (c < 0) continue;
+                const ColliderH& C = w.colliders[size_t(c)];
+                w.leaf_info[id] = LeafInfo{C.body, C.category, C.mask};
             }
         }
         // the row tables now hold each collider's tree leaf at the next sync
