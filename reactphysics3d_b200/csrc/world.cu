@@ -571,7 +571,6 @@ struct ColliderH {
     uint16_t category = 1, mask = 0xffff;
     bool trigger = false;  // Collider::setIsTrigger: not a simulation collider
     std::vector<uint64_t> pairs;  // ColliderComponents::mOverlappingPairs
-    uint64_t moved_at = 0;        // the world clock when it last joined the moved set
 };
 struct PairH {
     uint64_t id = 0;
@@ -759,8 +758,9 @@ struct WorldH {
     rp3dg::order::IdSet moved;
     // askForBroadPhaseCollisionCheck marks every pair of a moved collider for
     // the overlap test; instead of visiting them, each mark and each clear
-    // takes the next value of this clock (ColliderH::moved_at, PairH::reset_at)
+    // takes the next value of this clock (moved_at, PairH::reset_at)
     uint64_t clock = 0;
+    std::vector<uint64_t> moved_at;    // by collider id: the clock when it last joined the moved set
     std::vector<int> bp_to_collider;
     std::vector<LeafInfo> leaf_info;   // by tree leaf: what the broad phase's pair filter reads of its collider
     // overlapping pairs (OverlappingPairs::mConvexPairs / mDisabledConvexPairs,
@@ -1197,12 +1197,12 @@ void enable_pair(Group* g, WorldH& w, uint64_t id) {
 // BroadPhaseSystem::addMovedCollider + notifyOverlappingPairsToTestOverlap
 void add_moved(WorldH& w, int c) {
     w.moved.add(w.colliders[size_t(c)].bp);
-    w.colliders[size_t(c)].moved_at = ++w.clock;
+    w.moved_at[size_t(c)] = ++w.clock;
 }
 
 // OverlappingPair::needToTestOverlap
 bool need_test(const WorldH& w, const PairH& p) {
-    return w.colliders[size_t(p.c1)].moved_at > p.reset_at || w.colliders[size_t(p.c2)].moved_at > p.reset_at;
+    return w.moved_at[size_t(p.c1)] > p.reset_at || w.moved_at[size_t(p.c2)] > p.reset_at;
 }
 
 // PhysicsWorld::setBodyDisabled (PhysicsWorld.cpp:168-186)
@@ -2680,6 +2680,7 @@ int create_group(rp3dg_ctx* ctx, const rp3dg_world_settings* s, uint32_t nworlds
                 w.bp_to_collider[size_t(id)] = c;
                 w.moved.add(id);
             }
+            w.moved_at.assign(w.colliders.size(), 0);
             // the filter fields of each leaf's collider, side by side
             w.leaf_info.assign(w.bp_to_collider.size(), LeafInfo{});
             for (size_t id = 0; id < w.bp_to_collider.size(); id++) {
