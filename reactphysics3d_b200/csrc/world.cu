@@ -1425,6 +1425,8 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
     const auto t1 = g->profiling ? clk::now() : clk::time_point();
     // removeNonOverlappingPairs; a pair removed while it was colliding in
     // the previous frame becomes a lost contact pair (addLostContactPair)
+    // (collidingInPreviousFrame is the last step's coll_curr here: it moves
+    // into coll_prev in the item loops below)
     w.lost.clear();
     for (uint64_t i = 0; i < w.pairs.size(); i++) {
         PairH& p = w.pairs[i];
@@ -1432,7 +1434,7 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
         if (rp3dg::order::overlap(w.tree.nodes[size_t(p.bp1)].box, w.tree.nodes[size_t(p.bp2)].box)) {
             p.reset_at = ++w.clock;
         } else {
-            if (p.coll_prev) add_lost(w, p);
+            if (p.coll_curr) add_lost(w, p);
             remove_pair(w, uint32_t(i));
             i--;
         }
@@ -1443,7 +1445,7 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
         if (rp3dg::order::overlap(w.tree.nodes[size_t(p.bp1)].box, w.tree.nodes[size_t(p.bp2)].box)) {
             p.reset_at = ++w.clock;
         } else {
-            if (p.coll_prev) add_lost(w, p);
+            if (p.coll_curr) add_lost(w, p);
             remove_concave_pair(w, uint32_t(i));
             i--;
         }
@@ -1455,9 +1457,13 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
         w.hitems[a].clear();
         w.hitem_pair[a].clear();
     }
-    // rows in the order the device will have after this step's row sync
+    // rows in the order the device will have after this step's row sync;
+    // each pair's collidingInPreviousFrame is its last step's flag (for the
+    // enabled pairs, which are the ones the reference updates at the end of
+    // a step; a disabled pair keeps both flags as they were)
     for (uint32_t i = 0; i < w.pairs.size(); i++) {
         PairH& p = w.pairs[i];
+        p.coll_prev = p.coll_curr;
         p.coll_curr = false;
         const bool e1 = w.ccomp.enabled(p.c1), e2 = w.ccomp.enabled(p.c2);
         if (!(e1 || e2)) continue;
@@ -1472,6 +1478,7 @@ void broad_and_middle_phase(Group* g, WorldH& w) {
     // not tested this step loses its per-triangle records
     for (uint32_t i = 0; i < w.concave.size(); i++) {
         PairH& p = w.concave[i];
+        p.coll_prev = p.coll_curr;
         p.coll_curr = false;
         const bool e1 = w.ccomp.enabled(p.c1), e2 = w.ccomp.enabled(p.c2);
         if (!(e1 || e2)) {
@@ -1816,9 +1823,7 @@ void colliders_and_sleep(Group* g, WorldH& w, float dt, const uint8_t* h_moved, 
                     set_sleeping(g, w, w.isl_bodies[ib], true);
         }
     }
-    // collidingInPreviousFrame for the next step
-    for (auto& p : w.pairs) p.coll_prev = p.coll_curr;
-    for (auto& p : w.concave) p.coll_prev = p.coll_curr;
+    // (collidingInPreviousFrame moves at the next step's item loops)
     w.prev_cpairs.swap(w.cpairs);
     w.stats.disabled_pairs = uint32_t(w.disabled.size() + w.concave_dis.size());
     w.stats.enabled_bodies = w.bcomp.n_enabled;
